@@ -1,0 +1,118 @@
+/*
+ * qbxfmm.h -- C ABI of the B200 QBX-FMM layer-potential apply.
+ *
+ * The entry points replace the expansion-wrangler stages that pytential's FMM
+ * driver calls (pytential/qbx/fmm.py:414-594), one per stage, plus a whole-apply
+ * entry.  All array arguments are plain pointers.  Device pointers are owned by the
+ * caller; the library allocates no device memory.  Every call returns QBXFMM_OK or
+ * a negative status; QBXFMM_ERR_CUDA leaves the CUDA error in qbxfmm_last_error().
+ *
+ * Data layout (all int32 indices, float64 coordinates):
+ *   - coordinates are structure-of-arrays: x[dim][n];
+ *   - sources and targets are in tree order (boxtree's sorted order);
+ *   - strengths: [nrhs][nsources] in tree order, float64 for Laplace,
+ *     complex128 (interleaved re, im) for Helmholtz;
+ *   - box expansions (multipoles and locals): [nboxes][nrhs][ncoeff] complex128;
+ *   - QBX expansions: [ncenters][nrhs][ncoeff_qbx] complex128;
+ *   - potentials: [nrhs][n] float64 (Laplace) or complex128 (Helmholtz).
+ */
+#ifndef QBXFMM_H
+#define QBXFMM_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum qbxfmm_status {
+  QBXFMM_OK = 0,
+  QBXFMM_ERR_ARG = -1,          /* invalid argument (sizes, orders, null pointers) */
+  QBXFMM_ERR_CUDA = -2,         /* a CUDA runtime call failed */
+  QBXFMM_ERR_UNSUPPORTED = -3,  /* kernel family / order not built into this library */
+  QBXFMM_ERR_DEVICE = -4        /* a kernel reported an error word (bad list entry) */
+};
+
+enum qbxfmm_family { QBXFMM_LAPLACE = 0, QBXFMM_HELMHOLTZ = 1 };
+
+/* Which layer potential the sources carry.  The strength of each source is
+ * multiplied by charge_coeff for the single-layer part and by dipole_coeff (along
+ * the source normal) for the double-layer part, so S, D and D - i k S are one FMM
+ * (pytential groups source kernels with the same density the same way,
+ * pytential/qbx/__init__.py:526-532). */
+typedef struct qbxfmm_kernel {
+  int32_t family;            /* enum qbxfmm_family */
+  int32_t dim;               /* 2 or 3 */
+  double k_re, k_im;         /* Helmholtz wave number (ignored for Laplace) */
+  double charge_coeff_re, charge_coeff_im;
+  double dipole_coeff_re, dipole_coeff_im;
+  int32_t qbx_order;         /* order of the QBX local expansions */
+  int32_t fmm_order;         /* order of box multipole/local expansions */
+  int32_t nrhs;              /* number of densities applied in one traversal */
+  int32_t precision;         /* 0 = plain FP64, 1 = mixed (FP32 far field) */
+} qbxfmm_kernel;
+
+/* Tree, traversal and QBX geometry, field names after boxtree's Tree /
+ * FMMTraversalInfo and pytential's QBXFMMGeometryData
+ * (pytential/qbx/geometry.py:361-899).  All pointers address the same memory
+ * space (device memory for the CUDA library, host memory for the CPU checker). */
+typedef struct qbxfmm_geometry {
+  int32_t dim;
+  int32_t nboxes, nlevels, nsources, ntargets;
+  double root_extent;
+  const double* box_centers;                /* [dim][nboxes] */
+  const int32_t* box_levels;                /* [nboxes] */
+  const int32_t* box_parent_ids;            /* [nboxes], -1 at the root */
+  const int32_t* box_child_ids;             /* [2^dim][nboxes], 0 = no child */
+  const int32_t* box_source_starts;         /* [nboxes] */
+  const int32_t* box_source_counts_nonchild;
+  const int32_t* box_source_counts_cumul;
+  const double* sources;                    /* [dim][nsources], tree order */
+  const double* source_normals;             /* [dim][nsources], tree order */
+  const double* targets;                    /* [dim][ntargets], tree order */
+
+  int32_t nsource_boxes;
+  const int32_t* source_boxes;
+  const int32_t* level_start_source_box_nrs;           /* [nlevels+1] */
+  int32_t nsource_parent_boxes;
+  const int32_t* source_parent_boxes;
+  const int32_t* level_start_source_parent_box_nrs;    /* [nlevels+1] */
+  int32_t ntarget_boxes;
+  const int32_t* target_boxes;
+  int32_t nttp_boxes;                                  /* target_or_target_parent */
+  const int32_t* target_or_target_parent_boxes;
+  const int32_t* level_start_ttp_box_nrs;              /* [nlevels+1] */
+  const int32_t* list1_starts;   /* neighbor_source_boxes, by target box index */
+  const int32_t* list1_lists;
+  const int32_t* list2_starts;   /* from_sep_siblings, by ttp box index */
+  const int32_t* list2_lists;
+  const int32_t* list3_starts;   /* from_sep_smaller (all source levels), by target box index */
+  const int32_t* list3_lists;
+  const int32_t* list4_starts;   /* from_sep_bigger, by ttp box index */
+  const int32_t* list4_lists;
+
+  int32_t ncenters;
+  const double* centers;                    /* [dim][ncenters], interleaved -,+ */
+  const double* expansion_radii;            /* [ncenters] */
+  int32_t nglobal_qbx_centers;
+  const int32_t* global_qbx_centers;
+  const int32_t* qbx_center_to_target_box;  /* [ncenters] -> target box index */
+  const int32_t* center_to_targets_starts;  /* [ncenters+1] */
+  const int32_t* center_to_targets_lists;   /* tree target indices */
+
+  int32_t nfiltered_targets;                /* non-QBX targets */
+  const int32_t* nonqbx_box_target_starts;  /* [nboxes] into the filtered list */
+  const int32_t* nonqbx_box_target_counts_nonchild;
+  const double* nonqbx_targets;             /* [dim][nfiltered_targets] */
+  const int32_t* unfiltered_from_filtered_target_indices;
+  const int32_t* sorted_target_ids;         /* tree target -> user target */
+  const int32_t* user_source_ids;           /* tree source -> user source */
+
+  int32_t nuser_targets;                    /* user targets = ntargets - ncenters */
+} qbxfmm_geometry;
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* QBXFMM_H */

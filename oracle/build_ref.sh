@@ -1,0 +1,23 @@
+#!/usr/bin/env bash
+# Compile the reference's target-specific QBX module (pytential/qbx/target_specific:
+# impl.pyx + helmholtz_utils.c) from its sources into oracle/_ref/, as a CPU checker
+# for the 3D QBX near field.  Sources are read in place and never copied into the
+# repository; outputs go only to oracle/_ref/ (git-ignored).
+set -euo pipefail
+REF=${PYTENTIAL_REFERENCE:-/root/reference}
+SRC="$REF/pytential/qbx/target_specific"
+HERE="$(cd "$(dirname "$0")" && pwd)"
+OUT="$HERE/_ref"
+if [ ! -f "$SRC/impl.pyx" ]; then
+  echo "reference sources not found at $SRC" >&2
+  exit 1
+fi
+mkdir -p "$OUT/build"
+PY=${PYTHON:-python3}
+EXT=$($PY -c 'import sysconfig; print(sysconfig.get_config_var("EXT_SUFFIX"))')
+INC=$($PY -c 'import sysconfig; print(sysconfig.get_paths()["include"])')
+cython -3 "$SRC/impl.pyx" -o "$OUT/build/impl.c"
+/usr/bin/gcc -O2 -fopenmp -fPIC -shared -w -I"$INC" -I"$SRC" \
+  "$OUT/build/impl.c" "$SRC/helmholtz_utils.c" -o "$OUT/impl$EXT" -lm
+touch "$OUT/__init__.py"
+echo "built $OUT/impl$EXT"

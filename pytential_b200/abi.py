@@ -1,0 +1,181 @@
+"""ctypes mirror of ``include/qbxfmm.h`` and the host-side packing of geometry data.
+
+``geometry_arrays`` flattens a :class:`~pytential_b200.geometry.QBXFMMGeometryData`
+into the named, contiguous int32/float64 arrays the C ABI consumes; the same dict
+is uploaded once to the device (one tensor per entry) and its pointers are written
+into a :class:`QBXFMMGeometry` struct.
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+QBXFMM_LAPLACE = 0
+QBXFMM_HELMHOLTZ = 1
+
+QBXFMM_OK = 0
+QBXFMM_ERR_ARG = -1
+QBXFMM_ERR_CUDA = -2
+QBXFMM_ERR_UNSUPPORTED = -3
+QBXFMM_ERR_DEVICE = -4
+
+_i32 = ctypes.c_int32
+_f64 = ctypes.c_double
+_pi = ctypes.POINTER(ctypes.c_int32)
+_pd = ctypes.POINTER(ctypes.c_double)
+
+
+class QBXFMMKernel(ctypes.Structure):
+    _fields_ = [
+        ("family", _i32), ("dim", _i32),
+        ("k_re", _f64), ("k_im", _f64),
+        ("charge_coeff_re", _f64), ("charge_coeff_im", _f64),
+        ("dipole_coeff_re", _f64), ("dipole_coeff_im", _f64),
+        ("qbx_order", _i32), ("fmm_order", _i32), ("nrhs", _i32),
+        ("precision", _i32),
+    ]
+
+
+# (field name, kind) in declaration order; kind: "i" scalar int32, "d" scalar
+# float64, "pi"/"pd" pointers to int32/float64 arrays
+GEOMETRY_FIELDS = [
+    ("dim", "i"),
+    ("nboxes", "i"), ("nlevels", "i"), ("nsources", "i"), ("ntargets", "i"),
+    ("root_extent", "d"),
+    ("box_centers", "pd"), ("box_levels", "pi"), ("box_parent_ids", "pi"),
+    ("box_child_ids", "pi"),
+    ("box_source_starts", "pi"), ("box_source_counts_nonchild", "pi"),
+    ("box_source_counts_cumul", "pi"),
+    ("sources", "pd"), ("source_normals", "pd"), ("targets", "pd"),
+    ("nsource_boxes", "i"), ("source_boxes", "pi"), ("level_start_source_box_nrs", "pi"),
+    ("nsource_parent_boxes", "i"), ("source_parent_boxes", "pi"),
+    ("level_start_source_parent_box_nrs", "pi"),
+    ("ntarget_boxes", "i"), ("target_boxes", "pi"),
+    ("nttp_boxes", "i"), ("target_or_target_parent_boxes", "pi"),
+    ("level_start_ttp_box_nrs", "pi"),
+    ("list1_starts", "pi"), ("list1_lists", "pi"),
+    ("list2_starts", "pi"), ("list2_lists", "pi"),
+    ("list3_starts", "pi"), ("list3_lists", "pi"),
+    ("list4_starts", "pi"), ("list4_lists", "pi"),
+    ("ncenters", "i"), ("centers", "pd"), ("expansion_radii", "pd"),
+    ("nglobal_qbx_centers", "i"), ("global_qbx_centers", "pi"),
+    ("qbx_center_to_target_box", "pi"),
+    ("center_to_targets_starts", "pi"), ("center_to_targets_lists", "pi"),
+    ("nfiltered_targets", "i"), ("nonqbx_box_target_starts", "pi"),
+    ("nonqbx_box_target_counts_nonchild", "pi"), ("nonqbx_targets", "pd"),
+    ("unfiltered_from_filtered_target_indices", "pi"),
+    ("sorted_target_ids", "pi"), ("user_source_ids", "pi"),
+    ("nuser_targets", "i"),
+]
+
+_CT = {"i": _i32, "d": _f64, "pi": _pi, "pd": _pd}
+
+
+class QBXFMMGeometry(ctypes.Structure):
+    _fields_ = [(n, _CT[k]) for n, k in GEOMETRY_FIELDS]
+
+
+def _i(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _d(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def geometry_arrays(geo) -> tuple[dict, dict]:
+    """Return ``(scalars, arrays)`` for the C ABI from a geometry-data object."""
+    tree = geo.tree()
+    trav = geo.traversal()
+    nqbtl = geo.non_qbx_box_target_lists()
+    ctt = geo.center_to_tree_targets()
+    ti = geo.target_info()
+    arrays = {
+        "box_centers": _d(tree.box_centers),
+        "box_levels": _i(tree.box_levels),
+        "box_parent_ids": _i(tree.box_parent_ids),
+        "box_child_ids": _i(tree.box_child_ids),
+        "box_source_starts": _i(tree.box_source_starts),
+        "box_source_counts_nonchild": _i(tree.box_source_counts_nonchild),
+        "box_source_counts_cumul": _i(tree.box_source_counts_cumul),
+        "sources": _d(tree.sources),
+        "source_normals": _d(geo.tree_source_normals()),
+        "targets": _d(tree.targets),
+        "source_boxes": _i(trav.source_boxes),
+        "level_start_source_box_nrs": _i(trav.level_start_source_box_nrs),
+        "source_parent_boxes": _i(trav.source_parent_boxes),
+        "level_start_source_parent_box_nrs": _i(trav.level_start_source_parent_box_nrs),
+        "target_boxes": _i(trav.target_boxes),
+        "target_or_target_parent_boxes": _i(trav.target_or_target_parent_boxes),
+        "level_start_ttp_box_nrs": _i(trav.level_start_target_or_target_parent_box_nrs),
+        "list1_starts": _i(trav.neighbor_source_boxes_starts),
+        "list1_lists": _i(trav.neighbor_source_boxes_lists),
+        "list2_starts": _i(trav.from_sep_siblings_starts),
+        "list2_lists": _i(trav.from_sep_siblings_lists),
+        "list3_starts": _i(trav.from_sep_smaller_starts),
+        "list3_lists": _i(trav.from_sep_smaller_lists),
+        "list4_starts": _i(trav.from_sep_bigger_starts),
+        "list4_lists": _i(trav.from_sep_bigger_lists),
+        "centers": _d(geo.flat_centers()),
+        "expansion_radii": _d(geo.flat_expansion_radii()),
+        "global_qbx_centers": _i(geo.global_qbx_centers()),
+        "qbx_center_to_target_box": _i(geo.qbx_center_to_target_box()),
+        "center_to_targets_starts": _i(ctt.starts),
+        "center_to_targets_lists": _i(ctt.lists),
+        "nonqbx_box_target_starts": _i(nqbtl.box_target_starts),
+        "nonqbx_box_target_counts_nonchild": _i(nqbtl.box_target_counts_nonchild),
+        "nonqbx_targets": _d(nqbtl.targets),
+        "unfiltered_from_filtered_target_indices":
+            _i(nqbtl.unfiltered_from_filtered_target_indices),
+        "sorted_target_ids": _i(tree.sorted_target_ids),
+        "user_source_ids": _i(tree.user_source_ids),
+    }
+    scalars = {
+        "dim": tree.dimensions, "nboxes": tree.nboxes, "nlevels": tree.nlevels,
+        "nsources": tree.nsources, "ntargets": tree.ntargets,
+        "root_extent": float(tree.root_extent),
+        "nsource_boxes": len(trav.source_boxes),
+        "nsource_parent_boxes": len(trav.source_parent_boxes),
+        "ntarget_boxes": len(trav.target_boxes),
+        "nttp_boxes": len(trav.target_or_target_parent_boxes),
+        "ncenters": geo.ncenters,
+        "nglobal_qbx_centers": len(geo.global_qbx_centers()),
+        "nfiltered_targets": nqbtl.nfiltered_targets,
+        "nuser_targets": ti.ntargets - geo.ncenters,
+    }
+    # zero-length arrays still need a valid address
+    for k, v in arrays.items():
+        if v.size == 0:
+            arrays[k] = np.zeros(1, v.dtype)
+    return scalars, arrays
+
+
+def make_geometry_struct(scalars: dict, arrays: dict, ptr_of) -> QBXFMMGeometry:
+    """Fill a :class:`QBXFMMGeometry`; ``ptr_of(array)`` returns an integer address."""
+    g = QBXFMMGeometry()
+    for name, kind in GEOMETRY_FIELDS:
+        if kind in ("i", "d"):
+            setattr(g, name, scalars[name])
+        else:
+            typ = _CT[kind]
+            setattr(g, name, ctypes.cast(ctypes.c_void_p(ptr_of(arrays[name])), typ))
+    return g
+
+
+def make_kernel_struct(*, family, dim, qbx_order, fmm_order, nrhs=1, k=0.0,
+                       charge_coeff=0.0, dipole_coeff=0.0, precision=0) -> QBXFMMKernel:
+    k = complex(k)
+    cc = complex(charge_coeff)
+    dc = complex(dipole_coeff)
+    return QBXFMMKernel(family, dim, k.real, k.imag, cc.real, cc.imag, dc.real, dc.imag,
+                        qbx_order, fmm_order, nrhs, precision)
+
+
+def ncoeff(family: int, dim: int, order: int) -> int:
+    if family == QBXFMM_LAPLACE:
+        return (order + 1) * (order + 2) // 2 if dim == 3 else order + 1
+    if family == QBXFMM_HELMHOLTZ:
+        return (order + 1) ** 2 if dim == 3 else 2 * order + 1
+    raise ValueError(family)
