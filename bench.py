@@ -1,0 +1,323 @@
+#!/usr/bin/env python
+"""Benchmark: QBX-FMM node-applies/s on the 3D Laplace double-layer ellipsoid apply.
+
+Workload: ellipsoid (1, 1.5, 2) from an icosphere refined 3 times (1280 triangles),
+15 nodes per triangle (19200 nodes) upsampled to 45 (57600 sources), double
+layer, exterior limit on the surface plus 2000 targets in the shell
+2.5 <= r <= 3.5, qbx_order 3, fmm_order 10, float64.  node-applies = user
+targets x densities.  One step = one apply (upsample, weight, reorder, every FMM
+stage, assembly) with the density resident in HBM; the L2 cache (126 MB) is
+flushed between steps by writing a 256 MB buffer outside the per-step events.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+N > 1 (launched by torch.distributed.run): every rank applies its own density on
+its own GPU (weak scaling, no data-path collective); time is the max over ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "QBX-FMM node-applies/s at stated rel. err"
+UNIT = "node-applies/s"
+WORKLOAD = ("3D Laplace double-layer QBX apply, ellipsoid (1,1.5,2), icosphere-3 "
+            "(1280 tri), 19200 nodes -> 57600 sources, 19200 surface + 2000 shell "
+            "targets, qbx_order 3, fmm_order 10, FP64")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--nrefine", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def make_workload(nrefine, seed):
+    from pytential_b200.workloads import laplace3d_ellipsoid
+    return laplace3d_ellipsoid(nrefine=nrefine, op="D", seed=seed)
+
+
+def config_dict(wl, args, extra=None):
+    d = {"workload": WORKLOAD if args.nrefine == 3 else f"{wl.name} (reduced)",
+         "nodes": wl.discr.ndofs, "sources": wl.discr.nquad,
+         "user_targets": wl.nuser_targets, "nrhs": wl.nrhs,
+         "qbx_order": wl.qbx_order, "fmm_order": wl.fmm_order,
+         "l2": "flushed between steps (256 MB write)", "parallelism": f"replicas x{args.gpus}"}
+    if extra:
+        d.update(extra)
+    return d
+
+
+# {{{ clocks
+
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+
+    def summary(self):
+        if not self.lines:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except (ValueError, IndexError):
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+# }}}
+
+
+def cpu_reference(wl, reps, threads):
+    """The CPU checker's full apply (float64, OpenMP) on the host cores."""
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    from oracle.oracle import Oracle
+    sp = wl.spec
+    o = Oracle(wl.geometry(), dim=3, qbx_order=wl.qbx_order, fmm_order=wl.fmm_order,
+               nrhs=wl.nrhs, charge_coeff=sp.charge_coeff, dipole_coeff=sp.dipole_coeff)
+    s = wl.tree_strengths()
+    o.apply(s)   # warm (page-in, thread pool)
+    times = []
+    out = None
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        out = o.apply(s)
+        times.append(time.perf_counter() - t0)
+    return out, times
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    wl = make_workload(args.nrefine, seed=0)
+    _, times = cpu_reference(wl, max(args.steps, 1), threads)
+    t = statistics.mean(times)
+    value = wl.nuser_targets * wl.nrhs / t
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * t, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": config_dict(wl, args),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": "full apply of the workload per step (C/OpenMP float64 "
+                                   "restatement; the reference's pyopencl/sumpy apply is "
+                                   "not installable here)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_b200(args):
+    import torch
+    import torch.distributed as dist
+
+    from pytential_b200 import costs
+    from pytential_b200.fmm import QBXApply
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=dev)
+
+    wl = make_workload(args.nrefine, seed=rank)
+    geo = wl.geometry()
+    ap = QBXApply(geo, wl.spec, wl.qbx_order, wl.fmm_order, device=dev)
+    dens = torch.from_numpy(wl.density).to(dev)
+    out = ap.new_output()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    scal, arr = ap.dgeo.scalars, ap.dgeo.host_arrays
+    launches_per_step = costs.apply_launch_count(scal, arr)
+    pairs = costs.p2qbxl_pairs(arr, scal)
+    sp = wl.spec
+    fpp = costs.p2qbxl_flops_per_pair(3, wl.qbx_order, sp.charge_coeff != 0,
+                                      sp.dipole_coeff != 0)
+    node_applies = wl.nuser_targets * wl.nrhs
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for _ in range(max(args.warmup, 3)):
+        ap.apply_into(dens, out)
+    torch.cuda.synchronize()
+
+    K = args.steps
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(K)]
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for i in range(K):
+            flush.zero_()
+            ev[i][0].record()
+            ap.apply_into(dens, out)
+            ev[i][1].record()
+        torch.cuda.synchronize()
+    barrier()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    t_local = sum(step_ms) / 1e3
+    t_all = torch.tensor([t_local], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t_all, op=dist.ReduceOp.MAX)
+    t_max = float(t_all.item())
+    value = world * node_applies * K / t_max
+
+    # dominant kernel (P2QBXL) timed alone on the same stream, flushed L2
+    st = torch.cuda.current_stream()
+    import ctypes
+    kev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(K)]
+    ws = ap.ws
+    for i in range(K):
+        flush.zero_()
+        kev[i][0].record()
+        ap.plan.call("qbxfmm_form_global_qbx_locals", ctypes.c_void_p(ws.strengths),
+                     ctypes.c_void_p(ws.qbx_exps), ws.error_word,
+                     ctypes.c_void_p(st.cuda_stream))
+        kev[i][1].record()
+    torch.cuda.synchronize()
+    k_ms = statistics.mean(a.elapsed_time(b) for a, b in kev)
+    k_flops = pairs * fpp
+    fp64_peak = measure_fp64_peak(torch, dev)
+
+    # end to end through the public host-buffer entry (H2D + apply + D2H + sync)
+    ap.alloc_host_buffers()
+    ap.h_in.copy_(torch.from_numpy(wl.density))
+    for _ in range(3):
+        ap.apply_host()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(K):
+        ap.apply_host()
+    t_e2e = time.perf_counter() - t0
+    te = torch.tensor([t_e2e], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = world * node_applies * K / float(te.item())
+
+    res_gpu = ap.h_out.numpy().copy()
+    ap.check_error_word()
+
+    line = None
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
+            "warmup": max(args.warmup, 3), "ms_per_step": 1e3 * t_max / K,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (seeded analytic geometry and density)",
+            "config": config_dict(wl, args),
+            "roofline": {
+                "kernel": "P2QBXL (form_global_qbx_locals)", "bound": "fp64",
+                "achieved": k_flops / (k_ms * 1e-3) / 1e12,
+                "peak": fp64_peak, "unit": "TFLOP/s",
+                "frac": (k_flops / (k_ms * 1e-3) / 1e12) / fp64_peak,
+                "peak_source": "measured here: cuBLAS float64 GEMM 8192^3, best of 5",
+                "algorithmic_flops_per_launch": k_flops, "pairs": pairs,
+                "flops_per_pair": fpp, "kernel_ms": k_ms,
+                "share_of_step": k_ms / (1e3 * t_max / K), "traffic": None},
+            "e2e": {"value": e2e_value, "unit": UNIT,
+                    "h2d_bytes_per_step": ap.h2d_bytes, "d2h_bytes_per_step": ap.d2h_bytes},
+            "gpu_launches": launches_per_step * K,
+            "clocks": clk.summary(),
+        }
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    if world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        ref, times = cpu_reference(wl, 2, threads)
+        cpu_t = statistics.mean(times)
+        line["cpu_baseline"] = {
+            "value": node_applies / cpu_t, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": "2 full applies of the same workload (C/OpenMP float64 restatement)"}
+        line["rel_err_vs_fp64_oracle"] = float(np.abs(res_gpu - ref).max() / np.abs(ref).max())
+    print(json.dumps(line), flush=True)
+
+
+def measure_fp64_peak(torch, dev):
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    for _ in range(2):
+        torch.matmul(a, b)
+    best = 0.0
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        torch.cuda.synchronize()
+        best = max(best, 2 * n ** 3 / (s.elapsed_time(e) * 1e-3) / 1e12)
+    del a, b
+    return best
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

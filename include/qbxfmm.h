@@ -109,7 +109,42 @@ typedef struct qbxfmm_geometry {
   const int32_t* user_source_ids;           /* tree source -> user source */
 
   int32_t nuser_targets;                    /* user targets = ntargets - ncenters */
+
+  /* Work schedule for the QBX near-field kernels, derived from the lists above:
+   * global QBX centers grouped by target box, cut into chunks of at most
+   * QBXFMM_CENTER_CHUNK centers, ordered by decreasing list-1 work. */
+  int32_t nqbx_chunks;
+  const int32_t* qbx_chunk_target_box;      /* target box index per chunk */
+  const int32_t* qbx_chunk_start;           /* offset into centers_by_target_box */
+  const int32_t* qbx_chunk_count;
+  const int32_t* centers_by_target_box;     /* [nglobal_qbx_centers] */
 } qbxfmm_geometry;
+
+#define QBXFMM_CENTER_CHUNK 32
+
+/* Element-local upsampling of a stage-1 density to the quad-stage-2 sources and
+ * weighting by area element x quadrature weight
+ * (pytential/qbx/__init__.py:1075-1096), fused with the reorder into tree order
+ * (pytential/qbx/fmm.py:199-200). */
+typedef struct qbxfmm_upsample {
+  int32_t nelements;
+  int32_t nodes_per_element;       /* stage-1 */
+  int32_t quad_nodes_per_element;  /* quad stage 2 */
+  const double* matrix;            /* [quad_nodes_per_element][nodes_per_element] */
+  const double* quad_weights;      /* [nsources], user source order */
+} qbxfmm_upsample;
+
+/* Caller-owned device workspace for one apply (sizes for the kernel's orders and
+ * nrhs; see qbxfmm_workspace_sizes). */
+typedef struct qbxfmm_workspace {
+  void* strengths;    /* [nrhs][nsources] tree order */
+  void* mpoles;       /* [nboxes][nrhs][ncoeff(fmm_order)] complex128 */
+  void* locals;       /* [nboxes][nrhs][ncoeff(fmm_order)] complex128 */
+  void* qbx_exps;     /* [ncenters][nrhs][ncoeff(qbx_order)] complex128 */
+  void* pot_nonqbx;   /* [nrhs][nfiltered_targets] */
+  void* pot_tree;     /* [nrhs][ntargets] */
+  int32_t* error_word;/* one int32, set by kernels that meet an out-of-range index */
+} qbxfmm_workspace;
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,109 @@
+/*
+ * qbxfmm_api.h -- entry points of libqbxfmm.so.
+ *
+ * Each stage entry replaces one method of pytential's QBX expansion wrangler
+ * (the sumpy-backed QBXExpansionWrangler, pytential/qbx/fmm.py:118-396, and the
+ * SumpyExpansionWrangler methods it inherits) as called by drive_fmm
+ * (pytential/qbx/fmm.py:414-594).  Outputs are accumulated (+=) into caller-owned
+ * device buffers, so a caller can reproduce the driver's "new array per stage, then
+ * sum" semantics by passing zeroed buffers, or let stages accumulate in place.
+ * All calls are asynchronous on `stream` (a cudaStream_t, NULL = legacy default
+ * stream) except qbxfmm_plan_create and qbxfmm_apply_host.
+ */
+#ifndef QBXFMM_API_H
+#define QBXFMM_API_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "qbxfmm.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct qbxfmm_plan qbxfmm_plan;
+
+int qbxfmm_version(void);
+/* message of the last failing call on this host thread */
+const char* qbxfmm_last_error(void);
+
+/* Validate kernel + geometry and copy the per-level box ranges to the host.
+ * Replaces the wrangler constructor (pytential/qbx/fmm.py:141-170) and the
+ * backend dispatch in QBXLayerPotentialSource._tree_indep_data_for_wrangler
+ * (pytential/qbx/__init__.py:617-659). */
+int qbxfmm_plan_create(const qbxfmm_kernel* kernel, const qbxfmm_geometry* geometry,
+                       qbxfmm_plan** plan);
+int qbxfmm_plan_destroy(qbxfmm_plan* plan);
+
+/* byte sizes of the six workspace buffers, in qbxfmm_workspace field order */
+int qbxfmm_workspace_sizes(const qbxfmm_plan* plan, size_t* sizes6);
+
+/* get_flat_strengths_from_densities + reorder_sources
+ * (pytential/qbx/__init__.py:1075-1096; pytential/qbx/fmm.py:199-200).
+ * density: [nrhs][nelements * nodes_per_element] stage-1, element-major. */
+int qbxfmm_form_strengths(const qbxfmm_plan* plan, const qbxfmm_upsample* up,
+                          const void* density, void* strengths, void* stream);
+
+/* form_multipoles (P2M; pytential/qbx/fmm.py:441-445) */
+int qbxfmm_form_multipoles(const qbxfmm_plan* plan, const void* strengths, void* mpoles,
+                           void* stream);
+/* coarsen_multipoles (M2M; pytential/qbx/fmm.py:451-455) */
+int qbxfmm_coarsen_multipoles(const qbxfmm_plan* plan, void* mpoles, void* stream);
+/* eval_direct (P2P over list 1 at non-QBX targets; pytential/qbx/fmm.py:461-466) */
+int qbxfmm_eval_direct(const qbxfmm_plan* plan, const void* strengths, void* pot_nonqbx,
+                       int32_t* error_word, void* stream);
+/* multipole_to_local (M2L over list 2; pytential/qbx/fmm.py:472-478) */
+int qbxfmm_multipole_to_local(const qbxfmm_plan* plan, const void* mpoles, void* locals,
+                              int32_t* error_word, void* stream);
+/* eval_multipoles (M2P over list 3 at non-QBX targets; pytential/qbx/fmm.py:487-493) */
+int qbxfmm_eval_multipoles(const qbxfmm_plan* plan, const void* mpoles, void* pot_nonqbx,
+                           int32_t* error_word, void* stream);
+/* form_locals (P2L over list 4; pytential/qbx/fmm.py:502-510) */
+int qbxfmm_form_locals(const qbxfmm_plan* plan, const void* strengths, void* locals,
+                       int32_t* error_word, void* stream);
+/* refine_locals (L2L; pytential/qbx/fmm.py:519-523) */
+int qbxfmm_refine_locals(const qbxfmm_plan* plan, void* locals, void* stream);
+/* eval_locals (L2P at non-QBX targets; pytential/qbx/fmm.py:529-535) */
+int qbxfmm_eval_locals(const qbxfmm_plan* plan, const void* locals, void* pot_nonqbx,
+                       void* stream);
+/* form_global_qbx_locals (P2QBXL; pytential/qbx/fmm.py:231-265,
+ * pytential/qbx/interactions.py:40-167) */
+int qbxfmm_form_global_qbx_locals(const qbxfmm_plan* plan, const void* strengths,
+                                  void* qbx_exps, int32_t* error_word, void* stream);
+/* translate_box_multipoles_to_qbx_local (M2QBXL, all source levels in one launch;
+ * pytential/qbx/fmm.py:267-312, pytential/qbx/interactions.py:174-294) */
+int qbxfmm_translate_box_multipoles_to_qbx_local(const qbxfmm_plan* plan, const void* mpoles,
+                                                 void* qbx_exps, int32_t* error_word,
+                                                 void* stream);
+/* translate_box_local_to_qbx_local (L2QBXL, all levels in one launch;
+ * pytential/qbx/fmm.py:314-356, pytential/qbx/interactions.py:301-412) */
+int qbxfmm_translate_box_local_to_qbx_local(const qbxfmm_plan* plan, const void* locals,
+                                            void* qbx_exps, void* stream);
+/* eval_qbx_expansions (QBXL2P; pytential/qbx/fmm.py:358-389,
+ * pytential/qbx/interactions.py:419-532); writes pot_tree entries of QBX targets */
+int qbxfmm_eval_qbx_expansions(const qbxfmm_plan* plan, const void* qbx_exps, void* pot_tree,
+                               void* stream);
+/* potential assembly: scatter the non-QBX part, add the QBX part, reorder to user
+ * targets, apply the kernel scaling (pytential/qbx/fmm.py:569-588,
+ * pytential/qbx/__init__.py:775-793).  out: [nrhs][nuser_targets] (written). */
+int qbxfmm_assemble(const qbxfmm_plan* plan, const void* pot_nonqbx, const void* pot_tree,
+                    void* out, void* stream);
+
+/* The whole apply in drive_fmm's order, from the stage-1 density to user-order
+ * potentials; clears the workspace first.  Graph-capturable (no host syncs). */
+int qbxfmm_apply(const qbxfmm_plan* plan, const qbxfmm_upsample* up,
+                 const qbxfmm_workspace* ws, const void* density, void* out, void* stream);
+
+/* End-to-end apply from host buffers: copies the density host->device, applies,
+ * copies the potentials device->host, synchronizes, and checks the error word.
+ * Pinned host buffers give asynchronous copies. */
+int qbxfmm_apply_host(const qbxfmm_plan* plan, const qbxfmm_upsample* up,
+                      const qbxfmm_workspace* ws, const void* density_host, void* out_host,
+                      void* density_dev, void* out_dev, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* QBXFMM_API_H */

@@ -68,13 +68,64 @@ GEOMETRY_FIELDS = [
     ("unfiltered_from_filtered_target_indices", "pi"),
     ("sorted_target_ids", "pi"), ("user_source_ids", "pi"),
     ("nuser_targets", "i"),
+    ("nqbx_chunks", "i"), ("qbx_chunk_target_box", "pi"), ("qbx_chunk_start", "pi"),
+    ("qbx_chunk_count", "pi"), ("centers_by_target_box", "pi"),
 ]
+
+CENTER_CHUNK = 32
 
 _CT = {"i": _i32, "d": _f64, "pi": _pi, "pd": _pd}
 
 
 class QBXFMMGeometry(ctypes.Structure):
     _fields_ = [(n, _CT[k]) for n, k in GEOMETRY_FIELDS]
+
+
+class QBXFMMUpsample(ctypes.Structure):
+    _fields_ = [("nelements", _i32), ("nodes_per_element", _i32),
+                ("quad_nodes_per_element", _i32), ("matrix", _pd), ("quad_weights", _pd)]
+
+
+class QBXFMMWorkspace(ctypes.Structure):
+    _fields_ = [("strengths", ctypes.c_void_p), ("mpoles", ctypes.c_void_p),
+                ("locals", ctypes.c_void_p), ("qbx_exps", ctypes.c_void_p),
+                ("pot_nonqbx", ctypes.c_void_p), ("pot_tree", ctypes.c_void_p),
+                ("error_word", _pi)]
+
+
+def qbx_center_schedule(global_qbx_centers, qbx_center_to_target_box, list1_starts,
+                        list1_lists, box_source_counts_nonchild, chunk: int = CENTER_CHUNK):
+    """Global QBX centers grouped by target box and cut into chunks of at most
+    ``chunk`` centers, ordered by decreasing list-1 work (centers x sources).
+
+    Returns ``(chunk_target_box, chunk_start, chunk_count, centers_by_target_box)``.
+    """
+    gc = np.asarray(global_qbx_centers, np.int64)
+    c2tb = np.asarray(qbx_center_to_target_box, np.int64)
+    if len(gc) == 0:
+        z = np.zeros(0, np.int32)
+        return z, z, z, z
+    tb = c2tb[gc]
+    order = np.lexsort((gc, tb))
+    cbt = gc[order]
+    tbs = tb[order]
+    cnt = np.asarray(box_source_counts_nonchild)[np.asarray(list1_lists)]
+    csum = np.concatenate([[0], np.cumsum(cnt)])
+    l1s = np.asarray(list1_starts)
+    nsrc = csum[l1s[1:]] - csum[l1s[:-1]]
+    boxes, first, counts = np.unique(tbs, return_index=True, return_counts=True)
+    ch_tb, ch_start, ch_count = [], [], []
+    for b, f, c in zip(boxes, first, counts):
+        for off in range(0, c, chunk):
+            ch_tb.append(b)
+            ch_start.append(f + off)
+            ch_count.append(min(chunk, c - off))
+    ch_tb = np.array(ch_tb, np.int64)
+    ch_count = np.array(ch_count, np.int64)
+    cost = ch_count * nsrc[ch_tb]
+    o = np.argsort(-cost, kind="stable")
+    return (ch_tb[o].astype(np.int32), np.array(ch_start, np.int32)[o],
+            ch_count[o].astype(np.int32), cbt.astype(np.int32))
 
 
 def _i(a):
@@ -132,7 +183,15 @@ def geometry_arrays(geo) -> tuple[dict, dict]:
         "sorted_target_ids": _i(tree.sorted_target_ids),
         "user_source_ids": _i(tree.user_source_ids),
     }
+    ch_tb, ch_start, ch_count, cbt = qbx_center_schedule(
+        arrays["global_qbx_centers"], arrays["qbx_center_to_target_box"],
+        arrays["list1_starts"], arrays["list1_lists"], arrays["box_source_counts_nonchild"])
+    arrays.update({
+        "qbx_chunk_target_box": ch_tb, "qbx_chunk_start": ch_start,
+        "qbx_chunk_count": ch_count, "centers_by_target_box": cbt,
+    })
     scalars = {
+        "nqbx_chunks": len(ch_tb),
         "dim": tree.dimensions, "nboxes": tree.nboxes, "nlevels": tree.nlevels,
         "nsources": tree.nsources, "ntargets": tree.ntargets,
         "root_extent": float(tree.root_extent),

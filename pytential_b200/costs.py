@@ -1,0 +1,84 @@
+"""Algorithmic work of the QBX-FMM stages, counted from the traversal lists.
+
+The per-unit constants are the float64 operation counts of the expansion
+arithmetic as formulated in the CUDA kernels (an FMA counts as 2 flops), written
+out here so the roofline numbers can be recomputed:
+
+P2QBXL, 3D Laplace, QBX order Q (N = Q + 1 when a double layer is present, else Q):
+  prelude: u = (y - c)/rho (6), |u|^2 (5), rsqrt and square (2)          = 13
+  singular-harmonic table to order N: diagonal entries 9 flops each (N of
+  them), first sub-diagonal 4 flops (N), the rest 9 flops (N (N - 1) / 2)
+  accumulation per coefficient: single layer 4 (real x complex FMA), double
+  layer 20 (three complex FMAs on neighbouring table entries)
+  source factors: 2 (single layer) + 7 (double layer)
+P2QBXL, 2D Laplace: tau^-1 (11), log|t| (4, single layer), Q complex powers
+  (6 each), per coefficient 6 (single layer) / 8 (double layer).
+
+The unit count (pairs) is sum over used QBX centers of the number of sources in
+the list-1 boxes of the center's target box (pytential/qbx/fmm.py:231-265).
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+
+def ncoeff_laplace(dim, q):
+    return (q + 1) * (q + 2) // 2 if dim == 3 else q + 1
+
+
+def p2qbxl_flops_per_pair(dim: int, q: int, charge: bool, dipole: bool) -> int:
+    if dim == 3:
+        n = q + (1 if dipole else 0)
+        table = 9 * n + 4 * n + 9 * n * (n - 1) // 2
+        acc = ncoeff_laplace(3, q) * (4 * charge + 20 * dipole)
+        return 13 + table + acc + 2 * charge + 7 * dipole
+    acc = (q + 1) * (6 * charge + 8 * dipole)
+    return 11 + 4 * charge + 6 * q + acc
+
+
+def p2qbxl_pairs(arrays: dict, scalars: dict) -> int:
+    """Number of (used center, list-1 source) pairs."""
+    gc = arrays["global_qbx_centers"][:scalars["nglobal_qbx_centers"]]
+    if len(gc) == 0:
+        return 0
+    tb = arrays["qbx_center_to_target_box"][gc]
+    l1s = arrays["list1_starts"].astype(np.int64)
+    cnt = arrays["box_source_counts_nonchild"][arrays["list1_lists"]].astype(np.int64)
+    csum = np.concatenate([[0], np.cumsum(cnt)])
+    nsrc = csum[l1s[1:]] - csum[l1s[:-1]]
+    return int(nsrc[tb].sum())
+
+
+def p2p_pairs(arrays: dict, scalars: dict) -> int:
+    """(non-QBX target, list-1 source) pairs of eval_direct."""
+    if scalars["nfiltered_targets"] == 0:
+        return 0
+    tb = arrays["target_boxes"]
+    nt = arrays["nonqbx_box_target_counts_nonchild"][tb].astype(np.int64)
+    l1s = arrays["list1_starts"].astype(np.int64)
+    cnt = arrays["box_source_counts_nonchild"][arrays["list1_lists"]].astype(np.int64)
+    csum = np.concatenate([[0], np.cumsum(cnt)])
+    nsrc = csum[l1s[1:]] - csum[l1s[:-1]]
+    return int((nt * nsrc).sum())
+
+
+def apply_launch_count(scalars: dict, arrays: dict) -> int:
+    """Kernels of this library launched by one qbxfmm_apply."""
+    nl = scalars["nlevels"]
+    lsp = arrays["level_start_source_parent_box_nrs"]
+    lttp = arrays["level_start_ttp_box_nrs"]
+    n = 1                                                   # strengths
+    n += scalars["nsource_boxes"] > 0                       # P2M
+    n += sum(1 for lev in range(nl - 1) if lsp[lev + 1] > lsp[lev])   # M2M
+    nf = scalars["nfiltered_targets"] > 0 and scalars["ntarget_boxes"] > 0
+    n += nf                                                 # P2P
+    n += scalars["nttp_boxes"] > 0                          # M2L
+    n += nf                                                 # M2P
+    n += scalars["nttp_boxes"] > 0                          # P2L
+    n += sum(1 for lev in range(1, nl) if lttp[lev + 1] > lttp[lev])  # L2L
+    n += nf                                                 # L2P
+    n += 2 * (scalars["nqbx_chunks"] > 0)                   # P2QBXL, M2QBXL
+    n += 2 * (scalars["nglobal_qbx_centers"] > 0)           # L2QBXL, QBXL2P
+    n += (scalars["ntargets"] > 0) + (scalars["nfiltered_targets"] > 0)  # assembly
+    return int(n)

@@ -1,0 +1,334 @@
+// extern "C" entry points of libqbxfmm.so (declared in include/qbxfmm_api.h).
+//
+// Each stage entry mirrors one method of pytential's QBX expansion wrangler as
+// called by the FMM driver (pytential/qbx/fmm.py:414-594); qbxfmm_apply runs them
+// all in the driver's order.  Stage outputs are accumulated (+=) into caller-owned
+// device buffers; the library allocates no device memory.
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/qbxfmm_api.h"
+#include "kernels.h"
+
+using namespace qbx;
+
+struct qbxfmm_plan {
+  qbxfmm_kernel kern;
+  qbxfmm_geometry geo;
+  std::vector<int32_t> lvl_source_parent;  // host copy of level_start_source_parent_box_nrs
+  std::vector<int32_t> lvl_ttp;            // host copy of level_start_ttp_box_nrs
+  SourceCoeffs sc;
+  int ncf, ncq;
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg)
+{
+  g_last_error = msg;
+  return code;
+}
+
+int cuda_check(cudaError_t e, const char* where)
+{
+  if (e == cudaSuccess) return QBXFMM_OK;
+  return fail(QBXFMM_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+cudaStream_t S(void* stream) { return reinterpret_cast<cudaStream_t>(stream); }
+
+int check_plan(const qbxfmm_plan* p)
+{
+  if (!p) return fail(QBXFMM_ERR_ARG, "null plan");
+  return QBXFMM_OK;
+}
+
+#define QBX_TRY(expr, where)                         \
+  do {                                               \
+    int _rc = cuda_check((expr), where);             \
+    if (_rc != QBXFMM_OK) return _rc;                \
+  } while (0)
+
+}  // namespace
+
+extern "C" {
+
+int qbxfmm_version(void) { return 1; }
+
+const char* qbxfmm_last_error(void) { return g_last_error.c_str(); }
+
+int qbxfmm_plan_create(const qbxfmm_kernel* kernel, const qbxfmm_geometry* geometry,
+                       qbxfmm_plan** out)
+{
+  if (!kernel || !geometry || !out) return fail(QBXFMM_ERR_ARG, "null argument");
+  *out = nullptr;
+  const qbxfmm_kernel& k = *kernel;
+  const qbxfmm_geometry& g = *geometry;
+  if (k.family != QBXFMM_LAPLACE)
+    return fail(QBXFMM_ERR_UNSUPPORTED, "only the Laplace family is built into this library");
+  if (k.dim != 2 && k.dim != 3) return fail(QBXFMM_ERR_ARG, "dim must be 2 or 3");
+  if (g.dim != k.dim) return fail(QBXFMM_ERR_ARG, "kernel and geometry dimensions differ");
+  if (k.qbx_order < 0 || k.qbx_order > 8)
+    return fail(QBXFMM_ERR_UNSUPPORTED, "qbx_order must be in [0, 8]");
+  if (k.fmm_order < 1 || k.fmm_order > 20)
+    return fail(QBXFMM_ERR_UNSUPPORTED, "fmm_order must be in [1, 20]");
+  if (k.nrhs < 1) return fail(QBXFMM_ERR_ARG, "nrhs must be >= 1");
+  if (k.precision != 0) return fail(QBXFMM_ERR_UNSUPPORTED, "only precision 0 (FP64)");
+  if (k.charge_coeff_im != 0.0 || k.dipole_coeff_im != 0.0)
+    return fail(QBXFMM_ERR_ARG, "Laplace source coefficients must be real");
+  if (g.nlevels < 1 || g.nboxes < 1 || g.nlevels > 40) return fail(QBXFMM_ERR_ARG, "bad tree sizes");
+  if (k.dipole_coeff_re != 0.0 && !g.source_normals)
+    return fail(QBXFMM_ERR_ARG, "double layer requested without source normals");
+
+  qbxfmm_plan* p = new (std::nothrow) qbxfmm_plan;
+  if (!p) return fail(QBXFMM_ERR_ARG, "out of host memory");
+  p->kern = k;
+  p->geo = g;
+  p->sc.cq = k.charge_coeff_re;
+  p->sc.cd = k.dipole_coeff_re;
+  p->ncf = ncoeff(k.family, k.dim, k.fmm_order);
+  p->ncq = ncoeff(k.family, k.dim, k.qbx_order);
+  p->lvl_source_parent.resize(g.nlevels + 1);
+  p->lvl_ttp.resize(g.nlevels + 1);
+  cudaError_t e = cudaMemcpy(p->lvl_source_parent.data(), g.level_start_source_parent_box_nrs,
+                             sizeof(int32_t) * (g.nlevels + 1), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(p->lvl_ttp.data(), g.level_start_ttp_box_nrs, sizeof(int32_t) * (g.nlevels + 1),
+                   cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) {
+    delete p;
+    return cuda_check(e, "qbxfmm_plan_create");
+  }
+  *out = p;
+  return QBXFMM_OK;
+}
+
+int qbxfmm_plan_destroy(qbxfmm_plan* plan)
+{
+  delete plan;
+  return QBXFMM_OK;
+}
+
+int qbxfmm_form_strengths(const qbxfmm_plan* p, const qbxfmm_upsample* up, const void* density,
+                          void* strengths, void* stream)
+{
+  if (int rc = check_plan(p)) return rc;
+  if (!up || !density || !strengths) return fail(QBXFMM_ERR_ARG, "null argument");
+  if (up->quad_nodes_per_element * up->nelements != p->geo.nsources)
+    return fail(QBXFMM_ERR_ARG, "upsampler does not match the number of sources");
+  QBX_TRY(launch_form_strengths(p->geo, *up, p->kern.nrhs, (const double*)density,
+                                (double*)strengths, S(stream)),
+          "form_strengths");
+  return QBXFMM_OK;
+}
+
+int qbxfmm_form_multipoles(const qbxfmm_plan* p, const void* strengths, void* mpoles, void* stream)
+{
+  if (int rc = check_plan(p)) return rc;
+  QBX_TRY(launch_p2m(p->geo, p->sc, p->kern.fmm_order, p->kern.nrhs, (const double*)strengths,
+                     (double2*)mpoles, S(stream)),
+          "form_multipoles");
+  return QBXFMM_OK;
+}
+
+int qbxfmm_coarsen_multipoles(const qbxfmm_plan* p, void* mpoles, void* stream)
+{
+  if (int rc = check_plan(p)) return rc;
+  QBX_TRY(launch_m2m(p->geo, p->lvl_source_parent.data(), p->kern.fmm_order, p->kern.nrhs,
+                     (double2*)mpoles, S(stream)),
+          "coarsen_multipoles");
+  return QBXFMM_OK;
+}
+
+int qbxfmm_eval_direct(const qbxfmm_plan* p, const void* strengths, void* pot_nonqbx,
+                       int32_t* error_word, void* stream)
+{
+  if (int rc = check_plan(p)) return rc;
+  QBX_TRY(launch_eval_direct(p->geo, p->sc, p->kern.nrhs, (const double*)strengths,
+                             (double*)pot_nonqbx, error_word, S(stream)),
+          "eval_direct");
+  return QBXFMM_OK;
+}
+
+int qbxfmm_multipole_to_local(const qbxfmm_plan* p, const void* mpoles, void* locals,
+                              int32_t* error_word, void* stream)
+{
+  if (int rc = check_plan(p)) return rc;
+  QBX_TRY(launch_m2l(p->geo, p->kern.fmm_order, p->kern.nrhs, (const double2*)mpoles,
+                     (double2*)locals, error_word, S(stream)),
+          "multipole_to_local");
+  return QBXFMM_OK;
+}
+
+int qbxfmm_eval_multipoles(const qbxfmm_plan* p, const void* mpoles, void* pot_nonqbx,
+                           int32_t* error_word, void* stream)
+{
+  if (int rc = check_plan(p)) return rc;
+  QBX_TRY(launch_eval_multipoles(p->geo, p->kern.fmm_order, p->kern.nrhs, (const double2*)mpoles,
+                                 (double*)pot_nonqbx, error_word, S(stream)),
+          "eval_multipoles");
+  return QBXFMM_OK;
+}
+
+int qbxfmm_form_locals(const qbxfmm_plan* p, const void* strengths, void* locals,
+                       int32_t* error_word, void* stream)
+{
+  if (int rc = check_plan(p)) return rc;
+  QBX_TRY(launch_p2l(p->geo, p->sc, p->kern.fmm_order, p->kern.nrhs, (const double*)strengths,
+                     (double2*)locals, error_word, S(stream)),
+          "form_locals");
+  return QBXFMM_OK;
+}
+
+int qbxfmm_refine_locals(const qbxfmm_plan* p, void* locals, void* stream)
+{
+  if (int rc = check_plan(p)) return rc;
+  QBX_TRY(launch_l2l(p->geo, p->lvl_ttp.data(), p->kern.fmm_order, p->kern.nrhs,
+                     (double2*)locals, S(stream)),
+          "refine_locals");
+  return QBXFMM_OK;
+}
+
+int qbxfmm_eval_locals(const qbxfmm_plan* p, const void* locals, void* pot_nonqbx, void* stream)
+{
+  if (int rc = check_plan(p)) return rc;
+  QBX_TRY(launch_eval_locals(p->geo, p->kern.fmm_order, p->kern.nrhs, (const double2*)locals,
+                             (double*)pot_nonqbx, S(stream)),
+          "eval_locals");
+  return QBXFMM_OK;
+}
+
+int qbxfmm_form_global_qbx_locals(const qbxfmm_plan* p, const void* strengths, void* qbx_exps,
+                                  int32_t* error_word, void* stream)
+{
+  if (int rc = check_plan(p)) return rc;
+  QBX_TRY(launch_p2qbxl(p->geo, p->sc, p->kern.qbx_order, p->kern.nrhs, (const double*)strengths,
+                        (double2*)qbx_exps, error_word, S(stream)),
+          "form_global_qbx_locals");
+  return QBXFMM_OK;
+}
+
+int qbxfmm_translate_box_multipoles_to_qbx_local(const qbxfmm_plan* p, const void* mpoles,
+                                                 void* qbx_exps, int32_t* error_word, void* stream)
+{
+  if (int rc = check_plan(p)) return rc;
+  QBX_TRY(launch_m2qbxl(p->geo, p->kern.fmm_order, p->kern.qbx_order, p->kern.nrhs,
+                        (const double2*)mpoles, (double2*)qbx_exps, error_word, S(stream)),
+          "translate_box_multipoles_to_qbx_local");
+  return QBXFMM_OK;
+}
+
+int qbxfmm_translate_box_local_to_qbx_local(const qbxfmm_plan* p, const void* locals,
+                                            void* qbx_exps, void* stream)
+{
+  if (int rc = check_plan(p)) return rc;
+  QBX_TRY(launch_l2qbxl(p->geo, p->kern.fmm_order, p->kern.qbx_order, p->kern.nrhs,
+                        (const double2*)locals, (double2*)qbx_exps, S(stream)),
+          "translate_box_local_to_qbx_local");
+  return QBXFMM_OK;
+}
+
+int qbxfmm_eval_qbx_expansions(const qbxfmm_plan* p, const void* qbx_exps, void* pot_tree,
+                               void* stream)
+{
+  if (int rc = check_plan(p)) return rc;
+  QBX_TRY(launch_qbxl2p(p->geo, p->kern.qbx_order, p->kern.nrhs, (const double2*)qbx_exps,
+                        (double*)pot_tree, S(stream)),
+          "eval_qbx_expansions");
+  return QBXFMM_OK;
+}
+
+int qbxfmm_assemble(const qbxfmm_plan* p, const void* pot_nonqbx, const void* pot_tree, void* out,
+                    void* stream)
+{
+  if (int rc = check_plan(p)) return rc;
+  QBX_TRY(launch_assemble(p->geo, p->kern.nrhs, (const double*)pot_nonqbx,
+                          (const double*)pot_tree, (double*)out, S(stream)),
+          "assemble");
+  return QBXFMM_OK;
+}
+
+int qbxfmm_workspace_sizes(const qbxfmm_plan* p, size_t* sizes6)
+{
+  if (int rc = check_plan(p)) return rc;
+  if (!sizes6) return fail(QBXFMM_ERR_ARG, "null sizes");
+  const qbxfmm_geometry& g = p->geo;
+  size_t nr = (size_t)p->kern.nrhs;
+  size_t scal = (p->kern.family == QBXFMM_LAPLACE) ? sizeof(double) : 2 * sizeof(double);
+  sizes6[0] = nr * g.nsources * scal;
+  sizes6[1] = (size_t)g.nboxes * nr * p->ncf * 2 * sizeof(double);
+  sizes6[2] = sizes6[1];
+  sizes6[3] = (size_t)g.ncenters * nr * p->ncq * 2 * sizeof(double);
+  sizes6[4] = nr * (size_t)(g.nfiltered_targets > 0 ? g.nfiltered_targets : 1) * scal;
+  sizes6[5] = nr * (size_t)g.ntargets * scal;
+  return QBXFMM_OK;
+}
+
+int qbxfmm_apply(const qbxfmm_plan* p, const qbxfmm_upsample* up, const qbxfmm_workspace* ws,
+                 const void* density, void* out, void* stream)
+{
+  if (int rc = check_plan(p)) return rc;
+  if (!up || !ws || !density || !out) return fail(QBXFMM_ERR_ARG, "null argument");
+  if (!ws->strengths || !ws->mpoles || !ws->locals || !ws->qbx_exps || !ws->pot_nonqbx ||
+      !ws->pot_tree)
+    return fail(QBXFMM_ERR_ARG, "incomplete workspace");
+  size_t sz[6];
+  qbxfmm_workspace_sizes(p, sz);
+  cudaStream_t st = S(stream);
+  QBX_TRY(cudaMemsetAsync(ws->mpoles, 0, sz[1], st), "apply: clear");
+  QBX_TRY(cudaMemsetAsync(ws->locals, 0, sz[2], st), "apply: clear");
+  QBX_TRY(cudaMemsetAsync(ws->qbx_exps, 0, sz[3], st), "apply: clear");
+  QBX_TRY(cudaMemsetAsync(ws->pot_nonqbx, 0, sz[4], st), "apply: clear");
+  QBX_TRY(cudaMemsetAsync(ws->pot_tree, 0, sz[5], st), "apply: clear");
+  if (ws->error_word) QBX_TRY(cudaMemsetAsync(ws->error_word, 0, sizeof(int32_t), st), "apply: clear");
+  int rc;
+  // drive_fmm order (fmm.py:436-588)
+  if ((rc = qbxfmm_form_strengths(p, up, density, ws->strengths, stream))) return rc;
+  if ((rc = qbxfmm_form_multipoles(p, ws->strengths, ws->mpoles, stream))) return rc;
+  if ((rc = qbxfmm_coarsen_multipoles(p, ws->mpoles, stream))) return rc;
+  if ((rc = qbxfmm_eval_direct(p, ws->strengths, ws->pot_nonqbx, ws->error_word, stream))) return rc;
+  if ((rc = qbxfmm_multipole_to_local(p, ws->mpoles, ws->locals, ws->error_word, stream))) return rc;
+  if ((rc = qbxfmm_eval_multipoles(p, ws->mpoles, ws->pot_nonqbx, ws->error_word, stream))) return rc;
+  if ((rc = qbxfmm_form_locals(p, ws->strengths, ws->locals, ws->error_word, stream))) return rc;
+  if ((rc = qbxfmm_refine_locals(p, ws->locals, stream))) return rc;
+  if ((rc = qbxfmm_eval_locals(p, ws->locals, ws->pot_nonqbx, stream))) return rc;
+  if ((rc = qbxfmm_form_global_qbx_locals(p, ws->strengths, ws->qbx_exps, ws->error_word, stream)))
+    return rc;
+  if ((rc = qbxfmm_translate_box_multipoles_to_qbx_local(p, ws->mpoles, ws->qbx_exps,
+                                                         ws->error_word, stream)))
+    return rc;
+  if ((rc = qbxfmm_translate_box_local_to_qbx_local(p, ws->locals, ws->qbx_exps, stream))) return rc;
+  if ((rc = qbxfmm_eval_qbx_expansions(p, ws->qbx_exps, ws->pot_tree, stream))) return rc;
+  return qbxfmm_assemble(p, ws->pot_nonqbx, ws->pot_tree, out, stream);
+}
+
+int qbxfmm_apply_host(const qbxfmm_plan* p, const qbxfmm_upsample* up, const qbxfmm_workspace* ws,
+                      const void* density_host, void* out_host, void* density_dev, void* out_dev,
+                      void* stream)
+{
+  if (int rc = check_plan(p)) return rc;
+  if (!density_host || !out_host || !density_dev || !out_dev)
+    return fail(QBXFMM_ERR_ARG, "null argument");
+  size_t scal = (p->kern.family == QBXFMM_LAPLACE) ? sizeof(double) : 2 * sizeof(double);
+  size_t nin = (size_t)p->kern.nrhs * up->nelements * up->nodes_per_element * scal;
+  size_t nout = (size_t)p->kern.nrhs * p->geo.nuser_targets * scal;
+  cudaStream_t st = S(stream);
+  QBX_TRY(cudaMemcpyAsync(density_dev, density_host, nin, cudaMemcpyHostToDevice, st), "apply_host: h2d");
+  int rc = qbxfmm_apply(p, up, ws, density_dev, out_dev, stream);
+  if (rc) return rc;
+  QBX_TRY(cudaMemcpyAsync(out_host, out_dev, nout, cudaMemcpyDeviceToHost, st), "apply_host: d2h");
+  QBX_TRY(cudaStreamSynchronize(st), "apply_host: sync");
+  if (ws->error_word) {
+    int32_t w = 0;
+    QBX_TRY(cudaMemcpy(&w, ws->error_word, sizeof(int32_t), cudaMemcpyDeviceToHost), "apply_host: error word");
+    if (w != 0) return fail(QBXFMM_ERR_DEVICE, "a kernel met an out-of-range index (code " + std::to_string(w) + ")");
+  }
+  return QBXFMM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,39 @@
+// Internal launcher declarations (one per wrangler stage).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace qbx {
+
+cudaError_t launch_form_strengths(const qbxfmm_geometry& g, const qbxfmm_upsample& up, int nrhs,
+                                  const double* density, double* strengths, cudaStream_t st);
+cudaError_t launch_p2m(const qbxfmm_geometry& g, SourceCoeffs sc, int p, int nrhs,
+                       const double* s, double2* mp, cudaStream_t st);
+cudaError_t launch_m2m(const qbxfmm_geometry& g, const int32_t* lvl_host, int p, int nrhs,
+                       double2* mp, cudaStream_t st);
+cudaError_t launch_m2l(const qbxfmm_geometry& g, int p, int nrhs, const double2* mp, double2* lo,
+                       int32_t* err, cudaStream_t st);
+cudaError_t launch_p2l(const qbxfmm_geometry& g, SourceCoeffs sc, int p, int nrhs,
+                       const double* s, double2* lo, int32_t* err, cudaStream_t st);
+cudaError_t launch_l2l(const qbxfmm_geometry& g, const int32_t* lvl_host, int p, int nrhs,
+                       double2* lo, cudaStream_t st);
+cudaError_t launch_eval_direct(const qbxfmm_geometry& g, SourceCoeffs sc, int nrhs,
+                               const double* s, double* pot, int32_t* err, cudaStream_t st);
+cudaError_t launch_eval_multipoles(const qbxfmm_geometry& g, int p, int nrhs, const double2* mp,
+                                   double* pot, int32_t* err, cudaStream_t st);
+cudaError_t launch_eval_locals(const qbxfmm_geometry& g, int p, int nrhs, const double2* lo,
+                               double* pot, cudaStream_t st);
+cudaError_t launch_p2qbxl(const qbxfmm_geometry& g, SourceCoeffs sc, int q, int nrhs,
+                          const double* s, double2* qe, int32_t* err, cudaStream_t st);
+cudaError_t launch_m2qbxl(const qbxfmm_geometry& g, int pf, int q, int nrhs, const double2* mp,
+                          double2* qe, int32_t* err, cudaStream_t st);
+cudaError_t launch_l2qbxl(const qbxfmm_geometry& g, int pf, int q, int nrhs, const double2* lo,
+                          double2* qe, cudaStream_t st);
+cudaError_t launch_qbxl2p(const qbxfmm_geometry& g, int q, int nrhs, const double2* qe,
+                          double* pt, cudaStream_t st);
+cudaError_t launch_assemble(const qbxfmm_geometry& g, int nrhs, const double* pot_nonqbx,
+                            const double* pot_tree, double* out, cudaStream_t st);
+
+}  // namespace qbx

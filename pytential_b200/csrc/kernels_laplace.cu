@@ -1,0 +1,1430 @@
+// Laplace QBX-FMM stage kernels (2D and 3D), float64, sm_100a.
+//
+// One kernel per wrangler stage of pytential's FMM driver
+// (pytential/qbx/fmm.py:414-594).  Box kernels assign one CTA per box of the
+// relevant traversal list and stage sources / expansions / translation tables in
+// shared memory; the QBX near-field kernel assigns one CTA per chunk of centers
+// that share a target box, holds each center's coefficients in registers and
+// streams that box's list-1 sources through shared memory in tiles of 128.
+#include "laplace.cuh"
+#include "kernels.h"
+
+namespace qbx {
+
+constexpr int NT = 128;
+
+// {{{ strengths: upsample + weight + reorder to tree order
+
+// get_flat_strengths_from_densities (pytential/qbx/__init__.py:1075-1096) and
+// reorder_sources (pytential/qbx/fmm.py:199-200), one thread per tree source.
+__global__ void __launch_bounds__(256)
+k_form_strengths(int nsources, int ndofs, int npe, int nqpe,
+                 const double* __restrict__ U, const double* __restrict__ qw,
+                 const int32_t* __restrict__ user_source_ids,
+                 const double* __restrict__ density, double* __restrict__ out)
+{
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  int r = blockIdx.y;
+  if (t >= nsources) return;
+  int j = __ldg(user_source_ids + t);
+  int e = j / nqpe;
+  int jj = j - e * nqpe;
+  const double* u = U + (size_t)jj * npe;
+  const double* d = density + (size_t)r * ndofs + (size_t)e * npe;
+  double acc = 0.0;
+  for (int i = 0; i < npe; ++i) acc = fma(__ldg(u + i), __ldg(d + i), acc);
+  out[(size_t)r * nsources + t] = acc * __ldg(qw + j);
+}
+
+// }}}
+
+// {{{ helpers
+
+struct SrcTile {
+  double* x;   // [3][NT]
+  double* n;   // [3][NT]
+  double* q;   // [NT]
+};
+
+// decode coefficient index -> (n, m) for the 3D triangular layout
+QBX_D void decode3(int c, int& n, int& m)
+{
+  n = (int)((sqrt(8.0 * c + 1.0) - 1.0) * 0.5);
+  while ((n + 1) * (n + 2) / 2 <= c) ++n;
+  while (n * (n + 1) / 2 > c) --n;
+  m = c - n * (n + 1) / 2;
+}
+
+// }}}
+
+// {{{ P2M (form_multipoles, fmm.py:441-445)
+
+// tables of R_n^m((y - c)/rho) for SUB sources at a time, one thread per column
+template <int DIM>
+__global__ void __launch_bounds__(NT)
+k_p2m(qbxfmm_geometry g, SourceCoeffs sc, int p, int ncf, int nrhs,
+      const double* __restrict__ strengths, double2* __restrict__ mpoles)
+{
+  constexpr int SUB = 16;
+  extern __shared__ double2 smem2[];
+  double2* tab = smem2;                                  // [SUB][ncf]
+  __shared__ double s_u[SUB][3], s_n[SUB][3], s_q[SUB];
+
+  int b = g.source_boxes[blockIdx.x];
+  int r = blockIdx.y;
+  double rho = level_width(g, g.box_levels[b]);
+  double c[3];
+  load_point<DIM>(g.box_centers, g.nboxes, b, c);
+  int s0 = g.box_source_starts[b];
+  int ns = g.box_source_counts_nonchild[b];
+  const double* st = strengths + (size_t)r * g.nsources;
+
+  double2 acc[2] = {c2(0.0), c2(0.0)};
+  for (int base = 0; base < ns; base += SUB) {
+    int cnt = min(SUB, ns - base);
+    if (threadIdx.x < cnt) {
+      int s = s0 + base + threadIdx.x;
+      double y[3];
+      load_point<DIM>(g.sources, g.nsources, s, y);
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) s_u[threadIdx.x][d] = (y[d] - c[d]) / rho;
+      if (sc.cd != 0.0) {
+        double nv[3];
+        load_point<DIM>(g.source_normals, g.nsources, s, nv);
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) s_n[threadIdx.x][d] = nv[d];
+      }
+      s_q[threadIdx.x] = __ldg(st + s);
+    }
+    __syncthreads();
+    if (DIM == 3) {
+      for (int w = threadIdx.x; w < cnt * (p + 1); w += NT) {
+        int j = w / (p + 1), m = w - j * (p + 1);
+        // column m of R for source j
+        double x = s_u[j][0], y = s_u[j][1], z = s_u[j][2];
+        double r2 = x * x + y * y + z * z;
+        double2 a = c2(1.0);
+        for (int k = 1; k <= m; ++k) a = cscale(1.0 / (2 * k), cmul(a, c2(x, y)));
+        double2* T = tab + (size_t)j * ncf;
+        T[idx3(m, m)] = a;
+        double2 prev = c2(0.0);
+        for (int n = m + 1; n <= p; ++n) {
+          double2 bb = cscale(1.0 / ((double)(n + m) * (n - m)),
+                              csub(cscale((2.0 * n - 1) * z, a), cscale(r2, prev)));
+          T[idx3(n, m)] = bb;
+          prev = a;
+          a = bb;
+        }
+      }
+    } else {
+      for (int j = threadIdx.x; j < cnt; j += NT) {
+        double2 u = c2(s_u[j][0], s_u[j][1]);
+        double2* T = tab + (size_t)j * ncf;
+        double2 a = c2(1.0);
+        for (int k = 0; k <= p; ++k) {
+          T[k] = a;  // u^k
+          a = cmul(a, u);
+        }
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      int ci = threadIdx.x + h * NT;
+      if (ci >= ncf) break;
+      double2 a = acc[h];
+      if (DIM == 3) {
+        int n, m;
+        decode3(ci, n, m);
+        for (int j = 0; j < cnt; ++j) {
+          const double2* T = tab + (size_t)j * ncf;
+          double q = s_q[j];
+          a = caxpy(sc.cq * q, cconj(T[idx3(n, m)]), a);
+          if (sc.cd != 0.0 && n >= 1) {
+            double f = sc.cd * q / rho;
+            double dx = s_n[j][0], dy = s_n[j][1], dz = s_n[j][2];
+            // conj(dz R_{n-1}^m + (dx+idy)/2 R_{n-1}^{m-1} - (dx-idy)/2 R_{n-1}^{m+1})
+            double2 v = cscale(dz, sh3_get(T, n - 1, m));
+            v = cfma(c2(0.5 * dx, 0.5 * dy), sh3_get(T, n - 1, m - 1), v);
+            v = cfma(c2(-0.5 * dx, 0.5 * dy), sh3_get(T, n - 1, m + 1), v);
+            a = caxpy(f, cconj(v), a);
+          }
+        }
+      } else {
+        int k = ci;
+        for (int j = 0; j < cnt; ++j) {
+          const double2* T = tab + (size_t)j * ncf;
+          double q = s_q[j];
+          if (k == 0) {
+            a.x += sc.cq * q;
+          } else {
+            a = caxpy(-sc.cq * q / k, T[k], a);
+            if (sc.cd != 0.0) {
+              double2 nu = c2(s_n[j][0], s_n[j][1]);
+              a = cfma(cscale(-sc.cd * q / rho, nu), T[k - 1], a);
+            }
+          }
+        }
+      }
+      acc[h] = a;
+    }
+    __syncthreads();
+  }
+  double2* M = mpoles + ((size_t)b * nrhs + r) * ncf;
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    int ci = threadIdx.x + h * NT;
+    if (ci < ncf) M[ci] = cadd(M[ci], acc[h]);
+  }
+}
+
+// }}}
+
+// {{{ M2M (coarsen_multipoles, fmm.py:451-455), one launch per parent level
+
+template <int DIM>
+__global__ void __launch_bounds__(NT)
+k_m2m(qbxfmm_geometry g, int p, int ncf, int nrhs, int i0, double2* __restrict__ mpoles)
+{
+  extern __shared__ double2 smem2[];
+  double2* tab = smem2;          // [ncf] R table / powers
+  double2* Min = smem2 + ncf;    // [ncf]
+  int b = g.source_parent_boxes[i0 + blockIdx.x];
+  int r = blockIdx.y;
+  int lev = g.box_levels[b];
+  double rho_p = level_width(g, lev), rho_c = level_width(g, lev + 1);
+  double ratio = rho_c / rho_p;
+  double cp[3];
+  load_point<DIM>(g.box_centers, g.nboxes, b, cp);
+  double2 acc[2] = {c2(0.0), c2(0.0)};
+  const int nch = 1 << DIM;
+  for (int ci = 0; ci < nch; ++ci) {
+    int ch = g.box_child_ids[(size_t)ci * g.nboxes + b];
+    if (ch == 0 || g.box_source_counts_cumul[ch] == 0) continue;
+    double cc[3], d[3];
+    load_point<DIM>(g.box_centers, g.nboxes, ch, cc);
+#pragma unroll
+    for (int k = 0; k < DIM; ++k) d[k] = (cc[k] - cp[k]) / rho_p;
+    const double2* src = mpoles + ((size_t)ch * nrhs + r) * ncf;
+    for (int i = threadIdx.x; i < ncf; i += NT) Min[i] = src[i];
+    if (DIM == 3) {
+      sh3_R_table(p, d[0], d[1], d[2], tab, threadIdx.x, NT);
+    } else if (threadIdx.x == 0) {
+      double2 t = c2(d[0], d[1]), a = c2(1.0);
+      for (int k = 0; k <= p; ++k) {
+        tab[k] = a;
+        a = cmul(a, t);
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      int o = threadIdx.x + h * NT;
+      if (o >= ncf) break;
+      double2 a = acc[h];
+      if (DIM == 3) {
+        int n, m;
+        decode3(o, n, m);
+        double rk = 1.0;
+        for (int k = 0; k <= n; ++k, rk *= ratio)
+          for (int l = -k; l <= k; ++l) {
+            int dm = m - l;
+            if (dm > n - k || -dm > n - k) continue;
+            a = cfmac(cscale(rk, sh3_get(Min, k, l)), sh3_get(tab, n - k, dm), a);
+          }
+      } else {
+        int l = o;
+        if (l == 0) {
+          a = cadd(a, Min[0]);
+        } else {
+          a = cfma(cscale(-1.0 / l, Min[0]), tab[l], a);
+          double rk = ratio, bin = 1.0;  // C(l-1, k-1)
+          for (int k = 1; k <= l; ++k) {
+            a = cfma(cscale(rk * bin, Min[k]), tab[l - k], a);
+            rk *= ratio;
+            bin = bin * (l - k) / k;
+          }
+        }
+      }
+      acc[h] = a;
+    }
+    __syncthreads();
+  }
+  double2* M = mpoles + ((size_t)b * nrhs + r) * ncf;
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    int o = threadIdx.x + h * NT;
+    if (o < ncf) M[o] = cadd(M[o], acc[h]);
+  }
+}
+
+// }}}
+
+// {{{ M2L (multipole_to_local, fmm.py:472-478), one CTA per target-or-parent box
+
+template <int DIM>
+__global__ void __launch_bounds__(NT)
+k_m2l(qbxfmm_geometry g, int p, int ncf, int nrhs, const double2* __restrict__ mpoles,
+      double2* __restrict__ locals, int32_t* err)
+{
+  extern __shared__ double2 smem2[];
+  double2* Min = smem2;             // [ncf]
+  double2* tab = smem2 + ncf;       // [ncoeff(2p)]
+  int i = blockIdx.x;
+  int tb = g.target_or_target_parent_boxes[i];
+  int r = blockIdx.y;
+  double rho = level_width(g, g.box_levels[tb]);
+  double ct[3];
+  load_point<DIM>(g.box_centers, g.nboxes, tb, ct);
+  double2 acc[2] = {c2(0.0), c2(0.0)};
+  int l0 = g.list2_starts[i], l1 = g.list2_starts[i + 1];
+  for (int li = l0; li < l1; ++li) {
+    int sb = g.list2_lists[li];
+    if ((unsigned)sb >= (unsigned)g.nboxes) {
+      report(err, QBX_DEVERR_BAD_BOX);
+      continue;
+    }
+    double cs[3], d[3];
+    load_point<DIM>(g.box_centers, g.nboxes, sb, cs);
+#pragma unroll
+    for (int k = 0; k < DIM; ++k) d[k] = (ct[k] - cs[k]) / rho;
+    const double2* src = mpoles + ((size_t)sb * nrhs + r) * ncf;
+    for (int q = threadIdx.x; q < ncf; q += NT) Min[q] = src[q];
+    if (DIM == 3) {
+      sh3_S_table(2 * p, d[0], d[1], d[2], tab, threadIdx.x, NT);
+    } else if (threadIdx.x == 0) {
+      double2 tinv = cinv(c2(d[0], d[1])), a = tinv;
+      tab[0] = clog_(c2(d[0] * rho, d[1] * rho));
+      for (int k = 1; k <= 2 * p + 1; ++k) {
+        tab[k] = a;  // tau^-k
+        a = cmul(a, tinv);
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      int o = threadIdx.x + h * NT;
+      if (o >= ncf) break;
+      double2 a = acc[h];
+      if (DIM == 3) {
+        int j, ii;
+        decode3(o, j, ii);
+        double2 s = c2(0.0);
+        for (int k = 0; k <= p; ++k)
+          for (int l = -k; l <= k; ++l) s = cfma(sh3_get(Min, k, l), sh3_get(tab, k + j, l + ii), s);
+        a = caxpy((j & 1) ? -1.0 / rho : 1.0 / rho, s, a);
+      } else {
+        int l = o;
+        if (l == 0) {
+          double2 s = cmul(Min[0], tab[0]);
+          for (int k = 1; k <= p; ++k) s = cfma(Min[k], tab[k], s);
+          a = cadd(a, s);
+        } else {
+          double2 s = c2(0.0);
+          double bin = 1.0;  // C(k+l-1, l) at k = 1
+          for (int k = 1; k <= p; ++k) {
+            s = cfma(cscale(bin, Min[k]), tab[k], s);
+            bin = bin * (k + l) / k;
+          }
+          double2 v = cscale(((l & 1) ? 1.0 : -1.0) / l, Min[0]);
+          v = cadd(v, cscale((l & 1) ? -1.0 : 1.0, s));
+          a = cfma(v, tab[l], a);
+        }
+      }
+      acc[h] = a;
+    }
+    __syncthreads();
+  }
+  double2* L = locals + ((size_t)tb * nrhs + r) * ncf;
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    int o = threadIdx.x + h * NT;
+    if (o < ncf) L[o] = cadd(L[o], acc[h]);
+  }
+}
+
+// }}}
+
+// {{{ P2L (form_locals, list 4, fmm.py:502-510)
+
+template <int DIM>
+__global__ void __launch_bounds__(NT)
+k_p2l(qbxfmm_geometry g, SourceCoeffs sc, int p, int ncf, int nrhs,
+      const double* __restrict__ strengths, double2* __restrict__ locals, int32_t* err)
+{
+  constexpr int SUB = 16;
+  extern __shared__ double2 smem2[];
+  double2* tab = smem2;   // [SUB][ncoeff(p+1)]
+  __shared__ double s_u[SUB][3], s_n[SUB][3], s_q[SUB];
+  int nct = (DIM == 3) ? (p + 2) * (p + 3) / 2 : p + 3;
+  int i = blockIdx.x;
+  int tb = g.target_or_target_parent_boxes[i];
+  int r = blockIdx.y;
+  double rho = level_width(g, g.box_levels[tb]);
+  double c[3];
+  load_point<DIM>(g.box_centers, g.nboxes, tb, c);
+  const double* st = strengths + (size_t)r * g.nsources;
+  double2 acc[2] = {c2(0.0), c2(0.0)};
+  for (int li = g.list4_starts[i]; li < g.list4_starts[i + 1]; ++li) {
+    int sb = g.list4_lists[li];
+    if ((unsigned)sb >= (unsigned)g.nboxes) {
+      report(err, QBX_DEVERR_BAD_BOX);
+      continue;
+    }
+    int s0 = g.box_source_starts[sb], ns = g.box_source_counts_nonchild[sb];
+    for (int base = 0; base < ns; base += SUB) {
+      int cnt = min(SUB, ns - base);
+      if (threadIdx.x < cnt) {
+        int s = s0 + base + threadIdx.x;
+        double y[3];
+        load_point<DIM>(g.sources, g.nsources, s, y);
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) s_u[threadIdx.x][d] = (y[d] - c[d]) / rho;
+        if (sc.cd != 0.0) {
+          double nv[3];
+          load_point<DIM>(g.source_normals, g.nsources, s, nv);
+#pragma unroll
+          for (int d = 0; d < DIM; ++d) s_n[threadIdx.x][d] = nv[d];
+        }
+        s_q[threadIdx.x] = __ldg(st + s);
+      }
+      __syncthreads();
+      if (DIM == 3) {
+        for (int w = threadIdx.x; w < cnt * (p + 2); w += NT) {
+          int j = w / (p + 2), m = w - j * (p + 2);
+          double x = s_u[j][0], y = s_u[j][1], z = s_u[j][2];
+          double rinv2 = 1.0 / (x * x + y * y + z * z);
+          double2 a = c2(sqrt(rinv2));
+          for (int k = 1; k <= m; ++k) a = cscale((2.0 * k - 1) * rinv2, cmul(a, c2(x, y)));
+          double2* T = tab + (size_t)j * nct;
+          T[idx3(m, m)] = a;
+          double2 prev = c2(0.0);
+          for (int n = m + 1; n <= p + 1; ++n) {
+            double2 bb = cscale(rinv2, csub(cscale((2.0 * n - 1) * z, a),
+                                            cscale((double)(n + m - 1) * (n - m - 1), prev)));
+            T[idx3(n, m)] = bb;
+            prev = a;
+            a = bb;
+          }
+        }
+      } else {
+        for (int j = threadIdx.x; j < cnt; j += NT) {
+          double2 tinv = cinv(c2(s_u[j][0], s_u[j][1]));
+          double2* T = tab + (size_t)j * nct;
+          double2 a = c2(1.0);
+          for (int k = 0; k <= p + 1; ++k) {
+            T[k] = a;   // tau^-k
+            a = cmul(a, tinv);
+          }
+          T[p + 2] = c2(0.5 * log((s_u[j][0] * s_u[j][0] + s_u[j][1] * s_u[j][1])
+                                  * rho * rho));
+        }
+      }
+      __syncthreads();
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        int ci = threadIdx.x + h * NT;
+        if (ci >= ncf) break;
+        double2 a = acc[h];
+        for (int j = 0; j < cnt; ++j) {
+          const double2* T = tab + (size_t)j * nct;
+          double q = s_q[j];
+          if (DIM == 3) {
+            int n, m;
+            decode3(ci, n, m);
+            a = caxpy(sc.cq * q / rho, T[idx3(n, m)], a);
+            if (sc.cd != 0.0) {
+              double f = sc.cd * q / (rho * rho);
+              double dx = s_n[j][0], dy = s_n[j][1], dz = s_n[j][2];
+              double2 v = cscale(-dz, sh3_get(T, n + 1, m));
+              v = cfma(c2(0.5 * dx, 0.5 * dy), sh3_get(T, n + 1, m - 1), v);
+              v = cfma(c2(-0.5 * dx, 0.5 * dy), sh3_get(T, n + 1, m + 1), v);
+              a = caxpy(f, v, a);
+            }
+          } else {
+            int l = ci;
+            if (l == 0) a.x += sc.cq * q * T[p + 2].x;
+            else a = caxpy(-sc.cq * q / l, T[l], a);
+            if (sc.cd != 0.0) {
+              double2 nu = c2(s_n[j][0], s_n[j][1]);
+              a = cfma(cscale(sc.cd * q / rho, nu), T[l + 1], a);
+            }
+          }
+        }
+        acc[h] = a;
+      }
+      __syncthreads();
+    }
+  }
+  double2* L = locals + ((size_t)tb * nrhs + r) * ncf;
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    int o = threadIdx.x + h * NT;
+    if (o < ncf) L[o] = cadd(L[o], acc[h]);
+  }
+}
+
+// }}}
+
+// {{{ L2L (refine_locals, fmm.py:519-523), one launch per child level
+
+template <int DIM>
+__global__ void __launch_bounds__(NT)
+k_l2l(qbxfmm_geometry g, int p, int ncf, int nrhs, int i0, double2* __restrict__ locals)
+{
+  extern __shared__ double2 smem2[];
+  double2* tab = smem2;
+  double2* Lin = smem2 + ncf;
+  int b = g.target_or_target_parent_boxes[i0 + blockIdx.x];
+  int r = blockIdx.y;
+  int par = g.box_parent_ids[b];
+  int lev = g.box_levels[b];
+  double rho_p = level_width(g, lev - 1), rho_c = level_width(g, lev);
+  double ratio = rho_c / rho_p;
+  double cp[3], cc[3], d[3];
+  load_point<DIM>(g.box_centers, g.nboxes, par, cp);
+  load_point<DIM>(g.box_centers, g.nboxes, b, cc);
+#pragma unroll
+  for (int k = 0; k < DIM; ++k) d[k] = (cc[k] - cp[k]) / rho_p;
+  const double2* src = locals + ((size_t)par * nrhs + r) * ncf;
+  for (int q = threadIdx.x; q < ncf; q += NT) Lin[q] = src[q];
+  if (DIM == 3) {
+    sh3_R_table(p, d[0], d[1], d[2], tab, threadIdx.x, NT);
+  } else if (threadIdx.x == 0) {
+    double2 s = c2(d[0], d[1]), a = c2(1.0);
+    for (int k = 0; k <= p; ++k) {
+      tab[k] = a;
+      a = cmul(a, s);
+    }
+  }
+  __syncthreads();
+  double2* L = locals + ((size_t)b * nrhs + r) * ncf;
+  for (int o = threadIdx.x; o < ncf; o += NT) {
+    double2 a = c2(0.0);
+    if (DIM == 3) {
+      int k, l;
+      decode3(o, k, l);
+      for (int n = k; n <= p; ++n)
+        for (int m = -n; m <= n; ++m) {
+          int dm = m - l;
+          if (dm > n - k || -dm > n - k) continue;
+          a = cfmac(sh3_get(Lin, n, m), sh3_get(tab, n - k, dm), a);
+        }
+      a = cscale(pow(ratio, (double)k), a);
+    } else {
+      int l = o;
+      double bin = 1.0;  // C(k, l)
+      for (int k = l; k <= p; ++k) {
+        a = cfma(cscale(bin, Lin[k]), tab[k - l], a);
+        bin = bin * (k + 1) / (k + 1 - l);
+      }
+      a = cscale(pow(ratio, (double)l), a);
+    }
+    L[o] = cadd(L[o], a);
+  }
+}
+
+// }}}
+
+// {{{ point evaluations at non-QBX targets: P2P (list 1), M2P (list 3), L2P
+
+template <int DIM>
+__global__ void __launch_bounds__(NT)
+k_eval_direct(qbxfmm_geometry g, SourceCoeffs sc, int nrhs, const double* __restrict__ strengths,
+              double* __restrict__ pot, int32_t* err)
+{
+  __shared__ double s_y[3][NT], s_n[3][NT], s_q[NT];
+  int itb = blockIdx.x;
+  int tb = g.target_boxes[itb];
+  int r = blockIdx.y;
+  int t0 = g.nonqbx_box_target_starts[tb];
+  int nt = g.nonqbx_box_target_counts_nonchild[tb];
+  if (nt == 0) return;
+  const double* st = strengths + (size_t)r * g.nsources;
+  for (int tbase = 0; tbase < nt; tbase += NT) {
+    int t = tbase + threadIdx.x;
+    bool active = t < nt;
+    double x[3] = {0, 0, 0};
+    if (active) load_point<DIM>(g.nonqbx_targets, g.nfiltered_targets, t0 + t, x);
+    double acc = 0.0;
+    for (int li = g.list1_starts[itb]; li < g.list1_starts[itb + 1]; ++li) {
+      int sb = g.list1_lists[li];
+      if ((unsigned)sb >= (unsigned)g.nboxes) {
+        report(err, QBX_DEVERR_BAD_BOX);
+        continue;
+      }
+      int s0 = g.box_source_starts[sb], ns = g.box_source_counts_nonchild[sb];
+      for (int base = 0; base < ns; base += NT) {
+        int cnt = min(NT, ns - base);
+        if (threadIdx.x < cnt) {
+          int s = s0 + base + threadIdx.x;
+          double y[3], nv[3] = {0, 0, 0};
+          load_point<DIM>(g.sources, g.nsources, s, y);
+          if (sc.cd != 0.0) load_point<DIM>(g.source_normals, g.nsources, s, nv);
+#pragma unroll
+          for (int d = 0; d < DIM; ++d) {
+            s_y[d][threadIdx.x] = y[d];
+            s_n[d][threadIdx.x] = nv[d];
+          }
+          s_q[threadIdx.x] = __ldg(st + s);
+        }
+        __syncthreads();
+        if (active) {
+          for (int j = 0; j < cnt; ++j) {
+            double dx = x[0] - s_y[0][j], dy = x[1] - s_y[1][j];
+            double dz = (DIM == 3) ? x[2] - s_y[2][j] : 0.0;
+            double r2 = dx * dx + dy * dy + dz * dz;
+            if (r2 == 0.0) continue;
+            double q = s_q[j];
+            if (DIM == 3) {
+              double rinv = rsqrt(r2);
+              double v = sc.cq * rinv;
+              if (sc.cd != 0.0)
+                v += sc.cd * (s_n[0][j] * dx + s_n[1][j] * dy + s_n[2][j] * dz) * rinv * rinv * rinv;
+              acc = fma(q, v, acc);
+            } else {
+              double v = 0.5 * sc.cq * log(r2);
+              if (sc.cd != 0.0) v -= sc.cd * (s_n[0][j] * dx + s_n[1][j] * dy) / r2;
+              acc = fma(q, v, acc);
+            }
+          }
+        }
+        __syncthreads();
+      }
+    }
+    if (active) pot[(size_t)r * g.nfiltered_targets + t0 + t] += acc;
+  }
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(NT)
+k_eval_multipoles(qbxfmm_geometry g, int p, int ncf, int nrhs,
+                  const double2* __restrict__ mpoles, double* __restrict__ pot, int32_t* err)
+{
+  extern __shared__ double2 smem2[];
+  double2* M = smem2;
+  int itb = blockIdx.x;
+  int tb = g.target_boxes[itb];
+  int r = blockIdx.y;
+  int t0 = g.nonqbx_box_target_starts[tb];
+  int nt = g.nonqbx_box_target_counts_nonchild[tb];
+  if (nt == 0) return;
+  for (int tbase = 0; tbase < nt; tbase += NT) {
+    int t = tbase + threadIdx.x;
+    bool active = t < nt;
+    double x[3] = {0, 0, 0};
+    if (active) load_point<DIM>(g.nonqbx_targets, g.nfiltered_targets, t0 + t, x);
+    double acc = 0.0;
+    for (int li = g.list3_starts[itb]; li < g.list3_starts[itb + 1]; ++li) {
+      int sb = g.list3_lists[li];
+      if ((unsigned)sb >= (unsigned)g.nboxes) {
+        report(err, QBX_DEVERR_BAD_BOX);
+        continue;
+      }
+      const double2* src = mpoles + ((size_t)sb * nrhs + r) * ncf;
+      for (int q = threadIdx.x; q < ncf; q += NT) M[q] = src[q];
+      __syncthreads();
+      if (active) {
+        double rho = level_width(g, g.box_levels[sb]);
+        double cs[3];
+        load_point<DIM>(g.box_centers, g.nboxes, sb, cs);
+        double u0 = (x[0] - cs[0]) / rho, u1 = (x[1] - cs[1]) / rho;
+        if (DIM == 3) {
+          double u2 = (x[2] - cs[2]) / rho;
+          double rinv2 = 1.0 / (u0 * u0 + u1 * u1 + u2 * u2);
+          double2 mm = c2(sqrt(rinv2));
+          double s = 0.0;
+          for (int m = 0; m <= p; ++m) {
+            if (m > 0) mm = cscale((2.0 * m - 1) * rinv2, cmul(mm, c2(u0, u1)));
+            double w = (m == 0) ? 1.0 : 2.0;
+            double2 a = mm, prev = c2(0.0);
+            for (int n = m; n <= p; ++n) {
+              if (n > m) {
+                double2 bb = cscale(rinv2, csub(cscale((2.0 * n - 1) * u2, a),
+                                                cscale((double)(n + m - 1) * (n - m - 1), prev)));
+                prev = a;
+                a = bb;
+              }
+              double2 cm = M[idx3(n, m)];
+              s += w * (cm.x * a.x - cm.y * a.y);
+            }
+          }
+          acc += s / rho;
+        } else {
+          double2 zc = c2(x[0] - cs[0], x[1] - cs[1]);
+          double2 uinv = cinv(c2(u0, u1));
+          double2 sum = cmul(M[0], clog_(zc));
+          double2 pw = uinv;
+          for (int k = 1; k <= p; ++k) {
+            sum = cfma(M[k], pw, sum);
+            pw = cmul(pw, uinv);
+          }
+          acc += sum.x;
+        }
+      }
+      __syncthreads();
+    }
+    if (active) pot[(size_t)r * g.nfiltered_targets + t0 + t] += acc;
+  }
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(NT)
+k_eval_locals(qbxfmm_geometry g, int p, int ncf, int nrhs, const double2* __restrict__ locals,
+              double* __restrict__ pot)
+{
+  extern __shared__ double2 smem2[];
+  double2* L = smem2;
+  int itb = blockIdx.x;
+  int tb = g.target_boxes[itb];
+  int r = blockIdx.y;
+  int t0 = g.nonqbx_box_target_starts[tb];
+  int nt = g.nonqbx_box_target_counts_nonchild[tb];
+  if (nt == 0) return;
+  const double2* src = locals + ((size_t)tb * nrhs + r) * ncf;
+  for (int q = threadIdx.x; q < ncf; q += NT) L[q] = src[q];
+  __syncthreads();
+  double rho = level_width(g, g.box_levels[tb]);
+  double cb[3];
+  load_point<DIM>(g.box_centers, g.nboxes, tb, cb);
+  for (int t = threadIdx.x; t < nt; t += NT) {
+    double x[3];
+    load_point<DIM>(g.nonqbx_targets, g.nfiltered_targets, t0 + t, x);
+    double u0 = (x[0] - cb[0]) / rho, u1 = (x[1] - cb[1]) / rho;
+    double acc = 0.0;
+    if (DIM == 3) {
+      double u2 = (x[2] - cb[2]) / rho;
+      double r2 = u0 * u0 + u1 * u1 + u2 * u2;
+      double2 mm = c2(1.0);
+      for (int m = 0; m <= p; ++m) {
+        if (m > 0) mm = cscale(1.0 / (2 * m), cmul(mm, c2(u0, u1)));
+        double w = (m == 0) ? 1.0 : 2.0;
+        double2 a = mm, prev = c2(0.0);
+        for (int n = m; n <= p; ++n) {
+          if (n > m) {
+            double2 bb = cscale(1.0 / ((double)(n + m) * (n - m)),
+                                csub(cscale((2.0 * n - 1) * u2, a), cscale(r2, prev)));
+            prev = a;
+            a = bb;
+          }
+          double2 cl = L[idx3(n, m)];
+          acc += w * (cl.x * a.x + cl.y * a.y);   // Re(L conj(R))
+        }
+      }
+    } else {
+      double2 u = c2(u0, u1), pw = c2(1.0), sum = c2(0.0);
+      for (int k = 0; k <= p; ++k) {
+        sum = cfma(L[k], pw, sum);
+        pw = cmul(pw, u);
+      }
+      acc = sum.x;
+    }
+    pot[(size_t)r * g.nfiltered_targets + t0 + t] += acc;
+  }
+}
+
+// }}}
+
+// {{{ QBX stages
+
+// P2QBXL (form_global_qbx_locals, fmm.py:231-265; interactions.py:84-124).
+// CTA = 4 warps over one chunk of <= 32 centers of a target box (lane = center);
+// the list-1 sources stream through shared memory in tiles of 128, each warp
+// taking 32 of them; the warps' partial expansions are summed at the end.
+template <int DIM, int Q, bool CHG, bool DIP>
+__global__ void __launch_bounds__(NT)
+k_p2qbxl(qbxfmm_geometry g, SourceCoeffs sc, int nrhs, const double* __restrict__ strengths,
+         double2* __restrict__ qbx_exps, int32_t* err)
+{
+  constexpr int NC = (DIM == 3) ? (Q + 1) * (Q + 2) / 2 : Q + 1;
+  constexpr int NW = NT / 32;
+  constexpr int MAXB = 128;
+  __shared__ double s_y[3][NT];
+  __shared__ double s_n[3][NT];
+  __shared__ double s_q[NT];
+  __shared__ int s_pref[MAXB + 1];
+  __shared__ int s_start[MAXB];
+  extern __shared__ double2 s_red[];   // [NW-1][32][NC]
+
+  int chunk = blockIdx.x;
+  int r = blockIdx.y;
+  int itb = g.qbx_chunk_target_box[chunk];
+  int cstart = g.qbx_chunk_start[chunk];
+  int ccount = g.qbx_chunk_count[chunk];
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  bool has_center = lane < ccount;
+  int ctr = has_center ? g.centers_by_target_box[cstart + lane] : 0;
+  if ((unsigned)ctr >= (unsigned)g.ncenters) {
+    report(err, QBX_DEVERR_BAD_CENTER);
+    has_center = false;
+    ctr = 0;
+  }
+  double cc[3] = {0, 0, 0};
+  load_point<DIM>(g.centers, g.ncenters, ctr, cc);
+  double rho = g.expansion_radii[ctr];
+  double rinv = 1.0 / rho;
+  const double* st = strengths + (size_t)r * g.nsources;
+
+  double2 acc[NC];
+#pragma unroll
+  for (int i = 0; i < NC; ++i) acc[i] = c2(0.0);
+
+  int l0 = g.list1_starts[itb], l1 = g.list1_starts[itb + 1];
+  for (int gb = l0; gb < l1; gb += MAXB) {
+    int nb = min(MAXB, l1 - gb);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int tot = 0;
+      for (int k = 0; k < nb; ++k) {
+        int sb = g.list1_lists[gb + k];
+        int cnt = 0, s0 = 0;
+        if ((unsigned)sb < (unsigned)g.nboxes) {
+          s0 = g.box_source_starts[sb];
+          cnt = g.box_source_counts_nonchild[sb];
+        } else {
+          report(err, QBX_DEVERR_BAD_BOX);
+        }
+        s_pref[k] = tot;
+        s_start[k] = s0;
+        tot += cnt;
+      }
+      s_pref[nb] = tot;
+    }
+    __syncthreads();
+    int total = s_pref[nb];
+    for (int base = 0; base < total; base += NT) {
+      int v = base + threadIdx.x;
+      if (v < total) {
+        int lo = 0, hi = nb - 1;
+        while (lo < hi) {
+          int mid = (lo + hi + 1) >> 1;
+          if (s_pref[mid] <= v) lo = mid;
+          else hi = mid - 1;
+        }
+        int s = s_start[lo] + (v - s_pref[lo]);
+        double y[3], nv[3] = {0, 0, 0};
+        load_point<DIM>(g.sources, g.nsources, s, y);
+        if (DIP) load_point<DIM>(g.source_normals, g.nsources, s, nv);
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+          s_y[d][threadIdx.x] = y[d];
+          s_n[d][threadIdx.x] = nv[d];
+        }
+        s_q[threadIdx.x] = __ldg(st + s);
+      }
+      __syncthreads();
+      int jbeg = warp * 32;
+      int jend = min(jbeg + 32, total - base);
+      if (has_center) {
+        for (int j = jbeg; j < jend; ++j) {
+          double q = s_q[j];
+          if (DIM == 3) {
+            double ux = (s_y[0][j] - cc[0]) * rinv;
+            double uy = (s_y[1][j] - cc[1]) * rinv;
+            double uz = (s_y[2][j] - cc[2]) * rinv;
+            double r2 = ux * ux + uy * uy + uz * uz;
+            double ri = rsqrt(r2);
+            double ri2 = ri * ri;
+            SRegs<DIP ? Q + 1 : Q> S;
+            S.build(ux, uy, uz, ri, ri2);
+            double fq = sc.cq * q * rinv;
+            double fd = sc.cd * q * rinv * rinv;
+            double dz = fd * s_n[2][j];
+            double2 dp = c2(0.5 * fd * s_n[0][j], 0.5 * fd * s_n[1][j]);
+            double2 dm = c2(0.5 * fd * s_n[0][j], -0.5 * fd * s_n[1][j]);
+#pragma unroll
+            for (int n = 0; n <= Q; ++n)
+#pragma unroll
+              for (int m = 0; m <= n; ++m) {
+                double2 a = acc[idx3(n, m)];
+                if (CHG) a = caxpy(fq, S.v[idx3(n, m)], a);
+                if (DIP) {
+                  a = caxpy(-dz, S.v[idx3(n + 1, m)], a);
+                  a = cfma(dp, S.get(n + 1, m - 1), a);
+                  a = cfma(c2(-dm.x, -dm.y), S.v[idx3(n + 1, m + 1)], a);
+                }
+                acc[idx3(n, m)] = a;
+              }
+          } else {
+            double tx = s_y[0][j] - cc[0], ty = s_y[1][j] - cc[1];
+            double2 tinv = cinv(c2(tx * rinv, ty * rinv));
+            double2 pw = tinv;   // tau^-l
+            if (CHG) acc[0].x += sc.cq * q * 0.5 * log(tx * tx + ty * ty);
+            double2 fnu = c2(sc.cd * q * rinv * s_n[0][j], sc.cd * q * rinv * s_n[1][j]);
+#pragma unroll
+            for (int l = 0; l <= Q; ++l) {
+              if (l > 0) {
+                if (CHG) acc[l] = caxpy(-sc.cq * q / l, pw, acc[l]);
+                pw = cmul(pw, tinv);
+              }
+              if (DIP) acc[l] = cfma(fnu, pw, acc[l]);   // pw = tau^-(l+1)
+            }
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  // reduce the warps' partial sums
+  if (warp > 0) {
+#pragma unroll
+    for (int i = 0; i < NC; ++i) s_red[((warp - 1) * 32 + lane) * NC + i] = acc[i];
+  }
+  __syncthreads();
+  if (warp == 0 && has_center) {
+    double2* out = qbx_exps + ((size_t)ctr * nrhs + r) * NC;
+#pragma unroll
+    for (int i = 0; i < NC; ++i) {
+      double2 a = acc[i];
+      for (int w = 1; w < NW; ++w) a = cadd(a, s_red[((w - 1) * 32 + lane) * NC + i]);
+      out[i] = cadd(out[i], a);
+    }
+  }
+}
+
+// M2QBXL (translate_box_multipoles_to_qbx_local, fmm.py:267-312;
+// interactions.py:196-235): one warp per center chunk; list-3 multipoles staged in
+// shared memory; each lane runs the singular-harmonic recurrence for its center and
+// scatters into its register-resident QBX coefficients.
+template <int DIM, int Q>
+__global__ void __launch_bounds__(32)
+k_m2qbxl(qbxfmm_geometry g, int pf, int ncf, int nrhs, const double2* __restrict__ mpoles,
+         double2* __restrict__ qbx_exps, int32_t* err)
+{
+  constexpr int NC = (DIM == 3) ? (Q + 1) * (Q + 2) / 2 : Q + 1;
+  extern __shared__ double2 smem2[];
+  double2* M = smem2;
+  int chunk = blockIdx.x;
+  int r = blockIdx.y;
+  int itb = g.qbx_chunk_target_box[chunk];
+  int lane = threadIdx.x;
+  bool has_center = lane < g.qbx_chunk_count[chunk];
+  int ctr = has_center ? g.centers_by_target_box[g.qbx_chunk_start[chunk] + lane] : 0;
+  double cc[3] = {0, 0, 0};
+  load_point<DIM>(g.centers, g.ncenters, ctr, cc);
+  double rho_t = g.expansion_radii[ctr];
+  double2 acc[NC];
+#pragma unroll
+  for (int i = 0; i < NC; ++i) acc[i] = c2(0.0);
+  for (int li = g.list3_starts[itb]; li < g.list3_starts[itb + 1]; ++li) {
+    int sb = g.list3_lists[li];
+    if ((unsigned)sb >= (unsigned)g.nboxes) {
+      report(err, QBX_DEVERR_BAD_BOX);
+      continue;
+    }
+    __syncwarp();
+    const double2* src = mpoles + ((size_t)sb * nrhs + r) * ncf;
+    for (int q = lane; q < ncf; q += 32) M[q] = src[q];
+    __syncwarp();
+    if (!has_center) continue;
+    double rho_s = level_width(g, g.box_levels[sb]);
+    double cs[3];
+    load_point<DIM>(g.box_centers, g.nboxes, sb, cs);
+    double ratio = rho_t / rho_s;
+    if (DIM == 3) {
+      double d0 = (cc[0] - cs[0]) / rho_s, d1 = (cc[1] - cs[1]) / rho_s, d2 = (cc[2] - cs[2]) / rho_s;
+      double rinv2 = 1.0 / (d0 * d0 + d1 * d1 + d2 * d2);
+      int nmax = pf + Q;
+      double2 part[NC];
+#pragma unroll
+      for (int i = 0; i < NC; ++i) part[i] = c2(0.0);
+      double2 mm = c2(sqrt(rinv2));
+      for (int mp = 0; mp <= nmax; ++mp) {
+        if (mp > 0) mm = cscale((2.0 * mp - 1) * rinv2, cmul(mm, c2(d0, d1)));
+        double2 a = mm, prev = c2(0.0);
+        for (int np = mp; np <= nmax; ++np) {
+          if (np > mp) {
+            double2 bb = cscale(rinv2, csub(cscale((2.0 * np - 1) * d2, a),
+                                            cscale((double)(np + mp - 1) * (np - mp - 1), prev)));
+            prev = a;
+            a = bb;
+          }
+          // S_{np}^{mp} = a ; S_{np}^{-mp} = (-1)^mp conj(a)
+          double2 aneg = (mp & 1) ? c2(-a.x, a.y) : c2(a.x, -a.y);
+#pragma unroll
+          for (int j = 0; j <= Q; ++j)
+#pragma unroll
+            for (int ii = 0; ii <= j; ++ii) {
+              int k = np - j;
+              if (k < 0 || k > pf) continue;
+              int l = mp - ii;
+              if (l <= k && -l <= k) part[idx3(j, ii)] = cfma(sh3_get(M, k, l), a, part[idx3(j, ii)]);
+              if (mp > 0) {
+                int l2 = -mp - ii;
+                if (-l2 <= k) part[idx3(j, ii)] = cfma(sh3_get(M, k, l2), aneg, part[idx3(j, ii)]);
+              }
+            }
+        }
+      }
+      double rj = 1.0 / rho_s;
+#pragma unroll
+      for (int j = 0; j <= Q; ++j) {
+#pragma unroll
+        for (int ii = 0; ii <= j; ++ii)
+          acc[idx3(j, ii)] = caxpy((j & 1) ? -rj : rj, part[idx3(j, ii)], acc[idx3(j, ii)]);
+        rj *= ratio;
+      }
+    } else {
+      double2 tau = c2((cc[0] - cs[0]) / rho_s, (cc[1] - cs[1]) / rho_s);
+      double2 tinv = cinv(tau);
+      double2 t = c2(cc[0] - cs[0], cc[1] - cs[1]);
+      // L0 = M0 log t + sum_k Mk tau^-k ;
+      // Ll = ratio^l [M0 (-1)^(l+1)/(l tau^l) + (-1)^l tau^-l sum_k Mk C(k+l-1,l) tau^-k]
+      double2 s0 = cmul(M[0], clog_(t));
+      double2 sl[Q + 1];
+      double bin[Q + 1];
+#pragma unroll
+      for (int l = 0; l <= Q; ++l) {
+        sl[l] = c2(0.0);
+        bin[l] = 1.0;
+      }
+      double2 pw = tinv;
+      for (int k = 1; k <= pf; ++k) {
+        double2 mk = cmul(M[k], pw);
+        s0 = cadd(s0, mk);
+#pragma unroll
+        for (int l = 1; l <= Q; ++l) {
+          sl[l] = caxpy(bin[l], mk, sl[l]);
+          bin[l] = bin[l] * (k + l) / k;
+        }
+        pw = cmul(pw, tinv);
+      }
+      acc[0] = cadd(acc[0], s0);
+      double2 tl = tinv;
+      double rl = ratio;
+#pragma unroll
+      for (int l = 1; l <= Q; ++l) {
+        double2 v = cscale(((l & 1) ? 1.0 : -1.0) / l, M[0]);
+        v = cadd(v, cscale((l & 1) ? -1.0 : 1.0, sl[l]));
+        acc[l] = cadd(acc[l], cscale(rl, cmul(v, tl)));
+        tl = cmul(tl, tinv);
+        rl *= ratio;
+      }
+    }
+  }
+  if (has_center) {
+    double2* out = qbx_exps + ((size_t)ctr * nrhs + r) * NC;
+#pragma unroll
+    for (int i = 0; i < NC; ++i) out[i] = cadd(out[i], acc[i]);
+  }
+}
+
+// L2QBXL (translate_box_local_to_qbx_local, fmm.py:314-356; interactions.py:318-356)
+template <int DIM, int Q>
+__global__ void __launch_bounds__(NT)
+k_l2qbxl(qbxfmm_geometry g, int pf, int ncf, int nrhs, const double2* __restrict__ locals,
+         double2* __restrict__ qbx_exps)
+{
+  constexpr int NC = (DIM == 3) ? (Q + 1) * (Q + 2) / 2 : Q + 1;
+  int ig = blockIdx.x * blockDim.x + threadIdx.x;
+  int r = blockIdx.y;
+  if (ig >= g.nglobal_qbx_centers) return;
+  int ctr = g.global_qbx_centers[ig];
+  int tb = g.target_boxes[g.qbx_center_to_target_box[ctr]];
+  double cc[3], cb[3];
+  load_point<DIM>(g.centers, g.ncenters, ctr, cc);
+  load_point<DIM>(g.box_centers, g.nboxes, tb, cb);
+  double rho_b = level_width(g, g.box_levels[tb]);
+  double rho_c = g.expansion_radii[ctr];
+  double ratio = rho_c / rho_b;
+  const double2* Lin = locals + ((size_t)tb * nrhs + r) * ncf;
+  double2 acc[NC];
+#pragma unroll
+  for (int i = 0; i < NC; ++i) acc[i] = c2(0.0);
+  if (DIM == 3) {
+    double d0 = (cc[0] - cb[0]) / rho_b, d1 = (cc[1] - cb[1]) / rho_b, d2 = (cc[2] - cb[2]) / rho_b;
+    double r2 = d0 * d0 + d1 * d1 + d2 * d2;
+    double2 mm = c2(1.0);
+    // R_a^b(d): output (k,l) += L_{a+k}^{b+l} conj(R_a^b)
+    for (int bm = 0; bm <= pf; ++bm) {
+      if (bm > 0) mm = cscale(1.0 / (2 * bm), cmul(mm, c2(d0, d1)));
+      double2 a = mm, prev = c2(0.0);
+      for (int an = bm; an <= pf; ++an) {
+        if (an > bm) {
+          double2 bb = cscale(1.0 / ((double)(an + bm) * (an - bm)),
+                              csub(cscale((2.0 * an - 1) * d2, a), cscale(r2, prev)));
+          prev = a;
+          a = bb;
+        }
+        double2 aneg = (bm & 1) ? c2(-a.x, a.y) : c2(a.x, -a.y);  // R_an^{-bm}
+#pragma unroll
+        for (int k = 0; k <= Q; ++k)
+#pragma unroll
+          for (int l = 0; l <= k; ++l) {
+            int n = an + k;
+            if (n > pf) continue;
+            int m = bm + l;
+            if (m <= n) acc[idx3(k, l)] = cfmac(sh3_get(Lin, n, m), a, acc[idx3(k, l)]);
+            if (bm > 0) {
+              int m2 = -bm + l;
+              if (-m2 <= n && m2 <= n)
+                acc[idx3(k, l)] = cfmac(sh3_get(Lin, n, m2), aneg, acc[idx3(k, l)]);
+            }
+          }
+      }
+    }
+    double rk = 1.0;
+#pragma unroll
+    for (int k = 0; k <= Q; ++k) {
+#pragma unroll
+      for (int l = 0; l <= k; ++l) acc[idx3(k, l)] = cscale(rk, acc[idx3(k, l)]);
+      rk *= ratio;
+    }
+  } else {
+    double2 s = c2((cc[0] - cb[0]) / rho_b, (cc[1] - cb[1]) / rho_b);
+    double rl = 1.0;
+#pragma unroll
+    for (int l = 0; l <= Q; ++l) {
+      double2 a = c2(0.0), sp = c2(1.0);
+      double bin = 1.0;
+      for (int k = l; k <= pf; ++k) {
+        a = cfma(cscale(bin, Lin[k]), sp, a);
+        sp = cmul(sp, s);
+        bin = bin * (k + 1) / (k + 1 - l);
+      }
+      acc[l] = cscale(rl, a);
+      rl *= ratio;
+    }
+  }
+  double2* out = qbx_exps + ((size_t)ctr * nrhs + r) * NC;
+#pragma unroll
+  for (int i = 0; i < NC; ++i) out[i] = cadd(out[i], acc[i]);
+}
+
+// QBXL2P (eval_qbx_expansions, fmm.py:358-389; interactions.py:442-479)
+template <int DIM, int Q>
+__global__ void __launch_bounds__(NT)
+k_qbxl2p(qbxfmm_geometry g, int nrhs, const double2* __restrict__ qbx_exps,
+         double* __restrict__ pot_tree)
+{
+  constexpr int NC = (DIM == 3) ? (Q + 1) * (Q + 2) / 2 : Q + 1;
+  int ig = blockIdx.x * blockDim.x + threadIdx.x;
+  int r = blockIdx.y;
+  if (ig >= g.nglobal_qbx_centers) return;
+  int ctr = g.global_qbx_centers[ig];
+  double cc[3];
+  load_point<DIM>(g.centers, g.ncenters, ctr, cc);
+  double rinv = 1.0 / g.expansion_radii[ctr];
+  double2 L[NC];
+  const double2* src = qbx_exps + ((size_t)ctr * nrhs + r) * NC;
+#pragma unroll
+  for (int i = 0; i < NC; ++i) L[i] = src[i];
+  for (int it = g.center_to_targets_starts[ctr]; it < g.center_to_targets_starts[ctr + 1]; ++it) {
+    int t = g.center_to_targets_lists[it];
+    double x[3];
+    load_point<DIM>(g.targets, g.ntargets, t, x);
+    double acc = 0.0;
+    if (DIM == 3) {
+      RRegs<Q> R;
+      R.build((x[0] - cc[0]) * rinv, (x[1] - cc[1]) * rinv, (x[2] - cc[2]) * rinv);
+#pragma unroll
+      for (int n = 0; n <= Q; ++n)
+#pragma unroll
+        for (int m = 0; m <= n; ++m) {
+          double2 a = L[idx3(n, m)], b = R.v[idx3(n, m)];
+          acc += (m == 0 ? 1.0 : 2.0) * (a.x * b.x + a.y * b.y);
+        }
+    } else {
+      double2 u = c2((x[0] - cc[0]) * rinv, (x[1] - cc[1]) * rinv), pw = c2(1.0), s = c2(0.0);
+#pragma unroll
+      for (int k = 0; k <= Q; ++k) {
+        s = cfma(L[k], pw, s);
+        pw = cmul(pw, u);
+      }
+      acc = s.x;
+    }
+    pot_tree[(size_t)r * g.ntargets + t] = acc;
+  }
+}
+
+// }}}
+
+// {{{ assembly (fmm.py:569-588; qbx/__init__.py:775-793)
+
+__global__ void k_assemble_tree(qbxfmm_geometry g, double scale, int nrhs,
+                                const double* __restrict__ pot_tree, double* __restrict__ out)
+{
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  int r = blockIdx.y;
+  if (t >= g.ntargets) return;
+  int u = g.sorted_target_ids[t] - g.ncenters;
+  if (u >= 0) out[(size_t)r * g.nuser_targets + u] = scale * pot_tree[(size_t)r * g.ntargets + t];
+}
+
+__global__ void k_assemble_nonqbx(qbxfmm_geometry g, double scale, int nrhs,
+                                  const double* __restrict__ pot_nonqbx, double* __restrict__ out)
+{
+  int f = blockIdx.x * blockDim.x + threadIdx.x;
+  int r = blockIdx.y;
+  if (f >= g.nfiltered_targets) return;
+  int t = g.unfiltered_from_filtered_target_indices[f];
+  int u = g.sorted_target_ids[t] - g.ncenters;
+  if (u >= 0) out[(size_t)r * g.nuser_targets + u] += scale * pot_nonqbx[(size_t)r * g.nfiltered_targets + f];
+}
+
+// }}}
+
+// {{{ launchers
+
+static int grid_y(int nrhs) { return nrhs; }
+
+static size_t ncoef_dim(int dim, int p) { return dim == 3 ? (size_t)(p + 1) * (p + 2) / 2 : (size_t)p + 1; }
+
+cudaError_t launch_form_strengths(const qbxfmm_geometry& g, const qbxfmm_upsample& up, int nrhs,
+                                  const double* density, double* strengths, cudaStream_t st)
+{
+  dim3 grid((g.nsources + 255) / 256, nrhs);
+  k_form_strengths<<<grid, 256, 0, st>>>(g.nsources, up.nelements * up.nodes_per_element,
+                                         up.nodes_per_element, up.quad_nodes_per_element,
+                                         up.matrix, up.quad_weights, g.user_source_ids, density,
+                                         strengths);
+  return cudaGetLastError();
+}
+
+template <int DIM>
+static cudaError_t p2m_(const qbxfmm_geometry& g, SourceCoeffs sc, int p, int nrhs,
+                        const double* s, double2* mp, cudaStream_t st)
+{
+  int ncf = (int)ncoef_dim(DIM, p);
+  size_t sh = 16 * (size_t)ncf * sizeof(double2);
+  if (g.nsource_boxes == 0) return cudaSuccess;
+  cudaFuncSetAttribute(k_p2m<DIM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+  k_p2m<DIM><<<dim3(g.nsource_boxes, grid_y(nrhs)), NT, sh, st>>>(g, sc, p, ncf, nrhs, s, mp);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_p2m(const qbxfmm_geometry& g, SourceCoeffs sc, int p, int nrhs,
+                       const double* s, double2* mp, cudaStream_t st)
+{
+  return g.dim == 3 ? p2m_<3>(g, sc, p, nrhs, s, mp, st) : p2m_<2>(g, sc, p, nrhs, s, mp, st);
+}
+
+template <int DIM>
+static cudaError_t m2m_(const qbxfmm_geometry& g, const int32_t* lvl_host, int p, int nrhs,
+                        double2* mp, cudaStream_t st)
+{
+  int ncf = (int)ncoef_dim(DIM, p);
+  size_t sh = 2 * (size_t)ncf * sizeof(double2);
+  for (int lev = g.nlevels - 2; lev >= 0; --lev) {
+    int i0 = lvl_host[lev], i1 = lvl_host[lev + 1];
+    if (i1 <= i0) continue;
+    k_m2m<DIM><<<dim3(i1 - i0, grid_y(nrhs)), NT, sh, st>>>(g, p, ncf, nrhs, i0, mp);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+cudaError_t launch_m2m(const qbxfmm_geometry& g, const int32_t* lvl_host, int p, int nrhs,
+                       double2* mp, cudaStream_t st)
+{
+  return g.dim == 3 ? m2m_<3>(g, lvl_host, p, nrhs, mp, st) : m2m_<2>(g, lvl_host, p, nrhs, mp, st);
+}
+
+template <int DIM>
+static cudaError_t m2l_(const qbxfmm_geometry& g, int p, int nrhs, const double2* mp,
+                        double2* lo, int32_t* err, cudaStream_t st)
+{
+  if (g.nttp_boxes == 0) return cudaSuccess;
+  int ncf = (int)ncoef_dim(DIM, p);
+  size_t sh = ((size_t)ncf + (DIM == 3 ? ncoef_dim(3, 2 * p) : (size_t)2 * p + 2)) * sizeof(double2);
+  cudaFuncSetAttribute(k_m2l<DIM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+  k_m2l<DIM><<<dim3(g.nttp_boxes, grid_y(nrhs)), NT, sh, st>>>(g, p, ncf, nrhs, mp, lo, err);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_m2l(const qbxfmm_geometry& g, int p, int nrhs, const double2* mp, double2* lo,
+                       int32_t* err, cudaStream_t st)
+{
+  return g.dim == 3 ? m2l_<3>(g, p, nrhs, mp, lo, err, st) : m2l_<2>(g, p, nrhs, mp, lo, err, st);
+}
+
+template <int DIM>
+static cudaError_t p2l_(const qbxfmm_geometry& g, SourceCoeffs sc, int p, int nrhs,
+                        const double* s, double2* lo, int32_t* err, cudaStream_t st)
+{
+  if (g.nttp_boxes == 0) return cudaSuccess;
+  int ncf = (int)ncoef_dim(DIM, p);
+  int nct = DIM == 3 ? (p + 2) * (p + 3) / 2 : p + 3;
+  size_t sh = 16 * (size_t)nct * sizeof(double2);
+  cudaFuncSetAttribute(k_p2l<DIM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+  k_p2l<DIM><<<dim3(g.nttp_boxes, grid_y(nrhs)), NT, sh, st>>>(g, sc, p, ncf, nrhs, s, lo, err);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_p2l(const qbxfmm_geometry& g, SourceCoeffs sc, int p, int nrhs,
+                       const double* s, double2* lo, int32_t* err, cudaStream_t st)
+{
+  return g.dim == 3 ? p2l_<3>(g, sc, p, nrhs, s, lo, err, st) : p2l_<2>(g, sc, p, nrhs, s, lo, err, st);
+}
+
+template <int DIM>
+static cudaError_t l2l_(const qbxfmm_geometry& g, const int32_t* lvl_host, int p, int nrhs,
+                        double2* lo, cudaStream_t st)
+{
+  int ncf = (int)ncoef_dim(DIM, p);
+  size_t sh = 2 * (size_t)ncf * sizeof(double2);
+  for (int lev = 1; lev < g.nlevels; ++lev) {
+    int i0 = lvl_host[lev], i1 = lvl_host[lev + 1];
+    if (i1 <= i0) continue;
+    k_l2l<DIM><<<dim3(i1 - i0, grid_y(nrhs)), NT, sh, st>>>(g, p, ncf, nrhs, i0, lo);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+cudaError_t launch_l2l(const qbxfmm_geometry& g, const int32_t* lvl_host, int p, int nrhs,
+                       double2* lo, cudaStream_t st)
+{
+  return g.dim == 3 ? l2l_<3>(g, lvl_host, p, nrhs, lo, st) : l2l_<2>(g, lvl_host, p, nrhs, lo, st);
+}
+
+cudaError_t launch_eval_direct(const qbxfmm_geometry& g, SourceCoeffs sc, int nrhs,
+                               const double* s, double* pot, int32_t* err, cudaStream_t st)
+{
+  if (g.ntarget_boxes == 0 || g.nfiltered_targets == 0) return cudaSuccess;
+  dim3 grid(g.ntarget_boxes, grid_y(nrhs));
+  if (g.dim == 3) k_eval_direct<3><<<grid, NT, 0, st>>>(g, sc, nrhs, s, pot, err);
+  else k_eval_direct<2><<<grid, NT, 0, st>>>(g, sc, nrhs, s, pot, err);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_eval_multipoles(const qbxfmm_geometry& g, int p, int nrhs, const double2* mp,
+                                   double* pot, int32_t* err, cudaStream_t st)
+{
+  if (g.ntarget_boxes == 0 || g.nfiltered_targets == 0) return cudaSuccess;
+  int ncf = (int)ncoef_dim(g.dim, p);
+  size_t sh = (size_t)ncf * sizeof(double2);
+  dim3 grid(g.ntarget_boxes, grid_y(nrhs));
+  if (g.dim == 3) k_eval_multipoles<3><<<grid, NT, sh, st>>>(g, p, ncf, nrhs, mp, pot, err);
+  else k_eval_multipoles<2><<<grid, NT, sh, st>>>(g, p, ncf, nrhs, mp, pot, err);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_eval_locals(const qbxfmm_geometry& g, int p, int nrhs, const double2* lo,
+                               double* pot, cudaStream_t st)
+{
+  if (g.ntarget_boxes == 0 || g.nfiltered_targets == 0) return cudaSuccess;
+  int ncf = (int)ncoef_dim(g.dim, p);
+  size_t sh = (size_t)ncf * sizeof(double2);
+  dim3 grid(g.ntarget_boxes, grid_y(nrhs));
+  if (g.dim == 3) k_eval_locals<3><<<grid, NT, sh, st>>>(g, p, ncf, nrhs, lo, pot);
+  else k_eval_locals<2><<<grid, NT, sh, st>>>(g, p, ncf, nrhs, lo, pot);
+  return cudaGetLastError();
+}
+
+template <int DIM, int Q>
+static cudaError_t p2qbxl_q(const qbxfmm_geometry& g, SourceCoeffs sc, int nrhs, const double* s,
+                            double2* qe, int32_t* err, cudaStream_t st)
+{
+  constexpr int NC = (DIM == 3) ? (Q + 1) * (Q + 2) / 2 : Q + 1;
+  size_t sh = (size_t)(NT / 32 - 1) * 32 * NC * sizeof(double2);
+  dim3 grid(g.nqbx_chunks, grid_y(nrhs));
+  if (sc.cq != 0.0 && sc.cd != 0.0) {
+    cudaFuncSetAttribute(k_p2qbxl<DIM, Q, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+    k_p2qbxl<DIM, Q, true, true><<<grid, NT, sh, st>>>(g, sc, nrhs, s, qe, err);
+  } else if (sc.cd != 0.0) {
+    cudaFuncSetAttribute(k_p2qbxl<DIM, Q, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+    k_p2qbxl<DIM, Q, false, true><<<grid, NT, sh, st>>>(g, sc, nrhs, s, qe, err);
+  } else {
+    cudaFuncSetAttribute(k_p2qbxl<DIM, Q, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+    k_p2qbxl<DIM, Q, true, false><<<grid, NT, sh, st>>>(g, sc, nrhs, s, qe, err);
+  }
+  return cudaGetLastError();
+}
+
+template <int DIM, int Q>
+static cudaError_t m2qbxl_q(const qbxfmm_geometry& g, int pf, int nrhs, const double2* mp,
+                            double2* qe, int32_t* err, cudaStream_t st)
+{
+  int ncf = (int)ncoef_dim(DIM, pf);
+  size_t sh = (size_t)ncf * sizeof(double2);
+  k_m2qbxl<DIM, Q><<<dim3(g.nqbx_chunks, grid_y(nrhs)), 32, sh, st>>>(g, pf, ncf, nrhs, mp, qe, err);
+  return cudaGetLastError();
+}
+
+template <int DIM, int Q>
+static cudaError_t l2qbxl_q(const qbxfmm_geometry& g, int pf, int nrhs, const double2* lo,
+                            double2* qe, cudaStream_t st)
+{
+  int ncf = (int)ncoef_dim(DIM, pf);
+  dim3 grid((g.nglobal_qbx_centers + NT - 1) / NT, grid_y(nrhs));
+  k_l2qbxl<DIM, Q><<<grid, NT, 0, st>>>(g, pf, ncf, nrhs, lo, qe);
+  return cudaGetLastError();
+}
+
+template <int DIM, int Q>
+static cudaError_t qbxl2p_q(const qbxfmm_geometry& g, int nrhs, const double2* qe, double* pt,
+                            cudaStream_t st)
+{
+  dim3 grid((g.nglobal_qbx_centers + NT - 1) / NT, grid_y(nrhs));
+  k_qbxl2p<DIM, Q><<<grid, NT, 0, st>>>(g, nrhs, qe, pt);
+  return cudaGetLastError();
+}
+
+#define QBX_DISPATCH_Q(FN, DIM, Q, ...)                               \
+  switch (Q) {                                                        \
+    case 0: return FN<DIM, 0>(__VA_ARGS__);                            \
+    case 1: return FN<DIM, 1>(__VA_ARGS__);                            \
+    case 2: return FN<DIM, 2>(__VA_ARGS__);                            \
+    case 3: return FN<DIM, 3>(__VA_ARGS__);                            \
+    case 4: return FN<DIM, 4>(__VA_ARGS__);                            \
+    case 5: return FN<DIM, 5>(__VA_ARGS__);                            \
+    case 6: return FN<DIM, 6>(__VA_ARGS__);                            \
+    case 7: return FN<DIM, 7>(__VA_ARGS__);                            \
+    case 8: return FN<DIM, 8>(__VA_ARGS__);                            \
+    default: return cudaErrorInvalidValue;                            \
+  }
+
+cudaError_t launch_p2qbxl(const qbxfmm_geometry& g, SourceCoeffs sc, int q, int nrhs,
+                          const double* s, double2* qe, int32_t* err, cudaStream_t st)
+{
+  if (g.nqbx_chunks == 0) return cudaSuccess;
+  if (g.dim == 3) { QBX_DISPATCH_Q(p2qbxl_q, 3, q, g, sc, nrhs, s, qe, err, st) }
+  QBX_DISPATCH_Q(p2qbxl_q, 2, q, g, sc, nrhs, s, qe, err, st)
+}
+
+cudaError_t launch_m2qbxl(const qbxfmm_geometry& g, int pf, int q, int nrhs, const double2* mp,
+                          double2* qe, int32_t* err, cudaStream_t st)
+{
+  if (g.nqbx_chunks == 0) return cudaSuccess;
+  if (g.dim == 3) { QBX_DISPATCH_Q(m2qbxl_q, 3, q, g, pf, nrhs, mp, qe, err, st) }
+  QBX_DISPATCH_Q(m2qbxl_q, 2, q, g, pf, nrhs, mp, qe, err, st)
+}
+
+cudaError_t launch_l2qbxl(const qbxfmm_geometry& g, int pf, int q, int nrhs, const double2* lo,
+                          double2* qe, cudaStream_t st)
+{
+  if (g.nglobal_qbx_centers == 0) return cudaSuccess;
+  if (g.dim == 3) { QBX_DISPATCH_Q(l2qbxl_q, 3, q, g, pf, nrhs, lo, qe, st) }
+  QBX_DISPATCH_Q(l2qbxl_q, 2, q, g, pf, nrhs, lo, qe, st)
+}
+
+cudaError_t launch_qbxl2p(const qbxfmm_geometry& g, int q, int nrhs, const double2* qe,
+                          double* pt, cudaStream_t st)
+{
+  if (g.nglobal_qbx_centers == 0) return cudaSuccess;
+  if (g.dim == 3) { QBX_DISPATCH_Q(qbxl2p_q, 3, q, g, nrhs, qe, pt, st) }
+  QBX_DISPATCH_Q(qbxl2p_q, 2, q, g, nrhs, qe, pt, st)
+}
+
+cudaError_t launch_assemble(const qbxfmm_geometry& g, int nrhs, const double* pot_nonqbx,
+                            const double* pot_tree, double* out, cudaStream_t st)
+{
+  double scale = g.dim == 3 ? 0.25 / M_PI : -0.5 / M_PI;
+  if (g.ntargets > 0) {
+    k_assemble_tree<<<dim3((g.ntargets + 255) / 256, nrhs), 256, 0, st>>>(g, scale, nrhs, pot_tree, out);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  if (g.nfiltered_targets > 0) {
+    k_assemble_nonqbx<<<dim3((g.nfiltered_targets + 255) / 256, nrhs), 256, 0, st>>>(
+        g, scale, nrhs, pot_nonqbx, out);
+  }
+  return cudaGetLastError();
+}
+
+// }}}
+
+}  // namespace qbx

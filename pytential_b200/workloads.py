@@ -1,0 +1,96 @@
+"""Synthetic workloads with the shapes of the benchmark configurations.
+
+All inputs are analytic geometry plus seeded noise (``numpy.random.default_rng``);
+nothing is read from disk.
+
+* ``laplace2d_starfish``: closed 5-arm starfish ``(1 + 0.25 cos 5t)(cos t, sin t)``,
+  ``nelements`` x 16 Gauss-Legendre nodes upsampled to 64 per element;
+  single layer, exterior limit on the surface plus 1000 volume points in
+  ``[-2, 2]^2``; density ``cos 3t + 0.1 N(0, 1)``; qbx_order 4, fmm_order 10.
+* ``laplace3d_ellipsoid``: ellipsoid (1, 1.5, 2) from an icosphere refined
+  ``nrefine`` times, 15 nodes per triangle upsampled to 45; double layer,
+  exterior limit on the surface plus 2000 points uniform in the shell
+  2.5 <= r <= 3.5; density Re Y_3^2 on the parameter sphere + 0.05 N(0, 1);
+  qbx_order 3, fmm_order 10.
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .discretization import Discretization, make_ellipsoid, make_starfish
+from .fmm import LaplaceKernel, SourceKernelSpec
+from .geometry import QBXFMMGeometryData
+
+
+@dataclass
+class Workload:
+    name: str
+    discr: Discretization
+    targets: list            # [(points (dim, n), side)]
+    density: np.ndarray      # (nrhs, ndofs)
+    spec: SourceKernelSpec
+    qbx_order: int
+    fmm_order: int
+    seed: int
+    info: dict = field(default_factory=dict)
+    _geo: QBXFMMGeometryData | None = None
+
+    @property
+    def nrhs(self):
+        return self.density.shape[0]
+
+    def geometry(self) -> QBXFMMGeometryData:
+        if self._geo is None:
+            self._geo = QBXFMMGeometryData(self.discr, self.targets)
+        return self._geo
+
+    @property
+    def nuser_targets(self):
+        return sum(p.shape[1] for p, _ in self.targets)
+
+    def tree_strengths(self):
+        """Flat strengths in tree order (float64, (nrhs, nsources)) for the checker."""
+        geo = self.geometry()
+        w = self.discr.upsample_density(self.density) * self.discr.quad_weights
+        return np.ascontiguousarray(w[:, geo.tree().user_source_ids])
+
+
+def laplace2d_starfish(nelements: int = 64, nvolume: int = 1000, seed: int = 0,
+                       op: str = "S", qbx_order: int = 4, fmm_order: int = 10,
+                       nrhs: int = 1) -> Workload:
+    rng = np.random.default_rng(seed)
+    d = make_starfish(nelements)
+    t = d.param[:, 0]
+    dens = np.stack([np.cos(3 * t) + 0.1 * rng.normal(size=d.ndofs) for _ in range(nrhs)])
+    vol = rng.uniform(-2, 2, size=(2, nvolume))
+    spec = SourceKernelSpec(LaplaceKernel(2), charge_coeff=1.0 if op == "S" else 0.0,
+                            dipole_coeff=1.0 if op == "D" else 0.0)
+    return Workload(f"2D Laplace {op}, starfish {nelements}x16 nodes", d,
+                    [(d.nodes, +1), (vol, 0)], dens, spec, qbx_order, fmm_order, seed)
+
+
+def _real_y32(points):
+    s = points / np.linalg.norm(points, axis=0)
+    ct = s[2]
+    st2 = 1 - ct ** 2
+    phi = np.arctan2(s[1], s[0])
+    return np.sqrt(105 / (32 * np.pi)) * st2 * ct * np.cos(2 * phi)
+
+
+def laplace3d_ellipsoid(nrefine: int = 3, nshell: int = 2000, seed: int = 0,
+                        op: str = "D", qbx_order: int = 3, fmm_order: int = 10,
+                        nrhs: int = 1) -> Workload:
+    rng = np.random.default_rng(seed)
+    d = make_ellipsoid(nrefine)
+    base = _real_y32(d.nodes)
+    dens = np.stack([base + 0.05 * rng.normal(size=d.ndofs) for _ in range(nrhs)])
+    v = rng.normal(size=(3, nshell))
+    v /= np.linalg.norm(v, axis=0)
+    r = rng.uniform(2.5 ** 3, 3.5 ** 3, nshell) ** (1 / 3)
+    spec = SourceKernelSpec(LaplaceKernel(3), charge_coeff=1.0 if op == "S" else 0.0,
+                            dipole_coeff=1.0 if op == "D" else 0.0)
+    return Workload(f"3D Laplace {op}, ellipsoid icosphere-{nrefine} ({d.nelements} tri)",
+                    d, [(d.nodes, +1), (v * r, 0)], dens, spec, qbx_order, fmm_order, seed)

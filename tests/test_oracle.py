@@ -1,0 +1,106 @@
+"""The CPU checker itself, pinned before it is trusted.
+
+* against the reference's own compiled target-specific QBX module (golden fixture
+  tests/golden/tsqbx_laplace3d.npz, tolerance 1e-13 as in
+  test/test_target_specific_qbx.py:218);
+* FMM against direct (non-FMM) QBX with the same truncation, at the FMM's
+  truncation level (test/test_layer_pot.py:153-230 checks 1e-3);
+* linearity of the apply.
+"""
+
+import ctypes
+
+import numpy as np
+import pytest
+
+from oracle.oracle import Oracle, lib
+from pytential_b200 import abi
+
+from helpers import golden_geometry, golden_tsqbx, relerr, workload
+
+
+def oracle_for(wl, nrhs=None):
+    sp = wl.spec
+    return Oracle(wl.geometry(), dim=sp.kernel.dim, qbx_order=wl.qbx_order,
+                  fmm_order=wl.fmm_order, nrhs=nrhs or wl.nrhs,
+                  charge_coeff=sp.charge_coeff, dipole_coeff=sp.dipole_coeff)
+
+
+@pytest.mark.parametrize("op", ["S", "D"])
+def test_oracle_matches_reference_tsqbx(op):
+    z = golden_tsqbx()
+    scalars, arrays = golden_geometry(z)
+    g = abi.make_geometry_struct(scalars, arrays, lambda a: a.ctypes.data)
+    s = np.ascontiguousarray(z["strengths"][None, :])
+    mask = np.zeros(scalars["ntargets"], bool)
+    mask[z["center_to_targets_lists"]] = True
+    for q in z["orders"]:
+        k = abi.make_kernel_struct(family=abi.QBXFMM_LAPLACE, dim=3, qbx_order=int(q),
+                                   fmm_order=4, charge_coeff=float(op == "S"),
+                                   dipole_coeff=float(op == "D"))
+        nc = abi.ncoeff(0, 3, int(q))
+        qe = np.zeros((scalars["ncenters"], 1, nc), np.complex128)
+        pt = np.zeros((1, scalars["ntargets"]))
+        L = lib()
+        assert L.orc_form_global_qbx_locals(ctypes.byref(k), ctypes.byref(g),
+                                            ctypes.c_void_p(s.ctypes.data),
+                                            ctypes.c_void_p(qe.ctypes.data)) == 0
+        assert L.orc_eval_qbx_expansions(ctypes.byref(k), ctypes.byref(g),
+                                         ctypes.c_void_p(qe.ctypes.data),
+                                         ctypes.c_void_p(pt.ctypes.data)) == 0
+        ref = z[f"pot_{op}_{q}"]
+        assert relerr(pt[0][mask], ref[mask]) < 1e-13, (op, q)
+
+
+@pytest.mark.parametrize("name,tol", [("2d-S", 1e-6), ("2d-D", 5e-6), ("3d-S-small", 1e-5),
+                                      ("3d-D-small", 1e-5)])
+def test_oracle_fmm_vs_direct_qbx(name, tol):
+    wl = workload(name)
+    o = oracle_for(wl)
+    s = wl.tree_strengths()
+    a = o.apply(s)
+    b = o.apply_direct(s)
+    assert relerr(a, b) < tol
+
+
+def test_oracle_linearity():
+    wl = workload("2d-S-small")
+    o = oracle_for(wl)
+    rng = np.random.default_rng(3)
+    s1 = rng.normal(size=(1, wl.geometry().tree().nsources))
+    s2 = rng.normal(size=s1.shape)
+    a = o.apply(2 * s1 - 3 * s2)
+    b = 2 * o.apply(s1) - 3 * o.apply(s2)
+    assert relerr(a, b) < 1e-12
+
+
+def test_oracle_multi_rhs_equals_single():
+    wl = workload("2d-D-nrhs3")
+    o3 = oracle_for(wl)
+    o1 = oracle_for(wl, nrhs=1)
+    s = wl.tree_strengths()
+    a = o3.apply(s)
+    for r in range(3):
+        assert relerr(a[r], o1.apply(s[r:r + 1])[0]) < 1e-14
+
+
+def test_on_surface_jump_relation_2d():
+    """Exterior limit of D on a closed curve: D_+ sigma = D_pv sigma + sigma/2 with
+    the reference's sign (G = -log r / 2 pi, normal derivative at the source):
+    for sigma = 1, D_+ 1 = 0 outside and the interior limit is -1."""
+    from pytential_b200.workloads import laplace2d_starfish
+    wl = laplace2d_starfish(op="D", qbx_order=8, fmm_order=16)
+    wl.density[:] = 1.0
+    o = oracle_for(wl)
+    out = o.apply(wl.tree_strengths())[0]
+    nsurf = wl.discr.ndofs
+    assert np.abs(out[:nsurf]).max() < 1e-6          # exterior limit of D[1] is 0
+    vol = wl.targets[1][0]
+    r = np.hypot(vol[0], vol[1])
+    th = np.arctan2(vol[1], vol[0])
+    rb = 1 + 0.25 * np.cos(5 * th)
+    inside = r < rb - 0.1
+    outside = r > rb + 0.1
+    # volume potential: -1 inside, 0 outside (Gauss's identity, this sign convention)
+    assert np.abs(out[nsurf:][inside] + 1).max() < 1e-6
+    assert np.abs(out[nsurf:][outside]).max() < 1e-6
