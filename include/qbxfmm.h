@@ -118,6 +118,14 @@ typedef struct qbxfmm_geometry {
   const int32_t* qbx_chunk_start;           /* offset into centers_by_target_box */
   const int32_t* qbx_chunk_count;
   const int32_t* centers_by_target_box;     /* [nglobal_qbx_centers] */
+
+  /* Work schedule for the point evaluations at non-QBX targets: the filtered
+   * targets of each target box cut into chunks of at most QBXFMM_CENTER_CHUNK,
+   * ordered by decreasing list-1 + list-3 work. */
+  int32_t nnonqbx_chunks;
+  const int32_t* nonqbx_chunk_target_box;   /* target box index per chunk */
+  const int32_t* nonqbx_chunk_start;        /* first filtered target of the chunk */
+  const int32_t* nonqbx_chunk_count;
 } qbxfmm_geometry;
 
 #define QBXFMM_CENTER_CHUNK 32

@@ -60,6 +60,7 @@ class Oracle:
             family=family, dim=dim, qbx_order=qbx_order, fmm_order=fmm_order,
             nrhs=nrhs, k=k, charge_coeff=charge_coeff, dipole_coeff=dipole_coeff)
         self.nrhs = nrhs
+        self.dtype = np.complex128 if family == abi.QBXFMM_HELMHOLTZ else np.float64
         self.ncf = abi.ncoeff(family, dim, fmm_order)
         self.ncq = abi.ncoeff(family, dim, qbx_order)
 
@@ -77,29 +78,29 @@ class Oracle:
         return np.zeros((self.scalars["ncenters"], self.nrhs, self.ncq), np.complex128)
 
     def zeros_nonqbx(self):
-        return np.zeros((self.nrhs, max(self.scalars["nfiltered_targets"], 1)))
+        return np.zeros((self.nrhs, max(self.scalars["nfiltered_targets"], 1)), self.dtype)
 
     def zeros_tree_pot(self):
-        return np.zeros((self.nrhs, self.scalars["ntargets"]))
+        return np.zeros((self.nrhs, self.scalars["ntargets"]), self.dtype)
 
     # }}}
 
     def tree_strengths(self, flat_strengths_user_order):
         """``reorder_sources`` (fmm.py:199-200): user order -> tree order."""
-        s = np.atleast_2d(np.asarray(flat_strengths_user_order, np.float64))
+        s = np.atleast_2d(np.asarray(flat_strengths_user_order, self.dtype))
         return np.ascontiguousarray(s[:, self.arrays["user_source_ids"]])
 
     def stage(self, name, *arrays):
         self._call("orc_" + name, *[_p(np.ascontiguousarray(a)) for a in arrays])
 
     def apply(self, tree_strengths):
-        out = np.zeros((self.nrhs, self.scalars["nuser_targets"]))
-        s = np.ascontiguousarray(tree_strengths, np.float64)
+        out = np.zeros((self.nrhs, self.scalars["nuser_targets"]), self.dtype)
+        s = np.ascontiguousarray(tree_strengths, self.dtype)
         self._call("orc_apply", _p(s), _p(out))
         return out
 
     def apply_direct(self, tree_strengths):
-        out = np.zeros((self.nrhs, self.scalars["nuser_targets"]))
-        s = np.ascontiguousarray(tree_strengths, np.float64)
+        out = np.zeros((self.nrhs, self.scalars["nuser_targets"]), self.dtype)
+        s = np.ascontiguousarray(tree_strengths, self.dtype)
         self._call("orc_apply_direct", _p(s), _p(out))
         return out

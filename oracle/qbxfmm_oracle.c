@@ -53,7 +53,8 @@ int orc_ncoeff(const qbxfmm_kernel* k, int order)
     if (k->dim == 3) return (order + 1) * (order + 2) / 2;
     return order + 1;
   }
-  return -1;
+  if (k->dim == 2) return 2 * order + 1;
+  return (order + 1) * (order + 1);
 }
 
 static double level_width(const qbxfmm_geometry* g, int level)
@@ -390,11 +391,32 @@ static int work_size(int p) { return (p + 3) * (p + 4) / 2 * 4 + 64; }
 
 /* }}} */
 
+
+/* {{{ 2D Helmholtz forward declarations (qbxfmm_oracle_helm2d.c) */
+static int h2_form_multipoles(const qbxfmm_kernel*, const qbxfmm_geometry*, const cplx*, cplx*);
+static int h2_coarsen_multipoles(const qbxfmm_kernel*, const qbxfmm_geometry*, cplx*);
+static int h2_eval_direct(const qbxfmm_kernel*, const qbxfmm_geometry*, const cplx*, cplx*);
+static int h2_multipole_to_local(const qbxfmm_kernel*, const qbxfmm_geometry*, const cplx*, cplx*);
+static int h2_eval_multipoles(const qbxfmm_kernel*, const qbxfmm_geometry*, const cplx*, cplx*);
+static int h2_form_locals(const qbxfmm_kernel*, const qbxfmm_geometry*, const cplx*, cplx*);
+static int h2_refine_locals(const qbxfmm_kernel*, const qbxfmm_geometry*, cplx*);
+static int h2_eval_locals(const qbxfmm_kernel*, const qbxfmm_geometry*, const cplx*, cplx*);
+static int h2_p2qbxl(const qbxfmm_kernel*, const qbxfmm_geometry*, const cplx*, cplx*, int);
+static int h2_m2qbxl(const qbxfmm_kernel*, const qbxfmm_geometry*, const cplx*, cplx*);
+static int h2_l2qbxl(const qbxfmm_kernel*, const qbxfmm_geometry*, const cplx*, cplx*);
+static int h2_eval_qbx_expansions(const qbxfmm_kernel*, const qbxfmm_geometry*, const cplx*, cplx*);
+static int h2_assemble(const qbxfmm_kernel*, const qbxfmm_geometry*, const cplx*, const cplx*, cplx*);
+static int h2_apply(const qbxfmm_kernel*, const qbxfmm_geometry*, const cplx*, cplx*, int);
+/* }}} */
+
+#define IS_HELM(k) ((k)->family == QBXFMM_HELMHOLTZ)
+
 /* {{{ stages */
 
 int orc_form_multipoles(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
                         const double* strengths, cplx* mpoles)
 {
+  if (IS_HELM(kern)) return h2_form_multipoles(kern, g, (const cplx*)strengths, mpoles);
   ctx_t c;
   int rc = make_ctx(kern, &c);
   if (rc) return rc;
@@ -429,6 +451,7 @@ int orc_form_multipoles(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
 int orc_coarsen_multipoles(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
                            cplx* mpoles)
 {
+  if (IS_HELM(kern)) return h2_coarsen_multipoles(kern, g, mpoles);
   ctx_t c;
   int rc = make_ctx(kern, &c);
   if (rc) return rc;
@@ -468,6 +491,7 @@ int orc_coarsen_multipoles(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
 int orc_eval_direct(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
                     const double* strengths, double* pot)
 {
+  if (IS_HELM(kern)) return h2_eval_direct(kern, g, (const cplx*)strengths, (cplx*)pot);
   ctx_t c;
   int rc = make_ctx(kern, &c);
   if (rc) return rc;
@@ -503,6 +527,7 @@ int orc_eval_direct(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
 int orc_multipole_to_local(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
                            const cplx* mpoles, cplx* locals)
 {
+  if (IS_HELM(kern)) return h2_multipole_to_local(kern, g, mpoles, locals);
   ctx_t c;
   int rc = make_ctx(kern, &c);
   if (rc) return rc;
@@ -536,6 +561,7 @@ int orc_multipole_to_local(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
 int orc_eval_multipoles(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
                         const cplx* mpoles, double* pot)
 {
+  if (IS_HELM(kern)) return h2_eval_multipoles(kern, g, mpoles, (cplx*)pot);
   ctx_t c;
   int rc = make_ctx(kern, &c);
   if (rc) return rc;
@@ -571,6 +597,7 @@ int orc_eval_multipoles(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
 int orc_form_locals(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
                     const double* strengths, cplx* locals)
 {
+  if (IS_HELM(kern)) return h2_form_locals(kern, g, (const cplx*)strengths, locals);
   ctx_t c;
   int rc = make_ctx(kern, &c);
   if (rc) return rc;
@@ -605,6 +632,7 @@ int orc_form_locals(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
 
 int orc_refine_locals(const qbxfmm_kernel* kern, const qbxfmm_geometry* g, cplx* locals)
 {
+  if (IS_HELM(kern)) return h2_refine_locals(kern, g, locals);
   ctx_t c;
   int rc = make_ctx(kern, &c);
   if (rc) return rc;
@@ -638,6 +666,7 @@ int orc_refine_locals(const qbxfmm_kernel* kern, const qbxfmm_geometry* g, cplx*
 int orc_eval_locals(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
                     const cplx* locals, double* pot)
 {
+  if (IS_HELM(kern)) return h2_eval_locals(kern, g, locals, (cplx*)pot);
   ctx_t c;
   int rc = make_ctx(kern, &c);
   if (rc) return rc;
@@ -716,6 +745,7 @@ static int p2qbxl_impl(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
 int orc_form_global_qbx_locals(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
                                const double* strengths, cplx* qbx_exps)
 {
+  if (IS_HELM(kern)) return h2_p2qbxl(kern, g, (const cplx*)strengths, qbx_exps, 0);
   return p2qbxl_impl(kern, g, strengths, qbx_exps, 0);
 }
 
@@ -724,6 +754,7 @@ int orc_translate_box_multipoles_to_qbx_local(const qbxfmm_kernel* kern,
                                               const qbxfmm_geometry* g,
                                               const cplx* mpoles, cplx* qbx_exps)
 {
+  if (IS_HELM(kern)) return h2_m2qbxl(kern, g, mpoles, qbx_exps);
   ctx_t c;
   int rc = make_ctx(kern, &c);
   if (rc) return rc;
@@ -760,6 +791,7 @@ int orc_translate_box_local_to_qbx_local(const qbxfmm_kernel* kern,
                                          const qbxfmm_geometry* g,
                                          const cplx* locals, cplx* qbx_exps)
 {
+  if (IS_HELM(kern)) return h2_l2qbxl(kern, g, locals, qbx_exps);
   ctx_t c;
   int rc = make_ctx(kern, &c);
   if (rc) return rc;
@@ -792,6 +824,7 @@ int orc_translate_box_local_to_qbx_local(const qbxfmm_kernel* kern,
 int orc_eval_qbx_expansions(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
                             const cplx* qbx_exps, double* pot_tree)
 {
+  if (IS_HELM(kern)) return h2_eval_qbx_expansions(kern, g, qbx_exps, (cplx*)pot_tree);
   ctx_t c;
   int rc = make_ctx(kern, &c);
   if (rc) return rc;
@@ -828,6 +861,8 @@ static double kernel_scaling(int dim) { return dim == 3 ? 0.25 / M_PI : -0.5 / M
 int orc_assemble(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
                  const double* pot_nonqbx, const double* pot_tree, double* out)
 {
+  if (IS_HELM(kern))
+    return h2_assemble(kern, g, (const cplx*)pot_nonqbx, (const cplx*)pot_tree, (cplx*)out);
   ctx_t c;
   int rc = make_ctx(kern, &c);
   if (rc) return rc;
@@ -852,6 +887,7 @@ int orc_assemble(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
 int orc_apply(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
               const double* strengths, double* out)
 {
+  if (IS_HELM(kern)) return h2_apply(kern, g, (const cplx*)strengths, (cplx*)out, 0);
   ctx_t c;
   int rc = make_ctx(kern, &c);
   if (rc) return rc;
@@ -888,6 +924,7 @@ int orc_apply(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
 int orc_apply_direct(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
                      const double* strengths, double* out)
 {
+  if (IS_HELM(kern)) return h2_apply(kern, g, (const cplx*)strengths, (cplx*)out, 1);
   ctx_t c;
   int rc = make_ctx(kern, &c);
   if (rc) return rc;
@@ -920,3 +957,5 @@ int orc_apply_direct(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
 }
 
 /* }}} */
+
+#include "qbxfmm_oracle_helm2d.c"

@@ -70,6 +70,8 @@ GEOMETRY_FIELDS = [
     ("nuser_targets", "i"),
     ("nqbx_chunks", "i"), ("qbx_chunk_target_box", "pi"), ("qbx_chunk_start", "pi"),
     ("qbx_chunk_count", "pi"), ("centers_by_target_box", "pi"),
+    ("nnonqbx_chunks", "i"), ("nonqbx_chunk_target_box", "pi"), ("nonqbx_chunk_start", "pi"),
+    ("nonqbx_chunk_count", "pi"),
 ]
 
 CENTER_CHUNK = 32
@@ -126,6 +128,39 @@ def qbx_center_schedule(global_qbx_centers, qbx_center_to_target_box, list1_star
     o = np.argsort(-cost, kind="stable")
     return (ch_tb[o].astype(np.int32), np.array(ch_start, np.int32)[o],
             ch_count[o].astype(np.int32), cbt.astype(np.int32))
+
+
+def nonqbx_target_schedule(target_boxes, nonqbx_box_target_starts,
+                           nonqbx_box_target_counts_nonchild, list1_starts, list1_lists,
+                           list3_starts, box_source_counts_nonchild, chunk: int = CENTER_CHUNK,
+                           mpole_cost: int = 66):
+    """Chunks of at most ``chunk`` non-QBX targets per target box, ordered by
+    decreasing work (targets x (list-1 sources + mpole_cost x list-3 boxes)).
+
+    Returns ``(chunk_target_box, chunk_start, chunk_count)``."""
+    tb = np.asarray(target_boxes)
+    st = np.asarray(nonqbx_box_target_starts)[tb]
+    nt = np.asarray(nonqbx_box_target_counts_nonchild)[tb].astype(np.int64)
+    cnt = np.asarray(box_source_counts_nonchild)[np.asarray(list1_lists)]
+    csum = np.concatenate([[0], np.cumsum(cnt)])
+    l1s = np.asarray(list1_starts)
+    nsrc = csum[l1s[1:]] - csum[l1s[:-1]]
+    n3 = np.diff(np.asarray(list3_starts))
+    ch_tb, ch_start, ch_count = [], [], []
+    for i in np.where(nt > 0)[0]:
+        for off in range(0, nt[i], chunk):
+            ch_tb.append(i)
+            ch_start.append(st[i] + off)
+            ch_count.append(min(chunk, nt[i] - off))
+    if not ch_tb:
+        z = np.zeros(0, np.int32)
+        return z, z, z
+    ch_tb = np.array(ch_tb, np.int64)
+    ch_count = np.array(ch_count, np.int64)
+    cost = ch_count * (nsrc[ch_tb] + mpole_cost * n3[ch_tb])
+    o = np.argsort(-cost, kind="stable")
+    return (ch_tb[o].astype(np.int32), np.array(ch_start, np.int32)[o],
+            ch_count[o].astype(np.int32))
 
 
 def _i(a):
@@ -190,7 +225,14 @@ def geometry_arrays(geo) -> tuple[dict, dict]:
         "qbx_chunk_target_box": ch_tb, "qbx_chunk_start": ch_start,
         "qbx_chunk_count": ch_count, "centers_by_target_box": cbt,
     })
+    nq_tb, nq_start, nq_count = nonqbx_target_schedule(
+        arrays["target_boxes"], arrays["nonqbx_box_target_starts"],
+        arrays["nonqbx_box_target_counts_nonchild"], arrays["list1_starts"],
+        arrays["list1_lists"], arrays["list3_starts"], arrays["box_source_counts_nonchild"])
+    arrays.update({"nonqbx_chunk_target_box": nq_tb, "nonqbx_chunk_start": nq_start,
+                   "nonqbx_chunk_count": nq_count})
     scalars = {
+        "nnonqbx_chunks": len(nq_tb),
         "nqbx_chunks": len(ch_tb),
         "dim": tree.dimensions, "nboxes": tree.nboxes, "nlevels": tree.nlevels,
         "nsources": tree.nsources, "ntargets": tree.ntargets,

@@ -6,6 +6,8 @@
 // shared memory; the QBX near-field kernel assigns one CTA per chunk of centers
 // that share a target box, holds each center's coefficients in registers and
 // streams that box's list-1 sources through shared memory in tiles of 128.
+#include <algorithm>
+
 #include "laplace.cuh"
 #include "kernels.h"
 
@@ -40,11 +42,8 @@ k_form_strengths(int nsources, int ndofs, int npe, int nqpe,
 
 // {{{ helpers
 
-struct SrcTile {
-  double* x;   // [3][NT]
-  double* n;   // [3][NT]
-  double* q;   // [NT]
-};
+constexpr int NW = NT / 32;     // warps per CTA
+constexpr int MAXB = 128;       // list boxes staged per pass
 
 // decode coefficient index -> (n, m) for the 3D triangular layout
 QBX_D void decode3(int c, int& n, int& m)
@@ -53,6 +52,82 @@ QBX_D void decode3(int c, int& n, int& m)
   while ((n + 1) * (n + 2) / 2 <= c) ++n;
   while (n * (n + 1) / 2 > c) --n;
   m = c - n * (n + 1) / 2;
+}
+
+// Warp 0 writes the running source counts of list boxes [gb, gb + nb) (nb <= 128)
+// into s_pref[0..nb] and their first source into s_start; caller syncs.
+QBX_D void list_prefix(const qbxfmm_geometry& g, const int32_t* __restrict__ lists, int gb,
+                       int nb, int* s_pref, int* s_start, int32_t* err)
+{
+  if (threadIdx.x >= 32) return;
+  int lane = threadIdx.x;
+  int cnt[4], loc = 0;
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    int k = lane * 4 + u;
+    cnt[u] = 0;
+    if (k < nb) {
+      int sb = lists[gb + k];
+      int s0 = 0;
+      if ((unsigned)sb < (unsigned)g.nboxes) {
+        s0 = g.box_source_starts[sb];
+        cnt[u] = g.box_source_counts_nonchild[sb];
+      } else {
+        report(err, QBX_DEVERR_BAD_BOX);
+      }
+      s_start[k] = s0;
+    }
+    loc += cnt[u];
+  }
+  int incl = loc;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    int v = __shfl_up_sync(0xffffffffu, incl, off);
+    if (lane >= off) incl += v;
+  }
+  int run = incl - loc;
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    int k = lane * 4 + u;
+    if (k < nb) s_pref[k] = run;
+    run += cnt[u];
+  }
+  if (lane == 31) s_pref[nb] = incl;
+}
+
+// tree source index of virtual stream position v (0 <= v < s_pref[nb])
+QBX_D int stream_source(int v, int nb, const int* s_pref, const int* s_start)
+{
+  int lo = 0, hi = nb - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (s_pref[mid] <= v) lo = mid;
+    else hi = mid - 1;
+  }
+  return s_start[lo] + (v - s_pref[lo]);
+}
+
+// Stage sources [base, base + NT) of the stream into shared memory.
+template <int DIM, bool NORMALS>
+QBX_D void load_stream_tile(const qbxfmm_geometry& g, const double* __restrict__ st, int total,
+                            int nb, int base, const int* s_pref, const int* s_start,
+                            double (*s_y)[NT], double (*s_n)[NT], double* s_q)
+{
+  int v = base + threadIdx.x;
+  if (v < total) {
+    int s = stream_source(v, nb, s_pref, s_start);
+    double y[3];
+    load_point<DIM>(g.sources, g.nsources, s, y);
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) s_y[d][threadIdx.x] = y[d];
+    if (NORMALS) {
+      double nv[3];
+      load_point<DIM>(g.source_normals, g.nsources, s, nv);
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) s_n[d][threadIdx.x] = nv[d];
+    }
+    s_q[threadIdx.x] = __ldg(st + s);
+  }
 }
 
 // }}}
@@ -262,21 +337,156 @@ k_m2m(qbxfmm_geometry g, int p, int ncf, int nrhs, int i0, double2* __restrict__
 
 // {{{ M2L (multipole_to_local, fmm.py:472-478), one CTA per target-or-parent box
 
-template <int DIM>
+// 3D: L_j^i = (-1)^j / rho sum_{k<=p, |l|<=k} M_k^l S_{k+j}^{l+i}(d).  Batches of PB
+// list-2 pairs: the singular-harmonic tables (rows 0..2p, columns -p..2p) and the
+// multipoles (rows 0..p, columns -p..p) are expanded into zero-padded dense arrays
+// in shared memory, so the inner product is branch-free.  Each output's sum is
+// split over two threads (k ranges with about equal term counts).
 __global__ void __launch_bounds__(NT)
-k_m2l(qbxfmm_geometry g, int p, int ncf, int nrhs, const double2* __restrict__ mpoles,
-      double2* __restrict__ locals, int32_t* err)
+k_m2l3(qbxfmm_geometry g, int p, int ncf, int nrhs, int pb_max, const double2* __restrict__ mpoles,
+       double2* __restrict__ locals, int32_t* err)
 {
   extern __shared__ double2 smem2[];
-  double2* Min = smem2;             // [ncf]
-  double2* tab = smem2 + ncf;       // [ncoeff(2p)]
+  const int SW = 3 * p + 1, SR = 2 * p + 1, SS = SR * SW;   // S table
+  const int MW = 2 * p + 1, MS = (p + 1) * MW;              // M table
+  double2* Spad = smem2;                                    // [pb_max][SS]
+  double2* Mpad = Spad + (size_t)pb_max * SS;               // [pb_max][MS]
+  double2* red = Mpad + (size_t)pb_max * MS;                // [ncf]
+  __shared__ int s_sb[8];
+  __shared__ double s_d[8][3];
+
   int i = blockIdx.x;
   int tb = g.target_or_target_parent_boxes[i];
   int r = blockIdx.y;
   double rho = level_width(g, g.box_levels[tb]);
   double ct[3];
-  load_point<DIM>(g.box_centers, g.nboxes, tb, ct);
+  load_point<3>(g.box_centers, g.nboxes, tb, ct);
+
+  for (int q = threadIdx.x; q < pb_max * (SS + MS); q += NT) smem2[q] = c2(0.0);
+
+  // k split point: first half takes rows 0..ksplit-1
+  int ksplit = 0;
+  {
+    int half = (p + 1) * (p + 1) / 2, cum = 0;
+    while (ksplit <= p && cum + ksplit <= half) cum += 2 * ksplit + 1, ++ksplit;
+  }
   double2 acc[2] = {c2(0.0), c2(0.0)};
+  int l0 = g.list2_starts[i], l1 = g.list2_starts[i + 1];
+  for (int lb = l0; lb < l1; lb += pb_max) {
+    int nbat = min(pb_max, l1 - lb);
+    __syncthreads();
+    if (threadIdx.x < nbat) {
+      int sb = g.list2_lists[lb + threadIdx.x];
+      if ((unsigned)sb >= (unsigned)g.nboxes) {
+        report(err, QBX_DEVERR_BAD_BOX);
+        sb = -1;
+      }
+      s_sb[threadIdx.x] = sb;
+      if (sb >= 0) {
+        double cs[3];
+        load_point<3>(g.box_centers, g.nboxes, sb, cs);
+        for (int d = 0; d < 3; ++d) s_d[threadIdx.x][d] = (ct[d] - cs[d]) / rho;
+      }
+    }
+    __syncthreads();
+    // S tables: one thread per (pair, column m in 0..2p); negative columns by symmetry
+    for (int w = threadIdx.x; w < nbat * (2 * p + 1); w += NT) {
+      int b = w / (2 * p + 1), m = w - b * (2 * p + 1);
+      double2* S = Spad + (size_t)b * SS;
+      if (s_sb[b] < 0) {
+        for (int n = m; n <= 2 * p; ++n) {
+          S[n * SW + p + m] = c2(0.0);
+          if (m >= 1 && m <= p) S[n * SW + p - m] = c2(0.0);
+        }
+        continue;
+      }
+      double x = s_d[b][0], y = s_d[b][1], z = s_d[b][2];
+      double rinv2 = 1.0 / (x * x + y * y + z * z);
+      double2 a = c2(sqrt(rinv2));
+      for (int k = 1; k <= m; ++k) a = cscale((2.0 * k - 1) * rinv2, cmul(a, c2(x, y)));
+      double2 prev = c2(0.0);
+      for (int n = m; n <= 2 * p; ++n) {
+        if (n > m) {
+          double2 bb = cscale(rinv2, csub(cscale((2.0 * n - 1) * z, a),
+                                          cscale((double)(n + m - 1) * (n - m - 1), prev)));
+          prev = a;
+          a = bb;
+        }
+        S[n * SW + p + m] = a;
+        if (m >= 1 && m <= p) S[n * SW + p - m] = (m & 1) ? c2(-a.x, a.y) : c2(a.x, -a.y);
+      }
+    }
+    // M tables
+    for (int w = threadIdx.x; w < nbat * ncf; w += NT) {
+      int b = w / ncf, c = w - b * ncf;
+      int k, l;
+      decode3(c, k, l);
+      double2 v = c2(0.0);
+      if (s_sb[b] >= 0) v = mpoles[((size_t)s_sb[b] * nrhs + r) * ncf + c];
+      double2* M = Mpad + (size_t)b * MS;
+      M[k * MW + p + l] = v;
+      if (l > 0) M[k * MW + p - l] = (l & 1) ? c2(-v.x, v.y) : c2(v.x, -v.y);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      int job = threadIdx.x + h * NT;
+      if (job >= 2 * ncf) break;
+      int o = job >> 1, half = job & 1;
+      int j, ii;
+      decode3(o, j, ii);
+      int k0 = half ? ksplit : 0, k1 = half ? p + 1 : ksplit;
+      double2 a = acc[h];
+      for (int b = 0; b < nbat; ++b) {
+        const double2* M = Mpad + (size_t)b * MS;
+        const double2* S = Spad + (size_t)b * SS;
+        for (int k = k0; k < k1; ++k) {
+          const double2* mrow = M + k * MW + p - k;
+          const double2* srow = S + (k + j) * SW + p + ii - k;
+          for (int l = 0; l <= 2 * k; ++l) a = cfma(mrow[l], srow[l], a);
+        }
+      }
+      acc[h] = a;
+    }
+  }
+  // combine the two halves of each output
+  __syncthreads();
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    int job = threadIdx.x + h * NT;
+    if (job < 2 * ncf && (job & 1)) red[job >> 1] = acc[h];
+  }
+  __syncthreads();
+  double2* L = locals + ((size_t)tb * nrhs + r) * ncf;
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    int job = threadIdx.x + h * NT;
+    if (job < 2 * ncf && !(job & 1)) {
+      int o = job >> 1;
+      int j, ii;
+      decode3(o, j, ii);
+      double2 v = cadd(acc[h], red[o]);
+      L[o] = caxpy((j & 1) ? -1.0 / rho : 1.0 / rho, v, L[o]);
+    }
+  }
+}
+
+// 2D: L_0 = M_0 log t + sum_k M_k tau^-k,
+//     L_l = (-1)^(l+1) M_0 / (l tau^l) + (-1)^l tau^-l sum_k M_k C(k+l-1, l) tau^-k.
+__global__ void __launch_bounds__(NT)
+k_m2l2(qbxfmm_geometry g, int p, int ncf, int nrhs, const double2* __restrict__ mpoles,
+       double2* __restrict__ locals, int32_t* err)
+{
+  extern __shared__ double2 smem2[];
+  double2* Min = smem2;             // [ncf]
+  double2* tab = smem2 + ncf;       // [2p+2]
+  int i = blockIdx.x;
+  int tb = g.target_or_target_parent_boxes[i];
+  int r = blockIdx.y;
+  double rho = level_width(g, g.box_levels[tb]);
+  double ct[3];
+  load_point<2>(g.box_centers, g.nboxes, tb, ct);
+  double2 acc = c2(0.0);
   int l0 = g.list2_starts[i], l1 = g.list2_starts[i + 1];
   for (int li = l0; li < l1; ++li) {
     int sb = g.list2_lists[li];
@@ -284,62 +494,43 @@ k_m2l(qbxfmm_geometry g, int p, int ncf, int nrhs, const double2* __restrict__ m
       report(err, QBX_DEVERR_BAD_BOX);
       continue;
     }
-    double cs[3], d[3];
-    load_point<DIM>(g.box_centers, g.nboxes, sb, cs);
-#pragma unroll
-    for (int k = 0; k < DIM; ++k) d[k] = (ct[k] - cs[k]) / rho;
+    double cs[3];
+    load_point<2>(g.box_centers, g.nboxes, sb, cs);
+    double d0 = (ct[0] - cs[0]) / rho, d1 = (ct[1] - cs[1]) / rho;
     const double2* src = mpoles + ((size_t)sb * nrhs + r) * ncf;
     for (int q = threadIdx.x; q < ncf; q += NT) Min[q] = src[q];
-    if (DIM == 3) {
-      sh3_S_table(2 * p, d[0], d[1], d[2], tab, threadIdx.x, NT);
-    } else if (threadIdx.x == 0) {
-      double2 tinv = cinv(c2(d[0], d[1])), a = tinv;
-      tab[0] = clog_(c2(d[0] * rho, d[1] * rho));
+    if (threadIdx.x == 0) {
+      double2 tinv = cinv(c2(d0, d1)), a = tinv;
+      tab[0] = clog_(c2(d0 * rho, d1 * rho));
       for (int k = 1; k <= 2 * p + 1; ++k) {
         tab[k] = a;  // tau^-k
         a = cmul(a, tinv);
       }
     }
     __syncthreads();
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      int o = threadIdx.x + h * NT;
-      if (o >= ncf) break;
-      double2 a = acc[h];
-      if (DIM == 3) {
-        int j, ii;
-        decode3(o, j, ii);
-        double2 s = c2(0.0);
-        for (int k = 0; k <= p; ++k)
-          for (int l = -k; l <= k; ++l) s = cfma(sh3_get(Min, k, l), sh3_get(tab, k + j, l + ii), s);
-        a = caxpy((j & 1) ? -1.0 / rho : 1.0 / rho, s, a);
+    int l = threadIdx.x;
+    if (l < ncf) {
+      if (l == 0) {
+        double2 s = cmul(Min[0], tab[0]);
+        for (int k = 1; k <= p; ++k) s = cfma(Min[k], tab[k], s);
+        acc = cadd(acc, s);
       } else {
-        int l = o;
-        if (l == 0) {
-          double2 s = cmul(Min[0], tab[0]);
-          for (int k = 1; k <= p; ++k) s = cfma(Min[k], tab[k], s);
-          a = cadd(a, s);
-        } else {
-          double2 s = c2(0.0);
-          double bin = 1.0;  // C(k+l-1, l) at k = 1
-          for (int k = 1; k <= p; ++k) {
-            s = cfma(cscale(bin, Min[k]), tab[k], s);
-            bin = bin * (k + l) / k;
-          }
-          double2 v = cscale(((l & 1) ? 1.0 : -1.0) / l, Min[0]);
-          v = cadd(v, cscale((l & 1) ? -1.0 : 1.0, s));
-          a = cfma(v, tab[l], a);
+        double2 s = c2(0.0);
+        double bin = 1.0;  // C(k+l-1, l) at k = 1
+        for (int k = 1; k <= p; ++k) {
+          s = cfma(cscale(bin, Min[k]), tab[k], s);
+          bin = bin * (k + l) / k;
         }
+        double2 v = cscale(((l & 1) ? 1.0 : -1.0) / l, Min[0]);
+        v = cadd(v, cscale((l & 1) ? -1.0 : 1.0, s));
+        acc = cfma(v, tab[l], acc);
       }
-      acc[h] = a;
     }
     __syncthreads();
   }
-  double2* L = locals + ((size_t)tb * nrhs + r) * ncf;
-#pragma unroll
-  for (int h = 0; h < 2; ++h) {
-    int o = threadIdx.x + h * NT;
-    if (o < ncf) L[o] = cadd(L[o], acc[h]);
+  if (threadIdx.x < ncf) {
+    double2* L = locals + ((size_t)tb * nrhs + r) * ncf;
+    L[threadIdx.x] = cadd(L[threadIdx.x], acc);
   }
 }
 
@@ -347,16 +538,21 @@ k_m2l(qbxfmm_geometry g, int p, int ncf, int nrhs, const double2* __restrict__ m
 
 // {{{ P2L (form_locals, list 4, fmm.py:502-510)
 
+// One CTA per target-or-parent box; its list-4 sources stream through shared memory
+// in sub-tiles of SUB; per sub-tile each source's singular-harmonic table (orders
+// 0..p+1) is built by one thread per (source, column), then each thread accumulates
+// its coefficient(s) with precomputed table offsets.
 template <int DIM>
 __global__ void __launch_bounds__(NT)
 k_p2l(qbxfmm_geometry g, SourceCoeffs sc, int p, int ncf, int nrhs,
       const double* __restrict__ strengths, double2* __restrict__ locals, int32_t* err)
 {
-  constexpr int SUB = 16;
+  constexpr int SUB = 32;
   extern __shared__ double2 smem2[];
-  double2* tab = smem2;   // [SUB][ncoeff(p+1)]
+  double2* tab = smem2;   // [SUB][nct]
   __shared__ double s_u[SUB][3], s_n[SUB][3], s_q[SUB];
-  int nct = (DIM == 3) ? (p + 2) * (p + 3) / 2 : p + 3;
+  __shared__ int s_pref[MAXB + 1], s_start[MAXB];
+  const int nct = (DIM == 3) ? (p + 2) * (p + 3) / 2 : p + 3;
   int i = blockIdx.x;
   int tb = g.target_or_target_parent_boxes[i];
   int r = blockIdx.y;
@@ -364,23 +560,47 @@ k_p2l(qbxfmm_geometry g, SourceCoeffs sc, int p, int ncf, int nrhs,
   double c[3];
   load_point<DIM>(g.box_centers, g.nboxes, tb, c);
   const double* st = strengths + (size_t)r * g.nsources;
-  double2 acc[2] = {c2(0.0), c2(0.0)};
-  for (int li = g.list4_starts[i]; li < g.list4_starts[i + 1]; ++li) {
-    int sb = g.list4_lists[li];
-    if ((unsigned)sb >= (unsigned)g.nboxes) {
-      report(err, QBX_DEVERR_BAD_BOX);
-      continue;
+  const bool dip = sc.cd != 0.0;
+
+  // per-thread coefficient bookkeeping (3D): table offsets of S_n^m and the
+  // dipole neighbours S_{n+1}^{m-1}, S_{n+1}^m, S_{n+1}^{m+1}
+  int o_nm[2], o_a[2], o_b[2], o_c[2];
+  double sb_sign[2];
+  bool valid[2];
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    int ci = threadIdx.x + h * NT;
+    valid[h] = ci < ncf;
+    o_nm[h] = o_a[h] = o_b[h] = o_c[h] = 0;
+    sb_sign[h] = 1.0;
+    if (DIM == 3 && valid[h]) {
+      int n, m;
+      decode3(ci, n, m);
+      o_nm[h] = idx3(n, m);
+      o_a[h] = idx3(n + 1, m);
+      o_b[h] = idx3(n + 1, m > 0 ? m - 1 : 1);   // m = 0: S_{n+1}^{-1} = -conj(S_{n+1}^1)
+      sb_sign[h] = m > 0 ? 1.0 : -1.0;
+      o_c[h] = idx3(n + 1, m + 1);
     }
-    int s0 = g.box_source_starts[sb], ns = g.box_source_counts_nonchild[sb];
-    for (int base = 0; base < ns; base += SUB) {
-      int cnt = min(SUB, ns - base);
+  }
+
+  double2 acc[2] = {c2(0.0), c2(0.0)};
+  int l0 = g.list4_starts[i], l1 = g.list4_starts[i + 1];
+  for (int gb = l0; gb < l1; gb += MAXB) {
+    int nb = min(MAXB, l1 - gb);
+    __syncthreads();
+    list_prefix(g, g.list4_lists, gb, nb, s_pref, s_start, err);
+    __syncthreads();
+    int total = s_pref[nb];
+    for (int base = 0; base < total; base += SUB) {
+      int cnt = min(SUB, total - base);
       if (threadIdx.x < cnt) {
-        int s = s0 + base + threadIdx.x;
+        int s = stream_source(base + threadIdx.x, nb, s_pref, s_start);
         double y[3];
         load_point<DIM>(g.sources, g.nsources, s, y);
 #pragma unroll
         for (int d = 0; d < DIM; ++d) s_u[threadIdx.x][d] = (y[d] - c[d]) / rho;
-        if (sc.cd != 0.0) {
+        if (dip) {
           double nv[3];
           load_point<DIM>(g.source_normals, g.nsources, s, nv);
 #pragma unroll
@@ -416,36 +636,35 @@ k_p2l(qbxfmm_geometry g, SourceCoeffs sc, int p, int ncf, int nrhs,
             T[k] = a;   // tau^-k
             a = cmul(a, tinv);
           }
-          T[p + 2] = c2(0.5 * log((s_u[j][0] * s_u[j][0] + s_u[j][1] * s_u[j][1])
-                                  * rho * rho));
+          T[p + 2] = c2(0.5 * log((s_u[j][0] * s_u[j][0] + s_u[j][1] * s_u[j][1]) * rho * rho));
         }
       }
       __syncthreads();
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
+        if (!valid[h]) continue;
         int ci = threadIdx.x + h * NT;
-        if (ci >= ncf) break;
         double2 a = acc[h];
         for (int j = 0; j < cnt; ++j) {
           const double2* T = tab + (size_t)j * nct;
           double q = s_q[j];
           if (DIM == 3) {
-            int n, m;
-            decode3(ci, n, m);
-            a = caxpy(sc.cq * q / rho, T[idx3(n, m)], a);
-            if (sc.cd != 0.0) {
+            a = caxpy(sc.cq * q / rho, T[o_nm[h]], a);
+            if (dip) {
               double f = sc.cd * q / (rho * rho);
               double dx = s_n[j][0], dy = s_n[j][1], dz = s_n[j][2];
-              double2 v = cscale(-dz, sh3_get(T, n + 1, m));
-              v = cfma(c2(0.5 * dx, 0.5 * dy), sh3_get(T, n + 1, m - 1), v);
-              v = cfma(c2(-0.5 * dx, 0.5 * dy), sh3_get(T, n + 1, m + 1), v);
+              double2 tb_ = T[o_b[h]];
+              if (sb_sign[h] < 0) tb_ = c2(-tb_.x, tb_.y);
+              double2 v = cscale(-dz, T[o_a[h]]);
+              v = cfma(c2(0.5 * dx, 0.5 * dy), tb_, v);
+              v = cfma(c2(-0.5 * dx, 0.5 * dy), T[o_c[h]], v);
               a = caxpy(f, v, a);
             }
           } else {
             int l = ci;
             if (l == 0) a.x += sc.cq * q * T[p + 2].x;
             else a = caxpy(-sc.cq * q / l, T[l], a);
-            if (sc.cd != 0.0) {
+            if (dip) {
               double2 nu = c2(s_n[j][0], s_n[j][1]);
               a = cfma(cscale(sc.cd * q / rho, nu), T[l + 1], a);
             }
@@ -528,143 +747,147 @@ k_l2l(qbxfmm_geometry g, int p, int ncf, int nrhs, int i0, double2* __restrict__
 
 // {{{ point evaluations at non-QBX targets: P2P (list 1), M2P (list 3), L2P
 
+// P2P over list 1 (eval_direct, fmm.py:461-466).  CTA = 4 warps over one chunk of
+// <= 32 non-QBX targets of a target box (lane = target); the list-1 sources stream
+// through shared memory in tiles of 128, each warp taking 32 of them.
 template <int DIM>
 __global__ void __launch_bounds__(NT)
 k_eval_direct(qbxfmm_geometry g, SourceCoeffs sc, int nrhs, const double* __restrict__ strengths,
               double* __restrict__ pot, int32_t* err)
 {
   __shared__ double s_y[3][NT], s_n[3][NT], s_q[NT];
-  int itb = blockIdx.x;
-  int tb = g.target_boxes[itb];
+  __shared__ int s_pref[MAXB + 1], s_start[MAXB];
+  __shared__ double s_red[NW - 1][32];
+  int chunk = blockIdx.x;
   int r = blockIdx.y;
-  int t0 = g.nonqbx_box_target_starts[tb];
-  int nt = g.nonqbx_box_target_counts_nonchild[tb];
-  if (nt == 0) return;
+  int itb = g.nonqbx_chunk_target_box[chunk];
+  int t0 = g.nonqbx_chunk_start[chunk];
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  bool active = lane < g.nonqbx_chunk_count[chunk];
+  int t = t0 + lane;
+  double x[3] = {0, 0, 0};
+  if (active) load_point<DIM>(g.nonqbx_targets, g.nfiltered_targets, t, x);
   const double* st = strengths + (size_t)r * g.nsources;
-  for (int tbase = 0; tbase < nt; tbase += NT) {
-    int t = tbase + threadIdx.x;
-    bool active = t < nt;
-    double x[3] = {0, 0, 0};
-    if (active) load_point<DIM>(g.nonqbx_targets, g.nfiltered_targets, t0 + t, x);
-    double acc = 0.0;
-    for (int li = g.list1_starts[itb]; li < g.list1_starts[itb + 1]; ++li) {
-      int sb = g.list1_lists[li];
-      if ((unsigned)sb >= (unsigned)g.nboxes) {
-        report(err, QBX_DEVERR_BAD_BOX);
-        continue;
-      }
-      int s0 = g.box_source_starts[sb], ns = g.box_source_counts_nonchild[sb];
-      for (int base = 0; base < ns; base += NT) {
-        int cnt = min(NT, ns - base);
-        if (threadIdx.x < cnt) {
-          int s = s0 + base + threadIdx.x;
-          double y[3], nv[3] = {0, 0, 0};
-          load_point<DIM>(g.sources, g.nsources, s, y);
-          if (sc.cd != 0.0) load_point<DIM>(g.source_normals, g.nsources, s, nv);
-#pragma unroll
-          for (int d = 0; d < DIM; ++d) {
-            s_y[d][threadIdx.x] = y[d];
-            s_n[d][threadIdx.x] = nv[d];
-          }
-          s_q[threadIdx.x] = __ldg(st + s);
-        }
-        __syncthreads();
-        if (active) {
-          for (int j = 0; j < cnt; ++j) {
-            double dx = x[0] - s_y[0][j], dy = x[1] - s_y[1][j];
-            double dz = (DIM == 3) ? x[2] - s_y[2][j] : 0.0;
-            double r2 = dx * dx + dy * dy + dz * dz;
-            if (r2 == 0.0) continue;
-            double q = s_q[j];
-            if (DIM == 3) {
-              double rinv = rsqrt(r2);
-              double v = sc.cq * rinv;
-              if (sc.cd != 0.0)
-                v += sc.cd * (s_n[0][j] * dx + s_n[1][j] * dy + s_n[2][j] * dz) * rinv * rinv * rinv;
-              acc = fma(q, v, acc);
-            } else {
-              double v = 0.5 * sc.cq * log(r2);
-              if (sc.cd != 0.0) v -= sc.cd * (s_n[0][j] * dx + s_n[1][j] * dy) / r2;
-              acc = fma(q, v, acc);
-            }
+  const bool dip = sc.cd != 0.0;
+  double acc = 0.0;
+  int l0 = g.list1_starts[itb], l1 = g.list1_starts[itb + 1];
+  for (int gb = l0; gb < l1; gb += MAXB) {
+    int nb = min(MAXB, l1 - gb);
+    __syncthreads();
+    list_prefix(g, g.list1_lists, gb, nb, s_pref, s_start, err);
+    __syncthreads();
+    int total = s_pref[nb];
+    for (int base = 0; base < total; base += NT) {
+      if (dip) load_stream_tile<DIM, true>(g, st, total, nb, base, s_pref, s_start, s_y, s_n, s_q);
+      else load_stream_tile<DIM, false>(g, st, total, nb, base, s_pref, s_start, s_y, s_n, s_q);
+      __syncthreads();
+      int jbeg = warp * 32, jend = min(jbeg + 32, total - base);
+      if (active) {
+        for (int j = jbeg; j < jend; ++j) {
+          double dx = x[0] - s_y[0][j], dy = x[1] - s_y[1][j];
+          double dz = (DIM == 3) ? x[2] - s_y[2][j] : 0.0;
+          double r2 = dx * dx + dy * dy + dz * dz;
+          if (r2 == 0.0) continue;
+          double q = s_q[j];
+          if (DIM == 3) {
+            double rinv = rsqrt(r2);
+            double v = sc.cq * rinv;
+            if (dip)
+              v += sc.cd * (s_n[0][j] * dx + s_n[1][j] * dy + s_n[2][j] * dz) * rinv * rinv * rinv;
+            acc = fma(q, v, acc);
+          } else {
+            double v = 0.5 * sc.cq * log(r2);
+            if (dip) v -= sc.cd * (s_n[0][j] * dx + s_n[1][j] * dy) / r2;
+            acc = fma(q, v, acc);
           }
         }
-        __syncthreads();
       }
+      __syncthreads();
     }
-    if (active) pot[(size_t)r * g.nfiltered_targets + t0 + t] += acc;
+  }
+  if (warp > 0) s_red[warp - 1][lane] = acc;
+  __syncthreads();
+  if (warp == 0 && active) {
+    for (int w = 1; w < NW; ++w) acc += s_red[w - 1][lane];
+    pot[(size_t)r * g.nfiltered_targets + t] += acc;
   }
 }
 
+// M2P over list 3 (eval_multipoles, fmm.py:487-493).  Same chunking; the warps
+// split the list-3 boxes and stage each multipole in their own shared slice.
 template <int DIM>
 __global__ void __launch_bounds__(NT)
 k_eval_multipoles(qbxfmm_geometry g, int p, int ncf, int nrhs,
                   const double2* __restrict__ mpoles, double* __restrict__ pot, int32_t* err)
 {
   extern __shared__ double2 smem2[];
-  double2* M = smem2;
-  int itb = blockIdx.x;
-  int tb = g.target_boxes[itb];
+  __shared__ double s_red[NW - 1][32];
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double2* M = smem2 + (size_t)warp * ncf;
+  int chunk = blockIdx.x;
   int r = blockIdx.y;
-  int t0 = g.nonqbx_box_target_starts[tb];
-  int nt = g.nonqbx_box_target_counts_nonchild[tb];
-  if (nt == 0) return;
-  for (int tbase = 0; tbase < nt; tbase += NT) {
-    int t = tbase + threadIdx.x;
-    bool active = t < nt;
-    double x[3] = {0, 0, 0};
-    if (active) load_point<DIM>(g.nonqbx_targets, g.nfiltered_targets, t0 + t, x);
-    double acc = 0.0;
-    for (int li = g.list3_starts[itb]; li < g.list3_starts[itb + 1]; ++li) {
-      int sb = g.list3_lists[li];
-      if ((unsigned)sb >= (unsigned)g.nboxes) {
-        report(err, QBX_DEVERR_BAD_BOX);
-        continue;
-      }
-      const double2* src = mpoles + ((size_t)sb * nrhs + r) * ncf;
-      for (int q = threadIdx.x; q < ncf; q += NT) M[q] = src[q];
-      __syncthreads();
-      if (active) {
-        double rho = level_width(g, g.box_levels[sb]);
-        double cs[3];
-        load_point<DIM>(g.box_centers, g.nboxes, sb, cs);
-        double u0 = (x[0] - cs[0]) / rho, u1 = (x[1] - cs[1]) / rho;
-        if (DIM == 3) {
-          double u2 = (x[2] - cs[2]) / rho;
-          double rinv2 = 1.0 / (u0 * u0 + u1 * u1 + u2 * u2);
-          double2 mm = c2(sqrt(rinv2));
-          double s = 0.0;
-          for (int m = 0; m <= p; ++m) {
-            if (m > 0) mm = cscale((2.0 * m - 1) * rinv2, cmul(mm, c2(u0, u1)));
-            double w = (m == 0) ? 1.0 : 2.0;
-            double2 a = mm, prev = c2(0.0);
-            for (int n = m; n <= p; ++n) {
-              if (n > m) {
-                double2 bb = cscale(rinv2, csub(cscale((2.0 * n - 1) * u2, a),
-                                                cscale((double)(n + m - 1) * (n - m - 1), prev)));
-                prev = a;
-                a = bb;
-              }
-              double2 cm = M[idx3(n, m)];
-              s += w * (cm.x * a.x - cm.y * a.y);
-            }
+  int itb = g.nonqbx_chunk_target_box[chunk];
+  int t = g.nonqbx_chunk_start[chunk] + lane;
+  bool active = lane < g.nonqbx_chunk_count[chunk];
+  double x[3] = {0, 0, 0};
+  if (active) load_point<DIM>(g.nonqbx_targets, g.nfiltered_targets, t, x);
+  double acc = 0.0;
+  for (int li = g.list3_starts[itb] + warp; li < g.list3_starts[itb + 1]; li += NW) {
+    int sb = g.list3_lists[li];
+    if ((unsigned)sb >= (unsigned)g.nboxes) {
+      report(err, QBX_DEVERR_BAD_BOX);
+      continue;
+    }
+    __syncwarp();
+    const double2* src = mpoles + ((size_t)sb * nrhs + r) * ncf;
+    for (int q = lane; q < ncf; q += 32) M[q] = src[q];
+    __syncwarp();
+    if (!active) continue;
+    double rho = level_width(g, g.box_levels[sb]);
+    double cs[3];
+    load_point<DIM>(g.box_centers, g.nboxes, sb, cs);
+    double u0 = (x[0] - cs[0]) / rho, u1 = (x[1] - cs[1]) / rho;
+    if (DIM == 3) {
+      double u2 = (x[2] - cs[2]) / rho;
+      double rinv2 = 1.0 / (u0 * u0 + u1 * u1 + u2 * u2);
+      double2 mm = c2(sqrt(rinv2));
+      double s = 0.0;
+      for (int m = 0; m <= p; ++m) {
+        if (m > 0) mm = cscale((2.0 * m - 1) * rinv2, cmul(mm, c2(u0, u1)));
+        double w = (m == 0) ? 1.0 : 2.0;
+        double2 a = mm, prev = c2(0.0);
+        const double2* mc = M + idx3(m, m);
+        for (int n = m; n <= p; ++n) {
+          if (n > m) {
+            double2 bb = cscale(rinv2, csub(cscale((2.0 * n - 1) * u2, a),
+                                            cscale((double)(n + m - 1) * (n - m - 1), prev)));
+            prev = a;
+            a = bb;
           }
-          acc += s / rho;
-        } else {
-          double2 zc = c2(x[0] - cs[0], x[1] - cs[1]);
-          double2 uinv = cinv(c2(u0, u1));
-          double2 sum = cmul(M[0], clog_(zc));
-          double2 pw = uinv;
-          for (int k = 1; k <= p; ++k) {
-            sum = cfma(M[k], pw, sum);
-            pw = cmul(pw, uinv);
-          }
-          acc += sum.x;
+          double2 cm = *mc;
+          mc += n + 1;   // idx3(n+1, m) - idx3(n, m)
+          s += w * (cm.x * a.x - cm.y * a.y);
         }
       }
-      __syncthreads();
+      acc += s / rho;
+    } else {
+      double2 zc = c2(x[0] - cs[0], x[1] - cs[1]);
+      double2 uinv = cinv(c2(u0, u1));
+      double2 sum = cmul(M[0], clog_(zc));
+      double2 pw = uinv;
+      for (int k = 1; k <= p; ++k) {
+        sum = cfma(M[k], pw, sum);
+        pw = cmul(pw, uinv);
+      }
+      acc += sum.x;
     }
-    if (active) pot[(size_t)r * g.nfiltered_targets + t0 + t] += acc;
+  }
+  __syncthreads();
+  if (warp > 0) s_red[warp - 1][lane] = acc;
+  __syncthreads();
+  if (warp == 0 && active) {
+    for (int w = 1; w < NW; ++w) acc += s_red[w - 1][lane];
+    pot[(size_t)r * g.nfiltered_targets + t] += acc;
   }
 }
 
@@ -737,8 +960,6 @@ k_p2qbxl(qbxfmm_geometry g, SourceCoeffs sc, int nrhs, const double* __restrict_
          double2* __restrict__ qbx_exps, int32_t* err)
 {
   constexpr int NC = (DIM == 3) ? (Q + 1) * (Q + 2) / 2 : Q + 1;
-  constexpr int NW = NT / 32;
-  constexpr int MAXB = 128;
   __shared__ double s_y[3][NT];
   __shared__ double s_n[3][NT];
   __shared__ double s_q[NT];
@@ -773,45 +994,11 @@ k_p2qbxl(qbxfmm_geometry g, SourceCoeffs sc, int nrhs, const double* __restrict_
   for (int gb = l0; gb < l1; gb += MAXB) {
     int nb = min(MAXB, l1 - gb);
     __syncthreads();
-    if (threadIdx.x == 0) {
-      int tot = 0;
-      for (int k = 0; k < nb; ++k) {
-        int sb = g.list1_lists[gb + k];
-        int cnt = 0, s0 = 0;
-        if ((unsigned)sb < (unsigned)g.nboxes) {
-          s0 = g.box_source_starts[sb];
-          cnt = g.box_source_counts_nonchild[sb];
-        } else {
-          report(err, QBX_DEVERR_BAD_BOX);
-        }
-        s_pref[k] = tot;
-        s_start[k] = s0;
-        tot += cnt;
-      }
-      s_pref[nb] = tot;
-    }
+    list_prefix(g, g.list1_lists, gb, nb, s_pref, s_start, err);
     __syncthreads();
     int total = s_pref[nb];
     for (int base = 0; base < total; base += NT) {
-      int v = base + threadIdx.x;
-      if (v < total) {
-        int lo = 0, hi = nb - 1;
-        while (lo < hi) {
-          int mid = (lo + hi + 1) >> 1;
-          if (s_pref[mid] <= v) lo = mid;
-          else hi = mid - 1;
-        }
-        int s = s_start[lo] + (v - s_pref[lo]);
-        double y[3], nv[3] = {0, 0, 0};
-        load_point<DIM>(g.sources, g.nsources, s, y);
-        if (DIP) load_point<DIM>(g.source_normals, g.nsources, s, nv);
-#pragma unroll
-        for (int d = 0; d < DIM; ++d) {
-          s_y[d][threadIdx.x] = y[d];
-          s_n[d][threadIdx.x] = nv[d];
-        }
-        s_q[threadIdx.x] = __ldg(st + s);
-      }
+      load_stream_tile<DIM, DIP>(g, st, total, nb, base, s_pref, s_start, s_y, s_n, s_q);
       __syncthreads();
       int jbeg = warp * 32;
       int jend = min(jbeg + 32, total - base);
@@ -883,30 +1070,50 @@ k_p2qbxl(qbxfmm_geometry g, SourceCoeffs sc, int nrhs, const double* __restrict_
 }
 
 // M2QBXL (translate_box_multipoles_to_qbx_local, fmm.py:267-312;
-// interactions.py:196-235): one warp per center chunk; list-3 multipoles staged in
-// shared memory; each lane runs the singular-harmonic recurrence for its center and
-// scatters into its register-resident QBX coefficients.
+// interactions.py:196-235), all source levels in one launch.  CTA = 4 warps over
+// one chunk of <= 32 centers (lane = center); the warps split the list-3 boxes.
+// 3D: each warp expands the source multipole into a zero-padded dense table
+// Mpad[k][l] (rows k in [-Q, pf+Q], columns l in [-(pf+2Q), pf+Q]); each lane runs the
+// singular-harmonic recurrence for its center column by column and scatters every
+// S_{n'}^{m'} into its register-resident coefficients (j, i) through
+// Mpad[n'-j][m'-i]: one broadcast shared load and one complex FMA per term, no
+// branches.
 template <int DIM, int Q>
-__global__ void __launch_bounds__(32)
+__global__ void __launch_bounds__(NT)
 k_m2qbxl(qbxfmm_geometry g, int pf, int ncf, int nrhs, const double2* __restrict__ mpoles,
          double2* __restrict__ qbx_exps, int32_t* err)
 {
   constexpr int NC = (DIM == 3) ? (Q + 1) * (Q + 2) / 2 : Q + 1;
   extern __shared__ double2 smem2[];
-  double2* M = smem2;
+  const int MW = 2 * pf + 3 * Q + 1;      // columns l + (pf + 2Q)
+  const int MR = pf + 2 * Q + 1;          // rows k + Q
+  const int MSZ = (DIM == 3) ? MR * MW : ncf;
+  const int loff = pf + 2 * Q;
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double2* Mw = smem2 + (size_t)warp * MSZ;
+  double2* red = smem2 + (size_t)NW * MSZ;   // [NW-1][32][NC]
+
   int chunk = blockIdx.x;
   int r = blockIdx.y;
   int itb = g.qbx_chunk_target_box[chunk];
-  int lane = threadIdx.x;
   bool has_center = lane < g.qbx_chunk_count[chunk];
   int ctr = has_center ? g.centers_by_target_box[g.qbx_chunk_start[chunk] + lane] : 0;
+  if ((unsigned)ctr >= (unsigned)g.ncenters) {
+    report(err, QBX_DEVERR_BAD_CENTER);
+    has_center = false;
+    ctr = 0;
+  }
   double cc[3] = {0, 0, 0};
   load_point<DIM>(g.centers, g.ncenters, ctr, cc);
   double rho_t = g.expansion_radii[ctr];
+  if (DIM == 3)
+    for (int q = lane; q < MSZ; q += 32) Mw[q] = c2(0.0);
   double2 acc[NC];
 #pragma unroll
   for (int i = 0; i < NC; ++i) acc[i] = c2(0.0);
-  for (int li = g.list3_starts[itb]; li < g.list3_starts[itb + 1]; ++li) {
+
+  int l0 = g.list3_starts[itb], l1 = g.list3_starts[itb + 1];
+  for (int li = l0 + warp; li < l1; li += NW) {
     int sb = g.list3_lists[li];
     if ((unsigned)sb >= (unsigned)g.nboxes) {
       report(err, QBX_DEVERR_BAD_BOX);
@@ -914,7 +1121,17 @@ k_m2qbxl(qbxfmm_geometry g, int pf, int ncf, int nrhs, const double2* __restrict
     }
     __syncwarp();
     const double2* src = mpoles + ((size_t)sb * nrhs + r) * ncf;
-    for (int q = lane; q < ncf; q += 32) M[q] = src[q];
+    if (DIM == 3) {
+      for (int q = lane; q < ncf; q += 32) {
+        int k, l;
+        decode3(q, k, l);
+        double2 v = src[q];
+        Mw[(k + Q) * MW + loff + l] = v;
+        if (l > 0) Mw[(k + Q) * MW + loff - l] = (l & 1) ? c2(-v.x, v.y) : c2(v.x, -v.y);
+      }
+    } else {
+      for (int q = lane; q < ncf; q += 32) Mw[q] = src[q];
+    }
     __syncwarp();
     if (!has_center) continue;
     double rho_s = level_width(g, g.box_levels[sb]);
@@ -922,7 +1139,8 @@ k_m2qbxl(qbxfmm_geometry g, int pf, int ncf, int nrhs, const double2* __restrict
     load_point<DIM>(g.box_centers, g.nboxes, sb, cs);
     double ratio = rho_t / rho_s;
     if (DIM == 3) {
-      double d0 = (cc[0] - cs[0]) / rho_s, d1 = (cc[1] - cs[1]) / rho_s, d2 = (cc[2] - cs[2]) / rho_s;
+      double d0 = (cc[0] - cs[0]) / rho_s, d1 = (cc[1] - cs[1]) / rho_s,
+             d2 = (cc[2] - cs[2]) / rho_s;
       double rinv2 = 1.0 / (d0 * d0 + d1 * d1 + d2 * d2);
       int nmax = pf + Q;
       double2 part[NC];
@@ -932,6 +1150,8 @@ k_m2qbxl(qbxfmm_geometry g, int pf, int ncf, int nrhs, const double2* __restrict
       for (int mp = 0; mp <= nmax; ++mp) {
         if (mp > 0) mm = cscale((2.0 * mp - 1) * rinv2, cmul(mm, c2(d0, d1)));
         double2 a = mm, prev = c2(0.0);
+        const double2* bpos = Mw + (mp + Q) * MW + loff + mp;   // row n'=mp, column m'
+        const double2* bneg = Mw + (mp + Q) * MW + loff - mp;   // column -m'
         for (int np = mp; np <= nmax; ++np) {
           if (np > mp) {
             double2 bb = cscale(rinv2, csub(cscale((2.0 * np - 1) * d2, a),
@@ -939,21 +1159,21 @@ k_m2qbxl(qbxfmm_geometry g, int pf, int ncf, int nrhs, const double2* __restrict
             prev = a;
             a = bb;
           }
-          // S_{np}^{mp} = a ; S_{np}^{-mp} = (-1)^mp conj(a)
-          double2 aneg = (mp & 1) ? c2(-a.x, a.y) : c2(a.x, -a.y);
 #pragma unroll
           for (int j = 0; j <= Q; ++j)
 #pragma unroll
-            for (int ii = 0; ii <= j; ++ii) {
-              int k = np - j;
-              if (k < 0 || k > pf) continue;
-              int l = mp - ii;
-              if (l <= k && -l <= k) part[idx3(j, ii)] = cfma(sh3_get(M, k, l), a, part[idx3(j, ii)]);
-              if (mp > 0) {
-                int l2 = -mp - ii;
-                if (-l2 <= k) part[idx3(j, ii)] = cfma(sh3_get(M, k, l2), aneg, part[idx3(j, ii)]);
-              }
-            }
+            for (int ii = 0; ii <= j; ++ii)
+              part[idx3(j, ii)] = cfma(bpos[-j * MW - ii], a, part[idx3(j, ii)]);
+          if (mp > 0) {
+            double2 aneg = (mp & 1) ? c2(-a.x, a.y) : c2(a.x, -a.y);
+#pragma unroll
+            for (int j = 0; j <= Q; ++j)
+#pragma unroll
+              for (int ii = 0; ii <= j; ++ii)
+                part[idx3(j, ii)] = cfma(bneg[-j * MW - ii], aneg, part[idx3(j, ii)]);
+          }
+          bpos += MW;
+          bneg += MW;
         }
       }
       double rj = 1.0 / rho_s;
@@ -965,11 +1185,10 @@ k_m2qbxl(qbxfmm_geometry g, int pf, int ncf, int nrhs, const double2* __restrict
         rj *= ratio;
       }
     } else {
+      const double2* M = Mw;
       double2 tau = c2((cc[0] - cs[0]) / rho_s, (cc[1] - cs[1]) / rho_s);
       double2 tinv = cinv(tau);
       double2 t = c2(cc[0] - cs[0], cc[1] - cs[1]);
-      // L0 = M0 log t + sum_k Mk tau^-k ;
-      // Ll = ratio^l [M0 (-1)^(l+1)/(l tau^l) + (-1)^l tau^-l sum_k Mk C(k+l-1,l) tau^-k]
       double2 s0 = cmul(M[0], clog_(t));
       double2 sl[Q + 1];
       double bin[Q + 1];
@@ -1002,10 +1221,20 @@ k_m2qbxl(qbxfmm_geometry g, int pf, int ncf, int nrhs, const double2* __restrict
       }
     }
   }
-  if (has_center) {
+  __syncthreads();
+  if (warp > 0) {
+#pragma unroll
+    for (int i = 0; i < NC; ++i) red[((warp - 1) * 32 + lane) * NC + i] = acc[i];
+  }
+  __syncthreads();
+  if (warp == 0 && has_center) {
     double2* out = qbx_exps + ((size_t)ctr * nrhs + r) * NC;
 #pragma unroll
-    for (int i = 0; i < NC; ++i) out[i] = cadd(out[i], acc[i]);
+    for (int i = 0; i < NC; ++i) {
+      double2 a = acc[i];
+      for (int w = 1; w < NW; ++w) a = cadd(a, red[((w - 1) * 32 + lane) * NC + i]);
+      out[i] = cadd(out[i], a);
+    }
   }
 }
 
@@ -1221,22 +1450,22 @@ cudaError_t launch_m2m(const qbxfmm_geometry& g, const int32_t* lvl_host, int p,
   return g.dim == 3 ? m2m_<3>(g, lvl_host, p, nrhs, mp, st) : m2m_<2>(g, lvl_host, p, nrhs, mp, st);
 }
 
-template <int DIM>
-static cudaError_t m2l_(const qbxfmm_geometry& g, int p, int nrhs, const double2* mp,
-                        double2* lo, int32_t* err, cudaStream_t st)
-{
-  if (g.nttp_boxes == 0) return cudaSuccess;
-  int ncf = (int)ncoef_dim(DIM, p);
-  size_t sh = ((size_t)ncf + (DIM == 3 ? ncoef_dim(3, 2 * p) : (size_t)2 * p + 2)) * sizeof(double2);
-  cudaFuncSetAttribute(k_m2l<DIM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
-  k_m2l<DIM><<<dim3(g.nttp_boxes, grid_y(nrhs)), NT, sh, st>>>(g, p, ncf, nrhs, mp, lo, err);
-  return cudaGetLastError();
-}
-
 cudaError_t launch_m2l(const qbxfmm_geometry& g, int p, int nrhs, const double2* mp, double2* lo,
                        int32_t* err, cudaStream_t st)
 {
-  return g.dim == 3 ? m2l_<3>(g, p, nrhs, mp, lo, err, st) : m2l_<2>(g, p, nrhs, mp, lo, err, st);
+  if (g.nttp_boxes == 0) return cudaSuccess;
+  int ncf = (int)ncoef_dim(g.dim, p);
+  if (g.dim == 3) {
+    size_t per = ((size_t)(2 * p + 1) * (3 * p + 1) + (size_t)(p + 1) * (2 * p + 1)) * sizeof(double2);
+    int pb = (int)std::min<size_t>(4, std::max<size_t>(1, (160 * 1024 - ncf * sizeof(double2)) / per));
+    size_t sh = pb * per + ncf * sizeof(double2);
+    cudaFuncSetAttribute(k_m2l3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+    k_m2l3<<<dim3(g.nttp_boxes, grid_y(nrhs)), NT, sh, st>>>(g, p, ncf, nrhs, pb, mp, lo, err);
+  } else {
+    size_t sh = ((size_t)ncf + 2 * p + 2) * sizeof(double2);
+    k_m2l2<<<dim3(g.nttp_boxes, grid_y(nrhs)), NT, sh, st>>>(g, p, ncf, nrhs, mp, lo, err);
+  }
+  return cudaGetLastError();
 }
 
 template <int DIM>
@@ -1246,7 +1475,7 @@ static cudaError_t p2l_(const qbxfmm_geometry& g, SourceCoeffs sc, int p, int nr
   if (g.nttp_boxes == 0) return cudaSuccess;
   int ncf = (int)ncoef_dim(DIM, p);
   int nct = DIM == 3 ? (p + 2) * (p + 3) / 2 : p + 3;
-  size_t sh = 16 * (size_t)nct * sizeof(double2);
+  size_t sh = 32 * (size_t)nct * sizeof(double2);
   cudaFuncSetAttribute(k_p2l<DIM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
   k_p2l<DIM><<<dim3(g.nttp_boxes, grid_y(nrhs)), NT, sh, st>>>(g, sc, p, ncf, nrhs, s, lo, err);
   return cudaGetLastError();
@@ -1283,8 +1512,8 @@ cudaError_t launch_l2l(const qbxfmm_geometry& g, const int32_t* lvl_host, int p,
 cudaError_t launch_eval_direct(const qbxfmm_geometry& g, SourceCoeffs sc, int nrhs,
                                const double* s, double* pot, int32_t* err, cudaStream_t st)
 {
-  if (g.ntarget_boxes == 0 || g.nfiltered_targets == 0) return cudaSuccess;
-  dim3 grid(g.ntarget_boxes, grid_y(nrhs));
+  if (g.nnonqbx_chunks == 0) return cudaSuccess;
+  dim3 grid(g.nnonqbx_chunks, grid_y(nrhs));
   if (g.dim == 3) k_eval_direct<3><<<grid, NT, 0, st>>>(g, sc, nrhs, s, pot, err);
   else k_eval_direct<2><<<grid, NT, 0, st>>>(g, sc, nrhs, s, pot, err);
   return cudaGetLastError();
@@ -1293,10 +1522,10 @@ cudaError_t launch_eval_direct(const qbxfmm_geometry& g, SourceCoeffs sc, int nr
 cudaError_t launch_eval_multipoles(const qbxfmm_geometry& g, int p, int nrhs, const double2* mp,
                                    double* pot, int32_t* err, cudaStream_t st)
 {
-  if (g.ntarget_boxes == 0 || g.nfiltered_targets == 0) return cudaSuccess;
+  if (g.nnonqbx_chunks == 0) return cudaSuccess;
   int ncf = (int)ncoef_dim(g.dim, p);
-  size_t sh = (size_t)ncf * sizeof(double2);
-  dim3 grid(g.ntarget_boxes, grid_y(nrhs));
+  size_t sh = (size_t)NW * ncf * sizeof(double2);
+  dim3 grid(g.nnonqbx_chunks, grid_y(nrhs));
   if (g.dim == 3) k_eval_multipoles<3><<<grid, NT, sh, st>>>(g, p, ncf, nrhs, mp, pot, err);
   else k_eval_multipoles<2><<<grid, NT, sh, st>>>(g, p, ncf, nrhs, mp, pot, err);
   return cudaGetLastError();
@@ -1339,8 +1568,11 @@ static cudaError_t m2qbxl_q(const qbxfmm_geometry& g, int pf, int nrhs, const do
                             double2* qe, int32_t* err, cudaStream_t st)
 {
   int ncf = (int)ncoef_dim(DIM, pf);
-  size_t sh = (size_t)ncf * sizeof(double2);
-  k_m2qbxl<DIM, Q><<<dim3(g.nqbx_chunks, grid_y(nrhs)), 32, sh, st>>>(g, pf, ncf, nrhs, mp, qe, err);
+  constexpr int NC = (DIM == 3) ? (Q + 1) * (Q + 2) / 2 : Q + 1;
+  size_t msz = DIM == 3 ? (size_t)(pf + 2 * Q + 1) * (2 * pf + 3 * Q + 1) : (size_t)ncf;
+  size_t sh = (NW * msz + (size_t)(NW - 1) * 32 * NC) * sizeof(double2);
+  cudaFuncSetAttribute(k_m2qbxl<DIM, Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+  k_m2qbxl<DIM, Q><<<dim3(g.nqbx_chunks, grid_y(nrhs)), NT, sh, st>>>(g, pf, ncf, nrhs, mp, qe, err);
   return cudaGetLastError();
 }
 
