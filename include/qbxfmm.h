@@ -50,6 +50,11 @@ typedef struct qbxfmm_kernel {
   int32_t fmm_order;         /* order of box multipole/local expansions */
   int32_t nrhs;              /* number of densities applied in one traversal */
   int32_t precision;         /* 0 = plain FP64, 1 = mixed (FP32 far field) */
+  int32_t target_specific_qbx; /* 1: the list-1 near field of each QBX target is
+                                  evaluated target-specifically (Legendre / line
+                                  series per target and source) instead of through
+                                  the center's expansion (pytential's
+                                  _use_target_specific_qbx, fmm.py:391-394) */
 } qbxfmm_kernel;
 
 /* Tree, traversal and QBX geometry, field names after boxtree's Tree /
@@ -126,6 +131,15 @@ typedef struct qbxfmm_geometry {
   const int32_t* nonqbx_chunk_target_box;   /* target box index per chunk */
   const int32_t* nonqbx_chunk_start;        /* first filtered target of the chunk */
   const int32_t* nonqbx_chunk_count;
+
+  /* Work schedule for the target-specific near field: (QBX target, center) pairs
+   * grouped by the center's target box, in chunks of at most QBXFMM_CENTER_CHUNK. */
+  int32_t ntsqbx_chunks;
+  const int32_t* tsqbx_chunk_target_box;
+  const int32_t* tsqbx_chunk_start;
+  const int32_t* tsqbx_chunk_count;
+  const int32_t* tsqbx_targets;             /* tree target index per pair */
+  const int32_t* tsqbx_centers;             /* center index per pair */
 } qbxfmm_geometry;
 
 #define QBXFMM_CENTER_CHUNK 32

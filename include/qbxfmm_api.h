@@ -84,6 +84,14 @@ int qbxfmm_translate_box_local_to_qbx_local(const qbxfmm_plan* plan, const void*
  * pytential/qbx/interactions.py:419-532); writes pot_tree entries of QBX targets */
 int qbxfmm_eval_qbx_expansions(const qbxfmm_plan* plan, const void* qbx_exps, void* pot_tree,
                                void* stream);
+/* eval_target_specific_qbx_locals (pytential/qbx/fmm.py:391-394; the reference's
+ * native implementation is pytential/qbx/target_specific/impl.pyx:566-785): adds the
+ * list-1 near field of every QBX target, evaluated per (target, source) pair, to
+ * pot_tree.  Used instead of the list-1 part of form_global_qbx_locals when the
+ * kernel's target_specific_qbx flag is set (Laplace). */
+int qbxfmm_eval_target_specific_qbx_locals(const qbxfmm_plan* plan, const void* strengths,
+                                           void* pot_tree, int32_t* error_word, void* stream);
+
 /* potential assembly: scatter the non-QBX part, add the QBX part, reorder to user
  * targets, apply the kernel scaling (pytential/qbx/fmm.py:569-588,
  * pytential/qbx/__init__.py:775-793).  out: [nrhs][nuser_targets] (written). */

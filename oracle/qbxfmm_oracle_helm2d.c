@@ -14,14 +14,49 @@
  * Coefficients are scaled by rscale^|m| (multipoles divided, locals multiplied).
  */
 
+/* J_0..J_N by Miller's backward recurrence (normalized with J_0 + 2 sum J_2k = 1),
+ * Y_0, Y_1 from the C library and Y_{n+1} = (2n/x) Y_n - Y_{n-1}: the same published
+ * algorithms the device code uses, so the comparison tests the FMM, not two
+ * different Bessel implementations. */
+static void h2_bessel(int N, double x, double* Jv, double* Yv, int needY)
+{
+  double xinv = 1.0 / x;
+  int nmax = N > (int)x ? N : (int)x;
+  int start = 2 * ((nmax + 16 + (int)sqrt(40.0 * nmax)) / 2);
+  double fp1 = 0.0, f = 1e-200, sum = 0.0;
+  for (int j = 0; j <= N; ++j) Jv[j] = 0.0;
+  for (int k = start; k > 0; --k) {
+    double fm1 = 2.0 * k * xinv * f - fp1;
+    fp1 = f;
+    f = fm1;
+    if (k - 1 <= N) Jv[k - 1] = f;
+    if (((k - 1) & 1) == 0 && k - 1 > 0) sum += 2.0 * f;
+    if (fabs(f) > 1e200) {
+      f *= 1e-200;
+      fp1 *= 1e-200;
+      sum *= 1e-200;
+      for (int j = k - 1; j <= N; ++j) Jv[j] *= 1e-200;
+    }
+  }
+  sum += f;
+  for (int j = 0; j <= N; ++j) Jv[j] /= sum;
+  if (needY) {
+    Yv[0] = y0(x);
+    if (N >= 1) Yv[1] = y1(x);
+    for (int j = 1; j < N; ++j) Yv[j + 1] = 2.0 * j * xinv * Yv[j] - Yv[j - 1];
+  }
+}
+
 static void h2_zfun(int N, double k, double ux, double uy, cplx* J, cplx* H, int needH)
 {
   double r = sqrt(ux * ux + uy * uy);
   double th = atan2(uy, ux);
   double x = k * r;
+  double Jv[160], Yv[160];
+  h2_bessel(N, x, Jv, Yv, needH);
   for (int m = 0; m <= N; ++m) {
-    double jm = jn(m, x);
-    double ym = needH ? yn(m, x) : 0.0;
+    double jm = Jv[m];
+    double ym = needH ? Yv[m] : 0.0;
     cplx e = cexp(I * m * th);
     double sg = (m & 1) ? -1.0 : 1.0;
     J[N + m] = jm * e;

@@ -34,7 +34,7 @@ class QBXFMMKernel(ctypes.Structure):
         ("charge_coeff_re", _f64), ("charge_coeff_im", _f64),
         ("dipole_coeff_re", _f64), ("dipole_coeff_im", _f64),
         ("qbx_order", _i32), ("fmm_order", _i32), ("nrhs", _i32),
-        ("precision", _i32),
+        ("precision", _i32), ("target_specific_qbx", _i32),
     ]
 
 
@@ -72,6 +72,8 @@ GEOMETRY_FIELDS = [
     ("qbx_chunk_count", "pi"), ("centers_by_target_box", "pi"),
     ("nnonqbx_chunks", "i"), ("nonqbx_chunk_target_box", "pi"), ("nonqbx_chunk_start", "pi"),
     ("nonqbx_chunk_count", "pi"),
+    ("ntsqbx_chunks", "i"), ("tsqbx_chunk_target_box", "pi"), ("tsqbx_chunk_start", "pi"),
+    ("tsqbx_chunk_count", "pi"), ("tsqbx_targets", "pi"), ("tsqbx_centers", "pi"),
 ]
 
 CENTER_CHUNK = 32
@@ -163,6 +165,40 @@ def nonqbx_target_schedule(target_boxes, nonqbx_box_target_starts,
             ch_count[o].astype(np.int32))
 
 
+def tsqbx_schedule(centers_by_target_box, qbx_center_to_target_box, center_to_targets_starts,
+                   center_to_targets_lists, chunk: int = CENTER_CHUNK):
+    """(QBX target, center) pairs in the order of ``centers_by_target_box``, cut into
+    chunks of at most ``chunk`` pairs that share a target box.
+
+    Returns ``(chunk_target_box, chunk_start, chunk_count, targets, centers)``."""
+    cbt = np.asarray(centers_by_target_box)
+    c2tb = np.asarray(qbx_center_to_target_box)
+    st = np.asarray(center_to_targets_starts)
+    lists = np.asarray(center_to_targets_lists)
+    tg, ct, tb = [], [], []
+    for c in cbt:
+        for it in range(st[c], st[c + 1]):
+            tg.append(lists[it])
+            ct.append(c)
+            tb.append(c2tb[c])
+    z = np.zeros(0, np.int32)
+    if not tg:
+        return z, z, z, z, z
+    tb = np.array(tb)
+    ch_tb, ch_start, ch_count = [], [], []
+    i = 0
+    while i < len(tb):
+        j = i
+        while j < len(tb) and tb[j] == tb[i] and j - i < chunk:
+            j += 1
+        ch_tb.append(tb[i])
+        ch_start.append(i)
+        ch_count.append(j - i)
+        i = j
+    return (np.array(ch_tb, np.int32), np.array(ch_start, np.int32),
+            np.array(ch_count, np.int32), np.array(tg, np.int32), np.array(ct, np.int32))
+
+
 def _i(a):
     return np.ascontiguousarray(a, dtype=np.int32)
 
@@ -231,7 +267,12 @@ def geometry_arrays(geo) -> tuple[dict, dict]:
         arrays["list1_lists"], arrays["list3_starts"], arrays["box_source_counts_nonchild"])
     arrays.update({"nonqbx_chunk_target_box": nq_tb, "nonqbx_chunk_start": nq_start,
                    "nonqbx_chunk_count": nq_count})
+    ts = tsqbx_schedule(cbt, arrays["qbx_center_to_target_box"],
+                        arrays["center_to_targets_starts"], arrays["center_to_targets_lists"])
+    arrays.update(dict(zip(["tsqbx_chunk_target_box", "tsqbx_chunk_start", "tsqbx_chunk_count",
+                            "tsqbx_targets", "tsqbx_centers"], ts)))
     scalars = {
+        "ntsqbx_chunks": len(ts[0]),
         "nnonqbx_chunks": len(nq_tb),
         "nqbx_chunks": len(ch_tb),
         "dim": tree.dimensions, "nboxes": tree.nboxes, "nlevels": tree.nlevels,
@@ -266,12 +307,13 @@ def make_geometry_struct(scalars: dict, arrays: dict, ptr_of) -> QBXFMMGeometry:
 
 
 def make_kernel_struct(*, family, dim, qbx_order, fmm_order, nrhs=1, k=0.0,
-                       charge_coeff=0.0, dipole_coeff=0.0, precision=0) -> QBXFMMKernel:
+                       charge_coeff=0.0, dipole_coeff=0.0, precision=0,
+                       target_specific_qbx=False) -> QBXFMMKernel:
     k = complex(k)
     cc = complex(charge_coeff)
     dc = complex(dipole_coeff)
     return QBXFMMKernel(family, dim, k.real, k.imag, cc.real, cc.imag, dc.real, dc.imag,
-                        qbx_order, fmm_order, nrhs, precision)
+                        qbx_order, fmm_order, nrhs, precision, int(bool(target_specific_qbx)))
 
 
 def ncoeff(family: int, dim: int, order: int) -> int:

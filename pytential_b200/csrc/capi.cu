@@ -21,6 +21,8 @@ struct qbxfmm_plan {
   std::vector<int32_t> lvl_source_parent;  // host copy of level_start_source_parent_box_nrs
   std::vector<int32_t> lvl_ttp;            // host copy of level_start_ttp_box_nrs
   SourceCoeffs sc;
+  HelmCoeffs hc;
+  bool helm;
   int ncf, ncq;
 };
 
@@ -69,17 +71,23 @@ int qbxfmm_plan_create(const qbxfmm_kernel* kernel, const qbxfmm_geometry* geome
   *out = nullptr;
   const qbxfmm_kernel& k = *kernel;
   const qbxfmm_geometry& g = *geometry;
-  if (k.family != QBXFMM_LAPLACE)
-    return fail(QBXFMM_ERR_UNSUPPORTED, "only the Laplace family is built into this library");
+  if (k.family != QBXFMM_LAPLACE && k.family != QBXFMM_HELMHOLTZ)
+    return fail(QBXFMM_ERR_UNSUPPORTED, "kernel family must be Laplace or Helmholtz");
   if (k.dim != 2 && k.dim != 3) return fail(QBXFMM_ERR_ARG, "dim must be 2 or 3");
+  if (k.family == QBXFMM_HELMHOLTZ && k.dim != 2)
+    return fail(QBXFMM_ERR_UNSUPPORTED, "the Helmholtz family is built for 2D only");
+  if (k.family == QBXFMM_HELMHOLTZ && (k.k_im != 0.0 || !(k.k_re > 0.0)))
+    return fail(QBXFMM_ERR_UNSUPPORTED, "Helmholtz wave number must be real and positive");
   if (g.dim != k.dim) return fail(QBXFMM_ERR_ARG, "kernel and geometry dimensions differ");
   if (k.qbx_order < 0 || k.qbx_order > 8)
     return fail(QBXFMM_ERR_UNSUPPORTED, "qbx_order must be in [0, 8]");
-  if (k.fmm_order < 1 || k.fmm_order > 20)
+  if (k.fmm_order < 1 || k.fmm_order > 20 || (k.family == QBXFMM_HELMHOLTZ && k.qbx_order + k.fmm_order > 28))
     return fail(QBXFMM_ERR_UNSUPPORTED, "fmm_order must be in [1, 20]");
   if (k.nrhs < 1) return fail(QBXFMM_ERR_ARG, "nrhs must be >= 1");
   if (k.precision != 0) return fail(QBXFMM_ERR_UNSUPPORTED, "only precision 0 (FP64)");
-  if (k.charge_coeff_im != 0.0 || k.dipole_coeff_im != 0.0)
+  if (k.target_specific_qbx && k.family != QBXFMM_LAPLACE)
+    return fail(QBXFMM_ERR_UNSUPPORTED, "target-specific QBX is built for the Laplace family");
+  if (k.family == QBXFMM_LAPLACE && (k.charge_coeff_im != 0.0 || k.dipole_coeff_im != 0.0))
     return fail(QBXFMM_ERR_ARG, "Laplace source coefficients must be real");
   if (g.nlevels < 1 || g.nboxes < 1 || g.nlevels > 40) return fail(QBXFMM_ERR_ARG, "bad tree sizes");
   if (k.dipole_coeff_re != 0.0 && !g.source_normals)
@@ -91,6 +99,10 @@ int qbxfmm_plan_create(const qbxfmm_kernel* kernel, const qbxfmm_geometry* geome
   p->geo = g;
   p->sc.cq = k.charge_coeff_re;
   p->sc.cd = k.dipole_coeff_re;
+  p->helm = k.family == QBXFMM_HELMHOLTZ;
+  p->hc.cq = make_double2(k.charge_coeff_re, k.charge_coeff_im);
+  p->hc.cd = make_double2(k.dipole_coeff_re, k.dipole_coeff_im);
+  p->hc.k = k.k_re;
   p->ncf = ncoeff(k.family, k.dim, k.fmm_order);
   p->ncq = ncoeff(k.family, k.dim, k.qbx_order);
   p->lvl_source_parent.resize(g.nlevels + 1);
@@ -121,27 +133,42 @@ int qbxfmm_form_strengths(const qbxfmm_plan* p, const qbxfmm_upsample* up, const
   if (!up || !density || !strengths) return fail(QBXFMM_ERR_ARG, "null argument");
   if (up->quad_nodes_per_element * up->nelements != p->geo.nsources)
     return fail(QBXFMM_ERR_ARG, "upsampler does not match the number of sources");
-  QBX_TRY(launch_form_strengths(p->geo, *up, p->kern.nrhs, (const double*)density,
-                                (double*)strengths, S(stream)),
-          "form_strengths");
+  if (p->helm)
+    QBX_TRY(h2_launch_form_strengths(p->geo, *up, p->kern.nrhs, (const double2*)density,
+                                     (double2*)strengths, S(stream)),
+            "form_strengths");
+  else
+    QBX_TRY(launch_form_strengths(p->geo, *up, p->kern.nrhs, (const double*)density,
+                                  (double*)strengths, S(stream)),
+            "form_strengths");
   return QBXFMM_OK;
 }
 
 int qbxfmm_form_multipoles(const qbxfmm_plan* p, const void* strengths, void* mpoles, void* stream)
 {
   if (int rc = check_plan(p)) return rc;
-  QBX_TRY(launch_p2m(p->geo, p->sc, p->kern.fmm_order, p->kern.nrhs, (const double*)strengths,
-                     (double2*)mpoles, S(stream)),
-          "form_multipoles");
+  if (p->helm)
+    QBX_TRY(h2_launch_p2m(p->geo, p->hc, p->kern.fmm_order, p->kern.nrhs,
+                          (const double2*)strengths, (double2*)mpoles, nullptr, S(stream)),
+            "form_multipoles");
+  else
+    QBX_TRY(launch_p2m(p->geo, p->sc, p->kern.fmm_order, p->kern.nrhs, (const double*)strengths,
+                       (double2*)mpoles, S(stream)),
+            "form_multipoles");
   return QBXFMM_OK;
 }
 
 int qbxfmm_coarsen_multipoles(const qbxfmm_plan* p, void* mpoles, void* stream)
 {
   if (int rc = check_plan(p)) return rc;
-  QBX_TRY(launch_m2m(p->geo, p->lvl_source_parent.data(), p->kern.fmm_order, p->kern.nrhs,
-                     (double2*)mpoles, S(stream)),
-          "coarsen_multipoles");
+  if (p->helm)
+    QBX_TRY(h2_launch_m2m(p->geo, p->lvl_source_parent.data(), p->hc, p->kern.fmm_order,
+                          p->kern.nrhs, (double2*)mpoles, nullptr, S(stream)),
+            "coarsen_multipoles");
+  else
+    QBX_TRY(launch_m2m(p->geo, p->lvl_source_parent.data(), p->kern.fmm_order, p->kern.nrhs,
+                       (double2*)mpoles, S(stream)),
+            "coarsen_multipoles");
   return QBXFMM_OK;
 }
 
@@ -149,9 +176,14 @@ int qbxfmm_eval_direct(const qbxfmm_plan* p, const void* strengths, void* pot_no
                        int32_t* error_word, void* stream)
 {
   if (int rc = check_plan(p)) return rc;
-  QBX_TRY(launch_eval_direct(p->geo, p->sc, p->kern.nrhs, (const double*)strengths,
-                             (double*)pot_nonqbx, error_word, S(stream)),
-          "eval_direct");
+  if (p->helm)
+    QBX_TRY(h2_launch_eval_direct(p->geo, p->hc, p->kern.nrhs, (const double2*)strengths,
+                                  (double2*)pot_nonqbx, error_word, S(stream)),
+            "eval_direct");
+  else
+    QBX_TRY(launch_eval_direct(p->geo, p->sc, p->kern.nrhs, (const double*)strengths,
+                               (double*)pot_nonqbx, error_word, S(stream)),
+            "eval_direct");
   return QBXFMM_OK;
 }
 
@@ -159,9 +191,14 @@ int qbxfmm_multipole_to_local(const qbxfmm_plan* p, const void* mpoles, void* lo
                               int32_t* error_word, void* stream)
 {
   if (int rc = check_plan(p)) return rc;
-  QBX_TRY(launch_m2l(p->geo, p->kern.fmm_order, p->kern.nrhs, (const double2*)mpoles,
-                     (double2*)locals, error_word, S(stream)),
-          "multipole_to_local");
+  if (p->helm)
+    QBX_TRY(h2_launch_m2l(p->geo, p->hc, p->kern.fmm_order, p->kern.nrhs, (const double2*)mpoles,
+                          (double2*)locals, error_word, S(stream)),
+            "multipole_to_local");
+  else
+    QBX_TRY(launch_m2l(p->geo, p->kern.fmm_order, p->kern.nrhs, (const double2*)mpoles,
+                       (double2*)locals, error_word, S(stream)),
+            "multipole_to_local");
   return QBXFMM_OK;
 }
 
@@ -169,9 +206,15 @@ int qbxfmm_eval_multipoles(const qbxfmm_plan* p, const void* mpoles, void* pot_n
                            int32_t* error_word, void* stream)
 {
   if (int rc = check_plan(p)) return rc;
-  QBX_TRY(launch_eval_multipoles(p->geo, p->kern.fmm_order, p->kern.nrhs, (const double2*)mpoles,
-                                 (double*)pot_nonqbx, error_word, S(stream)),
-          "eval_multipoles");
+  if (p->helm)
+    QBX_TRY(h2_launch_eval_multipoles(p->geo, p->hc, p->kern.fmm_order, p->kern.nrhs,
+                                      (const double2*)mpoles, (double2*)pot_nonqbx, error_word,
+                                      S(stream)),
+            "eval_multipoles");
+  else
+    QBX_TRY(launch_eval_multipoles(p->geo, p->kern.fmm_order, p->kern.nrhs, (const double2*)mpoles,
+                                   (double*)pot_nonqbx, error_word, S(stream)),
+            "eval_multipoles");
   return QBXFMM_OK;
 }
 
@@ -179,27 +222,42 @@ int qbxfmm_form_locals(const qbxfmm_plan* p, const void* strengths, void* locals
                        int32_t* error_word, void* stream)
 {
   if (int rc = check_plan(p)) return rc;
-  QBX_TRY(launch_p2l(p->geo, p->sc, p->kern.fmm_order, p->kern.nrhs, (const double*)strengths,
-                     (double2*)locals, error_word, S(stream)),
-          "form_locals");
+  if (p->helm)
+    QBX_TRY(h2_launch_p2l(p->geo, p->hc, p->kern.fmm_order, p->kern.nrhs,
+                          (const double2*)strengths, (double2*)locals, error_word, S(stream)),
+            "form_locals");
+  else
+    QBX_TRY(launch_p2l(p->geo, p->sc, p->kern.fmm_order, p->kern.nrhs, (const double*)strengths,
+                       (double2*)locals, error_word, S(stream)),
+            "form_locals");
   return QBXFMM_OK;
 }
 
 int qbxfmm_refine_locals(const qbxfmm_plan* p, void* locals, void* stream)
 {
   if (int rc = check_plan(p)) return rc;
-  QBX_TRY(launch_l2l(p->geo, p->lvl_ttp.data(), p->kern.fmm_order, p->kern.nrhs,
-                     (double2*)locals, S(stream)),
-          "refine_locals");
+  if (p->helm)
+    QBX_TRY(h2_launch_l2l(p->geo, p->lvl_ttp.data(), p->hc, p->kern.fmm_order, p->kern.nrhs,
+                          (double2*)locals, nullptr, S(stream)),
+            "refine_locals");
+  else
+    QBX_TRY(launch_l2l(p->geo, p->lvl_ttp.data(), p->kern.fmm_order, p->kern.nrhs,
+                       (double2*)locals, S(stream)),
+            "refine_locals");
   return QBXFMM_OK;
 }
 
 int qbxfmm_eval_locals(const qbxfmm_plan* p, const void* locals, void* pot_nonqbx, void* stream)
 {
   if (int rc = check_plan(p)) return rc;
-  QBX_TRY(launch_eval_locals(p->geo, p->kern.fmm_order, p->kern.nrhs, (const double2*)locals,
-                             (double*)pot_nonqbx, S(stream)),
-          "eval_locals");
+  if (p->helm)
+    QBX_TRY(h2_launch_eval_locals(p->geo, p->hc, p->kern.fmm_order, p->kern.nrhs,
+                                  (const double2*)locals, (double2*)pot_nonqbx, nullptr, S(stream)),
+            "eval_locals");
+  else
+    QBX_TRY(launch_eval_locals(p->geo, p->kern.fmm_order, p->kern.nrhs, (const double2*)locals,
+                               (double*)pot_nonqbx, S(stream)),
+            "eval_locals");
   return QBXFMM_OK;
 }
 
@@ -207,9 +265,14 @@ int qbxfmm_form_global_qbx_locals(const qbxfmm_plan* p, const void* strengths, v
                                   int32_t* error_word, void* stream)
 {
   if (int rc = check_plan(p)) return rc;
-  QBX_TRY(launch_p2qbxl(p->geo, p->sc, p->kern.qbx_order, p->kern.nrhs, (const double*)strengths,
-                        (double2*)qbx_exps, error_word, S(stream)),
-          "form_global_qbx_locals");
+  if (p->helm)
+    QBX_TRY(h2_launch_p2qbxl(p->geo, p->hc, p->kern.qbx_order, p->kern.nrhs,
+                             (const double2*)strengths, (double2*)qbx_exps, error_word, S(stream)),
+            "form_global_qbx_locals");
+  else
+    QBX_TRY(launch_p2qbxl(p->geo, p->sc, p->kern.qbx_order, p->kern.nrhs, (const double*)strengths,
+                          (double2*)qbx_exps, error_word, S(stream)),
+            "form_global_qbx_locals");
   return QBXFMM_OK;
 }
 
@@ -217,9 +280,14 @@ int qbxfmm_translate_box_multipoles_to_qbx_local(const qbxfmm_plan* p, const voi
                                                  void* qbx_exps, int32_t* error_word, void* stream)
 {
   if (int rc = check_plan(p)) return rc;
-  QBX_TRY(launch_m2qbxl(p->geo, p->kern.fmm_order, p->kern.qbx_order, p->kern.nrhs,
-                        (const double2*)mpoles, (double2*)qbx_exps, error_word, S(stream)),
-          "translate_box_multipoles_to_qbx_local");
+  if (p->helm)
+    QBX_TRY(h2_launch_m2qbxl(p->geo, p->hc, p->kern.fmm_order, p->kern.qbx_order, p->kern.nrhs,
+                             (const double2*)mpoles, (double2*)qbx_exps, error_word, S(stream)),
+            "translate_box_multipoles_to_qbx_local");
+  else
+    QBX_TRY(launch_m2qbxl(p->geo, p->kern.fmm_order, p->kern.qbx_order, p->kern.nrhs,
+                          (const double2*)mpoles, (double2*)qbx_exps, error_word, S(stream)),
+            "translate_box_multipoles_to_qbx_local");
   return QBXFMM_OK;
 }
 
@@ -227,9 +295,14 @@ int qbxfmm_translate_box_local_to_qbx_local(const qbxfmm_plan* p, const void* lo
                                             void* qbx_exps, void* stream)
 {
   if (int rc = check_plan(p)) return rc;
-  QBX_TRY(launch_l2qbxl(p->geo, p->kern.fmm_order, p->kern.qbx_order, p->kern.nrhs,
-                        (const double2*)locals, (double2*)qbx_exps, S(stream)),
-          "translate_box_local_to_qbx_local");
+  if (p->helm)
+    QBX_TRY(h2_launch_l2qbxl(p->geo, p->hc, p->kern.fmm_order, p->kern.qbx_order, p->kern.nrhs,
+                             (const double2*)locals, (double2*)qbx_exps, nullptr, S(stream)),
+            "translate_box_local_to_qbx_local");
+  else
+    QBX_TRY(launch_l2qbxl(p->geo, p->kern.fmm_order, p->kern.qbx_order, p->kern.nrhs,
+                          (const double2*)locals, (double2*)qbx_exps, S(stream)),
+            "translate_box_local_to_qbx_local");
   return QBXFMM_OK;
 }
 
@@ -237,9 +310,26 @@ int qbxfmm_eval_qbx_expansions(const qbxfmm_plan* p, const void* qbx_exps, void*
                                void* stream)
 {
   if (int rc = check_plan(p)) return rc;
-  QBX_TRY(launch_qbxl2p(p->geo, p->kern.qbx_order, p->kern.nrhs, (const double2*)qbx_exps,
-                        (double*)pot_tree, S(stream)),
-          "eval_qbx_expansions");
+  if (p->helm)
+    QBX_TRY(h2_launch_qbxl2p(p->geo, p->hc, p->kern.qbx_order, p->kern.nrhs,
+                             (const double2*)qbx_exps, (double2*)pot_tree, S(stream)),
+            "eval_qbx_expansions");
+  else
+    QBX_TRY(launch_qbxl2p(p->geo, p->kern.qbx_order, p->kern.nrhs, (const double2*)qbx_exps,
+                          (double*)pot_tree, S(stream)),
+            "eval_qbx_expansions");
+  return QBXFMM_OK;
+}
+
+int qbxfmm_eval_target_specific_qbx_locals(const qbxfmm_plan* p, const void* strengths,
+                                           void* pot_tree, int32_t* error_word, void* stream)
+{
+  if (int rc = check_plan(p)) return rc;
+  if (p->helm)
+    return fail(QBXFMM_ERR_UNSUPPORTED, "target-specific QBX is built for the Laplace family");
+  QBX_TRY(launch_tsqbx(p->geo, p->sc, p->kern.qbx_order, p->kern.nrhs, (const double*)strengths,
+                       (double*)pot_tree, error_word, S(stream)),
+          "eval_target_specific_qbx_locals");
   return QBXFMM_OK;
 }
 
@@ -247,9 +337,14 @@ int qbxfmm_assemble(const qbxfmm_plan* p, const void* pot_nonqbx, const void* po
                     void* stream)
 {
   if (int rc = check_plan(p)) return rc;
-  QBX_TRY(launch_assemble(p->geo, p->kern.nrhs, (const double*)pot_nonqbx,
-                          (const double*)pot_tree, (double*)out, S(stream)),
-          "assemble");
+  if (p->helm)
+    QBX_TRY(h2_launch_assemble(p->geo, p->kern.nrhs, (const double2*)pot_nonqbx,
+                               (const double2*)pot_tree, (double2*)out, S(stream)),
+            "assemble");
+  else
+    QBX_TRY(launch_assemble(p->geo, p->kern.nrhs, (const double*)pot_nonqbx,
+                            (const double*)pot_tree, (double*)out, S(stream)),
+            "assemble");
   return QBXFMM_OK;
 }
 
@@ -297,13 +392,19 @@ int qbxfmm_apply(const qbxfmm_plan* p, const qbxfmm_upsample* up, const qbxfmm_w
   if ((rc = qbxfmm_form_locals(p, ws->strengths, ws->locals, ws->error_word, stream))) return rc;
   if ((rc = qbxfmm_refine_locals(p, ws->locals, stream))) return rc;
   if ((rc = qbxfmm_eval_locals(p, ws->locals, ws->pot_nonqbx, stream))) return rc;
-  if ((rc = qbxfmm_form_global_qbx_locals(p, ws->strengths, ws->qbx_exps, ws->error_word, stream)))
+  const bool tsqbx = p->kern.target_specific_qbx != 0;
+  if (!tsqbx &&
+      (rc = qbxfmm_form_global_qbx_locals(p, ws->strengths, ws->qbx_exps, ws->error_word, stream)))
     return rc;
   if ((rc = qbxfmm_translate_box_multipoles_to_qbx_local(p, ws->mpoles, ws->qbx_exps,
                                                          ws->error_word, stream)))
     return rc;
   if ((rc = qbxfmm_translate_box_local_to_qbx_local(p, ws->locals, ws->qbx_exps, stream))) return rc;
   if ((rc = qbxfmm_eval_qbx_expansions(p, ws->qbx_exps, ws->pot_tree, stream))) return rc;
+  if (tsqbx &&
+      (rc = qbxfmm_eval_target_specific_qbx_locals(p, ws->strengths, ws->pot_tree,
+                                                   ws->error_word, stream)))
+    return rc;
   return qbxfmm_assemble(p, ws->pot_nonqbx, ws->pot_tree, out, stream);
 }
 

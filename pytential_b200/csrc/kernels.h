@@ -33,7 +33,39 @@ cudaError_t launch_l2qbxl(const qbxfmm_geometry& g, int pf, int q, int nrhs, con
                           double2* qe, cudaStream_t st);
 cudaError_t launch_qbxl2p(const qbxfmm_geometry& g, int q, int nrhs, const double2* qe,
                           double* pt, cudaStream_t st);
+cudaError_t launch_tsqbx(const qbxfmm_geometry& g, SourceCoeffs sc, int q, int nrhs,
+                         const double* s, double* pt, int32_t* err, cudaStream_t st);
 cudaError_t launch_assemble(const qbxfmm_geometry& g, int nrhs, const double* pot_nonqbx,
                             const double* pot_tree, double* out, cudaStream_t st);
+
+// 2D Helmholtz (complex128 strengths and potentials)
+cudaError_t h2_launch_form_strengths(const qbxfmm_geometry& g, const qbxfmm_upsample& up, int nrhs,
+                                     const double2* density, double2* strengths, cudaStream_t st);
+cudaError_t h2_launch_p2m(const qbxfmm_geometry& g, HelmCoeffs hc, int p, int nrhs,
+                          const double2* s, double2* mp, int32_t* err, cudaStream_t st);
+cudaError_t h2_launch_m2m(const qbxfmm_geometry& g, const int32_t* lvl_host, HelmCoeffs hc, int p,
+                          int nrhs, double2* mp, int32_t* err, cudaStream_t st);
+cudaError_t h2_launch_eval_direct(const qbxfmm_geometry& g, HelmCoeffs hc, int nrhs,
+                                  const double2* s, double2* pot, int32_t* err, cudaStream_t st);
+cudaError_t h2_launch_m2l(const qbxfmm_geometry& g, HelmCoeffs hc, int p, int nrhs,
+                          const double2* mp, double2* lo, int32_t* err, cudaStream_t st);
+cudaError_t h2_launch_eval_multipoles(const qbxfmm_geometry& g, HelmCoeffs hc, int p, int nrhs,
+                                      const double2* mp, double2* pot, int32_t* err, cudaStream_t st);
+cudaError_t h2_launch_p2l(const qbxfmm_geometry& g, HelmCoeffs hc, int p, int nrhs,
+                          const double2* s, double2* lo, int32_t* err, cudaStream_t st);
+cudaError_t h2_launch_l2l(const qbxfmm_geometry& g, const int32_t* lvl_host, HelmCoeffs hc, int p,
+                          int nrhs, double2* lo, int32_t* err, cudaStream_t st);
+cudaError_t h2_launch_eval_locals(const qbxfmm_geometry& g, HelmCoeffs hc, int p, int nrhs,
+                                  const double2* lo, double2* pot, int32_t* err, cudaStream_t st);
+cudaError_t h2_launch_p2qbxl(const qbxfmm_geometry& g, HelmCoeffs hc, int q, int nrhs,
+                             const double2* s, double2* qe, int32_t* err, cudaStream_t st);
+cudaError_t h2_launch_m2qbxl(const qbxfmm_geometry& g, HelmCoeffs hc, int pf, int q, int nrhs,
+                             const double2* mp, double2* qe, int32_t* err, cudaStream_t st);
+cudaError_t h2_launch_l2qbxl(const qbxfmm_geometry& g, HelmCoeffs hc, int pf, int q, int nrhs,
+                             const double2* lo, double2* qe, int32_t* err, cudaStream_t st);
+cudaError_t h2_launch_qbxl2p(const qbxfmm_geometry& g, HelmCoeffs hc, int q, int nrhs,
+                             const double2* qe, double2* pt, cudaStream_t st);
+cudaError_t h2_launch_assemble(const qbxfmm_geometry& g, int nrhs, const double2* pot_nonqbx,
+                               const double2* pot_tree, double2* out, cudaStream_t st);
 
 }  // namespace qbx

@@ -1,0 +1,895 @@
+// 2D Helmholtz QBX-FMM stage kernels (H2D expansions), complex128, sm_100a.
+//
+// Same stage set and work decomposition as the Laplace kernels
+// (pytential/qbx/fmm.py:414-594): box kernels one CTA per box, point evaluations
+// and the QBX near field over the chunked schedules, with complex densities and
+// Bessel/Hankel bases (helmholtz.cuh).  Per source the single- and double-layer
+// weights are folded into three complex factors
+//   q = cq s,  a = (k/2) cd s conj(nu),  b = (k/2) cd s nu      (nu = n_x + i n_y)
+// so that a multipole coefficient gets q conj(J_m) + a conj(J_{m-1}) - b conj(J_{m+1})
+// and a local coefficient q Hb_m + a Hb_{m-1} - b Hb_{m+1}.
+#include "helmholtz.cuh"
+#include "kernels.h"
+
+namespace qbx {
+
+namespace {
+
+constexpr int NT = 128;
+constexpr int NW = NT / 32;
+constexpr int MAXB = 128;
+constexpr int ZMAX = 2 * 20 + 2;   // Bessel scratch: orders 0..2 * max fmm_order + 1
+
+QBX_D void h_list_prefix(const qbxfmm_geometry& g, const int32_t* __restrict__ lists, int gb,
+                         int nb, int* s_pref, int* s_start, int32_t* err)
+{
+  if (threadIdx.x >= 32) return;
+  int lane = threadIdx.x;
+  int cnt[4], loc = 0;
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    int k = lane * 4 + u;
+    cnt[u] = 0;
+    if (k < nb) {
+      int sb = lists[gb + k];
+      int s0 = 0;
+      if ((unsigned)sb < (unsigned)g.nboxes) {
+        s0 = g.box_source_starts[sb];
+        cnt[u] = g.box_source_counts_nonchild[sb];
+      } else {
+        report(err, QBX_DEVERR_BAD_BOX);
+      }
+      s_start[k] = s0;
+    }
+    loc += cnt[u];
+  }
+  int incl = loc;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    int v = __shfl_up_sync(0xffffffffu, incl, off);
+    if (lane >= off) incl += v;
+  }
+  int run = incl - loc;
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    int k = lane * 4 + u;
+    if (k < nb) s_pref[k] = run;
+    run += cnt[u];
+  }
+  if (lane == 31) s_pref[nb] = incl;
+}
+
+QBX_D int h_stream_source(int v, int nb, const int* s_pref, const int* s_start)
+{
+  int lo = 0, hi = nb - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (s_pref[mid] <= v) lo = mid;
+    else hi = mid - 1;
+  }
+  return s_start[lo] + (v - s_pref[lo]);
+}
+
+// the three per-source factors (see the file comment)
+QBX_D void source_factors(const HelmCoeffs& hc, double2 s, double nx, double ny, bool dip,
+                          double2& q, double2& a, double2& b)
+{
+  q = cmul(hc.cq, s);
+  if (dip) {
+    double2 sig = cscale(0.5 * hc.k, cmul(hc.cd, s));
+    a = cmul(sig, c2(nx, -ny));
+    b = cmul(sig, c2(nx, ny));
+  } else {
+    a = b = c2(0.0);
+  }
+}
+
+QBX_D double2 cneg(double2 a) { return c2(-a.x, -a.y); }
+
+// Hb_m(u) = (-1)^m H_{-m}(u) from a Z table centred at index N
+QBX_D double2 hbar(const double2* Z, int N, int m)
+{
+  double2 v = Z[N - m];
+  return (m & 1) ? cneg(v) : v;
+}
+
+}  // namespace
+
+// {{{ strengths (complex density)
+
+__global__ void __launch_bounds__(256)
+k_h2_form_strengths(int nsources, int ndofs, int npe, int nqpe, const double* __restrict__ U,
+                    const double* __restrict__ qw, const int32_t* __restrict__ user_source_ids,
+                    const double2* __restrict__ density, double2* __restrict__ out)
+{
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  int r = blockIdx.y;
+  if (t >= nsources) return;
+  int j = __ldg(user_source_ids + t);
+  int e = j / nqpe;
+  int jj = j - e * nqpe;
+  const double* u = U + (size_t)jj * npe;
+  const double2* d = density + (size_t)r * ndofs + (size_t)e * npe;
+  double2 acc = c2(0.0);
+  for (int i = 0; i < npe; ++i) acc = caxpy(__ldg(u + i), d[i], acc);
+  out[(size_t)r * nsources + t] = cscale(__ldg(qw + j), acc);
+}
+
+// }}}
+
+// {{{ P2M (source boxes) and P2L (list 4)
+
+template <bool LOCAL>
+__global__ void __launch_bounds__(NT)
+k_h2_p2e(qbxfmm_geometry g, HelmCoeffs hc, int p, int nrhs, const double2* __restrict__ strengths,
+         double2* __restrict__ exps, int32_t* err)
+{
+  constexpr int SUB = 32;
+  extern __shared__ double2 smem2[];
+  const int N = p + 1, ZW = 2 * N + 1;
+  double2* Z = smem2;                                  // [SUB][ZW]
+  __shared__ double2 s_q[SUB], s_a[SUB], s_b[SUB];
+  __shared__ int s_pref[MAXB + 1], s_start[MAXB];
+  int i = blockIdx.x;
+  int r = blockIdx.y;
+  int b, l0, l1;
+  const int32_t* lists;
+  if (LOCAL) {
+    b = g.target_or_target_parent_boxes[i];
+    lists = g.list4_lists;
+    l0 = g.list4_starts[i];
+    l1 = g.list4_starts[i + 1];
+  } else {
+    b = g.source_boxes[i];
+    lists = g.source_boxes;   // the box's own sources
+    l0 = i;
+    l1 = i + 1;
+  }
+  double rho = level_width(g, g.box_levels[b]);
+  double c[2];
+  load_point<2>(g.box_centers, g.nboxes, b, c);
+  const double2* st = strengths + (size_t)r * g.nsources;
+  const bool dip = hc.cd.x != 0.0 || hc.cd.y != 0.0;
+  double Jb[ZMAX], Yb[ZMAX];
+  int m = (int)threadIdx.x - p;
+  double2 acc = c2(0.0);
+  for (int gb = l0; gb < l1; gb += MAXB) {
+    int nb = min(MAXB, l1 - gb);
+    __syncthreads();
+    h_list_prefix(g, lists, gb, nb, s_pref, s_start, err);
+    __syncthreads();
+    int total = s_pref[nb];
+    for (int base = 0; base < total; base += SUB) {
+      int cnt = min(SUB, total - base);
+      if (threadIdx.x < cnt) {
+        int s = h_stream_source(base + threadIdx.x, nb, s_pref, s_start);
+        double y[2], nv[2] = {0, 0};
+        load_point<2>(g.sources, g.nsources, s, y);
+        if (dip) load_point<2>(g.source_normals, g.nsources, s, nv);
+        double2 q, a, bb;
+        source_factors(hc, st[s], nv[0], nv[1], dip, q, a, bb);
+        s_q[threadIdx.x] = q;
+        s_a[threadIdx.x] = a;
+        s_b[threadIdx.x] = bb;
+        h2_zfun(N, hc.k, y[0] - c[0], y[1] - c[1], Jb, Yb, Z + (size_t)threadIdx.x * ZW, LOCAL);
+      }
+      __syncthreads();
+      if (m <= p) {
+        for (int j = 0; j < cnt; ++j) {
+          const double2* Zt = Z + (size_t)j * ZW;
+          if (!LOCAL) {
+            acc = cfmac(s_q[j], Zt[N + m], acc);
+            if (dip) {
+              acc = cfmac(s_a[j], Zt[N + m - 1], acc);
+              acc = cfmac(cneg(s_b[j]), Zt[N + m + 1], acc);
+            }
+          } else {
+            acc = cfma(s_q[j], hbar(Zt, N, m), acc);
+            if (dip) {
+              acc = cfma(s_a[j], hbar(Zt, N, m - 1), acc);
+              acc = cfma(cneg(s_b[j]), hbar(Zt, N, m + 1), acc);
+            }
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  if (m <= p) {
+    int am = m < 0 ? -m : m;
+    double sc = LOCAL ? pow(rho, (double)am) : pow(rho, -(double)am);
+    double2* E = exps + ((size_t)b * nrhs + r) * (2 * p + 1);
+    E[m + p] = caxpy(sc, acc, E[m + p]);
+  }
+}
+
+// }}}
+
+// {{{ translations: M2M, L2L (per level), M2L (list 2)
+
+// Eout_m += fout(m) sum_n Ein_n fin(n) Z_{n-m}(d) with Z = J (M2M, L2L) or H (M2L).
+// One CTA per output box; thread m. Z tables (order 2p) for up to NT source boxes
+// are built one per thread into shared memory.
+template <int KIND>   // 0 = M2M, 1 = M2L, 2 = L2L
+__global__ void __launch_bounds__(NT)
+k_h2_translate(qbxfmm_geometry g, HelmCoeffs hc, int p, int nrhs, int i0,
+               const double2* __restrict__ ein, double2* __restrict__ eout, int32_t* err)
+{
+  constexpr int PB = 16;
+  extern __shared__ double2 smem2[];
+  const int NZ = 2 * p, ZW = 2 * NZ + 1, NC = 2 * p + 1;
+  double2* Z = smem2;                       // [PB][ZW]
+  double2* E = Z + (size_t)PB * ZW;         // [PB][NC]
+  __shared__ int s_src[PB];
+  __shared__ double s_rin[PB];
+  double Jb[ZMAX], Yb[ZMAX];
+  int ib = i0 + blockIdx.x;
+  int r = blockIdx.y;
+  int tb;
+  int l0, l1;
+  if (KIND == 0) {
+    tb = g.source_parent_boxes[ib];
+    l0 = 0;
+    l1 = 4;     // children
+  } else if (KIND == 1) {
+    tb = g.target_or_target_parent_boxes[ib];
+    l0 = g.list2_starts[ib];
+    l1 = g.list2_starts[ib + 1];
+  } else {
+    tb = g.target_or_target_parent_boxes[ib];
+    l0 = 0;
+    l1 = 1;     // parent
+  }
+  double rho_t = level_width(g, g.box_levels[tb]);
+  double ct[2];
+  load_point<2>(g.box_centers, g.nboxes, tb, ct);
+  int m = (int)threadIdx.x - p;
+  double2 acc = c2(0.0);
+  for (int lb = l0; lb < l1; lb += PB) {
+    int nbat = min(PB, l1 - lb);
+    __syncthreads();
+    if (threadIdx.x < nbat) {
+      int sb;
+      if (KIND == 0) {
+        sb = g.box_child_ids[(size_t)(lb + threadIdx.x) * g.nboxes + tb];
+        if (sb == 0 || g.box_source_counts_cumul[sb] == 0) sb = -1;
+      } else if (KIND == 1) {
+        sb = g.list2_lists[lb + threadIdx.x];
+        if ((unsigned)sb >= (unsigned)g.nboxes) {
+          report(err, QBX_DEVERR_BAD_BOX);
+          sb = -1;
+        }
+      } else {
+        sb = g.box_parent_ids[tb];
+      }
+      s_src[threadIdx.x] = sb;
+      double2* Zt = Z + (size_t)threadIdx.x * ZW;
+      if (sb >= 0) {
+        double cs[2];
+        load_point<2>(g.box_centers, g.nboxes, sb, cs);
+        s_rin[threadIdx.x] = level_width(g, g.box_levels[sb]);
+        // d = c_out - c_in
+        h2_zfun(NZ, hc.k, ct[0] - cs[0], ct[1] - cs[1], Jb, Yb, Zt, KIND == 1);
+      }
+    }
+    __syncthreads();
+    for (int w = threadIdx.x; w < nbat * NC; w += NT) {
+      int bb = w / NC, n = w - bb * NC - p;
+      int sb = s_src[bb];
+      double2 v = c2(0.0);
+      if (sb >= 0) {
+        int an = n < 0 ? -n : n;
+        double f = (KIND == 2) ? pow(s_rin[bb], -(double)an) : pow(s_rin[bb], (double)an);
+        v = cscale(f, ein[((size_t)sb * nrhs + r) * NC + n + p]);
+      }
+      E[(size_t)bb * NC + n + p] = v;
+    }
+    __syncthreads();
+    if (m <= p) {
+      for (int bb = 0; bb < nbat; ++bb) {
+        if (s_src[bb] < 0) continue;
+        const double2* Zt = Z + (size_t)bb * ZW;
+        const double2* Eb = E + (size_t)bb * NC;
+        for (int n = -p; n <= p; ++n) acc = cfma(Eb[n + p], Zt[NZ + n - m], acc);
+      }
+    }
+  }
+  if (m <= p) {
+    int am = m < 0 ? -m : m;
+    double f = (KIND == 0) ? pow(rho_t, -(double)am) : pow(rho_t, (double)am);
+    double2* Eo = eout + ((size_t)tb * nrhs + r) * (2 * p + 1);
+    Eo[m + p] = caxpy(f, acc, Eo[m + p]);
+  }
+}
+
+// }}}
+
+// {{{ point evaluations at non-QBX targets
+
+__global__ void __launch_bounds__(NT)
+k_h2_eval_direct(qbxfmm_geometry g, HelmCoeffs hc, int nrhs, const double2* __restrict__ strengths,
+                 double2* __restrict__ pot, int32_t* err)
+{
+  __shared__ double s_y[2][NT], s_n[2][NT];
+  __shared__ double2 s_q[NT], s_d[NT];
+  __shared__ int s_pref[MAXB + 1], s_start[MAXB];
+  __shared__ double2 s_red[NW - 1][32];
+  int chunk = blockIdx.x;
+  int r = blockIdx.y;
+  int itb = g.nonqbx_chunk_target_box[chunk];
+  int t = g.nonqbx_chunk_start[chunk] + (threadIdx.x & 31);
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  bool active = lane < g.nonqbx_chunk_count[chunk];
+  double x[2] = {0, 0};
+  if (active) load_point<2>(g.nonqbx_targets, g.nfiltered_targets, t, x);
+  const double2* st = strengths + (size_t)r * g.nsources;
+  const bool dip = hc.cd.x != 0.0 || hc.cd.y != 0.0;
+  double2 acc = c2(0.0);
+  int l0 = g.list1_starts[itb], l1 = g.list1_starts[itb + 1];
+  for (int gb = l0; gb < l1; gb += MAXB) {
+    int nb = min(MAXB, l1 - gb);
+    __syncthreads();
+    h_list_prefix(g, g.list1_lists, gb, nb, s_pref, s_start, err);
+    __syncthreads();
+    int total = s_pref[nb];
+    for (int base = 0; base < total; base += NT) {
+      int v = base + threadIdx.x;
+      if (v < total) {
+        int s = h_stream_source(v, nb, s_pref, s_start);
+        double y[2], nv[2] = {0, 0};
+        load_point<2>(g.sources, g.nsources, s, y);
+        if (dip) load_point<2>(g.source_normals, g.nsources, s, nv);
+        s_y[0][threadIdx.x] = y[0];
+        s_y[1][threadIdx.x] = y[1];
+        s_n[0][threadIdx.x] = nv[0];
+        s_n[1][threadIdx.x] = nv[1];
+        s_q[threadIdx.x] = cmul(hc.cq, st[s]);
+        s_d[threadIdx.x] = cscale(hc.k, cmul(hc.cd, st[s]));
+      }
+      __syncthreads();
+      int jbeg = warp * 32, jend = min(jbeg + 32, total - base);
+      if (active) {
+        for (int j = jbeg; j < jend; ++j) {
+          double dx = x[0] - s_y[0][j], dy = x[1] - s_y[1][j];
+          double r2 = dx * dx + dy * dy;
+          if (r2 == 0.0) continue;
+          double rr = sqrt(r2), kr = hc.k * rr;
+          acc = cfma(s_q[j], c2(j0(kr), y0(kr)), acc);
+          if (dip) {
+            double cn = (s_n[0][j] * dx + s_n[1][j] * dy) / rr;
+            acc = cfma(cscale(cn, s_d[j]), c2(j1(kr), y1(kr)), acc);
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  if (warp > 0) s_red[warp - 1][lane] = acc;
+  __syncthreads();
+  if (warp == 0 && active) {
+    for (int w = 1; w < NW; ++w) acc = cadd(acc, s_red[w - 1][lane]);
+    double2* P = pot + (size_t)r * g.nfiltered_targets + t;
+    *P = cadd(*P, acc);
+  }
+}
+
+// M2P over list 3 (lanes = targets, warps split the boxes) and L2P (own box)
+template <bool LOCAL>
+__global__ void __launch_bounds__(NT)
+k_h2_eval_exp(qbxfmm_geometry g, HelmCoeffs hc, int p, int nrhs, const double2* __restrict__ exps,
+              double2* __restrict__ pot, int32_t* err)
+{
+  __shared__ double2 s_red[NW - 1][32];
+  double Jb[ZMAX], Yb[ZMAX];
+  double2 Zt[2 * 21 + 1];
+  int chunk = blockIdx.x;
+  int r = blockIdx.y;
+  int itb = g.nonqbx_chunk_target_box[chunk];
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int t = g.nonqbx_chunk_start[chunk] + lane;
+  bool active = lane < g.nonqbx_chunk_count[chunk];
+  double x[2] = {0, 0};
+  if (active) load_point<2>(g.nonqbx_targets, g.nfiltered_targets, t, x);
+  double2 acc = c2(0.0);
+  int l0, l1;
+  if (LOCAL) {
+    l0 = 0;
+    l1 = 1;
+  } else {
+    l0 = g.list3_starts[itb];
+    l1 = g.list3_starts[itb + 1];
+  }
+  for (int li = l0 + warp; li < l1 && active; li += NW) {
+    int sb = LOCAL ? g.target_boxes[itb] : g.list3_lists[li];
+    if ((unsigned)sb >= (unsigned)g.nboxes) {
+      report(err, QBX_DEVERR_BAD_BOX);
+      continue;
+    }
+    double rho = level_width(g, g.box_levels[sb]);
+    double cs[2];
+    load_point<2>(g.box_centers, g.nboxes, sb, cs);
+    h2_zfun(p, hc.k, x[0] - cs[0], x[1] - cs[1], Jb, Yb, Zt, !LOCAL);
+    const double2* E = exps + ((size_t)sb * nrhs + r) * (2 * p + 1);
+    double f = 1.0, finv = 1.0, rinv = 1.0 / rho;
+    for (int am = 0; am <= p; ++am) {
+      double sc = LOCAL ? finv : f;
+      acc = cfma(cscale(sc, E[p + am]), Zt[p + am], acc);
+      if (am > 0) acc = cfma(cscale(sc, E[p - am]), Zt[p - am], acc);
+      f *= rho;
+      finv *= rinv;
+    }
+  }
+  __syncthreads();
+  if (warp > 0) s_red[warp - 1][lane] = acc;
+  __syncthreads();
+  if (warp == 0 && active) {
+    for (int w = 1; w < NW; ++w) acc = cadd(acc, s_red[w - 1][lane]);
+    double2* P = pot + (size_t)r * g.nfiltered_targets + t;
+    *P = cadd(*P, acc);
+  }
+}
+
+// }}}
+
+// {{{ QBX stages
+
+// P2QBXL: lanes = centers of a chunk, warps split the list-1 source tiles; the
+// Hankel table of each (center, source) pair is built in registers (orders
+// 0..Q+1 by Miller's recurrence, downward part unrolled).
+template <int Q>
+__global__ void __launch_bounds__(NT)
+k_h2_p2qbxl(qbxfmm_geometry g, HelmCoeffs hc, int nrhs, const double2* __restrict__ strengths,
+            double2* __restrict__ qbx_exps, int32_t* err)
+{
+  constexpr int NC = 2 * Q + 1;
+  constexpr int N = Q + 1;
+  __shared__ double s_y[2][NT];
+  __shared__ double2 s_q[NT], s_a[NT], s_b[NT];
+  __shared__ int s_pref[MAXB + 1], s_start[MAXB];
+  extern __shared__ double2 s_red[];   // [NW-1][32][NC]
+  int chunk = blockIdx.x;
+  int r = blockIdx.y;
+  int itb = g.qbx_chunk_target_box[chunk];
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  bool has_center = lane < g.qbx_chunk_count[chunk];
+  int ctr = has_center ? g.centers_by_target_box[g.qbx_chunk_start[chunk] + lane] : 0;
+  if ((unsigned)ctr >= (unsigned)g.ncenters) {
+    report(err, QBX_DEVERR_BAD_CENTER);
+    has_center = false;
+    ctr = 0;
+  }
+  double cc[2];
+  load_point<2>(g.centers, g.ncenters, ctr, cc);
+  double rho = g.expansion_radii[ctr];
+  const double2* st = strengths + (size_t)r * g.nsources;
+  const bool dip = hc.cd.x != 0.0 || hc.cd.y != 0.0;
+  double2 acc[NC];
+#pragma unroll
+  for (int i = 0; i < NC; ++i) acc[i] = c2(0.0);
+  int l0 = g.list1_starts[itb], l1 = g.list1_starts[itb + 1];
+  for (int gb = l0; gb < l1; gb += MAXB) {
+    int nb = min(MAXB, l1 - gb);
+    __syncthreads();
+    h_list_prefix(g, g.list1_lists, gb, nb, s_pref, s_start, err);
+    __syncthreads();
+    int total = s_pref[nb];
+    for (int base = 0; base < total; base += NT) {
+      int v = base + threadIdx.x;
+      if (v < total) {
+        int s = h_stream_source(v, nb, s_pref, s_start);
+        double y[2], nv[2] = {0, 0};
+        load_point<2>(g.sources, g.nsources, s, y);
+        if (dip) load_point<2>(g.source_normals, g.nsources, s, nv);
+        s_y[0][threadIdx.x] = y[0];
+        s_y[1][threadIdx.x] = y[1];
+        double2 q, a, b;
+        source_factors(hc, st[s], nv[0], nv[1], dip, q, a, b);
+        s_q[threadIdx.x] = q;
+        s_a[threadIdx.x] = a;
+        s_b[threadIdx.x] = b;
+      }
+      __syncthreads();
+      int jbeg = warp * 32, jend = min(jbeg + 32, total - base);
+      if (has_center) {
+        for (int j = jbeg; j < jend; ++j) {
+          double ux = s_y[0][j] - cc[0], uy = s_y[1][j] - cc[1];
+          double r2 = ux * ux + uy * uy;
+          double rr = sqrt(r2);
+          double x = hc.k * rr, xinv = 1.0 / x;
+          // Miller: downward from an even start to N+1 (runtime), then unrolled to 0
+          int nmax = N > (int)x ? N : (int)x;
+          int start = 2 * ((nmax + 16 + (int)sqrt(40.0 * nmax)) / 2);
+          double fp1 = 0.0, f = 1e-200, sum = 0.0;
+          for (int k = start; k > N + 1; --k) {
+            double fm1 = 2.0 * k * xinv * f - fp1;
+            fp1 = f;
+            f = fm1;
+            if (((k - 1) & 1) == 0) sum += 2.0 * f;
+            if (fabs(f) > 1e200) {
+              f *= 1e-200;
+              fp1 *= 1e-200;
+              sum *= 1e-200;
+            }
+          }
+          double J[N + 1];
+          // f = f_{N+1}, fp1 = f_{N+2}
+#pragma unroll
+          for (int k = N + 1; k > 0; --k) {
+            double fm1 = 2.0 * k * xinv * f - fp1;
+            fp1 = f;
+            f = fm1;
+            J[k - 1] = f;
+            if (((k - 1) & 1) == 0 && k - 1 > 0) sum += 2.0 * f;
+          }
+          sum += f;
+          double norm = 1.0 / sum;
+          double Y[N + 1];
+          Y[0] = y0(x);
+          Y[1] = y1(x);
+#pragma unroll
+          for (int k = 1; k < N; ++k) Y[k + 1] = 2.0 * k * xinv * Y[k] - Y[k - 1];
+          // Hb_m = H_m(kr) e^{-i m th} for m >= 0; Hb_{-m} = (-1)^m H_m(kr) e^{i m th}
+          double2 e1 = c2(ux / rr, -uy / rr);   // e^{-i th}
+          double2 e = c2(1.0);
+          double2 hp[N + 1], hm[N + 1];
+#pragma unroll
+          for (int m = 0; m <= N; ++m) {
+            double2 h = c2(J[m] * norm, Y[m]);
+            hp[m] = cmul(h, e);                       // Hb_m
+            double2 w = cmul(h, cconj(e));
+            hm[m] = (m & 1) ? cneg(w) : w;            // Hb_{-m}
+            e = cmul(e, e1);
+          }
+          double2 q = s_q[j], a = s_a[j], b = s_b[j];
+#pragma unroll
+          for (int m = -Q; m <= Q; ++m) {
+            double2 h0 = m >= 0 ? hp[m] : hm[-m];
+            double2 hl = (m - 1) >= 0 ? hp[m - 1] : hm[1 - m];
+            double2 hr = (m + 1) >= 0 ? hp[m + 1] : hm[-m - 1];
+            double2 v = cmul(q, h0);
+            if (dip) {
+              v = cfma(a, hl, v);
+              v = cfma(cneg(b), hr, v);
+            }
+            acc[m + Q] = cadd(acc[m + Q], v);
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  if (warp > 0) {
+#pragma unroll
+    for (int i = 0; i < NC; ++i) s_red[((warp - 1) * 32 + lane) * NC + i] = acc[i];
+  }
+  __syncthreads();
+  if (warp == 0 && has_center) {
+    double2* out = qbx_exps + ((size_t)ctr * nrhs + r) * NC;
+    double f = 1.0;
+#pragma unroll
+    for (int am = 0; am <= Q; ++am) {
+      double2 ap = acc[Q + am], an = acc[Q - am];
+      for (int w = 1; w < NW; ++w) {
+        ap = cadd(ap, s_red[((w - 1) * 32 + lane) * NC + Q + am]);
+        if (am > 0) an = cadd(an, s_red[((w - 1) * 32 + lane) * NC + Q - am]);
+      }
+      out[Q + am] = caxpy(f, ap, out[Q + am]);
+      if (am > 0) out[Q - am] = caxpy(f, an, out[Q - am]);
+      f *= rho;
+    }
+  }
+}
+
+// M2QBXL (list 3) and L2QBXL (own target box): one thread per center.
+template <int Q, bool FROM_LOCAL>
+__global__ void __launch_bounds__(NT)
+k_h2_e2qbxl(qbxfmm_geometry g, HelmCoeffs hc, int pf, int nrhs, const double2* __restrict__ exps,
+            double2* __restrict__ qbx_exps, int32_t* err)
+{
+  constexpr int NC = 2 * Q + 1;
+  double Jb[ZMAX], Yb[ZMAX];
+  double2 Z[2 * (20 + 8) + 1];
+  int ig = blockIdx.x * blockDim.x + threadIdx.x;
+  int r = blockIdx.y;
+  if (ig >= g.nglobal_qbx_centers) return;
+  int ctr = g.global_qbx_centers[ig];
+  int itb = g.qbx_center_to_target_box[ctr];
+  double cc[2];
+  load_point<2>(g.centers, g.ncenters, ctr, cc);
+  double rho_t = g.expansion_radii[ctr];
+  int NZ = pf + Q;
+  double2 acc[NC];
+#pragma unroll
+  for (int i = 0; i < NC; ++i) acc[i] = c2(0.0);
+  int l0 = FROM_LOCAL ? 0 : g.list3_starts[itb];
+  int l1 = FROM_LOCAL ? 1 : g.list3_starts[itb + 1];
+  for (int li = l0; li < l1; ++li) {
+    int sb = FROM_LOCAL ? g.target_boxes[itb] : g.list3_lists[li];
+    if ((unsigned)sb >= (unsigned)g.nboxes) {
+      report(err, QBX_DEVERR_BAD_BOX);
+      continue;
+    }
+    double rho_s = level_width(g, g.box_levels[sb]);
+    double cs[2];
+    load_point<2>(g.box_centers, g.nboxes, sb, cs);
+    h2_zfun(NZ, hc.k, cc[0] - cs[0], cc[1] - cs[1], Jb, Yb, Z, !FROM_LOCAL);
+    const double2* E = exps + ((size_t)sb * nrhs + r) * (2 * pf + 1);
+    double fn = 1.0, rfac = FROM_LOCAL ? 1.0 / rho_s : rho_s;
+    for (int an = 0; an <= pf; ++an) {
+      double2 ep = cscale(fn, E[pf + an]);
+      double2 en = cscale(fn, E[pf - an]);
+#pragma unroll
+      for (int m = -Q; m <= Q; ++m) {
+        acc[m + Q] = cfma(ep, Z[NZ + an - m], acc[m + Q]);
+        if (an > 0) acc[m + Q] = cfma(en, Z[NZ - an - m], acc[m + Q]);
+      }
+      fn *= rfac;
+    }
+  }
+  double2* out = qbx_exps + ((size_t)ctr * nrhs + r) * NC;
+  double f = 1.0;
+#pragma unroll
+  for (int am = 0; am <= Q; ++am) {
+    out[Q + am] = caxpy(f, acc[Q + am], out[Q + am]);
+    if (am > 0) out[Q - am] = caxpy(f, acc[Q - am], out[Q - am]);
+    f *= rho_t;
+  }
+}
+
+template <int Q>
+__global__ void __launch_bounds__(NT)
+k_h2_qbxl2p(qbxfmm_geometry g, HelmCoeffs hc, int nrhs, const double2* __restrict__ qbx_exps,
+            double2* __restrict__ pot_tree)
+{
+  constexpr int NC = 2 * Q + 1;
+  double Jb[Q + 2], Yb[Q + 2];
+  double2 Z[2 * Q + 1];
+  int ig = blockIdx.x * blockDim.x + threadIdx.x;
+  int r = blockIdx.y;
+  if (ig >= g.nglobal_qbx_centers) return;
+  int ctr = g.global_qbx_centers[ig];
+  double cc[2];
+  load_point<2>(g.centers, g.ncenters, ctr, cc);
+  double rinv = 1.0 / g.expansion_radii[ctr];
+  const double2* L = qbx_exps + ((size_t)ctr * nrhs + r) * NC;
+  for (int it = g.center_to_targets_starts[ctr]; it < g.center_to_targets_starts[ctr + 1]; ++it) {
+    int t = g.center_to_targets_lists[it];
+    double x[2];
+    load_point<2>(g.targets, g.ntargets, t, x);
+    double2 acc = c2(0.0);
+    double ux = x[0] - cc[0], uy = x[1] - cc[1];
+    if (ux * ux + uy * uy == 0.0) {
+      acc = L[Q];   // J_0(0) = 1, J_m(0) = 0
+    } else {
+      h2_zfun(Q, hc.k, ux, uy, Jb, Yb, Z, false);
+      double f = 1.0;
+#pragma unroll
+      for (int am = 0; am <= Q; ++am) {
+        acc = cfma(cscale(f, L[Q + am]), Z[Q + am], acc);
+        if (am > 0) acc = cfma(cscale(f, L[Q - am]), Z[Q - am], acc);
+        f *= rinv;
+      }
+    }
+    pot_tree[(size_t)r * g.ntargets + t] = acc;
+  }
+}
+
+// }}}
+
+// {{{ assembly
+
+__global__ void k_h2_assemble_tree(qbxfmm_geometry g, int nrhs, const double2* __restrict__ pot_tree,
+                                   double2* __restrict__ out)
+{
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  int r = blockIdx.y;
+  if (t >= g.ntargets) return;
+  int u = g.sorted_target_ids[t] - g.ncenters;
+  double2 v = pot_tree[(size_t)r * g.ntargets + t];
+  if (u >= 0) out[(size_t)r * g.nuser_targets + u] = c2(-0.25 * v.y, 0.25 * v.x);   // (i/4) v
+}
+
+__global__ void k_h2_assemble_nonqbx(qbxfmm_geometry g, int nrhs,
+                                     const double2* __restrict__ pot_nonqbx, double2* __restrict__ out)
+{
+  int f = blockIdx.x * blockDim.x + threadIdx.x;
+  int r = blockIdx.y;
+  if (f >= g.nfiltered_targets) return;
+  int t = g.unfiltered_from_filtered_target_indices[f];
+  int u = g.sorted_target_ids[t] - g.ncenters;
+  double2 v = pot_nonqbx[(size_t)r * g.nfiltered_targets + f];
+  if (u >= 0) {
+    double2* o = out + (size_t)r * g.nuser_targets + u;
+    *o = cadd(*o, c2(-0.25 * v.y, 0.25 * v.x));
+  }
+}
+
+// }}}
+
+// {{{ launchers
+
+static size_t zsh(int p) { return (size_t)(2 * (p + 1) + 1); }
+
+cudaError_t h2_launch_form_strengths(const qbxfmm_geometry& g, const qbxfmm_upsample& up, int nrhs,
+                                     const double2* density, double2* strengths, cudaStream_t st)
+{
+  dim3 grid((g.nsources + 255) / 256, nrhs);
+  k_h2_form_strengths<<<grid, 256, 0, st>>>(g.nsources, up.nelements * up.nodes_per_element,
+                                            up.nodes_per_element, up.quad_nodes_per_element,
+                                            up.matrix, up.quad_weights, g.user_source_ids, density,
+                                            strengths);
+  return cudaGetLastError();
+}
+
+cudaError_t h2_launch_p2m(const qbxfmm_geometry& g, HelmCoeffs hc, int p, int nrhs,
+                          const double2* s, double2* mp, int32_t* err, cudaStream_t st)
+{
+  if (g.nsource_boxes == 0) return cudaSuccess;
+  size_t sh = 32 * zsh(p) * sizeof(double2);
+  k_h2_p2e<false><<<dim3(g.nsource_boxes, nrhs), NT, sh, st>>>(g, hc, p, nrhs, s, mp, err);
+  return cudaGetLastError();
+}
+
+cudaError_t h2_launch_p2l(const qbxfmm_geometry& g, HelmCoeffs hc, int p, int nrhs,
+                          const double2* s, double2* lo, int32_t* err, cudaStream_t st)
+{
+  if (g.nttp_boxes == 0) return cudaSuccess;
+  size_t sh = 32 * zsh(p) * sizeof(double2);
+  k_h2_p2e<true><<<dim3(g.nttp_boxes, nrhs), NT, sh, st>>>(g, hc, p, nrhs, s, lo, err);
+  return cudaGetLastError();
+}
+
+static size_t trans_sh(int p) { return (16 * (size_t)(4 * p + 1) + 16 * (size_t)(2 * p + 1)) * sizeof(double2); }
+
+cudaError_t h2_launch_m2m(const qbxfmm_geometry& g, const int32_t* lvl_host, HelmCoeffs hc, int p,
+                          int nrhs, double2* mp, int32_t* err, cudaStream_t st)
+{
+  size_t sh = trans_sh(p);
+  cudaFuncSetAttribute(k_h2_translate<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+  for (int lev = g.nlevels - 2; lev >= 0; --lev) {
+    int i0 = lvl_host[lev], i1 = lvl_host[lev + 1];
+    if (i1 <= i0) continue;
+    k_h2_translate<0><<<dim3(i1 - i0, nrhs), NT, sh, st>>>(g, hc, p, nrhs, i0, mp, mp, err);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+cudaError_t h2_launch_m2l(const qbxfmm_geometry& g, HelmCoeffs hc, int p, int nrhs,
+                          const double2* mp, double2* lo, int32_t* err, cudaStream_t st)
+{
+  if (g.nttp_boxes == 0) return cudaSuccess;
+  size_t sh = trans_sh(p);
+  cudaFuncSetAttribute(k_h2_translate<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+  k_h2_translate<1><<<dim3(g.nttp_boxes, nrhs), NT, sh, st>>>(g, hc, p, nrhs, 0, mp, lo, err);
+  return cudaGetLastError();
+}
+
+cudaError_t h2_launch_l2l(const qbxfmm_geometry& g, const int32_t* lvl_host, HelmCoeffs hc, int p,
+                          int nrhs, double2* lo, int32_t* err, cudaStream_t st)
+{
+  size_t sh = trans_sh(p);
+  cudaFuncSetAttribute(k_h2_translate<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+  for (int lev = 1; lev < g.nlevels; ++lev) {
+    int i0 = lvl_host[lev], i1 = lvl_host[lev + 1];
+    if (i1 <= i0) continue;
+    k_h2_translate<2><<<dim3(i1 - i0, nrhs), NT, sh, st>>>(g, hc, p, nrhs, i0, lo, lo, err);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+cudaError_t h2_launch_eval_direct(const qbxfmm_geometry& g, HelmCoeffs hc, int nrhs,
+                                  const double2* s, double2* pot, int32_t* err, cudaStream_t st)
+{
+  if (g.nnonqbx_chunks == 0) return cudaSuccess;
+  k_h2_eval_direct<<<dim3(g.nnonqbx_chunks, nrhs), NT, 0, st>>>(g, hc, nrhs, s, pot, err);
+  return cudaGetLastError();
+}
+
+cudaError_t h2_launch_eval_multipoles(const qbxfmm_geometry& g, HelmCoeffs hc, int p, int nrhs,
+                                      const double2* mp, double2* pot, int32_t* err, cudaStream_t st)
+{
+  if (g.nnonqbx_chunks == 0) return cudaSuccess;
+  k_h2_eval_exp<false><<<dim3(g.nnonqbx_chunks, nrhs), NT, 0, st>>>(g, hc, p, nrhs, mp, pot, err);
+  return cudaGetLastError();
+}
+
+cudaError_t h2_launch_eval_locals(const qbxfmm_geometry& g, HelmCoeffs hc, int p, int nrhs,
+                                  const double2* lo, double2* pot, int32_t* err, cudaStream_t st)
+{
+  if (g.nnonqbx_chunks == 0) return cudaSuccess;
+  k_h2_eval_exp<true><<<dim3(g.nnonqbx_chunks, nrhs), NT, 0, st>>>(g, hc, p, nrhs, lo, pot, err);
+  return cudaGetLastError();
+}
+
+template <int Q>
+static cudaError_t h2_p2qbxl_q(const qbxfmm_geometry& g, HelmCoeffs hc, int nrhs, const double2* s,
+                               double2* qe, int32_t* err, cudaStream_t st)
+{
+  size_t sh = (size_t)(NW - 1) * 32 * (2 * Q + 1) * sizeof(double2);
+  k_h2_p2qbxl<Q><<<dim3(g.nqbx_chunks, nrhs), NT, sh, st>>>(g, hc, nrhs, s, qe, err);
+  return cudaGetLastError();
+}
+
+template <int Q>
+static cudaError_t h2_e2qbxl_q(const qbxfmm_geometry& g, HelmCoeffs hc, int pf, int nrhs,
+                               const double2* e, double2* qe, int32_t* err, bool from_local,
+                               cudaStream_t st)
+{
+  dim3 grid((g.nglobal_qbx_centers + NT - 1) / NT, nrhs);
+  if (from_local) k_h2_e2qbxl<Q, true><<<grid, NT, 0, st>>>(g, hc, pf, nrhs, e, qe, err);
+  else k_h2_e2qbxl<Q, false><<<grid, NT, 0, st>>>(g, hc, pf, nrhs, e, qe, err);
+  return cudaGetLastError();
+}
+
+template <int Q>
+static cudaError_t h2_qbxl2p_q(const qbxfmm_geometry& g, HelmCoeffs hc, int nrhs, const double2* qe,
+                               double2* pt, cudaStream_t st)
+{
+  dim3 grid((g.nglobal_qbx_centers + NT - 1) / NT, nrhs);
+  k_h2_qbxl2p<Q><<<grid, NT, 0, st>>>(g, hc, nrhs, qe, pt);
+  return cudaGetLastError();
+}
+
+#define QBX_H2_DISPATCH(FN, Q, ...)                                  \
+  switch (Q) {                                                       \
+    case 0: return FN<0>(__VA_ARGS__);                               \
+    case 1: return FN<1>(__VA_ARGS__);                               \
+    case 2: return FN<2>(__VA_ARGS__);                               \
+    case 3: return FN<3>(__VA_ARGS__);                               \
+    case 4: return FN<4>(__VA_ARGS__);                               \
+    case 5: return FN<5>(__VA_ARGS__);                               \
+    case 6: return FN<6>(__VA_ARGS__);                               \
+    case 7: return FN<7>(__VA_ARGS__);                               \
+    case 8: return FN<8>(__VA_ARGS__);                               \
+    default: return cudaErrorInvalidValue;                           \
+  }
+
+cudaError_t h2_launch_p2qbxl(const qbxfmm_geometry& g, HelmCoeffs hc, int q, int nrhs,
+                             const double2* s, double2* qe, int32_t* err, cudaStream_t st)
+{
+  if (g.nqbx_chunks == 0) return cudaSuccess;
+  QBX_H2_DISPATCH(h2_p2qbxl_q, q, g, hc, nrhs, s, qe, err, st)
+}
+
+cudaError_t h2_launch_m2qbxl(const qbxfmm_geometry& g, HelmCoeffs hc, int pf, int q, int nrhs,
+                             const double2* mp, double2* qe, int32_t* err, cudaStream_t st)
+{
+  if (g.nglobal_qbx_centers == 0) return cudaSuccess;
+  QBX_H2_DISPATCH(h2_e2qbxl_q, q, g, hc, pf, nrhs, mp, qe, err, false, st)
+}
+
+cudaError_t h2_launch_l2qbxl(const qbxfmm_geometry& g, HelmCoeffs hc, int pf, int q, int nrhs,
+                             const double2* lo, double2* qe, int32_t* err, cudaStream_t st)
+{
+  if (g.nglobal_qbx_centers == 0) return cudaSuccess;
+  QBX_H2_DISPATCH(h2_e2qbxl_q, q, g, hc, pf, nrhs, lo, qe, err, true, st)
+}
+
+cudaError_t h2_launch_qbxl2p(const qbxfmm_geometry& g, HelmCoeffs hc, int q, int nrhs,
+                             const double2* qe, double2* pt, cudaStream_t st)
+{
+  if (g.nglobal_qbx_centers == 0) return cudaSuccess;
+  QBX_H2_DISPATCH(h2_qbxl2p_q, q, g, hc, nrhs, qe, pt, st)
+}
+
+cudaError_t h2_launch_assemble(const qbxfmm_geometry& g, int nrhs, const double2* pot_nonqbx,
+                               const double2* pot_tree, double2* out, cudaStream_t st)
+{
+  if (g.ntargets > 0) {
+    k_h2_assemble_tree<<<dim3((g.ntargets + 255) / 256, nrhs), 256, 0, st>>>(g, nrhs, pot_tree, out);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  if (g.nfiltered_targets > 0)
+    k_h2_assemble_nonqbx<<<dim3((g.nfiltered_targets + 255) / 256, nrhs), 256, 0, st>>>(
+        g, nrhs, pot_nonqbx, out);
+  return cudaGetLastError();
+}
+
+// }}}
+
+}  // namespace qbx

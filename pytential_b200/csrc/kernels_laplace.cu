@@ -148,6 +148,7 @@ k_p2m(qbxfmm_geometry g, SourceCoeffs sc, int p, int ncf, int nrhs,
   int b = g.source_boxes[blockIdx.x];
   int r = blockIdx.y;
   double rho = level_width(g, g.box_levels[b]);
+  double rinv = 1.0 / rho;
   double c[3];
   load_point<DIM>(g.box_centers, g.nboxes, b, c);
   int s0 = g.box_source_starts[b];
@@ -162,7 +163,7 @@ k_p2m(qbxfmm_geometry g, SourceCoeffs sc, int p, int ncf, int nrhs,
       double y[3];
       load_point<DIM>(g.sources, g.nsources, s, y);
 #pragma unroll
-      for (int d = 0; d < DIM; ++d) s_u[threadIdx.x][d] = (y[d] - c[d]) / rho;
+      for (int d = 0; d < DIM; ++d) s_u[threadIdx.x][d] = (y[d] - c[d]) * rinv;
       if (sc.cd != 0.0) {
         double nv[3];
         load_point<DIM>(g.source_normals, g.nsources, s, nv);
@@ -179,12 +180,12 @@ k_p2m(qbxfmm_geometry g, SourceCoeffs sc, int p, int ncf, int nrhs,
         double x = s_u[j][0], y = s_u[j][1], z = s_u[j][2];
         double r2 = x * x + y * y + z * z;
         double2 a = c2(1.0);
-        for (int k = 1; k <= m; ++k) a = cscale(1.0 / (2 * k), cmul(a, c2(x, y)));
+        for (int k = 1; k <= m; ++k) a = cscale(0.5 * rcp(k), cmul(a, c2(x, y)));
         double2* T = tab + (size_t)j * ncf;
         T[idx3(m, m)] = a;
         double2 prev = c2(0.0);
         for (int n = m + 1; n <= p; ++n) {
-          double2 bb = cscale(1.0 / ((double)(n + m) * (n - m)),
+          double2 bb = cscale(rcp(n + m) * rcp(n - m),
                               csub(cscale((2.0 * n - 1) * z, a), cscale(r2, prev)));
           T[idx3(n, m)] = bb;
           prev = a;
@@ -216,7 +217,7 @@ k_p2m(qbxfmm_geometry g, SourceCoeffs sc, int p, int ncf, int nrhs,
           double q = s_q[j];
           a = caxpy(sc.cq * q, cconj(T[idx3(n, m)]), a);
           if (sc.cd != 0.0 && n >= 1) {
-            double f = sc.cd * q / rho;
+            double f = sc.cd * q * rinv;
             double dx = s_n[j][0], dy = s_n[j][1], dz = s_n[j][2];
             // conj(dz R_{n-1}^m + (dx+idy)/2 R_{n-1}^{m-1} - (dx-idy)/2 R_{n-1}^{m+1})
             double2 v = cscale(dz, sh3_get(T, n - 1, m));
@@ -233,10 +234,10 @@ k_p2m(qbxfmm_geometry g, SourceCoeffs sc, int p, int ncf, int nrhs,
           if (k == 0) {
             a.x += sc.cq * q;
           } else {
-            a = caxpy(-sc.cq * q / k, T[k], a);
+            a = caxpy(-sc.cq * q * rcp(k), T[k], a);
             if (sc.cd != 0.0) {
               double2 nu = c2(s_n[j][0], s_n[j][1]);
-              a = cfma(cscale(-sc.cd * q / rho, nu), T[k - 1], a);
+              a = cfma(cscale(-sc.cd * q * rinv, nu), T[k - 1], a);
             }
           }
         }
@@ -312,12 +313,12 @@ k_m2m(qbxfmm_geometry g, int p, int ncf, int nrhs, int i0, double2* __restrict__
         if (l == 0) {
           a = cadd(a, Min[0]);
         } else {
-          a = cfma(cscale(-1.0 / l, Min[0]), tab[l], a);
+          a = cfma(cscale(-rcp(l), Min[0]), tab[l], a);
           double rk = ratio, bin = 1.0;  // C(l-1, k-1)
           for (int k = 1; k <= l; ++k) {
             a = cfma(cscale(rk * bin, Min[k]), tab[l - k], a);
             rk *= ratio;
-            bin = bin * (l - k) / k;
+            bin = bin * (l - k) * rcp(k);
           }
         }
       }
@@ -519,9 +520,9 @@ k_m2l2(qbxfmm_geometry g, int p, int ncf, int nrhs, const double2* __restrict__ 
         double bin = 1.0;  // C(k+l-1, l) at k = 1
         for (int k = 1; k <= p; ++k) {
           s = cfma(cscale(bin, Min[k]), tab[k], s);
-          bin = bin * (k + l) / k;
+          bin = bin * (k + l) * rcp(k);
         }
-        double2 v = cscale(((l & 1) ? 1.0 : -1.0) / l, Min[0]);
+        double2 v = cscale(((l & 1) ? 1.0 : -1.0) * rcp(l), Min[0]);
         v = cadd(v, cscale((l & 1) ? -1.0 : 1.0, s));
         acc = cfma(v, tab[l], acc);
       }
@@ -557,6 +558,7 @@ k_p2l(qbxfmm_geometry g, SourceCoeffs sc, int p, int ncf, int nrhs,
   int tb = g.target_or_target_parent_boxes[i];
   int r = blockIdx.y;
   double rho = level_width(g, g.box_levels[tb]);
+  double rinv = 1.0 / rho;
   double c[3];
   load_point<DIM>(g.box_centers, g.nboxes, tb, c);
   const double* st = strengths + (size_t)r * g.nsources;
@@ -599,7 +601,7 @@ k_p2l(qbxfmm_geometry g, SourceCoeffs sc, int p, int ncf, int nrhs,
         double y[3];
         load_point<DIM>(g.sources, g.nsources, s, y);
 #pragma unroll
-        for (int d = 0; d < DIM; ++d) s_u[threadIdx.x][d] = (y[d] - c[d]) / rho;
+        for (int d = 0; d < DIM; ++d) s_u[threadIdx.x][d] = (y[d] - c[d]) * rinv;
         if (dip) {
           double nv[3];
           load_point<DIM>(g.source_normals, g.nsources, s, nv);
@@ -649,9 +651,9 @@ k_p2l(qbxfmm_geometry g, SourceCoeffs sc, int p, int ncf, int nrhs,
           const double2* T = tab + (size_t)j * nct;
           double q = s_q[j];
           if (DIM == 3) {
-            a = caxpy(sc.cq * q / rho, T[o_nm[h]], a);
+            a = caxpy(sc.cq * q * rinv, T[o_nm[h]], a);
             if (dip) {
-              double f = sc.cd * q / (rho * rho);
+              double f = sc.cd * q * rinv * rinv;
               double dx = s_n[j][0], dy = s_n[j][1], dz = s_n[j][2];
               double2 tb_ = T[o_b[h]];
               if (sb_sign[h] < 0) tb_ = c2(-tb_.x, tb_.y);
@@ -663,10 +665,10 @@ k_p2l(qbxfmm_geometry g, SourceCoeffs sc, int p, int ncf, int nrhs,
           } else {
             int l = ci;
             if (l == 0) a.x += sc.cq * q * T[p + 2].x;
-            else a = caxpy(-sc.cq * q / l, T[l], a);
+            else a = caxpy(-sc.cq * q * rcp(l), T[l], a);
             if (dip) {
               double2 nu = c2(s_n[j][0], s_n[j][1]);
-              a = cfma(cscale(sc.cd * q / rho, nu), T[l + 1], a);
+              a = cfma(cscale(sc.cd * q * rinv, nu), T[l + 1], a);
             }
           }
         }
@@ -735,7 +737,7 @@ k_l2l(qbxfmm_geometry g, int p, int ncf, int nrhs, int i0, double2* __restrict__
       double bin = 1.0;  // C(k, l)
       for (int k = l; k <= p; ++k) {
         a = cfma(cscale(bin, Lin[k]), tab[k - l], a);
-        bin = bin * (k + 1) / (k + 1 - l);
+        bin = bin * (k + 1) * rcp(k + 1 - l);
       }
       a = cscale(pow(ratio, (double)l), a);
     }
@@ -797,7 +799,10 @@ k_eval_direct(qbxfmm_geometry g, SourceCoeffs sc, int nrhs, const double* __rest
             acc = fma(q, v, acc);
           } else {
             double v = 0.5 * sc.cq * log(r2);
-            if (dip) v -= sc.cd * (s_n[0][j] * dx + s_n[1][j] * dy) / r2;
+            if (dip) {
+              double ri = rsqrt(r2);
+              v -= sc.cd * (s_n[0][j] * dx + s_n[1][j] * dy) * ri * ri;
+            }
             acc = fma(q, v, acc);
           }
         }
@@ -920,12 +925,12 @@ k_eval_locals(qbxfmm_geometry g, int p, int ncf, int nrhs, const double2* __rest
       double r2 = u0 * u0 + u1 * u1 + u2 * u2;
       double2 mm = c2(1.0);
       for (int m = 0; m <= p; ++m) {
-        if (m > 0) mm = cscale(1.0 / (2 * m), cmul(mm, c2(u0, u1)));
+        if (m > 0) mm = cscale(0.5 * rcp(m), cmul(mm, c2(u0, u1)));
         double w = (m == 0) ? 1.0 : 2.0;
         double2 a = mm, prev = c2(0.0);
         for (int n = m; n <= p; ++n) {
           if (n > m) {
-            double2 bb = cscale(1.0 / ((double)(n + m) * (n - m)),
+            double2 bb = cscale(rcp(n + m) * rcp(n - m),
                                 csub(cscale((2.0 * n - 1) * u2, a), cscale(r2, prev)));
             prev = a;
             a = bb;
@@ -1041,7 +1046,7 @@ k_p2qbxl(qbxfmm_geometry g, SourceCoeffs sc, int nrhs, const double* __restrict_
 #pragma unroll
             for (int l = 0; l <= Q; ++l) {
               if (l > 0) {
-                if (CHG) acc[l] = caxpy(-sc.cq * q / l, pw, acc[l]);
+                if (CHG) acc[l] = caxpy(-sc.cq * q * rcp(l), pw, acc[l]);
                 pw = cmul(pw, tinv);
               }
               if (DIP) acc[l] = cfma(fnu, pw, acc[l]);   // pw = tau^-(l+1)
@@ -1204,7 +1209,7 @@ k_m2qbxl(qbxfmm_geometry g, int pf, int ncf, int nrhs, const double2* __restrict
 #pragma unroll
         for (int l = 1; l <= Q; ++l) {
           sl[l] = caxpy(bin[l], mk, sl[l]);
-          bin[l] = bin[l] * (k + l) / k;
+          bin[l] = bin[l] * (k + l) * rcp(k);
         }
         pw = cmul(pw, tinv);
       }
@@ -1213,7 +1218,7 @@ k_m2qbxl(qbxfmm_geometry g, int pf, int ncf, int nrhs, const double2* __restrict
       double rl = ratio;
 #pragma unroll
       for (int l = 1; l <= Q; ++l) {
-        double2 v = cscale(((l & 1) ? 1.0 : -1.0) / l, M[0]);
+        double2 v = cscale(((l & 1) ? 1.0 : -1.0) * rcp(l), M[0]);
         v = cadd(v, cscale((l & 1) ? -1.0 : 1.0, sl[l]));
         acc[l] = cadd(acc[l], cscale(rl, cmul(v, tl)));
         tl = cmul(tl, tinv);
@@ -1235,6 +1240,139 @@ k_m2qbxl(qbxfmm_geometry g, int pf, int ncf, int nrhs, const double2* __restrict
       for (int w = 1; w < NW; ++w) a = cadd(a, red[((w - 1) * 32 + lane) * NC + i]);
       out[i] = cadd(out[i], a);
     }
+  }
+}
+
+// Target-specific near field (eval_target_specific_qbx_locals, fmm.py:391-394;
+// reference native code pytential/qbx/target_specific/impl.pyx:222-362, 566-785).
+// For a QBX target t with center c and a list-1 source s, a = t - c, b = s - c:
+//   3D: 1/|t-s| ~ sum_{n<=Q} |a|^n / |b|^{n+1} P_n(cos g),  cos g = a.b / (|a||b|),
+//       double layer d.grad_s = sum_n |a|^n/|b|^{n+2} [-(n+1)(d.b^) P_n + (d.a^ - cos g d.b^) P_n']
+//   2D: log|t-s| ~ log|b| - Re sum_{n=1..Q} (a/b)^n / n,
+//       double layer Re(nu / b sum_{n=0..Q} (a/b)^n)      (nu = n_x + i n_y)
+// the same truncation as forming the order-Q QBX local from the list-1 sources and
+// evaluating it at t.  CTA = 4 warps over a chunk of <= 32 (target, center) pairs of
+// one target box (lane = pair); warps split the list-1 source tiles.
+template <int DIM, int Q, bool CHG, bool DIP>
+__global__ void __launch_bounds__(NT)
+k_tsqbx(qbxfmm_geometry g, SourceCoeffs sc, int nrhs, const double* __restrict__ strengths,
+        double* __restrict__ pot_tree, int32_t* err)
+{
+  __shared__ double s_y[3][NT];
+  __shared__ double s_n[3][NT];
+  __shared__ double s_q[NT];
+  __shared__ int s_pref[MAXB + 1], s_start[MAXB];
+  __shared__ double s_red[NW - 1][32];
+  int chunk = blockIdx.x;
+  int r = blockIdx.y;
+  int itb = g.tsqbx_chunk_target_box[chunk];
+  int i0 = g.tsqbx_chunk_start[chunk];
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  bool active = lane < g.tsqbx_chunk_count[chunk];
+  int t = active ? g.tsqbx_targets[i0 + lane] : 0;
+  int ctr = active ? g.tsqbx_centers[i0 + lane] : 0;
+  if ((unsigned)ctr >= (unsigned)g.ncenters || (unsigned)t >= (unsigned)g.ntargets) {
+    report(err, QBX_DEVERR_BAD_CENTER);
+    active = false;
+    t = ctr = 0;
+  }
+  double cc[3] = {0, 0, 0}, x[3] = {0, 0, 0};
+  load_point<DIM>(g.centers, g.ncenters, ctr, cc);
+  load_point<DIM>(g.targets, g.ntargets, t, x);
+  double a[3] = {x[0] - cc[0], x[1] - cc[1], DIM == 3 ? x[2] - cc[2] : 0.0};
+  double alen = sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+  double ainv = alen > 0.0 ? 1.0 / alen : 0.0;
+  double ah[3] = {a[0] * ainv, a[1] * ainv, a[2] * ainv};
+  const double* st = strengths + (size_t)r * g.nsources;
+  double acc = 0.0;
+  int l0 = g.list1_starts[itb], l1 = g.list1_starts[itb + 1];
+  for (int gb = l0; gb < l1; gb += MAXB) {
+    int nb = min(MAXB, l1 - gb);
+    __syncthreads();
+    list_prefix(g, g.list1_lists, gb, nb, s_pref, s_start, err);
+    __syncthreads();
+    int total = s_pref[nb];
+    for (int base = 0; base < total; base += NT) {
+      load_stream_tile<DIM, DIP>(g, st, total, nb, base, s_pref, s_start, s_y, s_n, s_q);
+      __syncthreads();
+      int jbeg = warp * 32, jend = min(jbeg + 32, total - base);
+      if (active) {
+        for (int j = jbeg; j < jend; ++j) {
+          double q = s_q[j];
+          if (DIM == 3) {
+            double b0 = s_y[0][j] - cc[0], b1 = s_y[1][j] - cc[1], b2 = s_y[2][j] - cc[2];
+            double b2s = b0 * b0 + b1 * b1 + b2 * b2;
+            double binv = rsqrt(b2s);
+            double cg = (ah[0] * b0 + ah[1] * b1 + ah[2] * b2) * binv;   // cos g
+            double ratio = alen * binv;                                  // |a| / |b|
+            // Legendre P_n, P_n' by recurrence; R_n = ratio^n / |b|
+            double pm1 = 1.0, pm2 = 0.0, dm1 = 0.0, dm2 = 0.0;
+            double rn = binv;
+            double sS = 0.0, sA = 0.0, sB = 0.0;
+#pragma unroll
+            for (int n = 0; n <= Q; ++n) {
+              double pn, dn;
+              if (n == 0) {
+                pn = 1.0;
+                dn = 0.0;
+              } else if (n == 1) {
+                pn = cg;
+                dn = 1.0;
+              } else {
+                pn = ((2.0 * n - 1) * cg * pm1 - (n - 1.0) * pm2) * (1.0 / n);
+                dn = n * pm1 + cg * dm1;
+              }
+              if (CHG) sS = fma(rn, pn, sS);
+              if (DIP) {
+                sA = fma(-(n + 1.0) * rn, pn, sA);
+                sB = fma(rn, dn, sB);
+              }
+              pm2 = pm1;
+              pm1 = pn;
+              dm2 = dm1;
+              dm1 = dn;
+              rn *= ratio;
+            }
+            double v = 0.0;
+            if (CHG) v = sc.cq * sS;
+            if (DIP) {
+              double db = (s_n[0][j] * b0 + s_n[1][j] * b1 + s_n[2][j] * b2) * binv;
+              double da = s_n[0][j] * ah[0] + s_n[1][j] * ah[1] + s_n[2][j] * ah[2];
+              v += sc.cd * binv * (sA * db + sB * (da - cg * db));
+            }
+            acc = fma(q, v, acc);
+            (void)dm2;
+          } else {
+            double2 bb = c2(s_y[0][j] - cc[0], s_y[1][j] - cc[1]);
+            double2 binv = cinv(bb);
+            double2 w = cmul(c2(a[0], a[1]), binv);   // a / b
+            double2 pw = w;
+            double2 sl = c2(0.0);   // sum_{n>=1} w^n / n
+            double2 sd = c2(1.0);   // sum_{n>=0} w^n
+#pragma unroll
+            for (int n = 1; n <= Q; ++n) {
+              if (CHG) sl = caxpy(1.0 / n, pw, sl);
+              if (DIP) sd = cadd(sd, pw);
+              pw = cmul(pw, w);
+            }
+            double v = 0.0;
+            if (CHG) v = sc.cq * (0.5 * log(bb.x * bb.x + bb.y * bb.y) - sl.x);
+            if (DIP) {
+              double2 f = cmul(cmul(c2(s_n[0][j], s_n[1][j]), binv), sd);
+              v += sc.cd * f.x;
+            }
+            acc = fma(q, v, acc);
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  if (warp > 0) s_red[warp - 1][lane] = acc;
+  __syncthreads();
+  if (warp == 0 && active) {
+    for (int w = 1; w < NW; ++w) acc += s_red[w - 1][lane];
+    pot_tree[(size_t)r * g.ntargets + t] += acc;
   }
 }
 
@@ -1266,11 +1404,11 @@ k_l2qbxl(qbxfmm_geometry g, int pf, int ncf, int nrhs, const double2* __restrict
     double2 mm = c2(1.0);
     // R_a^b(d): output (k,l) += L_{a+k}^{b+l} conj(R_a^b)
     for (int bm = 0; bm <= pf; ++bm) {
-      if (bm > 0) mm = cscale(1.0 / (2 * bm), cmul(mm, c2(d0, d1)));
+      if (bm > 0) mm = cscale(0.5 * rcp(bm), cmul(mm, c2(d0, d1)));
       double2 a = mm, prev = c2(0.0);
       for (int an = bm; an <= pf; ++an) {
         if (an > bm) {
-          double2 bb = cscale(1.0 / ((double)(an + bm) * (an - bm)),
+          double2 bb = cscale(rcp(an + bm) * rcp(an - bm),
                               csub(cscale((2.0 * an - 1) * d2, a), cscale(r2, prev)));
           prev = a;
           a = bb;
@@ -1639,6 +1777,25 @@ cudaError_t launch_qbxl2p(const qbxfmm_geometry& g, int q, int nrhs, const doubl
   if (g.nglobal_qbx_centers == 0) return cudaSuccess;
   if (g.dim == 3) { QBX_DISPATCH_Q(qbxl2p_q, 3, q, g, nrhs, qe, pt, st) }
   QBX_DISPATCH_Q(qbxl2p_q, 2, q, g, nrhs, qe, pt, st)
+}
+
+template <int DIM, int Q>
+static cudaError_t tsqbx_q(const qbxfmm_geometry& g, SourceCoeffs sc, int nrhs, const double* s,
+                           double* pt, int32_t* err, cudaStream_t st)
+{
+  dim3 grid(g.ntsqbx_chunks, grid_y(nrhs));
+  if (sc.cq != 0.0 && sc.cd != 0.0) k_tsqbx<DIM, Q, true, true><<<grid, NT, 0, st>>>(g, sc, nrhs, s, pt, err);
+  else if (sc.cd != 0.0) k_tsqbx<DIM, Q, false, true><<<grid, NT, 0, st>>>(g, sc, nrhs, s, pt, err);
+  else k_tsqbx<DIM, Q, true, false><<<grid, NT, 0, st>>>(g, sc, nrhs, s, pt, err);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_tsqbx(const qbxfmm_geometry& g, SourceCoeffs sc, int q, int nrhs,
+                         const double* s, double* pt, int32_t* err, cudaStream_t st)
+{
+  if (g.ntsqbx_chunks == 0) return cudaSuccess;
+  if (g.dim == 3) { QBX_DISPATCH_Q(tsqbx_q, 3, q, g, sc, nrhs, s, pt, err, st) }
+  QBX_DISPATCH_Q(tsqbx_q, 2, q, g, sc, nrhs, s, pt, err, st)
 }
 
 cudaError_t launch_assemble(const qbxfmm_geometry& g, int nrhs, const double* pot_nonqbx,

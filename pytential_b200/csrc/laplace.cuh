@@ -22,10 +22,10 @@ QBX_D double2 sh3_R_nm(int n, int m, double x, double y, double z)
   if (n < 0 || am > n) return c2(0.0);
   double r2 = x * x + y * y + z * z;
   double2 a = c2(1.0);
-  for (int j = 1; j <= am; ++j) a = cscale(1.0 / (2 * j), cmul(a, c2(x, y)));
+  for (int j = 1; j <= am; ++j) a = cscale(0.5 * rcp(j), cmul(a, c2(x, y)));
   double2 prev = c2(0.0);
   for (int k = am + 1; k <= n; ++k) {
-    double2 b = cscale(1.0 / ((double)(k + am) * (k - am)),
+    double2 b = cscale(rcp(k + am) * rcp(k - am),
                        csub(cscale((2.0 * k - 1) * z, a), cscale(r2, prev)));
     prev = a;
     a = b;
@@ -68,11 +68,11 @@ QBX_D void sh3_R_table(int p, double x, double y, double z, double2* tab, int ti
   double r2 = x * x + y * y + z * z;
   for (int m = tid; m <= p; m += nt) {
     double2 a = c2(1.0);
-    for (int j = 1; j <= m; ++j) a = cscale(1.0 / (2 * j), cmul(a, c2(x, y)));
+    for (int j = 1; j <= m; ++j) a = cscale(0.5 * rcp(j), cmul(a, c2(x, y)));
     tab[idx3(m, m)] = a;
     double2 prev = c2(0.0);
     for (int n = m + 1; n <= p; ++n) {
-      double2 b = cscale(1.0 / ((double)(n + m) * (n - m)),
+      double2 b = cscale(rcp(n + m) * rcp(n - m),
                          csub(cscale((2.0 * n - 1) * z, a), cscale(r2, prev)));
       tab[idx3(n, m)] = b;
       prev = a;

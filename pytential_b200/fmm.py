@@ -52,17 +52,36 @@ class LaplaceKernel:
 
 
 @dataclass(frozen=True)
+class HelmholtzKernel:
+    """G = (i/4) H_0^(1)(k|x - y|) (2D)."""
+    dim: int
+    k: float
+    family: int = abi.QBXFMM_HELMHOLTZ
+
+    def global_scaling_const(self) -> complex:
+        return 0.25j
+
+
+@dataclass(frozen=True)
 class SourceKernelSpec:
     """Which layer potential(s) the density feeds: ``charge_coeff * S +
     dipole_coeff * D`` with the same density (merged source kernels,
     pytential/qbx/__init__.py:526-532)."""
-    kernel: LaplaceKernel
-    charge_coeff: float = 0.0
-    dipole_coeff: float = 0.0
+    kernel: LaplaceKernel | HelmholtzKernel
+    charge_coeff: complex = 0.0
+    dipole_coeff: complex = 0.0
 
     @property
     def needs_normals(self):
         return self.dipole_coeff != 0.0
+
+    @property
+    def is_complex(self):
+        return self.kernel.family == abi.QBXFMM_HELMHOLTZ
+
+    @property
+    def wave_number(self):
+        return getattr(self.kernel, "k", 0.0)
 
 
 # }}}
@@ -122,8 +141,9 @@ class Plan:
     the Python object."""
 
     def __init__(self, dgeo: DeviceGeometry, spec: SourceKernelSpec, qbx_order: int,
-                 fmm_order: int, nrhs: int = 1):
+                 fmm_order: int, nrhs: int = 1, target_specific_qbx: bool = False):
         self.dgeo = dgeo
+        self.target_specific_qbx = target_specific_qbx
         self.spec = spec
         self.qbx_order = qbx_order
         self.fmm_order = fmm_order
@@ -131,7 +151,8 @@ class Plan:
         self.kernel = abi.make_kernel_struct(
             family=spec.kernel.family, dim=spec.kernel.dim, qbx_order=qbx_order,
             fmm_order=fmm_order, nrhs=nrhs, charge_coeff=spec.charge_coeff,
-            dipole_coeff=spec.dipole_coeff)
+            dipole_coeff=spec.dipole_coeff, k=spec.wave_number,
+            target_specific_qbx=target_specific_qbx)
         h = ctypes.c_void_p()
         native.check("qbxfmm_plan_create", native.lib().qbxfmm_plan_create(
             ctypes.byref(self.kernel), ctypes.byref(dgeo.struct), ctypes.byref(h)))
@@ -186,8 +207,7 @@ class B200QBXExpansionWrangler:
                  source_extra_kwargs=None, kernel_extra_kwargs=None,
                  _use_target_specific_qbx=None, *, nrhs: int = 1, device="cuda",
                  device_geometry: DeviceGeometry | None = None):
-        if _use_target_specific_qbx:
-            raise ValueError("target-specific QBX is not part of this wrangler")
+        self.using_tsqbx = bool(_use_target_specific_qbx)
         self.tree_indep = tree_indep
         self.geo_data = geo_data
         self.dtype = dtype
@@ -205,7 +225,8 @@ class B200QBXExpansionWrangler:
         self.nrhs = nrhs
         self.dgeo = device_geometry or DeviceGeometry(geo_data, device)
         self.device = self.dgeo.device
-        self.plan = Plan(self.dgeo, tree_indep.spec, qbx_order, fmm_order, nrhs)
+        self.plan = Plan(self.dgeo, tree_indep.spec, qbx_order, fmm_order, nrhs,
+                         target_specific_qbx=self.using_tsqbx)
         self.traversal = geo_data.traversal()
         self.tree = self.traversal.tree
         self.error_word = torch.zeros(1, dtype=torch.int32, device=self.device)
@@ -217,6 +238,10 @@ class B200QBXExpansionWrangler:
         return torch.zeros(*shape, dtype=torch.complex128 if complex_ else torch.float64,
                            device=self.device)
 
+    @property
+    def _pot_complex(self):
+        return self.tree_indep.spec.is_complex
+
     def multipole_expansion_zeros(self, actx=None):
         return self._z(self.dgeo.nboxes, self.nrhs, self.plan.ncf, complex_=True)
 
@@ -227,10 +252,11 @@ class B200QBXExpansionWrangler:
 
     def output_zeros(self, actx=None):
         """Non-QBX targets only (fmm.py:174-186)."""
-        return self._z(self.nrhs, max(self.dgeo.nfiltered_targets, 1))
+        return self._z(self.nrhs, max(self.dgeo.nfiltered_targets, 1),
+                       complex_=self._pot_complex)
 
     def full_output_zeros(self, actx=None):
-        return self._z(self.nrhs, self.dgeo.ntargets)
+        return self._z(self.nrhs, self.dgeo.ntargets, complex_=self._pot_complex)
 
     def _err(self):
         return ctypes.cast(ctypes.c_void_p(_ptr(self.error_word)),
@@ -243,9 +269,10 @@ class B200QBXExpansionWrangler:
 
     def reorder_sources(self, source_array):
         """User source order -> tree order (fmm.py:199-200)."""
-        w = torch.as_tensor(source_array, dtype=torch.float64, device=self.device)
+        dt = torch.complex128 if self._pot_complex else torch.float64
+        w = torch.as_tensor(source_array, dtype=dt, device=self.device)
         w = w.reshape(self.nrhs, -1).contiguous()
-        out = self._z(self.nrhs, self.dgeo.nsources)
+        out = self._z(self.nrhs, self.dgeo.nsources, complex_=self._pot_complex)
         self.plan.call("qbxfmm_form_strengths", ctypes.byref(self._reorder.struct),
                        ctypes.c_void_p(_ptr(w)), ctypes.c_void_p(_ptr(out)), self._s())
         return out
@@ -306,6 +333,9 @@ class B200QBXExpansionWrangler:
 
     def form_global_qbx_locals(self, actx, src_weight_vecs):
         qe = self.qbx_local_expansion_zeros()
+        if self.using_tsqbx:
+            # the list-1 part is evaluated per target by eval_target_specific_qbx_locals
+            return qe
         self.plan.call("qbxfmm_form_global_qbx_locals",
                        ctypes.c_void_p(_ptr(self._w(src_weight_vecs))),
                        ctypes.c_void_p(_ptr(qe)), self._err(), self._s())
@@ -331,12 +361,18 @@ class B200QBXExpansionWrangler:
         return pot
 
     def eval_target_specific_qbx_locals(self, actx, src_weight_vecs):
-        return self.full_output_zeros()
+        pot = self.full_output_zeros()
+        if not self.using_tsqbx:
+            return pot
+        self.plan.call("qbxfmm_eval_target_specific_qbx_locals",
+                       ctypes.c_void_p(_ptr(self._w(src_weight_vecs))),
+                       ctypes.c_void_p(_ptr(pot)), self._err(), self._s())
+        return pot
 
     def assemble_potentials(self, non_qbx_potentials, qbx_potentials):
         """Scatter/add/reorder with kernel scaling (fmm.py:569-588):
         ``(nrhs, nuser_targets)`` in user target order."""
-        out = self._z(self.nrhs, self.dgeo.nuser_targets)
+        out = self._z(self.nrhs, self.dgeo.nuser_targets, complex_=self._pot_complex)
         self.plan.call("qbxfmm_assemble", ctypes.c_void_p(_ptr(non_qbx_potentials.contiguous())),
                        ctypes.c_void_p(_ptr(qbx_potentials.contiguous())),
                        ctypes.c_void_p(_ptr(out)), self._s())
@@ -418,12 +454,14 @@ class QBXApply:
 
     def __init__(self, geo: QBXFMMGeometryData, spec: SourceKernelSpec, qbx_order: int,
                  fmm_order: int, nrhs: int = 1, device="cuda",
-                 device_geometry: DeviceGeometry | None = None):
+                 device_geometry: DeviceGeometry | None = None,
+                 target_specific_qbx: bool = False):
         self.geo = geo
         self.device = torch.device(device)
         self.dgeo = device_geometry or DeviceGeometry(geo, device)
         self.up = DeviceUpsampler(geo.discr, device)
-        self.plan = Plan(self.dgeo, spec, qbx_order, fmm_order, nrhs)
+        self.plan = Plan(self.dgeo, spec, qbx_order, fmm_order, nrhs,
+                         target_specific_qbx=target_specific_qbx)
         self.nrhs = nrhs
         sizes = self.plan.workspace_sizes()
         self._ws_tensors = [torch.zeros(max(s, 8) // 8 + 1, dtype=torch.float64,
@@ -435,14 +473,14 @@ class QBXApply:
                                ctypes.POINTER(ctypes.c_int32)))
         self.ndofs = geo.discr.ndofs
         self.nuser_targets = self.dgeo.nuser_targets
+        self.dtype = torch.complex128 if spec.is_complex else torch.float64
         self._graph = None
 
     def new_output(self):
-        return torch.empty(self.nrhs, self.nuser_targets, dtype=torch.float64,
-                           device=self.device)
+        return torch.empty(self.nrhs, self.nuser_targets, dtype=self.dtype, device=self.device)
 
     def apply_into(self, density: torch.Tensor, out: torch.Tensor, stream=None):
-        assert density.is_cuda and density.dtype == torch.float64 and density.is_contiguous()
+        assert density.is_cuda and density.dtype == self.dtype and density.is_contiguous()
         assert density.numel() == self.nrhs * self.ndofs
         assert out.is_contiguous() and out.numel() == self.nrhs * self.nuser_targets
         self.plan.call("qbxfmm_apply", ctypes.byref(self.up.struct), ctypes.byref(self.ws),
@@ -451,7 +489,7 @@ class QBXApply:
         return out
 
     def __call__(self, density: torch.Tensor) -> torch.Tensor:
-        density = torch.as_tensor(density, dtype=torch.float64, device=self.device)
+        density = torch.as_tensor(density, dtype=self.dtype, device=self.device)
         density = density.reshape(self.nrhs, self.ndofs).contiguous()
         return self.apply_into(density, self.new_output())
 
@@ -459,7 +497,7 @@ class QBXApply:
 
     def capture(self):
         """Capture the apply into a CUDA graph over static input/output buffers."""
-        self.g_in = torch.zeros(self.nrhs, self.ndofs, dtype=torch.float64, device=self.device)
+        self.g_in = torch.zeros(self.nrhs, self.ndofs, dtype=self.dtype, device=self.device)
         self.g_out = self.new_output()
         s = torch.cuda.Stream(device=self.device)
         s.wait_stream(torch.cuda.current_stream())
@@ -483,9 +521,9 @@ class QBXApply:
     # {{{ end to end from host buffers
 
     def alloc_host_buffers(self):
-        self.h_in = torch.zeros(self.nrhs, self.ndofs, dtype=torch.float64).pin_memory()
-        self.h_out = torch.zeros(self.nrhs, self.nuser_targets, dtype=torch.float64).pin_memory()
-        self.d_in = torch.zeros(self.nrhs, self.ndofs, dtype=torch.float64, device=self.device)
+        self.h_in = torch.zeros(self.nrhs, self.ndofs, dtype=self.dtype).pin_memory()
+        self.h_out = torch.zeros(self.nrhs, self.nuser_targets, dtype=self.dtype).pin_memory()
+        self.d_in = torch.zeros(self.nrhs, self.ndofs, dtype=self.dtype, device=self.device)
         self.d_out = self.new_output()
 
     def apply_host(self, density_host=None, stream=None) -> torch.Tensor:
@@ -504,11 +542,11 @@ class QBXApply:
 
     @property
     def h2d_bytes(self):
-        return self.nrhs * self.ndofs * 8
+        return self.nrhs * self.ndofs * self.h_in.element_size()
 
     @property
     def d2h_bytes(self):
-        return self.nrhs * self.nuser_targets * 8
+        return self.nrhs * self.nuser_targets * self.h_out.element_size()
 
     # }}}
 

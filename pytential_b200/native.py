@@ -35,6 +35,7 @@ _STAGES = {
     "qbxfmm_translate_box_multipoles_to_qbx_local": [_vp, _vp, _pi, _vp],
     "qbxfmm_translate_box_local_to_qbx_local": [_vp, _vp, _vp],
     "qbxfmm_eval_qbx_expansions": [_vp, _vp, _vp],
+    "qbxfmm_eval_target_specific_qbx_locals": [_vp, _vp, _pi, _vp],
     "qbxfmm_assemble": [_vp, _vp, _vp, _vp],
     "qbxfmm_workspace_sizes": [ctypes.POINTER(ctypes.c_size_t)],
     "qbxfmm_apply": [ctypes.POINTER(abi.QBXFMMUpsample), ctypes.POINTER(abi.QBXFMMWorkspace),

@@ -21,7 +21,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from .discretization import Discretization, make_ellipsoid, make_starfish
-from .fmm import LaplaceKernel, SourceKernelSpec
+from .fmm import HelmholtzKernel, LaplaceKernel, SourceKernelSpec
 from .geometry import QBXFMMGeometryData
 
 
@@ -52,7 +52,7 @@ class Workload:
         return sum(p.shape[1] for p, _ in self.targets)
 
     def tree_strengths(self):
-        """Flat strengths in tree order (float64, (nrhs, nsources)) for the checker."""
+        """Flat strengths in tree order ((nrhs, nsources)) for the checker."""
         geo = self.geometry()
         w = self.discr.upsample_density(self.density) * self.discr.quad_weights
         return np.ascontiguousarray(w[:, geo.tree().user_source_ids])
@@ -94,3 +94,25 @@ def laplace3d_ellipsoid(nrefine: int = 3, nshell: int = 2000, seed: int = 0,
                             dipole_coeff=1.0 if op == "D" else 0.0)
     return Workload(f"3D Laplace {op}, ellipsoid icosphere-{nrefine} ({d.nelements} tri)",
                     d, [(d.nodes, +1), (v * r, 0)], dens, spec, qbx_order, fmm_order, seed)
+
+
+def helmholtz2d_starfish(nelements: int = 2048, k: float = 20.0, nrhs: int = 64, seed: int = 0,
+                         op: str = "BW", qbx_order: int = 5, fmm_order: int = 20,
+                         nvolume: int = 0) -> Workload:
+    """2D Helmholtz on the starfish: Brakhage-Werner combined field ``D - i k S``
+    (op "BW"), or "S"/"D"; exterior limit on the surface.  Densities: negated
+    incident plane waves ``-exp(i k d.x)`` at ``nrhs`` uniform angles, restricted to
+    the surface (the right-hand sides of the exterior Dirichlet problem)."""
+    rng = np.random.default_rng(seed)
+    d = make_starfish(nelements)
+    ang = 2 * np.pi * np.arange(nrhs) / nrhs
+    dirs = np.stack([np.cos(ang), np.sin(ang)])
+    dens = -np.exp(1j * k * (dirs.T @ d.nodes))
+    cq = {"BW": -1j * k, "S": 1.0, "D": 0.0}[op]
+    cd = {"BW": 1.0, "S": 0.0, "D": 1.0}[op]
+    spec = SourceKernelSpec(HelmholtzKernel(2, k), charge_coeff=cq, dipole_coeff=cd)
+    targets = [(d.nodes, +1)]
+    if nvolume:
+        targets.append((rng.uniform(-2, 2, size=(2, nvolume)), 0))
+    return Workload(f"2D Helmholtz k={k:g} {op}, starfish {nelements}x16 nodes, {nrhs} rhs",
+                    d, targets, dens, spec, qbx_order, fmm_order, seed)

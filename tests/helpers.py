@@ -8,7 +8,8 @@ import os
 import numpy as np
 
 from pytential_b200 import abi
-from pytential_b200.workloads import laplace2d_starfish, laplace3d_ellipsoid
+from pytential_b200.workloads import (helmholtz2d_starfish, laplace2d_starfish,
+                                     laplace3d_ellipsoid)
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
@@ -29,7 +30,22 @@ def workload(name: str):
         return laplace3d_ellipsoid(nrefine=2, nshell=500, op="S", qbx_order=4, fmm_order=8)
     if name == "2d-D-nrhs3":
         return laplace2d_starfish(nelements=32, nvolume=300, op="D", nrhs=3)
+    if name == "h2d-BW-small":
+        return helmholtz2d_starfish(nelements=48, nrhs=2, nvolume=300, op="BW")
+    if name == "h2d-S-small":
+        return helmholtz2d_starfish(nelements=32, nrhs=1, nvolume=200, op="S", fmm_order=16)
+    if name == "h2d-D-small":
+        return helmholtz2d_starfish(nelements=32, nrhs=3, nvolume=200, op="D", qbx_order=4)
     raise KeyError(name)
+
+
+def oracle_for(wl, nrhs=None):
+    from oracle.oracle import Oracle
+    sp = wl.spec
+    return Oracle(wl.geometry(), dim=sp.kernel.dim, qbx_order=wl.qbx_order,
+                  fmm_order=wl.fmm_order, nrhs=nrhs or wl.nrhs,
+                  charge_coeff=sp.charge_coeff, dipole_coeff=sp.dipole_coeff,
+                  family=sp.kernel.family, k=sp.wave_number)
 
 
 def relerr(a, b):
@@ -64,6 +80,11 @@ def golden_geometry(z):
     for k, v in zip(["qbx_chunk_target_box", "qbx_chunk_start", "qbx_chunk_count",
                      "centers_by_target_box"], ch):
         arrays[k] = v
+    ts = abi.tsqbx_schedule(ch[3], z["qbx_center_to_target_box"], z["center_to_targets_starts"],
+                            z["center_to_targets_lists"])
+    for k, v in zip(["tsqbx_chunk_target_box", "tsqbx_chunk_start", "tsqbx_chunk_count",
+                     "tsqbx_targets", "tsqbx_centers"], ts):
+        arrays[k] = v
     nboxes = len(z["box_source_starts"])
     scalars = {name: 0 for name, kind in abi.GEOMETRY_FIELDS if kind in ("i", "d")}
     scalars.update(dim=3, nboxes=nboxes, nlevels=1, nsources=z["sources"].shape[1],
@@ -71,5 +92,5 @@ def golden_geometry(z):
                    ncenters=z["centers"].shape[1],
                    nglobal_qbx_centers=len(z["global_qbx_centers"]),
                    ntarget_boxes=len(z["list1_starts"]) - 1,
-                   nqbx_chunks=len(ch[0]))
+                   nqbx_chunks=len(ch[0]), ntsqbx_chunks=len(ts[0]))
     return scalars, arrays

@@ -16,18 +16,11 @@ from pytential_b200 import abi, native
 from pytential_b200.fmm import (B200QBXExpansionWrangler, B200TreeIndependentDataForWrangler,
                                 QBXApply, drive_fmm)
 
-from helpers import golden_geometry, golden_tsqbx, relerr, workload
+from helpers import golden_geometry, golden_tsqbx, oracle_for, relerr, workload
 
 pytestmark = pytest.mark.gpu
 
 TOL = 1e-12
-
-
-def oracle_for(wl):
-    sp = wl.spec
-    return Oracle(wl.geometry(), dim=sp.kernel.dim, qbx_order=wl.qbx_order,
-                  fmm_order=wl.fmm_order, nrhs=wl.nrhs, charge_coeff=sp.charge_coeff,
-                  dipole_coeff=sp.dipole_coeff)
 
 
 _cache = {}
@@ -51,7 +44,11 @@ def host(t):
     return t.cpu().numpy()
 
 
-@pytest.mark.parametrize("name", ["2d-S", "2d-D", "3d-D-small", "3d-S-small", "2d-D-nrhs3"])
+ALL = ["2d-S", "2d-D", "3d-D-small", "3d-S-small", "2d-D-nrhs3", "h2d-BW-small",
+       "h2d-S-small", "h2d-D-small"]
+
+
+@pytest.mark.parametrize("name", ALL)
 def test_each_stage_matches_checker(name):
     wl, w, o = wrangler_for(name)
     s = wl.tree_strengths()
@@ -119,7 +116,7 @@ def test_each_stage_matches_checker(name):
     w.check_error_word()
 
 
-@pytest.mark.parametrize("name", ["2d-S", "2d-D", "3d-D-small", "3d-S-small", "2d-D-nrhs3"])
+@pytest.mark.parametrize("name", ALL)
 def test_drive_fmm_and_apply_match_checker(name):
     wl, w, o = wrangler_for(name)
     ref = o.apply(wl.tree_strengths())
@@ -131,6 +128,23 @@ def test_drive_fmm_and_apply_match_checker(name):
     got2 = host(ap(dev(wl.density)))
     assert relerr(got2, ref) < TOL
     ap.check_error_word()
+
+
+@pytest.mark.parametrize("name", ["2d-S", "2d-D", "3d-D-small", "3d-S-small", "2d-D-nrhs3"])
+def test_target_specific_mode_matches_checker(name):
+    """With target-specific QBX the list-1 near field is evaluated per target; the
+    truncation is the same, so the apply equals the checker's (expansion-based) one."""
+    wl, w, o = wrangler_for(name)
+    ref = o.apply(wl.tree_strengths())
+    ap = QBXApply(wl.geometry(), wl.spec, wl.qbx_order, wl.fmm_order, nrhs=wl.nrhs,
+                  device_geometry=w.dgeo, target_specific_qbx=True)
+    got = host(ap(dev(wl.density)))
+    assert relerr(got, ref) < TOL
+    wt = B200QBXExpansionWrangler(B200TreeIndependentDataForWrangler(wl.spec), wl.geometry(),
+                                  np.float64, wl.qbx_order, wl.fmm_order, nrhs=wl.nrhs,
+                                  device_geometry=w.dgeo, _use_target_specific_qbx=True)
+    flat = wl.discr.upsample_density(wl.density) * wl.discr.quad_weights
+    assert relerr(host(drive_fmm(None, wt, [dev(flat)])), ref) < TOL
 
 
 def test_full_size_3d_double_layer_apply():
@@ -188,10 +202,16 @@ def test_near_field_matches_reference_tsqbx_golden(op):
                     ctypes.c_void_p(qe.data_ptr()), errp, st)
         native.call("qbxfmm_eval_qbx_expansions", h, ctypes.c_void_p(qe.data_ptr()),
                     ctypes.c_void_p(pt.data_ptr()), st)
+        # the target-specific kernel (the reference module's own algorithm) on the same data
+        pt2 = torch.zeros_like(pt)
+        native.call("qbxfmm_eval_target_specific_qbx_locals", h, ctypes.c_void_p(s.data_ptr()),
+                    ctypes.c_void_p(pt2.data_ptr()), errp, st)
         L.qbxfmm_plan_destroy(h)
         got = host(pt)[0]
+        got2 = host(pt2)[0]
         assert int(err.item()) == 0
         assert relerr(got[mask], z[f"pot_{op}_{q}"][mask]) < TOL, (op, q)
+        assert relerr(got2[mask], z[f"pot_{op}_{q}"][mask]) < TOL, ("tsqbx", op, q)
 
 
 def test_bad_list_entry_reports_instead_of_faulting():

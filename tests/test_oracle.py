@@ -16,14 +16,7 @@ import pytest
 from oracle.oracle import Oracle, lib
 from pytential_b200 import abi
 
-from helpers import golden_geometry, golden_tsqbx, relerr, workload
-
-
-def oracle_for(wl, nrhs=None):
-    sp = wl.spec
-    return Oracle(wl.geometry(), dim=sp.kernel.dim, qbx_order=wl.qbx_order,
-                  fmm_order=wl.fmm_order, nrhs=nrhs or wl.nrhs,
-                  charge_coeff=sp.charge_coeff, dipole_coeff=sp.dipole_coeff)
+from helpers import golden_geometry, golden_tsqbx, oracle_for, relerr, workload
 
 
 @pytest.mark.parametrize("op", ["S", "D"])
@@ -104,3 +97,46 @@ def test_on_surface_jump_relation_2d():
     # volume potential: -1 inside, 0 outside (Gauss's identity, this sign convention)
     assert np.abs(out[nsurf:][inside] + 1).max() < 1e-6
     assert np.abs(out[nsurf:][outside]).max() < 1e-6
+
+
+def test_helmholtz2d_green_representation():
+    """S[du/dn] - D[u] = u inside, 0 outside, for u = G(x - x0) with x0 outside
+    (interior Green's representation; checks H2D multipole/local/QBX arithmetic
+    end to end against an exact solution)."""
+    from scipy.special import hankel1
+
+    from pytential_b200 import abi
+    from pytential_b200.discretization import make_starfish
+    from pytential_b200.geometry import QBXFMMGeometryData
+    from oracle.oracle import Oracle
+
+    k = 20.0
+    d = make_starfish(128)
+    rng = np.random.default_rng(0)
+    th = rng.uniform(0, 2 * np.pi, 300)
+    rad = rng.uniform(0.1, 1.8, 300)
+    pts = np.array([rad * np.cos(th), rad * np.sin(th)])
+    rb = 1 + 0.25 * np.cos(5 * th)
+    inside = rad < rb - 0.08
+    outside = rad > rb + 0.08
+    keep = inside | outside
+    pts, inside = pts[:, keep], inside[keep]
+    g = QBXFMMGeometryData(d, [(pts, 0)])
+    x0 = np.array([2.5, 0.7])
+
+    def u(x):
+        return 0.25j * hankel1(0, k * np.linalg.norm(x - x0[:, None], axis=0))
+
+    def dudn(x, n):
+        dx = x - x0[:, None]
+        r = np.linalg.norm(dx, axis=0)
+        return -0.25j * k * hankel1(1, k * r) * (dx * n).sum(0) / r
+
+    kw = dict(dim=2, qbx_order=6, fmm_order=24, family=abi.QBXFMM_HELMHOLTZ, k=k)
+    oS = Oracle(g, charge_coeff=1.0, **kw)
+    oD = Oracle(g, dipole_coeff=1.0, **kw)
+    sS = oS.tree_strengths(d.upsample_density(dudn(d.nodes, d.normals)) * d.quad_weights)
+    sD = oD.tree_strengths(d.upsample_density(u(d.nodes)) * d.quad_weights)
+    val = oS.apply(sS)[0] - oD.apply(sD)[0]
+    ref = np.where(inside, u(pts), 0)
+    assert relerr(val, ref) < 1e-6
