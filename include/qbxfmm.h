@@ -140,6 +140,29 @@ typedef struct qbxfmm_geometry {
   const int32_t* tsqbx_chunk_count;
   const int32_t* tsqbx_targets;             /* tree target index per pair */
   const int32_t* tsqbx_centers;             /* center index per pair */
+
+  /* Translation classes for the matrix form of M2L / M2M / L2L.  A class is a
+   * translation vector in units of the (source) box width; within a class every
+   * translation is the same matrix (up to a per-level factor for M2L), so each
+   * class is one dense matrix product over all its pairs.
+   *   M2L: list-2 pairs grouped by offset (target - source) / width.
+   *   M2M: (child -> parent) pairs grouped by (parent level, child position).
+   *   L2L: (parent -> child) pairs grouped by (child level, child position). */
+  int32_t m2l_nclasses;
+  const int32_t* m2l_class_offsets;         /* [dim][m2l_nclasses] integer offsets */
+  const int32_t* m2l_class_starts;          /* [m2l_nclasses + 1] into the pair arrays */
+  const int32_t* m2l_pair_src;              /* source box per pair (class order) */
+  const int32_t* m2l_tgt_pair_starts;       /* [nttp_boxes + 1] */
+  const int32_t* m2l_tgt_pairs;             /* pair indices per target (list-2 order) */
+  int32_t m2m_npairs;
+  const int32_t* m2m_group_starts;          /* [nlevels * 2^dim + 1]: group = (level, child pos) */
+  const int32_t* m2m_pair_src;              /* child box per pair */
+  const int32_t* m2m_par_pair_starts;       /* [nsource_parent_boxes + 1] */
+  const int32_t* m2m_par_pairs;             /* pair indices per source parent box */
+  int32_t l2l_npairs;
+  const int32_t* l2l_group_starts;          /* [nlevels * 2^dim + 1]: group = (level, child pos) */
+  const int32_t* l2l_pair_src;              /* parent box per pair */
+  const int32_t* l2l_pair_dst;              /* child box per pair */
 } qbxfmm_geometry;
 
 #define QBXFMM_CENTER_CHUNK 32

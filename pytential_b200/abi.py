@@ -74,6 +74,12 @@ GEOMETRY_FIELDS = [
     ("nonqbx_chunk_count", "pi"),
     ("ntsqbx_chunks", "i"), ("tsqbx_chunk_target_box", "pi"), ("tsqbx_chunk_start", "pi"),
     ("tsqbx_chunk_count", "pi"), ("tsqbx_targets", "pi"), ("tsqbx_centers", "pi"),
+    ("m2l_nclasses", "i"), ("m2l_class_offsets", "pi"), ("m2l_class_starts", "pi"),
+    ("m2l_pair_src", "pi"), ("m2l_tgt_pair_starts", "pi"), ("m2l_tgt_pairs", "pi"),
+    ("m2m_npairs", "i"), ("m2m_group_starts", "pi"), ("m2m_pair_src", "pi"),
+    ("m2m_par_pair_starts", "pi"), ("m2m_par_pairs", "pi"),
+    ("l2l_npairs", "i"), ("l2l_group_starts", "pi"), ("l2l_pair_src", "pi"),
+    ("l2l_pair_dst", "pi"),
 ]
 
 CENTER_CHUNK = 32
@@ -199,6 +205,80 @@ def tsqbx_schedule(centers_by_target_box, qbx_center_to_target_box, center_to_ta
             np.array(ch_count, np.int32), np.array(tg, np.int32), np.array(ct, np.int32))
 
 
+def translation_classes(tree, trav):
+    """Class lists for the matrix form of M2L / M2M / L2L (see qbxfmm_geometry)."""
+    dim = tree.dimensions
+    nch = 2 ** dim
+    ipos = tree.box_ipos.astype(np.int64)
+    out = {}
+    # M2L: list-2 pairs by integer offset
+    l2s = np.asarray(trav.from_sep_siblings_starts)
+    l2l = np.asarray(trav.from_sep_siblings_lists, np.int64)
+    ttp = np.asarray(trav.target_or_target_parent_boxes, np.int64)
+    tgt_idx = np.repeat(np.arange(len(ttp)), np.diff(l2s))
+    tgt_box = ttp[tgt_idx]
+    off = ipos[:, tgt_box] - ipos[:, l2l]                       # (dim, npairs)
+    R = int(np.abs(off).max()) if off.size else 0
+    key = np.zeros(off.shape[1], np.int64)
+    for d in range(dim):
+        key = key * (2 * R + 1) + (off[d] + R)
+    order = np.lexsort((tgt_idx, key))                        # class, then target
+    ukeys, first = np.unique(key[order], return_index=True)
+    out["m2l_nclasses"] = len(ukeys)
+    cls_off = off[:, order][:, first] if len(ukeys) else np.zeros((dim, 0), np.int64)
+    out["m2l_class_offsets"] = np.ascontiguousarray(cls_off, np.int32)
+    out["m2l_class_starts"] = np.concatenate([first, [len(order)]]).astype(np.int32)
+    out["m2l_pair_src"] = l2l[order].astype(np.int32)
+    pos = np.empty(len(order), np.int64)
+    pos[order] = np.arange(len(order))                        # list-2 entry -> pair index
+    out["m2l_tgt_pair_starts"] = l2s.astype(np.int32)
+    out["m2l_tgt_pairs"] = pos.astype(np.int32)
+    # M2M / L2L: (level, child position) groups
+    nlev = tree.nlevels
+    child = np.asarray(tree.box_child_ids)
+    has_src = tree.box_source_counts_cumul > 0
+    spb = np.asarray(trav.source_parent_boxes, np.int64)
+    m_src, m_grp, m_par = [], [], []
+    for i, b in enumerate(spb):
+        for ci in range(nch):
+            c = child[ci, b]
+            if c != 0 and has_src[c]:
+                m_src.append(c)
+                m_grp.append(tree.box_levels[b] * nch + ci)
+                m_par.append(i)
+    m_src = np.array(m_src, np.int64)
+    m_grp = np.array(m_grp, np.int64)
+    m_par = np.array(m_par, np.int64)
+    o = np.lexsort((m_src, m_grp))
+    out["m2m_npairs"] = len(o)
+    out["m2m_group_starts"] = np.searchsorted(m_grp[o], np.arange(nlev * nch + 1)).astype(np.int32)
+    out["m2m_pair_src"] = m_src[o].astype(np.int32)
+    pos = np.empty(len(o), np.int64)
+    pos[o] = np.arange(len(o))
+    o2 = np.lexsort((m_src, m_par))
+    out["m2m_par_pair_starts"] = np.searchsorted(m_par[o2], np.arange(len(spb) + 1)).astype(np.int32)
+    out["m2m_par_pairs"] = pos[o2].astype(np.int32)
+    # L2L
+    l_src, l_dst, l_grp = [], [], []
+    for b in ttp:
+        par = tree.box_parent_ids[b]
+        if par < 0:
+            continue
+        ci = int(np.where(child[:, par] == b)[0][0])
+        l_src.append(par)
+        l_dst.append(b)
+        l_grp.append(tree.box_levels[b] * nch + ci)
+    l_src = np.array(l_src, np.int64)
+    l_dst = np.array(l_dst, np.int64)
+    l_grp = np.array(l_grp, np.int64)
+    o = np.lexsort((l_dst, l_grp))
+    out["l2l_npairs"] = len(o)
+    out["l2l_group_starts"] = np.searchsorted(l_grp[o], np.arange(nlev * nch + 1)).astype(np.int32)
+    out["l2l_pair_src"] = l_src[o].astype(np.int32)
+    out["l2l_pair_dst"] = l_dst[o].astype(np.int32)
+    return out
+
+
 def _i(a):
     return np.ascontiguousarray(a, dtype=np.int32)
 
@@ -271,7 +351,12 @@ def geometry_arrays(geo) -> tuple[dict, dict]:
                         arrays["center_to_targets_starts"], arrays["center_to_targets_lists"])
     arrays.update(dict(zip(["tsqbx_chunk_target_box", "tsqbx_chunk_start", "tsqbx_chunk_count",
                             "tsqbx_targets", "tsqbx_centers"], ts)))
+    tc = translation_classes(tree, trav)
+    arrays.update({k_: np.ascontiguousarray(v, np.int32) for k_, v in tc.items()
+                   if not k_.endswith(("nclasses", "npairs"))})
     scalars = {
+        "m2l_nclasses": tc["m2l_nclasses"], "m2m_npairs": tc["m2m_npairs"],
+        "l2l_npairs": tc["l2l_npairs"],
         "ntsqbx_chunks": len(ts[0]),
         "nnonqbx_chunks": len(nq_tb),
         "nqbx_chunks": len(ch_tb),

@@ -21,6 +21,15 @@ from helpers import golden_geometry, golden_tsqbx, oracle_for, relerr, workload
 pytestmark = pytest.mark.gpu
 
 TOL = 1e-12
+# 2D Helmholtz: the order-2p Hankel translations sum terms much larger than their
+# result (|H_n(x)| grows like (n-1)! (2/x)^n), so last-bit differences between two
+# float64 implementations of the special functions surface at a few 1e-12 of the
+# largest coefficient.
+TOL_HELM = 5e-12
+
+
+def tol_for(wl):
+    return TOL_HELM if wl.spec.is_complex else TOL
 
 
 _cache = {}
@@ -51,6 +60,7 @@ ALL = ["2d-S", "2d-D", "3d-D-small", "3d-S-small", "2d-D-nrhs3", "h2d-BW-small",
 @pytest.mark.parametrize("name", ALL)
 def test_each_stage_matches_checker(name):
     wl, w, o = wrangler_for(name)
+    TOL = tol_for(wl)
     s = wl.tree_strengths()
     sw = [dev(s)]
 
@@ -119,6 +129,7 @@ def test_each_stage_matches_checker(name):
 @pytest.mark.parametrize("name", ALL)
 def test_drive_fmm_and_apply_match_checker(name):
     wl, w, o = wrangler_for(name)
+    TOL = tol_for(wl)
     ref = o.apply(wl.tree_strengths())
     flat = wl.discr.upsample_density(wl.density) * wl.discr.quad_weights
     got = host(drive_fmm(None, w, [dev(flat)]))
