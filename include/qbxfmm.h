@@ -189,6 +189,10 @@ typedef struct qbxfmm_workspace {
   void* pot_nonqbx;   /* [nrhs][nfiltered_targets] */
   void* pot_tree;     /* [nrhs][ntargets] */
   int32_t* error_word;/* one int32, set by kernels that meet an out-of-range index */
+  void* translations; /* translation-class matrices (filled by
+                         qbxfmm_precompute_translations); NULL selects the
+                         per-pair translation kernels */
+  void* pair_scratch; /* per-pair translation results, reduced per output box */
 } qbxfmm_workspace;
 
 #ifdef __cplusplus

@@ -36,8 +36,16 @@ int qbxfmm_plan_create(const qbxfmm_kernel* kernel, const qbxfmm_geometry* geome
                        qbxfmm_plan** plan);
 int qbxfmm_plan_destroy(qbxfmm_plan* plan);
 
-/* byte sizes of the six workspace buffers, in qbxfmm_workspace field order */
-int qbxfmm_workspace_sizes(const qbxfmm_plan* plan, size_t* sizes6);
+/* byte sizes of the workspace buffers, in qbxfmm_workspace field order:
+ * strengths, mpoles, locals, qbx_exps, pot_nonqbx, pot_tree, translations,
+ * pair_scratch (the last two are 0 when the matrix form is not available) */
+int qbxfmm_workspace_sizes(const qbxfmm_plan* plan, size_t* sizes8);
+
+/* Build the translation-class matrices of M2L / M2M / L2L into ws->translations
+ * (the reference's translation-class precompute, pytential/qbx/fmm.py:155-161,
+ * 399-407).  Once per plan and workspace, before qbxfmm_apply. */
+int qbxfmm_precompute_translations(const qbxfmm_plan* plan, const qbxfmm_workspace* ws,
+                                   void* stream);
 
 /* get_flat_strengths_from_densities + reorder_sources
  * (pytential/qbx/__init__.py:1075-1096; pytential/qbx/fmm.py:199-200).

@@ -100,7 +100,8 @@ class QBXFMMWorkspace(ctypes.Structure):
     _fields_ = [("strengths", ctypes.c_void_p), ("mpoles", ctypes.c_void_p),
                 ("locals", ctypes.c_void_p), ("qbx_exps", ctypes.c_void_p),
                 ("pot_nonqbx", ctypes.c_void_p), ("pot_tree", ctypes.c_void_p),
-                ("error_word", _pi)]
+                ("error_word", _pi), ("translations", ctypes.c_void_p),
+                ("pair_scratch", ctypes.c_void_p)]
 
 
 def qbx_center_schedule(global_qbx_centers, qbx_center_to_target_box, list1_starts,

@@ -4,6 +4,7 @@
 // called by the FMM driver (pytential/qbx/fmm.py:414-594); qbxfmm_apply runs them
 // all in the driver's order.  Stage outputs are accumulated (+=) into caller-owned
 // device buffers; the library allocates no device memory.
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <new>
@@ -24,6 +25,8 @@ struct qbxfmm_plan {
   HelmCoeffs hc;
   bool helm;
   int ncf, ncq;
+  bool trans_ok;                           // matrix form of M2L / M2M / L2L available
+  TransHost th;
 };
 
 namespace {
@@ -112,6 +115,27 @@ int qbxfmm_plan_create(const qbxfmm_kernel* kernel, const qbxfmm_geometry* geome
   if (e == cudaSuccess)
     e = cudaMemcpy(p->lvl_ttp.data(), g.level_start_ttp_box_nrs, sizeof(int32_t) * (g.nlevels + 1),
                    cudaMemcpyDeviceToHost);
+  p->trans_ok = !p->helm && k.dim == 3 && trans_supported(k.fmm_order) && g.nlevels <= 64;
+  if (e == cudaSuccess && p->trans_ok) {
+    const int nch = 8;
+    std::vector<int32_t> cs(g.m2l_nclasses + 1), ms(g.nlevels * nch + 1), ls(g.nlevels * nch + 1);
+    e = cudaMemcpy(cs.data(), g.m2l_class_starts, sizeof(int32_t) * cs.size(), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess)
+      e = cudaMemcpy(ms.data(), g.m2m_group_starts, sizeof(int32_t) * ms.size(), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess)
+      e = cudaMemcpy(ls.data(), g.l2l_group_starts, sizeof(int32_t) * ls.size(), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) {
+      for (int c = 0; c < g.m2l_nclasses; ++c)
+        p->th.m2l_max_pairs = std::max(p->th.m2l_max_pairs, cs[c + 1] - cs[c]);
+      for (int lev = 0; lev < g.nlevels; ++lev)
+        for (int ci = 0; ci < nch; ++ci) {
+          int gi = lev * nch + ci;
+          p->th.m2m_level_max_group[lev] = std::max(p->th.m2m_level_max_group[lev], ms[gi + 1] - ms[gi]);
+          p->th.l2l_level_max_group[lev] = std::max(p->th.l2l_level_max_group[lev], ls[gi + 1] - ls[gi]);
+        }
+      p->th.lvl_source_parent = p->lvl_source_parent.data();
+    }
+  }
   if (e != cudaSuccess) {
     delete p;
     return cuda_check(e, "qbxfmm_plan_create");
@@ -348,7 +372,7 @@ int qbxfmm_assemble(const qbxfmm_plan* p, const void* pot_nonqbx, const void* po
   return QBXFMM_OK;
 }
 
-int qbxfmm_workspace_sizes(const qbxfmm_plan* p, size_t* sizes6)
+int qbxfmm_workspace_sizes(const qbxfmm_plan* p, size_t* sizes6 /* 8 entries */)
 {
   if (int rc = check_plan(p)) return rc;
   if (!sizes6) return fail(QBXFMM_ERR_ARG, "null sizes");
@@ -361,6 +385,27 @@ int qbxfmm_workspace_sizes(const qbxfmm_plan* p, size_t* sizes6)
   sizes6[3] = (size_t)g.ncenters * nr * p->ncq * 2 * sizeof(double);
   sizes6[4] = nr * (size_t)(g.nfiltered_targets > 0 ? g.nfiltered_targets : 1) * scal;
   sizes6[5] = nr * (size_t)g.ntargets * scal;
+  if (p->trans_ok) {
+    int npairs = 0;
+    cudaError_t e = cudaMemcpy(&npairs, g.m2l_class_starts + g.m2l_nclasses, sizeof(int32_t),
+                               cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_check(e, "workspace_sizes");
+    npairs = std::max(npairs, g.m2m_npairs);
+    sizes6[6] = trans_matrix_bytes(p->kern.fmm_order, g.m2l_nclasses);
+    sizes6[7] = trans_scratch_bytes(p->kern.fmm_order, npairs, p->kern.nrhs);
+  } else {
+    sizes6[6] = sizes6[7] = 0;
+  }
+  return QBXFMM_OK;
+}
+
+int qbxfmm_precompute_translations(const qbxfmm_plan* p, const qbxfmm_workspace* ws, void* stream)
+{
+  if (int rc = check_plan(p)) return rc;
+  if (!ws) return fail(QBXFMM_ERR_ARG, "null workspace");
+  if (!p->trans_ok || !ws->translations) return QBXFMM_OK;
+  QBX_TRY(launch_trans_build(p->geo, p->kern.fmm_order, (double*)ws->translations, S(stream)),
+          "precompute_translations");
   return QBXFMM_OK;
 }
 
@@ -372,8 +417,9 @@ int qbxfmm_apply(const qbxfmm_plan* p, const qbxfmm_upsample* up, const qbxfmm_w
   if (!ws->strengths || !ws->mpoles || !ws->locals || !ws->qbx_exps || !ws->pot_nonqbx ||
       !ws->pot_tree)
     return fail(QBXFMM_ERR_ARG, "incomplete workspace");
-  size_t sz[6];
-  qbxfmm_workspace_sizes(p, sz);
+  size_t sz[8];
+  if (int rc = qbxfmm_workspace_sizes(p, sz)) return rc;
+  const bool gemm = p->trans_ok && ws->translations && ws->pair_scratch;
   cudaStream_t st = S(stream);
   QBX_TRY(cudaMemsetAsync(ws->mpoles, 0, sz[1], st), "apply: clear");
   QBX_TRY(cudaMemsetAsync(ws->locals, 0, sz[2], st), "apply: clear");
@@ -385,12 +431,31 @@ int qbxfmm_apply(const qbxfmm_plan* p, const qbxfmm_upsample* up, const qbxfmm_w
   // drive_fmm order (fmm.py:436-588)
   if ((rc = qbxfmm_form_strengths(p, up, density, ws->strengths, stream))) return rc;
   if ((rc = qbxfmm_form_multipoles(p, ws->strengths, ws->mpoles, stream))) return rc;
-  if ((rc = qbxfmm_coarsen_multipoles(p, ws->mpoles, stream))) return rc;
+  if (gemm)
+    QBX_TRY(launch_m2m_gemm(p->geo, p->th, p->kern.fmm_order, p->kern.nrhs,
+                            (const double*)ws->translations, (double2*)ws->mpoles,
+                            (double*)ws->pair_scratch, ws->error_word, S(stream)),
+            "coarsen_multipoles (matrix form)");
+  else if ((rc = qbxfmm_coarsen_multipoles(p, ws->mpoles, stream)))
+    return rc;
   if ((rc = qbxfmm_eval_direct(p, ws->strengths, ws->pot_nonqbx, ws->error_word, stream))) return rc;
-  if ((rc = qbxfmm_multipole_to_local(p, ws->mpoles, ws->locals, ws->error_word, stream))) return rc;
+  if (gemm)
+    QBX_TRY(launch_m2l_gemm(p->geo, p->th, p->kern.fmm_order, p->kern.nrhs,
+                            (const double*)ws->translations, (const double2*)ws->mpoles,
+                            (double2*)ws->locals, (double*)ws->pair_scratch, ws->error_word,
+                            S(stream)),
+            "multipole_to_local (matrix form)");
+  else if ((rc = qbxfmm_multipole_to_local(p, ws->mpoles, ws->locals, ws->error_word, stream)))
+    return rc;
   if ((rc = qbxfmm_eval_multipoles(p, ws->mpoles, ws->pot_nonqbx, ws->error_word, stream))) return rc;
   if ((rc = qbxfmm_form_locals(p, ws->strengths, ws->locals, ws->error_word, stream))) return rc;
-  if ((rc = qbxfmm_refine_locals(p, ws->locals, stream))) return rc;
+  if (gemm)
+    QBX_TRY(launch_l2l_gemm(p->geo, p->th, p->kern.fmm_order, p->kern.nrhs,
+                            (const double*)ws->translations, (double2*)ws->locals, ws->error_word,
+                            S(stream)),
+            "refine_locals (matrix form)");
+  else if ((rc = qbxfmm_refine_locals(p, ws->locals, stream)))
+    return rc;
   if ((rc = qbxfmm_eval_locals(p, ws->locals, ws->pot_nonqbx, stream))) return rc;
   const bool tsqbx = p->kern.target_specific_qbx != 0;
   if (!tsqbx &&

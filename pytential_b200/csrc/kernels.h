@@ -7,6 +7,27 @@
 
 namespace qbx {
 
+// host-side sizes for the translation-matrix kernels, filled at plan creation
+struct TransHost {
+  int m2l_max_pairs = 0;                 // largest M2L class
+  int m2m_level_max_group[64] = {0};     // largest (level, child position) group per level
+  int l2l_level_max_group[64] = {0};
+  const int32_t* lvl_source_parent = nullptr;   // host copy (owned by the plan)
+};
+
+bool trans_supported(int p);
+size_t trans_matrix_bytes(int p, int nclasses);
+size_t trans_scratch_bytes(int p, int npairs, int nrhs);
+cudaError_t launch_trans_build(const qbxfmm_geometry& g, int p, double* T, cudaStream_t st);
+cudaError_t launch_m2l_gemm(const qbxfmm_geometry& g, const TransHost& th, int p, int nrhs,
+                            const double* T, const double2* mp, double2* lo, double* cpair,
+                            int32_t* err, cudaStream_t st);
+cudaError_t launch_m2m_gemm(const qbxfmm_geometry& g, const TransHost& th, int p, int nrhs,
+                            const double* T, double2* mp, double* cpair, int32_t* err,
+                            cudaStream_t st);
+cudaError_t launch_l2l_gemm(const qbxfmm_geometry& g, const TransHost& th, int p, int nrhs,
+                            const double* T, double2* lo, int32_t* err, cudaStream_t st);
+
 cudaError_t launch_form_strengths(const qbxfmm_geometry& g, const qbxfmm_upsample& up, int nrhs,
                                   const double* density, double* strengths, cudaStream_t st);
 cudaError_t launch_p2m(const qbxfmm_geometry& g, SourceCoeffs sc, int p, int nrhs,

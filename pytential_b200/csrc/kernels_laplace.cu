@@ -45,15 +45,6 @@ k_form_strengths(int nsources, int ndofs, int npe, int nqpe,
 constexpr int NW = NT / 32;     // warps per CTA
 constexpr int MAXB = 128;       // list boxes staged per pass
 
-// decode coefficient index -> (n, m) for the 3D triangular layout
-QBX_D void decode3(int c, int& n, int& m)
-{
-  n = (int)((sqrt(8.0 * c + 1.0) - 1.0) * 0.5);
-  while ((n + 1) * (n + 2) / 2 <= c) ++n;
-  while (n * (n + 1) / 2 > c) --n;
-  m = c - n * (n + 1) / 2;
-}
-
 // Warp 0 writes the running source counts of list boxes [gb, gb + nb) (nb <= 128)
 // into s_pref[0..nb] and their first source into s_start; caller syncs.
 QBX_D void list_prefix(const qbxfmm_geometry& g, const int32_t* __restrict__ lists, int gb,

@@ -1,0 +1,383 @@
+// Matrix form of the 3D Laplace box translations (M2L, M2M, L2L) on the FP64
+// tensor cores (mma.sync m8n8k4 f64), sm_100a.
+//
+// With rscale-scaled coefficients a translation between boxes depends only on the
+// translation vector in units of the box width: every list-2 pair with the same
+// integer offset uses the same matrix (times 1/rho of the level, applied in the
+// reduction), every M2M / L2L pair with the same child position uses the same
+// matrix at every level.  A translation acts on the stored coefficients
+// (m >= 0, the rest by conjugate symmetry) as a real-linear map, so each class is a
+// real (2 ncoeff) x (2 ncoeff) matrix T acting on interleaved (re, im) vectors.
+//
+//   k_trans_build  : one CTA per class, T from the harmonic table of the class vector
+//   k_trans_gemm   : one CTA per (class, 32 pairs x rhs): C = T X with X the gathered
+//                    source expansions; T and X staged in shared memory
+//   k_trans_reduce : deterministic sum of each output box's pair results (list order)
+#include "laplace.cuh"
+#include "kernels.h"
+
+namespace qbx {
+
+namespace {
+
+constexpr int NT = 128;
+constexpr int NTILE = 32;            // max columns (pair x rhs) per CTA
+constexpr int XS = NTILE + 4;        // padded X row stride (conflict-free B fragments)
+
+QBX_D void dmma_8x8x4(double& d0, double& d1, double a, double b)
+{
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+}  // namespace
+
+// {{{ T construction
+
+// kind 0 = M2L (class vector d = offset, S table of order 2p; value (-1)^j S),
+// kind 1 = M2M (d = (child - parent) / rho_parent, R table of order p),
+// kind 2 = L2L (same d, R table).
+__global__ void __launch_bounds__(NT)
+k_trans_build(int kind, int p, int ncf, int rp, int kp, int nclasses, const int32_t* __restrict__ offs,
+              double* __restrict__ T)
+{
+  extern __shared__ double2 tab[];
+  int cls = blockIdx.x;
+  double d[3];
+  if (kind == 0) {
+    for (int k = 0; k < 3; ++k) d[k] = (double)offs[k * nclasses + cls];
+  } else {
+    // child position bits -> +-1/4 per axis (child centre relative to the parent)
+    for (int k = 0; k < 3; ++k) d[k] = ((cls >> k) & 1) ? 0.25 : -0.25;
+  }
+  if (kind == 0) sh3_S_table(2 * p, d[0], d[1], d[2], tab, threadIdx.x, NT);
+  else sh3_R_table(p, d[0], d[1], d[2], tab, threadIdx.x, NT);
+  __syncthreads();
+  double* Tc = T + (size_t)cls * rp * kp;
+  const int R = 2 * ncf;
+  for (int e = threadIdx.x; e < rp * kp; e += NT) {
+    int row = e / kp, col = e - row * kp;
+    double v = 0.0;
+    if (row < R && col < R) {
+      int co = row >> 1, ci = col >> 1;
+      int no, mo, ni, mi;
+      decode3(co, no, mo);
+      decode3(ci, ni, mi);
+      // unit input u at stored (ni, mi); its symmetric partner at -mi is u' = (-1)^mi conj(u)
+      double2 u = (col & 1) ? c2(0.0, 1.0) : c2(1.0, 0.0);
+      double2 up = cconj(u);
+      if (mi & 1) up = c2(-up.x, -up.y);
+      double2 val = c2(0.0);
+      if (kind == 0) {
+        // L_j^i = (-1)^j sum M_k^l S_{k+j}^{l+i}
+        val = cmul(u, sh3_get(tab, ni + no, mi + mo));
+        if (mi > 0) val = cadd(val, cmul(up, sh3_get(tab, ni + no, -mi + mo)));
+        if (no & 1) val = c2(-val.x, -val.y);
+      } else if (kind == 1) {
+        // M'_n^m = sum (1/2)^k M_k^l conj(R_{n-k}^{m-l})
+        double rk = ldexp(1.0, -ni);
+        val = cmulc(u, sh3_get(tab, no - ni, mo - mi));
+        if (mi > 0) val = cadd(val, cmulc(up, sh3_get(tab, no - ni, mo + mi)));
+        val = cscale(rk, val);
+      } else {
+        // L''_k^l = (1/2)^k sum L_n^m conj(R_{n-k}^{m-l})
+        double rk = ldexp(1.0, -no);
+        val = cmulc(u, sh3_get(tab, ni - no, mi - mo));
+        if (mi > 0) val = cadd(val, cmulc(up, sh3_get(tab, ni - no, -mi - mo)));
+        val = cscale(rk, val);
+      }
+      v = (row & 1) ? val.y : val.x;
+    }
+    Tc[e] = v;
+  }
+}
+
+// }}}
+
+// {{{ GEMM
+
+constexpr int KC = 32;               // K chunk staged per step
+constexpr int TSTR = KC + 4;         // padded T-chunk row stride (== 4 mod 16 doubles)
+
+// C = T X for one group (class) and one tile of columns (pair x rhs).  Warps are
+// arranged NWN (column tiles of 8) x NWM (row groups); each warp holds MTW m-tiles
+// of 8 rows x one 8-column tile in registers.  T and X are streamed in K chunks of
+// KC through shared memory.  If pair_dst is given the result is added (x scale)
+// into the destination box's expansion (each destination occurs once per launch),
+// else stored into cpair[pair * nrhs + r][0..rp).
+template <int MTW>
+__global__ void __launch_bounds__(NT)
+k_trans_gemm(int ncf, int rp, int kp, int nrhs, int nwm, const double* __restrict__ T,
+             int mat_base, int mat_mod, const int32_t* __restrict__ group_starts, int g0,
+             const int32_t* __restrict__ pair_src, const int32_t* __restrict__ pair_dst,
+             const double2* __restrict__ ein, double2* __restrict__ eout, double scale,
+             double* __restrict__ cpair, int32_t* err, int nboxes)
+{
+  extern __shared__ double sm[];
+  const int nwn = 4 / nwm;
+  const int ntile = 8 * nwn;
+  double* Ts = sm;                          // [rp][TSTR]
+  double* Xs = sm + (size_t)rp * TSTR;      // [KC][XS]
+  __shared__ int s_src[NTILE];
+  int grp = g0 + blockIdx.y;
+  int p0 = group_starts[grp], p1 = group_starts[grp + 1];
+  int ncol = (p1 - p0) * nrhs;
+  int c0 = blockIdx.x * ntile;
+  if (c0 >= ncol) return;
+  int mat = mat_base + (mat_mod > 0 ? (grp % mat_mod) : grp);
+  const double* Tg = T + (size_t)mat * rp * kp;
+  const int R = 2 * ncf;
+  for (int j = threadIdx.x; j < ntile; j += NT) {
+    int c = c0 + j;
+    int src = -1;
+    if (c < ncol) {
+      src = pair_src[p0 + c / nrhs];
+      if ((unsigned)src >= (unsigned)nboxes) {
+        report(err, QBX_DEVERR_BAD_BOX);
+        src = -1;
+      }
+    }
+    s_src[j] = src;
+  }
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int g = lane >> 2, tq = lane & 3;
+  int wn = warp % nwn, wm = warp / nwn;
+  int mt = rp / 8;
+  int mtw = (mt + nwm - 1) / nwm;
+  int mbeg = wm * mtw;
+  double acc[MTW][2];
+#pragma unroll
+  for (int i = 0; i < MTW; ++i) acc[i][0] = acc[i][1] = 0.0;
+  for (int kc = 0; kc < kp; kc += KC) {
+    int kw = min(KC, kp - kc);
+    __syncthreads();
+    for (int e = threadIdx.x; e < rp * KC; e += NT) {
+      int row = e / KC, col = e - row * KC;
+      Ts[row * TSTR + col] = col < kw ? __ldg(Tg + (size_t)row * kp + kc + col) : 0.0;
+    }
+    for (int e = threadIdx.x; e < ntile * KC; e += NT) {
+      int j = e / KC, k = e - j * KC;
+      int src = s_src[j];
+      double v = 0.0;
+      if (src >= 0 && k < kw && kc + k < R) {
+        int r = (c0 + j) % nrhs;
+        const double* x = reinterpret_cast<const double*>(ein + ((size_t)src * nrhs + r) * ncf);
+        v = __ldg(x + kc + k);
+      }
+      Xs[k * XS + j] = v;
+    }
+    __syncthreads();
+    for (int k0 = 0; k0 < kw; k0 += 4) {
+      double b = Xs[(k0 + tq) * XS + wn * 8 + g];
+#pragma unroll
+      for (int i = 0; i < MTW; ++i) {
+        int mi = mbeg + i;
+        if (mi < mt) {
+          double a = Ts[(mi * 8 + g) * TSTR + k0 + tq];
+          dmma_8x8x4(acc[i][0], acc[i][1], a, b);
+        }
+      }
+    }
+  }
+  // epilogue: acc[i][v] = C[row = (mbeg + i) * 8 + g][col = wn * 8 + 2 tq + v]
+#pragma unroll
+  for (int v = 0; v < 2; ++v) {
+    int j = wn * 8 + 2 * tq + v;
+    int c = c0 + j;
+    if (c >= ncol) continue;
+    int pr = p0 + c / nrhs, r = c % nrhs;
+    if (pair_dst) {
+      int dst = pair_dst[pr];
+      if ((unsigned)dst >= (unsigned)nboxes) {
+        report(err, QBX_DEVERR_BAD_BOX);
+        continue;
+      }
+      double* y = reinterpret_cast<double*>(eout + ((size_t)dst * nrhs + r) * ncf);
+#pragma unroll
+      for (int i = 0; i < MTW; ++i) {
+        int row = (mbeg + i) * 8 + g;
+        if (mbeg + i < mt && row < R) y[row] += scale * acc[i][v];
+      }
+    } else {
+      double* y = cpair + ((size_t)pr * nrhs + r) * rp;
+#pragma unroll
+      for (int i = 0; i < MTW; ++i) {
+        int row = (mbeg + i) * 8 + g;
+        if (mbeg + i < mt) y[row] = acc[i][v];
+      }
+    }
+  }
+}
+
+// out box o (o = boxes[obase + blockIdx.x]): eout[o][r] += scale(o) sum_{pairs} cpair[pair][r]
+// scale(o) = 1 / width(level(o)) when div_by_width, else 1.
+__global__ void __launch_bounds__(NT)
+k_trans_reduce(int ncf, int rp, int nrhs, const int32_t* __restrict__ boxes, int obase,
+               const int32_t* __restrict__ starts, const int32_t* __restrict__ pairs,
+               const double* __restrict__ cpair, double2* __restrict__ eout, int div_by_width,
+               const int32_t* __restrict__ box_levels, double root_extent)
+{
+  int i = obase + blockIdx.x;
+  int o = boxes[i];
+  int r = blockIdx.y;
+  double sc = div_by_width ? ldexp(1.0, box_levels[o]) / root_extent : 1.0;
+  int R = 2 * ncf;
+  double* y = reinterpret_cast<double*>(eout + ((size_t)o * nrhs + r) * ncf);
+  for (int row = threadIdx.x; row < R; row += NT) {
+    double acc = 0.0;
+    for (int q = starts[i]; q < starts[i + 1]; ++q)
+      acc += cpair[((size_t)pairs[q] * nrhs + r) * rp + row];
+    y[row] += sc * acc;
+  }
+}
+
+// }}}
+
+// {{{ launchers
+
+void trans_dims(int p, int& ncf, int& rp, int& kp)
+{
+  ncf = (p + 1) * (p + 2) / 2;
+  rp = (2 * ncf + 7) / 8 * 8;
+  kp = (2 * ncf + 3) / 4 * 4;
+}
+
+size_t trans_matrix_bytes(int p, int nclasses)
+{
+  int ncf, rp, kp;
+  trans_dims(p, ncf, rp, kp);
+  return (size_t)(nclasses + 16) * rp * kp * sizeof(double);
+}
+
+size_t trans_scratch_bytes(int p, int npairs, int nrhs)
+{
+  int ncf, rp, kp;
+  trans_dims(p, ncf, rp, kp);
+  return (size_t)(npairs > 0 ? npairs : 1) * nrhs * rp * sizeof(double);
+}
+
+static size_t gemm_smem(int rp) { return ((size_t)rp * TSTR + (size_t)KC * XS) * sizeof(double); }
+
+// warp arrangement: nwm row groups so that each warp holds <= 24 m-tiles
+static int gemm_nwm(int rp)
+{
+  int mt = rp / 8;
+  return mt <= 24 ? 1 : (mt <= 48 ? 2 : 4);
+}
+
+bool trans_supported(int p)
+{
+  int ncf, rp, kp;
+  trans_dims(p, ncf, rp, kp);
+  return rp / 8 <= 96 && gemm_smem(rp) <= 200 * 1024;
+}
+
+// T layout: [0, nclasses) M2L classes, [nclasses, +8) M2M, [nclasses+8, +8) L2L
+cudaError_t launch_trans_build(const qbxfmm_geometry& g, int p, double* T, cudaStream_t st)
+{
+  int ncf, rp, kp;
+  trans_dims(p, ncf, rp, kp);
+  size_t sh = (size_t)(2 * p + 1) * (2 * p + 2) / 2 * sizeof(double2);
+  size_t stride = (size_t)rp * kp;
+  if (g.m2l_nclasses > 0)
+    k_trans_build<<<g.m2l_nclasses, NT, sh, st>>>(0, p, ncf, rp, kp, g.m2l_nclasses,
+                                                   g.m2l_class_offsets, T);
+  k_trans_build<<<8, NT, sh, st>>>(1, p, ncf, rp, kp, 8, nullptr, T + g.m2l_nclasses * stride);
+  k_trans_build<<<8, NT, sh, st>>>(2, p, ncf, rp, kp, 8, nullptr, T + (g.m2l_nclasses + 8) * stride);
+  return cudaGetLastError();
+}
+
+static cudaError_t gemm_launch(const qbxfmm_geometry& g, int p, int nrhs, const double* T,
+                               int mat_base, int mat_mod, const int32_t* group_starts_dev,
+                               int g0, int ngroups, int maxcols, const int32_t* pair_src,
+                               const int32_t* pair_dst, const double2* ein, double2* eout,
+                               double scale, double* cpair, int32_t* err, cudaStream_t st)
+{
+  if (ngroups <= 0 || maxcols <= 0) return cudaSuccess;
+  int ncf, rp, kp;
+  trans_dims(p, ncf, rp, kp);
+  size_t sh = gemm_smem(rp);
+  int nwm = gemm_nwm(rp);
+  int ntile = 8 * (4 / nwm);
+  int mtw = (rp / 8 + nwm - 1) / nwm;
+  dim3 grid((maxcols + ntile - 1) / ntile, ngroups);
+#define QBX_GEMM_CASE(W)                                                                        \
+  if (mtw <= W) {                                                                               \
+    cudaFuncSetAttribute(k_trans_gemm<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh); \
+    k_trans_gemm<W><<<grid, NT, sh, st>>>(ncf, rp, kp, nrhs, nwm, T, mat_base, mat_mod,         \
+                                          group_starts_dev, g0, pair_src, pair_dst, ein, eout,  \
+                                          scale, cpair, err, g.nboxes);                         \
+    return cudaGetLastError();                                                                  \
+  }
+  QBX_GEMM_CASE(8)
+  QBX_GEMM_CASE(12)
+  QBX_GEMM_CASE(16)
+  QBX_GEMM_CASE(20)
+  QBX_GEMM_CASE(24)
+#undef QBX_GEMM_CASE
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_m2l_gemm(const qbxfmm_geometry& g, const TransHost& th, int p, int nrhs,
+                            const double* T, const double2* mp, double2* lo, double* cpair,
+                            int32_t* err, cudaStream_t st)
+{
+  if (g.m2l_nclasses == 0) return cudaSuccess;
+  int ncf, rp, kp;
+  trans_dims(p, ncf, rp, kp);
+  cudaError_t e = gemm_launch(g, p, nrhs, T, 0, 0, g.m2l_class_starts, 0, g.m2l_nclasses,
+                              th.m2l_max_pairs * nrhs, g.m2l_pair_src, nullptr, mp, nullptr, 1.0,
+                              cpair, err, st);
+  if (e != cudaSuccess) return e;
+  k_trans_reduce<<<dim3(g.nttp_boxes, nrhs), NT, 0, st>>>(
+      ncf, rp, nrhs, g.target_or_target_parent_boxes, 0, g.m2l_tgt_pair_starts, g.m2l_tgt_pairs,
+      cpair, lo, 1, g.box_levels, g.root_extent);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_m2m_gemm(const qbxfmm_geometry& g, const TransHost& th, int p, int nrhs,
+                            const double* T, double2* mp, double* cpair, int32_t* err,
+                            cudaStream_t st)
+{
+  int ncf, rp, kp;
+  trans_dims(p, ncf, rp, kp);
+  const int nch = 8;
+  for (int lev = g.nlevels - 2; lev >= 0; --lev) {
+    int g0 = lev * nch;
+    int maxp = th.m2m_level_max_group[lev];
+    if (maxp == 0) continue;
+    cudaError_t e = gemm_launch(g, p, nrhs, T, g.m2l_nclasses, nch, g.m2m_group_starts, g0, nch,
+                                maxp * nrhs, g.m2m_pair_src, nullptr, mp, nullptr, 1.0, cpair,
+                                err, st);
+    if (e != cudaSuccess) return e;
+    int i0 = th.lvl_source_parent[lev], i1 = th.lvl_source_parent[lev + 1];
+    if (i1 > i0)
+      k_trans_reduce<<<dim3(i1 - i0, nrhs), NT, 0, st>>>(ncf, rp, nrhs, g.source_parent_boxes, i0,
+                                                         g.m2m_par_pair_starts, g.m2m_par_pairs,
+                                                         cpair, mp, 0, g.box_levels, g.root_extent);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+cudaError_t launch_l2l_gemm(const qbxfmm_geometry& g, const TransHost& th, int p, int nrhs,
+                            const double* T, double2* lo, int32_t* err, cudaStream_t st)
+{
+  const int nch = 8;
+  for (int lev = 1; lev < g.nlevels; ++lev) {
+    int g0 = lev * nch;
+    int maxp = th.l2l_level_max_group[lev];
+    if (maxp == 0) continue;
+    cudaError_t e = gemm_launch(g, p, nrhs, T, g.m2l_nclasses + 8, nch, g.l2l_group_starts, g0, nch,
+                                maxp * nrhs, g.l2l_pair_src, g.l2l_pair_dst, lo, lo, 1.0, nullptr,
+                                err, st);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+// }}}
+
+}  // namespace qbx

@@ -14,6 +14,15 @@
 
 namespace qbx {
 
+// decode a 3D coefficient index -> (n, m) for the triangular layout idx3(n, m)
+QBX_HD void decode3(int c, int& n, int& m)
+{
+  n = (int)((sqrt(8.0 * c + 1.0) - 1.0) * 0.5);
+  while ((n + 1) * (n + 2) / 2 <= c) ++n;
+  while (n * (n + 1) / 2 > c) --n;
+  m = c - n * (n + 1) / 2;
+}
+
 // {{{ 3D single entries by recurrence along n (used where a thread owns one coefficient)
 
 QBX_D double2 sh3_R_nm(int n, int m, double x, double y, double z)

@@ -173,7 +173,7 @@ class Plan:
         native.call(name, self.handle, *args)
 
     def workspace_sizes(self):
-        sizes = (ctypes.c_size_t * 6)()
+        sizes = (ctypes.c_size_t * 8)()
         self.call("qbxfmm_workspace_sizes", sizes)
         return list(sizes)
 
@@ -455,7 +455,7 @@ class QBXApply:
     def __init__(self, geo: QBXFMMGeometryData, spec: SourceKernelSpec, qbx_order: int,
                  fmm_order: int, nrhs: int = 1, device="cuda",
                  device_geometry: DeviceGeometry | None = None,
-                 target_specific_qbx: bool = False):
+                 target_specific_qbx: bool = False, translation_matrices: bool = True):
         self.geo = geo
         self.device = torch.device(device)
         self.dgeo = device_geometry or DeviceGeometry(geo, device)
@@ -464,13 +464,22 @@ class QBXApply:
                          target_specific_qbx=target_specific_qbx)
         self.nrhs = nrhs
         sizes = self.plan.workspace_sizes()
+        use_mats = translation_matrices and sizes[6] > 0
         self._ws_tensors = [torch.zeros(max(s, 8) // 8 + 1, dtype=torch.float64,
-                                        device=self.device) for s in sizes]
+                                        device=self.device) for s in sizes[:6]]
+        self._mat_tensors = [torch.zeros(s // 8 + 1, dtype=torch.float64, device=self.device)
+                             for s in sizes[6:]] if use_mats else []
         self.error_word = torch.zeros(1, dtype=torch.int32, device=self.device)
         ptrs = [ctypes.c_void_p(_ptr(t)) for t in self._ws_tensors]
+        mats = ([ctypes.c_void_p(_ptr(t)) for t in self._mat_tensors] if use_mats
+                else [ctypes.c_void_p(0), ctypes.c_void_p(0)])
         self.ws = abi.QBXFMMWorkspace(
             *ptrs, ctypes.cast(ctypes.c_void_p(_ptr(self.error_word)),
-                               ctypes.POINTER(ctypes.c_int32)))
+                               ctypes.POINTER(ctypes.c_int32)), *mats)
+        self.uses_translation_matrices = use_mats
+        if use_mats:
+            self.plan.call("qbxfmm_precompute_translations", ctypes.byref(self.ws),
+                           _stream_handle())
         self.ndofs = geo.discr.ndofs
         self.nuser_targets = self.dgeo.nuser_targets
         self.dtype = torch.complex128 if spec.is_complex else torch.float64

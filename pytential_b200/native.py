@@ -38,6 +38,7 @@ _STAGES = {
     "qbxfmm_eval_target_specific_qbx_locals": [_vp, _vp, _pi, _vp],
     "qbxfmm_assemble": [_vp, _vp, _vp, _vp],
     "qbxfmm_workspace_sizes": [ctypes.POINTER(ctypes.c_size_t)],
+    "qbxfmm_precompute_translations": [ctypes.POINTER(abi.QBXFMMWorkspace), _vp],
     "qbxfmm_apply": [ctypes.POINTER(abi.QBXFMMUpsample), ctypes.POINTER(abi.QBXFMMWorkspace),
                      _vp, _vp, _vp],
     "qbxfmm_apply_host": [ctypes.POINTER(abi.QBXFMMUpsample),
