@@ -118,6 +118,21 @@ int qbxfmm_apply_host(const qbxfmm_plan* plan, const qbxfmm_upsample* up,
                       const qbxfmm_workspace* ws, const void* density_host, void* out_host,
                       void* density_dev, void* out_dev, void* stream);
 
+/* Size of the device array qbxfmm_apply_noalloc works in (64 MiB). */
+#define QBXFMM_NOALLOC_SCRATCH_BYTES (64u << 20)
+
+/* The whole apply (as qbxfmm_apply) for callers that cannot allocate device memory:
+ * the caller passes only the density and the output; the intermediate arrays live
+ * in a fixed device array of QBXFMM_NOALLOC_SCRATCH_BYTES inside the library, kept by
+ * every GPU that loads it until the process exits.  No counterpart in the
+ * reference (pytential allocates through its array context).  The first call on a
+ * device resolves that array's address and should come before any stream capture;
+ * calls that overlap on the GPU share the array and race; problems that need more
+ * scratch are rejected with QBXFMM_ERR_ARG before any launch.  Uses the per-pair
+ * translation kernels. */
+int qbxfmm_apply_noalloc(const qbxfmm_plan* plan, const qbxfmm_upsample* up,
+                         const void* density, void* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

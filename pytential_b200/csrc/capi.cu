@@ -61,6 +61,29 @@ int check_plan(const qbxfmm_plan* p)
 
 }  // namespace
 
+namespace qbx {
+
+// Byte sizes of the first six workspace buffers (no device access), for the
+// allocation-free entry point.
+int plan_base_workspace_sizes(const qbxfmm_plan* p, size_t* sizes6)
+{
+  if (int rc = check_plan(p)) return rc;
+  const qbxfmm_geometry& g = p->geo;
+  size_t nr = (size_t)p->kern.nrhs;
+  size_t scal = (p->kern.family == QBXFMM_LAPLACE) ? sizeof(double) : 2 * sizeof(double);
+  sizes6[0] = nr * g.nsources * scal;
+  sizes6[1] = (size_t)g.nboxes * nr * p->ncf * 2 * sizeof(double);
+  sizes6[2] = sizes6[1];
+  sizes6[3] = (size_t)g.ncenters * nr * p->ncq * 2 * sizeof(double);
+  sizes6[4] = nr * (size_t)(g.nfiltered_targets > 0 ? g.nfiltered_targets : 1) * scal;
+  sizes6[5] = nr * (size_t)g.ntargets * scal;
+  return QBXFMM_OK;
+}
+
+int set_last_error(int code, const std::string& msg) { return fail(code, msg); }
+
+}  // namespace qbx
+
 extern "C" {
 
 int qbxfmm_version(void) { return 1; }

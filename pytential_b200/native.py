@@ -41,6 +41,7 @@ _STAGES = {
     "qbxfmm_precompute_translations": [ctypes.POINTER(abi.QBXFMMWorkspace), _vp],
     "qbxfmm_apply": [ctypes.POINTER(abi.QBXFMMUpsample), ctypes.POINTER(abi.QBXFMMWorkspace),
                      _vp, _vp, _vp],
+    "qbxfmm_apply_noalloc": [ctypes.POINTER(abi.QBXFMMUpsample), _vp, _vp, _vp],
     "qbxfmm_apply_host": [ctypes.POINTER(abi.QBXFMMUpsample),
                           ctypes.POINTER(abi.QBXFMMWorkspace), _vp, _vp, _vp, _vp, _vp],
 }
