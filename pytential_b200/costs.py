@@ -63,22 +63,96 @@ def p2p_pairs(arrays: dict, scalars: dict) -> int:
     return int((nt * nsrc).sum())
 
 
-def apply_launch_count(scalars: dict, arrays: dict) -> int:
-    """Kernels of this library launched by one qbxfmm_apply."""
+def apply_launch_count(scalars: dict, arrays: dict, matrices: bool = False,
+                       tsqbx: bool = False) -> int:
+    """Kernels of this library launched by one qbxfmm_apply (3D matrix-form
+    translations when ``matrices``; target-specific near field when ``tsqbx``)."""
     nl = scalars["nlevels"]
     lsp = arrays["level_start_source_parent_box_nrs"]
     lttp = arrays["level_start_ttp_box_nrs"]
+    nch = 2 ** scalars["dim"]
     n = 1                                                   # strengths
     n += scalars["nsource_boxes"] > 0                       # P2M
-    n += sum(1 for lev in range(nl - 1) if lsp[lev + 1] > lsp[lev])   # M2M
-    nf = scalars["nfiltered_targets"] > 0 and scalars["ntarget_boxes"] > 0
+    if matrices:
+        mg = arrays["m2m_group_starts"]
+        lg = arrays["l2l_group_starts"]
+        for lev in range(nl - 1):
+            if mg[(lev + 1) * nch] > mg[lev * nch]:
+                n += 1                                      # M2M products
+                n += lsp[lev + 1] > lsp[lev]                # M2M reduction
+        n += 2 * (scalars["m2l_nclasses"] > 0)              # M2L products + reduction
+        n += sum(1 for lev in range(1, nl) if lg[(lev + 1) * nch] > lg[lev * nch])  # L2L
+    else:
+        n += sum(1 for lev in range(nl - 1) if lsp[lev + 1] > lsp[lev])   # M2M
+        n += scalars["nttp_boxes"] > 0                      # M2L
+        n += sum(1 for lev in range(1, nl) if lttp[lev + 1] > lttp[lev])  # L2L
+    nf = scalars["nnonqbx_chunks"] > 0
     n += nf                                                 # P2P
-    n += scalars["nttp_boxes"] > 0                          # M2L
     n += nf                                                 # M2P
     n += scalars["nttp_boxes"] > 0                          # P2L
-    n += sum(1 for lev in range(1, nl) if lttp[lev + 1] > lttp[lev])  # L2L
     n += nf                                                 # L2P
-    n += 2 * (scalars["nqbx_chunks"] > 0)                   # P2QBXL, M2QBXL
+    if tsqbx:
+        n += scalars["ntsqbx_chunks"] > 0                   # target-specific near field
+    else:
+        n += scalars["nqbx_chunks"] > 0                     # P2QBXL
+    n += scalars["nqbx_chunks"] > 0                         # M2QBXL
     n += 2 * (scalars["nglobal_qbx_centers"] > 0)           # L2QBXL, QBXL2P
     n += (scalars["ntargets"] > 0) + (scalars["nfiltered_targets"] > 0)  # assembly
     return int(n)
+
+
+def tsqbx_flops_per_pair(dim: int, q: int, charge: bool, dipole: bool) -> int:
+    """Target-specific near field per (target, source) pair: prelude 15 (b = s - c,
+    |b|^2, 1/|b|, cos), per order n Legendre and derivative recurrences 9 and
+    accumulation 2 (single layer) / 6 (double layer), final dot products 12."""
+    if dim == 3:
+        return 15 + (q + 1) * (9 * dipole + 3 * charge + 2 * charge + 6 * dipole) + 12 * dipole
+    return 15 + q * (6 + 2 * charge + 2 * dipole) + 8
+
+
+def tsqbx_pairs(arrays: dict, scalars: dict) -> int:
+    """(QBX target, list-1 source) pairs of the target-specific near field."""
+    n = scalars.get("ntsqbx_chunks", 0)
+    if n == 0:
+        return 0
+    tb = arrays["tsqbx_chunk_target_box"][:n].astype(np.int64)
+    cnt = arrays["tsqbx_chunk_count"][:n].astype(np.int64)
+    l1s = arrays["list1_starts"].astype(np.int64)
+    c = arrays["box_source_counts_nonchild"][arrays["list1_lists"]].astype(np.int64)
+    csum = np.concatenate([[0], np.cumsum(c)])
+    nsrc = csum[l1s[1:]] - csum[l1s[:-1]]
+    return int((cnt * nsrc[tb]).sum())
+
+
+def m2qbxl_flops_per_pair(pf: int, q: int) -> int:
+    """3D Laplace multipole (order pf) -> QBX local (order q) per (center, box) pair:
+    singular-harmonic table to order pf + q (9 flops per entry) and 8 flops per
+    complex multiply-add over the (q+1)(q+2)/2 outputs x (pf+1)^2 inputs."""
+    nt = (pf + q + 1) * (pf + q + 2) // 2
+    return 9 * nt + 8 * ncoeff_laplace(3, q) * (pf + 1) ** 2
+
+
+def m2qbxl_pairs(arrays: dict, scalars: dict) -> int:
+    gc = arrays["global_qbx_centers"][:scalars["nglobal_qbx_centers"]]
+    if len(gc) == 0:
+        return 0
+    tb = arrays["qbx_center_to_target_box"][gc]
+    n3 = np.diff(arrays["list3_starts"].astype(np.int64))
+    return int(n3[tb].sum())
+
+
+def m2l_matrix_flops(arrays: dict, scalars: dict, p: int, nrhs: int = 1) -> int:
+    """Real translation-matrix products: 2 (2 ncoeff)^2 flops per list-2 pair."""
+    r = 2 * ncoeff_laplace(3, p)
+    npairs = int(arrays["m2l_class_starts"][scalars["m2l_nclasses"]]) if scalars["m2l_nclasses"] else 0
+    return 2 * r * r * npairs * nrhs
+
+
+def p2l_flops(arrays: dict, scalars: dict, p: int, charge: bool, dipole: bool) -> int:
+    """3D list-4 P2L: harmonic table to order p+1 (9 flops per entry) + per
+    coefficient 4 (single layer) / 20 (double layer) flops, per (box, source) pair."""
+    l4s = arrays["list4_starts"].astype(np.int64)
+    c = arrays["box_source_counts_nonchild"][arrays["list4_lists"]].astype(np.int64)
+    npairs = int(c.sum()) if len(l4s) > 1 and l4s[-1] > 0 else 0
+    nt = (p + 2) * (p + 3) // 2
+    return npairs * (9 * nt + ncoeff_laplace(3, p) * (4 * charge + 20 * dipole))
