@@ -67,15 +67,60 @@ def config_dict(wl, args, extra=None):
 # {{{ clocks
 
 class ClockSampler:
+    """SM clock and clock-event reasons sampled during the timed region.
+
+    Polls NVML (read-only queries) every 5 ms from a thread; falls back to
+    ``nvidia-smi -lms 200`` when NVML is unavailable."""
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", 0x8), ("sw_thermal_slowdown", 0x20),
+               ("hw_thermal_slowdown", 0x40), ("sw_power_cap", 0x4),
+               ("hw_power_brake_slowdown", 0x80))
 
     def __init__(self, index):
         self.index = index
         self.proc = None
+        self.thread = None
+        self.samples = []          # (sm_mhz, reason bitmask)
+        self.sm_max = None
+        self.lines = []
+
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            uuid = str(torch.cuda.get_device_properties(self.index).uuid)
+            if not uuid.startswith("GPU-"):
+                uuid = "GPU-" + uuid
+            return pynvml, pynvml.nvmlDeviceGetHandleByUUID(uuid)
+        except Exception:
+            vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+            idx = int(vis.split(",")[self.index]) if vis and vis.split(",")[self.index].isdigit() \
+                else self.index
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(idx)
+
+    def _poll(self, pynvml, h):
+        while not self.stop.is_set():
+            try:
+                sm = pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)
+                rs = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.samples.append((float(sm), int(rs)))
+            except Exception:
+                pass
+            self.stop.wait(0.005)
 
     def __enter__(self):
+        import threading
+        try:
+            pynvml, h = self._nvml_handle()
+            self.sm_max = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+            self.stop = threading.Event()
+            self.thread = threading.Thread(target=self._poll, args=(pynvml, h), daemon=True)
+            self.thread.start()
+            return self
+        except Exception:
+            self.thread = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
@@ -86,7 +131,9 @@ class ClockSampler:
         return self
 
     def __exit__(self, *exc):
-        self.lines = []
+        if self.thread is not None:
+            self.stop.set()
+            self.thread.join()
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -97,8 +144,13 @@ class ClockSampler:
             self.lines = [ln for ln in out.splitlines() if ln.strip()]
 
     def summary(self):
+        if self.samples:
+            reasons = {nm for nm, bit in self.REASONS for _, rs in self.samples if rs & bit}
+            return {"sm_mhz": statistics.median(s for s, _ in self.samples),
+                    "sm_max_mhz": self.sm_max, "reasons": sorted(reasons),
+                    "samples": len(self.samples), "source": "nvml, 5 ms"}
         if not self.lines:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["clock sampling unavailable"]}
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for ln in self.lines:
@@ -112,9 +164,29 @@ class ClockSampler:
                 if v.lower() == "active":
                     reasons.add(nm)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "source": "nvidia-smi, 200 ms"}
 
 # }}}
+
+
+KERNEL_SYMBOLS = {
+    "target-specific near field (eval_target_specific_qbx_locals)": "k_tsqbx",
+    "M2QBXL (translate_box_multipoles_to_qbx_local)": "k_m2qbxl",
+    "P2L list 4 (form_locals)": "k_p2l",
+    "P2QBXL (form_global_qbx_locals)": "k_p2qbxl",
+}
+
+
+def ncu_traffic(label):
+    """DRAM bytes per launch of a kernel from the committed ncu capture summary
+    (``profiles/ncu_dram_bytes.json``), or None."""
+    try:
+        with open(os.path.join(os.path.dirname(os.path.abspath(__file__)),
+                               "profiles", "ncu_dram_bytes.json")) as f:
+            data = json.load(f)
+        return data["bytes_per_launch"].get(KERNEL_SYMBOLS.get(label, ""))
+    except (OSError, ValueError, KeyError):
+        return None
 
 
 def cpu_reference(wl, reps, threads):
@@ -265,6 +337,7 @@ def run_b200(args):
     in_step = {k: v for k, v in ktimes.items() if not k.startswith("P2QBXL")}
     dom = max(in_step, key=lambda k: in_step[k][0])
     k_ms, k_flops = in_step[dom]
+    traffic = ncu_traffic(dom)
     fp64_peak = measure_fp64_peak(torch, dev)
 
     # end to end through the public host-buffer entry (H2D + apply + D2H + sync)
@@ -302,7 +375,9 @@ def run_b200(args):
                 "frac": (k_flops / (k_ms * 1e-3) / 1e12) / fp64_peak,
                 "peak_source": "measured here: cuBLAS float64 GEMM 8192^3, best of 5",
                 "algorithmic_flops_per_launch": k_flops, "kernel_ms": k_ms,
-                "share_of_step": k_ms / (1e3 * t_max / K), "traffic": None,
+                "share_of_step": k_ms / (1e3 * t_max / K), "traffic": traffic,
+                "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum, one launch, "
+                                   "profiles/ncu_dram_bytes.json") if traffic else None,
                 "kernels_ms": {k: round(v[0], 4) for k, v in ktimes.items()},
                 "kernels_tflops": {k: round(v[1] / (v[0] * 1e-3) / 1e12, 3)
                                    for k, v in ktimes.items()}},
