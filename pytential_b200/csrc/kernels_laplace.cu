@@ -8,8 +8,12 @@
 // streams that box's list-1 sources through shared memory in tiles of 128.
 #include <algorithm>
 
+#include <cooperative_groups.h>
+
 #include "laplace.cuh"
 #include "kernels.h"
+
+namespace cg = cooperative_groups;
 
 namespace qbx {
 
@@ -126,14 +130,21 @@ QBX_D void load_stream_tile(const qbxfmm_geometry& g, const double* __restrict__
 // {{{ P2M (form_multipoles, fmm.py:441-445)
 
 // tables of R_n^m((y - c)/rho) for SUB sources at a time, one thread per column
+// The per-source tables are stored entry-major, tab[entry * P2M_TS + source]: the lanes
+// building one column write consecutive words, and the padded stride spreads the
+// lanes that read different entries of one source over the banks.
+constexpr int P2M_SUB = 16;
+constexpr int P2M_TS = P2M_SUB + 1;
+
 template <int DIM>
 __global__ void __launch_bounds__(NT)
 k_p2m(qbxfmm_geometry g, SourceCoeffs sc, int p, int ncf, int nrhs,
       const double* __restrict__ strengths, double2* __restrict__ mpoles)
 {
-  constexpr int SUB = 16;
+  constexpr int SUB = P2M_SUB;
+  constexpr int TS = P2M_TS;
   extern __shared__ double2 smem2[];
-  double2* tab = smem2;                                  // [SUB][ncf]
+  double2* tab = smem2;                                  // [ncf][TS]
   __shared__ double s_u[SUB][3], s_n[SUB][3], s_q[SUB];
 
   int b = g.source_boxes[blockIdx.x];
@@ -145,6 +156,32 @@ k_p2m(qbxfmm_geometry g, SourceCoeffs sc, int p, int ncf, int nrhs,
   int s0 = g.box_source_starts[b];
   int ns = g.box_source_counts_nonchild[b];
   const double* st = strengths + (size_t)r * g.nsources;
+  const bool dip = sc.cd != 0.0;
+
+  // per-thread coefficient bookkeeping (3D): table offsets of R_n^m and of the dipole
+  // neighbours R_{n-1}^m, R_{n-1}^{m-1}, R_{n-1}^{m+1} (weight 0 where outside the
+  // table; R_{n-1}^{-1} = -conj(R_{n-1}^1))
+  int o_nm[2], o_a[2], o_b[2], o_c[2];
+  double w_a[2], w_b[2], w_c[2];
+  bool valid[2];
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    int ci = threadIdx.x + h * NT;
+    valid[h] = ci < ncf;
+    o_nm[h] = o_a[h] = o_b[h] = o_c[h] = 0;
+    w_a[h] = w_b[h] = w_c[h] = 0.0;
+    if (DIM == 3 && valid[h]) {
+      int n, m;
+      decode3(ci, n, m);
+      o_nm[h] = idx3(n, m) * TS;
+      if (n >= 1) {
+        if (m <= n - 1) { o_a[h] = idx3(n - 1, m) * TS; w_a[h] = 1.0; }
+        if (m >= 1) { o_b[h] = idx3(n - 1, m - 1) * TS; w_b[h] = 1.0; }
+        else if (n - 1 >= 1) { o_b[h] = idx3(n - 1, 1) * TS; w_b[h] = -1.0; }
+        if (m + 1 <= n - 1) { o_c[h] = idx3(n - 1, m + 1) * TS; w_c[h] = 1.0; }
+      }
+    }
+  }
 
   double2 acc[2] = {c2(0.0), c2(0.0)};
   for (int base = 0; base < ns; base += SUB) {
@@ -155,7 +192,7 @@ k_p2m(qbxfmm_geometry g, SourceCoeffs sc, int p, int ncf, int nrhs,
       load_point<DIM>(g.sources, g.nsources, s, y);
 #pragma unroll
       for (int d = 0; d < DIM; ++d) s_u[threadIdx.x][d] = (y[d] - c[d]) * rinv;
-      if (sc.cd != 0.0) {
+      if (dip) {
         double nv[3];
         load_point<DIM>(g.source_normals, g.nsources, s, nv);
 #pragma unroll
@@ -166,19 +203,19 @@ k_p2m(qbxfmm_geometry g, SourceCoeffs sc, int p, int ncf, int nrhs,
     __syncthreads();
     if (DIM == 3) {
       for (int w = threadIdx.x; w < cnt * (p + 1); w += NT) {
-        int j = w / (p + 1), m = w - j * (p + 1);
+        int m = w / cnt, j = w - m * cnt;
         // column m of R for source j
         double x = s_u[j][0], y = s_u[j][1], z = s_u[j][2];
         double r2 = x * x + y * y + z * z;
         double2 a = c2(1.0);
         for (int k = 1; k <= m; ++k) a = cscale(0.5 * rcp(k), cmul(a, c2(x, y)));
-        double2* T = tab + (size_t)j * ncf;
-        T[idx3(m, m)] = a;
+        double2* T = tab + j;
+        T[idx3(m, m) * TS] = a;
         double2 prev = c2(0.0);
         for (int n = m + 1; n <= p; ++n) {
           double2 bb = cscale(rcp(n + m) * rcp(n - m),
                               csub(cscale((2.0 * n - 1) * z, a), cscale(r2, prev)));
-          T[idx3(n, m)] = bb;
+          T[idx3(n, m) * TS] = bb;
           prev = a;
           a = bb;
         }
@@ -186,10 +223,10 @@ k_p2m(qbxfmm_geometry g, SourceCoeffs sc, int p, int ncf, int nrhs,
     } else {
       for (int j = threadIdx.x; j < cnt; j += NT) {
         double2 u = c2(s_u[j][0], s_u[j][1]);
-        double2* T = tab + (size_t)j * ncf;
+        double2* T = tab + j;
         double2 a = c2(1.0);
         for (int k = 0; k <= p; ++k) {
-          T[k] = a;  // u^k
+          T[k * TS] = a;  // u^k
           a = cmul(a, u);
         }
       }
@@ -197,38 +234,39 @@ k_p2m(qbxfmm_geometry g, SourceCoeffs sc, int p, int ncf, int nrhs,
     __syncthreads();
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
+      if (!valid[h]) continue;
       int ci = threadIdx.x + h * NT;
-      if (ci >= ncf) break;
       double2 a = acc[h];
       if (DIM == 3) {
-        int n, m;
-        decode3(ci, n, m);
         for (int j = 0; j < cnt; ++j) {
-          const double2* T = tab + (size_t)j * ncf;
+          const double2* T = tab + j;
           double q = s_q[j];
-          a = caxpy(sc.cq * q, cconj(T[idx3(n, m)]), a);
-          if (sc.cd != 0.0 && n >= 1) {
+          a = caxpy(sc.cq * q, cconj(T[o_nm[h]]), a);
+          if (dip) {
             double f = sc.cd * q * rinv;
             double dx = s_n[j][0], dy = s_n[j][1], dz = s_n[j][2];
             // conj(dz R_{n-1}^m + (dx+idy)/2 R_{n-1}^{m-1} - (dx-idy)/2 R_{n-1}^{m+1})
-            double2 v = cscale(dz, sh3_get(T, n - 1, m));
-            v = cfma(c2(0.5 * dx, 0.5 * dy), sh3_get(T, n - 1, m - 1), v);
-            v = cfma(c2(-0.5 * dx, 0.5 * dy), sh3_get(T, n - 1, m + 1), v);
+            double2 tb_ = T[o_b[h]];
+            if (w_b[h] < 0) tb_ = c2(-tb_.x, tb_.y);
+            else tb_ = cscale(w_b[h], tb_);
+            double2 v = cscale(dz * w_a[h], T[o_a[h]]);
+            v = cfma(c2(0.5 * dx, 0.5 * dy), tb_, v);
+            v = cfma(c2(-0.5 * dx * w_c[h], 0.5 * dy * w_c[h]), T[o_c[h]], v);
             a = caxpy(f, cconj(v), a);
           }
         }
       } else {
         int k = ci;
         for (int j = 0; j < cnt; ++j) {
-          const double2* T = tab + (size_t)j * ncf;
+          const double2* T = tab + j;
           double q = s_q[j];
           if (k == 0) {
             a.x += sc.cq * q;
           } else {
-            a = caxpy(-sc.cq * q * rcp(k), T[k], a);
-            if (sc.cd != 0.0) {
+            a = caxpy(-sc.cq * q * rcp(k), T[k * TS], a);
+            if (dip) {
               double2 nu = c2(s_n[j][0], s_n[j][1]);
-              a = cfma(cscale(-sc.cd * q * rinv, nu), T[k - 1], a);
+              a = cfma(cscale(-sc.cd * q * rinv, nu), T[(k - 1) * TS], a);
             }
           }
         }
@@ -533,18 +571,24 @@ k_m2l2(qbxfmm_geometry g, int p, int ncf, int nrhs, const double2* __restrict__ 
 // One CTA per target-or-parent box; its list-4 sources stream through shared memory
 // in sub-tiles of SUB; per sub-tile each source's singular-harmonic table (orders
 // 0..p+1) is built by one thread per (source, column), then each thread accumulates
-// its coefficient(s) with precomputed table offsets.
+// its coefficient(s) with precomputed table offsets.  The tables are stored
+// entry-major, tab[entry * P2L_TS + source], so the lanes of a warp building one
+// column write consecutive words, and the lanes reading different entries of one
+// source are spread over the banks by the padded stride.
+constexpr int P2L_SUB = 32;
+constexpr int P2L_TS = P2L_SUB + 1;
+
 template <int DIM>
 __global__ void __launch_bounds__(NT)
 k_p2l(qbxfmm_geometry g, SourceCoeffs sc, int p, int ncf, int nrhs,
       const double* __restrict__ strengths, double2* __restrict__ locals, int32_t* err)
 {
-  constexpr int SUB = 32;
+  constexpr int SUB = P2L_SUB;
+  constexpr int TS = P2L_TS;
   extern __shared__ double2 smem2[];
-  double2* tab = smem2;   // [SUB][nct]
+  double2* tab = smem2;   // [nct][TS]
   __shared__ double s_u[SUB][3], s_n[SUB][3], s_q[SUB];
   __shared__ int s_pref[MAXB + 1], s_start[MAXB];
-  const int nct = (DIM == 3) ? (p + 2) * (p + 3) / 2 : p + 3;
   int i = blockIdx.x;
   int tb = g.target_or_target_parent_boxes[i];
   int r = blockIdx.y;
@@ -569,11 +613,11 @@ k_p2l(qbxfmm_geometry g, SourceCoeffs sc, int p, int ncf, int nrhs,
     if (DIM == 3 && valid[h]) {
       int n, m;
       decode3(ci, n, m);
-      o_nm[h] = idx3(n, m);
-      o_a[h] = idx3(n + 1, m);
-      o_b[h] = idx3(n + 1, m > 0 ? m - 1 : 1);   // m = 0: S_{n+1}^{-1} = -conj(S_{n+1}^1)
+      o_nm[h] = idx3(n, m) * TS;
+      o_a[h] = idx3(n + 1, m) * TS;
+      o_b[h] = idx3(n + 1, m > 0 ? m - 1 : 1) * TS;   // m = 0: S_{n+1}^{-1} = -conj(S_{n+1}^1)
       sb_sign[h] = m > 0 ? 1.0 : -1.0;
-      o_c[h] = idx3(n + 1, m + 1);
+      o_c[h] = idx3(n + 1, m + 1) * TS;
     }
   }
 
@@ -604,18 +648,18 @@ k_p2l(qbxfmm_geometry g, SourceCoeffs sc, int p, int ncf, int nrhs,
       __syncthreads();
       if (DIM == 3) {
         for (int w = threadIdx.x; w < cnt * (p + 2); w += NT) {
-          int j = w / (p + 2), m = w - j * (p + 2);
+          int m = w / cnt, j = w - m * cnt;
           double x = s_u[j][0], y = s_u[j][1], z = s_u[j][2];
           double rinv2 = 1.0 / (x * x + y * y + z * z);
           double2 a = c2(sqrt(rinv2));
           for (int k = 1; k <= m; ++k) a = cscale((2.0 * k - 1) * rinv2, cmul(a, c2(x, y)));
-          double2* T = tab + (size_t)j * nct;
-          T[idx3(m, m)] = a;
+          double2* T = tab + j;
+          T[idx3(m, m) * TS] = a;
           double2 prev = c2(0.0);
           for (int n = m + 1; n <= p + 1; ++n) {
             double2 bb = cscale(rinv2, csub(cscale((2.0 * n - 1) * z, a),
                                             cscale((double)(n + m - 1) * (n - m - 1), prev)));
-            T[idx3(n, m)] = bb;
+            T[idx3(n, m) * TS] = bb;
             prev = a;
             a = bb;
           }
@@ -623,13 +667,14 @@ k_p2l(qbxfmm_geometry g, SourceCoeffs sc, int p, int ncf, int nrhs,
       } else {
         for (int j = threadIdx.x; j < cnt; j += NT) {
           double2 tinv = cinv(c2(s_u[j][0], s_u[j][1]));
-          double2* T = tab + (size_t)j * nct;
+          double2* T = tab + j;
           double2 a = c2(1.0);
           for (int k = 0; k <= p + 1; ++k) {
-            T[k] = a;   // tau^-k
+            T[k * TS] = a;   // tau^-k
             a = cmul(a, tinv);
           }
-          T[p + 2] = c2(0.5 * log((s_u[j][0] * s_u[j][0] + s_u[j][1] * s_u[j][1]) * rho * rho));
+          T[(p + 2) * TS] =
+              c2(0.5 * log((s_u[j][0] * s_u[j][0] + s_u[j][1] * s_u[j][1]) * rho * rho));
         }
       }
       __syncthreads();
@@ -639,7 +684,7 @@ k_p2l(qbxfmm_geometry g, SourceCoeffs sc, int p, int ncf, int nrhs,
         int ci = threadIdx.x + h * NT;
         double2 a = acc[h];
         for (int j = 0; j < cnt; ++j) {
-          const double2* T = tab + (size_t)j * nct;
+          const double2* T = tab + j;
           double q = s_q[j];
           if (DIM == 3) {
             a = caxpy(sc.cq * q * rinv, T[o_nm[h]], a);
@@ -655,11 +700,11 @@ k_p2l(qbxfmm_geometry g, SourceCoeffs sc, int p, int ncf, int nrhs,
             }
           } else {
             int l = ci;
-            if (l == 0) a.x += sc.cq * q * T[p + 2].x;
-            else a = caxpy(-sc.cq * q * rcp(l), T[l], a);
+            if (l == 0) a.x += sc.cq * q * T[(p + 2) * TS].x;
+            else a = caxpy(-sc.cq * q * rcp(l), T[l * TS], a);
             if (dip) {
               double2 nu = c2(s_n[j][0], s_n[j][1]);
-              a = cfma(cscale(sc.cd * q * rinv, nu), T[l + 1], a);
+              a = cfma(cscale(sc.cd * q * rinv, nu), T[(l + 1) * TS], a);
             }
           }
         }
@@ -740,18 +785,45 @@ k_l2l(qbxfmm_geometry g, int p, int ncf, int nrhs, int i0, double2* __restrict__
 
 // {{{ point evaluations at non-QBX targets: P2P (list 1), M2P (list 3), L2P
 
-// P2P over list 1 (eval_direct, fmm.py:461-466).  CTA = 4 warps over one chunk of
-// <= 32 non-QBX targets of a target box (lane = target); the list-1 sources stream
-// through shared memory in tiles of 128, each warp taking 32 of them.
+// P2P over list 1 (eval_direct, fmm.py:461-466).  A cluster of PSPLIT CTAs serves one
+// chunk of <= 32 non-QBX targets of a target box (lane = target): the list-1 sources
+// stream through shared memory in tiles of 128, tile t going to CTA t % PSPLIT of the
+// cluster and, within it, 32 sources to each warp.  The partial sums are combined in
+// a fixed order through distributed shared memory by CTA 0 of the cluster.
+constexpr int PSPLIT = 8;
+
+// Sum of acc over the CTA's warps and then over the cluster's CTAs, in a fixed order;
+// returns the total in lane t of warp 0 of CTA 0 (other threads: unspecified).
+QBX_D double cluster_lane_sum(double acc, double (*s_red)[32], double* s_part)
+{
+  cg::cluster_group cl = cg::this_cluster();
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();
+  if (warp > 0) s_red[warp - 1][lane] = acc;
+  __syncthreads();
+  if (warp == 0) {
+    for (int w = 1; w < NW; ++w) acc += s_red[w - 1][lane];
+    s_part[lane] = acc;
+  }
+  cl.sync();
+  if (cl.block_rank() == 0 && warp == 0) {
+    for (unsigned q = 1; q < cl.num_blocks(); ++q) acc += *cl.map_shared_rank(s_part + lane, q);
+  }
+  cl.sync();
+  return acc;
+}
+
 template <int DIM>
-__global__ void __launch_bounds__(NT)
+__global__ void __cluster_dims__(PSPLIT, 1, 1) __launch_bounds__(NT)
 k_eval_direct(qbxfmm_geometry g, SourceCoeffs sc, int nrhs, const double* __restrict__ strengths,
               double* __restrict__ pot, int32_t* err)
 {
   __shared__ double s_y[3][NT], s_n[3][NT], s_q[NT];
   __shared__ int s_pref[MAXB + 1], s_start[MAXB];
   __shared__ double s_red[NW - 1][32];
-  int chunk = blockIdx.x;
+  __shared__ double s_part[32];
+  int chunk = blockIdx.x / PSPLIT;
+  int part = blockIdx.x - chunk * PSPLIT;
   int r = blockIdx.y;
   int itb = g.nonqbx_chunk_target_box[chunk];
   int t0 = g.nonqbx_chunk_start[chunk];
@@ -764,13 +836,15 @@ k_eval_direct(qbxfmm_geometry g, SourceCoeffs sc, int nrhs, const double* __rest
   const bool dip = sc.cd != 0.0;
   double acc = 0.0;
   int l0 = g.list1_starts[itb], l1 = g.list1_starts[itb + 1];
+  int tile = 0;
   for (int gb = l0; gb < l1; gb += MAXB) {
     int nb = min(MAXB, l1 - gb);
     __syncthreads();
     list_prefix(g, g.list1_lists, gb, nb, s_pref, s_start, err);
     __syncthreads();
     int total = s_pref[nb];
-    for (int base = 0; base < total; base += NT) {
+    for (int base = 0; base < total; base += NT, ++tile) {
+      if (tile % PSPLIT != part) continue;
       if (dip) load_stream_tile<DIM, true>(g, st, total, nb, base, s_pref, s_start, s_y, s_n, s_q);
       else load_stream_tile<DIM, false>(g, st, total, nb, base, s_pref, s_start, s_y, s_n, s_q);
       __syncthreads();
@@ -801,26 +875,25 @@ k_eval_direct(qbxfmm_geometry g, SourceCoeffs sc, int nrhs, const double* __rest
       __syncthreads();
     }
   }
-  if (warp > 0) s_red[warp - 1][lane] = acc;
-  __syncthreads();
-  if (warp == 0 && active) {
-    for (int w = 1; w < NW; ++w) acc += s_red[w - 1][lane];
-    pot[(size_t)r * g.nfiltered_targets + t] += acc;
-  }
+  acc = cluster_lane_sum(acc, s_red, s_part);
+  if (part == 0 && warp == 0 && active) pot[(size_t)r * g.nfiltered_targets + t] += acc;
 }
 
-// M2P over list 3 (eval_multipoles, fmm.py:487-493).  Same chunking; the warps
-// split the list-3 boxes and stage each multipole in their own shared slice.
+// M2P over list 3 (eval_multipoles, fmm.py:487-493).  Same clusters; the list-3 boxes
+// are dealt round-robin to the PSPLIT x 4 warps, each staging its multipole in its own
+// shared slice.
 template <int DIM>
-__global__ void __launch_bounds__(NT)
+__global__ void __cluster_dims__(PSPLIT, 1, 1) __launch_bounds__(NT)
 k_eval_multipoles(qbxfmm_geometry g, int p, int ncf, int nrhs,
                   const double2* __restrict__ mpoles, double* __restrict__ pot, int32_t* err)
 {
   extern __shared__ double2 smem2[];
   __shared__ double s_red[NW - 1][32];
+  __shared__ double s_part[32];
   int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   double2* M = smem2 + (size_t)warp * ncf;
-  int chunk = blockIdx.x;
+  int chunk = blockIdx.x / PSPLIT;
+  int part = blockIdx.x - chunk * PSPLIT;
   int r = blockIdx.y;
   int itb = g.nonqbx_chunk_target_box[chunk];
   int t = g.nonqbx_chunk_start[chunk] + lane;
@@ -828,7 +901,8 @@ k_eval_multipoles(qbxfmm_geometry g, int p, int ncf, int nrhs,
   double x[3] = {0, 0, 0};
   if (active) load_point<DIM>(g.nonqbx_targets, g.nfiltered_targets, t, x);
   double acc = 0.0;
-  for (int li = g.list3_starts[itb] + warp; li < g.list3_starts[itb + 1]; li += NW) {
+  for (int li = g.list3_starts[itb] + part * NW + warp; li < g.list3_starts[itb + 1];
+       li += NW * PSPLIT) {
     int sb = g.list3_lists[li];
     if ((unsigned)sb >= (unsigned)g.nboxes) {
       report(err, QBX_DEVERR_BAD_BOX);
@@ -878,13 +952,8 @@ k_eval_multipoles(qbxfmm_geometry g, int p, int ncf, int nrhs,
       acc += sum.x;
     }
   }
-  __syncthreads();
-  if (warp > 0) s_red[warp - 1][lane] = acc;
-  __syncthreads();
-  if (warp == 0 && active) {
-    for (int w = 1; w < NW; ++w) acc += s_red[w - 1][lane];
-    pot[(size_t)r * g.nfiltered_targets + t] += acc;
-  }
+  acc = cluster_lane_sum(acc, s_red, s_part);
+  if (part == 0 && warp == 0 && active) pot[(size_t)r * g.nfiltered_targets + t] += acc;
 }
 
 template <int DIM>
@@ -1544,7 +1613,7 @@ static cudaError_t p2m_(const qbxfmm_geometry& g, SourceCoeffs sc, int p, int nr
                         const double* s, double2* mp, cudaStream_t st)
 {
   int ncf = (int)ncoef_dim(DIM, p);
-  size_t sh = 16 * (size_t)ncf * sizeof(double2);
+  size_t sh = (size_t)P2M_TS * ncf * sizeof(double2);
   if (g.nsource_boxes == 0) return cudaSuccess;
   cudaFuncSetAttribute(k_p2m<DIM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
   k_p2m<DIM><<<dim3(g.nsource_boxes, grid_y(nrhs)), NT, sh, st>>>(g, sc, p, ncf, nrhs, s, mp);
@@ -1604,7 +1673,7 @@ static cudaError_t p2l_(const qbxfmm_geometry& g, SourceCoeffs sc, int p, int nr
   if (g.nttp_boxes == 0) return cudaSuccess;
   int ncf = (int)ncoef_dim(DIM, p);
   int nct = DIM == 3 ? (p + 2) * (p + 3) / 2 : p + 3;
-  size_t sh = 32 * (size_t)nct * sizeof(double2);
+  size_t sh = (size_t)P2L_TS * nct * sizeof(double2);
   cudaFuncSetAttribute(k_p2l<DIM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
   k_p2l<DIM><<<dim3(g.nttp_boxes, grid_y(nrhs)), NT, sh, st>>>(g, sc, p, ncf, nrhs, s, lo, err);
   return cudaGetLastError();
@@ -1642,7 +1711,7 @@ cudaError_t launch_eval_direct(const qbxfmm_geometry& g, SourceCoeffs sc, int nr
                                const double* s, double* pot, int32_t* err, cudaStream_t st)
 {
   if (g.nnonqbx_chunks == 0) return cudaSuccess;
-  dim3 grid(g.nnonqbx_chunks, grid_y(nrhs));
+  dim3 grid(g.nnonqbx_chunks * PSPLIT, grid_y(nrhs));   // one cluster per chunk
   if (g.dim == 3) k_eval_direct<3><<<grid, NT, 0, st>>>(g, sc, nrhs, s, pot, err);
   else k_eval_direct<2><<<grid, NT, 0, st>>>(g, sc, nrhs, s, pot, err);
   return cudaGetLastError();
@@ -1654,7 +1723,7 @@ cudaError_t launch_eval_multipoles(const qbxfmm_geometry& g, int p, int nrhs, co
   if (g.nnonqbx_chunks == 0) return cudaSuccess;
   int ncf = (int)ncoef_dim(g.dim, p);
   size_t sh = (size_t)NW * ncf * sizeof(double2);
-  dim3 grid(g.nnonqbx_chunks, grid_y(nrhs));
+  dim3 grid(g.nnonqbx_chunks * PSPLIT, grid_y(nrhs));   // one cluster per chunk
   if (g.dim == 3) k_eval_multipoles<3><<<grid, NT, sh, st>>>(g, p, ncf, nrhs, mp, pot, err);
   else k_eval_multipoles<2><<<grid, NT, sh, st>>>(g, p, ncf, nrhs, mp, pot, err);
   return cudaGetLastError();
