@@ -20,8 +20,9 @@ _LIB = None
 
 def build(force: bool = False) -> str:
     path = os.path.join(_HERE, "liboracle.so")
-    src = os.path.join(_HERE, "qbxfmm_oracle.c")
-    if force or not os.path.exists(path) or os.path.getmtime(path) < os.path.getmtime(src):
+    srcs = [os.path.join(_HERE, f) for f in os.listdir(_HERE) if f.endswith(".c")]
+    if force or not os.path.exists(path) or \
+            os.path.getmtime(path) < max(os.path.getmtime(f) for f in srcs):
         subprocess.run(["make", "-s", "-C", _HERE, "liboracle.so"], check=True)
     return path
 

@@ -409,6 +409,23 @@ static int h2_assemble(const qbxfmm_kernel*, const qbxfmm_geometry*, const cplx*
 static int h2_apply(const qbxfmm_kernel*, const qbxfmm_geometry*, const cplx*, cplx*, int);
 /* }}} */
 
+/* {{{ 3D Helmholtz forward declarations (qbxfmm_oracle_helm3d.c) */
+static int h3_form_multipoles(const qbxfmm_kernel*, const qbxfmm_geometry*, const cplx*, cplx*);
+static int h3_coarsen_multipoles(const qbxfmm_kernel*, const qbxfmm_geometry*, cplx*);
+static int h3_eval_direct(const qbxfmm_kernel*, const qbxfmm_geometry*, const cplx*, cplx*);
+static int h3_multipole_to_local(const qbxfmm_kernel*, const qbxfmm_geometry*, const cplx*, cplx*);
+static int h3_eval_multipoles(const qbxfmm_kernel*, const qbxfmm_geometry*, const cplx*, cplx*);
+static int h3_form_locals(const qbxfmm_kernel*, const qbxfmm_geometry*, const cplx*, cplx*);
+static int h3_refine_locals(const qbxfmm_kernel*, const qbxfmm_geometry*, cplx*);
+static int h3_eval_locals(const qbxfmm_kernel*, const qbxfmm_geometry*, const cplx*, cplx*);
+static int h3_p2qbxl(const qbxfmm_kernel*, const qbxfmm_geometry*, const cplx*, cplx*, int);
+static int h3_m2qbxl(const qbxfmm_kernel*, const qbxfmm_geometry*, const cplx*, cplx*);
+static int h3_l2qbxl(const qbxfmm_kernel*, const qbxfmm_geometry*, const cplx*, cplx*);
+static int h3_eval_qbx_expansions(const qbxfmm_kernel*, const qbxfmm_geometry*, const cplx*, cplx*);
+static int h3_assemble(const qbxfmm_kernel*, const qbxfmm_geometry*, const cplx*, const cplx*, cplx*);
+static int h3_apply(const qbxfmm_kernel*, const qbxfmm_geometry*, const cplx*, cplx*, int);
+/* }}} */
+
 #define IS_HELM(k) ((k)->family == QBXFMM_HELMHOLTZ)
 
 /* {{{ stages */
@@ -416,7 +433,7 @@ static int h2_apply(const qbxfmm_kernel*, const qbxfmm_geometry*, const cplx*, c
 int orc_form_multipoles(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
                         const double* strengths, cplx* mpoles)
 {
-  if (IS_HELM(kern)) return h2_form_multipoles(kern, g, (const cplx*)strengths, mpoles);
+  if (IS_HELM(kern)) return kern->dim == 3 ? h3_form_multipoles(kern, g, (const cplx*)strengths, mpoles) : h2_form_multipoles(kern, g, (const cplx*)strengths, mpoles);
   ctx_t c;
   int rc = make_ctx(kern, &c);
   if (rc) return rc;
@@ -451,7 +468,7 @@ int orc_form_multipoles(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
 int orc_coarsen_multipoles(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
                            cplx* mpoles)
 {
-  if (IS_HELM(kern)) return h2_coarsen_multipoles(kern, g, mpoles);
+  if (IS_HELM(kern)) return kern->dim == 3 ? h3_coarsen_multipoles(kern, g, mpoles) : h2_coarsen_multipoles(kern, g, mpoles);
   ctx_t c;
   int rc = make_ctx(kern, &c);
   if (rc) return rc;
@@ -491,7 +508,7 @@ int orc_coarsen_multipoles(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
 int orc_eval_direct(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
                     const double* strengths, double* pot)
 {
-  if (IS_HELM(kern)) return h2_eval_direct(kern, g, (const cplx*)strengths, (cplx*)pot);
+  if (IS_HELM(kern)) return kern->dim == 3 ? h3_eval_direct(kern, g, (const cplx*)strengths, (cplx*)pot) : h2_eval_direct(kern, g, (const cplx*)strengths, (cplx*)pot);
   ctx_t c;
   int rc = make_ctx(kern, &c);
   if (rc) return rc;
@@ -527,7 +544,7 @@ int orc_eval_direct(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
 int orc_multipole_to_local(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
                            const cplx* mpoles, cplx* locals)
 {
-  if (IS_HELM(kern)) return h2_multipole_to_local(kern, g, mpoles, locals);
+  if (IS_HELM(kern)) return kern->dim == 3 ? h3_multipole_to_local(kern, g, mpoles, locals) : h2_multipole_to_local(kern, g, mpoles, locals);
   ctx_t c;
   int rc = make_ctx(kern, &c);
   if (rc) return rc;
@@ -561,7 +578,7 @@ int orc_multipole_to_local(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
 int orc_eval_multipoles(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
                         const cplx* mpoles, double* pot)
 {
-  if (IS_HELM(kern)) return h2_eval_multipoles(kern, g, mpoles, (cplx*)pot);
+  if (IS_HELM(kern)) return kern->dim == 3 ? h3_eval_multipoles(kern, g, mpoles, (cplx*)pot) : h2_eval_multipoles(kern, g, mpoles, (cplx*)pot);
   ctx_t c;
   int rc = make_ctx(kern, &c);
   if (rc) return rc;
@@ -597,7 +614,7 @@ int orc_eval_multipoles(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
 int orc_form_locals(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
                     const double* strengths, cplx* locals)
 {
-  if (IS_HELM(kern)) return h2_form_locals(kern, g, (const cplx*)strengths, locals);
+  if (IS_HELM(kern)) return kern->dim == 3 ? h3_form_locals(kern, g, (const cplx*)strengths, locals) : h2_form_locals(kern, g, (const cplx*)strengths, locals);
   ctx_t c;
   int rc = make_ctx(kern, &c);
   if (rc) return rc;
@@ -632,7 +649,7 @@ int orc_form_locals(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
 
 int orc_refine_locals(const qbxfmm_kernel* kern, const qbxfmm_geometry* g, cplx* locals)
 {
-  if (IS_HELM(kern)) return h2_refine_locals(kern, g, locals);
+  if (IS_HELM(kern)) return kern->dim == 3 ? h3_refine_locals(kern, g, locals) : h2_refine_locals(kern, g, locals);
   ctx_t c;
   int rc = make_ctx(kern, &c);
   if (rc) return rc;
@@ -666,7 +683,7 @@ int orc_refine_locals(const qbxfmm_kernel* kern, const qbxfmm_geometry* g, cplx*
 int orc_eval_locals(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
                     const cplx* locals, double* pot)
 {
-  if (IS_HELM(kern)) return h2_eval_locals(kern, g, locals, (cplx*)pot);
+  if (IS_HELM(kern)) return kern->dim == 3 ? h3_eval_locals(kern, g, locals, (cplx*)pot) : h2_eval_locals(kern, g, locals, (cplx*)pot);
   ctx_t c;
   int rc = make_ctx(kern, &c);
   if (rc) return rc;
@@ -745,7 +762,7 @@ static int p2qbxl_impl(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
 int orc_form_global_qbx_locals(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
                                const double* strengths, cplx* qbx_exps)
 {
-  if (IS_HELM(kern)) return h2_p2qbxl(kern, g, (const cplx*)strengths, qbx_exps, 0);
+  if (IS_HELM(kern)) return kern->dim == 3 ? h3_p2qbxl(kern, g, (const cplx*)strengths, qbx_exps, 0) : h2_p2qbxl(kern, g, (const cplx*)strengths, qbx_exps, 0);
   return p2qbxl_impl(kern, g, strengths, qbx_exps, 0);
 }
 
@@ -754,7 +771,7 @@ int orc_translate_box_multipoles_to_qbx_local(const qbxfmm_kernel* kern,
                                               const qbxfmm_geometry* g,
                                               const cplx* mpoles, cplx* qbx_exps)
 {
-  if (IS_HELM(kern)) return h2_m2qbxl(kern, g, mpoles, qbx_exps);
+  if (IS_HELM(kern)) return kern->dim == 3 ? h3_m2qbxl(kern, g, mpoles, qbx_exps) : h2_m2qbxl(kern, g, mpoles, qbx_exps);
   ctx_t c;
   int rc = make_ctx(kern, &c);
   if (rc) return rc;
@@ -791,7 +808,7 @@ int orc_translate_box_local_to_qbx_local(const qbxfmm_kernel* kern,
                                          const qbxfmm_geometry* g,
                                          const cplx* locals, cplx* qbx_exps)
 {
-  if (IS_HELM(kern)) return h2_l2qbxl(kern, g, locals, qbx_exps);
+  if (IS_HELM(kern)) return kern->dim == 3 ? h3_l2qbxl(kern, g, locals, qbx_exps) : h2_l2qbxl(kern, g, locals, qbx_exps);
   ctx_t c;
   int rc = make_ctx(kern, &c);
   if (rc) return rc;
@@ -824,7 +841,7 @@ int orc_translate_box_local_to_qbx_local(const qbxfmm_kernel* kern,
 int orc_eval_qbx_expansions(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
                             const cplx* qbx_exps, double* pot_tree)
 {
-  if (IS_HELM(kern)) return h2_eval_qbx_expansions(kern, g, qbx_exps, (cplx*)pot_tree);
+  if (IS_HELM(kern)) return kern->dim == 3 ? h3_eval_qbx_expansions(kern, g, qbx_exps, (cplx*)pot_tree) : h2_eval_qbx_expansions(kern, g, qbx_exps, (cplx*)pot_tree);
   ctx_t c;
   int rc = make_ctx(kern, &c);
   if (rc) return rc;
@@ -862,7 +879,9 @@ int orc_assemble(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
                  const double* pot_nonqbx, const double* pot_tree, double* out)
 {
   if (IS_HELM(kern))
-    return h2_assemble(kern, g, (const cplx*)pot_nonqbx, (const cplx*)pot_tree, (cplx*)out);
+    return kern->dim == 3
+               ? h3_assemble(kern, g, (const cplx*)pot_nonqbx, (const cplx*)pot_tree, (cplx*)out)
+               : h2_assemble(kern, g, (const cplx*)pot_nonqbx, (const cplx*)pot_tree, (cplx*)out);
   ctx_t c;
   int rc = make_ctx(kern, &c);
   if (rc) return rc;
@@ -887,7 +906,7 @@ int orc_assemble(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
 int orc_apply(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
               const double* strengths, double* out)
 {
-  if (IS_HELM(kern)) return h2_apply(kern, g, (const cplx*)strengths, (cplx*)out, 0);
+  if (IS_HELM(kern)) return kern->dim == 3 ? h3_apply(kern, g, (const cplx*)strengths, (cplx*)out, 0) : h2_apply(kern, g, (const cplx*)strengths, (cplx*)out, 0);
   ctx_t c;
   int rc = make_ctx(kern, &c);
   if (rc) return rc;
@@ -924,7 +943,7 @@ int orc_apply(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
 int orc_apply_direct(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
                      const double* strengths, double* out)
 {
-  if (IS_HELM(kern)) return h2_apply(kern, g, (const cplx*)strengths, (cplx*)out, 1);
+  if (IS_HELM(kern)) return kern->dim == 3 ? h3_apply(kern, g, (const cplx*)strengths, (cplx*)out, 1) : h2_apply(kern, g, (const cplx*)strengths, (cplx*)out, 1);
   ctx_t c;
   int rc = make_ctx(kern, &c);
   if (rc) return rc;
@@ -959,3 +978,4 @@ int orc_apply_direct(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
 /* }}} */
 
 #include "qbxfmm_oracle_helm2d.c"
+#include "qbxfmm_oracle_helm3d.c"

@@ -1,0 +1,833 @@
+/*
+ * 3D Helmholtz part of the CPU checker (TEST INFRASTRUCTURE ONLY), included by
+ * qbxfmm_oracle.c.
+ *
+ * Kernel G(x, y) = e^{ik|x-y|} / |x-y| (k real, > 0); the double layer is the
+ * source-normal derivative; the scaling 1/(4 pi) is applied at assembly.
+ *
+ * Expansions are spherical-wave expansions, the basis of the reference's fmmlib
+ * backend (pytential/qbx/fmmlib.py) and of its target-specific module
+ * (pytential/qbx/target_specific/impl.pyx:363-563), which pins the near field:
+ *   Y_n^m(v) = p_n^|m|(cos t) sin^|m| t e^{i m phi}, orthonormal, no Condon-Shortley
+ *              phase (Y_n^-m = conj(Y_n^m)),
+ *   R_n^m(v) = j_n(k|v|) Y_n^m(v),   S_n^m(v) = h_n(k|v|) Y_n^m(v)   (h = h^(1)),
+ *   G(x, y) = 4 pi i k sum_{n,m} S_n^m(x - c) conj(R_n^m(y - c))      (|y-c| < |x-c|)
+ *           = ik sum_n (2n+1) j_n(k|y-c|) h_n(k|x-c|) P_n(cos gamma).
+ * Multipole about c: phi(x) = sum M_nm S_n^m(x - c), M_nm = 4 pi i k q R_n^-m(y - c);
+ * local about c:     phi(x) = sum L_nm R_n^m(x - c), L_nm = 4 pi i k q S_n^-m(y - c).
+ * Translations (addition theorem through the plane-wave representation
+ * j_n Y_n^m(x) = i^-n / (4 pi) int e^{ik s.x} Y_n^m(s) ds):
+ *   F_n^m(r + b) = sum_{nu,mu} c_{nu mu; n m}(b) R_nu^mu(r),
+ *   c_{nu mu; n m}(b) = 4 pi sum_l i^{nu + l - n} f_l(k|b|) Y_l^{m-mu}(b) G(n,m; nu,mu; l),
+ * with F = S, f = h for multipole-to-local (|r| < |b|), F = R, f = j for
+ * local-to-local; multipole-to-multipole (|r| > |b|) uses f = j and S_nu^mu(r) on the
+ * right.  G(n,m; nu,mu; l) = int Y_n^m conj(Y_nu^mu) conj(Y_l^{m-mu}) (Gaunt integral),
+ * computed here by Gauss-Legendre quadrature in cos t (exact: the integrand is a
+ * polynomial of degree <= n + nu + l).
+ * Gradients (source-normal derivatives) by the ladder relations
+ *   d_z F_n^m           = k (a_{n-1}^m F_{n-1}^m - a_n^m F_{n+1}^m),
+ *   (d_x + i d_y) F_n^m = k (-c1 F_{n+1}^{m+1} + c2 F_{n-1}^{m+1}),
+ *   (d_x - i d_y) F_n^m = k (-c3 F_{n+1}^{m-1} + c4 F_{n-1}^{m-1}),
+ * a_n^m = sqrt((n+1-m)(n+1+m) / ((2n+1)(2n+3))), c1 = sg(m) A(m), c2 = -sg(m) B(m),
+ * c3 = sg(-m) A(-m), c4 = -sg(-m) B(-m), A(m) = sqrt((n+m+1)(n+m+2)/((2n+1)(2n+3))),
+ * B(m) = sqrt((n-m)(n-m-1)/((2n-1)(2n+1))), sg(m) = +1 for m >= 0, -1 for m < 0.
+ * Coefficients are scaled with s = min(1, k rho) (rho = box width or expansion
+ * radius), multipoles divided by s^n and locals multiplied by s^n, as fmmlib does.
+ * j_n by Miller's backward recurrence (normalized by j_0 or j_1), h_n by the upward
+ * recurrence from h_0, h_1.
+ */
+
+#define H3Q(n, m) ((n) * (n) + (n) + (m))
+#define H3_NMAX 48
+
+/* {{{ special functions */
+
+static void h3_sph_j(int N, double x, double* jv)
+{
+  for (int n = 0; n <= N; ++n) jv[n] = 0.0;
+  if (x == 0.0) {
+    jv[0] = 1.0;
+    return;
+  }
+  int nmax = N > (int)x ? N : (int)x;
+  int start = nmax + 16 + (int)sqrt(40.0 * (nmax + 1));
+  double fp1 = 0.0, f = 1e-200, f0 = 0.0, f1 = 0.0;
+  for (int n = start; n >= 1; --n) {
+    double fm1 = (2.0 * n + 1.0) / x * f - fp1;   /* f_{n-1} */
+    fp1 = f;
+    f = fm1;
+    if (n - 1 <= N) jv[n - 1] = f;
+    if (n - 1 == 1) f1 = f;
+    if (fabs(f) > 1e200) {
+      f *= 1e-200;
+      fp1 *= 1e-200;
+      f1 *= 1e-200;
+      for (int j = n - 1; j <= N; ++j) jv[j] *= 1e-200;
+    }
+  }
+  f0 = f;
+  double scale;
+  if (x < 1.0 || fabs(sin(x)) >= 0.5) scale = (sin(x) / x) / f0;
+  else scale = ((sin(x) / x - cos(x)) / x) / f1;
+  for (int n = 0; n <= N; ++n) jv[n] *= scale;
+}
+
+static void h3_sph_h(int N, double x, cplx* hv)
+{
+  cplx e = cexp(I * x);
+  hv[0] = -I * e / x;
+  if (N >= 1) hv[1] = -e * (x + I) / (x * x);
+  for (int n = 1; n < N; ++n) hv[n + 1] = (2.0 * n + 1.0) / x * hv[n] - hv[n - 1];
+}
+
+/* Y_n^m(v) for n <= N, all m, at Y[H3Q(n, m)] */
+static void h3_ylm(int N, const double* v, cplx* Y)
+{
+  double r = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+  double t = 1.0;
+  cplx w = 0.0;
+  if (r > 0.0) {
+    t = v[2] / r;
+    w = (v[0] + I * v[1]) / r;
+  }
+  double pmm = 0.5 / sqrt(M_PI);   /* p_0^0 */
+  cplx wm = 1.0;
+  for (int m = 0; m <= N; ++m) {
+    if (m > 0) {
+      pmm *= sqrt((2.0 * m + 1.0) / (2.0 * m));
+      wm *= w;
+    }
+    double pm2 = 0.0, pm1 = pmm;
+    Y[H3Q(m, m)] = pm1 * wm;
+    if (m > 0) Y[H3Q(m, -m)] = conj(Y[H3Q(m, m)]);
+    for (int n = m + 1; n <= N; ++n) {
+      double pn;
+      if (n == m + 1) {
+        pn = sqrt(2.0 * m + 3.0) * t * pm1;
+      } else {
+        double a = sqrt((4.0 * n * n - 1.0) / ((double)n * n - (double)m * m));
+        double b = sqrt(((n - 1.0) * (n - 1.0) - (double)m * m) / (4.0 * (n - 1.0) * (n - 1.0) - 1.0));
+        pn = a * (t * pm1 - b * pm2);
+      }
+      pm2 = pm1;
+      pm1 = pn;
+      Y[H3Q(n, m)] = pn * wm;
+      if (m > 0) Y[H3Q(n, -m)] = conj(Y[H3Q(n, m)]);
+    }
+  }
+}
+
+/* F_n^m(v) = f_n(k|v|) Y_n^m(v), f = j (singular = 0) or h (singular = 1), n <= N */
+static void h3_waves(int N, double k, const double* v, int singular, cplx* F)
+{
+  double jv[H3_NMAX + 2];
+  cplx hv[H3_NMAX + 2];
+  double r = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+  h3_ylm(N, v, F);
+  if (singular) h3_sph_h(N, k * r, hv);
+  else h3_sph_j(N, k * r, jv);
+  for (int n = 0; n <= N; ++n)
+    for (int m = -n; m <= n; ++m) F[H3Q(n, m)] *= singular ? hv[n] : jv[n];
+}
+
+static inline cplx h3_get(const cplx* F, int N, int n, int m)
+{
+  if (n < 0 || n > N || m > n || -m > n) return 0.0;
+  return F[H3Q(n, m)];
+}
+
+/* nu . grad F_n^m from a wave table of order N >= n + 1 */
+static cplx h3_dgrad(const cplx* F, int N, int n, int m, double k, const double* nu)
+{
+  double an = sqrt((double)(n + 1 - m) * (n + 1 + m) / ((2.0 * n + 1) * (2.0 * n + 3)));
+  double anm1 = (n >= 1) ? sqrt((double)(n - m) * (n + m) / ((2.0 * n - 1) * (2.0 * n + 1))) : 0.0;
+  cplx dz = k * (anm1 * h3_get(F, N, n - 1, m) - an * h3_get(F, N, n + 1, m));
+  double sgp = m >= 0 ? 1.0 : -1.0, sgm = -m >= 0 ? 1.0 : -1.0;
+  double Ap = sqrt((double)(n + m + 1) * (n + m + 2) / ((2.0 * n + 1) * (2.0 * n + 3)));
+  double Bp = (n >= 1 && n - m - 1 >= 0)
+                  ? sqrt((double)(n - m) * (n - m - 1) / ((2.0 * n - 1) * (2.0 * n + 1))) : 0.0;
+  double Am = sqrt((double)(n - m + 1) * (n - m + 2) / ((2.0 * n + 1) * (2.0 * n + 3)));
+  double Bm = (n >= 1 && n + m - 1 >= 0)
+                  ? sqrt((double)(n + m) * (n + m - 1) / ((2.0 * n - 1) * (2.0 * n + 1))) : 0.0;
+  cplx dplus = k * (-sgp * Ap * h3_get(F, N, n + 1, m + 1) - sgp * Bp * h3_get(F, N, n - 1, m + 1));
+  cplx dminus = k * (-sgm * Am * h3_get(F, N, n + 1, m - 1) - sgm * Bm * h3_get(F, N, n - 1, m - 1));
+  return 0.5 * (nu[0] - I * nu[1]) * dplus + 0.5 * (nu[0] + I * nu[1]) * dminus + nu[2] * dz;
+}
+
+/* }}} */
+
+/* {{{ Gaunt table */
+
+/* Gauss-Legendre nodes/weights on [-1, 1] (Newton on P_n) */
+static void h3_gauss_legendre(int n, double* x, double* w)
+{
+  for (int i = 0; i < n; ++i) {
+    double z = cos(M_PI * (i + 0.75) / (n + 0.5)), pp = 0.0;
+    for (int it = 0; it < 100; ++it) {
+      double p1 = 1.0, p2 = 0.0;
+      for (int j = 1; j <= n; ++j) {
+        double p3 = p2;
+        p2 = p1;
+        p1 = ((2.0 * j - 1.0) * z * p2 - (j - 1.0) * p3) / j;
+      }
+      pp = n * (z * p1 - p2) / (z * z - 1.0);
+      double z1 = z;
+      z = z1 - p1 / pp;
+      if (fabs(z - z1) < 1e-16) break;
+    }
+    x[i] = z;
+    w[i] = 2.0 / ((1.0 - z * z) * pp * pp);
+  }
+}
+
+typedef struct {
+  int p;          /* table covers n, nu <= p */
+  int nl;         /* l slots: l = |n - nu| + 2 j, j < nl */
+  double* G;      /* [(p+1)^2][(p+1)^2][nl] */
+} h3gaunt_t;
+
+static h3gaunt_t g_h3gaunt = {-1, 0, NULL};
+
+static const h3gaunt_t* h3_gaunt(int p)
+{
+  if (g_h3gaunt.p == p) return &g_h3gaunt;
+  free(g_h3gaunt.G);
+  int C = (p + 1) * (p + 1), nl = p + 1, L = 2 * p;
+  int ng = 2 * p + 2;
+  double* x = malloc(sizeof(double) * ng);
+  double* w = malloc(sizeof(double) * ng);
+  h3_gauss_legendre(ng, x, w);
+  /* polynomial parts p_n^m(t) (Y_n^m = p_n^m sin^m e^{im phi}) at the nodes, n <= L */
+  int NP = (L + 1) * (L + 1);
+  double* P = malloc(sizeof(double) * NP * ng);
+  for (int i = 0; i < ng; ++i) {
+    double v[3] = {sqrt(1.0 - x[i] * x[i]), 0.0, x[i]};   /* phi = 0 */
+    cplx* Y = malloc(sizeof(cplx) * NP);
+    h3_ylm(L, v, Y);
+    double st = v[0];
+    for (int n = 0; n <= L; ++n)
+      for (int m = 0; m <= n; ++m) P[(size_t)(n * n + n + m) * ng + i] = creal(Y[H3Q(n, m)]) / pow(st, m);
+    free(Y);
+  }
+  double* G = calloc((size_t)C * C * nl, sizeof(double));
+  for (int n = 0; n <= p; ++n)
+    for (int m = -n; m <= n; ++m)
+      for (int nu = 0; nu <= p; ++nu)
+        for (int mu = -nu; mu <= nu; ++mu) {
+          int lam = m - mu;
+          int am = abs(m), amu = abs(mu), alam = abs(lam);
+          int e = (am + amu + alam) / 2;
+          for (int j = 0; j < nl; ++j) {
+            int l = abs(n - nu) + 2 * j;
+            if (l > n + nu || alam > l) continue;
+            double s = 0.0;
+            for (int i = 0; i < ng; ++i) {
+              double om = 1.0;
+              for (int u = 0; u < e; ++u) om *= 1.0 - x[i] * x[i];
+              s += w[i] * P[(size_t)(n * n + n + am) * ng + i] * P[(size_t)(nu * nu + nu + amu) * ng + i] *
+                   P[(size_t)(l * l + l + alam) * ng + i] * om;
+            }
+            G[((size_t)H3Q(n, m) * C + H3Q(nu, mu)) * nl + j] = 2.0 * M_PI * s;
+          }
+        }
+  free(P);
+  free(x);
+  free(w);
+  g_h3gaunt.p = p;
+  g_h3gaunt.nl = nl;
+  g_h3gaunt.G = G;
+  return &g_h3gaunt;
+}
+
+/* Eout (order pout) += translation of Ein (order pin) through wave table Fb of
+ * order pin + pout at the translation vector (f = h or j):
+ *   Eout_{nu mu} += s_out^{e_out nu} sum_{n m} c_{nu mu; n m} s_in^{e_in n} Ein_{n m} */
+static void h3_translate(const h3gaunt_t* gt, int pin, int pout, const cplx* Ein, cplx* Eout,
+                         const cplx* Fb, double s_in, int e_in, double s_out, int e_out)
+{
+  int C = (gt->p + 1) * (gt->p + 1);
+  static const cplx ipow4[4] = {1.0, I, -1.0, -I};
+  for (int nu = 0; nu <= pout; ++nu) {
+    double fo = pow(s_out, e_out * nu);
+    for (int mu = -nu; mu <= nu; ++mu) {
+      cplx acc = 0.0;
+      for (int n = 0; n <= pin; ++n) {
+        double fi = pow(s_in, e_in * n);
+        for (int m = -n; m <= n; ++m) {
+          cplx ein = Ein[H3Q(n, m)];
+          if (ein == 0.0) continue;
+          int lam = m - mu;
+          cplx t = 0.0;
+          const double* g = gt->G + ((size_t)H3Q(n, m) * C + H3Q(nu, mu)) * gt->nl;
+          for (int j = 0; j <= (n < nu ? n : nu); ++j) {
+            int l = abs(n - nu) + 2 * j;
+            if (abs(lam) > l) continue;
+            int e = ((nu + l - n) % 4 + 4) % 4;
+            t += ipow4[e] * Fb[H3Q(l, lam)] * g[j];
+          }
+          acc += 4.0 * M_PI * t * fi * ein;
+        }
+      }
+      Eout[H3Q(nu, mu)] += fo * acc;
+    }
+  }
+}
+
+/* }}} */
+
+typedef struct {
+  int pf, pq, nrhs, ncf, ncq;
+  double k;
+  cplx cq, cd;
+} h3ctx_t;
+
+static int h3_ctx(const qbxfmm_kernel* kern, h3ctx_t* c)
+{
+  if (kern->dim != 3 || kern->k_im != 0.0 || !(kern->k_re > 0.0)) return QBXFMM_ERR_UNSUPPORTED;
+  if (kern->fmm_order > 22 || kern->qbx_order > kern->fmm_order) return QBXFMM_ERR_UNSUPPORTED;
+  c->pf = kern->fmm_order;
+  c->pq = kern->qbx_order;
+  c->nrhs = kern->nrhs;
+  c->ncf = (c->pf + 1) * (c->pf + 1);
+  c->ncq = (c->pq + 1) * (c->pq + 1);
+  c->k = kern->k_re;
+  c->cq = kern->charge_coeff_re + I * kern->charge_coeff_im;
+  c->cd = kern->dipole_coeff_re + I * kern->dipole_coeff_im;
+  return 0;
+}
+
+static double h3_scale(double k, double rho) { return k * rho < 1.0 ? k * rho : 1.0; }
+
+/* P2M (local = 0) / P2L (local = 1) of one source into E (order p, scale s) */
+static void h3_p2e(const h3ctx_t* c, int p, double s, const double* ctr, const double* y,
+                   cplx q, cplx sigma, const double* nv, cplx* E, int local, cplx* F)
+{
+  double u[3] = {y[0] - ctr[0], y[1] - ctr[1], y[2] - ctr[2]};
+  int N = p + 1;
+  h3_waves(N, c->k, u, local, F);
+  cplx pre = 4.0 * M_PI * I * c->k;
+  for (int n = 0; n <= p; ++n) {
+    double f = local ? pow(s, n) : pow(s, -n);
+    for (int m = -n; m <= n; ++m) {
+      cplx v = q * F[H3Q(n, -m)];
+      if (sigma != 0.0) v += sigma * h3_dgrad(F, N, n, -m, c->k, nv);
+      E[H3Q(n, m)] += pre * f * v;
+    }
+  }
+}
+
+/* evaluate E (order p, scale s) at x: multipole (local = 0) or local (local = 1) */
+static cplx h3_e2p(const h3ctx_t* c, int p, double s, const double* ctr, const double* x,
+                   const cplx* E, int local, cplx* F)
+{
+  double u[3] = {x[0] - ctr[0], x[1] - ctr[1], x[2] - ctr[2]};
+  h3_waves(p, c->k, u, !local, F);
+  cplx acc = 0.0;
+  for (int n = 0; n <= p; ++n) {
+    double f = local ? pow(s, -n) : pow(s, n);
+    for (int m = -n; m <= n; ++m) acc += f * E[H3Q(n, m)] * F[H3Q(n, m)];
+  }
+  return acc;
+}
+
+static cplx h3_p2p(double k, const double* x, const double* y, cplx q, cplx sigma,
+                   const double* nv)
+{
+  double d[3] = {x[0] - y[0], x[1] - y[1], x[2] - y[2]};
+  double r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+  if (r == 0) return 0;
+  cplx e = cexp(I * k * r);
+  cplx v = q * e / r;
+  /* d/dn_y e^{ikr}/r = (n . (x - y)) / r * e^{ikr} (1 - ikr) / r^2 */
+  if (sigma != 0.0)
+    v += sigma * (nv[0] * d[0] + nv[1] * d[1] + nv[2] * d[2]) * e * (1.0 - I * k * r) / (r * r * r);
+  return v;
+}
+
+#define H3_WORK (size_t)((2 * H3_NMAX + 2) * (2 * H3_NMAX + 2))
+
+static int h3_form_multipoles(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
+                              const cplx* strengths, cplx* mpoles)
+{
+  h3ctx_t c;
+  int rc = h3_ctx(kern, &c);
+  if (rc) return rc;
+#pragma omp parallel
+  {
+    cplx* F = malloc(sizeof(cplx) * H3_WORK);
+#pragma omp for schedule(dynamic, 4)
+    for (int isb = 0; isb < g->nsource_boxes; ++isb) {
+      int b = g->source_boxes[isb];
+      double s = h3_scale(c.k, level_width(g, g->box_levels[b]));
+      double ctr[3], y[3], nv[3] = {0, 0, 0};
+      load(g->box_centers, g->nboxes, b, 3, ctr);
+      int s0 = g->box_source_starts[b], s1 = s0 + g->box_source_counts_nonchild[b];
+      for (int r = 0; r < c.nrhs; ++r) {
+        cplx* M = mpoles + ((size_t)b * c.nrhs + r) * c.ncf;
+        for (int si = s0; si < s1; ++si) {
+          load(g->sources, g->nsources, si, 3, y);
+          if (c.cd != 0.0) load(g->source_normals, g->nsources, si, 3, nv);
+          cplx st = strengths[(size_t)r * g->nsources + si];
+          h3_p2e(&c, c.pf, s, ctr, y, c.cq * st, c.cd * st, nv, M, 0, F);
+        }
+      }
+    }
+    free(F);
+  }
+  return 0;
+}
+
+static int h3_coarsen_multipoles(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
+                                 cplx* mpoles)
+{
+  h3ctx_t c;
+  int rc = h3_ctx(kern, &c);
+  if (rc) return rc;
+  const h3gaunt_t* gt = h3_gaunt(c.pf);
+  for (int lev = g->nlevels - 2; lev >= 0; --lev) {
+    int i0 = g->level_start_source_parent_box_nrs[lev];
+    int i1 = g->level_start_source_parent_box_nrs[lev + 1];
+#pragma omp parallel
+    {
+      cplx* F = malloc(sizeof(cplx) * H3_WORK);
+#pragma omp for schedule(dynamic, 1)
+      for (int i = i0; i < i1; ++i) {
+        int b = g->source_parent_boxes[i];
+        double sp = h3_scale(c.k, level_width(g, lev)), sc = h3_scale(c.k, level_width(g, lev + 1));
+        double cp[3], cc[3];
+        load(g->box_centers, g->nboxes, b, 3, cp);
+        for (int ci = 0; ci < 8; ++ci) {
+          int ch = g->box_child_ids[(size_t)ci * g->nboxes + b];
+          if (ch == 0 || g->box_source_counts_cumul[ch] == 0) continue;
+          load(g->box_centers, g->nboxes, ch, 3, cc);
+          double bv[3] = {cp[0] - cc[0], cp[1] - cc[1], cp[2] - cc[2]};
+          h3_waves(2 * c.pf, c.k, bv, 0, F);
+          for (int r = 0; r < c.nrhs; ++r)
+            h3_translate(gt, c.pf, c.pf, mpoles + ((size_t)ch * c.nrhs + r) * c.ncf,
+                         mpoles + ((size_t)b * c.nrhs + r) * c.ncf, F, sc, 1, sp, -1);
+        }
+      }
+      free(F);
+    }
+  }
+  return 0;
+}
+
+static int h3_eval_direct(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
+                          const cplx* strengths, cplx* pot)
+{
+  h3ctx_t c;
+  int rc = h3_ctx(kern, &c);
+  if (rc) return rc;
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int itb = 0; itb < g->ntarget_boxes; ++itb) {
+    int tb = g->target_boxes[itb];
+    int t0 = g->nonqbx_box_target_starts[tb];
+    int t1 = t0 + g->nonqbx_box_target_counts_nonchild[tb];
+    for (int t = t0; t < t1; ++t) {
+      double x[3], y[3], nv[3] = {0, 0, 0};
+      load(g->nonqbx_targets, g->nfiltered_targets, t, 3, x);
+      for (int r = 0; r < c.nrhs; ++r) {
+        cplx acc = 0;
+        for (int li = g->list1_starts[itb]; li < g->list1_starts[itb + 1]; ++li) {
+          int sb = g->list1_lists[li];
+          int s0 = g->box_source_starts[sb], s1 = s0 + g->box_source_counts_nonchild[sb];
+          for (int si = s0; si < s1; ++si) {
+            load(g->sources, g->nsources, si, 3, y);
+            if (c.cd != 0.0) load(g->source_normals, g->nsources, si, 3, nv);
+            cplx st = strengths[(size_t)r * g->nsources + si];
+            acc += h3_p2p(c.k, x, y, c.cq * st, c.cd * st, nv);
+          }
+        }
+        pot[(size_t)r * g->nfiltered_targets + t] += acc;
+      }
+    }
+  }
+  return 0;
+}
+
+static int h3_multipole_to_local(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
+                                 const cplx* mpoles, cplx* locals)
+{
+  h3ctx_t c;
+  int rc = h3_ctx(kern, &c);
+  if (rc) return rc;
+  const h3gaunt_t* gt = h3_gaunt(c.pf);
+#pragma omp parallel
+  {
+    cplx* F = malloc(sizeof(cplx) * H3_WORK);
+#pragma omp for schedule(dynamic, 1)
+    for (int i = 0; i < g->nttp_boxes; ++i) {
+      int tb = g->target_or_target_parent_boxes[i];
+      double s = h3_scale(c.k, level_width(g, g->box_levels[tb]));
+      double ct[3], cs[3];
+      load(g->box_centers, g->nboxes, tb, 3, ct);
+      for (int li = g->list2_starts[i]; li < g->list2_starts[i + 1]; ++li) {
+        int sb = g->list2_lists[li];
+        load(g->box_centers, g->nboxes, sb, 3, cs);
+        double bv[3] = {ct[0] - cs[0], ct[1] - cs[1], ct[2] - cs[2]};
+        h3_waves(2 * c.pf, c.k, bv, 1, F);
+        for (int r = 0; r < c.nrhs; ++r)
+          h3_translate(gt, c.pf, c.pf, mpoles + ((size_t)sb * c.nrhs + r) * c.ncf,
+                       locals + ((size_t)tb * c.nrhs + r) * c.ncf, F, s, 1, s, 1);
+      }
+    }
+    free(F);
+  }
+  return 0;
+}
+
+static int h3_eval_multipoles(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
+                              const cplx* mpoles, cplx* pot)
+{
+  h3ctx_t c;
+  int rc = h3_ctx(kern, &c);
+  if (rc) return rc;
+#pragma omp parallel
+  {
+    cplx* F = malloc(sizeof(cplx) * H3_WORK);
+#pragma omp for schedule(dynamic, 1)
+    for (int itb = 0; itb < g->ntarget_boxes; ++itb) {
+      int tb = g->target_boxes[itb];
+      int t0 = g->nonqbx_box_target_starts[tb];
+      int t1 = t0 + g->nonqbx_box_target_counts_nonchild[tb];
+      for (int t = t0; t < t1; ++t) {
+        double x[3], cs[3];
+        load(g->nonqbx_targets, g->nfiltered_targets, t, 3, x);
+        for (int li = g->list3_starts[itb]; li < g->list3_starts[itb + 1]; ++li) {
+          int sb = g->list3_lists[li];
+          double s = h3_scale(c.k, level_width(g, g->box_levels[sb]));
+          load(g->box_centers, g->nboxes, sb, 3, cs);
+          for (int r = 0; r < c.nrhs; ++r)
+            pot[(size_t)r * g->nfiltered_targets + t] +=
+                h3_e2p(&c, c.pf, s, cs, x, mpoles + ((size_t)sb * c.nrhs + r) * c.ncf, 0, F);
+        }
+      }
+    }
+    free(F);
+  }
+  return 0;
+}
+
+static int h3_form_locals(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
+                          const cplx* strengths, cplx* locals)
+{
+  h3ctx_t c;
+  int rc = h3_ctx(kern, &c);
+  if (rc) return rc;
+#pragma omp parallel
+  {
+    cplx* F = malloc(sizeof(cplx) * H3_WORK);
+#pragma omp for schedule(dynamic, 1)
+    for (int i = 0; i < g->nttp_boxes; ++i) {
+      int tb = g->target_or_target_parent_boxes[i];
+      double s = h3_scale(c.k, level_width(g, g->box_levels[tb]));
+      double ct[3], y[3], nv[3] = {0, 0, 0};
+      load(g->box_centers, g->nboxes, tb, 3, ct);
+      for (int li = g->list4_starts[i]; li < g->list4_starts[i + 1]; ++li) {
+        int sb = g->list4_lists[li];
+        int s0 = g->box_source_starts[sb], s1 = s0 + g->box_source_counts_nonchild[sb];
+        for (int si = s0; si < s1; ++si) {
+          load(g->sources, g->nsources, si, 3, y);
+          if (c.cd != 0.0) load(g->source_normals, g->nsources, si, 3, nv);
+          for (int r = 0; r < c.nrhs; ++r) {
+            cplx st = strengths[(size_t)r * g->nsources + si];
+            h3_p2e(&c, c.pf, s, ct, y, c.cq * st, c.cd * st, nv,
+                   locals + ((size_t)tb * c.nrhs + r) * c.ncf, 1, F);
+          }
+        }
+      }
+    }
+    free(F);
+  }
+  return 0;
+}
+
+static int h3_refine_locals(const qbxfmm_kernel* kern, const qbxfmm_geometry* g, cplx* locals)
+{
+  h3ctx_t c;
+  int rc = h3_ctx(kern, &c);
+  if (rc) return rc;
+  const h3gaunt_t* gt = h3_gaunt(c.pf);
+  for (int lev = 1; lev < g->nlevels; ++lev) {
+    int i0 = g->level_start_ttp_box_nrs[lev], i1 = g->level_start_ttp_box_nrs[lev + 1];
+#pragma omp parallel
+    {
+      cplx* F = malloc(sizeof(cplx) * H3_WORK);
+#pragma omp for schedule(dynamic, 4)
+      for (int i = i0; i < i1; ++i) {
+        int b = g->target_or_target_parent_boxes[i];
+        int par = g->box_parent_ids[b];
+        double sp = h3_scale(c.k, level_width(g, lev - 1)), sc = h3_scale(c.k, level_width(g, lev));
+        double cp[3], cc[3];
+        load(g->box_centers, g->nboxes, par, 3, cp);
+        load(g->box_centers, g->nboxes, b, 3, cc);
+        double bv[3] = {cc[0] - cp[0], cc[1] - cp[1], cc[2] - cp[2]};
+        h3_waves(2 * c.pf, c.k, bv, 0, F);
+        for (int r = 0; r < c.nrhs; ++r)
+          h3_translate(gt, c.pf, c.pf, locals + ((size_t)par * c.nrhs + r) * c.ncf,
+                       locals + ((size_t)b * c.nrhs + r) * c.ncf, F, sp, -1, sc, 1);
+      }
+      free(F);
+    }
+  }
+  return 0;
+}
+
+static int h3_eval_locals(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
+                          const cplx* locals, cplx* pot)
+{
+  h3ctx_t c;
+  int rc = h3_ctx(kern, &c);
+  if (rc) return rc;
+#pragma omp parallel
+  {
+    cplx* F = malloc(sizeof(cplx) * H3_WORK);
+#pragma omp for schedule(dynamic, 4)
+    for (int itb = 0; itb < g->ntarget_boxes; ++itb) {
+      int tb = g->target_boxes[itb];
+      int t0 = g->nonqbx_box_target_starts[tb];
+      int t1 = t0 + g->nonqbx_box_target_counts_nonchild[tb];
+      double s = h3_scale(c.k, level_width(g, g->box_levels[tb]));
+      double ct[3], x[3];
+      load(g->box_centers, g->nboxes, tb, 3, ct);
+      for (int t = t0; t < t1; ++t) {
+        load(g->nonqbx_targets, g->nfiltered_targets, t, 3, x);
+        for (int r = 0; r < c.nrhs; ++r)
+          pot[(size_t)r * g->nfiltered_targets + t] +=
+              h3_e2p(&c, c.pf, s, ct, x, locals + ((size_t)tb * c.nrhs + r) * c.ncf, 1, F);
+      }
+    }
+    free(F);
+  }
+  return 0;
+}
+
+static int h3_p2qbxl(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
+                     const cplx* strengths, cplx* qbx_exps, int all_sources)
+{
+  h3ctx_t c;
+  int rc = h3_ctx(kern, &c);
+  if (rc) return rc;
+#pragma omp parallel
+  {
+    cplx* F = malloc(sizeof(cplx) * H3_WORK);
+#pragma omp for schedule(dynamic, 16)
+    for (int ig = 0; ig < g->nglobal_qbx_centers; ++ig) {
+      int ctr = g->global_qbx_centers[ig];
+      double cc[3], y[3], nv[3] = {0, 0, 0};
+      load(g->centers, g->ncenters, ctr, 3, cc);
+      double s = h3_scale(c.k, g->expansion_radii[ctr]);
+      int itb = g->qbx_center_to_target_box[ctr];
+      int l0 = all_sources ? 0 : g->list1_starts[itb];
+      int l1 = all_sources ? 1 : g->list1_starts[itb + 1];
+      for (int li = l0; li < l1; ++li) {
+        int s0, s1;
+        if (all_sources) {
+          s0 = 0;
+          s1 = g->nsources;
+        } else {
+          int sb = g->list1_lists[li];
+          s0 = g->box_source_starts[sb];
+          s1 = s0 + g->box_source_counts_nonchild[sb];
+        }
+        for (int si = s0; si < s1; ++si) {
+          load(g->sources, g->nsources, si, 3, y);
+          if (c.cd != 0.0) load(g->source_normals, g->nsources, si, 3, nv);
+          for (int r = 0; r < c.nrhs; ++r) {
+            cplx st = strengths[(size_t)r * g->nsources + si];
+            h3_p2e(&c, c.pq, s, cc, y, c.cq * st, c.cd * st, nv,
+                   qbx_exps + ((size_t)ctr * c.nrhs + r) * c.ncq, 1, F);
+          }
+        }
+      }
+    }
+    free(F);
+  }
+  return 0;
+}
+
+static int h3_m2qbxl(const qbxfmm_kernel* kern, const qbxfmm_geometry* g, const cplx* mpoles,
+                     cplx* qbx_exps)
+{
+  h3ctx_t c;
+  int rc = h3_ctx(kern, &c);
+  if (rc) return rc;
+  const h3gaunt_t* gt = h3_gaunt(c.pf);
+#pragma omp parallel
+  {
+    cplx* F = malloc(sizeof(cplx) * H3_WORK);
+#pragma omp for schedule(dynamic, 16)
+    for (int ig = 0; ig < g->nglobal_qbx_centers; ++ig) {
+      int ctr = g->global_qbx_centers[ig];
+      double cc[3], cs[3];
+      load(g->centers, g->ncenters, ctr, 3, cc);
+      double st = h3_scale(c.k, g->expansion_radii[ctr]);
+      int itb = g->qbx_center_to_target_box[ctr];
+      for (int li = g->list3_starts[itb]; li < g->list3_starts[itb + 1]; ++li) {
+        int sb = g->list3_lists[li];
+        double ss = h3_scale(c.k, level_width(g, g->box_levels[sb]));
+        load(g->box_centers, g->nboxes, sb, 3, cs);
+        double bv[3] = {cc[0] - cs[0], cc[1] - cs[1], cc[2] - cs[2]};
+        h3_waves(c.pf + c.pq, c.k, bv, 1, F);
+        for (int r = 0; r < c.nrhs; ++r)
+          h3_translate(gt, c.pf, c.pq, mpoles + ((size_t)sb * c.nrhs + r) * c.ncf,
+                       qbx_exps + ((size_t)ctr * c.nrhs + r) * c.ncq, F, ss, 1, st, 1);
+      }
+    }
+    free(F);
+  }
+  return 0;
+}
+
+static int h3_l2qbxl(const qbxfmm_kernel* kern, const qbxfmm_geometry* g, const cplx* locals,
+                     cplx* qbx_exps)
+{
+  h3ctx_t c;
+  int rc = h3_ctx(kern, &c);
+  if (rc) return rc;
+  const h3gaunt_t* gt = h3_gaunt(c.pf);
+#pragma omp parallel
+  {
+    cplx* F = malloc(sizeof(cplx) * H3_WORK);
+#pragma omp for schedule(dynamic, 16)
+    for (int ig = 0; ig < g->nglobal_qbx_centers; ++ig) {
+      int ctr = g->global_qbx_centers[ig];
+      int tb = g->target_boxes[g->qbx_center_to_target_box[ctr]];
+      double cc[3], cb[3];
+      load(g->centers, g->ncenters, ctr, 3, cc);
+      load(g->box_centers, g->nboxes, tb, 3, cb);
+      double sb_ = h3_scale(c.k, level_width(g, g->box_levels[tb]));
+      double sc = h3_scale(c.k, g->expansion_radii[ctr]);
+      double bv[3] = {cc[0] - cb[0], cc[1] - cb[1], cc[2] - cb[2]};
+      h3_waves(c.pf + c.pq, c.k, bv, 0, F);
+      for (int r = 0; r < c.nrhs; ++r)
+        h3_translate(gt, c.pf, c.pq, locals + ((size_t)tb * c.nrhs + r) * c.ncf,
+                     qbx_exps + ((size_t)ctr * c.nrhs + r) * c.ncq, F, sb_, -1, sc, 1);
+    }
+    free(F);
+  }
+  return 0;
+}
+
+static int h3_eval_qbx_expansions(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
+                                  const cplx* qbx_exps, cplx* pot_tree)
+{
+  h3ctx_t c;
+  int rc = h3_ctx(kern, &c);
+  if (rc) return rc;
+#pragma omp parallel
+  {
+    cplx* F = malloc(sizeof(cplx) * H3_WORK);
+#pragma omp for schedule(dynamic, 16)
+    for (int ig = 0; ig < g->nglobal_qbx_centers; ++ig) {
+      int ctr = g->global_qbx_centers[ig];
+      double cc[3], x[3];
+      load(g->centers, g->ncenters, ctr, 3, cc);
+      double s = h3_scale(c.k, g->expansion_radii[ctr]);
+      for (int it = g->center_to_targets_starts[ctr]; it < g->center_to_targets_starts[ctr + 1];
+           ++it) {
+        int t = g->center_to_targets_lists[it];
+        load(g->targets, g->ntargets, t, 3, x);
+        for (int r = 0; r < c.nrhs; ++r)
+          pot_tree[(size_t)r * g->ntargets + t] =
+              h3_e2p(&c, c.pq, s, cc, x, qbx_exps + ((size_t)ctr * c.nrhs + r) * c.ncq, 1, F);
+      }
+    }
+    free(F);
+  }
+  return 0;
+}
+
+static int h3_assemble(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
+                       const cplx* pot_nonqbx, const cplx* pot_tree, cplx* out)
+{
+  h3ctx_t c;
+  int rc = h3_ctx(kern, &c);
+  if (rc) return rc;
+  double scale = 0.25 / M_PI;
+  cplx* full = malloc(sizeof(cplx) * (g->ntargets + 1));
+  for (int r = 0; r < c.nrhs; ++r) {
+    memcpy(full, pot_tree + (size_t)r * g->ntargets, sizeof(cplx) * g->ntargets);
+    for (int f = 0; f < g->nfiltered_targets; ++f)
+      full[g->unfiltered_from_filtered_target_indices[f]] +=
+          pot_nonqbx[(size_t)r * g->nfiltered_targets + f];
+    for (int t = 0; t < g->ntargets; ++t) {
+      int u = g->sorted_target_ids[t] - g->ncenters;
+      if (u >= 0) out[(size_t)r * g->nuser_targets + u] = scale * full[t];
+    }
+  }
+  free(full);
+  return 0;
+}
+
+static int h3_apply(const qbxfmm_kernel* kern, const qbxfmm_geometry* g, const cplx* strengths,
+                    cplx* out, int direct)
+{
+  h3ctx_t c;
+  int rc = h3_ctx(kern, &c);
+  if (rc) return rc;
+  size_t nexp = (size_t)g->nboxes * c.nrhs * c.ncf;
+  cplx* mpoles = calloc(nexp, sizeof(cplx));
+  cplx* locals = calloc(nexp, sizeof(cplx));
+  cplx* qexp = calloc((size_t)g->ncenters * c.nrhs * c.ncq, sizeof(cplx));
+  cplx* pnq = calloc((size_t)c.nrhs * g->nfiltered_targets + 1, sizeof(cplx));
+  cplx* ptree = calloc((size_t)c.nrhs * g->ntargets + 1, sizeof(cplx));
+  if (!direct) {
+    h3_form_multipoles(kern, g, strengths, mpoles);
+    h3_coarsen_multipoles(kern, g, mpoles);
+    h3_eval_direct(kern, g, strengths, pnq);
+    h3_multipole_to_local(kern, g, mpoles, locals);
+    h3_eval_multipoles(kern, g, mpoles, pnq);
+    h3_form_locals(kern, g, strengths, locals);
+    h3_refine_locals(kern, g, locals);
+    h3_eval_locals(kern, g, locals, pnq);
+    h3_p2qbxl(kern, g, strengths, qexp, 0);
+    h3_m2qbxl(kern, g, mpoles, qexp);
+    h3_l2qbxl(kern, g, locals, qexp);
+  } else {
+    h3_p2qbxl(kern, g, strengths, qexp, 1);
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int t = 0; t < g->nfiltered_targets; ++t) {
+      double x[3], y[3], nv[3] = {0, 0, 0};
+      load(g->nonqbx_targets, g->nfiltered_targets, t, 3, x);
+      for (int r = 0; r < c.nrhs; ++r) {
+        cplx acc = 0;
+        for (int si = 0; si < g->nsources; ++si) {
+          load(g->sources, g->nsources, si, 3, y);
+          if (c.cd != 0.0) load(g->source_normals, g->nsources, si, 3, nv);
+          cplx st = strengths[(size_t)r * g->nsources + si];
+          acc += h3_p2p(c.k, x, y, c.cq * st, c.cd * st, nv);
+        }
+        pnq[(size_t)r * g->nfiltered_targets + t] = acc;
+      }
+    }
+  }
+  h3_eval_qbx_expansions(kern, g, qexp, ptree);
+  h3_assemble(kern, g, pnq, ptree, out);
+  free(mpoles);
+  free(locals);
+  free(qexp);
+  free(pnq);
+  free(ptree);
+  return 0;
+}
+
+/* test hooks: special functions and wave tables */
+void orc_h3_sph_j(int N, double x, double* out) { h3_sph_j(N, x, out); }
+void orc_h3_sph_h(int N, double x, cplx* out) { h3_sph_h(N, x, out); }
+void orc_h3_ylm(int N, const double* v, cplx* out) { h3_ylm(N, v, out); }
+void orc_h3_waves(int N, double k, const double* v, int singular, cplx* out)
+{
+  h3_waves(N, k, v, singular, out);
+}
+cplx orc_h3_dgrad(const cplx* F, int N, int n, int m, double k, const double* nu)
+{
+  return h3_dgrad(F, N, n, m, k, nu);
+}
+void orc_h3_gaunt(int p, double* out)
+{
+  const h3gaunt_t* gt = h3_gaunt(p);
+  int C = (p + 1) * (p + 1);
+  memcpy(out, gt->G, sizeof(double) * (size_t)C * C * gt->nl);
+}

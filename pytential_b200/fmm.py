@@ -53,13 +53,13 @@ class LaplaceKernel:
 
 @dataclass(frozen=True)
 class HelmholtzKernel:
-    """G = (i/4) H_0^(1)(k|x - y|) (2D)."""
+    """G = (i/4) H_0^(1)(k|x - y|) (2D), G = e^{ik|x - y|} / (4 pi |x - y|) (3D)."""
     dim: int
     k: float
     family: int = abi.QBXFMM_HELMHOLTZ
 
     def global_scaling_const(self) -> complex:
-        return 0.25j
+        return 0.25j if self.dim == 2 else 0.25 / np.pi
 
 
 @dataclass(frozen=True)

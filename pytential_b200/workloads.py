@@ -116,3 +116,29 @@ def helmholtz2d_starfish(nelements: int = 2048, k: float = 20.0, nrhs: int = 64,
         targets.append((rng.uniform(-2, 2, size=(2, nvolume)), 0))
     return Workload(f"2D Helmholtz k={k:g} {op}, starfish {nelements}x16 nodes, {nrhs} rhs",
                     d, targets, dens, spec, qbx_order, fmm_order, seed)
+
+
+def helmholtz3d_ellipsoid(nrefine: int = 5, k: float = 10.0, nrhs: int = 16, seed: int = 0,
+                          op: str = "CF", qbx_order: int = 5, fmm_order: int = 15,
+                          nshell: int = 0) -> Workload:
+    """3D Helmholtz on the ellipsoid (1, 1.5, 2): combined field ``D - i k S`` (op
+    "CF"), or "S"/"D"; exterior limit on the surface.  Densities: plane waves
+    ``exp(i k d.x)`` at ``nrhs`` seeded unit directions, restricted to the surface.
+    ``nshell`` adds volume targets uniform in the shell 2.5 <= r <= 3.5."""
+    rng = np.random.default_rng(seed)
+    d = make_ellipsoid(nrefine)
+    dirs = rng.normal(size=(3, nrhs))
+    dirs /= np.linalg.norm(dirs, axis=0)
+    dens = np.exp(1j * k * (dirs.T @ d.nodes))
+    cq = {"CF": -1j * k, "S": 1.0, "D": 0.0}[op]
+    cd = {"CF": 1.0, "S": 0.0, "D": 1.0}[op]
+    spec = SourceKernelSpec(HelmholtzKernel(3, k), charge_coeff=cq, dipole_coeff=cd)
+    targets = [(d.nodes, +1)]
+    if nshell:
+        v = rng.normal(size=(3, nshell))
+        v /= np.linalg.norm(v, axis=0)
+        r = rng.uniform(2.5 ** 3, 3.5 ** 3, nshell) ** (1 / 3)
+        targets.append((v * r, 0))
+    return Workload(f"3D Helmholtz k={k:g} {op}, ellipsoid icosphere-{nrefine} "
+                    f"({d.nelements} tri), {nrhs} rhs", d, targets, dens, spec, qbx_order,
+                    fmm_order, seed)

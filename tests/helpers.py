@@ -8,8 +8,8 @@ import os
 import numpy as np
 
 from pytential_b200 import abi
-from pytential_b200.workloads import (helmholtz2d_starfish, laplace2d_starfish,
-                                     laplace3d_ellipsoid)
+from pytential_b200.workloads import (helmholtz2d_starfish, helmholtz3d_ellipsoid,
+                                     laplace2d_starfish, laplace3d_ellipsoid)
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
@@ -36,6 +36,15 @@ def workload(name: str):
         return helmholtz2d_starfish(nelements=32, nrhs=1, nvolume=200, op="S", fmm_order=16)
     if name == "h2d-D-small":
         return helmholtz2d_starfish(nelements=32, nrhs=3, nvolume=200, op="D", qbx_order=4)
+    if name == "h3d-CF-small":
+        return helmholtz3d_ellipsoid(nrefine=1, k=3.0, nrhs=2, op="CF", qbx_order=3,
+                                     fmm_order=10, nshell=200)
+    if name == "h3d-S-small":
+        return helmholtz3d_ellipsoid(nrefine=1, k=2.0, nrhs=1, op="S", qbx_order=4,
+                                     fmm_order=12, nshell=100)
+    if name == "h3d-D-small":
+        return helmholtz3d_ellipsoid(nrefine=1, k=4.0, nrhs=3, op="D", qbx_order=2,
+                                     fmm_order=8, nshell=100)
     raise KeyError(name)
 
 
@@ -54,8 +63,8 @@ def relerr(a, b):
     return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
 
 
-def golden_tsqbx():
-    return np.load(os.path.join(GOLDEN, "tsqbx_laplace3d.npz"))
+def golden_tsqbx(kind="laplace3d"):
+    return np.load(os.path.join(GOLDEN, f"tsqbx_{kind}.npz"))
 
 
 def golden_geometry(z):

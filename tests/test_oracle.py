@@ -3,6 +3,8 @@
 * against the reference's own compiled target-specific QBX module (golden fixture
   tests/golden/tsqbx_laplace3d.npz, tolerance 1e-13 as in
   test/test_target_specific_qbx.py:218);
+* the same for the 3D Helmholtz near field (tests/golden/tsqbx_helmholtz3d.npz);
+* the 3D Helmholtz special functions against scipy;
 * FMM against direct (non-FMM) QBX with the same truncation, at the FMM's
   truncation level (test/test_layer_pot.py:153-230 checks 1e-3);
 * linearity of the apply.
@@ -45,8 +47,65 @@ def test_oracle_matches_reference_tsqbx(op):
         assert relerr(pt[0][mask], ref[mask]) < 1e-13, (op, q)
 
 
+@pytest.mark.parametrize("op", ["S", "D"])
+def test_oracle_matches_reference_tsqbx_helmholtz3d(op):
+    z = golden_tsqbx("helmholtz3d")
+    scalars, arrays = golden_geometry(z)
+    g = abi.make_geometry_struct(scalars, arrays, lambda a: a.ctypes.data)
+    s = np.ascontiguousarray(z["strengths"][None, :])
+    mask = np.zeros(scalars["ntargets"], bool)
+    mask[z["center_to_targets_lists"]] = True
+    for q in z["orders"]:
+        k = abi.make_kernel_struct(family=abi.QBXFMM_HELMHOLTZ, dim=3, qbx_order=int(q),
+                                   fmm_order=6, k=float(z["k"]), charge_coeff=float(op == "S"),
+                                   dipole_coeff=float(op == "D"))
+        nc = abi.ncoeff(abi.QBXFMM_HELMHOLTZ, 3, int(q))
+        qe = np.zeros((scalars["ncenters"], 1, nc), np.complex128)
+        pt = np.zeros((1, scalars["ntargets"]), np.complex128)
+        L = lib()
+        assert L.orc_form_global_qbx_locals(ctypes.byref(k), ctypes.byref(g),
+                                            ctypes.c_void_p(s.ctypes.data),
+                                            ctypes.c_void_p(qe.ctypes.data)) == 0
+        assert L.orc_eval_qbx_expansions(ctypes.byref(k), ctypes.byref(g),
+                                         ctypes.c_void_p(qe.ctypes.data),
+                                         ctypes.c_void_p(pt.ctypes.data)) == 0
+        ref = z[f"pot_{op}_{q}"]
+        assert relerr(pt[0][mask], ref[mask]) < 1e-13, (op, q)
+
+
+def test_oracle_helmholtz3d_special_functions():
+    sp = pytest.importorskip("scipy.special")
+    L = lib()
+    P = lambda a: ctypes.c_void_p(a.ctypes.data)  # noqa: E731
+    n = np.arange(21)
+    for x in [1e-6, 0.01, 0.3, 1.0, 6.2, 12.5, 40.0]:
+        j = np.zeros(21)
+        L.orc_h3_sph_j(20, ctypes.c_double(x), P(j))
+        ref = sp.spherical_jn(n, x)
+        assert np.all(np.abs(j - ref) <= 1e-12 * np.maximum(np.abs(ref), 1e-300) + 1e-300)
+        h = np.zeros(21, complex)
+        L.orc_h3_sph_h(20, ctypes.c_double(x), P(h))
+        href = ref + 1j * sp.spherical_yn(n, x)
+        assert np.max(np.abs(h - href) / np.abs(href)) < 1e-12
+    v = np.array([0.3, -0.5, 0.7])
+    Y = np.zeros(21 * 21, complex)
+    L.orc_h3_ylm(20, P(v), P(Y))
+    th = np.arccos(v[2] / np.linalg.norm(v))
+    ph = np.arctan2(v[1], v[0])
+    for nn in range(21):
+        for m in range(-nn, nn + 1):
+            if hasattr(sp, "sph_harm_y"):
+                ref = sp.sph_harm_y(nn, m, th, ph)
+            else:
+                ref = sp.sph_harm(m, nn, ph, th)
+            if m > 0:
+                ref *= (-1) ** m     # no Condon-Shortley phase
+            assert abs(Y[nn * nn + nn + m] - ref) < 1e-13
+
+
 @pytest.mark.parametrize("name,tol", [("2d-S", 1e-6), ("2d-D", 5e-6), ("3d-S-small", 1e-5),
-                                      ("3d-D-small", 1e-5)])
+                                      ("3d-D-small", 1e-5), ("h3d-CF-small", 1e-5),
+                                      ("h3d-S-small", 1e-6), ("h3d-D-small", 3e-3)])
 def test_oracle_fmm_vs_direct_qbx(name, tol):
     wl = workload(name)
     o = oracle_for(wl)
