@@ -150,6 +150,8 @@ typedef struct qbxfmm_geometry {
    *   L2L: (parent -> child) pairs grouped by (child level, child position). */
   int32_t m2l_nclasses;
   const int32_t* m2l_class_offsets;         /* [dim][m2l_nclasses] integer offsets */
+  const int32_t* m2l_class_levels;          /* [m2l_nclasses] level of each class, or NULL when
+                                               classes are shared by all levels (Laplace) */
   const int32_t* m2l_class_starts;          /* [m2l_nclasses + 1] into the pair arrays */
   const int32_t* m2l_pair_src;              /* source box per pair (class order) */
   const int32_t* m2l_tgt_pair_starts;       /* [nttp_boxes + 1] */

@@ -74,7 +74,8 @@ GEOMETRY_FIELDS = [
     ("nonqbx_chunk_count", "pi"),
     ("ntsqbx_chunks", "i"), ("tsqbx_chunk_target_box", "pi"), ("tsqbx_chunk_start", "pi"),
     ("tsqbx_chunk_count", "pi"), ("tsqbx_targets", "pi"), ("tsqbx_centers", "pi"),
-    ("m2l_nclasses", "i"), ("m2l_class_offsets", "pi"), ("m2l_class_starts", "pi"),
+    ("m2l_nclasses", "i"), ("m2l_class_offsets", "pi"), ("m2l_class_levels", "pi"),
+    ("m2l_class_starts", "pi"),
     ("m2l_pair_src", "pi"), ("m2l_tgt_pair_starts", "pi"), ("m2l_tgt_pairs", "pi"),
     ("m2m_npairs", "i"), ("m2m_group_starts", "pi"), ("m2m_pair_src", "pi"),
     ("m2m_par_pair_starts", "pi"), ("m2m_par_pairs", "pi"),
@@ -206,8 +207,12 @@ def tsqbx_schedule(centers_by_target_box, qbx_center_to_target_box, center_to_ta
             np.array(ch_count, np.int32), np.array(tg, np.int32), np.array(ct, np.int32))
 
 
-def translation_classes(tree, trav):
-    """Class lists for the matrix form of M2L / M2M / L2L (see qbxfmm_geometry)."""
+def translation_classes(tree, trav, per_level: bool = False):
+    """Class lists for the matrix form of M2L / M2M / L2L (see qbxfmm_geometry).
+
+    M2L classes are list-2 pairs with one integer offset (in box widths); with
+    ``per_level`` a class also has one level (kernels whose translations are not
+    scale-invariant, e.g. Helmholtz)."""
     dim = tree.dimensions
     nch = 2 ** dim
     ipos = tree.box_ipos.astype(np.int64)
@@ -221,6 +226,8 @@ def translation_classes(tree, trav):
     off = ipos[:, tgt_box] - ipos[:, l2l]                       # (dim, npairs)
     R = int(np.abs(off).max()) if off.size else 0
     key = np.zeros(off.shape[1], np.int64)
+    if per_level:
+        key = np.asarray(tree.box_levels, np.int64)[tgt_box]
     for d in range(dim):
         key = key * (2 * R + 1) + (off[d] + R)
     order = np.lexsort((tgt_idx, key))                        # class, then target
@@ -228,6 +235,9 @@ def translation_classes(tree, trav):
     out["m2l_nclasses"] = len(ukeys)
     cls_off = off[:, order][:, first] if len(ukeys) else np.zeros((dim, 0), np.int64)
     out["m2l_class_offsets"] = np.ascontiguousarray(cls_off, np.int32)
+    if per_level:
+        out["m2l_class_levels"] = np.asarray(tree.box_levels, np.int32)[tgt_box[order][first]] \
+            if len(ukeys) else np.zeros(0, np.int32)
     out["m2l_class_starts"] = np.concatenate([first, [len(order)]]).astype(np.int32)
     out["m2l_pair_src"] = l2l[order].astype(np.int32)
     pos = np.empty(len(order), np.int64)
@@ -288,8 +298,11 @@ def _d(a):
     return np.ascontiguousarray(a, dtype=np.float64)
 
 
-def geometry_arrays(geo) -> tuple[dict, dict]:
-    """Return ``(scalars, arrays)`` for the C ABI from a geometry-data object."""
+def geometry_arrays(geo, per_level_classes: bool = False) -> tuple[dict, dict]:
+    """Return ``(scalars, arrays)`` for the C ABI from a geometry-data object.
+
+    ``per_level_classes``: M2L translation classes per (level, offset), as kernels
+    without scale invariance (3D Helmholtz) need; otherwise per offset."""
     tree = geo.tree()
     trav = geo.traversal()
     nqbtl = geo.non_qbx_box_target_lists()
@@ -352,7 +365,7 @@ def geometry_arrays(geo) -> tuple[dict, dict]:
                         arrays["center_to_targets_starts"], arrays["center_to_targets_lists"])
     arrays.update(dict(zip(["tsqbx_chunk_target_box", "tsqbx_chunk_start", "tsqbx_chunk_count",
                             "tsqbx_targets", "tsqbx_centers"], ts)))
-    tc = translation_classes(tree, trav)
+    tc = translation_classes(tree, trav, per_level=per_level_classes)
     arrays.update({k_: np.ascontiguousarray(v, np.int32) for k_, v in tc.items()
                    if not k_.endswith(("nclasses", "npairs"))})
     scalars = {
@@ -388,7 +401,9 @@ def make_geometry_struct(scalars: dict, arrays: dict, ptr_of) -> QBXFMMGeometry:
             setattr(g, name, scalars[name])
         else:
             typ = _CT[kind]
-            setattr(g, name, ctypes.cast(ctypes.c_void_p(ptr_of(arrays[name])), typ))
+            a = arrays.get(name)
+            addr = ptr_of(a) if a is not None else None     # absent optional array: NULL
+            setattr(g, name, ctypes.cast(ctypes.c_void_p(addr), typ))
     return g
 
 

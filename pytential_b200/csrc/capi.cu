@@ -5,6 +5,7 @@
 // all in the driver's order.  Stage outputs are accumulated (+=) into caller-owned
 // device buffers; the library allocates no device memory.
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <new>
@@ -27,6 +28,13 @@ struct qbxfmm_plan {
   int ncf, ncq;
   bool trans_ok;                           // matrix form of M2L / M2M / L2L available
   TransHost th;
+  TransCfg tc;
+  bool h3;                                 // 3D Helmholtz
+  std::vector<double> h3gaunt;             // Gaunt table, [(nu,mu)][(n,m)][j]
+  // 3D Helmholtz: translation buffer and pair scratch registered by
+  // qbxfmm_precompute_translations, used by the translation stage entries
+  mutable const double* trans_dev = nullptr;
+  mutable double* scratch_dev = nullptr;
 };
 
 namespace {
@@ -51,6 +59,79 @@ int check_plan(const qbxfmm_plan* p)
 {
   if (!p) return fail(QBXFMM_ERR_ARG, "null plan");
   return QBXFMM_OK;
+}
+
+// Gaunt integrals G(n,m; nu,mu; l) = int Y_n^m conj(Y_nu^mu) conj(Y_l^{m-mu}) for
+// n, nu <= p (orthonormal spherical harmonics without the Condon-Shortley phase),
+// l = |n - nu| + 2 j, j <= min(n, nu); layout [(nu,mu)][(n,m)][j], j < p + 1.  Exact
+// Gauss-Legendre quadrature in cos(theta) of the polynomial integrand.
+std::vector<double> h3_gaunt_table(int p)
+{
+  const int C = (p + 1) * (p + 1), nl = p + 1, L = 2 * p, ng = 2 * p + 2;
+  std::vector<double> x(ng), w(ng);
+  for (int i = 0; i < ng; ++i) {
+    double z = std::cos(M_PI * (i + 0.75) / (ng + 0.5)), pp = 0.0;
+    for (int it = 0; it < 100; ++it) {
+      double p1 = 1.0, p2 = 0.0;
+      for (int j = 1; j <= ng; ++j) {
+        double p3 = p2;
+        p2 = p1;
+        p1 = ((2.0 * j - 1.0) * z * p2 - (j - 1.0) * p3) / j;
+      }
+      pp = ng * (z * p1 - p2) / (z * z - 1.0);
+      double z1 = z;
+      z = z1 - p1 / pp;
+      if (std::fabs(z - z1) < 1e-16) break;
+    }
+    x[i] = z;
+    w[i] = 2.0 / ((1.0 - z * z) * pp * pp);
+  }
+  // polynomial parts p_n^m(t) (normalized; Y_n^m = p_n^m sin^m e^{i m phi}), n <= L
+  auto pidx = [](int n, int m) { return n * (n + 1) / 2 + m; };
+  std::vector<double> P((size_t)(L + 1) * (L + 2) / 2 * ng);
+  for (int i = 0; i < ng; ++i) {
+    double t = x[i], pmm = 0.28209479177387814347;
+    for (int m = 0; m <= L; ++m) {
+      if (m > 0) pmm *= std::sqrt((2.0 * m + 1.0) / (2.0 * m));
+      double pm2 = 0.0, pm1 = pmm;
+      P[(size_t)pidx(m, m) * ng + i] = pmm;
+      for (int n = m + 1; n <= L; ++n) {
+        double pn;
+        if (n == m + 1) {
+          pn = std::sqrt(2.0 * m + 3.0) * t * pm1;
+        } else {
+          double a = std::sqrt((4.0 * n * n - 1.0) / ((double)n * n - (double)m * m));
+          double b = std::sqrt(((n - 1.0) * (n - 1.0) - (double)m * m) / (4.0 * (n - 1.0) * (n - 1.0) - 1.0));
+          pn = a * (t * pm1 - b * pm2);
+        }
+        pm2 = pm1;
+        pm1 = pn;
+        P[(size_t)pidx(n, m) * ng + i] = pn;
+      }
+    }
+  }
+  std::vector<double> G((size_t)C * C * nl, 0.0);
+  for (int nu = 0; nu <= p; ++nu)
+    for (int mu = -nu; mu <= nu; ++mu)
+      for (int n = 0; n <= p; ++n)
+        for (int m = -n; m <= n; ++m) {
+          int lam = m - mu, am = std::abs(m), amu = std::abs(mu), alam = std::abs(lam);
+          int e = (am + amu + alam) / 2;
+          size_t base = ((size_t)(nu * nu + nu + mu) * C + (n * n + n + m)) * nl;
+          for (int j = 0; j <= std::min(n, nu); ++j) {
+            int l = std::abs(n - nu) + 2 * j;
+            if (alam > l) continue;
+            double acc = 0.0;
+            for (int i = 0; i < ng; ++i) {
+              double om = 1.0;
+              for (int u = 0; u < e; ++u) om *= 1.0 - x[i] * x[i];
+              acc += w[i] * P[(size_t)pidx(n, am) * ng + i] * P[(size_t)pidx(nu, amu) * ng + i] *
+                     P[(size_t)pidx(l, alam) * ng + i] * om;
+            }
+            G[base + j] = 2.0 * M_PI * acc;
+          }
+        }
+  return G;
 }
 
 #define QBX_TRY(expr, where)                         \
@@ -100,8 +181,6 @@ int qbxfmm_plan_create(const qbxfmm_kernel* kernel, const qbxfmm_geometry* geome
   if (k.family != QBXFMM_LAPLACE && k.family != QBXFMM_HELMHOLTZ)
     return fail(QBXFMM_ERR_UNSUPPORTED, "kernel family must be Laplace or Helmholtz");
   if (k.dim != 2 && k.dim != 3) return fail(QBXFMM_ERR_ARG, "dim must be 2 or 3");
-  if (k.family == QBXFMM_HELMHOLTZ && k.dim != 2)
-    return fail(QBXFMM_ERR_UNSUPPORTED, "the Helmholtz family is built for 2D only");
   if (k.family == QBXFMM_HELMHOLTZ && (k.k_im != 0.0 || !(k.k_re > 0.0)))
     return fail(QBXFMM_ERR_UNSUPPORTED, "Helmholtz wave number must be real and positive");
   if (g.dim != k.dim) return fail(QBXFMM_ERR_ARG, "kernel and geometry dimensions differ");
@@ -113,6 +192,14 @@ int qbxfmm_plan_create(const qbxfmm_kernel* kernel, const qbxfmm_geometry* geome
   if (k.precision != 0) return fail(QBXFMM_ERR_UNSUPPORTED, "only precision 0 (FP64)");
   if (k.target_specific_qbx && k.family != QBXFMM_LAPLACE)
     return fail(QBXFMM_ERR_UNSUPPORTED, "target-specific QBX is built for the Laplace family");
+  if (k.family == QBXFMM_HELMHOLTZ && k.dim == 3) {
+    if (k.qbx_order > 5 || k.qbx_order > k.fmm_order)
+      return fail(QBXFMM_ERR_UNSUPPORTED, "3D Helmholtz: qbx_order must be <= min(5, fmm_order)");
+    if (k.fmm_order > 17)
+      return fail(QBXFMM_ERR_UNSUPPORTED, "3D Helmholtz: fmm_order must be <= 17");
+    if (g.m2l_nclasses > 0 && !g.m2l_class_levels)
+      return fail(QBXFMM_ERR_ARG, "3D Helmholtz needs per-level M2L classes (m2l_class_levels)");
+  }
   if (k.family == QBXFMM_LAPLACE && (k.charge_coeff_im != 0.0 || k.dipole_coeff_im != 0.0))
     return fail(QBXFMM_ERR_ARG, "Laplace source coefficients must be real");
   if (g.nlevels < 1 || g.nboxes < 1 || g.nlevels > 40) return fail(QBXFMM_ERR_ARG, "bad tree sizes");
@@ -138,7 +225,16 @@ int qbxfmm_plan_create(const qbxfmm_kernel* kernel, const qbxfmm_geometry* geome
   if (e == cudaSuccess)
     e = cudaMemcpy(p->lvl_ttp.data(), g.level_start_ttp_box_nrs, sizeof(int32_t) * (g.nlevels + 1),
                    cudaMemcpyDeviceToHost);
-  p->trans_ok = !p->helm && k.dim == 3 && trans_supported(k.fmm_order) && g.nlevels <= 64;
+  p->h3 = p->helm && k.dim == 3;
+  if (k.dim == 3)
+    p->tc = p->h3 ? trans_cfg_helm3(k.fmm_order, g.m2l_nclasses, g.nlevels)
+                  : trans_cfg_laplace3(k.fmm_order, g.m2l_nclasses);
+  p->trans_ok = k.dim == 3 && trans_supported(p->tc) && g.nlevels <= 64;
+  if (p->h3 && !p->trans_ok) {
+    delete p;
+    return fail(QBXFMM_ERR_UNSUPPORTED, "3D Helmholtz: translation matrices unsupported for this order");
+  }
+  if (p->h3) p->h3gaunt = h3_gaunt_table(k.fmm_order);
   if (e == cudaSuccess && p->trans_ok) {
     const int nch = 8;
     std::vector<int32_t> cs(g.m2l_nclasses + 1), ms(g.nlevels * nch + 1), ls(g.nlevels * nch + 1);
@@ -194,6 +290,12 @@ int qbxfmm_form_strengths(const qbxfmm_plan* p, const qbxfmm_upsample* up, const
 int qbxfmm_form_multipoles(const qbxfmm_plan* p, const void* strengths, void* mpoles, void* stream)
 {
   if (int rc = check_plan(p)) return rc;
+  if (p->h3) {
+    QBX_TRY(h3_launch_p2m(p->geo, p->hc, p->kern.fmm_order, p->kern.nrhs, (const double2*)strengths,
+                          (double2*)mpoles, S(stream)),
+            "form_multipoles");
+    return QBXFMM_OK;
+  }
   if (p->helm)
     QBX_TRY(h2_launch_p2m(p->geo, p->hc, p->kern.fmm_order, p->kern.nrhs,
                           (const double2*)strengths, (double2*)mpoles, nullptr, S(stream)),
@@ -208,6 +310,14 @@ int qbxfmm_form_multipoles(const qbxfmm_plan* p, const void* strengths, void* mp
 int qbxfmm_coarsen_multipoles(const qbxfmm_plan* p, void* mpoles, void* stream)
 {
   if (int rc = check_plan(p)) return rc;
+  if (p->h3) {
+    if (!p->trans_dev || !p->scratch_dev)
+      return fail(QBXFMM_ERR_ARG, "3D Helmholtz: call qbxfmm_precompute_translations first");
+    QBX_TRY(launch_m2m_gemm(p->geo, p->th, p->tc, p->kern.nrhs, p->trans_dev, (double2*)mpoles,
+                            p->scratch_dev, nullptr, S(stream)),
+            "coarsen_multipoles");
+    return QBXFMM_OK;
+  }
   if (p->helm)
     QBX_TRY(h2_launch_m2m(p->geo, p->lvl_source_parent.data(), p->hc, p->kern.fmm_order,
                           p->kern.nrhs, (double2*)mpoles, nullptr, S(stream)),
@@ -223,6 +333,12 @@ int qbxfmm_eval_direct(const qbxfmm_plan* p, const void* strengths, void* pot_no
                        int32_t* error_word, void* stream)
 {
   if (int rc = check_plan(p)) return rc;
+  if (p->h3) {
+    QBX_TRY(h3_launch_eval_direct(p->geo, p->hc, p->kern.nrhs, (const double2*)strengths,
+                                  (double2*)pot_nonqbx, error_word, S(stream)),
+            "eval_direct");
+    return QBXFMM_OK;
+  }
   if (p->helm)
     QBX_TRY(h2_launch_eval_direct(p->geo, p->hc, p->kern.nrhs, (const double2*)strengths,
                                   (double2*)pot_nonqbx, error_word, S(stream)),
@@ -238,6 +354,15 @@ int qbxfmm_multipole_to_local(const qbxfmm_plan* p, const void* mpoles, void* lo
                               int32_t* error_word, void* stream)
 {
   if (int rc = check_plan(p)) return rc;
+  if (p->h3) {
+    if (!p->trans_dev || !p->scratch_dev)
+      return fail(QBXFMM_ERR_ARG, "3D Helmholtz: call qbxfmm_precompute_translations first");
+    QBX_TRY(launch_m2l_gemm(p->geo, p->th, p->tc, p->kern.nrhs, p->trans_dev,
+                            (const double2*)mpoles, (double2*)locals, p->scratch_dev, error_word,
+                            S(stream)),
+            "multipole_to_local");
+    return QBXFMM_OK;
+  }
   if (p->helm)
     QBX_TRY(h2_launch_m2l(p->geo, p->hc, p->kern.fmm_order, p->kern.nrhs, (const double2*)mpoles,
                           (double2*)locals, error_word, S(stream)),
@@ -253,6 +378,13 @@ int qbxfmm_eval_multipoles(const qbxfmm_plan* p, const void* mpoles, void* pot_n
                            int32_t* error_word, void* stream)
 {
   if (int rc = check_plan(p)) return rc;
+  if (p->h3) {
+    QBX_TRY(h3_launch_eval_multipoles(p->geo, p->hc, p->kern.fmm_order, p->kern.nrhs,
+                                      (const double2*)mpoles, (double2*)pot_nonqbx, error_word,
+                                      S(stream)),
+            "eval_multipoles");
+    return QBXFMM_OK;
+  }
   if (p->helm)
     QBX_TRY(h2_launch_eval_multipoles(p->geo, p->hc, p->kern.fmm_order, p->kern.nrhs,
                                       (const double2*)mpoles, (double2*)pot_nonqbx, error_word,
@@ -269,6 +401,12 @@ int qbxfmm_form_locals(const qbxfmm_plan* p, const void* strengths, void* locals
                        int32_t* error_word, void* stream)
 {
   if (int rc = check_plan(p)) return rc;
+  if (p->h3) {
+    QBX_TRY(h3_launch_p2l(p->geo, p->hc, p->kern.fmm_order, p->kern.nrhs, (const double2*)strengths,
+                          (double2*)locals, error_word, S(stream)),
+            "form_locals");
+    return QBXFMM_OK;
+  }
   if (p->helm)
     QBX_TRY(h2_launch_p2l(p->geo, p->hc, p->kern.fmm_order, p->kern.nrhs,
                           (const double2*)strengths, (double2*)locals, error_word, S(stream)),
@@ -283,6 +421,14 @@ int qbxfmm_form_locals(const qbxfmm_plan* p, const void* strengths, void* locals
 int qbxfmm_refine_locals(const qbxfmm_plan* p, void* locals, void* stream)
 {
   if (int rc = check_plan(p)) return rc;
+  if (p->h3) {
+    if (!p->trans_dev)
+      return fail(QBXFMM_ERR_ARG, "3D Helmholtz: call qbxfmm_precompute_translations first");
+    QBX_TRY(launch_l2l_gemm(p->geo, p->th, p->tc, p->kern.nrhs, p->trans_dev, (double2*)locals,
+                            nullptr, S(stream)),
+            "refine_locals");
+    return QBXFMM_OK;
+  }
   if (p->helm)
     QBX_TRY(h2_launch_l2l(p->geo, p->lvl_ttp.data(), p->hc, p->kern.fmm_order, p->kern.nrhs,
                           (double2*)locals, nullptr, S(stream)),
@@ -297,6 +443,12 @@ int qbxfmm_refine_locals(const qbxfmm_plan* p, void* locals, void* stream)
 int qbxfmm_eval_locals(const qbxfmm_plan* p, const void* locals, void* pot_nonqbx, void* stream)
 {
   if (int rc = check_plan(p)) return rc;
+  if (p->h3) {
+    QBX_TRY(h3_launch_eval_locals(p->geo, p->hc, p->kern.fmm_order, p->kern.nrhs,
+                                  (const double2*)locals, (double2*)pot_nonqbx, S(stream)),
+            "eval_locals");
+    return QBXFMM_OK;
+  }
   if (p->helm)
     QBX_TRY(h2_launch_eval_locals(p->geo, p->hc, p->kern.fmm_order, p->kern.nrhs,
                                   (const double2*)locals, (double2*)pot_nonqbx, nullptr, S(stream)),
@@ -312,6 +464,12 @@ int qbxfmm_form_global_qbx_locals(const qbxfmm_plan* p, const void* strengths, v
                                   int32_t* error_word, void* stream)
 {
   if (int rc = check_plan(p)) return rc;
+  if (p->h3) {
+    QBX_TRY(h3_launch_p2qbxl(p->geo, p->hc, p->kern.qbx_order, p->kern.nrhs,
+                             (const double2*)strengths, (double2*)qbx_exps, error_word, S(stream)),
+            "form_global_qbx_locals");
+    return QBXFMM_OK;
+  }
   if (p->helm)
     QBX_TRY(h2_launch_p2qbxl(p->geo, p->hc, p->kern.qbx_order, p->kern.nrhs,
                              (const double2*)strengths, (double2*)qbx_exps, error_word, S(stream)),
@@ -327,6 +485,15 @@ int qbxfmm_translate_box_multipoles_to_qbx_local(const qbxfmm_plan* p, const voi
                                                  void* qbx_exps, int32_t* error_word, void* stream)
 {
   if (int rc = check_plan(p)) return rc;
+  if (p->h3) {
+    if (!p->trans_dev)
+      return fail(QBXFMM_ERR_ARG, "3D Helmholtz: call qbxfmm_precompute_translations first");
+    QBX_TRY(h3_launch_m2qbxl(p->geo, p->hc, p->kern.fmm_order, p->kern.qbx_order, p->kern.nrhs,
+                             (const double2*)mpoles, p->trans_dev + p->tc.nmatrices * p->tc.rp * p->tc.kp,
+                             (double2*)qbx_exps, error_word, S(stream)),
+            "translate_box_multipoles_to_qbx_local");
+    return QBXFMM_OK;
+  }
   if (p->helm)
     QBX_TRY(h2_launch_m2qbxl(p->geo, p->hc, p->kern.fmm_order, p->kern.qbx_order, p->kern.nrhs,
                              (const double2*)mpoles, (double2*)qbx_exps, error_word, S(stream)),
@@ -342,6 +509,15 @@ int qbxfmm_translate_box_local_to_qbx_local(const qbxfmm_plan* p, const void* lo
                                             void* qbx_exps, void* stream)
 {
   if (int rc = check_plan(p)) return rc;
+  if (p->h3) {
+    if (!p->trans_dev)
+      return fail(QBXFMM_ERR_ARG, "3D Helmholtz: call qbxfmm_precompute_translations first");
+    QBX_TRY(h3_launch_l2qbxl(p->geo, p->hc, p->kern.fmm_order, p->kern.qbx_order, p->kern.nrhs,
+                             (const double2*)locals, p->trans_dev + p->tc.nmatrices * p->tc.rp * p->tc.kp,
+                             (double2*)qbx_exps, nullptr, S(stream)),
+            "translate_box_local_to_qbx_local");
+    return QBXFMM_OK;
+  }
   if (p->helm)
     QBX_TRY(h2_launch_l2qbxl(p->geo, p->hc, p->kern.fmm_order, p->kern.qbx_order, p->kern.nrhs,
                              (const double2*)locals, (double2*)qbx_exps, nullptr, S(stream)),
@@ -357,6 +533,12 @@ int qbxfmm_eval_qbx_expansions(const qbxfmm_plan* p, const void* qbx_exps, void*
                                void* stream)
 {
   if (int rc = check_plan(p)) return rc;
+  if (p->h3) {
+    QBX_TRY(h3_launch_qbxl2p(p->geo, p->hc, p->kern.qbx_order, p->kern.nrhs,
+                             (const double2*)qbx_exps, (double2*)pot_tree, S(stream)),
+            "eval_qbx_expansions");
+    return QBXFMM_OK;
+  }
   if (p->helm)
     QBX_TRY(h2_launch_qbxl2p(p->geo, p->hc, p->kern.qbx_order, p->kern.nrhs,
                              (const double2*)qbx_exps, (double2*)pot_tree, S(stream)),
@@ -384,6 +566,12 @@ int qbxfmm_assemble(const qbxfmm_plan* p, const void* pot_nonqbx, const void* po
                     void* stream)
 {
   if (int rc = check_plan(p)) return rc;
+  if (p->h3) {
+    QBX_TRY(h3_launch_assemble(p->geo, p->kern.nrhs, (const double2*)pot_nonqbx,
+                               (const double2*)pot_tree, (double2*)out, S(stream)),
+            "assemble");
+    return QBXFMM_OK;
+  }
   if (p->helm)
     QBX_TRY(h2_launch_assemble(p->geo, p->kern.nrhs, (const double2*)pot_nonqbx,
                                (const double2*)pot_tree, (double2*)out, S(stream)),
@@ -414,8 +602,8 @@ int qbxfmm_workspace_sizes(const qbxfmm_plan* p, size_t* sizes6 /* 8 entries */)
                                cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return cuda_check(e, "workspace_sizes");
     npairs = std::max(npairs, g.m2m_npairs);
-    sizes6[6] = trans_matrix_bytes(p->kern.fmm_order, g.m2l_nclasses);
-    sizes6[7] = trans_scratch_bytes(p->kern.fmm_order, npairs, p->kern.nrhs);
+    sizes6[6] = trans_matrix_bytes(p->tc) + p->h3gaunt.size() * sizeof(double);
+    sizes6[7] = trans_scratch_bytes(p->tc, npairs, p->kern.nrhs);
   } else {
     sizes6[6] = sizes6[7] = 0;
   }
@@ -426,8 +614,22 @@ int qbxfmm_precompute_translations(const qbxfmm_plan* p, const qbxfmm_workspace*
 {
   if (int rc = check_plan(p)) return rc;
   if (!ws) return fail(QBXFMM_ERR_ARG, "null workspace");
+  if (p->h3) {
+    if (!ws->translations || !ws->pair_scratch)
+      return fail(QBXFMM_ERR_ARG, "3D Helmholtz needs the translations and pair-scratch buffers");
+    double* T = (double*)ws->translations;
+    double* G = T + p->tc.nmatrices * p->tc.rp * p->tc.kp;
+    QBX_TRY(cudaMemcpyAsync(G, p->h3gaunt.data(), p->h3gaunt.size() * sizeof(double),
+                            cudaMemcpyHostToDevice, S(stream)),
+            "precompute_translations: Gaunt table");
+    QBX_TRY(h3_launch_trans_build(p->geo, p->tc, p->kern.k_re, G, T, S(stream)),
+            "precompute_translations");
+    p->trans_dev = T;
+    p->scratch_dev = (double*)ws->pair_scratch;
+    return QBXFMM_OK;
+  }
   if (!p->trans_ok || !ws->translations) return QBXFMM_OK;
-  QBX_TRY(launch_trans_build(p->geo, p->kern.fmm_order, (double*)ws->translations, S(stream)),
+  QBX_TRY(launch_trans_build(p->geo, p->tc, (double*)ws->translations, S(stream)),
           "precompute_translations");
   return QBXFMM_OK;
 }
@@ -442,7 +644,13 @@ int qbxfmm_apply(const qbxfmm_plan* p, const qbxfmm_upsample* up, const qbxfmm_w
     return fail(QBXFMM_ERR_ARG, "incomplete workspace");
   size_t sz[8];
   if (int rc = qbxfmm_workspace_sizes(p, sz)) return rc;
-  const bool gemm = p->trans_ok && ws->translations && ws->pair_scratch;
+  const bool gemm = !p->h3 && p->trans_ok && ws->translations && ws->pair_scratch;
+  if (p->h3) {
+    if (!ws->translations || !ws->pair_scratch)
+      return fail(QBXFMM_ERR_ARG, "3D Helmholtz needs the translations and pair-scratch buffers");
+    p->trans_dev = (const double*)ws->translations;
+    p->scratch_dev = (double*)ws->pair_scratch;
+  }
   cudaStream_t st = S(stream);
   QBX_TRY(cudaMemsetAsync(ws->mpoles, 0, sz[1], st), "apply: clear");
   QBX_TRY(cudaMemsetAsync(ws->locals, 0, sz[2], st), "apply: clear");
@@ -455,7 +663,7 @@ int qbxfmm_apply(const qbxfmm_plan* p, const qbxfmm_upsample* up, const qbxfmm_w
   if ((rc = qbxfmm_form_strengths(p, up, density, ws->strengths, stream))) return rc;
   if ((rc = qbxfmm_form_multipoles(p, ws->strengths, ws->mpoles, stream))) return rc;
   if (gemm)
-    QBX_TRY(launch_m2m_gemm(p->geo, p->th, p->kern.fmm_order, p->kern.nrhs,
+    QBX_TRY(launch_m2m_gemm(p->geo, p->th, p->tc, p->kern.nrhs,
                             (const double*)ws->translations, (double2*)ws->mpoles,
                             (double*)ws->pair_scratch, ws->error_word, S(stream)),
             "coarsen_multipoles (matrix form)");
@@ -463,7 +671,7 @@ int qbxfmm_apply(const qbxfmm_plan* p, const qbxfmm_upsample* up, const qbxfmm_w
     return rc;
   if ((rc = qbxfmm_eval_direct(p, ws->strengths, ws->pot_nonqbx, ws->error_word, stream))) return rc;
   if (gemm)
-    QBX_TRY(launch_m2l_gemm(p->geo, p->th, p->kern.fmm_order, p->kern.nrhs,
+    QBX_TRY(launch_m2l_gemm(p->geo, p->th, p->tc, p->kern.nrhs,
                             (const double*)ws->translations, (const double2*)ws->mpoles,
                             (double2*)ws->locals, (double*)ws->pair_scratch, ws->error_word,
                             S(stream)),
@@ -473,7 +681,7 @@ int qbxfmm_apply(const qbxfmm_plan* p, const qbxfmm_upsample* up, const qbxfmm_w
   if ((rc = qbxfmm_eval_multipoles(p, ws->mpoles, ws->pot_nonqbx, ws->error_word, stream))) return rc;
   if ((rc = qbxfmm_form_locals(p, ws->strengths, ws->locals, ws->error_word, stream))) return rc;
   if (gemm)
-    QBX_TRY(launch_l2l_gemm(p->geo, p->th, p->kern.fmm_order, p->kern.nrhs,
+    QBX_TRY(launch_l2l_gemm(p->geo, p->th, p->tc, p->kern.nrhs,
                             (const double*)ws->translations, (double2*)ws->locals, ws->error_word,
                             S(stream)),
             "refine_locals (matrix form)");

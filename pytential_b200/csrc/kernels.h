@@ -15,18 +15,30 @@ struct TransHost {
   const int32_t* lvl_source_parent = nullptr;   // host copy (owned by the plan)
 };
 
-bool trans_supported(int p);
-size_t trans_matrix_bytes(int p, int nclasses);
-size_t trans_scratch_bytes(int p, int npairs, int nrhs);
-cudaError_t launch_trans_build(const qbxfmm_geometry& g, int p, double* T, cudaStream_t st);
-cudaError_t launch_m2l_gemm(const qbxfmm_geometry& g, const TransHost& th, int p, int nrhs,
-                            const double* T, const double2* mp, double2* lo, double* cpair,
-                            int32_t* err, cudaStream_t st);
-cudaError_t launch_m2m_gemm(const qbxfmm_geometry& g, const TransHost& th, int p, int nrhs,
-                            const double* T, double2* mp, double* cpair, int32_t* err,
+// shape of the matrix-form translations: real (rp x kp) matrices acting on
+// interleaved (re, im) vectors of ncf complex coefficients
+struct TransCfg {
+  int p = 0, ncf = 0, rp = 0, kp = 0;
+  int m2m_mat_mod = 8;        // M2M / L2L matrix = base + group % mod (mod 0: base + group)
+  size_t m2m_base = 0, l2l_base = 0;
+  int m2l_div_by_width = 1;   // M2L reduction scales by 1 / box width (Laplace)
+  size_t nmatrices = 0;
+};
+
+TransCfg trans_cfg_laplace3(int p, int nclasses);
+TransCfg trans_cfg_helm3(int p, int nclasses, int nlevels);
+bool trans_supported(const TransCfg& c);
+size_t trans_matrix_bytes(const TransCfg& c);
+size_t trans_scratch_bytes(const TransCfg& c, int npairs, int nrhs);
+cudaError_t launch_trans_build(const qbxfmm_geometry& g, const TransCfg& c, double* T, cudaStream_t st);
+cudaError_t launch_m2l_gemm(const qbxfmm_geometry& g, const TransHost& th, const TransCfg& c,
+                            int nrhs, const double* T, const double2* mp, double2* lo,
+                            double* cpair, int32_t* err, cudaStream_t st);
+cudaError_t launch_m2m_gemm(const qbxfmm_geometry& g, const TransHost& th, const TransCfg& c,
+                            int nrhs, const double* T, double2* mp, double* cpair, int32_t* err,
                             cudaStream_t st);
-cudaError_t launch_l2l_gemm(const qbxfmm_geometry& g, const TransHost& th, int p, int nrhs,
-                            const double* T, double2* lo, int32_t* err, cudaStream_t st);
+cudaError_t launch_l2l_gemm(const qbxfmm_geometry& g, const TransHost& th, const TransCfg& c,
+                            int nrhs, const double* T, double2* lo, int32_t* err, cudaStream_t st);
 
 cudaError_t launch_form_strengths(const qbxfmm_geometry& g, const qbxfmm_upsample& up, int nrhs,
                                   const double* density, double* strengths, cudaStream_t st);
@@ -88,5 +100,31 @@ cudaError_t h2_launch_qbxl2p(const qbxfmm_geometry& g, HelmCoeffs hc, int q, int
                              const double2* qe, double2* pt, cudaStream_t st);
 cudaError_t h2_launch_assemble(const qbxfmm_geometry& g, int nrhs, const double2* pot_nonqbx,
                                const double2* pot_tree, double2* out, cudaStream_t st);
+
+// 3D Helmholtz (complex128; translations through the matrices / Gaunt table)
+cudaError_t h3_launch_p2m(const qbxfmm_geometry& g, HelmCoeffs hc, int p, int nrhs,
+                          const double2* s, double2* mp, cudaStream_t st);
+cudaError_t h3_launch_p2l(const qbxfmm_geometry& g, HelmCoeffs hc, int p, int nrhs,
+                          const double2* s, double2* lo, int32_t* err, cudaStream_t st);
+cudaError_t h3_launch_eval_direct(const qbxfmm_geometry& g, HelmCoeffs hc, int nrhs,
+                                  const double2* s, double2* pot, int32_t* err, cudaStream_t st);
+cudaError_t h3_launch_eval_multipoles(const qbxfmm_geometry& g, HelmCoeffs hc, int p, int nrhs,
+                                      const double2* mp, double2* pot, int32_t* err, cudaStream_t st);
+cudaError_t h3_launch_eval_locals(const qbxfmm_geometry& g, HelmCoeffs hc, int p, int nrhs,
+                                  const double2* lo, double2* pot, cudaStream_t st);
+cudaError_t h3_launch_p2qbxl(const qbxfmm_geometry& g, HelmCoeffs hc, int q, int nrhs,
+                             const double2* s, double2* qe, int32_t* err, cudaStream_t st);
+cudaError_t h3_launch_m2qbxl(const qbxfmm_geometry& g, HelmCoeffs hc, int pf, int q, int nrhs,
+                             const double2* mp, const double* gaunt, double2* qe, int32_t* err,
+                             cudaStream_t st);
+cudaError_t h3_launch_l2qbxl(const qbxfmm_geometry& g, HelmCoeffs hc, int pf, int q, int nrhs,
+                             const double2* lo, const double* gaunt, double2* qe, int32_t* err,
+                             cudaStream_t st);
+cudaError_t h3_launch_qbxl2p(const qbxfmm_geometry& g, HelmCoeffs hc, int q, int nrhs,
+                             const double2* qe, double2* pt, cudaStream_t st);
+cudaError_t h3_launch_assemble(const qbxfmm_geometry& g, int nrhs, const double2* pot_nonqbx,
+                               const double2* pot_tree, double2* out, cudaStream_t st);
+cudaError_t h3_launch_trans_build(const qbxfmm_geometry& g, const TransCfg& tc, double k,
+                                  const double* gaunt, double* T, cudaStream_t st);
 
 }  // namespace qbx

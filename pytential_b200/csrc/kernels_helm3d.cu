@@ -1,0 +1,1223 @@
+// 3D Helmholtz QBX-FMM stage kernels, complex128, sm_100a.
+//
+// Kernel G(x, y) = e^{ik|x-y|} / |x-y| (k real), scaled by 1/(4 pi) at assembly.
+// Spherical-wave expansions (the basis of pytential's fmmlib backend,
+// pytential/qbx/fmmlib.py, and of its target-specific module,
+// pytential/qbx/target_specific/impl.pyx:363-563):
+//   Y_n^m = p_n^|m|(cos t) sin^|m| t e^{i m phi} (orthonormal, no Condon-Shortley phase),
+//   R_n^m(v) = j_n(k|v|) Y_n^m(v),  S_n^m(v) = h_n(k|v|) Y_n^m(v),
+//   multipole about c: sum M_nm S_n^m(x - c), M_nm = 4 pi i k q R_n^-m(y - c) / s^n,
+//   local about c:     sum L_nm R_n^m(x - c), L_nm = 4 pi i k q S_n^-m(y - c) s^n,
+// with s = min(1, k rho) (rho = box width or expansion radius) and coefficient index
+// n^2 + n + m.  Translations use the addition theorem
+//   F_n^m(r + b) = sum c_{nu mu; n m}(b) R_nu^mu(r),
+//   c_{nu mu; n m}(b) = 4 pi sum_l i^{nu + l - n} f_l(k|b|) Y_l^{m - mu}(b) G(n,m; nu,mu; l)
+// (G: Gaunt integrals, a host-computed table), applied as per-level, per-class
+// complex matrices on the FP64 tensor cores for M2M / M2L / L2L and directly for the
+// point-to-box translations into QBX centers.  Source-normal derivatives use the
+// ladder relations of R and S.
+#include <cooperative_groups.h>
+
+#include "laplace.cuh"
+#include "kernels.h"
+
+namespace cg = cooperative_groups;
+
+namespace qbx {
+
+namespace {
+
+constexpr int NT = 128;
+constexpr int NW = NT / 32;
+constexpr int MAXB = 128;
+constexpr int H3_LMAX = 44;        // largest order of a radial / harmonic table
+constexpr double FOUR_PI = 12.566370614359172953850573533118;
+
+QBX_HD int hq(int n, int m) { return n * n + n + m; }
+
+QBX_HD void hq_decode(int c, int& n, int& m)
+{
+  n = (int)sqrt((double)c);
+  while ((n + 1) * (n + 1) <= c) ++n;
+  while (n * n > c) --n;
+  m = c - n * n - n;
+}
+
+// Recurrence table for the normalized associated Legendre polynomial parts, n <= N:
+// rec[idx3(n, m)] = (p_m^m, 0) at n = m, (sqrt(2m + 3), 0) at n = m + 1, else
+// (a_nm, b_nm) with p_n^m = a_nm (t p_{n-1}^m - b_nm p_{n-2}^m).
+QBX_D void h3_rec_table(int N, double2* rec, int tid, int nt)
+{
+  int tot = (N + 1) * (N + 2) / 2;
+  for (int e = tid; e < tot; e += nt) {
+    int n, m;
+    decode3(e, n, m);
+    double a, b = 0.0;
+    if (n == m) {
+      a = 0.28209479177387814347;   // 1 / sqrt(4 pi)
+      for (int i = 1; i <= m; ++i) a *= sqrt((2.0 * i + 1.0) / (2.0 * i));
+    } else if (n == m + 1) {
+      a = sqrt(2.0 * m + 3.0);
+    } else {
+      a = sqrt((4.0 * n * n - 1.0) / ((double)n * n - (double)m * m));
+      b = sqrt(((n - 1.0) * (n - 1.0) - (double)m * m) / (4.0 * (n - 1.0) * (n - 1.0) - 1.0));
+    }
+    rec[e] = c2(a, b);
+  }
+}
+
+// t = cos(theta), w = sin(theta) e^{i phi} of v (v = 0: t = 1, w = 0)
+QBX_D double h3_dir(const double* v, double2& w, double& r)
+{
+  r = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+  if (r == 0.0) {
+    w = c2(0.0);
+    return 1.0;
+  }
+  double ri = 1.0 / r;
+  w = c2(v[0] * ri, v[1] * ri);
+  return v[2] * ri;
+}
+
+// j_n(x), n <= N, by Miller's backward recurrence normalized with j_0 or j_1
+QBX_D void h3_sph_j(int N, double x, double* jv)
+{
+  for (int n = 0; n <= N; ++n) jv[n] = 0.0;
+  if (x == 0.0) {
+    jv[0] = 1.0;
+    return;
+  }
+  int nmax = max(N, (int)x);
+  int start = nmax + 16 + (int)sqrt(40.0 * (nmax + 1));
+  double xi = 1.0 / x;
+  double fp1 = 0.0, f = 1e-200, f1 = 0.0;
+  for (int n = start; n >= 1; --n) {
+    double fm1 = (2.0 * n + 1.0) * xi * f - fp1;
+    fp1 = f;
+    f = fm1;
+    if (n - 1 <= N) jv[n - 1] = f;
+    if (n - 1 == 1) f1 = f;
+    if (fabs(f) > 1e200) {
+      f *= 1e-200;
+      fp1 *= 1e-200;
+      f1 *= 1e-200;
+      for (int j = n - 1; j <= N; ++j) jv[j] *= 1e-200;
+    }
+  }
+  double s, c;
+  sincos(x, &s, &c);
+  double scale = (x < 1.0 || fabs(s) >= 0.5) ? (s * xi) / f : ((s * xi - c) * xi) / f1;
+  for (int n = 0; n <= N; ++n) jv[n] *= scale;
+}
+
+// h_n(x) = j_n(x) + i y_n(x), n <= N, by the upward recurrence
+QBX_D void h3_sph_h(int N, double x, double2* hv)
+{
+  double s, c;
+  sincos(x, &s, &c);
+  double xi = 1.0 / x;
+  hv[0] = c2(s * xi, -c * xi);
+  if (N >= 1) hv[1] = c2((s - c * x) * xi * xi, -(s * x + c) * xi * xi);
+  for (int n = 1; n < N; ++n) {
+    double f = (2.0 * n + 1.0) * xi;
+    hv[n + 1] = c2(f * hv[n].x - hv[n - 1].x, f * hv[n].y - hv[n - 1].y);
+  }
+}
+
+// Ladder terms of nu . grad F_n^mm (mm = -m for the source coefficient (n, m)):
+// six table entries with real weights (0 where the entry is outside the table).
+// Order: z-, z+ (times nu_z), p+, p- (times (nu_x - i nu_y) / 2), m+, m- (times
+// (nu_x + i nu_y) / 2); entry offsets are hq() indices.
+struct Ladder {
+  int o[6];
+  double w[6];
+};
+
+QBX_HD Ladder h3_ladder(int n, int mm, double k)
+{
+  Ladder L;
+  for (int i = 0; i < 6; ++i) {
+    L.o[i] = 0;
+    L.w[i] = 0.0;
+  }
+  double an = sqrt((double)(n + 1 - mm) * (n + 1 + mm) / ((2.0 * n + 1) * (2.0 * n + 3)));
+  if (n >= 1 && abs(mm) <= n - 1) {
+    L.o[0] = hq(n - 1, mm);
+    L.w[0] = k * sqrt((double)(n - mm) * (n + mm) / ((2.0 * n - 1) * (2.0 * n + 1)));
+  }
+  L.o[1] = hq(n + 1, mm);
+  L.w[1] = -k * an;
+  double sgp = mm >= 0 ? 1.0 : -1.0, sgm = -mm >= 0 ? 1.0 : -1.0;
+  L.o[2] = hq(n + 1, mm + 1);
+  L.w[2] = -k * sgp * sqrt((double)(n + mm + 1) * (n + mm + 2) / ((2.0 * n + 1) * (2.0 * n + 3)));
+  if (n >= 1 && abs(mm + 1) <= n - 1) {
+    L.o[3] = hq(n - 1, mm + 1);
+    L.w[3] = -k * sgp * sqrt((double)(n - mm) * (n - mm - 1) / ((2.0 * n - 1) * (2.0 * n + 1)));
+  }
+  L.o[4] = hq(n + 1, mm - 1);
+  L.w[4] = -k * sgm * sqrt((double)(n - mm + 1) * (n - mm + 2) / ((2.0 * n + 1) * (2.0 * n + 3)));
+  if (n >= 1 && abs(mm - 1) <= n - 1) {
+    L.o[5] = hq(n - 1, mm - 1);
+    L.w[5] = -k * sgm * sqrt((double)(n + mm) * (n + mm - 1) / ((2.0 * n - 1) * (2.0 * n + 1)));
+  }
+  return L;
+}
+
+// Fill column m (n = m..N) of a wave table: T[hq(n, +-m) * ts] = f_n Y_n^{+-m}
+// (f = radial values, complex), given t, w and the recurrence table.
+QBX_D void h3_wave_column(int m, int N, double t, double2 w, const double2* rec, const double2* rad,
+                          double2* T, int ts)
+{
+  double2 wm = c2(1.0);
+  for (int i = 0; i < m; ++i) wm = cmul(wm, w);
+  double pm1 = rec[idx3(m, m)].x, pm2 = 0.0;
+  for (int n = m; n <= N; ++n) {
+    double pn;
+    if (n == m) {
+      pn = pm1;
+    } else if (n == m + 1) {
+      pn = rec[idx3(n, m)].x * t * pm1;
+      pm2 = pm1;
+      pm1 = pn;
+    } else {
+      double2 ab = rec[idx3(n, m)];
+      pn = ab.x * (t * pm1 - ab.y * pm2);
+      pm2 = pm1;
+      pm1 = pn;
+    }
+    double2 y = cscale(pn, wm);
+    T[hq(n, m) * ts] = cmul(rad[n], y);
+    if (m > 0) T[hq(n, -m) * ts] = cmul(rad[n], cconj(y));
+  }
+}
+
+QBX_D double h3_scale(double k, double rho) { return fmin(1.0, k * rho); }
+
+// i^e for integer e
+QBX_D double2 ipow(int e)
+{
+  switch (e & 3) {
+    case 0: return c2(1.0, 0.0);
+    case 1: return c2(0.0, 1.0);
+    case 2: return c2(-1.0, 0.0);
+    default: return c2(0.0, -1.0);
+  }
+}
+
+// list helpers (as in the Laplace kernels)
+QBX_D void h3_list_prefix(const qbxfmm_geometry& g, const int32_t* __restrict__ lists, int gb,
+                          int nb, int* s_pref, int* s_start, int32_t* err)
+{
+  if (threadIdx.x >= 32) return;
+  int lane = threadIdx.x;
+  int cnt[4], loc = 0;
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    int k = lane * 4 + u;
+    cnt[u] = 0;
+    if (k < nb) {
+      int sb = lists[gb + k];
+      int s0 = 0;
+      if ((unsigned)sb < (unsigned)g.nboxes) {
+        s0 = g.box_source_starts[sb];
+        cnt[u] = g.box_source_counts_nonchild[sb];
+      } else {
+        report(err, QBX_DEVERR_BAD_BOX);
+      }
+      s_start[k] = s0;
+    }
+    loc += cnt[u];
+  }
+  int incl = loc;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    int v = __shfl_up_sync(0xffffffffu, incl, off);
+    if (lane >= off) incl += v;
+  }
+  int run = incl - loc;
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    int k = lane * 4 + u;
+    if (k < nb) s_pref[k] = run;
+    run += cnt[u];
+  }
+  if (lane == 31) s_pref[nb] = incl;
+}
+
+QBX_D int h3_stream_source(int v, int nb, const int* s_pref, const int* s_start)
+{
+  int lo = 0, hi = nb - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (s_pref[mid] <= v) lo = mid;
+    else hi = mid - 1;
+  }
+  return s_start[lo] + (v - s_pref[lo]);
+}
+
+}  // namespace
+
+// {{{ P2M / P2L
+
+// One CTA per box (P2M: source boxes, own sources; P2L: target-or-parent boxes, list-4
+// sources).  Sources in sub-tiles of SUB: one thread per source computes the radial
+// values (j_n for P2M, h_n for P2L, n <= p + 1), one thread per (column, source)
+// fills the wave table (entry-major, padded stride), then one thread per coefficient
+// accumulates q F_n^-m + sigma nu . grad F_n^-m with precomputed ladder offsets.
+constexpr int H3_SUB = 16;
+constexpr int H3_TS = H3_SUB + 1;
+constexpr int H3_NH = 3;          // coefficients per thread: (p+1)^2 <= 3 * 128
+
+template <bool LOCAL>
+__global__ void __launch_bounds__(NT)
+k_h3_p2e(qbxfmm_geometry g, HelmCoeffs hc, int p, int nrhs, const double2* __restrict__ strengths,
+         double2* __restrict__ exps, int32_t* err)
+{
+  constexpr int SUB = H3_SUB, TS = H3_TS;
+  extern __shared__ double2 smem2[];
+  const int N = p + 1;
+  const int ncf = (p + 1) * (p + 1);
+  double2* tab = smem2;                              // [(N+1)^2][TS]
+  double2* rec = smem2 + (size_t)(N + 1) * (N + 1) * TS;   // [(N+1)(N+2)/2]
+  __shared__ double2 s_rad[SUB][H3_LMAX + 2];
+  __shared__ double s_t[SUB];
+  __shared__ double2 s_w[SUB], s_q[SUB], s_d[SUB], s_np[SUB], s_nm[SUB];
+  __shared__ double s_nz[SUB];
+  __shared__ int s_pref[MAXB + 1], s_start[MAXB];
+
+  int b, l0 = 0, l1 = 0;
+  if (LOCAL) {
+    int i = blockIdx.x;
+    b = g.target_or_target_parent_boxes[i];
+    l0 = g.list4_starts[i];
+    l1 = g.list4_starts[i + 1];
+    if (l1 <= l0) return;
+  } else {
+    b = g.source_boxes[blockIdx.x];
+  }
+  int r = blockIdx.y;
+  double rho = level_width(g, g.box_levels[b]);
+  double sc = h3_scale(hc.k, rho);
+  double c[3];
+  load_point<3>(g.box_centers, g.nboxes, b, c);
+  const double2* st = strengths + (size_t)r * g.nsources;
+  const bool dip = hc.cd.x != 0.0 || hc.cd.y != 0.0;
+  h3_rec_table(N, rec, threadIdx.x, NT);
+
+  int o_c[H3_NH];
+  Ladder lad[H3_NH];
+  bool valid[H3_NH];
+#pragma unroll
+  for (int h = 0; h < H3_NH; ++h) {
+    int ci = threadIdx.x + h * NT;
+    valid[h] = ci < ncf;
+    int n = 0, m = 0;
+    if (valid[h]) hq_decode(ci, n, m);
+    o_c[h] = hq(n, -m) * TS;
+    lad[h] = h3_ladder(n, -m, hc.k);
+#pragma unroll
+    for (int u = 0; u < 6; ++u) lad[h].o[u] *= TS;
+  }
+  double2 acc[H3_NH];
+#pragma unroll
+  for (int h = 0; h < H3_NH; ++h) acc[h] = c2(0.0);
+
+  // one stream over the box's own sources (P2M) or the list-4 boxes' sources (P2L)
+  for (int gb = l0; gb < (LOCAL ? l1 : 1); gb += MAXB) {
+    int nb = 0, total;
+    __syncthreads();
+    if (LOCAL) {
+      nb = min(MAXB, l1 - gb);
+      h3_list_prefix(g, g.list4_lists, gb, nb, s_pref, s_start, err);
+      __syncthreads();
+      total = s_pref[nb];
+    } else {
+      total = g.box_source_counts_nonchild[b];
+    }
+    int s0 = LOCAL ? 0 : g.box_source_starts[b];
+    for (int base = 0; base < total; base += SUB) {
+      int cnt = min(SUB, total - base);
+      __syncthreads();
+      if (threadIdx.x < cnt) {
+        int j = threadIdx.x;
+        int s = LOCAL ? h3_stream_source(base + j, nb, s_pref, s_start) : s0 + base + j;
+        double y[3], u[3], rr;
+        load_point<3>(g.sources, g.nsources, s, y);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) u[d] = y[d] - c[d];
+        double2 w;
+        s_t[j] = h3_dir(u, w, rr);
+        s_w[j] = w;
+        double x = hc.k * rr;
+        if (LOCAL) {
+          h3_sph_h(N, x, s_rad[j]);
+        } else {
+          double jv[H3_LMAX + 2];
+          h3_sph_j(N, x, jv);
+          for (int n = 0; n <= N; ++n) s_rad[j][n] = c2(jv[n]);
+        }
+        double2 sv = st[s];
+        s_q[j] = cmul(hc.cq, sv);
+        s_d[j] = cmul(hc.cd, sv);
+        if (dip) {
+          double nv[3];
+          load_point<3>(g.source_normals, g.nsources, s, nv);
+          s_np[j] = c2(0.5 * nv[0], -0.5 * nv[1]);
+          s_nm[j] = c2(0.5 * nv[0], 0.5 * nv[1]);
+          s_nz[j] = nv[2];
+        }
+      }
+      __syncthreads();
+      for (int wk = threadIdx.x; wk < cnt * (N + 1); wk += NT) {
+        int m = wk / cnt, j = wk - m * cnt;
+        h3_wave_column(m, N, s_t[j], s_w[j], rec, s_rad[j], tab + j, TS);
+      }
+      __syncthreads();
+#pragma unroll
+      for (int h = 0; h < H3_NH; ++h) {
+        if (!valid[h]) continue;
+        double2 a = acc[h];
+        for (int j = 0; j < cnt; ++j) {
+          const double2* T = tab + j;
+          a = cfma(s_q[j], T[o_c[h]], a);
+          if (dip) {
+            const Ladder& L = lad[h];
+            double2 vz = caxpy(L.w[0], T[L.o[0]], cscale(L.w[1], T[L.o[1]]));
+            double2 vp = caxpy(L.w[2], T[L.o[2]], cscale(L.w[3], T[L.o[3]]));
+            double2 vm = caxpy(L.w[4], T[L.o[4]], cscale(L.w[5], T[L.o[5]]));
+            double2 v = cfma(s_np[j], vp, cfma(s_nm[j], vm, cscale(s_nz[j], vz)));
+            a = cfma(s_d[j], v, a);
+          }
+        }
+        acc[h] = a;
+      }
+    }
+  }
+  double2* E = exps + ((size_t)b * nrhs + r) * ncf;
+#pragma unroll
+  for (int h = 0; h < H3_NH; ++h) {
+    if (!valid[h]) continue;
+    int ci = threadIdx.x + h * NT;
+    int n, m;
+    hq_decode(ci, n, m);
+    double f = FOUR_PI * hc.k * (LOCAL ? pow(sc, (double)n) : pow(sc, -(double)n));
+    // 4 pi i k f acc
+    E[ci] = cadd(E[ci], c2(-f * acc[h].y, f * acc[h].x));
+  }
+}
+
+// }}}
+
+// {{{ point evaluations at non-QBX targets
+
+constexpr int H3_PSPLIT = 8;
+
+QBX_D double2 h3_cluster_lane_sum(double2 acc, double2 (*s_red)[32], double2* s_part)
+{
+  cg::cluster_group cl = cg::this_cluster();
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();
+  if (warp > 0) s_red[warp - 1][lane] = acc;
+  __syncthreads();
+  if (warp == 0) {
+    for (int w = 1; w < NW; ++w) acc = cadd(acc, s_red[w - 1][lane]);
+    s_part[lane] = acc;
+  }
+  cl.sync();
+  if (cl.block_rank() == 0 && warp == 0) {
+    for (unsigned q = 1; q < cl.num_blocks(); ++q) acc = cadd(acc, *cl.map_shared_rank(s_part + lane, q));
+  }
+  cl.sync();
+  return acc;
+}
+
+// P2P over list 1: a cluster of H3_PSPLIT CTAs per chunk of <= 32 non-QBX targets,
+// source tiles dealt round-robin to the CTAs, fixed-order reduction over DSMEM.
+__global__ void __cluster_dims__(H3_PSPLIT, 1, 1) __launch_bounds__(NT)
+k_h3_eval_direct(qbxfmm_geometry g, HelmCoeffs hc, int nrhs, const double2* __restrict__ strengths,
+                 double2* __restrict__ pot, int32_t* err)
+{
+  __shared__ double s_y[3][NT], s_n[3][NT];
+  __shared__ double2 s_q[NT], s_d[NT];
+  __shared__ int s_pref[MAXB + 1], s_start[MAXB];
+  __shared__ double2 s_red[NW - 1][32];
+  __shared__ double2 s_part[32];
+  int chunk = blockIdx.x / H3_PSPLIT;
+  int part = blockIdx.x - chunk * H3_PSPLIT;
+  int r = blockIdx.y;
+  int itb = g.nonqbx_chunk_target_box[chunk];
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  bool active = lane < g.nonqbx_chunk_count[chunk];
+  int t = g.nonqbx_chunk_start[chunk] + lane;
+  double x[3] = {0, 0, 0};
+  if (active) load_point<3>(g.nonqbx_targets, g.nfiltered_targets, t, x);
+  const double2* st = strengths + (size_t)r * g.nsources;
+  const bool dip = hc.cd.x != 0.0 || hc.cd.y != 0.0;
+  double2 acc = c2(0.0);
+  int l0 = g.list1_starts[itb], l1 = g.list1_starts[itb + 1];
+  int tile = 0;
+  for (int gb = l0; gb < l1; gb += MAXB) {
+    int nb = min(MAXB, l1 - gb);
+    __syncthreads();
+    h3_list_prefix(g, g.list1_lists, gb, nb, s_pref, s_start, err);
+    __syncthreads();
+    int total = s_pref[nb];
+    for (int base = 0; base < total; base += NT, ++tile) {
+      if (tile % H3_PSPLIT != part) continue;
+      int v = base + threadIdx.x;
+      if (v < total) {
+        int s = h3_stream_source(v, nb, s_pref, s_start);
+        double y[3], nv[3] = {0, 0, 0};
+        load_point<3>(g.sources, g.nsources, s, y);
+        if (dip) load_point<3>(g.source_normals, g.nsources, s, nv);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          s_y[d][threadIdx.x] = y[d];
+          s_n[d][threadIdx.x] = nv[d];
+        }
+        double2 sv = st[s];
+        s_q[threadIdx.x] = cmul(hc.cq, sv);
+        s_d[threadIdx.x] = cmul(hc.cd, sv);
+      }
+      __syncthreads();
+      int jbeg = warp * 32, jend = min(jbeg + 32, total - base);
+      if (active) {
+        for (int j = jbeg; j < jend; ++j) {
+          double dx = x[0] - s_y[0][j], dy = x[1] - s_y[1][j], dz = x[2] - s_y[2][j];
+          double r2 = dx * dx + dy * dy + dz * dz;
+          if (r2 == 0.0) continue;
+          double rinv = rsqrt(r2);
+          double rr = r2 * rinv;
+          double sn, cs;
+          sincos(hc.k * rr, &sn, &cs);
+          double2 e = c2(cs * rinv, sn * rinv);   // e^{ikr} / r
+          acc = cfma(s_q[j], e, acc);
+          if (dip) {
+            // n . (x - y) e^{ikr} (1 - ikr) / r^3
+            double f = (s_n[0][j] * dx + s_n[1][j] * dy + s_n[2][j] * dz) * rinv * rinv;
+            double2 v = cmul(e, c2(f, -f * hc.k * rr));
+            acc = cfma(s_d[j], v, acc);
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  acc = h3_cluster_lane_sum(acc, s_red, s_part);
+  if (part == 0 && warp == 0 && active) {
+    double2* P = pot + (size_t)r * g.nfiltered_targets + t;
+    *P = cadd(*P, acc);
+  }
+}
+
+// Evaluate an expansion (order p, scale s) of box b at point x: multipole (singular
+// waves, coefficient * s^n) or local (regular waves, coefficient / s^n).
+QBX_D double2 h3_e2p(const double2* E, int p, bool local, double k, double s, const double* cb,
+                     const double* x, const double2* rec)
+{
+  double u[3] = {x[0] - cb[0], x[1] - cb[1], x[2] - cb[2]};
+  double2 w;
+  double rr;
+  double t = h3_dir(u, w, rr);
+  double2 rad[H3_LMAX + 2];
+  if (local) {
+    double jv[H3_LMAX + 2];
+    h3_sph_j(p, k * rr, jv);
+    double f = 1.0, si = 1.0 / s;
+    for (int n = 0; n <= p; ++n, f *= si) rad[n] = c2(jv[n] * f);
+  } else {
+    h3_sph_h(p, k * rr, rad);
+    double f = 1.0;
+    for (int n = 0; n <= p; ++n, f *= s) rad[n] = cscale(f, rad[n]);
+  }
+  double2 acc = c2(0.0);
+  double2 wm = c2(1.0);
+  for (int m = 0; m <= p; ++m) {
+    if (m > 0) wm = cmul(wm, w);
+    double pm1 = rec[idx3(m, m)].x, pm2 = 0.0;
+    for (int n = m; n <= p; ++n) {
+      double pn;
+      if (n == m) {
+        pn = pm1;
+      } else if (n == m + 1) {
+        pn = rec[idx3(n, m)].x * t * pm1;
+        pm2 = pm1;
+        pm1 = pn;
+      } else {
+        double2 ab = rec[idx3(n, m)];
+        pn = ab.x * (t * pm1 - ab.y * pm2);
+        pm2 = pm1;
+        pm1 = pn;
+      }
+      double2 y = cscale(pn, wm);
+      double2 v = cmul(E[hq(n, m)], y);
+      if (m > 0) v = cadd(v, cmul(E[hq(n, -m)], cconj(y)));
+      acc = cfma(rad[n], v, acc);
+    }
+  }
+  return acc;
+}
+
+// M2P over list 3: CTA per chunk of <= 32 non-QBX targets (lane = target), the warps
+// split the list-3 boxes and stage each multipole in their own shared slice.
+__global__ void __launch_bounds__(NT)
+k_h3_eval_multipoles(qbxfmm_geometry g, HelmCoeffs hc, int p, int nrhs,
+                     const double2* __restrict__ mpoles, double2* __restrict__ pot, int32_t* err)
+{
+  extern __shared__ double2 smem2[];
+  const int ncf = (p + 1) * (p + 1);
+  double2* rec = smem2;                                  // [(p+1)(p+2)/2]
+  int nrec = (p + 1) * (p + 2) / 2;
+  __shared__ double2 s_red[NW - 1][32];
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double2* M = smem2 + nrec + (size_t)warp * ncf;
+  h3_rec_table(p, rec, threadIdx.x, NT);
+  __syncthreads();
+  int chunk = blockIdx.x;
+  int r = blockIdx.y;
+  int itb = g.nonqbx_chunk_target_box[chunk];
+  int t = g.nonqbx_chunk_start[chunk] + lane;
+  bool active = lane < g.nonqbx_chunk_count[chunk];
+  double x[3] = {0, 0, 0};
+  if (active) load_point<3>(g.nonqbx_targets, g.nfiltered_targets, t, x);
+  double2 acc = c2(0.0);
+  for (int li = g.list3_starts[itb] + warp; li < g.list3_starts[itb + 1]; li += NW) {
+    int sb = g.list3_lists[li];
+    if ((unsigned)sb >= (unsigned)g.nboxes) {
+      report(err, QBX_DEVERR_BAD_BOX);
+      continue;
+    }
+    __syncwarp();
+    const double2* src = mpoles + ((size_t)sb * nrhs + r) * ncf;
+    for (int q = lane; q < ncf; q += 32) M[q] = src[q];
+    __syncwarp();
+    if (!active) continue;
+    double cs[3];
+    load_point<3>(g.box_centers, g.nboxes, sb, cs);
+    double s = h3_scale(hc.k, level_width(g, g.box_levels[sb]));
+    acc = cadd(acc, h3_e2p(M, p, false, hc.k, s, cs, x, rec));
+  }
+  __syncthreads();
+  if (warp > 0) s_red[warp - 1][lane] = acc;
+  __syncthreads();
+  if (warp == 0 && active) {
+    for (int w = 1; w < NW; ++w) acc = cadd(acc, s_red[w - 1][lane]);
+    double2* P = pot + (size_t)r * g.nfiltered_targets + t;
+    *P = cadd(*P, acc);
+  }
+}
+
+// L2P: one thread per non-QBX target, its own box's local expansion
+__global__ void __launch_bounds__(NT)
+k_h3_eval_locals(qbxfmm_geometry g, HelmCoeffs hc, int p, int nrhs,
+                 const double2* __restrict__ locals, double2* __restrict__ pot)
+{
+  extern __shared__ double2 smem2[];
+  double2* rec = smem2;
+  h3_rec_table(p, rec, threadIdx.x, NT);
+  __syncthreads();
+  int chunk = blockIdx.x;
+  int r = blockIdx.y;
+  int lane = threadIdx.x;
+  if (lane >= 32 || lane >= g.nonqbx_chunk_count[chunk]) return;
+  int itb = g.nonqbx_chunk_target_box[chunk];
+  int tb = g.target_boxes[itb];
+  int t = g.nonqbx_chunk_start[chunk] + lane;
+  double x[3], cb[3];
+  load_point<3>(g.nonqbx_targets, g.nfiltered_targets, t, x);
+  load_point<3>(g.box_centers, g.nboxes, tb, cb);
+  double s = h3_scale(hc.k, level_width(g, g.box_levels[tb]));
+  const int ncf = (p + 1) * (p + 1);
+  double2 v = h3_e2p(locals + ((size_t)tb * nrhs + r) * ncf, p, true, hc.k, s, cb, x, rec);
+  double2* P = pot + (size_t)r * g.nfiltered_targets + t;
+  *P = cadd(*P, v);
+}
+
+// }}}
+
+// {{{ QBX: P2QBXL, M2QBXL / L2QBXL, QBXL2P
+
+// P2QBXL over list 1: CTA per chunk of <= 32 centers of one target box (lane =
+// center, coefficients in registers); the list-1 sources stream through shared memory
+// in tiles of 128, each warp taking 32; per (center, source) pair the lane builds its
+// singular-wave table (order Q + 1) in its own column of a lane-minor shared array.
+template <int Q>
+__global__ void __launch_bounds__(NT)
+k_h3_p2qbxl(qbxfmm_geometry g, HelmCoeffs hc, int nrhs, const double2* __restrict__ strengths,
+            double2* __restrict__ qbx_exps, int32_t* err)
+{
+  constexpr int N = Q + 1;
+  constexpr int NE = (N + 1) * (N + 1);    // wave-table entries
+  constexpr int NC = (Q + 1) * (Q + 1);
+  extern __shared__ double2 smem2[];
+  double2* tabs = smem2;                          // [NW][NE][32]
+  __shared__ double2 rec[(N + 1) * (N + 2) / 2];
+  __shared__ Ladder s_lad[NC];
+  __shared__ double s_y[3][NT], s_n[3][NT];
+  __shared__ double2 s_q[NT], s_d[NT];
+  __shared__ int s_pref[MAXB + 1], s_start[MAXB];
+  h3_rec_table(N, rec, threadIdx.x, NT);
+  for (int ci = threadIdx.x; ci < NC; ci += NT) {
+    int n, m;
+    hq_decode(ci, n, m);
+    s_lad[ci] = h3_ladder(n, -m, hc.k);
+  }
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double2* T = tabs + (size_t)warp * NE * 32 + lane;
+  int chunk = blockIdx.x;
+  int r = blockIdx.y;
+  int itb = g.qbx_chunk_target_box[chunk];
+  bool has_center = lane < g.qbx_chunk_count[chunk];
+  int ctr = has_center ? g.centers_by_target_box[g.qbx_chunk_start[chunk] + lane] : 0;
+  if ((unsigned)ctr >= (unsigned)g.ncenters) {
+    report(err, QBX_DEVERR_BAD_CENTER);
+    has_center = false;
+    ctr = 0;
+  }
+  double cc[3];
+  load_point<3>(g.centers, g.ncenters, ctr, cc);
+  const double2* st = strengths + (size_t)r * g.nsources;
+  const bool dip = hc.cd.x != 0.0 || hc.cd.y != 0.0;
+  double2 acc[NC];
+#pragma unroll
+  for (int i = 0; i < NC; ++i) acc[i] = c2(0.0);
+  int l0 = g.list1_starts[itb], l1 = g.list1_starts[itb + 1];
+  for (int gb = l0; gb < l1; gb += MAXB) {
+    int nb = min(MAXB, l1 - gb);
+    __syncthreads();
+    h3_list_prefix(g, g.list1_lists, gb, nb, s_pref, s_start, err);
+    __syncthreads();
+    int total = s_pref[nb];
+    for (int base = 0; base < total; base += NT) {
+      int v = base + threadIdx.x;
+      if (v < total) {
+        int s = h3_stream_source(v, nb, s_pref, s_start);
+        double y[3], nv[3] = {0, 0, 0};
+        load_point<3>(g.sources, g.nsources, s, y);
+        if (dip) load_point<3>(g.source_normals, g.nsources, s, nv);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          s_y[d][threadIdx.x] = y[d];
+          s_n[d][threadIdx.x] = nv[d];
+        }
+        double2 sv = st[s];
+        s_q[threadIdx.x] = cmul(hc.cq, sv);
+        s_d[threadIdx.x] = cmul(hc.cd, sv);
+      }
+      __syncthreads();
+      int jbeg = warp * 32, jend = min(jbeg + 32, total - base);
+      if (has_center) {
+        for (int j = jbeg; j < jend; ++j) {
+          double u[3] = {s_y[0][j] - cc[0], s_y[1][j] - cc[1], s_y[2][j] - cc[2]};
+          double2 w;
+          double rr;
+          double t = h3_dir(u, w, rr);
+          if (rr == 0.0) continue;
+          double2 rad[N + 1];
+          h3_sph_h(N, hc.k * rr, rad);
+#pragma unroll
+          for (int m = 0; m <= N; ++m) h3_wave_column(m, N, t, w, rec, rad, T, 32);
+          double2 q = s_q[j];
+#pragma unroll
+          for (int n = 0; n <= Q; ++n)
+#pragma unroll
+            for (int m = -n; m <= n; ++m) acc[hq(n, m)] = cfma(q, T[hq(n, -m) * 32], acc[hq(n, m)]);
+          if (dip) {
+            double2 np = c2(0.5 * s_n[0][j], -0.5 * s_n[1][j]);
+            double2 nm = c2(0.5 * s_n[0][j], 0.5 * s_n[1][j]);
+            double nz = s_n[2][j];
+            double2 d = s_d[j];
+#pragma unroll
+            for (int ci = 0; ci < NC; ++ci) {
+              const Ladder& L = s_lad[ci];
+              double2 vz = caxpy(L.w[0], T[L.o[0] * 32], cscale(L.w[1], T[L.o[1] * 32]));
+              double2 vp = caxpy(L.w[2], T[L.o[2] * 32], cscale(L.w[3], T[L.o[3] * 32]));
+              double2 vm = caxpy(L.w[4], T[L.o[4] * 32], cscale(L.w[5], T[L.o[5] * 32]));
+              double2 vv = cfma(np, vp, cfma(nm, vm, cscale(nz, vz)));
+              acc[ci] = cfma(d, vv, acc[ci]);
+            }
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  // reduce the warps' partial sums through the (now free) table space
+  __syncthreads();
+  double2* red = tabs;   // [NW-1][32][NC]
+  if (warp > 0) {
+#pragma unroll
+    for (int i = 0; i < NC; ++i) red[((warp - 1) * 32 + lane) * NC + i] = acc[i];
+  }
+  __syncthreads();
+  if (warp == 0 && has_center) {
+    double s = h3_scale(hc.k, g.expansion_radii[ctr]);
+    double2* out = qbx_exps + ((size_t)ctr * nrhs + r) * NC;
+    double fs = FOUR_PI * hc.k;
+#pragma unroll
+    for (int i = 0; i < NC; ++i) {
+      double2 a = acc[i];
+      for (int w = 1; w < NW; ++w) a = cadd(a, red[((w - 1) * 32 + lane) * NC + i]);
+      int n, m;
+      hq_decode(i, n, m);
+      double f = fs * pow(s, (double)n);
+      out[i] = cadd(out[i], c2(-f * a.y, f * a.x));
+    }
+  }
+}
+
+// Box expansion (order pf) -> QBX local (order Q) at a center, by the addition theorem
+// with the Gaunt table (layout [(nu,mu) out][(n,m) in][j], l = |n - nu| + 2 j).
+// CTA per chunk of <= 32 centers of one target box.  M2QBXL (FROM_LOCAL = false):
+// the warps take the target box's list-3 boxes in turn, stage each multipole
+// (times s_s^n i^-n) and run over the chunk's centers, accumulating into per-center
+// shared sums.  L2QBXL (FROM_LOCAL = true): the warps take the centers in turn,
+// each translating the target box's local (times s_b^-n i^-n).  Per (center, box):
+// the warp builds w_l^lam = 4 pi i^l f_l(k|b|) Y_l^lam(b) (f = h or j) in shared
+// memory; lane o owns outputs o and o + 32.
+template <bool FROM_LOCAL>
+__global__ void __launch_bounds__(NT)
+k_h3_e2qbxl(qbxfmm_geometry g, HelmCoeffs hc, int pf, int q, int nrhs,
+            const double2* __restrict__ exps, const double* __restrict__ gaunt,
+            double2* __restrict__ qbx_exps, int32_t* err)
+{
+  extern __shared__ double2 smem2[];
+  const int ncf = (pf + 1) * (pf + 1), ncq = (q + 1) * (q + 1);
+  const int L = pf + q;
+  const int nw = (L + 1) * (L + 1);
+  const int nrec = (L + 1) * (L + 2) / 2;
+  const int Cp = ncf, nl = pf + 1;
+  double2* rec = smem2;                                          // [nrec]
+  double2* Ew = rec + nrec + (size_t)(threadIdx.x >> 5) * (ncf + nw + 2 * (L + 2));
+  double2* Wt = Ew + ncf;                                        // [nw]
+  double2* rad = Wt + nw;                                        // [L + 2]
+  double2* sums = rec + nrec + (size_t)NW * (ncf + nw + 2 * (L + 2));   // [NW][32][ncq]
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  h3_rec_table(L, rec, threadIdx.x, NT);
+  int chunk = blockIdx.x;
+  int r = blockIdx.y;
+  int itb = g.qbx_chunk_target_box[chunk];
+  int nctr = g.qbx_chunk_count[chunk];
+  for (int e = threadIdx.x; e < NW * 32 * ncq; e += NT) sums[e] = c2(0.0);
+  __syncthreads();
+
+  // one (center, box) translation by this warp into sums[warp][ci][*]
+  auto translate = [&](int ci, const double* cb, bool singular) {
+    int ctr = g.centers_by_target_box[g.qbx_chunk_start[chunk] + ci];
+    double cc[3];
+    load_point<3>(g.centers, g.ncenters, ctr, cc);
+    double bv[3] = {cc[0] - cb[0], cc[1] - cb[1], cc[2] - cb[2]};
+    double2 w;
+    double rr;
+    double t = h3_dir(bv, w, rr);
+    if (lane == 0) {
+      if (singular) {
+        h3_sph_h(L, hc.k * rr, rad);
+      } else {
+        double jv[H3_LMAX + 2];
+        h3_sph_j(L, hc.k * rr, jv);
+        for (int l = 0; l <= L; ++l) rad[l] = c2(jv[l]);
+      }
+      for (int l = 0; l <= L; ++l) rad[l] = cmul(cscale(FOUR_PI, ipow(l)), rad[l]);
+    }
+    __syncwarp();
+    for (int m = lane; m <= L; m += 32) h3_wave_column(m, L, t, w, rec, rad, Wt, 1);
+    __syncwarp();
+    double st = h3_scale(hc.k, g.expansion_radii[ctr]);
+    for (int o = lane; o < ncq; o += 32) {
+      int nu, mu;
+      hq_decode(o, nu, mu);
+      double2 a = c2(0.0);
+      const double* G = gaunt + (size_t)o * Cp * nl;
+      for (int n = 0; n <= pf; ++n) {
+        int jmax = min(n, nu);
+        int lbase = abs(n - nu);
+        for (int m = -n; m <= n; ++m) {
+          int lam = m - mu;
+          const double* Gc = G + (size_t)hq(n, m) * nl;
+          double2 tt = c2(0.0);
+          for (int j = 0; j <= jmax; ++j) {
+            int l = lbase + 2 * j;
+            if (abs(lam) > l) continue;
+            tt = caxpy(Gc[j], Wt[hq(l, lam)], tt);
+          }
+          a = cfma(Ew[hq(n, m)], tt, a);
+        }
+      }
+      // times i^nu s_t^nu
+      a = cscale(pow(st, (double)nu), cmul(ipow(nu), a));
+      double2* S = sums + ((size_t)warp * 32 + ci) * ncq + o;
+      *S = cadd(*S, a);
+    }
+    __syncwarp();
+  };
+
+  if (FROM_LOCAL) {
+    int tb = g.target_boxes[itb];
+    double cb[3];
+    load_point<3>(g.box_centers, g.nboxes, tb, cb);
+    double sb = h3_scale(hc.k, level_width(g, g.box_levels[tb]));
+    const double2* src = exps + ((size_t)tb * nrhs + r) * ncf;
+    for (int e = lane; e < ncf; e += 32) {
+      int n, m;
+      hq_decode(e, n, m);
+      Ew[e] = cscale(pow(sb, -(double)n), cmul(ipow(-n), src[e]));
+    }
+    __syncwarp();
+    for (int ci = warp; ci < nctr; ci += NW) translate(ci, cb, false);
+  } else {
+    for (int li = g.list3_starts[itb] + warp; li < g.list3_starts[itb + 1]; li += NW) {
+      int sbx = g.list3_lists[li];
+      if ((unsigned)sbx >= (unsigned)g.nboxes) {
+        report(err, QBX_DEVERR_BAD_BOX);
+        continue;
+      }
+      double cb[3];
+      load_point<3>(g.box_centers, g.nboxes, sbx, cb);
+      double ss = h3_scale(hc.k, level_width(g, g.box_levels[sbx]));
+      const double2* src = exps + ((size_t)sbx * nrhs + r) * ncf;
+      __syncwarp();
+      for (int e = lane; e < ncf; e += 32) {
+        int n, m;
+        hq_decode(e, n, m);
+        Ew[e] = cscale(pow(ss, (double)n), cmul(ipow(-n), src[e]));
+      }
+      __syncwarp();
+      for (int ci = 0; ci < nctr; ++ci) translate(ci, cb, true);
+    }
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < nctr * ncq; e += NT) {
+    int ci = e / ncq, o = e - ci * ncq;
+    int ctr = g.centers_by_target_box[g.qbx_chunk_start[chunk] + ci];
+    if ((unsigned)ctr >= (unsigned)g.ncenters) {
+      report(err, QBX_DEVERR_BAD_CENTER);
+      continue;
+    }
+    double2 a = c2(0.0);
+    for (int w = 0; w < NW; ++w) a = cadd(a, sums[((size_t)w * 32 + ci) * ncq + o]);
+    double2* out = qbx_exps + ((size_t)ctr * nrhs + r) * ncq + o;
+    *out = cadd(*out, a);
+  }
+}
+
+// QBXL2P: one thread per used center, over its targets
+__global__ void __launch_bounds__(NT)
+k_h3_qbxl2p(qbxfmm_geometry g, HelmCoeffs hc, int q, int nrhs, const double2* __restrict__ qbx_exps,
+            double2* __restrict__ pot_tree)
+{
+  extern __shared__ double2 smem2[];
+  double2* rec = smem2;
+  h3_rec_table(q, rec, threadIdx.x, NT);
+  __syncthreads();
+  int ig = blockIdx.x * blockDim.x + threadIdx.x;
+  int r = blockIdx.y;
+  if (ig >= g.nglobal_qbx_centers) return;
+  int ctr = g.global_qbx_centers[ig];
+  double cc[3];
+  load_point<3>(g.centers, g.ncenters, ctr, cc);
+  double s = h3_scale(hc.k, g.expansion_radii[ctr]);
+  int ncq = (q + 1) * (q + 1);
+  const double2* Lc = qbx_exps + ((size_t)ctr * nrhs + r) * ncq;
+  for (int it = g.center_to_targets_starts[ctr]; it < g.center_to_targets_starts[ctr + 1]; ++it) {
+    int t = g.center_to_targets_lists[it];
+    double x[3];
+    load_point<3>(g.targets, g.ntargets, t, x);
+    pot_tree[(size_t)r * g.ntargets + t] = h3_e2p(Lc, q, true, hc.k, s, cc, x, rec);
+  }
+}
+
+// }}}
+
+// {{{ translation matrices
+
+// One CTA per matrix.  kind 0: M2L class (level and integer offset; b = offset * width),
+// kind 1: M2M (parent level lev, child position ci; b = c_parent - c_child),
+// kind 2: L2L (child level lev, child position ci; b = c_child - c_parent).
+// T is the real (rp x kp) form of the complex (ncf x ncf) matrix acting on
+// interleaved (re, im) coefficient vectors; entries outside 2 ncf are zero.
+__global__ void __launch_bounds__(NT)
+k_h3_trans_build(int kind, int p, int rp, int kp, double k, double root_extent, int nclasses,
+                 const int32_t* __restrict__ offs, const int32_t* __restrict__ cls_levels,
+                 int lev0, const double* __restrict__ gaunt, double* __restrict__ T)
+{
+  extern __shared__ double2 smem2[];
+  const int L = 2 * p;
+  const int ncf = (p + 1) * (p + 1);
+  const int nl = p + 1;
+  double2* rec = smem2;                                  // [(L+1)(L+2)/2]
+  double2* Wt = rec + (L + 1) * (L + 2) / 2;              // [(L+1)^2]
+  double2* rad = Wt + (L + 1) * (L + 1);                 // [L+2]
+  double* pw = reinterpret_cast<double*>(rad + L + 2);   // [2][p+1]: s_in^{e n}, s_out^{e nu}
+  int mi = blockIdx.x;
+  double b[3];
+  double s_in, s_out;
+  int e_in, e_out;
+  bool singular;
+  if (kind == 0) {
+    int lev = cls_levels[mi];
+    double wdt = ldexp(root_extent, -lev);
+    for (int d = 0; d < 3; ++d) b[d] = offs[d * nclasses + mi] * wdt;
+    s_in = s_out = fmin(1.0, k * wdt);
+    e_in = e_out = 1;
+    singular = true;
+  } else {
+    int lev = lev0 + mi / 8, ci = mi % 8;
+    int plev = (kind == 1) ? lev : lev - 1;        // parent level
+    double wp = ldexp(root_extent, -plev);
+    double sgn = (kind == 1) ? -1.0 : 1.0;         // M2M: c_p - c_c; L2L: c_c - c_p
+    for (int d = 0; d < 3; ++d) b[d] = sgn * (((ci >> d) & 1) ? 0.25 : -0.25) * wp;
+    double sp = fmin(1.0, k * wp), sc = fmin(1.0, k * 0.5 * wp);
+    if (kind == 1) {
+      s_in = sc; e_in = 1; s_out = sp; e_out = -1;
+    } else {
+      s_in = sp; e_in = -1; s_out = sc; e_out = 1;
+    }
+    singular = false;
+  }
+  h3_rec_table(L, rec, threadIdx.x, NT);
+  double2 w;
+  double rr;
+  double t = h3_dir(b, w, rr);
+  if (threadIdx.x == 0) {
+    if (singular) {
+      h3_sph_h(L, k * rr, rad);
+    } else {
+      double jv[H3_LMAX + 2];
+      h3_sph_j(L, k * rr, jv);
+      for (int l = 0; l <= L; ++l) rad[l] = c2(jv[l]);
+    }
+    for (int l = 0; l <= L; ++l) rad[l] = cmul(cscale(FOUR_PI, ipow(l)), rad[l]);
+  }
+  for (int n = threadIdx.x; n <= p; n += NT) {
+    pw[n] = pow(s_in, (double)(e_in * n));
+    pw[p + 1 + n] = pow(s_out, (double)(e_out * n));
+  }
+  __syncthreads();
+  for (int m = threadIdx.x; m <= L; m += NT) h3_wave_column(m, L, t, w, rec, rad, Wt, 1);
+  __syncthreads();
+  double* Tm = T + (size_t)mi * rp * kp;
+  for (int e = threadIdx.x; e < ncf * ncf; e += NT) {
+    int o = e / ncf, i = e - o * ncf;      // row (nu, mu), column (n, m)
+    int nu, mu, n, m;
+    hq_decode(o, nu, mu);
+    hq_decode(i, n, m);
+    const double* Gc = gaunt + ((size_t)o * ncf + i) * nl;
+    int lam = m - mu, lbase = abs(n - nu), jmax = min(n, nu);
+    double2 tt = c2(0.0);
+    for (int j = 0; j <= jmax; ++j) {
+      int l = lbase + 2 * j;
+      if (abs(lam) > l) continue;
+      tt = caxpy(Gc[j], Wt[hq(l, lam)], tt);
+    }
+    // c = i^{nu - n} tt, scaled
+    double2 v = cscale(pw[n] * pw[p + 1 + nu], cmul(ipow(nu - n + 4 * p), tt));
+    size_t r0 = (size_t)(2 * o) * kp + 2 * i;
+    Tm[r0] = v.x;
+    Tm[r0 + 1] = -v.y;
+    Tm[r0 + kp] = v.y;
+    Tm[r0 + kp + 1] = v.x;
+  }
+  // zero padding
+  for (size_t e = threadIdx.x; e < (size_t)rp * kp; e += NT) {
+    int row = (int)(e / kp), col = (int)(e % kp);
+    if (row >= 2 * ncf || col >= 2 * ncf) Tm[e] = 0.0;
+  }
+}
+
+// }}}
+
+// {{{ assembly
+
+__global__ void k_h3_assemble_tree(qbxfmm_geometry g, int nrhs, const double2* __restrict__ pot_tree,
+                                   double2* __restrict__ out)
+{
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  int r = blockIdx.y;
+  if (t >= g.ntargets) return;
+  int u = g.sorted_target_ids[t] - g.ncenters;
+  if (u >= 0) out[(size_t)r * g.nuser_targets + u] = cscale(1.0 / FOUR_PI, pot_tree[(size_t)r * g.ntargets + t]);
+}
+
+__global__ void k_h3_assemble_nonqbx(qbxfmm_geometry g, int nrhs,
+                                     const double2* __restrict__ pot_nonqbx, double2* __restrict__ out)
+{
+  int f = blockIdx.x * blockDim.x + threadIdx.x;
+  int r = blockIdx.y;
+  if (f >= g.nfiltered_targets) return;
+  int t = g.unfiltered_from_filtered_target_indices[f];
+  int u = g.sorted_target_ids[t] - g.ncenters;
+  if (u >= 0) {
+    double2* o = out + (size_t)r * g.nuser_targets + u;
+    *o = caxpy(1.0 / FOUR_PI, pot_nonqbx[(size_t)r * g.nfiltered_targets + f], *o);
+  }
+}
+
+// }}}
+
+// {{{ launchers
+
+static int gridy(int nrhs) { return nrhs; }
+
+cudaError_t h3_launch_p2m(const qbxfmm_geometry& g, HelmCoeffs hc, int p, int nrhs,
+                          const double2* s, double2* mp, cudaStream_t st)
+{
+  if (g.nsource_boxes == 0) return cudaSuccess;
+  int N = p + 1;
+  size_t sh = ((size_t)(N + 1) * (N + 1) * H3_TS + (size_t)(N + 1) * (N + 2) / 2) * sizeof(double2);
+  cudaFuncSetAttribute(k_h3_p2e<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+  k_h3_p2e<false><<<dim3(g.nsource_boxes, gridy(nrhs)), NT, sh, st>>>(g, hc, p, nrhs, s, mp, nullptr);
+  return cudaGetLastError();
+}
+
+cudaError_t h3_launch_p2l(const qbxfmm_geometry& g, HelmCoeffs hc, int p, int nrhs,
+                          const double2* s, double2* lo, int32_t* err, cudaStream_t st)
+{
+  if (g.nttp_boxes == 0) return cudaSuccess;
+  int N = p + 1;
+  size_t sh = ((size_t)(N + 1) * (N + 1) * H3_TS + (size_t)(N + 1) * (N + 2) / 2) * sizeof(double2);
+  cudaFuncSetAttribute(k_h3_p2e<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+  k_h3_p2e<true><<<dim3(g.nttp_boxes, gridy(nrhs)), NT, sh, st>>>(g, hc, p, nrhs, s, lo, err);
+  return cudaGetLastError();
+}
+
+cudaError_t h3_launch_eval_direct(const qbxfmm_geometry& g, HelmCoeffs hc, int nrhs,
+                                  const double2* s, double2* pot, int32_t* err, cudaStream_t st)
+{
+  if (g.nnonqbx_chunks == 0) return cudaSuccess;
+  k_h3_eval_direct<<<dim3(g.nnonqbx_chunks * H3_PSPLIT, gridy(nrhs)), NT, 0, st>>>(g, hc, nrhs, s,
+                                                                                  pot, err);
+  return cudaGetLastError();
+}
+
+cudaError_t h3_launch_eval_multipoles(const qbxfmm_geometry& g, HelmCoeffs hc, int p, int nrhs,
+                                      const double2* mp, double2* pot, int32_t* err, cudaStream_t st)
+{
+  if (g.nnonqbx_chunks == 0) return cudaSuccess;
+  size_t sh = ((size_t)(p + 1) * (p + 2) / 2 + (size_t)NW * (p + 1) * (p + 1)) * sizeof(double2);
+  cudaFuncSetAttribute(k_h3_eval_multipoles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+  k_h3_eval_multipoles<<<dim3(g.nnonqbx_chunks, gridy(nrhs)), NT, sh, st>>>(g, hc, p, nrhs, mp, pot,
+                                                                            err);
+  return cudaGetLastError();
+}
+
+cudaError_t h3_launch_eval_locals(const qbxfmm_geometry& g, HelmCoeffs hc, int p, int nrhs,
+                                  const double2* lo, double2* pot, cudaStream_t st)
+{
+  if (g.nnonqbx_chunks == 0) return cudaSuccess;
+  size_t sh = (size_t)(p + 1) * (p + 2) / 2 * sizeof(double2);
+  k_h3_eval_locals<<<dim3(g.nnonqbx_chunks, gridy(nrhs)), NT, sh, st>>>(g, hc, p, nrhs, lo, pot);
+  return cudaGetLastError();
+}
+
+template <int Q>
+static cudaError_t h3_p2qbxl_q(const qbxfmm_geometry& g, HelmCoeffs hc, int nrhs, const double2* s,
+                               double2* qe, int32_t* err, cudaStream_t st)
+{
+  constexpr int N = Q + 1;
+  size_t sh = (size_t)NW * (N + 1) * (N + 1) * 32 * sizeof(double2);
+  size_t red = (size_t)(NW - 1) * 32 * (Q + 1) * (Q + 1) * sizeof(double2);
+  sh = std::max(sh, red);
+  cudaFuncSetAttribute(k_h3_p2qbxl<Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+  k_h3_p2qbxl<Q><<<dim3(g.nqbx_chunks, gridy(nrhs)), NT, sh, st>>>(g, hc, nrhs, s, qe, err);
+  return cudaGetLastError();
+}
+
+cudaError_t h3_launch_p2qbxl(const qbxfmm_geometry& g, HelmCoeffs hc, int q, int nrhs,
+                             const double2* s, double2* qe, int32_t* err, cudaStream_t st)
+{
+  if (g.nqbx_chunks == 0) return cudaSuccess;
+  switch (q) {
+    case 0: return h3_p2qbxl_q<0>(g, hc, nrhs, s, qe, err, st);
+    case 1: return h3_p2qbxl_q<1>(g, hc, nrhs, s, qe, err, st);
+    case 2: return h3_p2qbxl_q<2>(g, hc, nrhs, s, qe, err, st);
+    case 3: return h3_p2qbxl_q<3>(g, hc, nrhs, s, qe, err, st);
+    case 4: return h3_p2qbxl_q<4>(g, hc, nrhs, s, qe, err, st);
+    case 5: return h3_p2qbxl_q<5>(g, hc, nrhs, s, qe, err, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+static size_t e2qbxl_smem(int pf, int q)
+{
+  int ncf = (pf + 1) * (pf + 1), ncq = (q + 1) * (q + 1), L = pf + q;
+  size_t nrec = (size_t)(L + 1) * (L + 2) / 2;
+  size_t per = (size_t)ncf + (size_t)(L + 1) * (L + 1) + 2 * (L + 2);
+  return (nrec + NW * per + (size_t)NW * 32 * ncq) * sizeof(double2);
+}
+
+cudaError_t h3_launch_m2qbxl(const qbxfmm_geometry& g, HelmCoeffs hc, int pf, int q, int nrhs,
+                             const double2* mp, const double* gaunt, double2* qe, int32_t* err,
+                             cudaStream_t st)
+{
+  if (g.nqbx_chunks == 0) return cudaSuccess;
+  size_t sh = e2qbxl_smem(pf, q);
+  cudaFuncSetAttribute(k_h3_e2qbxl<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+  k_h3_e2qbxl<false><<<dim3(g.nqbx_chunks, gridy(nrhs)), NT, sh, st>>>(g, hc, pf, q, nrhs, mp, gaunt,
+                                                                       qe, err);
+  return cudaGetLastError();
+}
+
+cudaError_t h3_launch_l2qbxl(const qbxfmm_geometry& g, HelmCoeffs hc, int pf, int q, int nrhs,
+                             const double2* lo, const double* gaunt, double2* qe, int32_t* err,
+                             cudaStream_t st)
+{
+  if (g.nqbx_chunks == 0) return cudaSuccess;
+  size_t sh = e2qbxl_smem(pf, q);
+  cudaFuncSetAttribute(k_h3_e2qbxl<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+  k_h3_e2qbxl<true><<<dim3(g.nqbx_chunks, gridy(nrhs)), NT, sh, st>>>(g, hc, pf, q, nrhs, lo, gaunt,
+                                                                      qe, err);
+  return cudaGetLastError();
+}
+
+cudaError_t h3_launch_qbxl2p(const qbxfmm_geometry& g, HelmCoeffs hc, int q, int nrhs,
+                             const double2* qe, double2* pt, cudaStream_t st)
+{
+  if (g.nglobal_qbx_centers == 0) return cudaSuccess;
+  size_t sh = (size_t)(q + 1) * (q + 2) / 2 * sizeof(double2);
+  k_h3_qbxl2p<<<dim3((g.nglobal_qbx_centers + NT - 1) / NT, gridy(nrhs)), NT, sh, st>>>(g, hc, q, nrhs,
+                                                                                       qe, pt);
+  return cudaGetLastError();
+}
+
+cudaError_t h3_launch_assemble(const qbxfmm_geometry& g, int nrhs, const double2* pot_nonqbx,
+                               const double2* pot_tree, double2* out, cudaStream_t st)
+{
+  if (g.ntargets > 0) {
+    k_h3_assemble_tree<<<dim3((g.ntargets + 255) / 256, nrhs), 256, 0, st>>>(g, nrhs, pot_tree, out);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  if (g.nfiltered_targets > 0)
+    k_h3_assemble_nonqbx<<<dim3((g.nfiltered_targets + 255) / 256, nrhs), 256, 0, st>>>(
+        g, nrhs, pot_nonqbx, out);
+  return cudaGetLastError();
+}
+
+cudaError_t h3_launch_trans_build(const qbxfmm_geometry& g, const TransCfg& tc, double k,
+                                  const double* gaunt, double* T, cudaStream_t st)
+{
+  int p = tc.p, L = 2 * p;
+  size_t sh = ((size_t)(L + 1) * (L + 2) / 2 + (size_t)(L + 1) * (L + 1) + (L + 2)) * sizeof(double2) +
+              2 * (size_t)(p + 1) * sizeof(double);
+  cudaFuncSetAttribute(k_h3_trans_build, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+  size_t stride = (size_t)tc.rp * tc.kp;
+  if (g.m2l_nclasses > 0)
+    k_h3_trans_build<<<g.m2l_nclasses, NT, sh, st>>>(0, p, tc.rp, tc.kp, k, g.root_extent,
+                                                      g.m2l_nclasses, g.m2l_class_offsets,
+                                                      g.m2l_class_levels, 0, gaunt, T);
+  // M2M: parent levels 0 .. nlevels-2; L2L: child levels 1 .. nlevels-1 (8 per level)
+  if (g.nlevels > 1) {
+    k_h3_trans_build<<<8 * (g.nlevels - 1), NT, sh, st>>>(
+        1, p, tc.rp, tc.kp, k, g.root_extent, 0, nullptr, nullptr, 0, gaunt,
+        T + tc.m2m_base * stride);
+    k_h3_trans_build<<<8 * (g.nlevels - 1), NT, sh, st>>>(
+        2, p, tc.rp, tc.kp, k, g.root_extent, 0, nullptr, nullptr, 1, gaunt,
+        T + (tc.l2l_base + 8) * stride);
+  }
+  return cudaGetLastError();
+}
+
+// }}}
+
+}  // namespace qbx

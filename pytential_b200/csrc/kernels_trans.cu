@@ -236,25 +236,45 @@ k_trans_reduce(int ncf, int rp, int nrhs, const int32_t* __restrict__ boxes, int
 
 // {{{ launchers
 
-void trans_dims(int p, int& ncf, int& rp, int& kp)
+static void dims_from_ncf(int ncf, int& rp, int& kp)
 {
-  ncf = (p + 1) * (p + 2) / 2;
   rp = (2 * ncf + 7) / 8 * 8;
   kp = (2 * ncf + 3) / 4 * 4;
 }
 
-size_t trans_matrix_bytes(int p, int nclasses)
+TransCfg trans_cfg_laplace3(int p, int nclasses)
 {
-  int ncf, rp, kp;
-  trans_dims(p, ncf, rp, kp);
-  return (size_t)(nclasses + 16) * rp * kp * sizeof(double);
+  TransCfg c;
+  c.p = p;
+  c.ncf = (p + 1) * (p + 2) / 2;
+  dims_from_ncf(c.ncf, c.rp, c.kp);
+  c.m2m_mat_mod = 8;
+  c.m2m_base = nclasses;
+  c.l2l_base = nclasses + 8;
+  c.m2l_div_by_width = 1;
+  c.nmatrices = nclasses + 16;
+  return c;
 }
 
-size_t trans_scratch_bytes(int p, int npairs, int nrhs)
+TransCfg trans_cfg_helm3(int p, int nclasses, int nlevels)
 {
-  int ncf, rp, kp;
-  trans_dims(p, ncf, rp, kp);
-  return (size_t)(npairs > 0 ? npairs : 1) * nrhs * rp * sizeof(double);
+  TransCfg c;
+  c.p = p;
+  c.ncf = (p + 1) * (p + 1);
+  dims_from_ncf(c.ncf, c.rp, c.kp);
+  c.m2m_mat_mod = 0;
+  c.m2m_base = nclasses;
+  c.l2l_base = nclasses + 8 * (size_t)nlevels;
+  c.m2l_div_by_width = 0;
+  c.nmatrices = nclasses + 16 * (size_t)nlevels;
+  return c;
+}
+
+size_t trans_matrix_bytes(const TransCfg& c) { return c.nmatrices * c.rp * c.kp * sizeof(double); }
+
+size_t trans_scratch_bytes(const TransCfg& c, int npairs, int nrhs)
+{
+  return (size_t)(npairs > 0 ? npairs : 1) * nrhs * c.rp * sizeof(double);
 }
 
 static size_t gemm_smem(int rp) { return ((size_t)rp * TSTR + (size_t)KC * XS) * sizeof(double); }
@@ -266,46 +286,40 @@ static int gemm_nwm(int rp)
   return mt <= 24 ? 1 : (mt <= 48 ? 2 : 4);
 }
 
-bool trans_supported(int p)
-{
-  int ncf, rp, kp;
-  trans_dims(p, ncf, rp, kp);
-  return rp / 8 <= 96 && gemm_smem(rp) <= 200 * 1024;
-}
+bool trans_supported(const TransCfg& c) { return c.rp / 8 <= 96 && gemm_smem(c.rp) <= 200 * 1024; }
 
-// T layout: [0, nclasses) M2L classes, [nclasses, +8) M2M, [nclasses+8, +8) L2L
-cudaError_t launch_trans_build(const qbxfmm_geometry& g, int p, double* T, cudaStream_t st)
+// T layout: [0, nclasses) M2L classes, then M2M and L2L matrices (TransCfg bases)
+cudaError_t launch_trans_build(const qbxfmm_geometry& g, const TransCfg& c, double* T, cudaStream_t st)
 {
-  int ncf, rp, kp;
-  trans_dims(p, ncf, rp, kp);
+  int p = c.p;
   size_t sh = (size_t)(2 * p + 1) * (2 * p + 2) / 2 * sizeof(double2);
-  size_t stride = (size_t)rp * kp;
+  size_t stride = (size_t)c.rp * c.kp;
   if (g.m2l_nclasses > 0)
-    k_trans_build<<<g.m2l_nclasses, NT, sh, st>>>(0, p, ncf, rp, kp, g.m2l_nclasses,
+    k_trans_build<<<g.m2l_nclasses, NT, sh, st>>>(0, p, c.ncf, c.rp, c.kp, g.m2l_nclasses,
                                                    g.m2l_class_offsets, T);
-  k_trans_build<<<8, NT, sh, st>>>(1, p, ncf, rp, kp, 8, nullptr, T + g.m2l_nclasses * stride);
-  k_trans_build<<<8, NT, sh, st>>>(2, p, ncf, rp, kp, 8, nullptr, T + (g.m2l_nclasses + 8) * stride);
+  k_trans_build<<<8, NT, sh, st>>>(1, p, c.ncf, c.rp, c.kp, 8, nullptr, T + c.m2m_base * stride);
+  k_trans_build<<<8, NT, sh, st>>>(2, p, c.ncf, c.rp, c.kp, 8, nullptr, T + c.l2l_base * stride);
   return cudaGetLastError();
 }
 
-static cudaError_t gemm_launch(const qbxfmm_geometry& g, int p, int nrhs, const double* T,
-                               int mat_base, int mat_mod, const int32_t* group_starts_dev,
+static cudaError_t gemm_launch(const qbxfmm_geometry& g, const TransCfg& c, int nrhs, const double* T,
+                               size_t mat_base, int mat_mod, const int32_t* group_starts_dev,
                                int g0, int ngroups, int maxcols, const int32_t* pair_src,
                                const int32_t* pair_dst, const double2* ein, double2* eout,
                                double scale, double* cpair, int32_t* err, cudaStream_t st)
 {
   if (ngroups <= 0 || maxcols <= 0) return cudaSuccess;
-  int ncf, rp, kp;
-  trans_dims(p, ncf, rp, kp);
+  int ncf = c.ncf, rp = c.rp, kp = c.kp;
   size_t sh = gemm_smem(rp);
   int nwm = gemm_nwm(rp);
   int ntile = 8 * (4 / nwm);
   int mtw = (rp / 8 + nwm - 1) / nwm;
   dim3 grid((maxcols + ntile - 1) / ntile, ngroups);
+  const double* Tb = T + mat_base * (size_t)rp * kp;
 #define QBX_GEMM_CASE(W)                                                                        \
   if (mtw <= W) {                                                                               \
     cudaFuncSetAttribute(k_trans_gemm<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh); \
-    k_trans_gemm<W><<<grid, NT, sh, st>>>(ncf, rp, kp, nrhs, nwm, T, mat_base, mat_mod,         \
+    k_trans_gemm<W><<<grid, NT, sh, st>>>(ncf, rp, kp, nrhs, nwm, Tb, 0, mat_mod,               \
                                           group_starts_dev, g0, pair_src, pair_dst, ein, eout,  \
                                           scale, cpair, err, g.nboxes);                         \
     return cudaGetLastError();                                                                  \
@@ -319,42 +333,38 @@ static cudaError_t gemm_launch(const qbxfmm_geometry& g, int p, int nrhs, const 
   return cudaErrorInvalidValue;
 }
 
-cudaError_t launch_m2l_gemm(const qbxfmm_geometry& g, const TransHost& th, int p, int nrhs,
-                            const double* T, const double2* mp, double2* lo, double* cpair,
-                            int32_t* err, cudaStream_t st)
+cudaError_t launch_m2l_gemm(const qbxfmm_geometry& g, const TransHost& th, const TransCfg& c,
+                            int nrhs, const double* T, const double2* mp, double2* lo,
+                            double* cpair, int32_t* err, cudaStream_t st)
 {
   if (g.m2l_nclasses == 0) return cudaSuccess;
-  int ncf, rp, kp;
-  trans_dims(p, ncf, rp, kp);
-  cudaError_t e = gemm_launch(g, p, nrhs, T, 0, 0, g.m2l_class_starts, 0, g.m2l_nclasses,
+  cudaError_t e = gemm_launch(g, c, nrhs, T, 0, 0, g.m2l_class_starts, 0, g.m2l_nclasses,
                               th.m2l_max_pairs * nrhs, g.m2l_pair_src, nullptr, mp, nullptr, 1.0,
                               cpair, err, st);
   if (e != cudaSuccess) return e;
   k_trans_reduce<<<dim3(g.nttp_boxes, nrhs), NT, 0, st>>>(
-      ncf, rp, nrhs, g.target_or_target_parent_boxes, 0, g.m2l_tgt_pair_starts, g.m2l_tgt_pairs,
-      cpair, lo, 1, g.box_levels, g.root_extent);
+      c.ncf, c.rp, nrhs, g.target_or_target_parent_boxes, 0, g.m2l_tgt_pair_starts,
+      g.m2l_tgt_pairs, cpair, lo, c.m2l_div_by_width, g.box_levels, g.root_extent);
   return cudaGetLastError();
 }
 
-cudaError_t launch_m2m_gemm(const qbxfmm_geometry& g, const TransHost& th, int p, int nrhs,
-                            const double* T, double2* mp, double* cpair, int32_t* err,
+cudaError_t launch_m2m_gemm(const qbxfmm_geometry& g, const TransHost& th, const TransCfg& c,
+                            int nrhs, const double* T, double2* mp, double* cpair, int32_t* err,
                             cudaStream_t st)
 {
-  int ncf, rp, kp;
-  trans_dims(p, ncf, rp, kp);
   const int nch = 8;
   for (int lev = g.nlevels - 2; lev >= 0; --lev) {
     int g0 = lev * nch;
     int maxp = th.m2m_level_max_group[lev];
     if (maxp == 0) continue;
-    cudaError_t e = gemm_launch(g, p, nrhs, T, g.m2l_nclasses, nch, g.m2m_group_starts, g0, nch,
-                                maxp * nrhs, g.m2m_pair_src, nullptr, mp, nullptr, 1.0, cpair,
+    cudaError_t e = gemm_launch(g, c, nrhs, T, c.m2m_base, c.m2m_mat_mod, g.m2m_group_starts, g0,
+                                nch, maxp * nrhs, g.m2m_pair_src, nullptr, mp, nullptr, 1.0, cpair,
                                 err, st);
     if (e != cudaSuccess) return e;
     int i0 = th.lvl_source_parent[lev], i1 = th.lvl_source_parent[lev + 1];
     if (i1 > i0)
-      k_trans_reduce<<<dim3(i1 - i0, nrhs), NT, 0, st>>>(ncf, rp, nrhs, g.source_parent_boxes, i0,
-                                                         g.m2m_par_pair_starts, g.m2m_par_pairs,
+      k_trans_reduce<<<dim3(i1 - i0, nrhs), NT, 0, st>>>(c.ncf, c.rp, nrhs, g.source_parent_boxes,
+                                                         i0, g.m2m_par_pair_starts, g.m2m_par_pairs,
                                                          cpair, mp, 0, g.box_levels, g.root_extent);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
@@ -362,17 +372,17 @@ cudaError_t launch_m2m_gemm(const qbxfmm_geometry& g, const TransHost& th, int p
   return cudaSuccess;
 }
 
-cudaError_t launch_l2l_gemm(const qbxfmm_geometry& g, const TransHost& th, int p, int nrhs,
-                            const double* T, double2* lo, int32_t* err, cudaStream_t st)
+cudaError_t launch_l2l_gemm(const qbxfmm_geometry& g, const TransHost& th, const TransCfg& c,
+                            int nrhs, const double* T, double2* lo, int32_t* err, cudaStream_t st)
 {
   const int nch = 8;
   for (int lev = 1; lev < g.nlevels; ++lev) {
     int g0 = lev * nch;
     int maxp = th.l2l_level_max_group[lev];
     if (maxp == 0) continue;
-    cudaError_t e = gemm_launch(g, p, nrhs, T, g.m2l_nclasses + 8, nch, g.l2l_group_starts, g0, nch,
-                                maxp * nrhs, g.l2l_pair_src, g.l2l_pair_dst, lo, lo, 1.0, nullptr,
-                                err, st);
+    cudaError_t e = gemm_launch(g, c, nrhs, T, c.l2l_base, c.m2m_mat_mod, g.l2l_group_starts, g0,
+                                nch, maxp * nrhs, g.l2l_pair_src, g.l2l_pair_dst, lo, lo, 1.0,
+                                nullptr, err, st);
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;

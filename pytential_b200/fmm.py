@@ -92,10 +92,11 @@ class SourceKernelSpec:
 class DeviceGeometry:
     """The geometry arrays of one :class:`QBXFMMGeometryData` on a CUDA device."""
 
-    def __init__(self, geo: QBXFMMGeometryData, device="cuda"):
+    def __init__(self, geo: QBXFMMGeometryData, device="cuda", per_level_classes: bool = False):
         self.geo = geo
         self.device = torch.device(device)
-        self.scalars, host = abi.geometry_arrays(geo)
+        self.per_level_classes = per_level_classes
+        self.scalars, host = abi.geometry_arrays(geo, per_level_classes=per_level_classes)
         self.host_arrays = host
         self.arrays = {k: torch.from_numpy(v).to(self.device) for k, v in host.items()}
         self.struct = abi.make_geometry_struct(self.scalars, self.arrays, _ptr)
@@ -105,6 +106,19 @@ class DeviceGeometry:
         if scal is not None and name in scal:
             return scal[name]
         raise AttributeError(name)
+
+
+def needs_per_level_classes(spec: SourceKernelSpec) -> bool:
+    """3D Helmholtz translations depend on the level (k times the box width)."""
+    return spec.kernel.family == abi.QBXFMM_HELMHOLTZ and spec.kernel.dim == 3
+
+
+def _device_geometry(geo, spec, device, device_geometry):
+    if device_geometry is None:
+        return DeviceGeometry(geo, device, per_level_classes=needs_per_level_classes(spec))
+    if needs_per_level_classes(spec) and not device_geometry.per_level_classes:
+        raise ValueError("3D Helmholtz needs a DeviceGeometry built with per_level_classes=True")
+    return device_geometry
 
 
 class DeviceUpsampler:
@@ -223,10 +237,21 @@ class B200QBXExpansionWrangler:
             fmm_order = int(fmm_level_to_order)
         self.fmm_order = fmm_order
         self.nrhs = nrhs
-        self.dgeo = device_geometry or DeviceGeometry(geo_data, device)
+        self.dgeo = _device_geometry(geo_data, tree_indep.spec, device, device_geometry)
         self.device = self.dgeo.device
         self.plan = Plan(self.dgeo, tree_indep.spec, qbx_order, fmm_order, nrhs,
                          target_specific_qbx=self.using_tsqbx)
+        self._translations = None
+        if needs_per_level_classes(tree_indep.spec):
+            # the translation stages of this kernel run on precomputed matrices
+            sizes = self.plan.workspace_sizes()
+            self._translations = [torch.zeros(sz // 8 + 1, dtype=torch.float64,
+                                              device=self.device) for sz in sizes[6:]]
+            z = ctypes.c_void_p(0)
+            ws = abi.QBXFMMWorkspace(z, z, z, z, z, z, None,
+                                     ctypes.c_void_p(_ptr(self._translations[0])),
+                                     ctypes.c_void_p(_ptr(self._translations[1])))
+            self.plan.call("qbxfmm_precompute_translations", ctypes.byref(ws), _stream_handle())
         self.traversal = geo_data.traversal()
         self.tree = self.traversal.tree
         self.error_word = torch.zeros(1, dtype=torch.int32, device=self.device)
@@ -458,13 +483,13 @@ class QBXApply:
                  target_specific_qbx: bool = False, translation_matrices: bool = True):
         self.geo = geo
         self.device = torch.device(device)
-        self.dgeo = device_geometry or DeviceGeometry(geo, device)
+        self.dgeo = _device_geometry(geo, spec, device, device_geometry)
         self.up = DeviceUpsampler(geo.discr, device)
         self.plan = Plan(self.dgeo, spec, qbx_order, fmm_order, nrhs,
                          target_specific_qbx=target_specific_qbx)
         self.nrhs = nrhs
         sizes = self.plan.workspace_sizes()
-        use_mats = translation_matrices and sizes[6] > 0
+        use_mats = (translation_matrices or needs_per_level_classes(spec)) and sizes[6] > 0
         self._ws_tensors = [torch.zeros(max(s, 8) // 8 + 1, dtype=torch.float64,
                                         device=self.device) for s in sizes[:6]]
         self._mat_tensors = [torch.zeros(s // 8 + 1, dtype=torch.float64, device=self.device)

@@ -54,7 +54,7 @@ def host(t):
 
 
 ALL = ["2d-S", "2d-D", "3d-D-small", "3d-S-small", "2d-D-nrhs3", "h2d-BW-small",
-       "h2d-S-small", "h2d-D-small"]
+       "h2d-S-small", "h2d-D-small", "h3d-CF-small", "h3d-S-small", "h3d-D-small"]
 
 
 @pytest.mark.parametrize("name", ALL)
