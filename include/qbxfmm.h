@@ -145,7 +145,8 @@ typedef struct qbxfmm_geometry {
    * translation vector in units of the (source) box width; within a class every
    * translation is the same matrix (up to a per-level factor for M2L), so each
    * class is one dense matrix product over all its pairs.
-   *   M2L: list-2 pairs grouped by offset (target - source) / width.
+   *   M2L: list-2 pairs grouped by offset (target - source) / width; with
+   *        m2l_class_levels also by level, the classes of one offset consecutive.
    *   M2M: (child -> parent) pairs grouped by (parent level, child position).
    *   L2L: (parent -> child) pairs grouped by (child level, child position). */
   int32_t m2l_nclasses;
@@ -154,11 +155,13 @@ typedef struct qbxfmm_geometry {
                                                classes are shared by all levels (Laplace) */
   const int32_t* m2l_class_starts;          /* [m2l_nclasses + 1] into the pair arrays */
   const int32_t* m2l_pair_src;              /* source box per pair (class order) */
+  const int32_t* m2l_pair_dst;              /* target box per pair (class order) */
   const int32_t* m2l_tgt_pair_starts;       /* [nttp_boxes + 1] */
   const int32_t* m2l_tgt_pairs;             /* pair indices per target (list-2 order) */
   int32_t m2m_npairs;
   const int32_t* m2m_group_starts;          /* [nlevels * 2^dim + 1]: group = (level, child pos) */
   const int32_t* m2m_pair_src;              /* child box per pair */
+  const int32_t* m2m_pair_dst;              /* parent box per pair */
   const int32_t* m2m_par_pair_starts;       /* [nsource_parent_boxes + 1] */
   const int32_t* m2m_par_pairs;             /* pair indices per source parent box */
   int32_t l2l_npairs;

@@ -76,8 +76,9 @@ GEOMETRY_FIELDS = [
     ("tsqbx_chunk_count", "pi"), ("tsqbx_targets", "pi"), ("tsqbx_centers", "pi"),
     ("m2l_nclasses", "i"), ("m2l_class_offsets", "pi"), ("m2l_class_levels", "pi"),
     ("m2l_class_starts", "pi"),
-    ("m2l_pair_src", "pi"), ("m2l_tgt_pair_starts", "pi"), ("m2l_tgt_pairs", "pi"),
-    ("m2m_npairs", "i"), ("m2m_group_starts", "pi"), ("m2m_pair_src", "pi"),
+    ("m2l_pair_src", "pi"), ("m2l_pair_dst", "pi"), ("m2l_tgt_pair_starts", "pi"),
+    ("m2l_tgt_pairs", "pi"),
+    ("m2m_npairs", "i"), ("m2m_group_starts", "pi"), ("m2m_pair_src", "pi"), ("m2m_pair_dst", "pi"),
     ("m2m_par_pair_starts", "pi"), ("m2m_par_pairs", "pi"),
     ("l2l_npairs", "i"), ("l2l_group_starts", "pi"), ("l2l_pair_src", "pi"),
     ("l2l_pair_dst", "pi"),
@@ -226,10 +227,12 @@ def translation_classes(tree, trav, per_level: bool = False):
     off = ipos[:, tgt_box] - ipos[:, l2l]                       # (dim, npairs)
     R = int(np.abs(off).max()) if off.size else 0
     key = np.zeros(off.shape[1], np.int64)
-    if per_level:
-        key = np.asarray(tree.box_levels, np.int64)[tgt_box]
     for d in range(dim):
         key = key * (2 * R + 1) + (off[d] + R)
+    if per_level:
+        # classes of one offset are consecutive (one per level): their target boxes are
+        # distinct, so a launch over them may add into the targets directly
+        key = key * (tree.nlevels + 1) + np.asarray(tree.box_levels, np.int64)[tgt_box]
     order = np.lexsort((tgt_idx, key))                        # class, then target
     ukeys, first = np.unique(key[order], return_index=True)
     out["m2l_nclasses"] = len(ukeys)
@@ -240,6 +243,7 @@ def translation_classes(tree, trav, per_level: bool = False):
             if len(ukeys) else np.zeros(0, np.int32)
     out["m2l_class_starts"] = np.concatenate([first, [len(order)]]).astype(np.int32)
     out["m2l_pair_src"] = l2l[order].astype(np.int32)
+    out["m2l_pair_dst"] = tgt_box[order].astype(np.int32)
     pos = np.empty(len(order), np.int64)
     pos[order] = np.arange(len(order))                        # list-2 entry -> pair index
     out["m2l_tgt_pair_starts"] = l2s.astype(np.int32)
@@ -264,6 +268,7 @@ def translation_classes(tree, trav, per_level: bool = False):
     out["m2m_npairs"] = len(o)
     out["m2m_group_starts"] = np.searchsorted(m_grp[o], np.arange(nlev * nch + 1)).astype(np.int32)
     out["m2m_pair_src"] = m_src[o].astype(np.int32)
+    out["m2m_pair_dst"] = spb[m_par[o]].astype(np.int32)
     pos = np.empty(len(o), np.int64)
     pos[o] = np.arange(len(o))
     o2 = np.lexsort((m_src, m_par))

@@ -30,7 +30,8 @@ struct qbxfmm_plan {
   TransHost th;
   TransCfg tc;
   bool h3;                                 // 3D Helmholtz
-  std::vector<double> h3gaunt;             // Gaunt table, [(nu,mu)][(n,m)][j]
+  std::vector<double> h3gaunt;             // Gaunt table, [(nu,mu)][j][(n,m)]
+  std::vector<int32_t> m2l_waves;          // runs of M2L classes with one offset (3D Helmholtz)
   // 3D Helmholtz: translation buffer and pair scratch registered by
   // qbxfmm_precompute_translations, used by the translation stage entries
   mutable const double* trans_dev = nullptr;
@@ -63,7 +64,7 @@ int check_plan(const qbxfmm_plan* p)
 
 // Gaunt integrals G(n,m; nu,mu; l) = int Y_n^m conj(Y_nu^mu) conj(Y_l^{m-mu}) for
 // n, nu <= p (orthonormal spherical harmonics without the Condon-Shortley phase),
-// l = |n - nu| + 2 j, j <= min(n, nu); layout [(nu,mu)][(n,m)][j], j < p + 1.  Exact
+// l = |n - nu| + 2 j, j <= min(n, nu); layout [(nu,mu)][j][(n,m)], j < p + 1.  Exact
 // Gauss-Legendre quadrature in cos(theta) of the polynomial integrand.
 std::vector<double> h3_gaunt_table(int p)
 {
@@ -117,7 +118,7 @@ std::vector<double> h3_gaunt_table(int p)
         for (int m = -n; m <= n; ++m) {
           int lam = m - mu, am = std::abs(m), amu = std::abs(mu), alam = std::abs(lam);
           int e = (am + amu + alam) / 2;
-          size_t base = ((size_t)(nu * nu + nu + mu) * C + (n * n + n + m)) * nl;
+          size_t orow = nu * nu + nu + mu, icol = n * n + n + m;
           for (int j = 0; j <= std::min(n, nu); ++j) {
             int l = std::abs(n - nu) + 2 * j;
             if (alam > l) continue;
@@ -128,7 +129,7 @@ std::vector<double> h3_gaunt_table(int p)
               acc += w[i] * P[(size_t)pidx(n, am) * ng + i] * P[(size_t)pidx(nu, amu) * ng + i] *
                      P[(size_t)pidx(l, alam) * ng + i] * om;
             }
-            G[base + j] = 2.0 * M_PI * acc;
+            G[(orow * nl + j) * C + icol] = 2.0 * M_PI * acc;
           }
         }
   return G;
@@ -190,8 +191,8 @@ int qbxfmm_plan_create(const qbxfmm_kernel* kernel, const qbxfmm_geometry* geome
     return fail(QBXFMM_ERR_UNSUPPORTED, "fmm_order must be in [1, 20]");
   if (k.nrhs < 1) return fail(QBXFMM_ERR_ARG, "nrhs must be >= 1");
   if (k.precision != 0) return fail(QBXFMM_ERR_UNSUPPORTED, "only precision 0 (FP64)");
-  if (k.target_specific_qbx && k.family != QBXFMM_LAPLACE)
-    return fail(QBXFMM_ERR_UNSUPPORTED, "target-specific QBX is built for the Laplace family");
+  if (k.target_specific_qbx && k.family != QBXFMM_LAPLACE && k.dim != 3)
+    return fail(QBXFMM_ERR_UNSUPPORTED, "target-specific QBX is built for Laplace and 3D Helmholtz");
   if (k.family == QBXFMM_HELMHOLTZ && k.dim == 3) {
     if (k.qbx_order > 5 || k.qbx_order > k.fmm_order)
       return fail(QBXFMM_ERR_UNSUPPORTED, "3D Helmholtz: qbx_order must be <= min(5, fmm_order)");
@@ -234,7 +235,21 @@ int qbxfmm_plan_create(const qbxfmm_kernel* kernel, const qbxfmm_geometry* geome
     delete p;
     return fail(QBXFMM_ERR_UNSUPPORTED, "3D Helmholtz: translation matrices unsupported for this order");
   }
-  if (p->h3) p->h3gaunt = h3_gaunt_table(k.fmm_order);
+  if (p->h3) {
+    p->h3gaunt = h3_gaunt_table(k.fmm_order);
+    std::vector<int32_t> off(3 * (size_t)g.m2l_nclasses);
+    if (g.m2l_nclasses > 0)
+      e = cudaMemcpy(off.data(), g.m2l_class_offsets, sizeof(int32_t) * off.size(),
+                     cudaMemcpyDeviceToHost);
+    p->m2l_waves.push_back(0);
+    for (int c = 1; c < g.m2l_nclasses; ++c) {
+      bool same = true;
+      for (int d = 0; d < 3; ++d) same = same && off[(size_t)d * g.m2l_nclasses + c] ==
+                                                   off[(size_t)d * g.m2l_nclasses + c - 1];
+      if (!same) p->m2l_waves.push_back(c);
+    }
+    p->m2l_waves.push_back(g.m2l_nclasses);
+  }
   if (e == cudaSuccess && p->trans_ok) {
     const int nch = 8;
     std::vector<int32_t> cs(g.m2l_nclasses + 1), ms(g.nlevels * nch + 1), ls(g.nlevels * nch + 1);
@@ -311,10 +326,10 @@ int qbxfmm_coarsen_multipoles(const qbxfmm_plan* p, void* mpoles, void* stream)
 {
   if (int rc = check_plan(p)) return rc;
   if (p->h3) {
-    if (!p->trans_dev || !p->scratch_dev)
+    if (!p->trans_dev)
       return fail(QBXFMM_ERR_ARG, "3D Helmholtz: call qbxfmm_precompute_translations first");
-    QBX_TRY(launch_m2m_gemm(p->geo, p->th, p->tc, p->kern.nrhs, p->trans_dev, (double2*)mpoles,
-                            p->scratch_dev, nullptr, S(stream)),
+    QBX_TRY(launch_m2m_direct(p->geo, p->th, p->tc, p->kern.nrhs, p->trans_dev, (double2*)mpoles,
+                              nullptr, S(stream)),
             "coarsen_multipoles");
     return QBXFMM_OK;
   }
@@ -355,11 +370,11 @@ int qbxfmm_multipole_to_local(const qbxfmm_plan* p, const void* mpoles, void* lo
 {
   if (int rc = check_plan(p)) return rc;
   if (p->h3) {
-    if (!p->trans_dev || !p->scratch_dev)
+    if (!p->trans_dev)
       return fail(QBXFMM_ERR_ARG, "3D Helmholtz: call qbxfmm_precompute_translations first");
-    QBX_TRY(launch_m2l_gemm(p->geo, p->th, p->tc, p->kern.nrhs, p->trans_dev,
-                            (const double2*)mpoles, (double2*)locals, p->scratch_dev, error_word,
-                            S(stream)),
+    QBX_TRY(launch_m2l_direct(p->geo, p->th, p->tc, p->m2l_waves.data(),
+                              (int)p->m2l_waves.size() - 1, p->kern.nrhs, p->trans_dev,
+                              (const double2*)mpoles, (double2*)locals, error_word, S(stream)),
             "multipole_to_local");
     return QBXFMM_OK;
   }
@@ -424,8 +439,8 @@ int qbxfmm_refine_locals(const qbxfmm_plan* p, void* locals, void* stream)
   if (p->h3) {
     if (!p->trans_dev)
       return fail(QBXFMM_ERR_ARG, "3D Helmholtz: call qbxfmm_precompute_translations first");
-    QBX_TRY(launch_l2l_gemm(p->geo, p->th, p->tc, p->kern.nrhs, p->trans_dev, (double2*)locals,
-                            nullptr, S(stream)),
+    QBX_TRY(launch_l2l_direct(p->geo, p->th, p->tc, p->kern.nrhs, p->trans_dev, (double2*)locals,
+                              nullptr, S(stream)),
             "refine_locals");
     return QBXFMM_OK;
   }
@@ -554,8 +569,14 @@ int qbxfmm_eval_target_specific_qbx_locals(const qbxfmm_plan* p, const void* str
                                            void* pot_tree, int32_t* error_word, void* stream)
 {
   if (int rc = check_plan(p)) return rc;
+  if (p->h3) {
+    QBX_TRY(h3_launch_tsqbx(p->geo, p->hc, p->kern.qbx_order, p->kern.nrhs, (const double2*)strengths,
+                            (double2*)pot_tree, error_word, S(stream)),
+            "eval_target_specific_qbx_locals");
+    return QBXFMM_OK;
+  }
   if (p->helm)
-    return fail(QBXFMM_ERR_UNSUPPORTED, "target-specific QBX is built for the Laplace family");
+    return fail(QBXFMM_ERR_UNSUPPORTED, "target-specific QBX is built for Laplace and 3D Helmholtz");
   QBX_TRY(launch_tsqbx(p->geo, p->sc, p->kern.qbx_order, p->kern.nrhs, (const double*)strengths,
                        (double*)pot_tree, error_word, S(stream)),
           "eval_target_specific_qbx_locals");
@@ -603,7 +624,7 @@ int qbxfmm_workspace_sizes(const qbxfmm_plan* p, size_t* sizes6 /* 8 entries */)
     if (e != cudaSuccess) return cuda_check(e, "workspace_sizes");
     npairs = std::max(npairs, g.m2m_npairs);
     sizes6[6] = trans_matrix_bytes(p->tc) + p->h3gaunt.size() * sizeof(double);
-    sizes6[7] = trans_scratch_bytes(p->tc, npairs, p->kern.nrhs);
+    sizes6[7] = p->h3 ? 0 : trans_scratch_bytes(p->tc, npairs, p->kern.nrhs);
   } else {
     sizes6[6] = sizes6[7] = 0;
   }
@@ -615,8 +636,8 @@ int qbxfmm_precompute_translations(const qbxfmm_plan* p, const qbxfmm_workspace*
   if (int rc = check_plan(p)) return rc;
   if (!ws) return fail(QBXFMM_ERR_ARG, "null workspace");
   if (p->h3) {
-    if (!ws->translations || !ws->pair_scratch)
-      return fail(QBXFMM_ERR_ARG, "3D Helmholtz needs the translations and pair-scratch buffers");
+    if (!ws->translations)
+      return fail(QBXFMM_ERR_ARG, "3D Helmholtz needs the translations buffer");
     double* T = (double*)ws->translations;
     double* G = T + p->tc.nmatrices * p->tc.rp * p->tc.kp;
     QBX_TRY(cudaMemcpyAsync(G, p->h3gaunt.data(), p->h3gaunt.size() * sizeof(double),
@@ -646,8 +667,8 @@ int qbxfmm_apply(const qbxfmm_plan* p, const qbxfmm_upsample* up, const qbxfmm_w
   if (int rc = qbxfmm_workspace_sizes(p, sz)) return rc;
   const bool gemm = !p->h3 && p->trans_ok && ws->translations && ws->pair_scratch;
   if (p->h3) {
-    if (!ws->translations || !ws->pair_scratch)
-      return fail(QBXFMM_ERR_ARG, "3D Helmholtz needs the translations and pair-scratch buffers");
+    if (!ws->translations)
+      return fail(QBXFMM_ERR_ARG, "3D Helmholtz needs the translations buffer");
     p->trans_dev = (const double*)ws->translations;
     p->scratch_dev = (double*)ws->pair_scratch;
   }

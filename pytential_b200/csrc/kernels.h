@@ -39,6 +39,14 @@ cudaError_t launch_m2m_gemm(const qbxfmm_geometry& g, const TransHost& th, const
                             cudaStream_t st);
 cudaError_t launch_l2l_gemm(const qbxfmm_geometry& g, const TransHost& th, const TransCfg& c,
                             int nrhs, const double* T, double2* lo, int32_t* err, cudaStream_t st);
+// scratch-free forms on the tiled kernel (per-level classes, 3D Helmholtz)
+cudaError_t launch_m2l_direct(const qbxfmm_geometry& g, const TransHost& th, const TransCfg& c,
+                              const int32_t* waves, int nwaves, int nrhs, const double* T,
+                              const double2* mp, double2* lo, int32_t* err, cudaStream_t st);
+cudaError_t launch_m2m_direct(const qbxfmm_geometry& g, const TransHost& th, const TransCfg& c,
+                              int nrhs, const double* T, double2* mp, int32_t* err, cudaStream_t st);
+cudaError_t launch_l2l_direct(const qbxfmm_geometry& g, const TransHost& th, const TransCfg& c,
+                              int nrhs, const double* T, double2* lo, int32_t* err, cudaStream_t st);
 
 cudaError_t launch_form_strengths(const qbxfmm_geometry& g, const qbxfmm_upsample& up, int nrhs,
                                   const double* density, double* strengths, cudaStream_t st);
@@ -122,6 +130,8 @@ cudaError_t h3_launch_l2qbxl(const qbxfmm_geometry& g, HelmCoeffs hc, int pf, in
                              cudaStream_t st);
 cudaError_t h3_launch_qbxl2p(const qbxfmm_geometry& g, HelmCoeffs hc, int q, int nrhs,
                              const double2* qe, double2* pt, cudaStream_t st);
+cudaError_t h3_launch_tsqbx(const qbxfmm_geometry& g, HelmCoeffs hc, int q, int nrhs,
+                            const double2* s, double2* pt, int32_t* err, cudaStream_t st);
 cudaError_t h3_launch_assemble(const qbxfmm_geometry& g, int nrhs, const double2* pot_nonqbx,
                                const double2* pot_tree, double2* out, cudaStream_t st);
 cudaError_t h3_launch_trans_build(const qbxfmm_geometry& g, const TransCfg& tc, double k,

@@ -12,7 +12,7 @@
 // n^2 + n + m.  Translations use the addition theorem
 //   F_n^m(r + b) = sum c_{nu mu; n m}(b) R_nu^mu(r),
 //   c_{nu mu; n m}(b) = 4 pi sum_l i^{nu + l - n} f_l(k|b|) Y_l^{m - mu}(b) G(n,m; nu,mu; l)
-// (G: Gaunt integrals, a host-computed table), applied as per-level, per-class
+// (G: Gaunt integrals, a host-computed table, layout [(nu,mu)][j][(n,m)]), applied as per-level, per-class
 // complex matrices on the FP64 tensor cores for M2M / M2L / L2L and directly for the
 // point-to-box translations into QBX centers.  Source-normal derivatives use the
 // ladder relations of R and S.
@@ -766,138 +766,328 @@ k_h3_p2qbxl(qbxfmm_geometry g, HelmCoeffs hc, int nrhs, const double2* __restric
   }
 }
 
-// Box expansion (order pf) -> QBX local (order Q) at a center, by the addition theorem
-// with the Gaunt table (layout [(nu,mu) out][(n,m) in][j], l = |n - nu| + 2 j).
-// CTA per chunk of <= 32 centers of one target box.  M2QBXL (FROM_LOCAL = false):
-// the warps take the target box's list-3 boxes in turn, stage each multipole
-// (times s_s^n i^-n) and run over the chunk's centers, accumulating into per-center
-// shared sums.  L2QBXL (FROM_LOCAL = true): the warps take the centers in turn,
-// each translating the target box's local (times s_b^-n i^-n).  Per (center, box):
-// the warp builds w_l^lam = 4 pi i^l f_l(k|b|) Y_l^lam(b) (f = h or j) in shared
-// memory; lane o owns outputs o and o + 32.
-template <bool FROM_LOCAL>
+// Box expansion (order pf) -> QBX local (order q) at a center, by the addition theorem
+// with the Gaunt table (layout [(nu,mu) out][j][(n,m) in], l = |n - nu| + 2 j).
+// H3_E2Q_ZS CTAs per chunk of <= 32 centers of one target box (split over the
+// centers), RB densities per CTA.  M2QBXL
+// (FROM_LOCAL = false): the CTA runs over the target box's list-3 boxes, staging each
+// multipole (times s_s^n i^-n) for the RB densities in shared memory; L2QBXL: the one
+// box is the target box itself (local times s_b^-n i^-n).  For each (center, box) the
+// warp owning the center builds w_l^lam = 4 pi i^l f_l(k|b|) Y_l^lam(b) (f = h or j),
+// then, per output coefficient (nu, mu), the operator row
+//   c_{nu mu; n m} = sum_j G w_{l, m - mu}   (all (n, m), lanes split the row)
+// once and applies it to the RB staged expansions: lane = (density, part of the row),
+// a shuffle reduction over the parts, and the result (times i^nu s_t^nu) added into the
+// center's expansion.  Every center belongs to one CTA, so the additions need no atomics.
+constexpr int H3_E2Q_ZS = 4;             // CTAs sharing one chunk (split over its centers)
+
+template <bool FROM_LOCAL, int RB>
 __global__ void __launch_bounds__(NT)
 k_h3_e2qbxl(qbxfmm_geometry g, HelmCoeffs hc, int pf, int q, int nrhs,
             const double2* __restrict__ exps, const double* __restrict__ gaunt,
             double2* __restrict__ qbx_exps, int32_t* err)
 {
+  constexpr int NPART = 32 / RB;          // lanes per density
   extern __shared__ double2 smem2[];
+  __shared__ short2 s_nm[(H3_LMAX + 1) * (H3_LMAX + 1)];
   const int ncf = (pf + 1) * (pf + 1), ncq = (q + 1) * (q + 1);
   const int L = pf + q;
   const int nw = (L + 1) * (L + 1);
   const int nrec = (L + 1) * (L + 2) / 2;
-  const int Cp = ncf, nl = pf + 1;
+  const int nl = pf + 1;
+  const int per = ncf + nw + (L + 2);
   double2* rec = smem2;                                          // [nrec]
-  double2* Ew = rec + nrec + (size_t)(threadIdx.x >> 5) * (ncf + nw + 2 * (L + 2));
-  double2* Wt = Ew + ncf;                                        // [nw]
+  double2* Es = rec + nrec;                                      // [ncf][RB]
+  double2* Rw = Es + (size_t)ncf * RB + (size_t)(threadIdx.x >> 5) * per;
+  double2* row = Rw;                                             // [ncf]
+  double2* Wt = Rw + ncf;                                        // [nw]
   double2* rad = Wt + nw;                                        // [L + 2]
-  double2* sums = rec + nrec + (size_t)NW * (ncf + nw + 2 * (L + 2));   // [NW][32][ncq]
   int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int rr = lane / NPART, part = lane - rr * NPART;
   h3_rec_table(L, rec, threadIdx.x, NT);
+  for (int e = threadIdx.x; e < ncf; e += NT) {
+    int n, m;
+    hq_decode(e, n, m);
+    s_nm[e] = make_short2((short)n, (short)m);
+  }
+  __syncthreads();
   int chunk = blockIdx.x;
-  int r = blockIdx.y;
+  int r0 = blockIdx.y * RB;
   int itb = g.qbx_chunk_target_box[chunk];
   int nctr = g.qbx_chunk_count[chunk];
-  for (int e = threadIdx.x; e < NW * 32 * ncq; e += NT) sums[e] = c2(0.0);
-  __syncthreads();
 
-  // one (center, box) translation by this warp into sums[warp][ci][*]
-  auto translate = [&](int ci, const double* cb, bool singular) {
-    int ctr = g.centers_by_target_box[g.qbx_chunk_start[chunk] + ci];
-    double cc[3];
-    load_point<3>(g.centers, g.ncenters, ctr, cc);
+  int nbox;
+  if (FROM_LOCAL) nbox = 1;
+  else nbox = g.list3_starts[itb + 1] - g.list3_starts[itb];
+  for (int bi = 0; bi < nbox; ++bi) {
+    int sbx;
+    if (FROM_LOCAL) sbx = g.target_boxes[itb];
+    else sbx = g.list3_lists[g.list3_starts[itb] + bi];
+    if ((unsigned)sbx >= (unsigned)g.nboxes) {
+      report(err, QBX_DEVERR_BAD_BOX);
+      continue;
+    }
+    double cb[3];
+    load_point<3>(g.box_centers, g.nboxes, sbx, cb);
+    double sb = h3_scale(hc.k, level_width(g, g.box_levels[sbx]));
+    __syncthreads();
+    for (int e = threadIdx.x; e < ncf * RB; e += NT) {
+      int ei = e / RB, ri = e - ei * RB;
+      int n, m;
+      hq_decode(ei, n, m);
+      double2 v = c2(0.0);
+      if (r0 + ri < nrhs) {
+        v = exps[((size_t)sbx * nrhs + r0 + ri) * ncf + ei];
+        v = cscale(pow(sb, FROM_LOCAL ? -(double)n : (double)n), cmul(ipow(-n), v));
+      }
+      Es[e] = v;
+    }
+    __syncthreads();
+    for (int ci = blockIdx.z * NW + warp; ci < nctr; ci += NW * H3_E2Q_ZS) {
+      int ctr = g.centers_by_target_box[g.qbx_chunk_start[chunk] + ci];
+      if ((unsigned)ctr >= (unsigned)g.ncenters) {
+        report(err, QBX_DEVERR_BAD_CENTER);
+        continue;
+      }
+      double cc[3];
+      load_point<3>(g.centers, g.ncenters, ctr, cc);
+      double bv[3] = {cc[0] - cb[0], cc[1] - cb[1], cc[2] - cb[2]};
+      double2 w;
+      double rr_;
+      double t = h3_dir(bv, w, rr_);
+      if (lane == 0) {
+        if (FROM_LOCAL) {
+          double jv[H3_LMAX + 2];
+          h3_sph_j(L, hc.k * rr_, jv);
+          for (int l = 0; l <= L; ++l) rad[l] = c2(jv[l]);
+        } else {
+          h3_sph_h(L, hc.k * rr_, rad);
+        }
+        for (int l = 0; l <= L; ++l) rad[l] = cmul(cscale(FOUR_PI, ipow(l)), rad[l]);
+      }
+      __syncwarp();
+      for (int m = lane; m <= L; m += 32) h3_wave_column(m, L, t, w, rec, rad, Wt, 1);
+      __syncwarp();
+      double st = h3_scale(hc.k, g.expansion_radii[ctr]);
+      for (int o = 0; o < ncq; ++o) {
+        int nu, mu;
+        hq_decode(o, nu, mu);
+        // operator row c_{o, e}, e = (n, m)
+        for (int e = lane; e < ncf; e += 32) {
+          short2 nm = s_nm[e];
+          int n = nm.x, m = nm.y;
+          int lam = m - mu, lbase = abs(n - nu), jmax = min(n, nu);
+          const double* G = gaunt + (size_t)o * nl * ncf + e;
+          double2 tt = c2(0.0);
+          for (int j = 0; j <= jmax; ++j) {
+            int l = lbase + 2 * j;
+            if (abs(lam) <= l) tt = caxpy(G[(size_t)j * ncf], Wt[hq(l, lam)], tt);
+          }
+          row[e] = tt;
+        }
+        __syncwarp();
+        double2 a0 = c2(0.0), a1 = c2(0.0), a2 = c2(0.0), a3 = c2(0.0);
+        int e = part;
+        for (; e + 3 * NPART < ncf; e += 4 * NPART) {
+          a0 = cfma(row[e], Es[e * RB + rr], a0);
+          a1 = cfma(row[e + NPART], Es[(e + NPART) * RB + rr], a1);
+          a2 = cfma(row[e + 2 * NPART], Es[(e + 2 * NPART) * RB + rr], a2);
+          a3 = cfma(row[e + 3 * NPART], Es[(e + 3 * NPART) * RB + rr], a3);
+        }
+        for (; e < ncf; e += NPART) a0 = cfma(row[e], Es[e * RB + rr], a0);
+        double2 a = cadd(cadd(a0, a1), cadd(a2, a3));
+#pragma unroll
+        for (int off = NPART / 2; off > 0; off >>= 1) {
+          a.x += __shfl_xor_sync(0xffffffffu, a.x, off);
+          a.y += __shfl_xor_sync(0xffffffffu, a.y, off);
+        }
+        if (part == 0 && r0 + rr < nrhs) {
+          a = cscale(pow(st, (double)nu), cmul(ipow(nu), a));
+          double2* out = qbx_exps + ((size_t)ctr * nrhs + r0 + rr) * ncq + o;
+          *out = cadd(*out, a);
+        }
+        __syncwarp();
+      }
+    }
+  }
+}
+
+// The same translations for RB >= 4 densities with the operator applied on the FP64
+// tensor cores.  One warp per center (H3_MMA_ZS CTAs x 4 warps cover a chunk of <= 32
+// centers); per (center, box) the warp builds the operator rows c_{o, e} four at a time
+// and multiplies them into its register accumulators with mma.sync m8n8k4 f64, in the
+// real form [Cr; Ci] = [[Cr_op, -Ci_op], [Ci_op, Cr_op]] [Er; Ei]: an m-tile is four
+// complex rows (real parts in rows 0-3, imaginary parts in rows 4-7), K runs over the
+// real then the imaginary parts of the staged expansions, N over the densities.
+constexpr int H3_MMA_ZS = 8;
+constexpr int H3_MT_MAX = 9;        // m-tiles: ceil((q+1)^2 / 4), q <= 5
+
+QBX_D void dmma_f64(double& d0, double& d1, double a, double b)
+{
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+template <bool FROM_LOCAL, int RB>
+__global__ void __launch_bounds__(NT)
+k_h3_e2qbxl_mma(qbxfmm_geometry g, HelmCoeffs hc, int pf, int q, int nrhs,
+                const double2* __restrict__ exps, const double* __restrict__ gaunt,
+                double2* __restrict__ qbx_exps, int32_t* err)
+{
+  constexpr int NTN = (RB + 7) / 8;
+  extern __shared__ double2 smem2[];
+  __shared__ short2 s_nm[(H3_LMAX + 1) * (H3_LMAX + 1)];
+  const int ncf = (pf + 1) * (pf + 1), ncq = (q + 1) * (q + 1);
+  const int L = pf + q;
+  const int nw = (L + 1) * (L + 1);
+  const int nrec = (L + 1) * (L + 2) / 2;
+  const int nl = pf + 1;
+  const int nmt = (ncq + 3) / 4;
+  const int K2 = 2 * ncf, Kp = (K2 + 3) / 4 * 4;
+  const int per = nw + (L + 2) + 4 * ncf;
+  double2* rec = smem2;                                          // [nrec]
+  double2* Es = rec + nrec;                                      // [ncf][RB]
+  double2* Wt = Es + (size_t)ncf * RB + (size_t)(threadIdx.x >> 5) * per;   // [nw]
+  double2* rad = Wt + nw;                                        // [L + 2]
+  double2* rows = rad + (L + 2);                                 // [4][ncf]
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int gq = lane >> 2, tq = lane & 3;
+  h3_rec_table(L, rec, threadIdx.x, NT);
+  for (int e = threadIdx.x; e < ncf; e += NT) {
+    int n, m;
+    hq_decode(e, n, m);
+    s_nm[e] = make_short2((short)n, (short)m);
+  }
+  __syncthreads();   // s_nm and rec are read below, also when there is no box
+  int chunk = blockIdx.x;
+  int r0 = blockIdx.y * RB;
+  int itb = g.qbx_chunk_target_box[chunk];
+  int nctr = g.qbx_chunk_count[chunk];
+  int ci = blockIdx.z * NW + warp;
+  bool has = ci < nctr;
+  int ctr = has ? g.centers_by_target_box[g.qbx_chunk_start[chunk] + ci] : 0;
+  if ((unsigned)ctr >= (unsigned)g.ncenters) {
+    report(err, QBX_DEVERR_BAD_CENTER);
+    has = false;
+    ctr = 0;
+  }
+  if (blockIdx.z * NW >= nctr) return;     // the whole CTA is idle
+  double cc[3];
+  load_point<3>(g.centers, g.ncenters, ctr, cc);
+  double acc[H3_MT_MAX][NTN][2];
+#pragma unroll
+  for (int i = 0; i < H3_MT_MAX; ++i)
+#pragma unroll
+    for (int j = 0; j < NTN; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+
+  int nbox = FROM_LOCAL ? 1 : g.list3_starts[itb + 1] - g.list3_starts[itb];
+  for (int bi = 0; bi < nbox; ++bi) {
+    int sbx = FROM_LOCAL ? g.target_boxes[itb] : g.list3_lists[g.list3_starts[itb] + bi];
+    if ((unsigned)sbx >= (unsigned)g.nboxes) {
+      report(err, QBX_DEVERR_BAD_BOX);
+      continue;
+    }
+    double cb[3];
+    load_point<3>(g.box_centers, g.nboxes, sbx, cb);
+    double sb = h3_scale(hc.k, level_width(g, g.box_levels[sbx]));
+    __syncthreads();
+    for (int e = threadIdx.x; e < ncf * RB; e += NT) {
+      int ei = e / RB, ri = e - ei * RB;
+      int n = s_nm[ei].x;
+      double2 v = c2(0.0);
+      if (r0 + ri < nrhs) {
+        v = exps[((size_t)sbx * nrhs + r0 + ri) * ncf + ei];
+        v = cscale(pow(sb, FROM_LOCAL ? -(double)n : (double)n), cmul(ipow(-n), v));
+      }
+      Es[e] = v;
+    }
+    __syncthreads();
+    if (!has) continue;
     double bv[3] = {cc[0] - cb[0], cc[1] - cb[1], cc[2] - cb[2]};
     double2 w;
-    double rr;
-    double t = h3_dir(bv, w, rr);
+    double rr_;
+    double t = h3_dir(bv, w, rr_);
     if (lane == 0) {
-      if (singular) {
-        h3_sph_h(L, hc.k * rr, rad);
-      } else {
+      if (FROM_LOCAL) {
         double jv[H3_LMAX + 2];
-        h3_sph_j(L, hc.k * rr, jv);
+        h3_sph_j(L, hc.k * rr_, jv);
         for (int l = 0; l <= L; ++l) rad[l] = c2(jv[l]);
+      } else {
+        h3_sph_h(L, hc.k * rr_, rad);
       }
       for (int l = 0; l <= L; ++l) rad[l] = cmul(cscale(FOUR_PI, ipow(l)), rad[l]);
     }
     __syncwarp();
     for (int m = lane; m <= L; m += 32) h3_wave_column(m, L, t, w, rec, rad, Wt, 1);
     __syncwarp();
-    double st = h3_scale(hc.k, g.expansion_radii[ctr]);
-    for (int o = lane; o < ncq; o += 32) {
-      int nu, mu;
-      hq_decode(o, nu, mu);
-      double2 a = c2(0.0);
-      const double* G = gaunt + (size_t)o * Cp * nl;
-      for (int n = 0; n <= pf; ++n) {
-        int jmax = min(n, nu);
-        int lbase = abs(n - nu);
-        for (int m = -n; m <= n; ++m) {
-          int lam = m - mu;
-          const double* Gc = G + (size_t)hq(n, m) * nl;
-          double2 tt = c2(0.0);
+#pragma unroll
+    for (int mt = 0; mt < H3_MT_MAX; ++mt) {
+      if (mt >= nmt) break;
+      // four operator rows o = 4 mt + rl into rows[rl][e]
+      for (int x = lane; x < 4 * ncf; x += 32) {
+        int rl = x / ncf, e = x - rl * ncf;
+        int o = 4 * mt + rl;
+        double2 tt = c2(0.0);
+        if (o < ncq) {
+          int nu = s_nm[o].x, mu = s_nm[o].y;
+          short2 nm = s_nm[e];
+          int n = nm.x, m = nm.y;
+          int lam = m - mu, lbase = abs(n - nu), jmax = min(n, nu);
+          const double* G = gaunt + (size_t)o * nl * ncf + e;
           for (int j = 0; j <= jmax; ++j) {
             int l = lbase + 2 * j;
-            if (abs(lam) > l) continue;
-            tt = caxpy(Gc[j], Wt[hq(l, lam)], tt);
+            if (abs(lam) <= l) tt = caxpy(G[(size_t)j * ncf], Wt[hq(l, lam)], tt);
           }
-          a = cfma(Ew[hq(n, m)], tt, a);
+        }
+        rows[x] = tt;
+      }
+      __syncwarp();
+      const double2* rrow = rows + (gq & 3) * ncf;
+      const bool imrow = gq >= 4;
+      for (int k0 = 0; k0 < Kp; k0 += 4) {
+        int k = k0 + tq;
+        double a = 0.0;
+        bool lo = k < ncf;
+        int e = lo ? k : k - ncf;
+        if (k < K2) {
+          double2 c = rrow[e];
+          a = imrow ? (lo ? c.y : c.x) : (lo ? c.x : -c.y);
+        }
+#pragma unroll
+        for (int nt = 0; nt < NTN; ++nt) {
+          int col = nt * 8 + gq;
+          double b = 0.0;
+          if (k < K2 && col < RB) {
+            double2 ev = Es[e * RB + col];
+            b = lo ? ev.x : ev.y;
+          }
+          dmma_f64(acc[mt][nt][0], acc[mt][nt][1], a, b);
         }
       }
-      // times i^nu s_t^nu
-      a = cscale(pow(st, (double)nu), cmul(ipow(nu), a));
-      double2* S = sums + ((size_t)warp * 32 + ci) * ncq + o;
-      *S = cadd(*S, a);
-    }
-    __syncwarp();
-  };
-
-  if (FROM_LOCAL) {
-    int tb = g.target_boxes[itb];
-    double cb[3];
-    load_point<3>(g.box_centers, g.nboxes, tb, cb);
-    double sb = h3_scale(hc.k, level_width(g, g.box_levels[tb]));
-    const double2* src = exps + ((size_t)tb * nrhs + r) * ncf;
-    for (int e = lane; e < ncf; e += 32) {
-      int n, m;
-      hq_decode(e, n, m);
-      Ew[e] = cscale(pow(sb, -(double)n), cmul(ipow(-n), src[e]));
-    }
-    __syncwarp();
-    for (int ci = warp; ci < nctr; ci += NW) translate(ci, cb, false);
-  } else {
-    for (int li = g.list3_starts[itb] + warp; li < g.list3_starts[itb + 1]; li += NW) {
-      int sbx = g.list3_lists[li];
-      if ((unsigned)sbx >= (unsigned)g.nboxes) {
-        report(err, QBX_DEVERR_BAD_BOX);
-        continue;
-      }
-      double cb[3];
-      load_point<3>(g.box_centers, g.nboxes, sbx, cb);
-      double ss = h3_scale(hc.k, level_width(g, g.box_levels[sbx]));
-      const double2* src = exps + ((size_t)sbx * nrhs + r) * ncf;
       __syncwarp();
-      for (int e = lane; e < ncf; e += 32) {
-        int n, m;
-        hq_decode(e, n, m);
-        Ew[e] = cscale(pow(ss, (double)n), cmul(ipow(-n), src[e]));
-      }
-      __syncwarp();
-      for (int ci = 0; ci < nctr; ++ci) translate(ci, cb, true);
     }
   }
-  __syncthreads();
-  for (int e = threadIdx.x; e < nctr * ncq; e += NT) {
-    int ci = e / ncq, o = e - ci * ncq;
-    int ctr = g.centers_by_target_box[g.qbx_chunk_start[chunk] + ci];
-    if ((unsigned)ctr >= (unsigned)g.ncenters) {
-      report(err, QBX_DEVERR_BAD_CENTER);
-      continue;
-    }
-    double2 a = c2(0.0);
-    for (int w = 0; w < NW; ++w) a = cadd(a, sums[((size_t)w * 32 + ci) * ncq + o]);
-    double2* out = qbx_exps + ((size_t)ctr * nrhs + r) * ncq + o;
-    *out = cadd(*out, a);
+  if (!has) return;
+  // C'[row gq][col nt*8 + 2 tq + v]: rows 0-3 real, 4-7 imaginary parts of o = 4 mt + (gq & 3)
+  double st = h3_scale(hc.k, g.expansion_radii[ctr]);
+#pragma unroll
+  for (int mt = 0; mt < H3_MT_MAX; ++mt) {
+    if (mt >= nmt) break;
+#pragma unroll
+    for (int nt = 0; nt < NTN; ++nt)
+#pragma unroll
+      for (int v = 0; v < 2; ++v) {
+        double im = __shfl_down_sync(0xffffffffu, acc[mt][nt][v], 16);
+        int o = 4 * mt + gq;
+        int col = nt * 8 + 2 * tq + v;
+        if (gq < 4 && o < ncq && col < RB && r0 + col < nrhs) {
+          int nu = s_nm[o].x;
+          double2 a = cscale(pow(st, (double)nu), cmul(ipow(nu), c2(acc[mt][nt][v], im)));
+          double2* out = qbx_exps + ((size_t)ctr * nrhs + r0 + col) * ncq + o;
+          *out = cadd(*out, a);
+        }
+      }
   }
 }
 
@@ -924,6 +1114,154 @@ k_h3_qbxl2p(qbxfmm_geometry g, HelmCoeffs hc, int q, int nrhs, const double2* __
     double x[3];
     load_point<3>(g.targets, g.ntargets, t, x);
     pot_tree[(size_t)r * g.ntargets + t] = h3_e2p(Lc, q, true, hc.k, s, cc, x, rec);
+  }
+}
+
+// Target-specific near field (eval_target_specific_qbx_locals, pytential/qbx/fmm.py:391-394;
+// the reference's native module pytential/qbx/target_specific/impl.pyx:363-563):
+// per (target t, its center c, list-1 source y), with a = t - c, b = y - c,
+//   K_S = ik sum_{n<=Q} (2n+1) j_n(k|a|) h_n(k|b|) P_n(cos g),
+//   K_D = ik sum (2n+1) j_n(k|a|) (k h_n'(k|b|) P_n nu.bh + h_n P_n' (nu.ah - cos g nu.bh) / |b|),
+// the order-Q spherical-wave QBX expansion evaluated without forming it.  The kernel
+// value K = cq K_S + cd K_D is computed once per pair and applied to RB densities at
+// a time (lane = target; 4 warps split each 128-source tile; strengths of the tile's
+// sources for the RB densities staged in shared memory).
+template <int Q, int RB>
+__global__ void __launch_bounds__(NT)
+k_h3_tsqbx(qbxfmm_geometry g, HelmCoeffs hc, int nrhs, const double2* __restrict__ strengths,
+           double2* __restrict__ pot_tree, int32_t* err)
+{
+  __shared__ double s_y[3][NT], s_n[3][NT];
+  __shared__ double2 s_q[RB][NT];
+  __shared__ int s_pref[MAXB + 1], s_start[MAXB];
+  extern __shared__ double2 smem2[];
+  double2* s_red = smem2;   // [NW-1][32][RB]
+  int chunk = blockIdx.x;
+  int r0 = blockIdx.y * RB;
+  int itb = g.tsqbx_chunk_target_box[chunk];
+  int i0 = g.tsqbx_chunk_start[chunk];
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  bool active = lane < g.tsqbx_chunk_count[chunk];
+  int t = active ? g.tsqbx_targets[i0 + lane] : 0;
+  int ctr = active ? g.tsqbx_centers[i0 + lane] : 0;
+  if ((unsigned)ctr >= (unsigned)g.ncenters || (unsigned)t >= (unsigned)g.ntargets) {
+    report(err, QBX_DEVERR_BAD_CENTER);
+    active = false;
+    t = ctr = 0;
+  }
+  double cc[3], x[3];
+  load_point<3>(g.centers, g.ncenters, ctr, cc);
+  load_point<3>(g.targets, g.ntargets, t, x);
+  double a[3] = {x[0] - cc[0], x[1] - cc[1], x[2] - cc[2]};
+  double alen = sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+  double ainv = alen > 0.0 ? 1.0 / alen : 0.0;
+  double ah[3] = {a[0] * ainv, a[1] * ainv, a[2] * ainv};
+  double jn[Q + 1];
+  {
+    double jv[H3_LMAX + 2];
+    h3_sph_j(Q, hc.k * alen, jv);
+#pragma unroll
+    for (int n = 0; n <= Q; ++n) jn[n] = (2.0 * n + 1.0) * jv[n];
+  }
+  const bool chg = hc.cq.x != 0.0 || hc.cq.y != 0.0;
+  const bool dip = hc.cd.x != 0.0 || hc.cd.y != 0.0;
+  // ik cq, ik cd
+  const double2 kq = c2(-hc.k * hc.cq.y, hc.k * hc.cq.x), kd = c2(-hc.k * hc.cd.y, hc.k * hc.cd.x);
+  double2 acc[RB];
+#pragma unroll
+  for (int i = 0; i < RB; ++i) acc[i] = c2(0.0);
+  int l0 = g.list1_starts[itb], l1 = g.list1_starts[itb + 1];
+  for (int gb = l0; gb < l1; gb += MAXB) {
+    int nb = min(MAXB, l1 - gb);
+    __syncthreads();
+    h3_list_prefix(g, g.list1_lists, gb, nb, s_pref, s_start, err);
+    __syncthreads();
+    int total = s_pref[nb];
+    for (int base = 0; base < total; base += NT) {
+      int v = base + threadIdx.x;
+      if (v < total) {
+        int s = h3_stream_source(v, nb, s_pref, s_start);
+        double y[3], nv[3] = {0, 0, 0};
+        load_point<3>(g.sources, g.nsources, s, y);
+        if (dip) load_point<3>(g.source_normals, g.nsources, s, nv);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          s_y[d][threadIdx.x] = y[d];
+          s_n[d][threadIdx.x] = nv[d];
+        }
+#pragma unroll
+        for (int i = 0; i < RB; ++i)
+          s_q[i][threadIdx.x] = (r0 + i < nrhs) ? strengths[(size_t)(r0 + i) * g.nsources + s] : c2(0.0);
+      }
+      __syncthreads();
+      int jbeg = warp * 32, jend = min(jbeg + 32, total - base);
+      if (active) {
+        for (int j = jbeg; j < jend; ++j) {
+          double b0 = s_y[0][j] - cc[0], b1 = s_y[1][j] - cc[1], b2 = s_y[2][j] - cc[2];
+          double b2s = b0 * b0 + b1 * b1 + b2 * b2;
+          if (b2s == 0.0) continue;
+          double binv = rsqrt(b2s);
+          double blen = b2s * binv;
+          double cg = (ah[0] * b0 + ah[1] * b1 + ah[2] * b2) * binv;
+          double2 h[Q + 2];
+          h3_sph_h(Q + 1, hc.k * blen, h);
+          double xinv = 1.0 / (hc.k * blen);
+          double pm1 = 1.0, pm2 = 0.0, dm1 = 0.0;
+          double2 sS = c2(0.0), sA = c2(0.0), sB = c2(0.0);
+#pragma unroll
+          for (int n = 0; n <= Q; ++n) {
+            double pn, dn;
+            if (n == 0) {
+              pn = 1.0;
+              dn = 0.0;
+            } else if (n == 1) {
+              pn = cg;
+              dn = 1.0;
+            } else {
+              pn = ((2.0 * n - 1) * cg * pm1 - (n - 1.0) * pm2) * (1.0 / n);
+              dn = n * pm1 + cg * dm1;
+            }
+            if (chg) sS = caxpy(jn[n] * pn, h[n], sS);
+            if (dip) {
+              // h_n'(x) = h_{n-1} - (n+1)/x h_n  (n >= 1), h_0' = -h_1
+              double2 hd = (n == 0) ? c2(-h[1].x, -h[1].y)
+                                    : caxpy(-(n + 1.0) * xinv, h[n], h[n - 1]);
+              sA = caxpy(jn[n] * pn * hc.k, hd, sA);
+              sB = caxpy(jn[n] * dn, h[n], sB);
+            }
+            pm2 = pm1;
+            pm1 = pn;
+            dm1 = dn;
+          }
+          double2 K = c2(0.0);
+          if (chg) K = cmul(kq, sS);
+          if (dip) {
+            double db = (s_n[0][j] * b0 + s_n[1][j] * b1 + s_n[2][j] * b2) * binv;
+            double da = s_n[0][j] * ah[0] + s_n[1][j] * ah[1] + s_n[2][j] * ah[2];
+            double2 vd = caxpy(db, sA, cscale((da - cg * db) * binv, sB));
+            K = cfma(kd, vd, K);
+          }
+#pragma unroll
+          for (int i = 0; i < RB; ++i) acc[i] = cfma(K, s_q[i][j], acc[i]);
+        }
+      }
+      __syncthreads();
+    }
+  }
+  if (warp > 0) {
+#pragma unroll
+    for (int i = 0; i < RB; ++i) s_red[((warp - 1) * 32 + lane) * RB + i] = acc[i];
+  }
+  __syncthreads();
+  if (warp == 0 && active) {
+#pragma unroll
+    for (int i = 0; i < RB; ++i) {
+      if (r0 + i >= nrhs) continue;
+      double2 v = acc[i];
+      for (int w = 1; w < NW; ++w) v = cadd(v, s_red[((w - 1) * 32 + lane) * RB + i]);
+      double2* P = pot_tree + (size_t)(r0 + i) * g.ntargets + t;
+      *P = cadd(*P, v);
+    }
   }
 }
 
@@ -1002,13 +1340,13 @@ k_h3_trans_build(int kind, int p, int rp, int kp, double k, double root_extent, 
     int nu, mu, n, m;
     hq_decode(o, nu, mu);
     hq_decode(i, n, m);
-    const double* Gc = gaunt + ((size_t)o * ncf + i) * nl;
+    const double* Gc = gaunt + (size_t)o * nl * ncf + i;
     int lam = m - mu, lbase = abs(n - nu), jmax = min(n, nu);
     double2 tt = c2(0.0);
     for (int j = 0; j <= jmax; ++j) {
       int l = lbase + 2 * j;
       if (abs(lam) > l) continue;
-      tt = caxpy(Gc[j], Wt[hq(l, lam)], tt);
+      tt = caxpy(Gc[(size_t)j * ncf], Wt[hq(l, lam)], tt);
     }
     // c = i^{nu - n} tt, scaled
     double2 v = cscale(pw[n] * pw[p + 1 + nu], cmul(ipow(nu - n + 4 * p), tt));
@@ -1138,36 +1476,101 @@ cudaError_t h3_launch_p2qbxl(const qbxfmm_geometry& g, HelmCoeffs hc, int q, int
   }
 }
 
-static size_t e2qbxl_smem(int pf, int q)
+template <int Q, int RB>
+static cudaError_t h3_tsqbx_qr(const qbxfmm_geometry& g, HelmCoeffs hc, int nrhs, const double2* s,
+                               double2* pt, int32_t* err, cudaStream_t st)
 {
-  int ncf = (pf + 1) * (pf + 1), ncq = (q + 1) * (q + 1), L = pf + q;
+  size_t sh = (size_t)(NW - 1) * 32 * RB * sizeof(double2);
+  dim3 grid(g.ntsqbx_chunks, (nrhs + RB - 1) / RB);
+  cudaFuncSetAttribute(k_h3_tsqbx<Q, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+  k_h3_tsqbx<Q, RB><<<grid, NT, sh, st>>>(g, hc, nrhs, s, pt, err);
+  return cudaGetLastError();
+}
+
+template <int Q>
+static cudaError_t h3_tsqbx_q(const qbxfmm_geometry& g, HelmCoeffs hc, int nrhs, const double2* s,
+                              double2* pt, int32_t* err, cudaStream_t st)
+{
+  if (nrhs == 1) return h3_tsqbx_qr<Q, 1>(g, hc, nrhs, s, pt, err, st);
+  if (nrhs <= 4) return h3_tsqbx_qr<Q, 4>(g, hc, nrhs, s, pt, err, st);
+  return h3_tsqbx_qr<Q, 16>(g, hc, nrhs, s, pt, err, st);
+}
+
+cudaError_t h3_launch_tsqbx(const qbxfmm_geometry& g, HelmCoeffs hc, int q, int nrhs,
+                            const double2* s, double2* pt, int32_t* err, cudaStream_t st)
+{
+  if (g.ntsqbx_chunks == 0) return cudaSuccess;
+  switch (q) {
+    case 0: return h3_tsqbx_q<0>(g, hc, nrhs, s, pt, err, st);
+    case 1: return h3_tsqbx_q<1>(g, hc, nrhs, s, pt, err, st);
+    case 2: return h3_tsqbx_q<2>(g, hc, nrhs, s, pt, err, st);
+    case 3: return h3_tsqbx_q<3>(g, hc, nrhs, s, pt, err, st);
+    case 4: return h3_tsqbx_q<4>(g, hc, nrhs, s, pt, err, st);
+    case 5: return h3_tsqbx_q<5>(g, hc, nrhs, s, pt, err, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+static size_t e2qbxl_smem(int pf, int q, int rb)
+{
+  int ncf = (pf + 1) * (pf + 1), L = pf + q;
   size_t nrec = (size_t)(L + 1) * (L + 2) / 2;
-  size_t per = (size_t)ncf + (size_t)(L + 1) * (L + 1) + 2 * (L + 2);
-  return (nrec + NW * per + (size_t)NW * 32 * ncq) * sizeof(double2);
+  size_t per = (size_t)ncf + (size_t)(L + 1) * (L + 1) + (L + 2);
+  return (nrec + (size_t)ncf * rb + NW * per) * sizeof(double2);
+}
+
+template <bool FROM_LOCAL, int RB>
+static cudaError_t h3_e2qbxl_rb(const qbxfmm_geometry& g, HelmCoeffs hc, int pf, int q, int nrhs,
+                                const double2* e, const double* gaunt, double2* qe, int32_t* err,
+                                cudaStream_t st)
+{
+  size_t sh = e2qbxl_smem(pf, q, RB);
+  cudaFuncSetAttribute(k_h3_e2qbxl<FROM_LOCAL, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)sh);
+  dim3 grid(g.nqbx_chunks, (nrhs + RB - 1) / RB, H3_E2Q_ZS);
+  k_h3_e2qbxl<FROM_LOCAL, RB><<<grid, NT, sh, st>>>(g, hc, pf, q, nrhs, e, gaunt, qe, err);
+  return cudaGetLastError();
+}
+
+template <bool FROM_LOCAL, int RB>
+static cudaError_t h3_e2qbxl_mma_rb(const qbxfmm_geometry& g, HelmCoeffs hc, int pf, int q,
+                                    int nrhs, const double2* e, const double* gaunt, double2* qe,
+                                    int32_t* err, cudaStream_t st)
+{
+  int ncf = (pf + 1) * (pf + 1), L = pf + q;
+  size_t nrec = (size_t)(L + 1) * (L + 2) / 2;
+  size_t per = (size_t)(L + 1) * (L + 1) + (L + 2) + 4 * (size_t)ncf;
+  size_t sh = (nrec + (size_t)ncf * RB + NW * per) * sizeof(double2);
+  cudaFuncSetAttribute(k_h3_e2qbxl_mma<FROM_LOCAL, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)sh);
+  dim3 grid(g.nqbx_chunks, (nrhs + RB - 1) / RB, H3_MMA_ZS);
+  k_h3_e2qbxl_mma<FROM_LOCAL, RB><<<grid, NT, sh, st>>>(g, hc, pf, q, nrhs, e, gaunt, qe, err);
+  return cudaGetLastError();
+}
+
+template <bool FROM_LOCAL>
+static cudaError_t h3_e2qbxl(const qbxfmm_geometry& g, HelmCoeffs hc, int pf, int q, int nrhs,
+                             const double2* e, const double* gaunt, double2* qe, int32_t* err,
+                             cudaStream_t st)
+{
+  if (g.nqbx_chunks == 0) return cudaSuccess;
+  if (nrhs == 1) return h3_e2qbxl_rb<FROM_LOCAL, 1>(g, hc, pf, q, nrhs, e, gaunt, qe, err, st);
+  if (nrhs <= 8) return h3_e2qbxl_mma_rb<FROM_LOCAL, 8>(g, hc, pf, q, nrhs, e, gaunt, qe, err, st);
+  return h3_e2qbxl_mma_rb<FROM_LOCAL, 16>(g, hc, pf, q, nrhs, e, gaunt, qe, err, st);
 }
 
 cudaError_t h3_launch_m2qbxl(const qbxfmm_geometry& g, HelmCoeffs hc, int pf, int q, int nrhs,
                              const double2* mp, const double* gaunt, double2* qe, int32_t* err,
                              cudaStream_t st)
 {
-  if (g.nqbx_chunks == 0) return cudaSuccess;
-  size_t sh = e2qbxl_smem(pf, q);
-  cudaFuncSetAttribute(k_h3_e2qbxl<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
-  k_h3_e2qbxl<false><<<dim3(g.nqbx_chunks, gridy(nrhs)), NT, sh, st>>>(g, hc, pf, q, nrhs, mp, gaunt,
-                                                                       qe, err);
-  return cudaGetLastError();
+  return h3_e2qbxl<false>(g, hc, pf, q, nrhs, mp, gaunt, qe, err, st);
 }
 
 cudaError_t h3_launch_l2qbxl(const qbxfmm_geometry& g, HelmCoeffs hc, int pf, int q, int nrhs,
                              const double2* lo, const double* gaunt, double2* qe, int32_t* err,
                              cudaStream_t st)
 {
-  if (g.nqbx_chunks == 0) return cudaSuccess;
-  size_t sh = e2qbxl_smem(pf, q);
-  cudaFuncSetAttribute(k_h3_e2qbxl<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
-  k_h3_e2qbxl<true><<<dim3(g.nqbx_chunks, gridy(nrhs)), NT, sh, st>>>(g, hc, pf, q, nrhs, lo, gaunt,
-                                                                      qe, err);
-  return cudaGetLastError();
+  return h3_e2qbxl<true>(g, hc, pf, q, nrhs, lo, gaunt, qe, err, st);
 }
 
 cudaError_t h3_launch_qbxl2p(const qbxfmm_geometry& g, HelmCoeffs hc, int q, int nrhs,

@@ -210,6 +210,115 @@ k_trans_gemm(int ncf, int rp, int kp, int nrhs, int nwm, const double* __restric
   }
 }
 
+// Tiled form for large matrices (rp >= 256): CTA tile of 64 rows x 64 columns
+// (pair x rhs), K streamed in chunks of 32; warp (wm, wn) owns 32 x 32 of the tile
+// as 4 x 4 m8n8 accumulators.  Groups g0 .. g0 + gridDim.z - 1 (blockIdx.z).  The
+// result is added (x scale) into pair_dst's expansion when given (the caller
+// guarantees each destination occurs once per launch), else stored per pair.
+constexpr int GT_M = 64, GT_N = 64, GT_K = 32;
+constexpr int GT_AS = GT_K + 4;      // A row stride (doubles)
+constexpr int GT_BS = GT_N + 8;      // B row stride (doubles)
+
+__global__ void __launch_bounds__(NT)
+k_trans_gemm_tiled(int ncf, int rp, int kp, int nrhs, const double* __restrict__ T, int mat_mod,
+                   const int32_t* __restrict__ group_starts, int g0,
+                   const int32_t* __restrict__ pair_src, const int32_t* __restrict__ pair_dst,
+                   const double2* __restrict__ ein, double2* __restrict__ eout, double scale,
+                   double* __restrict__ cpair, int32_t* err, int nboxes)
+{
+  __shared__ double As[GT_M][GT_AS];
+  __shared__ double Bs[GT_K][GT_BS];
+  __shared__ int s_src[GT_N];
+  int grp = g0 + blockIdx.z;
+  int p0 = group_starts[grp], p1 = group_starts[grp + 1];
+  int ncol = (p1 - p0) * nrhs;
+  int c0 = blockIdx.x * GT_N;
+  int m0 = blockIdx.y * GT_M;
+  if (c0 >= ncol || m0 >= rp) return;
+  int mat = mat_mod > 0 ? (grp % mat_mod) : grp;
+  const double* Tg = T + (size_t)mat * rp * kp;
+  const int R = 2 * ncf;
+  for (int j = threadIdx.x; j < GT_N; j += NT) {
+    int c = c0 + j;
+    int src = -1;
+    if (c < ncol) {
+      src = pair_src[p0 + c / nrhs];
+      if ((unsigned)src >= (unsigned)nboxes) {
+        report(err, QBX_DEVERR_BAD_BOX);
+        src = -1;
+      }
+    }
+    s_src[j] = src;
+  }
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int g = lane >> 2, tq = lane & 3;
+  int wm = warp & 1, wn = warp >> 1;
+  double acc[4][4][2];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+  for (int kc = 0; kc < kp; kc += GT_K) {
+    __syncthreads();
+    for (int e = threadIdx.x; e < GT_M * GT_K; e += NT) {
+      int row = e / GT_K, k = e - row * GT_K;
+      As[row][k] = (m0 + row < rp && kc + k < kp) ? __ldg(Tg + (size_t)(m0 + row) * kp + kc + k) : 0.0;
+    }
+    for (int e = threadIdx.x; e < GT_N * GT_K; e += NT) {
+      int j = e / GT_K, k = e - j * GT_K;
+      int src = s_src[j];
+      double v = 0.0;
+      if (src >= 0 && kc + k < R) {
+        int r = (c0 + j) % nrhs;
+        v = __ldg(reinterpret_cast<const double*>(ein + ((size_t)src * nrhs + r) * ncf) + kc + k);
+      }
+      Bs[k][j] = v;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k0 = 0; k0 < GT_K; k0 += 4) {
+      double a[4], b[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = As[wm * 32 + i * 8 + g][k0 + tq];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) b[j] = Bs[k0 + tq][wn * 32 + j * 8 + g];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+    }
+  }
+  // epilogue: acc[i][j][v] = C[row = m0 + wm*32 + i*8 + g][col = c0 + wn*32 + j*8 + 2 tq + v]
+#pragma unroll
+  for (int j = 0; j < 4; ++j)
+#pragma unroll
+    for (int v = 0; v < 2; ++v) {
+      int c = c0 + wn * 32 + j * 8 + 2 * tq + v;
+      if (c >= ncol) continue;
+      int pr = p0 + c / nrhs, r = c % nrhs;
+      if (pair_dst) {
+        int dst = pair_dst[pr];
+        if ((unsigned)dst >= (unsigned)nboxes) {
+          report(err, QBX_DEVERR_BAD_BOX);
+          continue;
+        }
+        double* y = reinterpret_cast<double*>(eout + ((size_t)dst * nrhs + r) * ncf);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          int row = m0 + wm * 32 + i * 8 + g;
+          if (row < R) y[row] += scale * acc[i][j][v];
+        }
+      } else {
+        double* y = cpair + ((size_t)pr * nrhs + r) * rp;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          int row = m0 + wm * 32 + i * 8 + g;
+          if (row < rp) y[row] = acc[i][j][v];
+        }
+      }
+    }
+}
+
 // out box o (o = boxes[obase + blockIdx.x]): eout[o][r] += scale(o) sum_{pairs} cpair[pair][r]
 // scale(o) = 1 / width(level(o)) when div_by_width, else 1.
 __global__ void __launch_bounds__(NT)
@@ -383,6 +492,71 @@ cudaError_t launch_l2l_gemm(const qbxfmm_geometry& g, const TransHost& th, const
     cudaError_t e = gemm_launch(g, c, nrhs, T, c.l2l_base, c.m2m_mat_mod, g.l2l_group_starts, g0,
                                 nch, maxp * nrhs, g.l2l_pair_src, g.l2l_pair_dst, lo, lo, 1.0,
                                 nullptr, err, st);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+static cudaError_t gemm_tiled_launch(const qbxfmm_geometry& g, const TransCfg& c, int nrhs,
+                                     const double* T, size_t mat_base, int mat_mod,
+                                     const int32_t* group_starts_dev, int g0, int ngroups,
+                                     int maxcols, const int32_t* pair_src, const int32_t* pair_dst,
+                                     const double2* ein, double2* eout, double scale,
+                                     double* cpair, int32_t* err, cudaStream_t st)
+{
+  if (ngroups <= 0 || maxcols <= 0) return cudaSuccess;
+  dim3 grid((maxcols + GT_N - 1) / GT_N, (c.rp + GT_M - 1) / GT_M, ngroups);
+  k_trans_gemm_tiled<<<grid, NT, 0, st>>>(c.ncf, c.rp, c.kp, nrhs, T + mat_base * (size_t)c.rp * c.kp,
+                                          mat_mod, group_starts_dev, g0, pair_src, pair_dst, ein,
+                                          eout, scale, cpair, err, g.nboxes);
+  return cudaGetLastError();
+}
+
+// M2L without pair scratch: one launch per run of consecutive classes whose targets
+// are distinct (waves[w] .. waves[w+1]), adding into the targets' locals directly.
+cudaError_t launch_m2l_direct(const qbxfmm_geometry& g, const TransHost& th, const TransCfg& c,
+                              const int32_t* waves, int nwaves, int nrhs, const double* T,
+                              const double2* mp, double2* lo, int32_t* err, cudaStream_t st)
+{
+  for (int w = 0; w < nwaves; ++w) {
+    cudaError_t e = gemm_tiled_launch(g, c, nrhs, T, 0, 0, g.m2l_class_starts, waves[w],
+                                      waves[w + 1] - waves[w], th.m2l_max_pairs * nrhs,
+                                      g.m2l_pair_src, g.m2l_pair_dst, mp, lo, 1.0, nullptr, err, st);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+// M2M without pair scratch: one launch per (parent level, child position) group,
+// whose parents are distinct.
+cudaError_t launch_m2m_direct(const qbxfmm_geometry& g, const TransHost& th, const TransCfg& c,
+                              int nrhs, const double* T, double2* mp, int32_t* err, cudaStream_t st)
+{
+  const int nch = 8;
+  for (int lev = g.nlevels - 2; lev >= 0; --lev) {
+    int maxp = th.m2m_level_max_group[lev];
+    if (maxp == 0) continue;
+    for (int ci = 0; ci < nch; ++ci) {
+      cudaError_t e = gemm_tiled_launch(g, c, nrhs, T, c.m2m_base, c.m2m_mat_mod, g.m2m_group_starts,
+                                        lev * nch + ci, 1, maxp * nrhs, g.m2m_pair_src,
+                                        g.m2m_pair_dst, mp, mp, 1.0, nullptr, err, st);
+      if (e != cudaSuccess) return e;
+    }
+  }
+  return cudaSuccess;
+}
+
+// L2L on the tiled kernel (children are distinct across a level's eight groups)
+cudaError_t launch_l2l_direct(const qbxfmm_geometry& g, const TransHost& th, const TransCfg& c,
+                              int nrhs, const double* T, double2* lo, int32_t* err, cudaStream_t st)
+{
+  const int nch = 8;
+  for (int lev = 1; lev < g.nlevels; ++lev) {
+    int maxp = th.l2l_level_max_group[lev];
+    if (maxp == 0) continue;
+    cudaError_t e = gemm_tiled_launch(g, c, nrhs, T, c.l2l_base, c.m2m_mat_mod, g.l2l_group_starts,
+                                      lev * nch, nch, maxp * nrhs, g.l2l_pair_src, g.l2l_pair_dst,
+                                      lo, lo, 1.0, nullptr, err, st);
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;

@@ -141,11 +141,13 @@ def test_drive_fmm_and_apply_match_checker(name):
     ap.check_error_word()
 
 
-@pytest.mark.parametrize("name", ["2d-S", "2d-D", "3d-D-small", "3d-S-small", "2d-D-nrhs3"])
+@pytest.mark.parametrize("name", ["2d-S", "2d-D", "3d-D-small", "3d-S-small", "2d-D-nrhs3",
+                                  "h3d-CF-small", "h3d-S-small", "h3d-D-small"])
 def test_target_specific_mode_matches_checker(name):
     """With target-specific QBX the list-1 near field is evaluated per target; the
     truncation is the same, so the apply equals the checker's (expansion-based) one."""
     wl, w, o = wrangler_for(name)
+    TOL = tol_for(wl)
     ref = o.apply(wl.tree_strengths())
     ap = QBXApply(wl.geometry(), wl.spec, wl.qbx_order, wl.fmm_order, nrhs=wl.nrhs,
                   device_geometry=w.dgeo, target_specific_qbx=True)
@@ -223,6 +225,54 @@ def test_near_field_matches_reference_tsqbx_golden(op):
         assert int(err.item()) == 0
         assert relerr(got[mask], z[f"pot_{op}_{q}"][mask]) < TOL, (op, q)
         assert relerr(got2[mask], z[f"pot_{op}_{q}"][mask]) < TOL, ("tsqbx", op, q)
+
+
+@pytest.mark.parametrize("op", ["S", "D"])
+def test_helmholtz3d_near_field_matches_reference_tsqbx_golden(op):
+    """3D Helmholtz: P2QBXL + QBXL2P and the target-specific kernel on the GPU against
+    the reference TSQBX module's output (k = 2.5, complex strengths)."""
+    z = golden_tsqbx("helmholtz3d")
+    scalars, arrays = golden_geometry(z)
+    arrays["m2m_group_starts"] = np.zeros(9, np.int32)
+    arrays["l2l_group_starts"] = np.zeros(9, np.int32)
+    darr = {k: dev(v) for k, v in arrays.items()}
+    g = abi.make_geometry_struct(scalars, darr, lambda t: t.data_ptr())
+    lv = dev(np.array([0, 0], np.int32))
+    g.level_start_source_parent_box_nrs = ctypes.cast(ctypes.c_void_p(lv.data_ptr()),
+                                                      ctypes.POINTER(ctypes.c_int32))
+    g.level_start_ttp_box_nrs = g.level_start_source_parent_box_nrs
+    s = dev(z["strengths"][None, :])
+    mask = np.zeros(scalars["ntargets"], bool)
+    mask[z["center_to_targets_lists"]] = True
+    L = native.lib()
+    for q in z["orders"]:
+        q = int(q)
+        k = abi.make_kernel_struct(family=abi.QBXFMM_HELMHOLTZ, dim=3, qbx_order=q, fmm_order=6,
+                                   k=float(z["k"]), charge_coeff=float(op == "S"),
+                                   dipole_coeff=float(op == "D"))
+        h = ctypes.c_void_p()
+        native.check("plan", L.qbxfmm_plan_create(ctypes.byref(k), ctypes.byref(g),
+                                                  ctypes.byref(h)))
+        nc = abi.ncoeff(abi.QBXFMM_HELMHOLTZ, 3, q)
+        qe = torch.zeros(scalars["ncenters"], 1, nc, dtype=torch.complex128, device="cuda")
+        pt = torch.zeros(1, scalars["ntargets"], dtype=torch.complex128, device="cuda")
+        err = torch.zeros(1, dtype=torch.int32, device="cuda")
+        errp = ctypes.cast(ctypes.c_void_p(err.data_ptr()), ctypes.POINTER(ctypes.c_int32))
+        st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        native.call("qbxfmm_form_global_qbx_locals", h, ctypes.c_void_p(s.data_ptr()),
+                    ctypes.c_void_p(qe.data_ptr()), errp, st)
+        native.call("qbxfmm_eval_qbx_expansions", h, ctypes.c_void_p(qe.data_ptr()),
+                    ctypes.c_void_p(pt.data_ptr()), st)
+        pt2 = torch.zeros_like(pt)
+        native.call("qbxfmm_eval_target_specific_qbx_locals", h, ctypes.c_void_p(s.data_ptr()),
+                    ctypes.c_void_p(pt2.data_ptr()), errp, st)
+        L.qbxfmm_plan_destroy(h)
+        got = host(pt)[0]
+        got2 = host(pt2)[0]
+        assert int(err.item()) == 0
+        ref = z[f"pot_{op}_{q}"]
+        assert relerr(got[mask], ref[mask]) < 1e-12, (op, q)
+        assert relerr(got2[mask], ref[mask]) < 1e-12, ("tsqbx", op, q)
 
 
 def test_bad_list_entry_reports_instead_of_faulting():
