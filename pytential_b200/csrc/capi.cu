@@ -191,8 +191,6 @@ int qbxfmm_plan_create(const qbxfmm_kernel* kernel, const qbxfmm_geometry* geome
     return fail(QBXFMM_ERR_UNSUPPORTED, "fmm_order must be in [1, 20]");
   if (k.nrhs < 1) return fail(QBXFMM_ERR_ARG, "nrhs must be >= 1");
   if (k.precision != 0) return fail(QBXFMM_ERR_UNSUPPORTED, "only precision 0 (FP64)");
-  if (k.target_specific_qbx && k.family != QBXFMM_LAPLACE && k.dim != 3)
-    return fail(QBXFMM_ERR_UNSUPPORTED, "target-specific QBX is built for Laplace and 3D Helmholtz");
   if (k.family == QBXFMM_HELMHOLTZ && k.dim == 3) {
     if (k.qbx_order > 5 || k.qbx_order > k.fmm_order)
       return fail(QBXFMM_ERR_UNSUPPORTED, "3D Helmholtz: qbx_order must be <= min(5, fmm_order)");
@@ -575,8 +573,12 @@ int qbxfmm_eval_target_specific_qbx_locals(const qbxfmm_plan* p, const void* str
             "eval_target_specific_qbx_locals");
     return QBXFMM_OK;
   }
-  if (p->helm)
-    return fail(QBXFMM_ERR_UNSUPPORTED, "target-specific QBX is built for Laplace and 3D Helmholtz");
+  if (p->helm) {
+    QBX_TRY(h2_launch_tsqbx(p->geo, p->hc, p->kern.qbx_order, p->kern.nrhs, (const double2*)strengths,
+                            (double2*)pot_tree, error_word, S(stream)),
+            "eval_target_specific_qbx_locals");
+    return QBXFMM_OK;
+  }
   QBX_TRY(launch_tsqbx(p->geo, p->sc, p->kern.qbx_order, p->kern.nrhs, (const double*)strengths,
                        (double*)pot_tree, error_word, S(stream)),
           "eval_target_specific_qbx_locals");

@@ -106,6 +106,8 @@ cudaError_t h2_launch_l2qbxl(const qbxfmm_geometry& g, HelmCoeffs hc, int pf, in
                              const double2* lo, double2* qe, int32_t* err, cudaStream_t st);
 cudaError_t h2_launch_qbxl2p(const qbxfmm_geometry& g, HelmCoeffs hc, int q, int nrhs,
                              const double2* qe, double2* pt, cudaStream_t st);
+cudaError_t h2_launch_tsqbx(const qbxfmm_geometry& g, HelmCoeffs hc, int q, int nrhs,
+                            const double2* s, double2* pt, int32_t* err, cudaStream_t st);
 cudaError_t h2_launch_assemble(const qbxfmm_geometry& g, int nrhs, const double2* pot_nonqbx,
                                const double2* pot_tree, double2* out, cudaStream_t st);
 

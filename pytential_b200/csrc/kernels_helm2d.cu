@@ -580,6 +580,156 @@ k_h2_p2qbxl(qbxfmm_geometry g, HelmCoeffs hc, int nrhs, const double2* __restric
   }
 }
 
+// Target-specific near field (eval_target_specific_qbx_locals, pytential/qbx/fmm.py:391-394)
+// for the H2D expansion: per (target t, its center c, list-1 source y) the order-Q
+// QBX expansion is evaluated without forming it,
+//   K = sum_{|m|<=Q} Z_m(t - c) (cq Hb_m(y - c) + (k/2) cd (conj(nu) Hb_{m-1} - nu Hb_{m+1})),
+// Z_m = J_m e^{i m th}, the same series as P2QBXL followed by QBXL2P.  H_m(k|y - c|)
+// by the upward recurrence from H_0, H_1 (dominant solution).  K is computed once per
+// pair and applied to RB densities (lane = target; warps split each source tile).
+template <int Q, int RB>
+__global__ void __launch_bounds__(NT)
+k_h2_tsqbx(qbxfmm_geometry g, HelmCoeffs hc, int nrhs, const double2* __restrict__ strengths,
+           double2* __restrict__ pot_tree, int32_t* err)
+{
+  __shared__ double s_y[2][NT], s_n[2][NT];
+  __shared__ double2 s_q[RB][NT];
+  __shared__ int s_pref[MAXB + 1], s_start[MAXB];
+  extern __shared__ double2 s_red[];   // [NW-1][32][RB]
+  int chunk = blockIdx.x;
+  int r0 = blockIdx.y * RB;
+  int itb = g.tsqbx_chunk_target_box[chunk];
+  int i0 = g.tsqbx_chunk_start[chunk];
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  bool active = lane < g.tsqbx_chunk_count[chunk];
+  int t = active ? g.tsqbx_targets[i0 + lane] : 0;
+  int ctr = active ? g.tsqbx_centers[i0 + lane] : 0;
+  if ((unsigned)ctr >= (unsigned)g.ncenters || (unsigned)t >= (unsigned)g.ntargets) {
+    report(err, QBX_DEVERR_BAD_CENTER);
+    active = false;
+    t = ctr = 0;
+  }
+  double cc[2], x[2];
+  load_point<2>(g.centers, g.ncenters, ctr, cc);
+  load_point<2>(g.targets, g.ntargets, t, x);
+  // Z_m(t - c), m in [-Q, Q], at Zt[Q + m]
+  double2 Zt[2 * Q + 1];
+  {
+    double ax = x[0] - cc[0], ay = x[1] - cc[1];
+    double alen = sqrt(ax * ax + ay * ay);
+    double J[Q + 1];
+    if (alen > 0.0) {
+      double Yd[1];
+      bessel_jy(Q, hc.k * alen, J, Yd, false);
+    } else {
+#pragma unroll
+      for (int m = 0; m <= Q; ++m) J[m] = (m == 0) ? 1.0 : 0.0;
+    }
+    double2 e1 = alen > 0.0 ? c2(ax / alen, ay / alen) : c2(1.0);
+    double2 e = c2(1.0);
+#pragma unroll
+    for (int m = 0; m <= Q; ++m) {
+      Zt[Q + m] = cscale(J[m], e);
+      double2 w = cscale(J[m], cconj(e));
+      Zt[Q - m] = (m & 1) ? cneg(w) : w;
+      e = cmul(e, e1);
+    }
+  }
+  const bool chg = hc.cq.x != 0.0 || hc.cq.y != 0.0;
+  const bool dip = hc.cd.x != 0.0 || hc.cd.y != 0.0;
+  const double2 kd = cscale(0.5 * hc.k, hc.cd);
+  double2 acc[RB];
+#pragma unroll
+  for (int i = 0; i < RB; ++i) acc[i] = c2(0.0);
+  int l0 = g.list1_starts[itb], l1 = g.list1_starts[itb + 1];
+  for (int gb = l0; gb < l1; gb += MAXB) {
+    int nb = min(MAXB, l1 - gb);
+    __syncthreads();
+    h_list_prefix(g, g.list1_lists, gb, nb, s_pref, s_start, err);
+    __syncthreads();
+    int total = s_pref[nb];
+    for (int base = 0; base < total; base += NT) {
+      int v = base + threadIdx.x;
+      if (v < total) {
+        int s = h_stream_source(v, nb, s_pref, s_start);
+        double y[2], nv[2] = {0, 0};
+        load_point<2>(g.sources, g.nsources, s, y);
+        if (dip) load_point<2>(g.source_normals, g.nsources, s, nv);
+        s_y[0][threadIdx.x] = y[0];
+        s_y[1][threadIdx.x] = y[1];
+        s_n[0][threadIdx.x] = nv[0];
+        s_n[1][threadIdx.x] = nv[1];
+#pragma unroll
+        for (int i = 0; i < RB; ++i)
+          s_q[i][threadIdx.x] = (r0 + i < nrhs) ? strengths[(size_t)(r0 + i) * g.nsources + s] : c2(0.0);
+      }
+      __syncthreads();
+      int jbeg = warp * 32, jend = min(jbeg + 32, total - base);
+      if (active) {
+        for (int j = jbeg; j < jend; ++j) {
+          double ux = s_y[0][j] - cc[0], uy = s_y[1][j] - cc[1];
+          double b2 = ux * ux + uy * uy;
+          if (b2 == 0.0) continue;
+          double binv = rsqrt(b2);
+          double xx = hc.k * b2 * binv, xinv = 1.0 / xx;
+          double2 H[Q + 2];
+          H[0] = c2(j0(xx), y0(xx));
+          H[1] = c2(j1(xx), y1(xx));
+#pragma unroll
+          for (int m = 1; m <= Q; ++m)
+            H[m + 1] = c2(2.0 * m * xinv * H[m].x - H[m - 1].x, 2.0 * m * xinv * H[m].y - H[m - 1].y);
+          // Hb_m for m in [-(Q+1), Q+1] at Hb[Q + 1 + m]
+          double2 Hb[2 * Q + 3];
+          double2 e1 = c2(ux * binv, -uy * binv);     // e^{-i th}
+          double2 e = c2(1.0);
+#pragma unroll
+          for (int m = 0; m <= Q + 1; ++m) {
+            Hb[Q + 1 + m] = cmul(H[m], e);
+            double2 w = cmul(H[m], cconj(e));
+            Hb[Q + 1 - m] = (m & 1) ? cneg(w) : w;
+            e = cmul(e, e1);
+          }
+          double2 K = c2(0.0);
+          if (chg) {
+            double2 s0 = c2(0.0);
+#pragma unroll
+            for (int m = -Q; m <= Q; ++m) s0 = cfma(Zt[Q + m], Hb[Q + 1 + m], s0);
+            K = cmul(hc.cq, s0);
+          }
+          if (dip) {
+            double2 sm = c2(0.0), sp = c2(0.0);
+#pragma unroll
+            for (int m = -Q; m <= Q; ++m) {
+              sm = cfma(Zt[Q + m], Hb[Q + m], sm);
+              sp = cfma(Zt[Q + m], Hb[Q + 2 + m], sp);
+            }
+            double2 nu = c2(s_n[0][j], s_n[1][j]);
+            K = cfma(kd, csub(cmul(cconj(nu), sm), cmul(nu, sp)), K);
+          }
+#pragma unroll
+          for (int i = 0; i < RB; ++i) acc[i] = cfma(K, s_q[i][j], acc[i]);
+        }
+      }
+      __syncthreads();
+    }
+  }
+  if (warp > 0) {
+#pragma unroll
+    for (int i = 0; i < RB; ++i) s_red[((warp - 1) * 32 + lane) * RB + i] = acc[i];
+  }
+  __syncthreads();
+  if (warp == 0 && active) {
+#pragma unroll
+    for (int i = 0; i < RB; ++i) {
+      if (r0 + i >= nrhs) continue;
+      double2 vv = acc[i];
+      for (int w = 1; w < NW; ++w) vv = cadd(vv, s_red[((w - 1) * 32 + lane) * RB + i]);
+      double2* P = pot_tree + (size_t)(r0 + i) * g.ntargets + t;
+      *P = cadd(*P, vv);
+    }
+  }
+}
+
 // M2QBXL (list 3) and L2QBXL (own target box): one thread per center.
 template <int Q, bool FROM_LOCAL>
 __global__ void __launch_bounds__(NT)
@@ -874,6 +1024,33 @@ cudaError_t h2_launch_qbxl2p(const qbxfmm_geometry& g, HelmCoeffs hc, int q, int
 {
   if (g.nglobal_qbx_centers == 0) return cudaSuccess;
   QBX_H2_DISPATCH(h2_qbxl2p_q, q, g, hc, nrhs, qe, pt, st)
+}
+
+template <int Q, int RB>
+static cudaError_t h2_tsqbx_qr(const qbxfmm_geometry& g, HelmCoeffs hc, int nrhs, const double2* s,
+                               double2* pt, int32_t* err, cudaStream_t st)
+{
+  size_t sh = (size_t)(NW - 1) * 32 * RB * sizeof(double2);
+  cudaFuncSetAttribute(k_h2_tsqbx<Q, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+  dim3 grid(g.ntsqbx_chunks, (nrhs + RB - 1) / RB);
+  k_h2_tsqbx<Q, RB><<<grid, NT, sh, st>>>(g, hc, nrhs, s, pt, err);
+  return cudaGetLastError();
+}
+
+template <int Q>
+static cudaError_t h2_tsqbx_q(const qbxfmm_geometry& g, HelmCoeffs hc, int nrhs, const double2* s,
+                              double2* pt, int32_t* err, cudaStream_t st)
+{
+  if (nrhs == 1) return h2_tsqbx_qr<Q, 1>(g, hc, nrhs, s, pt, err, st);
+  if (nrhs <= 4) return h2_tsqbx_qr<Q, 4>(g, hc, nrhs, s, pt, err, st);
+  return h2_tsqbx_qr<Q, 16>(g, hc, nrhs, s, pt, err, st);
+}
+
+cudaError_t h2_launch_tsqbx(const qbxfmm_geometry& g, HelmCoeffs hc, int q, int nrhs,
+                            const double2* s, double2* pt, int32_t* err, cudaStream_t st)
+{
+  if (g.ntsqbx_chunks == 0) return cudaSuccess;
+  QBX_H2_DISPATCH(h2_tsqbx_q, q, g, hc, nrhs, s, pt, err, st)
 }
 
 cudaError_t h2_launch_assemble(const qbxfmm_geometry& g, int nrhs, const double2* pot_nonqbx,
