@@ -30,6 +30,8 @@ struct qbxfmm_plan {
   TransHost th;
   TransCfg tc;
   bool h3;                                 // 3D Helmholtz
+  bool mixed;                              // FP32 far field (3D Laplace)
+  bool tf32_ok;                            // split-TF32 translation matrices in use
   std::vector<double> h3gaunt;             // Gaunt table, [(nu,mu)][j][(n,m)]
   std::vector<int32_t> m2l_waves;          // runs of M2L classes with one offset (3D Helmholtz)
   // 3D Helmholtz: translation buffer and pair scratch registered by
@@ -190,7 +192,10 @@ int qbxfmm_plan_create(const qbxfmm_kernel* kernel, const qbxfmm_geometry* geome
   if (k.fmm_order < 1 || k.fmm_order > 20 || (k.family == QBXFMM_HELMHOLTZ && k.qbx_order + k.fmm_order > 28))
     return fail(QBXFMM_ERR_UNSUPPORTED, "fmm_order must be in [1, 20]");
   if (k.nrhs < 1) return fail(QBXFMM_ERR_ARG, "nrhs must be >= 1");
-  if (k.precision != 0) return fail(QBXFMM_ERR_UNSUPPORTED, "only precision 0 (FP64)");
+  if (k.precision != 0 && k.precision != 1)
+    return fail(QBXFMM_ERR_ARG, "precision must be 0 (FP64) or 1 (mixed)");
+  if (k.precision == 1 && !(k.family == QBXFMM_LAPLACE && k.dim == 3))
+    return fail(QBXFMM_ERR_UNSUPPORTED, "the mixed-precision form is built for 3D Laplace");
   if (k.family == QBXFMM_HELMHOLTZ && k.dim == 3) {
     if (k.qbx_order > 5 || k.qbx_order > k.fmm_order)
       return fail(QBXFMM_ERR_UNSUPPORTED, "3D Helmholtz: qbx_order must be <= min(5, fmm_order)");
@@ -225,10 +230,12 @@ int qbxfmm_plan_create(const qbxfmm_kernel* kernel, const qbxfmm_geometry* geome
     e = cudaMemcpy(p->lvl_ttp.data(), g.level_start_ttp_box_nrs, sizeof(int32_t) * (g.nlevels + 1),
                    cudaMemcpyDeviceToHost);
   p->h3 = p->helm && k.dim == 3;
+  p->mixed = k.precision == 1;
   if (k.dim == 3)
     p->tc = p->h3 ? trans_cfg_helm3(k.fmm_order, g.m2l_nclasses, g.nlevels)
                   : trans_cfg_laplace3(k.fmm_order, g.m2l_nclasses);
   p->trans_ok = k.dim == 3 && trans_supported(p->tc) && g.nlevels <= 64;
+  p->tf32_ok = p->mixed && p->trans_ok && tf32_supported(p->tc);
   if (p->h3 && !p->trans_ok) {
     delete p;
     return fail(QBXFMM_ERR_UNSUPPORTED, "3D Helmholtz: translation matrices unsupported for this order");
@@ -312,6 +319,10 @@ int qbxfmm_form_multipoles(const qbxfmm_plan* p, const void* strengths, void* mp
   if (p->helm)
     QBX_TRY(h2_launch_p2m(p->geo, p->hc, p->kern.fmm_order, p->kern.nrhs,
                           (const double2*)strengths, (double2*)mpoles, nullptr, S(stream)),
+            "form_multipoles");
+  else if (p->mixed)
+    QBX_TRY(launch_p2m_mixed(p->geo, p->sc, p->kern.fmm_order, p->kern.nrhs,
+                             (const double*)strengths, (double2*)mpoles, S(stream)),
             "form_multipoles");
   else
     QBX_TRY(launch_p2m(p->geo, p->sc, p->kern.fmm_order, p->kern.nrhs, (const double*)strengths,
@@ -424,6 +435,10 @@ int qbxfmm_form_locals(const qbxfmm_plan* p, const void* strengths, void* locals
     QBX_TRY(h2_launch_p2l(p->geo, p->hc, p->kern.fmm_order, p->kern.nrhs,
                           (const double2*)strengths, (double2*)locals, error_word, S(stream)),
             "form_locals");
+  else if (p->mixed)
+    QBX_TRY(launch_p2l_mixed(p->geo, p->sc, p->kern.fmm_order, p->kern.nrhs,
+                             (const double*)strengths, (double2*)locals, error_word, S(stream)),
+            "form_locals");
   else
     QBX_TRY(launch_p2l(p->geo, p->sc, p->kern.fmm_order, p->kern.nrhs, (const double*)strengths,
                        (double2*)locals, error_word, S(stream)),
@@ -510,6 +525,10 @@ int qbxfmm_translate_box_multipoles_to_qbx_local(const qbxfmm_plan* p, const voi
   if (p->helm)
     QBX_TRY(h2_launch_m2qbxl(p->geo, p->hc, p->kern.fmm_order, p->kern.qbx_order, p->kern.nrhs,
                              (const double2*)mpoles, (double2*)qbx_exps, error_word, S(stream)),
+            "translate_box_multipoles_to_qbx_local");
+  else if (p->mixed)
+    QBX_TRY(launch_m2qbxl_mixed(p->geo, p->kern.fmm_order, p->kern.qbx_order, p->kern.nrhs,
+                                (const double2*)mpoles, (double2*)qbx_exps, error_word, S(stream)),
             "translate_box_multipoles_to_qbx_local");
   else
     QBX_TRY(launch_m2qbxl(p->geo, p->kern.fmm_order, p->kern.qbx_order, p->kern.nrhs,
@@ -625,7 +644,8 @@ int qbxfmm_workspace_sizes(const qbxfmm_plan* p, size_t* sizes6 /* 8 entries */)
                                cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return cuda_check(e, "workspace_sizes");
     npairs = std::max(npairs, g.m2m_npairs);
-    sizes6[6] = trans_matrix_bytes(p->tc) + p->h3gaunt.size() * sizeof(double);
+    sizes6[6] = trans_matrix_bytes(p->tc) + p->h3gaunt.size() * sizeof(double) +
+                (p->tf32_ok ? tf32_matrix_bytes(p->tc) : 0);
     sizes6[7] = p->h3 ? 0 : trans_scratch_bytes(p->tc, npairs, p->kern.nrhs);
   } else {
     sizes6[6] = sizes6[7] = 0;
@@ -654,6 +674,12 @@ int qbxfmm_precompute_translations(const qbxfmm_plan* p, const qbxfmm_workspace*
   if (!p->trans_ok || !ws->translations) return QBXFMM_OK;
   QBX_TRY(launch_trans_build(p->geo, p->tc, (double*)ws->translations, S(stream)),
           "precompute_translations");
+  if (p->tf32_ok)
+    QBX_TRY(launch_trans_split_tf32(p->tc, (const double*)ws->translations,
+                                    reinterpret_cast<uint32_t*>((double*)ws->translations +
+                                                                trans_matrix_bytes(p->tc) / sizeof(double)),
+                                    S(stream)),
+            "precompute_translations (TF32 planes)");
   return QBXFMM_OK;
 }
 
@@ -685,7 +711,15 @@ int qbxfmm_apply(const qbxfmm_plan* p, const qbxfmm_upsample* up, const qbxfmm_w
   // drive_fmm order (fmm.py:436-588)
   if ((rc = qbxfmm_form_strengths(p, up, density, ws->strengths, stream))) return rc;
   if ((rc = qbxfmm_form_multipoles(p, ws->strengths, ws->mpoles, stream))) return rc;
-  if (gemm)
+  const uint32_t* T32 = (gemm && p->tf32_ok)
+                            ? reinterpret_cast<const uint32_t*>((const double*)ws->translations +
+                                                                trans_matrix_bytes(p->tc) / sizeof(double))
+                            : nullptr;
+  if (T32)
+    QBX_TRY(launch_m2m_gemm_mixed(p->geo, p->th, p->tc, p->kern.nrhs, T32, (double2*)ws->mpoles,
+                                  (double*)ws->pair_scratch, ws->error_word, S(stream)),
+            "coarsen_multipoles (split TF32)");
+  else if (gemm)
     QBX_TRY(launch_m2m_gemm(p->geo, p->th, p->tc, p->kern.nrhs,
                             (const double*)ws->translations, (double2*)ws->mpoles,
                             (double*)ws->pair_scratch, ws->error_word, S(stream)),
@@ -693,7 +727,12 @@ int qbxfmm_apply(const qbxfmm_plan* p, const qbxfmm_upsample* up, const qbxfmm_w
   else if ((rc = qbxfmm_coarsen_multipoles(p, ws->mpoles, stream)))
     return rc;
   if ((rc = qbxfmm_eval_direct(p, ws->strengths, ws->pot_nonqbx, ws->error_word, stream))) return rc;
-  if (gemm)
+  if (T32)
+    QBX_TRY(launch_m2l_gemm_mixed(p->geo, p->th, p->tc, p->kern.nrhs, T32, (const double2*)ws->mpoles,
+                                  (double2*)ws->locals, (double*)ws->pair_scratch, ws->error_word,
+                                  S(stream)),
+            "multipole_to_local (split TF32)");
+  else if (gemm)
     QBX_TRY(launch_m2l_gemm(p->geo, p->th, p->tc, p->kern.nrhs,
                             (const double*)ws->translations, (const double2*)ws->mpoles,
                             (double2*)ws->locals, (double*)ws->pair_scratch, ws->error_word,
@@ -703,7 +742,11 @@ int qbxfmm_apply(const qbxfmm_plan* p, const qbxfmm_upsample* up, const qbxfmm_w
     return rc;
   if ((rc = qbxfmm_eval_multipoles(p, ws->mpoles, ws->pot_nonqbx, ws->error_word, stream))) return rc;
   if ((rc = qbxfmm_form_locals(p, ws->strengths, ws->locals, ws->error_word, stream))) return rc;
-  if (gemm)
+  if (T32)
+    QBX_TRY(launch_l2l_gemm_mixed(p->geo, p->th, p->tc, p->kern.nrhs, T32, (double2*)ws->locals,
+                                  ws->error_word, S(stream)),
+            "refine_locals (split TF32)");
+  else if (gemm)
     QBX_TRY(launch_l2l_gemm(p->geo, p->th, p->tc, p->kern.nrhs,
                             (const double*)ws->translations, (double2*)ws->locals, ws->error_word,
                             S(stream)),

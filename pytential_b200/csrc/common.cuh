@@ -46,6 +46,29 @@ QBX_HD double2 caxpy(double s, double2 a, double2 acc)
 
 // }}}
 
+// {{{ complex float as float2 (mixed-precision far field)
+
+QBX_HD float2 f2(float re, float im = 0.0f) { return make_float2(re, im); }
+QBX_HD float2 fadd(float2 a, float2 b) { return f2(a.x + b.x, a.y + b.y); }
+QBX_HD float2 fsub(float2 a, float2 b) { return f2(a.x - b.x, a.y - b.y); }
+QBX_HD float2 fscale(float s, float2 a) { return f2(s * a.x, s * a.y); }
+QBX_HD float2 fconj(float2 a) { return f2(a.x, -a.y); }
+QBX_HD float2 fmul(float2 a, float2 b)
+{
+  return f2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+// acc + a * b
+QBX_HD float2 ffma(float2 a, float2 b, float2 acc)
+{
+  return f2(fmaf(a.x, b.x, fmaf(-a.y, b.y, acc.x)), fmaf(a.x, b.y, fmaf(a.y, b.x, acc.y)));
+}
+// acc + s * a  (s real)
+QBX_HD float2 faxpy(float s, float2 a, float2 acc) { return f2(fmaf(s, a.x, acc.x), fmaf(s, a.y, acc.y)); }
+QBX_HD float2 tof(double2 a) { return f2((float)a.x, (float)a.y); }
+QBX_HD double2 tod(float2 a) { return c2((double)a.x, (double)a.y); }
+
+// }}}
+
 QBX_HD int idx3(int n, int m) { return n * (n + 1) / 2 + m; }
 
 // reciprocals of small integers (c_rcp[i] = 1/i, c_rcp[0] = 0): keeps float64

@@ -39,6 +39,32 @@ cudaError_t launch_m2m_gemm(const qbxfmm_geometry& g, const TransHost& th, const
                             cudaStream_t st);
 cudaError_t launch_l2l_gemm(const qbxfmm_geometry& g, const TransHost& th, const TransCfg& c,
                             int nrhs, const double* T, double2* lo, int32_t* err, cudaStream_t st);
+cudaError_t launch_trans_reduce_m2l(const qbxfmm_geometry& g, const TransCfg& c, int nrhs,
+                                    const double* cpair, double2* lo, cudaStream_t st);
+cudaError_t launch_trans_reduce_m2m(const qbxfmm_geometry& g, const TransHost& th, const TransCfg& c,
+                                    int lev, int nrhs, const double* cpair, double2* mp,
+                                    cudaStream_t st);
+// mixed precision (3D Laplace): FP32 far field, split-TF32 translations
+cudaError_t launch_p2m_mixed(const qbxfmm_geometry& g, SourceCoeffs sc, int p, int nrhs,
+                             const double* s, double2* mp, cudaStream_t st);
+cudaError_t launch_p2l_mixed(const qbxfmm_geometry& g, SourceCoeffs sc, int p, int nrhs,
+                             const double* s, double2* lo, int32_t* err, cudaStream_t st);
+cudaError_t launch_m2qbxl_mixed(const qbxfmm_geometry& g, int pf, int q, int nrhs,
+                                const double2* mp, double2* qe, int32_t* err, cudaStream_t st);
+void tf32_dims(const TransCfg& c, int& rp16, int& kp8);
+bool tf32_supported(const TransCfg& c);
+size_t tf32_matrix_bytes(const TransCfg& c);
+cudaError_t launch_trans_split_tf32(const TransCfg& c, const double* T, uint32_t* T32,
+                                    cudaStream_t st);
+cudaError_t launch_m2l_gemm_mixed(const qbxfmm_geometry& g, const TransHost& th, const TransCfg& c,
+                                  int nrhs, const uint32_t* T32, const double2* mp, double2* lo,
+                                  double* cpair, int32_t* err, cudaStream_t st);
+cudaError_t launch_m2m_gemm_mixed(const qbxfmm_geometry& g, const TransHost& th, const TransCfg& c,
+                                  int nrhs, const uint32_t* T32, double2* mp, double* cpair,
+                                  int32_t* err, cudaStream_t st);
+cudaError_t launch_l2l_gemm_mixed(const qbxfmm_geometry& g, const TransHost& th, const TransCfg& c,
+                                  int nrhs, const uint32_t* T32, double2* lo, int32_t* err,
+                                  cudaStream_t st);
 // scratch-free forms on the tiled kernel (per-level classes, 3D Helmholtz)
 cudaError_t launch_m2l_direct(const qbxfmm_geometry& g, const TransHost& th, const TransCfg& c,
                               const int32_t* waves, int nwaves, int nrhs, const double* T,

@@ -1,0 +1,756 @@
+// Mixed-precision far field of the 3D Laplace apply (qbxfmm_kernel.precision = 1).
+//
+// The far-field stages compute in FP32 while the expansions stay stored in FP64
+// (each kernel loads FP64, computes in FP32, accumulates its result back into the
+// FP64 array): P2M, P2L and M2QBXL on the FP32 pipe, and the matrix-form
+// translations (M2M, M2L, L2L) on the tensor cores as split-TF32 products
+// (a = a_hi + a_lo in TF32, a b ~ a_hi b_hi + a_hi b_lo + a_lo b_hi, FP32 accumulation:
+// mma.sync m16n8k8 tf32).  The QBX near field (P2QBXL / target-specific, QBXL2P), the
+// non-QBX point evaluations and L2QBXL stay FP64.  Expansions, scalings and work
+// decomposition are those of the FP64 kernels in kernels_laplace.cu / kernels_trans.cu.
+#include <algorithm>
+
+#include "laplace.cuh"
+#include "kernels.h"
+
+namespace qbx {
+
+namespace {
+
+constexpr int NT = 128;
+constexpr int NW = NT / 32;
+constexpr int MAXB = 128;
+
+QBX_D float frcp(int i) { return (float)rcp(i); }
+
+QBX_D void mx_list_prefix(const qbxfmm_geometry& g, const int32_t* __restrict__ lists, int gb,
+                          int nb, int* s_pref, int* s_start, int32_t* err)
+{
+  if (threadIdx.x >= 32) return;
+  int lane = threadIdx.x;
+  int cnt[4], loc = 0;
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    int k = lane * 4 + u;
+    cnt[u] = 0;
+    if (k < nb) {
+      int sb = lists[gb + k];
+      int s0 = 0;
+      if ((unsigned)sb < (unsigned)g.nboxes) {
+        s0 = g.box_source_starts[sb];
+        cnt[u] = g.box_source_counts_nonchild[sb];
+      } else {
+        report(err, QBX_DEVERR_BAD_BOX);
+      }
+      s_start[k] = s0;
+    }
+    loc += cnt[u];
+  }
+  int incl = loc;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    int v = __shfl_up_sync(0xffffffffu, incl, off);
+    if (lane >= off) incl += v;
+  }
+  int run = incl - loc;
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    int k = lane * 4 + u;
+    if (k < nb) s_pref[k] = run;
+    run += cnt[u];
+  }
+  if (lane == 31) s_pref[nb] = incl;
+}
+
+QBX_D int mx_stream_source(int v, int nb, const int* s_pref, const int* s_start)
+{
+  int lo = 0, hi = nb - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (s_pref[mid] <= v) lo = mid;
+    else hi = mid - 1;
+  }
+  return s_start[lo] + (v - s_pref[lo]);
+}
+
+}  // namespace
+
+// {{{ P2M (FP32)
+
+constexpr int MX_SUB = 16;
+constexpr int MX_TS = MX_SUB + 1;
+
+__global__ void __launch_bounds__(NT)
+k_p2m3_f32(qbxfmm_geometry g, SourceCoeffs sc, int p, int ncf, int nrhs,
+           const double* __restrict__ strengths, double2* __restrict__ mpoles)
+{
+  constexpr int SUB = MX_SUB, TS = MX_TS;
+  extern __shared__ float2 smf[];
+  float2* tab = smf;                                   // [ncf][TS]
+  __shared__ float s_u[SUB][3], s_n[SUB][3], s_q[SUB];
+  int b = g.source_boxes[blockIdx.x];
+  int r = blockIdx.y;
+  double rho = level_width(g, g.box_levels[b]);
+  double rinv = 1.0 / rho;
+  double c[3];
+  load_point<3>(g.box_centers, g.nboxes, b, c);
+  int s0 = g.box_source_starts[b];
+  int ns = g.box_source_counts_nonchild[b];
+  const double* st = strengths + (size_t)r * g.nsources;
+  const bool dip = sc.cd != 0.0;
+  const float cq = (float)sc.cq, cdr = (float)(sc.cd * rinv);
+
+  int o_nm[2], o_a[2], o_b[2], o_c[2];
+  float w_a[2], w_b[2], w_c[2];
+  bool valid[2];
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    int ci = threadIdx.x + h * NT;
+    valid[h] = ci < ncf;
+    o_nm[h] = o_a[h] = o_b[h] = o_c[h] = 0;
+    w_a[h] = w_b[h] = w_c[h] = 0.0f;
+    if (valid[h]) {
+      int n, m;
+      decode3(ci, n, m);
+      o_nm[h] = idx3(n, m) * TS;
+      if (n >= 1) {
+        if (m <= n - 1) { o_a[h] = idx3(n - 1, m) * TS; w_a[h] = 1.0f; }
+        if (m >= 1) { o_b[h] = idx3(n - 1, m - 1) * TS; w_b[h] = 1.0f; }
+        else if (n - 1 >= 1) { o_b[h] = idx3(n - 1, 1) * TS; w_b[h] = -1.0f; }
+        if (m + 1 <= n - 1) { o_c[h] = idx3(n - 1, m + 1) * TS; w_c[h] = 1.0f; }
+      }
+    }
+  }
+  float2 acc[2] = {f2(0.0f), f2(0.0f)};
+  for (int base = 0; base < ns; base += SUB) {
+    int cnt = min(SUB, ns - base);
+    if (threadIdx.x < cnt) {
+      int s = s0 + base + threadIdx.x;
+      double y[3];
+      load_point<3>(g.sources, g.nsources, s, y);
+#pragma unroll
+      for (int d = 0; d < 3; ++d) s_u[threadIdx.x][d] = (float)((y[d] - c[d]) * rinv);
+      if (dip) {
+        double nv[3];
+        load_point<3>(g.source_normals, g.nsources, s, nv);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) s_n[threadIdx.x][d] = (float)nv[d];
+      }
+      s_q[threadIdx.x] = (float)__ldg(st + s);
+    }
+    __syncthreads();
+    for (int w = threadIdx.x; w < cnt * (p + 1); w += NT) {
+      int m = w / cnt, j = w - m * cnt;
+      float x = s_u[j][0], y = s_u[j][1], z = s_u[j][2];
+      float r2 = x * x + y * y + z * z;
+      float2 a = f2(1.0f);
+      for (int k = 1; k <= m; ++k) a = fscale(0.5f * frcp(k), fmul(a, f2(x, y)));
+      float2* T = tab + j;
+      T[idx3(m, m) * TS] = a;
+      float2 prev = f2(0.0f);
+      for (int n = m + 1; n <= p; ++n) {
+        float2 bb = fscale(frcp(n + m) * frcp(n - m), fsub(fscale((2.0f * n - 1) * z, a), fscale(r2, prev)));
+        T[idx3(n, m) * TS] = bb;
+        prev = a;
+        a = bb;
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      if (!valid[h]) continue;
+      float2 a = acc[h];
+      for (int j = 0; j < cnt; ++j) {
+        const float2* T = tab + j;
+        float q = s_q[j];
+        a = faxpy(cq * q, fconj(T[o_nm[h]]), a);
+        if (dip) {
+          float f = cdr * q;
+          float dx = s_n[j][0], dy = s_n[j][1], dz = s_n[j][2];
+          float2 tb_ = T[o_b[h]];
+          tb_ = (w_b[h] < 0.0f) ? f2(-tb_.x, tb_.y) : fscale(w_b[h], tb_);
+          float2 v = fscale(dz * w_a[h], T[o_a[h]]);
+          v = ffma(f2(0.5f * dx, 0.5f * dy), tb_, v);
+          v = ffma(f2(-0.5f * dx * w_c[h], 0.5f * dy * w_c[h]), T[o_c[h]], v);
+          a = faxpy(f, fconj(v), a);
+        }
+      }
+      acc[h] = a;
+    }
+    __syncthreads();
+  }
+  double2* M = mpoles + ((size_t)b * nrhs + r) * ncf;
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    int ci = threadIdx.x + h * NT;
+    if (ci < ncf) M[ci] = cadd(M[ci], tod(acc[h]));
+  }
+}
+
+// }}}
+
+// {{{ P2L (FP32)
+
+constexpr int MX_LSUB = 32;
+constexpr int MX_LTS = MX_LSUB + 1;
+
+__global__ void __launch_bounds__(NT)
+k_p2l3_f32(qbxfmm_geometry g, SourceCoeffs sc, int p, int ncf, int nrhs,
+           const double* __restrict__ strengths, double2* __restrict__ locals, int32_t* err)
+{
+  constexpr int SUB = MX_LSUB, TS = MX_LTS;
+  extern __shared__ float2 smf[];
+  float2* tab = smf;   // [nct][TS]
+  __shared__ float s_u[SUB][3], s_n[SUB][3], s_q[SUB];
+  __shared__ int s_pref[MAXB + 1], s_start[MAXB];
+  int i = blockIdx.x;
+  int tb = g.target_or_target_parent_boxes[i];
+  int r = blockIdx.y;
+  int l0 = g.list4_starts[i], l1 = g.list4_starts[i + 1];
+  if (l1 <= l0) return;
+  double rho = level_width(g, g.box_levels[tb]);
+  double rinv = 1.0 / rho;
+  double c[3];
+  load_point<3>(g.box_centers, g.nboxes, tb, c);
+  const double* st = strengths + (size_t)r * g.nsources;
+  const bool dip = sc.cd != 0.0;
+  const float cqr = (float)(sc.cq * rinv), cdr2 = (float)(sc.cd * rinv * rinv);
+  int o_nm[2], o_a[2], o_b[2], o_c[2];
+  float sb_sign[2];
+  bool valid[2];
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    int ci = threadIdx.x + h * NT;
+    valid[h] = ci < ncf;
+    o_nm[h] = o_a[h] = o_b[h] = o_c[h] = 0;
+    sb_sign[h] = 1.0f;
+    if (valid[h]) {
+      int n, m;
+      decode3(ci, n, m);
+      o_nm[h] = idx3(n, m) * TS;
+      o_a[h] = idx3(n + 1, m) * TS;
+      o_b[h] = idx3(n + 1, m > 0 ? m - 1 : 1) * TS;
+      sb_sign[h] = m > 0 ? 1.0f : -1.0f;
+      o_c[h] = idx3(n + 1, m + 1) * TS;
+    }
+  }
+  float2 acc[2] = {f2(0.0f), f2(0.0f)};
+  for (int gb = l0; gb < l1; gb += MAXB) {
+    int nb = min(MAXB, l1 - gb);
+    __syncthreads();
+    mx_list_prefix(g, g.list4_lists, gb, nb, s_pref, s_start, err);
+    __syncthreads();
+    int total = s_pref[nb];
+    for (int base = 0; base < total; base += SUB) {
+      int cnt = min(SUB, total - base);
+      if (threadIdx.x < cnt) {
+        int s = mx_stream_source(base + threadIdx.x, nb, s_pref, s_start);
+        double y[3];
+        load_point<3>(g.sources, g.nsources, s, y);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) s_u[threadIdx.x][d] = (float)((y[d] - c[d]) * rinv);
+        if (dip) {
+          double nv[3];
+          load_point<3>(g.source_normals, g.nsources, s, nv);
+#pragma unroll
+          for (int d = 0; d < 3; ++d) s_n[threadIdx.x][d] = (float)nv[d];
+        }
+        s_q[threadIdx.x] = (float)__ldg(st + s);
+      }
+      __syncthreads();
+      for (int w = threadIdx.x; w < cnt * (p + 2); w += NT) {
+        int m = w / cnt, j = w - m * cnt;
+        float x = s_u[j][0], y = s_u[j][1], z = s_u[j][2];
+        float rinv2 = 1.0f / (x * x + y * y + z * z);
+        float2 a = f2(sqrtf(rinv2));
+        for (int k = 1; k <= m; ++k) a = fscale((2.0f * k - 1) * rinv2, fmul(a, f2(x, y)));
+        float2* T = tab + j;
+        T[idx3(m, m) * TS] = a;
+        float2 prev = f2(0.0f);
+        for (int n = m + 1; n <= p + 1; ++n) {
+          float2 bb = fscale(rinv2, fsub(fscale((2.0f * n - 1) * z, a),
+                                         fscale((float)((n + m - 1) * (n - m - 1)), prev)));
+          T[idx3(n, m) * TS] = bb;
+          prev = a;
+          a = bb;
+        }
+      }
+      __syncthreads();
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        if (!valid[h]) continue;
+        float2 a = acc[h];
+        for (int j = 0; j < cnt; ++j) {
+          const float2* T = tab + j;
+          float q = s_q[j];
+          a = faxpy(cqr * q, T[o_nm[h]], a);
+          if (dip) {
+            float f = cdr2 * q;
+            float dx = s_n[j][0], dy = s_n[j][1], dz = s_n[j][2];
+            float2 tb_ = T[o_b[h]];
+            if (sb_sign[h] < 0.0f) tb_ = f2(-tb_.x, tb_.y);
+            float2 v = fscale(-dz, T[o_a[h]]);
+            v = ffma(f2(0.5f * dx, 0.5f * dy), tb_, v);
+            v = ffma(f2(-0.5f * dx, 0.5f * dy), T[o_c[h]], v);
+            a = faxpy(f, v, a);
+          }
+        }
+        acc[h] = a;
+      }
+      __syncthreads();
+    }
+  }
+  double2* L = locals + ((size_t)tb * nrhs + r) * ncf;
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    int o = threadIdx.x + h * NT;
+    if (o < ncf) L[o] = cadd(L[o], tod(acc[h]));
+  }
+}
+
+// }}}
+
+// {{{ M2QBXL (FP32)
+
+template <int Q>
+__global__ void __launch_bounds__(NT)
+k_m2qbxl3_f32(qbxfmm_geometry g, int pf, int ncf, int nrhs, const double2* __restrict__ mpoles,
+              double2* __restrict__ qbx_exps, int32_t* err)
+{
+  constexpr int NC = (Q + 1) * (Q + 2) / 2;
+  extern __shared__ float2 smf[];
+  const int MW = 2 * pf + 3 * Q + 1;
+  const int MR = pf + 2 * Q + 1;
+  const int MSZ = MR * MW;
+  const int loff = pf + 2 * Q;
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  float2* Mw = smf + (size_t)warp * MSZ;
+  float2* red = smf + (size_t)NW * MSZ;   // [NW-1][32][NC]
+  int chunk = blockIdx.x;
+  int r = blockIdx.y;
+  int itb = g.qbx_chunk_target_box[chunk];
+  bool has_center = lane < g.qbx_chunk_count[chunk];
+  int ctr = has_center ? g.centers_by_target_box[g.qbx_chunk_start[chunk] + lane] : 0;
+  if ((unsigned)ctr >= (unsigned)g.ncenters) {
+    report(err, QBX_DEVERR_BAD_CENTER);
+    has_center = false;
+    ctr = 0;
+  }
+  double cc[3];
+  load_point<3>(g.centers, g.ncenters, ctr, cc);
+  double rho_t = g.expansion_radii[ctr];
+  for (int q = lane; q < MSZ; q += 32) Mw[q] = f2(0.0f);
+  float2 acc[NC];
+#pragma unroll
+  for (int i = 0; i < NC; ++i) acc[i] = f2(0.0f);
+  int l0 = g.list3_starts[itb], l1 = g.list3_starts[itb + 1];
+  for (int li = l0 + warp; li < l1; li += NW) {
+    int sb = g.list3_lists[li];
+    if ((unsigned)sb >= (unsigned)g.nboxes) {
+      report(err, QBX_DEVERR_BAD_BOX);
+      continue;
+    }
+    __syncwarp();
+    const double2* src = mpoles + ((size_t)sb * nrhs + r) * ncf;
+    for (int q = lane; q < ncf; q += 32) {
+      int k, l;
+      decode3(q, k, l);
+      float2 v = tof(src[q]);
+      Mw[(k + Q) * MW + loff + l] = v;
+      if (l > 0) Mw[(k + Q) * MW + loff - l] = (l & 1) ? f2(-v.x, v.y) : f2(v.x, -v.y);
+    }
+    __syncwarp();
+    if (!has_center) continue;
+    double rho_s = level_width(g, g.box_levels[sb]);
+    double cs[3];
+    load_point<3>(g.box_centers, g.nboxes, sb, cs);
+    float ratio = (float)(rho_t / rho_s);
+    float d0 = (float)((cc[0] - cs[0]) / rho_s), d1 = (float)((cc[1] - cs[1]) / rho_s),
+          d2 = (float)((cc[2] - cs[2]) / rho_s);
+    float rinv2 = 1.0f / (d0 * d0 + d1 * d1 + d2 * d2);
+    int nmax = pf + Q;
+    float2 part[NC];
+#pragma unroll
+    for (int i = 0; i < NC; ++i) part[i] = f2(0.0f);
+    float2 mm = f2(sqrtf(rinv2));
+    for (int mp = 0; mp <= nmax; ++mp) {
+      if (mp > 0) mm = fscale((2.0f * mp - 1) * rinv2, fmul(mm, f2(d0, d1)));
+      float2 a = mm, prev = f2(0.0f);
+      const float2* bpos = Mw + (mp + Q) * MW + loff + mp;
+      const float2* bneg = Mw + (mp + Q) * MW + loff - mp;
+      for (int np = mp; np <= nmax; ++np) {
+        if (np > mp) {
+          float2 bb = fscale(rinv2, fsub(fscale((2.0f * np - 1) * d2, a),
+                                         fscale((float)((np + mp - 1) * (np - mp - 1)), prev)));
+          prev = a;
+          a = bb;
+        }
+#pragma unroll
+        for (int j = 0; j <= Q; ++j)
+#pragma unroll
+          for (int ii = 0; ii <= j; ++ii)
+            part[idx3(j, ii)] = ffma(bpos[-j * MW - ii], a, part[idx3(j, ii)]);
+        if (mp > 0) {
+          float2 aneg = (mp & 1) ? f2(-a.x, a.y) : f2(a.x, -a.y);
+#pragma unroll
+          for (int j = 0; j <= Q; ++j)
+#pragma unroll
+            for (int ii = 0; ii <= j; ++ii)
+              part[idx3(j, ii)] = ffma(bneg[-j * MW - ii], aneg, part[idx3(j, ii)]);
+        }
+        bpos += MW;
+        bneg += MW;
+      }
+    }
+    float rj = (float)(1.0 / rho_s);
+#pragma unroll
+    for (int j = 0; j <= Q; ++j) {
+#pragma unroll
+      for (int ii = 0; ii <= j; ++ii)
+        acc[idx3(j, ii)] = faxpy((j & 1) ? -rj : rj, part[idx3(j, ii)], acc[idx3(j, ii)]);
+      rj *= ratio;
+    }
+  }
+  __syncthreads();
+  if (warp > 0) {
+#pragma unroll
+    for (int i = 0; i < NC; ++i) red[((warp - 1) * 32 + lane) * NC + i] = acc[i];
+  }
+  __syncthreads();
+  if (warp == 0 && has_center) {
+    double2* out = qbx_exps + ((size_t)ctr * nrhs + r) * NC;
+#pragma unroll
+    for (int i = 0; i < NC; ++i) {
+      float2 a = acc[i];
+      for (int w = 1; w < NW; ++w) a = fadd(a, red[((w - 1) * 32 + lane) * NC + i]);
+      out[i] = cadd(out[i], tod(a));
+    }
+  }
+}
+
+// }}}
+
+// {{{ split-TF32 translation GEMM
+
+QBX_D uint32_t to_tf32(float x)
+{
+  uint32_t u;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(u) : "f"(x));
+  return u;
+}
+
+QBX_D void mma_tf32(float* d, const uint32_t* a, const uint32_t* b)
+{
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, "
+      "{%8, %9}, {%0, %1, %2, %3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+// FP64 matrices [nmat][rp][kp] -> TF32 hi / lo planes [nmat][rp16][kp8] (zero padded)
+__global__ void k_trans_split_tf32(int nmat, int rp, int kp, int rp16, int kp8, int R,
+                                   const double* __restrict__ T, uint32_t* __restrict__ Thi,
+                                   uint32_t* __restrict__ Tlo)
+{
+  size_t n = (size_t)nmat * rp16 * kp8;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n;
+       e += (size_t)gridDim.x * blockDim.x) {
+    size_t mat = e / ((size_t)rp16 * kp8);
+    int rem = (int)(e - mat * rp16 * kp8);
+    int row = rem / kp8, col = rem - row * kp8;
+    float v = (row < R && col < R) ? (float)T[(mat * rp + row) * kp + col] : 0.0f;
+    uint32_t hi = to_tf32(v);
+    Thi[e] = hi;
+    Tlo[e] = to_tf32(v - __uint_as_float(hi));
+  }
+}
+
+constexpr int X3_KC = 32;      // K staged per step
+constexpr int X3_AS = X3_KC + 4;
+constexpr int X3_NW = 4;       // warps, one n8 column tile each
+constexpr int X3_N = 8 * X3_NW;
+constexpr int X3_MT = 16;      // max m16 tiles (rows <= 256)
+
+// C = T X (split TF32, FP32 accumulation) for one group and 32 columns (pair x rhs);
+// all row tiles in every warp.  Output as in k_trans_gemm: added (x scale) into
+// pair_dst's expansion, or stored per pair into cpair (FP64, row stride rp).
+__global__ void __launch_bounds__(NT)
+k_trans_gemm_x3(int ncf, int rp, int rp16, int kp8, int nrhs, const uint32_t* __restrict__ Thi,
+                const uint32_t* __restrict__ Tlo, int mat_mod, const int32_t* __restrict__ group_starts,
+                int g0, const int32_t* __restrict__ pair_src, const int32_t* __restrict__ pair_dst,
+                const double2* __restrict__ ein, double2* __restrict__ eout, double scale,
+                double* __restrict__ cpair, int32_t* err, int nboxes)
+{
+  extern __shared__ uint32_t smu[];
+  uint32_t* Ah = smu;                                   // [rp16][X3_AS]
+  uint32_t* Al = Ah + (size_t)rp16 * X3_AS;             // [rp16][X3_AS]
+  uint32_t* Bh = Al + (size_t)rp16 * X3_AS;             // [X3_KC][X3_N + 4]
+  uint32_t* Bl = Bh + (size_t)X3_KC * (X3_N + 4);
+  __shared__ int s_src[X3_N];
+  const int BS = X3_N + 4;
+  int grp = g0 + blockIdx.y;
+  int p0 = group_starts[grp], p1 = group_starts[grp + 1];
+  int ncol = (p1 - p0) * nrhs;
+  int c0 = blockIdx.x * X3_N;
+  if (c0 >= ncol) return;
+  int mat = mat_mod > 0 ? (grp % mat_mod) : grp;
+  const uint32_t* Th = Thi + (size_t)mat * rp16 * kp8;
+  const uint32_t* Tl = Tlo + (size_t)mat * rp16 * kp8;
+  const int R = 2 * ncf;
+  for (int j = threadIdx.x; j < X3_N; j += NT) {
+    int c = c0 + j;
+    int src = -1;
+    if (c < ncol) {
+      src = pair_src[p0 + c / nrhs];
+      if ((unsigned)src >= (unsigned)nboxes) {
+        report(err, QBX_DEVERR_BAD_BOX);
+        src = -1;
+      }
+    }
+    s_src[j] = src;
+  }
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int g = lane >> 2, tq = lane & 3;
+  int mt = rp16 / 16;
+  float acc[X3_MT][4];
+#pragma unroll
+  for (int i = 0; i < X3_MT; ++i) acc[i][0] = acc[i][1] = acc[i][2] = acc[i][3] = 0.0f;
+  for (int kc = 0; kc < kp8; kc += X3_KC) {
+    int kw = min(X3_KC, kp8 - kc);
+    __syncthreads();
+    for (int e = threadIdx.x; e < rp16 * X3_KC; e += NT) {
+      int row = e / X3_KC, col = e - row * X3_KC;
+      bool ok = col < kw;
+      Ah[row * X3_AS + col] = ok ? __ldg(Th + (size_t)row * kp8 + kc + col) : 0u;
+      Al[row * X3_AS + col] = ok ? __ldg(Tl + (size_t)row * kp8 + kc + col) : 0u;
+    }
+    for (int e = threadIdx.x; e < X3_N * X3_KC; e += NT) {
+      int j = e / X3_KC, k = e - j * X3_KC;
+      int src = s_src[j];
+      float v = 0.0f;
+      if (src >= 0 && k < kw && kc + k < R) {
+        int r = (c0 + j) % nrhs;
+        v = (float)__ldg(reinterpret_cast<const double*>(ein + ((size_t)src * nrhs + r) * ncf) + kc + k);
+      }
+      uint32_t hi = to_tf32(v);
+      Bh[k * BS + j] = hi;
+      Bl[k * BS + j] = to_tf32(v - __uint_as_float(hi));
+    }
+    __syncthreads();
+    for (int k0 = 0; k0 < kw; k0 += 8) {
+      uint32_t bh[2], bl[2];
+      int col = warp * 8 + g;
+      bh[0] = Bh[(k0 + tq) * BS + col];
+      bh[1] = Bh[(k0 + tq + 4) * BS + col];
+      bl[0] = Bl[(k0 + tq) * BS + col];
+      bl[1] = Bl[(k0 + tq + 4) * BS + col];
+#pragma unroll
+      for (int i = 0; i < X3_MT; ++i) {
+        if (i >= mt) break;
+        int r0 = i * 16 + g;
+        uint32_t ah[4], al[4];
+        ah[0] = Ah[r0 * X3_AS + k0 + tq];
+        ah[1] = Ah[(r0 + 8) * X3_AS + k0 + tq];
+        ah[2] = Ah[r0 * X3_AS + k0 + tq + 4];
+        ah[3] = Ah[(r0 + 8) * X3_AS + k0 + tq + 4];
+        al[0] = Al[r0 * X3_AS + k0 + tq];
+        al[1] = Al[(r0 + 8) * X3_AS + k0 + tq];
+        al[2] = Al[r0 * X3_AS + k0 + tq + 4];
+        al[3] = Al[(r0 + 8) * X3_AS + k0 + tq + 4];
+        mma_tf32(acc[i], al, bh);
+        mma_tf32(acc[i], ah, bl);
+        mma_tf32(acc[i], ah, bh);
+      }
+    }
+  }
+  // epilogue: acc[i][v] = C[row = i*16 + g + 8 (v >> 1)][col = warp*8 + 2 tq + (v & 1)]
+#pragma unroll
+  for (int v = 0; v < 4; ++v) {
+    int c = c0 + warp * 8 + 2 * tq + (v & 1);
+    if (c >= ncol) continue;
+    int pr = p0 + c / nrhs, r = c % nrhs;
+    if (pair_dst) {
+      int dst = pair_dst[pr];
+      if ((unsigned)dst >= (unsigned)nboxes) {
+        report(err, QBX_DEVERR_BAD_BOX);
+        continue;
+      }
+      double* y = reinterpret_cast<double*>(eout + ((size_t)dst * nrhs + r) * ncf);
+#pragma unroll
+      for (int i = 0; i < X3_MT; ++i) {
+        if (i >= mt) break;
+        int row = i * 16 + g + 8 * (v >> 1);
+        if (row < R) y[row] += scale * (double)acc[i][v];
+      }
+    } else {
+      double* y = cpair + ((size_t)pr * nrhs + r) * rp;
+#pragma unroll
+      for (int i = 0; i < X3_MT; ++i) {
+        if (i >= mt) break;
+        int row = i * 16 + g + 8 * (v >> 1);
+        if (row < R) y[row] = (double)acc[i][v];
+      }
+    }
+  }
+}
+
+// }}}
+
+// {{{ launchers
+
+cudaError_t launch_p2m_mixed(const qbxfmm_geometry& g, SourceCoeffs sc, int p, int nrhs,
+                             const double* s, double2* mp, cudaStream_t st)
+{
+  if (g.nsource_boxes == 0) return cudaSuccess;
+  int ncf = (p + 1) * (p + 2) / 2;
+  size_t sh = (size_t)MX_TS * ncf * sizeof(float2);
+  cudaFuncSetAttribute(k_p2m3_f32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+  k_p2m3_f32<<<dim3(g.nsource_boxes, nrhs), NT, sh, st>>>(g, sc, p, ncf, nrhs, s, mp);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_p2l_mixed(const qbxfmm_geometry& g, SourceCoeffs sc, int p, int nrhs,
+                             const double* s, double2* lo, int32_t* err, cudaStream_t st)
+{
+  if (g.nttp_boxes == 0) return cudaSuccess;
+  int ncf = (p + 1) * (p + 2) / 2;
+  int nct = (p + 2) * (p + 3) / 2;
+  size_t sh = (size_t)MX_LTS * nct * sizeof(float2);
+  cudaFuncSetAttribute(k_p2l3_f32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+  k_p2l3_f32<<<dim3(g.nttp_boxes, nrhs), NT, sh, st>>>(g, sc, p, ncf, nrhs, s, lo, err);
+  return cudaGetLastError();
+}
+
+template <int Q>
+static cudaError_t m2qbxl_mixed_q(const qbxfmm_geometry& g, int pf, int nrhs, const double2* mp,
+                                  double2* qe, int32_t* err, cudaStream_t st)
+{
+  constexpr int NC = (Q + 1) * (Q + 2) / 2;
+  int ncf = (pf + 1) * (pf + 2) / 2;
+  size_t msz = (size_t)(pf + 2 * Q + 1) * (2 * pf + 3 * Q + 1);
+  size_t sh = (NW * msz + (size_t)(NW - 1) * 32 * NC) * sizeof(float2);
+  cudaFuncSetAttribute(k_m2qbxl3_f32<Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+  k_m2qbxl3_f32<Q><<<dim3(g.nqbx_chunks, nrhs), NT, sh, st>>>(g, pf, ncf, nrhs, mp, qe, err);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_m2qbxl_mixed(const qbxfmm_geometry& g, int pf, int q, int nrhs,
+                                const double2* mp, double2* qe, int32_t* err, cudaStream_t st)
+{
+  if (g.nqbx_chunks == 0) return cudaSuccess;
+  switch (q) {
+    case 0: return m2qbxl_mixed_q<0>(g, pf, nrhs, mp, qe, err, st);
+    case 1: return m2qbxl_mixed_q<1>(g, pf, nrhs, mp, qe, err, st);
+    case 2: return m2qbxl_mixed_q<2>(g, pf, nrhs, mp, qe, err, st);
+    case 3: return m2qbxl_mixed_q<3>(g, pf, nrhs, mp, qe, err, st);
+    case 4: return m2qbxl_mixed_q<4>(g, pf, nrhs, mp, qe, err, st);
+    case 5: return m2qbxl_mixed_q<5>(g, pf, nrhs, mp, qe, err, st);
+    case 6: return m2qbxl_mixed_q<6>(g, pf, nrhs, mp, qe, err, st);
+    case 7: return m2qbxl_mixed_q<7>(g, pf, nrhs, mp, qe, err, st);
+    case 8: return m2qbxl_mixed_q<8>(g, pf, nrhs, mp, qe, err, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+void tf32_dims(const TransCfg& c, int& rp16, int& kp8)
+{
+  rp16 = (2 * c.ncf + 15) / 16 * 16;
+  kp8 = (2 * c.ncf + 7) / 8 * 8;
+}
+
+bool tf32_supported(const TransCfg& c)
+{
+  int rp16, kp8;
+  tf32_dims(c, rp16, kp8);
+  return rp16 / 16 <= X3_MT;
+}
+
+size_t tf32_matrix_bytes(const TransCfg& c)
+{
+  int rp16, kp8;
+  tf32_dims(c, rp16, kp8);
+  return 2 * c.nmatrices * (size_t)rp16 * kp8 * sizeof(uint32_t);
+}
+
+cudaError_t launch_trans_split_tf32(const TransCfg& c, const double* T, uint32_t* T32,
+                                    cudaStream_t st)
+{
+  int rp16, kp8;
+  tf32_dims(c, rp16, kp8);
+  size_t n = c.nmatrices * (size_t)rp16 * kp8;
+  int blocks = (int)std::min<size_t>((n + 255) / 256, 148 * 16);
+  k_trans_split_tf32<<<blocks, 256, 0, st>>>((int)c.nmatrices, c.rp, c.kp, rp16, kp8, 2 * c.ncf, T,
+                                             T32, T32 + n);
+  return cudaGetLastError();
+}
+
+static cudaError_t x3_launch(const qbxfmm_geometry& g, const TransCfg& c, int nrhs, const uint32_t* T32,
+                             size_t mat_base, int mat_mod, const int32_t* group_starts, int g0,
+                             int ngroups, int maxcols, const int32_t* pair_src,
+                             const int32_t* pair_dst, const double2* ein, double2* eout,
+                             double scale, double* cpair, int32_t* err, cudaStream_t st)
+{
+  if (ngroups <= 0 || maxcols <= 0) return cudaSuccess;
+  int rp16, kp8;
+  tf32_dims(c, rp16, kp8);
+  size_t n = c.nmatrices * (size_t)rp16 * kp8;
+  size_t plane = (size_t)rp16 * kp8;
+  size_t sh = (2 * (size_t)rp16 * X3_AS + 2 * (size_t)X3_KC * (X3_N + 4)) * sizeof(uint32_t);
+  cudaFuncSetAttribute(k_trans_gemm_x3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+  dim3 grid((maxcols + X3_N - 1) / X3_N, ngroups);
+  k_trans_gemm_x3<<<grid, NT, sh, st>>>(c.ncf, c.rp, rp16, kp8, nrhs, T32 + mat_base * plane,
+                                        T32 + n + mat_base * plane, mat_mod, group_starts, g0,
+                                        pair_src, pair_dst, ein, eout, scale, cpair, err, g.nboxes);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_m2l_gemm_mixed(const qbxfmm_geometry& g, const TransHost& th, const TransCfg& c,
+                                  int nrhs, const uint32_t* T32, const double2* mp, double2* lo,
+                                  double* cpair, int32_t* err, cudaStream_t st)
+{
+  if (g.m2l_nclasses == 0) return cudaSuccess;
+  cudaError_t e = x3_launch(g, c, nrhs, T32, 0, 0, g.m2l_class_starts, 0, g.m2l_nclasses,
+                            th.m2l_max_pairs * nrhs, g.m2l_pair_src, nullptr, mp, nullptr, 1.0,
+                            cpair, err, st);
+  if (e != cudaSuccess) return e;
+  return launch_trans_reduce_m2l(g, c, nrhs, cpair, lo, st);
+}
+
+cudaError_t launch_m2m_gemm_mixed(const qbxfmm_geometry& g, const TransHost& th, const TransCfg& c,
+                                  int nrhs, const uint32_t* T32, double2* mp, double* cpair,
+                                  int32_t* err, cudaStream_t st)
+{
+  const int nch = 8;
+  for (int lev = g.nlevels - 2; lev >= 0; --lev) {
+    int maxp = th.m2m_level_max_group[lev];
+    if (maxp == 0) continue;
+    cudaError_t e = x3_launch(g, c, nrhs, T32, c.m2m_base, c.m2m_mat_mod, g.m2m_group_starts,
+                              lev * nch, nch, maxp * nrhs, g.m2m_pair_src, nullptr, mp, nullptr,
+                              1.0, cpair, err, st);
+    if (e != cudaSuccess) return e;
+    e = launch_trans_reduce_m2m(g, th, c, lev, nrhs, cpair, mp, st);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+cudaError_t launch_l2l_gemm_mixed(const qbxfmm_geometry& g, const TransHost& th, const TransCfg& c,
+                                  int nrhs, const uint32_t* T32, double2* lo, int32_t* err,
+                                  cudaStream_t st)
+{
+  const int nch = 8;
+  for (int lev = 1; lev < g.nlevels; ++lev) {
+    int maxp = th.l2l_level_max_group[lev];
+    if (maxp == 0) continue;
+    cudaError_t e = x3_launch(g, c, nrhs, T32, c.l2l_base, c.m2m_mat_mod, g.l2l_group_starts,
+                              lev * nch, nch, maxp * nrhs, g.l2l_pair_src, g.l2l_pair_dst, lo, lo,
+                              1.0, nullptr, err, st);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+// }}}
+
+}  // namespace qbx

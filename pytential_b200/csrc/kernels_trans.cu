@@ -497,6 +497,28 @@ cudaError_t launch_l2l_gemm(const qbxfmm_geometry& g, const TransHost& th, const
   return cudaSuccess;
 }
 
+cudaError_t launch_trans_reduce_m2l(const qbxfmm_geometry& g, const TransCfg& c, int nrhs,
+                                    const double* cpair, double2* lo, cudaStream_t st)
+{
+  if (g.nttp_boxes == 0) return cudaSuccess;
+  k_trans_reduce<<<dim3(g.nttp_boxes, nrhs), NT, 0, st>>>(
+      c.ncf, c.rp, nrhs, g.target_or_target_parent_boxes, 0, g.m2l_tgt_pair_starts,
+      g.m2l_tgt_pairs, cpair, lo, c.m2l_div_by_width, g.box_levels, g.root_extent);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_trans_reduce_m2m(const qbxfmm_geometry& g, const TransHost& th, const TransCfg& c,
+                                    int lev, int nrhs, const double* cpair, double2* mp,
+                                    cudaStream_t st)
+{
+  int i0 = th.lvl_source_parent[lev], i1 = th.lvl_source_parent[lev + 1];
+  if (i1 > i0)
+    k_trans_reduce<<<dim3(i1 - i0, nrhs), NT, 0, st>>>(c.ncf, c.rp, nrhs, g.source_parent_boxes, i0,
+                                                       g.m2m_par_pair_starts, g.m2m_par_pairs, cpair,
+                                                       mp, 0, g.box_levels, g.root_extent);
+  return cudaGetLastError();
+}
+
 static cudaError_t gemm_tiled_launch(const qbxfmm_geometry& g, const TransCfg& c, int nrhs,
                                      const double* T, size_t mat_base, int mat_mod,
                                      const int32_t* group_starts_dev, int g0, int ngroups,

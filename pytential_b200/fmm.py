@@ -108,6 +108,10 @@ class DeviceGeometry:
         raise AttributeError(name)
 
 
+PRECISION_FP64 = 0
+PRECISION_MIXED = 1     # FP32 far field, split-TF32 translations (3D Laplace)
+
+
 def needs_per_level_classes(spec: SourceKernelSpec) -> bool:
     """3D Helmholtz translations depend on the level (k times the box width)."""
     return spec.kernel.family == abi.QBXFMM_HELMHOLTZ and spec.kernel.dim == 3
@@ -155,8 +159,10 @@ class Plan:
     the Python object."""
 
     def __init__(self, dgeo: DeviceGeometry, spec: SourceKernelSpec, qbx_order: int,
-                 fmm_order: int, nrhs: int = 1, target_specific_qbx: bool = False):
+                 fmm_order: int, nrhs: int = 1, target_specific_qbx: bool = False,
+                 precision: int = PRECISION_FP64):
         self.dgeo = dgeo
+        self.precision = precision
         self.target_specific_qbx = target_specific_qbx
         self.spec = spec
         self.qbx_order = qbx_order
@@ -166,7 +172,7 @@ class Plan:
             family=spec.kernel.family, dim=spec.kernel.dim, qbx_order=qbx_order,
             fmm_order=fmm_order, nrhs=nrhs, charge_coeff=spec.charge_coeff,
             dipole_coeff=spec.dipole_coeff, k=spec.wave_number,
-            target_specific_qbx=target_specific_qbx)
+            target_specific_qbx=target_specific_qbx, precision=precision)
         h = ctypes.c_void_p()
         native.check("qbxfmm_plan_create", native.lib().qbxfmm_plan_create(
             ctypes.byref(self.kernel), ctypes.byref(dgeo.struct), ctypes.byref(h)))
@@ -480,13 +486,14 @@ class QBXApply:
     def __init__(self, geo: QBXFMMGeometryData, spec: SourceKernelSpec, qbx_order: int,
                  fmm_order: int, nrhs: int = 1, device="cuda",
                  device_geometry: DeviceGeometry | None = None,
-                 target_specific_qbx: bool = False, translation_matrices: bool = True):
+                 target_specific_qbx: bool = False, translation_matrices: bool = True,
+                 precision: int = PRECISION_FP64):
         self.geo = geo
         self.device = torch.device(device)
         self.dgeo = _device_geometry(geo, spec, device, device_geometry)
         self.up = DeviceUpsampler(geo.discr, device)
         self.plan = Plan(self.dgeo, spec, qbx_order, fmm_order, nrhs,
-                         target_specific_qbx=target_specific_qbx)
+                         target_specific_qbx=target_specific_qbx, precision=precision)
         self.nrhs = nrhs
         sizes = self.plan.workspace_sizes()
         use_mats = (translation_matrices or needs_per_level_classes(spec)) and sizes[6] > 0

@@ -161,6 +161,26 @@ def test_target_specific_mode_matches_checker(name):
     assert relerr(host(drive_fmm(None, wt, [dev(flat)])), ref) < TOL
 
 
+@pytest.mark.parametrize("name", ["3d-D-small", "3d-S-small", "3d-D"])
+def test_mixed_precision_apply_error(name):
+    """Mixed form (FP32 P2M/P2L/M2QBXL, split-TF32 M2M/M2L/L2L, FP64 QBX near field):
+    its error against the FP64 checker is stated and bounded (1e-6 relative,
+    max-norm); the near field alone stays FP64, so the target-specific variant has the
+    same bound."""
+    from pytential_b200.fmm import PRECISION_MIXED
+    wl = workload(name)
+    o = oracle_for(wl)
+    ref = o.apply(wl.tree_strengths())
+    for tsq in (False, True):
+        ap = QBXApply(wl.geometry(), wl.spec, wl.qbx_order, wl.fmm_order, nrhs=wl.nrhs,
+                      target_specific_qbx=tsq, precision=PRECISION_MIXED)
+        assert ap.uses_translation_matrices
+        got = host(ap(dev(wl.density)))
+        err = relerr(got, ref)
+        assert 0.0 < err < 1e-6, (tsq, err)
+        ap.check_error_word()
+
+
 def test_full_size_3d_double_layer_apply():
     """The benchmark workload (19200 nodes, 57600 sources, qbx 3 / fmm 10)."""
     wl = workload("3d-D")
