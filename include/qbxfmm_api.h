@@ -133,6 +133,14 @@ int qbxfmm_apply_host(const qbxfmm_plan* plan, const qbxfmm_upsample* up,
 int qbxfmm_apply_noalloc(const qbxfmm_plan* plan, const qbxfmm_upsample* up,
                          const void* density, void* out, void* stream);
 
+/* Gradient of the 3D Laplace single-layer potential, by direct summation, at targets
+ * far from the sources: grad[d][t] = -1/(4 pi) sum_s charges[s] (x_t - y_s)_d / |x_t - y_s|^3
+ * (sources, targets and grad structure-of-arrays [3][n], device pointers).  Supplies the
+ * target-position gradient of the adjoint apply; the reference obtains the same
+ * quantity from its derivative kernels (a gradient target kernel in the FMM). */
+int qbxfmm_laplace3d_grad_direct(int nsources, const double* sources, const double* charges,
+                                 int ntargets, const double* targets, double* grad, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,136 @@
+"""Adjoint of the 3D Laplace single-layer apply at far targets, behind
+``torch.autograd.Function``.
+
+Forward: ``u = A sigma`` with ``A = K W U`` (``U``: stage-1 -> quad-stage-2
+upsampling, ``W``: area element x quadrature weight, ``K``: the kernel
+``1/(4 pi |x - y|)`` from the quad nodes to targets that lie away from the surface,
+so that no target needs QBX) -- the QBX-FMM apply of this library.
+
+Backward:
+
+* ``dJ/dsigma = A^T r = U^T W K^T r``: ``K`` is symmetric, so ``K^T r`` is the same FMM
+  with sources and targets exchanged -- point sources at the targets with strengths
+  ``r``, evaluated at the quad nodes (this library's apply on a point-cloud source
+  "discretization");
+* ``dJ/dx_t = r_t grad u(x_t)`` with ``grad u`` summed directly on the GPU
+  (``qbxfmm_laplace3d_grad_direct``).
+
+Both directions run in FP64 or in the mixed form (FP32 far field).  Targets close to
+the surface (which need QBX in the forward apply) are not supported here: their
+adjoint would need the transposed QBX stages.
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import native
+from .discretization import Discretization
+from .fmm import PRECISION_FP64, LaplaceKernel, QBXApply, SourceKernelSpec
+from .geometry import QBXFMMGeometryData
+
+
+def point_cloud(points: np.ndarray, radius: float = 1e-9) -> Discretization:
+    """Points as a 'discretization' with one node per element, unit weights and no
+    upsampling (the sources of the exchanged FMM)."""
+    points = np.ascontiguousarray(points, dtype=np.float64)
+    dim, n = points.shape
+    nrm = points / np.maximum(np.linalg.norm(points, axis=0), 1e-300)
+    ones = np.ones(n)
+    return Discretization(
+        ambient_dim=dim, nelements=n, nodes_per_element=1, quad_nodes_per_element=1,
+        nodes=points, normals=nrm, weights=ones, quad_nodes=points, quad_normals=nrm,
+        quad_weights=ones, upsample=np.ones((1, 1)), element_stretch=np.full(n, radius),
+        param=np.zeros((n, 1)))
+
+
+class FarFieldSingleLayer:
+    """``u = S sigma`` at fixed targets away from the surface, with its adjoint."""
+
+    def __init__(self, discr: Discretization, targets: np.ndarray, qbx_order: int,
+                 fmm_order: int, precision: int = PRECISION_FP64, device="cuda"):
+        if discr.ambient_dim != 3:
+            raise NotImplementedError("the adjoint is built for 3D Laplace")
+        self.discr = discr
+        self.targets = np.ascontiguousarray(targets, dtype=np.float64)
+        self.device = torch.device(device)
+        spec = SourceKernelSpec(LaplaceKernel(3), charge_coeff=1.0)
+        self.geo = QBXFMMGeometryData(discr, [(self.targets, 0)])
+        if self.geo.global_qbx_centers().size:
+            raise ValueError("a target needs QBX; the adjoint covers far targets only")
+        self.fwd = QBXApply(self.geo, spec, qbx_order, fmm_order, device=device,
+                            precision=precision)
+        self.geo_adj = QBXFMMGeometryData(point_cloud(self.targets), [(discr.quad_nodes, 0)])
+        self.adj = QBXApply(self.geo_adj, spec, qbx_order, fmm_order, device=device,
+                            precision=precision)
+        self.U = torch.from_numpy(np.ascontiguousarray(discr.upsample)).to(self.device)
+        self.w = torch.from_numpy(discr.quad_weights).to(self.device)
+        self.quad_nodes = torch.from_numpy(np.ascontiguousarray(discr.quad_nodes)).to(self.device)
+        self.targets_dev = torch.from_numpy(self.targets).to(self.device)
+
+    @property
+    def ndofs(self):
+        return self.discr.ndofs
+
+    @property
+    def ntargets(self):
+        return self.targets.shape[1]
+
+    def apply(self, sigma: torch.Tensor) -> torch.Tensor:
+        """(ndofs,) -> (ntargets,)"""
+        return self.fwd(sigma.reshape(1, -1).contiguous())[0].clone()
+
+    def strengths(self, sigma: torch.Tensor) -> torch.Tensor:
+        """Quad-node strengths W U sigma, (nquad,)."""
+        d = self.discr
+        s = sigma.reshape(d.nelements, d.nodes_per_element) @ self.U.T
+        return s.reshape(-1) * self.w
+
+    def adjoint(self, r: torch.Tensor) -> torch.Tensor:
+        """A^T r: (ntargets,) -> (ndofs,)"""
+        d = self.discr
+        kt = self.adj(r.reshape(1, -1).contiguous())[0]          # K^T r at the quad nodes
+        v = (kt * self.w).reshape(d.nelements, d.quad_nodes_per_element)
+        return (v @ self.U).reshape(-1)
+
+    def target_gradient(self, sigma: torch.Tensor) -> torch.Tensor:
+        """grad u at the targets, (3, ntargets)."""
+        q = self.strengths(sigma).contiguous()
+        grad = torch.empty(3, self.ntargets, dtype=torch.float64, device=self.device)
+        st = ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
+        native.check("qbxfmm_laplace3d_grad_direct", native.lib().qbxfmm_laplace3d_grad_direct(
+            q.numel(), ctypes.c_void_p(self.quad_nodes.data_ptr()), ctypes.c_void_p(q.data_ptr()),
+            self.ntargets, ctypes.c_void_p(self.targets_dev.data_ptr()),
+            ctypes.c_void_p(grad.data_ptr()), st))
+        return grad
+
+
+class _SingleLayer(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, sigma, targets, op):
+        ctx.op = op
+        ctx.save_for_backward(sigma)
+        return op.apply(sigma)
+
+    @staticmethod
+    def backward(ctx, gu):
+        (sigma,) = ctx.saved_tensors
+        op = ctx.op
+        g_sigma = op.adjoint(gu.contiguous()) if ctx.needs_input_grad[0] else None
+        g_targets = gu[None, :] * op.target_gradient(sigma) if ctx.needs_input_grad[1] else None
+        return g_sigma, g_targets, None
+
+
+def single_layer(op: FarFieldSingleLayer, sigma: torch.Tensor,
+                 targets: torch.Tensor | None = None) -> torch.Tensor:
+    """Differentiable ``S sigma`` at ``op``'s targets.  Pass ``targets`` (a (3, nt)
+    tensor holding ``op.targets``) to get gradients with respect to the target
+    positions."""
+    if targets is None:
+        targets = torch.zeros(0, dtype=torch.float64, device=sigma.device)
+    elif targets.shape != (3, op.ntargets):
+        raise ValueError("targets must have shape (3, ntargets)")
+    return _SingleLayer.apply(sigma, targets, op)

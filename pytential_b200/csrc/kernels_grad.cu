@@ -1,0 +1,80 @@
+// Direct gradient of the 3D Laplace single-layer potential at far targets, used for
+// the target-position gradient of the adjoint (the forward apply's targets are far
+// from the surface there, so the sum needs no QBX):
+//   grad u(x_t) = -1/(4 pi) sum_y q_y (x_t - y) / |x_t - y|^3.
+// CTA of 128 targets (thread = target); the sources stream through shared memory in
+// tiles of 256.
+#include <string>
+
+#include "../../include/qbxfmm_api.h"
+#include "kernels.h"
+
+namespace qbx {
+int set_last_error(int code, const std::string& msg);
+
+constexpr int GT = 128;
+constexpr int GS = 256;
+
+namespace {
+
+__global__ void __launch_bounds__(GT)
+k_lap3_grad_direct(int nsrc, const double* __restrict__ src, const double* __restrict__ q,
+                   int ntgt, const double* __restrict__ tgt, double* __restrict__ grad)
+{
+  __shared__ double s_y[3][GS], s_q[GS];
+  int t = blockIdx.x * GT + threadIdx.x;
+  bool active = t < ntgt;
+  double x[3] = {0, 0, 0};
+  if (active)
+    for (int d = 0; d < 3; ++d) x[d] = tgt[(size_t)d * ntgt + t];
+  double g0 = 0.0, g1 = 0.0, g2 = 0.0;
+  for (int base = 0; base < nsrc; base += GS) {
+    int cnt = min(GS, nsrc - base);
+    __syncthreads();
+    for (int j = threadIdx.x; j < cnt; j += GT) {
+      for (int d = 0; d < 3; ++d) s_y[d][j] = src[(size_t)d * nsrc + base + j];
+      s_q[j] = q[base + j];
+    }
+    __syncthreads();
+    if (active) {
+      for (int j = 0; j < cnt; ++j) {
+        double dx = x[0] - s_y[0][j], dy = x[1] - s_y[1][j], dz = x[2] - s_y[2][j];
+        double r2 = dx * dx + dy * dy + dz * dz;
+        if (r2 == 0.0) continue;
+        double ri = rsqrt(r2);
+        double f = s_q[j] * ri * ri * ri;
+        g0 = fma(f, dx, g0);
+        g1 = fma(f, dy, g1);
+        g2 = fma(f, dz, g2);
+      }
+    }
+  }
+  if (active) {
+    const double c = -0.079577471545947667884;   // -1 / (4 pi)
+    grad[t] = c * g0;
+    grad[(size_t)ntgt + t] = c * g1;
+    grad[2 * (size_t)ntgt + t] = c * g2;
+  }
+}
+
+}  // namespace
+
+}  // namespace qbx
+
+extern "C" int qbxfmm_laplace3d_grad_direct(int nsources, const double* sources,
+                                            const double* charges, int ntargets,
+                                            const double* targets, double* grad, void* stream)
+{
+  if (nsources < 0 || ntargets < 0 || (nsources > 0 && (!sources || !charges)) ||
+      (ntargets > 0 && (!targets || !grad)))
+    return qbx::set_last_error(QBXFMM_ERR_ARG, "qbxfmm_laplace3d_grad_direct: bad arguments");
+  if (ntargets == 0) return QBXFMM_OK;
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  qbx::k_lap3_grad_direct<<<(ntargets + qbx::GT - 1) / qbx::GT, qbx::GT, 0, st>>>(
+      nsources, sources, charges, ntargets, targets, grad);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess)
+    return qbx::set_last_error(QBXFMM_ERR_CUDA, std::string("qbxfmm_laplace3d_grad_direct: ") +
+                                                    cudaGetErrorString(e));
+  return QBXFMM_OK;
+}

@@ -47,8 +47,13 @@ _STAGES = {
 }
 
 # every symbol include/qbxfmm_api.h declares
+# entries that take no plan
+_FREE = {
+    "qbxfmm_laplace3d_grad_direct": [_int, _vp, _vp, _int, _vp, _vp, _vp],
+}
+
 EXPORTED_SYMBOLS = ["qbxfmm_version", "qbxfmm_last_error", "qbxfmm_plan_create",
-                    "qbxfmm_plan_destroy", *_STAGES]
+                    "qbxfmm_plan_destroy", *_STAGES, *_FREE]
 
 
 class QBXFMMError(RuntimeError):
@@ -77,6 +82,10 @@ def lib():
     for name, args in _STAGES.items():
         f = getattr(L, name)
         f.argtypes = [_vp, *args]
+        f.restype = _int
+    for name, args in _FREE.items():
+        f = getattr(L, name)
+        f.argtypes = args
         f.restype = _int
     _lib = L
     return L

@@ -142,3 +142,36 @@ def helmholtz3d_ellipsoid(nrefine: int = 5, k: float = 10.0, nrhs: int = 16, see
     return Workload(f"3D Helmholtz k={k:g} {op}, ellipsoid icosphere-{nrefine} "
                     f"({d.nelements} tri), {nrhs} rhs", d, targets, dens, spec, qbx_order,
                     fmm_order, seed)
+
+
+@dataclass
+class AdjointWorkload:
+    """3D Laplace single layer at far targets with a least-squares loss
+    J = 0.5 || S sigma - g ||^2 (g: field of point charges inside the ellipsoid)."""
+    discr: Discretization
+    targets: np.ndarray        # (3, nt) on the sphere of radius 3
+    sigma: np.ndarray          # (ndofs,)
+    charges: np.ndarray        # (3, nc) unit point charges
+    qbx_order: int
+    fmm_order: int
+    seed: int
+
+    def g(self, x):
+        """Field of the unit point charges, 1/(4 pi |x - c|), at x (3, n)."""
+        d = x[:, :, None] - self.charges[:, None, :]
+        return (1.0 / (4 * np.pi * np.sqrt((d ** 2).sum(0)))).sum(1)
+
+
+def laplace3d_adjoint(nrefine: int = 4, ntargets: int = 5000, ncharges: int = 8, seed: int = 0,
+                      qbx_order: int = 4, fmm_order: int = 12) -> AdjointWorkload:
+    """Ellipsoid (1, 1.5, 2) from an icosphere refined ``nrefine`` times (order-4
+    nodes), sigma = N(0, 1), targets uniform on the sphere of radius 3, g from
+    ``ncharges`` unit charges uniform in the ball of radius 0.5."""
+    rng = np.random.default_rng(seed)
+    d = make_ellipsoid(nrefine)
+    sigma = rng.normal(size=d.ndofs)
+    v = rng.normal(size=(3, ntargets))
+    v /= np.linalg.norm(v, axis=0)
+    c = rng.normal(size=(3, ncharges))
+    c *= 0.5 * rng.uniform(size=ncharges) ** (1 / 3) / np.linalg.norm(c, axis=0)
+    return AdjointWorkload(d, 3.0 * v, sigma, c, qbx_order, fmm_order, seed)
