@@ -34,6 +34,7 @@ struct qbxfmm_plan {
   bool tf32_ok;                            // split-TF32 translation matrices in use
   std::vector<double> h3gaunt;             // Gaunt table, [(nu,mu)][j][(n,m)]
   std::vector<int32_t> m2l_waves;          // runs of M2L classes with one offset (3D Helmholtz)
+  std::vector<double> h3rot;               // rotation tables, after the Gaunt table
   // 3D Helmholtz: translation buffer and pair scratch registered by
   // qbxfmm_precompute_translations, used by the translation stage entries
   mutable const double* trans_dev = nullptr;
@@ -135,6 +136,46 @@ std::vector<double> h3_gaunt_table(int p)
           }
         }
   return G;
+}
+
+// Wigner small-d tables for the rotation-based point-to-box translations, for
+// m in [-p, p], mu in [-q, q] (index (m + p) (2q + 1) + mu + q):
+//   start[4 idx]     = sign x sqrt(factorial ratio) of the single surviving term of
+//                      Wigner's formula at n0 = max(|m|, |mu|), and the exponents of
+//                      cos(beta/2) and sin(beta/2);
+//   rec[3 (idx (p+1) + n)] = (c1, c2, c3) with
+//                      d^{n+1} = (c1 cos(beta) - c2) d^n - c3 d^{n-1}   (n >= 1),
+// the three-term recurrence of d^n_{m mu}(beta) in n.
+std::vector<double> h3_rotation_tables(int p, int q)
+{
+  const int nm = 2 * p + 1, nmu = 2 * q + 1;
+  std::vector<double> t((size_t)nm * nmu * 4 + (size_t)nm * nmu * (p + 1) * 3, 0.0);
+  double* start = t.data();
+  double* rec = start + (size_t)nm * nmu * 4;
+  for (int m = -p; m <= p; ++m)
+    for (int mu = -q; mu <= q; ++mu) {
+      size_t idx = (size_t)(m + p) * nmu + (mu + q);
+      int j = std::max(std::abs(m), std::abs(mu));
+      int kk = std::max(0, mu - m);
+      int a1 = j + mu - kk, a3 = j - kk - m, a4 = kk - mu + m;
+      double lf = 0.5 * (std::lgamma(j + m + 1.0) + std::lgamma(j - m + 1.0) +
+                         std::lgamma(j + mu + 1.0) + std::lgamma(j - mu + 1.0)) -
+                  (std::lgamma(a1 + 1.0) + std::lgamma(kk + 1.0) + std::lgamma(a3 + 1.0) +
+                   std::lgamma(a4 + 1.0));
+      start[4 * idx] = (((kk - mu + m) & 1) ? -1.0 : 1.0) * std::exp(lf);
+      start[4 * idx + 1] = 2 * j + mu - m - 2 * kk;
+      start[4 * idx + 2] = 2 * kk - mu + m;
+      for (int n = std::max(j, 1); n < p; ++n) {
+        double a = n * std::sqrt(((n + 1.0) * (n + 1.0) - (double)m * m) *
+                                 ((n + 1.0) * (n + 1.0) - (double)mu * mu));
+        double b = (n + 1.0) * std::sqrt(((double)n * n - (double)m * m) * ((double)n * n - (double)mu * mu));
+        double* r = rec + 3 * (idx * (p + 1) + n);
+        r[0] = (2.0 * n + 1.0) * n * (n + 1.0) / a;
+        r[1] = (2.0 * n + 1.0) * (double)m * mu / a;
+        r[2] = b / a;
+      }
+    }
+  return t;
 }
 
 #define QBX_TRY(expr, where)                         \
@@ -242,6 +283,7 @@ int qbxfmm_plan_create(const qbxfmm_kernel* kernel, const qbxfmm_geometry* geome
   }
   if (p->h3) {
     p->h3gaunt = h3_gaunt_table(k.fmm_order);
+    p->h3rot = h3_rotation_tables(k.fmm_order, k.qbx_order);
     std::vector<int32_t> off(3 * (size_t)g.m2l_nclasses);
     if (g.m2l_nclasses > 0)
       e = cudaMemcpy(off.data(), g.m2l_class_offsets, sizeof(int32_t) * off.size(),
@@ -518,6 +560,7 @@ int qbxfmm_translate_box_multipoles_to_qbx_local(const qbxfmm_plan* p, const voi
       return fail(QBXFMM_ERR_ARG, "3D Helmholtz: call qbxfmm_precompute_translations first");
     QBX_TRY(h3_launch_m2qbxl(p->geo, p->hc, p->kern.fmm_order, p->kern.qbx_order, p->kern.nrhs,
                              (const double2*)mpoles, p->trans_dev + p->tc.nmatrices * p->tc.rp * p->tc.kp,
+                             p->trans_dev + p->tc.nmatrices * p->tc.rp * p->tc.kp + p->h3gaunt.size(),
                              (double2*)qbx_exps, error_word, S(stream)),
             "translate_box_multipoles_to_qbx_local");
     return QBXFMM_OK;
@@ -546,6 +589,7 @@ int qbxfmm_translate_box_local_to_qbx_local(const qbxfmm_plan* p, const void* lo
       return fail(QBXFMM_ERR_ARG, "3D Helmholtz: call qbxfmm_precompute_translations first");
     QBX_TRY(h3_launch_l2qbxl(p->geo, p->hc, p->kern.fmm_order, p->kern.qbx_order, p->kern.nrhs,
                              (const double2*)locals, p->trans_dev + p->tc.nmatrices * p->tc.rp * p->tc.kp,
+                             p->trans_dev + p->tc.nmatrices * p->tc.rp * p->tc.kp + p->h3gaunt.size(),
                              (double2*)qbx_exps, nullptr, S(stream)),
             "translate_box_local_to_qbx_local");
     return QBXFMM_OK;
@@ -644,7 +688,7 @@ int qbxfmm_workspace_sizes(const qbxfmm_plan* p, size_t* sizes6 /* 8 entries */)
                                cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return cuda_check(e, "workspace_sizes");
     npairs = std::max(npairs, g.m2m_npairs);
-    sizes6[6] = trans_matrix_bytes(p->tc) + p->h3gaunt.size() * sizeof(double) +
+    sizes6[6] = trans_matrix_bytes(p->tc) + (p->h3gaunt.size() + p->h3rot.size()) * sizeof(double) +
                 (p->tf32_ok ? tf32_matrix_bytes(p->tc) : 0);
     sizes6[7] = p->h3 ? 0 : trans_scratch_bytes(p->tc, npairs, p->kern.nrhs);
   } else {
@@ -665,6 +709,9 @@ int qbxfmm_precompute_translations(const qbxfmm_plan* p, const qbxfmm_workspace*
     QBX_TRY(cudaMemcpyAsync(G, p->h3gaunt.data(), p->h3gaunt.size() * sizeof(double),
                             cudaMemcpyHostToDevice, S(stream)),
             "precompute_translations: Gaunt table");
+    QBX_TRY(cudaMemcpyAsync(G + p->h3gaunt.size(), p->h3rot.data(), p->h3rot.size() * sizeof(double),
+                            cudaMemcpyHostToDevice, S(stream)),
+            "precompute_translations: rotation tables");
     QBX_TRY(h3_launch_trans_build(p->geo, p->tc, p->kern.k_re, G, T, S(stream)),
             "precompute_translations");
     p->trans_dev = T;

@@ -766,204 +766,83 @@ k_h3_p2qbxl(qbxfmm_geometry g, HelmCoeffs hc, int nrhs, const double2* __restric
   }
 }
 
-// Box expansion (order pf) -> QBX local (order q) at a center, by the addition theorem
-// with the Gaunt table (layout [(nu,mu) out][j][(n,m) in], l = |n - nu| + 2 j).
-// H3_E2Q_ZS CTAs per chunk of <= 32 centers of one target box (split over the
-// centers), RB densities per CTA.  M2QBXL
-// (FROM_LOCAL = false): the CTA runs over the target box's list-3 boxes, staging each
-// multipole (times s_s^n i^-n) for the RB densities in shared memory; L2QBXL: the one
-// box is the target box itself (local times s_b^-n i^-n).  For each (center, box) the
-// warp owning the center builds w_l^lam = 4 pi i^l f_l(k|b|) Y_l^lam(b) (f = h or j),
-// then, per output coefficient (nu, mu), the operator row
-//   c_{nu mu; n m} = sum_j G w_{l, m - mu}   (all (n, m), lanes split the row)
-// once and applies it to the RB staged expansions: lane = (density, part of the row),
-// a shuffle reduction over the parts, and the result (times i^nu s_t^nu) added into the
-// center's expansion.  Every center belongs to one CTA, so the additions need no atomics.
-constexpr int H3_E2Q_ZS = 4;             // CTAs sharing one chunk (split over its centers)
+// M2QBXL (list-3 multipoles) and L2QBXL (own box's local) into the QBX local of order
+// Q at a center, by rotation: rotate the frame so that the translation vector b lies
+// on the z axis, translate coaxially, rotate back,
+//   c(b) = R_back(-beta, alpha) . coax(|b|) . R(beta, alpha),
+// with, for the orthonormal harmonics without the Condon-Shortley phase,
+//   rotated coefficients  M'_{n mu} = sum_m e^{i m alpha} eps_m eps_mu d^n_{m mu}(beta) M_{n m},
+//   coaxial coefficients  c^mu_{nu n} = 4 pi sum_l i^{nu + l - n} f_l(k|b|) Y_l^0(z) G(n,mu; nu,mu; l),
+//   back rotation         L_{nu mu''} = e^{-i mu'' alpha} sum_mu eps_mu eps_mu'' d^nu_{mu mu''}(-beta) L'_{nu mu},
+// (d: Wigner's small-d matrices, eps_m = (-1)^m for m > 0, else 1; beta, alpha the
+// polar and azimuthal angles of b).  Equal in exact arithmetic to the Gaunt sum
+// c_{nu mu; n m}(b) of the file comment; only |mu| <= Q of the rotated source
+// coefficients are needed, so the work per (center, box) pair is O(pf^2 Q) per
+// density instead of O(pf^2 Q^2).  d^n_{m mu} for fixed (m, mu) by the three-term
+// recurrence in n (Jacobi polynomials), started at n0 = max(|m|, |mu|) from the single
+// surviving term of Wigner's formula; start values and recurrence coefficients come
+// precomputed (rot tables, built with the Gaunt table).
+// One warp per center (H3_ROT_ZS CTAs x 4 warps per chunk of <= 32 centers), RB
+// densities per CTA staged in shared memory per box; per (center, box) the warp
+// builds the rotation and coaxial tables in its shared slice; lane tasks are
+// (mu, density) for the rotation + coaxial step and (output, density) for the back
+// rotation, whose results stay in registers across the boxes.
+constexpr int H3_ROT_ZS = 8;
 
-template <bool FROM_LOCAL, int RB>
+template <bool FROM_LOCAL, int Q, int RB>
 __global__ void __launch_bounds__(NT)
-k_h3_e2qbxl(qbxfmm_geometry g, HelmCoeffs hc, int pf, int q, int nrhs,
-            const double2* __restrict__ exps, const double* __restrict__ gaunt,
-            double2* __restrict__ qbx_exps, int32_t* err)
+k_h3_e2qbxl_rot(qbxfmm_geometry g, HelmCoeffs hc, int pf, int nrhs,
+                const double2* __restrict__ exps, const double* __restrict__ gaunt,
+                const double* __restrict__ rot, double2* __restrict__ qbx_exps, int32_t* err)
 {
-  constexpr int NPART = 32 / RB;          // lanes per density
+  constexpr int NCQ = (Q + 1) * (Q + 1);
+  constexpr int NMU = 2 * Q + 1;
+  constexpr int NOUT = (NCQ * RB + 31) / 32;
   extern __shared__ double2 smem2[];
-  __shared__ short2 s_nm[(H3_LMAX + 1) * (H3_LMAX + 1)];
-  const int ncf = (pf + 1) * (pf + 1), ncq = (q + 1) * (q + 1);
-  const int L = pf + q;
-  const int nw = (L + 1) * (L + 1);
-  const int nrec = (L + 1) * (L + 2) / 2;
+  const int ncf = (pf + 1) * (pf + 1);
+  const int L = pf + Q;
   const int nl = pf + 1;
-  const int per = ncf + nw + (L + 2);
-  double2* rec = smem2;                                          // [nrec]
-  double2* Es = rec + nrec;                                      // [ncf][RB]
-  double2* Rw = Es + (size_t)ncf * RB + (size_t)(threadIdx.x >> 5) * per;
-  double2* row = Rw;                                             // [ncf]
-  double2* Wt = Rw + ncf;                                        // [nw]
-  double2* rad = Wt + nw;                                        // [L + 2]
+  const int nm = 2 * pf + 1;
+  const int TS = ncf + 1;                                    // padded T row
+  const double* rstart = rot;                                 // [nm][NMU][4]
+  const double* rrec = rot + (size_t)nm * NMU * 4;            // [nm][NMU][pf+1][3]
+  // CTA-wide
+  double2* Es = smem2;                                        // [ncf][RB]
+  // (both double arrays padded to an even length: the per-warp slices that follow hold
+  // double2 and must stay 16-byte aligned)
+  double* G0 = reinterpret_cast<double*>(Es + (size_t)ncf * RB);   // [NCQ][Q+1][nl]
+  double* spow = G0 + (((size_t)NCQ * (Q + 1) * nl + 1) & ~(size_t)1);   // [nl]: s_box^{+-n}
+  double2* wbase = reinterpret_cast<double2*>(spow + ((nl + 1) & ~1));
+  // per warp
+  const size_t per = (size_t)NMU * TS / 2 + (size_t)NMU * NCQ / 2 + 1 + (size_t)NCQ * nl +
+                     (size_t)NCQ * RB + (L + 2) + nm;
   int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  int rr = lane / NPART, part = lane - rr * NPART;
-  h3_rec_table(L, rec, threadIdx.x, NT);
-  for (int e = threadIdx.x; e < ncf; e += NT) {
-    int n, m;
-    hq_decode(e, n, m);
-    s_nm[e] = make_short2((short)n, (short)m);
+  double2* wb = wbase + (size_t)warp * per;
+  double* T = reinterpret_cast<double*>(wb);                 // [NMU][TS]
+  double* Tb = T + (size_t)NMU * TS;                          // [NMU][NCQ]
+  double2* coax = wb + (size_t)NMU * TS / 2 + (size_t)NMU * NCQ / 2 + 1;    // [NCQ][nl]
+  double2* Lp = coax + (size_t)NCQ * nl;                      // [NCQ][RB]
+  double2* rad = Lp + (size_t)NCQ * RB;                       // [L + 2]
+  double2* ph = rad + (L + 2);                                // [nm]: e^{i m alpha}, m = -pf..pf
+
+  __syncthreads();
+  // lambda = 0 slice of the Gaunt table: G0[o][j][n] = G(n,mu; nu,mu; |n - nu| + 2 j)
+  for (int x = threadIdx.x; x < NCQ * (Q + 1) * nl; x += NT) {
+    int o = x / ((Q + 1) * nl), rem = x - o * (Q + 1) * nl;
+    int j = rem / nl, n = rem - j * nl;
+    int nu = (int)sqrt((double)o);
+    while ((nu + 1) * (nu + 1) <= o) ++nu;
+    while (nu * nu > o) --nu;
+    int mu = o - nu * nu - nu;
+    G0[x] = (n >= abs(mu) && j <= min(n, nu)) ? __ldg(gaunt + ((size_t)o * nl + j) * ncf + hq(n, mu))
+                                             : 0.0;
   }
   __syncthreads();
   int chunk = blockIdx.x;
   int r0 = blockIdx.y * RB;
   int itb = g.qbx_chunk_target_box[chunk];
   int nctr = g.qbx_chunk_count[chunk];
-
-  int nbox;
-  if (FROM_LOCAL) nbox = 1;
-  else nbox = g.list3_starts[itb + 1] - g.list3_starts[itb];
-  for (int bi = 0; bi < nbox; ++bi) {
-    int sbx;
-    if (FROM_LOCAL) sbx = g.target_boxes[itb];
-    else sbx = g.list3_lists[g.list3_starts[itb] + bi];
-    if ((unsigned)sbx >= (unsigned)g.nboxes) {
-      report(err, QBX_DEVERR_BAD_BOX);
-      continue;
-    }
-    double cb[3];
-    load_point<3>(g.box_centers, g.nboxes, sbx, cb);
-    double sb = h3_scale(hc.k, level_width(g, g.box_levels[sbx]));
-    __syncthreads();
-    for (int e = threadIdx.x; e < ncf * RB; e += NT) {
-      int ei = e / RB, ri = e - ei * RB;
-      int n, m;
-      hq_decode(ei, n, m);
-      double2 v = c2(0.0);
-      if (r0 + ri < nrhs) {
-        v = exps[((size_t)sbx * nrhs + r0 + ri) * ncf + ei];
-        v = cscale(pow(sb, FROM_LOCAL ? -(double)n : (double)n), cmul(ipow(-n), v));
-      }
-      Es[e] = v;
-    }
-    __syncthreads();
-    for (int ci = blockIdx.z * NW + warp; ci < nctr; ci += NW * H3_E2Q_ZS) {
-      int ctr = g.centers_by_target_box[g.qbx_chunk_start[chunk] + ci];
-      if ((unsigned)ctr >= (unsigned)g.ncenters) {
-        report(err, QBX_DEVERR_BAD_CENTER);
-        continue;
-      }
-      double cc[3];
-      load_point<3>(g.centers, g.ncenters, ctr, cc);
-      double bv[3] = {cc[0] - cb[0], cc[1] - cb[1], cc[2] - cb[2]};
-      double2 w;
-      double rr_;
-      double t = h3_dir(bv, w, rr_);
-      if (lane == 0) {
-        if (FROM_LOCAL) {
-          double jv[H3_LMAX + 2];
-          h3_sph_j(L, hc.k * rr_, jv);
-          for (int l = 0; l <= L; ++l) rad[l] = c2(jv[l]);
-        } else {
-          h3_sph_h(L, hc.k * rr_, rad);
-        }
-        for (int l = 0; l <= L; ++l) rad[l] = cmul(cscale(FOUR_PI, ipow(l)), rad[l]);
-      }
-      __syncwarp();
-      for (int m = lane; m <= L; m += 32) h3_wave_column(m, L, t, w, rec, rad, Wt, 1);
-      __syncwarp();
-      double st = h3_scale(hc.k, g.expansion_radii[ctr]);
-      for (int o = 0; o < ncq; ++o) {
-        int nu, mu;
-        hq_decode(o, nu, mu);
-        // operator row c_{o, e}, e = (n, m)
-        for (int e = lane; e < ncf; e += 32) {
-          short2 nm = s_nm[e];
-          int n = nm.x, m = nm.y;
-          int lam = m - mu, lbase = abs(n - nu), jmax = min(n, nu);
-          const double* G = gaunt + (size_t)o * nl * ncf + e;
-          double2 tt = c2(0.0);
-          for (int j = 0; j <= jmax; ++j) {
-            int l = lbase + 2 * j;
-            if (abs(lam) <= l) tt = caxpy(G[(size_t)j * ncf], Wt[hq(l, lam)], tt);
-          }
-          row[e] = tt;
-        }
-        __syncwarp();
-        double2 a0 = c2(0.0), a1 = c2(0.0), a2 = c2(0.0), a3 = c2(0.0);
-        int e = part;
-        for (; e + 3 * NPART < ncf; e += 4 * NPART) {
-          a0 = cfma(row[e], Es[e * RB + rr], a0);
-          a1 = cfma(row[e + NPART], Es[(e + NPART) * RB + rr], a1);
-          a2 = cfma(row[e + 2 * NPART], Es[(e + 2 * NPART) * RB + rr], a2);
-          a3 = cfma(row[e + 3 * NPART], Es[(e + 3 * NPART) * RB + rr], a3);
-        }
-        for (; e < ncf; e += NPART) a0 = cfma(row[e], Es[e * RB + rr], a0);
-        double2 a = cadd(cadd(a0, a1), cadd(a2, a3));
-#pragma unroll
-        for (int off = NPART / 2; off > 0; off >>= 1) {
-          a.x += __shfl_xor_sync(0xffffffffu, a.x, off);
-          a.y += __shfl_xor_sync(0xffffffffu, a.y, off);
-        }
-        if (part == 0 && r0 + rr < nrhs) {
-          a = cscale(pow(st, (double)nu), cmul(ipow(nu), a));
-          double2* out = qbx_exps + ((size_t)ctr * nrhs + r0 + rr) * ncq + o;
-          *out = cadd(*out, a);
-        }
-        __syncwarp();
-      }
-    }
-  }
-}
-
-// The same translations for RB >= 4 densities with the operator applied on the FP64
-// tensor cores.  One warp per center (H3_MMA_ZS CTAs x 4 warps cover a chunk of <= 32
-// centers); per (center, box) the warp builds the operator rows c_{o, e} four at a time
-// and multiplies them into its register accumulators with mma.sync m8n8k4 f64, in the
-// real form [Cr; Ci] = [[Cr_op, -Ci_op], [Ci_op, Cr_op]] [Er; Ei]: an m-tile is four
-// complex rows (real parts in rows 0-3, imaginary parts in rows 4-7), K runs over the
-// real then the imaginary parts of the staged expansions, N over the densities.
-constexpr int H3_MMA_ZS = 8;
-constexpr int H3_MT_MAX = 9;        // m-tiles: ceil((q+1)^2 / 4), q <= 5
-
-QBX_D void dmma_f64(double& d0, double& d1, double a, double b)
-{
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
-               : "+d"(d0), "+d"(d1)
-               : "d"(a), "d"(b));
-}
-
-template <bool FROM_LOCAL, int RB>
-__global__ void __launch_bounds__(NT)
-k_h3_e2qbxl_mma(qbxfmm_geometry g, HelmCoeffs hc, int pf, int q, int nrhs,
-                const double2* __restrict__ exps, const double* __restrict__ gaunt,
-                double2* __restrict__ qbx_exps, int32_t* err)
-{
-  constexpr int NTN = (RB + 7) / 8;
-  extern __shared__ double2 smem2[];
-  __shared__ short2 s_nm[(H3_LMAX + 1) * (H3_LMAX + 1)];
-  const int ncf = (pf + 1) * (pf + 1), ncq = (q + 1) * (q + 1);
-  const int L = pf + q;
-  const int nw = (L + 1) * (L + 1);
-  const int nrec = (L + 1) * (L + 2) / 2;
-  const int nl = pf + 1;
-  const int nmt = (ncq + 3) / 4;
-  const int K2 = 2 * ncf, Kp = (K2 + 3) / 4 * 4;
-  const int per = nw + (L + 2) + 4 * ncf;
-  double2* rec = smem2;                                          // [nrec]
-  double2* Es = rec + nrec;                                      // [ncf][RB]
-  double2* Wt = Es + (size_t)ncf * RB + (size_t)(threadIdx.x >> 5) * per;   // [nw]
-  double2* rad = Wt + nw;                                        // [L + 2]
-  double2* rows = rad + (L + 2);                                 // [4][ncf]
-  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  int gq = lane >> 2, tq = lane & 3;
-  h3_rec_table(L, rec, threadIdx.x, NT);
-  for (int e = threadIdx.x; e < ncf; e += NT) {
-    int n, m;
-    hq_decode(e, n, m);
-    s_nm[e] = make_short2((short)n, (short)m);
-  }
-  __syncthreads();   // s_nm and rec are read below, also when there is no box
-  int chunk = blockIdx.x;
-  int r0 = blockIdx.y * RB;
-  int itb = g.qbx_chunk_target_box[chunk];
-  int nctr = g.qbx_chunk_count[chunk];
+  if (blockIdx.z * NW >= nctr) return;     // the whole CTA is idle
   int ci = blockIdx.z * NW + warp;
   bool has = ci < nctr;
   int ctr = has ? g.centers_by_target_box[g.qbx_chunk_start[chunk] + ci] : 0;
@@ -972,14 +851,11 @@ k_h3_e2qbxl_mma(qbxfmm_geometry g, HelmCoeffs hc, int pf, int q, int nrhs,
     has = false;
     ctr = 0;
   }
-  if (blockIdx.z * NW >= nctr) return;     // the whole CTA is idle
   double cc[3];
   load_point<3>(g.centers, g.ncenters, ctr, cc);
-  double acc[H3_MT_MAX][NTN][2];
+  double2 acc[NOUT];
 #pragma unroll
-  for (int i = 0; i < H3_MT_MAX; ++i)
-#pragma unroll
-    for (int j = 0; j < NTN; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+  for (int i = 0; i < NOUT; ++i) acc[i] = c2(0.0);
 
   int nbox = FROM_LOCAL ? 1 : g.list3_starts[itb + 1] - g.list3_starts[itb];
   for (int bi = 0; bi < nbox; ++bi) {
@@ -992,102 +868,156 @@ k_h3_e2qbxl_mma(qbxfmm_geometry g, HelmCoeffs hc, int pf, int q, int nrhs,
     load_point<3>(g.box_centers, g.nboxes, sbx, cb);
     double sb = h3_scale(hc.k, level_width(g, g.box_levels[sbx]));
     __syncthreads();
+    if (threadIdx.x == 0) {
+      double f = 1.0, fs = FROM_LOCAL ? 1.0 / sb : sb;
+      for (int n = 0; n < nl; ++n, f *= fs) spow[n] = f;
+    }
+    __syncthreads();
     for (int e = threadIdx.x; e < ncf * RB; e += NT) {
       int ei = e / RB, ri = e - ei * RB;
-      int n = s_nm[ei].x;
+      int n = (int)sqrt((double)ei);
+      while ((n + 1) * (n + 1) <= ei) ++n;
+      while (n * n > ei) --n;
       double2 v = c2(0.0);
-      if (r0 + ri < nrhs) {
-        v = exps[((size_t)sbx * nrhs + r0 + ri) * ncf + ei];
-        v = cscale(pow(sb, FROM_LOCAL ? -(double)n : (double)n), cmul(ipow(-n), v));
-      }
+      if (r0 + ri < nrhs) v = cscale(spow[n], exps[((size_t)sbx * nrhs + r0 + ri) * ncf + ei]);
       Es[e] = v;
     }
     __syncthreads();
     if (!has) continue;
+    // translation vector and its angles
     double bv[3] = {cc[0] - cb[0], cc[1] - cb[1], cc[2] - cb[2]};
-    double2 w;
-    double rr_;
-    double t = h3_dir(bv, w, rr_);
+    double bl = sqrt(bv[0] * bv[0] + bv[1] * bv[1] + bv[2] * bv[2]);
+    double cbeta = bl > 0.0 ? fmin(1.0, fmax(-1.0, bv[2] / bl)) : 1.0;
+    double alpha = (bv[0] == 0.0 && bv[1] == 0.0) ? 0.0 : atan2(bv[1], bv[0]);
+    double beta = acos(cbeta);
+    double ch = cos(0.5 * beta), sh = sin(0.5 * beta);
     if (lane == 0) {
       if (FROM_LOCAL) {
         double jv[H3_LMAX + 2];
-        h3_sph_j(L, hc.k * rr_, jv);
+        h3_sph_j(L, hc.k * bl, jv);
         for (int l = 0; l <= L; ++l) rad[l] = c2(jv[l]);
       } else {
-        h3_sph_h(L, hc.k * rr_, rad);
+        h3_sph_h(L, hc.k * bl, rad);
       }
-      for (int l = 0; l <= L; ++l) rad[l] = cmul(cscale(FOUR_PI, ipow(l)), rad[l]);
+      // 4 pi Y_l^0(z) i^l f_l, Y_l^0(z) = sqrt((2l+1)/(4 pi))
+      for (int l = 0; l <= L; ++l) rad[l] = cmul(cscale(sqrt(FOUR_PI * (2.0 * l + 1.0)), ipow(l)), rad[l]);
+    }
+    for (int m = lane; m < nm; m += 32) {
+      double sn, cs;
+      sincos((m - pf) * alpha, &sn, &cs);
+      ph[m] = c2(cs, sn);
+    }
+    // rotation tables: T[(mu+Q)][hq(n,m)] = eps_m eps_mu d^n_{m mu}(beta) (n >= n0),
+    // Tb[(mu+Q)][hq(nu,mu2)] = eps_mu eps_mu2 d^nu_{mu mu2}(-beta), nu <= Q
+    for (int task = lane; task < nm * NMU + NMU * NMU; task += 32) {
+      bool back = task >= nm * NMU;
+      int m, mu, nmax;
+      double sgn_s = 1.0;
+      if (!back) {
+        m = task / NMU - pf;
+        mu = task % NMU - Q;
+        nmax = pf;
+      } else {
+        int t2 = task - nm * NMU;
+        m = t2 / NMU - Q;      // first index: mu of the rotated local
+        mu = t2 % NMU - Q;     // second index: mu'' of the output
+        nmax = Q;
+        sgn_s = -1.0;          // sin(-beta/2) = -sin(beta/2)
+      }
+      int n0 = max(abs(m), abs(mu));
+      if (n0 > nmax) continue;
+      size_t idx = (size_t)(m + pf) * NMU + (mu + Q);
+      double v = __ldg(rstart + 4 * idx);
+      int ec = (int)__ldg(rstart + 4 * idx + 1), es = (int)__ldg(rstart + 4 * idx + 2);
+      for (int u = 0; u < ec; ++u) v *= ch;
+      for (int u = 0; u < es; ++u) v *= sgn_s * sh;
+      double epsw = ((m > 0 && (m & 1)) ? -1.0 : 1.0) * ((mu > 0 && (mu & 1)) ? -1.0 : 1.0);
+      double prev = 0.0, cur = v;
+      const double* rc = rrec + 3 * idx * (pf + 1);
+      for (int n = n0; n <= nmax; ++n) {
+        if (!back) T[(mu + Q) * TS + hq(n, m)] = epsw * cur;
+        else Tb[(m + Q) * NCQ + hq(n, mu)] = epsw * cur;
+        if (n == nmax) break;
+        double nxt;
+        if (n == 0) {
+          nxt = cbeta * cur;
+        } else {
+          const double* c3 = rc + 3 * n;
+          nxt = fma(fma(__ldg(c3), cbeta, -__ldg(c3 + 1)), cur, -__ldg(c3 + 2) * prev);
+        }
+        prev = cur;
+        cur = nxt;
+      }
     }
     __syncwarp();
-    for (int m = lane; m <= L; m += 32) h3_wave_column(m, L, t, w, rec, rad, Wt, 1);
-    __syncwarp();
-#pragma unroll
-    for (int mt = 0; mt < H3_MT_MAX; ++mt) {
-      if (mt >= nmt) break;
-      // four operator rows o = 4 mt + rl into rows[rl][e]
-      for (int x = lane; x < 4 * ncf; x += 32) {
-        int rl = x / ncf, e = x - rl * ncf;
-        int o = 4 * mt + rl;
-        double2 tt = c2(0.0);
-        if (o < ncq) {
-          int nu = s_nm[o].x, mu = s_nm[o].y;
-          short2 nm = s_nm[e];
-          int n = nm.x, m = nm.y;
-          int lam = m - mu, lbase = abs(n - nu), jmax = min(n, nu);
-          const double* G = gaunt + (size_t)o * nl * ncf + e;
-          for (int j = 0; j <= jmax; ++j) {
-            int l = lbase + 2 * j;
-            if (abs(lam) <= l) tt = caxpy(G[(size_t)j * ncf], Wt[hq(l, lam)], tt);
-          }
-        }
-        rows[x] = tt;
+    // coaxial coefficients coax[hq(nu,mu)][n] = i^{nu-n} sum_j G(nu,mu; j; n,mu) rad[l]
+    for (int x = lane; x < NCQ * nl; x += 32) {
+      int o = x / nl, n = x - o * nl;
+      int nu = (int)sqrt((double)o);
+      while ((nu + 1) * (nu + 1) <= o) ++nu;
+      while (nu * nu > o) --nu;
+      int mu = o - nu * nu - nu;
+      double2 tt = c2(0.0);
+      if (n >= abs(mu)) {
+        const double* G = G0 + (size_t)o * (Q + 1) * nl + n;
+        int lbase = abs(n - nu), jmax = min(n, nu);
+        for (int j = 0; j <= jmax; ++j) tt = caxpy(G[j * nl], rad[lbase + 2 * j], tt);
+        tt = cmul(ipow(nu - n + 4 * pf), tt);
       }
-      __syncwarp();
-      const double2* rrow = rows + (gq & 3) * ncf;
-      const bool imrow = gq >= 4;
-      for (int k0 = 0; k0 < Kp; k0 += 4) {
-        int k = k0 + tq;
-        double a = 0.0;
-        bool lo = k < ncf;
-        int e = lo ? k : k - ncf;
-        if (k < K2) {
-          double2 c = rrow[e];
-          a = imrow ? (lo ? c.y : c.x) : (lo ? c.x : -c.y);
-        }
-#pragma unroll
-        for (int nt = 0; nt < NTN; ++nt) {
-          int col = nt * 8 + gq;
-          double b = 0.0;
-          if (k < K2 && col < RB) {
-            double2 ev = Es[e * RB + col];
-            b = lo ? ev.x : ev.y;
-          }
-          dmma_f64(acc[mt][nt][0], acc[mt][nt][1], a, b);
-        }
-      }
-      __syncwarp();
+      coax[x] = tt;
     }
+    __syncwarp();
+    // rotate (only |mu| <= Q) and translate coaxially: lane task (mu, density)
+    for (int task = lane; task < NMU * RB; task += 32) {
+      int mu = task / RB - Q, r = task - (task / RB) * RB;
+      int amu = abs(mu);
+      double2 lacc[Q + 1];
+#pragma unroll
+      for (int nu = 0; nu <= Q; ++nu) lacc[nu] = c2(0.0);
+      const double* Tm = T + (mu + Q) * TS;
+      for (int n = amu; n <= pf; ++n) {
+        double2 mr = c2(0.0);
+        int base = n * n + n;
+        for (int m = -n; m <= n; ++m)
+          mr = cfma(cscale(Tm[base + m], ph[m + pf]), Es[(base + m) * RB + r], mr);
+#pragma unroll
+        for (int nu = 0; nu <= Q; ++nu)
+          if (nu >= amu) lacc[nu] = cfma(coax[hq(nu, mu) * nl + n], mr, lacc[nu]);
+      }
+#pragma unroll
+      for (int nu = 0; nu <= Q; ++nu)
+        if (nu >= amu) Lp[hq(nu, mu) * RB + r] = lacc[nu];
+    }
+    __syncwarp();
+    // rotate back into the register outputs: lane task (o = (nu, mu2), density)
+#pragma unroll
+    for (int i = 0; i < NOUT; ++i) {
+      int task = lane + 32 * i;
+      if (task >= NCQ * RB) break;
+      int o = task / RB, r = task - o * RB;
+      int nu = (int)sqrt((double)o);
+      while ((nu + 1) * (nu + 1) <= o) ++nu;
+      while (nu * nu > o) --nu;
+      int mu2 = o - nu * nu - nu;
+      double2 a = c2(0.0);
+      for (int mu = -nu; mu <= nu; ++mu) a = caxpy(Tb[(mu + Q) * NCQ + o], Lp[hq(nu, mu) * RB + r], a);
+      acc[i] = cfma(cconj(ph[mu2 + pf]), a, acc[i]);
+    }
+    __syncwarp();
   }
   if (!has) return;
-  // C'[row gq][col nt*8 + 2 tq + v]: rows 0-3 real, 4-7 imaginary parts of o = 4 mt + (gq & 3)
   double st = h3_scale(hc.k, g.expansion_radii[ctr]);
 #pragma unroll
-  for (int mt = 0; mt < H3_MT_MAX; ++mt) {
-    if (mt >= nmt) break;
-#pragma unroll
-    for (int nt = 0; nt < NTN; ++nt)
-#pragma unroll
-      for (int v = 0; v < 2; ++v) {
-        double im = __shfl_down_sync(0xffffffffu, acc[mt][nt][v], 16);
-        int o = 4 * mt + gq;
-        int col = nt * 8 + 2 * tq + v;
-        if (gq < 4 && o < ncq && col < RB && r0 + col < nrhs) {
-          int nu = s_nm[o].x;
-          double2 a = cscale(pow(st, (double)nu), cmul(ipow(nu), c2(acc[mt][nt][v], im)));
-          double2* out = qbx_exps + ((size_t)ctr * nrhs + r0 + col) * ncq + o;
-          *out = cadd(*out, a);
-        }
-      }
+  for (int i = 0; i < NOUT; ++i) {
+    int task = lane + 32 * i;
+    if (task >= NCQ * RB) break;
+    int o = task / RB, r = task - o * RB;
+    if (r0 + r >= nrhs) continue;
+    int nu = (int)sqrt((double)o);
+    while ((nu + 1) * (nu + 1) <= o) ++nu;
+    while (nu * nu > o) --nu;
+    double2* out = qbx_exps + ((size_t)ctr * nrhs + r0 + r) * NCQ + o;
+    *out = caxpy(pow(st, (double)nu), acc[i], *out);
   }
 }
 
@@ -1511,66 +1441,77 @@ cudaError_t h3_launch_tsqbx(const qbxfmm_geometry& g, HelmCoeffs hc, int q, int 
   }
 }
 
-static size_t e2qbxl_smem(int pf, int q, int rb)
+template <bool FROM_LOCAL, int Q, int RB>
+static size_t h3_rot_smem(int pf)
 {
-  int ncf = (pf + 1) * (pf + 1), L = pf + q;
-  size_t nrec = (size_t)(L + 1) * (L + 2) / 2;
-  size_t per = (size_t)ncf + (size_t)(L + 1) * (L + 1) + (L + 2);
-  return (nrec + (size_t)ncf * rb + NW * per) * sizeof(double2);
+  constexpr int NCQ = (Q + 1) * (Q + 1), NMU = 2 * Q + 1;
+  int ncf = (pf + 1) * (pf + 1), L = pf + Q, nl = pf + 1, nm = 2 * pf + 1;
+  size_t per = (size_t)NMU * (ncf + 1) / 2 + (size_t)NMU * NCQ / 2 + 1 + (size_t)NCQ * nl +
+               (size_t)NCQ * RB + (L + 2) + nm;
+  size_t cta = (size_t)ncf * RB * sizeof(double2) +
+               (((size_t)NCQ * (Q + 1) * nl + 1) & ~(size_t)1) * sizeof(double) +
+               ((nl + 1) & ~1) * sizeof(double);
+  return cta + NW * per * sizeof(double2);
 }
 
-template <bool FROM_LOCAL, int RB>
-static cudaError_t h3_e2qbxl_rb(const qbxfmm_geometry& g, HelmCoeffs hc, int pf, int q, int nrhs,
-                                const double2* e, const double* gaunt, double2* qe, int32_t* err,
-                                cudaStream_t st)
+template <bool FROM_LOCAL, int Q, int RB>
+static cudaError_t h3_rot_launch(const qbxfmm_geometry& g, HelmCoeffs hc, int pf, int nrhs,
+                                 const double2* e, const double* gaunt, const double* rot,
+                                 double2* qe, int32_t* err, cudaStream_t st)
 {
-  size_t sh = e2qbxl_smem(pf, q, RB);
-  cudaFuncSetAttribute(k_h3_e2qbxl<FROM_LOCAL, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)sh);
-  dim3 grid(g.nqbx_chunks, (nrhs + RB - 1) / RB, H3_E2Q_ZS);
-  k_h3_e2qbxl<FROM_LOCAL, RB><<<grid, NT, sh, st>>>(g, hc, pf, q, nrhs, e, gaunt, qe, err);
+  size_t sh = h3_rot_smem<FROM_LOCAL, Q, RB>(pf);
+  cudaFuncSetAttribute(k_h3_e2qbxl_rot<FROM_LOCAL, Q, RB>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+  dim3 grid(g.nqbx_chunks, (nrhs + RB - 1) / RB, H3_ROT_ZS);
+  k_h3_e2qbxl_rot<FROM_LOCAL, Q, RB><<<grid, NT, sh, st>>>(g, hc, pf, nrhs, e, gaunt, rot, qe, err);
   return cudaGetLastError();
 }
 
-template <bool FROM_LOCAL, int RB>
-static cudaError_t h3_e2qbxl_mma_rb(const qbxfmm_geometry& g, HelmCoeffs hc, int pf, int q,
-                                    int nrhs, const double2* e, const double* gaunt, double2* qe,
-                                    int32_t* err, cudaStream_t st)
+// densities per CTA: the largest of 8, 4, 2, 1 that fits the shared memory
+template <bool FROM_LOCAL, int Q>
+static cudaError_t h3_rot_q(const qbxfmm_geometry& g, HelmCoeffs hc, int pf, int nrhs,
+                            const double2* e, const double* gaunt, const double* rot, double2* qe,
+                            int32_t* err, cudaStream_t st)
 {
-  int ncf = (pf + 1) * (pf + 1), L = pf + q;
-  size_t nrec = (size_t)(L + 1) * (L + 2) / 2;
-  size_t per = (size_t)(L + 1) * (L + 1) + (L + 2) + 4 * (size_t)ncf;
-  size_t sh = (nrec + (size_t)ncf * RB + NW * per) * sizeof(double2);
-  cudaFuncSetAttribute(k_h3_e2qbxl_mma<FROM_LOCAL, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)sh);
-  dim3 grid(g.nqbx_chunks, (nrhs + RB - 1) / RB, H3_MMA_ZS);
-  k_h3_e2qbxl_mma<FROM_LOCAL, RB><<<grid, NT, sh, st>>>(g, hc, pf, q, nrhs, e, gaunt, qe, err);
-  return cudaGetLastError();
+  const size_t lim = 220 * 1024;
+  if (nrhs >= 8 && h3_rot_smem<FROM_LOCAL, Q, 8>(pf) <= lim)
+    return h3_rot_launch<FROM_LOCAL, Q, 8>(g, hc, pf, nrhs, e, gaunt, rot, qe, err, st);
+  if (nrhs >= 4 && h3_rot_smem<FROM_LOCAL, Q, 4>(pf) <= lim)
+    return h3_rot_launch<FROM_LOCAL, Q, 4>(g, hc, pf, nrhs, e, gaunt, rot, qe, err, st);
+  if (nrhs >= 2 && h3_rot_smem<FROM_LOCAL, Q, 2>(pf) <= lim)
+    return h3_rot_launch<FROM_LOCAL, Q, 2>(g, hc, pf, nrhs, e, gaunt, rot, qe, err, st);
+  return h3_rot_launch<FROM_LOCAL, Q, 1>(g, hc, pf, nrhs, e, gaunt, rot, qe, err, st);
 }
 
 template <bool FROM_LOCAL>
 static cudaError_t h3_e2qbxl(const qbxfmm_geometry& g, HelmCoeffs hc, int pf, int q, int nrhs,
-                             const double2* e, const double* gaunt, double2* qe, int32_t* err,
-                             cudaStream_t st)
+                             const double2* e, const double* gaunt, const double* rot, double2* qe,
+                             int32_t* err, cudaStream_t st)
 {
   if (g.nqbx_chunks == 0) return cudaSuccess;
-  if (nrhs == 1) return h3_e2qbxl_rb<FROM_LOCAL, 1>(g, hc, pf, q, nrhs, e, gaunt, qe, err, st);
-  if (nrhs <= 8) return h3_e2qbxl_mma_rb<FROM_LOCAL, 8>(g, hc, pf, q, nrhs, e, gaunt, qe, err, st);
-  return h3_e2qbxl_mma_rb<FROM_LOCAL, 16>(g, hc, pf, q, nrhs, e, gaunt, qe, err, st);
+  switch (q) {
+    case 0: return h3_rot_q<FROM_LOCAL, 0>(g, hc, pf, nrhs, e, gaunt, rot, qe, err, st);
+    case 1: return h3_rot_q<FROM_LOCAL, 1>(g, hc, pf, nrhs, e, gaunt, rot, qe, err, st);
+    case 2: return h3_rot_q<FROM_LOCAL, 2>(g, hc, pf, nrhs, e, gaunt, rot, qe, err, st);
+    case 3: return h3_rot_q<FROM_LOCAL, 3>(g, hc, pf, nrhs, e, gaunt, rot, qe, err, st);
+    case 4: return h3_rot_q<FROM_LOCAL, 4>(g, hc, pf, nrhs, e, gaunt, rot, qe, err, st);
+    case 5: return h3_rot_q<FROM_LOCAL, 5>(g, hc, pf, nrhs, e, gaunt, rot, qe, err, st);
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 cudaError_t h3_launch_m2qbxl(const qbxfmm_geometry& g, HelmCoeffs hc, int pf, int q, int nrhs,
-                             const double2* mp, const double* gaunt, double2* qe, int32_t* err,
-                             cudaStream_t st)
+                             const double2* mp, const double* gaunt, const double* rot,
+                             double2* qe, int32_t* err, cudaStream_t st)
 {
-  return h3_e2qbxl<false>(g, hc, pf, q, nrhs, mp, gaunt, qe, err, st);
+  return h3_e2qbxl<false>(g, hc, pf, q, nrhs, mp, gaunt, rot, qe, err, st);
 }
 
 cudaError_t h3_launch_l2qbxl(const qbxfmm_geometry& g, HelmCoeffs hc, int pf, int q, int nrhs,
-                             const double2* lo, const double* gaunt, double2* qe, int32_t* err,
-                             cudaStream_t st)
+                             const double2* lo, const double* gaunt, const double* rot,
+                             double2* qe, int32_t* err, cudaStream_t st)
 {
-  return h3_e2qbxl<true>(g, hc, pf, q, nrhs, lo, gaunt, qe, err, st);
+  return h3_e2qbxl<true>(g, hc, pf, q, nrhs, lo, gaunt, rot, qe, err, st);
 }
 
 cudaError_t h3_launch_qbxl2p(const qbxfmm_geometry& g, HelmCoeffs hc, int q, int nrhs,
