@@ -39,6 +39,18 @@ struct qbxfmm_plan {
   // qbxfmm_precompute_translations, used by the translation stage entries
   mutable const double* trans_dev = nullptr;
   mutable double* scratch_dev = nullptr;
+  // qbxfmm_apply runs the independent branches of the stage graph on two side
+  // streams joined back into the caller's stream by events (fork/join, also
+  // under stream capture): near field + M2P, and P2L
+  cudaStream_t side[2] = {nullptr, nullptr};
+  cudaEvent_t ev_fork = nullptr, ev_mpoles = nullptr, ev_near = nullptr, ev_p2l = nullptr;
+  ~qbxfmm_plan()
+  {
+    for (cudaStream_t s : side)
+      if (s) cudaStreamDestroy(s);
+    for (cudaEvent_t e : {ev_fork, ev_mpoles, ev_near, ev_p2l})
+      if (e) cudaEventDestroy(e);
+  }
 };
 
 namespace {
@@ -308,6 +320,7 @@ int qbxfmm_plan_create(const qbxfmm_kernel* kernel, const qbxfmm_geometry* geome
     if (e == cudaSuccess) {
       for (int c = 0; c < g.m2l_nclasses; ++c)
         p->th.m2l_max_pairs = std::max(p->th.m2l_max_pairs, cs[c + 1] - cs[c]);
+      p->th.m2l_npairs = cs[g.m2l_nclasses];
       for (int lev = 0; lev < g.nlevels; ++lev)
         for (int ci = 0; ci < nch; ++ci) {
           int gi = lev * nch + ci;
@@ -317,6 +330,10 @@ int qbxfmm_plan_create(const qbxfmm_kernel* kernel, const qbxfmm_geometry* geome
       p->th.lvl_source_parent = p->lvl_source_parent.data();
     }
   }
+  for (int i = 0; i < 2 && e == cudaSuccess; ++i)
+    e = cudaStreamCreateWithFlags(&p->side[i], cudaStreamNonBlocking);
+  for (cudaEvent_t* ev : {&p->ev_fork, &p->ev_mpoles, &p->ev_near, &p->ev_p2l})
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
   if (e != cudaSuccess) {
     delete p;
     return cuda_check(e, "qbxfmm_plan_create");
@@ -683,11 +700,7 @@ int qbxfmm_workspace_sizes(const qbxfmm_plan* p, size_t* sizes6 /* 8 entries */)
   sizes6[4] = nr * (size_t)(g.nfiltered_targets > 0 ? g.nfiltered_targets : 1) * scal;
   sizes6[5] = nr * (size_t)g.ntargets * scal;
   if (p->trans_ok) {
-    int npairs = 0;
-    cudaError_t e = cudaMemcpy(&npairs, g.m2l_class_starts + g.m2l_nclasses, sizeof(int32_t),
-                               cudaMemcpyDeviceToHost);
-    if (e != cudaSuccess) return cuda_check(e, "workspace_sizes");
-    npairs = std::max(npairs, g.m2m_npairs);
+    int npairs = std::max(p->th.m2l_npairs, g.m2m_npairs);
     sizes6[6] = trans_matrix_bytes(p->tc) + (p->h3gaunt.size() + p->h3rot.size()) * sizeof(double) +
                 (p->tf32_ok ? tf32_matrix_bytes(p->tc) : 0);
     sizes6[7] = p->h3 ? 0 : trans_scratch_bytes(p->tc, npairs, p->kern.nrhs);
@@ -755,65 +768,122 @@ int qbxfmm_apply(const qbxfmm_plan* p, const qbxfmm_upsample* up, const qbxfmm_w
   QBX_TRY(cudaMemsetAsync(ws->pot_tree, 0, sz[5], st), "apply: clear");
   if (ws->error_word) QBX_TRY(cudaMemsetAsync(ws->error_word, 0, sizeof(int32_t), st), "apply: clear");
   int rc;
-  // drive_fmm order (fmm.py:436-588)
-  if ((rc = qbxfmm_form_strengths(p, up, density, ws->strengths, stream))) return rc;
-  if ((rc = qbxfmm_form_multipoles(p, ws->strengths, ws->mpoles, stream))) return rc;
   const uint32_t* T32 = (gemm && p->tf32_ok)
                             ? reinterpret_cast<const uint32_t*>((const double*)ws->translations +
                                                                 trans_matrix_bytes(p->tc) / sizeof(double))
                             : nullptr;
-  if (T32)
-    QBX_TRY(launch_m2m_gemm_mixed(p->geo, p->th, p->tc, p->kern.nrhs, T32, (double2*)ws->mpoles,
-                                  (double*)ws->pair_scratch, ws->error_word, S(stream)),
-            "coarsen_multipoles (split TF32)");
-  else if (gemm)
-    QBX_TRY(launch_m2m_gemm(p->geo, p->th, p->tc, p->kern.nrhs,
-                            (const double*)ws->translations, (double2*)ws->mpoles,
-                            (double*)ws->pair_scratch, ws->error_word, S(stream)),
-            "coarsen_multipoles (matrix form)");
-  else if ((rc = qbxfmm_coarsen_multipoles(p, ws->mpoles, stream)))
-    return rc;
-  if ((rc = qbxfmm_eval_direct(p, ws->strengths, ws->pot_nonqbx, ws->error_word, stream))) return rc;
-  if (T32)
-    QBX_TRY(launch_m2l_gemm_mixed(p->geo, p->th, p->tc, p->kern.nrhs, T32, (const double2*)ws->mpoles,
-                                  (double2*)ws->locals, (double*)ws->pair_scratch, ws->error_word,
-                                  S(stream)),
-            "multipole_to_local (split TF32)");
-  else if (gemm)
-    QBX_TRY(launch_m2l_gemm(p->geo, p->th, p->tc, p->kern.nrhs,
-                            (const double*)ws->translations, (const double2*)ws->mpoles,
-                            (double2*)ws->locals, (double*)ws->pair_scratch, ws->error_word,
-                            S(stream)),
-            "multipole_to_local (matrix form)");
-  else if ((rc = qbxfmm_multipole_to_local(p, ws->mpoles, ws->locals, ws->error_word, stream)))
-    return rc;
-  if ((rc = qbxfmm_eval_multipoles(p, ws->mpoles, ws->pot_nonqbx, ws->error_word, stream))) return rc;
-  if ((rc = qbxfmm_form_locals(p, ws->strengths, ws->locals, ws->error_word, stream))) return rc;
-  if (T32)
-    QBX_TRY(launch_l2l_gemm_mixed(p->geo, p->th, p->tc, p->kern.nrhs, T32, (double2*)ws->locals,
-                                  ws->error_word, S(stream)),
-            "refine_locals (split TF32)");
-  else if (gemm)
-    QBX_TRY(launch_l2l_gemm(p->geo, p->th, p->tc, p->kern.nrhs,
-                            (const double*)ws->translations, (double2*)ws->locals, ws->error_word,
-                            S(stream)),
-            "refine_locals (matrix form)");
-  else if ((rc = qbxfmm_refine_locals(p, ws->locals, stream)))
-    return rc;
-  if ((rc = qbxfmm_eval_locals(p, ws->locals, ws->pot_nonqbx, stream))) return rc;
+  auto m2m = [&]() -> int {
+    if (T32)
+      QBX_TRY(launch_m2m_gemm_mixed(p->geo, p->th, p->tc, p->kern.nrhs, T32, (double2*)ws->mpoles,
+                                    (double*)ws->pair_scratch, ws->error_word, st),
+              "coarsen_multipoles (split TF32)");
+    else if (gemm)
+      QBX_TRY(launch_m2m_gemm(p->geo, p->th, p->tc, p->kern.nrhs, (const double*)ws->translations,
+                              (double2*)ws->mpoles, (double*)ws->pair_scratch, ws->error_word, st),
+              "coarsen_multipoles (matrix form)");
+    else
+      return qbxfmm_coarsen_multipoles(p, ws->mpoles, stream);
+    return QBXFMM_OK;
+  };
+  auto m2l = [&]() -> int {
+    if (T32)
+      QBX_TRY(launch_m2l_gemm_mixed(p->geo, p->th, p->tc, p->kern.nrhs, T32,
+                                    (const double2*)ws->mpoles, (double2*)ws->locals,
+                                    (double*)ws->pair_scratch, ws->error_word, st),
+              "multipole_to_local (split TF32)");
+    else if (gemm)
+      QBX_TRY(launch_m2l_gemm(p->geo, p->th, p->tc, p->kern.nrhs, (const double*)ws->translations,
+                              (const double2*)ws->mpoles, (double2*)ws->locals,
+                              (double*)ws->pair_scratch, ws->error_word, st),
+              "multipole_to_local (matrix form)");
+    else
+      return qbxfmm_multipole_to_local(p, ws->mpoles, ws->locals, ws->error_word, stream);
+    return QBXFMM_OK;
+  };
+  auto l2l = [&]() -> int {
+    if (T32)
+      QBX_TRY(launch_l2l_gemm_mixed(p->geo, p->th, p->tc, p->kern.nrhs, T32, (double2*)ws->locals,
+                                    ws->error_word, st),
+              "refine_locals (split TF32)");
+    else if (gemm)
+      QBX_TRY(launch_l2l_gemm(p->geo, p->th, p->tc, p->kern.nrhs, (const double*)ws->translations,
+                              (double2*)ws->locals, ws->error_word, st),
+              "refine_locals (matrix form)");
+    else
+      return qbxfmm_refine_locals(p, ws->locals, stream);
+    return QBXFMM_OK;
+  };
+  // The stage graph of drive_fmm (fmm.py:436-588) on three streams.  Every buffer
+  // that several stages add into is written by one stream at a time:
+  //   caller's stream: strengths, P2M, M2M | M2QBXL, M2L, L2L | L2P, L2QBXL, QBXL2P,
+  //                    assembly
+  //   side[0]:         P2P, target-specific near field (or P2QBXL) | M2P
+  //   side[1]:         P2L
+  // with events: fork after the strengths; M2P waits for M2M; M2L waits for P2L
+  // (both add into the locals); L2P / QBXL2P wait for side[0] (pot_nonqbx,
+  // pot_tree; every stage adds into its outputs, so the order of the writers of one
+  // buffer does not matter, only that they do not overlap).  Without the
+  // target-specific near field, P2QBXL (side[0]) and M2QBXL both add into the QBX
+  // expansions, so M2QBXL moves after that join.
+  void* s1 = p->side[0];
+  void* s2 = p->side[1];
+  cudaStream_t side1 = p->side[0], side2 = p->side[1];
   const bool tsqbx = p->kern.target_specific_qbx != 0;
+  bool forked = false;
+  // on an error, join the side streams before returning, so that a stream capture
+  // of the caller's stream stays well formed
+  auto join = [&](int code) -> int {
+    if (forked) {
+      cudaEventRecord(p->ev_near, side1);
+      cudaEventRecord(p->ev_p2l, side2);
+      cudaStreamWaitEvent(st, p->ev_near, 0);
+      cudaStreamWaitEvent(st, p->ev_p2l, 0);
+    }
+    return code;
+  };
+#define QBX_STEP(call)                  \
+  do {                                  \
+    if ((rc = (call))) return join(rc); \
+  } while (0)
+#define QBX_CUDA_STEP(call, what)                            \
+  do {                                                       \
+    if ((rc = cuda_check((call), what))) return join(rc);   \
+  } while (0)
+  if ((rc = qbxfmm_form_strengths(p, up, density, ws->strengths, stream))) return rc;
+  QBX_CUDA_STEP(cudaEventRecord(p->ev_fork, st), "apply: fork");
+  QBX_CUDA_STEP(cudaStreamWaitEvent(side1, p->ev_fork, 0), "apply: fork");
+  QBX_CUDA_STEP(cudaStreamWaitEvent(side2, p->ev_fork, 0), "apply: fork");
+  forked = true;
+  QBX_STEP(qbxfmm_form_locals(p, ws->strengths, ws->locals, ws->error_word, s2));
+  QBX_CUDA_STEP(cudaEventRecord(p->ev_p2l, side2), "apply: P2L event");
+  QBX_STEP(qbxfmm_eval_direct(p, ws->strengths, ws->pot_nonqbx, ws->error_word, s1));
+  if (tsqbx)
+    QBX_STEP(qbxfmm_eval_target_specific_qbx_locals(p, ws->strengths, ws->pot_tree, ws->error_word, s1));
+  else
+    QBX_STEP(qbxfmm_form_global_qbx_locals(p, ws->strengths, ws->qbx_exps, ws->error_word, s1));
+  QBX_STEP(qbxfmm_form_multipoles(p, ws->strengths, ws->mpoles, stream));
+  QBX_STEP(m2m());
+  QBX_CUDA_STEP(cudaEventRecord(p->ev_mpoles, st), "apply: multipole event");
+  QBX_CUDA_STEP(cudaStreamWaitEvent(side1, p->ev_mpoles, 0), "apply: multipole event");
+  QBX_STEP(qbxfmm_eval_multipoles(p, ws->mpoles, ws->pot_nonqbx, ws->error_word, s1));
+  QBX_CUDA_STEP(cudaEventRecord(p->ev_near, side1), "apply: near-field event");
+  if (tsqbx)
+    QBX_STEP(qbxfmm_translate_box_multipoles_to_qbx_local(p, ws->mpoles, ws->qbx_exps,
+                                                          ws->error_word, stream));
+  QBX_CUDA_STEP(cudaStreamWaitEvent(st, p->ev_p2l, 0), "apply: join P2L");
+  QBX_STEP(m2l());
+  QBX_STEP(l2l());
+  QBX_CUDA_STEP(cudaStreamWaitEvent(st, p->ev_near, 0), "apply: join near field");
+  forked = false;
   if (!tsqbx &&
-      (rc = qbxfmm_form_global_qbx_locals(p, ws->strengths, ws->qbx_exps, ws->error_word, stream)))
-    return rc;
-  if ((rc = qbxfmm_translate_box_multipoles_to_qbx_local(p, ws->mpoles, ws->qbx_exps,
+      (rc = qbxfmm_translate_box_multipoles_to_qbx_local(p, ws->mpoles, ws->qbx_exps,
                                                          ws->error_word, stream)))
     return rc;
+#undef QBX_STEP
+#undef QBX_CUDA_STEP
+  if ((rc = qbxfmm_eval_locals(p, ws->locals, ws->pot_nonqbx, stream))) return rc;
   if ((rc = qbxfmm_translate_box_local_to_qbx_local(p, ws->locals, ws->qbx_exps, stream))) return rc;
   if ((rc = qbxfmm_eval_qbx_expansions(p, ws->qbx_exps, ws->pot_tree, stream))) return rc;
-  if (tsqbx &&
-      (rc = qbxfmm_eval_target_specific_qbx_locals(p, ws->strengths, ws->pot_tree,
-                                                   ws->error_word, stream)))
-    return rc;
   return qbxfmm_assemble(p, ws->pot_nonqbx, ws->pot_tree, out, stream);
 }
 

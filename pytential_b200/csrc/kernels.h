@@ -10,6 +10,7 @@ namespace qbx {
 // host-side sizes for the translation-matrix kernels, filled at plan creation
 struct TransHost {
   int m2l_max_pairs = 0;                 // largest M2L class
+  int m2l_npairs = 0;                    // all M2L pairs (pair-scratch rows)
   int m2m_level_max_group[64] = {0};     // largest (level, child position) group per level
   int l2l_level_max_group[64] = {0};
   const int32_t* lvl_source_parent = nullptr;   // host copy (owned by the plan)

@@ -820,7 +820,8 @@ k_h2_qbxl2p(qbxfmm_geometry g, HelmCoeffs hc, int nrhs, const double2* __restric
         f *= rinv;
       }
     }
-    pot_tree[(size_t)r * g.ntargets + t] = acc;
+    double2* P = pot_tree + (size_t)r * g.ntargets + t;
+    *P = cadd(*P, acc);
   }
 }
 

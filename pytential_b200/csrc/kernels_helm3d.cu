@@ -1043,7 +1043,8 @@ k_h3_qbxl2p(qbxfmm_geometry g, HelmCoeffs hc, int q, int nrhs, const double2* __
     int t = g.center_to_targets_lists[it];
     double x[3];
     load_point<3>(g.targets, g.ntargets, t, x);
-    pot_tree[(size_t)r * g.ntargets + t] = h3_e2p(Lc, q, true, hc.k, s, cc, x, rec);
+    double2* P = pot_tree + (size_t)r * g.ntargets + t;
+    *P = cadd(*P, h3_e2p(Lc, q, true, hc.k, s, cc, x, rec));
   }
 }
 

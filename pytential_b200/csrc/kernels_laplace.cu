@@ -1560,7 +1560,7 @@ k_qbxl2p(qbxfmm_geometry g, int nrhs, const double2* __restrict__ qbx_exps,
       }
       acc = s.x;
     }
-    pot_tree[(size_t)r * g.ntargets + t] = acc;
+    pot_tree[(size_t)r * g.ntargets + t] += acc;
   }
 }
 
