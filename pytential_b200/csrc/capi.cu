@@ -39,16 +39,18 @@ struct qbxfmm_plan {
   // qbxfmm_precompute_translations, used by the translation stage entries
   mutable const double* trans_dev = nullptr;
   mutable double* scratch_dev = nullptr;
-  // qbxfmm_apply runs the independent branches of the stage graph on two side
+  // qbxfmm_apply runs the independent branches of the stage graph on three side
   // streams joined back into the caller's stream by events (fork/join, also
-  // under stream capture): near field + M2P, and P2L
-  cudaStream_t side[2] = {nullptr, nullptr};
-  cudaEvent_t ev_fork = nullptr, ev_mpoles = nullptr, ev_near = nullptr, ev_p2l = nullptr;
+  // under stream capture): near field + M2P; P2L; P2QBXL + M2QBXL (the longest
+  // branch, on a high-priority stream)
+  cudaStream_t side[3] = {nullptr, nullptr, nullptr};
+  cudaEvent_t ev_fork = nullptr, ev_mpoles = nullptr, ev_near = nullptr, ev_p2l = nullptr,
+              ev_qbx = nullptr;
   ~qbxfmm_plan()
   {
     for (cudaStream_t s : side)
       if (s) cudaStreamDestroy(s);
-    for (cudaEvent_t e : {ev_fork, ev_mpoles, ev_near, ev_p2l})
+    for (cudaEvent_t e : {ev_fork, ev_mpoles, ev_near, ev_p2l, ev_qbx})
       if (e) cudaEventDestroy(e);
   }
 };
@@ -330,9 +332,12 @@ int qbxfmm_plan_create(const qbxfmm_kernel* kernel, const qbxfmm_geometry* geome
       p->th.lvl_source_parent = p->lvl_source_parent.data();
     }
   }
-  for (int i = 0; i < 2 && e == cudaSuccess; ++i)
-    e = cudaStreamCreateWithFlags(&p->side[i], cudaStreamNonBlocking);
-  for (cudaEvent_t* ev : {&p->ev_fork, &p->ev_mpoles, &p->ev_near, &p->ev_p2l})
+  int prio_least = 0, prio_greatest = 0;
+  if (e == cudaSuccess) e = cudaDeviceGetStreamPriorityRange(&prio_least, &prio_greatest);
+  for (int i = 0; i < 3 && e == cudaSuccess; ++i)
+    e = cudaStreamCreateWithPriority(&p->side[i], cudaStreamNonBlocking,
+                                     i == 2 ? prio_greatest : prio_least);
+  for (cudaEvent_t* ev : {&p->ev_fork, &p->ev_mpoles, &p->ev_near, &p->ev_p2l, &p->ev_qbx})
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
   if (e != cudaSuccess) {
     delete p;
@@ -813,21 +818,21 @@ int qbxfmm_apply(const qbxfmm_plan* p, const qbxfmm_upsample* up, const qbxfmm_w
       return qbxfmm_refine_locals(p, ws->locals, stream);
     return QBXFMM_OK;
   };
-  // The stage graph of drive_fmm (fmm.py:436-588) on three streams.  Every buffer
+  // The stage graph of drive_fmm (fmm.py:436-588) on four streams.  Every buffer
   // that several stages add into is written by one stream at a time:
-  //   caller's stream: strengths, P2M, M2M | M2QBXL, M2L, L2L | L2P, L2QBXL, QBXL2P,
-  //                    assembly
-  //   side[0]:         P2P, target-specific near field (or P2QBXL) | M2P
+  //   caller's stream: strengths, P2M, M2M | M2L, L2L | L2P | L2QBXL, QBXL2P, assembly
+  //   side[0]:         P2P, target-specific near field | M2P
   //   side[1]:         P2L
-  // with events: fork after the strengths; M2P waits for M2M; M2L waits for P2L
-  // (both add into the locals); L2P / QBXL2P wait for side[0] (pot_nonqbx,
-  // pot_tree; every stage adds into its outputs, so the order of the writers of one
-  // buffer does not matter, only that they do not overlap).  Without the
-  // target-specific near field, P2QBXL (side[0]) and M2QBXL both add into the QBX
-  // expansions, so M2QBXL moves after that join.
+  //   side[2]:         P2QBXL | M2QBXL
+  // with events: fork after the strengths; M2P and M2QBXL wait for M2M; M2L waits
+  // for P2L (both add into the locals); L2P and QBXL2P wait for side[0]
+  // (pot_nonqbx, pot_tree); L2QBXL waits for side[2] (the QBX expansions).  Every
+  // stage adds into its outputs, so the order of the writers of one buffer does not
+  // matter, only that they do not overlap.
   void* s1 = p->side[0];
   void* s2 = p->side[1];
-  cudaStream_t side1 = p->side[0], side2 = p->side[1];
+  void* s3 = p->side[2];
+  cudaStream_t side1 = p->side[0], side2 = p->side[1], side3 = p->side[2];
   const bool tsqbx = p->kern.target_specific_qbx != 0;
   bool forked = false;
   // on an error, join the side streams before returning, so that a stream capture
@@ -836,8 +841,10 @@ int qbxfmm_apply(const qbxfmm_plan* p, const qbxfmm_upsample* up, const qbxfmm_w
     if (forked) {
       cudaEventRecord(p->ev_near, side1);
       cudaEventRecord(p->ev_p2l, side2);
+      cudaEventRecord(p->ev_qbx, side3);
       cudaStreamWaitEvent(st, p->ev_near, 0);
       cudaStreamWaitEvent(st, p->ev_p2l, 0);
+      cudaStreamWaitEvent(st, p->ev_qbx, 0);
     }
     return code;
   };
@@ -851,37 +858,36 @@ int qbxfmm_apply(const qbxfmm_plan* p, const qbxfmm_upsample* up, const qbxfmm_w
   } while (0)
   if ((rc = qbxfmm_form_strengths(p, up, density, ws->strengths, stream))) return rc;
   QBX_CUDA_STEP(cudaEventRecord(p->ev_fork, st), "apply: fork");
-  QBX_CUDA_STEP(cudaStreamWaitEvent(side1, p->ev_fork, 0), "apply: fork");
-  QBX_CUDA_STEP(cudaStreamWaitEvent(side2, p->ev_fork, 0), "apply: fork");
+  for (cudaStream_t s : {side1, side2, side3})
+    QBX_CUDA_STEP(cudaStreamWaitEvent(s, p->ev_fork, 0), "apply: fork");
   forked = true;
   QBX_STEP(qbxfmm_form_locals(p, ws->strengths, ws->locals, ws->error_word, s2));
   QBX_CUDA_STEP(cudaEventRecord(p->ev_p2l, side2), "apply: P2L event");
   QBX_STEP(qbxfmm_eval_direct(p, ws->strengths, ws->pot_nonqbx, ws->error_word, s1));
-  if (tsqbx)
+  if (tsqbx) {
     QBX_STEP(qbxfmm_eval_target_specific_qbx_locals(p, ws->strengths, ws->pot_tree, ws->error_word, s1));
-  else
-    QBX_STEP(qbxfmm_form_global_qbx_locals(p, ws->strengths, ws->qbx_exps, ws->error_word, s1));
+  } else {
+    QBX_STEP(qbxfmm_form_global_qbx_locals(p, ws->strengths, ws->qbx_exps, ws->error_word, s3));
+  }
   QBX_STEP(qbxfmm_form_multipoles(p, ws->strengths, ws->mpoles, stream));
   QBX_STEP(m2m());
   QBX_CUDA_STEP(cudaEventRecord(p->ev_mpoles, st), "apply: multipole event");
+  QBX_CUDA_STEP(cudaStreamWaitEvent(side3, p->ev_mpoles, 0), "apply: multipole event");
+  QBX_STEP(qbxfmm_translate_box_multipoles_to_qbx_local(p, ws->mpoles, ws->qbx_exps,
+                                                        ws->error_word, s3));
+  QBX_CUDA_STEP(cudaEventRecord(p->ev_qbx, side3), "apply: QBX-expansion event");
   QBX_CUDA_STEP(cudaStreamWaitEvent(side1, p->ev_mpoles, 0), "apply: multipole event");
   QBX_STEP(qbxfmm_eval_multipoles(p, ws->mpoles, ws->pot_nonqbx, ws->error_word, s1));
   QBX_CUDA_STEP(cudaEventRecord(p->ev_near, side1), "apply: near-field event");
-  if (tsqbx)
-    QBX_STEP(qbxfmm_translate_box_multipoles_to_qbx_local(p, ws->mpoles, ws->qbx_exps,
-                                                          ws->error_word, stream));
   QBX_CUDA_STEP(cudaStreamWaitEvent(st, p->ev_p2l, 0), "apply: join P2L");
   QBX_STEP(m2l());
   QBX_STEP(l2l());
   QBX_CUDA_STEP(cudaStreamWaitEvent(st, p->ev_near, 0), "apply: join near field");
+  QBX_STEP(qbxfmm_eval_locals(p, ws->locals, ws->pot_nonqbx, stream));
+  QBX_CUDA_STEP(cudaStreamWaitEvent(st, p->ev_qbx, 0), "apply: join QBX expansions");
   forked = false;
-  if (!tsqbx &&
-      (rc = qbxfmm_translate_box_multipoles_to_qbx_local(p, ws->mpoles, ws->qbx_exps,
-                                                         ws->error_word, stream)))
-    return rc;
 #undef QBX_STEP
 #undef QBX_CUDA_STEP
-  if ((rc = qbxfmm_eval_locals(p, ws->locals, ws->pot_nonqbx, stream))) return rc;
   if ((rc = qbxfmm_translate_box_local_to_qbx_local(p, ws->locals, ws->qbx_exps, stream))) return rc;
   if ((rc = qbxfmm_eval_qbx_expansions(p, ws->qbx_exps, ws->pot_tree, stream))) return rc;
   return qbxfmm_assemble(p, ws->pot_nonqbx, ws->pot_tree, out, stream);

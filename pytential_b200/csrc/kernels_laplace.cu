@@ -1135,15 +1135,19 @@ k_p2qbxl(qbxfmm_geometry g, SourceCoeffs sc, int nrhs, const double* __restrict_
 }
 
 // M2QBXL (translate_box_multipoles_to_qbx_local, fmm.py:267-312;
-// interactions.py:196-235), all source levels in one launch.  CTA = 4 warps over
-// one chunk of <= 32 centers (lane = center); the warps split the list-3 boxes.
+// interactions.py:196-235), all source levels in one launch.  A cluster of MZ CTAs
+// x 4 warps per chunk of <= 32 centers (lane = center); the MZ * 4 warps split the
+// list-3 boxes, and the partial sums meet in CTA 0 of the cluster in a fixed order
+// (warps through shared memory, CTAs through distributed shared memory), so the
+// result does not depend on scheduling.  Splitting a chunk over MZ CTAs evens out
+// chunks with long list-3 runs.
 // 3D: each warp expands the source multipole into a zero-padded dense table
 // Mpad[k][l] (rows k in [-Q, pf+Q], columns l in [-(pf+2Q), pf+Q]); each lane runs the
 // singular-harmonic recurrence for its center column by column and scatters every
 // S_{n'}^{m'} into its register-resident coefficients (j, i) through
 // Mpad[n'-j][m'-i]: one broadcast shared load and one complex FMA per term, no
 // branches.
-template <int DIM, int Q>
+template <int DIM, int Q, int MZ>
 __global__ void __launch_bounds__(NT)
 k_m2qbxl(qbxfmm_geometry g, int pf, int ncf, int nrhs, const double2* __restrict__ mpoles,
          double2* __restrict__ qbx_exps, int32_t* err)
@@ -1157,8 +1161,10 @@ k_m2qbxl(qbxfmm_geometry g, int pf, int ncf, int nrhs, const double2* __restrict
   int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   double2* Mw = smem2 + (size_t)warp * MSZ;
   double2* red = smem2 + (size_t)NW * MSZ;   // [NW-1][32][NC]
+  double2* cpart = red + (NW - 1) * 32 * NC;  // [32][NC]: this CTA's sum (MZ > 1)
 
-  int chunk = blockIdx.x;
+  int chunk = blockIdx.x / MZ;
+  int zpart = blockIdx.x - chunk * MZ;
   int r = blockIdx.y;
   int itb = g.qbx_chunk_target_box[chunk];
   bool has_center = lane < g.qbx_chunk_count[chunk];
@@ -1178,7 +1184,7 @@ k_m2qbxl(qbxfmm_geometry g, int pf, int ncf, int nrhs, const double2* __restrict
   for (int i = 0; i < NC; ++i) acc[i] = c2(0.0);
 
   int l0 = g.list3_starts[itb], l1 = g.list3_starts[itb + 1];
-  for (int li = l0 + warp; li < l1; li += NW) {
+  for (int li = l0 + zpart * NW + warp; li < l1; li += MZ * NW) {
     int sb = g.list3_lists[li];
     if ((unsigned)sb >= (unsigned)g.nboxes) {
       report(err, QBX_DEVERR_BAD_BOX);
@@ -1186,11 +1192,17 @@ k_m2qbxl(qbxfmm_geometry g, int pf, int ncf, int nrhs, const double2* __restrict
     }
     __syncwarp();
     const double2* src = mpoles + ((size_t)sb * nrhs + r) * ncf;
+    double rho_s = level_width(g, g.box_levels[sb]);
     if (DIM == 3) {
+      // rows scaled by rho_s^k: with the harmonics taken at the unscaled offset
+      // c - c_s, the per-box factor rho_s^-(j+1) of the scaled form moves into the
+      // table and the boxes' terms add into acc directly
       for (int q = lane; q < ncf; q += 32) {
         int k, l;
         decode3(q, k, l);
-        double2 v = src[q];
+        double sc = 1.0;
+        for (int u = 0; u < k; ++u) sc *= rho_s;
+        double2 v = cscale(sc, src[q]);
         Mw[(k + Q) * MW + loff + l] = v;
         if (l > 0) Mw[(k + Q) * MW + loff - l] = (l & 1) ? c2(-v.x, v.y) : c2(v.x, -v.y);
       }
@@ -1199,18 +1211,14 @@ k_m2qbxl(qbxfmm_geometry g, int pf, int ncf, int nrhs, const double2* __restrict
     }
     __syncwarp();
     if (!has_center) continue;
-    double rho_s = level_width(g, g.box_levels[sb]);
     double cs[3];
     load_point<DIM>(g.box_centers, g.nboxes, sb, cs);
     double ratio = rho_t / rho_s;
     if (DIM == 3) {
-      double d0 = (cc[0] - cs[0]) / rho_s, d1 = (cc[1] - cs[1]) / rho_s,
-             d2 = (cc[2] - cs[2]) / rho_s;
+      double d0 = cc[0] - cs[0], d1 = cc[1] - cs[1], d2 = cc[2] - cs[2];
       double rinv2 = 1.0 / (d0 * d0 + d1 * d1 + d2 * d2);
       int nmax = pf + Q;
-      double2 part[NC];
-#pragma unroll
-      for (int i = 0; i < NC; ++i) part[i] = c2(0.0);
+      double2* part = acc;
       double2 mm = c2(sqrt(rinv2));
       for (int mp = 0; mp <= nmax; ++mp) {
         if (mp > 0) mm = cscale((2.0 * mp - 1) * rinv2, cmul(mm, c2(d0, d1)));
@@ -1240,14 +1248,6 @@ k_m2qbxl(qbxfmm_geometry g, int pf, int ncf, int nrhs, const double2* __restrict
           bpos += MW;
           bneg += MW;
         }
-      }
-      double rj = 1.0 / rho_s;
-#pragma unroll
-      for (int j = 0; j <= Q; ++j) {
-#pragma unroll
-        for (int ii = 0; ii <= j; ++ii)
-          acc[idx3(j, ii)] = caxpy((j & 1) ? -rj : rj, part[idx3(j, ii)], acc[idx3(j, ii)]);
-        rj *= ratio;
       }
     } else {
       const double2* M = Mw;
@@ -1292,14 +1292,41 @@ k_m2qbxl(qbxfmm_geometry g, int pf, int ncf, int nrhs, const double2* __restrict
     for (int i = 0; i < NC; ++i) red[((warp - 1) * 32 + lane) * NC + i] = acc[i];
   }
   __syncthreads();
-  if (warp == 0 && has_center) {
-    double2* out = qbx_exps + ((size_t)ctr * nrhs + r) * NC;
+  if (warp == 0) {
 #pragma unroll
-    for (int i = 0; i < NC; ++i) {
-      double2 a = acc[i];
-      for (int w = 1; w < NW; ++w) a = cadd(a, red[((w - 1) * 32 + lane) * NC + i]);
-      out[i] = cadd(out[i], a);
+    for (int i = 0; i < NC; ++i)
+      for (int w = 1; w < NW; ++w) acc[i] = cadd(acc[i], red[((w - 1) * 32 + lane) * NC + i]);
+  }
+  if (MZ > 1) {
+    cg::cluster_group cl = cg::this_cluster();
+    if (warp == 0) {
+#pragma unroll
+      for (int i = 0; i < NC; ++i) cpart[lane * NC + i] = acc[i];
     }
+    cl.sync();
+    if (zpart == 0 && warp == 0) {
+      for (unsigned q = 1; q < MZ; ++q) {
+        const double2* rp = cl.map_shared_rank(cpart, q) + lane * NC;
+#pragma unroll
+        for (int i = 0; i < NC; ++i) acc[i] = cadd(acc[i], rp[i]);
+      }
+    }
+    cl.sync();
+  }
+  if (zpart == 0 && warp == 0 && has_center) {
+    double2* out = qbx_exps + ((size_t)ctr * nrhs + r) * NC;
+    if (DIM == 3) {
+      // (-1)^j rho_t^j of the local coefficient of order j
+      double f = 1.0;
+#pragma unroll
+      for (int j = 0; j <= Q; ++j) {
+#pragma unroll
+        for (int ii = 0; ii <= j; ++ii) acc[idx3(j, ii)] = cscale(f, acc[idx3(j, ii)]);
+        f *= -rho_t;
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < NC; ++i) out[i] = cadd(out[i], acc[i]);
   }
 }
 
@@ -1761,6 +1788,9 @@ static cudaError_t p2qbxl_q(const qbxfmm_geometry& g, SourceCoeffs sc, int nrhs,
   return cudaGetLastError();
 }
 
+// CTAs per chunk in the 3D M2QBXL cluster launch
+constexpr int M2QBXL_Z = 4;
+
 template <int DIM, int Q>
 static cudaError_t m2qbxl_q(const qbxfmm_geometry& g, int pf, int nrhs, const double2* mp,
                             double2* qe, int32_t* err, cudaStream_t st)
@@ -1768,10 +1798,30 @@ static cudaError_t m2qbxl_q(const qbxfmm_geometry& g, int pf, int nrhs, const do
   int ncf = (int)ncoef_dim(DIM, pf);
   constexpr int NC = (DIM == 3) ? (Q + 1) * (Q + 2) / 2 : Q + 1;
   size_t msz = DIM == 3 ? (size_t)(pf + 2 * Q + 1) * (2 * pf + 3 * Q + 1) : (size_t)ncf;
-  size_t sh = (NW * msz + (size_t)(NW - 1) * 32 * NC) * sizeof(double2);
-  cudaFuncSetAttribute(k_m2qbxl<DIM, Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
-  k_m2qbxl<DIM, Q><<<dim3(g.nqbx_chunks, grid_y(nrhs)), NT, sh, st>>>(g, pf, ncf, nrhs, mp, qe, err);
-  return cudaGetLastError();
+  size_t sh = (NW * msz + (size_t)NW * 32 * NC) * sizeof(double2);
+  if constexpr (DIM == 2) {
+    cudaFuncSetAttribute(k_m2qbxl<DIM, Q, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+    k_m2qbxl<DIM, Q, 1><<<dim3(g.nqbx_chunks, grid_y(nrhs)), NT, sh, st>>>(g, pf, ncf, nrhs, mp, qe,
+                                                                          err);
+    return cudaGetLastError();
+  } else {
+  // 3D: clusters of M2QBXL_Z CTAs per chunk
+  constexpr int MZ = M2QBXL_Z;
+  cudaFuncSetAttribute(k_m2qbxl<DIM, Q, MZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(g.nqbx_chunks * MZ, grid_y(nrhs));
+  cfg.blockDim = dim3(NT);
+  cfg.dynamicSmemBytes = sh;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = MZ;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k_m2qbxl<DIM, Q, MZ>, g, pf, ncf, nrhs, mp, qe, err);
+  }
 }
 
 template <int DIM, int Q>
