@@ -64,9 +64,11 @@ def p2p_pairs(arrays: dict, scalars: dict) -> int:
 
 
 def apply_launch_count(scalars: dict, arrays: dict, matrices: bool = False,
-                       tsqbx: bool = False) -> int:
+                       tsqbx: bool = False, m2m_by_parent: bool = True) -> int:
     """Kernels of this library launched by one qbxfmm_apply (3D matrix-form
-    translations when ``matrices``; target-specific near field when ``tsqbx``)."""
+    translations when ``matrices``: M2M as one matrix-vector launch per level when
+    ``m2m_by_parent`` (the FP64 form), else products + reduction; target-specific
+    near field when ``tsqbx``)."""
     nl = scalars["nlevels"]
     lsp = arrays["level_start_source_parent_box_nrs"]
     lttp = arrays["level_start_ttp_box_nrs"]
@@ -79,7 +81,8 @@ def apply_launch_count(scalars: dict, arrays: dict, matrices: bool = False,
         for lev in range(nl - 1):
             if mg[(lev + 1) * nch] > mg[lev * nch]:
                 n += 1                                      # M2M products
-                n += lsp[lev + 1] > lsp[lev]                # M2M reduction
+                if not m2m_by_parent:
+                    n += lsp[lev + 1] > lsp[lev]            # M2M reduction
         n += 2 * (scalars["m2l_nclasses"] > 0)              # M2L products + reduction
         n += sum(1 for lev in range(1, nl) if lg[(lev + 1) * nch] > lg[lev * nch])  # L2L
     else:

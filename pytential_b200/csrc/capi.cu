@@ -329,6 +329,8 @@ int qbxfmm_plan_create(const qbxfmm_kernel* kernel, const qbxfmm_geometry* geome
           p->th.m2m_level_max_group[lev] = std::max(p->th.m2m_level_max_group[lev], ms[gi + 1] - ms[gi]);
           p->th.l2l_level_max_group[lev] = std::max(p->th.l2l_level_max_group[lev], ls[gi + 1] - ls[gi]);
         }
+      for (int lev = 0; lev < g.nlevels; ++lev)
+        p->th.l2l_level_pairs[lev] = ls[(lev + 1) * nch] - ls[lev * nch];
       p->th.lvl_source_parent = p->lvl_source_parent.data();
     }
   }
@@ -782,6 +784,10 @@ int qbxfmm_apply(const qbxfmm_plan* p, const qbxfmm_upsample* up, const qbxfmm_w
       QBX_TRY(launch_m2m_gemm_mixed(p->geo, p->th, p->tc, p->kern.nrhs, T32, (double2*)ws->mpoles,
                                     (double*)ws->pair_scratch, ws->error_word, st),
               "coarsen_multipoles (split TF32)");
+    else if (gemm && trans_mv_supported(p->tc))
+      QBX_TRY(launch_m2m_mv(p->geo, p->th, p->tc, p->kern.nrhs, (const double*)ws->translations,
+                            (double2*)ws->mpoles, ws->error_word, st),
+              "coarsen_multipoles (matrix form)");
     else if (gemm)
       QBX_TRY(launch_m2m_gemm(p->geo, p->th, p->tc, p->kern.nrhs, (const double*)ws->translations,
                               (double2*)ws->mpoles, (double*)ws->pair_scratch, ws->error_word, st),
@@ -810,6 +816,10 @@ int qbxfmm_apply(const qbxfmm_plan* p, const qbxfmm_upsample* up, const qbxfmm_w
       QBX_TRY(launch_l2l_gemm_mixed(p->geo, p->th, p->tc, p->kern.nrhs, T32, (double2*)ws->locals,
                                     ws->error_word, st),
               "refine_locals (split TF32)");
+    else if (gemm && trans_mv_supported(p->tc))
+      QBX_TRY(launch_l2l_mv(p->geo, p->th, p->tc, p->kern.nrhs, (const double*)ws->translations,
+                            (double2*)ws->locals, ws->error_word, st),
+              "refine_locals (matrix form)");
     else if (gemm)
       QBX_TRY(launch_l2l_gemm(p->geo, p->th, p->tc, p->kern.nrhs, (const double*)ws->translations,
                               (double2*)ws->locals, ws->error_word, st),

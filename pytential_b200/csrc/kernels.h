@@ -13,6 +13,7 @@ struct TransHost {
   int m2l_npairs = 0;                    // all M2L pairs (pair-scratch rows)
   int m2m_level_max_group[64] = {0};     // largest (level, child position) group per level
   int l2l_level_max_group[64] = {0};
+  int l2l_level_pairs[64] = {0};         // L2L pairs whose child is on a level
   const int32_t* lvl_source_parent = nullptr;   // host copy (owned by the plan)
 };
 
@@ -38,6 +39,11 @@ cudaError_t launch_m2l_gemm(const qbxfmm_geometry& g, const TransHost& th, const
 cudaError_t launch_m2m_gemm(const qbxfmm_geometry& g, const TransHost& th, const TransCfg& c,
                             int nrhs, const double* T, double2* mp, double* cpair, int32_t* err,
                             cudaStream_t st);
+bool trans_mv_supported(const TransCfg& c);
+cudaError_t launch_m2m_mv(const qbxfmm_geometry& g, const TransHost& th, const TransCfg& c,
+                          int nrhs, const double* T, double2* mp, int32_t* err, cudaStream_t st);
+cudaError_t launch_l2l_mv(const qbxfmm_geometry& g, const TransHost& th, const TransCfg& c,
+                          int nrhs, const double* T, double2* lo, int32_t* err, cudaStream_t st);
 cudaError_t launch_l2l_gemm(const qbxfmm_geometry& g, const TransHost& th, const TransCfg& c,
                             int nrhs, const double* T, double2* lo, int32_t* err, cudaStream_t st);
 cudaError_t launch_trans_reduce_m2l(const qbxfmm_geometry& g, const TransCfg& c, int nrhs,

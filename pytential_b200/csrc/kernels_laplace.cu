@@ -1464,15 +1464,21 @@ k_tsqbx(qbxfmm_geometry g, SourceCoeffs sc, int nrhs, const double* __restrict__
 }
 
 // L2QBXL (translate_box_local_to_qbx_local, fmm.py:314-356; interactions.py:318-356)
+// 3D: L2Q_SPLIT adjacent lanes per center split the columns b of the regular-harmonic
+// table (b = lane part, + L2Q_SPLIT, ...) and meet by shuffles; 2D: one lane per center.
+constexpr int L2Q_SPLIT = 4;
+
 template <int DIM, int Q>
 __global__ void __launch_bounds__(NT)
 k_l2qbxl(qbxfmm_geometry g, int pf, int ncf, int nrhs, const double2* __restrict__ locals,
          double2* __restrict__ qbx_exps)
 {
   constexpr int NC = (DIM == 3) ? (Q + 1) * (Q + 2) / 2 : Q + 1;
-  int ig = blockIdx.x * blockDim.x + threadIdx.x;
+  constexpr int SPLIT = (DIM == 3) ? L2Q_SPLIT : 1;
+  int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  int ig = gt / SPLIT, part = gt - ig * SPLIT;
   int r = blockIdx.y;
-  if (ig >= g.nglobal_qbx_centers) return;
+  if (ig >= g.nglobal_qbx_centers) return;   // whole groups of SPLIT lanes leave together
   int ctr = g.global_qbx_centers[ig];
   int tb = g.target_boxes[g.qbx_center_to_target_box[ctr]];
   double cc[3], cb[3];
@@ -1488,11 +1494,13 @@ k_l2qbxl(qbxfmm_geometry g, int pf, int ncf, int nrhs, const double2* __restrict
   if (DIM == 3) {
     double d0 = (cc[0] - cb[0]) / rho_b, d1 = (cc[1] - cb[1]) / rho_b, d2 = (cc[2] - cb[2]) / rho_b;
     double r2 = d0 * d0 + d1 * d1 + d2 * d2;
+    // R_a^b(d): output (k,l) += L_{a+k}^{b+l} conj(R_a^b); the lanes of a center
+    // take the columns b = part, part + SPLIT, ... in lockstep
     double2 mm = c2(1.0);
-    // R_a^b(d): output (k,l) += L_{a+k}^{b+l} conj(R_a^b)
-    for (int bm = 0; bm <= pf; ++bm) {
-      if (bm > 0) mm = cscale(0.5 * rcp(bm), cmul(mm, c2(d0, d1)));
+    for (int b = 1; b <= part; ++b) mm = cscale(0.5 * rcp(b), cmul(mm, c2(d0, d1)));
+    for (int bm = part; bm <= pf; bm += SPLIT) {
       double2 a = mm, prev = c2(0.0);
+      for (int b = bm + 1; b <= bm + SPLIT; ++b) mm = cscale(0.5 * rcp(b), cmul(mm, c2(d0, d1)));
       for (int an = bm; an <= pf; ++an) {
         if (an > bm) {
           double2 bb = cscale(rcp(an + bm) * rcp(an - bm),
@@ -1517,6 +1525,16 @@ k_l2qbxl(qbxfmm_geometry g, int pf, int ncf, int nrhs, const double2* __restrict
           }
       }
     }
+    // the SPLIT lanes of a center are adjacent and all present (SPLIT divides 32)
+    const unsigned gmask = ((1u << SPLIT) - 1u) << ((threadIdx.x & 31) & ~(SPLIT - 1));
+#pragma unroll
+    for (int off = 1; off < SPLIT; off <<= 1)
+#pragma unroll
+      for (int i = 0; i < NC; ++i) {
+        acc[i].x += __shfl_xor_sync(gmask, acc[i].x, off, SPLIT);
+        acc[i].y += __shfl_xor_sync(gmask, acc[i].y, off, SPLIT);
+      }
+    if (part != 0) return;
     double rk = 1.0;
 #pragma unroll
     for (int k = 0; k <= Q; ++k) {
@@ -1829,7 +1847,8 @@ static cudaError_t l2qbxl_q(const qbxfmm_geometry& g, int pf, int nrhs, const do
                             double2* qe, cudaStream_t st)
 {
   int ncf = (int)ncoef_dim(DIM, pf);
-  dim3 grid((g.nglobal_qbx_centers + NT - 1) / NT, grid_y(nrhs));
+  size_t lanes = (size_t)g.nglobal_qbx_centers * (DIM == 3 ? L2Q_SPLIT : 1);
+  dim3 grid((unsigned)((lanes + NT - 1) / NT), grid_y(nrhs));
   k_l2qbxl<DIM, Q><<<grid, NT, 0, st>>>(g, pf, ncf, nrhs, lo, qe);
   return cudaGetLastError();
 }

@@ -16,6 +16,9 @@
 #include "laplace.cuh"
 #include "kernels.h"
 
+#include <cooperative_groups.h>
+namespace cg = cooperative_groups;
+
 namespace qbx {
 
 namespace {
@@ -343,6 +346,140 @@ k_trans_reduce(int ncf, int rp, int nrhs, const int32_t* __restrict__ boxes, int
 
 // }}}
 
+// {{{ M2M / L2L as matrix-vector products (small matrices)
+
+// group g of a pair: group_starts[g] <= pr < group_starts[g + 1], g in [g0, g0 + 8)
+QBX_D int pair_group(const int32_t* __restrict__ group_starts, int g0, int pr)
+{
+  int grp = g0;
+  while (grp + 1 < g0 + 8 && group_starts[grp + 1] <= pr) ++grp;
+  return grp;
+}
+
+// y[row] += sum_k T[row][k] x[k] over one matrix, rows row0 and row0 + NT; x in
+// shared memory (kp doubles, zero-padded).  Eight row loads are issued before their
+// products, so that a thread keeps 128 bytes of the (L2-resident) matrix in flight.
+QBX_D void mv_rows(const double* __restrict__ Tm, int kp, int R, const double* x, double* acc2,
+                   int row0)
+{
+  const int n2 = kp / 2;
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    int row = row0 + h * NT;
+    if (row >= R) break;
+    const double2* tr = reinterpret_cast<const double2*>(Tm + (size_t)row * kp);
+    const double2* xv = reinterpret_cast<const double2*>(x);
+    double a[4] = {0.0, 0.0, 0.0, 0.0};
+    int k2 = 0;
+    for (; k2 + 8 <= n2; k2 += 8) {
+      double2 t[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) t[u] = __ldg(tr + k2 + u);
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        double2 xx = xv[k2 + u];
+        a[u & 3] = fma(t[u].x, xx.x, a[u & 3]);
+        a[u & 3] = fma(t[u].y, xx.y, a[u & 3]);
+      }
+    }
+    for (; k2 < n2; ++k2) {
+      double2 t0 = __ldg(tr + k2), x0 = xv[k2];
+      a[0] = fma(t0.x, x0.x, a[0]);
+      a[1] = fma(t0.y, x0.y, a[1]);
+    }
+    acc2[h] += (a[0] + a[1]) + (a[2] + a[3]);
+  }
+}
+
+// M2M of one level: a cluster of eight CTAs per source parent box (i = i0 +
+// blockIdx.x / 8, density blockIdx.y); CTA c multiplies child slot c's multipole by
+// its (child position) matrix, and CTA 0 adds the eight products into the parent in
+// a fixed order through distributed shared memory.
+__global__ void __cluster_dims__(8, 1, 1) __launch_bounds__(NT)
+k_trans_m2m_mv(int ncf, int rp, int kp, int nrhs, const double* __restrict__ T, size_t mat_base,
+               int mat_mod, const int32_t* __restrict__ group_starts, int g0,
+               const int32_t* __restrict__ parents, int i0, const int32_t* __restrict__ par_starts,
+               const int32_t* __restrict__ par_pairs, const int32_t* __restrict__ pair_src,
+               double2* __restrict__ mp, int32_t* err, int nboxes)
+{
+  extern __shared__ double xs[];   // [kp] child multipole, then [2 NT] product rows
+  double* res = xs + kp;
+  cg::cluster_group cl = cg::this_cluster();
+  int i = i0 + blockIdx.x / 8;
+  int slot = blockIdx.x & 7;
+  int r = blockIdx.y;
+  int q0 = par_starts[i];
+  int nch = min(par_starts[i + 1] - q0, 8);
+  const int R = 2 * ncf;
+  double acc[2] = {0.0, 0.0};
+  if (slot < nch) {
+    int pr = par_pairs[q0 + slot];
+    int src = pair_src[pr];
+    int grp = pair_group(group_starts, g0, pr);
+    bool ok = (unsigned)src < (unsigned)nboxes;
+    if (!ok && threadIdx.x == 0) report(err, QBX_DEVERR_BAD_BOX);
+    const double* x = reinterpret_cast<const double*>(mp + ((size_t)(ok ? src : 0) * nrhs + r) * ncf);
+    for (int k = threadIdx.x; k < kp; k += NT) xs[k] = (ok && k < R) ? x[k] : 0.0;
+    __syncthreads();
+    int mat = (int)mat_base + (mat_mod > 0 ? grp % mat_mod : grp);
+    mv_rows(T + (size_t)mat * rp * kp, kp, R, xs, acc, threadIdx.x);
+  }
+  res[threadIdx.x] = acc[0];
+  res[threadIdx.x + NT] = acc[1];
+  cl.sync();
+  if (slot == 0) {
+    int parent = parents[i];
+    if ((unsigned)parent >= (unsigned)nboxes) {
+      if (threadIdx.x == 0) report(err, QBX_DEVERR_BAD_BOX);
+    } else {
+      double s0 = 0.0, s1 = 0.0;
+      for (int q = 0; q < nch; ++q) {
+        const double* rq = cl.map_shared_rank(res, q);
+        s0 += rq[threadIdx.x];
+        s1 += rq[threadIdx.x + NT];
+      }
+      double* y = reinterpret_cast<double*>(mp + ((size_t)parent * nrhs + r) * ncf);
+      if (threadIdx.x < R) y[threadIdx.x] += s0;
+      if (threadIdx.x + NT < R) y[threadIdx.x + NT] += s1;
+    }
+  }
+  cl.sync();
+}
+
+// L2L of one level: CTA per (parent, child) pair p0 + blockIdx.x of the level's
+// eight groups; child local += T_{child position} parent local.
+__global__ void __launch_bounds__(NT)
+k_trans_l2l_mv(int ncf, int rp, int kp, int nrhs, const double* __restrict__ T, size_t mat_base,
+               int mat_mod, const int32_t* __restrict__ group_starts, int g0,
+               const int32_t* __restrict__ pair_src, const int32_t* __restrict__ pair_dst,
+               double2* __restrict__ lo, int32_t* err, int nboxes)
+{
+  extern __shared__ double xs[];   // [kp]
+  int pr = group_starts[g0] + blockIdx.x;
+  int r = blockIdx.y;
+  int grp = pair_group(group_starts, g0, pr);
+  int src = pair_src[pr], dst = pair_dst[pr];
+  if ((unsigned)src >= (unsigned)nboxes || (unsigned)dst >= (unsigned)nboxes) {
+    if (threadIdx.x == 0) report(err, QBX_DEVERR_BAD_BOX);
+    return;
+  }
+  const int R = 2 * ncf;
+  const double* x = reinterpret_cast<const double*>(lo + ((size_t)src * nrhs + r) * ncf);
+  for (int k = threadIdx.x; k < kp; k += NT) xs[k] = k < R ? x[k] : 0.0;
+  __syncthreads();
+  double acc[2] = {0.0, 0.0};
+  int mat = (int)mat_base + (mat_mod > 0 ? grp % mat_mod : grp);
+  mv_rows(T + (size_t)mat * rp * kp, kp, R, xs, acc, threadIdx.x);
+  double* y = reinterpret_cast<double*>(lo + ((size_t)dst * nrhs + r) * ncf);
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    int row = threadIdx.x + h * NT;
+    if (row < R) y[row] += acc[h];
+  }
+}
+
+// }}}
+
 // {{{ launchers
 
 static void dims_from_ncf(int ncf, int& rp, int& kp)
@@ -579,6 +716,44 @@ cudaError_t launch_l2l_direct(const qbxfmm_geometry& g, const TransHost& th, con
     cudaError_t e = gemm_tiled_launch(g, c, nrhs, T, c.l2l_base, c.m2m_mat_mod, g.l2l_group_starts,
                                       lev * nch, nch, maxp * nrhs, g.l2l_pair_src, g.l2l_pair_dst,
                                       lo, lo, 1.0, nullptr, err, st);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+
+bool trans_mv_supported(const TransCfg& c) { return 2 * c.ncf <= 2 * NT && c.kp % 2 == 0; }
+
+// M2M level by level as matrix-vector products, eight CTAs per parent (small matrices)
+cudaError_t launch_m2m_mv(const qbxfmm_geometry& g, const TransHost& th, const TransCfg& c,
+                          int nrhs, const double* T, double2* mp, int32_t* err, cudaStream_t st)
+{
+  size_t sh = ((size_t)c.kp + 2 * NT) * sizeof(double);
+  for (int lev = g.nlevels - 2; lev >= 0; --lev) {
+    int i0 = th.lvl_source_parent[lev], i1 = th.lvl_source_parent[lev + 1];
+    if (i1 <= i0) continue;
+    k_trans_m2m_mv<<<dim3(8 * (i1 - i0), nrhs), NT, sh, st>>>(
+        c.ncf, c.rp, c.kp, nrhs, T, c.m2m_base, c.m2m_mat_mod, g.m2m_group_starts, lev * 8,
+        g.source_parent_boxes, i0, g.m2m_par_pair_starts, g.m2m_par_pairs, g.m2m_pair_src, mp, err,
+        g.nboxes);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+// L2L level by level, CTA per (parent, child) pair
+cudaError_t launch_l2l_mv(const qbxfmm_geometry& g, const TransHost& th, const TransCfg& c,
+                          int nrhs, const double* T, double2* lo, int32_t* err, cudaStream_t st)
+{
+  size_t sh = (size_t)c.kp * sizeof(double);
+  for (int lev = 1; lev < g.nlevels; ++lev) {
+    int n = th.l2l_level_pairs[lev];
+    if (n == 0) continue;
+    k_trans_l2l_mv<<<dim3(n, nrhs), NT, sh, st>>>(c.ncf, c.rp, c.kp, nrhs, T, c.l2l_base,
+                                                  c.m2m_mat_mod, g.l2l_group_starts, lev * 8,
+                                                  g.l2l_pair_src, g.l2l_pair_dst, lo, err, g.nboxes);
+    cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
