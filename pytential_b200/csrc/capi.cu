@@ -152,24 +152,29 @@ std::vector<double> h3_gaunt_table(int p)
   return G;
 }
 
-// Wigner small-d tables for the rotation-based point-to-box translations, for
-// m in [-p, p], mu in [-q, q] (index (m + p) (2q + 1) + mu + q):
-//   start[4 idx]     = sign x sqrt(factorial ratio) of the single surviving term of
-//                      Wigner's formula at n0 = max(|m|, |mu|), and the exponents of
-//                      cos(beta/2) and sin(beta/2);
-//   rec[3 (idx (p+1) + n)] = (c1, c2, c3) with
-//                      d^{n+1} = (c1 cos(beta) - c2) d^n - c3 d^{n-1}   (n >= 1),
-// the three-term recurrence of d^n_{m mu}(beta) in n.
-std::vector<double> h3_rotation_tables(int p, int q)
+// Tables of the rotation-based M2QBXL / L2QBXL (p = fmm order, q = QBX order):
+//   start values of d^n_{m mu}(beta) at n0 = max(|m|, mu), mu >= 0: [2p+1][q+1][4] =
+//     (coefficient, exponent of cos(beta/2), exponent of sin(beta/2), unused), from
+//     the single surviving term of Wigner's formula;
+//   isq[N][k] = 1 / sqrt(N^2 - k^2) (N > k, else 0), N <= p + 1, k <= p;
+//   rt[n][k] = sqrt(n^2 - k^2) / sqrt((n+1)^2 - k^2) (n >= k, else 0), n, k <= p;
+//   the lambda = 0 Gaunt slice g0[(nu,mu)][n][j] = G(n,mu; nu,mu; |n - nu| + 2 j),
+//     nu <= q, n <= p, j <= q (zero outside n >= |mu|, j <= min(n, nu)),
+//     read from the Gaunt table (layout [(nu,mu)][j][(n,m)]).
+std::vector<double> h3_rotation_tables(int p, int q, const std::vector<double>& gaunt)
 {
-  const int nm = 2 * p + 1, nmu = 2 * q + 1;
-  std::vector<double> t((size_t)nm * nmu * 4 + (size_t)nm * nmu * (p + 1) * 3, 0.0);
+  const int nm = 2 * p + 1, ncf = (p + 1) * (p + 1), nl = p + 1, ncq = (q + 1) * (q + 1);
+  const size_t nstart = (size_t)nm * (q + 1) * 4, nisq = (size_t)(p + 2) * (p + 1),
+               nrt = (size_t)(p + 1) * (p + 1), ng0 = (size_t)ncq * nl * (q + 1);
+  std::vector<double> t(nstart + nisq + nrt + ng0, 0.0);
   double* start = t.data();
-  double* rec = start + (size_t)nm * nmu * 4;
+  double* isq = start + nstart;
+  double* rt = isq + nisq;
+  double* g0 = rt + nrt;
   for (int m = -p; m <= p; ++m)
-    for (int mu = -q; mu <= q; ++mu) {
-      size_t idx = (size_t)(m + p) * nmu + (mu + q);
-      int j = std::max(std::abs(m), std::abs(mu));
+    for (int mu = 0; mu <= q; ++mu) {
+      size_t idx = (size_t)(m + p) * (q + 1) + mu;
+      int j = std::max(std::abs(m), mu);
       int kk = std::max(0, mu - m);
       int a1 = j + mu - kk, a3 = j - kk - m, a4 = kk - mu + m;
       double lf = 0.5 * (std::lgamma(j + m + 1.0) + std::lgamma(j - m + 1.0) +
@@ -179,15 +184,21 @@ std::vector<double> h3_rotation_tables(int p, int q)
       start[4 * idx] = (((kk - mu + m) & 1) ? -1.0 : 1.0) * std::exp(lf);
       start[4 * idx + 1] = 2 * j + mu - m - 2 * kk;
       start[4 * idx + 2] = 2 * kk - mu + m;
-      for (int n = std::max(j, 1); n < p; ++n) {
-        double a = n * std::sqrt(((n + 1.0) * (n + 1.0) - (double)m * m) *
-                                 ((n + 1.0) * (n + 1.0) - (double)mu * mu));
-        double b = (n + 1.0) * std::sqrt(((double)n * n - (double)m * m) * ((double)n * n - (double)mu * mu));
-        double* r = rec + 3 * (idx * (p + 1) + n);
-        r[0] = (2.0 * n + 1.0) * n * (n + 1.0) / a;
-        r[1] = (2.0 * n + 1.0) * (double)m * mu / a;
-        r[2] = b / a;
-      }
+    }
+  for (int N = 0; N <= p + 1; ++N)
+    for (int k = 0; k <= p; ++k)
+      isq[(size_t)N * (p + 1) + k] = N > k ? 1.0 / std::sqrt((double)N * N - (double)k * k) : 0.0;
+  for (int n = 0; n <= p; ++n)
+    for (int k = 0; k <= p; ++k)
+      rt[(size_t)n * (p + 1) + k] =
+          n >= k ? std::sqrt(((double)n * n - (double)k * k) / ((n + 1.0) * (n + 1.0) - (double)k * k))
+                 : 0.0;
+  for (int nu = 0; nu <= q; ++nu)
+    for (int mu = -nu; mu <= nu; ++mu) {
+      int o = nu * nu + nu + mu;
+      for (int n = std::abs(mu); n <= p; ++n)
+        for (int j = 0; j <= std::min(n, nu); ++j)
+          g0[((size_t)o * nl + n) * (q + 1) + j] = gaunt[((size_t)o * nl + j) * ncf + n * n + n + mu];
     }
   return t;
 }
@@ -297,7 +308,7 @@ int qbxfmm_plan_create(const qbxfmm_kernel* kernel, const qbxfmm_geometry* geome
   }
   if (p->h3) {
     p->h3gaunt = h3_gaunt_table(k.fmm_order);
-    p->h3rot = h3_rotation_tables(k.fmm_order, k.qbx_order);
+    p->h3rot = h3_rotation_tables(k.fmm_order, k.qbx_order, p->h3gaunt);
     std::vector<int32_t> off(3 * (size_t)g.m2l_nclasses);
     if (g.m2l_nclasses > 0)
       e = cudaMemcpy(off.data(), g.m2l_class_offsets, sizeof(int32_t) * off.size(),
@@ -583,7 +594,7 @@ int qbxfmm_translate_box_multipoles_to_qbx_local(const qbxfmm_plan* p, const voi
     if (!p->trans_dev)
       return fail(QBXFMM_ERR_ARG, "3D Helmholtz: call qbxfmm_precompute_translations first");
     QBX_TRY(h3_launch_m2qbxl(p->geo, p->hc, p->kern.fmm_order, p->kern.qbx_order, p->kern.nrhs,
-                             (const double2*)mpoles, p->trans_dev + p->tc.nmatrices * p->tc.rp * p->tc.kp,
+                             (const double2*)mpoles,
                              p->trans_dev + p->tc.nmatrices * p->tc.rp * p->tc.kp + p->h3gaunt.size(),
                              (double2*)qbx_exps, error_word, S(stream)),
             "translate_box_multipoles_to_qbx_local");
@@ -612,7 +623,7 @@ int qbxfmm_translate_box_local_to_qbx_local(const qbxfmm_plan* p, const void* lo
     if (!p->trans_dev)
       return fail(QBXFMM_ERR_ARG, "3D Helmholtz: call qbxfmm_precompute_translations first");
     QBX_TRY(h3_launch_l2qbxl(p->geo, p->hc, p->kern.fmm_order, p->kern.qbx_order, p->kern.nrhs,
-                             (const double2*)locals, p->trans_dev + p->tc.nmatrices * p->tc.rp * p->tc.kp,
+                             (const double2*)locals,
                              p->trans_dev + p->tc.nmatrices * p->tc.rp * p->tc.kp + p->h3gaunt.size(),
                              (double2*)qbx_exps, nullptr, S(stream)),
             "translate_box_local_to_qbx_local");

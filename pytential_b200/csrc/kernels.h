@@ -157,12 +157,14 @@ cudaError_t h3_launch_eval_locals(const qbxfmm_geometry& g, HelmCoeffs hc, int p
                                   const double2* lo, double2* pot, cudaStream_t st);
 cudaError_t h3_launch_p2qbxl(const qbxfmm_geometry& g, HelmCoeffs hc, int q, int nrhs,
                              const double2* s, double2* qe, int32_t* err, cudaStream_t st);
+// rot: rotation tables of h3_rotation_tables (start values, recurrence factors,
+// lambda = 0 Gaunt slice)
 cudaError_t h3_launch_m2qbxl(const qbxfmm_geometry& g, HelmCoeffs hc, int pf, int q, int nrhs,
-                             const double2* mp, const double* gaunt, const double* rot,
-                             double2* qe, int32_t* err, cudaStream_t st);
+                             const double2* mp, const double* rot, double2* qe, int32_t* err,
+                             cudaStream_t st);
 cudaError_t h3_launch_l2qbxl(const qbxfmm_geometry& g, HelmCoeffs hc, int pf, int q, int nrhs,
-                             const double2* lo, const double* gaunt, const double* rot,
-                             double2* qe, int32_t* err, cudaStream_t st);
+                             const double2* lo, const double* rot, double2* qe, int32_t* err,
+                             cudaStream_t st);
 cudaError_t h3_launch_qbxl2p(const qbxfmm_geometry& g, HelmCoeffs hc, int q, int nrhs,
                              const double2* qe, double2* pt, cudaStream_t st);
 cudaError_t h3_launch_tsqbx(const qbxfmm_geometry& g, HelmCoeffs hc, int q, int nrhs,

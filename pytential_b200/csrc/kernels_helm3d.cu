@@ -778,65 +778,69 @@ k_h3_p2qbxl(qbxfmm_geometry g, HelmCoeffs hc, int nrhs, const double2* __restric
 // polar and azimuthal angles of b).  Equal in exact arithmetic to the Gaunt sum
 // c_{nu mu; n m}(b) of the file comment; only |mu| <= Q of the rotated source
 // coefficients are needed, so the work per (center, box) pair is O(pf^2 Q) per
-// density instead of O(pf^2 Q^2).  d^n_{m mu} for fixed (m, mu) by the three-term
-// recurrence in n (Jacobi polynomials), started at n0 = max(|m|, |mu|) from the single
-// surviving term of Wigner's formula; start values and recurrence coefficients come
-// precomputed (rot tables, built with the Gaunt table).
+// density instead of O(pf^2 Q^2).
+// The pass runs over the source order n: d^n_{m mu} for fixed (m, mu >= 0) follows
+// the three-term recurrence in n (Jacobi polynomials),
+//   n s_{n+1} d^{n+1} = (2n+1)(n(n+1) cos(beta) - m mu) d^n - (n+1) s_n d^{n-1},
+//   s_n = sqrt((n^2 - m^2)(n^2 - mu^2)),
+// started at n0 = max(|m|, mu) from the single surviving term of Wigner's formula;
+// each lane advances its (m, mu) recurrences in registers, the slice of order n
+// (with d^n_{m,-mu} = (-1)^{m+mu} d^n_{-m,mu} and the phases) goes through shared
+// memory to the lanes that rotate and translate, and the coaxial coefficients of
+// order n are formed on the fly, so no table of all orders is stored.  The slices of
+// orders n <= Q are also the back-rotation matrices (d^nu_{mu mu''}(-beta) =
+// d^nu_{mu'' mu}(beta)).
 // One warp per center (H3_ROT_ZS CTAs x 4 warps per chunk of <= 32 centers), RB
-// densities per CTA staged in shared memory per box; per (center, box) the warp
-// builds the rotation and coaxial tables in its shared slice; lane tasks are
-// (mu, density) for the rotation + coaxial step and (output, density) for the back
-// rotation, whose results stay in registers across the boxes.
+// densities per CTA staged in shared memory per box; lane tasks are (m, mu)
+// recurrences, (mu, density) for the rotation + coaxial step and (output, density)
+// for the back rotation, whose results stay in registers across the boxes.
 constexpr int H3_ROT_ZS = 8;
+constexpr int H3_ROT_SLOTS = 7;   // recurrence tasks per lane: (2 pf + 1)(Q + 1) <= 7 x 32
 
 template <bool FROM_LOCAL, int Q, int RB>
 __global__ void __launch_bounds__(NT)
 k_h3_e2qbxl_rot(qbxfmm_geometry g, HelmCoeffs hc, int pf, int nrhs,
-                const double2* __restrict__ exps, const double* __restrict__ gaunt,
-                const double* __restrict__ rot, double2* __restrict__ qbx_exps, int32_t* err)
+                const double2* __restrict__ exps, const double* __restrict__ rot,
+                double2* __restrict__ qbx_exps, int32_t* err)
 {
   constexpr int NCQ = (Q + 1) * (Q + 1);
   constexpr int NMU = 2 * Q + 1;
   constexpr int NOUT = (NCQ * RB + 31) / 32;
+  constexpr int TPL = (NMU * RB + 31) / 32;
+  constexpr int RSL = H3_ROT_SLOTS;
   extern __shared__ double2 smem2[];
   const int ncf = (pf + 1) * (pf + 1);
   const int L = pf + Q;
   const int nl = pf + 1;
   const int nm = 2 * pf + 1;
-  const int TS = ncf + 1;                                    // padded T row
-  const double* rstart = rot;                                 // [nm][NMU][4]
-  const double* rrec = rot + (size_t)nm * NMU * 4;            // [nm][NMU][pf+1][3]
+  const int ntask = nm * (Q + 1);
+  const int nisq = (pf + 2) * (pf + 1), nrt = (pf + 1) * (pf + 1);
+  const double* rstart = rot;                                   // [nm][Q+1][4]
+  const double* g_isq = rstart + (size_t)nm * (Q + 1) * 4;      // [pf+2][pf+1]
+  const double* g_rt = g_isq + nisq;                            // [pf+1][pf+1]
+  const double* g0c = g_rt + nrt;                               // [NCQ][nl][Q+1]
   // CTA-wide
-  double2* Es = smem2;                                        // [ncf][RB]
-  // (both double arrays padded to an even length: the per-warp slices that follow hold
-  // double2 and must stay 16-byte aligned)
-  double* G0 = reinterpret_cast<double*>(Es + (size_t)ncf * RB);   // [NCQ][Q+1][nl]
-  double* spow = G0 + (((size_t)NCQ * (Q + 1) * nl + 1) & ~(size_t)1);   // [nl]: s_box^{+-n}
-  double2* wbase = reinterpret_cast<double2*>(spow + ((nl + 1) & ~1));
+  double2* Es = smem2;                                          // [ncf][RB]
+  double* s_isq = reinterpret_cast<double*>(Es + (size_t)ncf * RB);
+  double* s_rt = s_isq + nisq;
+  double* spow = s_rt + nrt;                                    // [nl]: s_box^{+-n}
+  const size_t ctad = ((size_t)nisq + nrt + nl + 1) & ~(size_t)1;
+  double2* wbase = reinterpret_cast<double2*>(s_isq + ctad);
   // per warp
-  const size_t per = (size_t)NMU * TS / 2 + (size_t)NMU * NCQ / 2 + 1 + (size_t)NCQ * nl +
-                     (size_t)NCQ * RB + (L + 2) + nm;
+  const size_t perd = ((size_t)nm * (Q + 1) + (size_t)NMU * NCQ + 2 * (size_t)nm + 1) / 2;
+  const size_t per = (size_t)nm * NMU + NCQ + (size_t)NCQ * RB + (L + 2) + nm + perd;
   int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  double2* wb = wbase + (size_t)warp * per;
-  double* T = reinterpret_cast<double*>(wb);                 // [NMU][TS]
-  double* Tb = T + (size_t)NMU * TS;                          // [NMU][NCQ]
-  double2* coax = wb + (size_t)NMU * TS / 2 + (size_t)NMU * NCQ / 2 + 1;    // [NCQ][nl]
-  double2* Lp = coax + (size_t)NCQ * nl;                      // [NCQ][RB]
-  double2* rad = Lp + (size_t)NCQ * RB;                       // [L + 2]
-  double2* ph = rad + (L + 2);                                // [nm]: e^{i m alpha}, m = -pf..pf
+  double2* Dph = wbase + (size_t)warp * per;                    // [nm][NMU] slice x phase
+  double2* coaxn = Dph + (size_t)nm * NMU;                      // [NCQ] coaxial column n
+  double2* Lp = coaxn + NCQ;                                    // [NCQ][RB]
+  double2* rad = Lp + (size_t)NCQ * RB;                         // [L + 2]
+  double2* ph = rad + (L + 2);                                  // [nm]: e^{i m alpha}
+  double* Draw = reinterpret_cast<double*>(ph + nm);            // [nm][Q+1] d^n_{m mu>=0}
+  double* Tb = Draw + (size_t)nm * (Q + 1);                     // [NMU][NCQ]
+  double* chp = Tb + (size_t)NMU * NCQ;                         // [nm] cos(beta/2)^k
+  double* shp = chp + nm;                                       // [nm] sin(beta/2)^k
 
-  __syncthreads();
-  // lambda = 0 slice of the Gaunt table: G0[o][j][n] = G(n,mu; nu,mu; |n - nu| + 2 j)
-  for (int x = threadIdx.x; x < NCQ * (Q + 1) * nl; x += NT) {
-    int o = x / ((Q + 1) * nl), rem = x - o * (Q + 1) * nl;
-    int j = rem / nl, n = rem - j * nl;
-    int nu = (int)sqrt((double)o);
-    while ((nu + 1) * (nu + 1) <= o) ++nu;
-    while (nu * nu > o) --nu;
-    int mu = o - nu * nu - nu;
-    G0[x] = (n >= abs(mu) && j <= min(n, nu)) ? __ldg(gaunt + ((size_t)o * nl + j) * ncf + hq(n, mu))
-                                             : 0.0;
-  }
+  for (int x = threadIdx.x; x < nisq + nrt; x += NT) s_isq[x] = __ldg(g_isq + x);
   __syncthreads();
   int chunk = blockIdx.x;
   int r0 = blockIdx.y * RB;
@@ -906,87 +910,116 @@ k_h3_e2qbxl_rot(qbxfmm_geometry g, HelmCoeffs hc, int pf, int nrhs,
       double sn, cs;
       sincos((m - pf) * alpha, &sn, &cs);
       ph[m] = c2(cs, sn);
-    }
-    // rotation tables: T[(mu+Q)][hq(n,m)] = eps_m eps_mu d^n_{m mu}(beta) (n >= n0),
-    // Tb[(mu+Q)][hq(nu,mu2)] = eps_mu eps_mu2 d^nu_{mu mu2}(-beta), nu <= Q
-    for (int task = lane; task < nm * NMU + NMU * NMU; task += 32) {
-      bool back = task >= nm * NMU;
-      int m, mu, nmax;
-      double sgn_s = 1.0;
-      if (!back) {
-        m = task / NMU - pf;
-        mu = task % NMU - Q;
-        nmax = pf;
-      } else {
-        int t2 = task - nm * NMU;
-        m = t2 / NMU - Q;      // first index: mu of the rotated local
-        mu = t2 % NMU - Q;     // second index: mu'' of the output
-        nmax = Q;
-        sgn_s = -1.0;          // sin(-beta/2) = -sin(beta/2)
+      double a = 1.0, b = 1.0;
+      for (int u = 0; u < m; ++u) {
+        a *= ch;
+        b *= sh;
       }
-      int n0 = max(abs(m), abs(mu));
-      if (n0 > nmax) continue;
-      size_t idx = (size_t)(m + pf) * NMU + (mu + Q);
-      double v = __ldg(rstart + 4 * idx);
-      int ec = (int)__ldg(rstart + 4 * idx + 1), es = (int)__ldg(rstart + 4 * idx + 2);
-      for (int u = 0; u < ec; ++u) v *= ch;
-      for (int u = 0; u < es; ++u) v *= sgn_s * sh;
-      double epsw = ((m > 0 && (m & 1)) ? -1.0 : 1.0) * ((mu > 0 && (mu & 1)) ? -1.0 : 1.0);
-      double prev = 0.0, cur = v;
-      const double* rc = rrec + 3 * idx * (pf + 1);
-      for (int n = n0; n <= nmax; ++n) {
-        if (!back) T[(mu + Q) * TS + hq(n, m)] = epsw * cur;
-        else Tb[(m + Q) * NCQ + hq(n, mu)] = epsw * cur;
-        if (n == nmax) break;
-        double nxt;
-        if (n == 0) {
-          nxt = cbeta * cur;
-        } else {
-          const double* c3 = rc + 3 * n;
-          nxt = fma(fma(__ldg(c3), cbeta, -__ldg(c3 + 1)), cur, -__ldg(c3 + 2) * prev);
-        }
-        prev = cur;
-        cur = nxt;
-      }
+      chp[m] = a;
+      shp[m] = b;
     }
     __syncwarp();
-    // coaxial coefficients coax[hq(nu,mu)][n] = i^{nu-n} sum_j G(nu,mu; j; n,mu) rad[l]
-    for (int x = lane; x < NCQ * nl; x += 32) {
-      int o = x / nl, n = x - o * nl;
-      int nu = (int)sqrt((double)o);
-      while ((nu + 1) * (nu + 1) <= o) ++nu;
-      while (nu * nu > o) --nu;
-      int mu = o - nu * nu - nu;
-      double2 tt = c2(0.0);
-      if (n >= abs(mu)) {
-        const double* G = G0 + (size_t)o * (Q + 1) * nl + n;
-        int lbase = abs(n - nu), jmax = min(n, nu);
-        for (int j = 0; j <= jmax; ++j) tt = caxpy(G[j * nl], rad[lbase + 2 * j], tt);
-        tt = cmul(ipow(nu - n + 4 * pf), tt);
-      }
-      coax[x] = tt;
-    }
-    __syncwarp();
-    // rotate (only |mu| <= Q) and translate coaxially: lane task (mu, density)
-    for (int task = lane; task < NMU * RB; task += 32) {
-      int mu = task / RB - Q, r = task - (task / RB) * RB;
-      int amu = abs(mu);
-      double2 lacc[Q + 1];
+    // recurrence tasks t = (m + pf) (Q + 1) + mu, mu >= 0: start values
+    double cur[RSL], prev[RSL], v0[RSL];
+    int n0[RSL];
 #pragma unroll
-      for (int nu = 0; nu <= Q; ++nu) lacc[nu] = c2(0.0);
-      const double* Tm = T + (mu + Q) * TS;
-      for (int n = amu; n <= pf; ++n) {
+    for (int sl = 0; sl < RSL; ++sl) {
+      int t = lane + 32 * sl;
+      cur[sl] = prev[sl] = v0[sl] = 0.0;
+      n0[sl] = 1 << 20;
+      if (t < ntask) {
+        int m = t / (Q + 1) - pf, mu = t % (Q + 1);
+        n0[sl] = max(abs(m), mu);
+        v0[sl] = __ldg(rstart + 4 * t) * chp[(int)__ldg(rstart + 4 * t + 1)] *
+                 shp[(int)__ldg(rstart + 4 * t + 2)];
+      }
+    }
+    double2 lacc[TPL][Q + 1];
+#pragma unroll
+    for (int ts = 0; ts < TPL; ++ts)
+#pragma unroll
+      for (int nu = 0; nu <= Q; ++nu) lacc[ts][nu] = c2(0.0);
+
+    for (int n = 0; n <= pf; ++n) {
+      // (1) the raw slice d^n_{m mu}, mu >= 0, and the step to n + 1
+      double rn = n > 0 ? 1.0 / n : 0.0;
+      double h1 = (2.0 * n + 1.0) * n * (n + 1.0) * cbeta;
+#pragma unroll
+      for (int sl = 0; sl < RSL; ++sl) {
+        int t = lane + 32 * sl;
+        if (t >= ntask) continue;
+        if (n == n0[sl]) cur[sl] = v0[sl];
+        Draw[t] = n >= n0[sl] ? cur[sl] : 0.0;
+        if (n >= n0[sl] && n < pf) {
+          double nxt;
+          if (n == 0) {
+            nxt = cbeta * cur[sl];
+          } else {
+            int m = t / (Q + 1) - pf, mu = t % (Q + 1);
+            int am = abs(m);
+            double w = rn * s_isq[(n + 1) * (pf + 1) + am] * s_isq[(n + 1) * (pf + 1) + mu];
+            double A = (h1 - (2.0 * n + 1.0) * m * mu) * w;
+            double C = (n + 1.0) * rn * s_rt[n * (pf + 1) + am] * s_rt[n * (pf + 1) + mu];
+            nxt = fma(A, cur[sl], -C * prev[sl]);
+          }
+          prev[sl] = cur[sl];
+          cur[sl] = nxt;
+        }
+      }
+      // (2) coaxial column n: coaxn[(nu,mu)] = i^{nu-n} sum_j G(nu,mu; j; n,mu) rad[|n-nu|+2j]
+      for (int o = lane; o < NCQ; o += 32) {
+        int nu = (int)sqrt((double)o);
+        while ((nu + 1) * (nu + 1) <= o) ++nu;
+        while (nu * nu > o) --nu;
+        int mu = o - nu * nu - nu;
+        double2 tt = c2(0.0);
+        if (n >= abs(mu)) {
+          const double* G = g0c + ((size_t)o * nl + n) * (Q + 1);
+          int lbase = abs(n - nu), jmax = min(n, nu);
+          for (int j = 0; j <= jmax; ++j) tt = caxpy(__ldg(G + j), rad[lbase + 2 * j], tt);
+          tt = cmul(ipow(nu - n + 4 * pf), tt);
+        }
+        coaxn[o] = tt;
+      }
+      __syncwarp();
+      // (3) the signed, phased slice for |m| <= n, all mu; orders n <= Q also give
+      // the back-rotation matrices
+      for (int e = lane; e < (2 * n + 1) * NMU; e += 32) {
+        int mm = e / NMU - n, mu = e % NMU - Q;
+        double val = mu >= 0 ? Draw[(mm + pf) * (Q + 1) + mu]
+                             : (((mm - mu) & 1) ? -1.0 : 1.0) * Draw[(pf - mm) * (Q + 1) - mu];
+        val *= ((mm > 0 && (mm & 1)) ? -1.0 : 1.0) * ((mu > 0 && (mu & 1)) ? -1.0 : 1.0);
+        if (n <= Q && abs(mm) <= Q) Tb[(mu + Q) * NCQ + n * n + n + mm] = val;
+        Dph[(mm + pf) * NMU + mu + Q] = cscale(val, ph[mm + pf]);
+      }
+      __syncwarp();
+      // (4) rotate and translate coaxially: lane task (mu, density)
+      const int base = n * n + n;
+#pragma unroll
+      for (int ts = 0; ts < TPL; ++ts) {
+        int task = lane + 32 * ts;
+        if (task >= NMU * RB) continue;
+        int mu = task / RB - Q, r = task - (task / RB) * RB;
+        int amu = abs(mu);
+        if (amu > n) continue;
         double2 mr = c2(0.0);
-        int base = n * n + n;
+        const double2* Dm = Dph + mu + Q;
         for (int m = -n; m <= n; ++m)
-          mr = cfma(cscale(Tm[base + m], ph[m + pf]), Es[(base + m) * RB + r], mr);
+          mr = cfma(Dm[(m + pf) * NMU], Es[(base + m) * RB + r], mr);
 #pragma unroll
         for (int nu = 0; nu <= Q; ++nu)
-          if (nu >= amu) lacc[nu] = cfma(coax[hq(nu, mu) * nl + n], mr, lacc[nu]);
+          if (nu >= amu) lacc[ts][nu] = cfma(coaxn[nu * nu + nu + mu], mr, lacc[ts][nu]);
       }
+      __syncwarp();
+    }
+#pragma unroll
+    for (int ts = 0; ts < TPL; ++ts) {
+      int task = lane + 32 * ts;
+      if (task >= NMU * RB) continue;
+      int mu = task / RB - Q, r = task - (task / RB) * RB;
 #pragma unroll
       for (int nu = 0; nu <= Q; ++nu)
-        if (nu >= amu) Lp[hq(nu, mu) * RB + r] = lacc[nu];
+        if (nu >= abs(mu)) Lp[(nu * nu + nu + mu) * RB + r] = lacc[ts][nu];
     }
     __syncwarp();
     // rotate back into the register outputs: lane task (o = (nu, mu2), density)
@@ -1000,7 +1033,7 @@ k_h3_e2qbxl_rot(qbxfmm_geometry g, HelmCoeffs hc, int pf, int nrhs,
       while (nu * nu > o) --nu;
       int mu2 = o - nu * nu - nu;
       double2 a = c2(0.0);
-      for (int mu = -nu; mu <= nu; ++mu) a = caxpy(Tb[(mu + Q) * NCQ + o], Lp[hq(nu, mu) * RB + r], a);
+      for (int mu = -nu; mu <= nu; ++mu) a = caxpy(Tb[(mu + Q) * NCQ + o], Lp[(nu * nu + nu + mu) * RB + r], a);
       acc[i] = cfma(cconj(ph[mu2 + pf]), a, acc[i]);
     }
     __syncwarp();
@@ -1447,72 +1480,70 @@ static size_t h3_rot_smem(int pf)
 {
   constexpr int NCQ = (Q + 1) * (Q + 1), NMU = 2 * Q + 1;
   int ncf = (pf + 1) * (pf + 1), L = pf + Q, nl = pf + 1, nm = 2 * pf + 1;
-  size_t per = (size_t)NMU * (ncf + 1) / 2 + (size_t)NMU * NCQ / 2 + 1 + (size_t)NCQ * nl +
-               (size_t)NCQ * RB + (L + 2) + nm;
-  size_t cta = (size_t)ncf * RB * sizeof(double2) +
-               (((size_t)NCQ * (Q + 1) * nl + 1) & ~(size_t)1) * sizeof(double) +
-               ((nl + 1) & ~1) * sizeof(double);
-  return cta + NW * per * sizeof(double2);
+  size_t nisq = (size_t)(pf + 2) * (pf + 1), nrt = (size_t)(pf + 1) * (pf + 1);
+  size_t ctad = (nisq + nrt + nl + 1) & ~(size_t)1;
+  size_t perd = ((size_t)nm * (Q + 1) + (size_t)NMU * NCQ + 2 * (size_t)nm + 1) / 2;
+  size_t per = (size_t)nm * NMU + NCQ + (size_t)NCQ * RB + (L + 2) + nm + perd;
+  return (size_t)ncf * RB * sizeof(double2) + ctad * sizeof(double) + NW * per * sizeof(double2);
 }
 
 template <bool FROM_LOCAL, int Q, int RB>
 static cudaError_t h3_rot_launch(const qbxfmm_geometry& g, HelmCoeffs hc, int pf, int nrhs,
-                                 const double2* e, const double* gaunt, const double* rot,
-                                 double2* qe, int32_t* err, cudaStream_t st)
+                                 const double2* e, const double* rot, double2* qe, int32_t* err,
+                                 cudaStream_t st)
 {
   size_t sh = h3_rot_smem<FROM_LOCAL, Q, RB>(pf);
   cudaFuncSetAttribute(k_h3_e2qbxl_rot<FROM_LOCAL, Q, RB>,
                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
   dim3 grid(g.nqbx_chunks, (nrhs + RB - 1) / RB, H3_ROT_ZS);
-  k_h3_e2qbxl_rot<FROM_LOCAL, Q, RB><<<grid, NT, sh, st>>>(g, hc, pf, nrhs, e, gaunt, rot, qe, err);
+  k_h3_e2qbxl_rot<FROM_LOCAL, Q, RB><<<grid, NT, sh, st>>>(g, hc, pf, nrhs, e, rot, qe, err);
   return cudaGetLastError();
 }
 
-// densities per CTA: the largest of 8, 4, 2, 1 that fits the shared memory
+// densities per CTA: 8 when two CTAs still fit an SM's shared memory, else 4, else 1
 template <bool FROM_LOCAL, int Q>
 static cudaError_t h3_rot_q(const qbxfmm_geometry& g, HelmCoeffs hc, int pf, int nrhs,
-                            const double2* e, const double* gaunt, const double* rot, double2* qe,
-                            int32_t* err, cudaStream_t st)
+                            const double2* e, const double* rot, double2* qe, int32_t* err,
+                            cudaStream_t st)
 {
-  const size_t lim = 220 * 1024;
-  if (nrhs >= 8 && h3_rot_smem<FROM_LOCAL, Q, 8>(pf) <= lim)
-    return h3_rot_launch<FROM_LOCAL, Q, 8>(g, hc, pf, nrhs, e, gaunt, rot, qe, err, st);
-  if (nrhs >= 4 && h3_rot_smem<FROM_LOCAL, Q, 4>(pf) <= lim)
-    return h3_rot_launch<FROM_LOCAL, Q, 4>(g, hc, pf, nrhs, e, gaunt, rot, qe, err, st);
-  if (nrhs >= 2 && h3_rot_smem<FROM_LOCAL, Q, 2>(pf) <= lim)
-    return h3_rot_launch<FROM_LOCAL, Q, 2>(g, hc, pf, nrhs, e, gaunt, rot, qe, err, st);
-  return h3_rot_launch<FROM_LOCAL, Q, 1>(g, hc, pf, nrhs, e, gaunt, rot, qe, err, st);
+  const size_t two_per_sm = 112 * 1024;
+  if (nrhs >= 8 && h3_rot_smem<FROM_LOCAL, Q, 8>(pf) <= two_per_sm)
+    return h3_rot_launch<FROM_LOCAL, Q, 8>(g, hc, pf, nrhs, e, rot, qe, err, st);
+  if (nrhs >= 4)
+    return h3_rot_launch<FROM_LOCAL, Q, 4>(g, hc, pf, nrhs, e, rot, qe, err, st);
+  return h3_rot_launch<FROM_LOCAL, Q, 1>(g, hc, pf, nrhs, e, rot, qe, err, st);
 }
 
 template <bool FROM_LOCAL>
 static cudaError_t h3_e2qbxl(const qbxfmm_geometry& g, HelmCoeffs hc, int pf, int q, int nrhs,
-                             const double2* e, const double* gaunt, const double* rot, double2* qe,
-                             int32_t* err, cudaStream_t st)
+                             const double2* e, const double* rot, double2* qe, int32_t* err,
+                             cudaStream_t st)
 {
   if (g.nqbx_chunks == 0) return cudaSuccess;
+  if (2 * pf + 1 > 35) return cudaErrorInvalidValue;   // recurrence slots per lane
   switch (q) {
-    case 0: return h3_rot_q<FROM_LOCAL, 0>(g, hc, pf, nrhs, e, gaunt, rot, qe, err, st);
-    case 1: return h3_rot_q<FROM_LOCAL, 1>(g, hc, pf, nrhs, e, gaunt, rot, qe, err, st);
-    case 2: return h3_rot_q<FROM_LOCAL, 2>(g, hc, pf, nrhs, e, gaunt, rot, qe, err, st);
-    case 3: return h3_rot_q<FROM_LOCAL, 3>(g, hc, pf, nrhs, e, gaunt, rot, qe, err, st);
-    case 4: return h3_rot_q<FROM_LOCAL, 4>(g, hc, pf, nrhs, e, gaunt, rot, qe, err, st);
-    case 5: return h3_rot_q<FROM_LOCAL, 5>(g, hc, pf, nrhs, e, gaunt, rot, qe, err, st);
+    case 0: return h3_rot_q<FROM_LOCAL, 0>(g, hc, pf, nrhs, e, rot, qe, err, st);
+    case 1: return h3_rot_q<FROM_LOCAL, 1>(g, hc, pf, nrhs, e, rot, qe, err, st);
+    case 2: return h3_rot_q<FROM_LOCAL, 2>(g, hc, pf, nrhs, e, rot, qe, err, st);
+    case 3: return h3_rot_q<FROM_LOCAL, 3>(g, hc, pf, nrhs, e, rot, qe, err, st);
+    case 4: return h3_rot_q<FROM_LOCAL, 4>(g, hc, pf, nrhs, e, rot, qe, err, st);
+    case 5: return h3_rot_q<FROM_LOCAL, 5>(g, hc, pf, nrhs, e, rot, qe, err, st);
     default: return cudaErrorInvalidValue;
   }
 }
 
 cudaError_t h3_launch_m2qbxl(const qbxfmm_geometry& g, HelmCoeffs hc, int pf, int q, int nrhs,
-                             const double2* mp, const double* gaunt, const double* rot,
-                             double2* qe, int32_t* err, cudaStream_t st)
+                             const double2* mp, const double* rot, double2* qe, int32_t* err,
+                             cudaStream_t st)
 {
-  return h3_e2qbxl<false>(g, hc, pf, q, nrhs, mp, gaunt, rot, qe, err, st);
+  return h3_e2qbxl<false>(g, hc, pf, q, nrhs, mp, rot, qe, err, st);
 }
 
 cudaError_t h3_launch_l2qbxl(const qbxfmm_geometry& g, HelmCoeffs hc, int pf, int q, int nrhs,
-                             const double2* lo, const double* gaunt, const double* rot,
-                             double2* qe, int32_t* err, cudaStream_t st)
+                             const double2* lo, const double* rot, double2* qe, int32_t* err,
+                             cudaStream_t st)
 {
-  return h3_e2qbxl<true>(g, hc, pf, q, nrhs, lo, gaunt, rot, qe, err, st);
+  return h3_e2qbxl<true>(g, hc, pf, q, nrhs, lo, rot, qe, err, st);
 }
 
 cudaError_t h3_launch_qbxl2p(const qbxfmm_geometry& g, HelmCoeffs hc, int q, int nrhs,
