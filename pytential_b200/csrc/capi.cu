@@ -5,11 +5,15 @@
 // all in the driver's order.  Stage outputs are accumulated (+=) into caller-owned
 // device buffers; the library allocates no device memory.
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <new>
+#include <numeric>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/qbxfmm_api.h"
@@ -33,8 +37,11 @@ struct qbxfmm_plan {
   bool mixed;                              // FP32 far field (3D Laplace)
   bool tf32_ok;                            // split-TF32 translation matrices in use
   std::vector<double> h3gaunt;             // Gaunt table, [(nu,mu)][j][(n,m)]
-  std::vector<int32_t> m2l_waves;          // runs of M2L classes with one offset (3D Helmholtz)
   std::vector<double> h3rot;               // rotation tables, after the Gaunt table
+  // host part of the rotation-based M2L tables (h3_m2l_host_tables), after the
+  // rotation tables; then the device-built direction and coaxial tables
+  std::vector<double> h3m2l;
+  int h3_ndir = 0, h3_ncoax = 0;
   // 3D Helmholtz: translation buffer and pair scratch registered by
   // qbxfmm_precompute_translations, used by the translation stage entries
   mutable const double* trans_dev = nullptr;
@@ -77,6 +84,28 @@ int check_plan(const qbxfmm_plan* p)
 {
   if (!p) return fail(QBXFMM_ERR_ARG, "null plan");
   return QBXFMM_OK;
+}
+
+size_t h3_rot_offset(const qbxfmm_plan* p);
+
+// Offsets in doubles of the 3D Helmholtz sections of the translation buffer, after
+// the M2M / L2L matrices: [0] Gaunt table, [1] rotation tables, [2] host M2L tables,
+// [3] M2L direction tables, [4] M2L coaxial tables (complex), [5] end.
+void h3_layout(const qbxfmm_plan* p, size_t o[6])
+{
+  o[0] = p->tc.nmatrices * p->tc.rp * p->tc.kp;
+  o[1] = o[0] + p->h3gaunt.size();
+  o[2] = (o[1] + p->h3rot.size() + 1) & ~(size_t)1;
+  o[3] = o[2] + p->h3m2l.size();
+  o[4] = o[3] + (size_t)p->h3_ndir * h3_m2l_dsize(p->kern.fmm_order);
+  o[5] = o[4] + 2 * (size_t)p->h3_ncoax * h3_m2l_csize(p->kern.fmm_order);
+}
+
+size_t h3_rot_offset(const qbxfmm_plan* p)
+{
+  size_t o[6];
+  h3_layout(p, o);
+  return o[1];
 }
 
 // Gaunt integrals G(n,m; nu,mu; l) = int Y_n^m conj(Y_nu^mu) conj(Y_l^{m-mu}) for
@@ -203,6 +232,71 @@ std::vector<double> h3_rotation_tables(int p, int q, const std::vector<double>& 
   return t;
 }
 
+// Host part of the 3D Helmholtz M2L tables (p = fmm order), laid out as
+//   start[(m + p)(2p + 1) + mu + p][4]: d^n_{m mu}(beta) at n0 = max(|m|, |mu|) for all
+//     |m|, |mu| <= p (coefficient, exponents of cos(beta/2) and sin(beta/2), unused);
+//   dirs[ndir][4]: the distinct directions of the M2L class offsets (unit vectors);
+//   coaxp[ncoax][2]: (k |b|, min(1, k width)) for the distinct (|offset|^2, level);
+//   clsmap[nclasses][2]: direction and coaxial table of each class;
+// padded to an even length.  offs: [3][nclasses] integer offsets in box widths.
+std::vector<double> h3_m2l_host_tables(int p, double k, double root_extent, int nclasses,
+                                       const std::vector<int32_t>& offs,
+                                       const std::vector<int32_t>& levels, int* ndir_out,
+                                       int* ncoax_out)
+{
+  const int nm = 2 * p + 1;
+  std::vector<double> start((size_t)nm * nm * 4, 0.0);
+  for (int m = -p; m <= p; ++m)
+    for (int mu = -p; mu <= p; ++mu) {
+      size_t idx = (size_t)(m + p) * nm + (mu + p);
+      int j = std::max(std::abs(m), std::abs(mu));
+      int kk = std::max(0, mu - m);
+      int a1 = j + mu - kk, a3 = j - kk - m, a4 = kk - mu + m;
+      double lf = 0.5 * (std::lgamma(j + m + 1.0) + std::lgamma(j - m + 1.0) +
+                         std::lgamma(j + mu + 1.0) + std::lgamma(j - mu + 1.0)) -
+                  (std::lgamma(a1 + 1.0) + std::lgamma(kk + 1.0) + std::lgamma(a3 + 1.0) +
+                   std::lgamma(a4 + 1.0));
+      start[4 * idx] = (((kk - mu + m) & 1) ? -1.0 : 1.0) * std::exp(lf);
+      start[4 * idx + 1] = 2 * j + mu - m - 2 * kk;
+      start[4 * idx + 2] = 2 * kk - mu + m;
+    }
+  std::map<std::array<int, 3>, int> dir_id;
+  std::map<std::pair<int, int>, int> coax_id;
+  std::vector<double> dirs, coaxp, clsmap(2 * (size_t)nclasses);
+  for (int c = 0; c < nclasses; ++c) {
+    int o[3] = {offs[c], offs[(size_t)nclasses + c], offs[2 * (size_t)nclasses + c]};
+    int gd = std::gcd(std::gcd(std::abs(o[0]), std::abs(o[1])), std::abs(o[2]));
+    if (gd == 0) gd = 1;
+    std::array<int, 3> key = {o[0] / gd, o[1] / gd, o[2] / gd};
+    auto it = dir_id.find(key);
+    if (it == dir_id.end()) {
+      double len = std::sqrt((double)key[0] * key[0] + (double)key[1] * key[1] + (double)key[2] * key[2]);
+      it = dir_id.emplace(key, (int)dir_id.size()).first;
+      dirs.insert(dirs.end(), {key[0] / len, key[1] / len, key[2] / len, 0.0});
+    }
+    int n2 = o[0] * o[0] + o[1] * o[1] + o[2] * o[2];
+    auto ck = std::make_pair(n2, levels[c]);
+    auto jt = coax_id.find(ck);
+    if (jt == coax_id.end()) {
+      double w = std::ldexp(root_extent, -levels[c]);
+      jt = coax_id.emplace(ck, (int)coax_id.size()).first;
+      coaxp.insert(coaxp.end(), {k * std::sqrt((double)n2) * w, std::min(1.0, k * w)});
+    }
+    clsmap[2 * (size_t)c] = it->second;
+    clsmap[2 * (size_t)c + 1] = jt->second;
+  }
+  *ndir_out = (int)dir_id.size();
+  *ncoax_out = (int)coax_id.size();
+  std::vector<double> t;
+  t.reserve(start.size() + dirs.size() + coaxp.size() + clsmap.size() + 1);
+  t.insert(t.end(), start.begin(), start.end());
+  t.insert(t.end(), dirs.begin(), dirs.end());
+  t.insert(t.end(), coaxp.begin(), coaxp.end());
+  t.insert(t.end(), clsmap.begin(), clsmap.end());
+  if (t.size() & 1) t.push_back(0.0);
+  return t;
+}
+
 #define QBX_TRY(expr, where)                         \
   do {                                               \
     int _rc = cuda_check((expr), where);             \
@@ -298,7 +392,7 @@ int qbxfmm_plan_create(const qbxfmm_kernel* kernel, const qbxfmm_geometry* geome
   p->h3 = p->helm && k.dim == 3;
   p->mixed = k.precision == 1;
   if (k.dim == 3)
-    p->tc = p->h3 ? trans_cfg_helm3(k.fmm_order, g.m2l_nclasses, g.nlevels)
+    p->tc = p->h3 ? trans_cfg_helm3(k.fmm_order, 0, g.nlevels)   // M2L by rotation, no class matrices
                   : trans_cfg_laplace3(k.fmm_order, g.m2l_nclasses);
   p->trans_ok = k.dim == 3 && trans_supported(p->tc) && g.nlevels <= 64;
   p->tf32_ok = p->mixed && p->trans_ok && tf32_supported(p->tc);
@@ -309,18 +403,16 @@ int qbxfmm_plan_create(const qbxfmm_kernel* kernel, const qbxfmm_geometry* geome
   if (p->h3) {
     p->h3gaunt = h3_gaunt_table(k.fmm_order);
     p->h3rot = h3_rotation_tables(k.fmm_order, k.qbx_order, p->h3gaunt);
-    std::vector<int32_t> off(3 * (size_t)g.m2l_nclasses);
-    if (g.m2l_nclasses > 0)
+    std::vector<int32_t> off(3 * (size_t)g.m2l_nclasses), lev(g.m2l_nclasses);
+    if (g.m2l_nclasses > 0 && e == cudaSuccess)
       e = cudaMemcpy(off.data(), g.m2l_class_offsets, sizeof(int32_t) * off.size(),
                      cudaMemcpyDeviceToHost);
-    p->m2l_waves.push_back(0);
-    for (int c = 1; c < g.m2l_nclasses; ++c) {
-      bool same = true;
-      for (int d = 0; d < 3; ++d) same = same && off[(size_t)d * g.m2l_nclasses + c] ==
-                                                   off[(size_t)d * g.m2l_nclasses + c - 1];
-      if (!same) p->m2l_waves.push_back(c);
-    }
-    p->m2l_waves.push_back(g.m2l_nclasses);
+    if (g.m2l_nclasses > 0 && e == cudaSuccess)
+      e = cudaMemcpy(lev.data(), g.m2l_class_levels, sizeof(int32_t) * lev.size(),
+                     cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess)
+      p->h3m2l = h3_m2l_host_tables(k.fmm_order, k.k_re, g.root_extent, g.m2l_nclasses, off, lev,
+                                    &p->h3_ndir, &p->h3_ncoax);
   }
   if (e == cudaSuccess && p->trans_ok) {
     const int nch = 8;
@@ -458,9 +550,15 @@ int qbxfmm_multipole_to_local(const qbxfmm_plan* p, const void* mpoles, void* lo
   if (p->h3) {
     if (!p->trans_dev)
       return fail(QBXFMM_ERR_ARG, "3D Helmholtz: call qbxfmm_precompute_translations first");
-    QBX_TRY(launch_m2l_direct(p->geo, p->th, p->tc, p->m2l_waves.data(),
-                              (int)p->m2l_waves.size() - 1, p->kern.nrhs, p->trans_dev,
-                              (const double2*)mpoles, (double2*)locals, error_word, S(stream)),
+    size_t o[6];
+    h3_layout(p, o);
+    const int nm = 2 * p->kern.fmm_order + 1;
+    const double* clsmap = p->trans_dev + o[2] + (size_t)nm * nm * 4 + 4 * (size_t)p->h3_ndir +
+                           2 * (size_t)p->h3_ncoax;
+    QBX_TRY(h3_launch_m2l_rot(p->geo, p->kern.fmm_order, p->kern.nrhs, (const double2*)mpoles,
+                              (double2*)locals, p->trans_dev + o[3],
+                              reinterpret_cast<const double2*>(p->trans_dev + o[4]), clsmap,
+                              error_word, S(stream)),
             "multipole_to_local");
     return QBXFMM_OK;
   }
@@ -595,7 +693,7 @@ int qbxfmm_translate_box_multipoles_to_qbx_local(const qbxfmm_plan* p, const voi
       return fail(QBXFMM_ERR_ARG, "3D Helmholtz: call qbxfmm_precompute_translations first");
     QBX_TRY(h3_launch_m2qbxl(p->geo, p->hc, p->kern.fmm_order, p->kern.qbx_order, p->kern.nrhs,
                              (const double2*)mpoles,
-                             p->trans_dev + p->tc.nmatrices * p->tc.rp * p->tc.kp + p->h3gaunt.size(),
+                             p->trans_dev + h3_rot_offset(p),
                              (double2*)qbx_exps, error_word, S(stream)),
             "translate_box_multipoles_to_qbx_local");
     return QBXFMM_OK;
@@ -624,7 +722,7 @@ int qbxfmm_translate_box_local_to_qbx_local(const qbxfmm_plan* p, const void* lo
       return fail(QBXFMM_ERR_ARG, "3D Helmholtz: call qbxfmm_precompute_translations first");
     QBX_TRY(h3_launch_l2qbxl(p->geo, p->hc, p->kern.fmm_order, p->kern.qbx_order, p->kern.nrhs,
                              (const double2*)locals,
-                             p->trans_dev + p->tc.nmatrices * p->tc.rp * p->tc.kp + p->h3gaunt.size(),
+                             p->trans_dev + h3_rot_offset(p),
                              (double2*)qbx_exps, nullptr, S(stream)),
             "translate_box_local_to_qbx_local");
     return QBXFMM_OK;
@@ -719,8 +817,10 @@ int qbxfmm_workspace_sizes(const qbxfmm_plan* p, size_t* sizes6 /* 8 entries */)
   sizes6[5] = nr * (size_t)g.ntargets * scal;
   if (p->trans_ok) {
     int npairs = std::max(p->th.m2l_npairs, g.m2m_npairs);
-    sizes6[6] = trans_matrix_bytes(p->tc) + (p->h3gaunt.size() + p->h3rot.size()) * sizeof(double) +
-                (p->tf32_ok ? tf32_matrix_bytes(p->tc) : 0);
+    size_t o[6];
+    h3_layout(p, o);
+    sizes6[6] = p->h3 ? o[5] * sizeof(double)
+                      : trans_matrix_bytes(p->tc) + (p->tf32_ok ? tf32_matrix_bytes(p->tc) : 0);
     sizes6[7] = p->h3 ? 0 : trans_scratch_bytes(p->tc, npairs, p->kern.nrhs);
   } else {
     sizes6[6] = sizes6[7] = 0;
@@ -736,15 +836,31 @@ int qbxfmm_precompute_translations(const qbxfmm_plan* p, const qbxfmm_workspace*
     if (!ws->translations)
       return fail(QBXFMM_ERR_ARG, "3D Helmholtz needs the translations buffer");
     double* T = (double*)ws->translations;
-    double* G = T + p->tc.nmatrices * p->tc.rp * p->tc.kp;
+    size_t o[6];
+    h3_layout(p, o);
+    const int pf = p->kern.fmm_order, q = p->kern.qbx_order, nm = 2 * pf + 1;
+    double* G = T + o[0];
+    double* R = T + o[1];
+    double* H = T + o[2];
     QBX_TRY(cudaMemcpyAsync(G, p->h3gaunt.data(), p->h3gaunt.size() * sizeof(double),
                             cudaMemcpyHostToDevice, S(stream)),
             "precompute_translations: Gaunt table");
-    QBX_TRY(cudaMemcpyAsync(G + p->h3gaunt.size(), p->h3rot.data(), p->h3rot.size() * sizeof(double),
+    QBX_TRY(cudaMemcpyAsync(R, p->h3rot.data(), p->h3rot.size() * sizeof(double),
                             cudaMemcpyHostToDevice, S(stream)),
             "precompute_translations: rotation tables");
+    QBX_TRY(cudaMemcpyAsync(H, p->h3m2l.data(), p->h3m2l.size() * sizeof(double),
+                            cudaMemcpyHostToDevice, S(stream)),
+            "precompute_translations: M2L tables");
     QBX_TRY(h3_launch_trans_build(p->geo, p->tc, p->kern.k_re, G, T, S(stream)),
             "precompute_translations");
+    // rotation-table layout (h3_rotation_tables): start values, then isq, then rt
+    const double* isq = R + (size_t)nm * (q + 1) * 4;
+    const double* rt = isq + (size_t)(pf + 2) * (pf + 1);
+    const double* dirs = H + (size_t)nm * nm * 4;
+    const double* coaxp = dirs + 4 * (size_t)p->h3_ndir;
+    QBX_TRY(h3_launch_m2l_tables(pf, p->h3_ndir, p->h3_ncoax, dirs, coaxp, H, isq, rt, G, T + o[3],
+                                 reinterpret_cast<double2*>(T + o[4]), S(stream)),
+            "precompute_translations: M2L tables");
     p->trans_dev = T;
     p->scratch_dev = (double*)ws->pair_scratch;
     return QBXFMM_OK;

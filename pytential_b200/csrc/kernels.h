@@ -73,9 +73,6 @@ cudaError_t launch_l2l_gemm_mixed(const qbxfmm_geometry& g, const TransHost& th,
                                   int nrhs, const uint32_t* T32, double2* lo, int32_t* err,
                                   cudaStream_t st);
 // scratch-free forms on the tiled kernel (per-level classes, 3D Helmholtz)
-cudaError_t launch_m2l_direct(const qbxfmm_geometry& g, const TransHost& th, const TransCfg& c,
-                              const int32_t* waves, int nwaves, int nrhs, const double* T,
-                              const double2* mp, double2* lo, int32_t* err, cudaStream_t st);
 cudaError_t launch_m2m_direct(const qbxfmm_geometry& g, const TransHost& th, const TransCfg& c,
                               int nrhs, const double* T, double2* mp, int32_t* err, cudaStream_t st);
 cudaError_t launch_l2l_direct(const qbxfmm_geometry& g, const TransHost& th, const TransCfg& c,
@@ -157,6 +154,19 @@ cudaError_t h3_launch_eval_locals(const qbxfmm_geometry& g, HelmCoeffs hc, int p
                                   const double2* lo, double2* pot, cudaStream_t st);
 cudaError_t h3_launch_p2qbxl(const qbxfmm_geometry& g, HelmCoeffs hc, int q, int nrhs,
                              const double2* s, double2* qe, int32_t* err, cudaStream_t st);
+// 3D Helmholtz M2L by rotation: per-direction rotation tables (Dtab, h3_m2l_dsize
+// doubles each) and per-(length, level) coaxial tables (Ctab, h3_m2l_csize complex
+// each) built by h3_launch_m2l_tables; clsmap[2 c] / [2 c + 1] = direction / coaxial
+// table of M2L class c.
+__host__ __device__ size_t h3_m2l_dsize(int pf);
+__host__ __device__ size_t h3_m2l_csize(int pf);
+cudaError_t h3_launch_m2l_tables(int pf, int ndir, int ncoax, const double* dirs,
+                                 const double* coaxp, const double* start, const double* isq,
+                                 const double* rt, const double* gaunt, double* Dtab,
+                                 double2* Ctab, cudaStream_t st);
+cudaError_t h3_launch_m2l_rot(const qbxfmm_geometry& g, int pf, int nrhs, const double2* mp,
+                              double2* lo, const double* Dtab, const double2* Ctab,
+                              const double* clsmap, int32_t* err, cudaStream_t st);
 // rot: rotation tables of h3_rotation_tables (start values, recurrence factors,
 // lambda = 0 Gaunt slice)
 cudaError_t h3_launch_m2qbxl(const qbxfmm_geometry& g, HelmCoeffs hc, int pf, int q, int nrhs,

@@ -31,6 +31,7 @@ constexpr int NT = 128;
 constexpr int NW = NT / 32;
 constexpr int MAXB = 128;
 constexpr int H3_LMAX = 44;        // largest order of a radial / harmonic table
+constexpr int H3_MAXP = 17;        // largest FMM order
 constexpr double FOUR_PI = 12.566370614359172953850573533118;
 
 QBX_HD int hq(int n, int m) { return n * n + n + m; }
@@ -1233,15 +1234,13 @@ k_h3_tsqbx(qbxfmm_geometry g, HelmCoeffs hc, int nrhs, const double2* __restrict
 
 // {{{ translation matrices
 
-// One CTA per matrix.  kind 0: M2L class (level and integer offset; b = offset * width),
-// kind 1: M2M (parent level lev, child position ci; b = c_parent - c_child),
-// kind 2: L2L (child level lev, child position ci; b = c_child - c_parent).
+// One CTA per matrix.  kind 1: M2M (parent level lev, child position ci; b = c_parent -
+// c_child), kind 2: L2L (child level lev, child position ci; b = c_child - c_parent).
 // T is the real (rp x kp) form of the complex (ncf x ncf) matrix acting on
 // interleaved (re, im) coefficient vectors; entries outside 2 ncf are zero.
 __global__ void __launch_bounds__(NT)
-k_h3_trans_build(int kind, int p, int rp, int kp, double k, double root_extent, int nclasses,
-                 const int32_t* __restrict__ offs, const int32_t* __restrict__ cls_levels,
-                 int lev0, const double* __restrict__ gaunt, double* __restrict__ T)
+k_h3_trans_build(int kind, int p, int rp, int kp, double k, double root_extent, int lev0,
+                 const double* __restrict__ gaunt, double* __restrict__ T)
 {
   extern __shared__ double2 smem2[];
   const int L = 2 * p;
@@ -1255,15 +1254,7 @@ k_h3_trans_build(int kind, int p, int rp, int kp, double k, double root_extent, 
   double b[3];
   double s_in, s_out;
   int e_in, e_out;
-  bool singular;
-  if (kind == 0) {
-    int lev = cls_levels[mi];
-    double wdt = ldexp(root_extent, -lev);
-    for (int d = 0; d < 3; ++d) b[d] = offs[d * nclasses + mi] * wdt;
-    s_in = s_out = fmin(1.0, k * wdt);
-    e_in = e_out = 1;
-    singular = true;
-  } else {
+  {
     int lev = lev0 + mi / 8, ci = mi % 8;
     int plev = (kind == 1) ? lev : lev - 1;        // parent level
     double wp = ldexp(root_extent, -plev);
@@ -1275,21 +1266,15 @@ k_h3_trans_build(int kind, int p, int rp, int kp, double k, double root_extent, 
     } else {
       s_in = sp; e_in = -1; s_out = sc; e_out = 1;
     }
-    singular = false;
   }
   h3_rec_table(L, rec, threadIdx.x, NT);
   double2 w;
   double rr;
   double t = h3_dir(b, w, rr);
   if (threadIdx.x == 0) {
-    if (singular) {
-      h3_sph_h(L, k * rr, rad);
-    } else {
-      double jv[H3_LMAX + 2];
-      h3_sph_j(L, k * rr, jv);
-      for (int l = 0; l <= L; ++l) rad[l] = c2(jv[l]);
-    }
-    for (int l = 0; l <= L; ++l) rad[l] = cmul(cscale(FOUR_PI, ipow(l)), rad[l]);
+    double jv[H3_LMAX + 2];
+    h3_sph_j(L, k * rr, jv);
+    for (int l = 0; l <= L; ++l) rad[l] = cmul(cscale(FOUR_PI, ipow(l)), c2(jv[l]));
   }
   for (int n = threadIdx.x; n <= p; n += NT) {
     pw[n] = pow(s_in, (double)(e_in * n));
@@ -1353,6 +1338,348 @@ __global__ void k_h3_assemble_nonqbx(qbxfmm_geometry g, int nrhs,
     double2* o = out + (size_t)r * g.nuser_targets + u;
     *o = caxpy(1.0 / FOUR_PI, pot_nonqbx[(size_t)r * g.nfiltered_targets + f], *o);
   }
+}
+
+// }}}
+
+// {{{ M2L by rotation (3D Helmholtz)
+
+// Multipole -> local translation between boxes of one level by rotation, coaxial
+// translation and back rotation (the same factorization as the QBX translations
+// above, with output order pf and all |mu| <= pf).  The rotation depends only on the
+// direction of the box offset and the coaxial part only on its length and the level,
+// so both are tabulated once per plan: per direction the phases e^{i m alpha} and the
+// blocks eps_m eps_mu d^n_{m mu}(beta), |m|, |mu| <= n <= pf (H3M2L_D doubles); per
+// (length, level) the coaxial blocks, one per mu, C^mu[n][nu] = s^nu s^n i^{nu-n}
+// sum_j G(n,mu; nu,mu; |n-nu|+2j) sqrt(4 pi (2l+1)) i^l h_l(k|b|) (l = |n-nu|+2j),
+// s = min(1, k width) (H3M2L_C complex entries).
+
+QBX_D int h3_dblock(int n) { return n * (4 * n * n - 1) / 3; }   // sum_{k<n} (2k+1)^2
+
+// start of mu's coaxial block, mu = -pf .. pf in that order
+QBX_D int h3_cblock(int pf, int mu)
+{
+  int o = 0;
+  for (int u = -pf; u < mu; ++u) {
+    int w = pf + 1 - abs(u);
+    o += w * w;
+  }
+  return o;
+}
+
+__host__ __device__ size_t h3_m2l_dsize(int pf)
+{
+  size_t nm = 2 * pf + 1;
+  size_t v = 2 * nm + (size_t)(pf + 1) * (4 * (pf + 1) * (pf + 1) - 1) / 3;
+  return (v + 1) & ~(size_t)1;
+}
+
+__host__ __device__ size_t h3_m2l_csize(int pf)
+{
+  size_t s = 0;
+  for (int u = -pf; u <= pf; ++u) {
+    size_t w = pf + 1 - (u < 0 ? -u : u);
+    s += w * w;
+  }
+  return s;
+}
+
+// Tables: CTAs [0, ndir) one direction each, [ndir, ndir + ncoax) one (length, level)
+// each.  dirs[4 d] = unit offset; coaxp[2 c] = (k |b|, s); start: [nm][nm][4] start
+// values of d^n_{m mu} (coefficient, exponents of cos and sin of beta/2); isq / rt: the
+// recurrence factors of the rotation tables; gaunt: [(nu,mu)][j][(n,m)].
+__global__ void __launch_bounds__(NT)
+k_h3_m2l_tables(int pf, int ndir, int ncoax, const double* __restrict__ dirs,
+                const double* __restrict__ coaxp, const double* __restrict__ start,
+                const double* __restrict__ isq, const double* __restrict__ rt,
+                const double* __restrict__ gaunt, double* __restrict__ Dtab,
+                double2* __restrict__ Ctab)
+{
+  __shared__ double2 s_rad[2 * H3_MAXP + 4];
+  __shared__ double s_pw[H3_MAXP + 1];
+  const int nm = 2 * pf + 1, nl = pf + 1, ncf = (pf + 1) * (pf + 1);
+  if ((int)blockIdx.x < ndir) {
+    const double* u = dirs + 4 * blockIdx.x;
+    double cbeta = fmin(1.0, fmax(-1.0, u[2]));
+    double alpha = (u[0] == 0.0 && u[1] == 0.0) ? 0.0 : atan2(u[1], u[0]);
+    double beta = acos(cbeta);
+    double ch = cos(0.5 * beta), sh = sin(0.5 * beta);
+    double* D = Dtab + blockIdx.x * h3_m2l_dsize(pf);
+    double2* ph = reinterpret_cast<double2*>(D);
+    double* blocks = D + 2 * nm;
+    for (int m = threadIdx.x; m < nm; m += NT) {
+      double sn, cs;
+      sincos((m - pf) * alpha, &sn, &cs);
+      ph[m] = c2(cs, sn);
+    }
+    for (int t = threadIdx.x; t < nm * nm; t += NT) {
+      int m = t / nm - pf, mu = t % nm - pf;
+      int am = abs(m), amu = abs(mu);
+      int n0 = max(am, amu);
+      double v = start[4 * t];
+      int ec = (int)start[4 * t + 1], es = (int)start[4 * t + 2];
+      for (int k = 0; k < ec; ++k) v *= ch;
+      for (int k = 0; k < es; ++k) v *= sh;
+      double eps = ((m > 0 && (m & 1)) ? -1.0 : 1.0) * ((mu > 0 && (mu & 1)) ? -1.0 : 1.0);
+      double prev = 0.0, cur = v;
+      for (int n = n0; n <= pf; ++n) {
+        blocks[h3_dblock(n) + (m + n) * (2 * n + 1) + (mu + n)] = eps * cur;
+        if (n == pf) break;
+        double nxt;
+        if (n == 0) {
+          nxt = cbeta * cur;
+        } else {
+          double rn = 1.0 / n;
+          double w = rn * isq[(n + 1) * (pf + 1) + am] * isq[(n + 1) * (pf + 1) + amu];
+          double A = (2.0 * n + 1.0) * (n * (n + 1.0) * cbeta - (double)m * mu) * w;
+          double C = (n + 1.0) * rn * rt[n * (pf + 1) + am] * rt[n * (pf + 1) + amu];
+          nxt = fma(A, cur, -C * prev);
+        }
+        prev = cur;
+        cur = nxt;
+      }
+    }
+    return;
+  }
+  int c = blockIdx.x - ndir;
+  if (c >= ncoax) return;
+  double kb = coaxp[2 * c], s = coaxp[2 * c + 1];
+  const int L = 2 * pf;
+  if (threadIdx.x == 0) {
+    h3_sph_h(L, kb, s_rad);
+    for (int l = 0; l <= L; ++l) s_rad[l] = cmul(cscale(sqrt(FOUR_PI * (2.0 * l + 1.0)), ipow(l)), s_rad[l]);
+  }
+  for (int n = threadIdx.x; n <= pf; n += NT) s_pw[n] = pow(s, (double)n);
+  __syncthreads();
+  double2* C = Ctab + (size_t)c * h3_m2l_csize(pf);
+  int total = (int)h3_m2l_csize(pf);
+  for (int e = threadIdx.x; e < total; e += NT) {
+    // decode (mu, n, nu)
+    int mu = -pf, off = 0;
+    for (;;) {
+      int w = pf + 1 - abs(mu);
+      if (e < off + w * w) break;
+      off += w * w;
+      ++mu;
+    }
+    int am = abs(mu), w = pf + 1 - am;
+    int n = am + (e - off) / w, nu = am + (e - off) % w;
+    int o = nu * nu + nu + mu;
+    int lbase = abs(n - nu), jmax = min(n, nu);
+    double2 tt = c2(0.0);
+    for (int j = 0; j <= jmax; ++j)
+      tt = caxpy(__ldg(gaunt + ((size_t)o * nl + j) * ncf + n * n + n + mu), s_rad[lbase + 2 * j], tt);
+    tt = cmul(ipow(nu - n + 4 * pf), tt);
+    C[e] = cscale(s_pw[nu] * s_pw[n], tt);
+  }
+}
+
+constexpr int H3M2L_NT = 256;
+// task groups of 4 outputs: sum_n ceil((2n+1)/4) <= 99 and sum_mu ceil((pf+1-|mu|)/4)
+// <= 116 for pf <= H3_MAXP
+constexpr int H3M2L_NG = 100;
+constexpr int H3M2L_NCG = 120;
+
+// One CTA per target-or-parent box (blockIdx.x) and group of RB densities; its
+// list-2 sources in turn: X = e^{i m alpha} M (shared), A = rotated (all n, |mu| <= n),
+// B = coaxially translated (into X), then the back rotation adds into register
+// accumulators owned by fixed (order, 4 consecutive m, density) tasks; the sum is
+// added into the box's local once.  Each task keeps four outputs, so one shared
+// load of the input feeds eight FMAs.
+template <int RB>
+__global__ void __launch_bounds__(H3M2L_NT)
+k_h3_m2l_rot(qbxfmm_geometry g, int pf, int nrhs, const double2* __restrict__ mp,
+             double2* __restrict__ lo, const double* __restrict__ Dtab,
+             const double2* __restrict__ Ctab, const double* __restrict__ clsmap,
+             int32_t* err)
+{
+  extern __shared__ double2 smem2[];
+  __shared__ int s_gn[H3M2L_NG], s_gm0[H3M2L_NG];        // rotation task groups
+  __shared__ int s_cmu[H3M2L_NCG], s_cnu0[H3M2L_NCG];    // coaxial task groups
+  __shared__ int s_ng, s_ncg;
+  constexpr int NTHR = H3M2L_NT;
+  constexpr int KMAX = (H3M2L_NG * RB + NTHR - 1) / NTHR;
+  const int ncf = (pf + 1) * (pf + 1), XS = ncf + 1, nm = 2 * pf + 1;
+  double2* X = smem2;                       // [RB][ncf + 1]
+  double2* A = smem2 + (size_t)RB * XS;     // [RB][ncf + 1]
+  if (threadIdx.x == 0) {
+    int ng = 0;
+    for (int n = 0; n <= pf; ++n)
+      for (int m0 = -n; m0 <= n; m0 += 4) {
+        s_gn[ng] = n;
+        s_gm0[ng] = m0;
+        ++ng;
+      }
+    s_ng = ng;
+    int ncg = 0;
+    for (int mu = -pf; mu <= pf; ++mu)
+      for (int nu0 = abs(mu); nu0 <= pf; nu0 += 4) {
+        s_cmu[ncg] = mu;
+        s_cnu0[ncg] = nu0;
+        ++ncg;
+      }
+    s_ncg = ncg;
+  }
+  __syncthreads();
+  const int i = blockIdx.x;
+  const int r0 = blockIdx.y * RB;
+  const int q0 = g.m2l_tgt_pair_starts[i], q1 = g.m2l_tgt_pair_starts[i + 1];
+  if (q1 <= q0) return;
+  const int ng = s_ng, ncg = s_ncg;
+  const size_t dsz = h3_m2l_dsize(pf), csz = h3_m2l_csize(pf);
+  double2 acc[KMAX][4];
+#pragma unroll
+  for (int k = 0; k < KMAX; ++k)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[k][j] = c2(0.0);
+
+  for (int q = q0; q < q1; ++q) {
+    int pr = g.m2l_tgt_pairs[q];
+    int src = g.m2l_pair_src[pr];
+    // class of the pair: m2l_class_starts[c] <= pr < m2l_class_starts[c + 1]
+    int lo_c = 0, hi_c = g.m2l_nclasses - 1;
+    while (lo_c < hi_c) {
+      int mid = (lo_c + hi_c + 1) >> 1;
+      if (g.m2l_class_starts[mid] <= pr) lo_c = mid;
+      else hi_c = mid - 1;
+    }
+    if ((unsigned)src >= (unsigned)g.nboxes) {
+      if (threadIdx.x == 0) report(err, QBX_DEVERR_BAD_BOX);
+      continue;   // uniform across the CTA
+    }
+    const double* D = Dtab + (size_t)clsmap[2 * lo_c] * dsz;
+    const double2* ph = reinterpret_cast<const double2*>(D);
+    const double* blocks = D + 2 * nm;
+    const double2* C = Ctab + (size_t)clsmap[2 * lo_c + 1] * csz;
+    // X = e^{i m alpha} M
+    for (int e = threadIdx.x; e < RB * ncf; e += NTHR) {
+      int r = e / ncf, ci = e - r * ncf;
+      int n = (int)sqrt((double)ci);
+      while ((n + 1) * (n + 1) <= ci) ++n;
+      while (n * n > ci) --n;
+      double2 v = c2(0.0);
+      if (r0 + r < nrhs) v = cmul(__ldg(ph + ci - n * n - n + pf), mp[((size_t)src * nrhs + r0 + r) * ncf + ci]);
+      X[r * XS + ci] = v;
+    }
+    __syncthreads();
+    // A[(n, mu)] = sum_m T^n[m][mu] X[(n, m)]
+    for (int t = threadIdx.x; t < ng * RB; t += NTHR) {
+      int grp = t / RB, r = t - grp * RB;
+      int n = s_gn[grp], mu0 = s_gm0[grp];
+      const double* Tn = blocks + h3_dblock(n) + (mu0 + n);
+      const int w = 2 * n + 1, nv = min(4, n - mu0 + 1);
+      double2 o[4] = {c2(0.0), c2(0.0), c2(0.0), c2(0.0)};
+      const double2* Xr = X + r * XS + n * n;
+      for (int m = 0; m < w; ++m) {
+        double2 x = Xr[m];
+        const double* row = Tn + m * w;
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          if (j < nv) o[j] = caxpy(__ldg(row + j), x, o[j]);
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        if (j < nv) A[r * XS + n * n + n + mu0 + j] = o[j];
+    }
+    __syncthreads();
+    // B[(nu, mu)] = sum_{n >= |mu|} C^mu[n][nu] A[(n, mu)]   (into X)
+    for (int t = threadIdx.x; t < ncg * RB; t += NTHR) {
+      int grp = t / RB, r = t - grp * RB;
+      int mu = s_cmu[grp], nu0 = s_cnu0[grp];
+      int am = abs(mu), w = pf + 1 - am, nv = min(4, pf - nu0 + 1);
+      const double2* Cb = C + h3_cblock(pf, mu) + (nu0 - am);
+      double2 o[4] = {c2(0.0), c2(0.0), c2(0.0), c2(0.0)};
+      const double2* Ar = A + r * XS;
+      for (int n = am; n <= pf; ++n) {
+        double2 a = Ar[n * n + n + mu];
+        const double2* row = Cb + (n - am) * w;
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          if (j < nv) o[j] = cfma(__ldg(row + j), a, o[j]);
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        int nu = nu0 + j;
+        if (j < nv) X[r * XS + nu * nu + nu + mu] = o[j];
+      }
+    }
+    __syncthreads();
+    // L[(nu, m2)] += e^{-i m2 alpha} sum_mu T^nu[m2][mu] B[(nu, mu)]
+#pragma unroll
+    for (int k = 0; k < KMAX; ++k) {
+      int t = threadIdx.x + k * NTHR;
+      if (t >= ng * RB) break;
+      int grp = t / RB, r = t - grp * RB;
+      int nu = s_gn[grp], m20 = s_gm0[grp];
+      const int w = 2 * nu + 1, nv = min(4, nu - m20 + 1);
+      const double* Tn = blocks + h3_dblock(nu) + (m20 + nu) * w;
+      double2 o[4] = {c2(0.0), c2(0.0), c2(0.0), c2(0.0)};
+      const double2* Br = X + r * XS + nu * nu;
+      for (int mu = 0; mu < w; ++mu) {
+        double2 b = Br[mu];
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          if (j < nv) o[j] = caxpy(__ldg(Tn + j * w + mu), b, o[j]);
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        if (j < nv) acc[k][j] = cfma(cconj(__ldg(ph + m20 + j + pf)), o[j], acc[k][j]);
+    }
+    __syncthreads();
+  }
+  int tb = g.target_or_target_parent_boxes[i];
+  if ((unsigned)tb >= (unsigned)g.nboxes) {
+    if (threadIdx.x == 0) report(err, QBX_DEVERR_BAD_BOX);
+    return;
+  }
+#pragma unroll
+  for (int k = 0; k < KMAX; ++k) {
+    int t = threadIdx.x + k * NTHR;
+    if (t >= ng * RB) break;
+    int grp = t / RB, r = t - grp * RB;
+    if (r0 + r >= nrhs) continue;
+    int nu = s_gn[grp], m20 = s_gm0[grp];
+    int nv = min(4, nu - m20 + 1);
+    double2* out = lo + ((size_t)tb * nrhs + r0 + r) * ncf + nu * nu + nu + m20;
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      if (j < nv) out[j] = cadd(out[j], acc[k][j]);
+  }
+}
+
+template <int RB>
+static cudaError_t h3_m2l_rot_launch(const qbxfmm_geometry& g, int pf, int nrhs, const double2* mp,
+                                     double2* lo, const double* Dtab, const double2* Ctab,
+                                     const double* clsmap, int32_t* err, cudaStream_t st)
+{
+  size_t sh = 2 * (size_t)RB * ((pf + 1) * (pf + 1) + 1) * sizeof(double2);
+  cudaFuncSetAttribute(k_h3_m2l_rot<RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+  dim3 grid(g.nttp_boxes, (nrhs + RB - 1) / RB);
+  k_h3_m2l_rot<RB><<<grid, H3M2L_NT, sh, st>>>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err);
+  return cudaGetLastError();
+}
+
+cudaError_t h3_launch_m2l_rot(const qbxfmm_geometry& g, int pf, int nrhs, const double2* mp,
+                              double2* lo, const double* Dtab, const double2* Ctab,
+                              const double* clsmap, int32_t* err, cudaStream_t st)
+{
+  if (g.nttp_boxes == 0 || g.m2l_nclasses == 0) return cudaSuccess;
+  if (pf > H3_MAXP) return cudaErrorInvalidValue;
+  if (nrhs >= 8) return h3_m2l_rot_launch<8>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err, st);
+  if (nrhs >= 2) return h3_m2l_rot_launch<4>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err, st);
+  return h3_m2l_rot_launch<1>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err, st);
+}
+
+cudaError_t h3_launch_m2l_tables(int pf, int ndir, int ncoax, const double* dirs,
+                                 const double* coaxp, const double* start, const double* isq,
+                                 const double* rt, const double* gaunt, double* Dtab,
+                                 double2* Ctab, cudaStream_t st)
+{
+  if (ndir + ncoax == 0) return cudaSuccess;
+  if (pf > H3_MAXP) return cudaErrorInvalidValue;
+  k_h3_m2l_tables<<<ndir + ncoax, NT, 0, st>>>(pf, ndir, ncoax, dirs, coaxp, start, isq, rt, gaunt,
+                                               Dtab, Ctab);
+  return cudaGetLastError();
 }
 
 // }}}
@@ -1578,18 +1905,12 @@ cudaError_t h3_launch_trans_build(const qbxfmm_geometry& g, const TransCfg& tc, 
               2 * (size_t)(p + 1) * sizeof(double);
   cudaFuncSetAttribute(k_h3_trans_build, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
   size_t stride = (size_t)tc.rp * tc.kp;
-  if (g.m2l_nclasses > 0)
-    k_h3_trans_build<<<g.m2l_nclasses, NT, sh, st>>>(0, p, tc.rp, tc.kp, k, g.root_extent,
-                                                      g.m2l_nclasses, g.m2l_class_offsets,
-                                                      g.m2l_class_levels, 0, gaunt, T);
   // M2M: parent levels 0 .. nlevels-2; L2L: child levels 1 .. nlevels-1 (8 per level)
   if (g.nlevels > 1) {
-    k_h3_trans_build<<<8 * (g.nlevels - 1), NT, sh, st>>>(
-        1, p, tc.rp, tc.kp, k, g.root_extent, 0, nullptr, nullptr, 0, gaunt,
-        T + tc.m2m_base * stride);
-    k_h3_trans_build<<<8 * (g.nlevels - 1), NT, sh, st>>>(
-        2, p, tc.rp, tc.kp, k, g.root_extent, 0, nullptr, nullptr, 1, gaunt,
-        T + (tc.l2l_base + 8) * stride);
+    k_h3_trans_build<<<8 * (g.nlevels - 1), NT, sh, st>>>(1, p, tc.rp, tc.kp, k, g.root_extent, 0,
+                                                          gaunt, T + tc.m2m_base * stride);
+    k_h3_trans_build<<<8 * (g.nlevels - 1), NT, sh, st>>>(2, p, tc.rp, tc.kp, k, g.root_extent, 1,
+                                                          gaunt, T + (tc.l2l_base + 8) * stride);
   }
   return cudaGetLastError();
 }

@@ -671,21 +671,6 @@ static cudaError_t gemm_tiled_launch(const qbxfmm_geometry& g, const TransCfg& c
   return cudaGetLastError();
 }
 
-// M2L without pair scratch: one launch per run of consecutive classes whose targets
-// are distinct (waves[w] .. waves[w+1]), adding into the targets' locals directly.
-cudaError_t launch_m2l_direct(const qbxfmm_geometry& g, const TransHost& th, const TransCfg& c,
-                              const int32_t* waves, int nwaves, int nrhs, const double* T,
-                              const double2* mp, double2* lo, int32_t* err, cudaStream_t st)
-{
-  for (int w = 0; w < nwaves; ++w) {
-    cudaError_t e = gemm_tiled_launch(g, c, nrhs, T, 0, 0, g.m2l_class_starts, waves[w],
-                                      waves[w + 1] - waves[w], th.m2l_max_pairs * nrhs,
-                                      g.m2l_pair_src, g.m2l_pair_dst, mp, lo, 1.0, nullptr, err, st);
-    if (e != cudaSuccess) return e;
-  }
-  return cudaSuccess;
-}
-
 // M2M without pair scratch: one launch per (parent level, child position) group,
 // whose parents are distinct.
 cudaError_t launch_m2m_direct(const qbxfmm_geometry& g, const TransHost& th, const TransCfg& c,
