@@ -261,15 +261,17 @@ QBX_D int h3_stream_source(int v, int nb, const int* s_pref, const int* s_start)
 // {{{ P2M / P2L
 
 // One CTA per box (P2M: source boxes, own sources; P2L: target-or-parent boxes, list-4
-// sources).  Sources in sub-tiles of SUB: one thread per source computes the radial
-// values (j_n for P2M, h_n for P2L, n <= p + 1), one thread per (column, source)
-// fills the wave table (entry-major, padded stride), then one thread per coefficient
-// accumulates q F_n^-m + sigma nu . grad F_n^-m with precomputed ladder offsets.
+// sources) and group of RB densities.  Sources in sub-tiles of SUB: one thread per
+// source computes the radial values (j_n for P2M, h_n for P2L, n <= p + 1), one thread
+// per (column, source) fills the wave table (entry-major, padded stride), then one
+// thread per coefficient forms the source's kernel row cq F_n^-m + cd nu . grad F_n^-m
+// (precomputed ladder offsets) once and adds density x row for each of the RB
+// densities, so the table and the row serve all densities of the group.
 constexpr int H3_SUB = 16;
 constexpr int H3_TS = H3_SUB + 1;
 constexpr int H3_NH = 3;          // coefficients per thread: (p+1)^2 <= 3 * 128
 
-template <bool LOCAL>
+template <bool LOCAL, int RB>
 __global__ void __launch_bounds__(NT)
 k_h3_p2e(qbxfmm_geometry g, HelmCoeffs hc, int p, int nrhs, const double2* __restrict__ strengths,
          double2* __restrict__ exps, int32_t* err)
@@ -282,7 +284,7 @@ k_h3_p2e(qbxfmm_geometry g, HelmCoeffs hc, int p, int nrhs, const double2* __res
   double2* rec = smem2 + (size_t)(N + 1) * (N + 1) * TS;   // [(N+1)(N+2)/2]
   __shared__ double2 s_rad[SUB][H3_LMAX + 2];
   __shared__ double s_t[SUB];
-  __shared__ double2 s_w[SUB], s_q[SUB], s_d[SUB], s_np[SUB], s_nm[SUB];
+  __shared__ double2 s_w[SUB], s_sig[SUB][RB], s_np[SUB], s_nm[SUB];
   __shared__ double s_nz[SUB];
   __shared__ int s_pref[MAXB + 1], s_start[MAXB];
 
@@ -296,12 +298,11 @@ k_h3_p2e(qbxfmm_geometry g, HelmCoeffs hc, int p, int nrhs, const double2* __res
   } else {
     b = g.source_boxes[blockIdx.x];
   }
-  int r = blockIdx.y;
+  int r0 = blockIdx.y * RB;
   double rho = level_width(g, g.box_levels[b]);
   double sc = h3_scale(hc.k, rho);
   double c[3];
   load_point<3>(g.box_centers, g.nboxes, b, c);
-  const double2* st = strengths + (size_t)r * g.nsources;
   const bool dip = hc.cd.x != 0.0 || hc.cd.y != 0.0;
   h3_rec_table(N, rec, threadIdx.x, NT);
 
@@ -319,9 +320,11 @@ k_h3_p2e(qbxfmm_geometry g, HelmCoeffs hc, int p, int nrhs, const double2* __res
 #pragma unroll
     for (int u = 0; u < 6; ++u) lad[h].o[u] *= TS;
   }
-  double2 acc[H3_NH];
+  double2 acc[H3_NH][RB];
 #pragma unroll
-  for (int h = 0; h < H3_NH; ++h) acc[h] = c2(0.0);
+  for (int h = 0; h < H3_NH; ++h)
+#pragma unroll
+    for (int rr = 0; rr < RB; ++rr) acc[h][rr] = c2(0.0);
 
   // one stream over the box's own sources (P2M) or the list-4 boxes' sources (P2L)
   for (int gb = l0; gb < (LOCAL ? l1 : 1); gb += MAXB) {
@@ -357,9 +360,9 @@ k_h3_p2e(qbxfmm_geometry g, HelmCoeffs hc, int p, int nrhs, const double2* __res
           h3_sph_j(N, x, jv);
           for (int n = 0; n <= N; ++n) s_rad[j][n] = c2(jv[n]);
         }
-        double2 sv = st[s];
-        s_q[j] = cmul(hc.cq, sv);
-        s_d[j] = cmul(hc.cd, sv);
+#pragma unroll
+        for (int rr = 0; rr < RB; ++rr)
+          s_sig[j][rr] = r0 + rr < nrhs ? strengths[(size_t)(r0 + rr) * g.nsources + s] : c2(0.0);
         if (dip) {
           double nv[3];
           load_point<3>(g.source_normals, g.nsources, s, nv);
@@ -377,24 +380,23 @@ k_h3_p2e(qbxfmm_geometry g, HelmCoeffs hc, int p, int nrhs, const double2* __res
 #pragma unroll
       for (int h = 0; h < H3_NH; ++h) {
         if (!valid[h]) continue;
-        double2 a = acc[h];
         for (int j = 0; j < cnt; ++j) {
           const double2* T = tab + j;
-          a = cfma(s_q[j], T[o_c[h]], a);
+          double2 kr = cmul(hc.cq, T[o_c[h]]);
           if (dip) {
             const Ladder& L = lad[h];
             double2 vz = caxpy(L.w[0], T[L.o[0]], cscale(L.w[1], T[L.o[1]]));
             double2 vp = caxpy(L.w[2], T[L.o[2]], cscale(L.w[3], T[L.o[3]]));
             double2 vm = caxpy(L.w[4], T[L.o[4]], cscale(L.w[5], T[L.o[5]]));
             double2 v = cfma(s_np[j], vp, cfma(s_nm[j], vm, cscale(s_nz[j], vz)));
-            a = cfma(s_d[j], v, a);
+            kr = cfma(hc.cd, v, kr);
           }
+#pragma unroll
+          for (int rr = 0; rr < RB; ++rr) acc[h][rr] = cfma(s_sig[j][rr], kr, acc[h][rr]);
         }
-        acc[h] = a;
       }
     }
   }
-  double2* E = exps + ((size_t)b * nrhs + r) * ncf;
 #pragma unroll
   for (int h = 0; h < H3_NH; ++h) {
     if (!valid[h]) continue;
@@ -402,8 +404,13 @@ k_h3_p2e(qbxfmm_geometry g, HelmCoeffs hc, int p, int nrhs, const double2* __res
     int n, m;
     hq_decode(ci, n, m);
     double f = FOUR_PI * hc.k * (LOCAL ? pow(sc, (double)n) : pow(sc, -(double)n));
-    // 4 pi i k f acc
-    E[ci] = cadd(E[ci], c2(-f * acc[h].y, f * acc[h].x));
+#pragma unroll
+    for (int rr = 0; rr < RB; ++rr) {
+      if (r0 + rr >= nrhs) break;
+      // 4 pi i k f acc
+      double2* E = exps + ((size_t)b * nrhs + r0 + rr) * ncf + ci;
+      *E = cadd(*E, c2(-f * acc[h][rr].y, f * acc[h][rr].x));
+    }
   }
 }
 
@@ -1688,15 +1695,33 @@ cudaError_t h3_launch_m2l_tables(int pf, int ndir, int ncoax, const double* dirs
 
 static int gridy(int nrhs) { return nrhs; }
 
+// densities per CTA: 8, 4 or 1
+template <bool LOCAL>
+static cudaError_t h3_p2e_launch(int nbox, size_t sh, const qbxfmm_geometry& g, HelmCoeffs hc, int p,
+                                 int nrhs, const double2* s, double2* e, int32_t* err,
+                                 cudaStream_t st)
+{
+#define QBX_H3_P2E(RB)                                                                          \
+  {                                                                                             \
+    cudaFuncSetAttribute(k_h3_p2e<LOCAL, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize,      \
+                         (int)sh);                                                              \
+    k_h3_p2e<LOCAL, RB><<<dim3(nbox, (nrhs + RB - 1) / RB), NT, sh, st>>>(g, hc, p, nrhs, s, e, \
+                                                                          err);                 \
+    return cudaGetLastError();                                                                  \
+  }
+  if (nrhs >= 8) QBX_H3_P2E(8)
+  if (nrhs >= 3) QBX_H3_P2E(4)
+  QBX_H3_P2E(1)
+#undef QBX_H3_P2E
+}
+
 cudaError_t h3_launch_p2m(const qbxfmm_geometry& g, HelmCoeffs hc, int p, int nrhs,
                           const double2* s, double2* mp, cudaStream_t st)
 {
   if (g.nsource_boxes == 0) return cudaSuccess;
   int N = p + 1;
   size_t sh = ((size_t)(N + 1) * (N + 1) * H3_TS + (size_t)(N + 1) * (N + 2) / 2) * sizeof(double2);
-  cudaFuncSetAttribute(k_h3_p2e<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
-  k_h3_p2e<false><<<dim3(g.nsource_boxes, gridy(nrhs)), NT, sh, st>>>(g, hc, p, nrhs, s, mp, nullptr);
-  return cudaGetLastError();
+  return h3_p2e_launch<false>(g.nsource_boxes, sh, g, hc, p, nrhs, s, mp, nullptr, st);
 }
 
 cudaError_t h3_launch_p2l(const qbxfmm_geometry& g, HelmCoeffs hc, int p, int nrhs,
@@ -1705,9 +1730,7 @@ cudaError_t h3_launch_p2l(const qbxfmm_geometry& g, HelmCoeffs hc, int p, int nr
   if (g.nttp_boxes == 0) return cudaSuccess;
   int N = p + 1;
   size_t sh = ((size_t)(N + 1) * (N + 1) * H3_TS + (size_t)(N + 1) * (N + 2) / 2) * sizeof(double2);
-  cudaFuncSetAttribute(k_h3_p2e<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
-  k_h3_p2e<true><<<dim3(g.nttp_boxes, gridy(nrhs)), NT, sh, st>>>(g, hc, p, nrhs, s, lo, err);
-  return cudaGetLastError();
+  return h3_p2e_launch<true>(g.nttp_boxes, sh, g, hc, p, nrhs, s, lo, err, st);
 }
 
 cudaError_t h3_launch_eval_direct(const qbxfmm_geometry& g, HelmCoeffs hc, int nrhs,
