@@ -848,7 +848,10 @@ k_h3_e2qbxl_rot(qbxfmm_geometry g, HelmCoeffs hc, int pf, int nrhs,
   double* chp = Tb + (size_t)NMU * NCQ;                         // [nm] cos(beta/2)^k
   double* shp = chp + nm;                                       // [nm] sin(beta/2)^k
 
+  __shared__ unsigned char s_nof[(H3_MAXP + 1) * (H3_MAXP + 1)];   // order n of coefficient (n, m)
   for (int x = threadIdx.x; x < nisq + nrt; x += NT) s_isq[x] = __ldg(g_isq + x);
+  for (int n = 0; n <= pf; ++n)
+    for (int x = n * n + threadIdx.x; x < (n + 1) * (n + 1); x += NT) s_nof[x] = (unsigned char)n;
   __syncthreads();
   int chunk = blockIdx.x;
   int r0 = blockIdx.y * RB;
@@ -887,9 +890,7 @@ k_h3_e2qbxl_rot(qbxfmm_geometry g, HelmCoeffs hc, int pf, int nrhs,
     __syncthreads();
     for (int e = threadIdx.x; e < ncf * RB; e += NT) {
       int ei = e / RB, ri = e - ei * RB;
-      int n = (int)sqrt((double)ei);
-      while ((n + 1) * (n + 1) <= ei) ++n;
-      while (n * n > ei) --n;
+      int n = s_nof[ei];
       double2 v = c2(0.0);
       if (r0 + ri < nrhs) v = cscale(spow[n], exps[((size_t)sbx * nrhs + r0 + ri) * ncf + ei]);
       Es[e] = v;
@@ -976,9 +977,7 @@ k_h3_e2qbxl_rot(qbxfmm_geometry g, HelmCoeffs hc, int pf, int nrhs,
       }
       // (2) coaxial column n: coaxn[(nu,mu)] = i^{nu-n} sum_j G(nu,mu; j; n,mu) rad[|n-nu|+2j]
       for (int o = lane; o < NCQ; o += 32) {
-        int nu = (int)sqrt((double)o);
-        while ((nu + 1) * (nu + 1) <= o) ++nu;
-        while (nu * nu > o) --nu;
+        int nu = s_nof[o];
         int mu = o - nu * nu - nu;
         double2 tt = c2(0.0);
         if (n >= abs(mu)) {
@@ -1010,10 +1009,16 @@ k_h3_e2qbxl_rot(qbxfmm_geometry g, HelmCoeffs hc, int pf, int nrhs,
         int mu = task / RB - Q, r = task - (task / RB) * RB;
         int amu = abs(mu);
         if (amu > n) continue;
-        double2 mr = c2(0.0);
-        const double2* Dm = Dph + mu + Q;
-        for (int m = -n; m <= n; ++m)
-          mr = cfma(Dm[(m + pf) * NMU], Es[(base + m) * RB + r], mr);
+        // two partial sums, so that consecutive multiply-adds do not wait on each other
+        double2 mr = c2(0.0), mr1 = c2(0.0);
+        const double2* Dm = Dph + (pf - n) * NMU + mu + Q;
+        const double2* Em = Es + (base - n) * RB + r;
+        int m = 0;
+        for (; m + 1 < 2 * n + 1; m += 2) {
+          mr = cfma(Dm[m * NMU], Em[m * RB], mr);
+          mr1 = cfma(Dm[(m + 1) * NMU], Em[(m + 1) * RB], mr1);
+        }
+        mr = cfma(Dm[m * NMU], Em[m * RB], cadd(mr, mr1));
 #pragma unroll
         for (int nu = 0; nu <= Q; ++nu)
           if (nu >= amu) lacc[ts][nu] = cfma(coaxn[nu * nu + nu + mu], mr, lacc[ts][nu]);
@@ -1036,9 +1041,7 @@ k_h3_e2qbxl_rot(qbxfmm_geometry g, HelmCoeffs hc, int pf, int nrhs,
       int task = lane + 32 * i;
       if (task >= NCQ * RB) break;
       int o = task / RB, r = task - o * RB;
-      int nu = (int)sqrt((double)o);
-      while ((nu + 1) * (nu + 1) <= o) ++nu;
-      while (nu * nu > o) --nu;
+      int nu = s_nof[o];
       int mu2 = o - nu * nu - nu;
       double2 a = c2(0.0);
       for (int mu = -nu; mu <= nu; ++mu) a = caxpy(Tb[(mu + Q) * NCQ + o], Lp[(nu * nu + nu + mu) * RB + r], a);
@@ -1054,9 +1057,7 @@ k_h3_e2qbxl_rot(qbxfmm_geometry g, HelmCoeffs hc, int pf, int nrhs,
     if (task >= NCQ * RB) break;
     int o = task / RB, r = task - o * RB;
     if (r0 + r >= nrhs) continue;
-    int nu = (int)sqrt((double)o);
-    while ((nu + 1) * (nu + 1) <= o) ++nu;
-    while (nu * nu > o) --nu;
+    int nu = s_nof[o];
     double2* out = qbx_exps + ((size_t)ctr * nrhs + r0 + r) * NCQ + o;
     *out = caxpy(pow(st, (double)nu), acc[i], *out);
   }
