@@ -1493,7 +1493,10 @@ constexpr int H3M2L_NCG = 120;
 // B = coaxially translated (into X), then the back rotation adds into register
 // accumulators owned by fixed (order, 4 consecutive m, density) tasks; the sum is
 // added into the box's local once.  Each task keeps four outputs, so one shared
-// load of the input feeds eight FMAs.
+// load of the input feeds eight FMAs.  The pair's rotation table, then its coaxial
+// table, then the rotation table again are copied into one shared buffer by all
+// threads (16-byte loads, all in flight together) before the step that reads them,
+// so the inner loops read shared memory only.
 template <int RB>
 __global__ void __launch_bounds__(H3M2L_NT)
 k_h3_m2l_rot(qbxfmm_geometry g, int pf, int nrhs, const double2* __restrict__ mp,
@@ -1505,11 +1508,13 @@ k_h3_m2l_rot(qbxfmm_geometry g, int pf, int nrhs, const double2* __restrict__ mp
   __shared__ int s_gn[H3M2L_NG], s_gm0[H3M2L_NG];        // rotation task groups
   __shared__ int s_cmu[H3M2L_NCG], s_cnu0[H3M2L_NCG];    // coaxial task groups
   __shared__ int s_ng, s_ncg;
+  __shared__ unsigned char s_nof[(H3_MAXP + 1) * (H3_MAXP + 1)];   // order n of coefficient (n, m)
   constexpr int NTHR = H3M2L_NT;
   constexpr int KMAX = (H3M2L_NG * RB + NTHR - 1) / NTHR;
   const int ncf = (pf + 1) * (pf + 1), XS = ncf + 1, nm = 2 * pf + 1;
   double2* X = smem2;                       // [RB][ncf + 1]
   double2* A = smem2 + (size_t)RB * XS;     // [RB][ncf + 1]
+  double2* Tbuf = A + (size_t)RB * XS;      // rotation or coaxial table of the pair
   if (threadIdx.x == 0) {
     int ng = 0;
     for (int n = 0; n <= pf; ++n)
@@ -1528,6 +1533,8 @@ k_h3_m2l_rot(qbxfmm_geometry g, int pf, int nrhs, const double2* __restrict__ mp
       }
     s_ncg = ncg;
   }
+  for (int n = 0; n <= pf; ++n)
+    for (int x = n * n + threadIdx.x; x < (n + 1) * (n + 1); x += NTHR) s_nof[x] = (unsigned char)n;
   __syncthreads();
   const int i = blockIdx.x;
   const int r0 = blockIdx.y * RB;
@@ -1555,18 +1562,19 @@ k_h3_m2l_rot(qbxfmm_geometry g, int pf, int nrhs, const double2* __restrict__ mp
       if (threadIdx.x == 0) report(err, QBX_DEVERR_BAD_BOX);
       continue;   // uniform across the CTA
     }
-    const double* D = Dtab + (size_t)clsmap[2 * lo_c] * dsz;
-    const double2* ph = reinterpret_cast<const double2*>(D);
-    const double* blocks = D + 2 * nm;
-    const double2* C = Ctab + (size_t)clsmap[2 * lo_c + 1] * csz;
+    const double2* Dg = reinterpret_cast<const double2*>(Dtab + (size_t)clsmap[2 * lo_c] * dsz);
+    const double2* Cg = Ctab + (size_t)clsmap[2 * lo_c + 1] * csz;
+    // the rotation table into Tbuf (phases, then the d blocks)
+    for (int x = threadIdx.x; x < (int)(dsz / 2); x += NTHR) Tbuf[x] = __ldg(Dg + x);
+    const double2* ph = Tbuf;
+    const double* blocks = reinterpret_cast<const double*>(Tbuf) + 2 * nm;
+    const double2* C = Tbuf;
     // X = e^{i m alpha} M
     for (int e = threadIdx.x; e < RB * ncf; e += NTHR) {
       int r = e / ncf, ci = e - r * ncf;
-      int n = (int)sqrt((double)ci);
-      while ((n + 1) * (n + 1) <= ci) ++n;
-      while (n * n > ci) --n;
+      int n = s_nof[ci];
       double2 v = c2(0.0);
-      if (r0 + r < nrhs) v = cmul(__ldg(ph + ci - n * n - n + pf), mp[((size_t)src * nrhs + r0 + r) * ncf + ci]);
+      if (r0 + r < nrhs) v = cmul(__ldg(Dg + ci - n * n - n + pf), mp[((size_t)src * nrhs + r0 + r) * ncf + ci]);
       X[r * XS + ci] = v;
     }
     __syncthreads();
@@ -1583,12 +1591,14 @@ k_h3_m2l_rot(qbxfmm_geometry g, int pf, int nrhs, const double2* __restrict__ mp
         const double* row = Tn + m * w;
 #pragma unroll
         for (int j = 0; j < 4; ++j)
-          if (j < nv) o[j] = caxpy(__ldg(row + j), x, o[j]);
+          if (j < nv) o[j] = caxpy(row[j], x, o[j]);
       }
 #pragma unroll
       for (int j = 0; j < 4; ++j)
         if (j < nv) A[r * XS + n * n + n + mu0 + j] = o[j];
     }
+    __syncthreads();
+    for (int x = threadIdx.x; x < (int)csz; x += NTHR) Tbuf[x] = __ldg(Cg + x);
     __syncthreads();
     // B[(nu, mu)] = sum_{n >= |mu|} C^mu[n][nu] A[(n, mu)]   (into X)
     for (int t = threadIdx.x; t < ncg * RB; t += NTHR) {
@@ -1603,7 +1613,7 @@ k_h3_m2l_rot(qbxfmm_geometry g, int pf, int nrhs, const double2* __restrict__ mp
         const double2* row = Cb + (n - am) * w;
 #pragma unroll
         for (int j = 0; j < 4; ++j)
-          if (j < nv) o[j] = cfma(__ldg(row + j), a, o[j]);
+          if (j < nv) o[j] = cfma(row[j], a, o[j]);
       }
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
@@ -1611,6 +1621,8 @@ k_h3_m2l_rot(qbxfmm_geometry g, int pf, int nrhs, const double2* __restrict__ mp
         if (j < nv) X[r * XS + nu * nu + nu + mu] = o[j];
       }
     }
+    __syncthreads();
+    for (int x = threadIdx.x; x < (int)(dsz / 2); x += NTHR) Tbuf[x] = __ldg(Dg + x);
     __syncthreads();
     // L[(nu, m2)] += e^{-i m2 alpha} sum_mu T^nu[m2][mu] B[(nu, mu)]
 #pragma unroll
@@ -1627,11 +1639,11 @@ k_h3_m2l_rot(qbxfmm_geometry g, int pf, int nrhs, const double2* __restrict__ mp
         double2 b = Br[mu];
 #pragma unroll
         for (int j = 0; j < 4; ++j)
-          if (j < nv) o[j] = caxpy(__ldg(Tn + j * w + mu), b, o[j]);
+          if (j < nv) o[j] = caxpy(Tn[j * w + mu], b, o[j]);
       }
 #pragma unroll
       for (int j = 0; j < 4; ++j)
-        if (j < nv) acc[k][j] = cfma(cconj(__ldg(ph + m20 + j + pf)), o[j], acc[k][j]);
+        if (j < nv) acc[k][j] = cfma(cconj(ph[m20 + j + pf]), o[j], acc[k][j]);
     }
     __syncthreads();
   }
@@ -1660,7 +1672,8 @@ static cudaError_t h3_m2l_rot_launch(const qbxfmm_geometry& g, int pf, int nrhs,
                                      double2* lo, const double* Dtab, const double2* Ctab,
                                      const double* clsmap, int32_t* err, cudaStream_t st)
 {
-  size_t sh = 2 * (size_t)RB * ((pf + 1) * (pf + 1) + 1) * sizeof(double2);
+  size_t sh = 2 * (size_t)RB * ((pf + 1) * (pf + 1) + 1) * sizeof(double2) +
+              std::max(h3_m2l_dsize(pf) * sizeof(double), h3_m2l_csize(pf) * sizeof(double2));
   cudaFuncSetAttribute(k_h3_m2l_rot<RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
   dim3 grid(g.nttp_boxes, (nrhs + RB - 1) / RB);
   k_h3_m2l_rot<RB><<<grid, H3M2L_NT, sh, st>>>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err);
