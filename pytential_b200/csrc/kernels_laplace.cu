@@ -723,6 +723,123 @@ k_p2l(qbxfmm_geometry g, SourceCoeffs sc, int p, int ncf, int nrhs,
 
 // }}}
 
+// 3D P2L with every coefficient split over two threads: a block of
+// P2L3_SPLIT x ncf threads (rounded up to whole warps) takes, per 32-source tile, the
+// sources [0, 16) in the first half of the threads and [16, 32) in the second, so no
+// thread waits idle through the accumulation (with one thread per coefficient, 62 of
+// 128 threads had nothing to accumulate at p = 10).  All threads build the tile's
+// harmonic tables; the halves are added in shared memory at the end.
+constexpr int P2L3_SPLIT = 2;
+constexpr int P2L3_MAXT = 256;
+
+__global__ void __launch_bounds__(P2L3_MAXT)
+k_p2l3s(qbxfmm_geometry g, SourceCoeffs sc, int p, int ncf, int nrhs,
+        const double* __restrict__ strengths, double2* __restrict__ locals, int32_t* err)
+{
+  constexpr int SUB = P2L_SUB;
+  constexpr int TS = P2L_TS;
+  constexpr int HALF = SUB / P2L3_SPLIT;
+  extern __shared__ double2 smem2[];
+  double2* tab = smem2;   // [nct][TS]
+  __shared__ double s_u[SUB][3], s_n[SUB][3], s_q[SUB];
+  __shared__ int s_pref[MAXB + 1], s_start[MAXB];
+  const int nthr = blockDim.x;
+  int i = blockIdx.x;
+  int tb = g.target_or_target_parent_boxes[i];
+  int r = blockIdx.y;
+  double rho = level_width(g, g.box_levels[tb]);
+  double rinv = 1.0 / rho;
+  double c[3];
+  load_point<3>(g.box_centers, g.nboxes, tb, c);
+  const double* st = strengths + (size_t)r * g.nsources;
+  const bool dip = sc.cd != 0.0;
+
+  // this thread's coefficient (n, m) and source half; table offsets of S_n^m and of
+  // the dipole neighbours S_{n+1}^{m-1}, S_{n+1}^m, S_{n+1}^{m+1}
+  const bool active = (int)threadIdx.x < P2L3_SPLIT * ncf;
+  const int ci = active ? (int)threadIdx.x % ncf : 0;
+  const int half = active ? (int)threadIdx.x / ncf : 0;
+  int n, m;
+  decode3(ci, n, m);
+  const int o_nm = idx3(n, m) * TS;
+  const int o_a = idx3(n + 1, m) * TS;
+  const int o_b = idx3(n + 1, m > 0 ? m - 1 : 1) * TS;   // m = 0: S_{n+1}^{-1} = -conj(S_{n+1}^1)
+  const double sb_sign = m > 0 ? 1.0 : -1.0;
+  const int o_c = idx3(n + 1, m + 1) * TS;
+
+  double2 acc = c2(0.0);
+  int l0 = g.list4_starts[i], l1 = g.list4_starts[i + 1];
+  for (int gb = l0; gb < l1; gb += MAXB) {
+    int nb = min(MAXB, l1 - gb);
+    __syncthreads();
+    list_prefix(g, g.list4_lists, gb, nb, s_pref, s_start, err);
+    __syncthreads();
+    int total = s_pref[nb];
+    for (int base = 0; base < total; base += SUB) {
+      int cnt = min(SUB, total - base);
+      if ((int)threadIdx.x < cnt) {
+        int s = stream_source(base + threadIdx.x, nb, s_pref, s_start);
+        double y[3];
+        load_point<3>(g.sources, g.nsources, s, y);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) s_u[threadIdx.x][d] = (y[d] - c[d]) * rinv;
+        if (dip) {
+          double nv[3];
+          load_point<3>(g.source_normals, g.nsources, s, nv);
+#pragma unroll
+          for (int d = 0; d < 3; ++d) s_n[threadIdx.x][d] = nv[d];
+        }
+        s_q[threadIdx.x] = __ldg(st + s);
+      }
+      __syncthreads();
+      for (int w = threadIdx.x; w < cnt * (p + 2); w += nthr) {
+        int mm = w / cnt, j = w - mm * cnt;
+        double x = s_u[j][0], yy = s_u[j][1], z = s_u[j][2];
+        double rinv2 = 1.0 / (x * x + yy * yy + z * z);
+        double2 a = c2(sqrt(rinv2));
+        for (int k = 1; k <= mm; ++k) a = cscale((2.0 * k - 1) * rinv2, cmul(a, c2(x, yy)));
+        double2* T = tab + j;
+        T[idx3(mm, mm) * TS] = a;
+        double2 prev = c2(0.0);
+        for (int nn = mm + 1; nn <= p + 1; ++nn) {
+          double2 bb = cscale(rinv2, csub(cscale((2.0 * nn - 1) * z, a),
+                                          cscale((double)(nn + mm - 1) * (nn - mm - 1), prev)));
+          T[idx3(nn, mm) * TS] = bb;
+          prev = a;
+          a = bb;
+        }
+      }
+      __syncthreads();
+      if (active) {
+        int jend = min(cnt, (half + 1) * HALF);
+        for (int j = half * HALF; j < jend; ++j) {
+          const double2* T = tab + j;
+          double q = s_q[j];
+          acc = caxpy(sc.cq * q * rinv, T[o_nm], acc);
+          if (dip) {
+            double f = sc.cd * q * rinv * rinv;
+            double dx = s_n[j][0], dy = s_n[j][1], dz = s_n[j][2];
+            double2 tb_ = T[o_b];
+            if (sb_sign < 0) tb_ = c2(-tb_.x, tb_.y);
+            double2 v = cscale(-dz, T[o_a]);
+            v = cfma(c2(0.5 * dx, 0.5 * dy), tb_, v);
+            v = cfma(c2(-0.5 * dx, 0.5 * dy), T[o_c], v);
+            acc = caxpy(f, v, acc);
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  // the second half's sums through the (now free) table space
+  if (active && half == 1) tab[ci] = acc;
+  __syncthreads();
+  if (active && half == 0) {
+    double2* L = locals + ((size_t)tb * nrhs + r) * ncf;
+    L[ci] = cadd(L[ci], cadd(acc, tab[ci]));
+  }
+}
+
 // {{{ L2L (refine_locals, fmm.py:519-523), one launch per child level
 
 template <int DIM>
@@ -1719,6 +1836,12 @@ static cudaError_t p2l_(const qbxfmm_geometry& g, SourceCoeffs sc, int p, int nr
   int ncf = (int)ncoef_dim(DIM, p);
   int nct = DIM == 3 ? (p + 2) * (p + 3) / 2 : p + 3;
   size_t sh = (size_t)P2L_TS * nct * sizeof(double2);
+  int nthr = (P2L3_SPLIT * ncf + 31) / 32 * 32;
+  if (DIM == 3 && nthr <= P2L3_MAXT) {
+    cudaFuncSetAttribute(k_p2l3s, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+    k_p2l3s<<<dim3(g.nttp_boxes, grid_y(nrhs)), nthr, sh, st>>>(g, sc, p, ncf, nrhs, s, lo, err);
+    return cudaGetLastError();
+  }
   cudaFuncSetAttribute(k_p2l<DIM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
   k_p2l<DIM><<<dim3(g.nttp_boxes, grid_y(nrhs)), NT, sh, st>>>(g, sc, p, ncf, nrhs, s, lo, err);
   return cudaGetLastError();
