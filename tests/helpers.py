@@ -42,6 +42,11 @@ def workload(name: str):
     if name == "h3d-S-small":
         return helmholtz3d_ellipsoid(nrefine=1, k=2.0, nrhs=1, op="S", qbx_order=4,
                                      fmm_order=12, nshell=100)
+    if name == "h3d-CF-p15":
+        # the orders, wave number and density count of the 3D Helmholtz benchmark
+        # (q = 5, p = 15, k = 10, 16 densities) on a small surface
+        return helmholtz3d_ellipsoid(nrefine=1, k=10.0, nrhs=16, op="CF", qbx_order=5,
+                                     fmm_order=15, nshell=100)
     if name == "h3d-D-small":
         return helmholtz3d_ellipsoid(nrefine=1, k=4.0, nrhs=3, op="D", qbx_order=2,
                                      fmm_order=8, nshell=100)
