@@ -912,8 +912,6 @@ k_h3_e2qbxl_rot(qbxfmm_geometry g, HelmCoeffs hc, int pf, int nrhs,
       } else {
         h3_sph_h(L, hc.k * bl, rad);
       }
-      // 4 pi Y_l^0(z) i^l f_l, Y_l^0(z) = sqrt((2l+1)/(4 pi))
-      for (int l = 0; l <= L; ++l) rad[l] = cmul(cscale(sqrt(FOUR_PI * (2.0 * l + 1.0)), ipow(l)), rad[l]);
     }
     for (int m = lane; m < nm; m += 32) {
       double sn, cs;
@@ -927,6 +925,9 @@ k_h3_e2qbxl_rot(qbxfmm_geometry g, HelmCoeffs hc, int pf, int nrhs,
       chp[m] = a;
       shp[m] = b;
     }
+    __syncwarp();
+    // 4 pi Y_l^0(z) i^l f_l, Y_l^0(z) = sqrt((2l+1)/(4 pi)), one lane per order
+    for (int l = lane; l <= L; l += 32) rad[l] = cmul(cscale(sqrt(FOUR_PI * (2.0 * l + 1.0)), ipow(l)), rad[l]);
     __syncwarp();
     // recurrence tasks t = (m + pf) (Q + 1) + mu, mu >= 0: start values
     double cur[RSL], prev[RSL], v0[RSL];
@@ -1000,28 +1001,37 @@ k_h3_e2qbxl_rot(qbxfmm_geometry g, HelmCoeffs hc, int pf, int nrhs,
         Dph[(mm + pf) * NMU + mu + Q] = cscale(val, ph[mm + pf]);
       }
       __syncwarp();
-      // (4) rotate and translate coaxially: lane task (mu, density)
+      // (4) rotate and translate coaxially: lane tasks (mu, density), all of a lane's
+      // tasks in one pass over m so that their multiply-adds interleave
       const int base = n * n + n;
+      {
+        double2 mr[TPL];
+        int toff[TPL], eoff[TPL];
+        bool act[TPL];
 #pragma unroll
-      for (int ts = 0; ts < TPL; ++ts) {
-        int task = lane + 32 * ts;
-        if (task >= NMU * RB) continue;
-        int mu = task / RB - Q, r = task - (task / RB) * RB;
-        int amu = abs(mu);
-        if (amu > n) continue;
-        // two partial sums, so that consecutive multiply-adds do not wait on each other
-        double2 mr = c2(0.0), mr1 = c2(0.0);
-        const double2* Dm = Dph + (pf - n) * NMU + mu + Q;
-        const double2* Em = Es + (base - n) * RB + r;
-        int m = 0;
-        for (; m + 1 < 2 * n + 1; m += 2) {
-          mr = cfma(Dm[m * NMU], Em[m * RB], mr);
-          mr1 = cfma(Dm[(m + 1) * NMU], Em[(m + 1) * RB], mr1);
+        for (int ts = 0; ts < TPL; ++ts) {
+          int task = lane + 32 * ts;
+          int mu = task / RB - Q, r = task - (task / RB) * RB;
+          act[ts] = task < NMU * RB && abs(mu) <= n;
+          toff[ts] = act[ts] ? (pf - n) * NMU + mu + Q : 0;
+          eoff[ts] = act[ts] ? (base - n) * RB + r : 0;
+          mr[ts] = c2(0.0);
         }
-        mr = cfma(Dm[m * NMU], Em[m * RB], cadd(mr, mr1));
+        for (int m = 0; m < 2 * n + 1; ++m) {
 #pragma unroll
-        for (int nu = 0; nu <= Q; ++nu)
-          if (nu >= amu) lacc[ts][nu] = cfma(coaxn[nu * nu + nu + mu], mr, lacc[ts][nu]);
+          for (int ts = 0; ts < TPL; ++ts)
+            if (act[ts]) mr[ts] = cfma(Dph[toff[ts] + m * NMU], Es[eoff[ts] + m * RB], mr[ts]);
+        }
+#pragma unroll
+        for (int ts = 0; ts < TPL; ++ts) {
+          if (!act[ts]) continue;
+          int task = lane + 32 * ts;
+          int mu = task / RB - Q;
+          int amu = abs(mu);
+#pragma unroll
+          for (int nu = 0; nu <= Q; ++nu)
+            if (nu >= amu) lacc[ts][nu] = cfma(coaxn[nu * nu + nu + mu], mr[ts], lacc[ts][nu]);
+        }
       }
       __syncwarp();
     }
