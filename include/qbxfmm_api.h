@@ -141,6 +141,19 @@ int qbxfmm_apply_noalloc(const qbxfmm_plan* plan, const qbxfmm_upsample* up,
 int qbxfmm_laplace3d_grad_direct(int nsources, const double* sources, const double* charges,
                                  int ntargets, const double* targets, double* grad, void* stream);
 
+/* Dense QBX matrix of the 3D Laplace layer potential with charge / dipole weights
+ * (replaces the reference's direct QBX evaluation and matrix builder,
+ * pytential/qbx/__init__.py:797-1068 and pytential/symbolic/matrix.py:450-523):
+ * K[t][s] (row-major, ntargets x nsources, written) = potential at target t of a unit
+ * source s, scaled by 1/(4 pi); targets with target_center[t] >= 0 use the order
+ * qbx_order QBX expansion about that center, the others the kernel itself.  Sources,
+ * normals, targets and centers are structure-of-arrays [3][n] device pointers. */
+int qbxfmm_laplace3d_qbx_matrix(int nsources, const double* sources, const double* normals,
+                                double charge_coeff, double dipole_coeff, int ntargets,
+                                const double* targets, const int32_t* target_center,
+                                int ncenters, const double* centers, int qbx_order, double* K,
+                                void* stream);
+
 #ifdef __cplusplus
 }
 #endif

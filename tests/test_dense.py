@@ -1,0 +1,31 @@
+"""Dense QBX matrix of the 3D Laplace layer potential (the reference's direct QBX
+evaluation / matrix builder) on the GPU, against the QBX-FMM apply at a high FMM
+order, where the two differ only by the FMM's truncation."""
+
+import numpy as np
+import pytest
+import torch
+
+from pytential_b200.dense import laplace3d_qbx_matrix
+from pytential_b200.fmm import QBXApply
+from pytential_b200.workloads import laplace3d_ellipsoid
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("op", ["S", "D"])
+def test_dense_qbx_matrix_times_density_equals_apply(op):
+    wl = laplace3d_ellipsoid(nrefine=1, nshell=200, op=op, qbx_order=3, fmm_order=20)
+    geo = wl.geometry()
+    M = laplace3d_qbx_matrix(geo, wl.spec, wl.qbx_order)
+    assert M.shape == (wl.nuser_targets, wl.discr.ndofs)
+    dens = torch.from_numpy(wl.density).cuda()
+    direct = (dens @ M.T).cpu().numpy()
+    ap = QBXApply(geo, wl.spec, wl.qbx_order, wl.fmm_order)
+    fmm = ap(dens).cpu().numpy()
+    # on-surface targets (QBX) and shell targets (plain kernel) both agree to the FMM's
+    # truncation at order 20
+    assert np.abs(direct - fmm).max() / np.abs(direct).max() < 1e-9
+    # linearity of the rows: M applied to a second density
+    d2 = torch.randn_like(dens)
+    assert np.abs((d2 @ M.T).cpu().numpy() - ap(d2).cpu().numpy()).max() / \
+        np.abs((d2 @ M.T).cpu().numpy()).max() < 1e-9
