@@ -175,3 +175,38 @@ def laplace3d_adjoint(nrefine: int = 4, ntargets: int = 5000, ncharges: int = 8,
     c = rng.normal(size=(3, ncharges))
     c *= 0.5 * rng.uniform(size=ncharges) ** (1 / 3) / np.linalg.norm(c, axis=0)
     return AdjointWorkload(d, 3.0 * v, sigma, c, qbx_order, fmm_order, seed)
+
+
+def _main(argv=None):
+    """``python -m pytential_b200.workloads NAME NREFINE [APPLIES]``: build one of the
+    3D workloads (``laplace3d`` double layer, or ``helmholtz3d`` combined field with
+    16 densities) and run ``APPLIES`` whole applies (target-specific near field) on
+    the current GPU, printing the time of the last; a driver for profilers."""
+    import argparse
+    import time
+
+    import torch
+
+    from .fmm import QBXApply
+    ap = argparse.ArgumentParser(prog="python -m pytential_b200.workloads")
+    ap.add_argument("name", choices=["laplace3d", "helmholtz3d"])
+    ap.add_argument("nrefine", type=int)
+    ap.add_argument("applies", type=int, nargs="?", default=1)
+    a = ap.parse_args(argv)
+    wl = (laplace3d_ellipsoid(nrefine=a.nrefine) if a.name == "laplace3d"
+          else helmholtz3d_ellipsoid(nrefine=a.nrefine))
+    qa = QBXApply(wl.geometry(), wl.spec, wl.qbx_order, wl.fmm_order, nrhs=wl.nrhs,
+                  target_specific_qbx=True)
+    dens = torch.from_numpy(wl.density).cuda()
+    out = qa.new_output()
+    for _ in range(a.applies):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        qa.apply_into(dens, out)
+        torch.cuda.synchronize()
+    qa.check_error_word()
+    print(f"{wl.name}: {1e3 * (time.perf_counter() - t0):.2f} ms per apply")
+
+
+if __name__ == "__main__":
+    _main()
