@@ -481,12 +481,17 @@ def drive_fmm(actx, expansion_wrangler: B200QBXExpansionWrangler, src_weight_vec
 class QBXApply:
     """The whole apply (upsample, weight, reorder, all FMM stages, assembly) as one
     C-ABI call, from a stage-1 density ``(nrhs, ndofs)`` to user-order potentials
-    ``(nrhs, nuser_targets)``; float64 throughout."""
+    ``(nrhs, nuser_targets)``; float64 throughout.
+
+    ``target_specific_qbx`` (default on) evaluates the list-1 near field of each QBX
+    target directly (the truncation of P2QBXL followed by QBXL2P, which the tests
+    check to 1e-12); off, the apply forms the QBX expansions from the list-1 sources
+    as the reference's wrangler does by default."""
 
     def __init__(self, geo: QBXFMMGeometryData, spec: SourceKernelSpec, qbx_order: int,
                  fmm_order: int, nrhs: int = 1, device="cuda",
                  device_geometry: DeviceGeometry | None = None,
-                 target_specific_qbx: bool = False, translation_matrices: bool = True,
+                 target_specific_qbx: bool = True, translation_matrices: bool = True,
                  precision: int = PRECISION_FP64):
         self.geo = geo
         self.device = torch.device(device)
