@@ -413,7 +413,7 @@ def run_b200(args):
             "gpu_launches": launches_per_step * K,
             "clocks": clk.summary(),
             "mixed": {
-                "form": "FP32 P2M/P2L/M2QBXL, split-TF32 tensor-core M2M/M2L/L2L, FP64 "
+                "form": "FP32 P2M/P2L/M2QBXL, split-TF32 tensor-core M2L, FP64 M2M/L2L, "
                         "target-specific near field and point evaluations",
                 "value": world * node_applies * K / tm, "unit": UNIT,
                 "ms_per_step": 1e3 * tm / K, "speedup_vs_fp64": t_max / tm,

@@ -906,15 +906,18 @@ int qbxfmm_apply(const qbxfmm_plan* p, const qbxfmm_upsample* up, const qbxfmm_w
                             ? reinterpret_cast<const uint32_t*>((const double*)ws->translations +
                                                                 trans_matrix_bytes(p->tc) / sizeof(double))
                             : nullptr;
+  // M2M / L2L: the FP64 matrix-vector kernels whenever the matrices are small (both
+  // precisions: they are latency-bound, a TF32 form would not be faster); M2L: split
+  // TF32 in the mixed form
   auto m2m = [&]() -> int {
-    if (T32)
-      QBX_TRY(launch_m2m_gemm_mixed(p->geo, p->th, p->tc, p->kern.nrhs, T32, (double2*)ws->mpoles,
-                                    (double*)ws->pair_scratch, ws->error_word, st),
-              "coarsen_multipoles (split TF32)");
-    else if (gemm && trans_mv_supported(p->tc))
+    if (gemm && trans_mv_supported(p->tc))
       QBX_TRY(launch_m2m_mv(p->geo, p->th, p->tc, p->kern.nrhs, (const double*)ws->translations,
                             (double2*)ws->mpoles, ws->error_word, st),
               "coarsen_multipoles (matrix form)");
+    else if (T32)
+      QBX_TRY(launch_m2m_gemm_mixed(p->geo, p->th, p->tc, p->kern.nrhs, T32, (double2*)ws->mpoles,
+                                    (double*)ws->pair_scratch, ws->error_word, st),
+              "coarsen_multipoles (split TF32)");
     else if (gemm)
       QBX_TRY(launch_m2m_gemm(p->geo, p->th, p->tc, p->kern.nrhs, (const double*)ws->translations,
                               (double2*)ws->mpoles, (double*)ws->pair_scratch, ws->error_word, st),
@@ -939,14 +942,14 @@ int qbxfmm_apply(const qbxfmm_plan* p, const qbxfmm_upsample* up, const qbxfmm_w
     return QBXFMM_OK;
   };
   auto l2l = [&]() -> int {
-    if (T32)
-      QBX_TRY(launch_l2l_gemm_mixed(p->geo, p->th, p->tc, p->kern.nrhs, T32, (double2*)ws->locals,
-                                    ws->error_word, st),
-              "refine_locals (split TF32)");
-    else if (gemm && trans_mv_supported(p->tc))
+    if (gemm && trans_mv_supported(p->tc))
       QBX_TRY(launch_l2l_mv(p->geo, p->th, p->tc, p->kern.nrhs, (const double*)ws->translations,
                             (double2*)ws->locals, ws->error_word, st),
               "refine_locals (matrix form)");
+    else if (T32)
+      QBX_TRY(launch_l2l_gemm_mixed(p->geo, p->th, p->tc, p->kern.nrhs, T32, (double2*)ws->locals,
+                                    ws->error_word, st),
+              "refine_locals (split TF32)");
     else if (gemm)
       QBX_TRY(launch_l2l_gemm(p->geo, p->th, p->tc, p->kern.nrhs, (const double*)ws->translations,
                               (double2*)ws->locals, ws->error_word, st),

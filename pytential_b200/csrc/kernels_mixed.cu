@@ -13,6 +13,9 @@
 #include "laplace.cuh"
 #include "kernels.h"
 
+#include <cooperative_groups.h>
+namespace cg = cooperative_groups;
+
 namespace qbx {
 
 namespace {
@@ -312,8 +315,12 @@ k_p2l3_f32(qbxfmm_geometry g, SourceCoeffs sc, int p, int ncf, int nrhs,
 
 // {{{ M2QBXL (FP32)
 
+// clusters of M2QBXL3_F32_Z CTAs per chunk split the list-3 boxes; partial sums meet
+// in CTA 0 of the cluster in a fixed order through distributed shared memory
+constexpr int M2QBXL3_F32_Z = 4;
+
 template <int Q>
-__global__ void __launch_bounds__(NT)
+__global__ void __cluster_dims__(M2QBXL3_F32_Z, 1, 1) __launch_bounds__(NT)
 k_m2qbxl3_f32(qbxfmm_geometry g, int pf, int ncf, int nrhs, const double2* __restrict__ mpoles,
               double2* __restrict__ qbx_exps, int32_t* err)
 {
@@ -324,9 +331,12 @@ k_m2qbxl3_f32(qbxfmm_geometry g, int pf, int ncf, int nrhs, const double2* __res
   const int MSZ = MR * MW;
   const int loff = pf + 2 * Q;
   int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int MZ = M2QBXL3_F32_Z;
   float2* Mw = smf + (size_t)warp * MSZ;
   float2* red = smf + (size_t)NW * MSZ;   // [NW-1][32][NC]
-  int chunk = blockIdx.x;
+  float2* cpart = red + (NW - 1) * 32 * NC;  // [32][NC]: this CTA's sum
+  int chunk = blockIdx.x / MZ;
+  int zpart = blockIdx.x - chunk * MZ;
   int r = blockIdx.y;
   int itb = g.qbx_chunk_target_box[chunk];
   bool has_center = lane < g.qbx_chunk_count[chunk];
@@ -344,7 +354,7 @@ k_m2qbxl3_f32(qbxfmm_geometry g, int pf, int ncf, int nrhs, const double2* __res
 #pragma unroll
   for (int i = 0; i < NC; ++i) acc[i] = f2(0.0f);
   int l0 = g.list3_starts[itb], l1 = g.list3_starts[itb + 1];
-  for (int li = l0 + warp; li < l1; li += NW) {
+  for (int li = l0 + zpart * NW + warp; li < l1; li += MZ * NW) {
     int sb = g.list3_lists[li];
     if ((unsigned)sb >= (unsigned)g.nboxes) {
       report(err, QBX_DEVERR_BAD_BOX);
@@ -417,14 +427,27 @@ k_m2qbxl3_f32(qbxfmm_geometry g, int pf, int ncf, int nrhs, const double2* __res
     for (int i = 0; i < NC; ++i) red[((warp - 1) * 32 + lane) * NC + i] = acc[i];
   }
   __syncthreads();
-  if (warp == 0 && has_center) {
-    double2* out = qbx_exps + ((size_t)ctr * nrhs + r) * NC;
+  if (warp == 0) {
 #pragma unroll
     for (int i = 0; i < NC; ++i) {
-      float2 a = acc[i];
-      for (int w = 1; w < NW; ++w) a = fadd(a, red[((w - 1) * 32 + lane) * NC + i]);
-      out[i] = cadd(out[i], tod(a));
+      for (int w = 1; w < NW; ++w) acc[i] = fadd(acc[i], red[((w - 1) * 32 + lane) * NC + i]);
+      cpart[lane * NC + i] = acc[i];
     }
+  }
+  cg::cluster_group cl = cg::this_cluster();
+  cl.sync();
+  if (zpart == 0 && warp == 0) {
+    for (unsigned q = 1; q < MZ; ++q) {
+      const float2* rp = cl.map_shared_rank(cpart, q) + lane * NC;
+#pragma unroll
+      for (int i = 0; i < NC; ++i) acc[i] = fadd(acc[i], rp[i]);
+    }
+  }
+  cl.sync();
+  if (zpart == 0 && warp == 0 && has_center) {
+    double2* out = qbx_exps + ((size_t)ctr * nrhs + r) * NC;
+#pragma unroll
+    for (int i = 0; i < NC; ++i) out[i] = cadd(out[i], tod(acc[i]));
   }
 }
 
@@ -629,9 +652,10 @@ static cudaError_t m2qbxl_mixed_q(const qbxfmm_geometry& g, int pf, int nrhs, co
   constexpr int NC = (Q + 1) * (Q + 2) / 2;
   int ncf = (pf + 1) * (pf + 2) / 2;
   size_t msz = (size_t)(pf + 2 * Q + 1) * (2 * pf + 3 * Q + 1);
-  size_t sh = (NW * msz + (size_t)(NW - 1) * 32 * NC) * sizeof(float2);
+  size_t sh = (NW * msz + (size_t)NW * 32 * NC) * sizeof(float2);
   cudaFuncSetAttribute(k_m2qbxl3_f32<Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
-  k_m2qbxl3_f32<Q><<<dim3(g.nqbx_chunks, nrhs), NT, sh, st>>>(g, pf, ncf, nrhs, mp, qe, err);
+  k_m2qbxl3_f32<Q><<<dim3(g.nqbx_chunks * M2QBXL3_F32_Z, nrhs), NT, sh, st>>>(g, pf, ncf, nrhs, mp,
+                                                                               qe, err);
   return cudaGetLastError();
 }
 
