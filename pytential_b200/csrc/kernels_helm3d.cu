@@ -802,6 +802,15 @@ k_h3_p2qbxl(qbxfmm_geometry g, HelmCoeffs hc, int nrhs, const double2* __restric
 // densities per CTA staged in shared memory per box; lane tasks are (m, mu)
 // recurrences, (mu, density) for the rotation + coaxial step and (output, density)
 // for the back rotation, whose results stay in registers across the boxes.
+// D (8x8, two per lane: row lane/4, columns 2 (lane%4) + {0,1}) += A (8x4, row major,
+// element (lane/4, lane%4)) B (4x8, column major, element (lane%4, lane/4)), FP64
+QBX_D void h3_dmma(double& d0, double& d1, double a, double b)
+{
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
 constexpr int H3_ROT_ZS = 8;
 constexpr int H3_ROT_SLOTS = 7;   // recurrence tasks per lane: (2 pf + 1)(Q + 1) <= 7 x 32
 
@@ -944,9 +953,13 @@ k_h3_e2qbxl_rot(qbxfmm_geometry g, HelmCoeffs hc, int pf, int nrhs,
                  shp[(int)__ldg(rstart + 4 * t + 2)];
       }
     }
-    double2 lacc[TPL][Q + 1];
+    // per-lane (mu, density) slots of the coaxially translated coefficients: the TPL
+    // lane tasks, or with 8 densities the 4 entries of the tensor-core output tiles
+    // this lane holds
+    constexpr int LSL = (RB == 8) ? 4 : TPL;
+    double2 lacc[LSL][Q + 1];
 #pragma unroll
-    for (int ts = 0; ts < TPL; ++ts)
+    for (int ts = 0; ts < LSL; ++ts)
 #pragma unroll
       for (int nu = 0; nu <= Q; ++nu) lacc[ts][nu] = c2(0.0);
 
@@ -1001,10 +1014,49 @@ k_h3_e2qbxl_rot(qbxfmm_geometry g, HelmCoeffs hc, int pf, int nrhs,
         Dph[(mm + pf) * NMU + mu + Q] = cscale(val, ph[mm + pf]);
       }
       __syncwarp();
-      // (4) rotate and translate coaxially: lane tasks (mu, density), all of a lane's
-      // tasks in one pass over m so that their multiply-adds interleave
+      // (4) rotate and translate coaxially
       const int base = n * n + n;
-      {
+      if constexpr (RB == 8) {
+        // the rotation of order n as a real product on the FP64 tensor cores:
+        // rows (mu, re / im) of the rotated coefficients, k = (m, re / im), columns the
+        // 8 densities; tiles 0/1 hold re/im of mu index 0..7, tiles 2/3 of 8..15,
+        // A[(mu, re)][(m, re)] = Re z, [(mu, re)][(m, im)] = -Im z, [(mu, im)][(m, re)] =
+        // Im z, [(mu, im)][(m, im)] = Re z with z = Dph[m][mu]; K = 2 (2n+1) padded to 4
+        constexpr int NTILE = (NMU > 8) ? 4 : 2;
+        const int rho = lane >> 2, kq = lane & 3;
+        double c[NTILE][2];
+#pragma unroll
+        for (int t = 0; t < NTILE; ++t) c[t][0] = c[t][1] = 0.0;
+        const double2* Eb = Es + (base - n) * RB + rho;
+        const double2* Db = Dph + (pf - n) * NMU;
+        for (int sk = 0; sk <= n; ++sk) {
+          const int kap = 4 * sk + kq, mi = kap >> 1, pin = kap & 1;
+          const bool vk = mi <= 2 * n;
+          double2 e = vk ? Eb[mi * RB] : c2(0.0);
+          double b = pin ? e.y : e.x;
+          double2 z0 = (vk && rho < NMU) ? Db[mi * NMU + rho] : c2(0.0);
+          h3_dmma(c[0][0], c[0][1], pin ? -z0.y : z0.x, b);
+          h3_dmma(c[1][0], c[1][1], pin ? z0.x : z0.y, b);
+          if (NTILE == 4) {
+            double2 z1 = (vk && 8 + rho < NMU) ? Db[mi * NMU + 8 + rho] : c2(0.0);
+            h3_dmma(c[NTILE - 2][0], c[NTILE - 2][1], pin ? -z1.y : z1.x, b);
+            h3_dmma(c[NTILE - 1][0], c[NTILE - 1][1], pin ? z1.x : z1.y, b);
+          }
+        }
+#pragma unroll
+        for (int sl = 0; sl < 4; ++sl) {
+          const int grp = sl >> 1, v = sl & 1;
+          const int mu = (grp ? 8 + rho : rho) - Q;
+          if (grp * 8 + rho >= NMU || abs(mu) > n || (grp && NTILE < 4)) continue;
+          double2 mr = c2(c[2 * grp][v], c[2 * grp + 1][v]);
+          const int amu = abs(mu);
+#pragma unroll
+          for (int nu = 0; nu <= Q; ++nu)
+            if (nu >= amu) lacc[sl][nu] = cfma(coaxn[nu * nu + nu + mu], mr, lacc[sl][nu]);
+        }
+      } else {
+        // lane tasks (mu, density), all of a lane's tasks in one pass over m so that
+        // their multiply-adds interleave
         double2 mr[TPL];
         int toff[TPL], eoff[TPL];
         bool act[TPL];
@@ -1035,14 +1087,27 @@ k_h3_e2qbxl_rot(qbxfmm_geometry g, HelmCoeffs hc, int pf, int nrhs,
       }
       __syncwarp();
     }
+    if constexpr (RB == 8) {
+      const int rho = lane >> 2;
 #pragma unroll
-    for (int ts = 0; ts < TPL; ++ts) {
-      int task = lane + 32 * ts;
-      if (task >= NMU * RB) continue;
-      int mu = task / RB - Q, r = task - (task / RB) * RB;
+      for (int sl = 0; sl < 4; ++sl) {
+        const int grp = sl >> 1, r = 2 * (lane & 3) + (sl & 1);
+        const int mu = (grp ? 8 + rho : rho) - Q;
+        if (grp * 8 + rho >= NMU) continue;
 #pragma unroll
-      for (int nu = 0; nu <= Q; ++nu)
-        if (nu >= abs(mu)) Lp[(nu * nu + nu + mu) * RB + r] = lacc[ts][nu];
+        for (int nu = 0; nu <= Q; ++nu)
+          if (nu >= abs(mu)) Lp[(nu * nu + nu + mu) * RB + r] = lacc[sl][nu];
+      }
+    } else {
+#pragma unroll
+      for (int ts = 0; ts < TPL; ++ts) {
+        int task = lane + 32 * ts;
+        if (task >= NMU * RB) continue;
+        int mu = task / RB - Q, r = task - (task / RB) * RB;
+#pragma unroll
+        for (int nu = 0; nu <= Q; ++nu)
+          if (nu >= abs(mu)) Lp[(nu * nu + nu + mu) * RB + r] = lacc[ts][nu];
+      }
     }
     __syncwarp();
     // rotate back into the register outputs: lane task (o = (nu, mu2), density)
