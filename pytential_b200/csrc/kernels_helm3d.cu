@@ -1432,38 +1432,34 @@ __global__ void k_h3_assemble_nonqbx(qbxfmm_geometry g, int nrhs,
 // above, with output order pf and all |mu| <= pf).  The rotation depends only on the
 // direction of the box offset and the coaxial part only on its length and the level,
 // so both are tabulated once per plan: per direction the phases e^{i m alpha} and the
-// blocks eps_m eps_mu d^n_{m mu}(beta), |m|, |mu| <= n <= pf (H3M2L_D doubles); per
-// (length, level) the coaxial blocks, one per mu, C^mu[n][nu] = s^nu s^n i^{nu-n}
-// sum_j G(n,mu; nu,mu; |n-nu|+2j) sqrt(4 pi (2l+1)) i^l h_l(k|b|) (l = |n-nu|+2j),
-// s = min(1, k width) (H3M2L_C complex entries).
+// blocks T^n[m][mu] = eps_m eps_mu d^n_{m mu}(beta), |mu| <= n <= pf, for m >= 0 only
+// (with these signs T^n[-m][-mu] = T^n[m][mu]); per (length, level) the coaxial
+// blocks for mu >= 0 (C^{-mu} = C^mu, the Gaunt coefficients of +-mu being equal),
+// C^mu[n][nu] = s^nu s^n i^{nu-n} sum_j G(n,mu; nu,mu; |n-nu|+2j) sqrt(4 pi (2l+1))
+// i^l h_l(k|b|) (l = |n-nu|+2j), s = min(1, k width).
 
-QBX_D int h3_dblock(int n) { return n * (4 * n * n - 1) / 3; }   // sum_{k<n} (2k+1)^2
+// start of order n's block: sum_{k<n} (k+1)(2k+1)
+QBX_D int h3_dblock(int n) { return n * (n - 1) * (2 * n - 1) / 3 + 3 * n * (n - 1) / 2 + n; }
 
-// start of mu's coaxial block, mu = -pf .. pf in that order
+// start of the coaxial block of |mu| = mu: sum_{u<mu} (pf+1-u)^2
 QBX_D int h3_cblock(int pf, int mu)
 {
   int o = 0;
-  for (int u = -pf; u < mu; ++u) {
-    int w = pf + 1 - abs(u);
-    o += w * w;
-  }
+  for (int u = 0; u < mu; ++u) o += (pf + 1 - u) * (pf + 1 - u);
   return o;
 }
 
 __host__ __device__ size_t h3_m2l_dsize(int pf)
 {
-  size_t nm = 2 * pf + 1;
-  size_t v = 2 * nm + (size_t)(pf + 1) * (4 * (pf + 1) * (pf + 1) - 1) / 3;
+  size_t nm = 2 * pf + 1, v = 2 * nm;
+  for (int n = 0; n <= pf; ++n) v += (size_t)(n + 1) * (2 * n + 1);
   return (v + 1) & ~(size_t)1;
 }
 
 __host__ __device__ size_t h3_m2l_csize(int pf)
 {
   size_t s = 0;
-  for (int u = -pf; u <= pf; ++u) {
-    size_t w = pf + 1 - (u < 0 ? -u : u);
-    s += w * w;
-  }
+  for (int u = 0; u <= pf; ++u) s += (size_t)(pf + 1 - u) * (pf + 1 - u);
   return s;
 }
 
@@ -1495,18 +1491,19 @@ k_h3_m2l_tables(int pf, int ndir, int ncoax, const double* __restrict__ dirs,
       sincos((m - pf) * alpha, &sn, &cs);
       ph[m] = c2(cs, sn);
     }
-    for (int t = threadIdx.x; t < nm * nm; t += NT) {
-      int m = t / nm - pf, mu = t % nm - pf;
+    for (int t = threadIdx.x; t < (pf + 1) * nm; t += NT) {
+      int m = t / nm, mu = t % nm - pf;   // rows m >= 0 (T^n[-m][-mu] = T^n[m][mu])
       int am = abs(m), amu = abs(mu);
       int n0 = max(am, amu);
-      double v = start[4 * t];
-      int ec = (int)start[4 * t + 1], es = (int)start[4 * t + 2];
+      const int ts = (m + pf) * nm + (mu + pf);   // index of the start table
+      double v = start[4 * ts];
+      int ec = (int)start[4 * ts + 1], es = (int)start[4 * ts + 2];
       for (int k = 0; k < ec; ++k) v *= ch;
       for (int k = 0; k < es; ++k) v *= sh;
       double eps = ((m > 0 && (m & 1)) ? -1.0 : 1.0) * ((mu > 0 && (mu & 1)) ? -1.0 : 1.0);
       double prev = 0.0, cur = v;
       for (int n = n0; n <= pf; ++n) {
-        blocks[h3_dblock(n) + (m + n) * (2 * n + 1) + (mu + n)] = eps * cur;
+        blocks[h3_dblock(n) + m * (2 * n + 1) + (mu + n)] = eps * cur;
         if (n == pf) break;
         double nxt;
         if (n == 0) {
@@ -1537,15 +1534,15 @@ k_h3_m2l_tables(int pf, int ndir, int ncoax, const double* __restrict__ dirs,
   double2* C = Ctab + (size_t)c * h3_m2l_csize(pf);
   int total = (int)h3_m2l_csize(pf);
   for (int e = threadIdx.x; e < total; e += NT) {
-    // decode (mu, n, nu)
-    int mu = -pf, off = 0;
+    // decode (mu >= 0, n, nu)
+    int mu = 0, off = 0;
     for (;;) {
-      int w = pf + 1 - abs(mu);
+      int w = pf + 1 - mu;
       if (e < off + w * w) break;
       off += w * w;
       ++mu;
     }
-    int am = abs(mu), w = pf + 1 - am;
+    int am = mu, w = pf + 1 - am;
     int n = am + (e - off) / w, nu = am + (e - off) % w;
     int o = nu * nu + nu + mu;
     int lbase = abs(n - nu), jmax = min(n, nu);
@@ -1657,16 +1654,19 @@ k_h3_m2l_rot(qbxfmm_geometry g, int pf, int nrhs, const double2* __restrict__ mp
     for (int t = threadIdx.x; t < ng * RB; t += NTHR) {
       int grp = t / RB, r = t - grp * RB;
       int n = s_gn[grp], mu0 = s_gm0[grp];
-      const double* Tn = blocks + h3_dblock(n) + (mu0 + n);
+      const double* Tn = blocks + h3_dblock(n);
       const int w = 2 * n + 1, nv = min(4, n - mu0 + 1);
       double2 o[4] = {c2(0.0), c2(0.0), c2(0.0), c2(0.0)};
       const double2* Xr = X + r * XS + n * n;
       for (int m = 0; m < w; ++m) {
         double2 x = Xr[m];
-        const double* row = Tn + m * w;
+        // T^n[m - n][mu0 + j]: row m - n >= 0 directly, else row n - m at -mu (reversed)
+        const int ma = m - n;
+        const double* row = ma >= 0 ? Tn + ma * w + (mu0 + n) : Tn + (-ma) * w + (n - mu0);
+        const int step = ma >= 0 ? 1 : -1;
 #pragma unroll
         for (int j = 0; j < 4; ++j)
-          if (j < nv) o[j] = caxpy(row[j], x, o[j]);
+          if (j < nv) o[j] = caxpy(row[step * j], x, o[j]);
       }
 #pragma unroll
       for (int j = 0; j < 4; ++j)
@@ -1680,7 +1680,7 @@ k_h3_m2l_rot(qbxfmm_geometry g, int pf, int nrhs, const double2* __restrict__ mp
       int grp = t / RB, r = t - grp * RB;
       int mu = s_cmu[grp], nu0 = s_cnu0[grp];
       int am = abs(mu), w = pf + 1 - am, nv = min(4, pf - nu0 + 1);
-      const double2* Cb = C + h3_cblock(pf, mu) + (nu0 - am);
+      const double2* Cb = C + h3_cblock(pf, am) + (nu0 - am);
       double2 o[4] = {c2(0.0), c2(0.0), c2(0.0), c2(0.0)};
       const double2* Ar = A + r * XS;
       for (int n = am; n <= pf; ++n) {
@@ -1707,14 +1707,23 @@ k_h3_m2l_rot(qbxfmm_geometry g, int pf, int nrhs, const double2* __restrict__ mp
       int grp = t / RB, r = t - grp * RB;
       int nu = s_gn[grp], m20 = s_gm0[grp];
       const int w = 2 * nu + 1, nv = min(4, nu - m20 + 1);
-      const double* Tn = blocks + h3_dblock(nu) + (m20 + nu) * w;
+      const double* Tn = blocks + h3_dblock(nu);
+      // T^nu[m2][mu] for m2 = m20 + j: row m2 >= 0 directly, else row -m2 at -mu
+      const double* pj[4];
+      int sj[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        int m2 = m20 + j;
+        pj[j] = m2 >= 0 ? Tn + m2 * w : Tn + (-m2) * w + 2 * nu;
+        sj[j] = m2 >= 0 ? 1 : -1;
+      }
       double2 o[4] = {c2(0.0), c2(0.0), c2(0.0), c2(0.0)};
       const double2* Br = X + r * XS + nu * nu;
       for (int mu = 0; mu < w; ++mu) {
         double2 b = Br[mu];
 #pragma unroll
         for (int j = 0; j < 4; ++j)
-          if (j < nv) o[j] = caxpy(Tn[j * w + mu], b, o[j]);
+          if (j < nv) o[j] = caxpy(pj[j][sj[j] * mu], b, o[j]);
       }
 #pragma unroll
       for (int j = 0; j < 4; ++j)
