@@ -2,34 +2,45 @@
 // the target-position gradient of the adjoint (the forward apply's targets are far
 // from the surface there, so the sum needs no QBX):
 //   grad u(x_t) = -1/(4 pi) sum_y q_y (x_t - y) / |x_t - y|^3.
-// CTA of 128 targets (thread = target); the sources stream through shared memory in
-// tiles of 256.
+// A cluster of GSPLIT CTAs per 64 targets (thread = target): CTA y of the cluster takes
+// the y-th contiguous chunk of the sources, streamed through shared memory in tiles
+// of 256, and CTA 0 adds the GSPLIT partial sums in a fixed order through
+// distributed shared memory (deterministic; a few thousand targets still fill the
+// GPU).
 #include <string>
+
+#include <cooperative_groups.h>
 
 #include "../../include/qbxfmm_api.h"
 #include "kernels.h"
 
+namespace cg = cooperative_groups;
+
 namespace qbx {
 int set_last_error(int code, const std::string& msg);
 
-constexpr int GT = 128;
+constexpr int GT = 64;
 constexpr int GS = 256;
+constexpr int GSPLIT = 8;
 
 namespace {
 
-__global__ void __launch_bounds__(GT)
+__global__ void __cluster_dims__(1, GSPLIT, 1) __launch_bounds__(GT)
 k_lap3_grad_direct(int nsrc, const double* __restrict__ src, const double* __restrict__ q,
                    int ntgt, const double* __restrict__ tgt, double* __restrict__ grad)
 {
   __shared__ double s_y[3][GS], s_q[GS];
+  __shared__ double s_part[3][GT];
   int t = blockIdx.x * GT + threadIdx.x;
   bool active = t < ntgt;
   double x[3] = {0, 0, 0};
   if (active)
     for (int d = 0; d < 3; ++d) x[d] = tgt[(size_t)d * ntgt + t];
   double g0 = 0.0, g1 = 0.0, g2 = 0.0;
-  for (int base = 0; base < nsrc; base += GS) {
-    int cnt = min(GS, nsrc - base);
+  const int chunk = (nsrc + GSPLIT - 1) / GSPLIT;
+  const int s0 = blockIdx.y * chunk, s1 = min(nsrc, s0 + chunk);
+  for (int base = s0; base < s1; base += GS) {
+    int cnt = min(GS, s1 - base);
     __syncthreads();
     for (int j = threadIdx.x; j < cnt; j += GT) {
       for (int d = 0; d < 3; ++d) s_y[d][j] = src[(size_t)d * nsrc + base + j];
@@ -49,12 +60,24 @@ k_lap3_grad_direct(int nsrc, const double* __restrict__ src, const double* __res
       }
     }
   }
-  if (active) {
+  s_part[0][threadIdx.x] = g0;
+  s_part[1][threadIdx.x] = g1;
+  s_part[2][threadIdx.x] = g2;
+  cg::cluster_group cl = cg::this_cluster();
+  cl.sync();
+  if (blockIdx.y == 0 && active) {
+    for (unsigned r = 1; r < GSPLIT; ++r) {
+      const double* pr = cl.map_shared_rank(&s_part[0][0], r);
+      g0 += pr[threadIdx.x];
+      g1 += pr[GT + threadIdx.x];
+      g2 += pr[2 * GT + threadIdx.x];
+    }
     const double c = -0.079577471545947667884;   // -1 / (4 pi)
     grad[t] = c * g0;
     grad[(size_t)ntgt + t] = c * g1;
     grad[2 * (size_t)ntgt + t] = c * g2;
   }
+  cl.sync();
 }
 
 }  // namespace
@@ -70,7 +93,8 @@ extern "C" int qbxfmm_laplace3d_grad_direct(int nsources, const double* sources,
     return qbx::set_last_error(QBXFMM_ERR_ARG, "qbxfmm_laplace3d_grad_direct: bad arguments");
   if (ntargets == 0) return QBXFMM_OK;
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-  qbx::k_lap3_grad_direct<<<(ntargets + qbx::GT - 1) / qbx::GT, qbx::GT, 0, st>>>(
+  dim3 grid((ntargets + qbx::GT - 1) / qbx::GT, qbx::GSPLIT);
+  qbx::k_lap3_grad_direct<<<grid, qbx::GT, 0, st>>>(
       nsources, sources, charges, ntargets, targets, grad);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess)
