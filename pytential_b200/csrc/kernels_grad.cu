@@ -48,16 +48,37 @@ k_lap3_grad_direct(int nsrc, const double* __restrict__ src, const double* __res
     }
     __syncthreads();
     if (active) {
-      for (int j = 0; j < cnt; ++j) {
+      // two sources per step into two sets of sums (independent dependency chains)
+      double h0 = 0.0, h1 = 0.0, h2 = 0.0;
+      int j = 0;
+      for (; j + 1 < cnt; j += 2) {
+        double dx = x[0] - s_y[0][j], dy = x[1] - s_y[1][j], dz = x[2] - s_y[2][j];
+        double ex = x[0] - s_y[0][j + 1], ey = x[1] - s_y[1][j + 1], ez = x[2] - s_y[2][j + 1];
+        double r2 = dx * dx + dy * dy + dz * dz;
+        double e2 = ex * ex + ey * ey + ez * ez;
+        double ri = r2 > 0.0 ? rsqrt(r2) : 0.0;
+        double ei = e2 > 0.0 ? rsqrt(e2) : 0.0;
+        double f = s_q[j] * ri * ri * ri;
+        double fe = s_q[j + 1] * ei * ei * ei;
+        g0 = fma(f, dx, g0);
+        g1 = fma(f, dy, g1);
+        g2 = fma(f, dz, g2);
+        h0 = fma(fe, ex, h0);
+        h1 = fma(fe, ey, h1);
+        h2 = fma(fe, ez, h2);
+      }
+      if (j < cnt) {
         double dx = x[0] - s_y[0][j], dy = x[1] - s_y[1][j], dz = x[2] - s_y[2][j];
         double r2 = dx * dx + dy * dy + dz * dz;
-        if (r2 == 0.0) continue;
-        double ri = rsqrt(r2);
+        double ri = r2 > 0.0 ? rsqrt(r2) : 0.0;
         double f = s_q[j] * ri * ri * ri;
         g0 = fma(f, dx, g0);
         g1 = fma(f, dy, g1);
         g2 = fma(f, dz, g2);
       }
+      g0 += h0;
+      g1 += h1;
+      g2 += h2;
     }
   }
   s_part[0][threadIdx.x] = g0;
