@@ -207,24 +207,33 @@ k_h2_p2e(qbxfmm_geometry g, HelmCoeffs hc, int p, int nrhs, const double2* __res
 
 // {{{ translations: M2M, L2L (per level), M2L (list 2)
 
-// Eout_m += fout(m) sum_n Ein_n fin(n) Z_{n-m}(d) with Z = J (M2M, L2L) or H (M2L).
-// One CTA per output box; thread m. Z tables (order 2p) for up to NT source boxes
-// are built one per thread into shared memory.
-template <int KIND>   // 0 = M2M, 1 = M2L, 2 = L2L
+// Eout_m[r] += fout(m) sum_n Z_{n-m}(d) fin(n) Ein_n[r] with Z = J (M2M, L2L) or H (M2L):
+// per source box a Toeplitz (2p+1) x (2p+1) matrix applied to a tile of right-hand
+// sides.  One CTA per (output box, tile of RW * TR right-hand sides); thread t takes
+// the right-hand sides rl + RW j (rl = t % RW, j < TR) and the coefficients
+// mg + G i (mg = t / RW, G = NT / RW, i < TM), all in registers.  The Z tables (order
+// 2p) of up to PB source boxes are built one per thread into shared memory, once for
+// the whole tile; each source box's coefficient block ([rhs][coef], contiguous in
+// global memory) is staged scaled by fin(n) into shared memory with coalesced loads.
+template <int KIND, int RW, int TR>   // KIND 0 = M2M, 1 = M2L, 2 = L2L
 __global__ void __launch_bounds__(NT)
 k_h2_translate(qbxfmm_geometry g, HelmCoeffs hc, int p, int nrhs, int i0,
                const double2* __restrict__ ein, double2* __restrict__ eout, int32_t* err)
 {
   constexpr int PB = 16;
+  constexpr int G = NT / RW;
+  constexpr int TM = (2 * 20 + 1 + G - 1) / G;
+  constexpr int RC = RW * TR;
   extern __shared__ double2 smem2[];
   const int NZ = 2 * p, ZW = 2 * NZ + 1, NC = 2 * p + 1;
   double2* Z = smem2;                       // [PB][ZW]
-  double2* E = Z + (size_t)PB * ZW;         // [PB][NC]
+  double2* E = Z + (size_t)PB * ZW;         // [RC][NC]
   __shared__ int s_src[PB];
-  __shared__ double s_rin[PB];
+  __shared__ double s_fin[PB][2 * 20 + 1];
   double Jb[ZMAX], Yb[ZMAX];
   int ib = i0 + blockIdx.x;
-  int r = blockIdx.y;
+  int r0 = blockIdx.y * RC;
+  int nr = min(RC, nrhs - r0);
   int tb;
   int l0, l1;
   if (KIND == 0) {
@@ -240,11 +249,14 @@ k_h2_translate(qbxfmm_geometry g, HelmCoeffs hc, int p, int nrhs, int i0,
     l0 = 0;
     l1 = 1;     // parent
   }
-  double rho_t = level_width(g, g.box_levels[tb]);
   double ct[2];
   load_point<2>(g.box_centers, g.nboxes, tb, ct);
-  int m = (int)threadIdx.x - p;
-  double2 acc = c2(0.0);
+  const int rl = threadIdx.x % RW, mg = threadIdx.x / RW;
+  double2 acc[TM][TR];
+#pragma unroll
+  for (int i = 0; i < TM; ++i)
+#pragma unroll
+    for (int j = 0; j < TR; ++j) acc[i][j] = c2(0.0);
   for (int lb = l0; lb < l1; lb += PB) {
     int nbat = min(PB, l1 - lb);
     __syncthreads();
@@ -263,43 +275,68 @@ k_h2_translate(qbxfmm_geometry g, HelmCoeffs hc, int p, int nrhs, int i0,
         sb = g.box_parent_ids[tb];
       }
       s_src[threadIdx.x] = sb;
-      double2* Zt = Z + (size_t)threadIdx.x * ZW;
       if (sb >= 0) {
         double cs[2];
         load_point<2>(g.box_centers, g.nboxes, sb, cs);
-        s_rin[threadIdx.x] = level_width(g, g.box_levels[sb]);
         // d = c_out - c_in
-        h2_zfun(NZ, hc.k, ct[0] - cs[0], ct[1] - cs[1], Jb, Yb, Zt, KIND == 1);
+        h2_zfun(NZ, hc.k, ct[0] - cs[0], ct[1] - cs[1], Jb, Yb, Z + (size_t)threadIdx.x * ZW,
+                KIND == 1);
       }
     }
     __syncthreads();
     for (int w = threadIdx.x; w < nbat * NC; w += NT) {
       int bb = w / NC, n = w - bb * NC - p;
       int sb = s_src[bb];
-      double2 v = c2(0.0);
       if (sb >= 0) {
+        double rin = level_width(g, g.box_levels[sb]);
         int an = n < 0 ? -n : n;
-        double f = (KIND == 2) ? pow(s_rin[bb], -(double)an) : pow(s_rin[bb], (double)an);
-        v = cscale(f, ein[((size_t)sb * nrhs + r) * NC + n + p]);
+        s_fin[bb][n + p] = (KIND == 2) ? pow(rin, -(double)an) : pow(rin, (double)an);
       }
-      E[(size_t)bb * NC + n + p] = v;
     }
-    __syncthreads();
-    if (m <= p) {
-      for (int bb = 0; bb < nbat; ++bb) {
-        if (s_src[bb] < 0) continue;
-        const double2* Zt = Z + (size_t)bb * ZW;
-        const double2* Eb = E + (size_t)bb * NC;
-        for (int n = -p; n <= p; ++n) acc = cfma(Eb[n + p], Zt[NZ + n - m], acc);
+    for (int bb = 0; bb < nbat; ++bb) {
+      int sb = s_src[bb];
+      if (sb < 0) continue;      // uniform over the CTA
+      __syncthreads();           // E free, s_fin written
+      const double2* src = ein + ((size_t)sb * nrhs + r0) * NC;
+      for (int w = threadIdx.x; w < nr * NC; w += NT) {
+        int n = w % NC;
+        E[w] = cscale(s_fin[bb][n], src[w]);
+      }
+      __syncthreads();
+      // Z_{n-m} for coefficient indices n, m in [0, 2p] at Zt[n - m]
+      const double2* Zt = Z + (size_t)bb * ZW + NZ;
+      for (int n = 0; n < NC; ++n) {
+        double2 e[TR];
+#pragma unroll
+        for (int j = 0; j < TR; ++j) e[j] = E[(rl + RW * j) * NC + n];
+#pragma unroll
+        for (int i = 0; i < TM; ++i) {
+          int m = min(mg + G * i, NC - 1);
+          double2 z = Zt[n - m];
+#pragma unroll
+          for (int j = 0; j < TR; ++j) acc[i][j] = cfma(z, e[j], acc[i][j]);
+        }
       }
     }
   }
-  if (m <= p) {
-    int am = m < 0 ? -m : m;
+  // the tile through shared memory, then one coalesced read-modify-write
+  double rho_t = level_width(g, g.box_levels[tb]);
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < TM; ++i) {
+    int m = mg + G * i;
+    if (m >= NC) continue;
+    int am = m - p < 0 ? p - m : m - p;
     double f = (KIND == 0) ? pow(rho_t, -(double)am) : pow(rho_t, (double)am);
-    double2* Eo = eout + ((size_t)tb * nrhs + r) * (2 * p + 1);
-    Eo[m + p] = caxpy(f, acc, Eo[m + p]);
+#pragma unroll
+    for (int j = 0; j < TR; ++j) {
+      int r = rl + RW * j;
+      if (r < nr) E[r * NC + m] = cscale(f, acc[i][j]);
+    }
   }
+  __syncthreads();
+  double2* dst = eout + ((size_t)tb * nrhs + r0) * NC;
+  for (int w = threadIdx.x; w < nr * NC; w += NT) dst[w] = cadd(dst[w], E[w]);
 }
 
 // }}}
@@ -890,18 +927,41 @@ cudaError_t h2_launch_p2l(const qbxfmm_geometry& g, HelmCoeffs hc, int p, int nr
   return cudaGetLastError();
 }
 
-static size_t trans_sh(int p) { return (16 * (size_t)(4 * p + 1) + 16 * (size_t)(2 * p + 1)) * sizeof(double2); }
+// right-hand-side tiling of the translation kernels: (lanes over rhs, rhs per lane)
+template <int KIND, int RW, int TR>
+static cudaError_t h2_translate_rt(const qbxfmm_geometry& g, HelmCoeffs hc, int p, int nrhs,
+                                   int i0, int nb, const double2* ein, double2* eout, int32_t* err,
+                                   cudaStream_t st)
+{
+  size_t sh = ((size_t)16 * (4 * p + 1) + (size_t)RW * TR * (2 * p + 1)) * sizeof(double2);
+  cudaError_t e = cudaFuncSetAttribute(k_h2_translate<KIND, RW, TR>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+  if (e != cudaSuccess) return e;
+  dim3 grid(nb, (nrhs + RW * TR - 1) / (RW * TR));
+  k_h2_translate<KIND, RW, TR><<<grid, NT, sh, st>>>(g, hc, p, nrhs, i0, ein, eout, err);
+  return cudaGetLastError();
+}
+
+template <int KIND>
+static cudaError_t h2_translate(const qbxfmm_geometry& g, HelmCoeffs hc, int p, int nrhs, int i0,
+                                int nb, const double2* ein, double2* eout, int32_t* err,
+                                cudaStream_t st)
+{
+  if (p > 20) return cudaErrorInvalidValue;
+  if (nrhs == 1) return h2_translate_rt<KIND, 1, 1>(g, hc, p, nrhs, i0, nb, ein, eout, err, st);
+  if (nrhs <= 4) return h2_translate_rt<KIND, 4, 1>(g, hc, p, nrhs, i0, nb, ein, eout, err, st);
+  if (nrhs <= 16) return h2_translate_rt<KIND, 16, 1>(g, hc, p, nrhs, i0, nb, ein, eout, err, st);
+  if (nrhs <= 32) return h2_translate_rt<KIND, 32, 1>(g, hc, p, nrhs, i0, nb, ein, eout, err, st);
+  return h2_translate_rt<KIND, 32, 2>(g, hc, p, nrhs, i0, nb, ein, eout, err, st);
+}
 
 cudaError_t h2_launch_m2m(const qbxfmm_geometry& g, const int32_t* lvl_host, HelmCoeffs hc, int p,
                           int nrhs, double2* mp, int32_t* err, cudaStream_t st)
 {
-  size_t sh = trans_sh(p);
-  cudaFuncSetAttribute(k_h2_translate<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
   for (int lev = g.nlevels - 2; lev >= 0; --lev) {
     int i0 = lvl_host[lev], i1 = lvl_host[lev + 1];
     if (i1 <= i0) continue;
-    k_h2_translate<0><<<dim3(i1 - i0, nrhs), NT, sh, st>>>(g, hc, p, nrhs, i0, mp, mp, err);
-    cudaError_t e = cudaGetLastError();
+    cudaError_t e = h2_translate<0>(g, hc, p, nrhs, i0, i1 - i0, mp, mp, err, st);
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
@@ -911,22 +971,16 @@ cudaError_t h2_launch_m2l(const qbxfmm_geometry& g, HelmCoeffs hc, int p, int nr
                           const double2* mp, double2* lo, int32_t* err, cudaStream_t st)
 {
   if (g.nttp_boxes == 0) return cudaSuccess;
-  size_t sh = trans_sh(p);
-  cudaFuncSetAttribute(k_h2_translate<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
-  k_h2_translate<1><<<dim3(g.nttp_boxes, nrhs), NT, sh, st>>>(g, hc, p, nrhs, 0, mp, lo, err);
-  return cudaGetLastError();
+  return h2_translate<1>(g, hc, p, nrhs, 0, g.nttp_boxes, mp, lo, err, st);
 }
 
 cudaError_t h2_launch_l2l(const qbxfmm_geometry& g, const int32_t* lvl_host, HelmCoeffs hc, int p,
                           int nrhs, double2* lo, int32_t* err, cudaStream_t st)
 {
-  size_t sh = trans_sh(p);
-  cudaFuncSetAttribute(k_h2_translate<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
   for (int lev = 1; lev < g.nlevels; ++lev) {
     int i0 = lvl_host[lev], i1 = lvl_host[lev + 1];
     if (i1 <= i0) continue;
-    k_h2_translate<2><<<dim3(i1 - i0, nrhs), NT, sh, st>>>(g, hc, p, nrhs, i0, lo, lo, err);
-    cudaError_t e = cudaGetLastError();
+    cudaError_t e = h2_translate<2>(g, hc, p, nrhs, i0, i1 - i0, lo, lo, err, st);
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;

@@ -36,6 +36,8 @@ def workload(name: str):
         return helmholtz2d_starfish(nelements=32, nrhs=1, nvolume=200, op="S", fmm_order=16)
     if name == "h2d-D-small":
         return helmholtz2d_starfish(nelements=32, nrhs=3, nvolume=200, op="D", qbx_order=4)
+    if name == "h2d-BW-nrhs40":
+        return helmholtz2d_starfish(nelements=32, nrhs=40, nvolume=100, op="BW", fmm_order=12)
     if name == "h3d-CF-small":
         return helmholtz3d_ellipsoid(nrefine=1, k=3.0, nrhs=2, op="CF", qbx_order=3,
                                      fmm_order=10, nshell=200)

@@ -54,8 +54,8 @@ def host(t):
 
 
 ALL = ["2d-S", "2d-D", "3d-D-small", "3d-S-small", "2d-D-nrhs3", "h2d-BW-small",
-       "h2d-S-small", "h2d-D-small", "h3d-CF-small", "h3d-S-small", "h3d-D-small",
-       "h3d-CF-p15"]
+       "h2d-S-small", "h2d-D-small", "h2d-BW-nrhs40", "h3d-CF-small", "h3d-S-small",
+       "h3d-D-small", "h3d-CF-p15"]
 
 
 @pytest.mark.parametrize("name", ALL)
@@ -144,7 +144,7 @@ def test_drive_fmm_and_apply_match_checker(name):
 
 @pytest.mark.parametrize("name", ["2d-S", "2d-D", "3d-D-small", "3d-S-small", "2d-D-nrhs3",
                                   "h2d-BW-small", "h2d-S-small", "h2d-D-small",
-                                  "h3d-CF-small", "h3d-S-small", "h3d-D-small", "h3d-CF-p15"])
+                                  "h2d-BW-nrhs40", "h3d-CF-small", "h3d-S-small", "h3d-D-small", "h3d-CF-p15"])
 def test_target_specific_mode_matches_checker(name):
     """With target-specific QBX the list-1 near field is evaluated per target; the
     truncation is the same, so the apply equals the checker's (expansion-based) one."""
