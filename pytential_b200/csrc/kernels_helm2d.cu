@@ -119,19 +119,33 @@ k_h2_form_strengths(int nsources, int ndofs, int npe, int nqpe, const double* __
 
 // {{{ P2M (source boxes) and P2L (list 4)
 
-template <bool LOCAL>
+// E_m[r] += f(m) sum_s W_s(m) str_s[r]: per source the weights
+//   P2M: W(m) = cq conj(Z_m) + kd (conj(nu) conj(Z_{m-1}) - nu conj(Z_{m+1})),  Z = J
+//   P2L: W(m) = cq Hb_m + kd (conj(nu) Hb_{m-1} - nu Hb_{m+1})
+// (kd = (k/2) cd) do not depend on the density, so a box is a (2p+1) x nsrc times
+// nsrc x rhs complex product.  One CTA per (box, tile of RW * TR right-hand sides),
+// thread layout as in k_h2_translate; SUB sources per stage: Bessel tables one per
+// thread, then W and the strengths tile in shared memory.
+template <bool LOCAL, int RW, int TR>
 __global__ void __launch_bounds__(NT)
 k_h2_p2e(qbxfmm_geometry g, HelmCoeffs hc, int p, int nrhs, const double2* __restrict__ strengths,
          double2* __restrict__ exps, int32_t* err)
 {
   constexpr int SUB = 32;
+  constexpr int G = NT / RW;
+  constexpr int TM = (2 * 20 + 1 + G - 1) / G;
+  constexpr int RC = RW * TR;
   extern __shared__ double2 smem2[];
-  const int N = p + 1, ZW = 2 * N + 1;
-  double2* Z = smem2;                                  // [SUB][ZW]
-  __shared__ double2 s_q[SUB], s_a[SUB], s_b[SUB];
+  const int N = p + 1, ZW = 2 * N + 1, NC = 2 * p + 1;
+  double2* Z = smem2;                        // [SUB][ZW]
+  double2* W = Z + (size_t)SUB * ZW;         // [SUB][NC]
+  double2* S = W + (size_t)SUB * NC;         // [SUB][RC + 1] (padded rows)
+  __shared__ double2 s_nu[SUB];
+  __shared__ int s_src[SUB];
   __shared__ int s_pref[MAXB + 1], s_start[MAXB];
   int i = blockIdx.x;
-  int r = blockIdx.y;
+  int r0 = blockIdx.y * RC;
+  int nr = min(RC, nrhs - r0);
   int b, l0, l1;
   const int32_t* lists;
   if (LOCAL) {
@@ -145,14 +159,17 @@ k_h2_p2e(qbxfmm_geometry g, HelmCoeffs hc, int p, int nrhs, const double2* __res
     l0 = i;
     l1 = i + 1;
   }
-  double rho = level_width(g, g.box_levels[b]);
   double c[2];
   load_point<2>(g.box_centers, g.nboxes, b, c);
-  const double2* st = strengths + (size_t)r * g.nsources;
   const bool dip = hc.cd.x != 0.0 || hc.cd.y != 0.0;
+  const double2 kd = cscale(0.5 * hc.k, hc.cd);
   double Jb[ZMAX], Yb[ZMAX];
-  int m = (int)threadIdx.x - p;
-  double2 acc = c2(0.0);
+  const int rl = threadIdx.x % RW, mg = threadIdx.x / RW;
+  double2 acc[TM][TR];
+#pragma unroll
+  for (int a = 0; a < TM; ++a)
+#pragma unroll
+    for (int j = 0; j < TR; ++j) acc[a][j] = c2(0.0);
   for (int gb = l0; gb < l1; gb += MAXB) {
     int nb = min(MAXB, l1 - gb);
     __syncthreads();
@@ -166,40 +183,63 @@ k_h2_p2e(qbxfmm_geometry g, HelmCoeffs hc, int p, int nrhs, const double2* __res
         double y[2], nv[2] = {0, 0};
         load_point<2>(g.sources, g.nsources, s, y);
         if (dip) load_point<2>(g.source_normals, g.nsources, s, nv);
-        double2 q, a, bb;
-        source_factors(hc, st[s], nv[0], nv[1], dip, q, a, bb);
-        s_q[threadIdx.x] = q;
-        s_a[threadIdx.x] = a;
-        s_b[threadIdx.x] = bb;
+        s_src[threadIdx.x] = s;
+        s_nu[threadIdx.x] = c2(nv[0], nv[1]);
         h2_zfun(N, hc.k, y[0] - c[0], y[1] - c[1], Jb, Yb, Z + (size_t)threadIdx.x * ZW, LOCAL);
       }
       __syncthreads();
-      if (m <= p) {
-        for (int j = 0; j < cnt; ++j) {
-          const double2* Zt = Z + (size_t)j * ZW;
-          if (!LOCAL) {
-            acc = cfmac(s_q[j], Zt[N + m], acc);
-            if (dip) {
-              acc = cfmac(s_a[j], Zt[N + m - 1], acc);
-              acc = cfmac(cneg(s_b[j]), Zt[N + m + 1], acc);
-            }
-          } else {
-            acc = cfma(s_q[j], hbar(Zt, N, m), acc);
-            if (dip) {
-              acc = cfma(s_a[j], hbar(Zt, N, m - 1), acc);
-              acc = cfma(cneg(s_b[j]), hbar(Zt, N, m + 1), acc);
-            }
+      for (int w = threadIdx.x; w < cnt * NC; w += NT) {
+        int j = w / NC, m = w - j * NC - p;
+        const double2* Zt = Z + (size_t)j * ZW;
+        double2 v;
+        if (!LOCAL) {
+          v = cmulc(hc.cq, Zt[N + m]);
+          if (dip) {
+            double2 nu = s_nu[j];
+            v = cfma(kd, csub(cmulc(cconj(nu), Zt[N + m - 1]), cmulc(nu, Zt[N + m + 1])), v);
           }
+        } else {
+          v = cmul(hc.cq, hbar(Zt, N, m));
+          if (dip) {
+            double2 nu = s_nu[j];
+            v = cfma(kd, csub(cmul(cconj(nu), hbar(Zt, N, m - 1)), cmul(nu, hbar(Zt, N, m + 1))), v);
+          }
+        }
+        W[w] = v;
+      }
+      for (int w = threadIdx.x; w < cnt * RC; w += NT) {
+        int r = w / cnt, j = w - r * cnt;
+        S[j * (RC + 1) + r] = r < nr ? strengths[(size_t)(r0 + r) * g.nsources + s_src[j]] : c2(0.0);
+      }
+      __syncthreads();
+      for (int j = 0; j < cnt; ++j) {
+        double2 e[TR];
+#pragma unroll
+        for (int jj = 0; jj < TR; ++jj) e[jj] = S[j * (RC + 1) + rl + RW * jj];
+#pragma unroll
+        for (int a = 0; a < TM; ++a) {
+          int m = min(mg + G * a, NC - 1);
+          double2 wv = W[j * NC + m];
+#pragma unroll
+          for (int jj = 0; jj < TR; ++jj) acc[a][jj] = cfma(wv, e[jj], acc[a][jj]);
         }
       }
       __syncthreads();
     }
   }
-  if (m <= p) {
-    int am = m < 0 ? -m : m;
+  double rho = level_width(g, g.box_levels[b]);
+  double2* E = exps + ((size_t)b * nrhs + r0) * NC;
+#pragma unroll
+  for (int a = 0; a < TM; ++a) {
+    int m = mg + G * a;
+    if (m >= NC) continue;
+    int am = m - p < 0 ? p - m : m - p;
     double sc = LOCAL ? pow(rho, (double)am) : pow(rho, -(double)am);
-    double2* E = exps + ((size_t)b * nrhs + r) * (2 * p + 1);
-    E[m + p] = caxpy(sc, acc, E[m + p]);
+#pragma unroll
+    for (int jj = 0; jj < TR; ++jj) {
+      int r = rl + RW * jj;
+      if (r < nr) E[(size_t)r * NC + m] = caxpy(sc, acc[a][jj], E[(size_t)r * NC + m]);
+    }
   }
 }
 
@@ -767,59 +807,114 @@ k_h2_tsqbx(qbxfmm_geometry g, HelmCoeffs hc, int nrhs, const double2* __restrict
   }
 }
 
-// M2QBXL (list 3) and L2QBXL (own target box): one thread per center.
-template <int Q, bool FROM_LOCAL>
-__global__ void __launch_bounds__(NT)
+// M2QBXL (list 3) and L2QBXL (own target box):
+//   Q_m[r] += rho_c^|m| sum_n Z_{n-m}(c - c_b) f(n) E_n[r],  f(n) = rho_b^{+-|n|},
+// Z = H (from multipoles) or J (from locals), m in [-Q, Q], n in [-pf, pf].  One CTA
+// per (CW centers of a QBX chunk, tile of RW * TR right-hand sides); all centers of a
+// chunk share a target box and so its list 3.  Thread t: rhs lane rl = t % RW (rhs
+// rl + RW j), center t / RW, all 2Q+1 coefficients in registers.  Per source box the
+// scaled coefficient block is staged once in shared memory and each center's Z table
+// (order pf + Q) is built once, by one thread.
+template <int Q, bool FROM_LOCAL, int RW, int TR, int CW>
+__global__ void __launch_bounds__(RW * CW)
 k_h2_e2qbxl(qbxfmm_geometry g, HelmCoeffs hc, int pf, int nrhs, const double2* __restrict__ exps,
             double2* __restrict__ qbx_exps, int32_t* err)
 {
-  constexpr int NC = 2 * Q + 1;
+  constexpr int NQ = 2 * Q + 1;
+  constexpr int NTH = RW * CW;
+  constexpr int RC = RW * TR;
+  constexpr int NSUB = 32 / CW;
+  extern __shared__ double2 smem2[];
+  const int NZ = pf + Q, ZW = 2 * NZ + 1, NC = 2 * pf + 1;
+  double2* Zc = smem2;                        // [CW][ZW]
+  double2* E = Zc + (size_t)CW * ZW;          // [RC][NC]
+  __shared__ double s_fn[2 * 20 + 1];
+  __shared__ int s_sb;
   double Jb[ZMAX], Yb[ZMAX];
-  double2 Z[2 * (20 + 8) + 1];
-  int ig = blockIdx.x * blockDim.x + threadIdx.x;
-  int r = blockIdx.y;
-  if (ig >= g.nglobal_qbx_centers) return;
-  int ctr = g.global_qbx_centers[ig];
-  int itb = g.qbx_center_to_target_box[ctr];
-  double cc[2];
-  load_point<2>(g.centers, g.ncenters, ctr, cc);
-  double rho_t = g.expansion_radii[ctr];
-  int NZ = pf + Q;
-  double2 acc[NC];
+  int chunk = blockIdx.x;
+  int sub = blockIdx.y % NSUB;
+  int r0 = (blockIdx.y / NSUB) * RC;
+  int nr = min(RC, nrhs - r0);
+  int ncen = g.qbx_chunk_count[chunk];
+  if (ncen > 32 && sub == 0 && threadIdx.x == 0) report(err, QBX_DEVERR_BAD_CENTER);
+  ncen -= sub * CW;
+  if (ncen <= 0) return;                       // uniform over the CTA
+  ncen = min(ncen, CW);
+  int itb = g.qbx_chunk_target_box[chunk];
+  const int rl = threadIdx.x % RW, cw = threadIdx.x / RW;
+  bool has_center = cw < ncen;
+  int ctr = has_center ? g.centers_by_target_box[g.qbx_chunk_start[chunk] + sub * CW + cw] : 0;
+  if ((unsigned)ctr >= (unsigned)g.ncenters) {
+    report(err, QBX_DEVERR_BAD_CENTER);
+    has_center = false;
+    ctr = 0;
+  }
+  double2 acc[NQ][TR];
 #pragma unroll
-  for (int i = 0; i < NC; ++i) acc[i] = c2(0.0);
+  for (int a = 0; a < NQ; ++a)
+#pragma unroll
+    for (int j = 0; j < TR; ++j) acc[a][j] = c2(0.0);
   int l0 = FROM_LOCAL ? 0 : g.list3_starts[itb];
   int l1 = FROM_LOCAL ? 1 : g.list3_starts[itb + 1];
   for (int li = l0; li < l1; ++li) {
-    int sb = FROM_LOCAL ? g.target_boxes[itb] : g.list3_lists[li];
-    if ((unsigned)sb >= (unsigned)g.nboxes) {
-      report(err, QBX_DEVERR_BAD_BOX);
-      continue;
+    __syncthreads();                           // E, Zc and s_fn free
+    if (threadIdx.x == 0) {
+      int sb = FROM_LOCAL ? g.target_boxes[itb] : g.list3_lists[li];
+      if ((unsigned)sb >= (unsigned)g.nboxes) {
+        report(err, QBX_DEVERR_BAD_BOX);
+        sb = -1;
+      }
+      s_sb = sb;
     }
+    __syncthreads();
+    int sb = s_sb;
+    if (sb < 0) continue;                      // uniform over the CTA
     double rho_s = level_width(g, g.box_levels[sb]);
     double cs[2];
     load_point<2>(g.box_centers, g.nboxes, sb, cs);
-    h2_zfun(NZ, hc.k, cc[0] - cs[0], cc[1] - cs[1], Jb, Yb, Z, !FROM_LOCAL);
-    const double2* E = exps + ((size_t)sb * nrhs + r) * (2 * pf + 1);
-    double fn = 1.0, rfac = FROM_LOCAL ? 1.0 / rho_s : rho_s;
-    for (int an = 0; an <= pf; ++an) {
-      double2 ep = cscale(fn, E[pf + an]);
-      double2 en = cscale(fn, E[pf - an]);
+    for (int w = threadIdx.x; w < NC; w += NTH) {
+      int an = w - pf < 0 ? pf - w : w - pf;
+      s_fn[w] = FROM_LOCAL ? pow(rho_s, -(double)an) : pow(rho_s, (double)an);
+    }
+    if (rl == 0 && has_center) {
+      double cc[2];
+      load_point<2>(g.centers, g.ncenters, ctr, cc);
+      h2_zfun(NZ, hc.k, cc[0] - cs[0], cc[1] - cs[1], Jb, Yb, Zc + (size_t)cw * ZW, !FROM_LOCAL);
+    }
+    __syncthreads();
+    const double2* src = exps + ((size_t)sb * nrhs + r0) * NC;
+    for (int w = threadIdx.x; w < nr * NC; w += NTH) E[w] = cscale(s_fn[w % NC], src[w]);
+    __syncthreads();
+    if (has_center) {
+      // Z_{n-m} for coefficient indices n in [0, 2pf], a = m + Q in [0, 2Q] at Zr[n - pf - a + Q]
+      const double2* Zr = Zc + (size_t)cw * ZW + NZ - pf + Q;
+      for (int n = 0; n < NC; ++n) {
+        double2 e[TR];
 #pragma unroll
-      for (int m = -Q; m <= Q; ++m) {
-        acc[m + Q] = cfma(ep, Z[NZ + an - m], acc[m + Q]);
-        if (an > 0) acc[m + Q] = cfma(en, Z[NZ - an - m], acc[m + Q]);
+        for (int j = 0; j < TR; ++j) e[j] = E[(rl + RW * j) * NC + n];
+#pragma unroll
+        for (int a = 0; a < NQ; ++a) {
+          double2 z = Zr[n - a];
+#pragma unroll
+          for (int j = 0; j < TR; ++j) acc[a][j] = cfma(z, e[j], acc[a][j]);
+        }
       }
-      fn *= rfac;
     }
   }
-  double2* out = qbx_exps + ((size_t)ctr * nrhs + r) * NC;
-  double f = 1.0;
+  if (!has_center) return;
+  double rho_t = g.expansion_radii[ctr];
 #pragma unroll
-  for (int am = 0; am <= Q; ++am) {
-    out[Q + am] = caxpy(f, acc[Q + am], out[Q + am]);
-    if (am > 0) out[Q - am] = caxpy(f, acc[Q - am], out[Q - am]);
-    f *= rho_t;
+  for (int j = 0; j < TR; ++j) {
+    int r = rl + RW * j;
+    if (r >= nr) continue;
+    double2* out = qbx_exps + ((size_t)ctr * nrhs + r0 + r) * NQ;
+    double f = 1.0;
+#pragma unroll
+    for (int am = 0; am <= Q; ++am) {
+      out[Q + am] = caxpy(f, acc[Q + am][j], out[Q + am]);
+      if (am > 0) out[Q - am] = caxpy(f, acc[Q - am][j], out[Q - am]);
+      f *= rho_t;
+    }
   }
 }
 
@@ -909,22 +1004,43 @@ cudaError_t h2_launch_form_strengths(const qbxfmm_geometry& g, const qbxfmm_upsa
   return cudaGetLastError();
 }
 
+template <bool LOCAL, int RW, int TR>
+static cudaError_t h2_p2e_rt(const qbxfmm_geometry& g, HelmCoeffs hc, int p, int nrhs, int nb,
+                             const double2* s, double2* e, int32_t* err, cudaStream_t st)
+{
+  size_t sh = (size_t)32 * (zsh(p) + (2 * p + 1) + RW * TR + 1) * sizeof(double2);
+  cudaError_t ce = cudaFuncSetAttribute(k_h2_p2e<LOCAL, RW, TR>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+  if (ce != cudaSuccess) return ce;
+  k_h2_p2e<LOCAL, RW, TR><<<dim3(nb, (nrhs + RW * TR - 1) / (RW * TR)), NT, sh, st>>>(
+      g, hc, p, nrhs, s, e, err);
+  return cudaGetLastError();
+}
+
+template <bool LOCAL>
+static cudaError_t h2_p2e(const qbxfmm_geometry& g, HelmCoeffs hc, int p, int nrhs, int nb,
+                          const double2* s, double2* e, int32_t* err, cudaStream_t st)
+{
+  if (p > 20) return cudaErrorInvalidValue;
+  if (nrhs == 1) return h2_p2e_rt<LOCAL, 1, 1>(g, hc, p, nrhs, nb, s, e, err, st);
+  if (nrhs <= 4) return h2_p2e_rt<LOCAL, 4, 1>(g, hc, p, nrhs, nb, s, e, err, st);
+  if (nrhs <= 16) return h2_p2e_rt<LOCAL, 16, 1>(g, hc, p, nrhs, nb, s, e, err, st);
+  if (nrhs <= 32) return h2_p2e_rt<LOCAL, 32, 1>(g, hc, p, nrhs, nb, s, e, err, st);
+  return h2_p2e_rt<LOCAL, 32, 2>(g, hc, p, nrhs, nb, s, e, err, st);
+}
+
 cudaError_t h2_launch_p2m(const qbxfmm_geometry& g, HelmCoeffs hc, int p, int nrhs,
                           const double2* s, double2* mp, int32_t* err, cudaStream_t st)
 {
   if (g.nsource_boxes == 0) return cudaSuccess;
-  size_t sh = 32 * zsh(p) * sizeof(double2);
-  k_h2_p2e<false><<<dim3(g.nsource_boxes, nrhs), NT, sh, st>>>(g, hc, p, nrhs, s, mp, err);
-  return cudaGetLastError();
+  return h2_p2e<false>(g, hc, p, nrhs, g.nsource_boxes, s, mp, err, st);
 }
 
 cudaError_t h2_launch_p2l(const qbxfmm_geometry& g, HelmCoeffs hc, int p, int nrhs,
                           const double2* s, double2* lo, int32_t* err, cudaStream_t st)
 {
   if (g.nttp_boxes == 0) return cudaSuccess;
-  size_t sh = 32 * zsh(p) * sizeof(double2);
-  k_h2_p2e<true><<<dim3(g.nttp_boxes, nrhs), NT, sh, st>>>(g, hc, p, nrhs, s, lo, err);
-  return cudaGetLastError();
+  return h2_p2e<true>(g, hc, p, nrhs, g.nttp_boxes, s, lo, err, st);
 }
 
 // right-hand-side tiling of the translation kernels: (lanes over rhs, rhs per lane)
@@ -1019,15 +1135,37 @@ static cudaError_t h2_p2qbxl_q(const qbxfmm_geometry& g, HelmCoeffs hc, int nrhs
   return cudaGetLastError();
 }
 
+template <int Q, bool FROM_LOCAL, int RW, int TR, int CW>
+static cudaError_t h2_e2qbxl_rt(const qbxfmm_geometry& g, HelmCoeffs hc, int pf, int nrhs,
+                                const double2* e, double2* qe, int32_t* err, cudaStream_t st)
+{
+  size_t sh = ((size_t)CW * (2 * (pf + Q) + 1) + (size_t)RW * TR * (2 * pf + 1)) * sizeof(double2);
+  cudaError_t ce = cudaFuncSetAttribute(k_h2_e2qbxl<Q, FROM_LOCAL, RW, TR, CW>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+  if (ce != cudaSuccess) return ce;
+  dim3 grid(g.nqbx_chunks, (32 / CW) * ((nrhs + RW * TR - 1) / (RW * TR)));
+  k_h2_e2qbxl<Q, FROM_LOCAL, RW, TR, CW><<<grid, RW * CW, sh, st>>>(g, hc, pf, nrhs, e, qe, err);
+  return cudaGetLastError();
+}
+
+template <int Q, bool FROM_LOCAL>
+static cudaError_t h2_e2qbxl_qf(const qbxfmm_geometry& g, HelmCoeffs hc, int pf, int nrhs,
+                                const double2* e, double2* qe, int32_t* err, cudaStream_t st)
+{
+  if (nrhs == 1) return h2_e2qbxl_rt<Q, FROM_LOCAL, 1, 1, 32>(g, hc, pf, nrhs, e, qe, err, st);
+  if (nrhs <= 4) return h2_e2qbxl_rt<Q, FROM_LOCAL, 4, 1, 32>(g, hc, pf, nrhs, e, qe, err, st);
+  if (nrhs <= 32) return h2_e2qbxl_rt<Q, FROM_LOCAL, 32, 1, 8>(g, hc, pf, nrhs, e, qe, err, st);
+  return h2_e2qbxl_rt<Q, FROM_LOCAL, 32, 2, 8>(g, hc, pf, nrhs, e, qe, err, st);
+}
+
 template <int Q>
 static cudaError_t h2_e2qbxl_q(const qbxfmm_geometry& g, HelmCoeffs hc, int pf, int nrhs,
                                const double2* e, double2* qe, int32_t* err, bool from_local,
                                cudaStream_t st)
 {
-  dim3 grid((g.nglobal_qbx_centers + NT - 1) / NT, nrhs);
-  if (from_local) k_h2_e2qbxl<Q, true><<<grid, NT, 0, st>>>(g, hc, pf, nrhs, e, qe, err);
-  else k_h2_e2qbxl<Q, false><<<grid, NT, 0, st>>>(g, hc, pf, nrhs, e, qe, err);
-  return cudaGetLastError();
+  if (pf > 20 || g.nqbx_chunks == 0) return pf > 20 ? cudaErrorInvalidValue : cudaSuccess;
+  if (from_local) return h2_e2qbxl_qf<Q, true>(g, hc, pf, nrhs, e, qe, err, st);
+  return h2_e2qbxl_qf<Q, false>(g, hc, pf, nrhs, e, qe, err, st);
 }
 
 template <int Q>
