@@ -807,6 +807,169 @@ k_h2_tsqbx(qbxfmm_geometry g, HelmCoeffs hc, int nrhs, const double2* __restrict
   }
 }
 
+// The same near field for many right-hand sides: per source tile of TS_ST sources the
+// kernel values K(t, y) of all (target, source) pairs of the chunk are computed once,
+// packed over all threads (a chunk holds the few targets of one box), into shared
+// memory; then pot[t][r] += sum_y K(t, y) str_y[r] over a tile of 64 right-hand sides
+// (thread: rhs tid % 64, targets tid / 64 + 2 i).
+constexpr int TS_ST = 32;
+constexpr int TS_RC = 64;
+
+template <int Q>
+__global__ void __launch_bounds__(NT)
+k_h2_tsqbx_many(qbxfmm_geometry g, HelmCoeffs hc, int nrhs, const double2* __restrict__ strengths,
+                double2* __restrict__ pot_tree, int32_t* err)
+{
+  constexpr int NQ = 2 * Q + 1;
+  extern __shared__ double2 smem2[];
+  double2* S = smem2;                         // [TS_ST][TS_RC]
+  double2* K = S + TS_ST * TS_RC;             // [TS_ST][32]
+  __shared__ double2 s_zt[32][NQ];
+  __shared__ double s_cc[2][32];
+  __shared__ double s_y[2][TS_ST], s_n[2][TS_ST];
+  __shared__ int s_src[TS_ST];
+  __shared__ int s_pref[MAXB + 1], s_start[MAXB];
+  int chunk = blockIdx.x;
+  int r0 = blockIdx.y * TS_RC;
+  int nr = min(TS_RC, nrhs - r0);
+  int itb = g.tsqbx_chunk_target_box[chunk];
+  int i0 = g.tsqbx_chunk_start[chunk];
+  int cnt = min(g.tsqbx_chunk_count[chunk], 32);
+  if (g.tsqbx_chunk_count[chunk] > 32 && blockIdx.y == 0 && threadIdx.x == 0)
+    report(err, QBX_DEVERR_BAD_CENTER);
+  // per target: its center and J_m(t - c) e^{i m th}
+  if (threadIdx.x < cnt) {
+    int t = g.tsqbx_targets[i0 + threadIdx.x];
+    int ctr = g.tsqbx_centers[i0 + threadIdx.x];
+    double cc[2] = {0, 0}, x[2] = {0, 0};
+    if ((unsigned)ctr >= (unsigned)g.ncenters || (unsigned)t >= (unsigned)g.ntargets) {
+      report(err, QBX_DEVERR_BAD_CENTER);
+    } else {
+      load_point<2>(g.centers, g.ncenters, ctr, cc);
+      load_point<2>(g.targets, g.ntargets, t, x);
+    }
+    s_cc[0][threadIdx.x] = cc[0];
+    s_cc[1][threadIdx.x] = cc[1];
+    double ax = x[0] - cc[0], ay = x[1] - cc[1];
+    double alen = sqrt(ax * ax + ay * ay);
+    double J[Q + 1];
+    if (alen > 0.0) {
+      double Yd[1];
+      bessel_jy(Q, hc.k * alen, J, Yd, false);
+    } else {
+#pragma unroll
+      for (int m = 0; m <= Q; ++m) J[m] = (m == 0) ? 1.0 : 0.0;
+    }
+    double2 e1 = alen > 0.0 ? c2(ax / alen, ay / alen) : c2(1.0);
+    double2 e = c2(1.0);
+#pragma unroll
+    for (int m = 0; m <= Q; ++m) {
+      s_zt[threadIdx.x][Q + m] = cscale(J[m], e);
+      double2 w = cscale(J[m], cconj(e));
+      s_zt[threadIdx.x][Q - m] = (m & 1) ? cneg(w) : w;
+      e = cmul(e, e1);
+    }
+  }
+  const bool chg = hc.cq.x != 0.0 || hc.cq.y != 0.0;
+  const bool dip = hc.cd.x != 0.0 || hc.cd.y != 0.0;
+  const double2 kd = cscale(0.5 * hc.k, hc.cd);
+  const int rr = threadIdx.x % TS_RC, th = threadIdx.x / TS_RC;
+  const int nti = (cnt - th + 1) / 2;           // targets th + 2 i, i < nti
+  double2 acc[16];
+#pragma unroll
+  for (int i = 0; i < 16; ++i) acc[i] = c2(0.0);
+  int l0 = g.list1_starts[itb], l1 = g.list1_starts[itb + 1];
+  for (int gb = l0; gb < l1; gb += MAXB) {
+    int nb = min(MAXB, l1 - gb);
+    __syncthreads();
+    h_list_prefix(g, g.list1_lists, gb, nb, s_pref, s_start, err);
+    __syncthreads();
+    int total = s_pref[nb];
+    for (int base = 0; base < total; base += TS_ST) {
+      int ns = min(TS_ST, total - base);
+      if (threadIdx.x < ns) {
+        int s = h_stream_source(base + threadIdx.x, nb, s_pref, s_start);
+        double y[2], nv[2] = {0, 0};
+        load_point<2>(g.sources, g.nsources, s, y);
+        if (dip) load_point<2>(g.source_normals, g.nsources, s, nv);
+        s_src[threadIdx.x] = s;
+        s_y[0][threadIdx.x] = y[0];
+        s_y[1][threadIdx.x] = y[1];
+        s_n[0][threadIdx.x] = nv[0];
+        s_n[1][threadIdx.x] = nv[1];
+      }
+      __syncthreads();
+      for (int w = threadIdx.x; w < ns * TS_RC; w += NT) {
+        int j = w / TS_RC, r = w - j * TS_RC;
+        S[w] = r < nr ? strengths[(size_t)(r0 + r) * g.nsources + s_src[j]] : c2(0.0);
+      }
+      for (int pr = threadIdx.x; pr < ns * cnt; pr += NT) {
+        int j = pr / cnt, t = pr - j * cnt;
+        double ux = s_y[0][j] - s_cc[0][t], uy = s_y[1][j] - s_cc[1][t];
+        double b2 = ux * ux + uy * uy;
+        double2 Kv = c2(0.0);
+        if (b2 != 0.0) {
+          double binv = rsqrt(b2);
+          double xx = hc.k * b2 * binv, xinv = 1.0 / xx;
+          double2 H[Q + 2];
+          H[0] = c2(j0(xx), y0(xx));
+          H[1] = c2(j1(xx), y1(xx));
+#pragma unroll
+          for (int m = 1; m <= Q; ++m)
+            H[m + 1] = c2(2.0 * m * xinv * H[m].x - H[m - 1].x, 2.0 * m * xinv * H[m].y - H[m - 1].y);
+          // Hb_m for m in [-(Q+1), Q+1] at Hb[Q + 1 + m]
+          double2 Hb[2 * Q + 3];
+          double2 e1 = c2(ux * binv, -uy * binv);     // e^{-i th}
+          double2 e = c2(1.0);
+#pragma unroll
+          for (int m = 0; m <= Q + 1; ++m) {
+            Hb[Q + 1 + m] = cmul(H[m], e);
+            double2 w = cmul(H[m], cconj(e));
+            Hb[Q + 1 - m] = (m & 1) ? cneg(w) : w;
+            e = cmul(e, e1);
+          }
+          const double2* Zt = s_zt[t];
+          if (chg) {
+            double2 s0 = c2(0.0);
+#pragma unroll
+            for (int m = -Q; m <= Q; ++m) s0 = cfma(Zt[Q + m], Hb[Q + 1 + m], s0);
+            Kv = cmul(hc.cq, s0);
+          }
+          if (dip) {
+            double2 sm = c2(0.0), sp = c2(0.0);
+#pragma unroll
+            for (int m = -Q; m <= Q; ++m) {
+              sm = cfma(Zt[Q + m], Hb[Q + m], sm);
+              sp = cfma(Zt[Q + m], Hb[Q + 2 + m], sp);
+            }
+            double2 nu = c2(s_n[0][j], s_n[1][j]);
+            Kv = cfma(kd, csub(cmul(cconj(nu), sm), cmul(nu, sp)), Kv);
+          }
+        }
+        K[j * 32 + t] = Kv;
+      }
+      __syncthreads();
+      for (int j = 0; j < ns; ++j) {
+        double2 sv = S[j * TS_RC + rr];
+        const double2* Kj = K + j * 32 + th;
+#pragma unroll
+        for (int i = 0; i < 16; ++i)
+          if (i < nti) acc[i] = cfma(Kj[2 * i], sv, acc[i]);
+      }
+      __syncthreads();
+    }
+  }
+  if (rr >= nr) return;
+#pragma unroll
+  for (int i = 0; i < 16; ++i) {
+    if (i >= nti) break;
+    int t = g.tsqbx_targets[i0 + th + 2 * i];
+    if ((unsigned)t >= (unsigned)g.ntargets) continue;
+    double2* P = pot_tree + (size_t)(r0 + rr) * g.ntargets + t;
+    *P = cadd(*P, acc[i]);
+  }
+}
+
 // M2QBXL (list 3) and L2QBXL (own target box):
 //   Q_m[r] += rho_c^|m| sum_n Z_{n-m}(c - c_b) f(n) E_n[r],  f(n) = rho_b^{+-|n|},
 // Z = H (from multipoles) or J (from locals), m in [-Q, Q], n in [-pf, pf].  One CTA
@@ -1231,9 +1394,23 @@ static cudaError_t h2_tsqbx_qr(const qbxfmm_geometry& g, HelmCoeffs hc, int nrhs
 }
 
 template <int Q>
+static cudaError_t h2_tsqbx_many_q(const qbxfmm_geometry& g, HelmCoeffs hc, int nrhs,
+                                   const double2* s, double2* pt, int32_t* err, cudaStream_t st)
+{
+  size_t sh = (size_t)TS_ST * (TS_RC + 32) * sizeof(double2);
+  cudaError_t ce = cudaFuncSetAttribute(k_h2_tsqbx_many<Q>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+  if (ce != cudaSuccess) return ce;
+  dim3 grid(g.ntsqbx_chunks, (nrhs + TS_RC - 1) / TS_RC);
+  k_h2_tsqbx_many<Q><<<grid, NT, sh, st>>>(g, hc, nrhs, s, pt, err);
+  return cudaGetLastError();
+}
+
+template <int Q>
 static cudaError_t h2_tsqbx_q(const qbxfmm_geometry& g, HelmCoeffs hc, int nrhs, const double2* s,
                               double2* pt, int32_t* err, cudaStream_t st)
 {
+  if (nrhs > 16) return h2_tsqbx_many_q<Q>(g, hc, nrhs, s, pt, err, st);
   if (nrhs == 1) return h2_tsqbx_qr<Q, 1>(g, hc, nrhs, s, pt, err, st);
   if (nrhs <= 4) return h2_tsqbx_qr<Q, 4>(g, hc, nrhs, s, pt, err, st);
   return h2_tsqbx_qr<Q, 16>(g, hc, nrhs, s, pt, err, st);
