@@ -975,9 +975,12 @@ k_h2_tsqbx_many(qbxfmm_geometry g, HelmCoeffs hc, int nrhs, const double2* __res
 // Z = H (from multipoles) or J (from locals), m in [-Q, Q], n in [-pf, pf].  One CTA
 // per (CW centers of a QBX chunk, tile of RW * TR right-hand sides); all centers of a
 // chunk share a target box and so its list 3.  Thread t: rhs lane rl = t % RW (rhs
-// rl + RW j), center t / RW, all 2Q+1 coefficients in registers.  Per source box the
-// scaled coefficient block is staged once in shared memory and each center's Z table
-// (order pf + Q) is built once, by one thread.
+// rl + RW j), center t / RW, all 2Q+1 coefficients in registers.  Source boxes go in
+// batches of E2Q_LB: the Z tables (order pf + Q) of all (center, box) pairs of a batch
+// are built in parallel, one per thread (CW * E2Q_LB = 32 for the 128-thread tiles); then per box the scaled coefficient block is
+// staged once in shared memory for all centers.
+constexpr int E2Q_LB = 8;
+
 template <int Q, bool FROM_LOCAL, int RW, int TR, int CW>
 __global__ void __launch_bounds__(RW * CW)
 k_h2_e2qbxl(qbxfmm_geometry g, HelmCoeffs hc, int pf, int nrhs, const double2* __restrict__ exps,
@@ -989,10 +992,11 @@ k_h2_e2qbxl(qbxfmm_geometry g, HelmCoeffs hc, int pf, int nrhs, const double2* _
   constexpr int NSUB = 32 / CW;
   extern __shared__ double2 smem2[];
   const int NZ = pf + Q, ZW = 2 * NZ + 1, NC = 2 * pf + 1;
-  double2* Zc = smem2;                        // [CW][ZW]
-  double2* E = Zc + (size_t)CW * ZW;          // [RC][NC]
-  __shared__ double s_fn[2 * 20 + 1];
-  __shared__ int s_sb;
+  double2* Zc = smem2;                                 // [E2Q_LB][CW][ZW]
+  double2* E = Zc + (size_t)E2Q_LB * CW * ZW;          // [RC][NC]
+  __shared__ double s_fn[E2Q_LB][2 * 20 + 1];
+  __shared__ int s_sb[E2Q_LB];
+  __shared__ double s_cc[2][CW];
   double Jb[ZMAX], Yb[ZMAX];
   int chunk = blockIdx.x;
   int sub = blockIdx.y % NSUB;
@@ -1012,6 +1016,12 @@ k_h2_e2qbxl(qbxfmm_geometry g, HelmCoeffs hc, int pf, int nrhs, const double2* _
     has_center = false;
     ctr = 0;
   }
+  if (rl == 0) {
+    double cc[2];
+    load_point<2>(g.centers, g.ncenters, ctr, cc);
+    s_cc[0][cw] = cc[0];
+    s_cc[1][cw] = cc[1];
+  }
   double2 acc[NQ][TR];
 #pragma unroll
   for (int a = 0; a < NQ; ++a)
@@ -1019,47 +1029,56 @@ k_h2_e2qbxl(qbxfmm_geometry g, HelmCoeffs hc, int pf, int nrhs, const double2* _
     for (int j = 0; j < TR; ++j) acc[a][j] = c2(0.0);
   int l0 = FROM_LOCAL ? 0 : g.list3_starts[itb];
   int l1 = FROM_LOCAL ? 1 : g.list3_starts[itb + 1];
-  for (int li = l0; li < l1; ++li) {
-    __syncthreads();                           // E, Zc and s_fn free
-    if (threadIdx.x == 0) {
-      int sb = FROM_LOCAL ? g.target_boxes[itb] : g.list3_lists[li];
+  for (int lb = l0; lb < l1; lb += E2Q_LB) {
+    int nbat = min(E2Q_LB, l1 - lb);
+    __syncthreads();                           // Zc, s_sb, s_fn free; s_cc written
+    if (threadIdx.x < nbat) {
+      int sb = FROM_LOCAL ? g.target_boxes[itb] : g.list3_lists[lb + threadIdx.x];
       if ((unsigned)sb >= (unsigned)g.nboxes) {
         report(err, QBX_DEVERR_BAD_BOX);
         sb = -1;
       }
-      s_sb = sb;
+      s_sb[threadIdx.x] = sb;
     }
     __syncthreads();
-    int sb = s_sb;
-    if (sb < 0) continue;                      // uniform over the CTA
-    double rho_s = level_width(g, g.box_levels[sb]);
-    double cs[2];
-    load_point<2>(g.box_centers, g.nboxes, sb, cs);
-    for (int w = threadIdx.x; w < NC; w += NTH) {
-      int an = w - pf < 0 ? pf - w : w - pf;
-      s_fn[w] = FROM_LOCAL ? pow(rho_s, -(double)an) : pow(rho_s, (double)an);
+    for (int pi = threadIdx.x; pi < nbat * CW; pi += NTH) {
+      int bb = pi / CW, c = pi % CW;
+      int sb = s_sb[bb];
+      if (sb >= 0 && c < ncen) {
+        double cs[2];
+        load_point<2>(g.box_centers, g.nboxes, sb, cs);
+        h2_zfun(NZ, hc.k, s_cc[0][c] - cs[0], s_cc[1][c] - cs[1], Jb, Yb,
+                Zc + ((size_t)bb * CW + c) * ZW, !FROM_LOCAL);
+      }
     }
-    if (rl == 0 && has_center) {
-      double cc[2];
-      load_point<2>(g.centers, g.ncenters, ctr, cc);
-      h2_zfun(NZ, hc.k, cc[0] - cs[0], cc[1] - cs[1], Jb, Yb, Zc + (size_t)cw * ZW, !FROM_LOCAL);
+    for (int w = threadIdx.x; w < nbat * NC; w += NTH) {
+      int bb = w / NC, n = w - bb * NC;
+      int sb = s_sb[bb];
+      if (sb < 0) continue;
+      double rho_s = level_width(g, g.box_levels[sb]);
+      int an = n - pf < 0 ? pf - n : n - pf;
+      s_fn[bb][n] = FROM_LOCAL ? pow(rho_s, -(double)an) : pow(rho_s, (double)an);
     }
-    __syncthreads();
-    const double2* src = exps + ((size_t)sb * nrhs + r0) * NC;
-    for (int w = threadIdx.x; w < nr * NC; w += NTH) E[w] = cscale(s_fn[w % NC], src[w]);
-    __syncthreads();
-    if (has_center) {
-      // Z_{n-m} for coefficient indices n in [0, 2pf], a = m + Q in [0, 2Q] at Zr[n - pf - a + Q]
-      const double2* Zr = Zc + (size_t)cw * ZW + NZ - pf + Q;
-      for (int n = 0; n < NC; ++n) {
-        double2 e[TR];
+    for (int bb = 0; bb < nbat; ++bb) {
+      int sb = s_sb[bb];
+      if (sb < 0) continue;                    // uniform over the CTA
+      __syncthreads();                         // E free; Zc, s_fn written
+      const double2* src = exps + ((size_t)sb * nrhs + r0) * NC;
+      for (int w = threadIdx.x; w < nr * NC; w += NTH) E[w] = cscale(s_fn[bb][w % NC], src[w]);
+      __syncthreads();
+      if (has_center) {
+        // Z_{n-m} for coefficient indices n in [0, 2pf], a = m + Q in [0, 2Q] at Zr[n - a]
+        const double2* Zr = Zc + ((size_t)bb * CW + cw) * ZW + NZ - pf + Q;
+        for (int n = 0; n < NC; ++n) {
+          double2 e[TR];
 #pragma unroll
-        for (int j = 0; j < TR; ++j) e[j] = E[(rl + RW * j) * NC + n];
+          for (int j = 0; j < TR; ++j) e[j] = E[(rl + RW * j) * NC + n];
 #pragma unroll
-        for (int a = 0; a < NQ; ++a) {
-          double2 z = Zr[n - a];
+          for (int a = 0; a < NQ; ++a) {
+            double2 z = Zr[n - a];
 #pragma unroll
-          for (int j = 0; j < TR; ++j) acc[a][j] = cfma(z, e[j], acc[a][j]);
+            for (int j = 0; j < TR; ++j) acc[a][j] = cfma(z, e[j], acc[a][j]);
+          }
         }
       }
     }
@@ -1302,7 +1321,8 @@ template <int Q, bool FROM_LOCAL, int RW, int TR, int CW>
 static cudaError_t h2_e2qbxl_rt(const qbxfmm_geometry& g, HelmCoeffs hc, int pf, int nrhs,
                                 const double2* e, double2* qe, int32_t* err, cudaStream_t st)
 {
-  size_t sh = ((size_t)CW * (2 * (pf + Q) + 1) + (size_t)RW * TR * (2 * pf + 1)) * sizeof(double2);
+  size_t sh = ((size_t)E2Q_LB * CW * (2 * (pf + Q) + 1) + (size_t)RW * TR * (2 * pf + 1)) *
+              sizeof(double2);
   cudaError_t ce = cudaFuncSetAttribute(k_h2_e2qbxl<Q, FROM_LOCAL, RW, TR, CW>,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
   if (ce != cudaSuccess) return ce;
@@ -1317,8 +1337,8 @@ static cudaError_t h2_e2qbxl_qf(const qbxfmm_geometry& g, HelmCoeffs hc, int pf,
 {
   if (nrhs == 1) return h2_e2qbxl_rt<Q, FROM_LOCAL, 1, 1, 32>(g, hc, pf, nrhs, e, qe, err, st);
   if (nrhs <= 4) return h2_e2qbxl_rt<Q, FROM_LOCAL, 4, 1, 32>(g, hc, pf, nrhs, e, qe, err, st);
-  if (nrhs <= 32) return h2_e2qbxl_rt<Q, FROM_LOCAL, 32, 1, 8>(g, hc, pf, nrhs, e, qe, err, st);
-  return h2_e2qbxl_rt<Q, FROM_LOCAL, 32, 2, 8>(g, hc, pf, nrhs, e, qe, err, st);
+  if (nrhs <= 32) return h2_e2qbxl_rt<Q, FROM_LOCAL, 32, 1, 4>(g, hc, pf, nrhs, e, qe, err, st);
+  return h2_e2qbxl_rt<Q, FROM_LOCAL, 32, 2, 4>(g, hc, pf, nrhs, e, qe, err, st);
 }
 
 template <int Q>
