@@ -822,8 +822,8 @@ k_h2_tsqbx_many(qbxfmm_geometry g, HelmCoeffs hc, int nrhs, const double2* __res
 {
   constexpr int NQ = 2 * Q + 1;
   extern __shared__ double2 smem2[];
-  double2* S = smem2;                         // [TS_ST][TS_RC]
-  double2* K = S + TS_ST * TS_RC;             // [TS_ST][32]
+  double2* S = smem2;                         // [TS_ST][TS_RC + 1] (padded rows)
+  double2* K = S + TS_ST * (TS_RC + 1);       // [TS_ST][32]
   __shared__ double2 s_zt[32][NQ];
   __shared__ double s_cc[2][32];
   __shared__ double s_y[2][TS_ST], s_n[2][TS_ST];
@@ -900,8 +900,8 @@ k_h2_tsqbx_many(qbxfmm_geometry g, HelmCoeffs hc, int nrhs, const double2* __res
       }
       __syncthreads();
       for (int w = threadIdx.x; w < ns * TS_RC; w += NT) {
-        int j = w / TS_RC, r = w - j * TS_RC;
-        S[w] = r < nr ? strengths[(size_t)(r0 + r) * g.nsources + s_src[j]] : c2(0.0);
+        int r = w / ns, j = w - r * ns;       // sources fastest: coalesced rows
+        S[j * (TS_RC + 1) + r] = r < nr ? strengths[(size_t)(r0 + r) * g.nsources + s_src[j]] : c2(0.0);
       }
       for (int pr = threadIdx.x; pr < ns * cnt; pr += NT) {
         int j = pr / cnt, t = pr - j * cnt;
@@ -950,7 +950,7 @@ k_h2_tsqbx_many(qbxfmm_geometry g, HelmCoeffs hc, int nrhs, const double2* __res
       }
       __syncthreads();
       for (int j = 0; j < ns; ++j) {
-        double2 sv = S[j * TS_RC + rr];
+        double2 sv = S[j * (TS_RC + 1) + rr];
         const double2* Kj = K + j * 32 + th;
 #pragma unroll
         for (int i = 0; i < 16; ++i)
@@ -998,9 +998,10 @@ k_h2_e2qbxl(qbxfmm_geometry g, HelmCoeffs hc, int pf, int nrhs, const double2* _
   __shared__ int s_sb[E2Q_LB];
   __shared__ double s_cc[2][CW];
   double Jb[ZMAX], Yb[ZMAX];
-  int chunk = blockIdx.x;
-  int sub = blockIdx.y % NSUB;
-  int r0 = (blockIdx.y / NSUB) * RC;
+  // the sub-chunks of a chunk are adjacent in launch order: they read the same boxes
+  int chunk = blockIdx.x / NSUB;
+  int sub = blockIdx.x % NSUB;
+  int r0 = blockIdx.y * RC;
   int nr = min(RC, nrhs - r0);
   int ncen = g.qbx_chunk_count[chunk];
   if (ncen > 32 && sub == 0 && threadIdx.x == 0) report(err, QBX_DEVERR_BAD_CENTER);
@@ -1326,7 +1327,7 @@ static cudaError_t h2_e2qbxl_rt(const qbxfmm_geometry& g, HelmCoeffs hc, int pf,
   cudaError_t ce = cudaFuncSetAttribute(k_h2_e2qbxl<Q, FROM_LOCAL, RW, TR, CW>,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
   if (ce != cudaSuccess) return ce;
-  dim3 grid(g.nqbx_chunks, (32 / CW) * ((nrhs + RW * TR - 1) / (RW * TR)));
+  dim3 grid(g.nqbx_chunks * (32 / CW), (nrhs + RW * TR - 1) / (RW * TR));
   k_h2_e2qbxl<Q, FROM_LOCAL, RW, TR, CW><<<grid, RW * CW, sh, st>>>(g, hc, pf, nrhs, e, qe, err);
   return cudaGetLastError();
 }
@@ -1417,7 +1418,7 @@ template <int Q>
 static cudaError_t h2_tsqbx_many_q(const qbxfmm_geometry& g, HelmCoeffs hc, int nrhs,
                                    const double2* s, double2* pt, int32_t* err, cudaStream_t st)
 {
-  size_t sh = (size_t)TS_ST * (TS_RC + 32) * sizeof(double2);
+  size_t sh = (size_t)TS_ST * (TS_RC + 1 + 32) * sizeof(double2);
   cudaError_t ce = cudaFuncSetAttribute(k_h2_tsqbx_many<Q>,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
   if (ce != cudaSuccess) return ce;

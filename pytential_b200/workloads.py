@@ -178,10 +178,12 @@ def laplace3d_adjoint(nrefine: int = 4, ntargets: int = 5000, ncharges: int = 8,
 
 
 def _main(argv=None):
-    """``python -m pytential_b200.workloads NAME NREFINE [APPLIES]``: build one of the
-    3D workloads (``laplace3d`` double layer, or ``helmholtz3d`` combined field with
-    16 densities) and run ``APPLIES`` whole applies (target-specific near field) on
-    the current GPU, printing the time of the last; a driver for profilers."""
+    """``python -m pytential_b200.workloads NAME SIZE [APPLIES]``: build one of the
+    workloads (``laplace3d`` double layer or ``helmholtz3d`` combined field with 16
+    densities, SIZE = icosphere refinements; ``helmholtz2d`` Brakhage-Werner with 64
+    densities, SIZE = starfish elements) and run ``APPLIES`` whole applies
+    (target-specific near field) on the current GPU, printing the time of the last; a
+    driver for profilers."""
     import argparse
     import time
 
@@ -189,12 +191,16 @@ def _main(argv=None):
 
     from .fmm import QBXApply
     ap = argparse.ArgumentParser(prog="python -m pytential_b200.workloads")
-    ap.add_argument("name", choices=["laplace3d", "helmholtz3d"])
-    ap.add_argument("nrefine", type=int)
+    ap.add_argument("name", choices=["laplace3d", "helmholtz3d", "helmholtz2d"])
+    ap.add_argument("size", type=int)
     ap.add_argument("applies", type=int, nargs="?", default=1)
     a = ap.parse_args(argv)
-    wl = (laplace3d_ellipsoid(nrefine=a.nrefine) if a.name == "laplace3d"
-          else helmholtz3d_ellipsoid(nrefine=a.nrefine))
+    if a.name == "laplace3d":
+        wl = laplace3d_ellipsoid(nrefine=a.size)
+    elif a.name == "helmholtz3d":
+        wl = helmholtz3d_ellipsoid(nrefine=a.size)
+    else:
+        wl = helmholtz2d_starfish(nelements=a.size)
     qa = QBXApply(wl.geometry(), wl.spec, wl.qbx_order, wl.fmm_order, nrhs=wl.nrhs,
                   target_specific_qbx=True)
     dens = torch.from_numpy(wl.density).cuda()
