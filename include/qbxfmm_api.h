@@ -154,6 +154,53 @@ int qbxfmm_laplace3d_qbx_matrix(int nsources, const double* sources, const doubl
                                 int ncenters, const double* centers, int qbx_order, double* K,
                                 void* stream);
 
+/* Target-to-QBX-center association (replaces pytential's QBXTargetAssociator:
+ * marking, pytential/qbx/target_assoc.py:544-633, and center finding, 243-363 and
+ * 637-749, with the side requests of the table at 81-103).  Points are searched on
+ * uniform cell grids: qbxfmm_cell_keys gives each point (structure-of-arrays
+ * [dim][n], device) the key (ix * ncells[1] + iy) * ncells[2] + iz of its cell,
+ * i = floor((x - lo) / h) clamped to [0, ncells), and the caller sorts the keys
+ * (ascending) with the permutation that sorts them.  A grid's cell width h must be at
+ * least the search radius: the largest source tunnel radius (source grid) and the
+ * largest tolerant center radius (center grid).  In 2D ncells[2] = 1. */
+typedef struct {
+  double lo[3];
+  double h;
+  int64_t ncells[3];
+} qbxfmm_cell_grid;
+
+int qbxfmm_cell_keys(int dim, int n, const double* points, const qbxfmm_cell_grid* grid,
+                     int64_t* keys, void* stream);
+
+typedef struct {
+  int32_t dim;
+  int32_t ntargets;
+  const double* targets;               /* [dim][ntargets] */
+  const int32_t* target_sides;         /* 0, +-1 (surface), +-2 */
+  int32_t nsources;                    /* 0: no marking (surface targets only) */
+  const double* sources;               /* [dim][nsources] */
+  const double* source_tunnel_radii;   /* [nsources] */
+  const int64_t* source_keys;          /* sorted cell keys of the sources */
+  const int32_t* source_order;         /* source of each sorted key */
+  qbxfmm_cell_grid source_grid;
+  int32_t ncenters;                    /* even: interior (-1), odd: exterior (+1) */
+  const double* centers;               /* [dim][ncenters] */
+  const double* center_tolerant_radii; /* r_c (1 + tolerance) */
+  const int64_t* center_keys;
+  const int32_t* center_order;
+  qbxfmm_cell_grid center_grid;
+} qbxfmm_assoc_problem;
+
+/* target_to_center[t] = the chosen center, -1 (target needs no QBX) or -2 (a close
+ * target without an admissible center: the reference's association failure).  A
+ * target is close if |side| = 1 or some source lies within its tunnel radius; among
+ * centers of an admissible side with |t - c| <= r_c (1 + tolerance) the one of least
+ * |t - c| / (r_c (1 + tolerance)) on each side is taken (ties: lower index), then the
+ * side whose center is nearer (ties: interior).  Equal to the host restatement bit
+ * for bit (every distance operation separately rounded). */
+int qbxfmm_associate_targets(const qbxfmm_assoc_problem* problem, int32_t* target_to_center,
+                             void* stream);
+
 #ifdef __cplusplus
 }
 #endif

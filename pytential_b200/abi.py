@@ -98,6 +98,21 @@ class QBXFMMUpsample(ctypes.Structure):
                 ("quad_nodes_per_element", _i32), ("matrix", _pd), ("quad_weights", _pd)]
 
 
+class QBXFMMCellGrid(ctypes.Structure):
+    _fields_ = [("lo", _f64 * 3), ("h", _f64), ("ncells", ctypes.c_int64 * 3)]
+
+
+class QBXFMMAssocProblem(ctypes.Structure):
+    _fields_ = [("dim", _i32), ("ntargets", _i32), ("targets", ctypes.c_void_p),
+                ("target_sides", ctypes.c_void_p),
+                ("nsources", _i32), ("sources", ctypes.c_void_p),
+                ("source_tunnel_radii", ctypes.c_void_p), ("source_keys", ctypes.c_void_p),
+                ("source_order", ctypes.c_void_p), ("source_grid", QBXFMMCellGrid),
+                ("ncenters", _i32), ("centers", ctypes.c_void_p),
+                ("center_tolerant_radii", ctypes.c_void_p), ("center_keys", ctypes.c_void_p),
+                ("center_order", ctypes.c_void_p), ("center_grid", QBXFMMCellGrid)]
+
+
 class QBXFMMWorkspace(ctypes.Structure):
     _fields_ = [("strengths", ctypes.c_void_p), ("mpoles", ctypes.c_void_p),
                 ("locals", ctypes.c_void_p), ("qbx_exps", ctypes.c_void_p),

@@ -1,8 +1,8 @@
 """QBX FMM geometry data: centers, tree, traversal, target association, CSR lists.
 
 Mirrors ``QBXFMMGeometryData`` (pytential/qbx/geometry.py:361-899) method by method.
-Everything here is built once on the host and memoized; the apply consumes it as
-device CSR index arrays.
+Everything here is built once and memoized (on the host; the target association
+on the GPU when one is present); the apply consumes it as device CSR index arrays.
 """
 
 from __future__ import annotations
@@ -13,9 +13,18 @@ from functools import cached_property
 import numpy as np
 
 from .discretization import Discretization
-from .target_assoc import NO_QBX_NEEDED, associate_targets_to_qbx_centers
+from .target_assoc import (NO_QBX_NEEDED, associate_targets_to_qbx_centers,
+                           associate_targets_to_qbx_centers_device)
 from .traversal import Traversal, build_traversal
 from .tree import Tree, build_tree
+
+
+def _cuda_available() -> bool:
+    try:
+        import torch
+    except ImportError:
+        return False
+    return torch.cuda.is_available()
 
 
 @dataclass
@@ -118,7 +127,11 @@ class QBXFMMGeometryData:
         user = ti.targets[:, self.ncenters:]
         sides = self.target_side_preferences()[self.ncenters:]
         tunnel = 0.5 * self.discr.quad_expansion_radii()
-        ttc = associate_targets_to_qbx_centers(
+        # on a CUDA machine the association runs on the GPU (the same result bit for
+        # bit); without one, on the host
+        assoc = (associate_targets_to_qbx_centers_device if _cuda_available()
+                 else associate_targets_to_qbx_centers)
+        ttc = assoc(
             user, sides, self.discr.quad_nodes, tunnel,
             self.flat_centers(), self.flat_expansion_radii(),
             self.target_association_tolerance)

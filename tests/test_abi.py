@@ -68,3 +68,22 @@ def test_struct_layout_matches_c(tmp_path):
                      ctypes.sizeof(abi.QBXFMMUpsample), ctypes.sizeof(abi.QBXFMMWorkspace)]
     offs = list(map(int, out[4:]))
     assert offs == [getattr(abi.QBXFMMGeometry, f).offset for f in fields]
+
+
+def test_association_structs_match_c(tmp_path):
+    fields = [n for n, _ in abi.QBXFMMAssocProblem._fields_]
+    prog = ['#include <stdio.h>', '#include <stddef.h>', '#include "qbxfmm_api.h"',
+            'int main(void) {',
+            'printf("%zu %zu\\n", sizeof(qbxfmm_cell_grid), sizeof(qbxfmm_assoc_problem));']
+    for f in fields:
+        prog.append(f'printf("%zu\\n", offsetof(qbxfmm_assoc_problem, {f}));')
+    prog.append("return 0; }")
+    c = tmp_path / "assoc.c"
+    c.write_text("\n".join(prog))
+    exe = tmp_path / "assoc"
+    subprocess.run(["/usr/bin/gcc", "-I", os.path.join(ROOT, "include"), str(c), "-o", str(exe)],
+                   check=True)
+    out = list(map(int, subprocess.run([str(exe)], capture_output=True, text=True,
+                                       check=True).stdout.split()))
+    assert out[:2] == [ctypes.sizeof(abi.QBXFMMCellGrid), ctypes.sizeof(abi.QBXFMMAssocProblem)]
+    assert out[2:] == [getattr(abi.QBXFMMAssocProblem, f).offset for f in fields]
