@@ -103,15 +103,16 @@ def build_tree(sources: np.ndarray, targets: np.ndarray,
     lo = bmin - 0.5 * 1e-6 * ext
     root_extent = ext * (1 + 1e-6)
 
-    # box table (grown per level)
-    levels = [0]
-    parents = [-1]
-    ipos = [np.zeros(dim, np.int64)]
-    children = [np.zeros(nchild, np.int64)]
+    # box table, one block of arrays per level
+    lv_parents = [np.array([-1], np.int64)]
+    lv_ipos = [np.zeros((1, dim), np.int64)]
+    lv_cidx = [np.zeros(1, np.int64)]
+    nboxes = 1
 
     pbox = np.zeros(npart, np.int64)
     settled = np.zeros(npart, bool)
     level_start = [0, 1]
+    box_ipos_all = lv_ipos[0]
 
     for level in range(max_levels):
         b0, b1 = level_start[-2], level_start[-1]
@@ -129,7 +130,7 @@ def build_tree(sources: np.ndarray, targets: np.ndarray,
         cand = movable & split[np.clip(pbox - b0, 0, b1 - b0 - 1)]
         idx = np.where(cand)[0]
         w_child = root_extent / 2.0 ** (level + 1)
-        bpos = np.array(ipos, dtype=np.int64)[pbox[idx]]          # (k, dim)
+        bpos = box_ipos_all[pbox[idx]]                            # (k, dim)
         rel = (pts[:, idx].T - lo) / w_child                      # in child units
         cpos = np.floor(rel).astype(np.int64)
         cpos = np.clip(cpos, 2 * bpos, 2 * bpos + 1)
@@ -145,46 +146,52 @@ def build_tree(sources: np.ndarray, targets: np.ndarray,
         # unique (parent, child index) pairs in parent order then child index
         key = pbox[mv] * nchild + cidx
         ukeys, inv = np.unique(key, return_inverse=True)
-        newstart = len(levels)
-        for j, kk in enumerate(ukeys):
-            par = int(kk // nchild)
-            ci = int(kk % nchild)
-            levels.append(level + 1)
-            parents.append(par)
-            p = ipos[par]
-            off = np.array([(ci >> d) & 1 for d in range(dim)], np.int64)
-            ipos.append(2 * p + off)
-            children.append(np.zeros(nchild, np.int64))
-            children[par][ci] = newstart + j
-        pbox[mv] = newstart + inv
-        level_start.append(len(levels))
-    nboxes = len(levels)
+        par = ukeys // nchild
+        ci = ukeys % nchild
+        off = (ci[:, None] >> np.arange(dim)[None, :]) & 1
+        newpos = 2 * box_ipos_all[par] + off
+        lv_parents.append(par)
+        lv_ipos.append(newpos)
+        lv_cidx.append(ci)
+        box_ipos_all = np.concatenate([box_ipos_all, newpos])
+        pbox[mv] = nboxes + inv.reshape(-1)
+        nboxes += len(ukeys)
+        level_start.append(nboxes)
     nlevels = len(level_start) - 1
     while nlevels > 0 and level_start[nlevels] == level_start[nlevels - 1]:
         nlevels -= 1
     level_start = np.array(level_start[:nlevels + 1], dtype=np.int32)
 
-    box_levels = np.array(levels, np.int32)
-    box_parent = np.array(parents, np.int32)
-    box_ipos = np.array(ipos, np.int64).T.copy()
-    box_child = np.array(children, np.int64).T.astype(np.int32).copy()
+    box_levels = np.concatenate([np.full(len(p), lv, np.int32)
+                                 for lv, p in enumerate(lv_parents)])
+    box_parent = np.concatenate(lv_parents).astype(np.int32)
+    box_ipos = box_ipos_all.T.copy()
+    child_index = np.concatenate(lv_cidx)
+    box_child = np.zeros((nchild, nboxes), np.int32)
+    nonroot = np.arange(1, nboxes)
+    box_child[child_index[1:], box_parent[1:]] = nonroot
     widths = root_extent / 2.0 ** box_levels
     box_centers = (box_ipos + 0.5) * widths[None, :] + lo[:, None]
 
-    # depth-first preorder rank
-    rank = np.empty(nboxes, np.int64)
-    stack = [0]
-    r = 0
-    while stack:
-        b = stack.pop()
-        rank[b] = r
-        r += 1
-        ch = [c for c in box_child[:, b] if c != 0]
-        stack.extend(reversed(ch))
-    # subtree end rank
+    # subtree sizes (bottom-up by level) and depth-first preorder ranks (top-down:
+    # a level's boxes are ordered by parent, then child index, so a child's rank is
+    # its parent's + 1 + the sizes of its earlier siblings)
     subtree = np.ones(nboxes, np.int64)
-    for b in range(nboxes - 1, 0, -1):
-        subtree[box_parent[b]] += subtree[b]
+    for lv in range(nlevels - 1, 0, -1):
+        b = np.arange(level_start[lv], level_start[lv + 1])
+        np.add.at(subtree, box_parent[b], subtree[b])
+    rank = np.zeros(nboxes, np.int64)
+    for lv in range(1, nlevels):
+        b = np.arange(level_start[lv], level_start[lv + 1])
+        if len(b) == 0:
+            continue
+        sz = subtree[b]
+        par = box_parent[b]
+        incl = np.cumsum(sz)
+        first = np.r_[True, par[1:] != par[:-1]]
+        grp_start = np.maximum.accumulate(np.where(first, np.arange(len(b)), 0))
+        before = incl - sz - (incl[grp_start] - sz[grp_start])
+        rank[b] = rank[par] + 1 + before
 
     def order_particles(sel_boxes):
         keys = rank[sel_boxes]
