@@ -1,8 +1,9 @@
 """QBX FMM geometry data: centers, tree, traversal, target association, CSR lists.
 
 Mirrors ``QBXFMMGeometryData`` (pytential/qbx/geometry.py:361-899) method by method.
-Everything here is built once and memoized (on the host; the target association
-on the GPU when one is present); the apply consumes it as device CSR index arrays.
+Everything here is built once and memoized (on the host; the target association and
+the tree's particle passes on the GPU when one is present, with identical results);
+the apply consumes it as device CSR index arrays.
 """
 
 from __future__ import annotations
@@ -16,7 +17,7 @@ from .discretization import Discretization
 from .target_assoc import (NO_QBX_NEEDED, associate_targets_to_qbx_centers,
                            associate_targets_to_qbx_centers_device)
 from .traversal import Traversal, build_traversal
-from .tree import Tree, build_tree
+from .tree import Tree, build_tree, build_tree_device
 
 
 def _cuda_available() -> bool:
@@ -152,9 +153,11 @@ class QBXFMMGeometryData:
             radii[:self.ncenters] = self.flat_expansion_radii()
         ttc = self.user_target_to_center()
         tw = (ttc == NO_QBX_NEEDED).astype(np.int64)
-        return build_tree(self.discr.quad_nodes, ti.targets, radii,
-                          np.ones(self.discr.nquad, np.int64), tw,
-                          self.max_leaf_refine_weight, self.stick_out_factor)
+        # the per-particle passes on the GPU when there is one (the same tree)
+        build = build_tree_device if _cuda_available() else build_tree
+        return build(self.discr.quad_nodes, ti.targets, radii,
+                     np.ones(self.discr.nquad, np.int64), tw,
+                     self.max_leaf_refine_weight, self.stick_out_factor)
 
     def tree(self) -> Tree:
         return self._tree

@@ -227,3 +227,168 @@ def build_tree(sources: np.ndarray, targets: np.ndarray,
         box_target_starts=ts, box_target_counts_nonchild=tnc,
         box_target_counts_cumul=tcu,
         stick_out_factor=stick_out_factor, box_target_stickout=stick)
+
+
+def build_tree_device(sources: np.ndarray, targets: np.ndarray,
+                      target_radii: np.ndarray | None,
+                      source_weights: np.ndarray, target_weights: np.ndarray,
+                      max_leaf_refine_weight: int, stick_out_factor: float = 0.5,
+                      max_levels: int = 40, device="cuda") -> Tree:
+    """:func:`build_tree` with the per-particle work on the GPU (tensors on ``device``):
+    the level passes (refine weights, child cells, stick-out fits, new box numbers)
+    and the final depth-first ordering.  The box table (thousands of boxes) is kept on
+    the host.  Every floating-point step is the same separately rounded IEEE operation
+    as in :func:`build_tree`, and sorts are stable, so the trees are identical."""
+    import torch
+
+    sources = np.ascontiguousarray(sources, dtype=np.float64)
+    targets = np.ascontiguousarray(targets, dtype=np.float64)
+    dim, ns = sources.shape
+    nt = targets.shape[1]
+    if target_radii is None:
+        target_radii = np.zeros(nt)
+    nchild = 2 ** dim
+
+    pts = np.concatenate([sources, targets], axis=1)
+    radii = np.concatenate([np.zeros(ns), np.asarray(target_radii, float)])
+    weights = np.concatenate([np.asarray(source_weights, np.int64),
+                              np.asarray(target_weights, np.int64)])
+    npart = ns + nt
+
+    bmin = pts.min(axis=1)
+    bmax = pts.max(axis=1)
+    ext = float((bmax - bmin).max())
+    ext = ext * (1 + 1e-6) + 1e-300
+    lo = bmin - 0.5 * 1e-6 * ext
+    root_extent = ext * (1 + 1e-6)
+
+    P = torch.from_numpy(pts).to(device)
+    R = torch.from_numpy(radii).to(device)
+    W = torch.from_numpy(weights).to(device)
+    LO = torch.from_numpy(lo).to(device)
+    bits = torch.tensor([1 << d for d in range(dim)], dtype=torch.int64, device=device)
+
+    lv_parents = [np.array([-1], np.int64)]
+    lv_ipos = [np.zeros((1, dim), np.int64)]
+    lv_cidx = [np.zeros(1, np.int64)]
+    nboxes = 1
+    pbox = torch.zeros(npart, dtype=torch.int64, device=device)
+    settled = torch.zeros(npart, dtype=torch.bool, device=device)
+    level_start = [0, 1]
+    box_ipos_all = lv_ipos[0]
+    IPOS = torch.from_numpy(box_ipos_all).to(device)
+
+    for level in range(max_levels):
+        b0, b1 = level_start[-2], level_start[-1]
+        if b1 == b0:
+            break
+        inlev = (pbox >= b0) & (pbox < b1)
+        movable = ~settled & inlev
+        wsum = torch.zeros(b1 - b0, dtype=torch.int64, device=device)
+        wsum.index_add_(0, pbox[inlev] - b0, W[inlev])
+        split = wsum > max_leaf_refine_weight
+        if not bool(split.any()):
+            level_start.pop()
+            level_start.append(b1)
+            break
+        cand = movable & split[torch.clamp(pbox - b0, 0, b1 - b0 - 1)]
+        idx = torch.nonzero(cand).squeeze(1)
+        w_child = root_extent / 2.0 ** (level + 1)
+        bpos = IPOS[pbox[idx]]                                     # (k, dim)
+        pk = P[:, idx].T
+        rel = (pk - LO) / w_child
+        cpos = torch.floor(rel).to(torch.int64)
+        cpos = torch.minimum(torch.maximum(cpos, 2 * bpos), 2 * bpos + 1)
+        ccent = (cpos.to(torch.float64) + 0.5) * w_child + LO
+        fits = ((pk - ccent).abs() + R[idx][:, None]
+                <= (0.5 + stick_out_factor) * w_child).all(dim=1)
+        fits |= R[idx] == 0
+        settled[idx[~fits]] = True
+        mv = idx[fits]
+        cpos = cpos[fits]
+        cidx = ((cpos - 2 * bpos[fits]) * bits[None, :]).sum(dim=1)
+        key = pbox[mv] * nchild + cidx
+        ukeys, inv = torch.unique(key, sorted=True, return_inverse=True)
+        uk = ukeys.cpu().numpy()
+        par = uk // nchild
+        ci = uk % nchild
+        off = (ci[:, None] >> np.arange(dim)[None, :]) & 1
+        newpos = 2 * box_ipos_all[par] + off
+        lv_parents.append(par)
+        lv_ipos.append(newpos)
+        lv_cidx.append(ci)
+        box_ipos_all = np.concatenate([box_ipos_all, newpos])
+        IPOS = torch.from_numpy(box_ipos_all).to(device)
+        pbox[mv] = nboxes + inv
+        nboxes += len(uk)
+        level_start.append(nboxes)
+    nlevels = len(level_start) - 1
+    while nlevels > 0 and level_start[nlevels] == level_start[nlevels - 1]:
+        nlevels -= 1
+    level_start = np.array(level_start[:nlevels + 1], dtype=np.int32)
+
+    box_levels = np.concatenate([np.full(len(p), lv, np.int32)
+                                 for lv, p in enumerate(lv_parents)])
+    box_parent = np.concatenate(lv_parents).astype(np.int32)
+    box_ipos = box_ipos_all.T.copy()
+    child_index = np.concatenate(lv_cidx)
+    box_child = np.zeros((nchild, nboxes), np.int32)
+    box_child[child_index[1:], box_parent[1:]] = np.arange(1, nboxes)
+    widths = root_extent / 2.0 ** box_levels
+    box_centers = (box_ipos + 0.5) * widths[None, :] + lo[:, None]
+
+    subtree = np.ones(nboxes, np.int64)
+    for lv in range(nlevels - 1, 0, -1):
+        b = np.arange(level_start[lv], level_start[lv + 1])
+        np.add.at(subtree, box_parent[b], subtree[b])
+    rank = np.zeros(nboxes, np.int64)
+    for lv in range(1, nlevels):
+        b = np.arange(level_start[lv], level_start[lv + 1])
+        if len(b) == 0:
+            continue
+        sz = subtree[b]
+        par = box_parent[b]
+        incl = np.cumsum(sz)
+        first = np.r_[True, par[1:] != par[:-1]]
+        grp_start = np.maximum.accumulate(np.where(first, np.arange(len(b)), 0))
+        before = incl - sz - (incl[grp_start] - sz[grp_start])
+        rank[b] = rank[par] + 1 + before
+
+    RANK = torch.from_numpy(rank).to(device)
+    RANK_END = torch.from_numpy(rank + subtree).to(device)
+
+    def order_particles(sel_boxes):
+        keys = RANK[sel_boxes]
+        k_sorted, perm = torch.sort(keys, stable=True)
+        starts = torch.searchsorted(k_sorted, RANK, side="left")
+        nonchild = torch.searchsorted(k_sorted, RANK, side="right") - starts
+        cumul = torch.searchsorted(k_sorted, RANK_END, side="left") - starts
+        return (perm.cpu().numpy(), starts.to(torch.int32).cpu().numpy(),
+                nonchild.to(torch.int32).cpu().numpy(), cumul.to(torch.int32).cpu().numpy())
+
+    sperm, ss, snc, scu = order_particles(pbox[:ns])
+    tperm, ts, tnc, tcu = order_particles(pbox[ns:])
+
+    # stick-out of nonchild targets (l-inf) beyond their box, per box
+    tb = pbox[ns:]
+    WID = torch.from_numpy(widths).to(device)
+    BC = torch.from_numpy(box_centers).to(device)
+    half = WID[tb] / 2
+    so = ((P[:, ns:] - BC[:, tb]).abs().max(dim=0).values + R[ns:]) - half
+    stick_d = torch.zeros(nboxes, dtype=torch.float64, device=device)
+    stick_d.scatter_reduce_(0, tb, torch.clamp(so, min=0.0), reduce="amax", include_self=True)
+    stick = stick_d.cpu().numpy()
+
+    return Tree(
+        dimensions=dim, nlevels=nlevels, nboxes=nboxes, root_extent=root_extent,
+        bounding_box=(bmin, bmax), box_centers=box_centers,
+        box_levels=box_levels, box_parent_ids=box_parent, box_child_ids=box_child,
+        box_ipos=box_ipos, level_start_box_nrs=level_start,
+        sources=sources[:, sperm].copy(), targets=targets[:, tperm].copy(),
+        target_radii=np.asarray(target_radii, float)[tperm].copy(),
+        user_source_ids=sperm.astype(np.int32), sorted_target_ids=tperm.astype(np.int32),
+        box_source_starts=ss, box_source_counts_nonchild=snc,
+        box_source_counts_cumul=scu,
+        box_target_starts=ts, box_target_counts_nonchild=tnc,
+        box_target_counts_cumul=tcu,
+        stick_out_factor=stick_out_factor, box_target_stickout=stick)
