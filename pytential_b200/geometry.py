@@ -1,9 +1,9 @@
 """QBX FMM geometry data: centers, tree, traversal, target association, CSR lists.
 
 Mirrors ``QBXFMMGeometryData`` (pytential/qbx/geometry.py:361-899) method by method.
-Everything here is built once and memoized (on the host; the target association and
-the tree's particle passes on the GPU when one is present, with identical results);
-the apply consumes it as device CSR index arrays.
+Everything here is built once and memoized: on the GPU when one is present (target
+association, the tree's particle passes, the interaction lists; identical results),
+else on the host; the apply consumes it as device CSR index arrays.
 """
 
 from __future__ import annotations
@@ -16,7 +16,7 @@ import numpy as np
 from .discretization import Discretization
 from .target_assoc import (NO_QBX_NEEDED, associate_targets_to_qbx_centers,
                            associate_targets_to_qbx_centers_device)
-from .traversal import Traversal, build_traversal
+from .traversal import Traversal, build_traversal, build_traversal_device
 from .tree import Tree, build_tree, build_tree_device
 
 
@@ -164,7 +164,8 @@ class QBXFMMGeometryData:
 
     @cached_property
     def _traversal(self) -> Traversal:
-        return build_traversal(self.tree(), self.well_sep_is_n_away)
+        build = build_traversal_device if _cuda_available() else build_traversal
+        return build(self.tree(), self.well_sep_is_n_away)
 
     def traversal(self) -> Traversal:
         return self._traversal
