@@ -154,6 +154,20 @@ int qbxfmm_laplace3d_qbx_matrix(int nsources, const double* sources, const doubl
                                 int ncenters, const double* centers, int qbx_order, double* K,
                                 void* stream);
 
+/* Dense QBX matrix of the 2D Helmholtz layer potential (the same reference routines as
+ * qbxfmm_laplace3d_qbx_matrix): K[t][s] (row-major complex128, ntargets x nsources,
+ * written) = potential at target t of a unit source s with charge weight
+ * charge_re + i charge_im and dipole weight dipole_re + i dipole_im, times i/4; QBX
+ * targets (target_center[t] >= 0) use the order qbx_order (<= 8) H2D expansion about
+ * that center, the others H_0 / H_1 themselves.  Sources, normals, targets and centers
+ * are structure-of-arrays [2][n] device pointers. */
+int qbxfmm_helmholtz2d_qbx_matrix(int nsources, const double* sources, const double* normals,
+                                  double k, double charge_re, double charge_im,
+                                  double dipole_re, double dipole_im, int ntargets,
+                                  const double* targets, const int32_t* target_center,
+                                  int ncenters, const double* centers, int qbx_order, void* K,
+                                  void* stream);
+
 /* Target-to-QBX-center association (replaces pytential's QBXTargetAssociator:
  * marking, pytential/qbx/target_assoc.py:544-633, and center finding, 243-363 and
  * 637-749, with the side requests of the table at 81-103).  Points are searched on

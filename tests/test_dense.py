@@ -1,6 +1,6 @@
-"""Dense QBX matrix of the 3D Laplace layer potential (the reference's direct QBX
-evaluation / matrix builder) on the GPU, against the QBX-FMM apply at a high FMM
-order, where the two differ only by the FMM's truncation."""
+"""Dense QBX matrices of the 3D Laplace and 2D Helmholtz layer potentials (the
+reference's direct QBX evaluation / matrix builder) on the GPU, against the QBX-FMM
+apply at a high FMM order, where the two differ only by the FMM's truncation."""
 
 import numpy as np
 import pytest
@@ -29,3 +29,21 @@ def test_dense_qbx_matrix_times_density_equals_apply(op):
     d2 = torch.randn_like(dens)
     assert np.abs((d2 @ M.T).cpu().numpy() - ap(d2).cpu().numpy()).max() / \
         np.abs((d2 @ M.T).cpu().numpy()).max() < 1e-9
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("op", ["S", "D", "BW"])
+def test_dense_helmholtz2d_matrix_times_density_equals_apply(op):
+    from pytential_b200.dense import helmholtz2d_qbx_matrix
+    from pytential_b200.workloads import helmholtz2d_starfish
+    wl = helmholtz2d_starfish(nelements=32, k=5.0, nrhs=2, nvolume=100, op=op, qbx_order=5,
+                              fmm_order=20)
+    geo = wl.geometry()
+    M = helmholtz2d_qbx_matrix(geo, wl.spec, wl.qbx_order)
+    assert M.shape == (wl.nuser_targets, wl.discr.ndofs) and M.dtype == torch.complex128
+    dens = torch.from_numpy(wl.density).cuda()
+    direct = (dens @ M.T).cpu().numpy()
+    ap = QBXApply(geo, wl.spec, wl.qbx_order, wl.fmm_order, nrhs=wl.nrhs)
+    fmm = ap(dens).cpu().numpy()
+    # on-surface (QBX) and volume (plain kernel) targets agree to the FMM's truncation
+    assert np.abs(direct - fmm).max() / np.abs(direct).max() < 1e-9
