@@ -168,6 +168,24 @@ int qbxfmm_helmholtz2d_qbx_matrix(int nsources, const double* sources, const dou
                                   int ncenters, const double* centers, int qbx_order, void* K,
                                   void* stream);
 
+/* The same for the 2D Laplace layer potential (structure-of-arrays [2][n]; kernel
+ * scaling -1/(2 pi), log|t - s| and its source-normal derivative; any qbx_order <= 32). */
+int qbxfmm_laplace2d_qbx_matrix(int nsources, const double* sources, const double* normals,
+                                double charge_coeff, double dipole_coeff, int ntargets,
+                                const double* targets, const int32_t* target_center,
+                                int ncenters, const double* centers, int qbx_order, double* K,
+                                void* stream);
+
+/* The same for the 3D Helmholtz layer potential (complex128 K, structure-of-arrays
+ * [3][n], e^{ik r} / (4 pi r); QBX targets through the spherical-wave series of order
+ * qbx_order <= 8 of the target-specific near field). */
+int qbxfmm_helmholtz3d_qbx_matrix(int nsources, const double* sources, const double* normals,
+                                  double k, double charge_re, double charge_im,
+                                  double dipole_re, double dipole_im, int ntargets,
+                                  const double* targets, const int32_t* target_center,
+                                  int ncenters, const double* centers, int qbx_order, void* K,
+                                  void* stream);
+
 /* Target-to-QBX-center association (replaces pytential's QBXTargetAssociator:
  * marking, pytential/qbx/target_assoc.py:544-633, and center finding, 243-363 and
  * 637-749, with the side requests of the table at 81-103).  Points are searched on

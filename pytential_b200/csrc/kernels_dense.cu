@@ -1,4 +1,4 @@
-// Dense QBX matrix of the 3D Laplace layer potential (the reference's direct QBX
+// Dense QBX matrices of the 3D and 2D Laplace layer potentials (the reference's direct QBX
 // evaluation, pytential/qbx/__init__.py:797-1068, and its matrix builder,
 // pytential/symbolic/matrix.py:450-523): entry (t, s) is the potential at target t of
 // a unit source at tree source s with the configured charge / dipole weights,
@@ -18,6 +18,7 @@
 
 #include "../../include/qbxfmm_api.h"
 #include "kernels.h"
+#include "laplace.cuh"
 
 namespace qbx {
 int set_last_error(int code, const std::string& msg);
@@ -112,8 +113,103 @@ k_lap3_qbx_matrix(int nsrc, const double* __restrict__ src, const double* __rest
   }
 }
 
+// 2D Laplace: with a = t - c, b = s - c (complex), w = a / b, the target-specific series
+//   S: log|b| - Re sum_{n=1..Q} w^n / n,   D: Re(nu / b sum_{n=0..Q} w^n)
+// for QBX targets (the series of nu.(s - t)/|s - t|^2), log|t - s| and
+// nu.(s - t)/|t - s|^2 for the others, times the kernel's scaling -1/(2 pi) (the 2D
+// Laplace apply's sign conventions).
+__global__ void __launch_bounds__(DS)
+k_lap2_qbx_matrix(int nsrc, const double* __restrict__ src, const double* __restrict__ nrm,
+                  double cq, double cd, int ntgt, const double* __restrict__ tgt,
+                  const int32_t* __restrict__ tcenter, int ncenters,
+                  const double* __restrict__ centers, int q, double* __restrict__ K)
+{
+  __shared__ double s_x[2][DTG], s_c[2][DTG];
+  __shared__ int s_qbx[DTG];
+  const int t0 = blockIdx.y * DTG;
+  for (int i = threadIdx.x; i < DTG; i += DS) {
+    int t = t0 + i;
+    int c = t < ntgt ? tcenter[t] : -1;
+    if (c >= ncenters) c = -1;
+    double x[2] = {0, 0}, cc[2] = {0, 0};
+    if (t < ntgt)
+      for (int d = 0; d < 2; ++d) x[d] = tgt[(size_t)d * ntgt + t];
+    if (c >= 0)
+      for (int d = 0; d < 2; ++d) cc[d] = centers[(size_t)d * ncenters + c];
+    s_x[0][i] = x[0];
+    s_x[1][i] = x[1];
+    s_c[0][i] = cc[0];
+    s_c[1][i] = cc[1];
+    s_qbx[i] = c >= 0;
+  }
+  __syncthreads();
+  const int s = blockIdx.x * DS + threadIdx.x;
+  if (s >= nsrc) return;
+  const double y[2] = {src[s], src[(size_t)nsrc + s]};
+  double nv[2] = {0, 0};
+  if (cd != 0.0) {
+    nv[0] = nrm[s];
+    nv[1] = nrm[(size_t)nsrc + s];
+  }
+  const double scale = -0.5 / M_PI;
+  const int tend = min(DTG, ntgt - t0);
+  for (int i = 0; i < tend; ++i) {
+    double v = 0.0;
+    if (s_qbx[i]) {
+      double2 bb = c2(y[0] - s_c[0][i], y[1] - s_c[1][i]);
+      if (bb.x != 0.0 || bb.y != 0.0) {
+        double2 binv = cinv(bb);
+        double2 w = cmul(c2(s_x[0][i] - s_c[0][i], s_x[1][i] - s_c[1][i]), binv);
+        double2 pw = w, sl = c2(0.0), sd = c2(1.0);
+        for (int n = 1; n <= q; ++n) {
+          sl = caxpy(1.0 / n, pw, sl);
+          sd = cadd(sd, pw);
+          pw = cmul(pw, w);
+        }
+        v = cq * (0.5 * log(bb.x * bb.x + bb.y * bb.y) - sl.x);
+        if (cd != 0.0) v += cd * cmul(cmul(c2(nv[0], nv[1]), binv), sd).x;
+      }
+    } else {
+      double dx = s_x[0][i] - y[0], dy = s_x[1][i] - y[1];
+      double r2 = dx * dx + dy * dy;
+      if (r2 > 0.0) {
+        v = 0.5 * cq * log(r2);
+        if (cd != 0.0) v -= cd * (nv[0] * dx + nv[1] * dy) / r2;
+      }
+    }
+    K[(size_t)(t0 + i) * nsrc + s] = scale * v;
+  }
+}
+
 }  // namespace
 }  // namespace qbx
+
+extern "C" int qbxfmm_laplace2d_qbx_matrix(int nsources, const double* sources,
+                                           const double* normals, double charge_coeff,
+                                           double dipole_coeff, int ntargets,
+                                           const double* targets, const int32_t* target_center,
+                                           int ncenters, const double* centers, int qbx_order,
+                                           double* K, void* stream)
+{
+  using namespace qbx;
+  if (nsources < 0 || ntargets < 0 || ncenters < 0)
+    return set_last_error(QBXFMM_ERR_ARG, "negative size");
+  if (qbx_order < 0 || qbx_order > 32)
+    return set_last_error(QBXFMM_ERR_UNSUPPORTED, "qbx_order must be in [0, 32]");
+  if (nsources == 0 || ntargets == 0) return QBXFMM_OK;
+  if (!sources || !targets || !target_center || !K || (ncenters > 0 && !centers) ||
+      (dipole_coeff != 0.0 && !normals))
+    return set_last_error(QBXFMM_ERR_ARG, "null argument");
+  dim3 grid((nsources + DS - 1) / DS, (ntargets + DTG - 1) / DTG);
+  if (grid.y > 65535) return set_last_error(QBXFMM_ERR_UNSUPPORTED, "too many targets");
+  k_lap2_qbx_matrix<<<grid, DS, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+      nsources, sources, normals, charge_coeff, dipole_coeff, ntargets, targets, target_center,
+      ncenters, centers, qbx_order, K);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess)
+    return set_last_error(QBXFMM_ERR_CUDA, std::string("laplace2d_qbx_matrix: ") + cudaGetErrorString(e));
+  return QBXFMM_OK;
+}
 
 extern "C" int qbxfmm_laplace3d_qbx_matrix(int nsources, const double* sources,
                                            const double* normals, double charge_coeff,

@@ -18,6 +18,9 @@
 // ladder relations of R and S.
 #include <cooperative_groups.h>
 
+#include <string>
+
+#include "../../include/qbxfmm_api.h"
 #include "laplace.cuh"
 #include "kernels.h"
 
@@ -2039,3 +2042,185 @@ cudaError_t h3_launch_trans_build(const qbxfmm_geometry& g, const TransCfg& tc, 
 // }}}
 
 }  // namespace qbx
+
+// {{{ dense QBX matrix
+
+namespace qbx {
+int set_last_error(int code, const std::string& msg);
+
+namespace {
+
+// Entry (t, s) of the 3D Helmholtz layer potential with charge / dipole weights:
+//   QBX targets (center c): the target-specific series of k_h3_tsqbx,
+//     ik sum_{n<=Q} (2n+1) j_n(k|a|) [cq h_n(k|b|) P_n(cos g) + cd (dipole terms)],
+//   other targets: cq e^{ikr}/r + cd nu.(t - s) e^{ikr} (1 - ikr) / r^3;
+// times 1/(4 pi).  CTA = 128 sources (thread = source) x 32 targets.
+constexpr int H3D_DS = 128;
+constexpr int H3D_DTG = 32;
+
+template <int Q>
+__global__ void __launch_bounds__(H3D_DS)
+k_h3_qbx_matrix(int nsrc, const double* __restrict__ src, const double* __restrict__ nrm,
+                HelmCoeffs hc, int ntgt, const double* __restrict__ tgt,
+                const int32_t* __restrict__ tcenter, int ncenters,
+                const double* __restrict__ centers, double2* __restrict__ K)
+{
+  __shared__ double s_x[3][H3D_DTG], s_c[3][H3D_DTG], s_ah[3][H3D_DTG];
+  __shared__ double s_jn[H3D_DTG][Q + 1];
+  __shared__ int s_qbx[H3D_DTG];
+  const int t0 = blockIdx.y * H3D_DTG;
+  if (threadIdx.x < H3D_DTG) {
+    const int i = threadIdx.x, t = t0 + i;
+    int c = t < ntgt ? tcenter[t] : -1;
+    if (c >= ncenters) c = -1;
+    double x[3] = {0, 0, 0}, cc[3] = {0, 0, 0};
+    if (t < ntgt)
+      for (int d = 0; d < 3; ++d) x[d] = tgt[(size_t)d * ntgt + t];
+    if (c >= 0)
+      for (int d = 0; d < 3; ++d) cc[d] = centers[(size_t)d * ncenters + c];
+    double a[3] = {x[0] - cc[0], x[1] - cc[1], x[2] - cc[2]};
+    double alen = sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+    double ainv = alen > 0.0 ? 1.0 / alen : 0.0;
+    for (int d = 0; d < 3; ++d) {
+      s_x[d][i] = x[d];
+      s_c[d][i] = cc[d];
+      s_ah[d][i] = a[d] * ainv;
+    }
+    s_qbx[i] = c >= 0;
+    double jv[H3_LMAX + 2];
+    h3_sph_j(Q, hc.k * alen, jv);
+#pragma unroll
+    for (int n = 0; n <= Q; ++n) s_jn[i][n] = (2.0 * n + 1.0) * jv[n];
+  }
+  __syncthreads();
+  const int s = blockIdx.x * H3D_DS + threadIdx.x;
+  if (s >= nsrc) return;
+  const double y[3] = {src[s], src[(size_t)nsrc + s], src[2 * (size_t)nsrc + s]};
+  const bool chg = hc.cq.x != 0.0 || hc.cq.y != 0.0;
+  const bool dip = hc.cd.x != 0.0 || hc.cd.y != 0.0;
+  double nv[3] = {0, 0, 0};
+  if (dip)
+    for (int d = 0; d < 3; ++d) nv[d] = nrm[(size_t)d * nsrc + s];
+  const double2 kq = c2(-hc.k * hc.cq.y, hc.k * hc.cq.x), kd = c2(-hc.k * hc.cd.y, hc.k * hc.cd.x);
+  const int tend = min(H3D_DTG, ntgt - t0);
+  for (int i = 0; i < tend; ++i) {
+    double2 v = c2(0.0);
+    if (s_qbx[i]) {
+      double b0 = y[0] - s_c[0][i], b1 = y[1] - s_c[1][i], b2 = y[2] - s_c[2][i];
+      double b2s = b0 * b0 + b1 * b1 + b2 * b2;
+      if (b2s != 0.0) {
+        double binv = rsqrt(b2s);
+        double blen = b2s * binv;
+        double cg = (s_ah[0][i] * b0 + s_ah[1][i] * b1 + s_ah[2][i] * b2) * binv;
+        double2 h[Q + 2];
+        h3_sph_h(Q + 1, hc.k * blen, h);
+        double xinv = 1.0 / (hc.k * blen);
+        double pm1 = 1.0, pm2 = 0.0, dm1 = 0.0;
+        double2 sS = c2(0.0), sA = c2(0.0), sB = c2(0.0);
+        const double* jn = s_jn[i];
+#pragma unroll
+        for (int n = 0; n <= Q; ++n) {
+          double pn, dn;
+          if (n == 0) {
+            pn = 1.0;
+            dn = 0.0;
+          } else if (n == 1) {
+            pn = cg;
+            dn = 1.0;
+          } else {
+            pn = ((2.0 * n - 1) * cg * pm1 - (n - 1.0) * pm2) * (1.0 / n);
+            dn = n * pm1 + cg * dm1;
+          }
+          if (chg) sS = caxpy(jn[n] * pn, h[n], sS);
+          if (dip) {
+            double2 hd = (n == 0) ? c2(-h[1].x, -h[1].y) : caxpy(-(n + 1.0) * xinv, h[n], h[n - 1]);
+            sA = caxpy(jn[n] * pn * hc.k, hd, sA);
+            sB = caxpy(jn[n] * dn, h[n], sB);
+          }
+          pm2 = pm1;
+          pm1 = pn;
+          dm1 = dn;
+        }
+        if (chg) v = cmul(kq, sS);
+        if (dip) {
+          double db = (nv[0] * b0 + nv[1] * b1 + nv[2] * b2) * binv;
+          double da = nv[0] * s_ah[0][i] + nv[1] * s_ah[1][i] + nv[2] * s_ah[2][i];
+          double2 vd = caxpy(db, sA, cscale((da - cg * db) * binv, sB));
+          v = cfma(kd, vd, v);
+        }
+      }
+    } else {
+      double dx = s_x[0][i] - y[0], dy = s_x[1][i] - y[1], dz = s_x[2][i] - y[2];
+      double r2 = dx * dx + dy * dy + dz * dz;
+      if (r2 > 0.0) {
+        double rinv = rsqrt(r2);
+        double rr = r2 * rinv;
+        double sn, cs;
+        sincos(hc.k * rr, &sn, &cs);
+        double2 e = c2(cs * rinv, sn * rinv);     // e^{ikr} / r
+        v = cmul(hc.cq, e);
+        if (dip) {
+          double f = (nv[0] * dx + nv[1] * dy + nv[2] * dz) * rinv * rinv;
+          v = cfma(hc.cd, cmul(e, c2(f, -f * hc.k * rr)), v);
+        }
+      }
+    }
+    K[(size_t)(t0 + i) * nsrc + s] = cscale(1.0 / FOUR_PI, v);
+  }
+}
+
+template <int Q>
+cudaError_t launch_h3_matrix(dim3 grid, cudaStream_t st, int nsrc, const double* src,
+                             const double* nrm, HelmCoeffs hc, int ntgt, const double* tgt,
+                             const int32_t* tc, int ncen, const double* cen, double2* K)
+{
+  k_h3_qbx_matrix<Q><<<grid, H3D_DS, 0, st>>>(nsrc, src, nrm, hc, ntgt, tgt, tc, ncen, cen, K);
+  return cudaGetLastError();
+}
+
+}  // namespace
+}  // namespace qbx
+
+extern "C" int qbxfmm_helmholtz3d_qbx_matrix(int nsources, const double* sources,
+                                             const double* normals, double k, double charge_re,
+                                             double charge_im, double dipole_re,
+                                             double dipole_im, int ntargets,
+                                             const double* targets, const int32_t* target_center,
+                                             int ncenters, const double* centers, int qbx_order,
+                                             void* K, void* stream)
+{
+  using namespace qbx;
+  if (nsources < 0 || ntargets < 0 || ncenters < 0)
+    return set_last_error(QBXFMM_ERR_ARG, "negative size");
+  if (qbx_order < 0 || qbx_order > 8)
+    return set_last_error(QBXFMM_ERR_UNSUPPORTED, "qbx_order must be in [0, 8]");
+  if (!(k > 0.0)) return set_last_error(QBXFMM_ERR_ARG, "wave number must be positive");
+  if (nsources == 0 || ntargets == 0) return QBXFMM_OK;
+  const bool dip = dipole_re != 0.0 || dipole_im != 0.0;
+  if (!sources || !targets || !target_center || !K || (ncenters > 0 && !centers) ||
+      (dip && !normals))
+    return set_last_error(QBXFMM_ERR_ARG, "null argument");
+  dim3 grid((nsources + H3D_DS - 1) / H3D_DS, (ntargets + H3D_DTG - 1) / H3D_DTG);
+  if (grid.y > 65535) return set_last_error(QBXFMM_ERR_UNSUPPORTED, "too many targets");
+  HelmCoeffs hc;
+  hc.k = k;
+  hc.cq = c2(charge_re, charge_im);
+  hc.cd = c2(dipole_re, dipole_im);
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  double2* Kd = static_cast<double2*>(K);
+  cudaError_t e;
+  switch (qbx_order) {
+#define QBX_H3M_CASE(QQ) \
+  case QQ: e = launch_h3_matrix<QQ>(grid, st, nsources, sources, normals, hc, ntargets, targets, \
+                                     target_center, ncenters, centers, Kd); break;
+    QBX_H3M_CASE(0) QBX_H3M_CASE(1) QBX_H3M_CASE(2) QBX_H3M_CASE(3) QBX_H3M_CASE(4)
+    QBX_H3M_CASE(5) QBX_H3M_CASE(6) QBX_H3M_CASE(7) QBX_H3M_CASE(8)
+#undef QBX_H3M_CASE
+    default: return set_last_error(QBXFMM_ERR_UNSUPPORTED, "qbx_order");
+  }
+  if (e != cudaSuccess)
+    return set_last_error(QBXFMM_ERR_CUDA, std::string("helmholtz3d_qbx_matrix: ") + cudaGetErrorString(e));
+  return QBXFMM_OK;
+}
+
+// }}}

@@ -1,10 +1,9 @@
-"""Dense QBX matrices of the 3D Laplace and 2D Helmholtz layer potentials on the GPU.
+"""Dense QBX matrices of the Laplace and Helmholtz layer potentials (2D and 3D) on the GPU.
 
 The reference builds this matrix with its direct QBX evaluation
 (``pytential/qbx/__init__.py:797-1068``, ``pytential/symbolic/matrix.py:450-523``):
 row t holds the potential at user target t of each stage-1 density DOF.  Here the
-kernel entries come from ``qbxfmm_laplace3d_qbx_matrix`` /
-``qbxfmm_helmholtz2d_qbx_matrix`` (every source through the QBX expansion of the
+kernel entries come from ``qbxfmm_{laplace,helmholtz}{2,3}d_qbx_matrix`` (every source through the QBX expansion of the
 target's center for QBX targets, the kernel itself for the others), in tree order;
 the rows are then taken in user-target order, the columns scattered to user source
 order and multiplied by the quadrature weights and the element-local upsampling
@@ -57,21 +56,53 @@ def _assemble(geo, scal, arr, d, K):
     return M.reshape(nuser, ne * npe)
 
 
-def laplace3d_qbx_matrix(geo: QBXFMMGeometryData, spec: SourceKernelSpec, qbx_order: int,
-                         device="cuda") -> torch.Tensor:
-    """(n_user_targets, ndofs) float64 matrix on ``device``."""
-    if not isinstance(spec.kernel, LaplaceKernel) or spec.kernel.dim != 3:
-        raise NotImplementedError("laplace3d_qbx_matrix is for 3D Laplace")
+def _real_matrix(name, geo, spec, qbx_order, device):
     dev = torch.device(device)
     scal, arr, d, (src, nrm, tgt, cen, tc) = _tree_inputs(geo, dev)
     nsrc, ntgt, ncen = scal["nsources"], scal["ntargets"], scal["ncenters"]
     K = torch.empty(ntgt, nsrc, dtype=torch.float64, device=dev)
     V = ctypes.c_void_p
-    native.check("qbxfmm_laplace3d_qbx_matrix", native.lib().qbxfmm_laplace3d_qbx_matrix(
+    native.check(name, getattr(native.lib(), name)(
         nsrc, V(src.data_ptr()), V(nrm.data_ptr()), float(spec.charge_coeff),
         float(spec.dipole_coeff), ntgt, V(tgt.data_ptr()), V(tc.data_ptr()), ncen,
         V(cen.data_ptr()), qbx_order, V(K.data_ptr()), _stream_handle()))
     return _assemble(geo, scal, arr, d, K)
+
+
+def _complex_matrix(name, geo, spec, qbx_order, device):
+    dev = torch.device(device)
+    scal, arr, d, (src, nrm, tgt, cen, tc) = _tree_inputs(geo, dev)
+    nsrc, ntgt, ncen = scal["nsources"], scal["ntargets"], scal["ncenters"]
+    K = torch.empty(ntgt, nsrc, dtype=torch.complex128, device=dev)
+    cq, cd = complex(spec.charge_coeff), complex(spec.dipole_coeff)
+    V = ctypes.c_void_p
+    native.check(name, getattr(native.lib(), name)(
+        nsrc, V(src.data_ptr()), V(nrm.data_ptr()), float(spec.kernel.k), cq.real, cq.imag,
+        cd.real, cd.imag, ntgt, V(tgt.data_ptr()), V(tc.data_ptr()), ncen, V(cen.data_ptr()),
+        qbx_order, V(K.data_ptr()), _stream_handle()))
+    return _assemble(geo, scal, arr, d, K)
+
+
+def qbx_matrix(geo: QBXFMMGeometryData, spec: SourceKernelSpec, qbx_order: int,
+               device="cuda") -> torch.Tensor:
+    """(n_user_targets, ndofs) matrix on ``device`` of the layer potential
+    ``charge_coeff S + dipole_coeff D`` with the kernel's scaling (float64 for
+    Laplace, complex128 for Helmholtz), for either kernel in 2D or 3D."""
+    dim = spec.kernel.dim
+    if isinstance(spec.kernel, LaplaceKernel):
+        return _real_matrix(f"qbxfmm_laplace{dim}d_qbx_matrix", geo, spec, qbx_order, device)
+    if isinstance(spec.kernel, HelmholtzKernel):
+        return _complex_matrix(f"qbxfmm_helmholtz{dim}d_qbx_matrix", geo, spec, qbx_order,
+                               device)
+    raise NotImplementedError(type(spec.kernel).__name__)
+
+
+def laplace3d_qbx_matrix(geo: QBXFMMGeometryData, spec: SourceKernelSpec, qbx_order: int,
+                         device="cuda") -> torch.Tensor:
+    """(n_user_targets, ndofs) float64 matrix on ``device``."""
+    if not isinstance(spec.kernel, LaplaceKernel) or spec.kernel.dim != 3:
+        raise NotImplementedError("laplace3d_qbx_matrix is for 3D Laplace")
+    return qbx_matrix(geo, spec, qbx_order, device)
 
 
 def helmholtz2d_qbx_matrix(geo: QBXFMMGeometryData, spec: SourceKernelSpec, qbx_order: int,
@@ -80,14 +111,4 @@ def helmholtz2d_qbx_matrix(geo: QBXFMMGeometryData, spec: SourceKernelSpec, qbx_
     potential ``charge_coeff S + dipole_coeff D`` (G = (i/4) H_0(k r))."""
     if not isinstance(spec.kernel, HelmholtzKernel) or spec.kernel.dim != 2:
         raise NotImplementedError("helmholtz2d_qbx_matrix is for 2D Helmholtz")
-    dev = torch.device(device)
-    scal, arr, d, (src, nrm, tgt, cen, tc) = _tree_inputs(geo, dev)
-    nsrc, ntgt, ncen = scal["nsources"], scal["ntargets"], scal["ncenters"]
-    K = torch.empty(ntgt, nsrc, dtype=torch.complex128, device=dev)
-    cq, cd = complex(spec.charge_coeff), complex(spec.dipole_coeff)
-    V = ctypes.c_void_p
-    native.check("qbxfmm_helmholtz2d_qbx_matrix", native.lib().qbxfmm_helmholtz2d_qbx_matrix(
-        nsrc, V(src.data_ptr()), V(nrm.data_ptr()), float(spec.kernel.k), cq.real, cq.imag,
-        cd.real, cd.imag, ntgt, V(tgt.data_ptr()), V(tc.data_ptr()), ncen, V(cen.data_ptr()),
-        qbx_order, V(K.data_ptr()), _stream_handle()))
-    return _assemble(geo, scal, arr, d, K)
+    return qbx_matrix(geo, spec, qbx_order, device)

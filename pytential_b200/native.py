@@ -55,6 +55,11 @@ _FREE = {
     "qbxfmm_helmholtz2d_qbx_matrix": [_int, _vp, _vp, ctypes.c_double, ctypes.c_double,
                                       ctypes.c_double, ctypes.c_double, ctypes.c_double, _int,
                                       _vp, _vp, _int, _vp, _int, _vp, _vp],
+    "qbxfmm_laplace2d_qbx_matrix": [_int, _vp, _vp, ctypes.c_double, ctypes.c_double, _int, _vp,
+                                    _vp, _int, _vp, _int, _vp, _vp],
+    "qbxfmm_helmholtz3d_qbx_matrix": [_int, _vp, _vp, ctypes.c_double, ctypes.c_double,
+                                      ctypes.c_double, ctypes.c_double, ctypes.c_double, _int,
+                                      _vp, _vp, _int, _vp, _int, _vp, _vp],
     "qbxfmm_cell_keys": [_int, _int, _vp, ctypes.POINTER(abi.QBXFMMCellGrid), _vp, _vp],
     "qbxfmm_associate_targets": [ctypes.POINTER(abi.QBXFMMAssocProblem), _vp, _vp],
 }
