@@ -195,32 +195,27 @@ def tsqbx_schedule(centers_by_target_box, qbx_center_to_target_box, center_to_ta
     chunks of at most ``chunk`` pairs that share a target box.
 
     Returns ``(chunk_target_box, chunk_start, chunk_count, targets, centers)``."""
-    cbt = np.asarray(centers_by_target_box)
-    c2tb = np.asarray(qbx_center_to_target_box)
-    st = np.asarray(center_to_targets_starts)
+    cbt = np.asarray(centers_by_target_box, np.int64)
+    c2tb = np.asarray(qbx_center_to_target_box, np.int64)
+    st = np.asarray(center_to_targets_starts, np.int64)
     lists = np.asarray(center_to_targets_lists)
-    tg, ct, tb = [], [], []
-    for c in cbt:
-        for it in range(st[c], st[c + 1]):
-            tg.append(lists[it])
-            ct.append(c)
-            tb.append(c2tb[c])
     z = np.zeros(0, np.int32)
-    if not tg:
+    counts = st[cbt + 1] - st[cbt] if len(cbt) else np.zeros(0, np.int64)
+    n = int(counts.sum())
+    if n == 0:
         return z, z, z, z, z
-    tb = np.array(tb)
-    ch_tb, ch_start, ch_count = [], [], []
-    i = 0
-    while i < len(tb):
-        j = i
-        while j < len(tb) and tb[j] == tb[i] and j - i < chunk:
-            j += 1
-        ch_tb.append(tb[i])
-        ch_start.append(i)
-        ch_count.append(j - i)
-        i = j
-    return (np.array(ch_tb, np.int32), np.array(ch_start, np.int32),
-            np.array(ch_count, np.int32), np.array(tg, np.int32), np.array(ct, np.int32))
+    # the targets of each center in order, centers in the order of centers_by_target_box
+    first = np.cumsum(counts) - counts
+    ct = np.repeat(cbt, counts)
+    tg = lists[np.repeat(st[cbt], counts) + np.arange(n) - np.repeat(first, counts)]
+    tb = c2tb[ct]
+    # runs of one target box, cut every `chunk` pairs
+    i = np.arange(n)
+    run_start = np.maximum.accumulate(np.where(np.r_[True, tb[1:] != tb[:-1]], i, 0))
+    starts = np.nonzero((i - run_start) % chunk == 0)[0]
+    ch_count = np.diff(np.r_[starts, n])
+    return (tb[starts].astype(np.int32), starts.astype(np.int32), ch_count.astype(np.int32),
+            tg.astype(np.int32), ct.astype(np.int32))
 
 
 def translation_classes(tree, trav, per_level: bool = False):
@@ -268,17 +263,13 @@ def translation_classes(tree, trav, per_level: bool = False):
     child = np.asarray(tree.box_child_ids)
     has_src = tree.box_source_counts_cumul > 0
     spb = np.asarray(trav.source_parent_boxes, np.int64)
-    m_src, m_grp, m_par = [], [], []
-    for i, b in enumerate(spb):
-        for ci in range(nch):
-            c = child[ci, b]
-            if c != 0 and has_src[c]:
-                m_src.append(c)
-                m_grp.append(tree.box_levels[b] * nch + ci)
-                m_par.append(i)
-    m_src = np.array(m_src, np.int64)
-    m_grp = np.array(m_grp, np.int64)
-    m_par = np.array(m_par, np.int64)
+    # (parent, child position) pairs in parent order, then child position
+    cs = child[:, spb].T.astype(np.int64)                     # (nparents, nch)
+    ok = (cs != 0) & has_src[cs]
+    m_par, m_ci = np.nonzero(ok)
+    m_src = cs[m_par, m_ci]
+    m_grp = np.asarray(tree.box_levels, np.int64)[spb[m_par]] * nch + m_ci
+    m_par = m_par.astype(np.int64)
     o = np.lexsort((m_src, m_grp))
     out["m2m_npairs"] = len(o)
     out["m2m_group_starts"] = np.searchsorted(m_grp[o], np.arange(nlev * nch + 1)).astype(np.int32)
@@ -290,18 +281,16 @@ def translation_classes(tree, trav, per_level: bool = False):
     out["m2m_par_pair_starts"] = np.searchsorted(m_par[o2], np.arange(len(spb) + 1)).astype(np.int32)
     out["m2m_par_pairs"] = pos[o2].astype(np.int32)
     # L2L
-    l_src, l_dst, l_grp = [], [], []
-    for b in ttp:
-        par = tree.box_parent_ids[b]
-        if par < 0:
-            continue
-        ci = int(np.where(child[:, par] == b)[0][0])
-        l_src.append(par)
-        l_dst.append(b)
-        l_grp.append(tree.box_levels[b] * nch + ci)
-    l_src = np.array(l_src, np.int64)
-    l_dst = np.array(l_dst, np.int64)
-    l_grp = np.array(l_grp, np.int64)
+    pars = np.asarray(tree.box_parent_ids, np.int64)[ttp]
+    keep = pars >= 0
+    l_dst = ttp[keep]
+    l_src = pars[keep]
+    # child position of each box within its parent
+    cpos = np.zeros(tree.nboxes, np.int64)
+    for ci in range(nch):
+        cb = child[ci]
+        cpos[cb[cb != 0]] = ci
+    l_grp = np.asarray(tree.box_levels, np.int64)[l_dst] * nch + cpos[l_dst]
     o = np.lexsort((l_dst, l_grp))
     out["l2l_npairs"] = len(o)
     out["l2l_group_starts"] = np.searchsorted(l_grp[o], np.arange(nlev * nch + 1)).astype(np.int32)
