@@ -141,6 +141,13 @@ int qbxfmm_apply_noalloc(const qbxfmm_plan* plan, const qbxfmm_upsample* up,
 int qbxfmm_laplace3d_grad_direct(int nsources, const double* sources, const double* charges,
                                  int ntargets, const double* targets, double* grad, void* stream);
 
+/* The same gradient computed in FP32 arithmetic (positions relative to a per-block
+ * origin, FP32 sums per tile of 256 sources added into FP64), for the mixed-precision
+ * adjoint; relative error about 1e-6 for targets well away from the sources. */
+int qbxfmm_laplace3d_grad_direct_f32(int nsources, const double* sources,
+                                     const double* charges, int ntargets,
+                                     const double* targets, double* grad, void* stream);
+
 /* Dense QBX matrix of the 3D Laplace layer potential with charge / dipole weights
  * (replaces the reference's direct QBX evaluation and matrix builder,
  * pytential/qbx/__init__.py:797-1068 and pytential/symbolic/matrix.py:450-523):

@@ -55,6 +55,7 @@ class FarFieldSingleLayer:
         if discr.ambient_dim != 3:
             raise NotImplementedError("the adjoint is built for 3D Laplace")
         self.discr = discr
+        self.precision = precision
         self.targets = np.ascontiguousarray(targets, dtype=np.float64)
         self.device = torch.device(device)
         spec = SourceKernelSpec(LaplaceKernel(3), charge_coeff=1.0)
@@ -101,7 +102,10 @@ class FarFieldSingleLayer:
         q = self.strengths(sigma).contiguous()
         grad = torch.empty(3, self.ntargets, dtype=torch.float64, device=self.device)
         st = ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
-        native.check("qbxfmm_laplace3d_grad_direct", native.lib().qbxfmm_laplace3d_grad_direct(
+        # the mixed-precision operator sums the gradient in FP32 arithmetic
+        name = ("qbxfmm_laplace3d_grad_direct" if self.precision == PRECISION_FP64
+                else "qbxfmm_laplace3d_grad_direct_f32")
+        native.check(name, getattr(native.lib(), name)(
             q.numel(), ctypes.c_void_p(self.quad_nodes.data_ptr()), ctypes.c_void_p(q.data_ptr()),
             self.ntargets, ctypes.c_void_p(self.targets_dev.data_ptr()),
             ctypes.c_void_p(grad.data_ptr()), st))

@@ -50,6 +50,7 @@ _STAGES = {
 # entries that take no plan
 _FREE = {
     "qbxfmm_laplace3d_grad_direct": [_int, _vp, _vp, _int, _vp, _vp, _vp],
+    "qbxfmm_laplace3d_grad_direct_f32": [_int, _vp, _vp, _int, _vp, _vp, _vp],
     "qbxfmm_laplace3d_qbx_matrix": [_int, _vp, _vp, ctypes.c_double, ctypes.c_double, _int, _vp,
                                     _vp, _int, _vp, _int, _vp, _vp],
     "qbxfmm_helmholtz2d_qbx_matrix": [_int, _vp, _vp, ctypes.c_double, ctypes.c_double,

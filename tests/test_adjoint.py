@@ -97,3 +97,16 @@ def test_mixed_adjoint_rechecked_in_fp64(small):
     a64 = op.adjoint(r).cpu().numpy()
     a32 = opm.adjoint(r).cpu().numpy()
     assert 0 < relerr(a32, a64) < 1e-5
+
+
+def test_mixed_target_gradient_rechecked_in_fp64(small):
+    """The FP32 direct target gradient of the mixed operator against the FP64 one."""
+    from pytential_b200.adjoint import FarFieldSingleLayer
+    from pytential_b200.fmm import PRECISION_MIXED
+    w, op = small
+    opm = FarFieldSingleLayer(w.discr, w.targets, w.qbx_order, w.fmm_order,
+                              precision=PRECISION_MIXED)
+    sig = torch.from_numpy(w.sigma).cuda()
+    g64 = op.target_gradient(sig).cpu().numpy()
+    g32 = opm.target_gradient(sig).cpu().numpy()
+    assert 0 < relerr(g32, g64) < 1e-5
