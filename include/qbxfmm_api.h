@@ -129,9 +129,17 @@ int qbxfmm_apply_host(const qbxfmm_plan* plan, const qbxfmm_upsample* up,
  * device resolves that array's address and should come before any stream capture;
  * calls that overlap on the GPU share the array and race; problems that need more
  * scratch are rejected with QBXFMM_ERR_ARG before any launch.  Uses the per-pair
- * translation kernels. */
+ * translation kernels, so it serves 2D and 3D Laplace and 2D Helmholtz plans; 3D
+ * Helmholtz plans (whose rotation and translation tables are a caller-owned buffer)
+ * are rejected with QBXFMM_ERR_ARG before any launch.  The plan's device must be the
+ * current device. */
 int qbxfmm_apply_noalloc(const qbxfmm_plan* plan, const qbxfmm_upsample* up,
                          const void* density, void* out, void* stream);
+
+/* The error word of the last qbxfmm_apply_noalloc on the current device (0: no kernel
+ * met an out-of-range list entry), copied to *host_out after `stream` has finished
+ * (synchronizes the stream).  Allocates nothing. */
+int qbxfmm_noalloc_error_word(int32_t* host_out, void* stream);
 
 /* Gradient of the 3D Laplace single-layer potential, by direct summation, at targets
  * far from the sources: grad[d][t] = -1/(4 pi) sum_s charges[s] (x_t - y_s)_d / |x_t - y_s|^3

@@ -9,8 +9,8 @@ SRC="$REF/pytential/qbx/target_specific"
 HERE="$(cd "$(dirname "$0")" && pwd)"
 OUT="$HERE/_ref"
 if [ ! -f "$SRC/impl.pyx" ]; then
-  echo "reference sources not found at $SRC" >&2
-  exit 1
+  echo "reference sources not found at $SRC: oracle/_ref not built (set PYTENTIAL_REFERENCE)" >&2
+  exit 0
 fi
 mkdir -p "$OUT/build"
 PY=${PYTHON:-python3}

@@ -33,6 +33,7 @@ struct qbxfmm_plan {
   bool trans_ok;                           // matrix form of M2L / M2M / L2L available
   TransHost th;
   TransCfg tc;
+  int device = -1;                         // CUDA device current at plan creation
   bool h3;                                 // 3D Helmholtz
   bool mixed;                              // FP32 far field (3D Laplace)
   bool tf32_ok;                            // split-TF32 translation matrices in use
@@ -326,6 +327,10 @@ int plan_base_workspace_sizes(const qbxfmm_plan* p, size_t* sizes6)
 
 int set_last_error(int code, const std::string& msg) { return fail(code, msg); }
 
+int plan_device(const qbxfmm_plan* p) { return p ? p->device : -1; }
+
+bool plan_needs_translation_tables(const qbxfmm_plan* p) { return p && p->h3; }
+
 }  // namespace qbx
 
 extern "C" {
@@ -389,6 +394,7 @@ int qbxfmm_plan_create(const qbxfmm_kernel* kernel, const qbxfmm_geometry* geome
   if (e == cudaSuccess)
     e = cudaMemcpy(p->lvl_ttp.data(), g.level_start_ttp_box_nrs, sizeof(int32_t) * (g.nlevels + 1),
                    cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaGetDevice(&p->device);
   p->h3 = p->helm && k.dim == 3;
   p->mixed = k.precision == 1;
   if (k.dim == 3)
@@ -807,14 +813,9 @@ int qbxfmm_workspace_sizes(const qbxfmm_plan* p, size_t* sizes6 /* 8 entries */)
   if (int rc = check_plan(p)) return rc;
   if (!sizes6) return fail(QBXFMM_ERR_ARG, "null sizes");
   const qbxfmm_geometry& g = p->geo;
-  size_t nr = (size_t)p->kern.nrhs;
-  size_t scal = (p->kern.family == QBXFMM_LAPLACE) ? sizeof(double) : 2 * sizeof(double);
-  sizes6[0] = nr * g.nsources * scal;
-  sizes6[1] = (size_t)g.nboxes * nr * p->ncf * 2 * sizeof(double);
-  sizes6[2] = sizes6[1];
-  sizes6[3] = (size_t)g.ncenters * nr * p->ncq * 2 * sizeof(double);
-  sizes6[4] = nr * (size_t)(g.nfiltered_targets > 0 ? g.nfiltered_targets : 1) * scal;
-  sizes6[5] = nr * (size_t)g.ntargets * scal;
+  // entries 0-5 come from the one formula the allocation-free apply lays out its
+  // array with
+  if (int rc = qbx::plan_base_workspace_sizes(p, sizes6)) return rc;
   if (p->trans_ok) {
     int npairs = std::max(p->th.m2l_npairs, g.m2m_npairs);
     size_t o[6];

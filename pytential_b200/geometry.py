@@ -3,7 +3,8 @@
 Mirrors ``QBXFMMGeometryData`` (pytential/qbx/geometry.py:361-899) method by method.
 Everything here is built once and memoized: on the GPU when one is present (target
 association, the tree's particle passes, the interaction lists; identical results),
-else on the host; the apply consumes it as device CSR index arrays.
+else on the host (``builders="host"`` forces the host builders, which load no CUDA
+code); the apply consumes it as device CSR index arrays.
 """
 
 from __future__ import annotations
@@ -64,7 +65,11 @@ class QBXFMMGeometryData:
                  expansion_stick_out_factor: float = 0.5,
                  well_sep_is_n_away: int = 2,
                  target_association_tolerance: float = 1e3 * np.finfo(float).eps,
-                 expansions_in_tree_have_extent: bool = True):
+                 expansions_in_tree_have_extent: bool = True,
+                 builders: str = "auto"):
+        if builders not in ("auto", "host", "device"):
+            raise ValueError(f"builders must be 'auto', 'host' or 'device', not {builders!r}")
+        self.builders = builders
         self.discr = discr
         self.target_discrs_and_qbx_sides = [
             (np.ascontiguousarray(p, dtype=np.float64), int(s))
@@ -80,6 +85,11 @@ class QBXFMMGeometryData:
     @property
     def ambient_dim(self):
         return self.discr.ambient_dim
+
+    def _on_device(self) -> bool:
+        if self.builders == "auto":
+            return _cuda_available()
+        return self.builders == "device"
 
     # {{{ centers / radii
 
@@ -130,7 +140,7 @@ class QBXFMMGeometryData:
         tunnel = 0.5 * self.discr.quad_expansion_radii()
         # on a CUDA machine the association runs on the GPU (the same result bit for
         # bit); without one, on the host
-        assoc = (associate_targets_to_qbx_centers_device if _cuda_available()
+        assoc = (associate_targets_to_qbx_centers_device if self._on_device()
                  else associate_targets_to_qbx_centers)
         ttc = assoc(
             user, sides, self.discr.quad_nodes, tunnel,
@@ -154,7 +164,7 @@ class QBXFMMGeometryData:
         ttc = self.user_target_to_center()
         tw = (ttc == NO_QBX_NEEDED).astype(np.int64)
         # the per-particle passes on the GPU when there is one (the same tree)
-        build = build_tree_device if _cuda_available() else build_tree
+        build = build_tree_device if self._on_device() else build_tree
         return build(self.discr.quad_nodes, ti.targets, radii,
                      np.ones(self.discr.nquad, np.int64), tw,
                      self.max_leaf_refine_weight, self.stick_out_factor)
@@ -164,7 +174,7 @@ class QBXFMMGeometryData:
 
     @cached_property
     def _traversal(self) -> Traversal:
-        build = build_traversal_device if _cuda_available() else build_traversal
+        build = build_traversal_device if self._on_device() else build_traversal
         return build(self.tree(), self.well_sep_is_n_away)
 
     def traversal(self) -> Traversal:

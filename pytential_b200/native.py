@@ -63,6 +63,7 @@ _FREE = {
                                       _vp, _vp, _int, _vp, _int, _vp, _vp],
     "qbxfmm_cell_keys": [_int, _int, _vp, ctypes.POINTER(abi.QBXFMMCellGrid), _vp, _vp],
     "qbxfmm_associate_targets": [ctypes.POINTER(abi.QBXFMMAssocProblem), _vp, _vp],
+    "qbxfmm_noalloc_error_word": [_pi, _vp],
 }
 
 EXPORTED_SYMBOLS = ["qbxfmm_version", "qbxfmm_last_error", "qbxfmm_plan_create",

@@ -42,9 +42,11 @@ class Workload:
     def nrhs(self):
         return self.density.shape[0]
 
-    def geometry(self) -> QBXFMMGeometryData:
+    def geometry(self, builders: str = "auto") -> QBXFMMGeometryData:
+        """The geometry data (memoized); ``builders="host"`` builds it with the host
+        builders only (no CUDA code is loaded)."""
         if self._geo is None:
-            self._geo = QBXFMMGeometryData(self.discr, self.targets)
+            self._geo = QBXFMMGeometryData(self.discr, self.targets, builders=builders)
         return self._geo
 
     @property

@@ -29,6 +29,13 @@ def noalloc(ap, density, out):
                 ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
 
 
+def noalloc_error_word():
+    w = ctypes.c_int32(-1)
+    native.call("qbxfmm_noalloc_error_word", ctypes.byref(w),
+                ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+    return w.value
+
+
 @pytest.mark.parametrize("name", ["3d-D-small", "2d-S", "h2d-D-small"])
 def test_noalloc_matches_apply_twice(name):
     wl = workload(name)
@@ -42,6 +49,7 @@ def test_noalloc_matches_apply_twice(name):
         noalloc(ap, dens, out)
         torch.cuda.synchronize()
         assert relerr(out.cpu().numpy(), ref) < tol
+        assert noalloc_error_word() == 0
 
 
 def test_noalloc_rejects_oversized_problem():
@@ -56,3 +64,19 @@ def test_noalloc_rejects_oversized_problem():
                     ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
     assert ei.value.code == abi.QBXFMM_ERR_ARG
     assert "maximum" in str(ei.value)
+
+
+def test_noalloc_rejects_helmholtz3d_plan():
+    """3D Helmholtz needs its translation tables in a caller-owned buffer: the entry
+    point refuses the plan before launching anything and leaves the output alone."""
+    wl = workload("h3d-D-small")
+    ap = QBXApply(wl.geometry(), wl.spec, wl.qbx_order, wl.fmm_order, nrhs=wl.nrhs)
+    dens = torch.from_numpy(wl.density).cuda()
+    out = ap.new_output()
+    out.fill_(7.0)
+    with pytest.raises(native.QBXFMMError) as ei:
+        noalloc(ap, dens, out)
+    assert ei.value.code == abi.QBXFMM_ERR_ARG
+    assert "3D Helmholtz" in str(ei.value)
+    torch.cuda.synchronize()
+    assert bool((out == 7.0).all())
