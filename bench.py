@@ -1,23 +1,29 @@
 #!/usr/bin/env python
-"""Benchmark: QBX-FMM node-applies/s on the 3D Laplace double-layer ellipsoid apply.
+"""Benchmark: QBX-FMM node-applies/s on the 3D Helmholtz combined-field apply.
 
-Workload: ellipsoid (1, 1.5, 2) from an icosphere refined 3 times (1280 triangles),
-15 nodes per triangle (19200 nodes) upsampled to 45 (57600 sources), double
-layer, exterior limit on the surface plus 2000 targets in the shell
-2.5 <= r <= 3.5, qbx_order 3, fmm_order 10, float64.  node-applies = user
-targets x densities.  One step = one apply (upsample, weight, reorder, every FMM
-stage, assembly) with the density resident in HBM; the L2 cache (126 MB) is
-flushed between steps by writing a 256 MB buffer outside the per-step events.
+Workload (headline): 3D Helmholtz combined field D - i k S, k = 10, on the ellipsoid
+(1, 1.5, 2) from an icosphere refined 5 times (20480 triangles), 15 nodes per triangle
+(307200 nodes) upsampled to 45 (921600 sources), exterior limit on the surface,
+16 plane-wave densities, qbx_order 5, fmm_order 15, complex128 (the plain FP64 form).
+node-applies = user targets x densities.  One step = one apply of all 16 densities
+(upsample, weight, reorder, every FMM stage, assembly) with the densities resident in
+HBM; the L2 cache (126 MB) is flushed between steps by writing a 256 MB buffer outside
+the per-step events.  Beside it: the same step in the mixed-precision form, the 3D
+Laplace double-layer apply (icosphere-3, 57600 sources, q 3 / p 10) and the CPU
+checker on a bounded sample.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
-N > 1 (launched by torch.distributed.run): every rank applies its own density on
-its own GPU (weak scaling, no data-path collective); time is the max over ranks.
+N > 1 (launched by torch.distributed.run): the 16 densities of the one job are split
+over the ranks (each rank applies its share on its own GPU, no exchange inside the
+apply) and the results are all-gathered in density order inside the timed step
+(NCCL); total work is fixed (strong scaling), time is the max over ranks.
 """
 
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import os
 import statistics
@@ -32,38 +38,50 @@ sys.path.insert(0, ROOT)
 
 METRIC = "QBX-FMM node-applies/s at stated rel. err"
 UNIT = "node-applies/s"
-WORKLOAD = ("3D Laplace double-layer QBX apply, ellipsoid (1,1.5,2), icosphere-3 "
-            "(1280 tri), 19200 nodes -> 57600 sources, 19200 surface + 2000 shell "
-            "targets, qbx_order 3, fmm_order 10, FP64")
+
+H3 = dict(nrefine=5, k=10.0, nrhs=16, qbx_order=5, fmm_order=15, op="CF")
+H3_SAMPLE = dict(nrefine=2, nrhs=1)   # CPU-checker sample: same operator and orders
+L3 = dict(nrefine=3, qbx_order=3, fmm_order=10, op="D")
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--nrefine", type=int, default=3)
+    ap.add_argument("--nrefine", type=int, default=H3["nrefine"],
+                    help="icosphere refinements of the headline surface (5: full size)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-helmholtz", action="store_true",
-                    help="skip the 3D Helmholtz measurement reported beside the headline")
+    ap.add_argument("--no-laplace", action="store_true",
+                    help="skip the 3D Laplace measurement reported beside the headline")
     return ap.parse_args()
 
 
-def make_workload(nrefine, seed):
-    from pytential_b200.workloads import laplace3d_ellipsoid
-    return laplace3d_ellipsoid(nrefine=nrefine, op="D", seed=seed)
+def h3_counts(nrefine):
+    ntri = 20 * 4 ** nrefine
+    return {"triangles": ntri, "nodes": 15 * ntri, "sources": 45 * ntri,
+            "user_targets": 15 * ntri}
 
 
-def config_dict(wl, args, extra=None):
-    d = {"workload": WORKLOAD if args.nrefine == 3 else f"{wl.name} (reduced)",
-         "nodes": wl.discr.ndofs, "sources": wl.discr.nquad,
-         "user_targets": wl.nuser_targets, "nrhs": wl.nrhs,
-         "qbx_order": wl.qbx_order, "fmm_order": wl.fmm_order,
-         "l2": "flushed between steps (256 MB write)", "parallelism": f"replicas x{args.gpus}"}
-    if extra:
-        d.update(extra)
-    return d
+def config_dict(args, world):
+    c = h3_counts(args.nrefine)
+    name = ("3D Helmholtz combined field D - ik S, k 10, ellipsoid (1,1.5,2), "
+            f"icosphere-{args.nrefine} ({c['triangles']} tri), {c['nodes']} nodes -> "
+            f"{c['sources']} sources, 16 plane-wave densities, qbx_order 5, fmm_order 15")
+    if args.nrefine != H3["nrefine"]:
+        name += " (reduced)"
+    return {"workload": name, "nodes": c["nodes"], "sources": c["sources"],
+            "user_targets": c["user_targets"], "nrhs": H3["nrhs"], "k": H3["k"],
+            "qbx_order": H3["qbx_order"], "fmm_order": H3["fmm_order"],
+            "l2": "flushed between steps (256 MB write)",
+            "parallelism": "single GPU" if world == 1 else f"densities sharded over {world} GPUs"}
+
+
+def h3_workload(nrefine, nrhs=H3["nrhs"], seed=0):
+    from pytential_b200.workloads import helmholtz3d_ellipsoid
+    return helmholtz3d_ellipsoid(nrefine=nrefine, k=H3["k"], nrhs=nrhs, seed=seed, op=H3["op"],
+                                 qbx_order=H3["qbx_order"], fmm_order=H3["fmm_order"])
 
 
 # {{{ clocks
@@ -90,6 +108,7 @@ class ClockSampler:
 
     def _nvml_handle(self):
         import pynvml
+        import torch
         pynvml.nvmlInit()
         try:
             uuid = str(torch.cuda.get_device_properties(self.index).uuid)
@@ -170,320 +189,46 @@ class ClockSampler:
 
 # }}}
 
+# {{{ helpers
 
-KERNEL_SYMBOLS = {
-    "target-specific near field (eval_target_specific_qbx_locals)": "k_tsqbx",
-    "M2QBXL (translate_box_multipoles_to_qbx_local)": "k_m2qbxl",
-    "P2L list 4 (form_locals)": "k_p2l",
-    "P2QBXL (form_global_qbx_locals)": "k_p2qbxl",
-}
+def _events(torch, n):
+    return [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+            for _ in range(n)]
 
 
-def ncu_traffic(label):
-    """DRAM bytes per launch of a kernel from the committed ncu capture summary
-    (``profiles/ncu_dram_bytes.json``), or None."""
-    try:
-        with open(os.path.join(os.path.dirname(os.path.abspath(__file__)),
-                               "profiles", "ncu_dram_bytes.json")) as f:
-            data = json.load(f)
-        return data["bytes_per_launch"].get(KERNEL_SYMBOLS.get(label, ""))
-    except (OSError, ValueError, KeyError):
-        return None
-
-
-def cpu_reference(wl, reps, threads):
-    """The CPU checker's full apply (float64, OpenMP) on the host cores."""
-    os.environ["OMP_NUM_THREADS"] = str(threads)
-    from oracle.oracle import Oracle
-    sp = wl.spec
-    o = Oracle(wl.geometry(), dim=3, qbx_order=wl.qbx_order, fmm_order=wl.fmm_order,
-               nrhs=wl.nrhs, charge_coeff=sp.charge_coeff, dipole_coeff=sp.dipole_coeff)
-    s = wl.tree_strengths()
-    o.apply(s)   # warm (page-in, thread pool)
-    times = []
-    out = None
-    for _ in range(reps):
-        t0 = time.perf_counter()
-        out = o.apply(s)
-        times.append(time.perf_counter() - t0)
-    return out, times
-
-
-def run_reference(args):
-    rank = int(os.environ.get("RANK", "0"))
-    if rank != 0:
-        return
-    threads = os.cpu_count() or 1
-    wl = make_workload(args.nrefine, seed=0)
-    _, times = cpu_reference(wl, max(args.steps, 1), threads)
-    t = statistics.mean(times)
-    value = wl.nuser_targets * wl.nrhs / t
-    line = {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
-        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 * t, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": config_dict(wl, args),
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": "full apply of the workload per step (C/OpenMP float64 "
-                                   "restatement; the reference's pyopencl/sumpy apply is "
-                                   "not installable here)"},
-        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-    }
-    print(json.dumps(line), flush=True)
-
-
-def run_b200(args):
-    import torch
-    import torch.distributed as dist
-
-    from pytential_b200 import costs
-    from pytential_b200.fmm import QBXApply
-
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    if world > 1:
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
-                                device_id=dev)
-
-    wl = make_workload(args.nrefine, seed=rank)
-    geo = wl.geometry()
-    # fastest verified configuration: translation-class matrices on the FP64 tensor
-    # cores and the target-specific near field (same truncation, tests/test_gpu_parity)
-    ap = QBXApply(geo, wl.spec, wl.qbx_order, wl.fmm_order, device=dev,
-                  target_specific_qbx=True)
-    dens = torch.from_numpy(wl.density).to(dev)
-    out = ap.new_output()
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
-    scal, arr = ap.dgeo.scalars, ap.dgeo.host_arrays
-    launches_per_step = costs.apply_launch_count(
-        scal, arr, matrices=ap.uses_translation_matrices, tsqbx=True)
-    pairs = costs.p2qbxl_pairs(arr, scal)
-    sp = wl.spec
-    fpp = costs.p2qbxl_flops_per_pair(3, wl.qbx_order, sp.charge_coeff != 0,
-                                      sp.dipole_coeff != 0)
-    node_applies = wl.nuser_targets * wl.nrhs
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    for _ in range(max(args.warmup, 3)):
-        ap.apply_into(dens, out)
-    torch.cuda.synchronize()
-
-    K = args.steps
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-          for _ in range(K)]
-    barrier()
-    torch.cuda.synchronize()
-    with ClockSampler(local) as clk:
-        for i in range(K):
-            flush.zero_()
-            ev[i][0].record()
-            ap.apply_into(dens, out)
-            ev[i][1].record()
-        torch.cuda.synchronize()
-    barrier()
-    step_ms = [a.elapsed_time(b) for a, b in ev]
-    t_local = sum(step_ms) / 1e3
-    t_all = torch.tensor([t_local], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t_all, op=dist.ReduceOp.MAX)
-    t_max = float(t_all.item())
-    value = world * node_applies * K / t_max
-
-    # the main kernels timed alone on the same stream (flushed L2); the dominant one
-    # gives the roofline entry
-    import ctypes
-    st = torch.cuda.current_stream()
-    ws = ap.ws
-    V = ctypes.c_void_p
-    S = V(st.cuda_stream)
-    ch, dp = sp.charge_coeff != 0, sp.dipole_coeff != 0
-    kernels = {
-        "target-specific near field (eval_target_specific_qbx_locals)": (
-            lambda: ap.plan.call("qbxfmm_eval_target_specific_qbx_locals", V(ws.strengths),
-                                 V(ws.pot_tree), ws.error_word, S),
-            costs.tsqbx_pairs(arr, scal) * costs.tsqbx_flops_per_pair(3, wl.qbx_order, ch, dp)),
-        "M2QBXL (translate_box_multipoles_to_qbx_local)": (
-            lambda: ap.plan.call("qbxfmm_translate_box_multipoles_to_qbx_local", V(ws.mpoles),
-                                 V(ws.qbx_exps), ws.error_word, S),
-            costs.m2qbxl_pairs(arr, scal) * costs.m2qbxl_flops_per_pair(wl.fmm_order, wl.qbx_order)),
-        "P2L list 4 (form_locals)": (
-            lambda: ap.plan.call("qbxfmm_form_locals", V(ws.strengths), V(ws.locals),
-                                 ws.error_word, S),
-            costs.p2l_flops(arr, scal, wl.fmm_order, ch, dp)),
-        "P2QBXL (form_global_qbx_locals)": (
-            lambda: ap.plan.call("qbxfmm_form_global_qbx_locals", V(ws.strengths),
-                                 V(ws.qbx_exps), ws.error_word, S),
-            pairs * fpp),
-    }
-    ktimes = {}
-    for name, (fn, fl) in kernels.items():
-        kev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-               for _ in range(K)]
-        for i in range(K):
-            flush.zero_()
-            kev[i][0].record()
-            fn()
-            kev[i][1].record()
-        torch.cuda.synchronize()
-        ktimes[name] = (statistics.mean(a.elapsed_time(b) for a, b in kev), fl)
-    # P2QBXL is not part of this configuration's step (the target-specific kernel
-    # replaces it); it is timed for reference only
-    in_step = {k: v for k, v in ktimes.items() if not k.startswith("P2QBXL")}
-    dom = max(in_step, key=lambda k: in_step[k][0])
-    k_ms, k_flops = in_step[dom]
-    traffic = ncu_traffic(dom)
-    fp64_peak = measure_fp64_peak(torch, dev)
-
-    # end to end through the public host-buffer entry (H2D + apply + D2H + sync)
-    ap.alloc_host_buffers()
-    ap.h_in.copy_(torch.from_numpy(wl.density))
-    for _ in range(3):
-        ap.apply_host()
-    barrier()
-    t0 = time.perf_counter()
-    for _ in range(K):
-        ap.apply_host()
-    t_e2e = time.perf_counter() - t0
-    te = torch.tensor([t_e2e], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = world * node_applies * K / float(te.item())
-
-    res_gpu = ap.h_out.numpy().copy()
-    ap.check_error_word()
-
-    # the mixed-precision form (FP32 far field, split-TF32 translations, FP64 QBX near
-    # field) on the same workload, timed the same way
-    from pytential_b200.fmm import PRECISION_MIXED
-    apm = QBXApply(geo, wl.spec, wl.qbx_order, wl.fmm_order, device=dev,
-                   device_geometry=ap.dgeo, target_specific_qbx=True, precision=PRECISION_MIXED)
-    outm = apm.new_output()
-    for _ in range(max(args.warmup, 3)):
-        apm.apply_into(dens, outm)
-    barrier()
-    evm = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-           for _ in range(K)]
-    for i in range(K):
-        flush.zero_()
-        evm[i][0].record()
-        apm.apply_into(dens, outm)
-        evm[i][1].record()
-    torch.cuda.synchronize()
-    tm = torch.tensor([sum(a.elapsed_time(b) for a, b in evm) / 1e3], dtype=torch.float64,
-                      device=dev)
-    if world > 1:
-        dist.all_reduce(tm, op=dist.ReduceOp.MAX)
-    tm = float(tm.item())
-    res_mixed = outm.cpu().numpy()
-    apm.check_error_word()
-
-    line = None
-    if rank == 0:
-        line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
-            "warmup": max(args.warmup, 3), "ms_per_step": 1e3 * t_max / K,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64", "data": "synthetic (seeded analytic geometry and density)",
-            "config": config_dict(wl, args, {
-                "near_field": "target-specific (per target and list-1 source)",
-                "translations": "translation-class matrices, FP64 tensor cores"}),
-            "roofline": {
-                "kernel": dom, "bound": "fp64",
-                "achieved": k_flops / (k_ms * 1e-3) / 1e12,
-                "peak": fp64_peak, "unit": "TFLOP/s",
-                "frac": (k_flops / (k_ms * 1e-3) / 1e12) / fp64_peak,
-                "peak_source": "measured here: cuBLAS float64 GEMM 8192^3, best of 5",
-                "algorithmic_flops_per_launch": k_flops, "kernel_ms": k_ms,
-                "share_of_step": k_ms / (1e3 * t_max / K), "traffic": traffic,
-                "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum, one launch, "
-                                   "profiles/ncu_dram_bytes.json") if traffic else None,
-                "kernels_ms": {k: round(v[0], 4) for k, v in ktimes.items()},
-                "kernels_tflops": {k: round(v[1] / (v[0] * 1e-3) / 1e12, 3)
-                                   for k, v in ktimes.items()}},
-            "e2e": {"value": e2e_value, "unit": UNIT,
-                    "h2d_bytes_per_step": ap.h2d_bytes, "d2h_bytes_per_step": ap.d2h_bytes},
-            "gpu_launches": launches_per_step * K,
-            "clocks": clk.summary(),
-            "mixed": {
-                "form": "FP32 P2M/P2L/M2QBXL, split-TF32 tensor-core M2L, FP64 M2M/L2L, "
-                        "target-specific near field and point evaluations",
-                "value": world * node_applies * K / tm, "unit": UNIT,
-                "ms_per_step": 1e3 * tm / K, "speedup_vs_fp64": t_max / tm,
-                "rel_err_vs_fp64_gpu": float(np.abs(res_mixed - res_gpu).max()
-                                             / np.abs(res_gpu).max())},
-        }
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
-    if rank != 0:
-        return
-    if world == 1 and not args.no_cpu_baseline:
-        threads = os.cpu_count() or 1
-        ref, times = cpu_reference(wl, 2, threads)
-        cpu_t = statistics.mean(times)
-        line["cpu_baseline"] = {
-            "value": node_applies / cpu_t, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": "2 full applies of the same workload (C/OpenMP float64 restatement)"}
-        line["rel_err_vs_fp64_oracle"] = float(np.abs(res_gpu - ref).max() / np.abs(ref).max())
-        line["mixed"]["rel_err_vs_fp64_oracle"] = float(np.abs(res_mixed - ref).max()
-                                                        / np.abs(ref).max())
-    if world == 1 and not args.no_helmholtz:
-        line["helmholtz3d"] = helmholtz3d_leg(torch, dev)
-    print(json.dumps(line), flush=True)
-
-
-def helmholtz3d_leg(torch, dev, steps=3, warmup=3):
-    """The 3D Helmholtz combined-field apply at full size (ellipsoid from an
-    icosphere refined 5 times: 20480 triangles, 307200 nodes -> 921600 sources, k 10,
-    16 plane-wave densities, qbx_order 5, fmm_order 15), timed like the headline step
-    with CUDA events; its working set (several GB) exceeds the L2, so no flush.  The
-    one-time geometry (host tree and traversal, target association on the GPU) and the
-    plan with its translation tables are timed apart."""
-    from pytential_b200.fmm import QBXApply
-    from pytential_b200.workloads import helmholtz3d_ellipsoid
-    w = helmholtz3d_ellipsoid(nrefine=5, nrhs=16)
-    geo = w.geometry()
-    t0 = time.perf_counter()
-    geo.traversal()
-    t_geo = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    ap = QBXApply(geo, w.spec, w.qbx_order, w.fmm_order, nrhs=w.nrhs, device=dev,
-                  target_specific_qbx=True)
-    torch.cuda.synchronize()
-    t_plan = time.perf_counter() - t0
-    dens = torch.from_numpy(w.density).to(dev)
-    out = ap.new_output()
-    for _ in range(warmup):
-        ap.apply_into(dens, out)
-    torch.cuda.synchronize()
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-          for _ in range(steps)]
+def time_calls(torch, fn, steps, flush):
+    """ms of each of ``steps`` calls of fn(), CUDA events on the current stream, the L2
+    flushed before each call outside the events."""
+    ev = _events(torch, steps)
     for a, b in ev:
+        flush.zero_()
         a.record()
-        ap.apply_into(dens, out)
+        fn()
         b.record()
     torch.cuda.synchronize()
-    ap.check_error_word()
-    ms = statistics.mean(a.elapsed_time(b) for a, b in ev)
-    nodes = ap.nuser_targets * w.nrhs
-    return {"workload": "3D Helmholtz combined field D - ik S, k 10, ellipsoid (1,1.5,2), "
-                        "icosphere-5 (20480 tri), 307200 nodes -> 921600 sources, 16 RHS, "
-                        "qbx_order 5, fmm_order 15, FP64, target-specific near field",
-            "metric": METRIC, "unit": UNIT, "value": nodes * 1e3 / ms, "ms_per_step": ms,
-            "steps": steps, "warmup": warmup, "node_applies_per_step": nodes,
-            "tree_and_lists_s": t_geo, "plan_and_precompute_s": t_plan,
-            "l2": "not flushed (working set several GB)"}
+    return [a.elapsed_time(b) for a, b in ev]
+
+
+def kernel_nodes(torch, ap, dens, out):
+    """Kernels of this library in one apply: the apply captured into a CUDA graph (not
+    instantiated), its kernel nodes counted."""
+    from cuda.bindings import runtime as rt
+    s = torch.cuda.Stream(device=ap.device)
+    s.wait_stream(torch.cuda.current_stream())
+    g = torch.cuda.CUDAGraph(keep_graph=True)
+    with torch.cuda.graph(g, stream=s):
+        ap.apply_into(dens, out, s)
+    graph = rt.cudaGraph_t(init_value=g.raw_cuda_graph())
+    err, _, n = rt.cudaGraphGetNodes(graph, 0)
+    err, nodes, n = rt.cudaGraphGetNodes(graph, n)
+    kinds = [rt.cudaGraphNodeGetType(nd)[1] for nd in nodes[:n]]
+    del g
+    return sum(1 for k in kinds if k == rt.cudaGraphNodeType.cudaGraphNodeTypeKernel)
 
 
 def measure_fp64_peak(torch, dev):
+    """Dense float64 GEMM (cuBLAS, 8192^3) on this GPU, best of 5: the FP64 roofline
+    denominator (the driver's measured peaks hold the HBM copy and bf16 GEMM only)."""
     n = 8192
     a = torch.randn(n, n, dtype=torch.float64, device=dev)
     b = torch.randn(n, n, dtype=torch.float64, device=dev)
@@ -499,6 +244,344 @@ def measure_fp64_peak(torch, dev):
         best = max(best, 2 * n ** 3 / (s.elapsed_time(e) * 1e-3) / 1e12)
     del a, b
     return best
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def ncu_traffic(workload, kernel, units):
+    """DRAM bytes of one launch of ``kernel`` scaled from the committed ncu capture of a
+    smaller case by the ratio of work units (``profiles/ncu_dram_bytes.json``)."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "ncu_dram_bytes.json")) as f:
+            e = json.load(f)[workload][kernel]
+        return e["bytes"] * units / e["units"], e["case"]
+    except (OSError, ValueError, KeyError, ZeroDivisionError):
+        return None, None
+
+
+# stage entry -> (kernel symbol of its main launch, argument names)
+STAGES = {
+    "form_multipoles": ("k_h3_p2e<0>", ("strengths", "mpoles")),
+    "coarsen_multipoles": ("k_trans_mv (M2M)", ("mpoles",)),
+    "multipole_to_local": ("k_h3_m2l_rot", ("mpoles", "locals", "err")),
+    "form_locals": ("k_h3_p2e<1>", ("strengths", "locals", "err")),
+    "refine_locals": ("k_trans_mv (L2L)", ("locals",)),
+    "translate_box_multipoles_to_qbx_local": ("k_h3_e2qbxl_rot<0>", ("mpoles", "qbx_exps", "err")),
+    "translate_box_local_to_qbx_local": ("k_h3_l2qbxl", ("locals", "qbx_exps")),
+    "eval_target_specific_qbx_locals": ("k_h3_tsqbx", ("strengths", "pot_tree", "err")),
+    "eval_qbx_expansions": ("k_h3_qbxl2p", ("qbx_exps", "pot_tree")),
+}
+
+
+def stage_times(torch, ap, steps, flush, names=STAGES):
+    """Each stage entry of the apply timed alone (CUDA events, L2 flushed), on the
+    workspace the last apply left."""
+    st = torch.cuda.current_stream()
+    S = ctypes.c_void_p(st.cuda_stream)
+    ws = ap.ws
+    bufs = {"strengths": ctypes.c_void_p(ws.strengths), "mpoles": ctypes.c_void_p(ws.mpoles),
+            "locals": ctypes.c_void_p(ws.locals), "qbx_exps": ctypes.c_void_p(ws.qbx_exps),
+            "pot_tree": ctypes.c_void_p(ws.pot_tree), "err": ws.error_word}
+    out = {}
+    for name, (_, args) in names.items():
+        fn = (lambda n=name, a=args: ap.plan.call("qbxfmm_" + n, *[bufs[x] for x in a], S))
+        out[name] = statistics.mean(time_calls(torch, fn, steps, flush))
+    return out
+
+# }}}
+
+
+def cpu_checker_sample(threads, reps=1):
+    """The CPU checker (C/OpenMP float64, all host threads) on the bounded sample of
+    the headline workload: the same operator, wave number and orders on the
+    icosphere-2 surface (320 triangles, 4800 nodes, 14400 sources) with one of the
+    densities; host-built geometry (no CUDA code is loaded)."""
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle.oracle import Oracle
+    wl = h3_workload(H3_SAMPLE["nrefine"], nrhs=H3_SAMPLE["nrhs"])
+    geo = wl.geometry(builders="host")
+    sp = wl.spec
+    o = Oracle(geo, dim=3, qbx_order=wl.qbx_order, fmm_order=wl.fmm_order, nrhs=wl.nrhs,
+               charge_coeff=sp.charge_coeff, dipole_coeff=sp.dipole_coeff,
+               family=sp.kernel.family, k=sp.wave_number)
+    s = wl.tree_strengths()
+    out, times = None, []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        out = o.apply(s)
+        times.append(time.perf_counter() - t0)
+    return wl, out, times
+
+
+SAMPLE_TEXT = ("the full apply of the same operator (D - ik S, k 10, qbx_order 5, fmm_order "
+               "15) on the icosphere-2 ellipsoid (320 tri, 4800 nodes -> 14400 sources) with "
+               "one of the 16 densities, scaled to node-applies/s")
+
+
+def run_reference(args):
+    """The reference arm: the CPU restatement of the reference's apply (the reference's
+    pyopencl/sumpy path cannot be installed here), all host threads, one bounded
+    sample per step."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    threads = os.cpu_count() or 1
+    wl, _, _ = cpu_checker_sample(threads, reps=max(args.warmup, 0))
+    _, _, times = cpu_checker_sample(threads, reps=max(args.steps, 1))
+    t = statistics.mean(times)
+    value = wl.nuser_targets * wl.nrhs / t
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * t, "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "c128",
+        "data": "synthetic (seeded analytic geometry and plane-wave densities)",
+        "config": config_dict(args, world),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": SAMPLE_TEXT},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def laplace_leg(torch, dev, steps, warmup, flush, fp64_peak, cpu):
+    """The 3D Laplace double-layer apply (ellipsoid, icosphere-3, 57600 sources, 19200
+    surface + 2000 shell targets, q 3 / p 10), FP64 and mixed, timed like the headline."""
+    from pytential_b200 import costs
+    from pytential_b200.fmm import PRECISION_MIXED, QBXApply
+    from pytential_b200.workloads import laplace3d_ellipsoid
+    wl = laplace3d_ellipsoid(nrefine=L3["nrefine"], op=L3["op"], qbx_order=L3["qbx_order"],
+                             fmm_order=L3["fmm_order"])
+    geo = wl.geometry()
+    ap = QBXApply(geo, wl.spec, wl.qbx_order, wl.fmm_order, device=dev, target_specific_qbx=True)
+    apm = QBXApply(geo, wl.spec, wl.qbx_order, wl.fmm_order, device=dev,
+                   device_geometry=ap.dgeo, target_specific_qbx=True, precision=PRECISION_MIXED)
+    dens = torch.from_numpy(wl.density).to(dev)
+    out, outm = ap.new_output(), apm.new_output()
+    for _ in range(warmup):
+        ap.apply_into(dens, out)
+        apm.apply_into(dens, outm)
+    ms = statistics.mean(time_calls(torch, lambda: ap.apply_into(dens, out), steps, flush))
+    msm = statistics.mean(time_calls(torch, lambda: apm.apply_into(dens, outm), steps, flush))
+    ap.check_error_word()
+    apm.check_error_word()
+    names = {k: v for k, v in STAGES.items() if k in (
+        "translate_box_multipoles_to_qbx_local", "form_locals", "multipole_to_local",
+        "eval_target_specific_qbx_locals")}
+    kt = stage_times(torch, ap, steps, flush, names)
+    ap.apply_into(dens, out)
+    res, resm = out.cpu().numpy(), outm.cpu().numpy()
+    scal, arr = ap.dgeo.scalars, ap.dgeo.host_arrays
+    alg = costs.algorithmic_flops(arr, scal, 3, False, wl.fmm_order, wl.qbx_order, wl.nrhs)
+    dom = max(kt, key=kt.get)
+    nodes = wl.nuser_targets * wl.nrhs
+    d = {"workload": "3D Laplace double layer, ellipsoid (1,1.5,2), icosphere-3 (1280 tri), "
+                     "19200 nodes -> 57600 sources, 19200 surface + 2000 shell targets, "
+                     "qbx_order 3, fmm_order 10, FP64, target-specific near field",
+         "value": nodes * 1e3 / ms, "unit": UNIT, "ms_per_step": ms,
+         "mixed": {"value": nodes * 1e3 / msm, "ms_per_step": msm, "speedup_vs_fp64": ms / msm,
+                   "rel_err_vs_fp64_gpu": float(np.abs(resm - res).max() / np.abs(res).max())},
+         "dominant_kernel": {"stage": dom, "ms": kt[dom], "algorithmic_flops": alg[dom],
+                             "tflops": alg[dom] / (kt[dom] * 1e-3) / 1e12,
+                             "frac_of_fp64_peak": alg[dom] / (kt[dom] * 1e-3) / 1e12 / fp64_peak},
+         "stages_ms": {k: round(v, 4) for k, v in kt.items()}}
+    if cpu:
+        from oracle.oracle import Oracle
+        sp = wl.spec
+        o = Oracle(geo, dim=3, qbx_order=wl.qbx_order, fmm_order=wl.fmm_order, nrhs=wl.nrhs,
+                   charge_coeff=sp.charge_coeff, dipole_coeff=sp.dipole_coeff)
+        t0 = time.perf_counter()
+        ref = o.apply(wl.tree_strengths())
+        d["cpu_checker_value"] = nodes / (time.perf_counter() - t0)
+        d["rel_err_vs_fp64_oracle"] = float(np.abs(res - ref).max() / np.abs(ref).max())
+        d["mixed"]["rel_err_vs_fp64_oracle"] = float(np.abs(resm - ref).max() / np.abs(ref).max())
+    return d
+
+
+def run_b200(args):
+    import torch
+    import torch.distributed as dist
+
+    from pytential_b200 import costs
+    from pytential_b200.fmm import PRECISION_MIXED, QBXApply
+    from pytential_b200.sharding import all_gather_rhs, rhs_split
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # one job: the same 16 densities on every rank, each rank applies its share
+    wl = h3_workload(args.nrefine)
+    nrhs = wl.nrhs
+    start, count = rhs_split(nrhs, world, rank)
+    t0 = time.perf_counter()
+    geo = wl.geometry()
+    geo.traversal()
+    geo.center_to_tree_targets()
+    t_geo = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    ap = QBXApply(geo, wl.spec, wl.qbx_order, wl.fmm_order, nrhs=count, device=dev,
+                  target_specific_qbx=True)
+    torch.cuda.synchronize()
+    t_plan = time.perf_counter() - t0
+    dens_all = torch.from_numpy(wl.density).to(dev)
+    dens = dens_all[start:start + count].contiguous()
+    out = ap.new_output()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    nodes_total = ap.nuser_targets * nrhs
+
+    def step():
+        ap.apply_into(dens, out)
+        if world > 1:
+            return all_gather_rhs(out, nrhs)
+        return out
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    K = args.steps
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        step_ms = time_calls(torch, step, K, flush)
+    barrier()
+    t_max = max_over_ranks(sum(step_ms) / 1e3)
+    value = nodes_total * K / t_max
+    full = step().cpu().numpy()
+    ap.check_error_word()
+    launches = kernel_nodes(torch, ap, dens, out)
+
+    # end to end through the host-buffer entry (H2D of this rank's densities, apply,
+    # D2H of its potentials, sync), device-timed around each call
+    ap.alloc_host_buffers()
+    ap.h_in.copy_(torch.from_numpy(wl.density[start:start + count]))
+    for _ in range(2):
+        ap.apply_host()
+    barrier()
+    ev = _events(torch, K)
+    for a, b in ev:
+        a.record()
+        ap.apply_host()
+        b.record()
+    torch.cuda.synchronize()
+    t_e2e = max_over_ranks(sum(a.elapsed_time(b) for a, b in ev) / 1e3)
+    e2e_value = nodes_total * K / t_e2e
+
+    # the mixed-precision form on the same job
+    mixed = {}
+    try:
+        apm = QBXApply(geo, wl.spec, wl.qbx_order, wl.fmm_order, nrhs=count, device=dev,
+                       device_geometry=ap.dgeo, target_specific_qbx=True,
+                       precision=PRECISION_MIXED)
+    except Exception as e:   # noqa: BLE001  (reported, not hidden)
+        apm = None
+        mixed = {"status": f"not available: {e}"}
+    if apm is not None:
+        outm = apm.new_output()
+        for _ in range(max(args.warmup, 3)):
+            apm.apply_into(dens, outm)
+        barrier()
+        msm = time_calls(torch, lambda: apm.apply_into(dens, outm), K, flush)
+        tm = max_over_ranks(sum(msm) / 1e3)
+        apm.check_error_word()
+        resm = outm.cpu().numpy()
+        resd = out.cpu().numpy()
+        mixed = {"value": nodes_total * K / tm, "unit": UNIT, "ms_per_step": 1e3 * tm / K,
+                 "speedup_vs_fp64": t_max / tm,
+                 "rel_err_vs_fp64_gpu": max_over_ranks(
+                     float(np.abs(resm - resd).max() / np.abs(resd).max()))}
+
+    line = None
+    if rank == 0:
+        # each stage alone, the dominant one gives the roofline entry
+        kt = stage_times(torch, ap, K, flush)
+        scal, arr = ap.dgeo.scalars, ap.dgeo.host_arrays
+        alg = costs.algorithmic_flops(arr, scal, 3, True, wl.fmm_order, wl.qbx_order, count)
+        dom = max(kt, key=kt.get)
+        fp64_peak = measure_fp64_peak(torch, dev)
+        achieved = alg[dom] / (kt[dom] * 1e-3) / 1e12
+        units = costs.m2qbxl_pairs(arr, scal) if dom.startswith("translate_box_mult") else None
+        traffic, tcase = ncu_traffic("helmholtz3d", STAGES[dom][0], units) if units else (None, None)
+        peaks = measured_peaks()
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
+            "warmup": max(args.warmup, 3), "ms_per_step": 1e3 * t_max / K,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+            "dtype": "c128", "data": "synthetic (seeded analytic geometry and plane-wave densities)",
+            "config": config_dict(args, world),
+            "roofline": {
+                "kernel": f"{STAGES[dom][0]} ({dom})", "bound": "fp64",
+                "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
+                "frac": achieved / fp64_peak,
+                "peak_source": ("of measured: cuBLAS float64 GEMM 8192^3 on this GPU, best of 5 "
+                                "(MEASURED_PEAKS.json holds no FP64 entry)"),
+                "algorithmic_flops_per_launch": alg[dom],
+                "algorithmic_count": "pytential_b200/costs.py algorithmic_flops",
+                "kernel_ms": kt[dom], "share_of_step": kt[dom] / (1e3 * t_max / K),
+                "traffic": traffic, "traffic_source": tcase,
+                "stages_ms": {k: round(v, 3) for k, v in kt.items()},
+                "stages_tflops_algorithmic": {
+                    k: round(alg[k] / (kt[k] * 1e-3) / 1e12, 3) for k in kt}},
+            "e2e": {"value": e2e_value, "unit": UNIT,
+                    "h2d_bytes_per_step": ap.h2d_bytes * world,
+                    "d2h_bytes_per_step": ap.d2h_bytes * world},
+            "gpu_launches": launches * K,
+            "clocks": clk.summary(),
+            "geometry_s": t_geo, "plan_and_precompute_s": t_plan,
+            "hbm_peak_gbs": peaks.get("hbm_gbs"),
+            "mixed": mixed,
+        }
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    if world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        swl, ref, times = cpu_checker_sample(threads, reps=1)
+        cpu_t = statistics.mean(times)
+        line["cpu_baseline"] = {"value": swl.nuser_targets * swl.nrhs / cpu_t, "unit": UNIT,
+                                "cores": threads, "kind": "port", "sample": SAMPLE_TEXT}
+        # parity spot check on the sample: the GPU forms against the checker
+        sap = QBXApply(swl.geometry(), swl.spec, swl.qbx_order, swl.fmm_order, nrhs=swl.nrhs,
+                       device=dev, target_specific_qbx=True)
+        got = sap(torch.from_numpy(swl.density).to(dev)).cpu().numpy()
+        line["rel_err_vs_fp64_oracle_sample"] = float(np.abs(got - ref).max() / np.abs(ref).max())
+        if "value" in mixed:
+            sapm = QBXApply(swl.geometry(), swl.spec, swl.qbx_order, swl.fmm_order,
+                            nrhs=swl.nrhs, device=dev, device_geometry=sap.dgeo,
+                            target_specific_qbx=True, precision=PRECISION_MIXED)
+            gotm = sapm(torch.from_numpy(swl.density).to(dev)).cpu().numpy()
+            mixed["rel_err_vs_fp64_oracle_sample"] = float(np.abs(gotm - ref).max()
+                                                           / np.abs(ref).max())
+    if world == 1 and not args.no_laplace:
+        flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+        line["laplace3d"] = laplace_leg(torch, dev, 20, 5, flush, line["roofline"]["peak"],
+                                        cpu=not args.no_cpu_baseline)
+    del full
+    print(json.dumps(line), flush=True)
 
 
 def main():

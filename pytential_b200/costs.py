@@ -159,3 +159,70 @@ def p2l_flops(arrays: dict, scalars: dict, p: int, charge: bool, dipole: bool) -
     npairs = int(c.sum()) if len(l4s) > 1 and l4s[-1] > 0 else 0
     nt = (p + 2) * (p + 3) // 2
     return npairs * (9 * nt + ncoeff_laplace(3, p) * (4 * charge + 20 * dipole))
+
+
+# {{{ algorithmic work of the stages (independent of the implementation)
+#
+# The roofline fractions use these counts, not the kernels' own operation counts.
+# C(p) is the coefficient count of the reference's default expansions: (p + 1)^2 in
+# 3D (compressed Taylor), 2 p + 1 in 2D; a real multiply-add is 2 flops and complex
+# arithmetic counts 4 real products per complex one.  Per stage and per density:
+#   P2M, L2P          particles x C_f x 2 x cx
+#   M2M, L2L          boxes x 2 C_f^2 x cx
+#   M2L               list-2 pairs x 2 C_f^2 x cx
+#   M2P               (target, list-3 box) pairs x C_f x 2 x cx
+#   P2L               (box, list-4 source) pairs x C_f x 2 x cx
+#   P2QBXL            (used center, list-1 source) pairs x C_q x 2 x cx
+#   M2QBXL            (used center, list-3 box) pairs x 2 C_f C_q x cx
+#   L2QBXL            used centers x 2 C_f C_q x cx
+#   QBXL2P            QBX targets x C_q x 2 x cx
+#   target-specific   (QBX target, list-1 source) pairs x (Q + 1) x 2 x cx (one term
+#                     of the order-Q line series per order)
+# with cx = 1 for Laplace (real) and 4 for Helmholtz (complex).
+
+def coeff_count(dim: int, p: int) -> int:
+    return (p + 1) ** 2 if dim == 3 else 2 * p + 1
+
+
+def _list_sources(arrays, starts_key, lists_key):
+    s = arrays[starts_key].astype(np.int64)
+    c = arrays["box_source_counts_nonchild"][arrays[lists_key]].astype(np.int64)
+    csum = np.concatenate([[0], np.cumsum(c)])
+    return csum[s[1:]] - csum[s[:-1]]
+
+
+def algorithmic_flops(arrays: dict, scalars: dict, dim: int, complex_: bool, pf: int,
+                      q: int, nrhs: int = 1) -> dict:
+    """Algorithmic flops of each stage of one apply (all densities), keyed by the
+    reference's wrangler method names."""
+    cx = 4 if complex_ else 1
+    cf, cq = coeff_count(dim, pf), coeff_count(dim, q)
+    nb = scalars["nboxes"]
+    gc = arrays["global_qbx_centers"][:scalars["nglobal_qbx_centers"]]
+    ng = len(gc)
+    out = {}
+    out["form_multipoles"] = scalars["nsources"] * cf * 2 * cx
+    out["coarsen_multipoles"] = nb * 2 * cf * cf * cx
+    out["refine_locals"] = nb * 2 * cf * cf * cx
+    n2 = int(arrays["list2_starts"][-1]) if len(arrays["list2_starts"]) else 0
+    out["multipole_to_local"] = n2 * 2 * cf * cf * cx
+    nf = scalars["nfiltered_targets"]
+    out["eval_locals"] = nf * cf * 2 * cx
+    if nf:
+        tb = arrays["target_boxes"]
+        nt = arrays["nonqbx_box_target_counts_nonchild"][tb].astype(np.int64)
+        n3 = np.diff(arrays["list3_starts"].astype(np.int64))
+        out["eval_multipoles"] = int((nt * n3).sum()) * cf * 2 * cx
+    else:
+        out["eval_multipoles"] = 0
+    out["form_locals"] = int(_list_sources(arrays, "list4_starts", "list4_lists").sum()) \
+        * cf * 2 * cx
+    out["form_global_qbx_locals"] = p2qbxl_pairs(arrays, scalars) * cq * 2 * cx
+    out["translate_box_multipoles_to_qbx_local"] = m2qbxl_pairs(arrays, scalars) * 2 * cf * cq * cx
+    out["translate_box_local_to_qbx_local"] = ng * 2 * cf * cq * cx
+    nqt = int(arrays["center_to_targets_starts"][-1]) if ng else 0
+    out["eval_qbx_expansions"] = nqt * cq * 2 * cx
+    out["eval_target_specific_qbx_locals"] = tsqbx_pairs(arrays, scalars) * (q + 1) * 2 * cx
+    return {k: int(v) * nrhs for k, v in out.items()}
+
+# }}}
