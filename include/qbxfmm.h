@@ -55,7 +55,17 @@ typedef struct qbxfmm_kernel {
                                   series per target and source) instead of through
                                   the center's expansion (pytential's
                                   _use_target_specific_qbx, fmm.py:391-394) */
+  int32_t fmm_backend;       /* whose expansions' truncation the apply reproduces:
+                                QBXFMM_BACKEND_SUMPY (0, the reference's default,
+                                fmm_backend="sumpy": sumpy's default expansions, PDE-
+                                compressed Cartesian Taylor in 3D) or
+                                QBXFMM_BACKEND_FMMLIB (1, fmm_backend="fmmlib":
+                                spherical-wave expansions), pytential/qbx/__init__.py:
+                                93, 191, 617-659.  Only 3D Helmholtz truncates
+                                differently; Laplace and 2D Helmholtz ignore it. */
 } qbxfmm_kernel;
+
+enum qbxfmm_backend { QBXFMM_BACKEND_SUMPY = 0, QBXFMM_BACKEND_FMMLIB = 1 };
 
 /* Tree, traversal and QBX geometry, field names after boxtree's Tree /
  * FMMTraversalInfo and pytential's QBXFMMGeometryData

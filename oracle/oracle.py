@@ -52,14 +52,16 @@ class Oracle:
     """Host-side QBX-FMM over a geometry-data object (float64/complex128)."""
 
     def __init__(self, geo, *, dim, qbx_order, fmm_order, nrhs=1,
-                 charge_coeff=0.0, dipole_coeff=0.0, family=abi.QBXFMM_LAPLACE, k=0.0):
+                 charge_coeff=0.0, dipole_coeff=0.0, family=abi.QBXFMM_LAPLACE, k=0.0,
+                 fmm_backend="sumpy"):
         self.geo = geo
         self.scalars, self.arrays = abi.geometry_arrays(geo)
         self.g = abi.make_geometry_struct(self.scalars, self.arrays,
                                           lambda a: a.ctypes.data)
         self.kern = abi.make_kernel_struct(
             family=family, dim=dim, qbx_order=qbx_order, fmm_order=fmm_order,
-            nrhs=nrhs, k=k, charge_coeff=charge_coeff, dipole_coeff=dipole_coeff)
+            nrhs=nrhs, k=k, charge_coeff=charge_coeff, dipole_coeff=dipole_coeff,
+            fmm_backend=fmm_backend)
         self.nrhs = nrhs
         self.dtype = np.complex128 if family == abi.QBXFMM_HELMHOLTZ else np.float64
         self.ncf = abi.ncoeff(family, dim, fmm_order)

@@ -35,6 +35,25 @@
  * radius), multipoles divided by s^n and locals multiplied by s^n, as fmmlib does.
  * j_n by Miller's backward recurrence (normalized by j_0 or j_1), h_n by the upward
  * recurrence from h_0, h_1.
+ *
+ * Two truncations are restated (qbxfmm_kernel.fmm_backend):
+ *  - fmmlib (the reference's fmm_backend="fmmlib", pytential/qbx/fmmlib.py): the
+ *    spherical-wave expansions above, translated by the addition theorem;
+ *  - sumpy (the reference's default, pytential/qbx/__init__.py:98-112): sumpy's
+ *    PDE-compressed Cartesian Taylor expansions of degree p (box) and q (QBX).  They
+ *    are kept here in the same coefficients: a degree-p Taylor polynomial of a
+ *    Helmholtz field sum L_nm j_n Y_n^m keeps the terms |v|^(n+2j) Y_n^m with
+ *    n + 2j <= p, i.e. j_n replaced by its power series truncated at total degree p,
+ *    j_n^[p]; a multipole formed from source moments of degree <= p has the moments
+ *    j_n^[p] Y_n^-m(y - c) (j_n^[p-1] in the normal derivative of a dipole).  The
+ *    stages sumpy defines through the compressed coefficients themselves are
+ *    restated step by step in the monomial basis (v = k x): M2M converts the child's
+ *    coefficients to its stored moments (those with exponent of z <= 1), shifts them
+ *    with the other moments taken as zero, and converts the parent's full moments
+ *    back; L2L and L2QBXL expand the local to its monomials, shift them to the new
+ *    center, keep the coefficients with exponent of z <= 1 up to the new order and
+ *    convert them back (sumpy rebuilds the others from the PDE, which is what the
+ *    order-(p or q) basis j_n^[.] Y_n^m spans).
  */
 
 #define H3Q(n, m) ((n) * (n) + (n) + (m))
@@ -158,6 +177,36 @@ static cplx h3_dgrad(const cplx* F, int N, int n, int m, double k, const double*
 
 /* {{{ Gaunt table */
 
+/* j_n^[T](x) = sum_{j: n + 2j <= T} (-x^2/2)^j x^n / (j! (2n + 2j + 1)!!), n <= N
+ * (zero for n > T): the power series of j_n truncated at total degree T */
+static void h3_sph_j_trunc(int N, double x, int T, double* jv)
+{
+  double xn = 1.0, dfac = 1.0;   /* x^n, (2n+1)!! */
+  for (int n = 0; n <= N; ++n) {
+    if (n > 0) {
+      xn *= x;
+      dfac *= 2.0 * n + 1.0;
+    }
+    double term = xn / dfac, acc = 0.0;
+    for (int j = 0; n + 2 * j <= T; ++j) {
+      acc += term;
+      term *= -x * x / (2.0 * (j + 1) * (2.0 * n + 2.0 * j + 3.0));
+    }
+    jv[n] = acc;
+  }
+}
+
+/* regular waves j_n^[T](k|v|) Y_n^m(v), n <= N */
+static void h3_waves_trunc(int N, double k, const double* v, int T, cplx* F)
+{
+  double jv[H3_NMAX + 2];
+  double r = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+  h3_ylm(N, v, F);
+  h3_sph_j_trunc(N, k * r, T, jv);
+  for (int n = 0; n <= N; ++n)
+    for (int m = -n; m <= n; ++m) F[H3Q(n, m)] *= jv[n];
+}
+
 /* Gauss-Legendre nodes/weights on [-1, 1] (Newton on P_n) */
 static void h3_gauss_legendre(int n, double* x, double* w)
 {
@@ -275,10 +324,324 @@ static void h3_translate(const h3gaunt_t* gt, int pin, int pout, const cplx* Ein
 
 /* }}} */
 
+/* {{{ sumpy's compressed Taylor truncation: the monomial basis */
+
+typedef long double complex lcplx;
+
+/* Monomial coefficients, in wave units v = k x, of the order-p local basis
+ * f_nm(v) = j_n^[p](|v|) Y_n^m(v) (n <= p): F[H3Q(n,m)][cube(a,b,c)], a + b + c <= p,
+ * cube(a,b,c) = (a (p+1) + b)(p+1) + c.  The multipole basis of the moments is
+ * e_nm = f_{n,-m}.  The stored multi-indices are the (p+1)^2 with c <= 1 (sumpy
+ * eliminates u_zz through the PDE); G[s][nm] = F[nm][stored s] is square and
+ * Ginv = G^-1 ([nm][s]) converts stored Taylor coefficients to basis coefficients. */
+typedef struct {
+  int p, D1, nst;
+  cplx* F;
+  int* st;          /* cube index of each stored multi-index */
+  int* sa;          /* [nst][3] its exponents */
+  cplx* Ginv;
+  double* fact;     /* 0! .. (2p+1)! */
+} h3tay_t;
+
+#define H3T_SLOTS 4
+static h3tay_t g_h3tay[H3T_SLOTS] = {{-1}, {-1}, {-1}, {-1}};
+static long g_h3tay_used[H3T_SLOTS], g_h3tay_clock = 0;
+
+static int h3t_cube(int a, int b, int c, int D1) { return (a * D1 + b) * D1 + c; }
+
+/* dense polynomial product, truncated at total degree D1 - 1 */
+static void h3t_mul(const lcplx* A, const lcplx* B, lcplx* C, int D1)
+{
+  int D = D1 - 1;
+  for (int i = 0; i < D1 * D1 * D1; ++i) C[i] = 0;
+  for (int a = 0; a <= D; ++a)
+    for (int b = 0; a + b <= D; ++b)
+      for (int c = 0; a + b + c <= D; ++c) {
+        lcplx x = A[h3t_cube(a, b, c, D1)];
+        if (x == 0) continue;
+        for (int a2 = 0; a + a2 <= D; ++a2)
+          for (int b2 = 0; a + a2 + b + b2 <= D; ++b2)
+            for (int c2 = 0; a + a2 + b + b2 + c + c2 <= D; ++c2) {
+              lcplx y = B[h3t_cube(a2, b2, c2, D1)];
+              if (y != 0) C[h3t_cube(a + a2, b + b2, c + c2, D1)] += x * y;
+            }
+      }
+}
+
+/* Gauss-Jordan inverse with partial pivoting (n x n, row-major), long double */
+static int h3t_invert(lcplx* A, lcplx* Ainv, int n)
+{
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < n; ++j) Ainv[(size_t)i * n + j] = (i == j) ? 1 : 0;
+  for (int col = 0; col < n; ++col) {
+    int piv = col;
+    for (int r = col + 1; r < n; ++r)
+      if (cabsl(A[(size_t)r * n + col]) > cabsl(A[(size_t)piv * n + col])) piv = r;
+    if (cabsl(A[(size_t)piv * n + col]) == 0) return -1;
+    if (piv != col)
+      for (int j = 0; j < n; ++j) {
+        lcplx t = A[(size_t)piv * n + j];
+        A[(size_t)piv * n + j] = A[(size_t)col * n + j];
+        A[(size_t)col * n + j] = t;
+        t = Ainv[(size_t)piv * n + j];
+        Ainv[(size_t)piv * n + j] = Ainv[(size_t)col * n + j];
+        Ainv[(size_t)col * n + j] = t;
+      }
+    lcplx d = 1 / A[(size_t)col * n + col];
+    for (int j = 0; j < n; ++j) {
+      A[(size_t)col * n + j] *= d;
+      Ainv[(size_t)col * n + j] *= d;
+    }
+    for (int r = 0; r < n; ++r) {
+      if (r == col) continue;
+      lcplx f = A[(size_t)r * n + col];
+      if (f == 0) continue;
+      for (int j = 0; j < n; ++j) {
+        A[(size_t)r * n + j] -= f * A[(size_t)col * n + j];
+        Ainv[(size_t)r * n + j] -= f * Ainv[(size_t)col * n + j];
+      }
+    }
+  }
+  return 0;
+}
+
+/* the table of order p (cached; least recently used slot replaced; not thread-safe:
+ * call outside parallel regions) */
+static const h3tay_t* h3_taylor(int p)
+{
+  for (int i = 0; i < H3T_SLOTS; ++i)
+    if (g_h3tay[i].p == p) {
+      g_h3tay_used[i] = ++g_h3tay_clock;
+      return &g_h3tay[i];
+    }
+  int victim = 0;
+  for (int i = 1; i < H3T_SLOTS; ++i)
+    if (g_h3tay_used[i] < g_h3tay_used[victim]) victim = i;
+  g_h3tay_used[victim] = ++g_h3tay_clock;
+  h3tay_t* t = &g_h3tay[victim];
+  if (t->p >= 0) {
+    free(t->F);
+    free(t->st);
+    free(t->sa);
+    free(t->Ginv);
+    free(t->fact);
+  }
+  const int D1 = p + 1, NC = D1 * D1 * D1, ncf = (p + 1) * (p + 1);
+  t->p = p;
+  t->D1 = D1;
+  t->nst = ncf;
+  t->F = calloc((size_t)ncf * NC, sizeof(cplx));
+  t->st = malloc(sizeof(int) * ncf);
+  t->sa = malloc(sizeof(int) * 3 * ncf);
+  t->Ginv = malloc(sizeof(cplx) * (size_t)ncf * ncf);
+  t->fact = malloc(sizeof(double) * (2 * p + 2));
+  t->fact[0] = 1.0;
+  for (int i = 1; i <= 2 * p + 1; ++i) t->fact[i] = t->fact[i - 1] * i;
+  /* (x^2 + y^2 + z^2)^i, i <= p/2 */
+  int nr = p / 2 + 1;
+  lcplx* r2 = calloc((size_t)nr * NC, sizeof(lcplx));
+  lcplx* base = calloc(NC, sizeof(lcplx));
+  r2[h3t_cube(0, 0, 0, D1)] = 1;
+  if (p >= 2) {
+    base[h3t_cube(2, 0, 0, D1)] = base[h3t_cube(0, 2, 0, D1)] = base[h3t_cube(0, 0, 2, D1)] = 1;
+    for (int i = 1; i < nr; ++i) h3t_mul(r2 + (size_t)(i - 1) * NC, base, r2 + (size_t)i * NC, D1);
+  }
+  /* normalized Legendre parts p_n^m(t) = sum_i A[n][m][i] t^i (the recurrence of h3_ylm) */
+  double* A = calloc((size_t)(p + 1) * (p + 1) * (p + 1), sizeof(double));
+#define PA(n, m, i) A[(((size_t)(n) * (p + 1)) + (m)) * (p + 1) + (i)]
+  double pmm = 0.5 / sqrt(M_PI);
+  for (int m = 0; m <= p; ++m) {
+    if (m > 0) pmm *= sqrt((2.0 * m + 1.0) / (2.0 * m));
+    PA(m, m, 0) = pmm;
+    if (m + 1 <= p)
+      for (int i = 0; i <= p - 1; ++i) PA(m + 1, m, i + 1) = sqrt(2.0 * m + 3.0) * PA(m, m, i);
+    for (int n = m + 2; n <= p; ++n) {
+      double a = sqrt((4.0 * n * n - 1.0) / ((double)n * n - (double)m * m));
+      double b = sqrt(((n - 1.0) * (n - 1.0) - (double)m * m) / (4.0 * (n - 1.0) * (n - 1.0) - 1.0));
+      for (int i = 0; i <= p; ++i)
+        PA(n, m, i) = a * ((i > 0 ? PA(n - 1, m, i - 1) : 0.0) - b * PA(n - 2, m, i));
+    }
+  }
+  lcplx* Q = calloc(NC, sizeof(lcplx));
+  lcplx* W = calloc(NC, sizeof(lcplx));
+  lcplx* R = calloc(NC, sizeof(lcplx));
+  lcplx* T = calloc(NC, sizeof(lcplx));
+  for (int n = 0; n <= p; ++n)
+    for (int m = 0; m <= n; ++m) {
+      /* |v|^(n-m) p_n^m(z/|v|) = sum_i A_{n-m-2i} z^(n-m-2i) |v|^(2i) */
+      for (int i = 0; i < NC; ++i) Q[i] = 0;
+      for (int i = 0; 2 * i <= n - m; ++i) {
+        double coef = PA(n, m, n - m - 2 * i);
+        if (coef == 0.0) continue;
+        for (int a = 0; a <= p; ++a)
+          for (int b = 0; a + b <= p; ++b)
+            for (int c = 0; a + b + c + (n - m - 2 * i) <= p; ++c) {
+              lcplx v = r2[(size_t)i * NC + h3t_cube(a, b, c, D1)];
+              if (v != 0) Q[h3t_cube(a, b, c + n - m - 2 * i, D1)] += coef * v;
+            }
+      }
+      /* (x + i y)^m */
+      for (int i = 0; i < NC; ++i) W[i] = 0;
+      {
+        long double bin = 1;
+        lcplx ip = 1;
+        for (int j = 0; j <= m; ++j) {
+          W[h3t_cube(m - j, j, 0, D1)] = bin * ip;
+          bin = bin * (m - j) / (j + 1);
+          ip *= I;
+        }
+      }
+      h3t_mul(Q, W, R, D1);   /* solid harmonic |v|^n Y_n^m */
+      /* f_nm = sum_j c_nj |v|^(2j) R, c_nj = (-1)^j / (2^j j! (2n+2j+1)!!) */
+      long double dfac = 1;
+      for (int i = 1; i <= n; ++i) dfac *= 2 * i + 1;
+      long double cj = 1 / dfac;
+      for (int j = 0; n + 2 * j <= p; ++j) {
+        h3t_mul(r2 + (size_t)j * NC, R, T, D1);
+        for (int i = 0; i < NC; ++i) {
+          if (T[i] == 0) continue;
+          lcplx v = cj * T[i];
+          t->F[(size_t)H3Q(n, m) * NC + i] += (cplx)v;
+          if (m > 0) t->F[(size_t)H3Q(n, -m) * NC + i] += (cplx)conjl(v);
+        }
+        cj *= -1.0L / (2.0L * (j + 1) * (2.0L * n + 2.0L * j + 3.0L));
+      }
+    }
+#undef PA
+  /* stored multi-indices and the inverse of G */
+  int s_ = 0;
+  for (int c = 0; c <= 1 && c <= p; ++c)
+    for (int a = 0; a + c <= p; ++a)
+      for (int b = 0; a + b + c <= p; ++b) {
+        t->st[s_] = h3t_cube(a, b, c, D1);
+        t->sa[3 * s_] = a;
+        t->sa[3 * s_ + 1] = b;
+        t->sa[3 * s_ + 2] = c;
+        ++s_;
+      }
+  lcplx* G = malloc(sizeof(lcplx) * (size_t)ncf * ncf);
+  lcplx* Gi = malloc(sizeof(lcplx) * (size_t)ncf * ncf);
+  for (int si = 0; si < ncf; ++si)
+    for (int c = 0; c < ncf; ++c) G[(size_t)si * ncf + c] = t->F[(size_t)c * NC + t->st[si]];
+  h3t_invert(G, Gi, ncf);
+  for (size_t i = 0; i < (size_t)ncf * ncf; ++i) t->Ginv[i] = (cplx)Gi[i];
+  free(G);
+  free(Gi);
+  free(r2);
+  free(base);
+  free(A);
+  free(Q);
+  free(W);
+  free(R);
+  free(T);
+  return t;
+}
+
+/* v^e / e! for e = (a, b, c), a + b + c <= D (cube of side D + 1) */
+static void h3t_powers(const double* v, int D, const double* fact, cplx* out)
+{
+  int D1 = D + 1;
+  for (int a = 0; a <= D; ++a)
+    for (int b = 0; a + b <= D; ++b)
+      for (int c = 0; a + b + c <= D; ++c)
+        out[h3t_cube(a, b, c, D1)] = pow(v[0], a) * pow(v[1], b) * pow(v[2], c) /
+                                     (fact[a] * fact[b] * fact[c]);
+}
+
+/* sumpy M2M of one density: child multipole ac (order p, field 4 pi i k sum
+ * ac_nm S_n^m, i.e. ac = M s^n without the 4 pi i k) about cc -> ap about the parent
+ * (added), vd = k (cc - cp), the translation of the stored moments with the others
+ * taken as zero. */
+static void h3t_m2m(const h3tay_t* t, const double* vd, const cplx* ac, cplx* ap, cplx* work)
+{
+  const int p = t->p, D1 = t->D1, NC = D1 * D1 * D1, ncf = t->nst;
+  cplx* mu = work;          /* moments, wave units, by cube index */
+  cplx* dpow = work + NC;   /* vd^e / e! */
+  for (int i = 0; i < NC; ++i) mu[i] = 0;
+  /* stored moments: mu_s = (1/s!) sum_nm Ginv[nm][s] ac_{n,-m} */
+  for (int si = 0; si < ncf; ++si) {
+    cplx acc = 0;
+    for (int n = 0; n <= p; ++n)
+      for (int m = -n; m <= n; ++m) acc += t->Ginv[(size_t)H3Q(n, m) * ncf + si] * ac[H3Q(n, -m)];
+    const int* e = t->sa + 3 * si;
+    mu[t->st[si]] = acc / (t->fact[e[0]] * t->fact[e[1]] * t->fact[e[2]]);
+  }
+  h3t_powers(vd, p, t->fact, dpow);
+  /* parent moments nu_b = sum_{a <= b} mu_a vd^(b-a) / (b-a)!, then
+   * ap_nm += sum_b b! [v^b] e_nm nu_b (e_nm = f_{n,-m}) */
+  for (int a = 0; a <= p; ++a)
+    for (int b = 0; a + b <= p; ++b)
+      for (int c = 0; a + b + c <= p; ++c) {
+        cplx nu = 0;
+        for (int a1 = 0; a1 <= a; ++a1)
+          for (int b1 = 0; b1 <= b; ++b1)
+            for (int c1 = 0; c1 <= c && c1 <= 1; ++c1) {
+              cplx m_ = mu[h3t_cube(a1, b1, c1, D1)];
+              if (m_ != 0) nu += m_ * dpow[h3t_cube(a - a1, b - b1, c - c1, D1)];
+            }
+        if (nu == 0) continue;
+        int cb = h3t_cube(a, b, c, D1);
+        double bf = t->fact[a] * t->fact[b] * t->fact[c];
+        for (int n = 0; n <= p; ++n)
+          for (int m = -n; m <= n; ++m) {
+            cplx f = t->F[(size_t)H3Q(n, -m) * NC + cb];
+            if (f != 0) ap[H3Q(n, m)] += bf * f * nu;
+          }
+      }
+  (void)ncf;
+}
+
+/* the monomial coefficients (wave units, about the box center) of the local
+ * sum_nm b_nm f_nm: P[cube] */
+static void h3t_local_monomials(const h3tay_t* t, const cplx* b, cplx* P)
+{
+  const int p = t->p, D1 = t->D1, NC = D1 * D1 * D1;
+  for (int i = 0; i < NC; ++i) P[i] = 0;
+  for (int n = 0; n <= p; ++n)
+    for (int m = -n; m <= n; ++m) {
+      cplx bv = b[H3Q(n, m)];
+      if (bv == 0) continue;
+      const cplx* F = t->F + (size_t)H3Q(n, m) * NC;
+      for (int i = 0; i < NC; ++i)
+        if (F[i] != 0) P[i] += bv * F[i];
+    }
+}
+
+/* sumpy L2L / L2QBXL of one density: the local polynomial P (monomials of the input
+ * order about the old center, wave units) shifted by vd = k (c_new - c_old), its
+ * coefficients with exponent of z <= 1 up to order to->p kept and converted to the
+ * order-to->p basis: bo_nm += sum_s Ginv[nm][s] P'_s. */
+static void h3t_l2l(const h3tay_t* from, const h3tay_t* to, const double* vd, const cplx* P,
+                    cplx* bo, cplx* work)
+{
+  const int pin = from->p, D1 = from->D1, q = to->p, ncq = to->nst;
+  cplx* dpow = work;   /* vd^e / e!, cube of the input order */
+  h3t_powers(vd, pin, from->fact, dpow);
+  for (int si = 0; si < ncq; ++si) {
+    const int* e = to->sa + 3 * si;
+    /* P'_e = sum_{b >= e} P_b binom(b, e) vd^(b-e) = sum_b P_b b!/e! vd^(b-e)/(b-e)! */
+    cplx acc = 0;
+    for (int a = e[0]; a <= pin; ++a)
+      for (int b = e[1]; a + b <= pin; ++b)
+        for (int c = e[2]; a + b + c <= pin; ++c) {
+          cplx pv = P[h3t_cube(a, b, c, D1)];
+          if (pv == 0) continue;
+          double ratio = from->fact[a] * from->fact[b] * from->fact[c] /
+                         (from->fact[e[0]] * from->fact[e[1]] * from->fact[e[2]]);
+          acc += pv * ratio * dpow[h3t_cube(a - e[0], b - e[1], c - e[2], D1)];
+        }
+    for (int n = 0; n <= q; ++n)
+      for (int m = -n; m <= n; ++m) bo[H3Q(n, m)] += to->Ginv[(size_t)H3Q(n, m) * ncq + si] * acc;
+  }
+}
+
+/* }}} */
+
 typedef struct {
   int pf, pq, nrhs, ncf, ncq;
   double k;
   cplx cq, cd;
+  int sumpy;      /* the reference's default (compressed Taylor) truncation */
 } h3ctx_t;
 
 static int h3_ctx(const qbxfmm_kernel* kern, h3ctx_t* c)
@@ -293,6 +656,7 @@ static int h3_ctx(const qbxfmm_kernel* kern, h3ctx_t* c)
   c->k = kern->k_re;
   c->cq = kern->charge_coeff_re + I * kern->charge_coeff_im;
   c->cd = kern->dipole_coeff_re + I * kern->dipole_coeff_im;
+  c->sumpy = kern->fmm_backend == QBXFMM_BACKEND_SUMPY;
   return 0;
 }
 
@@ -304,13 +668,23 @@ static void h3_p2e(const h3ctx_t* c, int p, double s, const double* ctr, const d
 {
   double u[3] = {y[0] - ctr[0], y[1] - ctr[1], y[2] - ctr[2]};
   int N = p + 1;
-  h3_waves(N, c->k, u, local, F);
+  /* sumpy multipoles: moments of degree <= p, j_n^[p] (charge) and the normal
+   * derivative of the degree-<=p moments, i.e. j_n^[p-1] in the ladder (dipole) */
+  int trunc = !local && c->sumpy;
+  cplx* Fd = F + (size_t)(N + 1) * (N + 1);
+  if (trunc) {
+    h3_waves_trunc(N, c->k, u, p, F);
+    h3_waves_trunc(N, c->k, u, p - 1, Fd);
+  } else {
+    h3_waves(N, c->k, u, local, F);
+    Fd = F;
+  }
   cplx pre = 4.0 * M_PI * I * c->k;
   for (int n = 0; n <= p; ++n) {
     double f = local ? pow(s, n) : pow(s, -n);
     for (int m = -n; m <= n; ++m) {
       cplx v = q * F[H3Q(n, -m)];
-      if (sigma != 0.0) v += sigma * h3_dgrad(F, N, n, -m, c->k, nv);
+      if (sigma != 0.0) v += sigma * h3_dgrad(Fd, N, n, -m, c->k, nv);
       E[H3Q(n, m)] += pre * f * v;
     }
   }
@@ -321,7 +695,9 @@ static cplx h3_e2p(const h3ctx_t* c, int p, double s, const double* ctr, const d
                    const cplx* E, int local, cplx* F)
 {
   double u[3] = {x[0] - ctr[0], x[1] - ctr[1], x[2] - ctr[2]};
-  h3_waves(p, c->k, u, !local, F);
+  /* sumpy locals: the degree-p Taylor polynomial, j_n^[p] */
+  if (local && c->sumpy) h3_waves_trunc(p, c->k, u, p, F);
+  else h3_waves(p, c->k, u, !local, F);
   cplx acc = 0.0;
   for (int n = 0; n <= p; ++n) {
     double f = local ? pow(s, -n) : pow(s, n);
@@ -383,6 +759,47 @@ static int h3_coarsen_multipoles(const qbxfmm_kernel* kern, const qbxfmm_geometr
   h3ctx_t c;
   int rc = h3_ctx(kern, &c);
   if (rc) return rc;
+  if (c.sumpy) {
+    const h3tay_t* t = h3_taylor(c.pf);
+    const size_t NC = (size_t)t->D1 * t->D1 * t->D1;
+    for (int lev = g->nlevels - 2; lev >= 0; --lev) {
+      int i0 = g->level_start_source_parent_box_nrs[lev];
+      int i1 = g->level_start_source_parent_box_nrs[lev + 1];
+      double sp = h3_scale(c.k, level_width(g, lev)), sc = h3_scale(c.k, level_width(g, lev + 1));
+#pragma omp parallel
+      {
+        cplx* work = malloc(sizeof(cplx) * (2 * NC + 2 * c.ncf));
+        cplx* ac = work + 2 * NC;
+        cplx* ap = ac + c.ncf;
+#pragma omp for schedule(dynamic, 1)
+        for (int i = i0; i < i1; ++i) {
+          int b = g->source_parent_boxes[i];
+          double cp[3], cc[3];
+          load(g->box_centers, g->nboxes, b, 3, cp);
+          for (int ci = 0; ci < 8; ++ci) {
+            int ch = g->box_child_ids[(size_t)ci * g->nboxes + b];
+            if (ch == 0 || g->box_source_counts_cumul[ch] == 0) continue;
+            load(g->box_centers, g->nboxes, ch, 3, cc);
+            double vd[3] = {c.k * (cc[0] - cp[0]), c.k * (cc[1] - cp[1]), c.k * (cc[2] - cp[2])};
+            for (int r = 0; r < c.nrhs; ++r) {
+              const cplx* Min = mpoles + ((size_t)ch * c.nrhs + r) * c.ncf;
+              cplx* Mout = mpoles + ((size_t)b * c.nrhs + r) * c.ncf;
+              for (int n = 0; n <= c.pf; ++n)
+                for (int m = -n; m <= n; ++m) {
+                  ac[H3Q(n, m)] = Min[H3Q(n, m)] * pow(sc, n);
+                  ap[H3Q(n, m)] = 0;
+                }
+              h3t_m2m(t, vd, ac, ap, work);
+              for (int n = 0; n <= c.pf; ++n)
+                for (int m = -n; m <= n; ++m) Mout[H3Q(n, m)] += ap[H3Q(n, m)] * pow(sp, -n);
+            }
+          }
+        }
+        free(work);
+      }
+    }
+    return 0;
+  }
   const h3gaunt_t* gt = h3_gaunt(c.pf);
   for (int lev = g->nlevels - 2; lev >= 0; --lev) {
     int i0 = g->level_start_source_parent_box_nrs[lev];
@@ -548,6 +965,45 @@ static int h3_refine_locals(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
   h3ctx_t c;
   int rc = h3_ctx(kern, &c);
   if (rc) return rc;
+  if (c.sumpy) {
+    const h3tay_t* t = h3_taylor(c.pf);
+    const size_t NC = (size_t)t->D1 * t->D1 * t->D1;
+    for (int lev = 1; lev < g->nlevels; ++lev) {
+      int i0 = g->level_start_ttp_box_nrs[lev], i1 = g->level_start_ttp_box_nrs[lev + 1];
+      double sp = h3_scale(c.k, level_width(g, lev - 1)), sc = h3_scale(c.k, level_width(g, lev));
+#pragma omp parallel
+      {
+        cplx* work = malloc(sizeof(cplx) * (2 * NC + 2 * c.ncf));
+        cplx* P = work + NC;
+        cplx* bp = P + NC;
+        cplx* bc = bp + c.ncf;
+#pragma omp for schedule(dynamic, 4)
+        for (int i = i0; i < i1; ++i) {
+          int b = g->target_or_target_parent_boxes[i];
+          int par = g->box_parent_ids[b];
+          double cp[3], cc[3];
+          load(g->box_centers, g->nboxes, par, 3, cp);
+          load(g->box_centers, g->nboxes, b, 3, cc);
+          double vd[3] = {c.k * (cc[0] - cp[0]), c.k * (cc[1] - cp[1]), c.k * (cc[2] - cp[2])};
+          for (int r = 0; r < c.nrhs; ++r) {
+            const cplx* Lin = locals + ((size_t)par * c.nrhs + r) * c.ncf;
+            cplx* Lout = locals + ((size_t)b * c.nrhs + r) * c.ncf;
+            for (int n = 0; n <= c.pf; ++n)
+              for (int m = -n; m <= n; ++m) {
+                bp[H3Q(n, m)] = Lin[H3Q(n, m)] * pow(sp, -n);
+                bc[H3Q(n, m)] = 0;
+              }
+            h3t_local_monomials(t, bp, P);
+            h3t_l2l(t, t, vd, P, bc, work);
+            for (int n = 0; n <= c.pf; ++n)
+              for (int m = -n; m <= n; ++m) Lout[H3Q(n, m)] += bc[H3Q(n, m)] * pow(sc, n);
+          }
+        }
+        free(work);
+      }
+    }
+    return 0;
+  }
   const h3gaunt_t* gt = h3_gaunt(c.pf);
   for (int lev = 1; lev < g->nlevels; ++lev) {
     int i0 = g->level_start_ttp_box_nrs[lev], i1 = g->level_start_ttp_box_nrs[lev + 1];
@@ -686,6 +1142,60 @@ static int h3_l2qbxl(const qbxfmm_kernel* kern, const qbxfmm_geometry* g, const 
   h3ctx_t c;
   int rc = h3_ctx(kern, &c);
   if (rc) return rc;
+  if (c.sumpy) {
+    const h3tay_t* tp = h3_taylor(c.pf);
+    const h3tay_t* tq = h3_taylor(c.pq);
+    const size_t NC = (size_t)tp->D1 * tp->D1 * tp->D1;
+    /* the monomials of every target box's local that holds a QBX center */
+    cplx* Pall = calloc((size_t)g->ntarget_boxes * c.nrhs * NC, sizeof(cplx));
+    char* need = calloc((size_t)g->ntarget_boxes, 1);
+    for (int ig = 0; ig < g->nglobal_qbx_centers; ++ig)
+      need[g->qbx_center_to_target_box[g->global_qbx_centers[ig]]] = 1;
+#pragma omp parallel
+    {
+      cplx* b = malloc(sizeof(cplx) * c.ncf);
+#pragma omp for schedule(dynamic, 4)
+      for (int itb = 0; itb < g->ntarget_boxes; ++itb) {
+        if (!need[itb]) continue;
+        int tb = g->target_boxes[itb];
+        double sb_ = h3_scale(c.k, level_width(g, g->box_levels[tb]));
+        for (int r = 0; r < c.nrhs; ++r) {
+          const cplx* Lin = locals + ((size_t)tb * c.nrhs + r) * c.ncf;
+          for (int n = 0; n <= c.pf; ++n)
+            for (int m = -n; m <= n; ++m) b[H3Q(n, m)] = Lin[H3Q(n, m)] * pow(sb_, -n);
+          h3t_local_monomials(tp, b, Pall + ((size_t)itb * c.nrhs + r) * NC);
+        }
+      }
+      free(b);
+    }
+#pragma omp parallel
+    {
+      cplx* work = malloc(sizeof(cplx) * (NC + c.ncq));
+      cplx* bq = work + NC;
+#pragma omp for schedule(dynamic, 16)
+      for (int ig = 0; ig < g->nglobal_qbx_centers; ++ig) {
+        int ctr = g->global_qbx_centers[ig];
+        int itb = g->qbx_center_to_target_box[ctr];
+        int tb = g->target_boxes[itb];
+        double cc[3], cb[3];
+        load(g->centers, g->ncenters, ctr, 3, cc);
+        load(g->box_centers, g->nboxes, tb, 3, cb);
+        double sc = h3_scale(c.k, g->expansion_radii[ctr]);
+        double vd[3] = {c.k * (cc[0] - cb[0]), c.k * (cc[1] - cb[1]), c.k * (cc[2] - cb[2])};
+        for (int r = 0; r < c.nrhs; ++r) {
+          for (int i = 0; i < c.ncq; ++i) bq[i] = 0;
+          h3t_l2l(tp, tq, vd, Pall + ((size_t)itb * c.nrhs + r) * NC, bq, work);
+          cplx* L = qbx_exps + ((size_t)ctr * c.nrhs + r) * c.ncq;
+          for (int n = 0; n <= c.pq; ++n)
+            for (int m = -n; m <= n; ++m) L[H3Q(n, m)] += bq[H3Q(n, m)] * pow(sc, n);
+        }
+      }
+      free(work);
+    }
+    free(Pall);
+    free(need);
+    return 0;
+  }
   const h3gaunt_t* gt = h3_gaunt(c.pf);
 #pragma omp parallel
   {

@@ -15,6 +15,10 @@ import numpy as np
 QBXFMM_LAPLACE = 0
 QBXFMM_HELMHOLTZ = 1
 
+QBXFMM_BACKEND_SUMPY = 0    # the reference's default expansions (sumpy)
+QBXFMM_BACKEND_FMMLIB = 1   # spherical-wave expansions (the reference's fmmlib backend)
+FMM_BACKENDS = {"sumpy": QBXFMM_BACKEND_SUMPY, "fmmlib": QBXFMM_BACKEND_FMMLIB}
+
 QBXFMM_OK = 0
 QBXFMM_ERR_ARG = -1
 QBXFMM_ERR_CUDA = -2
@@ -34,7 +38,7 @@ class QBXFMMKernel(ctypes.Structure):
         ("charge_coeff_re", _f64), ("charge_coeff_im", _f64),
         ("dipole_coeff_re", _f64), ("dipole_coeff_im", _f64),
         ("qbx_order", _i32), ("fmm_order", _i32), ("nrhs", _i32),
-        ("precision", _i32), ("target_specific_qbx", _i32),
+        ("precision", _i32), ("target_specific_qbx", _i32), ("fmm_backend", _i32),
     ]
 
 
@@ -418,12 +422,18 @@ def make_geometry_struct(scalars: dict, arrays: dict, ptr_of) -> QBXFMMGeometry:
 
 def make_kernel_struct(*, family, dim, qbx_order, fmm_order, nrhs=1, k=0.0,
                        charge_coeff=0.0, dipole_coeff=0.0, precision=0,
-                       target_specific_qbx=False) -> QBXFMMKernel:
+                       target_specific_qbx=False, fmm_backend="sumpy") -> QBXFMMKernel:
+    """``fmm_backend``: "sumpy" (the reference's default) or "fmmlib", the reference
+    backend whose expansion truncation the apply reproduces (differs for 3D
+    Helmholtz only)."""
     k = complex(k)
     cc = complex(charge_coeff)
     dc = complex(dipole_coeff)
+    if fmm_backend not in FMM_BACKENDS:
+        raise ValueError(f"fmm_backend must be one of {sorted(FMM_BACKENDS)}, not {fmm_backend!r}")
     return QBXFMMKernel(family, dim, k.real, k.imag, cc.real, cc.imag, dc.real, dc.imag,
-                        qbx_order, fmm_order, nrhs, precision, int(bool(target_specific_qbx)))
+                        qbx_order, fmm_order, nrhs, precision, int(bool(target_specific_qbx)),
+                        FMM_BACKENDS[fmm_backend])
 
 
 def ncoeff(family: int, dim: int, order: int) -> int:

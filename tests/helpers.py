@@ -55,13 +55,13 @@ def workload(name: str):
     raise KeyError(name)
 
 
-def oracle_for(wl, nrhs=None):
+def oracle_for(wl, nrhs=None, fmm_backend="sumpy"):
     from oracle.oracle import Oracle
     sp = wl.spec
     return Oracle(wl.geometry(), dim=sp.kernel.dim, qbx_order=wl.qbx_order,
                   fmm_order=wl.fmm_order, nrhs=nrhs or wl.nrhs,
                   charge_coeff=sp.charge_coeff, dipole_coeff=sp.dipole_coeff,
-                  family=sp.kernel.family, k=sp.wave_number)
+                  family=sp.kernel.family, k=sp.wave_number, fmm_backend=fmm_backend)
 
 
 def relerr(a, b):

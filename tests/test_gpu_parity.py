@@ -251,8 +251,9 @@ def test_near_field_matches_reference_tsqbx_golden(op):
 
 @pytest.mark.parametrize("op", ["S", "D"])
 def test_helmholtz3d_near_field_matches_reference_tsqbx_golden(op):
-    """3D Helmholtz: P2QBXL + QBXL2P and the target-specific kernel on the GPU against
-    the reference TSQBX module's output (k = 2.5, complex strengths)."""
+    """3D Helmholtz (fmmlib truncation): P2QBXL + QBXL2P and the target-specific
+    kernel on the GPU against the reference TSQBX module's output (k = 2.5, complex
+    strengths)."""
     z = golden_tsqbx("helmholtz3d")
     scalars, arrays = golden_geometry(z)
     arrays["m2m_group_starts"] = np.zeros(9, np.int32)
@@ -269,9 +270,11 @@ def test_helmholtz3d_near_field_matches_reference_tsqbx_golden(op):
     L = native.lib()
     for q in z["orders"]:
         q = int(q)
+        # the reference's target-specific module evaluates the spherical-wave (fmmlib
+        # backend) truncation
         k = abi.make_kernel_struct(family=abi.QBXFMM_HELMHOLTZ, dim=3, qbx_order=q, fmm_order=6,
                                    k=float(z["k"]), charge_coeff=float(op == "S"),
-                                   dipole_coeff=float(op == "D"))
+                                   dipole_coeff=float(op == "D"), fmm_backend="fmmlib")
         h = ctypes.c_void_p()
         native.check("plan", L.qbxfmm_plan_create(ctypes.byref(k), ctypes.byref(g),
                                                   ctypes.byref(h)))

@@ -56,9 +56,11 @@ def test_oracle_matches_reference_tsqbx_helmholtz3d(op):
     mask = np.zeros(scalars["ntargets"], bool)
     mask[z["center_to_targets_lists"]] = True
     for q in z["orders"]:
+        # the reference's target-specific module evaluates the spherical-wave
+        # (fmmlib backend) truncation
         k = abi.make_kernel_struct(family=abi.QBXFMM_HELMHOLTZ, dim=3, qbx_order=int(q),
                                    fmm_order=6, k=float(z["k"]), charge_coeff=float(op == "S"),
-                                   dipole_coeff=float(op == "D"))
+                                   dipole_coeff=float(op == "D"), fmm_backend="fmmlib")
         nc = abi.ncoeff(abi.QBXFMM_HELMHOLTZ, 3, int(q))
         qe = np.zeros((scalars["ncenters"], 1, nc), np.complex128)
         pt = np.zeros((1, scalars["ntargets"]), np.complex128)
@@ -103,16 +105,38 @@ def test_oracle_helmholtz3d_special_functions():
             assert abs(Y[nn * nn + nn + m] - ref) < 1e-13
 
 
-@pytest.mark.parametrize("name,tol", [("2d-S", 1e-6), ("2d-D", 5e-6), ("3d-S-small", 1e-5),
-                                      ("3d-D-small", 1e-5), ("h3d-CF-small", 1e-5),
-                                      ("h3d-S-small", 1e-6), ("h3d-D-small", 3e-3)])
-def test_oracle_fmm_vs_direct_qbx(name, tol):
+@pytest.mark.parametrize("name,tol,backend", [
+    ("2d-S", 1e-6, "sumpy"), ("2d-D", 5e-6, "sumpy"), ("3d-S-small", 1e-5, "sumpy"),
+    ("3d-D-small", 1e-5, "sumpy"),
+    # 3D Helmholtz: the spherical-wave (fmmlib) truncation, and the reference's default
+    # compressed Taylor one, whose box expansions need p well above k times the box
+    # size (the remainder of e^{ik a.x} at order p is (k|a|)^(p+1) / (p+1)!)
+    ("h3d-CF-small", 1e-5, "fmmlib"), ("h3d-S-small", 1e-6, "fmmlib"),
+    ("h3d-D-small", 3e-3, "fmmlib"),
+    ("h3d-CF-small", 1e-3, "sumpy"), ("h3d-S-small", 3e-7, "sumpy"),
+    ("h3d-D-small", 0.2, "sumpy")])
+def test_oracle_fmm_vs_direct_qbx(name, tol, backend):
     wl = workload(name)
-    o = oracle_for(wl)
+    o = oracle_for(wl, fmm_backend=backend)
     s = wl.tree_strengths()
     a = o.apply(s)
     b = o.apply_direct(s)
     assert relerr(a, b) < tol
+
+
+def test_oracle_taylor_fmm_converges_with_order():
+    """3D Helmholtz in the reference's default truncation: the FMM approaches the
+    direct QBX sum as the FMM order grows (k = 4, boxes up to k rho ~ 4)."""
+    from pytential_b200.workloads import helmholtz3d_ellipsoid
+    errs = []
+    for p in (8, 12, 16):
+        wl = helmholtz3d_ellipsoid(nrefine=1, k=4.0, nrhs=1, op="D", qbx_order=2,
+                                   fmm_order=p, nshell=100)
+        o = oracle_for(wl)
+        s = wl.tree_strengths()
+        errs.append(relerr(o.apply(s), o.apply_direct(s)))
+    assert errs[0] > 20 * errs[1] > 400 * errs[2], errs
+    assert errs[2] < 1e-4, errs
 
 
 def test_oracle_linearity():
