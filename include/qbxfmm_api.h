@@ -192,14 +192,17 @@ int qbxfmm_laplace2d_qbx_matrix(int nsources, const double* sources, const doubl
                                 void* stream);
 
 /* The same for the 3D Helmholtz layer potential (complex128 K, structure-of-arrays
- * [3][n], e^{ik r} / (4 pi r); QBX targets through the spherical-wave series of order
- * qbx_order <= 8 of the target-specific near field). */
+ * [3][n], e^{ik r} / (4 pi r); QBX targets through the series of order qbx_order <= 8
+ * of the target-specific near field, in the truncation of fmm_backend:
+ * QBXFMM_BACKEND_SUMPY (the reference's default: the degree-qbx_order Taylor
+ * polynomial about the center, j_n cut to its power series) or QBXFMM_BACKEND_FMMLIB
+ * (the spherical-wave series). */
 int qbxfmm_helmholtz3d_qbx_matrix(int nsources, const double* sources, const double* normals,
                                   double k, double charge_re, double charge_im,
                                   double dipole_re, double dipole_im, int ntargets,
                                   const double* targets, const int32_t* target_center,
-                                  int ncenters, const double* centers, int qbx_order, void* K,
-                                  void* stream);
+                                  int ncenters, const double* centers, int qbx_order,
+                                  int fmm_backend, void* K, void* stream);
 
 /* Target-to-QBX-center association (replaces pytential's QBXTargetAssociator:
  * marking, pytential/qbx/target_assoc.py:544-633, and center finding, 243-363 and

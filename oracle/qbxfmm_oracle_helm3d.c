@@ -1323,6 +1323,55 @@ static int h3_apply(const qbxfmm_kernel* kern, const qbxfmm_geometry* g, const c
   return 0;
 }
 
+/* The same recurrences at a complex argument (Miller's backward recurrence for j_n,
+ * normalized with j_0 = sin z / z or j_1; h_n upward from h_0, h_1), for the
+ * reference's own golden values of its spherical Bessel / Hankel routines. */
+static void h3_sph_j_complex(int N, cplx z, cplx* jv)
+{
+  for (int n = 0; n <= N; ++n) jv[n] = 0.0;
+  double az = cabs(z);
+  if (az == 0.0) {
+    jv[0] = 1.0;
+    return;
+  }
+  int nmax = N > (int)az ? N : (int)az;
+  int start = nmax + 16 + (int)sqrt(40.0 * (nmax + 1));
+  cplx fp1 = 0.0, f = 1e-200, f1 = 0.0;
+  for (int n = start; n >= 1; --n) {
+    cplx fm1 = (2.0 * n + 1.0) / z * f - fp1;
+    fp1 = f;
+    f = fm1;
+    if (n - 1 <= N) jv[n - 1] = f;
+    if (n - 1 == 1) f1 = f;
+    if (cabs(f) > 1e200) {
+      f *= 1e-200;
+      fp1 *= 1e-200;
+      f1 *= 1e-200;
+      for (int j = n - 1; j <= N; ++j) jv[j] *= 1e-200;
+    }
+  }
+  cplx sz = csin(z), cz = ccos(z);
+  cplx scale = (az < 1.0 || cabs(sz) >= 0.5) ? (sz / z) / f : ((sz / z - cz) / z) / f1;
+  for (int n = 0; n <= N; ++n) jv[n] *= scale;
+}
+
+static void h3_sph_h_complex(int N, cplx z, cplx* hv)
+{
+  cplx e = cexp(I * z);
+  hv[0] = -I * e / z;
+  if (N >= 1) hv[1] = -e * (z + I) / (z * z);
+  for (int n = 1; n < N; ++n) hv[n + 1] = (2.0 * n + 1.0) / z * hv[n] - hv[n - 1];
+}
+
+void orc_h3_sph_j_complex(int N, double zr, double zi, cplx* out)
+{
+  h3_sph_j_complex(N, zr + I * zi, out);
+}
+void orc_h3_sph_h_complex(int N, double zr, double zi, cplx* out)
+{
+  h3_sph_h_complex(N, zr + I * zi, out);
+}
+
 /* test hooks: special functions and wave tables */
 void orc_h3_sph_j(int N, double x, double* out) { h3_sph_j(N, x, out); }
 void orc_h3_sph_h(int N, double x, cplx* out) { h3_sph_h(N, x, out); }

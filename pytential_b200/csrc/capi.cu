@@ -18,6 +18,7 @@
 
 #include "../../include/qbxfmm_api.h"
 #include "kernels.h"
+#include "taylor_h3.h"
 
 using namespace qbx;
 
@@ -43,6 +44,9 @@ struct qbxfmm_plan {
   // rotation tables; then the device-built direction and coaxial tables
   std::vector<double> h3m2l;
   int h3_ndir = 0, h3_ncoax = 0;
+  // 3D Helmholtz in the reference's default truncation (hc.taylor): monomial tables
+  // of the box (order p) and QBX (order q) expansions
+  H3TaylorHost h3tp, h3tq;
   // 3D Helmholtz: translation buffer and pair scratch registered by
   // qbxfmm_precompute_translations, used by the translation stage entries
   mutable const double* trans_dev = nullptr;
@@ -91,20 +95,24 @@ size_t h3_rot_offset(const qbxfmm_plan* p);
 
 // Offsets in doubles of the 3D Helmholtz sections of the translation buffer, after
 // the M2M / L2L matrices: [0] Gaunt table, [1] rotation tables, [2] host M2L tables,
-// [3] M2L direction tables, [4] M2L coaxial tables (complex), [5] end.
-void h3_layout(const qbxfmm_plan* p, size_t o[6])
+// [3] M2L direction tables, [4] M2L coaxial tables (complex), [5] G0 of the order-p
+// monomial tables and [6] Ginv of the order-q ones (complex; the reference's default
+// truncation only, else empty), [7] end.
+void h3_layout(const qbxfmm_plan* p, size_t o[8])
 {
   o[0] = p->tc.nmatrices * p->tc.rp * p->tc.kp;
   o[1] = o[0] + p->h3gaunt.size();
   o[2] = (o[1] + p->h3rot.size() + 1) & ~(size_t)1;
   o[3] = o[2] + p->h3m2l.size();
   o[4] = o[3] + (size_t)p->h3_ndir * h3_m2l_dsize(p->kern.fmm_order);
-  o[5] = o[4] + 2 * (size_t)p->h3_ncoax * h3_m2l_csize(p->kern.fmm_order);
+  o[5] = (o[4] + 2 * (size_t)p->h3_ncoax * h3_m2l_csize(p->kern.fmm_order) + 1) & ~(size_t)1;
+  o[6] = o[5] + 2 * p->h3tp.G0.size();
+  o[7] = o[6] + 2 * p->h3tq.Ginv.size();
 }
 
 size_t h3_rot_offset(const qbxfmm_plan* p)
 {
-  size_t o[6];
+  size_t o[8];
   h3_layout(p, o);
   return o[1];
 }
@@ -359,8 +367,10 @@ int qbxfmm_plan_create(const qbxfmm_kernel* kernel, const qbxfmm_geometry* geome
   if (k.nrhs < 1) return fail(QBXFMM_ERR_ARG, "nrhs must be >= 1");
   if (k.precision != 0 && k.precision != 1)
     return fail(QBXFMM_ERR_ARG, "precision must be 0 (FP64) or 1 (mixed)");
-  if (k.precision == 1 && !(k.family == QBXFMM_LAPLACE && k.dim == 3))
-    return fail(QBXFMM_ERR_UNSUPPORTED, "the mixed-precision form is built for 3D Laplace");
+  if (k.fmm_backend != QBXFMM_BACKEND_SUMPY && k.fmm_backend != QBXFMM_BACKEND_FMMLIB)
+    return fail(QBXFMM_ERR_ARG, "fmm_backend must be QBXFMM_BACKEND_SUMPY or QBXFMM_BACKEND_FMMLIB");
+  if (k.precision == 1 && k.dim != 3)
+    return fail(QBXFMM_ERR_UNSUPPORTED, "the mixed-precision form is built for 3D Laplace and 3D Helmholtz");
   if (k.family == QBXFMM_HELMHOLTZ && k.dim == 3) {
     if (k.qbx_order > 5 || k.qbx_order > k.fmm_order)
       return fail(QBXFMM_ERR_UNSUPPORTED, "3D Helmholtz: qbx_order must be <= min(5, fmm_order)");
@@ -405,6 +415,15 @@ int qbxfmm_plan_create(const qbxfmm_kernel* kernel, const qbxfmm_geometry* geome
   if (p->h3 && !p->trans_ok) {
     delete p;
     return fail(QBXFMM_ERR_UNSUPPORTED, "3D Helmholtz: translation matrices unsupported for this order");
+  }
+  p->hc.taylor = p->h3 && k.fmm_backend == QBXFMM_BACKEND_SUMPY;
+  if (p->hc.taylor) {
+    p->h3tp = h3_taylor_host(k.fmm_order);
+    p->h3tq = h3_taylor_host(k.qbx_order);
+    if (p->h3tp.p < 0 || p->h3tq.p < 0) {
+      delete p;
+      return fail(QBXFMM_ERR_UNSUPPORTED, "3D Helmholtz: singular Taylor basis table");
+    }
   }
   if (p->h3) {
     p->h3gaunt = h3_gaunt_table(k.fmm_order);
@@ -556,7 +575,7 @@ int qbxfmm_multipole_to_local(const qbxfmm_plan* p, const void* mpoles, void* lo
   if (p->h3) {
     if (!p->trans_dev)
       return fail(QBXFMM_ERR_ARG, "3D Helmholtz: call qbxfmm_precompute_translations first");
-    size_t o[6];
+    size_t o[8];
     h3_layout(p, o);
     const int nm = 2 * p->kern.fmm_order + 1;
     const double* clsmap = p->trans_dev + o[2] + (size_t)nm * nm * 4 + 4 * (size_t)p->h3_ndir +
@@ -564,7 +583,7 @@ int qbxfmm_multipole_to_local(const qbxfmm_plan* p, const void* mpoles, void* lo
     QBX_TRY(h3_launch_m2l_rot(p->geo, p->kern.fmm_order, p->kern.nrhs, (const double2*)mpoles,
                               (double2*)locals, p->trans_dev + o[3],
                               reinterpret_cast<const double2*>(p->trans_dev + o[4]), clsmap,
-                              error_word, S(stream)),
+                              error_word, S(stream), p->mixed),
             "multipole_to_local");
     return QBXFMM_OK;
   }
@@ -700,7 +719,7 @@ int qbxfmm_translate_box_multipoles_to_qbx_local(const qbxfmm_plan* p, const voi
     QBX_TRY(h3_launch_m2qbxl(p->geo, p->hc, p->kern.fmm_order, p->kern.qbx_order, p->kern.nrhs,
                              (const double2*)mpoles,
                              p->trans_dev + h3_rot_offset(p),
-                             (double2*)qbx_exps, error_word, S(stream)),
+                             (double2*)qbx_exps, error_word, S(stream), p->mixed),
             "translate_box_multipoles_to_qbx_local");
     return QBXFMM_OK;
   }
@@ -726,6 +745,17 @@ int qbxfmm_translate_box_local_to_qbx_local(const qbxfmm_plan* p, const void* lo
   if (p->h3) {
     if (!p->trans_dev)
       return fail(QBXFMM_ERR_ARG, "3D Helmholtz: call qbxfmm_precompute_translations first");
+    if (p->hc.taylor) {
+      size_t o[8];
+      h3_layout(p, o);
+      QBX_TRY(h3_launch_l2qbxl_taylor(p->geo, p->hc, p->kern.fmm_order, p->kern.qbx_order,
+                                      p->kern.nrhs, (const double2*)locals,
+                                      reinterpret_cast<const double2*>(p->trans_dev + o[5]),
+                                      reinterpret_cast<const double2*>(p->trans_dev + o[6]),
+                                      (double2*)qbx_exps, nullptr, S(stream)),
+              "translate_box_local_to_qbx_local");
+      return QBXFMM_OK;
+    }
     QBX_TRY(h3_launch_l2qbxl(p->geo, p->hc, p->kern.fmm_order, p->kern.qbx_order, p->kern.nrhs,
                              (const double2*)locals,
                              p->trans_dev + h3_rot_offset(p),
@@ -818,9 +848,9 @@ int qbxfmm_workspace_sizes(const qbxfmm_plan* p, size_t* sizes6 /* 8 entries */)
   if (int rc = qbx::plan_base_workspace_sizes(p, sizes6)) return rc;
   if (p->trans_ok) {
     int npairs = std::max(p->th.m2l_npairs, g.m2m_npairs);
-    size_t o[6];
+    size_t o[8];
     h3_layout(p, o);
-    sizes6[6] = p->h3 ? o[5] * sizeof(double)
+    sizes6[6] = p->h3 ? o[7] * sizeof(double)
                       : trans_matrix_bytes(p->tc) + (p->tf32_ok ? tf32_matrix_bytes(p->tc) : 0);
     sizes6[7] = p->h3 ? 0 : trans_scratch_bytes(p->tc, npairs, p->kern.nrhs);
   } else {
@@ -837,7 +867,7 @@ int qbxfmm_precompute_translations(const qbxfmm_plan* p, const qbxfmm_workspace*
     if (!ws->translations)
       return fail(QBXFMM_ERR_ARG, "3D Helmholtz needs the translations buffer");
     double* T = (double*)ws->translations;
-    size_t o[6];
+    size_t o[8];
     h3_layout(p, o);
     const int pf = p->kern.fmm_order, q = p->kern.qbx_order, nm = 2 * pf + 1;
     double* G = T + o[0];
@@ -852,8 +882,24 @@ int qbxfmm_precompute_translations(const qbxfmm_plan* p, const qbxfmm_workspace*
     QBX_TRY(cudaMemcpyAsync(H, p->h3m2l.data(), p->h3m2l.size() * sizeof(double),
                             cudaMemcpyHostToDevice, S(stream)),
             "precompute_translations: M2L tables");
-    QBX_TRY(h3_launch_trans_build(p->geo, p->tc, p->kern.k_re, G, T, S(stream)),
-            "precompute_translations");
+    if (p->hc.taylor) {
+      // M2M / L2L of the reference's default truncation, built on the host; the monomial
+      // tables the L2QBXL kernel reads
+      QBX_TRY(h3_taylor_translations(p->h3tp, p->tc, p->kern.k_re, p->geo.root_extent,
+                                     p->geo.nlevels, T, S(stream)),
+              "precompute_translations: Taylor M2M / L2L");
+      QBX_TRY(cudaMemcpyAsync(T + o[5], p->h3tp.G0.data(), p->h3tp.G0.size() * sizeof(double2),
+                              cudaMemcpyHostToDevice, S(stream)),
+              "precompute_translations: Taylor tables");
+      QBX_TRY(cudaMemcpyAsync(T + o[6], p->h3tq.Ginv.data(),
+                              p->h3tq.Ginv.size() * sizeof(double2), cudaMemcpyHostToDevice,
+                              S(stream)),
+              "precompute_translations: Taylor tables");
+      QBX_TRY(cudaStreamSynchronize(S(stream)), "precompute_translations");
+    } else {
+      QBX_TRY(h3_launch_trans_build(p->geo, p->tc, p->kern.k_re, G, T, S(stream)),
+              "precompute_translations");
+    }
     // rotation-table layout (h3_rotation_tables): start values, then isq, then rt
     const double* isq = R + (size_t)nm * (q + 1) * 4;
     const double* rt = isq + (size_t)(pf + 2) * (pf + 1);

@@ -67,6 +67,27 @@ QBX_HD float2 faxpy(float s, float2 a, float2 acc) { return f2(fmaf(s, a.x, acc.
 QBX_HD float2 tof(double2 a) { return f2((float)a.x, (float)a.y); }
 QBX_HD double2 tod(float2 a) { return c2((double)a.x, (double)a.y); }
 
+// the double2 names for float2, so that kernels templated on the real type R (and
+// its complex type, cplx_t<R>) read the same in both precisions
+QBX_HD float2 cadd(float2 a, float2 b) { return fadd(a, b); }
+QBX_HD float2 cscale(float s, float2 a) { return fscale(s, a); }
+QBX_HD float2 cconj(float2 a) { return fconj(a); }
+QBX_HD float2 cmul(float2 a, float2 b) { return fmul(a, b); }
+QBX_HD float2 cfma(float2 a, float2 b, float2 acc) { return ffma(a, b, acc); }
+QBX_HD float2 caxpy(float s, float2 a, float2 acc) { return faxpy(s, a, acc); }
+
+template <typename R> struct cplx_of;
+template <> struct cplx_of<double> { using type = double2; };
+template <> struct cplx_of<float> { using type = float2; };
+template <typename R> using cplx_t = typename cplx_of<R>::type;
+template <typename R> QBX_HD cplx_t<R> cmake(R re, R im = R(0));
+template <> QBX_HD double2 cmake<double>(double re, double im) { return c2(re, im); }
+template <> QBX_HD float2 cmake<float>(float re, float im) { return f2(re, im); }
+QBX_HD double2 cto(double2 a, double2) { return a; }
+QBX_HD float2 cto(double2 a, float2) { return tof(a); }
+QBX_HD double2 c2d(double2 a) { return a; }
+QBX_HD double2 c2d(float2 a) { return tod(a); }
+
 // }}}
 
 QBX_HD int idx3(int n, int m) { return n * (n + 1) / 2 + m; }
@@ -115,6 +136,8 @@ struct HelmCoeffs {
   double2 cq;
   double2 cd;
   double k;
+  int taylor = 0;   // 3D: the reference's default truncation (sumpy's compressed Taylor
+                    // expansions: regular waves with j_n cut to its power series)
 };
 
 }  // namespace qbx

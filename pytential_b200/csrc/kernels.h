@@ -166,12 +166,14 @@ cudaError_t h3_launch_m2l_tables(int pf, int ndir, int ncoax, const double* dirs
                                  double2* Ctab, cudaStream_t st);
 cudaError_t h3_launch_m2l_rot(const qbxfmm_geometry& g, int pf, int nrhs, const double2* mp,
                               double2* lo, const double* Dtab, const double2* Ctab,
-                              const double* clsmap, int32_t* err, cudaStream_t st);
+                              const double* clsmap, int32_t* err, cudaStream_t st,
+                              bool fp32 = false);
 // rot: rotation tables of h3_rotation_tables (start values, recurrence factors,
 // lambda = 0 Gaunt slice)
+// fp32: the mixed-precision form (FP32 arithmetic, FP64 expansions in and out)
 cudaError_t h3_launch_m2qbxl(const qbxfmm_geometry& g, HelmCoeffs hc, int pf, int q, int nrhs,
                              const double2* mp, const double* rot, double2* qe, int32_t* err,
-                             cudaStream_t st);
+                             cudaStream_t st, bool fp32 = false);
 cudaError_t h3_launch_l2qbxl(const qbxfmm_geometry& g, HelmCoeffs hc, int pf, int q, int nrhs,
                              const double2* lo, const double* rot, double2* qe, int32_t* err,
                              cudaStream_t st);

@@ -19,6 +19,7 @@
 #include <cooperative_groups.h>
 
 #include <string>
+#include <type_traits>
 
 #include "../../include/qbxfmm_api.h"
 #include "laplace.cuh"
@@ -112,6 +113,30 @@ QBX_D void h3_sph_j(int N, double x, double* jv)
   sincos(x, &s, &c);
   double scale = (x < 1.0 || fabs(s) >= 0.5) ? (s * xi) / f : ((s * xi - c) * xi) / f1;
   for (int n = 0; n <= N; ++n) jv[n] *= scale;
+}
+
+// j_n^[T](x) = sum_{j: n + 2j <= T} (-x^2/2)^j x^n / (j! (2n+2j+1)!!), n <= N: the
+// power series of j_n cut at total degree T (zero for n > T); T < 0: j_n itself.  The
+// degree-T Taylor polynomial of sum L_nm j_n(k|v|) Y_n^m(v) is sum L_nm j_n^[T] Y_n^m.
+QBX_D void h3_sph_j_cut(int N, double x, int T, double* jv)
+{
+  if (T < 0) {
+    h3_sph_j(N, x, jv);
+    return;
+  }
+  double xn = 1.0, dfac = 1.0, mx2 = -0.5 * x * x;
+  for (int n = 0; n <= N; ++n) {
+    if (n > 0) {
+      xn *= x;
+      dfac *= 2.0 * n + 1.0;
+    }
+    double term = xn / dfac, acc = 0.0;
+    for (int j = 0; n + 2 * j <= T; ++j) {
+      acc += term;
+      term *= mx2 * rcp(j + 1) * rcp(2 * n + 2 * j + 3);
+    }
+    jv[n] = acc;
+  }
 }
 
 // h_n(x) = j_n(x) + i y_n(x), n <= N, by the upward recurrence
@@ -307,6 +332,11 @@ k_h3_p2e(qbxfmm_geometry g, HelmCoeffs hc, int p, int nrhs, const double2* __res
   double c[3];
   load_point<3>(g.box_centers, g.nboxes, b, c);
   const bool dip = hc.cd.x != 0.0 || hc.cd.y != 0.0;
+  // the reference's default multipoles (moments of degree <= p): the charge row from
+  // j_n^[p], the normal derivative from j_n^[p-1] (a second table)
+  const bool two = !LOCAL && hc.taylor && dip;
+  double2* tab2 = two ? rec + (size_t)(N + 1) * (N + 2) / 2 : tab;   // [(N+1)^2][TS]
+  double2* rad2 = two ? tab2 + (size_t)(N + 1) * (N + 1) * TS : nullptr;   // [SUB][N+2]
   h3_rec_table(N, rec, threadIdx.x, NT);
 
   int o_c[H3_NH];
@@ -360,8 +390,12 @@ k_h3_p2e(qbxfmm_geometry g, HelmCoeffs hc, int p, int nrhs, const double2* __res
           h3_sph_h(N, x, s_rad[j]);
         } else {
           double jv[H3_LMAX + 2];
-          h3_sph_j(N, x, jv);
+          h3_sph_j_cut(N, x, hc.taylor ? p : -1, jv);
           for (int n = 0; n <= N; ++n) s_rad[j][n] = c2(jv[n]);
+          if (two) {
+            h3_sph_j_cut(N, x, p - 1, jv);
+            for (int n = 0; n <= N; ++n) rad2[j * (N + 2) + n] = c2(jv[n]);
+          }
         }
 #pragma unroll
         for (int rr = 0; rr < RB; ++rr)
@@ -378,6 +412,7 @@ k_h3_p2e(qbxfmm_geometry g, HelmCoeffs hc, int p, int nrhs, const double2* __res
       for (int wk = threadIdx.x; wk < cnt * (N + 1); wk += NT) {
         int m = wk / cnt, j = wk - m * cnt;
         h3_wave_column(m, N, s_t[j], s_w[j], rec, s_rad[j], tab + j, TS);
+        if (two) h3_wave_column(m, N, s_t[j], s_w[j], rec, rad2 + j * (N + 2), tab2 + j, TS);
       }
       __syncthreads();
 #pragma unroll
@@ -387,6 +422,7 @@ k_h3_p2e(qbxfmm_geometry g, HelmCoeffs hc, int p, int nrhs, const double2* __res
           const double2* T = tab + j;
           double2 kr = cmul(hc.cq, T[o_c[h]]);
           if (dip) {
+            T = tab2 + j;
             const Ladder& L = lad[h];
             double2 vz = caxpy(L.w[0], T[L.o[0]], cscale(L.w[1], T[L.o[1]]));
             double2 vp = caxpy(L.w[2], T[L.o[2]], cscale(L.w[3], T[L.o[3]]));
@@ -523,8 +559,9 @@ k_h3_eval_direct(qbxfmm_geometry g, HelmCoeffs hc, int nrhs, const double2* __re
 
 // Evaluate an expansion (order p, scale s) of box b at point x: multipole (singular
 // waves, coefficient * s^n) or local (regular waves, coefficient / s^n).
+// (local: jcut >= 0 cuts j_n at total degree jcut, the reference's default truncation)
 QBX_D double2 h3_e2p(const double2* E, int p, bool local, double k, double s, const double* cb,
-                     const double* x, const double2* rec)
+                     const double* x, const double2* rec, int jcut = -1)
 {
   double u[3] = {x[0] - cb[0], x[1] - cb[1], x[2] - cb[2]};
   double2 w;
@@ -533,7 +570,7 @@ QBX_D double2 h3_e2p(const double2* E, int p, bool local, double k, double s, co
   double2 rad[H3_LMAX + 2];
   if (local) {
     double jv[H3_LMAX + 2];
-    h3_sph_j(p, k * rr, jv);
+    h3_sph_j_cut(p, k * rr, jcut, jv);
     double f = 1.0, si = 1.0 / s;
     for (int n = 0; n <= p; ++n, f *= si) rad[n] = c2(jv[n] * f);
   } else {
@@ -639,7 +676,8 @@ k_h3_eval_locals(qbxfmm_geometry g, HelmCoeffs hc, int p, int nrhs,
   load_point<3>(g.box_centers, g.nboxes, tb, cb);
   double s = h3_scale(hc.k, level_width(g, g.box_levels[tb]));
   const int ncf = (p + 1) * (p + 1);
-  double2 v = h3_e2p(locals + ((size_t)tb * nrhs + r) * ncf, p, true, hc.k, s, cb, x, rec);
+  double2 v = h3_e2p(locals + ((size_t)tb * nrhs + r) * ncf, p, true, hc.k, s, cb, x, rec,
+                     hc.taylor ? p : -1);
   double2* P = pot + (size_t)r * g.nfiltered_targets + t;
   *P = cadd(*P, v);
 }
@@ -817,12 +855,16 @@ QBX_D void h3_dmma(double& d0, double& d1, double a, double b)
 constexpr int H3_ROT_ZS = 8;
 constexpr int H3_ROT_SLOTS = 7;   // recurrence tasks per lane: (2 pf + 1)(Q + 1) <= 7 x 32
 
-template <bool FROM_LOCAL, int Q, int RB>
+template <typename R, bool FROM_LOCAL, int Q, int RB>
 __global__ void __launch_bounds__(NT)
 k_h3_e2qbxl_rot(qbxfmm_geometry g, HelmCoeffs hc, int pf, int nrhs,
                 const double2* __restrict__ exps, const double* __restrict__ rot,
                 double2* __restrict__ qbx_exps, int32_t* err)
 {
+  // R: the arithmetic (double, or float in the mixed-precision form; expansions are
+  // read and added in float64 either way)
+  using V = cplx_t<R>;
+  constexpr bool F64 = std::is_same<R, double>::value;
   constexpr int NCQ = (Q + 1) * (Q + 1);
   constexpr int NMU = 2 * Q + 1;
   constexpr int NOUT = (NCQ * RB + 31) / 32;
@@ -840,28 +882,28 @@ k_h3_e2qbxl_rot(qbxfmm_geometry g, HelmCoeffs hc, int pf, int nrhs,
   const double* g_rt = g_isq + nisq;                            // [pf+1][pf+1]
   const double* g0c = g_rt + nrt;                               // [NCQ][nl][Q+1]
   // CTA-wide
-  double2* Es = smem2;                                          // [ncf][RB]
-  double* s_isq = reinterpret_cast<double*>(Es + (size_t)ncf * RB);
-  double* s_rt = s_isq + nisq;
-  double* spow = s_rt + nrt;                                    // [nl]: s_box^{+-n}
+  V* Es = reinterpret_cast<V*>(smem2);                          // [ncf][RB]
+  R* s_isq = reinterpret_cast<R*>(Es + (size_t)ncf * RB);
+  R* s_rt = s_isq + nisq;
+  R* spow = s_rt + nrt;                                         // [nl]: s_box^{+-n}
   const size_t ctad = ((size_t)nisq + nrt + nl + 1) & ~(size_t)1;
-  double2* wbase = reinterpret_cast<double2*>(s_isq + ctad);
+  V* wbase = reinterpret_cast<V*>(s_isq + ctad);
   // per warp
   const size_t perd = ((size_t)nm * (Q + 1) + (size_t)NMU * NCQ + 2 * (size_t)nm + 1) / 2;
   const size_t per = (size_t)nm * NMU + NCQ + (size_t)NCQ * RB + (L + 2) + nm + perd;
   int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  double2* Dph = wbase + (size_t)warp * per;                    // [nm][NMU] slice x phase
-  double2* coaxn = Dph + (size_t)nm * NMU;                      // [NCQ] coaxial column n
-  double2* Lp = coaxn + NCQ;                                    // [NCQ][RB]
-  double2* rad = Lp + (size_t)NCQ * RB;                         // [L + 2]
-  double2* ph = rad + (L + 2);                                  // [nm]: e^{i m alpha}
-  double* Draw = reinterpret_cast<double*>(ph + nm);            // [nm][Q+1] d^n_{m mu>=0}
-  double* Tb = Draw + (size_t)nm * (Q + 1);                     // [NMU][NCQ]
-  double* chp = Tb + (size_t)NMU * NCQ;                         // [nm] cos(beta/2)^k
-  double* shp = chp + nm;                                       // [nm] sin(beta/2)^k
+  V* Dph = wbase + (size_t)warp * per;                          // [nm][NMU] slice x phase
+  V* coaxn = Dph + (size_t)nm * NMU;                            // [NCQ] coaxial column n
+  V* Lp = coaxn + NCQ;                                          // [NCQ][RB]
+  V* rad = Lp + (size_t)NCQ * RB;                               // [L + 2]
+  V* ph = rad + (L + 2);                                        // [nm]: e^{i m alpha}
+  R* Draw = reinterpret_cast<R*>(ph + nm);                      // [nm][Q+1] d^n_{m mu>=0}
+  R* Tb = Draw + (size_t)nm * (Q + 1);                          // [NMU][NCQ]
+  R* chp = Tb + (size_t)NMU * NCQ;                              // [nm] cos(beta/2)^k
+  R* shp = chp + nm;                                            // [nm] sin(beta/2)^k
 
   __shared__ unsigned char s_nof[(H3_MAXP + 1) * (H3_MAXP + 1)];   // order n of coefficient (n, m)
-  for (int x = threadIdx.x; x < nisq + nrt; x += NT) s_isq[x] = __ldg(g_isq + x);
+  for (int x = threadIdx.x; x < nisq + nrt; x += NT) s_isq[x] = (R)__ldg(g_isq + x);
   for (int n = 0; n <= pf; ++n)
     for (int x = n * n + threadIdx.x; x < (n + 1) * (n + 1); x += NT) s_nof[x] = (unsigned char)n;
   __syncthreads();
@@ -880,9 +922,9 @@ k_h3_e2qbxl_rot(qbxfmm_geometry g, HelmCoeffs hc, int pf, int nrhs,
   }
   double cc[3];
   load_point<3>(g.centers, g.ncenters, ctr, cc);
-  double2 acc[NOUT];
+  V acc[NOUT];
 #pragma unroll
-  for (int i = 0; i < NOUT; ++i) acc[i] = c2(0.0);
+  for (int i = 0; i < NOUT; ++i) acc[i] = cmake<R>(0);
 
   int nbox = FROM_LOCAL ? 1 : g.list3_starts[itb + 1] - g.list3_starts[itb];
   for (int bi = 0; bi < nbox; ++bi) {
@@ -897,14 +939,14 @@ k_h3_e2qbxl_rot(qbxfmm_geometry g, HelmCoeffs hc, int pf, int nrhs,
     __syncthreads();
     if (threadIdx.x == 0) {
       double f = 1.0, fs = FROM_LOCAL ? 1.0 / sb : sb;
-      for (int n = 0; n < nl; ++n, f *= fs) spow[n] = f;
+      for (int n = 0; n < nl; ++n, f *= fs) spow[n] = (R)f;
     }
     __syncthreads();
     for (int e = threadIdx.x; e < ncf * RB; e += NT) {
       int ei = e / RB, ri = e - ei * RB;
       int n = s_nof[ei];
-      double2 v = c2(0.0);
-      if (r0 + ri < nrhs) v = cscale(spow[n], exps[((size_t)sbx * nrhs + r0 + ri) * ncf + ei]);
+      V v = cmake<R>(0);
+      if (r0 + ri < nrhs) v = cscale(spow[n], cto(exps[((size_t)sbx * nrhs + r0 + ri) * ncf + ei], V()));
       Es[e] = v;
     }
     __syncthreads();
@@ -920,56 +962,62 @@ k_h3_e2qbxl_rot(qbxfmm_geometry g, HelmCoeffs hc, int pf, int nrhs,
       if (FROM_LOCAL) {
         double jv[H3_LMAX + 2];
         h3_sph_j(L, hc.k * bl, jv);
-        for (int l = 0; l <= L; ++l) rad[l] = c2(jv[l]);
+        for (int l = 0; l <= L; ++l) rad[l] = cmake<R>((R)jv[l]);
+      } else if constexpr (F64) {
+        h3_sph_h(L, hc.k * bl, reinterpret_cast<double2*>(rad));
       } else {
-        h3_sph_h(L, hc.k * bl, rad);
+        double2 hv[H3_LMAX + 2];
+        h3_sph_h(L, hc.k * bl, hv);
+        for (int l = 0; l <= L; ++l) rad[l] = cto(hv[l], V());
       }
     }
     for (int m = lane; m < nm; m += 32) {
       double sn, cs;
       sincos((m - pf) * alpha, &sn, &cs);
-      ph[m] = c2(cs, sn);
+      ph[m] = cmake<R>((R)cs, (R)sn);
       double a = 1.0, b = 1.0;
       for (int u = 0; u < m; ++u) {
         a *= ch;
         b *= sh;
       }
-      chp[m] = a;
-      shp[m] = b;
+      chp[m] = (R)a;
+      shp[m] = (R)b;
     }
     __syncwarp();
     // 4 pi Y_l^0(z) i^l f_l, Y_l^0(z) = sqrt((2l+1)/(4 pi)), one lane per order
-    for (int l = lane; l <= L; l += 32) rad[l] = cmul(cscale(sqrt(FOUR_PI * (2.0 * l + 1.0)), ipow(l)), rad[l]);
+    for (int l = lane; l <= L; l += 32)
+      rad[l] = cmul(cto(cscale(sqrt(FOUR_PI * (2.0 * l + 1.0)), ipow(l)), V()), rad[l]);
     __syncwarp();
     // recurrence tasks t = (m + pf) (Q + 1) + mu, mu >= 0: start values
-    double cur[RSL], prev[RSL], v0[RSL];
+    R cur[RSL], prev[RSL], v0[RSL];
     int n0[RSL];
 #pragma unroll
     for (int sl = 0; sl < RSL; ++sl) {
       int t = lane + 32 * sl;
-      cur[sl] = prev[sl] = v0[sl] = 0.0;
+      cur[sl] = prev[sl] = v0[sl] = R(0);
       n0[sl] = 1 << 20;
       if (t < ntask) {
         int m = t / (Q + 1) - pf, mu = t % (Q + 1);
         n0[sl] = max(abs(m), mu);
-        v0[sl] = __ldg(rstart + 4 * t) * chp[(int)__ldg(rstart + 4 * t + 1)] *
+        v0[sl] = (R)__ldg(rstart + 4 * t) * chp[(int)__ldg(rstart + 4 * t + 1)] *
                  shp[(int)__ldg(rstart + 4 * t + 2)];
       }
     }
     // per-lane (mu, density) slots of the coaxially translated coefficients: the TPL
     // lane tasks, or with 8 densities the 4 entries of the tensor-core output tiles
     // this lane holds
-    constexpr int LSL = (RB == 8) ? 4 : TPL;
-    double2 lacc[LSL][Q + 1];
+    constexpr bool DMMA = F64 && RB == 8;
+    constexpr int LSL = DMMA ? 4 : TPL;
+    V lacc[LSL][Q + 1];
 #pragma unroll
     for (int ts = 0; ts < LSL; ++ts)
 #pragma unroll
-      for (int nu = 0; nu <= Q; ++nu) lacc[ts][nu] = c2(0.0);
+      for (int nu = 0; nu <= Q; ++nu) lacc[ts][nu] = cmake<R>(0);
 
     for (int n = 0; n <= pf; ++n) {
       // (1) the raw slice d^n_{m mu}, mu >= 0, and the step to n + 1
-      double rn = n > 0 ? 1.0 / n : 0.0;
-      double h1 = (2.0 * n + 1.0) * n * (n + 1.0) * cbeta;
+      const R rn = n > 0 ? R(1) / R(n) : R(0);
+      const R h1 = (R)((2.0 * n + 1.0) * n * (n + 1.0) * cbeta);
 #pragma unroll
       for (int sl = 0; sl < RSL; ++sl) {
         int t = lane + 32 * sl;
@@ -977,15 +1025,15 @@ k_h3_e2qbxl_rot(qbxfmm_geometry g, HelmCoeffs hc, int pf, int nrhs,
         if (n == n0[sl]) cur[sl] = v0[sl];
         Draw[t] = n >= n0[sl] ? cur[sl] : 0.0;
         if (n >= n0[sl] && n < pf) {
-          double nxt;
+          R nxt;
           if (n == 0) {
-            nxt = cbeta * cur[sl];
+            nxt = (R)cbeta * cur[sl];
           } else {
             int m = t / (Q + 1) - pf, mu = t % (Q + 1);
             int am = abs(m);
-            double w = rn * s_isq[(n + 1) * (pf + 1) + am] * s_isq[(n + 1) * (pf + 1) + mu];
-            double A = (h1 - (2.0 * n + 1.0) * m * mu) * w;
-            double C = (n + 1.0) * rn * s_rt[n * (pf + 1) + am] * s_rt[n * (pf + 1) + mu];
+            R w = rn * s_isq[(n + 1) * (pf + 1) + am] * s_isq[(n + 1) * (pf + 1) + mu];
+            R A = (h1 - R((2 * n + 1) * m * mu)) * w;
+            R C = R(n + 1) * rn * s_rt[n * (pf + 1) + am] * s_rt[n * (pf + 1) + mu];
             nxt = fma(A, cur[sl], -C * prev[sl]);
           }
           prev[sl] = cur[sl];
@@ -996,12 +1044,12 @@ k_h3_e2qbxl_rot(qbxfmm_geometry g, HelmCoeffs hc, int pf, int nrhs,
       for (int o = lane; o < NCQ; o += 32) {
         int nu = s_nof[o];
         int mu = o - nu * nu - nu;
-        double2 tt = c2(0.0);
+        V tt = cmake<R>(0);
         if (n >= abs(mu)) {
           const double* G = g0c + ((size_t)o * nl + n) * (Q + 1);
           int lbase = abs(n - nu), jmax = min(n, nu);
-          for (int j = 0; j <= jmax; ++j) tt = caxpy(__ldg(G + j), rad[lbase + 2 * j], tt);
-          tt = cmul(ipow(nu - n + 4 * pf), tt);
+          for (int j = 0; j <= jmax; ++j) tt = caxpy((R)__ldg(G + j), rad[lbase + 2 * j], tt);
+          tt = cmul(cto(ipow(nu - n + 4 * pf), V()), tt);
         }
         coaxn[o] = tt;
       }
@@ -1010,16 +1058,16 @@ k_h3_e2qbxl_rot(qbxfmm_geometry g, HelmCoeffs hc, int pf, int nrhs,
       // the back-rotation matrices
       for (int e = lane; e < (2 * n + 1) * NMU; e += 32) {
         int mm = e / NMU - n, mu = e % NMU - Q;
-        double val = mu >= 0 ? Draw[(mm + pf) * (Q + 1) + mu]
-                             : (((mm - mu) & 1) ? -1.0 : 1.0) * Draw[(pf - mm) * (Q + 1) - mu];
-        val *= ((mm > 0 && (mm & 1)) ? -1.0 : 1.0) * ((mu > 0 && (mu & 1)) ? -1.0 : 1.0);
+        R val = mu >= 0 ? Draw[(mm + pf) * (Q + 1) + mu]
+                        : (((mm - mu) & 1) ? R(-1) : R(1)) * Draw[(pf - mm) * (Q + 1) - mu];
+        val *= ((mm > 0 && (mm & 1)) ? R(-1) : R(1)) * ((mu > 0 && (mu & 1)) ? R(-1) : R(1));
         if (n <= Q && abs(mm) <= Q) Tb[(mu + Q) * NCQ + n * n + n + mm] = val;
         Dph[(mm + pf) * NMU + mu + Q] = cscale(val, ph[mm + pf]);
       }
       __syncwarp();
       // (4) rotate and translate coaxially
       const int base = n * n + n;
-      if constexpr (RB == 8) {
+      if constexpr (DMMA) {
         // the rotation of order n as a real product on the FP64 tensor cores:
         // rows (mu, re / im) of the rotated coefficients, k = (m, re / im), columns the
         // 8 densities; tiles 0/1 hold re/im of mu index 0..7, tiles 2/3 of 8..15,
@@ -1060,7 +1108,7 @@ k_h3_e2qbxl_rot(qbxfmm_geometry g, HelmCoeffs hc, int pf, int nrhs,
       } else {
         // lane tasks (mu, density), all of a lane's tasks in one pass over m so that
         // their multiply-adds interleave
-        double2 mr[TPL];
+        V mr[TPL];
         int toff[TPL], eoff[TPL];
         bool act[TPL];
 #pragma unroll
@@ -1070,7 +1118,7 @@ k_h3_e2qbxl_rot(qbxfmm_geometry g, HelmCoeffs hc, int pf, int nrhs,
           act[ts] = task < NMU * RB && abs(mu) <= n;
           toff[ts] = act[ts] ? (pf - n) * NMU + mu + Q : 0;
           eoff[ts] = act[ts] ? (base - n) * RB + r : 0;
-          mr[ts] = c2(0.0);
+          mr[ts] = cmake<R>(0);
         }
         for (int m = 0; m < 2 * n + 1; ++m) {
 #pragma unroll
@@ -1090,7 +1138,7 @@ k_h3_e2qbxl_rot(qbxfmm_geometry g, HelmCoeffs hc, int pf, int nrhs,
       }
       __syncwarp();
     }
-    if constexpr (RB == 8) {
+    if constexpr (DMMA) {
       const int rho = lane >> 2;
 #pragma unroll
       for (int sl = 0; sl < 4; ++sl) {
@@ -1121,7 +1169,7 @@ k_h3_e2qbxl_rot(qbxfmm_geometry g, HelmCoeffs hc, int pf, int nrhs,
       int o = task / RB, r = task - o * RB;
       int nu = s_nof[o];
       int mu2 = o - nu * nu - nu;
-      double2 a = c2(0.0);
+      V a = cmake<R>(0);
       for (int mu = -nu; mu <= nu; ++mu) a = caxpy(Tb[(mu + Q) * NCQ + o], Lp[(nu * nu + nu + mu) * RB + r], a);
       acc[i] = cfma(cconj(ph[mu2 + pf]), a, acc[i]);
     }
@@ -1137,7 +1185,7 @@ k_h3_e2qbxl_rot(qbxfmm_geometry g, HelmCoeffs hc, int pf, int nrhs,
     if (r0 + r >= nrhs) continue;
     int nu = s_nof[o];
     double2* out = qbx_exps + ((size_t)ctr * nrhs + r0 + r) * NCQ + o;
-    *out = caxpy(pow(st, (double)nu), acc[i], *out);
+    *out = caxpy(pow(st, (double)nu), c2d(acc[i]), *out);
   }
 }
 
@@ -1164,7 +1212,7 @@ k_h3_qbxl2p(qbxfmm_geometry g, HelmCoeffs hc, int q, int nrhs, const double2* __
     double x[3];
     load_point<3>(g.targets, g.ntargets, t, x);
     double2* P = pot_tree + (size_t)r * g.ntargets + t;
-    *P = cadd(*P, h3_e2p(Lc, q, true, hc.k, s, cc, x, rec));
+    *P = cadd(*P, h3_e2p(Lc, q, true, hc.k, s, cc, x, rec, hc.taylor ? q : -1));
   }
 }
 
@@ -1210,7 +1258,7 @@ k_h3_tsqbx(qbxfmm_geometry g, HelmCoeffs hc, int nrhs, const double2* __restrict
   double jn[Q + 1];
   {
     double jv[H3_LMAX + 2];
-    h3_sph_j(Q, hc.k * alen, jv);
+    h3_sph_j_cut(Q, hc.k * alen, hc.taylor ? Q : -1, jv);
 #pragma unroll
     for (int n = 0; n <= Q; ++n) jn[n] = (2.0 * n + 1.0) * jv[n];
   }
@@ -1572,13 +1620,16 @@ constexpr int H3M2L_NCG = 120;
 // table, then the rotation table again are copied into one shared buffer by all
 // threads (16-byte loads, all in flight together) before the step that reads them,
 // so the inner loops read shared memory only.
-template <int RB>
+template <typename R, int RB>
 __global__ void __launch_bounds__(H3M2L_NT)
 k_h3_m2l_rot(qbxfmm_geometry g, int pf, int nrhs, const double2* __restrict__ mp,
              double2* __restrict__ lo, const double* __restrict__ Dtab,
              const double2* __restrict__ Ctab, const double* __restrict__ clsmap,
              int32_t* err)
 {
+  // R: the arithmetic (double, or float in the mixed-precision form; expansions are
+  // read and added in float64 either way)
+  using V = cplx_t<R>;
   extern __shared__ double2 smem2[];
   __shared__ int s_gn[H3M2L_NG], s_gm0[H3M2L_NG];        // rotation task groups
   __shared__ int s_cmu[H3M2L_NCG], s_cnu0[H3M2L_NCG];    // coaxial task groups
@@ -1587,9 +1638,9 @@ k_h3_m2l_rot(qbxfmm_geometry g, int pf, int nrhs, const double2* __restrict__ mp
   constexpr int NTHR = H3M2L_NT;
   constexpr int KMAX = (H3M2L_NG * RB + NTHR - 1) / NTHR;
   const int ncf = (pf + 1) * (pf + 1), XS = ncf + 1, nm = 2 * pf + 1;
-  double2* X = smem2;                       // [RB][ncf + 1]
-  double2* A = smem2 + (size_t)RB * XS;     // [RB][ncf + 1]
-  double2* Tbuf = A + (size_t)RB * XS;      // rotation or coaxial table of the pair
+  V* X = reinterpret_cast<V*>(smem2);      // [RB][ncf + 1]
+  V* A = X + (size_t)RB * XS;               // [RB][ncf + 1]
+  V* Tbuf = A + (size_t)RB * XS;            // rotation or coaxial table of the pair
   if (threadIdx.x == 0) {
     int ng = 0;
     for (int n = 0; n <= pf; ++n)
@@ -1617,11 +1668,11 @@ k_h3_m2l_rot(qbxfmm_geometry g, int pf, int nrhs, const double2* __restrict__ mp
   if (q1 <= q0) return;
   const int ng = s_ng, ncg = s_ncg;
   const size_t dsz = h3_m2l_dsize(pf), csz = h3_m2l_csize(pf);
-  double2 acc[KMAX][4];
+  V acc[KMAX][4];
 #pragma unroll
   for (int k = 0; k < KMAX; ++k)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) acc[k][j] = c2(0.0);
+    for (int j = 0; j < 4; ++j) acc[k][j] = cmake<R>(0);
 
   for (int q = q0; q < q1; ++q) {
     int pr = g.m2l_tgt_pairs[q];
@@ -1640,16 +1691,17 @@ k_h3_m2l_rot(qbxfmm_geometry g, int pf, int nrhs, const double2* __restrict__ mp
     const double2* Dg = reinterpret_cast<const double2*>(Dtab + (size_t)clsmap[2 * lo_c] * dsz);
     const double2* Cg = Ctab + (size_t)clsmap[2 * lo_c + 1] * csz;
     // the rotation table into Tbuf (phases, then the d blocks)
-    for (int x = threadIdx.x; x < (int)(dsz / 2); x += NTHR) Tbuf[x] = __ldg(Dg + x);
-    const double2* ph = Tbuf;
-    const double* blocks = reinterpret_cast<const double*>(Tbuf) + 2 * nm;
-    const double2* C = Tbuf;
+    for (int x = threadIdx.x; x < (int)(dsz / 2); x += NTHR) Tbuf[x] = cto(__ldg(Dg + x), V());
+    const V* ph = Tbuf;
+    const R* blocks = reinterpret_cast<const R*>(Tbuf) + 2 * nm;
+    const V* C = Tbuf;
     // X = e^{i m alpha} M
     for (int e = threadIdx.x; e < RB * ncf; e += NTHR) {
       int r = e / ncf, ci = e - r * ncf;
       int n = s_nof[ci];
-      double2 v = c2(0.0);
-      if (r0 + r < nrhs) v = cmul(__ldg(Dg + ci - n * n - n + pf), mp[((size_t)src * nrhs + r0 + r) * ncf + ci]);
+      V v = cmake<R>(0);
+      if (r0 + r < nrhs)
+        v = cto(cmul(__ldg(Dg + ci - n * n - n + pf), mp[((size_t)src * nrhs + r0 + r) * ncf + ci]), V());
       X[r * XS + ci] = v;
     }
     __syncthreads();
@@ -1657,15 +1709,15 @@ k_h3_m2l_rot(qbxfmm_geometry g, int pf, int nrhs, const double2* __restrict__ mp
     for (int t = threadIdx.x; t < ng * RB; t += NTHR) {
       int grp = t / RB, r = t - grp * RB;
       int n = s_gn[grp], mu0 = s_gm0[grp];
-      const double* Tn = blocks + h3_dblock(n);
+      const R* Tn = blocks + h3_dblock(n);
       const int w = 2 * n + 1, nv = min(4, n - mu0 + 1);
-      double2 o[4] = {c2(0.0), c2(0.0), c2(0.0), c2(0.0)};
-      const double2* Xr = X + r * XS + n * n;
+      V o[4] = {cmake<R>(0), cmake<R>(0), cmake<R>(0), cmake<R>(0)};
+      const V* Xr = X + r * XS + n * n;
       for (int m = 0; m < w; ++m) {
-        double2 x = Xr[m];
+        V x = Xr[m];
         // T^n[m - n][mu0 + j]: row m - n >= 0 directly, else row n - m at -mu (reversed)
         const int ma = m - n;
-        const double* row = ma >= 0 ? Tn + ma * w + (mu0 + n) : Tn + (-ma) * w + (n - mu0);
+        const R* row = ma >= 0 ? Tn + ma * w + (mu0 + n) : Tn + (-ma) * w + (n - mu0);
         const int step = ma >= 0 ? 1 : -1;
 #pragma unroll
         for (int j = 0; j < 4; ++j)
@@ -1676,19 +1728,19 @@ k_h3_m2l_rot(qbxfmm_geometry g, int pf, int nrhs, const double2* __restrict__ mp
         if (j < nv) A[r * XS + n * n + n + mu0 + j] = o[j];
     }
     __syncthreads();
-    for (int x = threadIdx.x; x < (int)csz; x += NTHR) Tbuf[x] = __ldg(Cg + x);
+    for (int x = threadIdx.x; x < (int)csz; x += NTHR) Tbuf[x] = cto(__ldg(Cg + x), V());
     __syncthreads();
     // B[(nu, mu)] = sum_{n >= |mu|} C^mu[n][nu] A[(n, mu)]   (into X)
     for (int t = threadIdx.x; t < ncg * RB; t += NTHR) {
       int grp = t / RB, r = t - grp * RB;
       int mu = s_cmu[grp], nu0 = s_cnu0[grp];
       int am = abs(mu), w = pf + 1 - am, nv = min(4, pf - nu0 + 1);
-      const double2* Cb = C + h3_cblock(pf, am) + (nu0 - am);
-      double2 o[4] = {c2(0.0), c2(0.0), c2(0.0), c2(0.0)};
-      const double2* Ar = A + r * XS;
+      const V* Cb = C + h3_cblock(pf, am) + (nu0 - am);
+      V o[4] = {cmake<R>(0), cmake<R>(0), cmake<R>(0), cmake<R>(0)};
+      const V* Ar = A + r * XS;
       for (int n = am; n <= pf; ++n) {
-        double2 a = Ar[n * n + n + mu];
-        const double2* row = Cb + (n - am) * w;
+        V a = Ar[n * n + n + mu];
+        const V* row = Cb + (n - am) * w;
 #pragma unroll
         for (int j = 0; j < 4; ++j)
           if (j < nv) o[j] = cfma(row[j], a, o[j]);
@@ -1700,7 +1752,7 @@ k_h3_m2l_rot(qbxfmm_geometry g, int pf, int nrhs, const double2* __restrict__ mp
       }
     }
     __syncthreads();
-    for (int x = threadIdx.x; x < (int)(dsz / 2); x += NTHR) Tbuf[x] = __ldg(Dg + x);
+    for (int x = threadIdx.x; x < (int)(dsz / 2); x += NTHR) Tbuf[x] = cto(__ldg(Dg + x), V());
     __syncthreads();
     // L[(nu, m2)] += e^{-i m2 alpha} sum_mu T^nu[m2][mu] B[(nu, mu)]
 #pragma unroll
@@ -1710,9 +1762,9 @@ k_h3_m2l_rot(qbxfmm_geometry g, int pf, int nrhs, const double2* __restrict__ mp
       int grp = t / RB, r = t - grp * RB;
       int nu = s_gn[grp], m20 = s_gm0[grp];
       const int w = 2 * nu + 1, nv = min(4, nu - m20 + 1);
-      const double* Tn = blocks + h3_dblock(nu);
+      const R* Tn = blocks + h3_dblock(nu);
       // T^nu[m2][mu] for m2 = m20 + j: row m2 >= 0 directly, else row -m2 at -mu
-      const double* pj[4];
+      const R* pj[4];
       int sj[4];
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
@@ -1720,10 +1772,10 @@ k_h3_m2l_rot(qbxfmm_geometry g, int pf, int nrhs, const double2* __restrict__ mp
         pj[j] = m2 >= 0 ? Tn + m2 * w : Tn + (-m2) * w + 2 * nu;
         sj[j] = m2 >= 0 ? 1 : -1;
       }
-      double2 o[4] = {c2(0.0), c2(0.0), c2(0.0), c2(0.0)};
-      const double2* Br = X + r * XS + nu * nu;
+      V o[4] = {cmake<R>(0), cmake<R>(0), cmake<R>(0), cmake<R>(0)};
+      const V* Br = X + r * XS + nu * nu;
       for (int mu = 0; mu < w; ++mu) {
-        double2 b = Br[mu];
+        V b = Br[mu];
 #pragma unroll
         for (int j = 0; j < 4; ++j)
           if (j < nv) o[j] = caxpy(pj[j][sj[j] * mu], b, o[j]);
@@ -1750,32 +1802,38 @@ k_h3_m2l_rot(qbxfmm_geometry g, int pf, int nrhs, const double2* __restrict__ mp
     double2* out = lo + ((size_t)tb * nrhs + r0 + r) * ncf + nu * nu + nu + m20;
 #pragma unroll
     for (int j = 0; j < 4; ++j)
-      if (j < nv) out[j] = cadd(out[j], acc[k][j]);
+      if (j < nv) out[j] = cadd(out[j], c2d(acc[k][j]));
   }
 }
 
-template <int RB>
+template <typename R, int RB>
 static cudaError_t h3_m2l_rot_launch(const qbxfmm_geometry& g, int pf, int nrhs, const double2* mp,
                                      double2* lo, const double* Dtab, const double2* Ctab,
                                      const double* clsmap, int32_t* err, cudaStream_t st)
 {
-  size_t sh = 2 * (size_t)RB * ((pf + 1) * (pf + 1) + 1) * sizeof(double2) +
-              std::max(h3_m2l_dsize(pf) * sizeof(double), h3_m2l_csize(pf) * sizeof(double2));
-  cudaFuncSetAttribute(k_h3_m2l_rot<RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+  using V = cplx_t<R>;
+  size_t sh = (2 * (size_t)RB * ((pf + 1) * (pf + 1) + 1) +
+               std::max(h3_m2l_dsize(pf) / 2, h3_m2l_csize(pf))) * sizeof(V);
+  cudaFuncSetAttribute(k_h3_m2l_rot<R, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
   dim3 grid(g.nttp_boxes, (nrhs + RB - 1) / RB);
-  k_h3_m2l_rot<RB><<<grid, H3M2L_NT, sh, st>>>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err);
+  k_h3_m2l_rot<R, RB><<<grid, H3M2L_NT, sh, st>>>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err);
   return cudaGetLastError();
 }
 
 cudaError_t h3_launch_m2l_rot(const qbxfmm_geometry& g, int pf, int nrhs, const double2* mp,
                               double2* lo, const double* Dtab, const double2* Ctab,
-                              const double* clsmap, int32_t* err, cudaStream_t st)
+                              const double* clsmap, int32_t* err, cudaStream_t st, bool fp32)
 {
   if (g.nttp_boxes == 0 || g.m2l_nclasses == 0) return cudaSuccess;
   if (pf > H3_MAXP) return cudaErrorInvalidValue;
-  if (nrhs >= 8) return h3_m2l_rot_launch<8>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err, st);
-  if (nrhs >= 2) return h3_m2l_rot_launch<4>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err, st);
-  return h3_m2l_rot_launch<1>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err, st);
+  if (fp32) {   // mixed form: FP32 arithmetic, all 16 densities of a pair's tables at once
+    if (nrhs >= 16) return h3_m2l_rot_launch<float, 16>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err, st);
+    if (nrhs >= 8) return h3_m2l_rot_launch<float, 8>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err, st);
+    return h3_m2l_rot_launch<float, 4>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err, st);
+  }
+  if (nrhs >= 8) return h3_m2l_rot_launch<double, 8>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err, st);
+  if (nrhs >= 2) return h3_m2l_rot_launch<double, 4>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err, st);
+  return h3_m2l_rot_launch<double, 1>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err, st);
 }
 
 cudaError_t h3_launch_m2l_tables(int pf, int ndir, int ncoax, const double* dirs,
@@ -1822,6 +1880,8 @@ cudaError_t h3_launch_p2m(const qbxfmm_geometry& g, HelmCoeffs hc, int p, int nr
   if (g.nsource_boxes == 0) return cudaSuccess;
   int N = p + 1;
   size_t sh = ((size_t)(N + 1) * (N + 1) * H3_TS + (size_t)(N + 1) * (N + 2) / 2) * sizeof(double2);
+  if (hc.taylor && (hc.cd.x != 0.0 || hc.cd.y != 0.0))   // second (dipole) table
+    sh += ((size_t)(N + 1) * (N + 1) * H3_TS + (size_t)H3_SUB * (N + 2)) * sizeof(double2);
   return h3_p2e_launch<false>(g.nsource_boxes, sh, g, hc, p, nrhs, s, mp, nullptr, st);
 }
 
@@ -1926,7 +1986,7 @@ cudaError_t h3_launch_tsqbx(const qbxfmm_geometry& g, HelmCoeffs hc, int q, int 
   }
 }
 
-template <bool FROM_LOCAL, int Q, int RB>
+template <typename R, bool FROM_LOCAL, int Q, int RB>
 static size_t h3_rot_smem(int pf)
 {
   constexpr int NCQ = (Q + 1) * (Q + 1), NMU = 2 * Q + 1;
@@ -1935,37 +1995,42 @@ static size_t h3_rot_smem(int pf)
   size_t ctad = (nisq + nrt + nl + 1) & ~(size_t)1;
   size_t perd = ((size_t)nm * (Q + 1) + (size_t)NMU * NCQ + 2 * (size_t)nm + 1) / 2;
   size_t per = (size_t)nm * NMU + NCQ + (size_t)NCQ * RB + (L + 2) + nm + perd;
-  return (size_t)ncf * RB * sizeof(double2) + ctad * sizeof(double) + NW * per * sizeof(double2);
+  return ((size_t)ncf * RB + NW * per) * sizeof(cplx_t<R>) + ctad * sizeof(R);
 }
 
-template <bool FROM_LOCAL, int Q, int RB>
+template <typename R, bool FROM_LOCAL, int Q, int RB>
 static cudaError_t h3_rot_launch(const qbxfmm_geometry& g, HelmCoeffs hc, int pf, int nrhs,
                                  const double2* e, const double* rot, double2* qe, int32_t* err,
                                  cudaStream_t st)
 {
-  size_t sh = h3_rot_smem<FROM_LOCAL, Q, RB>(pf);
-  cudaFuncSetAttribute(k_h3_e2qbxl_rot<FROM_LOCAL, Q, RB>,
+  size_t sh = h3_rot_smem<R, FROM_LOCAL, Q, RB>(pf);
+  cudaFuncSetAttribute(k_h3_e2qbxl_rot<R, FROM_LOCAL, Q, RB>,
                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
   dim3 grid(g.nqbx_chunks, (nrhs + RB - 1) / RB, H3_ROT_ZS);
-  k_h3_e2qbxl_rot<FROM_LOCAL, Q, RB><<<grid, NT, sh, st>>>(g, hc, pf, nrhs, e, rot, qe, err);
+  k_h3_e2qbxl_rot<R, FROM_LOCAL, Q, RB><<<grid, NT, sh, st>>>(g, hc, pf, nrhs, e, rot, qe, err);
   return cudaGetLastError();
 }
 
-// densities per CTA: 8 when two CTAs still fit an SM's shared memory, else 4, else 1
-template <bool FROM_LOCAL, int Q>
+// densities per CTA: FP64, 8 when two CTAs still fit an SM's shared memory, else 4,
+// else 1; FP32 (the mixed form), all 16 of a 16-density job in one CTA so that the
+// per-pair rotation tables serve every density
+template <typename R, bool FROM_LOCAL, int Q>
 static cudaError_t h3_rot_q(const qbxfmm_geometry& g, HelmCoeffs hc, int pf, int nrhs,
                             const double2* e, const double* rot, double2* qe, int32_t* err,
                             cudaStream_t st)
 {
   const size_t two_per_sm = 112 * 1024;
-  if (nrhs >= 8 && h3_rot_smem<FROM_LOCAL, Q, 8>(pf) <= two_per_sm)
-    return h3_rot_launch<FROM_LOCAL, Q, 8>(g, hc, pf, nrhs, e, rot, qe, err, st);
+  if constexpr (!std::is_same<R, double>::value)
+    if (nrhs >= 16 && h3_rot_smem<R, FROM_LOCAL, Q, 16>(pf) <= two_per_sm)
+      return h3_rot_launch<R, FROM_LOCAL, Q, 16>(g, hc, pf, nrhs, e, rot, qe, err, st);
+  if (nrhs >= 8 && h3_rot_smem<R, FROM_LOCAL, Q, 8>(pf) <= two_per_sm)
+    return h3_rot_launch<R, FROM_LOCAL, Q, 8>(g, hc, pf, nrhs, e, rot, qe, err, st);
   if (nrhs >= 4)
-    return h3_rot_launch<FROM_LOCAL, Q, 4>(g, hc, pf, nrhs, e, rot, qe, err, st);
-  return h3_rot_launch<FROM_LOCAL, Q, 1>(g, hc, pf, nrhs, e, rot, qe, err, st);
+    return h3_rot_launch<R, FROM_LOCAL, Q, 4>(g, hc, pf, nrhs, e, rot, qe, err, st);
+  return h3_rot_launch<R, FROM_LOCAL, Q, 1>(g, hc, pf, nrhs, e, rot, qe, err, st);
 }
 
-template <bool FROM_LOCAL>
+template <typename R, bool FROM_LOCAL>
 static cudaError_t h3_e2qbxl(const qbxfmm_geometry& g, HelmCoeffs hc, int pf, int q, int nrhs,
                              const double2* e, const double* rot, double2* qe, int32_t* err,
                              cudaStream_t st)
@@ -1973,28 +2038,29 @@ static cudaError_t h3_e2qbxl(const qbxfmm_geometry& g, HelmCoeffs hc, int pf, in
   if (g.nqbx_chunks == 0) return cudaSuccess;
   if (2 * pf + 1 > 35) return cudaErrorInvalidValue;   // recurrence slots per lane
   switch (q) {
-    case 0: return h3_rot_q<FROM_LOCAL, 0>(g, hc, pf, nrhs, e, rot, qe, err, st);
-    case 1: return h3_rot_q<FROM_LOCAL, 1>(g, hc, pf, nrhs, e, rot, qe, err, st);
-    case 2: return h3_rot_q<FROM_LOCAL, 2>(g, hc, pf, nrhs, e, rot, qe, err, st);
-    case 3: return h3_rot_q<FROM_LOCAL, 3>(g, hc, pf, nrhs, e, rot, qe, err, st);
-    case 4: return h3_rot_q<FROM_LOCAL, 4>(g, hc, pf, nrhs, e, rot, qe, err, st);
-    case 5: return h3_rot_q<FROM_LOCAL, 5>(g, hc, pf, nrhs, e, rot, qe, err, st);
+    case 0: return h3_rot_q<R, FROM_LOCAL, 0>(g, hc, pf, nrhs, e, rot, qe, err, st);
+    case 1: return h3_rot_q<R, FROM_LOCAL, 1>(g, hc, pf, nrhs, e, rot, qe, err, st);
+    case 2: return h3_rot_q<R, FROM_LOCAL, 2>(g, hc, pf, nrhs, e, rot, qe, err, st);
+    case 3: return h3_rot_q<R, FROM_LOCAL, 3>(g, hc, pf, nrhs, e, rot, qe, err, st);
+    case 4: return h3_rot_q<R, FROM_LOCAL, 4>(g, hc, pf, nrhs, e, rot, qe, err, st);
+    case 5: return h3_rot_q<R, FROM_LOCAL, 5>(g, hc, pf, nrhs, e, rot, qe, err, st);
     default: return cudaErrorInvalidValue;
   }
 }
 
 cudaError_t h3_launch_m2qbxl(const qbxfmm_geometry& g, HelmCoeffs hc, int pf, int q, int nrhs,
                              const double2* mp, const double* rot, double2* qe, int32_t* err,
-                             cudaStream_t st)
+                             cudaStream_t st, bool fp32)
 {
-  return h3_e2qbxl<false>(g, hc, pf, q, nrhs, mp, rot, qe, err, st);
+  if (fp32) return h3_e2qbxl<float, false>(g, hc, pf, q, nrhs, mp, rot, qe, err, st);
+  return h3_e2qbxl<double, false>(g, hc, pf, q, nrhs, mp, rot, qe, err, st);
 }
 
 cudaError_t h3_launch_l2qbxl(const qbxfmm_geometry& g, HelmCoeffs hc, int pf, int q, int nrhs,
                              const double2* lo, const double* rot, double2* qe, int32_t* err,
                              cudaStream_t st)
 {
-  return h3_e2qbxl<true>(g, hc, pf, q, nrhs, lo, rot, qe, err, st);
+  return h3_e2qbxl<double, true>(g, hc, pf, q, nrhs, lo, rot, qe, err, st);
 }
 
 cudaError_t h3_launch_qbxl2p(const qbxfmm_geometry& g, HelmCoeffs hc, int q, int nrhs,
@@ -2052,7 +2118,8 @@ namespace {
 
 // Entry (t, s) of the 3D Helmholtz layer potential with charge / dipole weights:
 //   QBX targets (center c): the target-specific series of k_h3_tsqbx,
-//     ik sum_{n<=Q} (2n+1) j_n(k|a|) [cq h_n(k|b|) P_n(cos g) + cd (dipole terms)],
+//     ik sum_{n<=Q} (2n+1) j_n(k|a|) [cq h_n(k|b|) P_n(cos g) + cd (dipole terms)]
+//     (j_n cut to its degree-Q power series in the reference's default truncation),
 //   other targets: cq e^{ikr}/r + cd nu.(t - s) e^{ikr} (1 - ikr) / r^3;
 // times 1/(4 pi).  CTA = 128 sources (thread = source) x 32 targets.
 constexpr int H3D_DS = 128;
@@ -2088,7 +2155,7 @@ k_h3_qbx_matrix(int nsrc, const double* __restrict__ src, const double* __restri
     }
     s_qbx[i] = c >= 0;
     double jv[H3_LMAX + 2];
-    h3_sph_j(Q, hc.k * alen, jv);
+    h3_sph_j_cut(Q, hc.k * alen, hc.taylor ? Q : -1, jv);
 #pragma unroll
     for (int n = 0; n <= Q; ++n) s_jn[i][n] = (2.0 * n + 1.0) * jv[n];
   }
@@ -2187,11 +2254,13 @@ extern "C" int qbxfmm_helmholtz3d_qbx_matrix(int nsources, const double* sources
                                              double dipole_im, int ntargets,
                                              const double* targets, const int32_t* target_center,
                                              int ncenters, const double* centers, int qbx_order,
-                                             void* K, void* stream)
+                                             int fmm_backend, void* K, void* stream)
 {
   using namespace qbx;
   if (nsources < 0 || ntargets < 0 || ncenters < 0)
     return set_last_error(QBXFMM_ERR_ARG, "negative size");
+  if (fmm_backend != QBXFMM_BACKEND_SUMPY && fmm_backend != QBXFMM_BACKEND_FMMLIB)
+    return set_last_error(QBXFMM_ERR_ARG, "fmm_backend must be QBXFMM_BACKEND_SUMPY or _FMMLIB");
   if (qbx_order < 0 || qbx_order > 8)
     return set_last_error(QBXFMM_ERR_UNSUPPORTED, "qbx_order must be in [0, 8]");
   if (!(k > 0.0)) return set_last_error(QBXFMM_ERR_ARG, "wave number must be positive");
@@ -2206,6 +2275,7 @@ extern "C" int qbxfmm_helmholtz3d_qbx_matrix(int nsources, const double* sources
   hc.k = k;
   hc.cq = c2(charge_re, charge_im);
   hc.cd = c2(dipole_re, dipole_im);
+  hc.taylor = fmm_backend == QBXFMM_BACKEND_SUMPY;
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   double2* Kd = static_cast<double2*>(K);
   cudaError_t e;

@@ -69,7 +69,7 @@ def _real_matrix(name, geo, spec, qbx_order, device):
     return _assemble(geo, scal, arr, d, K)
 
 
-def _complex_matrix(name, geo, spec, qbx_order, device):
+def _complex_matrix(name, geo, spec, qbx_order, device, extra=()):
     dev = torch.device(device)
     scal, arr, d, (src, nrm, tgt, cen, tc) = _tree_inputs(geo, dev)
     nsrc, ntgt, ncen = scal["nsources"], scal["ntargets"], scal["ncenters"]
@@ -79,21 +79,24 @@ def _complex_matrix(name, geo, spec, qbx_order, device):
     native.check(name, getattr(native.lib(), name)(
         nsrc, V(src.data_ptr()), V(nrm.data_ptr()), float(spec.kernel.k), cq.real, cq.imag,
         cd.real, cd.imag, ntgt, V(tgt.data_ptr()), V(tc.data_ptr()), ncen, V(cen.data_ptr()),
-        qbx_order, V(K.data_ptr()), _stream_handle()))
+        qbx_order, *extra, V(K.data_ptr()), _stream_handle()))
     return _assemble(geo, scal, arr, d, K)
 
 
 def qbx_matrix(geo: QBXFMMGeometryData, spec: SourceKernelSpec, qbx_order: int,
-               device="cuda") -> torch.Tensor:
+               device="cuda", fmm_backend: str = "sumpy") -> torch.Tensor:
     """(n_user_targets, ndofs) matrix on ``device`` of the layer potential
     ``charge_coeff S + dipole_coeff D`` with the kernel's scaling (float64 for
-    Laplace, complex128 for Helmholtz), for either kernel in 2D or 3D."""
+    Laplace, complex128 for Helmholtz), for either kernel in 2D or 3D.
+    ``fmm_backend``: whose QBX truncation (3D Helmholtz only; see
+    :class:`~pytential_b200.fmm.QBXApply`)."""
     dim = spec.kernel.dim
     if isinstance(spec.kernel, LaplaceKernel):
         return _real_matrix(f"qbxfmm_laplace{dim}d_qbx_matrix", geo, spec, qbx_order, device)
     if isinstance(spec.kernel, HelmholtzKernel):
+        extra = (abi.FMM_BACKENDS[fmm_backend],) if dim == 3 else ()
         return _complex_matrix(f"qbxfmm_helmholtz{dim}d_qbx_matrix", geo, spec, qbx_order,
-                               device)
+                               device, extra)
     raise NotImplementedError(type(spec.kernel).__name__)
 
 

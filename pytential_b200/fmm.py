@@ -160,8 +160,9 @@ class Plan:
 
     def __init__(self, dgeo: DeviceGeometry, spec: SourceKernelSpec, qbx_order: int,
                  fmm_order: int, nrhs: int = 1, target_specific_qbx: bool = False,
-                 precision: int = PRECISION_FP64):
+                 precision: int = PRECISION_FP64, fmm_backend: str = "sumpy"):
         self.dgeo = dgeo
+        self.fmm_backend = fmm_backend
         self.precision = precision
         self.target_specific_qbx = target_specific_qbx
         self.spec = spec
@@ -172,7 +173,8 @@ class Plan:
             family=spec.kernel.family, dim=spec.kernel.dim, qbx_order=qbx_order,
             fmm_order=fmm_order, nrhs=nrhs, charge_coeff=spec.charge_coeff,
             dipole_coeff=spec.dipole_coeff, k=spec.wave_number,
-            target_specific_qbx=target_specific_qbx, precision=precision)
+            target_specific_qbx=target_specific_qbx, precision=precision,
+            fmm_backend=fmm_backend)
         h = ctypes.c_void_p()
         native.check("qbxfmm_plan_create", native.lib().qbxfmm_plan_create(
             ctypes.byref(self.kernel), ctypes.byref(dgeo.struct), ctypes.byref(h)))
@@ -226,7 +228,7 @@ class B200QBXExpansionWrangler:
                  geo_data: QBXFMMGeometryData, dtype, qbx_order: int, fmm_level_to_order,
                  source_extra_kwargs=None, kernel_extra_kwargs=None,
                  _use_target_specific_qbx=None, *, nrhs: int = 1, device="cuda",
-                 device_geometry: DeviceGeometry | None = None):
+                 device_geometry: DeviceGeometry | None = None, fmm_backend: str = "sumpy"):
         self.using_tsqbx = bool(_use_target_specific_qbx)
         self.tree_indep = tree_indep
         self.geo_data = geo_data
@@ -246,7 +248,7 @@ class B200QBXExpansionWrangler:
         self.dgeo = _device_geometry(geo_data, tree_indep.spec, device, device_geometry)
         self.device = self.dgeo.device
         self.plan = Plan(self.dgeo, tree_indep.spec, qbx_order, fmm_order, nrhs,
-                         target_specific_qbx=self.using_tsqbx)
+                         target_specific_qbx=self.using_tsqbx, fmm_backend=fmm_backend)
         self._translations = None
         if needs_per_level_classes(tree_indep.spec):
             # the translation stages of this kernel run on precomputed matrices
@@ -486,19 +488,26 @@ class QBXApply:
     ``target_specific_qbx`` (default on) evaluates the list-1 near field of each QBX
     target directly (the truncation of P2QBXL followed by QBXL2P, which the tests
     check to 1e-12); off, the apply forms the QBX expansions from the list-1 sources
-    as the reference's wrangler does by default."""
+    as the reference's wrangler does by default.
+
+    ``fmm_backend`` picks whose expansions' truncation the apply reproduces, as the
+    reference's ``QBXLayerPotentialSource(fmm_backend=...)`` does
+    (pytential/qbx/__init__.py:93, 191): "sumpy" (the default: sumpy's default
+    expansions, compressed Cartesian Taylor in 3D, H2D in 2D Helmholtz) or "fmmlib"
+    (spherical waves); only 3D Helmholtz truncates differently."""
 
     def __init__(self, geo: QBXFMMGeometryData, spec: SourceKernelSpec, qbx_order: int,
                  fmm_order: int, nrhs: int = 1, device="cuda",
                  device_geometry: DeviceGeometry | None = None,
                  target_specific_qbx: bool = True, translation_matrices: bool = True,
-                 precision: int = PRECISION_FP64):
+                 precision: int = PRECISION_FP64, fmm_backend: str = "sumpy"):
         self.geo = geo
         self.device = torch.device(device)
         self.dgeo = _device_geometry(geo, spec, device, device_geometry)
         self.up = DeviceUpsampler(geo.discr, device)
         self.plan = Plan(self.dgeo, spec, qbx_order, fmm_order, nrhs,
-                         target_specific_qbx=target_specific_qbx, precision=precision)
+                         target_specific_qbx=target_specific_qbx, precision=precision,
+                         fmm_backend=fmm_backend)
         self.nrhs = nrhs
         sizes = self.plan.workspace_sizes()
         use_mats = (translation_matrices or needs_per_level_classes(spec)) and sizes[6] > 0

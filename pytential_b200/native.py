@@ -60,7 +60,7 @@ _FREE = {
                                     _vp, _int, _vp, _int, _vp, _vp],
     "qbxfmm_helmholtz3d_qbx_matrix": [_int, _vp, _vp, ctypes.c_double, ctypes.c_double,
                                       ctypes.c_double, ctypes.c_double, ctypes.c_double, _int,
-                                      _vp, _vp, _int, _vp, _int, _vp, _vp],
+                                      _vp, _vp, _int, _vp, _int, _int, _vp, _vp],
     "qbxfmm_cell_keys": [_int, _int, _vp, ctypes.POINTER(abi.QBXFMMCellGrid), _vp, _vp],
     "qbxfmm_associate_targets": [ctypes.POINTER(abi.QBXFMMAssocProblem), _vp, _vp],
     "qbxfmm_noalloc_error_word": [_pi, _vp],

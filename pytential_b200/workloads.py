@@ -180,22 +180,24 @@ def laplace3d_adjoint(nrefine: int = 4, ntargets: int = 5000, ncharges: int = 8,
 
 
 def _main(argv=None):
-    """``python -m pytential_b200.workloads NAME SIZE [APPLIES]``: build one of the
-    workloads (``laplace3d`` double layer or ``helmholtz3d`` combined field with 16
-    densities, SIZE = icosphere refinements; ``helmholtz2d`` Brakhage-Werner with 64
-    densities, SIZE = starfish elements) and run ``APPLIES`` whole applies
-    (target-specific near field) on the current GPU, printing the time of the last; a
-    driver for profilers."""
+    """``python -m pytential_b200.workloads NAME SIZE [APPLIES] [--mixed] [--fmm-backend
+    B]``: build one of the workloads (``laplace3d`` double layer or ``helmholtz3d``
+    combined field with 16 densities, SIZE = icosphere refinements; ``helmholtz2d``
+    Brakhage-Werner with 64 densities, SIZE = starfish elements) and run ``APPLIES``
+    whole applies (target-specific near field; FP64, or the mixed-precision form) on
+    the current GPU, printing the time of the last; a driver for profilers."""
     import argparse
     import time
 
     import torch
 
-    from .fmm import QBXApply
+    from .fmm import PRECISION_FP64, PRECISION_MIXED, QBXApply
     ap = argparse.ArgumentParser(prog="python -m pytential_b200.workloads")
     ap.add_argument("name", choices=["laplace3d", "helmholtz3d", "helmholtz2d"])
     ap.add_argument("size", type=int)
     ap.add_argument("applies", type=int, nargs="?", default=1)
+    ap.add_argument("--mixed", action="store_true", help="the mixed-precision form")
+    ap.add_argument("--fmm-backend", default="sumpy", choices=["sumpy", "fmmlib"])
     a = ap.parse_args(argv)
     if a.name == "laplace3d":
         wl = laplace3d_ellipsoid(nrefine=a.size)
@@ -204,7 +206,8 @@ def _main(argv=None):
     else:
         wl = helmholtz2d_starfish(nelements=a.size)
     qa = QBXApply(wl.geometry(), wl.spec, wl.qbx_order, wl.fmm_order, nrhs=wl.nrhs,
-                  target_specific_qbx=True)
+                  target_specific_qbx=True, fmm_backend=a.fmm_backend,
+                  precision=PRECISION_MIXED if a.mixed else PRECISION_FP64)
     dens = torch.from_numpy(wl.density).cuda()
     out = qa.new_output()
     for _ in range(a.applies):

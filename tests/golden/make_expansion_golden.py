@@ -93,6 +93,7 @@ def case_workload(kind):
     wl = c["make"]()
     geo = QBXFMMGeometryData(wl.discr, wl.targets, max_leaf_refine_weight=c["leaf"],
                              builders="host")
+    wl._geo = geo     # tree-order strengths (wl.tree_strengths) in this geometry's tree
     cq = c.get("cq", wl.spec.charge_coeff)
     cd = c.get("cd", wl.spec.dipole_coeff)
     return wl, geo, cq, cd
@@ -681,7 +682,7 @@ def compute(kind):
     k = float(np.real(wl.spec.wave_number)) if wl.spec.is_complex else 0.0
     fam = "helmholtz" if wl.spec.is_complex else "laplace"
     base = f"{fam}{wl.spec.kernel.dim}d"
-    s = wl.tree_strengths() if not hasattr(geo, "_x") else None
+    s = wl.tree_strengths()
     out = run_fmm(base, k, arrays, scalars, wl.fmm_order, wl.qbx_order, s, cq, cd)
     return dict(potentials=out, fingerprint=np.array(fingerprint(arrays)),
                 qbx_order=wl.qbx_order, fmm_order=wl.fmm_order, k=k, cq=cq, cd=cd,

@@ -35,12 +35,21 @@ def tol_for(wl):
 _cache = {}
 
 
+def backend_of(name):
+    """Workload names carry "@fmmlib" for the spherical-wave truncation of the
+    reference's fmmlib backend; otherwise the reference's default (sumpy)."""
+    base, _, be = name.partition("@")
+    return base, be or "sumpy"
+
+
 def wrangler_for(name):
     if name not in _cache:
-        wl = workload(name)
+        base, be = backend_of(name)
+        wl = workload(base)
         w = B200QBXExpansionWrangler(B200TreeIndependentDataForWrangler(wl.spec), wl.geometry(),
-                                     np.float64, wl.qbx_order, wl.fmm_order, nrhs=wl.nrhs)
-        _cache[name] = (wl, w, oracle_for(wl))
+                                     np.float64, wl.qbx_order, wl.fmm_order, nrhs=wl.nrhs,
+                                     fmm_backend=be)
+        _cache[name] = (wl, w, oracle_for(wl, fmm_backend=be))
     return _cache[name]
 
 
@@ -55,7 +64,8 @@ def host(t):
 
 ALL = ["2d-S", "2d-D", "3d-D-small", "3d-S-small", "2d-D-nrhs3", "h2d-BW-small",
        "h2d-S-small", "h2d-D-small", "h2d-BW-nrhs40", "h3d-CF-small", "h3d-S-small",
-       "h3d-D-small", "h3d-CF-p15"]
+       "h3d-D-small", "h3d-CF-p15", "h3d-CF-small@fmmlib", "h3d-D-small@fmmlib",
+       "h3d-CF-p15@fmmlib"]
 
 
 @pytest.mark.parametrize("name", ALL)
@@ -136,28 +146,29 @@ def test_drive_fmm_and_apply_match_checker(name):
     got = host(drive_fmm(None, w, [dev(flat)]))
     assert relerr(got, ref) < TOL
     ap = QBXApply(wl.geometry(), wl.spec, wl.qbx_order, wl.fmm_order, nrhs=wl.nrhs,
-                  device_geometry=w.dgeo, target_specific_qbx=False)
+                  device_geometry=w.dgeo, target_specific_qbx=False,
+                  fmm_backend=backend_of(name)[1])
     got2 = host(ap(dev(wl.density)))
     assert relerr(got2, ref) < TOL
     ap.check_error_word()
 
 
-@pytest.mark.parametrize("name", ["2d-S", "2d-D", "3d-D-small", "3d-S-small", "2d-D-nrhs3",
-                                  "h2d-BW-small", "h2d-S-small", "h2d-D-small",
-                                  "h2d-BW-nrhs40", "h3d-CF-small", "h3d-S-small", "h3d-D-small", "h3d-CF-p15"])
+@pytest.mark.parametrize("name", ALL)
 def test_target_specific_mode_matches_checker(name):
     """With target-specific QBX the list-1 near field is evaluated per target; the
     truncation is the same, so the apply equals the checker's (expansion-based) one."""
     wl, w, o = wrangler_for(name)
+    be = backend_of(name)[1]
     TOL = tol_for(wl)
     ref = o.apply(wl.tree_strengths())
     ap = QBXApply(wl.geometry(), wl.spec, wl.qbx_order, wl.fmm_order, nrhs=wl.nrhs,
-                  device_geometry=w.dgeo, target_specific_qbx=True)
+                  device_geometry=w.dgeo, target_specific_qbx=True, fmm_backend=be)
     got = host(ap(dev(wl.density)))
     assert relerr(got, ref) < TOL
     wt = B200QBXExpansionWrangler(B200TreeIndependentDataForWrangler(wl.spec), wl.geometry(),
                                   np.float64, wl.qbx_order, wl.fmm_order, nrhs=wl.nrhs,
-                                  device_geometry=w.dgeo, _use_target_specific_qbx=True)
+                                  device_geometry=w.dgeo, _use_target_specific_qbx=True,
+                                  fmm_backend=be)
     flat = wl.discr.upsample_density(wl.density) * wl.discr.quad_weights
     assert relerr(host(drive_fmm(None, wt, [dev(flat)])), ref) < TOL
 
@@ -320,3 +331,21 @@ def test_bad_list_entry_reports_instead_of_faulting():
         w.check_error_word()
     torch.cuda.synchronize()
     assert torch.ones(4, device="cuda").sum().item() == 4.0
+
+
+@pytest.mark.parametrize("name", ["h3d-CF-small", "h3d-CF-p15"])
+def test_mixed_precision_helmholtz3d_error(name):
+    """3D Helmholtz mixed form (FP32 arithmetic in M2QBXL and M2L, FP64 everywhere
+    else, FP64 expansions throughout): its error against the FP64 checker is stated
+    and bounded (max-norm, relative)."""
+    from pytential_b200.fmm import PRECISION_MIXED
+    wl, w, o = wrangler_for(name)
+    ref = o.apply(wl.tree_strengths())
+    for tsq in (False, True):
+        ap = QBXApply(wl.geometry(), wl.spec, wl.qbx_order, wl.fmm_order, nrhs=wl.nrhs,
+                      device_geometry=w.dgeo, target_specific_qbx=tsq, precision=PRECISION_MIXED)
+        got = host(ap(dev(wl.density)))
+        ap.check_error_word()
+        err = relerr(got, ref)
+        print(f"{name} tsqbx={tsq}: mixed vs FP64 checker {err:.2e}")
+        assert 0.0 < err < 1e-5, (tsq, err)

@@ -223,3 +223,27 @@ def test_helmholtz2d_green_representation():
     val = oS.apply(sS)[0] - oD.apply(sD)[0]
     ref = np.where(inside, u(pts), 0)
     assert relerr(val, ref) < 1e-6
+
+
+def test_oracle_bessel_hankel_match_reference_golden_values():
+    """The checker's spherical Bessel (Miller) and Hankel (upward) recurrences against
+    the reference's own golden values for its jfuns3d / h3dall routines
+    (test/test_target_specific_qbx.py:44-119: j_n, j_n' at z = 3i; h_n, h_n' at
+    z = 2 + 3i; n <= 9), at the tolerance of that test (numpy allclose)."""
+    import os
+
+    from helpers import GOLDEN
+    z = np.load(os.path.join(GOLDEN, "bessel_reference.npz"))
+    L = lib()
+    P = lambda a: ctypes.c_void_p(a.ctypes.data)  # noqa: E731
+    N = 10
+    for fn, zz, val, der in [("orc_h3_sph_j_complex", complex(z["j_z"]), z["j_expected"],
+                              z["jder_expected"]),
+                             ("orc_h3_sph_h_complex", complex(z["h_z"]), z["h_expected"],
+                              z["hder_expected"])]:
+        f = np.zeros(N + 1, complex)
+        getattr(L, fn)(N, ctypes.c_double(zz.real), ctypes.c_double(zz.imag), P(f))
+        # f_n' = f_{n-1} - (n + 1) / z f_n, f_0' = -f_1
+        d = np.array([-f[1]] + [f[n - 1] - (n + 1) / zz * f[n] for n in range(1, N)])
+        assert np.allclose(f[:N], val, rtol=1e-13, atol=1e-15), fn
+        assert np.allclose(d, der, rtol=1e-13, atol=1e-15), fn
