@@ -36,6 +36,23 @@ int qbxfmm_plan_create(const qbxfmm_kernel* kernel, const qbxfmm_geometry* geome
                        qbxfmm_plan** plan);
 int qbxfmm_plan_destroy(qbxfmm_plan* plan);
 
+/* Launch shapes of the 3D Helmholtz stage kernels: densities per CTA of each (0: the
+ * library's built-in choice from nrhs and shared-memory limits).  Set by an autotuner
+ * that times the candidates on the plan's own geometry (pytential_b200.autotune);
+ * the reference has no counterpart (loopy picks its work-group shapes at code
+ * generation, pytential/qbx/interactions.py:149, 273, 391, 516).  Results do not
+ * depend on the choice beyond the summation order. */
+typedef struct qbxfmm_tuning {
+  int32_t m2qbxl_densities;   /* 1, 4, 8 (16: mixed precision only) */
+  int32_t m2l_densities;      /* 1, 4, 8 (16: mixed precision only) */
+  int32_t p2e_densities;      /* P2M / P2L: 1, 4, 8 */
+  int32_t l2qbxl_densities;   /* 1, 4 */
+  int32_t tsqbx_densities;    /* 1, 4, 16 */
+} qbxfmm_tuning;
+
+int qbxfmm_plan_set_tuning(qbxfmm_plan* plan, const qbxfmm_tuning* tuning);
+int qbxfmm_plan_get_tuning(const qbxfmm_plan* plan, qbxfmm_tuning* tuning);
+
 /* byte sizes of the workspace buffers, in qbxfmm_workspace field order:
  * strengths, mpoles, locals, qbx_exps, pot_nonqbx, pot_tree, translations,
  * pair_scratch (the last two are 0 when the matrix form is not available) */

@@ -31,6 +31,13 @@ _pi = ctypes.POINTER(ctypes.c_int32)
 _pd = ctypes.POINTER(ctypes.c_double)
 
 
+class QBXFMMTuning(ctypes.Structure):
+    """Densities per CTA of the 3D Helmholtz stage kernels (0: built-in choice)."""
+    _fields_ = [("m2qbxl_densities", ctypes.c_int32), ("m2l_densities", ctypes.c_int32),
+                ("p2e_densities", ctypes.c_int32), ("l2qbxl_densities", ctypes.c_int32),
+                ("tsqbx_densities", ctypes.c_int32)]
+
+
 class QBXFMMKernel(ctypes.Structure):
     _fields_ = [
         ("family", _i32), ("dim", _i32),

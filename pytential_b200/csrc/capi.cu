@@ -6,6 +6,7 @@
 // device buffers; the library allocates no device memory.
 #include <algorithm>
 #include <array>
+#include <initializer_list>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -583,7 +584,7 @@ int qbxfmm_multipole_to_local(const qbxfmm_plan* p, const void* mpoles, void* lo
     QBX_TRY(h3_launch_m2l_rot(p->geo, p->kern.fmm_order, p->kern.nrhs, (const double2*)mpoles,
                               (double2*)locals, p->trans_dev + o[3],
                               reinterpret_cast<const double2*>(p->trans_dev + o[4]), clsmap,
-                              error_word, S(stream), p->mixed),
+                              error_word, S(stream), p->mixed, p->hc.rb_m2l),
             "multipole_to_local");
     return QBXFMM_OK;
   }
@@ -835,6 +836,42 @@ int qbxfmm_assemble(const qbxfmm_plan* p, const void* pot_nonqbx, const void* po
     QBX_TRY(launch_assemble(p->geo, p->kern.nrhs, (const double*)pot_nonqbx,
                             (const double*)pot_tree, (double*)out, S(stream)),
             "assemble");
+  return QBXFMM_OK;
+}
+
+int qbxfmm_plan_set_tuning(qbxfmm_plan* p, const qbxfmm_tuning* t)
+{
+  if (int rc = check_plan(p)) return rc;
+  if (!t) return fail(QBXFMM_ERR_ARG, "null tuning");
+  auto ok = [](int v, std::initializer_list<int> allowed) {
+    if (v == 0) return true;
+    for (int a : allowed)
+      if (v == a) return true;
+    return false;
+  };
+  if (!ok(t->m2qbxl_densities, {1, 4, 8, 16}) || !ok(t->m2l_densities, {1, 4, 8, 16}) ||
+      !ok(t->p2e_densities, {1, 4, 8}) || !ok(t->l2qbxl_densities, {1, 4}) ||
+      !ok(t->tsqbx_densities, {1, 4, 16}))
+    return fail(QBXFMM_ERR_ARG, "tuning: unsupported densities-per-CTA value");
+  if (!p->mixed && (t->m2qbxl_densities == 16 || t->m2l_densities == 16))
+    return fail(QBXFMM_ERR_ARG, "tuning: 16 densities per CTA is a mixed-precision shape");
+  p->hc.rb_rot = t->m2qbxl_densities;
+  p->hc.rb_m2l = t->m2l_densities;
+  p->hc.rb_p2e = t->p2e_densities;
+  p->hc.rb_l2q = t->l2qbxl_densities;
+  p->hc.rb_ts = t->tsqbx_densities;
+  return QBXFMM_OK;
+}
+
+int qbxfmm_plan_get_tuning(const qbxfmm_plan* p, qbxfmm_tuning* t)
+{
+  if (int rc = check_plan(p)) return rc;
+  if (!t) return fail(QBXFMM_ERR_ARG, "null tuning");
+  t->m2qbxl_densities = p->hc.rb_rot;
+  t->m2l_densities = p->hc.rb_m2l;
+  t->p2e_densities = p->hc.rb_p2e;
+  t->l2qbxl_densities = p->hc.rb_l2q;
+  t->tsqbx_densities = p->hc.rb_ts;
   return QBXFMM_OK;
 }
 

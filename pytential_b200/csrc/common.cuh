@@ -138,6 +138,9 @@ struct HelmCoeffs {
   double k;
   int taylor = 0;   // 3D: the reference's default truncation (sumpy's compressed Taylor
                     // expansions: regular waves with j_n cut to its power series)
+  // launch shapes picked by the plan's tuning (qbxfmm_tuning; 0: built-in choice):
+  // densities per CTA of M2QBXL, M2L, P2M / P2L, L2QBXL, the target-specific near field
+  int rb_rot = 0, rb_m2l = 0, rb_p2e = 0, rb_l2q = 0, rb_ts = 0;
 };
 
 }  // namespace qbx

@@ -167,7 +167,7 @@ cudaError_t h3_launch_m2l_tables(int pf, int ndir, int ncoax, const double* dirs
 cudaError_t h3_launch_m2l_rot(const qbxfmm_geometry& g, int pf, int nrhs, const double2* mp,
                               double2* lo, const double* Dtab, const double2* Ctab,
                               const double* clsmap, int32_t* err, cudaStream_t st,
-                              bool fp32 = false);
+                              bool fp32 = false, int rb = 0);
 // rot: rotation tables of h3_rotation_tables (start values, recurrence factors,
 // lambda = 0 Gaunt slice)
 // fp32: the mixed-precision form (FP32 arithmetic, FP64 expansions in and out)

@@ -1822,10 +1822,26 @@ static cudaError_t h3_m2l_rot_launch(const qbxfmm_geometry& g, int pf, int nrhs,
 
 cudaError_t h3_launch_m2l_rot(const qbxfmm_geometry& g, int pf, int nrhs, const double2* mp,
                               double2* lo, const double* Dtab, const double2* Ctab,
-                              const double* clsmap, int32_t* err, cudaStream_t st, bool fp32)
+                              const double* clsmap, int32_t* err, cudaStream_t st, bool fp32,
+                              int rb)
 {
   if (g.nttp_boxes == 0 || g.m2l_nclasses == 0) return cudaSuccess;
   if (pf > H3_MAXP) return cudaErrorInvalidValue;
+  switch (rb) {   // the plan's tuning
+    case 1:
+      return fp32 ? h3_m2l_rot_launch<float, 1>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err, st)
+                  : h3_m2l_rot_launch<double, 1>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err, st);
+    case 4:
+      return fp32 ? h3_m2l_rot_launch<float, 4>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err, st)
+                  : h3_m2l_rot_launch<double, 4>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err, st);
+    case 8:
+      return fp32 ? h3_m2l_rot_launch<float, 8>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err, st)
+                  : h3_m2l_rot_launch<double, 8>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err, st);
+    case 16:
+      if (fp32) return h3_m2l_rot_launch<float, 16>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err, st);
+      return cudaErrorInvalidValue;
+    default: break;
+  }
   if (fp32) {   // mixed form: FP32 arithmetic, all 16 densities of a pair's tables at once
     if (nrhs >= 16) return h3_m2l_rot_launch<float, 16>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err, st);
     if (nrhs >= 8) return h3_m2l_rot_launch<float, 8>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err, st);
@@ -1868,6 +1884,9 @@ static cudaError_t h3_p2e_launch(int nbox, size_t sh, const qbxfmm_geometry& g, 
                                                                           err);                 \
     return cudaGetLastError();                                                                  \
   }
+  if (hc.rb_p2e == 8) QBX_H3_P2E(8)   // the plan's tuning
+  if (hc.rb_p2e == 4) QBX_H3_P2E(4)
+  if (hc.rb_p2e == 1) QBX_H3_P2E(1)
   if (nrhs >= 8) QBX_H3_P2E(8)
   if (nrhs >= 3) QBX_H3_P2E(4)
   QBX_H3_P2E(1)
@@ -1966,6 +1985,12 @@ template <int Q>
 static cudaError_t h3_tsqbx_q(const qbxfmm_geometry& g, HelmCoeffs hc, int nrhs, const double2* s,
                               double2* pt, int32_t* err, cudaStream_t st)
 {
+  switch (hc.rb_ts) {   // the plan's tuning
+    case 1: return h3_tsqbx_qr<Q, 1>(g, hc, nrhs, s, pt, err, st);
+    case 4: return h3_tsqbx_qr<Q, 4>(g, hc, nrhs, s, pt, err, st);
+    case 16: return h3_tsqbx_qr<Q, 16>(g, hc, nrhs, s, pt, err, st);
+    default: break;
+  }
   if (nrhs == 1) return h3_tsqbx_qr<Q, 1>(g, hc, nrhs, s, pt, err, st);
   if (nrhs <= 4) return h3_tsqbx_qr<Q, 4>(g, hc, nrhs, s, pt, err, st);
   return h3_tsqbx_qr<Q, 16>(g, hc, nrhs, s, pt, err, st);
@@ -2019,6 +2044,16 @@ static cudaError_t h3_rot_q(const qbxfmm_geometry& g, HelmCoeffs hc, int pf, int
                             const double2* e, const double* rot, double2* qe, int32_t* err,
                             cudaStream_t st)
 {
+  switch (hc.rb_rot) {   // the plan's tuning
+    case 1: return h3_rot_launch<R, FROM_LOCAL, Q, 1>(g, hc, pf, nrhs, e, rot, qe, err, st);
+    case 4: return h3_rot_launch<R, FROM_LOCAL, Q, 4>(g, hc, pf, nrhs, e, rot, qe, err, st);
+    case 8: return h3_rot_launch<R, FROM_LOCAL, Q, 8>(g, hc, pf, nrhs, e, rot, qe, err, st);
+    case 16:
+      if constexpr (!std::is_same<R, double>::value)
+        return h3_rot_launch<R, FROM_LOCAL, Q, 16>(g, hc, pf, nrhs, e, rot, qe, err, st);
+      return cudaErrorInvalidValue;
+    default: break;
+  }
   const size_t two_per_sm = 112 * 1024;
   if constexpr (!std::is_same<R, double>::value)
     if (nrhs >= 16 && h3_rot_smem<R, FROM_LOCAL, Q, 16>(pf) <= two_per_sm)

@@ -545,7 +545,8 @@ cudaError_t l2qbxl_taylor_q(const qbxfmm_geometry& g, HelmCoeffs hc, int p, int 
                             const double2* lo, const double2* G0, const double2* Gq, double2* qe,
                             int32_t* err, cudaStream_t st)
 {
-  if (nrhs >= 4) return l2qbxl_taylor_launch<Q, 4>(g, hc, p, nrhs, lo, G0, Gq, qe, err, st);
+  if (hc.rb_l2q == 4 || (hc.rb_l2q == 0 && nrhs >= 4))   // the plan's tuning, else by nrhs
+    return l2qbxl_taylor_launch<Q, 4>(g, hc, p, nrhs, lo, G0, Gq, qe, err, st);
   return l2qbxl_taylor_launch<Q, 1>(g, hc, p, nrhs, lo, G0, Gq, qe, err, st);
 }
 

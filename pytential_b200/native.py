@@ -44,6 +44,8 @@ _STAGES = {
     "qbxfmm_apply_noalloc": [ctypes.POINTER(abi.QBXFMMUpsample), _vp, _vp, _vp],
     "qbxfmm_apply_host": [ctypes.POINTER(abi.QBXFMMUpsample),
                           ctypes.POINTER(abi.QBXFMMWorkspace), _vp, _vp, _vp, _vp, _vp],
+    "qbxfmm_plan_set_tuning": [ctypes.POINTER(abi.QBXFMMTuning)],
+    "qbxfmm_plan_get_tuning": [ctypes.POINTER(abi.QBXFMMTuning)],
 }
 
 # every symbol include/qbxfmm_api.h declares

@@ -181,11 +181,12 @@ def laplace3d_adjoint(nrefine: int = 4, ntargets: int = 5000, ncharges: int = 8,
 
 def _main(argv=None):
     """``python -m pytential_b200.workloads NAME SIZE [APPLIES] [--mixed] [--fmm-backend
-    B]``: build one of the workloads (``laplace3d`` double layer or ``helmholtz3d``
+    B] [--tune]``: build one of the workloads (``laplace3d`` double layer or ``helmholtz3d``
     combined field with 16 densities, SIZE = icosphere refinements; ``helmholtz2d``
     Brakhage-Werner with 64 densities, SIZE = starfish elements) and run ``APPLIES``
     whole applies (target-specific near field; FP64, or the mixed-precision form) on
-    the current GPU, printing the time of the last; a driver for profilers."""
+    the current GPU, printing the time of the last (after the autotuner's choice with
+    ``--tune``); a driver for profilers."""
     import argparse
     import time
 
@@ -198,6 +199,8 @@ def _main(argv=None):
     ap.add_argument("applies", type=int, nargs="?", default=1)
     ap.add_argument("--mixed", action="store_true", help="the mixed-precision form")
     ap.add_argument("--fmm-backend", default="sumpy", choices=["sumpy", "fmmlib"])
+    ap.add_argument("--tune", action="store_true",
+                    help="run the launch-shape autotuner first and print its choice")
     a = ap.parse_args(argv)
     if a.name == "laplace3d":
         wl = laplace3d_ellipsoid(nrefine=a.size)
@@ -210,6 +213,12 @@ def _main(argv=None):
                   precision=PRECISION_MIXED if a.mixed else PRECISION_FP64)
     dens = torch.from_numpy(wl.density).cuda()
     out = qa.new_output()
+    if a.tune:
+        from .autotune import autotune
+        res = autotune(qa)
+        print("tuning:", res["choice"])
+        for knob, ms in res["ms"].items():
+            print(f"  {knob}: " + ", ".join(f"{c}: {t:.3f} ms" for c, t in ms.items()))
     for _ in range(a.applies):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -219,5 +228,95 @@ def _main(argv=None):
     print(f"{wl.name}: {1e3 * (time.perf_counter() - t0):.2f} ms per apply")
 
 
+def _solve2d(argv=None):
+    """``python -m pytential_b200.workloads solve2d [NELEMENTS] [NRHS]``: the batched
+    Brakhage-Werner exterior Dirichlet solve of the 2D Helmholtz benchmark (k 20,
+    D - ik S, starfish, qbx_order 5, fmm_order 20, plane-wave right-hand sides, GMRES to
+    1e-8 with every density through one apply per iteration) on the current GPU:
+    prints iterations, wall time of a warm solve and the largest true residual."""
+    import time
+
+    import torch
+
+    from .fmm import QBXApply
+    from .gmres import gmres
+    argv = list(argv or [])
+    nel = int(argv[0]) if argv else 2048
+    nrhs = int(argv[1]) if len(argv) > 1 else 64
+    wl = helmholtz2d_starfish(nelements=nel, nrhs=nrhs)
+    ap = QBXApply(wl.geometry(), wl.spec, wl.qbx_order, wl.fmm_order, nrhs=wl.nrhs)
+    b = torch.from_numpy(wl.density).cuda()
+    napply = [0]
+
+    def op(X):
+        napply[0] += 1
+        return ap(X).clone()
+    gmres(op, b, tol=1e-8, restart=50, maxiter=300)          # warm-up solve
+    napply[0] = 0
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    res = gmres(op, b, tol=1e-8, restart=50, maxiter=300)
+    torch.cuda.synchronize()
+    t = time.perf_counter() - t0
+    r = b - ap(res.solution)
+    rel = float((torch.linalg.norm(r, dim=1) / torch.linalg.norm(b, dim=1)).max())
+    print(f"{wl.name}: {res.iteration_count} iterations, {napply[0]} applies, {t:.3f} s "
+          f"(warm), max true relative residual {rel:.2e}, success {res.success}")
+
+
+def _adjoint3d(argv=None):
+    """``python -m pytential_b200.workloads adjoint3d [NREFINE] [--mixed]``: the 3D
+    Laplace single-layer adjoint benchmark (ellipsoid, 5000 targets on the sphere of
+    radius 3, qbx_order 4, fmm_order 12): times the forward apply and forward +
+    backward (density and target-position gradients) on the current GPU."""
+    import time
+
+    import torch
+
+    from .adjoint import FarFieldSingleLayer, single_layer
+    from .fmm import PRECISION_FP64, PRECISION_MIXED
+    argv = list(argv or [])
+    mixed = "--mixed" in argv
+    argv = [a for a in argv if a != "--mixed"]
+    nref = int(argv[0]) if argv else 4
+    w = laplace3d_adjoint(nrefine=nref)
+    op = FarFieldSingleLayer(w.discr, w.targets, w.qbx_order, w.fmm_order,
+                             precision=PRECISION_MIXED if mixed else PRECISION_FP64)
+    sig0 = torch.from_numpy(w.sigma).cuda()
+    X0 = torch.from_numpy(w.targets).cuda()
+    g = torch.from_numpy(w.g(w.targets)).cuda()
+
+    def fwd_bwd():
+        sigma = sig0.clone().requires_grad_(True)
+        X = X0.clone().requires_grad_(True)
+        u = single_layer(op, sigma, X)
+        J = 0.5 * ((u - g) ** 2).sum()
+        J.backward()
+        return sigma.grad, X.grad
+    for _ in range(3):
+        op.apply(sig0)
+        fwd_bwd()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(5):
+        op.apply(sig0)
+    torch.cuda.synchronize()
+    tf = (time.perf_counter() - t0) / 5
+    t0 = time.perf_counter()
+    for _ in range(5):
+        fwd_bwd()
+    torch.cuda.synchronize()
+    tb = (time.perf_counter() - t0) / 5
+    print(f"3D Laplace S adjoint, icosphere-{nref} ({w.discr.ndofs} nodes), "
+          f"{w.targets.shape[1]} targets, {'mixed' if mixed else 'FP64'}: forward "
+          f"{1e3 * tf:.2f} ms, forward + backward {1e3 * tb:.2f} ms")
+
+
 if __name__ == "__main__":
-    _main()
+    import sys as _sys
+    if len(_sys.argv) > 1 and _sys.argv[1] == "solve2d":
+        _solve2d(_sys.argv[2:])
+    elif len(_sys.argv) > 1 and _sys.argv[1] == "adjoint3d":
+        _adjoint3d(_sys.argv[2:])
+    else:
+        _main()

@@ -66,7 +66,7 @@ def test_gradients_match_central_differences(small):
         uu = op.apply(torch.from_numpy(s).cuda()).cpu().numpy()
         return 0.5 * ((uu - w.g(w.targets)) ** 2).sum()
 
-    for _ in range(8):
+    for _ in range(32):     # the 32 seeded directions of the adjoint benchmark
         v = rng.normal(size=w.sigma.shape)
         fd = (J_sigma(w.sigma + h * v) - J_sigma(w.sigma - h * v)) / (2 * h)
         assert abs(fd - gs @ v) <= 1e-6 * abs(gs @ v) + 1e-12
@@ -79,7 +79,7 @@ def test_gradients_match_central_differences(small):
         uu = (A_s / (4 * np.pi * np.sqrt((dd ** 2).sum(0)))).sum(1)
         return 0.5 * ((uu - w.g(x)) ** 2).sum()
 
-    for _ in range(4):
+    for _ in range(32):
         V = rng.normal(size=w.targets.shape)
         fd = (J_x(w.targets + h * V) - J_x(w.targets - h * V)) / (2 * h)
         an = (gx * V).sum()
