@@ -43,7 +43,7 @@ int qbxfmm_plan_destroy(qbxfmm_plan* plan);
  * generation, pytential/qbx/interactions.py:149, 273, 391, 516).  Results do not
  * depend on the choice beyond the summation order. */
 typedef struct qbxfmm_tuning {
-  int32_t m2qbxl_densities;   /* 1, 4, 8 (16: mixed precision only) */
+  int32_t m2qbxl_densities;   /* 1, 4, 8, 16 (FP64: two warps per center share the tables) */
   int32_t m2l_densities;      /* 1, 4, 8 (16: mixed precision only) */
   int32_t p2e_densities;      /* P2M / P2L: 1, 4, 8 */
   int32_t l2qbxl_densities;   /* 1, 4 */
@@ -52,6 +52,21 @@ typedef struct qbxfmm_tuning {
 
 int qbxfmm_plan_set_tuning(qbxfmm_plan* plan, const qbxfmm_tuning* tuning);
 int qbxfmm_plan_get_tuning(const qbxfmm_plan* plan, qbxfmm_tuning* tuning);
+
+/* Per-level FMM orders: orders[l] (0 <= orders[l] <= the kernel's fmm_order) is the
+ * order of the multipole and local expansions of the boxes on tree level l; nlevels
+ * must equal the geometry's.  Replaces fmm_level_to_order(kernel, kernel_args, tree,
+ * level) (pytential/qbx/__init__.py:276-285; the wrangler's level_orders,
+ * pytential/qbx/fmm.py:163-166, read per source level at :280-283 and :327-330).  The box expansions stay allocated at fmm_order,
+ * which should be the largest level order; the stages that write them truncate each
+ * box to its level's order (M2M and L2L level by level), which equals translating
+ * between the two orders for every basis except the compressed-Taylor 3D Helmholtz
+ * one (fmm_backend QBXFMM_BACKEND_SUMPY, rejected with QBXFMM_ERR_UNSUPPORTED).  The
+ * matrix forms of the 3D Laplace translations are not used while level orders are
+ * set.  orders == NULL restores fmm_order on every level.  Boxes must be numbered
+ * by level (as boxtree numbers them). */
+int qbxfmm_plan_set_level_orders(qbxfmm_plan* plan, const int32_t* orders, int32_t nlevels);
+int qbxfmm_plan_get_level_orders(const qbxfmm_plan* plan, int32_t* orders, int32_t nlevels);
 
 /* byte sizes of the workspace buffers, in qbxfmm_workspace field order:
  * strengths, mpoles, locals, qbx_exps, pot_nonqbx, pot_tree, translations,

@@ -41,6 +41,7 @@ def lib():
             f = getattr(_LIB, name)
             f.restype = ctypes.c_int
         _LIB.orc_ncoeff.restype = ctypes.c_int
+        _LIB.orc_set_level_orders.restype = ctypes.c_int
     return _LIB
 
 
@@ -49,11 +50,21 @@ def _p(a):
 
 
 class Oracle:
-    """Host-side QBX-FMM over a geometry-data object (float64/complex128)."""
+    """Host-side QBX-FMM over a geometry-data object (float64/complex128).
+
+    ``level_orders`` (Laplace only): one FMM order per tree level, at most
+    ``fmm_order``, each box expansion truncated to its level's order and every
+    translation run between the orders of its two ends."""
 
     def __init__(self, geo, *, dim, qbx_order, fmm_order, nrhs=1,
                  charge_coeff=0.0, dipole_coeff=0.0, family=abi.QBXFMM_LAPLACE, k=0.0,
-                 fmm_backend="sumpy"):
+                 fmm_backend="sumpy", level_orders=None):
+        if level_orders is not None:
+            if family != abi.QBXFMM_LAPLACE:
+                raise NotImplementedError("the checker's per-level orders cover Laplace")
+            if max(level_orders) > fmm_order or min(level_orders) < 0:
+                raise ValueError("level orders must be in [0, fmm_order]")
+        self.level_orders = None if level_orders is None else [int(o) for o in level_orders]
         self.geo = geo
         self.scalars, self.arrays = abi.geometry_arrays(geo)
         self.g = abi.make_geometry_struct(self.scalars, self.arrays,
@@ -68,6 +79,11 @@ class Oracle:
         self.ncq = abi.ncoeff(family, dim, qbx_order)
 
     def _call(self, name, *args):
+        if self.level_orders is None:
+            lib().orc_set_level_orders(None, 0)
+        else:
+            n = len(self.level_orders)
+            lib().orc_set_level_orders((ctypes.c_int * n)(*self.level_orders), n)
         rc = getattr(lib(), name)(ctypes.byref(self.kern), ctypes.byref(self.g), *args)
         if rc != 0:
             raise RuntimeError(f"{name} failed with status {rc}")

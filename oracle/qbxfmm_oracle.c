@@ -367,6 +367,31 @@ typedef struct {
   double cq, cd;
 } ctx_t;
 
+/* Per-level FMM orders of the Laplace stages (the reference's fmm_level_to_order,
+   pytential/qbx/__init__.py:276-285, read per level as the wrangler's level_orders,
+   pytential/qbx/fmm.py:280-283, 327-330): each box expansion has its level's order and
+   every translation runs between the orders of its two ends (expansions are stored at
+   fmm_order with zeros above the box's order).  Empty: fmm_order everywhere. */
+static int g_lorders[64];
+static int g_nlorders = 0;
+
+int orc_set_level_orders(const int* orders, int nlevels)
+{
+  if (!orders || nlevels <= 0) {
+    g_nlorders = 0;
+    return 0;
+  }
+  if (nlevels > 64) return QBXFMM_ERR_ARG;
+  for (int l = 0; l < nlevels; ++l) g_lorders[l] = orders[l];
+  g_nlorders = nlevels;
+  return 0;
+}
+
+static int lp(const ctx_t* c, int level)
+{
+  return (g_nlorders && level >= 0 && level < g_nlorders) ? g_lorders[level] : c->pf;
+}
+
 static int make_ctx(const qbxfmm_kernel* k, ctx_t* c)
 {
   if (k->family != QBXFMM_LAPLACE) return QBXFMM_ERR_UNSUPPORTED;
@@ -454,9 +479,9 @@ int orc_form_multipoles(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
           if (c.cd != 0) load(g->source_normals, g->nsources, s, c.dim, nv);
           double st = strengths[(size_t)r * g->nsources + s];
           if (c.dim == 3)
-            lap3_p2m(c.pf, rho, ctr, y, c.cq * st, c.cd * st, nv, M, work);
+            lap3_p2m(lp(&c, g->box_levels[b]), rho, ctr, y, c.cq * st, c.cd * st, nv, M, work);
           else
-            lap2_p2m(c.pf, rho, ctr, y, c.cq * st, c.cd * st, nv, M);
+            lap2_p2m(lp(&c, g->box_levels[b]), rho, ctr, y, c.cq * st, c.cd * st, nv, M);
         }
       }
     }
@@ -493,8 +518,8 @@ int orc_coarsen_multipoles(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
           for (int r = 0; r < c.nrhs; ++r) {
             const cplx* Min = mpoles + ((size_t)ch * c.nrhs + r) * c.ncf;
             cplx* Mout = mpoles + ((size_t)b * c.nrhs + r) * c.ncf;
-            if (c.dim == 3) lap3_m2m(c.pf, rho_c, rho_p, d, Min, Mout, work);
-            else lap2_m2m(c.pf, rho_c, rho_p, d, Min, Mout);
+            if (c.dim == 3) lap3_m2m(lp(&c, lev), rho_c, rho_p, d, Min, Mout, work);
+            else lap2_m2m(lp(&c, lev), rho_c, rho_p, d, Min, Mout);
           }
         }
       }
@@ -564,8 +589,9 @@ int orc_multipole_to_local(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
         for (int r = 0; r < c.nrhs; ++r) {
           const cplx* Min = mpoles + ((size_t)sb * c.nrhs + r) * c.ncf;
           cplx* Lout = locals + ((size_t)tb * c.nrhs + r) * c.ncf;
-          if (c.dim == 3) lap3_m2l(c.pf, c.pf, rho, rho, d, Min, Lout, work);
-          else lap2_m2l(c.pf, c.pf, rho, rho, d, Min, Lout);
+          const int ps = lp(&c, g->box_levels[sb]), pt = lp(&c, g->box_levels[tb]);
+          if (c.dim == 3) lap3_m2l(ps, pt, rho, rho, d, Min, Lout, work);
+          else lap2_m2l(ps, pt, rho, rho, d, Min, Lout);
         }
       }
     }
@@ -600,7 +626,8 @@ int orc_eval_multipoles(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
           for (int r = 0; r < c.nrhs; ++r) {
             const cplx* M = mpoles + ((size_t)sb * c.nrhs + r) * c.ncf;
             pot[(size_t)r * g->nfiltered_targets + t] +=
-                (c.dim == 3) ? lap3_m2p(c.pf, rho, cs, x, M, work) : lap2_m2p(c.pf, rho, cs, x, M);
+                (c.dim == 3) ? lap3_m2p(lp(&c, g->box_levels[sb]), rho, cs, x, M, work)
+                             : lap2_m2p(lp(&c, g->box_levels[sb]), rho, cs, x, M);
           }
         }
       }
@@ -636,8 +663,8 @@ int orc_form_locals(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
           for (int r = 0; r < c.nrhs; ++r) {
             double st = strengths[(size_t)r * g->nsources + s];
             cplx* L = locals + ((size_t)tb * c.nrhs + r) * c.ncf;
-            if (c.dim == 3) lap3_p2l(c.pf, rho, ct, y, c.cq * st, c.cd * st, nv, L, work);
-            else lap2_p2l(c.pf, rho, ct, y, c.cq * st, c.cd * st, nv, L);
+            if (c.dim == 3) lap3_p2l(lp(&c, g->box_levels[tb]), rho, ct, y, c.cq * st, c.cd * st, nv, L, work);
+            else lap2_p2l(lp(&c, g->box_levels[tb]), rho, ct, y, c.cq * st, c.cd * st, nv, L);
           }
         }
       }
@@ -670,8 +697,8 @@ int orc_refine_locals(const qbxfmm_kernel* kern, const qbxfmm_geometry* g, cplx*
         for (int r = 0; r < c.nrhs; ++r) {
           const cplx* Lin = locals + ((size_t)par * c.nrhs + r) * c.ncf;
           cplx* Lout = locals + ((size_t)b * c.nrhs + r) * c.ncf;
-          if (c.dim == 3) lap3_l2l(c.pf, c.pf, rho_p, rho_c, d, Lin, Lout, work);
-          else lap2_l2l(c.pf, c.pf, rho_p, rho_c, d, Lin, Lout);
+          if (c.dim == 3) lap3_l2l(lp(&c, lev - 1), lp(&c, lev), rho_p, rho_c, d, Lin, Lout, work);
+          else lap2_l2l(lp(&c, lev - 1), lp(&c, lev), rho_p, rho_c, d, Lin, Lout);
         }
       }
       free(work);
@@ -703,7 +730,8 @@ int orc_eval_locals(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
         for (int r = 0; r < c.nrhs; ++r) {
           const cplx* L = locals + ((size_t)tb * c.nrhs + r) * c.ncf;
           pot[(size_t)r * g->nfiltered_targets + t] +=
-              (c.dim == 3) ? lap3_l2p(c.pf, rho, ct, x, L, work) : lap2_l2p(c.pf, rho, ct, x, L);
+              (c.dim == 3) ? lap3_l2p(lp(&c, g->box_levels[tb]), rho, ct, x, L, work)
+                           : lap2_l2p(lp(&c, g->box_levels[tb]), rho, ct, x, L);
         }
       }
     }
@@ -793,8 +821,8 @@ int orc_translate_box_multipoles_to_qbx_local(const qbxfmm_kernel* kern,
         for (int r = 0; r < c.nrhs; ++r) {
           const cplx* M = mpoles + ((size_t)sb * c.nrhs + r) * c.ncf;
           cplx* L = qbx_exps + ((size_t)ctr * c.nrhs + r) * c.ncq;
-          if (c.dim == 3) lap3_m2l(c.pf, c.pq, rho_s, rho_t, d, M, L, work);
-          else lap2_m2l(c.pf, c.pq, rho_s, rho_t, d, M, L);
+          if (c.dim == 3) lap3_m2l(lp(&c, g->box_levels[sb]), c.pq, rho_s, rho_t, d, M, L, work);
+          else lap2_m2l(lp(&c, g->box_levels[sb]), c.pq, rho_s, rho_t, d, M, L);
         }
       }
     }
@@ -828,8 +856,8 @@ int orc_translate_box_local_to_qbx_local(const qbxfmm_kernel* kern,
       for (int r = 0; r < c.nrhs; ++r) {
         const cplx* Lin = locals + ((size_t)tb * c.nrhs + r) * c.ncf;
         cplx* L = qbx_exps + ((size_t)ctr * c.nrhs + r) * c.ncq;
-        if (c.dim == 3) lap3_l2l(c.pf, c.pq, rho_b, rho_c, d, Lin, L, work);
-        else lap2_l2l(c.pf, c.pq, rho_b, rho_c, d, Lin, L);
+        if (c.dim == 3) lap3_l2l(lp(&c, g->box_levels[tb]), c.pq, rho_b, rho_c, d, Lin, L, work);
+        else lap2_l2l(lp(&c, g->box_levels[tb]), c.pq, rho_b, rho_c, d, Lin, L);
       }
     }
     free(work);

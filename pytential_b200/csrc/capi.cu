@@ -36,6 +36,10 @@ struct qbxfmm_plan {
   TransHost th;
   TransCfg tc;
   int device = -1;                         // CUDA device current at plan creation
+  // per-level FMM orders (empty: fmm_order at every level); level_box_start: the
+  // boxes of level l are [level_box_start[l], level_box_start[l + 1])
+  std::vector<int32_t> lorders, level_box_start;
+  int32_t* lorders_dev = nullptr;
   bool h3;                                 // 3D Helmholtz
   bool mixed;                              // FP32 far field (3D Laplace)
   bool tf32_ok;                            // split-TF32 translation matrices in use
@@ -65,6 +69,7 @@ struct qbxfmm_plan {
       if (s) cudaStreamDestroy(s);
     for (cudaEvent_t e : {ev_fork, ev_mpoles, ev_near, ev_p2l, ev_qbx})
       if (e) cudaEventDestroy(e);
+    if (lorders_dev) cudaFree(lorders_dev);
   }
 };
 
@@ -313,6 +318,50 @@ std::vector<double> h3_m2l_host_tables(int p, double k, double root_extent, int 
     if (_rc != QBXFMM_OK) return _rc;                \
   } while (0)
 
+// Per-level FMM orders: box expansions live at fmm_order (the largest level order);
+// after every stage that writes them, the coefficients above a box's level order are
+// zeroed, M2M and L2L level by level (a level's translations read the level written
+// before it).
+bool level_orders_on(const qbxfmm_plan* p) { return !p->lorders.empty(); }
+
+int mask_levels(const qbxfmm_plan* p, void* exps, int lev0, int lev1, cudaStream_t st)
+{
+  int b0 = p->level_box_start[lev0], b1 = p->level_box_start[lev1 + 1];
+  QBX_TRY(launch_level_mask(p->geo, b0, b1, p->lorders_dev, p->kern.family, p->ncf, p->kern.nrhs,
+                            (double2*)exps, st),
+          "per-level orders");
+  return QBXFMM_OK;
+}
+
+int mask_all_levels(const qbxfmm_plan* p, void* exps, cudaStream_t st)
+{
+  return level_orders_on(p) ? mask_levels(p, exps, 0, p->geo.nlevels - 1, st) : QBXFMM_OK;
+}
+
+// the host level-start array restricted to level lev (every other level empty)
+std::vector<int32_t> one_level(const std::vector<int32_t>& starts, int lev)
+{
+  std::vector<int32_t> r(starts.size());
+  for (size_t i = 0; i < r.size(); ++i) r[i] = (int)i <= lev ? starts[lev] : starts[lev + 1];
+  return r;
+}
+
+// the translation host table restricted to the M2M groups of parent level lev or
+// the L2L groups of child level lev
+TransHost one_level(const TransHost& th, int lev, bool m2m)
+{
+  TransHost r = th;
+  for (int l = 0; l < 64; ++l)
+    if (l != lev) {
+      if (m2m) r.m2m_level_max_group[l] = 0;
+      else {
+        r.l2l_level_max_group[l] = 0;
+        r.l2l_level_pairs[l] = 0;
+      }
+    }
+  return r;
+}
+
 }  // namespace
 
 namespace qbx {
@@ -509,7 +558,7 @@ int qbxfmm_form_multipoles(const qbxfmm_plan* p, const void* strengths, void* mp
     QBX_TRY(h3_launch_p2m(p->geo, p->hc, p->kern.fmm_order, p->kern.nrhs, (const double2*)strengths,
                           (double2*)mpoles, S(stream)),
             "form_multipoles");
-    return QBXFMM_OK;
+    return mask_all_levels(p, mpoles, S(stream));
   }
   if (p->helm)
     QBX_TRY(h2_launch_p2m(p->geo, p->hc, p->kern.fmm_order, p->kern.nrhs,
@@ -523,15 +572,37 @@ int qbxfmm_form_multipoles(const qbxfmm_plan* p, const void* strengths, void* mp
     QBX_TRY(launch_p2m(p->geo, p->sc, p->kern.fmm_order, p->kern.nrhs, (const double*)strengths,
                        (double2*)mpoles, S(stream)),
             "form_multipoles");
-  return QBXFMM_OK;
+  return mask_all_levels(p, mpoles, S(stream));
 }
 
 int qbxfmm_coarsen_multipoles(const qbxfmm_plan* p, void* mpoles, void* stream)
 {
   if (int rc = check_plan(p)) return rc;
+  if (p->h3 && !p->trans_dev)
+    return fail(QBXFMM_ERR_ARG, "3D Helmholtz: call qbxfmm_precompute_translations first");
+  if (level_orders_on(p)) {
+    // parents of level lev from children of level lev + 1, then truncated
+    for (int lev = p->geo.nlevels - 2; lev >= 0; --lev) {
+      if (p->h3) {
+        QBX_TRY(launch_m2m_direct(p->geo, one_level(p->th, lev, true), p->tc, p->kern.nrhs,
+                                  p->trans_dev, (double2*)mpoles, nullptr, S(stream)),
+                "coarsen_multipoles");
+      } else {
+        std::vector<int32_t> lv = one_level(p->lvl_source_parent, lev);
+        if (p->helm)
+          QBX_TRY(h2_launch_m2m(p->geo, lv.data(), p->hc, p->kern.fmm_order, p->kern.nrhs,
+                                (double2*)mpoles, nullptr, S(stream)),
+                  "coarsen_multipoles");
+        else
+          QBX_TRY(launch_m2m(p->geo, lv.data(), p->kern.fmm_order, p->kern.nrhs, (double2*)mpoles,
+                             S(stream)),
+                  "coarsen_multipoles");
+      }
+      if (int rc = mask_levels(p, mpoles, lev, lev, S(stream))) return rc;
+    }
+    return QBXFMM_OK;
+  }
   if (p->h3) {
-    if (!p->trans_dev)
-      return fail(QBXFMM_ERR_ARG, "3D Helmholtz: call qbxfmm_precompute_translations first");
     QBX_TRY(launch_m2m_direct(p->geo, p->th, p->tc, p->kern.nrhs, p->trans_dev, (double2*)mpoles,
                               nullptr, S(stream)),
             "coarsen_multipoles");
@@ -586,7 +657,7 @@ int qbxfmm_multipole_to_local(const qbxfmm_plan* p, const void* mpoles, void* lo
                               reinterpret_cast<const double2*>(p->trans_dev + o[4]), clsmap,
                               error_word, S(stream), p->mixed, p->hc.rb_m2l),
             "multipole_to_local");
-    return QBXFMM_OK;
+    return mask_all_levels(p, locals, S(stream));
   }
   if (p->helm)
     QBX_TRY(h2_launch_m2l(p->geo, p->hc, p->kern.fmm_order, p->kern.nrhs, (const double2*)mpoles,
@@ -596,7 +667,7 @@ int qbxfmm_multipole_to_local(const qbxfmm_plan* p, const void* mpoles, void* lo
     QBX_TRY(launch_m2l(p->geo, p->kern.fmm_order, p->kern.nrhs, (const double2*)mpoles,
                        (double2*)locals, error_word, S(stream)),
             "multipole_to_local");
-  return QBXFMM_OK;
+  return mask_all_levels(p, locals, S(stream));
 }
 
 int qbxfmm_eval_multipoles(const qbxfmm_plan* p, const void* mpoles, void* pot_nonqbx,
@@ -630,7 +701,7 @@ int qbxfmm_form_locals(const qbxfmm_plan* p, const void* strengths, void* locals
     QBX_TRY(h3_launch_p2l(p->geo, p->hc, p->kern.fmm_order, p->kern.nrhs, (const double2*)strengths,
                           (double2*)locals, error_word, S(stream)),
             "form_locals");
-    return QBXFMM_OK;
+    return mask_all_levels(p, locals, S(stream));
   }
   if (p->helm)
     QBX_TRY(h2_launch_p2l(p->geo, p->hc, p->kern.fmm_order, p->kern.nrhs,
@@ -644,15 +715,37 @@ int qbxfmm_form_locals(const qbxfmm_plan* p, const void* strengths, void* locals
     QBX_TRY(launch_p2l(p->geo, p->sc, p->kern.fmm_order, p->kern.nrhs, (const double*)strengths,
                        (double2*)locals, error_word, S(stream)),
             "form_locals");
-  return QBXFMM_OK;
+  return mask_all_levels(p, locals, S(stream));
 }
 
 int qbxfmm_refine_locals(const qbxfmm_plan* p, void* locals, void* stream)
 {
   if (int rc = check_plan(p)) return rc;
+  if (p->h3 && !p->trans_dev)
+    return fail(QBXFMM_ERR_ARG, "3D Helmholtz: call qbxfmm_precompute_translations first");
+  if (level_orders_on(p)) {
+    // children of level lev from parents of level lev - 1, then truncated
+    for (int lev = 1; lev < p->geo.nlevels; ++lev) {
+      if (p->h3) {
+        QBX_TRY(launch_l2l_direct(p->geo, one_level(p->th, lev, false), p->tc, p->kern.nrhs,
+                                  p->trans_dev, (double2*)locals, nullptr, S(stream)),
+                "refine_locals");
+      } else {
+        std::vector<int32_t> lv = one_level(p->lvl_ttp, lev);
+        if (p->helm)
+          QBX_TRY(h2_launch_l2l(p->geo, lv.data(), p->hc, p->kern.fmm_order, p->kern.nrhs,
+                                (double2*)locals, nullptr, S(stream)),
+                  "refine_locals");
+        else
+          QBX_TRY(launch_l2l(p->geo, lv.data(), p->kern.fmm_order, p->kern.nrhs, (double2*)locals,
+                             S(stream)),
+                  "refine_locals");
+      }
+      if (int rc = mask_levels(p, locals, lev, lev, S(stream))) return rc;
+    }
+    return QBXFMM_OK;
+  }
   if (p->h3) {
-    if (!p->trans_dev)
-      return fail(QBXFMM_ERR_ARG, "3D Helmholtz: call qbxfmm_precompute_translations first");
     QBX_TRY(launch_l2l_direct(p->geo, p->th, p->tc, p->kern.nrhs, p->trans_dev, (double2*)locals,
                               nullptr, S(stream)),
             "refine_locals");
@@ -853,8 +946,8 @@ int qbxfmm_plan_set_tuning(qbxfmm_plan* p, const qbxfmm_tuning* t)
       !ok(t->p2e_densities, {1, 4, 8}) || !ok(t->l2qbxl_densities, {1, 4}) ||
       !ok(t->tsqbx_densities, {1, 4, 16}))
     return fail(QBXFMM_ERR_ARG, "tuning: unsupported densities-per-CTA value");
-  if (!p->mixed && (t->m2qbxl_densities == 16 || t->m2l_densities == 16))
-    return fail(QBXFMM_ERR_ARG, "tuning: 16 densities per CTA is a mixed-precision shape");
+  if (!p->mixed && t->m2l_densities == 16)
+    return fail(QBXFMM_ERR_ARG, "tuning: 16 densities per CTA of M2L is a mixed-precision shape");
   p->hc.rb_rot = t->m2qbxl_densities;
   p->hc.rb_m2l = t->m2l_densities;
   p->hc.rb_p2e = t->p2e_densities;
@@ -872,6 +965,62 @@ int qbxfmm_plan_get_tuning(const qbxfmm_plan* p, qbxfmm_tuning* t)
   t->p2e_densities = p->hc.rb_p2e;
   t->l2qbxl_densities = p->hc.rb_l2q;
   t->tsqbx_densities = p->hc.rb_ts;
+  return QBXFMM_OK;
+}
+
+int qbxfmm_plan_set_level_orders(qbxfmm_plan* p, const int32_t* orders, int32_t nlevels)
+{
+  if (int rc = check_plan(p)) return rc;
+  if (!orders) {
+    p->lorders.clear();
+    return QBXFMM_OK;
+  }
+  if (nlevels != p->geo.nlevels)
+    return fail(QBXFMM_ERR_ARG, "level orders: one order per tree level expected");
+  bool all_max = true;
+  for (int l = 0; l < nlevels; ++l) {
+    if (orders[l] < 0 || orders[l] > p->kern.fmm_order)
+      return fail(QBXFMM_ERR_ARG, "level orders: each order must be in [0, fmm_order]");
+    all_max &= orders[l] == p->kern.fmm_order;
+  }
+  if (p->hc.taylor)
+    return fail(QBXFMM_ERR_UNSUPPORTED,
+                "level orders: not built for the compressed-Taylor 3D Helmholtz truncation "
+                "(fmm_backend QBXFMM_BACKEND_FMMLIB supports them)");
+  if (all_max) {
+    p->lorders.clear();
+    return QBXFMM_OK;
+  }
+  // boxes are numbered by level: find each level's range
+  std::vector<int32_t> lv(p->geo.nboxes);
+  cudaError_t e = cudaMemcpy(lv.data(), p->geo.box_levels, sizeof(int32_t) * lv.size(),
+                             cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_check(e, "qbxfmm_plan_set_level_orders");
+  std::vector<int32_t> starts(nlevels + 1, 0);
+  for (int b = 0; b < p->geo.nboxes; ++b) {
+    if (lv[b] < 0 || lv[b] >= nlevels || (b > 0 && lv[b] < lv[b - 1]))
+      return fail(QBXFMM_ERR_ARG, "level orders: boxes must be numbered by level");
+  }
+  for (int l = 0; l <= nlevels; ++l)
+    starts[l] = (int32_t)(std::lower_bound(lv.begin(), lv.end(), l) - lv.begin());
+  if (!p->lorders_dev) {
+    e = cudaMalloc(&p->lorders_dev, sizeof(int32_t) * 64);
+    if (e != cudaSuccess) return cuda_check(e, "qbxfmm_plan_set_level_orders");
+  }
+  e = cudaMemcpy(p->lorders_dev, orders, sizeof(int32_t) * nlevels, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return cuda_check(e, "qbxfmm_plan_set_level_orders");
+  p->lorders.assign(orders, orders + nlevels);
+  p->level_box_start = starts;
+  return QBXFMM_OK;
+}
+
+int qbxfmm_plan_get_level_orders(const qbxfmm_plan* p, int32_t* orders, int32_t nlevels)
+{
+  if (int rc = check_plan(p)) return rc;
+  if (!orders || nlevels != p->geo.nlevels)
+    return fail(QBXFMM_ERR_ARG, "level orders: one order per tree level expected");
+  for (int l = 0; l < nlevels; ++l)
+    orders[l] = p->lorders.empty() ? p->kern.fmm_order : p->lorders[l];
   return QBXFMM_OK;
 }
 
@@ -971,7 +1120,9 @@ int qbxfmm_apply(const qbxfmm_plan* p, const qbxfmm_upsample* up, const qbxfmm_w
     return fail(QBXFMM_ERR_ARG, "incomplete workspace");
   size_t sz[8];
   if (int rc = qbxfmm_workspace_sizes(p, sz)) return rc;
-  const bool gemm = !p->h3 && p->trans_ok && ws->translations && ws->pair_scratch;
+  // (per-level orders run the stage entries, which truncate level by level)
+  const bool gemm = !p->h3 && p->trans_ok && ws->translations && ws->pair_scratch &&
+                    !level_orders_on(p);
   if (p->h3) {
     if (!ws->translations)
       return fail(QBXFMM_ERR_ARG, "3D Helmholtz needs the translations buffer");

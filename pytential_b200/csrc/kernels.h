@@ -186,4 +186,8 @@ cudaError_t h3_launch_assemble(const qbxfmm_geometry& g, int nrhs, const double2
 cudaError_t h3_launch_trans_build(const qbxfmm_geometry& g, const TransCfg& tc, double k,
                                   const double* gaunt, double* T, cudaStream_t st);
 
+// per-level FMM orders: zero the coefficients of boxes [b0, b1) above their level's order
+cudaError_t launch_level_mask(const qbxfmm_geometry& g, int b0, int b1, const int32_t* orders,
+                              int family, int ncf, int nrhs, double2* exps, cudaStream_t st);
+
 }  // namespace qbx

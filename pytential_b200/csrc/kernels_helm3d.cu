@@ -18,6 +18,7 @@
 // ladder relations of R and S.
 #include <cooperative_groups.h>
 
+#include <algorithm>
 #include <string>
 #include <type_traits>
 
@@ -889,7 +890,7 @@ k_h3_e2qbxl_rot(qbxfmm_geometry g, HelmCoeffs hc, int pf, int nrhs,
   const size_t ctad = ((size_t)nisq + nrt + nl + 1) & ~(size_t)1;
   V* wbase = reinterpret_cast<V*>(s_isq + ctad);
   // per warp
-  const size_t perd = ((size_t)nm * (Q + 1) + (size_t)NMU * NCQ + 2 * (size_t)nm + 1) / 2;
+  const size_t perd = ((size_t)NMU * NCQ + 2 * (size_t)nm + 1) / 2;
   const size_t per = (size_t)nm * NMU + NCQ + (size_t)NCQ * RB + (L + 2) + nm + perd;
   int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   V* Dph = wbase + (size_t)warp * per;                          // [nm][NMU] slice x phase
@@ -897,8 +898,7 @@ k_h3_e2qbxl_rot(qbxfmm_geometry g, HelmCoeffs hc, int pf, int nrhs,
   V* Lp = coaxn + NCQ;                                          // [NCQ][RB]
   V* rad = Lp + (size_t)NCQ * RB;                               // [L + 2]
   V* ph = rad + (L + 2);                                        // [nm]: e^{i m alpha}
-  R* Draw = reinterpret_cast<R*>(ph + nm);                      // [nm][Q+1] d^n_{m mu>=0}
-  R* Tb = Draw + (size_t)nm * (Q + 1);                          // [NMU][NCQ]
+  R* Tb = reinterpret_cast<R*>(ph + nm);                        // [NMU][NCQ]
   R* chp = Tb + (size_t)NMU * NCQ;                              // [nm] cos(beta/2)^k
   R* shp = chp + nm;                                            // [nm] sin(beta/2)^k
 
@@ -1015,15 +1015,36 @@ k_h3_e2qbxl_rot(qbxfmm_geometry g, HelmCoeffs hc, int pf, int nrhs,
       for (int nu = 0; nu <= Q; ++nu) lacc[ts][nu] = cmake<R>(0);
 
     for (int n = 0; n <= pf; ++n) {
-      // (1) the raw slice d^n_{m mu}, mu >= 0, and the step to n + 1
+      // (1) the slice of order n, written by the recurrence lanes themselves: the
+      // task (m, mu >= 0) holds d = d^n_{m mu} and stores the signed, phased entries
+      // (m, mu) and, with d^n_{-m,-mu} = (-1)^{m+mu} d^n_{m mu}, (-m, -mu); orders
+      // n <= Q also give the back-rotation matrices (without the phase).  Rows
+      // |m| > n are not read at this order (tasks below their start order hold 0,
+      // which zero-fills the columns |mu| > n); then the step to n + 1
       const R rn = n > 0 ? R(1) / R(n) : R(0);
       const R h1 = (R)((2.0 * n + 1.0) * n * (n + 1.0) * cbeta);
+      const int tbase = n * n + n;
 #pragma unroll
       for (int sl = 0; sl < RSL; ++sl) {
         int t = lane + 32 * sl;
         if (t >= ntask) continue;
         if (n == n0[sl]) cur[sl] = v0[sl];
-        Draw[t] = n >= n0[sl] ? cur[sl] : 0.0;
+        {
+          const int m = t / (Q + 1) - pf, mu = t - (t / (Q + 1)) * (Q + 1);
+          if (abs(m) <= n) {
+            const R d = n >= n0[sl] ? cur[sl] : R(0);
+            const R v1 = (((m > 0) && (m & 1)) != ((mu & 1) != 0)) ? -d : d;
+            Dph[(m + pf) * NMU + mu + Q] = cscale(v1, ph[m + pf]);
+            if (n <= Q) Tb[(mu + Q) * NCQ + tbase + m] = v1;
+            if (mu > 0) {
+              // sign (-1)^{m+mu} eps_{-m}, eps_{-m} = (-1)^m for m < 0
+              const bool neg = (((m + mu) & 1) != 0) != ((m < 0) && (m & 1));
+              const R v2 = neg ? -d : d;
+              Dph[(pf - m) * NMU + Q - mu] = cscale(v2, ph[pf - m]);
+              if (n <= Q) Tb[(Q - mu) * NCQ + tbase - m] = v2;
+            }
+          }
+        }
         if (n >= n0[sl] && n < pf) {
           R nxt;
           if (n == 0) {
@@ -1041,31 +1062,31 @@ k_h3_e2qbxl_rot(qbxfmm_geometry g, HelmCoeffs hc, int pf, int nrhs,
         }
       }
       // (2) coaxial column n: coaxn[(nu,mu)] = i^{nu-n} sum_j G(nu,mu; j; n,mu) rad[|n-nu|+2j]
-      for (int o = lane; o < NCQ; o += 32) {
-        int nu = s_nof[o];
-        int mu = o - nu * nu - nu;
+      // for mu >= 0 only (G(n,-mu; nu,-mu; l) = G(n,mu; nu,mu; l): the column of -mu is
+      // that of mu), one lane per (nu, mu >= 0), its table reads issued before the sum
+      static_assert((Q + 1) * (Q + 2) / 2 <= 32, "one lane per coaxial entry");
+      if (lane < (Q + 1) * (Q + 2) / 2) {
+        int nu = (int)((sqrtf(8.0f * lane + 1.0f) - 1.0f) * 0.5f);
+        if ((nu + 1) * (nu + 2) / 2 <= lane) ++nu;
+        if (nu * (nu + 1) / 2 > lane) --nu;
+        const int mu = lane - nu * (nu + 1) / 2;
+        const int o = nu * nu + nu + mu;
         V tt = cmake<R>(0);
-        if (n >= abs(mu)) {
+        if (n >= mu) {
           const double* G = g0c + ((size_t)o * nl + n) * (Q + 1);
           int lbase = abs(n - nu), jmax = min(n, nu);
-          for (int j = 0; j <= jmax; ++j) tt = caxpy((R)__ldg(G + j), rad[lbase + 2 * j], tt);
+          R gj[Q + 1];
+#pragma unroll
+          for (int j = 0; j <= Q; ++j) gj[j] = j <= jmax ? (R)__ldg(G + j) : R(0);
+#pragma unroll
+          for (int j = 0; j <= Q; ++j)
+            if (j <= jmax) tt = caxpy(gj[j], rad[lbase + 2 * j], tt);
           tt = cmul(cto(ipow(nu - n + 4 * pf), V()), tt);
         }
         coaxn[o] = tt;
       }
       __syncwarp();
-      // (3) the signed, phased slice for |m| <= n, all mu; orders n <= Q also give
-      // the back-rotation matrices
-      for (int e = lane; e < (2 * n + 1) * NMU; e += 32) {
-        int mm = e / NMU - n, mu = e % NMU - Q;
-        R val = mu >= 0 ? Draw[(mm + pf) * (Q + 1) + mu]
-                        : (((mm - mu) & 1) ? R(-1) : R(1)) * Draw[(pf - mm) * (Q + 1) - mu];
-        val *= ((mm > 0 && (mm & 1)) ? R(-1) : R(1)) * ((mu > 0 && (mu & 1)) ? R(-1) : R(1));
-        if (n <= Q && abs(mm) <= Q) Tb[(mu + Q) * NCQ + n * n + n + mm] = val;
-        Dph[(mm + pf) * NMU + mu + Q] = cscale(val, ph[mm + pf]);
-      }
-      __syncwarp();
-      // (4) rotate and translate coaxially
+      // (3) rotate and translate coaxially
       const int base = n * n + n;
       if constexpr (DMMA) {
         // the rotation of order n as a real product on the FP64 tensor cores:
@@ -1103,7 +1124,7 @@ k_h3_e2qbxl_rot(qbxfmm_geometry g, HelmCoeffs hc, int pf, int nrhs,
           const int amu = abs(mu);
 #pragma unroll
           for (int nu = 0; nu <= Q; ++nu)
-            if (nu >= amu) lacc[sl][nu] = cfma(coaxn[nu * nu + nu + mu], mr, lacc[sl][nu]);
+            if (nu >= amu) lacc[sl][nu] = cfma(coaxn[nu * nu + nu + amu], mr, lacc[sl][nu]);
         }
       } else {
         // lane tasks (mu, density), all of a lane's tasks in one pass over m so that
@@ -1133,7 +1154,7 @@ k_h3_e2qbxl_rot(qbxfmm_geometry g, HelmCoeffs hc, int pf, int nrhs,
           int amu = abs(mu);
 #pragma unroll
           for (int nu = 0; nu <= Q; ++nu)
-            if (nu >= amu) lacc[ts][nu] = cfma(coaxn[nu * nu + nu + mu], mr[ts], lacc[ts][nu]);
+            if (nu >= amu) lacc[ts][nu] = cfma(coaxn[nu * nu + nu + amu], mr[ts], lacc[ts][nu]);
         }
       }
       __syncwarp();
@@ -1186,6 +1207,304 @@ k_h3_e2qbxl_rot(qbxfmm_geometry g, HelmCoeffs hc, int pf, int nrhs,
     int nu = s_nof[o];
     double2* out = qbx_exps + ((size_t)ctr * nrhs + r0 + r) * NCQ + o;
     *out = caxpy(pow(st, (double)nu), c2d(acc[i]), *out);
+  }
+}
+
+// M2QBXL in FP64 with the per-pair tables shared by 16 densities: the same rotation,
+// coaxial translation and back rotation as k_h3_e2qbxl_rot, but two warps per center
+// (CTA: 2 centers x 2 warps), each warp applying the tables to 8 of the 16 densities
+// on the FP64 tensor cores.  The pair of warps splits the table work of a (center,
+// box) pair: the Wigner-d recurrence tasks are interleaved between them (blocks of 32
+// tasks), warp 1 forms the coaxial column, warp 0 the radial factors and warp 1 the
+// phases; the slice and column of order n are double-buffered, so one named barrier
+// per order (64 threads, one per center) separates writing order n + 1 from reading
+// order n.  Shared memory per CTA stays at two CTAs per SM (the box's 16-density
+// multipole block is staged once for both centers).
+constexpr int H3P_SLOTS = 4;   // recurrence tasks per lane: (2 pf + 1)(Q + 1) <= 2 x 4 x 32
+
+// named barrier of the two warps of center cp (barrier 0 is __syncthreads)
+QBX_D void h3_pair_bar(int cp)
+{
+  if (cp == 0) asm volatile("bar.sync 1, 64;\n" ::: "memory");
+  else asm volatile("bar.sync 2, 64;\n" ::: "memory");
+}
+
+template <int Q>
+__global__ void __launch_bounds__(NT)
+k_h3_m2qbxl_pair(qbxfmm_geometry g, HelmCoeffs hc, int pf, int nrhs,
+                 const double2* __restrict__ exps, const double* __restrict__ rot,
+                 double2* __restrict__ qbx_exps, int32_t* err)
+{
+  constexpr int NCQ = (Q + 1) * (Q + 1);
+  constexpr int NMU = 2 * Q + 1;
+  constexpr int RB = 16, HB = 8;                 // densities per CTA / per warp
+  constexpr int NOUT = (NCQ * HB + 31) / 32;
+  constexpr int RSL = H3P_SLOTS;
+  constexpr int NTILE = (NMU > 8) ? 4 : 2;
+  extern __shared__ double2 smem2[];
+  const int ncf = (pf + 1) * (pf + 1);
+  const int L = pf + Q;
+  const int nl = pf + 1;
+  const int nm = 2 * pf + 1;
+  const int ntask = nm * (Q + 1);
+  const int nisq = (pf + 2) * (pf + 1), nrt = (pf + 1) * (pf + 1);
+  const double* rstart = rot;                                   // [nm][Q+1][4]
+  const double* g_isq = rstart + (size_t)nm * (Q + 1) * 4;      // [pf+2][pf+1]
+  const double* g_rt = g_isq + nisq;                            // [pf+1][pf+1]
+  const double* g0c = g_rt + nrt;                               // [NCQ][nl][Q+1]
+  // CTA-wide
+  double2* Es = smem2;                                          // [ncf][RB]
+  double* s_isq = reinterpret_cast<double*>(Es + (size_t)ncf * RB);
+  double* s_rt = s_isq + nisq;
+  double* spow = s_rt + nrt;                                    // [nl]: s_box^n
+  double2* cbase = reinterpret_cast<double2*>(s_isq + (((size_t)nisq + nrt + nl + 1) & ~(size_t)1));
+  // per center: slices (two buffers; after the order loop the two warps' [NCQ][HB]
+  // blocks of translated coefficients), coaxial columns (two buffers), radial
+  // factors, phases, back-rotation matrices, half-angle powers
+  const size_t nsl = max((size_t)2 * nm * NMU, (size_t)2 * NCQ * HB);
+  const size_t per = nsl + 2 * NCQ + (L + 2) + nm + ((size_t)NMU * NCQ + 2 * (size_t)nm + 1) / 2;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int cp = warp >> 1, half = warp & 1;
+  double2* Dsl = cbase + (size_t)cp * per;                      // [2][nm][NMU]
+  double2* Lp = Dsl + (size_t)half * NCQ * HB;                  // [NCQ][HB] (after the loop)
+  double2* coax = Dsl + nsl;                                    // [2][NCQ]
+  double2* rad = coax + 2 * NCQ;                                // [L + 2]
+  double2* ph = rad + (L + 2);                                  // [nm]: e^{i m alpha}
+  double* Tb = reinterpret_cast<double*>(ph + nm);              // [NMU][NCQ]
+  double* chp = Tb + (size_t)NMU * NCQ;                         // [nm] cos(beta/2)^k
+  double* shp = chp + nm;                                       // [nm] sin(beta/2)^k
+
+  __shared__ unsigned char s_nof[(H3_MAXP + 1) * (H3_MAXP + 1)];
+  for (int x = threadIdx.x; x < nisq + nrt; x += NT) s_isq[x] = __ldg(g_isq + x);
+  for (int n = 0; n <= pf; ++n)
+    for (int x = n * n + threadIdx.x; x < (n + 1) * (n + 1); x += NT) s_nof[x] = (unsigned char)n;
+  __syncthreads();
+  const int chunk = blockIdx.x;
+  const int r0 = blockIdx.y * RB;
+  const int itb = g.qbx_chunk_target_box[chunk];
+  const int nctr = g.qbx_chunk_count[chunk];
+  if (blockIdx.z * 2 >= nctr) return;      // the whole CTA is idle
+  const int ci = blockIdx.z * 2 + cp;
+  bool has = ci < nctr;                    // the same for both warps of a center
+  int ctr = has ? g.centers_by_target_box[g.qbx_chunk_start[chunk] + ci] : 0;
+  if ((unsigned)ctr >= (unsigned)g.ncenters) {
+    report(err, QBX_DEVERR_BAD_CENTER);
+    has = false;
+    ctr = 0;
+  }
+  double cc[3];
+  load_point<3>(g.centers, g.ncenters, ctr, cc);
+  double2 acc[NOUT];
+#pragma unroll
+  for (int i = 0; i < NOUT; ++i) acc[i] = c2(0.0);
+
+  const int nbox = g.list3_starts[itb + 1] - g.list3_starts[itb];
+  for (int bi = 0; bi < nbox; ++bi) {
+    const int sbx = g.list3_lists[g.list3_starts[itb] + bi];
+    if ((unsigned)sbx >= (unsigned)g.nboxes) {
+      report(err, QBX_DEVERR_BAD_BOX);
+      continue;                            // uniform over the CTA: the list is shared
+    }
+    double cb[3];
+    load_point<3>(g.box_centers, g.nboxes, sbx, cb);
+    const double sb = h3_scale(hc.k, level_width(g, g.box_levels[sbx]));
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double f = 1.0;
+      for (int n = 0; n < nl; ++n, f *= sb) spow[n] = f;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < ncf * RB; e += NT) {
+      const int ei = e / RB, ri = e - ei * RB;
+      double2 v = c2(0.0);
+      if (r0 + ri < nrhs) v = cscale(spow[s_nof[ei]], exps[((size_t)sbx * nrhs + r0 + ri) * ncf + ei]);
+      Es[e] = v;
+    }
+    __syncthreads();
+    if (!has) continue;
+    const double bv[3] = {cc[0] - cb[0], cc[1] - cb[1], cc[2] - cb[2]};
+    const double bl = sqrt(bv[0] * bv[0] + bv[1] * bv[1] + bv[2] * bv[2]);
+    const double cbeta = bl > 0.0 ? fmin(1.0, fmax(-1.0, bv[2] / bl)) : 1.0;
+    const double alpha = (bv[0] == 0.0 && bv[1] == 0.0) ? 0.0 : atan2(bv[1], bv[0]);
+    const double beta = acos(cbeta);
+    if (half == 0) {
+      // radial factors 4 pi Y_l^0(z) i^l h_l(k |b|), Y_l^0(z) = sqrt((2l+1)/(4 pi))
+      if (lane == 0) h3_sph_h(L, hc.k * bl, rad);
+      __syncwarp();
+      for (int l = lane; l <= L; l += 32)
+        rad[l] = cmul(cscale(sqrt(FOUR_PI * (2.0 * l + 1.0)), ipow(l)), rad[l]);
+    } else {
+      const double ch = cos(0.5 * beta), sh = sin(0.5 * beta);
+      for (int m = lane; m < nm; m += 32) {
+        double sn, cs;
+        sincos((m - pf) * alpha, &sn, &cs);
+        ph[m] = c2(cs, sn);
+        double a = 1.0, b = 1.0;
+        for (int u = 0; u < m; ++u) {
+          a *= ch;
+          b *= sh;
+        }
+        chp[m] = a;
+        shp[m] = b;
+      }
+    }
+    h3_pair_bar(cp);
+    // this warp's recurrence tasks t = (2 sl + half) 32 + lane, t = (m + pf)(Q + 1) + mu
+    double cur[RSL], prev[RSL], v0[RSL];
+    int n0[RSL];
+#pragma unroll
+    for (int sl = 0; sl < RSL; ++sl) {
+      const int t = (2 * sl + half) * 32 + lane;
+      cur[sl] = prev[sl] = v0[sl] = 0.0;
+      n0[sl] = 1 << 20;
+      if (t < ntask) {
+        const int m = t / (Q + 1) - pf, mu = t % (Q + 1);
+        n0[sl] = max(abs(m), mu);
+        v0[sl] = __ldg(rstart + 4 * t) * chp[(int)__ldg(rstart + 4 * t + 1)] *
+                 shp[(int)__ldg(rstart + 4 * t + 2)];
+      }
+    }
+    double2 lacc[4][Q + 1];
+#pragma unroll
+    for (int ts = 0; ts < 4; ++ts)
+#pragma unroll
+      for (int nu = 0; nu <= Q; ++nu) lacc[ts][nu] = c2(0.0);
+
+    for (int n = 0; n <= pf; ++n) {
+      double2* Dph = Dsl + (size_t)(n & 1) * nm * NMU;
+      double2* coaxn = coax + (n & 1) * NCQ;
+      // (1) slice of order n from this warp's recurrence tasks (as in k_h3_e2qbxl_rot)
+      const double rn = n > 0 ? 1.0 / n : 0.0;
+      const double h1 = (2.0 * n + 1.0) * n * (n + 1.0) * cbeta;
+      const int tbase = n * n + n;
+#pragma unroll
+      for (int sl = 0; sl < RSL; ++sl) {
+        const int t = (2 * sl + half) * 32 + lane;
+        if (t >= ntask) continue;
+        if (n == n0[sl]) cur[sl] = v0[sl];
+        const int m = t / (Q + 1) - pf, mu = t - (t / (Q + 1)) * (Q + 1);
+        if (abs(m) <= n) {
+          const double d = n >= n0[sl] ? cur[sl] : 0.0;
+          const double v1 = (((m > 0) && (m & 1)) != ((mu & 1) != 0)) ? -d : d;
+          Dph[(m + pf) * NMU + mu + Q] = cscale(v1, ph[m + pf]);
+          if (n <= Q) Tb[(mu + Q) * NCQ + tbase + m] = v1;
+          if (mu > 0) {
+            const bool neg = (((m + mu) & 1) != 0) != ((m < 0) && (m & 1));
+            const double v2 = neg ? -d : d;
+            Dph[(pf - m) * NMU + Q - mu] = cscale(v2, ph[pf - m]);
+            if (n <= Q) Tb[(Q - mu) * NCQ + tbase - m] = v2;
+          }
+        }
+        if (n >= n0[sl] && n < pf) {
+          double nxt;
+          if (n == 0) {
+            nxt = cbeta * cur[sl];
+          } else {
+            const int am = abs(m);
+            const double w = rn * s_isq[(n + 1) * (pf + 1) + am] * s_isq[(n + 1) * (pf + 1) + mu];
+            const double A = (h1 - (double)((2 * n + 1) * m * mu)) * w;
+            const double C = (n + 1) * rn * s_rt[n * (pf + 1) + am] * s_rt[n * (pf + 1) + mu];
+            nxt = fma(A, cur[sl], -C * prev[sl]);
+          }
+          prev[sl] = cur[sl];
+          cur[sl] = nxt;
+        }
+      }
+      // (2) warp 1: the coaxial column of order n for mu >= 0 (the column of -mu is
+      // the same), one lane per (nu, mu)
+      if (half == 1 && lane < (Q + 1) * (Q + 2) / 2) {
+        int nu = (int)((sqrtf(8.0f * lane + 1.0f) - 1.0f) * 0.5f);
+        if ((nu + 1) * (nu + 2) / 2 <= lane) ++nu;
+        if (nu * (nu + 1) / 2 > lane) --nu;
+        const int mu = lane - nu * (nu + 1) / 2;
+        const int o = nu * nu + nu + mu;
+        double2 tt = c2(0.0);
+        if (n >= mu) {
+          const double* G = g0c + ((size_t)o * nl + n) * (Q + 1);
+          const int lbase = abs(n - nu), jmax = min(n, nu);
+          double gj[Q + 1];
+#pragma unroll
+          for (int j = 0; j <= Q; ++j) gj[j] = j <= jmax ? __ldg(G + j) : 0.0;
+#pragma unroll
+          for (int j = 0; j <= Q; ++j)
+            if (j <= jmax) tt = caxpy(gj[j], rad[lbase + 2 * j], tt);
+          tt = cmul(ipow(nu - n + 4 * pf), tt);
+        }
+        coaxn[o] = tt;
+      }
+      h3_pair_bar(cp);     // slice and column of order n complete
+      // (3) rotate this warp's 8 densities on the FP64 tensor cores and translate
+      const int base = n * n + n;
+      const int rho = lane >> 2, kq = lane & 3;
+      double c[NTILE][2];
+#pragma unroll
+      for (int t = 0; t < NTILE; ++t) c[t][0] = c[t][1] = 0.0;
+      const double2* Eb = Es + (base - n) * RB + half * HB + rho;
+      const double2* Db = Dph + (pf - n) * NMU;
+      for (int sk = 0; sk <= n; ++sk) {
+        const int kap = 4 * sk + kq, mi = kap >> 1, pin = kap & 1;
+        const bool vk = mi <= 2 * n;
+        const double2 e = vk ? Eb[mi * RB] : c2(0.0);
+        const double b = pin ? e.y : e.x;
+        const double2 z0 = (vk && rho < NMU) ? Db[mi * NMU + rho] : c2(0.0);
+        h3_dmma(c[0][0], c[0][1], pin ? -z0.y : z0.x, b);
+        h3_dmma(c[1][0], c[1][1], pin ? z0.x : z0.y, b);
+        if (NTILE == 4) {
+          const double2 z1 = (vk && 8 + rho < NMU) ? Db[mi * NMU + 8 + rho] : c2(0.0);
+          h3_dmma(c[NTILE - 2][0], c[NTILE - 2][1], pin ? -z1.y : z1.x, b);
+          h3_dmma(c[NTILE - 1][0], c[NTILE - 1][1], pin ? z1.x : z1.y, b);
+        }
+      }
+#pragma unroll
+      for (int sl = 0; sl < 4; ++sl) {
+        const int grp = sl >> 1, v = sl & 1;
+        const int mu = (grp ? 8 + rho : rho) - Q;
+        if (grp * 8 + rho >= NMU || abs(mu) > n || (grp && NTILE < 4)) continue;
+        const double2 mr = c2(c[2 * grp][v], c[2 * grp + 1][v]);
+        const int amu = abs(mu);
+#pragma unroll
+        for (int nu = 0; nu <= Q; ++nu)
+          if (nu >= amu) lacc[sl][nu] = cfma(coaxn[nu * nu + nu + amu], mr, lacc[sl][nu]);
+      }
+    }
+    h3_pair_bar(cp);       // both warps done with the slices; back-rotation matrices complete
+    {
+      const int rho = lane >> 2;
+#pragma unroll
+      for (int sl = 0; sl < 4; ++sl) {
+        const int grp = sl >> 1, r = 2 * (lane & 3) + (sl & 1);
+        const int mu = (grp ? 8 + rho : rho) - Q;
+        if (grp * 8 + rho >= NMU) continue;
+#pragma unroll
+        for (int nu = 0; nu <= Q; ++nu)
+          if (nu >= abs(mu)) Lp[(nu * nu + nu + mu) * HB + r] = lacc[sl][nu];
+      }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int i = 0; i < NOUT; ++i) {
+      const int task = lane + 32 * i;
+      if (task >= NCQ * HB) break;
+      const int o = task / HB, r = task - o * HB;
+      const int nu = s_nof[o];
+      const int mu2 = o - nu * nu - nu;
+      double2 a = c2(0.0);
+      for (int mu = -nu; mu <= nu; ++mu) a = caxpy(Tb[(mu + Q) * NCQ + o], Lp[(nu * nu + nu + mu) * HB + r], a);
+      acc[i] = cfma(cconj(ph[mu2 + pf]), a, acc[i]);
+    }
+  }
+  if (!has) return;
+  const double st = h3_scale(hc.k, g.expansion_radii[ctr]);
+#pragma unroll
+  for (int i = 0; i < NOUT; ++i) {
+    const int task = lane + 32 * i;
+    if (task >= NCQ * HB) break;
+    const int o = task / HB, r = task - o * HB;
+    const int rr = r0 + half * HB + r;
+    if (rr >= nrhs) continue;
+    const int nu = s_nof[o];
+    double2* out = qbx_exps + ((size_t)ctr * nrhs + rr) * NCQ + o;
+    *out = caxpy(pow(st, (double)nu), acc[i], *out);
   }
 }
 
@@ -2018,9 +2337,34 @@ static size_t h3_rot_smem(int pf)
   int ncf = (pf + 1) * (pf + 1), L = pf + Q, nl = pf + 1, nm = 2 * pf + 1;
   size_t nisq = (size_t)(pf + 2) * (pf + 1), nrt = (size_t)(pf + 1) * (pf + 1);
   size_t ctad = (nisq + nrt + nl + 1) & ~(size_t)1;
-  size_t perd = ((size_t)nm * (Q + 1) + (size_t)NMU * NCQ + 2 * (size_t)nm + 1) / 2;
+  size_t perd = ((size_t)NMU * NCQ + 2 * (size_t)nm + 1) / 2;
   size_t per = (size_t)nm * NMU + NCQ + (size_t)NCQ * RB + (L + 2) + nm + perd;
   return ((size_t)ncf * RB + NW * per) * sizeof(cplx_t<R>) + ctad * sizeof(R);
+}
+
+template <int Q>
+static size_t h3_pair_smem(int pf)
+{
+  constexpr int NCQ = (Q + 1) * (Q + 1), NMU = 2 * Q + 1;
+  const size_t ncf = (size_t)(pf + 1) * (pf + 1), L = pf + Q, nl = pf + 1, nm = 2 * pf + 1;
+  const size_t nisq = (size_t)(pf + 2) * (pf + 1), nrt = (size_t)(pf + 1) * (pf + 1);
+  const size_t ctad = (nisq + nrt + nl + 1) & ~(size_t)1;
+  const size_t nsl = std::max((size_t)2 * nm * NMU, (size_t)2 * NCQ * 8);
+  const size_t per = nsl + 2 * NCQ + (L + 2) + nm + ((size_t)NMU * NCQ + 2 * nm + 1) / 2;
+  return (ncf * 16 + 2 * per) * sizeof(double2) + ctad * sizeof(double);
+}
+
+template <int Q>
+static cudaError_t h3_pair_launch(const qbxfmm_geometry& g, HelmCoeffs hc, int pf, int nrhs,
+                                  const double2* e, const double* rot, double2* qe, int32_t* err,
+                                  cudaStream_t st)
+{
+  if ((2 * pf + 1) * (Q + 1) > 2 * H3P_SLOTS * 32) return cudaErrorInvalidValue;
+  size_t sh = h3_pair_smem<Q>(pf);
+  cudaFuncSetAttribute(k_h3_m2qbxl_pair<Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+  dim3 grid(g.nqbx_chunks, (nrhs + 15) / 16, (H3_ROT_ZS * NW) / 2);
+  k_h3_m2qbxl_pair<Q><<<grid, NT, sh, st>>>(g, hc, pf, nrhs, e, rot, qe, err);
+  return cudaGetLastError();
 }
 
 template <typename R, bool FROM_LOCAL, int Q, int RB>
@@ -2036,14 +2380,16 @@ static cudaError_t h3_rot_launch(const qbxfmm_geometry& g, HelmCoeffs hc, int pf
   return cudaGetLastError();
 }
 
-// densities per CTA: FP64, 8 when two CTAs still fit an SM's shared memory, else 4,
-// else 1; FP32 (the mixed form), all 16 of a 16-density job in one CTA so that the
-// per-pair rotation tables serve every density
+// densities per CTA: FP64 M2QBXL with more than 8 densities, the two-warps-per-center
+// kernel (16 densities share each pair's tables); otherwise FP64, 8 when two CTAs
+// still fit an SM's shared memory, else 4, else 1; FP32 (the mixed form), all 16 of a
+// 16-density job in one CTA so that the per-pair rotation tables serve every density
 template <typename R, bool FROM_LOCAL, int Q>
 static cudaError_t h3_rot_q(const qbxfmm_geometry& g, HelmCoeffs hc, int pf, int nrhs,
                             const double2* e, const double* rot, double2* qe, int32_t* err,
                             cudaStream_t st)
 {
+  constexpr bool PAIR = std::is_same<R, double>::value && !FROM_LOCAL;
   switch (hc.rb_rot) {   // the plan's tuning
     case 1: return h3_rot_launch<R, FROM_LOCAL, Q, 1>(g, hc, pf, nrhs, e, rot, qe, err, st);
     case 4: return h3_rot_launch<R, FROM_LOCAL, Q, 4>(g, hc, pf, nrhs, e, rot, qe, err, st);
@@ -2051,6 +2397,8 @@ static cudaError_t h3_rot_q(const qbxfmm_geometry& g, HelmCoeffs hc, int pf, int
     case 16:
       if constexpr (!std::is_same<R, double>::value)
         return h3_rot_launch<R, FROM_LOCAL, Q, 16>(g, hc, pf, nrhs, e, rot, qe, err, st);
+      else if constexpr (PAIR)
+        return h3_pair_launch<Q>(g, hc, pf, nrhs, e, rot, qe, err, st);
       return cudaErrorInvalidValue;
     default: break;
   }
@@ -2058,6 +2406,10 @@ static cudaError_t h3_rot_q(const qbxfmm_geometry& g, HelmCoeffs hc, int pf, int
   if constexpr (!std::is_same<R, double>::value)
     if (nrhs >= 16 && h3_rot_smem<R, FROM_LOCAL, Q, 16>(pf) <= two_per_sm)
       return h3_rot_launch<R, FROM_LOCAL, Q, 16>(g, hc, pf, nrhs, e, rot, qe, err, st);
+  if constexpr (PAIR)
+    if (nrhs > 8 && h3_pair_smem<Q>(pf) <= two_per_sm &&
+        (2 * pf + 1) * (Q + 1) <= 2 * H3P_SLOTS * 32)
+      return h3_pair_launch<Q>(g, hc, pf, nrhs, e, rot, qe, err, st);
   if (nrhs >= 8 && h3_rot_smem<R, FROM_LOCAL, Q, 8>(pf) <= two_per_sm)
     return h3_rot_launch<R, FROM_LOCAL, Q, 8>(g, hc, pf, nrhs, e, rot, qe, err, st);
   if (nrhs >= 4)

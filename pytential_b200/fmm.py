@@ -154,13 +154,32 @@ class _IdentityUpsampler:
                         ctypes.POINTER(ctypes.c_double)))
 
 
+def resolve_fmm_orders(fmm_order, kernel, tree):
+    """``(largest order, per-level orders or None)`` from an FMM order given as an
+    int, a sequence with one order per tree level, or the reference's
+    ``fmm_level_to_order(kernel, kernel_args, tree, level)`` callable
+    (pytential/qbx/__init__.py:276-285)."""
+    if callable(fmm_order):
+        orders = [int(fmm_order(kernel, frozenset(), tree, lev)) for lev in range(tree.nlevels)]
+    elif isinstance(fmm_order, (list, tuple, np.ndarray)):
+        orders = [int(o) for o in fmm_order]
+        if len(orders) != tree.nlevels:
+            raise ValueError(f"{len(orders)} level orders for a tree of {tree.nlevels} levels")
+    else:
+        return int(fmm_order), None
+    pmax = max(orders)
+    return pmax, (orders if min(orders) != pmax else None)
+
+
 class Plan:
     """A ``qbxfmm_plan`` (validated kernel + geometry) with its lifetime tied to
-    the Python object."""
+    the Python object.  ``level_orders`` (one order per tree level, each at most
+    ``fmm_order``) truncates the box expansions of each level to its own order."""
 
     def __init__(self, dgeo: DeviceGeometry, spec: SourceKernelSpec, qbx_order: int,
                  fmm_order: int, nrhs: int = 1, target_specific_qbx: bool = False,
-                 precision: int = PRECISION_FP64, fmm_backend: str = "sumpy"):
+                 precision: int = PRECISION_FP64, fmm_backend: str = "sumpy",
+                 level_orders=None):
         self.dgeo = dgeo
         self.fmm_backend = fmm_backend
         self.precision = precision
@@ -181,6 +200,26 @@ class Plan:
         self.handle = h
         self.ncf = abi.ncoeff(spec.kernel.family, spec.kernel.dim, fmm_order)
         self.ncq = abi.ncoeff(spec.kernel.family, spec.kernel.dim, qbx_order)
+        self.level_orders = None
+        if level_orders is not None:
+            self.set_level_orders(level_orders)
+
+    def set_level_orders(self, orders):
+        """Per-level FMM orders (``qbxfmm_plan_set_level_orders``); None restores
+        ``fmm_order`` on every level."""
+        if orders is None:
+            self.call("qbxfmm_plan_set_level_orders", None, 0)
+            self.level_orders = None
+            return
+        arr = (ctypes.c_int32 * len(orders))(*[int(o) for o in orders])
+        self.call("qbxfmm_plan_set_level_orders", arr, len(orders))
+        self.level_orders = [int(o) for o in orders]
+
+    def get_level_orders(self):
+        n = int(self.dgeo.struct.nlevels)
+        arr = (ctypes.c_int32 * n)()
+        self.call("qbxfmm_plan_get_level_orders", arr, n)
+        return list(arr)
 
     def __del__(self):
         h = getattr(self, "handle", None)
@@ -234,21 +273,16 @@ class B200QBXExpansionWrangler:
         self.geo_data = geo_data
         self.dtype = dtype
         self.qbx_order = qbx_order
-        if callable(fmm_level_to_order):
-            orders = {fmm_level_to_order(tree_indep.spec.kernel, frozenset(),
-                                         geo_data.tree(), lev)
-                      for lev in range(geo_data.tree().nlevels)}
-            if len(orders) != 1:
-                raise NotImplementedError("per-level FMM orders")
-            fmm_order = orders.pop()
-        else:
-            fmm_order = int(fmm_level_to_order)
+        fmm_order, level_orders = resolve_fmm_orders(fmm_level_to_order,
+                                                     tree_indep.spec.kernel, geo_data.tree())
         self.fmm_order = fmm_order
+        self.level_orders = level_orders
         self.nrhs = nrhs
         self.dgeo = _device_geometry(geo_data, tree_indep.spec, device, device_geometry)
         self.device = self.dgeo.device
         self.plan = Plan(self.dgeo, tree_indep.spec, qbx_order, fmm_order, nrhs,
-                         target_specific_qbx=self.using_tsqbx, fmm_backend=fmm_backend)
+                         target_specific_qbx=self.using_tsqbx, fmm_backend=fmm_backend,
+                         level_orders=level_orders)
         self._translations = None
         if needs_per_level_classes(tree_indep.spec):
             # the translation stages of this kernel run on precomputed matrices
@@ -494,7 +528,12 @@ class QBXApply:
     reference's ``QBXLayerPotentialSource(fmm_backend=...)`` does
     (pytential/qbx/__init__.py:93, 191): "sumpy" (the default: sumpy's default
     expansions, compressed Cartesian Taylor in 3D, H2D in 2D Helmholtz) or "fmmlib"
-    (spherical waves); only 3D Helmholtz truncates differently."""
+    (spherical waves); only 3D Helmholtz truncates differently.
+
+    ``fmm_order`` is an int, one order per tree level, or the reference's
+    ``fmm_level_to_order(kernel, kernel_args, tree, level)`` callable; with orders that
+    differ by level the box expansions of each level are truncated to its order
+    (``Plan.set_level_orders``)."""
 
     def __init__(self, geo: QBXFMMGeometryData, spec: SourceKernelSpec, qbx_order: int,
                  fmm_order: int, nrhs: int = 1, device="cuda",
@@ -505,9 +544,10 @@ class QBXApply:
         self.device = torch.device(device)
         self.dgeo = _device_geometry(geo, spec, device, device_geometry)
         self.up = DeviceUpsampler(geo.discr, device)
+        fmm_order, level_orders = resolve_fmm_orders(fmm_order, spec.kernel, geo.tree())
         self.plan = Plan(self.dgeo, spec, qbx_order, fmm_order, nrhs,
                          target_specific_qbx=target_specific_qbx, precision=precision,
-                         fmm_backend=fmm_backend)
+                         fmm_backend=fmm_backend, level_orders=level_orders)
         self.nrhs = nrhs
         sizes = self.plan.workspace_sizes()
         use_mats = (translation_matrices or needs_per_level_classes(spec)) and sizes[6] > 0

@@ -46,6 +46,8 @@ _STAGES = {
                           ctypes.POINTER(abi.QBXFMMWorkspace), _vp, _vp, _vp, _vp, _vp],
     "qbxfmm_plan_set_tuning": [ctypes.POINTER(abi.QBXFMMTuning)],
     "qbxfmm_plan_get_tuning": [ctypes.POINTER(abi.QBXFMMTuning)],
+    "qbxfmm_plan_set_level_orders": [_pi, _int],
+    "qbxfmm_plan_get_level_orders": [_pi, _int],
 }
 
 # every symbol include/qbxfmm_api.h declares

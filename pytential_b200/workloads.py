@@ -201,6 +201,8 @@ def _main(argv=None):
     ap.add_argument("--fmm-backend", default="sumpy", choices=["sumpy", "fmmlib"])
     ap.add_argument("--tune", action="store_true",
                     help="run the launch-shape autotuner first and print its choice")
+    ap.add_argument("--no-translation-matrices", action="store_true",
+                    help="3D Laplace: translate box by box instead of by translation classes")
     a = ap.parse_args(argv)
     if a.name == "laplace3d":
         wl = laplace3d_ellipsoid(nrefine=a.size)
@@ -210,7 +212,8 @@ def _main(argv=None):
         wl = helmholtz2d_starfish(nelements=a.size)
     qa = QBXApply(wl.geometry(), wl.spec, wl.qbx_order, wl.fmm_order, nrhs=wl.nrhs,
                   target_specific_qbx=True, fmm_backend=a.fmm_backend,
-                  precision=PRECISION_MIXED if a.mixed else PRECISION_FP64)
+                  precision=PRECISION_MIXED if a.mixed else PRECISION_FP64,
+                  translation_matrices=not a.no_translation_matrices)
     dens = torch.from_numpy(wl.density).cuda()
     out = qa.new_output()
     if a.tune:
