@@ -269,10 +269,10 @@ def ncu_traffic(workload, kernel, units):
 STAGES = {
     "form_multipoles": ("k_h3_p2e<0>", ("strengths", "mpoles")),
     "coarsen_multipoles": ("k_trans_mv (M2M)", ("mpoles",)),
-    "multipole_to_local": ("k_h3_m2l_rot", ("mpoles", "locals", "err")),
+    "multipole_to_local": ("k_h3_m2l_bulk", ("mpoles", "locals", "err")),
     "form_locals": ("k_h3_p2e<1>", ("strengths", "locals", "err")),
     "refine_locals": ("k_trans_mv (L2L)", ("locals",)),
-    "translate_box_multipoles_to_qbx_local": ("k_h3_e2qbxl_rot<0>", ("mpoles", "qbx_exps", "err")),
+    "translate_box_multipoles_to_qbx_local": ("k_h3_m2qbxl_pair", ("mpoles", "qbx_exps", "err")),
     "translate_box_local_to_qbx_local": ("k_h3_l2qbxl", ("locals", "qbx_exps")),
     "eval_target_specific_qbx_locals": ("k_h3_tsqbx", ("strengths", "pot_tree", "err")),
     "eval_qbx_expansions": ("k_h3_qbxl2p", ("qbx_exps", "pot_tree")),

@@ -109,7 +109,7 @@ void h3_layout(const qbxfmm_plan* p, size_t o[8])
   o[0] = p->tc.nmatrices * p->tc.rp * p->tc.kp;
   o[1] = o[0] + p->h3gaunt.size();
   o[2] = (o[1] + p->h3rot.size() + 1) & ~(size_t)1;
-  o[3] = o[2] + p->h3m2l.size();
+  o[3] = (o[2] + p->h3m2l.size() + 1) & ~(size_t)1;    // 16-byte aligned for bulk copies
   o[4] = o[3] + (size_t)p->h3_ndir * h3_m2l_dsize(p->kern.fmm_order);
   o[5] = (o[4] + 2 * (size_t)p->h3_ncoax * h3_m2l_csize(p->kern.fmm_order) + 1) & ~(size_t)1;
   o[6] = o[5] + 2 * p->h3tp.G0.size();

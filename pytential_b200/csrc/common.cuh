@@ -118,7 +118,14 @@ QBX_D void load_point(const double* __restrict__ soa, int n, int i, double* out)
 
 // Device-side error word: the first failing kernel records a code and keeps going
 // without touching out-of-range memory.
-enum : int32_t { QBX_DEVERR_NONE = 0, QBX_DEVERR_BAD_BOX = 1, QBX_DEVERR_BAD_CENTER = 2 };
+// device error word codes: an out-of-range list entry (box, center), or a bulk copy
+// whose completion wait ran out
+enum : int32_t {
+  QBX_DEVERR_NONE = 0,
+  QBX_DEVERR_BAD_BOX = 1,
+  QBX_DEVERR_BAD_CENTER = 2,
+  QBX_DEVERR_COPY_TIMEOUT = 3
+};
 
 QBX_D void report(int32_t* err, int32_t code)
 {

@@ -1216,9 +1216,11 @@ k_h3_e2qbxl_rot(qbxfmm_geometry g, HelmCoeffs hc, int pf, int nrhs,
 // on the FP64 tensor cores.  The pair of warps splits the table work of a (center,
 // box) pair: the Wigner-d recurrence tasks are interleaved between them (blocks of 32
 // tasks), warp 1 forms the coaxial column, warp 0 the radial factors and warp 1 the
-// phases; the slice and column of order n are double-buffered, so one named barrier
-// per order (64 threads, one per center) separates writing order n + 1 from reading
-// order n.  Shared memory per CTA stays at two CTAs per SM (the box's 16-density
+// phases; the (real) slice and the column of order n are double-buffered, so one
+// named barrier per order (64 threads, one per center) separates writing order n + 1
+// from reading order n.  The phases e^{i m alpha} are applied to the source
+// coefficients as they enter the tensor-core product, so the rotation is a real
+// matrix times the real and imaginary parts: half the products of a complex one.  Shared memory per CTA stays at two CTAs per SM (the box's 16-density
 // multipole block is staged once for both centers).
 constexpr int H3P_SLOTS = 4;   // recurrence tasks per lane: (2 pf + 1)(Q + 1) <= 2 x 4 x 32
 
@@ -1258,14 +1260,15 @@ k_h3_m2qbxl_pair(qbxfmm_geometry g, HelmCoeffs hc, int pf, int nrhs,
   double* s_rt = s_isq + nisq;
   double* spow = s_rt + nrt;                                    // [nl]: s_box^n
   double2* cbase = reinterpret_cast<double2*>(s_isq + (((size_t)nisq + nrt + nl + 1) & ~(size_t)1));
-  // per center: slices (two buffers; after the order loop the two warps' [NCQ][HB]
-  // blocks of translated coefficients), coaxial columns (two buffers), radial
-  // factors, phases, back-rotation matrices, half-angle powers
-  const size_t nsl = max((size_t)2 * nm * NMU, (size_t)2 * NCQ * HB);
+  // per center: real slices eps_m eps_mu d^n_{m mu} (two buffers of [nm][NMU]; after
+  // the order loop the two warps' [NCQ][HB] blocks of translated coefficients),
+  // coaxial columns (two buffers), radial factors, phases, back-rotation matrices,
+  // half-angle powers
+  const size_t nsl = max((size_t)nm * NMU, (size_t)2 * NCQ * HB);
   const size_t per = nsl + 2 * NCQ + (L + 2) + nm + ((size_t)NMU * NCQ + 2 * (size_t)nm + 1) / 2;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int cp = warp >> 1, half = warp & 1;
-  double2* Dsl = cbase + (size_t)cp * per;                      // [2][nm][NMU]
+  double2* Dsl = cbase + (size_t)cp * per;                      // (double) [2][nm][NMU]
   double2* Lp = Dsl + (size_t)half * NCQ * HB;                  // [NCQ][HB] (after the loop)
   double2* coax = Dsl + nsl;                                    // [2][NCQ]
   double2* rad = coax + 2 * NCQ;                                // [L + 2]
@@ -1371,7 +1374,7 @@ k_h3_m2qbxl_pair(qbxfmm_geometry g, HelmCoeffs hc, int pf, int nrhs,
       for (int nu = 0; nu <= Q; ++nu) lacc[ts][nu] = c2(0.0);
 
     for (int n = 0; n <= pf; ++n) {
-      double2* Dph = Dsl + (size_t)(n & 1) * nm * NMU;
+      double* Dre = reinterpret_cast<double*>(Dsl) + (size_t)(n & 1) * nm * NMU;
       double2* coaxn = coax + (n & 1) * NCQ;
       // (1) slice of order n from this warp's recurrence tasks (as in k_h3_e2qbxl_rot)
       const double rn = n > 0 ? 1.0 / n : 0.0;
@@ -1386,12 +1389,12 @@ k_h3_m2qbxl_pair(qbxfmm_geometry g, HelmCoeffs hc, int pf, int nrhs,
         if (abs(m) <= n) {
           const double d = n >= n0[sl] ? cur[sl] : 0.0;
           const double v1 = (((m > 0) && (m & 1)) != ((mu & 1) != 0)) ? -d : d;
-          Dph[(m + pf) * NMU + mu + Q] = cscale(v1, ph[m + pf]);
+          Dre[(m + pf) * NMU + mu + Q] = v1;
           if (n <= Q) Tb[(mu + Q) * NCQ + tbase + m] = v1;
           if (mu > 0) {
             const bool neg = (((m + mu) & 1) != 0) != ((m < 0) && (m & 1));
             const double v2 = neg ? -d : d;
-            Dph[(pf - m) * NMU + Q - mu] = cscale(v2, ph[pf - m]);
+            Dre[(pf - m) * NMU + Q - mu] = v2;
             if (n <= Q) Tb[(Q - mu) * NCQ + tbase - m] = v2;
           }
         }
@@ -1433,26 +1436,29 @@ k_h3_m2qbxl_pair(qbxfmm_geometry g, HelmCoeffs hc, int pf, int nrhs,
         coaxn[o] = tt;
       }
       h3_pair_bar(cp);     // slice and column of order n complete
-      // (3) rotate this warp's 8 densities on the FP64 tensor cores and translate
+      // (3) rotate this warp's 8 densities on the FP64 tensor cores and translate:
+      // M'(mu, r) = sum_m A[mu][m] B[m][r] with the real A = eps_m eps_mu d^n_{m mu} and
+      // B = e^{i m alpha} M(n, m, r), whose real and imaginary parts are two column
+      // tiles (K = 2n + 1 padded to 4; row tiles mu index 0..7 and 8..15)
       const int base = n * n + n;
       const int rho = lane >> 2, kq = lane & 3;
-      double c[NTILE][2];
+      double c[2][2][2];
 #pragma unroll
-      for (int t = 0; t < NTILE; ++t) c[t][0] = c[t][1] = 0.0;
+      for (int t = 0; t < 2; ++t) c[t][0][0] = c[t][0][1] = c[t][1][0] = c[t][1][1] = 0.0;
       const double2* Eb = Es + (base - n) * RB + half * HB + rho;
-      const double2* Db = Dph + (pf - n) * NMU;
-      for (int sk = 0; sk <= n; ++sk) {
-        const int kap = 4 * sk + kq, mi = kap >> 1, pin = kap & 1;
-        const bool vk = mi <= 2 * n;
-        const double2 e = vk ? Eb[mi * RB] : c2(0.0);
-        const double b = pin ? e.y : e.x;
-        const double2 z0 = (vk && rho < NMU) ? Db[mi * NMU + rho] : c2(0.0);
-        h3_dmma(c[0][0], c[0][1], pin ? -z0.y : z0.x, b);
-        h3_dmma(c[1][0], c[1][1], pin ? z0.x : z0.y, b);
+      const double* Dr = Dre + (pf - n) * NMU;
+      const double2* phn = ph + (pf - n);
+      for (int sk = 0; 4 * sk <= 2 * n; ++sk) {
+        const int kap = 4 * sk + kq;
+        const bool vk = kap <= 2 * n;
+        const double2 b = vk ? cmul(Eb[kap * RB], phn[kap]) : c2(0.0);
+        const double a0 = (vk && rho < NMU) ? Dr[kap * NMU + rho] : 0.0;
+        h3_dmma(c[0][0][0], c[0][0][1], a0, b.x);
+        h3_dmma(c[0][1][0], c[0][1][1], a0, b.y);
         if (NTILE == 4) {
-          const double2 z1 = (vk && 8 + rho < NMU) ? Db[mi * NMU + 8 + rho] : c2(0.0);
-          h3_dmma(c[NTILE - 2][0], c[NTILE - 2][1], pin ? -z1.y : z1.x, b);
-          h3_dmma(c[NTILE - 1][0], c[NTILE - 1][1], pin ? z1.x : z1.y, b);
+          const double a1 = (vk && 8 + rho < NMU) ? Dr[kap * NMU + 8 + rho] : 0.0;
+          h3_dmma(c[1][0][0], c[1][0][1], a1, b.x);
+          h3_dmma(c[1][1][0], c[1][1][1], a1, b.y);
         }
       }
 #pragma unroll
@@ -1460,7 +1466,7 @@ k_h3_m2qbxl_pair(qbxfmm_geometry g, HelmCoeffs hc, int pf, int nrhs,
         const int grp = sl >> 1, v = sl & 1;
         const int mu = (grp ? 8 + rho : rho) - Q;
         if (grp * 8 + rho >= NMU || abs(mu) > n || (grp && NTILE < 4)) continue;
-        const double2 mr = c2(c[2 * grp][v], c[2 * grp + 1][v]);
+        const double2 mr = c2(c[grp][0][v], c[grp][1][v]);
         const int amu = abs(mu);
 #pragma unroll
         for (int nu = 0; nu <= Q; ++nu)
@@ -2125,6 +2131,298 @@ k_h3_m2l_rot(qbxfmm_geometry g, int pf, int nrhs, const double2* __restrict__ mp
   }
 }
 
+// {{{ M2L with the pair tables brought in by bulk copies
+
+QBX_D unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+QBX_D void mbar_init(uint64_t* mb)
+{
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_addr(mb)) : "memory");
+}
+
+// one arrival that also expects `bytes` of copy completion on the barrier
+QBX_D void mbar_expect(uint64_t* mb, unsigned bytes)
+{
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n"
+               ::"r"(smem_addr(mb)), "r"(bytes) : "memory");
+}
+
+// global -> this CTA's shared memory, completion counted on mb (16-byte aligned
+// addresses, size a multiple of 16)
+QBX_D void bulk_copy(void* dst, const void* src, unsigned bytes, uint64_t* mb)
+{
+  asm volatile("fence.proxy.async.shared::cta;\n"
+               "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n"
+               ::"r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(smem_addr(mb)) : "memory");
+}
+
+// bounded wait for the phase of the given parity; false if it did not complete
+QBX_D bool mbar_wait(uint64_t* mb, unsigned parity)
+{
+  for (int it = 0; it < (1 << 22); ++it) {
+    unsigned done;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                 " selp.u32 %0, 1, 0, p;\n}\n"
+                 : "=r"(done) : "r"(smem_addr(mb)), "r"(parity) : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+// The FP64 M2L of k_h3_m2l_rot with its pair tables brought in by bulk copies
+// (cp.async.bulk, completion on an mbarrier) into buffers of their own: the rotation
+// table once per pair (the register-staged form copies it twice, before the rotation
+// and again before the back rotation, because it shares one buffer with the coaxial
+// table) and the coaxial table of pair q + 1 while pair q's back rotation runs.  One
+// thread issues the copies; waits are bounded: a copy that does not arrive sets the
+// error word, the CTA waits (bounded) for the copies it issued and stops.
+template <int RB>
+__global__ void __launch_bounds__(H3M2L_NT)
+k_h3_m2l_bulk(qbxfmm_geometry g, int pf, int nrhs, const double2* __restrict__ mp,
+              double2* __restrict__ lo, const double* __restrict__ Dtab,
+              const double2* __restrict__ Ctab, const double* __restrict__ clsmap,
+              int32_t* err)
+{
+  extern __shared__ double2 smem2[];
+  __shared__ uint64_t mbD, mbC;
+  __shared__ int s_gn[H3M2L_NG], s_gm0[H3M2L_NG];
+  __shared__ int s_cmu[H3M2L_NCG], s_cnu0[H3M2L_NCG];
+  __shared__ int s_ng, s_ncg;
+  __shared__ unsigned char s_nof[(H3_MAXP + 1) * (H3_MAXP + 1)];
+  constexpr int NTHR = H3M2L_NT;
+  constexpr int KMAX = (H3M2L_NG * RB + NTHR - 1) / NTHR;
+  const int ncf = (pf + 1) * (pf + 1), XS = ncf + 1, nm = 2 * pf + 1;
+  const size_t dsz = h3_m2l_dsize(pf), csz = h3_m2l_csize(pf);
+  double2* X = smem2;                                              // [RB][ncf + 1]
+  double2* A = X + (size_t)RB * XS;                                // [RB][ncf + 1]
+  double* Db = reinterpret_cast<double*>(A + (size_t)RB * XS);     // [dsz]
+  double2* Cb = reinterpret_cast<double2*>(Db + dsz);              // [csz]
+  if (threadIdx.x == 0) {
+    int ng = 0;
+    for (int n = 0; n <= pf; ++n)
+      for (int m0 = -n; m0 <= n; m0 += 4) {
+        s_gn[ng] = n;
+        s_gm0[ng] = m0;
+        ++ng;
+      }
+    s_ng = ng;
+    int ncg = 0;
+    for (int mu = -pf; mu <= pf; ++mu)
+      for (int nu0 = abs(mu); nu0 <= pf; nu0 += 4) {
+        s_cmu[ncg] = mu;
+        s_cnu0[ncg] = nu0;
+        ++ncg;
+      }
+    s_ncg = ncg;
+    mbar_init(&mbD);
+    mbar_init(&mbC);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  for (int n = 0; n <= pf; ++n)
+    for (int x = n * n + threadIdx.x; x < (n + 1) * (n + 1); x += NTHR) s_nof[x] = (unsigned char)n;
+  __syncthreads();
+  const int i = blockIdx.x;
+  const int r0 = blockIdx.y * RB;
+  const int q0 = g.m2l_tgt_pair_starts[i], q1 = g.m2l_tgt_pair_starts[i + 1];
+  if (q1 <= q0) return;                    // before any copy is issued
+  const int ng = s_ng, ncg = s_ncg;
+  const unsigned dbytes = (unsigned)(dsz * sizeof(double)), cbytes = (unsigned)(csz * sizeof(double2));
+  auto cls_of = [&](int q) {
+    const int pr = g.m2l_tgt_pairs[q];
+    int lo_c = 0, hi_c = g.m2l_nclasses - 1;
+    while (lo_c < hi_c) {
+      const int mid = (lo_c + hi_c + 1) >> 1;
+      if (g.m2l_class_starts[mid] <= pr) lo_c = mid;
+      else hi_c = mid - 1;
+    }
+    return lo_c;
+  };
+  // copies issued / completed-and-waited per barrier (the phase parity of the next
+  // wait is the completed count's)
+  int nd_issued = 0, nd_done = 0, nc_issued = 0, nc_done = 0;
+  auto issue_D = [&](int q) {
+    if (threadIdx.x == 0) {
+      const int c = cls_of(q);
+      mbar_expect(&mbD, dbytes);
+      bulk_copy(Db, Dtab + (size_t)clsmap[2 * c] * dsz, dbytes, &mbD);
+    }
+    ++nd_issued;
+  };
+  auto issue_C = [&](int q) {
+    if (threadIdx.x == 0) {
+      const int c = cls_of(q);
+      mbar_expect(&mbC, cbytes);
+      bulk_copy(Cb, Ctab + (size_t)clsmap[2 * c + 1] * csz, cbytes, &mbC);
+    }
+    ++nc_issued;
+  };
+  auto wait_D = [&]() {
+    if (!mbar_wait(&mbD, nd_done & 1)) return 1;
+    ++nd_done;
+    return 0;
+  };
+  auto wait_C = [&]() {
+    if (!mbar_wait(&mbC, nc_done & 1)) return 1;
+    ++nc_done;
+    return 0;
+  };
+  // after a copy that did not arrive: report, then wait (bounded) for the copies
+  // still in flight so that none outlives the CTA
+  auto drain = [&]() {
+    if (threadIdx.x == 0) report(err, QBX_DEVERR_COPY_TIMEOUT);
+    for (; nd_done < nd_issued; ++nd_done) mbar_wait(&mbD, nd_done & 1);
+    for (; nc_done < nc_issued; ++nc_done) mbar_wait(&mbC, nc_done & 1);
+  };
+
+  double2 acc[KMAX][4];
+#pragma unroll
+  for (int k = 0; k < KMAX; ++k)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[k][j] = c2(0.0);
+
+  issue_D(q0);
+  issue_C(q0);
+  for (int q = q0; q < q1; ++q) {
+    const int src = g.m2l_pair_src[g.m2l_tgt_pairs[q]];
+    const bool bad = (unsigned)src >= (unsigned)g.nboxes;
+    if (bad && threadIdx.x == 0) report(err, QBX_DEVERR_BAD_BOX);
+    int fail = wait_D();
+    const double2* ph = reinterpret_cast<const double2*>(Db);
+    const double* blocks = Db + 2 * nm;
+    // X = e^{i m alpha} M
+    for (int e = threadIdx.x; e < RB * ncf; e += NTHR) {
+      const int r = e / ncf, ci = e - r * ncf;
+      const int n = s_nof[ci];
+      double2 v = c2(0.0);
+      if (!fail && !bad && r0 + r < nrhs)
+        v = cmul(ph[ci - n * n - n + pf], mp[((size_t)src * nrhs + r0 + r) * ncf + ci]);
+      X[r * XS + ci] = v;
+    }
+    if (__syncthreads_or(fail)) {
+      drain();
+      return;
+    }
+    // A[(n, mu)] = sum_m T^n[m][mu] X[(n, m)]
+    for (int t = threadIdx.x; t < ng * RB; t += NTHR) {
+      const int grp = t / RB, r = t - grp * RB;
+      const int n = s_gn[grp], mu0 = s_gm0[grp];
+      const double* Tn = blocks + h3_dblock(n);
+      const int w = 2 * n + 1, nv = min(4, n - mu0 + 1);
+      double2 o[4] = {c2(0.0), c2(0.0), c2(0.0), c2(0.0)};
+      const double2* Xr = X + r * XS + n * n;
+      for (int m = 0; m < w; ++m) {
+        const double2 x = Xr[m];
+        const int ma = m - n;
+        const double* row = ma >= 0 ? Tn + ma * w + (mu0 + n) : Tn + (-ma) * w + (n - mu0);
+        const int step = ma >= 0 ? 1 : -1;
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          if (j < nv) o[j] = caxpy(row[step * j], x, o[j]);
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        if (j < nv) A[r * XS + n * n + n + mu0 + j] = o[j];
+    }
+    fail = wait_C();
+    if (__syncthreads_or(fail)) {
+      drain();
+      return;
+    }
+    // B[(nu, mu)] = sum_{n >= |mu|} C^mu[n][nu] A[(n, mu)]   (into X)
+    for (int t = threadIdx.x; t < ncg * RB; t += NTHR) {
+      const int grp = t / RB, r = t - grp * RB;
+      const int mu = s_cmu[grp], nu0 = s_cnu0[grp];
+      const int am = abs(mu), w = pf + 1 - am, nv = min(4, pf - nu0 + 1);
+      const double2* Cq = Cb + h3_cblock(pf, am) + (nu0 - am);
+      double2 o[4] = {c2(0.0), c2(0.0), c2(0.0), c2(0.0)};
+      const double2* Ar = A + r * XS;
+      for (int n = am; n <= pf; ++n) {
+        const double2 a = Ar[n * n + n + mu];
+        const double2* row = Cq + (n - am) * w;
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          if (j < nv) o[j] = cfma(row[j], a, o[j]);
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int nu = nu0 + j;
+        if (j < nv) X[r * XS + nu * nu + nu + mu] = o[j];
+      }
+    }
+    __syncthreads();
+    // the coaxial buffer is free: the next pair's table lands during the back rotation
+    if (q + 1 < q1) issue_C(q + 1);
+    // L[(nu, m2)] += e^{-i m2 alpha} sum_mu T^nu[m2][mu] B[(nu, mu)]
+#pragma unroll
+    for (int k = 0; k < KMAX; ++k) {
+      const int t = threadIdx.x + k * NTHR;
+      if (t >= ng * RB) break;
+      const int grp = t / RB, r = t - grp * RB;
+      const int nu = s_gn[grp], m20 = s_gm0[grp];
+      const int w = 2 * nu + 1, nv = min(4, nu - m20 + 1);
+      const double* Tn = blocks + h3_dblock(nu);
+      const double* pj[4];
+      int sj[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int m2 = m20 + j;
+        pj[j] = m2 >= 0 ? Tn + m2 * w : Tn + (-m2) * w + 2 * nu;
+        sj[j] = m2 >= 0 ? 1 : -1;
+      }
+      double2 o[4] = {c2(0.0), c2(0.0), c2(0.0), c2(0.0)};
+      const double2* Br = X + r * XS + nu * nu;
+      for (int mu = 0; mu < w; ++mu) {
+        const double2 bb = Br[mu];
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          if (j < nv) o[j] = caxpy(pj[j][sj[j] * mu], bb, o[j]);
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        if (j < nv) acc[k][j] = cfma(cconj(ph[m20 + j + pf]), o[j], acc[k][j]);
+    }
+    __syncthreads();
+    // the rotation buffer is free
+    if (q + 1 < q1) issue_D(q + 1);
+  }
+  const int tb = g.target_or_target_parent_boxes[i];
+  if ((unsigned)tb >= (unsigned)g.nboxes) {
+    if (threadIdx.x == 0) report(err, QBX_DEVERR_BAD_BOX);
+    return;
+  }
+#pragma unroll
+  for (int k = 0; k < KMAX; ++k) {
+    const int t = threadIdx.x + k * NTHR;
+    if (t >= ng * RB) break;
+    const int grp = t / RB, r = t - grp * RB;
+    if (r0 + r >= nrhs) continue;
+    const int nu = s_gn[grp], m20 = s_gm0[grp];
+    const int nv = min(4, nu - m20 + 1);
+    double2* out = lo + ((size_t)tb * nrhs + r0 + r) * ncf + nu * nu + nu + m20;
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      if (j < nv) out[j] = cadd(out[j], acc[k][j]);
+  }
+}
+
+// }}}
+
+template <int RB>
+static cudaError_t h3_m2l_bulk_launch(const qbxfmm_geometry& g, int pf, int nrhs, const double2* mp,
+                                      double2* lo, const double* Dtab, const double2* Ctab,
+                                      const double* clsmap, int32_t* err, cudaStream_t st)
+{
+  // bulk copies need 16-byte aligned tables
+  if ((reinterpret_cast<uintptr_t>(Dtab) | reinterpret_cast<uintptr_t>(Ctab)) & 15)
+    return cudaErrorInvalidValue;
+  size_t sh = 2 * (size_t)RB * ((pf + 1) * (pf + 1) + 1) * sizeof(double2) +
+              h3_m2l_dsize(pf) * sizeof(double) + h3_m2l_csize(pf) * sizeof(double2);
+  cudaFuncSetAttribute(k_h3_m2l_bulk<RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+  dim3 grid(g.nttp_boxes, (nrhs + RB - 1) / RB);
+  k_h3_m2l_bulk<RB><<<grid, H3M2L_NT, sh, st>>>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err);
+  return cudaGetLastError();
+}
+
 template <typename R, int RB>
 static cudaError_t h3_m2l_rot_launch(const qbxfmm_geometry& g, int pf, int nrhs, const double2* mp,
                                      double2* lo, const double* Dtab, const double2* Ctab,
@@ -2155,7 +2453,7 @@ cudaError_t h3_launch_m2l_rot(const qbxfmm_geometry& g, int pf, int nrhs, const 
                   : h3_m2l_rot_launch<double, 4>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err, st);
     case 8:
       return fp32 ? h3_m2l_rot_launch<float, 8>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err, st)
-                  : h3_m2l_rot_launch<double, 8>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err, st);
+                  : h3_m2l_bulk_launch<8>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err, st);
     case 16:
       if (fp32) return h3_m2l_rot_launch<float, 16>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err, st);
       return cudaErrorInvalidValue;
@@ -2166,7 +2464,7 @@ cudaError_t h3_launch_m2l_rot(const qbxfmm_geometry& g, int pf, int nrhs, const 
     if (nrhs >= 8) return h3_m2l_rot_launch<float, 8>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err, st);
     return h3_m2l_rot_launch<float, 4>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err, st);
   }
-  if (nrhs >= 8) return h3_m2l_rot_launch<double, 8>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err, st);
+  if (nrhs >= 8) return h3_m2l_bulk_launch<8>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err, st);
   if (nrhs >= 2) return h3_m2l_rot_launch<double, 4>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err, st);
   return h3_m2l_rot_launch<double, 1>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err, st);
 }
@@ -2349,7 +2647,7 @@ static size_t h3_pair_smem(int pf)
   const size_t ncf = (size_t)(pf + 1) * (pf + 1), L = pf + Q, nl = pf + 1, nm = 2 * pf + 1;
   const size_t nisq = (size_t)(pf + 2) * (pf + 1), nrt = (size_t)(pf + 1) * (pf + 1);
   const size_t ctad = (nisq + nrt + nl + 1) & ~(size_t)1;
-  const size_t nsl = std::max((size_t)2 * nm * NMU, (size_t)2 * NCQ * 8);
+  const size_t nsl = std::max((size_t)nm * NMU, (size_t)2 * NCQ * 8);
   const size_t per = nsl + 2 * NCQ + (L + 2) + nm + ((size_t)NMU * NCQ + 2 * nm + 1) / 2;
   return (ncf * 16 + 2 * per) * sizeof(double2) + ctad * sizeof(double);
 }

@@ -451,8 +451,13 @@ class B200QBXExpansionWrangler:
     def check_error_word(self):
         w = int(self.error_word.item())
         if w != 0:
-            raise native.QBXFMMError("device", abi.QBXFMM_ERR_DEVICE,
-                                     f"a kernel met an out-of-range index (code {w})")
+            raise native.QBXFMMError("device", abi.QBXFMM_ERR_DEVICE, _device_error_text(w))
+
+
+def _device_error_text(w: int) -> str:
+    what = {1: "an out-of-range box index", 2: "an out-of-range center index",
+            3: "a table copy whose completion wait ran out"}.get(w, "an error")
+    return f"a kernel met {what} (device error code {w})"
 
 
 def drive_fmm(actx, expansion_wrangler: B200QBXExpansionWrangler, src_weight_vecs):
@@ -648,7 +653,6 @@ class QBXApply:
     def check_error_word(self):
         w = int(self.error_word.item())
         if w != 0:
-            raise native.QBXFMMError("device", abi.QBXFMM_ERR_DEVICE,
-                                     f"a kernel met an out-of-range index (code {w})")
+            raise native.QBXFMMError("device", abi.QBXFMM_ERR_DEVICE, _device_error_text(w))
 
 # }}}
