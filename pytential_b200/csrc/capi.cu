@@ -943,7 +943,7 @@ int qbxfmm_plan_set_tuning(qbxfmm_plan* p, const qbxfmm_tuning* t)
     return false;
   };
   if (!ok(t->m2qbxl_densities, {1, 4, 8, 16}) || !ok(t->m2l_densities, {1, 4, 8, 16}) ||
-      !ok(t->p2e_densities, {1, 4, 8}) || !ok(t->l2qbxl_densities, {1, 4}) ||
+      !ok(t->p2e_densities, {1, 4, 8, 16}) || !ok(t->l2qbxl_densities, {1, 4}) ||
       !ok(t->tsqbx_densities, {1, 4, 16}))
     return fail(QBXFMM_ERR_ARG, "tuning: unsupported densities-per-CTA value");
   if (!p->mixed && t->m2l_densities == 16)

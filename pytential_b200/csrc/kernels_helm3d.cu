@@ -300,8 +300,10 @@ constexpr int H3_SUB = 16;
 constexpr int H3_TS = H3_SUB + 1;
 constexpr int H3_NH = 3;          // coefficients per thread: (p+1)^2 <= 3 * 128
 
-template <bool LOCAL, int RB>
-__global__ void __launch_bounds__(NT)
+// TH threads per CTA, NH coefficients per thread ((p+1)^2 <= NH x TH): 128 x 3 with up
+// to 8 densities, or 256 x 1 with 16 (the wave tables of a source serve all 16)
+template <bool LOCAL, int RB, int TH = NT, int NH = H3_NH>
+__global__ void __launch_bounds__(TH, TH == NT ? 1 : 2)
 k_h3_p2e(qbxfmm_geometry g, HelmCoeffs hc, int p, int nrhs, const double2* __restrict__ strengths,
          double2* __restrict__ exps, int32_t* err)
 {
@@ -338,14 +340,14 @@ k_h3_p2e(qbxfmm_geometry g, HelmCoeffs hc, int p, int nrhs, const double2* __res
   const bool two = !LOCAL && hc.taylor && dip;
   double2* tab2 = two ? rec + (size_t)(N + 1) * (N + 2) / 2 : tab;   // [(N+1)^2][TS]
   double2* rad2 = two ? tab2 + (size_t)(N + 1) * (N + 1) * TS : nullptr;   // [SUB][N+2]
-  h3_rec_table(N, rec, threadIdx.x, NT);
+  h3_rec_table(N, rec, threadIdx.x, TH);
 
-  int o_c[H3_NH];
-  Ladder lad[H3_NH];
-  bool valid[H3_NH];
+  int o_c[NH];
+  Ladder lad[NH];
+  bool valid[NH];
 #pragma unroll
-  for (int h = 0; h < H3_NH; ++h) {
-    int ci = threadIdx.x + h * NT;
+  for (int h = 0; h < NH; ++h) {
+    int ci = threadIdx.x + h * TH;
     valid[h] = ci < ncf;
     int n = 0, m = 0;
     if (valid[h]) hq_decode(ci, n, m);
@@ -354,9 +356,9 @@ k_h3_p2e(qbxfmm_geometry g, HelmCoeffs hc, int p, int nrhs, const double2* __res
 #pragma unroll
     for (int u = 0; u < 6; ++u) lad[h].o[u] *= TS;
   }
-  double2 acc[H3_NH][RB];
+  double2 acc[NH][RB];
 #pragma unroll
-  for (int h = 0; h < H3_NH; ++h)
+  for (int h = 0; h < NH; ++h)
 #pragma unroll
     for (int rr = 0; rr < RB; ++rr) acc[h][rr] = c2(0.0);
 
@@ -410,14 +412,14 @@ k_h3_p2e(qbxfmm_geometry g, HelmCoeffs hc, int p, int nrhs, const double2* __res
         }
       }
       __syncthreads();
-      for (int wk = threadIdx.x; wk < cnt * (N + 1); wk += NT) {
+      for (int wk = threadIdx.x; wk < cnt * (N + 1); wk += TH) {
         int m = wk / cnt, j = wk - m * cnt;
         h3_wave_column(m, N, s_t[j], s_w[j], rec, s_rad[j], tab + j, TS);
         if (two) h3_wave_column(m, N, s_t[j], s_w[j], rec, rad2 + j * (N + 2), tab2 + j, TS);
       }
       __syncthreads();
 #pragma unroll
-      for (int h = 0; h < H3_NH; ++h) {
+      for (int h = 0; h < NH; ++h) {
         if (!valid[h]) continue;
         for (int j = 0; j < cnt; ++j) {
           const double2* T = tab + j;
@@ -438,9 +440,9 @@ k_h3_p2e(qbxfmm_geometry g, HelmCoeffs hc, int p, int nrhs, const double2* __res
     }
   }
 #pragma unroll
-  for (int h = 0; h < H3_NH; ++h) {
+  for (int h = 0; h < NH; ++h) {
     if (!valid[h]) continue;
-    int ci = threadIdx.x + h * NT;
+    int ci = threadIdx.x + h * TH;
     int n, m;
     hq_decode(ci, n, m);
     double f = FOUR_PI * hc.k * (LOCAL ? pow(sc, (double)n) : pow(sc, -(double)n));
@@ -2500,6 +2502,16 @@ static cudaError_t h3_p2e_launch(int nbox, size_t sh, const qbxfmm_geometry& g, 
     k_h3_p2e<LOCAL, RB><<<dim3(nbox, (nrhs + RB - 1) / RB), NT, sh, st>>>(g, hc, p, nrhs, s, e, \
                                                                           err);                 \
     return cudaGetLastError();                                                                  \
+  }
+  // 16 densities: 256 threads, one coefficient each
+  const bool wide = (p + 1) * (p + 1) <= 2 * NT;
+  if (hc.rb_p2e == 16 || (hc.rb_p2e == 0 && nrhs > 8 && wide)) {
+    if (!wide) return cudaErrorInvalidValue;
+    cudaFuncSetAttribute(k_h3_p2e<LOCAL, 16, 2 * NT, 1>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+    k_h3_p2e<LOCAL, 16, 2 * NT, 1><<<dim3(nbox, (nrhs + 15) / 16), 2 * NT, sh, st>>>(
+        g, hc, p, nrhs, s, e, err);
+    return cudaGetLastError();
   }
   if (hc.rb_p2e == 8) QBX_H3_P2E(8)   // the plan's tuning
   if (hc.rb_p2e == 4) QBX_H3_P2E(4)
