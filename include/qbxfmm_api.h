@@ -44,7 +44,7 @@ int qbxfmm_plan_destroy(qbxfmm_plan* plan);
  * depend on the choice beyond the summation order. */
 typedef struct qbxfmm_tuning {
   int32_t m2qbxl_densities;   /* 1, 4, 8, 16 (FP64: two warps per center share the tables) */
-  int32_t m2l_densities;      /* 1, 4, 8 (16: mixed precision only) */
+  int32_t m2l_densities;      /* 1, 4, 8, 16 */
   int32_t p2e_densities;      /* P2M / P2L: 1, 4, 8, 16 (16: orders p <= 15) */
   int32_t l2qbxl_densities;   /* 1, 4 */
   int32_t tsqbx_densities;    /* 1, 4, 16 */

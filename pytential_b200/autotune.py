@@ -28,7 +28,7 @@ from . import abi, native
 # knob -> (stage entry timed, candidate densities per CTA, mixed-precision-only values)
 KNOBS = {
     "m2qbxl_densities": ("qbxfmm_translate_box_multipoles_to_qbx_local", (1, 4, 8, 16), ()),
-    "m2l_densities": ("qbxfmm_multipole_to_local", (1, 4, 8, 16), (16,)),
+    "m2l_densities": ("qbxfmm_multipole_to_local", (1, 4, 8, 16), ()),
     "p2e_densities": ("qbxfmm_form_locals", (1, 4, 8, 16), ()),
     "l2qbxl_densities": ("qbxfmm_translate_box_local_to_qbx_local", (1, 4), ()),
     "tsqbx_densities": ("qbxfmm_eval_target_specific_qbx_locals", (1, 4, 16), ()),

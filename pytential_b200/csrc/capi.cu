@@ -946,8 +946,6 @@ int qbxfmm_plan_set_tuning(qbxfmm_plan* p, const qbxfmm_tuning* t)
       !ok(t->p2e_densities, {1, 4, 8, 16}) || !ok(t->l2qbxl_densities, {1, 4}) ||
       !ok(t->tsqbx_densities, {1, 4, 16}))
     return fail(QBXFMM_ERR_ARG, "tuning: unsupported densities-per-CTA value");
-  if (!p->mixed && t->m2l_densities == 16)
-    return fail(QBXFMM_ERR_ARG, "tuning: 16 densities per CTA of M2L is a mixed-precision shape");
   p->hc.rb_rot = t->m2qbxl_densities;
   p->hc.rb_m2l = t->m2l_densities;
   p->hc.rb_p2e = t->p2e_densities;

@@ -2178,8 +2178,8 @@ QBX_D bool mbar_wait(uint64_t* mb, unsigned parity)
 // table) and the coaxial table of pair q + 1 while pair q's back rotation runs.  One
 // thread issues the copies; waits are bounded: a copy that does not arrive sets the
 // error word, the CTA waits (bounded) for the copies it issued and stops.
-template <int RB>
-__global__ void __launch_bounds__(H3M2L_NT)
+template <int RB, int NTHR = H3M2L_NT>
+__global__ void __launch_bounds__(NTHR, NTHR == H3M2L_NT ? 2 : 1)
 k_h3_m2l_bulk(qbxfmm_geometry g, int pf, int nrhs, const double2* __restrict__ mp,
               double2* __restrict__ lo, const double* __restrict__ Dtab,
               const double2* __restrict__ Ctab, const double* __restrict__ clsmap,
@@ -2191,7 +2191,6 @@ k_h3_m2l_bulk(qbxfmm_geometry g, int pf, int nrhs, const double2* __restrict__ m
   __shared__ int s_cmu[H3M2L_NCG], s_cnu0[H3M2L_NCG];
   __shared__ int s_ng, s_ncg;
   __shared__ unsigned char s_nof[(H3_MAXP + 1) * (H3_MAXP + 1)];
-  constexpr int NTHR = H3M2L_NT;
   constexpr int KMAX = (H3M2L_NG * RB + NTHR - 1) / NTHR;
   const int ncf = (pf + 1) * (pf + 1), XS = ncf + 1, nm = 2 * pf + 1;
   const size_t dsz = h3_m2l_dsize(pf), csz = h3_m2l_csize(pf);
@@ -2409,7 +2408,7 @@ k_h3_m2l_bulk(qbxfmm_geometry g, int pf, int nrhs, const double2* __restrict__ m
 
 // }}}
 
-template <int RB>
+template <int RB, int NTHR = H3M2L_NT>
 static cudaError_t h3_m2l_bulk_launch(const qbxfmm_geometry& g, int pf, int nrhs, const double2* mp,
                                       double2* lo, const double* Dtab, const double2* Ctab,
                                       const double* clsmap, int32_t* err, cudaStream_t st)
@@ -2419,9 +2418,9 @@ static cudaError_t h3_m2l_bulk_launch(const qbxfmm_geometry& g, int pf, int nrhs
     return cudaErrorInvalidValue;
   size_t sh = 2 * (size_t)RB * ((pf + 1) * (pf + 1) + 1) * sizeof(double2) +
               h3_m2l_dsize(pf) * sizeof(double) + h3_m2l_csize(pf) * sizeof(double2);
-  cudaFuncSetAttribute(k_h3_m2l_bulk<RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+  cudaFuncSetAttribute(k_h3_m2l_bulk<RB, NTHR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
   dim3 grid(g.nttp_boxes, (nrhs + RB - 1) / RB);
-  k_h3_m2l_bulk<RB><<<grid, H3M2L_NT, sh, st>>>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err);
+  k_h3_m2l_bulk<RB, NTHR><<<grid, NTHR, sh, st>>>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err);
   return cudaGetLastError();
 }
 
@@ -2458,7 +2457,7 @@ cudaError_t h3_launch_m2l_rot(const qbxfmm_geometry& g, int pf, int nrhs, const 
                   : h3_m2l_bulk_launch<8>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err, st);
     case 16:
       if (fp32) return h3_m2l_rot_launch<float, 16>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err, st);
-      return cudaErrorInvalidValue;
+      return h3_m2l_bulk_launch<16, 2 * H3M2L_NT>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err, st);
     default: break;
   }
   if (fp32) {   // mixed form: FP32 arithmetic, all 16 densities of a pair's tables at once

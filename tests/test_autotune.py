@@ -24,7 +24,7 @@ def test_tuning_roundtrip_and_validation():
                          "l2qbxl_densities": 1, "tsqbx_densities": 16})
     assert get_tuning(ap.plan)["p2e_densities"] == 8
     with pytest.raises(native.QBXFMMError) as ei:
-        set_tuning(ap.plan, {"m2l_densities": 16})         # FP32-only shape on an FP64 plan
+        set_tuning(ap.plan, {"m2l_densities": 2})          # not a shape
     assert ei.value.code == abi.QBXFMM_ERR_ARG
 
 
