@@ -43,6 +43,21 @@ class CenterToTargetList:
     lists: np.ndarray
 
 
+def _center_to_tree_targets_device(tree_ttc: np.ndarray, ncenters: int) -> CenterToTargetList:
+    """The center -> tree-target CSR (pytential/qbx/geometry.py:839-872) on the GPU:
+    the QBX targets in tree order, stably sorted by their center (so each center's
+    targets stay in tree order), and the start of each center's run; identical to the
+    host construction."""
+    import torch
+    t = torch.from_numpy(np.ascontiguousarray(tree_ttc, np.int64)).cuda()
+    tgt = torch.nonzero(t >= 0).flatten()
+    ctr = t[tgt]
+    ctr_sorted, order = torch.sort(ctr, stable=True)
+    starts = torch.searchsorted(ctr_sorted, torch.arange(ncenters + 1, device=t.device))
+    return CenterToTargetList(starts.to(torch.int32).cpu().numpy(),
+                              tgt[order].to(torch.int32).cpu().numpy())
+
+
 @dataclass
 class FilteredTargetLists:
     """Non-QBX targets in tree order (boxtree ``FilteredTargetListsInTreeOrder``)."""
@@ -229,6 +244,8 @@ class QBXFMMGeometryData:
         tree = self.tree()
         ttc_user = self.user_target_to_center()
         tree_ttc = ttc_user[tree.sorted_target_ids]
+        if self._on_device():
+            return _center_to_tree_targets_device(tree_ttc, self.ncenters)
         tgt = np.where(tree_ttc >= 0)[0]
         ctr = tree_ttc[tgt]
         order = np.lexsort((tgt, ctr))

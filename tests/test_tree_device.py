@@ -80,3 +80,14 @@ def test_device_traversal_equals_host_large():
     from pytential_b200.workloads import helmholtz3d_ellipsoid
     tree = helmholtz3d_ellipsoid(nrefine=5, nrhs=1).geometry().tree()
     _same_traversal(build_traversal(tree), build_traversal_device(tree))
+
+
+@pytest.mark.parametrize("name", ["2d-S", "3d-D-small", "h3d-CF-small"])
+def test_device_center_to_target_csr_equals_host(name):
+    from pytential_b200.geometry import QBXFMMGeometryData
+    wl = workload(name)
+    dev = QBXFMMGeometryData(wl.discr, wl.targets, builders="device").center_to_tree_targets()
+    host = QBXFMMGeometryData(wl.discr, wl.targets, builders="host").center_to_tree_targets()
+    for f in ("starts", "lists"):
+        a, b = getattr(dev, f), getattr(host, f)
+        assert a.dtype == b.dtype and np.array_equal(a, b), f
