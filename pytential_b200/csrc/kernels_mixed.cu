@@ -620,6 +620,266 @@ k_trans_gemm_x3(int ncf, int rp, int rp16, int kp8, int nrhs, const uint32_t* __
 
 // }}}
 
+// {{{ split-TF32 M2L on the 5th-generation tensor cores (tcgen05, accumulator in TMEM)
+
+// C^T = X^T T^T for one translation class and 128 columns (pair x density): M = 128
+// columns, N = the matrix rows (rp16 <= 256), K = kp8 in chunks of 32, split TF32
+// (three products lo.hi, hi.lo, hi.hi into one FP32 accumulator in tensor memory).
+// Operands live in shared memory in the no-swizzle K-major layout (8-row x 16-byte
+// core matrices, contiguous).  The class matrix's TF32 planes are stored at precompute
+// in that layout chunk by chunk, so each chunk of B arrives with one bulk copy per
+// plane (cp.async.bulk, completion on an mbarrier); the threads split the gathered
+// source expansions (A) into TF32 hi / lo.  Two stages: while the tensor core works
+// on chunk i (one thread issues its MMAs and commits them to the stage's mbarrier),
+// the copy engine and the threads fill chunk i + 1.  The accumulator is read back with
+// tcgen05.ld (warps w and w + 4 own TMEM lanes 32 (w mod 4) .. + 31, i.e. those
+// columns, and split the rows) and stored per pair into the FP64 pair scratch.  Waits
+// are bounded: a wait that runs out sets the error word; the CTA then waits (bounded)
+// for its copies and MMAs, frees its tensor memory and stops.
+constexpr int UM_M = 128;        // columns per CTA (MMA M)
+constexpr int UM_KC = 32;        // K per chunk (four MMA K-steps of 8)
+constexpr int UM_TCOLS = 256;    // tensor-memory columns allocated (>= N, power of two)
+constexpr int UM_NT = 256;       // threads
+
+QBX_D unsigned um_smem(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+// no-swizzle K-major shared-memory descriptor: start address, leading byte offset
+// (between the two 16-byte K halves of an MMA K-step), stride byte offset (between
+// 8-row groups), version 1 (sm_100), layout type 0
+QBX_D uint64_t um_desc(unsigned saddr, unsigned lbo, unsigned sbo)
+{
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// offset (in 32-bit words) of element (row, k) of a [rows][UM_KC] operand chunk
+QBX_HD int um_off(int row, int k)
+{
+  return (((row >> 3) * (UM_KC / 4) + (k >> 2)) << 5) + ((row & 7) << 2) + (k & 3);
+}
+
+QBX_D void um_mma(unsigned tmem, uint64_t da, uint64_t db, unsigned idesc, int acc)
+{
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n}\n"
+      ::"r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+      : "memory");
+}
+
+QBX_D bool um_wait(uint64_t* mb, unsigned parity)
+{
+  const unsigned a = um_smem(mb);
+  for (int it = 0; it < (1 << 22); ++it) {
+    unsigned done;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                 " selp.u32 %0, 1, 0, p;\n}\n"
+                 : "=r"(done) : "r"(a), "r"(parity) : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+// FP64 matrices [nmat][rp][kp] -> TF32 hi / lo planes in the chunked core-matrix layout
+// [nmat][kp8 / 32 chunks][rp16 x 32] (zero padded)
+__global__ void k_trans_umma_planes(int nmat, int rp, int kp, int rp16, int nkc, int R,
+                                    const double* __restrict__ T, uint32_t* __restrict__ Uhi,
+                                    uint32_t* __restrict__ Ulo)
+{
+  const size_t per = (size_t)nkc * rp16 * UM_KC;
+  const size_t n = (size_t)nmat * per;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n;
+       e += (size_t)gridDim.x * blockDim.x) {
+    const size_t mat = e / per;
+    const int rem = (int)(e - mat * per);
+    const int kc = rem / (rp16 * UM_KC), w = rem - kc * (rp16 * UM_KC);
+    const int row = w / UM_KC, kk = w - row * UM_KC, k = kc * UM_KC + kk;
+    const float v = (row < R && k < R) ? (float)T[(mat * rp + row) * kp + k] : 0.0f;
+    const uint32_t hi = to_tf32(v);
+    const size_t o = mat * per + (size_t)kc * rp16 * UM_KC + um_off(row, kk);
+    Uhi[o] = hi;
+    Ulo[o] = to_tf32(v - __uint_as_float(hi));
+  }
+}
+
+__global__ void __launch_bounds__(UM_NT)
+k_trans_gemm_umma(int ncf, int rp, int rp16, int nkc, int nrhs, const uint32_t* __restrict__ Uhi,
+                  const uint32_t* __restrict__ Ulo, const int32_t* __restrict__ group_starts,
+                  const int32_t* __restrict__ pair_src, const double2* __restrict__ ein,
+                  double* __restrict__ cpair, int32_t* err, int nboxes)
+{
+  extern __shared__ __align__(1024) uint32_t smu[];
+  const int aw = UM_M * UM_KC, bw = rp16 * UM_KC;       // words per plane and stage
+  // stage s: A hi, A lo, B hi, B lo
+  auto Ah = [&](int st) { return smu + (size_t)st * 2 * (aw + bw); };
+  auto Al = [&](int st) { return Ah(st) + aw; };
+  auto Bh = [&](int st) { return Al(st) + aw; };
+  auto Bl = [&](int st) { return Bh(st) + bw; };
+  __shared__ uint64_t full[2], mdone[2];
+  __shared__ uint32_t s_tmem;
+  __shared__ int s_src[UM_M];
+  const int grp = blockIdx.y;
+  const int p0 = group_starts[grp], p1 = group_starts[grp + 1];
+  const int ncol = (p1 - p0) * nrhs;
+  const int c0 = blockIdx.x * UM_M;
+  if (c0 >= ncol) return;                               // uniform, before any allocation
+  const size_t mper = (size_t)nkc * bw;
+  const uint32_t* Th = Uhi + (size_t)grp * mper;
+  const uint32_t* Tl = Ulo + (size_t)grp * mper;
+  const int R = 2 * ncf;
+  const int warp = threadIdx.x >> 5;
+  if (threadIdx.x < UM_M) {
+    const int c = c0 + threadIdx.x;
+    int src = -1;
+    if (c < ncol) {
+      src = pair_src[p0 + c / nrhs];
+      if ((unsigned)src >= (unsigned)nboxes) {
+        report(err, QBX_DEVERR_BAD_BOX);
+        src = -1;
+      }
+    }
+    s_src[threadIdx.x] = src;
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n"
+                 ::"r"(um_smem(&s_tmem)), "r"(UM_TCOLS) : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+  }
+  if (threadIdx.x == 0) {
+    for (int b = 0; b < 2; ++b) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(um_smem(&full[b])) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(um_smem(&mdone[b])) : "memory");
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  const unsigned tmem = s_tmem;
+  // kind::tf32: D F32 (bit 4), A and B TF32 (bits 7, 10), both K-major, N >> 3 at bit
+  // 17, M >> 4 at bit 24
+  const unsigned idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((unsigned)(rp16 >> 3) << 17) |
+                         ((unsigned)(UM_M >> 4) << 24);
+  const unsigned LBO = 128, SBO = (UM_KC / 4) * 128;
+  const unsigned bbytes = (unsigned)bw * sizeof(uint32_t);
+  // this thread's part of A: column row, K half khalf
+  const int row = threadIdx.x & (UM_M - 1), khalf = threadIdx.x / UM_M;
+  const int src = s_src[row];
+  const double* xin = src >= 0
+      ? reinterpret_cast<const double*>(ein + ((size_t)src * nrhs + (c0 + row) % nrhs) * ncf)
+      : nullptr;
+  // issued / completed counts per barrier (the same in every thread)
+  int f_iss[2] = {0, 0}, f_done[2] = {0, 0}, m_iss[2] = {0, 0}, m_done[2] = {0, 0};
+  auto fill = [&](int kc, int st) {
+    if (threadIdx.x == 0) {
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n"
+                   ::"r"(um_smem(&full[st])), "r"(2 * bbytes) : "memory");
+      const uint32_t* gh = Th + (size_t)kc * bw;
+      const uint32_t* gl = Tl + (size_t)kc * bw;
+      asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n"
+                   ::"r"(um_smem(Bh(st))), "l"(gh), "r"(bbytes), "r"(um_smem(&full[st])) : "memory");
+      asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n"
+                   ::"r"(um_smem(Bl(st))), "l"(gl), "r"(bbytes), "r"(um_smem(&full[st])) : "memory");
+    }
+    ++f_iss[st];
+    uint32_t* ah = Ah(st);
+    uint32_t* al = Al(st);
+#pragma unroll 4
+    for (int j = 0; j < UM_KC / 2; ++j) {
+      const int k = khalf * (UM_KC / 2) + j, kg = kc * UM_KC + k;
+      float v = 0.0f;
+      if (xin && kg < R) v = (float)__ldg(xin + kg);
+      const uint32_t hi = to_tf32(v);
+      ah[um_off(row, k)] = hi;
+      al[um_off(row, k)] = to_tf32(v - __uint_as_float(hi));
+    }
+  };
+  bool fail = false;
+  fill(0, 0);
+  for (int kc = 0; kc < nkc; ++kc) {
+    const int st = kc & 1;
+    // chunk kc: its B copies have landed, its A is written (made visible to the
+    // tensor core through the proxy fence and the barrier)
+    if (!um_wait(&full[st], f_done[st] & 1)) fail = true;
+    else ++f_done[st];
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    if (__syncthreads_or(fail)) break;
+    if (threadIdx.x == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+      const unsigned sAh = um_smem(Ah(st)), sAl = um_smem(Al(st));
+      const unsigned sBh = um_smem(Bh(st)), sBl = um_smem(Bl(st));
+      for (int s = 0; s < UM_KC / 8; ++s) {
+        const unsigned off = (unsigned)s * 2 * 128;   // two 16-byte K halves per K-step
+        const uint64_t dAh = um_desc(sAh + off, LBO, SBO), dAl = um_desc(sAl + off, LBO, SBO);
+        const uint64_t dBh = um_desc(sBh + off, LBO, SBO), dBl = um_desc(sBl + off, LBO, SBO);
+        const int first = (kc == 0 && s == 0);
+        um_mma(tmem, dAl, dBh, idesc, !first);
+        um_mma(tmem, dAh, dBl, idesc, 1);
+        um_mma(tmem, dAh, dBh, idesc, 1);
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n"
+                   ::"r"(um_smem(&mdone[st])) : "memory");
+    }
+    ++m_iss[st];
+    if (kc + 1 < nkc) {
+      // the other stage is free once the MMAs of chunk kc - 1 have read it
+      const int so = st ^ 1;
+      if (m_iss[so] > m_done[so]) {
+        if (!um_wait(&mdone[so], m_done[so] & 1)) fail = true;
+        else ++m_done[so];
+      }
+      if (__syncthreads_or(fail)) break;
+      fill(kc + 1, so);
+    }
+  }
+  // the last chunk's MMAs complete the accumulator
+  if (!fail) {
+    const int sl = (nkc - 1) & 1;
+    if (m_iss[sl] > m_done[sl]) {
+      if (!um_wait(&mdone[sl], m_done[sl] & 1)) fail = true;
+      else ++m_done[sl];
+    }
+  }
+  if (__syncthreads_or(fail)) {
+    // drain (bounded) whatever is still in flight before the tensor memory goes
+    if (threadIdx.x == 0) report(err, QBX_DEVERR_COPY_TIMEOUT);
+    for (int b = 0; b < 2; ++b) {
+      for (; f_done[b] < f_iss[b]; ++f_done[b]) um_wait(&full[b], f_done[b] & 1);
+      for (; m_done[b] < m_iss[b]; ++m_done[b]) um_wait(&mdone[b], m_done[b] & 1);
+    }
+  } else {
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const int lane_base = 32 * (warp & 3), c = c0 + lane_base + (threadIdx.x & 31);
+    double* y = (c < ncol) ? cpair + ((size_t)(p0 + c / nrhs) * nrhs + c % nrhs) * rp : nullptr;
+    for (int nb = 16 * (warp >> 2); nb < rp16; nb += 32) {
+      uint32_t v[16];
+      const unsigned ta = tmem + ((unsigned)lane_base << 16) + (unsigned)nb;
+      asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, "
+                   "%9, %10, %11, %12, %13, %14, %15}, [%16];\n"
+                   : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
+                     "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]),
+                     "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+                   : "r"(ta));
+      asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+      if (y) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j)
+          if (nb + j < R) y[nb + j] = (double)__uint_as_float(v[j]);
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n"
+                 ::"r"(tmem), "r"(UM_TCOLS) : "memory");
+  }
+}
+
+// }}}
+
 // {{{ launchers
 
 cudaError_t launch_p2m_mixed(const qbxfmm_geometry& g, SourceCoeffs sc, int p, int nrhs,
@@ -690,11 +950,18 @@ bool tf32_supported(const TransCfg& c)
   return rp16 / 16 <= X3_MT;
 }
 
+static size_t umma_plane_words(const TransCfg& c);
+static bool umma_shape_ok(const TransCfg& c);
+static void umma_dims(const TransCfg& c, int& rp16, int& nkc);
+
+// the mma.sync planes [nmat][rp16][kp8] (hi, lo), then for the tcgen05 form the
+// chunked core-matrix planes (hi, lo)
 size_t tf32_matrix_bytes(const TransCfg& c)
 {
   int rp16, kp8;
   tf32_dims(c, rp16, kp8);
-  return 2 * c.nmatrices * (size_t)rp16 * kp8 * sizeof(uint32_t);
+  return (2 * c.nmatrices * (size_t)rp16 * kp8 + (umma_shape_ok(c) ? 2 * umma_plane_words(c) : 0)) *
+         sizeof(uint32_t);
 }
 
 cudaError_t launch_trans_split_tf32(const TransCfg& c, const double* T, uint32_t* T32,
@@ -706,6 +973,14 @@ cudaError_t launch_trans_split_tf32(const TransCfg& c, const double* T, uint32_t
   int blocks = (int)std::min<size_t>((n + 255) / 256, 148 * 16);
   k_trans_split_tf32<<<blocks, 256, 0, st>>>((int)c.nmatrices, c.rp, c.kp, rp16, kp8, 2 * c.ncf, T,
                                              T32, T32 + n);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess || !umma_shape_ok(c)) return e;
+  int nkc;
+  umma_dims(c, rp16, nkc);
+  const size_t nu = umma_plane_words(c);
+  blocks = (int)std::min<size_t>((nu + 255) / 256, 148 * 16);
+  k_trans_umma_planes<<<blocks, 256, 0, st>>>((int)c.nmatrices, c.rp, c.kp, rp16, nkc, 2 * c.ncf, T,
+                                              T32 + 2 * n, T32 + 2 * n + nu);
   return cudaGetLastError();
 }
 
@@ -729,14 +1004,63 @@ static cudaError_t x3_launch(const qbxfmm_geometry& g, const TransCfg& c, int nr
   return cudaGetLastError();
 }
 
+// the tcgen05 form for matrices of at most 256 rows (one MMA N), else the mma.sync one
+static void umma_dims(const TransCfg& c, int& rp16, int& nkc)
+{
+  int kp8;
+  tf32_dims(c, rp16, kp8);
+  nkc = (kp8 + UM_KC - 1) / UM_KC;
+}
+
+static bool umma_shape_ok(const TransCfg& c)
+{
+  int rp16, nkc;
+  umma_dims(c, rp16, nkc);
+  return rp16 % 16 == 0 && rp16 >= 16 && rp16 <= UM_TCOLS;
+}
+
+static size_t umma_plane_words(const TransCfg& c)
+{
+  int rp16, nkc;
+  umma_dims(c, rp16, nkc);
+  return c.nmatrices * (size_t)nkc * rp16 * UM_KC;
+}
+
+static cudaError_t umma_launch(const qbxfmm_geometry& g, const TransCfg& c, int nrhs,
+                               const uint32_t* U, int ngroups, int maxcols,
+                               const int32_t* group_starts, const int32_t* pair_src,
+                               const double2* ein, double* cpair, int32_t* err, cudaStream_t st)
+{
+  if (ngroups <= 0 || maxcols <= 0) return cudaSuccess;
+  int rp16, nkc;
+  umma_dims(c, rp16, nkc);
+  const size_t sh = 2 * (2 * (size_t)UM_M + 2 * (size_t)rp16) * UM_KC * sizeof(uint32_t);
+  cudaError_t e = cudaFuncSetAttribute(k_trans_gemm_umma,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+  if (e != cudaSuccess) return e;
+  dim3 grid((maxcols + UM_M - 1) / UM_M, ngroups);
+  k_trans_gemm_umma<<<grid, UM_NT, sh, st>>>(c.ncf, c.rp, rp16, nkc, nrhs, U,
+                                             U + umma_plane_words(c), group_starts, pair_src, ein,
+                                             cpair, err, g.nboxes);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_m2l_gemm_mixed(const qbxfmm_geometry& g, const TransHost& th, const TransCfg& c,
                                   int nrhs, const uint32_t* T32, const double2* mp, double2* lo,
                                   double* cpair, int32_t* err, cudaStream_t st)
 {
   if (g.m2l_nclasses == 0) return cudaSuccess;
-  cudaError_t e = x3_launch(g, c, nrhs, T32, 0, 0, g.m2l_class_starts, 0, g.m2l_nclasses,
-                            th.m2l_max_pairs * nrhs, g.m2l_pair_src, nullptr, mp, nullptr, 1.0,
-                            cpair, err, st);
+  int rp16, kp8;
+  tf32_dims(c, rp16, kp8);
+  const uint32_t* U = T32 + 2 * c.nmatrices * (size_t)rp16 * kp8;   // after the mma.sync planes
+  // (bulk copies need 16-byte aligned planes)
+  const bool umma = umma_shape_ok(c) && (reinterpret_cast<uintptr_t>(U) & 15) == 0;
+  cudaError_t e = umma
+      ? umma_launch(g, c, nrhs, U, g.m2l_nclasses, th.m2l_max_pairs * nrhs, g.m2l_class_starts,
+                    g.m2l_pair_src, mp, cpair, err, st)
+      : x3_launch(g, c, nrhs, T32, 0, 0, g.m2l_class_starts, 0, g.m2l_nclasses,
+                  th.m2l_max_pairs * nrhs, g.m2l_pair_src, nullptr, mp, nullptr, 1.0, cpair, err,
+                  st);
   if (e != cudaSuccess) return e;
   return launch_trans_reduce_m2l(g, c, nrhs, cpair, lo, st);
 }
