@@ -4,8 +4,9 @@
 // (each kernel loads FP64, computes in FP32, accumulates its result back into the
 // FP64 array): P2M, P2L and M2QBXL on the FP32 pipe, and the matrix-form
 // translations (M2M, M2L, L2L) on the tensor cores as split-TF32 products
-// (a = a_hi + a_lo in TF32, a b ~ a_hi b_hi + a_hi b_lo + a_lo b_hi, FP32 accumulation:
-// mma.sync m16n8k8 tf32).  The QBX near field (P2QBXL / target-specific, QBXL2P), the
+// (a = a_hi + a_lo in TF32, a b ~ a_hi b_hi + a_hi b_lo + a_lo b_hi, FP32 accumulation):
+// M2L on tcgen05 with the accumulator in tensor memory, the rest (and matrices of more
+// than 256 rows) with mma.sync m16n8k8 tf32.  The QBX near field (P2QBXL / target-specific, QBXL2P), the
 // non-QBX point evaluations and L2QBXL stay FP64.  Expansions, scalings and work
 // decomposition are those of the FP64 kernels in kernels_laplace.cu / kernels_trans.cu.
 #include <algorithm>
