@@ -26,6 +26,8 @@ def workload(name: str):
         return laplace3d_ellipsoid(nrefine=3, op="D")
     if name == "3d-D-small":
         return laplace3d_ellipsoid(nrefine=2, nshell=500, op="D")
+    if name == "3d-D-nrhs5":
+        return laplace3d_ellipsoid(nrefine=2, nshell=300, op="D", nrhs=5)
     if name == "3d-S-small":
         return laplace3d_ellipsoid(nrefine=2, nshell=500, op="S", qbx_order=4, fmm_order=8)
     if name == "2d-D-nrhs3":

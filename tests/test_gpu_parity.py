@@ -173,12 +173,12 @@ def test_target_specific_mode_matches_checker(name):
     assert relerr(host(drive_fmm(None, wt, [dev(flat)])), ref) < TOL
 
 
-@pytest.mark.parametrize("name", ["3d-D-small", "3d-S-small", "3d-D"])
+@pytest.mark.parametrize("name", ["3d-D-small", "3d-S-small", "3d-D", "3d-D-nrhs5"])
 def test_mixed_precision_apply_error(name):
-    """Mixed form (FP32 P2M/P2L/M2QBXL, split-TF32 M2M/M2L/L2L, FP64 QBX near field):
-    its error against the FP64 checker is stated and bounded (1e-6 relative,
-    max-norm); the near field alone stays FP64, so the target-specific variant has the
-    same bound."""
+    """Mixed form (FP32 P2M/P2L/M2QBXL, split-TF32 M2M/M2L/L2L -- M2L on tcgen05 with
+    columns of several densities in "3d-D-nrhs5" --, FP64 QBX near field): its error
+    against the FP64 checker is stated and bounded (1e-6 relative, max-norm); the near
+    field alone stays FP64, so the target-specific variant has the same bound."""
     from pytential_b200.fmm import PRECISION_MIXED
     wl = workload(name)
     o = oracle_for(wl)
