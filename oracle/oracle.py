@@ -37,7 +37,11 @@ def lib():
                      "orc_refine_locals", "orc_eval_locals", "orc_form_global_qbx_locals",
                      "orc_translate_box_multipoles_to_qbx_local",
                      "orc_translate_box_local_to_qbx_local", "orc_eval_qbx_expansions",
-                     "orc_assemble", "orc_apply", "orc_apply_direct"]:
+                     "orc_assemble", "orc_apply", "orc_apply_direct",
+                     "orc_transpose_eval_qbx_expansions",
+                     "orc_transpose_translate_box_local_to_qbx_local",
+                     "orc_transpose_translate_box_multipoles_to_qbx_local",
+                     "orc_transpose_form_global_qbx_locals"]:
             f = getattr(_LIB, name)
             f.restype = ctypes.c_int
         _LIB.orc_ncoeff.restype = ctypes.c_int
@@ -122,4 +126,52 @@ class Oracle:
         out = np.zeros((self.nrhs, self.scalars["nuser_targets"]), self.dtype)
         s = np.ascontiguousarray(tree_strengths, self.dtype)
         self._call("orc_apply_direct", _p(s), _p(out))
+        return out
+
+    def apply_transpose(self, user_target_values):
+        """The transpose of :meth:`apply` for the 3D Laplace single layer: values at
+        the user targets ``(nrhs, nuser_targets)`` -> values at the sources in tree
+        order ``(nrhs, nsources)``, so that ``sum(apply(s) * r) == sum(s *
+        apply_transpose(r))``.
+
+        The exchanged-role FMM over the same boxes with transposed lists
+        (``pytential_b200.transpose.TransposedGeometryData``): this checker's box
+        stages on that geometry, the QBX part by the transposed center stages of
+        ``qbxfmm_oracle.c`` (which scatter per center)."""
+        from pytential_b200.transpose import TransposedGeometryData
+        k = self.kern
+        if k.family != abi.QBXFMM_LAPLACE or k.dim != 3 or k.dipole_coeff_re != 0:
+            raise NotImplementedError("the transposed apply covers the 3D Laplace single layer")
+        if self.level_orders is not None:
+            raise NotImplementedError("the transposed apply takes one FMM order")
+        r = np.atleast_2d(np.asarray(user_target_values, np.float64))
+        sc, a = self.scalars, self.arrays
+        nt, nc = sc["ntargets"], sc["ncenters"]
+        sid = a["sorted_target_ids"][:nt].astype(np.int64)
+        r_tree = np.zeros((self.nrhs, nt))
+        user = sid >= nc
+        r_tree[:, user] = r[:, sid[user] - nc]
+        nf = sc["nfiltered_targets"]
+        s_dual = np.ascontiguousarray(
+            r_tree[:, a["unfiltered_from_filtered_target_indices"][:nf].astype(np.int64)])
+        d = Oracle(TransposedGeometryData(self.geo), dim=3, qbx_order=k.qbx_order,
+                   fmm_order=k.fmm_order, nrhs=self.nrhs, charge_coeff=k.charge_coeff_re,
+                   family=abi.QBXFMM_LAPLACE)
+        mp, lo = d.zeros_box_exps(), d.zeros_box_exps()
+        pot = d.zeros_nonqbx()
+        cm = self.zeros_qbx_exps()
+        d.stage("form_multipoles", s_dual, mp)
+        self.stage("transpose_eval_qbx_expansions", r_tree, cm)
+        self.stage("transpose_translate_box_local_to_qbx_local", cm, mp)
+        d.stage("coarsen_multipoles", mp)
+        d.stage("eval_direct", s_dual, pot)
+        d.stage("multipole_to_local", mp, lo)
+        d.stage("eval_multipoles", mp, pot)
+        d.stage("form_locals", s_dual, lo)
+        self.stage("transpose_translate_box_multipoles_to_qbx_local", cm, lo)
+        d.stage("refine_locals", lo)
+        d.stage("eval_locals", lo, pot)
+        self.stage("transpose_form_global_qbx_locals", cm, pot)
+        out = np.zeros((self.nrhs, d.scalars["nuser_targets"]))
+        d.stage("assemble", pot, d.zeros_tree_pot(), out)
         return out

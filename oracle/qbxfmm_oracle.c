@@ -1005,5 +1005,144 @@ int orc_apply_direct(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
 
 /* }}} */
 
+/* {{{ transposed QBX stages (3D Laplace single layer)
+ *
+ * The transposes of QBXL2P, L2QBXL, M2QBXL and P2QBXL (fmm.py:231-389) in the
+ * exchanged-role form: each global center carries the order-q multipole of its
+ * targets' values times the charge coefficient (P2M about the center, its expansion
+ * radius as rscale; the coefficient multiplies every path that starts there); it is
+ * shifted into the multipole of its target box (M2M from the center, the reciprocal
+ * of the box-to-center L2L), converted into the local of every box of the target
+ * box's list 3 (M2L from the center, the reciprocal of M2QBXL), and evaluated at
+ * the sources of every box of the target box's list 1 (M2P, the reciprocal of
+ * P2QBXL).  Each loop runs over the centers and scatters into boxes and sources,
+ * one thread. */
+
+static int transpose_ctx(const qbxfmm_kernel* kern, ctx_t* c)
+{
+  int rc = make_ctx(kern, c);
+  if (rc) return rc;
+  if (c->dim != 3 || c->cd != 0) return QBXFMM_ERR_UNSUPPORTED;
+  return 0;
+}
+
+/* tree_vals: [nrhs][ntargets] (tree target order); center_mpoles: [ncenters][nrhs][ncq] */
+int orc_transpose_eval_qbx_expansions(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
+                                      const double* tree_vals, cplx* center_mpoles)
+{
+  ctx_t c;
+  int rc = transpose_ctx(kern, &c);
+  if (rc) return rc;
+  cplx* work = malloc(sizeof(cplx) * work_size(c.pq));
+  double zero[3] = {0, 0, 0};
+  for (int ig = 0; ig < g->nglobal_qbx_centers; ++ig) {
+    int ctr = g->global_qbx_centers[ig];
+    double cc[3], x[3];
+    load(g->centers, g->ncenters, ctr, 3, cc);
+    double rho = g->expansion_radii[ctr];
+    for (int it = g->center_to_targets_starts[ctr]; it < g->center_to_targets_starts[ctr + 1];
+         ++it) {
+      int t = g->center_to_targets_lists[it];
+      load(g->targets, g->ntargets, t, 3, x);
+      for (int r = 0; r < c.nrhs; ++r)
+        lap3_p2m(c.pq, rho, cc, x, c.cq * tree_vals[(size_t)r * g->ntargets + t], 0, zero,
+                 center_mpoles + ((size_t)ctr * c.nrhs + r) * c.ncq, work);
+    }
+  }
+  free(work);
+  return 0;
+}
+
+int orc_transpose_translate_box_local_to_qbx_local(const qbxfmm_kernel* kern,
+                                                   const qbxfmm_geometry* g,
+                                                   const cplx* center_mpoles, cplx* mpoles)
+{
+  ctx_t c;
+  int rc = transpose_ctx(kern, &c);
+  if (rc) return rc;
+  cplx* work = malloc(sizeof(cplx) * work_size(c.pf));
+  cplx* pad = malloc(sizeof(cplx) * c.ncf);
+  for (int ig = 0; ig < g->nglobal_qbx_centers; ++ig) {
+    int ctr = g->global_qbx_centers[ig];
+    int tb = g->target_boxes[g->qbx_center_to_target_box[ctr]];
+    double cc[3], cb[3], d[3];
+    load(g->centers, g->ncenters, ctr, 3, cc);
+    load(g->box_centers, g->nboxes, tb, 3, cb);
+    double rho_b = level_width(g, g->box_levels[tb]);
+    double rho_c = g->expansion_radii[ctr];
+    for (int dd = 0; dd < 3; ++dd) d[dd] = (cc[dd] - cb[dd]) / rho_b;
+    for (int r = 0; r < c.nrhs; ++r) {
+      /* the center multipole zero-padded to the box order */
+      for (int i = 0; i < c.ncf; ++i) pad[i] = 0;
+      memcpy(pad, center_mpoles + ((size_t)ctr * c.nrhs + r) * c.ncq, sizeof(cplx) * c.ncq);
+      lap3_m2m(c.pf, rho_c, rho_b, d, pad, mpoles + ((size_t)tb * c.nrhs + r) * c.ncf, work);
+    }
+  }
+  free(pad);
+  free(work);
+  return 0;
+}
+
+int orc_transpose_translate_box_multipoles_to_qbx_local(const qbxfmm_kernel* kern,
+                                                        const qbxfmm_geometry* g,
+                                                        const cplx* center_mpoles, cplx* locals)
+{
+  ctx_t c;
+  int rc = transpose_ctx(kern, &c);
+  if (rc) return rc;
+  cplx* work = malloc(sizeof(cplx) * work_size(c.pf + c.pq));
+  for (int ig = 0; ig < g->nglobal_qbx_centers; ++ig) {
+    int ctr = g->global_qbx_centers[ig];
+    double cc[3], cs[3], d[3];
+    load(g->centers, g->ncenters, ctr, 3, cc);
+    double rho_c = g->expansion_radii[ctr];
+    int itb = g->qbx_center_to_target_box[ctr];
+    for (int li = g->list3_starts[itb]; li < g->list3_starts[itb + 1]; ++li) {
+      int sb = g->list3_lists[li];
+      double rho_s = level_width(g, g->box_levels[sb]);
+      load(g->box_centers, g->nboxes, sb, 3, cs);
+      for (int dd = 0; dd < 3; ++dd) d[dd] = (cs[dd] - cc[dd]) / rho_c;
+      for (int r = 0; r < c.nrhs; ++r)
+        lap3_m2l(c.pq, lp(&c, g->box_levels[sb]), rho_c, rho_s, d,
+                 center_mpoles + ((size_t)ctr * c.nrhs + r) * c.ncq,
+                 locals + ((size_t)sb * c.nrhs + r) * c.ncf, work);
+    }
+  }
+  free(work);
+  return 0;
+}
+
+/* source_vals: [nrhs][nsources] (tree source order), added to */
+int orc_transpose_form_global_qbx_locals(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
+                                         const cplx* center_mpoles, double* source_vals)
+{
+  ctx_t c;
+  int rc = transpose_ctx(kern, &c);
+  if (rc) return rc;
+  cplx* work = malloc(sizeof(cplx) * work_size(c.pq));
+  for (int ig = 0; ig < g->nglobal_qbx_centers; ++ig) {
+    int ctr = g->global_qbx_centers[ig];
+    double cc[3], y[3];
+    load(g->centers, g->ncenters, ctr, 3, cc);
+    double rho = g->expansion_radii[ctr];
+    int itb = g->qbx_center_to_target_box[ctr];
+    for (int li = g->list1_starts[itb]; li < g->list1_starts[itb + 1]; ++li) {
+      int sb = g->list1_lists[li];
+      int s0 = g->box_source_starts[sb], s1 = s0 + g->box_source_counts_nonchild[sb];
+      for (int s = s0; s < s1; ++s) {
+        load(g->sources, g->nsources, s, 3, y);
+        for (int r = 0; r < c.nrhs; ++r)
+          source_vals[(size_t)r * g->nsources + s] +=
+              lap3_m2p(c.pq, rho, cc, y, center_mpoles + ((size_t)ctr * c.nrhs + r) * c.ncq,
+                       work);
+      }
+    }
+  }
+  free(work);
+  return 0;
+}
+
+/* }}} */
+
 #include "qbxfmm_oracle_helm2d.c"
 #include "qbxfmm_oracle_helm3d.c"

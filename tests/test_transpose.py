@@ -1,0 +1,134 @@
+"""The transpose of the QBX-FMM apply (3D Laplace single layer) over the same tree:
+the exchanged-role geometry's lists are the transposed lists, and the checker's
+transposed apply (box stages on that geometry, QBX part by the transposed center
+stages) is the transpose of its apply -- dot products ``<A s, r> = <s, A^T r>`` to
+rounding, and on a small case the matrix itself, column by column.  The GPU part
+compares the library's transposed apply with the checker's."""
+
+import numpy as np
+import pytest
+
+from pytential_b200 import abi
+from pytential_b200.discretization import make_ellipsoid
+from pytential_b200.geometry import QBXFMMGeometryData
+from pytential_b200.transpose import TransposedGeometryData, transpose_index
+
+from helpers import relerr
+
+
+def _geometry(nrefine, near=0, shell=0, leaf=None, seed=0):
+    """Ellipsoid with on-surface QBX targets, ``near`` exterior points at a tenth of
+    the element size from the surface (QBX targets off the surface) and ``shell``
+    far points."""
+    rng = np.random.default_rng(seed)
+    d = make_ellipsoid(nrefine)
+    tg = [(d.nodes, +1)]
+    if near:
+        i = rng.integers(0, d.ndofs, near)
+        h = 0.1 * d.element_stretch[i // d.nodes_per_element]
+        tg.append((d.nodes[:, i] + h * d.normals[:, i], +1))
+    if shell:
+        v = rng.normal(size=(3, shell))
+        v *= rng.uniform(2.5, 3.5, shell) / np.linalg.norm(v, axis=0)
+        tg.append((v, 0))
+    kw = {} if leaf is None else {"max_leaf_refine_weight": leaf}
+    return QBXFMMGeometryData(d, tg, **kw)
+
+
+def _oracle(geo, nrhs, qbx_order=3, fmm_order=10):
+    from oracle.oracle import Oracle
+    return Oracle(geo, dim=3, qbx_order=qbx_order, fmm_order=fmm_order, nrhs=nrhs,
+                  charge_coeff=1.0, family=abi.QBXFMM_LAPLACE)
+
+
+CASES = {
+    "surface+shell": dict(nrefine=1, shell=300),
+    "near+deep": dict(nrefine=1, near=400, shell=100, leaf=64),
+    "near-only": dict(nrefine=2, near=300, leaf=128),
+}
+
+
+@pytest.fixture(scope="module", params=list(CASES))
+def case(request):
+    return request.param, _geometry(**CASES[request.param])
+
+
+def _csr_pairs(starts, lists, rows):
+    starts = np.asarray(starts)
+    return set(zip(np.repeat(np.asarray(rows), np.diff(starts)).tolist(),
+                   np.asarray(lists).tolist()))
+
+
+def test_transposed_lists(case):
+    _, geo = case
+    t = geo.traversal()
+    d = TransposedGeometryData(geo).traversal()
+    tb, ttp = t.target_boxes, t.target_or_target_parent_boxes
+    dtb, dttp = d.target_boxes, d.target_or_target_parent_boxes
+    flip = lambda pairs: {(b, a) for a, b in pairs}   # noqa: E731
+    assert _csr_pairs(d.neighbor_source_boxes_starts, d.neighbor_source_boxes_lists, dtb) == \
+        flip(_csr_pairs(t.neighbor_source_boxes_starts, t.neighbor_source_boxes_lists, tb))
+    assert _csr_pairs(d.from_sep_siblings_starts, d.from_sep_siblings_lists, dttp) == \
+        flip(_csr_pairs(t.from_sep_siblings_starts, t.from_sep_siblings_lists, ttp))
+    assert _csr_pairs(d.from_sep_smaller_starts, d.from_sep_smaller_lists, dtb) == \
+        flip(_csr_pairs(t.from_sep_bigger_starts, t.from_sep_bigger_lists, ttp))
+    assert _csr_pairs(d.from_sep_bigger_starts, d.from_sep_bigger_lists, dttp) == \
+        flip(_csr_pairs(t.from_sep_smaller_starts, t.from_sep_smaller_lists, tb))
+    # every list is non-trivial in at least the deeper cases
+    assert len(t.neighbor_source_boxes_lists) and len(t.from_sep_siblings_lists)
+
+
+def test_transpose_index(case):
+    _, geo = case
+    ix = transpose_index(geo)
+    t = geo.traversal()
+    gc = np.asarray(geo.global_qbx_centers())
+    cbox = np.asarray(t.target_boxes)[np.asarray(geo.qbx_center_to_target_box())[gc]]
+    assert sorted(ix.box_centers.tolist()) == sorted(gc.tolist())
+    for b in ix.center_boxes:
+        got = ix.box_centers[ix.box_center_starts[b]:ix.box_center_starts[b + 1]]
+        assert set(got.tolist()) == set(gc[cbox == b].tolist())
+    has_c = set(ix.center_boxes.tolist())
+    tb_of = {int(b): i for i, b in enumerate(t.target_boxes)}
+    for rows, st, li, (s0, l0) in (
+            (ix.list3_rows, ix.list3_rev_starts, ix.list3_rev_lists,
+             (t.from_sep_smaller_starts, t.from_sep_smaller_lists)),
+            (ix.list1_rows, ix.list1_rev_starts, ix.list1_rev_lists,
+             (t.neighbor_source_boxes_starts, t.neighbor_source_boxes_lists))):
+        want = {(int(s), int(b)) for b in has_c
+                for s in l0[s0[tb_of[b]]:s0[tb_of[b] + 1]]}
+        assert _csr_pairs(st, li, rows) == want
+
+
+def test_checker_transpose_dot_products(case):
+    _, geo = case
+    o = _oracle(geo, nrhs=3)
+    rng = np.random.default_rng(1)
+    s = rng.normal(size=(3, o.scalars["nsources"]))
+    r = rng.normal(size=(3, o.scalars["nuser_targets"]))
+    As = o.apply(s)
+    ATr = o.apply_transpose(r)
+    lhs, rhs = (As * r).sum(1), (s * ATr).sum(1)
+    scale = np.linalg.norm(As, axis=1) * np.linalg.norm(r, axis=1)
+    assert (np.abs(lhs - rhs) <= 1e-13 * scale).all()
+
+
+def test_checker_transpose_is_the_matrix_transpose():
+    """Every column of A^T (A^T applied to each unit vector) against the rows of A
+    (A applied to every unit vector) on the 20-triangle ellipsoid with far and near
+    targets."""
+    geo = _geometry(0, near=30, shell=20)
+    o1 = _oracle(geo, nrhs=1)
+    ns, nu = o1.scalars["nsources"], o1.scalars["nuser_targets"]
+    A = _oracle(geo, nrhs=ns).apply(np.eye(ns)).T                      # (nu, ns)
+    AT = _oracle(geo, nrhs=nu).apply_transpose(np.eye(nu))              # (nu, ns)
+    assert relerr(AT, A) < 1e-13
+
+
+def test_transposed_apply_needs_the_single_layer():
+    from oracle.oracle import Oracle
+    geo = _geometry(0, shell=10)
+    o = Oracle(geo, dim=3, qbx_order=3, fmm_order=8, dipole_coeff=1.0,
+               family=abi.QBXFMM_LAPLACE)
+    with pytest.raises(NotImplementedError):
+        o.apply_transpose(np.zeros((1, o.scalars["nuser_targets"])))
