@@ -210,6 +210,24 @@ typedef struct qbxfmm_workspace {
   void* pair_scratch; /* per-pair translation results, reduced per output box */
 } qbxfmm_workspace;
 
+/* Reversed QBX lists for the transposed apply (qbxfmm_transpose_*), by box id, in
+ * device memory; built on the host from the apply's geometry (every row's entries in
+ * increasing box order). */
+typedef struct qbxfmm_transpose_index {
+  int32_t ncenter_boxes;
+  const int32_t* center_boxes;       /* boxes holding global QBX centers (as target boxes) */
+  const int32_t* box_center_starts;  /* [nboxes + 1] into box_centers */
+  const int32_t* box_centers;        /* [nglobal_qbx_centers] grouped by box */
+  int32_t nlist3_rows;
+  const int32_t* list3_rows;         /* boxes in the list 3 of some center box */
+  const int32_t* list3_rev_starts;   /* [nlist3_rows + 1] */
+  const int32_t* list3_rev_lists;    /* the center boxes whose list 3 holds the row box */
+  int32_t nlist1_rows;
+  const int32_t* list1_rows;         /* source boxes in the list 1 of some center box */
+  const int32_t* list1_rev_starts;   /* [nlist1_rows + 1] */
+  const int32_t* list1_rev_lists;    /* the center boxes whose list 1 holds the row box */
+} qbxfmm_transpose_index;
+
 #ifdef __cplusplus
 }
 #endif

@@ -132,6 +132,46 @@ int qbxfmm_eval_qbx_expansions(const qbxfmm_plan* plan, const void* qbx_exps, vo
 int qbxfmm_eval_target_specific_qbx_locals(const qbxfmm_plan* plan, const void* strengths,
                                            void* pot_tree, int32_t* error_word, void* stream);
 
+/* {{{ transposed QBX stages (3D Laplace single layer, FP64, one FMM order)
+ *
+ * The transpose of the apply is the FMM with sources and targets exchanged over
+ * the same boxes with transposed lists (the stage entries above on that geometry),
+ * in which each global QBX center is a source carrying the order-q multipole of its
+ * targets' values.  These four entries are that part, each the transpose of one QBX
+ * stage of the apply; `plan` is the APPLY's plan (its centers, lists and sources),
+ * `index` its reversed lists.  center_mpoles: [ncenters][nrhs][ncoeff(qbx_order)]
+ * complex128.  Each output has one writer (no atomics).  QBXFMM_ERR_UNSUPPORTED for
+ * other kernels, the mixed-precision form, per-level orders, qbx_order > 14 or
+ * fmm_order > 21. */
+
+/* transpose of eval_qbx_expansions (fmm.py:358-389): target_values [nrhs][ntargets]
+ * in tree target order -> center_mpoles (written; zero for centers without targets) */
+int qbxfmm_transpose_eval_qbx_expansions(const qbxfmm_plan* plan, const void* target_values,
+                                         void* center_mpoles, int32_t* error_word,
+                                         void* stream);
+/* transpose of translate_box_local_to_qbx_local (fmm.py:314-356): adds each center
+ * multipole, shifted to its box center, into mpoles [nboxes][nrhs][ncoeff] */
+int qbxfmm_transpose_translate_box_local_to_qbx_local(const qbxfmm_plan* plan,
+                                                      const qbxfmm_transpose_index* index,
+                                                      const void* center_mpoles, void* mpoles,
+                                                      int32_t* error_word, void* stream);
+/* transpose of translate_box_multipoles_to_qbx_local (fmm.py:267-312): adds the M2L
+ * of each center multipole into the locals of the boxes in its box's list 3 */
+int qbxfmm_transpose_translate_box_multipoles_to_qbx_local(const qbxfmm_plan* plan,
+                                                           const qbxfmm_transpose_index* index,
+                                                           const void* center_mpoles,
+                                                           void* locals, int32_t* error_word,
+                                                           void* stream);
+/* transpose of form_global_qbx_locals (fmm.py:231-265): adds each center multipole,
+ * evaluated at the sources of the boxes in its box's list 1, into
+ * source_values [nrhs][nsources] (tree source order) */
+int qbxfmm_transpose_form_global_qbx_locals(const qbxfmm_plan* plan,
+                                            const qbxfmm_transpose_index* index,
+                                            const void* center_mpoles, void* source_values,
+                                            int32_t* error_word, void* stream);
+
+/* }}} */
+
 /* potential assembly: scatter the non-QBX part, add the QBX part, reorder to user
  * targets, apply the kernel scaling (pytential/qbx/fmm.py:569-588,
  * pytential/qbx/__init__.py:775-793).  out: [nrhs][nuser_targets] (written). */

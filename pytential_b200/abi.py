@@ -124,6 +124,13 @@ class QBXFMMAssocProblem(ctypes.Structure):
                 ("center_order", ctypes.c_void_p), ("center_grid", QBXFMMCellGrid)]
 
 
+class QBXFMMTransposeIndex(ctypes.Structure):
+    _fields_ = [("ncenter_boxes", _i32), ("center_boxes", _pi), ("box_center_starts", _pi),
+                ("box_centers", _pi), ("nlist3_rows", _i32), ("list3_rows", _pi),
+                ("list3_rev_starts", _pi), ("list3_rev_lists", _pi), ("nlist1_rows", _i32),
+                ("list1_rows", _pi), ("list1_rev_starts", _pi), ("list1_rev_lists", _pi)]
+
+
 class QBXFMMWorkspace(ctypes.Structure):
     _fields_ = [("strengths", ctypes.c_void_p), ("mpoles", ctypes.c_void_p),
                 ("locals", ctypes.c_void_p), ("qbx_exps", ctypes.c_void_p),

@@ -1266,6 +1266,79 @@ int qbxfmm_apply(const qbxfmm_plan* p, const qbxfmm_upsample* up, const qbxfmm_w
   return qbxfmm_assemble(p, ws->pot_nonqbx, ws->pot_tree, out, stream);
 }
 
+// {{{ transposed QBX stages
+
+namespace {
+
+int transpose_ok(const qbxfmm_plan* p)
+{
+  if (int rc = check_plan(p)) return rc;
+  if (p->helm || p->kern.dim != 3 || p->sc.cd != 0.0)
+    return fail(QBXFMM_ERR_UNSUPPORTED, "the transposed apply covers the 3D Laplace single layer");
+  if (p->mixed || level_orders_on(p))
+    return fail(QBXFMM_ERR_UNSUPPORTED,
+                "the transposed apply runs in FP64 with one FMM order");
+  if (p->kern.qbx_order > 14 || p->kern.fmm_order > 21)
+    return fail(QBXFMM_ERR_UNSUPPORTED, "the transposed apply takes qbx_order <= 14, fmm_order <= 21");
+  return QBXFMM_OK;
+}
+
+}  // namespace
+
+int qbxfmm_transpose_eval_qbx_expansions(const qbxfmm_plan* p, const void* target_values,
+                                         void* center_mpoles, int32_t* err, void* stream)
+{
+  if (int rc = transpose_ok(p)) return rc;
+  if (!target_values || !center_mpoles) return fail(QBXFMM_ERR_ARG, "null argument");
+  size_t bytes = (size_t)p->geo.ncenters * p->kern.nrhs * p->ncq * 2 * sizeof(double);
+  if (bytes) QBX_TRY(cudaMemsetAsync(center_mpoles, 0, bytes, S(stream)), "transpose: clear");
+  QBX_TRY(launch_tr_qbxl2p(p->geo, p->kern.qbx_order, p->kern.nrhs, p->sc.cq,
+                           (const double*)target_values, (double2*)center_mpoles, err, S(stream)),
+          "transpose_eval_qbx_expansions");
+  return QBXFMM_OK;
+}
+
+int qbxfmm_transpose_translate_box_local_to_qbx_local(const qbxfmm_plan* p,
+                                                      const qbxfmm_transpose_index* ix,
+                                                      const void* center_mpoles, void* mpoles,
+                                                      int32_t* err, void* stream)
+{
+  if (int rc = transpose_ok(p)) return rc;
+  if (!ix || !center_mpoles || !mpoles) return fail(QBXFMM_ERR_ARG, "null argument");
+  QBX_TRY(launch_tr_l2qbxl(p->geo, *ix, p->kern.fmm_order, p->kern.qbx_order, p->kern.nrhs,
+                           (const double2*)center_mpoles, (double2*)mpoles, err, S(stream)),
+          "transpose_translate_box_local_to_qbx_local");
+  return QBXFMM_OK;
+}
+
+int qbxfmm_transpose_translate_box_multipoles_to_qbx_local(const qbxfmm_plan* p,
+                                                           const qbxfmm_transpose_index* ix,
+                                                           const void* center_mpoles,
+                                                           void* locals, int32_t* err,
+                                                           void* stream)
+{
+  if (int rc = transpose_ok(p)) return rc;
+  if (!ix || !center_mpoles || !locals) return fail(QBXFMM_ERR_ARG, "null argument");
+  QBX_TRY(launch_tr_m2qbxl(p->geo, *ix, p->kern.fmm_order, p->kern.qbx_order, p->kern.nrhs,
+                           (const double2*)center_mpoles, (double2*)locals, err, S(stream)),
+          "transpose_translate_box_multipoles_to_qbx_local");
+  return QBXFMM_OK;
+}
+
+int qbxfmm_transpose_form_global_qbx_locals(const qbxfmm_plan* p, const qbxfmm_transpose_index* ix,
+                                            const void* center_mpoles, void* source_values,
+                                            int32_t* err, void* stream)
+{
+  if (int rc = transpose_ok(p)) return rc;
+  if (!ix || !center_mpoles || !source_values) return fail(QBXFMM_ERR_ARG, "null argument");
+  QBX_TRY(launch_tr_p2qbxl(p->geo, *ix, p->kern.qbx_order, p->kern.nrhs,
+                           (const double2*)center_mpoles, (double*)source_values, err, S(stream)),
+          "transpose_form_global_qbx_locals");
+  return QBXFMM_OK;
+}
+
+// }}}
+
 int qbxfmm_apply_host(const qbxfmm_plan* p, const qbxfmm_upsample* up, const qbxfmm_workspace* ws,
                       const void* density_host, void* out_host, void* density_dev, void* out_dev,
                       void* stream)

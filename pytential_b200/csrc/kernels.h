@@ -186,6 +186,19 @@ cudaError_t h3_launch_assemble(const qbxfmm_geometry& g, int nrhs, const double2
 cudaError_t h3_launch_trans_build(const qbxfmm_geometry& g, const TransCfg& tc, double k,
                                   const double* gaunt, double* T, cudaStream_t st);
 
+// transposed QBX stages (kernels_transpose.cu)
+cudaError_t launch_tr_qbxl2p(const qbxfmm_geometry& g, int q, int nrhs, double cq,
+                             const double* vals, double2* cmp, int32_t* err, cudaStream_t st);
+cudaError_t launch_tr_l2qbxl(const qbxfmm_geometry& g, const qbxfmm_transpose_index& ix, int p,
+                             int q, int nrhs, const double2* cmp, double2* mpoles, int32_t* err,
+                             cudaStream_t st);
+cudaError_t launch_tr_m2qbxl(const qbxfmm_geometry& g, const qbxfmm_transpose_index& ix, int p,
+                             int q, int nrhs, const double2* cmp, double2* locals, int32_t* err,
+                             cudaStream_t st);
+cudaError_t launch_tr_p2qbxl(const qbxfmm_geometry& g, const qbxfmm_transpose_index& ix, int q,
+                             int nrhs, const double2* cmp, double* vals, int32_t* err,
+                             cudaStream_t st);
+
 // per-level FMM orders: zero the coefficients of boxes [b0, b1) above their level's order
 cudaError_t launch_level_mask(const qbxfmm_geometry& g, int b0, int b1, const int32_t* orders,
                               int family, int ncf, int nrhs, double2* exps, cudaStream_t st);

@@ -46,6 +46,13 @@ _STAGES = {
                           ctypes.POINTER(abi.QBXFMMWorkspace), _vp, _vp, _vp, _vp, _vp],
     "qbxfmm_plan_set_tuning": [ctypes.POINTER(abi.QBXFMMTuning)],
     "qbxfmm_plan_get_tuning": [ctypes.POINTER(abi.QBXFMMTuning)],
+    "qbxfmm_transpose_eval_qbx_expansions": [_vp, _vp, _pi, _vp],
+    "qbxfmm_transpose_translate_box_local_to_qbx_local":
+        [ctypes.POINTER(abi.QBXFMMTransposeIndex), _vp, _vp, _pi, _vp],
+    "qbxfmm_transpose_translate_box_multipoles_to_qbx_local":
+        [ctypes.POINTER(abi.QBXFMMTransposeIndex), _vp, _vp, _pi, _vp],
+    "qbxfmm_transpose_form_global_qbx_locals":
+        [ctypes.POINTER(abi.QBXFMMTransposeIndex), _vp, _vp, _pi, _vp],
     "qbxfmm_plan_set_level_orders": [_pi, _int],
     "qbxfmm_plan_get_level_orders": [_pi, _int],
 }

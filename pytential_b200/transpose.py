@@ -34,10 +34,12 @@ Pieces:
 
 from __future__ import annotations
 
+import ctypes
 from dataclasses import dataclass
 
 import numpy as np
 
+from . import abi
 from .geometry import CenterToTargetList, FilteredTargetLists, TargetInfo
 from .traversal import Traversal, _level_starts
 from .tree import Tree
@@ -248,3 +250,123 @@ def transpose_index(geo) -> TransposeIndex:
     l1r, l1s, l1l = rev(trav.neighbor_source_boxes_starts, trav.neighbor_source_boxes_lists)
     return TransposeIndex(center_boxes, box_center_starts.astype(np.int32), box_centers,
                           l3r, l3s, l3l, l1r, l1s, l1l)
+
+
+class QBXTransposeApply:
+    """The transpose of a 3D Laplace single-layer :class:`~pytential_b200.fmm.QBXApply`
+    (FP64, one FMM order) on its device: ``A^T r`` for values ``r`` at the apply's
+    user targets, ``(nrhs, nuser_targets) -> (nrhs, ndofs)``, with ``A = K W U``
+    (upsampling ``U``, weights ``W``, the QBX-FMM kernel matrix ``K``) and
+    ``A^T = U^T W K^T``.  ``K^T`` runs over the apply's own tree: the exchanged-role
+    geometry's box stages (the library's stage entries) and the four transposed QBX
+    stages (``qbxfmm_transpose_*`` on the apply's plan)."""
+
+    def __init__(self, apply):
+        import torch
+
+        from .fmm import (PRECISION_FP64, B200QBXExpansionWrangler,
+                          B200TreeIndependentDataForWrangler, _ptr)
+        plan = apply.plan
+        spec = plan.spec
+        if spec.kernel.family != abi.QBXFMM_LAPLACE or spec.kernel.dim != 3 \
+                or spec.dipole_coeff != 0:
+            raise NotImplementedError("the transposed apply covers the 3D Laplace single layer")
+        if plan.precision != PRECISION_FP64 or len(set(plan.get_level_orders())) > 1:
+            raise NotImplementedError("the transposed apply runs in FP64 with one FMM order")
+        self.fwd = apply
+        self.nrhs = apply.nrhs
+        self.device = apply.device
+        self.dual_geo = TransposedGeometryData(apply.geo)
+        self.dual = B200QBXExpansionWrangler(
+            B200TreeIndependentDataForWrangler(spec), self.dual_geo, np.float64,
+            plan.qbx_order, plan.fmm_order, nrhs=self.nrhs, device=self.device)
+        dev = self.device
+
+        def put(a):
+            a = np.ascontiguousarray(a, np.int32)
+            return torch.from_numpy(a if a.size else np.zeros(1, np.int32)).to(dev)
+
+        ix = transpose_index(apply.geo)
+        self._ix = {f: put(getattr(ix, f)) for f in ix.__dataclass_fields__}
+        P = abi._pi
+
+        def ptr(name):
+            return ctypes.cast(ctypes.c_void_p(_ptr(self._ix[name])), P)
+        self.index = abi.QBXFMMTransposeIndex(
+            len(ix.center_boxes), ptr("center_boxes"), ptr("box_center_starts"),
+            ptr("box_centers"), len(ix.list3_rows), ptr("list3_rows"), ptr("list3_rev_starts"),
+            ptr("list3_rev_lists"), len(ix.list1_rows), ptr("list1_rows"),
+            ptr("list1_rev_starts"), ptr("list1_rev_lists"))
+        sc = apply.dgeo.scalars
+        host = apply.dgeo.host_arrays
+        nt, nc = sc["ntargets"], sc["ncenters"]
+        sid = host["sorted_target_ids"][:nt].astype(np.int64)
+        tt = np.nonzero(sid >= nc)[0]
+        self._tree_t = torch.from_numpy(tt).to(dev)
+        self._user_t = torch.from_numpy(sid[tt] - nc).to(dev)
+        nf = sc["nfiltered_targets"]
+        self._filt = torch.from_numpy(
+            host["unfiltered_from_filtered_target_indices"][:nf].astype(np.int64)).to(dev)
+        self._usid = torch.from_numpy(
+            host["user_source_ids"][:sc["nsources"]].astype(np.int64)).to(dev)
+        self.ntargets_tree, self.ncenters = nt, nc
+        self.nsources = sc["nsources"]
+        self.nuser_targets = sc["nuser_targets"]
+        self.ncq = plan.ncq
+        self.error_word = torch.zeros(1, dtype=torch.int32, device=dev)
+
+    def _call(self, name, *args):
+        from .fmm import _stream_handle
+        err = ctypes.cast(ctypes.c_void_p(self.error_word.data_ptr()), abi._pi)
+        self.fwd.plan.call(name, *args, err, _stream_handle())
+
+    def kernel_transpose(self, r):
+        """``K^T r``: ``(nrhs, nuser_targets)`` -> ``(nrhs, nsources)`` in user source
+        order (the flat quad sources)."""
+        import torch
+        vp = ctypes.c_void_p
+        r = torch.as_tensor(r, dtype=torch.float64, device=self.device)
+        r = r.reshape(self.nrhs, self.nuser_targets)
+        W = self.dual
+        r_tree = torch.zeros(self.nrhs, self.ntargets_tree, dtype=torch.float64, device=self.device)
+        r_tree[:, self._tree_t] = r[:, self._user_t]
+        s_dual = r_tree[:, self._filt].contiguous()
+        if s_dual.shape[1] == 0:
+            s_dual = torch.zeros(self.nrhs, 1, dtype=torch.float64, device=self.device)
+        cm = torch.zeros(max(self.ncenters, 1), self.nrhs, self.ncq, dtype=torch.complex128,
+                         device=self.device)
+        ix = ctypes.byref(self.index)
+        mp = W.form_multipoles(None, None, None, [s_dual])
+        self._call("qbxfmm_transpose_eval_qbx_expansions", vp(r_tree.data_ptr()), vp(cm.data_ptr()))
+        self._call("qbxfmm_transpose_translate_box_local_to_qbx_local", ix, vp(cm.data_ptr()),
+                   vp(mp.data_ptr()))
+        W.coarsen_multipoles(None, None, None, mp)
+        pot = W.eval_direct(None, None, None, None, [s_dual])
+        lo = W.multipole_to_local(None, None, None, None, None, mp)
+        pot += W.eval_multipoles(None, None, None, mp)
+        lo += W.form_locals(None, None, None, None, None, [s_dual])
+        self._call("qbxfmm_transpose_translate_box_multipoles_to_qbx_local", ix,
+                   vp(cm.data_ptr()), vp(lo.data_ptr()))
+        W.refine_locals(None, None, None, lo)
+        pot += W.eval_locals(None, None, None, lo)
+        self._call("qbxfmm_transpose_form_global_qbx_locals", ix, vp(cm.data_ptr()),
+                   vp(pot.data_ptr()))
+        out_tree = W.assemble_potentials(pot, W.full_output_zeros())
+        out = torch.empty_like(out_tree)
+        out[:, self._usid] = out_tree
+        return out
+
+    def __call__(self, r):
+        """``A^T r``: ``(nrhs, nuser_targets)`` -> ``(nrhs, ndofs)``."""
+        up = self.fwd.up
+        d = self.fwd.geo.discr
+        v = self.kernel_transpose(r) * up.quad_weights
+        v = v.reshape(self.nrhs, d.nelements, d.quad_nodes_per_element) @ up.matrix
+        return v.reshape(self.nrhs, d.ndofs)
+
+    def check_error_word(self):
+        from . import native
+        for w in (int(self.error_word.item()), int(self.dual.error_word.item())):
+            if w:
+                raise native.QBXFMMError("transpose", abi.QBXFMM_ERR_DEVICE,
+                                         f"a kernel met an out-of-range index (code {w})")

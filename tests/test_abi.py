@@ -70,6 +70,23 @@ def test_struct_layout_matches_c(tmp_path):
     assert offs == [getattr(abi.QBXFMMGeometry, f).offset for f in fields]
 
 
+def test_transpose_index_struct_matches_c(tmp_path):
+    fields = [n for n, _ in abi.QBXFMMTransposeIndex._fields_]
+    prog = ['#include <stdio.h>', '#include <stddef.h>', '#include "qbxfmm.h"',
+            'int main(void) {', 'printf("%zu\\n", sizeof(qbxfmm_transpose_index));']
+    prog += [f'printf("%zu\\n", offsetof(qbxfmm_transpose_index, {f}));' for f in fields]
+    prog.append("return 0; }")
+    c = tmp_path / "tindex.c"
+    c.write_text("\n".join(prog))
+    exe = tmp_path / "tindex"
+    subprocess.run(["/usr/bin/gcc", "-I", os.path.join(ROOT, "include"), str(c), "-o", str(exe)],
+                   check=True)
+    out = list(map(int, subprocess.run([str(exe)], capture_output=True, text=True,
+                                       check=True).stdout.split()))
+    assert out[0] == ctypes.sizeof(abi.QBXFMMTransposeIndex)
+    assert out[1:] == [getattr(abi.QBXFMMTransposeIndex, f).offset for f in fields]
+
+
 def test_association_structs_match_c(tmp_path):
     fields = [n for n, _ in abi.QBXFMMAssocProblem._fields_]
     prog = ['#include <stdio.h>', '#include <stddef.h>', '#include "qbxfmm_api.h"',

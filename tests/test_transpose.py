@@ -132,3 +132,80 @@ def test_transposed_apply_needs_the_single_layer():
                family=abi.QBXFMM_LAPLACE)
     with pytest.raises(NotImplementedError):
         o.apply_transpose(np.zeros((1, o.scalars["nuser_targets"])))
+
+
+# {{{ GPU
+
+@pytest.mark.gpu
+def test_gpu_transpose_matches_checker(case):
+    import torch
+
+    from pytential_b200.fmm import LaplaceKernel, QBXApply, SourceKernelSpec
+    from pytential_b200.transpose import QBXTransposeApply
+    _, geo = case
+    spec = SourceKernelSpec(LaplaceKernel(3), charge_coeff=1.0)
+    ap = QBXApply(geo, spec, 3, 10, nrhs=2, target_specific_qbx=False)
+    tr = QBXTransposeApply(ap)
+    rng = np.random.default_rng(3)
+    r = rng.normal(size=(2, ap.nuser_targets))
+    got = tr.kernel_transpose(torch.from_numpy(r).cuda()).cpu().numpy()
+    tr.check_error_word()
+    o = _oracle(geo, nrhs=2)
+    ref = o.apply_transpose(r)[:, np.argsort(o.arrays["user_source_ids"][:o.scalars["nsources"]])]
+    assert relerr(got, ref) < 1e-12
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("tsqbx", [False, True])
+def test_gpu_transpose_dot_products(case, tsqbx):
+    """<A sigma, r> = <sigma, A^T r> with the GPU apply (stage-1 densities, upsampling
+    and weights included); with the target-specific near field the apply is the same
+    matrix up to rounding."""
+    import torch
+
+    from pytential_b200.fmm import LaplaceKernel, QBXApply, SourceKernelSpec
+    from pytential_b200.transpose import QBXTransposeApply
+    _, geo = case
+    spec = SourceKernelSpec(LaplaceKernel(3), charge_coeff=1.0)
+    ap = QBXApply(geo, spec, 3, 10, nrhs=3, target_specific_qbx=tsqbx)
+    tr = QBXTransposeApply(ap)
+    rng = np.random.default_rng(4)
+    sig = torch.from_numpy(rng.normal(size=(3, ap.ndofs))).cuda()
+    r = torch.from_numpy(rng.normal(size=(3, ap.nuser_targets))).cuda()
+    As = ap(sig)
+    ATr = tr(r)
+    ap.check_error_word()
+    tr.check_error_word()
+    lhs = (As * r).sum(1)
+    rhs = (sig * ATr).sum(1)
+    scale = torch.linalg.norm(As, dim=1) * torch.linalg.norm(r, dim=1)
+    assert bool(((lhs - rhs).abs() <= 1e-12 * scale).all())
+
+
+@pytest.mark.gpu
+def test_gpu_transpose_rejects_other_operators():
+    from pytential_b200 import native
+    from pytential_b200.fmm import PRECISION_MIXED, LaplaceKernel, QBXApply, SourceKernelSpec
+    from pytential_b200.transpose import QBXTransposeApply
+    geo = _geometry(0, shell=10)
+    dl = QBXApply(geo, SourceKernelSpec(LaplaceKernel(3), dipole_coeff=1.0), 3, 8)
+    with pytest.raises(NotImplementedError):
+        QBXTransposeApply(dl)
+    mixed = QBXApply(geo, SourceKernelSpec(LaplaceKernel(3), charge_coeff=1.0), 3, 8,
+                     precision=PRECISION_MIXED)
+    with pytest.raises(NotImplementedError):
+        QBXTransposeApply(mixed)
+    # the C ABI refuses a double-layer plan as well, before any launch
+    import ctypes
+
+    import torch
+    vals = torch.zeros(1, dl.dgeo.ntargets, dtype=torch.float64, device="cuda")
+    cm = torch.zeros(dl.dgeo.ncenters, 1, dl.plan.ncq, dtype=torch.complex128, device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    with pytest.raises(native.QBXFMMError) as ei:
+        dl.plan.call("qbxfmm_transpose_eval_qbx_expansions", ctypes.c_void_p(vals.data_ptr()),
+                     ctypes.c_void_p(cm.data_ptr()),
+                     ctypes.cast(ctypes.c_void_p(err.data_ptr()), abi._pi), None)
+    assert ei.value.code == abi.QBXFMM_ERR_UNSUPPORTED
+
+# }}}
