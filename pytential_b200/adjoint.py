@@ -1,23 +1,26 @@
-"""Adjoint of the 3D Laplace single-layer apply at far targets, behind
-``torch.autograd.Function``.
+"""Adjoint of the 3D Laplace single-layer apply, behind ``torch.autograd.Function``.
 
 Forward: ``u = A sigma`` with ``A = K W U`` (``U``: stage-1 -> quad-stage-2
-upsampling, ``W``: area element x quadrature weight, ``K``: the kernel
-``1/(4 pi |x - y|)`` from the quad nodes to targets that lie away from the surface,
-so that no target needs QBX) -- the QBX-FMM apply of this library.
+upsampling, ``W``: area element x quadrature weight, ``K``: the QBX-FMM kernel
+matrix of ``1/(4 pi |x - y|)`` from the quad nodes to the targets) -- the apply of
+this library.
 
 Backward:
 
-* ``dJ/dsigma = A^T r = U^T W K^T r``: ``K`` is symmetric, so ``K^T r`` is the same FMM
-  with sources and targets exchanged -- point sources at the targets with strengths
-  ``r``, evaluated at the quad nodes (this library's apply on a point-cloud source
-  "discretization");
-* ``dJ/dx_t = r_t grad u(x_t)`` with ``grad u`` summed directly on the GPU
-  (``qbxfmm_laplace3d_grad_direct``).
+* ``dJ/dsigma = A^T r = U^T W K^T r`` with ``K^T`` the transpose of the apply over
+  the same tree and traversal (:class:`~pytential_b200.transpose.QBXTransposeApply`:
+  the exchanged-role FMM with transposed lists, the QBX centers carrying the
+  order-q multipoles of their targets' values), so targets that need QBX -- on the
+  surface or near it -- are covered, and ``A^T`` is the transpose of the apply's own
+  matrix (FP64);
+* ``dJ/dx_t = r_t grad u(x_t)`` at targets away from the surface, with ``grad u``
+  summed directly on the GPU (``qbxfmm_laplace3d_grad_direct``).
 
-Both directions run in FP64 or in the mixed form (FP32 far field).  Targets close to
-the surface (which need QBX in the forward apply) are not supported here: their
-adjoint would need the transposed QBX stages.
+:class:`SingleLayer` takes any targets; :class:`FarFieldSingleLayer` is the operator
+at targets away from the surface, also in the mixed form (FP32 far field), whose
+adjoint is the exchanged-role FMM on a second tree built over the targets.  The
+reference's check for both is the transpose of its dense matrix ``build_matrix``
+(pytential/symbolic/execution.py:1001-1070, pytential/symbolic/matrix.py:450-523).
 """
 
 from __future__ import annotations
@@ -31,6 +34,7 @@ from . import native
 from .discretization import Discretization
 from .fmm import PRECISION_FP64, LaplaceKernel, QBXApply, SourceKernelSpec
 from .geometry import QBXFMMGeometryData
+from .transpose import QBXTransposeApply
 
 
 def point_cloud(points: np.ndarray, radius: float = 1e-9) -> Discretization:
@@ -47,30 +51,8 @@ def point_cloud(points: np.ndarray, radius: float = 1e-9) -> Discretization:
         param=np.zeros((n, 1)))
 
 
-class FarFieldSingleLayer:
-    """``u = S sigma`` at fixed targets away from the surface, with its adjoint."""
-
-    def __init__(self, discr: Discretization, targets: np.ndarray, qbx_order: int,
-                 fmm_order: int, precision: int = PRECISION_FP64, device="cuda"):
-        if discr.ambient_dim != 3:
-            raise NotImplementedError("the adjoint is built for 3D Laplace")
-        self.discr = discr
-        self.precision = precision
-        self.targets = np.ascontiguousarray(targets, dtype=np.float64)
-        self.device = torch.device(device)
-        spec = SourceKernelSpec(LaplaceKernel(3), charge_coeff=1.0)
-        self.geo = QBXFMMGeometryData(discr, [(self.targets, 0)])
-        if self.geo.global_qbx_centers().size:
-            raise ValueError("a target needs QBX; the adjoint covers far targets only")
-        self.fwd = QBXApply(self.geo, spec, qbx_order, fmm_order, device=device,
-                            precision=precision)
-        self.geo_adj = QBXFMMGeometryData(point_cloud(self.targets), [(discr.quad_nodes, 0)])
-        self.adj = QBXApply(self.geo_adj, spec, qbx_order, fmm_order, device=device,
-                            precision=precision)
-        self.U = torch.from_numpy(np.ascontiguousarray(discr.upsample)).to(self.device)
-        self.w = torch.from_numpy(discr.quad_weights).to(self.device)
-        self.quad_nodes = torch.from_numpy(np.ascontiguousarray(discr.quad_nodes)).to(self.device)
-        self.targets_dev = torch.from_numpy(self.targets).to(self.device)
+class _Operator:
+    """Shared parts: stage-1 density -> quad strengths, the direct target gradient."""
 
     @property
     def ndofs(self):
@@ -79,6 +61,18 @@ class FarFieldSingleLayer:
     @property
     def ntargets(self):
         return self.targets.shape[1]
+
+    def _setup_common(self, discr, targets, device):
+        if discr.ambient_dim != 3:
+            raise NotImplementedError("the adjoint is built for 3D Laplace")
+        self.discr = discr
+        self.targets = np.ascontiguousarray(targets, dtype=np.float64)
+        self.device = torch.device(device)
+        self.spec = SourceKernelSpec(LaplaceKernel(3), charge_coeff=1.0)
+        self.U = torch.from_numpy(np.ascontiguousarray(discr.upsample)).to(self.device)
+        self.w = torch.from_numpy(discr.quad_weights).to(self.device)
+        self.quad_nodes = torch.from_numpy(np.ascontiguousarray(discr.quad_nodes)).to(self.device)
+        self.targets_dev = torch.from_numpy(self.targets).to(self.device)
 
     def apply(self, sigma: torch.Tensor) -> torch.Tensor:
         """(ndofs,) -> (ntargets,)"""
@@ -90,26 +84,81 @@ class FarFieldSingleLayer:
         s = sigma.reshape(d.nelements, d.nodes_per_element) @ self.U.T
         return s.reshape(-1) * self.w
 
+    def _grad_direct(self, sigma, fp64=True):
+        q = self.strengths(sigma).contiguous()
+        grad = torch.empty(3, self.ntargets, dtype=torch.float64, device=self.device)
+        st = ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
+        name = "qbxfmm_laplace3d_grad_direct" if fp64 else "qbxfmm_laplace3d_grad_direct_f32"
+        native.check(name, getattr(native.lib(), name)(
+            q.numel(), ctypes.c_void_p(self.quad_nodes.data_ptr()), ctypes.c_void_p(q.data_ptr()),
+            self.ntargets, ctypes.c_void_p(self.targets_dev.data_ptr()),
+            ctypes.c_void_p(grad.data_ptr()), st))
+        return grad
+
+
+class SingleLayer(_Operator):
+    """``u = S sigma`` at fixed targets anywhere -- on the surface (``qbx_side`` +1 or
+    -1, the one-sided limit), near it or far from it (``qbx_side`` 0) -- with the
+    adjoint ``A^T`` over the apply's own tree (FP64)."""
+
+    def __init__(self, discr: Discretization, targets: np.ndarray, qbx_order: int,
+                 fmm_order: int, qbx_side: int = 0, target_specific_qbx: bool = True,
+                 device="cuda"):
+        self._setup_common(discr, targets, device)
+        self.geo = QBXFMMGeometryData(discr, [(self.targets, qbx_side)])
+        self.fwd = QBXApply(self.geo, self.spec, qbx_order, fmm_order, device=device,
+                            target_specific_qbx=target_specific_qbx)
+        self.transpose = QBXTransposeApply(self.fwd)
+        self.targets_need_qbx = bool(self.geo.global_qbx_centers().size)
+
     def adjoint(self, r: torch.Tensor) -> torch.Tensor:
         """A^T r: (ntargets,) -> (ndofs,)"""
+        return self.transpose(r.reshape(1, -1).contiguous())[0]
+
+    def target_gradient(self, sigma: torch.Tensor) -> torch.Tensor:
+        """grad u at the targets, (3, ntargets); targets away from the surface only."""
+        if self.targets_need_qbx:
+            raise NotImplementedError("target-position gradients at targets evaluated "
+                                      "through QBX expansions")
+        return self._grad_direct(sigma)
+
+
+class FarFieldSingleLayer(_Operator):
+    """``u = S sigma`` at fixed targets away from the surface, with its adjoint: in
+    FP64 the transpose over the apply's own tree, in the mixed form the
+    exchanged-role FMM on a second tree built over the targets (point sources with
+    strengths ``r`` evaluated at the quad nodes, FP32 far field)."""
+
+    def __init__(self, discr: Discretization, targets: np.ndarray, qbx_order: int,
+                 fmm_order: int, precision: int = PRECISION_FP64, device="cuda"):
+        self._setup_common(discr, targets, device)
+        self.precision = precision
+        self.geo = QBXFMMGeometryData(discr, [(self.targets, 0)])
+        if self.geo.global_qbx_centers().size:
+            raise ValueError("a target needs QBX; use SingleLayer for targets near the surface")
+        self.fwd = QBXApply(self.geo, self.spec, qbx_order, fmm_order, device=device,
+                            precision=precision)
+        if precision == PRECISION_FP64:
+            self.transpose = QBXTransposeApply(self.fwd)
+        else:
+            self.transpose = None
+            self.geo_adj = QBXFMMGeometryData(point_cloud(self.targets), [(discr.quad_nodes, 0)])
+            self.adj = QBXApply(self.geo_adj, self.spec, qbx_order, fmm_order, device=device,
+                                precision=precision)
+
+    def adjoint(self, r: torch.Tensor) -> torch.Tensor:
+        """A^T r: (ntargets,) -> (ndofs,)"""
+        if self.transpose is not None:
+            return self.transpose(r.reshape(1, -1).contiguous())[0]
         d = self.discr
         kt = self.adj(r.reshape(1, -1).contiguous())[0]          # K^T r at the quad nodes
         v = (kt * self.w).reshape(d.nelements, d.quad_nodes_per_element)
         return (v @ self.U).reshape(-1)
 
     def target_gradient(self, sigma: torch.Tensor) -> torch.Tensor:
-        """grad u at the targets, (3, ntargets)."""
-        q = self.strengths(sigma).contiguous()
-        grad = torch.empty(3, self.ntargets, dtype=torch.float64, device=self.device)
-        st = ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
-        # the mixed-precision operator sums the gradient in FP32 arithmetic
-        name = ("qbxfmm_laplace3d_grad_direct" if self.precision == PRECISION_FP64
-                else "qbxfmm_laplace3d_grad_direct_f32")
-        native.check(name, getattr(native.lib(), name)(
-            q.numel(), ctypes.c_void_p(self.quad_nodes.data_ptr()), ctypes.c_void_p(q.data_ptr()),
-            self.ntargets, ctypes.c_void_p(self.targets_dev.data_ptr()),
-            ctypes.c_void_p(grad.data_ptr()), st))
-        return grad
+        """grad u at the targets, (3, ntargets); the mixed-precision operator sums it in
+        FP32 arithmetic."""
+        return self._grad_direct(sigma, fp64=self.precision == PRECISION_FP64)
 
 
 class _SingleLayer(torch.autograd.Function):
@@ -128,7 +177,7 @@ class _SingleLayer(torch.autograd.Function):
         return g_sigma, g_targets, None
 
 
-def single_layer(op: FarFieldSingleLayer, sigma: torch.Tensor,
+def single_layer(op: SingleLayer | FarFieldSingleLayer, sigma: torch.Tensor,
                  targets: torch.Tensor | None = None) -> torch.Tensor:
     """Differentiable ``S sigma`` at ``op``'s targets.  Pass ``targets`` (a (3, nt)
     tensor holding ``op.targets``) to get gradients with respect to the target

@@ -110,3 +110,75 @@ def test_mixed_target_gradient_rechecked_in_fp64(small):
     g64 = op.target_gradient(sig).cpu().numpy()
     g32 = opm.target_gradient(sig).cpu().numpy()
     assert 0 < relerr(g32, g64) < 1e-5
+
+
+# {{{ targets that need QBX: the transpose over the apply's own tree
+
+@pytest.fixture(scope="module")
+def on_surface():
+    """The single layer on the surface (exterior limit) of the 320-triangle ellipsoid,
+    q 4 / p 12, its adjoint over the apply's tree, and the dense QBX matrix."""
+    from pytential_b200.adjoint import SingleLayer
+    from pytential_b200.dense import qbx_matrix
+    from pytential_b200.workloads import laplace3d_adjoint
+    w = laplace3d_adjoint(nrefine=2, ntargets=8, seed=5)
+    op = SingleLayer(w.discr, w.discr.nodes, w.qbx_order, w.fmm_order, qbx_side=+1)
+    M = qbx_matrix(op.geo, op.spec, w.qbx_order).cpu().numpy()
+    return w, op, M
+
+
+def test_on_surface_adjoint_matches_dense_transpose(on_surface):
+    w, op, M = on_surface
+    assert op.targets_need_qbx
+    rng = np.random.default_rng(6)
+    sig = rng.normal(size=op.ndofs)
+    assert relerr(op.apply(torch.from_numpy(sig).cuda()).cpu().numpy(), M @ sig) < 1e-7
+    R = rng.normal(size=(8, op.ntargets))
+    got = np.stack([op.adjoint(torch.from_numpy(r).cuda()).cpu().numpy() for r in R])
+    assert relerr(got, R @ M) < 1e-7
+
+
+def test_on_surface_density_gradient_central_differences(on_surface):
+    """J = |S sigma - g|^2 / 2 on the surface; 32 seeded directions, h = 1e-6."""
+    from pytential_b200.adjoint import single_layer
+    w, op, _ = on_surface
+    g_np = w.g(w.discr.nodes)
+    sigma = torch.from_numpy(w.sigma).cuda().requires_grad_(True)
+    g = torch.from_numpy(g_np).cuda()
+    J = 0.5 * ((single_layer(op, sigma) - g) ** 2).sum()
+    J.backward()
+    gs = sigma.grad.cpu().numpy()
+
+    def J_sigma(s):
+        uu = op.apply(torch.from_numpy(s).cuda()).cpu().numpy()
+        return 0.5 * ((uu - g_np) ** 2).sum()
+
+    rng = np.random.default_rng(7)
+    h = 1e-6
+    for _ in range(32):
+        v = rng.normal(size=w.sigma.shape)
+        fd = (J_sigma(w.sigma + h * v) - J_sigma(w.sigma - h * v)) / (2 * h)
+        assert abs(fd - gs @ v) <= 1e-6 * abs(gs @ v) + 1e-10
+
+
+def test_near_targets_adjoint_dot_products():
+    from pytential_b200.adjoint import SingleLayer
+    from pytential_b200.workloads import laplace3d_adjoint
+    w = laplace3d_adjoint(nrefine=2, ntargets=8, seed=8)
+    d = w.discr
+    rng = np.random.default_rng(9)
+    i = rng.integers(0, d.ndofs, 600)
+    h = rng.uniform(0.05, 1.0, 600) * d.element_stretch[i // d.nodes_per_element]
+    X = np.concatenate([d.nodes[:, i] + h * d.normals[:, i], w.targets], axis=1)
+    op = SingleLayer(d, X, w.qbx_order, w.fmm_order)
+    assert op.targets_need_qbx
+    for _ in range(4):
+        sig = torch.from_numpy(rng.normal(size=op.ndofs)).cuda()
+        r = torch.from_numpy(rng.normal(size=op.ntargets)).cuda()
+        As, ATr = op.apply(sig), op.adjoint(r)
+        lhs, rhs = float((As * r).sum()), float((sig * ATr).sum())
+        assert abs(lhs - rhs) <= 1e-12 * float(torch.linalg.norm(As) * torch.linalg.norm(r))
+    with pytest.raises(NotImplementedError):
+        op.target_gradient(sig)
+
+# }}}
