@@ -170,6 +170,20 @@ int qbxfmm_transpose_form_global_qbx_locals(const qbxfmm_plan* plan,
                                             const void* center_mpoles, void* source_values,
                                             int32_t* error_word, void* stream);
 
+/* The whole transpose K^T r in one call: `plan` the apply's plan, `transposed` the
+ * plan of its exchanged-role geometry (same boxes, transposed lists, no centers; its
+ * translation matrices built into ws by qbxfmm_precompute_translations), ws a
+ * workspace of `transposed` (its qbx_exps unused).  target_values: [nrhs][ntargets]
+ * of the apply's tree targets; strengths: the same values at its non-QBX targets,
+ * [nrhs][nfiltered_targets]; center_mpoles: scratch [ncenters][nrhs][ncoeff(qbx_order)]
+ * complex128; out: [nrhs][nsources] at the apply's sources in tree order, with the
+ * kernel scaling (written).  Runs on the transposed plan's streams like
+ * qbxfmm_apply; graph-capturable. */
+int qbxfmm_apply_transpose(const qbxfmm_plan* plan, const qbxfmm_plan* transposed,
+                           const qbxfmm_transpose_index* index, const qbxfmm_workspace* ws,
+                           const void* target_values, const void* strengths,
+                           void* center_mpoles, void* out, void* stream);
+
 /* }}} */
 
 /* potential assembly: scatter the non-QBX part, add the QBX part, reorder to user

@@ -1108,6 +1108,79 @@ int qbxfmm_precompute_translations(const qbxfmm_plan* p, const qbxfmm_workspace*
   return QBXFMM_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// M2M / L2L: the FP64 matrix-vector kernels whenever the matrices are small (both
+// precisions: they are latency-bound, a TF32 form would not be faster); M2L: split
+// TF32 in the mixed form.  `gemm`: the translation matrices of ws are built; T32:
+// their split-TF32 planes (mixed form), or NULL.
+int run_m2m(const qbxfmm_plan* p, const qbxfmm_workspace* ws, const uint32_t* T32, bool gemm,
+            void* stream)
+{
+  cudaStream_t st = S(stream);
+  if (gemm && trans_mv_supported(p->tc))
+    QBX_TRY(launch_m2m_mv(p->geo, p->th, p->tc, p->kern.nrhs, (const double*)ws->translations,
+                          (double2*)ws->mpoles, ws->error_word, st),
+            "coarsen_multipoles (matrix form)");
+  else if (T32)
+    QBX_TRY(launch_m2m_gemm_mixed(p->geo, p->th, p->tc, p->kern.nrhs, T32, (double2*)ws->mpoles,
+                                  (double*)ws->pair_scratch, ws->error_word, st),
+            "coarsen_multipoles (split TF32)");
+  else if (gemm)
+    QBX_TRY(launch_m2m_gemm(p->geo, p->th, p->tc, p->kern.nrhs, (const double*)ws->translations,
+                            (double2*)ws->mpoles, (double*)ws->pair_scratch, ws->error_word, st),
+            "coarsen_multipoles (matrix form)");
+  else
+    return qbxfmm_coarsen_multipoles(p, ws->mpoles, stream);
+  return QBXFMM_OK;
+}
+
+int run_m2l(const qbxfmm_plan* p, const qbxfmm_workspace* ws, const uint32_t* T32, bool gemm,
+            void* stream)
+{
+  cudaStream_t st = S(stream);
+  if (T32)
+    QBX_TRY(launch_m2l_gemm_mixed(p->geo, p->th, p->tc, p->kern.nrhs, T32,
+                                  (const double2*)ws->mpoles, (double2*)ws->locals,
+                                  (double*)ws->pair_scratch, ws->error_word, st),
+            "multipole_to_local (split TF32)");
+  else if (gemm)
+    QBX_TRY(launch_m2l_gemm(p->geo, p->th, p->tc, p->kern.nrhs, (const double*)ws->translations,
+                            (const double2*)ws->mpoles, (double2*)ws->locals,
+                            (double*)ws->pair_scratch, ws->error_word, st),
+            "multipole_to_local (matrix form)");
+  else
+    return qbxfmm_multipole_to_local(p, ws->mpoles, ws->locals, ws->error_word, stream);
+  return QBXFMM_OK;
+}
+
+int run_l2l(const qbxfmm_plan* p, const qbxfmm_workspace* ws, const uint32_t* T32, bool gemm,
+            void* stream)
+{
+  cudaStream_t st = S(stream);
+  if (gemm && trans_mv_supported(p->tc))
+    QBX_TRY(launch_l2l_mv(p->geo, p->th, p->tc, p->kern.nrhs, (const double*)ws->translations,
+                          (double2*)ws->locals, ws->error_word, st),
+            "refine_locals (matrix form)");
+  else if (T32)
+    QBX_TRY(launch_l2l_gemm_mixed(p->geo, p->th, p->tc, p->kern.nrhs, T32, (double2*)ws->locals,
+                                  ws->error_word, st),
+            "refine_locals (split TF32)");
+  else if (gemm)
+    QBX_TRY(launch_l2l_gemm(p->geo, p->th, p->tc, p->kern.nrhs, (const double*)ws->translations,
+                            (double2*)ws->locals, ws->error_word, st),
+            "refine_locals (matrix form)");
+  else
+    return qbxfmm_refine_locals(p, ws->locals, stream);
+  return QBXFMM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
 int qbxfmm_apply(const qbxfmm_plan* p, const qbxfmm_upsample* up, const qbxfmm_workspace* ws,
                  const void* density, void* out, void* stream)
 {
@@ -1139,58 +1212,9 @@ int qbxfmm_apply(const qbxfmm_plan* p, const qbxfmm_upsample* up, const qbxfmm_w
                             ? reinterpret_cast<const uint32_t*>((const double*)ws->translations +
                                                                 trans_matrix_bytes(p->tc) / sizeof(double))
                             : nullptr;
-  // M2M / L2L: the FP64 matrix-vector kernels whenever the matrices are small (both
-  // precisions: they are latency-bound, a TF32 form would not be faster); M2L: split
-  // TF32 in the mixed form
-  auto m2m = [&]() -> int {
-    if (gemm && trans_mv_supported(p->tc))
-      QBX_TRY(launch_m2m_mv(p->geo, p->th, p->tc, p->kern.nrhs, (const double*)ws->translations,
-                            (double2*)ws->mpoles, ws->error_word, st),
-              "coarsen_multipoles (matrix form)");
-    else if (T32)
-      QBX_TRY(launch_m2m_gemm_mixed(p->geo, p->th, p->tc, p->kern.nrhs, T32, (double2*)ws->mpoles,
-                                    (double*)ws->pair_scratch, ws->error_word, st),
-              "coarsen_multipoles (split TF32)");
-    else if (gemm)
-      QBX_TRY(launch_m2m_gemm(p->geo, p->th, p->tc, p->kern.nrhs, (const double*)ws->translations,
-                              (double2*)ws->mpoles, (double*)ws->pair_scratch, ws->error_word, st),
-              "coarsen_multipoles (matrix form)");
-    else
-      return qbxfmm_coarsen_multipoles(p, ws->mpoles, stream);
-    return QBXFMM_OK;
-  };
-  auto m2l = [&]() -> int {
-    if (T32)
-      QBX_TRY(launch_m2l_gemm_mixed(p->geo, p->th, p->tc, p->kern.nrhs, T32,
-                                    (const double2*)ws->mpoles, (double2*)ws->locals,
-                                    (double*)ws->pair_scratch, ws->error_word, st),
-              "multipole_to_local (split TF32)");
-    else if (gemm)
-      QBX_TRY(launch_m2l_gemm(p->geo, p->th, p->tc, p->kern.nrhs, (const double*)ws->translations,
-                              (const double2*)ws->mpoles, (double2*)ws->locals,
-                              (double*)ws->pair_scratch, ws->error_word, st),
-              "multipole_to_local (matrix form)");
-    else
-      return qbxfmm_multipole_to_local(p, ws->mpoles, ws->locals, ws->error_word, stream);
-    return QBXFMM_OK;
-  };
-  auto l2l = [&]() -> int {
-    if (gemm && trans_mv_supported(p->tc))
-      QBX_TRY(launch_l2l_mv(p->geo, p->th, p->tc, p->kern.nrhs, (const double*)ws->translations,
-                            (double2*)ws->locals, ws->error_word, st),
-              "refine_locals (matrix form)");
-    else if (T32)
-      QBX_TRY(launch_l2l_gemm_mixed(p->geo, p->th, p->tc, p->kern.nrhs, T32, (double2*)ws->locals,
-                                    ws->error_word, st),
-              "refine_locals (split TF32)");
-    else if (gemm)
-      QBX_TRY(launch_l2l_gemm(p->geo, p->th, p->tc, p->kern.nrhs, (const double*)ws->translations,
-                              (double2*)ws->locals, ws->error_word, st),
-              "refine_locals (matrix form)");
-    else
-      return qbxfmm_refine_locals(p, ws->locals, stream);
-    return QBXFMM_OK;
-  };
+  auto m2m = [&]() -> int { return run_m2m(p, ws, T32, gemm, stream); };
+  auto m2l = [&]() -> int { return run_m2l(p, ws, T32, gemm, stream); };
+  auto l2l = [&]() -> int { return run_l2l(p, ws, T32, gemm, stream); };
   // The stage graph of drive_fmm (fmm.py:436-588) on four streams.  Every buffer
   // that several stages add into is written by one stream at a time:
   //   caller's stream: strengths, P2M, M2M | M2L, L2L | L2P | L2QBXL, QBXL2P, assembly
@@ -1335,6 +1359,97 @@ int qbxfmm_transpose_form_global_qbx_locals(const qbxfmm_plan* p, const qbxfmm_t
                            (const double2*)center_mpoles, (double*)source_values, err, S(stream)),
           "transpose_form_global_qbx_locals");
   return QBXFMM_OK;
+}
+
+int qbxfmm_apply_transpose(const qbxfmm_plan* p, const qbxfmm_plan* d,
+                           const qbxfmm_transpose_index* ix, const qbxfmm_workspace* ws,
+                           const void* target_values, const void* strengths,
+                           void* center_mpoles, void* out, void* stream)
+{
+  if (int rc = transpose_ok(p)) return rc;
+  if (int rc = check_plan(d)) return rc;
+  if (d->helm || d->kern.dim != 3 || d->mixed || level_orders_on(d) || d->geo.ncenters != 0 ||
+      d->kern.fmm_order != p->kern.fmm_order || d->kern.nrhs != p->kern.nrhs ||
+      d->geo.nboxes != p->geo.nboxes || d->geo.nsources != p->geo.nfiltered_targets ||
+      d->geo.ntargets != p->geo.nsources)
+    return fail(QBXFMM_ERR_ARG, "the second plan is not the exchanged-role plan of the first");
+  if (!ix || !ws || !target_values || !strengths || !center_mpoles || !out)
+    return fail(QBXFMM_ERR_ARG, "null argument");
+  if (!ws->mpoles || !ws->locals || !ws->pot_nonqbx || !ws->pot_tree)
+    return fail(QBXFMM_ERR_ARG, "incomplete workspace");
+  size_t sz[8];
+  if (int rc = qbxfmm_workspace_sizes(d, sz)) return rc;
+  const bool gemm = d->trans_ok && ws->translations && ws->pair_scratch;
+  cudaStream_t st = S(stream);
+  QBX_TRY(cudaMemsetAsync(ws->mpoles, 0, sz[1], st), "apply_transpose: clear");
+  QBX_TRY(cudaMemsetAsync(ws->locals, 0, sz[2], st), "apply_transpose: clear");
+  QBX_TRY(cudaMemsetAsync(ws->pot_nonqbx, 0, sz[4], st), "apply_transpose: clear");
+  QBX_TRY(cudaMemsetAsync(ws->pot_tree, 0, sz[5], st), "apply_transpose: clear");
+  if (ws->error_word)
+    QBX_TRY(cudaMemsetAsync(ws->error_word, 0, sizeof(int32_t), st), "apply_transpose: clear");
+  int rc;
+  if ((rc = qbxfmm_transpose_eval_qbx_expansions(p, target_values, center_mpoles, ws->error_word,
+                                                 stream)))
+    return rc;
+  // The exchanged-role stage graph on the second plan's four streams, as in
+  // qbxfmm_apply, with the transposed QBX stages where their outputs are consumed:
+  //   caller's stream: P2M, L2QBXL^T, M2M | M2L, L2L | L2P, assembly
+  //   side[0]:         P2P, P2QBXL^T | M2P
+  //   side[1]:         P2L, M2QBXL^T
+  // (every stage adds into its outputs; the writers of one buffer never overlap)
+  cudaStream_t side1 = d->side[0], side2 = d->side[1], side3 = d->side[2];
+  void* s1 = d->side[0];
+  void* s2 = d->side[1];
+  bool forked = false;
+  auto join = [&](int code) -> int {
+    if (forked) {
+      cudaEventRecord(d->ev_near, side1);
+      cudaEventRecord(d->ev_p2l, side2);
+      cudaEventRecord(d->ev_qbx, side3);
+      cudaStreamWaitEvent(st, d->ev_near, 0);
+      cudaStreamWaitEvent(st, d->ev_p2l, 0);
+      cudaStreamWaitEvent(st, d->ev_qbx, 0);
+    }
+    return code;
+  };
+#define QBX_STEP(call)                  \
+  do {                                  \
+    if ((rc = (call))) return join(rc); \
+  } while (0)
+#define QBX_CUDA_STEP(call, what)                            \
+  do {                                                       \
+    if ((rc = cuda_check((call), what))) return join(rc);   \
+  } while (0)
+  QBX_CUDA_STEP(cudaEventRecord(d->ev_fork, st), "apply_transpose: fork");
+  for (cudaStream_t s : {side1, side2, side3})
+    QBX_CUDA_STEP(cudaStreamWaitEvent(s, d->ev_fork, 0), "apply_transpose: fork");
+  forked = true;
+  QBX_STEP(qbxfmm_form_locals(d, strengths, ws->locals, ws->error_word, s2));
+  QBX_STEP(qbxfmm_transpose_translate_box_multipoles_to_qbx_local(p, ix, center_mpoles, ws->locals,
+                                                                  ws->error_word, s2));
+  QBX_CUDA_STEP(cudaEventRecord(d->ev_p2l, side2), "apply_transpose: P2L event");
+  QBX_STEP(qbxfmm_eval_direct(d, strengths, ws->pot_nonqbx, ws->error_word, s1));
+  QBX_STEP(qbxfmm_transpose_form_global_qbx_locals(p, ix, center_mpoles, ws->pot_nonqbx,
+                                                   ws->error_word, s1));
+  QBX_STEP(qbxfmm_form_multipoles(d, strengths, ws->mpoles, stream));
+  QBX_STEP(qbxfmm_transpose_translate_box_local_to_qbx_local(p, ix, center_mpoles, ws->mpoles,
+                                                             ws->error_word, stream));
+  QBX_STEP(run_m2m(d, ws, nullptr, gemm, stream));
+  QBX_CUDA_STEP(cudaEventRecord(d->ev_mpoles, st), "apply_transpose: multipole event");
+  QBX_CUDA_STEP(cudaStreamWaitEvent(side1, d->ev_mpoles, 0), "apply_transpose: multipole event");
+  QBX_STEP(qbxfmm_eval_multipoles(d, ws->mpoles, ws->pot_nonqbx, ws->error_word, s1));
+  QBX_CUDA_STEP(cudaEventRecord(d->ev_near, side1), "apply_transpose: near-field event");
+  QBX_CUDA_STEP(cudaEventRecord(d->ev_qbx, side3), "apply_transpose: idle stream");
+  QBX_CUDA_STEP(cudaStreamWaitEvent(st, d->ev_p2l, 0), "apply_transpose: join P2L");
+  QBX_STEP(run_m2l(d, ws, nullptr, gemm, stream));
+  QBX_STEP(run_l2l(d, ws, nullptr, gemm, stream));
+  QBX_CUDA_STEP(cudaStreamWaitEvent(st, d->ev_near, 0), "apply_transpose: join near field");
+  QBX_CUDA_STEP(cudaStreamWaitEvent(st, d->ev_qbx, 0), "apply_transpose: join");
+  QBX_STEP(qbxfmm_eval_locals(d, ws->locals, ws->pot_nonqbx, stream));
+  forked = false;
+#undef QBX_STEP
+#undef QBX_CUDA_STEP
+  return qbxfmm_assemble(d, ws->pot_nonqbx, ws->pot_tree, out, stream);
 }
 
 // }}}

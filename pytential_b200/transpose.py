@@ -257,15 +257,16 @@ class QBXTransposeApply:
     (FP64, one FMM order) on its device: ``A^T r`` for values ``r`` at the apply's
     user targets, ``(nrhs, nuser_targets) -> (nrhs, ndofs)``, with ``A = K W U``
     (upsampling ``U``, weights ``W``, the QBX-FMM kernel matrix ``K``) and
-    ``A^T = U^T W K^T``.  ``K^T`` runs over the apply's own tree: the exchanged-role
-    geometry's box stages (the library's stage entries) and the four transposed QBX
-    stages (``qbxfmm_transpose_*`` on the apply's plan)."""
+    ``A^T = U^T W K^T``.  ``K^T`` runs over the apply's own tree in one C-ABI call
+    (``qbxfmm_apply_transpose``): the exchanged-role geometry's plan with its
+    translation matrices, and the four transposed QBX stages on the apply's plan."""
 
     def __init__(self, apply):
         import torch
 
         from .fmm import (PRECISION_FP64, B200QBXExpansionWrangler,
-                          B200TreeIndependentDataForWrangler, _ptr)
+                          B200TreeIndependentDataForWrangler, DeviceGeometry, Plan, _ptr,
+                          _stream_handle)
         plan = apply.plan
         spec = plan.spec
         if spec.kernel.family != abi.QBXFMM_LAPLACE or spec.kernel.dim != 3 \
@@ -274,13 +275,30 @@ class QBXTransposeApply:
         if plan.precision != PRECISION_FP64 or len(set(plan.get_level_orders())) > 1:
             raise NotImplementedError("the transposed apply runs in FP64 with one FMM order")
         self.fwd = apply
-        self.nrhs = apply.nrhs
-        self.device = apply.device
+        self.nrhs = nrhs = apply.nrhs
+        self.device = dev = apply.device
         self.dual_geo = TransposedGeometryData(apply.geo)
-        self.dual = B200QBXExpansionWrangler(
-            B200TreeIndependentDataForWrangler(spec), self.dual_geo, np.float64,
-            plan.qbx_order, plan.fmm_order, nrhs=self.nrhs, device=self.device)
-        dev = self.device
+        self.dual_dgeo = DeviceGeometry(self.dual_geo, dev)
+        self.dual_plan = Plan(self.dual_dgeo, spec, plan.qbx_order, plan.fmm_order, nrhs)
+        self._wrangler_args = (B200QBXExpansionWrangler, B200TreeIndependentDataForWrangler)
+        self._dual_wrangler = None
+
+        # workspace of the exchanged-role plan, with its translation matrices
+        sizes = self.dual_plan.workspace_sizes()
+        self._ws_tensors = [torch.zeros(max(sz, 8) // 8 + 1, dtype=torch.float64, device=dev)
+                            for sz in sizes[:6]]
+        use_mats = sizes[6] > 0
+        self._mat_tensors = [torch.zeros(sz // 8 + 1, dtype=torch.float64, device=dev)
+                             for sz in sizes[6:]] if use_mats else []
+        self.error_word = torch.zeros(1, dtype=torch.int32, device=dev)
+        ptrs = [ctypes.c_void_p(_ptr(t)) for t in self._ws_tensors]
+        mats = ([ctypes.c_void_p(_ptr(t)) for t in self._mat_tensors] if use_mats
+                else [ctypes.c_void_p(0), ctypes.c_void_p(0)])
+        self.ws = abi.QBXFMMWorkspace(
+            *ptrs, ctypes.cast(ctypes.c_void_p(_ptr(self.error_word)), abi._pi), *mats)
+        if use_mats:
+            self.dual_plan.call("qbxfmm_precompute_translations", ctypes.byref(self.ws),
+                                _stream_handle())
 
         def put(a):
             a = np.ascontiguousarray(a, np.int32)
@@ -288,10 +306,9 @@ class QBXTransposeApply:
 
         ix = transpose_index(apply.geo)
         self._ix = {f: put(getattr(ix, f)) for f in ix.__dataclass_fields__}
-        P = abi._pi
 
         def ptr(name):
-            return ctypes.cast(ctypes.c_void_p(_ptr(self._ix[name])), P)
+            return ctypes.cast(ctypes.c_void_p(_ptr(self._ix[name])), abi._pi)
         self.index = abi.QBXFMMTransposeIndex(
             len(ix.center_boxes), ptr("center_boxes"), ptr("box_center_starts"),
             ptr("box_centers"), len(ix.list3_rows), ptr("list3_rows"), ptr("list3_rev_starts"),
@@ -313,48 +330,77 @@ class QBXTransposeApply:
         self.nsources = sc["nsources"]
         self.nuser_targets = sc["nuser_targets"]
         self.ncq = plan.ncq
-        self.error_word = torch.zeros(1, dtype=torch.int32, device=dev)
+        self._cm = torch.zeros(max(nc, 1), nrhs, self.ncq, dtype=torch.complex128, device=dev)
 
-    def _call(self, name, *args):
-        from .fmm import _stream_handle
-        err = ctypes.cast(ctypes.c_void_p(self.error_word.data_ptr()), abi._pi)
-        self.fwd.plan.call(name, *args, err, _stream_handle())
-
-    def kernel_transpose(self, r):
-        """``K^T r``: ``(nrhs, nuser_targets)`` -> ``(nrhs, nsources)`` in user source
-        order (the flat quad sources)."""
+    def _inputs(self, r):
+        """Tree-target values and the non-QBX ones (the exchanged-role strengths)."""
         import torch
-        vp = ctypes.c_void_p
         r = torch.as_tensor(r, dtype=torch.float64, device=self.device)
         r = r.reshape(self.nrhs, self.nuser_targets)
-        W = self.dual
         r_tree = torch.zeros(self.nrhs, self.ntargets_tree, dtype=torch.float64, device=self.device)
         r_tree[:, self._tree_t] = r[:, self._user_t]
         s_dual = r_tree[:, self._filt].contiguous()
         if s_dual.shape[1] == 0:
             s_dual = torch.zeros(self.nrhs, 1, dtype=torch.float64, device=self.device)
-        cm = torch.zeros(max(self.ncenters, 1), self.nrhs, self.ncq, dtype=torch.complex128,
-                         device=self.device)
+        return r_tree, s_dual
+
+    def _to_user(self, out_tree):
+        import torch
+        out = torch.empty_like(out_tree)
+        out[:, self._usid] = out_tree
+        return out
+
+    def kernel_transpose(self, r):
+        """``K^T r``: ``(nrhs, nuser_targets)`` -> ``(nrhs, nsources)`` in user source
+        order (the flat quad sources)."""
+        import torch
+
+        from .fmm import _ptr, _stream_handle
+        r_tree, s_dual = self._inputs(r)
+        out = torch.empty(self.nrhs, self.nsources, dtype=torch.float64, device=self.device)
+        vp = ctypes.c_void_p
+        self.fwd.plan.call("qbxfmm_apply_transpose", self.dual_plan.handle,
+                           ctypes.byref(self.index), ctypes.byref(self.ws), vp(_ptr(r_tree)),
+                           vp(_ptr(s_dual)), vp(_ptr(self._cm)), vp(_ptr(out)), _stream_handle())
+        return self._to_user(out)
+
+    def kernel_transpose_by_stages(self, r):
+        """``K^T r`` through the stage entries: the exchanged-role wrangler's box stages
+        (per-pair translation kernels) and the four ``qbxfmm_transpose_*`` entries, in
+        the order of the transposed stage graph."""
+        import torch
+
+        from .fmm import _stream_handle
+        if self._dual_wrangler is None:
+            Wcls, Tcls = self._wrangler_args
+            p = self.fwd.plan
+            self._dual_wrangler = Wcls(Tcls(p.spec), self.dual_geo, np.float64, p.qbx_order,
+                                       p.fmm_order, nrhs=self.nrhs, device=self.device,
+                                       device_geometry=self.dual_dgeo)
+        W = self._dual_wrangler
+        r_tree, s_dual = self._inputs(r)
+        cm = torch.zeros_like(self._cm)
+        vp = ctypes.c_void_p
         ix = ctypes.byref(self.index)
+        err = ctypes.cast(ctypes.c_void_p(self.error_word.data_ptr()), abi._pi)
+
+        def call(name, *args):
+            self.fwd.plan.call(name, *args, err, _stream_handle())
         mp = W.form_multipoles(None, None, None, [s_dual])
-        self._call("qbxfmm_transpose_eval_qbx_expansions", vp(r_tree.data_ptr()), vp(cm.data_ptr()))
-        self._call("qbxfmm_transpose_translate_box_local_to_qbx_local", ix, vp(cm.data_ptr()),
-                   vp(mp.data_ptr()))
+        call("qbxfmm_transpose_eval_qbx_expansions", vp(r_tree.data_ptr()), vp(cm.data_ptr()))
+        call("qbxfmm_transpose_translate_box_local_to_qbx_local", ix, vp(cm.data_ptr()),
+             vp(mp.data_ptr()))
         W.coarsen_multipoles(None, None, None, mp)
         pot = W.eval_direct(None, None, None, None, [s_dual])
         lo = W.multipole_to_local(None, None, None, None, None, mp)
         pot += W.eval_multipoles(None, None, None, mp)
         lo += W.form_locals(None, None, None, None, None, [s_dual])
-        self._call("qbxfmm_transpose_translate_box_multipoles_to_qbx_local", ix,
-                   vp(cm.data_ptr()), vp(lo.data_ptr()))
+        call("qbxfmm_transpose_translate_box_multipoles_to_qbx_local", ix, vp(cm.data_ptr()),
+             vp(lo.data_ptr()))
         W.refine_locals(None, None, None, lo)
         pot += W.eval_locals(None, None, None, lo)
-        self._call("qbxfmm_transpose_form_global_qbx_locals", ix, vp(cm.data_ptr()),
-                   vp(pot.data_ptr()))
-        out_tree = W.assemble_potentials(pot, W.full_output_zeros())
-        out = torch.empty_like(out_tree)
-        out[:, self._usid] = out_tree
-        return out
+        call("qbxfmm_transpose_form_global_qbx_locals", ix, vp(cm.data_ptr()), vp(pot.data_ptr()))
+        return self._to_user(W.assemble_potentials(pot, W.full_output_zeros()))
 
     def __call__(self, r):
         """``A^T r``: ``(nrhs, nuser_targets)`` -> ``(nrhs, ndofs)``."""
@@ -366,7 +412,10 @@ class QBXTransposeApply:
 
     def check_error_word(self):
         from . import native
-        for w in (int(self.error_word.item()), int(self.dual.error_word.item())):
+        words = [int(self.error_word.item())]
+        if self._dual_wrangler is not None:
+            words.append(int(self._dual_wrangler.error_word.item()))
+        for w in words:
             if w:
                 raise native.QBXFMMError("transpose", abi.QBXFMM_ERR_DEVICE,
                                          f"a kernel met an out-of-range index (code {w})")

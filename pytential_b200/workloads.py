@@ -268,51 +268,63 @@ def _solve2d(argv=None):
 
 
 def _adjoint3d(argv=None):
-    """``python -m pytential_b200.workloads adjoint3d [NREFINE] [--mixed]``: the 3D
-    Laplace single-layer adjoint benchmark (ellipsoid, 5000 targets on the sphere of
-    radius 3, qbx_order 4, fmm_order 12): times the forward apply and forward +
-    backward (density and target-position gradients) on the current GPU."""
+    """``python -m pytential_b200.workloads adjoint3d [NREFINE] [--mixed |
+    --on-surface]``: the 3D Laplace single-layer adjoint benchmark (ellipsoid, 5000
+    targets on the sphere of radius 3, qbx_order 4, fmm_order 12): times the forward
+    apply, the adjoint apply alone and forward + backward (density and
+    target-position gradients) on the current GPU.  ``--on-surface``: the targets are
+    the surface nodes (exterior limit, every target through QBX) and the backward
+    pass takes the density gradient only."""
     import time
 
     import torch
 
-    from .adjoint import FarFieldSingleLayer, single_layer
+    from .adjoint import FarFieldSingleLayer, SingleLayer, single_layer
     from .fmm import PRECISION_FP64, PRECISION_MIXED
     argv = list(argv or [])
     mixed = "--mixed" in argv
-    argv = [a for a in argv if a != "--mixed"]
+    surface = "--on-surface" in argv
+    argv = [a for a in argv if not a.startswith("--")]
     nref = int(argv[0]) if argv else 4
     w = laplace3d_adjoint(nrefine=nref)
-    op = FarFieldSingleLayer(w.discr, w.targets, w.qbx_order, w.fmm_order,
-                             precision=PRECISION_MIXED if mixed else PRECISION_FP64)
+    if surface:
+        X_np = w.discr.nodes
+        op = SingleLayer(w.discr, X_np, w.qbx_order, w.fmm_order, qbx_side=+1)
+    else:
+        X_np = w.targets
+        op = FarFieldSingleLayer(w.discr, X_np, w.qbx_order, w.fmm_order,
+                                 precision=PRECISION_MIXED if mixed else PRECISION_FP64)
     sig0 = torch.from_numpy(w.sigma).cuda()
-    X0 = torch.from_numpy(w.targets).cuda()
-    g = torch.from_numpy(w.g(w.targets)).cuda()
+    X0 = torch.from_numpy(np.ascontiguousarray(X_np)).cuda()
+    g = torch.from_numpy(w.g(X_np)).cuda()
+    r0 = torch.ones(op.ntargets, dtype=torch.float64, device="cuda")
 
     def fwd_bwd():
         sigma = sig0.clone().requires_grad_(True)
-        X = X0.clone().requires_grad_(True)
+        X = None if surface else X0.clone().requires_grad_(True)
         u = single_layer(op, sigma, X)
         J = 0.5 * ((u - g) ** 2).sum()
         J.backward()
-        return sigma.grad, X.grad
+        return sigma.grad
+
+    def timed(f):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(5):
+            f()
+        torch.cuda.synchronize()
+        return (time.perf_counter() - t0) / 5
     for _ in range(3):
         op.apply(sig0)
+        op.adjoint(r0)
         fwd_bwd()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for _ in range(5):
-        op.apply(sig0)
-    torch.cuda.synchronize()
-    tf = (time.perf_counter() - t0) / 5
-    t0 = time.perf_counter()
-    for _ in range(5):
-        fwd_bwd()
-    torch.cuda.synchronize()
-    tb = (time.perf_counter() - t0) / 5
-    print(f"3D Laplace S adjoint, icosphere-{nref} ({w.discr.ndofs} nodes), "
-          f"{w.targets.shape[1]} targets, {'mixed' if mixed else 'FP64'}: forward "
-          f"{1e3 * tf:.2f} ms, forward + backward {1e3 * tb:.2f} ms")
+    tf = timed(lambda: op.apply(sig0))
+    ta = timed(lambda: op.adjoint(r0))
+    tb = timed(fwd_bwd)
+    where = f"{op.ntargets} surface targets (QBX)" if surface else f"{op.ntargets} targets"
+    print(f"3D Laplace S adjoint, icosphere-{nref} ({w.discr.ndofs} nodes), {where}, "
+          f"{'mixed' if mixed else 'FP64'}: forward {1e3 * tf:.2f} ms, adjoint "
+          f"{1e3 * ta:.2f} ms, forward + backward {1e3 * tb:.2f} ms")
 
 
 if __name__ == "__main__":

@@ -148,11 +148,14 @@ def test_gpu_transpose_matches_checker(case):
     tr = QBXTransposeApply(ap)
     rng = np.random.default_rng(3)
     r = rng.normal(size=(2, ap.nuser_targets))
-    got = tr.kernel_transpose(torch.from_numpy(r).cuda()).cpu().numpy()
-    tr.check_error_word()
     o = _oracle(geo, nrhs=2)
     ref = o.apply_transpose(r)[:, np.argsort(o.arrays["user_source_ids"][:o.scalars["nsources"]])]
-    assert relerr(got, ref) < 1e-12
+    # the one-call transpose (matrix-form translations, four streams) and the stage
+    # entries one by one
+    for f in (tr.kernel_transpose, tr.kernel_transpose_by_stages):
+        got = f(torch.from_numpy(r).cuda()).cpu().numpy()
+        tr.check_error_word()
+        assert relerr(got, ref) < 1e-12, f.__name__
 
 
 @pytest.mark.gpu
