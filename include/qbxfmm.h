@@ -226,6 +226,9 @@ typedef struct qbxfmm_transpose_index {
   const int32_t* list1_rows;         /* source boxes in the list 1 of some center box */
   const int32_t* list1_rev_starts;   /* [nlist1_rows + 1] */
   const int32_t* list1_rev_lists;    /* the center boxes whose list 1 holds the row box */
+  const int32_t* box_pair_starts;    /* [nboxes + 1] into pair_targets / pair_centers */
+  const int32_t* pair_targets;       /* the (QBX target, center) pairs of each box's */
+  const int32_t* pair_centers;       /*   centers: tree target index, center index */
 } qbxfmm_transpose_index;
 
 #ifdef __cplusplus

@@ -141,7 +141,7 @@ int qbxfmm_eval_target_specific_qbx_locals(const qbxfmm_plan* plan, const void* 
  * stage of the apply; `plan` is the APPLY's plan (its centers, lists and sources),
  * `index` its reversed lists.  center_mpoles: [ncenters][nrhs][ncoeff(qbx_order)]
  * complex128.  Each output has one writer (no atomics).  QBXFMM_ERR_UNSUPPORTED for
- * other kernels, the mixed-precision form, per-level orders, qbx_order > 14 or
+ * other kernels, the mixed-precision form, per-level orders, qbx_order > 8 or
  * fmm_order > 21. */
 
 /* transpose of eval_qbx_expansions (fmm.py:358-389): target_values [nrhs][ntargets]
@@ -162,12 +162,14 @@ int qbxfmm_transpose_translate_box_multipoles_to_qbx_local(const qbxfmm_plan* pl
                                                            const void* center_mpoles,
                                                            void* locals, int32_t* error_word,
                                                            void* stream);
-/* transpose of form_global_qbx_locals (fmm.py:231-265): adds each center multipole,
- * evaluated at the sources of the boxes in its box's list 1, into
- * source_values [nrhs][nsources] (tree source order) */
+/* transpose of form_global_qbx_locals (fmm.py:231-265) with eval_qbx_expansions:
+ * adds, for every (QBX target, center) pair, the target's value times the truncated
+ * expansion entry (the target-specific form) into the values of the sources of the
+ * boxes in the center box's list 1.  target_values: [nrhs][ntargets] tree order;
+ * source_values: [nrhs][nsources] tree source order */
 int qbxfmm_transpose_form_global_qbx_locals(const qbxfmm_plan* plan,
                                             const qbxfmm_transpose_index* index,
-                                            const void* center_mpoles, void* source_values,
+                                            const void* target_values, void* source_values,
                                             int32_t* error_word, void* stream);
 
 /* The whole transpose K^T r in one call: `plan` the apply's plan, `transposed` the

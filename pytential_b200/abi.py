@@ -128,7 +128,8 @@ class QBXFMMTransposeIndex(ctypes.Structure):
     _fields_ = [("ncenter_boxes", _i32), ("center_boxes", _pi), ("box_center_starts", _pi),
                 ("box_centers", _pi), ("nlist3_rows", _i32), ("list3_rows", _pi),
                 ("list3_rev_starts", _pi), ("list3_rev_lists", _pi), ("nlist1_rows", _i32),
-                ("list1_rows", _pi), ("list1_rev_starts", _pi), ("list1_rev_lists", _pi)]
+                ("list1_rows", _pi), ("list1_rev_starts", _pi), ("list1_rev_lists", _pi),
+                ("box_pair_starts", _pi), ("pair_targets", _pi), ("pair_centers", _pi)]
 
 
 class QBXFMMWorkspace(ctypes.Structure):

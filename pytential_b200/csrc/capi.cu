@@ -1302,8 +1302,8 @@ int transpose_ok(const qbxfmm_plan* p)
   if (p->mixed || level_orders_on(p))
     return fail(QBXFMM_ERR_UNSUPPORTED,
                 "the transposed apply runs in FP64 with one FMM order");
-  if (p->kern.qbx_order > 14 || p->kern.fmm_order > 21)
-    return fail(QBXFMM_ERR_UNSUPPORTED, "the transposed apply takes qbx_order <= 14, fmm_order <= 21");
+  if (p->kern.qbx_order > 8 || p->kern.fmm_order > 21)
+    return fail(QBXFMM_ERR_UNSUPPORTED, "the transposed apply takes qbx_order <= 8, fmm_order <= 21");
   return QBXFMM_OK;
 }
 
@@ -1350,13 +1350,13 @@ int qbxfmm_transpose_translate_box_multipoles_to_qbx_local(const qbxfmm_plan* p,
 }
 
 int qbxfmm_transpose_form_global_qbx_locals(const qbxfmm_plan* p, const qbxfmm_transpose_index* ix,
-                                            const void* center_mpoles, void* source_values,
+                                            const void* target_values, void* source_values,
                                             int32_t* err, void* stream)
 {
   if (int rc = transpose_ok(p)) return rc;
-  if (!ix || !center_mpoles || !source_values) return fail(QBXFMM_ERR_ARG, "null argument");
-  QBX_TRY(launch_tr_p2qbxl(p->geo, *ix, p->kern.qbx_order, p->kern.nrhs,
-                           (const double2*)center_mpoles, (double*)source_values, err, S(stream)),
+  if (!ix || !target_values || !source_values) return fail(QBXFMM_ERR_ARG, "null argument");
+  QBX_TRY(launch_tr_p2qbxl(p->geo, *ix, p->kern.qbx_order, p->kern.nrhs, p->sc.cq,
+                           (const double*)target_values, (double*)source_values, err, S(stream)),
           "transpose_form_global_qbx_locals");
   return QBXFMM_OK;
 }
@@ -1429,7 +1429,7 @@ int qbxfmm_apply_transpose(const qbxfmm_plan* p, const qbxfmm_plan* d,
                                                                   ws->error_word, s2));
   QBX_CUDA_STEP(cudaEventRecord(d->ev_p2l, side2), "apply_transpose: P2L event");
   QBX_STEP(qbxfmm_eval_direct(d, strengths, ws->pot_nonqbx, ws->error_word, s1));
-  QBX_STEP(qbxfmm_transpose_form_global_qbx_locals(p, ix, center_mpoles, ws->pot_nonqbx,
+  QBX_STEP(qbxfmm_transpose_form_global_qbx_locals(p, ix, target_values, ws->pot_nonqbx,
                                                    ws->error_word, s1));
   QBX_STEP(qbxfmm_form_multipoles(d, strengths, ws->mpoles, stream));
   QBX_STEP(qbxfmm_transpose_translate_box_local_to_qbx_local(p, ix, center_mpoles, ws->mpoles,

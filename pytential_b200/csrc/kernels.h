@@ -196,7 +196,7 @@ cudaError_t launch_tr_m2qbxl(const qbxfmm_geometry& g, const qbxfmm_transpose_in
                              int q, int nrhs, const double2* cmp, double2* locals, int32_t* err,
                              cudaStream_t st);
 cudaError_t launch_tr_p2qbxl(const qbxfmm_geometry& g, const qbxfmm_transpose_index& ix, int q,
-                             int nrhs, const double2* cmp, double* vals, int32_t* err,
+                             int nrhs, double cq, const double* tvals, double* vals, int32_t* err,
                              cudaStream_t st);
 
 // per-level FMM orders: zero the coefficients of boxes [b0, b1) above their level's order

@@ -13,9 +13,10 @@
 //   k_tr_m2qbxl   transpose of M2QBXL (fmm.py:267-312): per box s, the M2L of the
 //                 center multipoles of every center box whose list 3 holds s into
 //                 the local of s
-//   k_tr_p2qbxl   transpose of P2QBXL (fmm.py:231-265): per source box s, the center
-//                 multipoles of every center box whose list 1 holds s evaluated at
-//                 the sources of s (M2P)
+//   k_tr_tsqbx    transpose of P2QBXL (fmm.py:231-265): per source box s, the
+//                 (target, center) pairs of every center box whose list 1 holds s,
+//                 evaluated at the sources of s in the target-specific form (the
+//                 Legendre sum of the truncated expansion, symmetric in the roles)
 //
 // Each output (a box expansion, a source value) has one writer: the kernels gather
 // over the reversed lists of qbxfmm_transpose_index, so results do not depend on
@@ -29,7 +30,6 @@ namespace qbx {
 namespace {
 
 constexpr int NT = 128;
-constexpr int TR_CB = 32;     // centers staged per batch in k_tr_p2qbxl
 
 QBX_D bool box_ok(const qbxfmm_geometry& g, int b, int32_t* err)
 {
@@ -156,14 +156,21 @@ k_tr_l2qbxl(qbxfmm_geometry g, qbxfmm_transpose_index ix, int p, int q, int ncf,
 
 // L_j^i += (-1)^j (rho_s / rho_c)^j / rho_c sum_{k <= q, |l| <= k} Mc_k^l S_{k+j}^{l+i}(d),
 // d = (box center - center) / rho_c: the entries of M2QBXL with the roles exchanged.
+// Batches of TR_MB centers per barrier: their S tables (order p + q, one task per
+// (center, column m)), multipoles and (-1)^j ratio^j / rho_c factors in shared memory.
+constexpr int TR_MB = 8;
+
 __global__ void __launch_bounds__(NT)
 k_tr_m2qbxl(qbxfmm_geometry g, qbxfmm_transpose_index ix, int p, int q, int ncf, int ncq,
             int nrhs, const double2* __restrict__ cmp, double2* __restrict__ locals, int32_t* err)
 {
   extern __shared__ double2 smem2[];
   const int nS = idx3(p + q + 1, 0);
-  double2* S = smem2;                 // [nS] S table of order p + q
-  double2* Min = smem2 + nS;          // [ncq]
+  double2* S = smem2;                                   // [TR_MB][nS]
+  double2* Min = S + TR_MB * nS;                        // [TR_MB][ncq]
+  double* fac = reinterpret_cast<double*>(Min + TR_MB * ncq);   // [TR_MB][p + 1]
+  __shared__ double s_d[TR_MB][3];
+  __shared__ int s_ctr[TR_MB];
   int s = ix.list3_rows[blockIdx.x];
   int r = blockIdx.y;
   if (!box_ok(g, s, err)) return;
@@ -174,35 +181,65 @@ k_tr_m2qbxl(qbxfmm_geometry g, qbxfmm_transpose_index ix, int p, int q, int ncf,
   for (int e = ix.list3_rev_starts[blockIdx.x]; e < ix.list3_rev_starts[blockIdx.x + 1]; ++e) {
     int b = ix.list3_rev_lists[e];
     if (!box_ok(g, b, err)) continue;
-    for (int k = ix.box_center_starts[b]; k < ix.box_center_starts[b + 1]; ++k) {
-      int ctr = ix.box_centers[k];
-      bool ok = center_ok(g, ctr, err);
-      // a bad center contributes nothing: a unit vector for the table, zero multipole
-      double cc[3] = {cs[0] - 1.0, cs[1], cs[2]};
-      double rho_c = 1.0;
-      if (ok) {
-        load_point<3>(g.centers, g.ncenters, ctr, cc);
-        rho_c = g.expansion_radii[ctr];
+    int k0 = ix.box_center_starts[b], k1 = ix.box_center_starts[b + 1];
+    for (int kb = k0; kb < k1; kb += TR_MB) {
+      int nb = min(TR_MB, k1 - kb);
+      __syncthreads();
+      if (threadIdx.x < nb) {
+        int ctr = ix.box_centers[kb + threadIdx.x];
+        bool ok = center_ok(g, ctr, err);
+        // a bad center contributes nothing: a unit vector for its table, zero factors
+        double cc[3] = {cs[0] - 1.0, cs[1], cs[2]};
+        double rho_c = 1.0;
+        if (ok) {
+          load_point<3>(g.centers, g.ncenters, ctr, cc);
+          rho_c = g.expansion_radii[ctr];
+        }
+        s_ctr[threadIdx.x] = ok ? ctr : -1;
+        for (int d = 0; d < 3; ++d) s_d[threadIdx.x][d] = (cs[d] - cc[d]) / rho_c;
+        double ratio = rho_s / rho_c, f = ok ? 1.0 / rho_c : 0.0;
+        for (int j = 0; j <= p; ++j, f *= -ratio) fac[threadIdx.x * (p + 1) + j] = f;
       }
       __syncthreads();
-      sh3_S_table(p + q, (cs[0] - cc[0]) / rho_c, (cs[1] - cc[1]) / rho_c,
-                  (cs[2] - cc[2]) / rho_c, S, threadIdx.x, NT);
-      for (int i = threadIdx.x; i < ncq; i += NT)
-        Min[i] = ok ? cmp[((size_t)ctr * nrhs + r) * ncq + i] : c2(0.0);
+      for (int w = threadIdx.x; w < nb * (p + q + 1); w += NT) {
+        int ci = w / (p + q + 1), m = w - ci * (p + q + 1);
+        double x = s_d[ci][0], y = s_d[ci][1], z = s_d[ci][2];
+        double rinv2 = 1.0 / (x * x + y * y + z * z);
+        double2 a = c2(sqrt(rinv2));
+        for (int jj = 1; jj <= m; ++jj) a = cscale((2.0 * jj - 1) * rinv2, cmul(a, c2(x, y)));
+        double2* T = S + ci * nS;
+        T[idx3(m, m)] = a;
+        double2 prev = c2(0.0);
+        for (int n = m + 1; n <= p + q; ++n) {
+          double2 bb = cscale(rinv2, csub(cscale((2.0 * n - 1) * z, a),
+                                          cscale((double)(n + m - 1) * (n - m - 1), prev)));
+          T[idx3(n, m)] = bb;
+          prev = a;
+          a = bb;
+        }
+      }
+      for (int w = threadIdx.x; w < nb * ncq; w += NT) {
+        int ci = w / ncq, i = w - ci * ncq;
+        int ctr = s_ctr[ci];
+        Min[w] = ctr >= 0 ? cmp[((size_t)ctr * nrhs + r) * ncq + i] : c2(0.0);
+      }
       __syncthreads();
-      double ratio = rho_s / rho_c;
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
         int o = threadIdx.x + h * NT;
         if (o >= ncf) break;
         int j, ii;
         decode3(o, j, ii);
-        double2 v = c2(0.0);
-        for (int kk = 0; kk <= q; ++kk)
-          for (int l = -kk; l <= kk; ++l) v = cfma(sh3_get(Min, kk, l), sh3_get(S, kk + j, l + ii), v);
-        double rj = 1.0 / rho_c;
-        for (int t = 0; t < j; ++t) rj *= ratio;
-        acc[h] = caxpy((j & 1) ? -rj : rj, v, acc[h]);
+        double2 a = acc[h];
+        for (int ci = 0; ci < nb; ++ci) {
+          const double2* M = Min + ci * ncq;
+          const double2* T = S + ci * nS;
+          double2 v = c2(0.0);
+          for (int kk = 0; kk <= q; ++kk)
+            for (int l = -kk; l <= kk; ++l) v = cfma(sh3_get(M, kk, l), sh3_get(T, kk + j, l + ii), v);
+          a = caxpy(fac[ci * (p + 1) + j], v, a);
+        }
+        acc[h] = a;
       }
     }
   }
@@ -216,17 +253,25 @@ k_tr_m2qbxl(qbxfmm_geometry g, qbxfmm_transpose_index ix, int p, int q, int ncf,
 
 // }}}
 
-// {{{ P2QBXL^T: center multipoles evaluated at the list-1 sources (M2P)
+// {{{ P2QBXL^T: the list-1 sources' values from the QBX targets (target-specific form)
 
-// value += sum_{n <= q} w_m Re(Mc_n^m S_n^m((y - c) / rho)) / rho, w_0 = 1, w_{m>0} = 2,
-// the S entries by the column recurrence, one thread per source.
+// For a QBX target t with center c and a source y in the list 1 of the center's box,
+// a = t - c, b = y - c: the P2QBXL + QBXL2P entry (the QBX local of order Q formed
+// from y, evaluated at t) is sum_{n <= Q} |a|^n / |b|^{n+1} P_n(cos g),
+// cos g = a.b / (|a||b|) -- symmetric in the roles, so the transpose adds
+// cq r_t times it to the value at y.  Equal to evaluating the center multipoles of
+// k_tr_qbxl2p at y (the addition theorem), without forming them.  CTA = one source
+// box of some center box's list 1; each thread holds up to TR_KS of its sources;
+// the (target, center) pairs of the boxes that list it are staged TR_PB at a time.
+constexpr int TR_KS = 4;
+constexpr int TR_PB = NT;
+
+template <int Q>
 __global__ void __launch_bounds__(NT)
-k_tr_p2qbxl(qbxfmm_geometry g, qbxfmm_transpose_index ix, int q, int ncq, int nrhs,
-            const double2* __restrict__ cmp, double* __restrict__ vals, int32_t* err)
+k_tr_tsqbx(qbxfmm_geometry g, qbxfmm_transpose_index ix, int nrhs, double cq,
+           const double* __restrict__ tvals, double* __restrict__ vals, int32_t* err)
 {
-  extern __shared__ double2 smem2[];
-  double2* Ms = smem2;                                   // [TR_CB][ncq]
-  __shared__ double s_c[TR_CB][4];                       // center, 1 / rho
+  __shared__ double s_c[3][TR_PB], s_ah[3][TR_PB], s_al[TR_PB], s_w[TR_PB];
   int s = ix.list1_rows[blockIdx.x];
   int r = blockIdx.y;
   if (!box_ok(g, s, err)) return;
@@ -235,68 +280,78 @@ k_tr_p2qbxl(qbxfmm_geometry g, qbxfmm_transpose_index ix, int q, int ncq, int nr
     report(err, QBX_DEVERR_BAD_BOX);
     return;
   }
-  for (int j0 = 0; j0 < ns; j0 += NT) {
-    int j = s0 + j0 + threadIdx.x;
-    bool active = j0 + threadIdx.x < ns;
-    double y[3] = {0.0, 0.0, 0.0};
-    if (active) load_point<3>(g.sources, g.nsources, j, y);
-    double acc = 0.0;
+  const double* tv = tvals + (size_t)r * g.ntargets;
+  for (int g0 = 0; g0 < ns; g0 += NT * TR_KS) {
+    double y[TR_KS][3], acc[TR_KS];
+#pragma unroll
+    for (int k = 0; k < TR_KS; ++k) {
+      int jj = g0 + threadIdx.x + k * NT;
+      acc[k] = 0.0;
+      if (jj < ns) load_point<3>(g.sources, g.nsources, s0 + jj, y[k]);
+      else y[k][0] = y[k][1] = y[k][2] = 0.0;
+    }
     for (int e = ix.list1_rev_starts[blockIdx.x]; e < ix.list1_rev_starts[blockIdx.x + 1]; ++e) {
       int b = ix.list1_rev_lists[e];
       if (!box_ok(g, b, err)) continue;
-      int k0 = ix.box_center_starts[b], k1 = ix.box_center_starts[b + 1];
-      for (int kb = k0; kb < k1; kb += TR_CB) {
-        int nb = min(TR_CB, k1 - kb);
+      int p0 = ix.box_pair_starts[b], p1 = ix.box_pair_starts[b + 1];
+      for (int pb = p0; pb < p1; pb += TR_PB) {
+        int np = min(TR_PB, p1 - pb);
         __syncthreads();
-        for (int w = threadIdx.x; w < nb * ncq; w += NT) {
-          int ci = w / ncq, i = w - ci * ncq;
-          int ctr = ix.box_centers[kb + ci];
-          Ms[w] = center_ok(g, ctr, err) ? cmp[((size_t)ctr * nrhs + r) * ncq + i] : c2(0.0);
-        }
-        if (threadIdx.x < nb) {
-          int ctr = ix.box_centers[kb + threadIdx.x];
-          double cc[3] = {0.0, 0.0, 0.0};
-          double rinv = 0.0;
-          if ((unsigned)ctr < (unsigned)g.ncenters) {
+        if (threadIdx.x < np) {
+          int t = ix.pair_targets[pb + threadIdx.x], ctr = ix.pair_centers[pb + threadIdx.x];
+          double w = 0.0, cc[3] = {0.0, 0.0, 0.0}, a[3] = {0.0, 0.0, 0.0};
+          if ((unsigned)t < (unsigned)g.ntargets && center_ok(g, ctr, err)) {
+            double x[3];
             load_point<3>(g.centers, g.ncenters, ctr, cc);
-            rinv = 1.0 / g.expansion_radii[ctr];
+            load_point<3>(g.targets, g.ntargets, t, x);
+            for (int d = 0; d < 3; ++d) a[d] = x[d] - cc[d];
+            w = cq * tv[t];
+          } else if ((unsigned)t >= (unsigned)g.ntargets) {
+            report(err, QBX_DEVERR_BAD_CENTER);
           }
-          s_c[threadIdx.x][0] = cc[0];
-          s_c[threadIdx.x][1] = cc[1];
-          s_c[threadIdx.x][2] = cc[2];
-          s_c[threadIdx.x][3] = rinv;
+          double al = sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+          double ainv = al > 0.0 ? 1.0 / al : 0.0;
+          for (int d = 0; d < 3; ++d) {
+            s_c[d][threadIdx.x] = cc[d];
+            s_ah[d][threadIdx.x] = a[d] * ainv;
+          }
+          s_al[threadIdx.x] = al;
+          s_w[threadIdx.x] = w;
         }
         __syncthreads();
-        if (!active) continue;
-        for (int ci = 0; ci < nb; ++ci) {
-          double rinv = s_c[ci][3];
-          if (rinv == 0.0) continue;
-          double ux = (y[0] - s_c[ci][0]) * rinv, uy = (y[1] - s_c[ci][1]) * rinv,
-                 uz = (y[2] - s_c[ci][2]) * rinv;
-          double rinv2 = 1.0 / (ux * ux + uy * uy + uz * uz);
-          const double2* M = Ms + ci * ncq;
-          double2 smm = c2(sqrt(rinv2));
-          double v = 0.0;
-          for (int m = 0; m <= q; ++m) {
-            if (m > 0) smm = cscale((2.0 * m - 1) * rinv2, cmul(smm, c2(ux, uy)));
-            double2 a = smm, prev = c2(0.0);
-            double w = m ? 2.0 : 1.0;
-            for (int n = m; n <= q; ++n) {
-              if (n > m) {
-                double2 bb = cscale(rinv2, csub(cscale((2.0 * n - 1) * uz, a),
-                                                cscale((double)(n + m - 1) * (n - m - 1), prev)));
-                prev = a;
-                a = bb;
-              }
-              double2 mv = M[idx3(n, m)];
-              v += w * (mv.x * a.x - mv.y * a.y);
+        for (int pi = 0; pi < np; ++pi) {
+          double w = s_w[pi];
+          if (w == 0.0) continue;
+          double cx = s_c[0][pi], cy = s_c[1][pi], cz = s_c[2][pi];
+          double hx = s_ah[0][pi], hy = s_ah[1][pi], hz = s_ah[2][pi], al = s_al[pi];
+#pragma unroll
+          for (int k = 0; k < TR_KS; ++k) {
+            if (g0 + threadIdx.x + k * NT >= ns) break;
+            double b0 = y[k][0] - cx, b1 = y[k][1] - cy, b2 = y[k][2] - cz;
+            double binv = rsqrt(b0 * b0 + b1 * b1 + b2 * b2);
+            double cg = (hx * b0 + hy * b1 + hz * b2) * binv;
+            double ratio = al * binv;
+            double pm1 = 1.0, pm2 = 0.0, rn = binv, sum = 0.0;
+#pragma unroll
+            for (int n = 0; n <= Q; ++n) {
+              double pn = n == 0 ? 1.0
+                        : n == 1 ? cg
+                                 : ((2.0 * n - 1) * cg * pm1 - (n - 1.0) * pm2) * (1.0 / n);
+              sum = fma(rn, pn, sum);
+              pm2 = pm1;
+              pm1 = pn;
+              rn *= ratio;
             }
+            acc[k] = fma(w, sum, acc[k]);
           }
-          acc += v * rinv;
         }
       }
     }
-    if (active) vals[(size_t)r * g.nsources + j] += acc;
+#pragma unroll
+    for (int k = 0; k < TR_KS; ++k) {
+      int jj = g0 + threadIdx.x + k * NT;
+      if (jj < ns) vals[(size_t)r * g.nsources + s0 + jj] += acc[k];
+    }
   }
 }
 
@@ -331,23 +386,41 @@ cudaError_t launch_tr_m2qbxl(const qbxfmm_geometry& g, const qbxfmm_transpose_in
 {
   if (ix.nlist3_rows == 0) return cudaSuccess;
   int ncf = idx3(p + 1, 0), ncq = idx3(q + 1, 0), nS = idx3(p + q + 1, 0);
-  k_tr_m2qbxl<<<dim3(ix.nlist3_rows, nrhs), NT, (nS + ncq) * sizeof(double2), st>>>(
-      g, ix, p, q, ncf, ncq, nrhs, cmp, locals, err);
+  size_t sh = (size_t)TR_MB * (nS + ncq) * sizeof(double2) + (size_t)TR_MB * (p + 1) * sizeof(double);
+  cudaError_t e = cudaFuncSetAttribute(k_tr_m2qbxl, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)sh);
+  if (e != cudaSuccess) return e;
+  k_tr_m2qbxl<<<dim3(ix.nlist3_rows, nrhs), NT, sh, st>>>(g, ix, p, q, ncf, ncq, nrhs, cmp, locals,
+                                                          err);
+  return cudaGetLastError();
+}
+
+template <int Q>
+static cudaError_t tr_tsqbx_q(const qbxfmm_geometry& g, const qbxfmm_transpose_index& ix,
+                              int nrhs, double cq, const double* tvals, double* vals, int32_t* err,
+                              cudaStream_t st)
+{
+  k_tr_tsqbx<Q><<<dim3(ix.nlist1_rows, nrhs), NT, 0, st>>>(g, ix, nrhs, cq, tvals, vals, err);
   return cudaGetLastError();
 }
 
 cudaError_t launch_tr_p2qbxl(const qbxfmm_geometry& g, const qbxfmm_transpose_index& ix, int q,
-                             int nrhs, const double2* cmp, double* vals, int32_t* err,
+                             int nrhs, double cq, const double* tvals, double* vals, int32_t* err,
                              cudaStream_t st)
 {
   if (ix.nlist1_rows == 0) return cudaSuccess;
-  int ncq = idx3(q + 1, 0);
-  size_t sh = (size_t)TR_CB * ncq * sizeof(double2);
-  cudaError_t e = cudaFuncSetAttribute(k_tr_p2qbxl, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)sh);
-  if (e != cudaSuccess) return e;
-  k_tr_p2qbxl<<<dim3(ix.nlist1_rows, nrhs), NT, sh, st>>>(g, ix, q, ncq, nrhs, cmp, vals, err);
-  return cudaGetLastError();
+  switch (q) {
+    case 0: return tr_tsqbx_q<0>(g, ix, nrhs, cq, tvals, vals, err, st);
+    case 1: return tr_tsqbx_q<1>(g, ix, nrhs, cq, tvals, vals, err, st);
+    case 2: return tr_tsqbx_q<2>(g, ix, nrhs, cq, tvals, vals, err, st);
+    case 3: return tr_tsqbx_q<3>(g, ix, nrhs, cq, tvals, vals, err, st);
+    case 4: return tr_tsqbx_q<4>(g, ix, nrhs, cq, tvals, vals, err, st);
+    case 5: return tr_tsqbx_q<5>(g, ix, nrhs, cq, tvals, vals, err, st);
+    case 6: return tr_tsqbx_q<6>(g, ix, nrhs, cq, tvals, vals, err, st);
+    case 7: return tr_tsqbx_q<7>(g, ix, nrhs, cq, tvals, vals, err, st);
+    case 8: return tr_tsqbx_q<8>(g, ix, nrhs, cq, tvals, vals, err, st);
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 // }}}

@@ -25,11 +25,12 @@ Pieces:
   (P2M, M2M, M2L, M2P, P2L, L2L, L2P, P2P) are the library's own stage entries.
 * :func:`transpose_index` -- the reversed lists of the QBX stages by box id: the
   global centers of each box, the boxes whose list 3 holds a box, the boxes whose
-  list 1 holds a source box.
+  list 1 holds a source box, the (target, center) pairs of each box's centers.
 * the four transposed QBX stages (``qbxfmm_transpose_*`` in the C ABI): QBXL2P^T
   (order-q multipoles of the targets' values at the centers), L2QBXL^T (center
   multipole -> multipole of the center's box), M2QBXL^T (center multipole -> local
-  of each list-3 box), P2QBXL^T (center multipole evaluated at the list-1 sources).
+  of each list-3 box), and P2QBXL^T with QBXL2P^T (each QBX target's value times the
+  truncated expansion entry at the list-1 sources, the target-specific form).
 """
 
 from __future__ import annotations
@@ -216,6 +217,9 @@ class TransposeIndex:
     list1_rows: np.ndarray          # source boxes in some center box's list 1
     list1_rev_starts: np.ndarray
     list1_rev_lists: np.ndarray     # center boxes whose list 1 holds the row box
+    box_pair_starts: np.ndarray     # [nboxes + 1] into the pair arrays
+    pair_targets: np.ndarray        # (QBX target, center) pairs of each box's centers:
+    pair_centers: np.ndarray        #   tree target index, center index
 
 
 def transpose_index(geo) -> TransposeIndex:
@@ -248,8 +252,19 @@ def transpose_index(geo) -> TransposeIndex:
 
     l3r, l3s, l3l = rev(trav.from_sep_smaller_starts, trav.from_sep_smaller_lists)
     l1r, l1s, l1l = rev(trav.neighbor_source_boxes_starts, trav.neighbor_source_boxes_lists)
+    # the (target, center) pairs of the centers in box order
+    ctt = geo.center_to_tree_targets()
+    cst = np.asarray(ctt.starts, np.int64)
+    ntc = cst[box_centers.astype(np.int64) + 1] - cst[box_centers.astype(np.int64)]
+    pair_centers = np.repeat(box_centers.astype(np.int64), ntc)
+    first = np.repeat(cst[box_centers.astype(np.int64)], ntc)
+    within = np.arange(len(pair_centers)) - np.repeat(np.cumsum(ntc) - ntc, ntc)
+    pair_targets = np.asarray(ctt.lists, np.int64)[first + within]
+    csum = np.concatenate([[0], np.cumsum(ntc)])
+    box_pair_starts = csum[box_center_starts]
     return TransposeIndex(center_boxes, box_center_starts.astype(np.int32), box_centers,
-                          l3r, l3s, l3l, l1r, l1s, l1l)
+                          l3r, l3s, l3l, l1r, l1s, l1l, box_pair_starts.astype(np.int32),
+                          pair_targets.astype(np.int32), pair_centers.astype(np.int32))
 
 
 class QBXTransposeApply:
@@ -313,7 +328,8 @@ class QBXTransposeApply:
             len(ix.center_boxes), ptr("center_boxes"), ptr("box_center_starts"),
             ptr("box_centers"), len(ix.list3_rows), ptr("list3_rows"), ptr("list3_rev_starts"),
             ptr("list3_rev_lists"), len(ix.list1_rows), ptr("list1_rows"),
-            ptr("list1_rev_starts"), ptr("list1_rev_lists"))
+            ptr("list1_rev_starts"), ptr("list1_rev_lists"), ptr("box_pair_starts"),
+            ptr("pair_targets"), ptr("pair_centers"))
         sc = apply.dgeo.scalars
         host = apply.dgeo.host_arrays
         nt, nc = sc["ntargets"], sc["ncenters"]
@@ -399,7 +415,8 @@ class QBXTransposeApply:
              vp(lo.data_ptr()))
         W.refine_locals(None, None, None, lo)
         pot += W.eval_locals(None, None, None, lo)
-        call("qbxfmm_transpose_form_global_qbx_locals", ix, vp(cm.data_ptr()), vp(pot.data_ptr()))
+        call("qbxfmm_transpose_form_global_qbx_locals", ix, vp(r_tree.data_ptr()),
+             vp(pot.data_ptr()))
         return self._to_user(W.assemble_potentials(pot, W.full_output_zeros()))
 
     def __call__(self, r):

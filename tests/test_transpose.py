@@ -98,6 +98,15 @@ def test_transpose_index(case):
         want = {(int(s), int(b)) for b in has_c
                 for s in l0[s0[tb_of[b]]:s0[tb_of[b] + 1]]}
         assert _csr_pairs(st, li, rows) == want
+    # the (target, center) pairs of each box's centers
+    ctt = geo.center_to_tree_targets()
+    for b in ix.center_boxes:
+        p0, p1 = ix.box_pair_starts[b], ix.box_pair_starts[b + 1]
+        want = {(int(t), int(c)) for c in ix.box_centers[ix.box_center_starts[b]:
+                                                         ix.box_center_starts[b + 1]]
+                for t in ctt.lists[ctt.starts[c]:ctt.starts[c + 1]]}
+        assert set(zip(ix.pair_targets[p0:p1].tolist(), ix.pair_centers[p0:p1].tolist())) == want
+    assert ix.box_pair_starts[-1] == len(ctt.lists)
 
 
 def test_checker_transpose_dot_products(case):
