@@ -25,6 +25,8 @@
 #include "laplace.cuh"
 #include "kernels.h"
 
+#include <algorithm>
+
 namespace qbx {
 
 namespace {
@@ -93,37 +95,83 @@ k_tr_qbxl2p(qbxfmm_geometry g, int q, int ncq, int nrhs, double cq,
 // {{{ L2QBXL^T: center multipoles into the multipole of their box (M2M from the center)
 
 // M_n^m += sum_{k <= min(n, q)} (rho_c / rho_b)^k sum_l Mc_k^l conj(R_{n-k}^{m-l}(d)),
-// d = (center - box center) / rho_b: the entries of the box-to-center L2L.
+// d = (center - box center) / rho_b: the entries of the box-to-center L2L.  Batches of
+// mb centers per barrier (one table column task per thread): their R tables (rows
+// 0..p, columns -q..p+q: the sums reach m - l up to p + q, zero beyond the row) and
+// multipoles (rows 0..q, columns -q..q) expanded into zero-padded dense arrays, so
+// the inner sums are branch-free.
 __global__ void __launch_bounds__(NT)
 k_tr_l2qbxl(qbxfmm_geometry g, qbxfmm_transpose_index ix, int p, int q, int ncf, int ncq,
-            int nrhs, const double2* __restrict__ cmp, double2* __restrict__ mpoles, int32_t* err)
+            int nrhs, int mb, const double2* __restrict__ cmp, double2* __restrict__ mpoles,
+            int32_t* err)
 {
   extern __shared__ double2 smem2[];
-  double2* tab = smem2;               // [ncf] R table of order p
-  double2* Min = smem2 + ncf;         // [ncq] the center multipole
+  const int RW = p + 2 * q + 1, RS = (p + 1) * RW;    // R table: rows 0..p, columns -q..p+q
+  const int MW = 2 * q + 1, MS = (q + 1) * MW;        // center multipole
+  double2* R = smem2;                                 // [mb][RS]
+  double2* Mp = R + (size_t)mb * RS;                  // [mb][MS]
+  double* rk = reinterpret_cast<double*>(Mp + (size_t)mb * MS);   // [mb][q + 1]
+  double* sd = rk + (size_t)mb * (q + 1);                          // [mb][3]
+  int* sctr = reinterpret_cast<int*>(sd + (size_t)mb * 3);         // [mb]
   int b = ix.center_boxes[blockIdx.x];
   int r = blockIdx.y;
   if (!box_ok(g, b, err)) return;
   double rho_b = level_width(g, g.box_levels[b]);
   double cb[3];
   load_point<3>(g.box_centers, g.nboxes, b, cb);
+  // the entries outside |m| <= n stay zero for every center
+  for (int i = threadIdx.x; i < mb * (RS + MS); i += NT) R[i] = c2(0.0);
   double2 acc[2] = {c2(0.0), c2(0.0)};
-  for (int k = ix.box_center_starts[b]; k < ix.box_center_starts[b + 1]; ++k) {
-    int ctr = ix.box_centers[k];
-    bool ok = center_ok(g, ctr, err);
-    double cc[3] = {cb[0], cb[1], cb[2]};
-    double rho_c = rho_b;
-    if (ok) {
-      load_point<3>(g.centers, g.ncenters, ctr, cc);
-      rho_c = g.expansion_radii[ctr];
+  int k0 = ix.box_center_starts[b], k1 = ix.box_center_starts[b + 1];
+  for (int kb = k0; kb < k1; kb += mb) {
+    int nb = min(mb, k1 - kb);
+    __syncthreads();
+    if (threadIdx.x < nb) {
+      int ctr = ix.box_centers[kb + threadIdx.x];
+      bool ok = center_ok(g, ctr, err);
+      double cc[3] = {cb[0], cb[1], cb[2]};
+      double rho_c = rho_b;
+      if (ok) {
+        load_point<3>(g.centers, g.ncenters, ctr, cc);
+        rho_c = g.expansion_radii[ctr];
+      }
+      sctr[threadIdx.x] = ok ? ctr : -1;
+      for (int d = 0; d < 3; ++d) sd[threadIdx.x * 3 + d] = (cc[d] - cb[d]) / rho_b;
+      double ratio = rho_c / rho_b, f = 1.0;
+      for (int kk = 0; kk <= q; ++kk, f *= ratio) rk[threadIdx.x * (q + 1) + kk] = f;
     }
     __syncthreads();
-    sh3_R_table(p, (cc[0] - cb[0]) / rho_b, (cc[1] - cb[1]) / rho_b, (cc[2] - cb[2]) / rho_b,
-                tab, threadIdx.x, NT);
-    for (int i = threadIdx.x; i < ncq; i += NT)
-      Min[i] = ok ? cmp[((size_t)ctr * nrhs + r) * ncq + i] : c2(0.0);
+    // R columns m = 0..p (negative columns down to -q by symmetry)
+    for (int w = threadIdx.x; w < nb * (p + 1); w += NT) {
+      int ci = w / (p + 1), m = w - ci * (p + 1);
+      double x = sd[ci * 3], y = sd[ci * 3 + 1], z = sd[ci * 3 + 2];
+      double r2 = x * x + y * y + z * z;
+      double2 a = c2(1.0);
+      for (int jj = 1; jj <= m; ++jj) a = cscale(0.5 * rcp(jj), cmul(a, c2(x, y)));
+      double2 prev = c2(0.0);
+      double2* T = R + (size_t)ci * RS + q;
+      for (int n = m; n <= p; ++n) {
+        if (n > m) {
+          double2 bb = cscale(rcp(n + m) * rcp(n - m),
+                              csub(cscale((2.0 * n - 1) * z, a), cscale(r2, prev)));
+          prev = a;
+          a = bb;
+        }
+        T[n * RW + m] = a;
+        if (m >= 1 && m <= q) T[n * RW - m] = (m & 1) ? c2(-a.x, a.y) : c2(a.x, -a.y);
+      }
+    }
+    for (int w = threadIdx.x; w < nb * ncq; w += NT) {
+      int ci = w / ncq, i = w - ci * ncq;
+      int ctr = sctr[ci];
+      int kk, l;
+      decode3(i, kk, l);
+      double2 v = ctr >= 0 ? cmp[((size_t)ctr * nrhs + r) * ncq + i] : c2(0.0);
+      double2* M = Mp + (size_t)ci * MS + q;
+      M[kk * MW + l] = v;
+      if (l > 0) M[kk * MW - l] = (l & 1) ? c2(-v.x, v.y) : c2(v.x, -v.y);
+    }
     __syncthreads();
-    double ratio = rho_c / rho_b;
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
       int o = threadIdx.x + h * NT;
@@ -131,14 +179,18 @@ k_tr_l2qbxl(qbxfmm_geometry g, qbxfmm_transpose_index ix, int p, int q, int ncf,
       int n, m;
       decode3(o, n, m);
       double2 a = acc[h];
-      double rk = 1.0;
       int kmax = n < q ? n : q;
-      for (int kk = 0; kk <= kmax; ++kk, rk *= ratio)
-        for (int l = -kk; l <= kk; ++l) {
-          int dm = m - l;
-          if (dm > n - kk || -dm > n - kk) continue;
-          a = cfmac(cscale(rk, sh3_get(Min, kk, l)), sh3_get(tab, n - kk, dm), a);
+      for (int ci = 0; ci < nb; ++ci) {
+        const double2* M = Mp + (size_t)ci * MS + q;
+        const double2* T = R + (size_t)ci * RS + q;
+        for (int kk = 0; kk <= kmax; ++kk) {
+          double2 v = c2(0.0);
+          const double2* mrow = M + kk * MW;
+          const double2* trow = T + (n - kk) * RW + m;
+          for (int l = -kk; l <= kk; ++l) v = cfmac(mrow[l], trow[-l], v);
+          a = caxpy(rk[ci * (q + 1) + kk], v, a);
         }
+      }
       acc[h] = a;
     }
   }
@@ -156,34 +208,37 @@ k_tr_l2qbxl(qbxfmm_geometry g, qbxfmm_transpose_index ix, int p, int q, int ncf,
 
 // L_j^i += (-1)^j (rho_s / rho_c)^j / rho_c sum_{k <= q, |l| <= k} Mc_k^l S_{k+j}^{l+i}(d),
 // d = (box center - center) / rho_c: the entries of M2QBXL with the roles exchanged.
-// Batches of TR_MB centers per barrier: their S tables (order p + q, one task per
-// (center, column m)), multipoles and (-1)^j ratio^j / rho_c factors in shared memory.
-constexpr int TR_MB = 8;
-
+// Batches of mb centers per barrier (one S column task per thread): their S tables
+// (rows 0..p+q, columns -q..p+q), multipoles (rows 0..q, columns -q..q) and
+// (-1)^j ratio^j / rho_c factors in zero-padded dense shared arrays, so the inner
+// sums are branch-free.
 __global__ void __launch_bounds__(NT)
 k_tr_m2qbxl(qbxfmm_geometry g, qbxfmm_transpose_index ix, int p, int q, int ncf, int ncq,
-            int nrhs, const double2* __restrict__ cmp, double2* __restrict__ locals, int32_t* err)
+            int nrhs, int mb, const double2* __restrict__ cmp, double2* __restrict__ locals,
+            int32_t* err)
 {
   extern __shared__ double2 smem2[];
-  const int nS = idx3(p + q + 1, 0);
-  double2* S = smem2;                                   // [TR_MB][nS]
-  double2* Min = S + TR_MB * nS;                        // [TR_MB][ncq]
-  double* fac = reinterpret_cast<double*>(Min + TR_MB * ncq);   // [TR_MB][p + 1]
-  __shared__ double s_d[TR_MB][3];
-  __shared__ int s_ctr[TR_MB];
+  const int SW = p + 2 * q + 1, SS = (p + q + 1) * SW;   // S: rows 0..p+q, columns -q..p+q
+  const int MW = 2 * q + 1, MS = (q + 1) * MW;
+  double2* S = smem2;                                    // [mb][SS]
+  double2* Mp = S + (size_t)mb * SS;                     // [mb][MS]
+  double* fac = reinterpret_cast<double*>(Mp + (size_t)mb * MS);   // [mb][p + 1]
+  double* sd = fac + (size_t)mb * (p + 1);                          // [mb][3]
+  int* sctr = reinterpret_cast<int*>(sd + (size_t)mb * 3);          // [mb]
   int s = ix.list3_rows[blockIdx.x];
   int r = blockIdx.y;
   if (!box_ok(g, s, err)) return;
   double rho_s = level_width(g, g.box_levels[s]);
   double cs[3];
   load_point<3>(g.box_centers, g.nboxes, s, cs);
+  for (int i = threadIdx.x; i < mb * (SS + MS); i += NT) S[i] = c2(0.0);
   double2 acc[2] = {c2(0.0), c2(0.0)};
   for (int e = ix.list3_rev_starts[blockIdx.x]; e < ix.list3_rev_starts[blockIdx.x + 1]; ++e) {
     int b = ix.list3_rev_lists[e];
     if (!box_ok(g, b, err)) continue;
     int k0 = ix.box_center_starts[b], k1 = ix.box_center_starts[b + 1];
-    for (int kb = k0; kb < k1; kb += TR_MB) {
-      int nb = min(TR_MB, k1 - kb);
+    for (int kb = k0; kb < k1; kb += mb) {
+      int nb = min(mb, k1 - kb);
       __syncthreads();
       if (threadIdx.x < nb) {
         int ctr = ix.box_centers[kb + threadIdx.x];
@@ -195,33 +250,40 @@ k_tr_m2qbxl(qbxfmm_geometry g, qbxfmm_transpose_index ix, int p, int q, int ncf,
           load_point<3>(g.centers, g.ncenters, ctr, cc);
           rho_c = g.expansion_radii[ctr];
         }
-        s_ctr[threadIdx.x] = ok ? ctr : -1;
-        for (int d = 0; d < 3; ++d) s_d[threadIdx.x][d] = (cs[d] - cc[d]) / rho_c;
+        sctr[threadIdx.x] = ok ? ctr : -1;
+        for (int d = 0; d < 3; ++d) sd[threadIdx.x * 3 + d] = (cs[d] - cc[d]) / rho_c;
         double ratio = rho_s / rho_c, f = ok ? 1.0 / rho_c : 0.0;
         for (int j = 0; j <= p; ++j, f *= -ratio) fac[threadIdx.x * (p + 1) + j] = f;
       }
       __syncthreads();
       for (int w = threadIdx.x; w < nb * (p + q + 1); w += NT) {
         int ci = w / (p + q + 1), m = w - ci * (p + q + 1);
-        double x = s_d[ci][0], y = s_d[ci][1], z = s_d[ci][2];
+        double x = sd[ci * 3], y = sd[ci * 3 + 1], z = sd[ci * 3 + 2];
         double rinv2 = 1.0 / (x * x + y * y + z * z);
         double2 a = c2(sqrt(rinv2));
         for (int jj = 1; jj <= m; ++jj) a = cscale((2.0 * jj - 1) * rinv2, cmul(a, c2(x, y)));
-        double2* T = S + ci * nS;
-        T[idx3(m, m)] = a;
         double2 prev = c2(0.0);
-        for (int n = m + 1; n <= p + q; ++n) {
-          double2 bb = cscale(rinv2, csub(cscale((2.0 * n - 1) * z, a),
-                                          cscale((double)(n + m - 1) * (n - m - 1), prev)));
-          T[idx3(n, m)] = bb;
-          prev = a;
-          a = bb;
+        double2* T = S + (size_t)ci * SS + q;
+        for (int n = m; n <= p + q; ++n) {
+          if (n > m) {
+            double2 bb = cscale(rinv2, csub(cscale((2.0 * n - 1) * z, a),
+                                            cscale((double)(n + m - 1) * (n - m - 1), prev)));
+            prev = a;
+            a = bb;
+          }
+          T[n * SW + m] = a;
+          if (m >= 1 && m <= q) T[n * SW - m] = (m & 1) ? c2(-a.x, a.y) : c2(a.x, -a.y);
         }
       }
       for (int w = threadIdx.x; w < nb * ncq; w += NT) {
         int ci = w / ncq, i = w - ci * ncq;
-        int ctr = s_ctr[ci];
-        Min[w] = ctr >= 0 ? cmp[((size_t)ctr * nrhs + r) * ncq + i] : c2(0.0);
+        int ctr = sctr[ci];
+        int kk, l;
+        decode3(i, kk, l);
+        double2 v = ctr >= 0 ? cmp[((size_t)ctr * nrhs + r) * ncq + i] : c2(0.0);
+        double2* M = Mp + (size_t)ci * MS + q;
+        M[kk * MW + l] = v;
+        if (l > 0) M[kk * MW - l] = (l & 1) ? c2(-v.x, v.y) : c2(v.x, -v.y);
       }
       __syncthreads();
 #pragma unroll
@@ -232,11 +294,14 @@ k_tr_m2qbxl(qbxfmm_geometry g, qbxfmm_transpose_index ix, int p, int q, int ncf,
         decode3(o, j, ii);
         double2 a = acc[h];
         for (int ci = 0; ci < nb; ++ci) {
-          const double2* M = Min + ci * ncq;
-          const double2* T = S + ci * nS;
+          const double2* M = Mp + (size_t)ci * MS + q;
+          const double2* T = S + (size_t)ci * SS + q;
           double2 v = c2(0.0);
-          for (int kk = 0; kk <= q; ++kk)
-            for (int l = -kk; l <= kk; ++l) v = cfma(sh3_get(M, kk, l), sh3_get(T, kk + j, l + ii), v);
+          for (int kk = 0; kk <= q; ++kk) {
+            const double2* mrow = M + kk * MW;
+            const double2* trow = T + (kk + j) * SW + ii;
+            for (int l = -kk; l <= kk; ++l) v = cfma(mrow[l], trow[l], v);
+          }
           a = caxpy(fac[ci * (p + 1) + j], v, a);
         }
         acc[h] = a;
@@ -375,8 +440,14 @@ cudaError_t launch_tr_l2qbxl(const qbxfmm_geometry& g, const qbxfmm_transpose_in
 {
   if (ix.ncenter_boxes == 0) return cudaSuccess;
   int ncf = idx3(p + 1, 0), ncq = idx3(q + 1, 0);
-  k_tr_l2qbxl<<<dim3(ix.ncenter_boxes, nrhs), NT, (ncf + ncq) * sizeof(double2), st>>>(
-      g, ix, p, q, ncf, ncq, nrhs, cmp, mpoles, err);
+  int mb = std::max(1, std::min(8, NT / (p + 1)));
+  size_t sh = (size_t)mb * ((p + 1) * (p + 2 * q + 1) + (q + 1) * (2 * q + 1)) * sizeof(double2) +
+              (size_t)mb * (q + 4) * sizeof(double) + (size_t)mb * sizeof(int);
+  cudaError_t e = cudaFuncSetAttribute(k_tr_l2qbxl, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)sh);
+  if (e != cudaSuccess) return e;
+  k_tr_l2qbxl<<<dim3(ix.ncenter_boxes, nrhs), NT, sh, st>>>(g, ix, p, q, ncf, ncq, nrhs, mb, cmp,
+                                                            mpoles, err);
   return cudaGetLastError();
 }
 
@@ -385,13 +456,15 @@ cudaError_t launch_tr_m2qbxl(const qbxfmm_geometry& g, const qbxfmm_transpose_in
                              cudaStream_t st)
 {
   if (ix.nlist3_rows == 0) return cudaSuccess;
-  int ncf = idx3(p + 1, 0), ncq = idx3(q + 1, 0), nS = idx3(p + q + 1, 0);
-  size_t sh = (size_t)TR_MB * (nS + ncq) * sizeof(double2) + (size_t)TR_MB * (p + 1) * sizeof(double);
+  int ncf = idx3(p + 1, 0), ncq = idx3(q + 1, 0);
+  int mb = std::max(1, std::min(8, NT / (p + q + 1)));
+  size_t sh = (size_t)mb * ((p + q + 1) * (p + 2 * q + 1) + (q + 1) * (2 * q + 1)) * sizeof(double2) +
+              (size_t)mb * (p + 4) * sizeof(double) + (size_t)mb * sizeof(int);
   cudaError_t e = cudaFuncSetAttribute(k_tr_m2qbxl, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)sh);
   if (e != cudaSuccess) return e;
-  k_tr_m2qbxl<<<dim3(ix.nlist3_rows, nrhs), NT, sh, st>>>(g, ix, p, q, ncf, ncq, nrhs, cmp, locals,
-                                                          err);
+  k_tr_m2qbxl<<<dim3(ix.nlist3_rows, nrhs), NT, sh, st>>>(g, ix, p, q, ncf, ncq, nrhs, mb, cmp,
+                                                          locals, err);
   return cudaGetLastError();
 }
 
