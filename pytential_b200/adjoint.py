@@ -124,21 +124,34 @@ class SingleLayer(_Operator):
 
 
 class FarFieldSingleLayer(_Operator):
-    """``u = S sigma`` at fixed targets away from the surface, with its adjoint: in
-    FP64 the transpose over the apply's own tree, in the mixed form the
-    exchanged-role FMM on a second tree built over the targets (point sources with
-    strengths ``r`` evaluated at the quad nodes, FP32 far field)."""
+    """``u = S sigma`` at fixed targets away from the surface, with its adjoint.
+
+    ``adjoint_form``: "transpose" (the default in FP64) -- the transpose over the
+    apply's own tree, exact to rounding; "exchanged-tree" (the only form of the mixed
+    precision) -- the exchanged-role FMM on a second tree built over the targets
+    (point sources with strengths ``r`` evaluated at the quad nodes), the same
+    operator's transpose within the FMM's truncation, cheaper when the targets are
+    few (the second tree is built over them)."""
 
     def __init__(self, discr: Discretization, targets: np.ndarray, qbx_order: int,
-                 fmm_order: int, precision: int = PRECISION_FP64, device="cuda"):
+                 fmm_order: int, precision: int = PRECISION_FP64, device="cuda",
+                 adjoint_form: str | None = None):
         self._setup_common(discr, targets, device)
         self.precision = precision
+        if adjoint_form is None:
+            adjoint_form = "transpose" if precision == PRECISION_FP64 else "exchanged-tree"
+        if adjoint_form not in ("transpose", "exchanged-tree"):
+            raise ValueError(f"adjoint_form must be 'transpose' or 'exchanged-tree', "
+                             f"not {adjoint_form!r}")
+        if adjoint_form == "transpose" and precision != PRECISION_FP64:
+            raise ValueError("the transpose form runs in FP64")
+        self.adjoint_form = adjoint_form
         self.geo = QBXFMMGeometryData(discr, [(self.targets, 0)])
         if self.geo.global_qbx_centers().size:
             raise ValueError("a target needs QBX; use SingleLayer for targets near the surface")
         self.fwd = QBXApply(self.geo, self.spec, qbx_order, fmm_order, device=device,
                             precision=precision)
-        if precision == PRECISION_FP64:
+        if adjoint_form == "transpose":
             self.transpose = QBXTransposeApply(self.fwd)
         else:
             self.transpose = None

@@ -269,12 +269,14 @@ def _solve2d(argv=None):
 
 def _adjoint3d(argv=None):
     """``python -m pytential_b200.workloads adjoint3d [NREFINE] [--mixed |
-    --on-surface]``: the 3D Laplace single-layer adjoint benchmark (ellipsoid, 5000
-    targets on the sphere of radius 3, qbx_order 4, fmm_order 12): times the forward
-    apply, the adjoint apply alone and forward + backward (density and
-    target-position gradients) on the current GPU.  ``--on-surface``: the targets are
-    the surface nodes (exterior limit, every target through QBX) and the backward
-    pass takes the density gradient only."""
+    --exchanged-tree | --on-surface]``: the 3D Laplace single-layer adjoint benchmark
+    (ellipsoid, 5000 targets on the sphere of radius 3, qbx_order 4, fmm_order 12):
+    times the forward apply, the adjoint apply alone and forward + backward (density
+    and target-position gradients) on the current GPU.  The adjoint is the transpose
+    over the apply's tree in FP64, the exchanged-role second tree with ``--mixed`` or
+    ``--exchanged-tree``.  ``--on-surface``: the targets are the surface nodes
+    (exterior limit, every target through QBX) and the backward pass takes the
+    density gradient only."""
     import time
 
     import torch
@@ -284,6 +286,7 @@ def _adjoint3d(argv=None):
     argv = list(argv or [])
     mixed = "--mixed" in argv
     surface = "--on-surface" in argv
+    sys_flags = set(a for a in argv if a.startswith("--"))
     argv = [a for a in argv if not a.startswith("--")]
     nref = int(argv[0]) if argv else 4
     w = laplace3d_adjoint(nrefine=nref)
@@ -293,7 +296,9 @@ def _adjoint3d(argv=None):
     else:
         X_np = w.targets
         op = FarFieldSingleLayer(w.discr, X_np, w.qbx_order, w.fmm_order,
-                                 precision=PRECISION_MIXED if mixed else PRECISION_FP64)
+                                 precision=PRECISION_MIXED if mixed else PRECISION_FP64,
+                                 adjoint_form="exchanged-tree"
+                                 if mixed or "--exchanged-tree" in sys_flags else "transpose")
     sig0 = torch.from_numpy(w.sigma).cuda()
     X0 = torch.from_numpy(np.ascontiguousarray(X_np)).cuda()
     g = torch.from_numpy(w.g(X_np)).cuda()
@@ -322,8 +327,9 @@ def _adjoint3d(argv=None):
     ta = timed(lambda: op.adjoint(r0))
     tb = timed(fwd_bwd)
     where = f"{op.ntargets} surface targets (QBX)" if surface else f"{op.ntargets} targets"
+    form = "" if surface else f" ({op.adjoint_form} adjoint)"
     print(f"3D Laplace S adjoint, icosphere-{nref} ({w.discr.ndofs} nodes), {where}, "
-          f"{'mixed' if mixed else 'FP64'}: forward {1e3 * tf:.2f} ms, adjoint "
+          f"{'mixed' if mixed else 'FP64'}{form}: forward {1e3 * tf:.2f} ms, adjoint "
           f"{1e3 * ta:.2f} ms, forward + backward {1e3 * tb:.2f} ms")
 
 

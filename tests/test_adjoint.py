@@ -182,3 +182,19 @@ def test_near_targets_adjoint_dot_products():
         op.target_gradient(sig)
 
 # }}}
+
+
+def test_exchanged_tree_adjoint_agrees_with_the_transpose(small):
+    """The FP64 exchanged-tree adjoint (second tree over the targets) against the
+    exact transpose: the same operator's transpose within the FMM's truncation."""
+    from pytential_b200.adjoint import FarFieldSingleLayer
+    w, op = small
+    assert op.adjoint_form == "transpose"
+    ex = FarFieldSingleLayer(w.discr, w.targets, w.qbx_order, w.fmm_order,
+                             adjoint_form="exchanged-tree")
+    r = torch.from_numpy(np.random.default_rng(12).normal(size=w.targets.shape[1])).cuda()
+    assert relerr(ex.adjoint(r).cpu().numpy(), op.adjoint(r).cpu().numpy()) < 1e-7
+    with pytest.raises(ValueError):
+        from pytential_b200.fmm import PRECISION_MIXED
+        FarFieldSingleLayer(w.discr, w.targets, w.qbx_order, w.fmm_order,
+                            precision=PRECISION_MIXED, adjoint_form="transpose")
