@@ -132,6 +132,18 @@ int qbxfmm_eval_qbx_expansions(const qbxfmm_plan* plan, const void* qbx_exps, vo
 int qbxfmm_eval_target_specific_qbx_locals(const qbxfmm_plan* plan, const void* strengths,
                                            void* pot_tree, int32_t* error_word, void* stream);
 
+/* Gradient of the 3D Laplace single-layer potential at the non-QBX targets from the
+ * FMM's own data of an apply (strengths in tree order, multipoles after
+ * coarsen_multipoles, locals after refine_locals -- the workspace of qbxfmm_apply
+ * holds them after the call): P2P over list 1, M2P over list 3, L2P of the target
+ * box's local, each differentiated at the target (the derivative of the apply's
+ * value with the tree held fixed), kernel scaling included.  The reference obtains
+ * it from derivative target kernels in its FMM.  grad: [nrhs][3][nfiltered_targets]
+ * (written).  QBXFMM_ERR_UNSUPPORTED for other kernels and per-level orders. */
+int qbxfmm_eval_target_gradients(const qbxfmm_plan* plan, const void* strengths,
+                                 const void* mpoles, const void* locals, void* grad,
+                                 int32_t* error_word, void* stream);
+
 /* {{{ transposed QBX stages (3D Laplace single layer, FP64, one FMM order)
  *
  * The transpose of the apply is the FMM with sources and targets exchanged over

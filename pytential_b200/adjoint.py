@@ -13,8 +13,10 @@ Backward:
   order-q multipoles of their targets' values), so targets that need QBX -- on the
   surface or near it -- are covered, and ``A^T`` is the transpose of the apply's own
   matrix (FP64);
-* ``dJ/dx_t = r_t grad u(x_t)`` at targets away from the surface, with ``grad u``
-  summed directly on the GPU (``qbxfmm_laplace3d_grad_direct``).
+* ``dJ/dx_t = r_t grad u(x_t)`` at targets away from the surface, with ``grad u`` the
+  derivative of the apply's own value (its P2P, M2P and L2P differentiated at the
+  target, ``qbxfmm_eval_target_gradients``), or summed directly over the quad nodes
+  (``qbxfmm_laplace3d_grad_direct``).
 
 :class:`SingleLayer` takes any targets; :class:`FarFieldSingleLayer` is the operator
 at targets away from the surface, also in the mixed form (FP32 far field), whose
@@ -76,7 +78,16 @@ class _Operator:
 
     def apply(self, sigma: torch.Tensor) -> torch.Tensor:
         """(ndofs,) -> (ntargets,)"""
-        return self.fwd(sigma.reshape(1, -1).contiguous())[0].clone()
+        out = self.fwd(sigma.reshape(1, -1).contiguous())[0].clone()
+        self._applied = (sigma.data_ptr(), sigma._version, sigma.numel())
+        return out
+
+    def _grad_fmm(self, sigma):
+        """grad u at the (non-QBX) targets from the apply's own FMM data, (3, ntargets):
+        the workspace of the last apply when it was this density, else a new apply."""
+        if getattr(self, "_applied", None) != (sigma.data_ptr(), sigma._version, sigma.numel()):
+            self.apply(sigma)
+        return self.fwd.nonqbx_target_gradients()[0]
 
     def strengths(self, sigma: torch.Tensor) -> torch.Tensor:
         """Quad-node strengths W U sigma, (nquad,)."""
@@ -115,12 +126,15 @@ class SingleLayer(_Operator):
         """A^T r: (ntargets,) -> (ndofs,)"""
         return self.transpose(r.reshape(1, -1).contiguous())[0]
 
-    def target_gradient(self, sigma: torch.Tensor) -> torch.Tensor:
-        """grad u at the targets, (3, ntargets); targets away from the surface only."""
+    def target_gradient(self, sigma: torch.Tensor, form: str = "fmm") -> torch.Tensor:
+        """grad u at the targets, (3, ntargets); targets away from the surface only.
+        ``form``: "fmm" -- the derivative of the apply's own value (P2P, M2P and L2P
+        differentiated at the target, ``qbxfmm_eval_target_gradients``); "direct" --
+        the kernel summed over all quad nodes."""
         if self.targets_need_qbx:
             raise NotImplementedError("target-position gradients at targets evaluated "
                                       "through QBX expansions")
-        return self._grad_direct(sigma)
+        return self._grad_fmm(sigma) if form == "fmm" else self._grad_direct(sigma)
 
 
 class FarFieldSingleLayer(_Operator):
@@ -168,9 +182,13 @@ class FarFieldSingleLayer(_Operator):
         v = (kt * self.w).reshape(d.nelements, d.quad_nodes_per_element)
         return (v @ self.U).reshape(-1)
 
-    def target_gradient(self, sigma: torch.Tensor) -> torch.Tensor:
-        """grad u at the targets, (3, ntargets); the mixed-precision operator sums it in
-        FP32 arithmetic."""
+    def target_gradient(self, sigma: torch.Tensor, form: str = "fmm") -> torch.Tensor:
+        """grad u at the targets, (3, ntargets).  ``form``: "fmm" -- the derivative of
+        the apply's own value (P2P, M2P and L2P differentiated at the target,
+        ``qbxfmm_eval_target_gradients``, from the apply's expansions); "direct" -- the
+        kernel summed over all quad nodes (FP32 arithmetic for the mixed operator)."""
+        if form == "fmm":
+            return self._grad_fmm(sigma)
         return self._grad_direct(sigma, fp64=self.precision == PRECISION_FP64)
 
 

@@ -1290,6 +1290,24 @@ int qbxfmm_apply(const qbxfmm_plan* p, const qbxfmm_upsample* up, const qbxfmm_w
   return qbxfmm_assemble(p, ws->pot_nonqbx, ws->pot_tree, out, stream);
 }
 
+int qbxfmm_eval_target_gradients(const qbxfmm_plan* p, const void* strengths, const void* mpoles,
+                                  const void* locals, void* grad, int32_t* err, void* stream)
+{
+  if (int rc = check_plan(p)) return rc;
+  if (p->helm || p->kern.dim != 3 || p->sc.cd != 0.0)
+    return fail(QBXFMM_ERR_UNSUPPORTED, "target gradients cover the 3D Laplace single layer");
+  if (level_orders_on(p))
+    return fail(QBXFMM_ERR_UNSUPPORTED, "target gradients take one FMM order");
+  if (!strengths || !mpoles || !locals || !grad) return fail(QBXFMM_ERR_ARG, "null argument");
+  size_t bytes = (size_t)p->kern.nrhs * 3 * p->geo.nfiltered_targets * sizeof(double);
+  if (bytes) QBX_TRY(cudaMemsetAsync(grad, 0, bytes, S(stream)), "eval_target_gradients: clear");
+  QBX_TRY(launch_grad_targets(p->geo, p->sc.cq, 0.25 / M_PI, p->kern.fmm_order, p->kern.nrhs,
+                              (const double*)strengths, (const double2*)mpoles,
+                              (const double2*)locals, (double*)grad, err, S(stream)),
+          "eval_target_gradients");
+  return QBXFMM_OK;
+}
+
 // {{{ transposed QBX stages
 
 namespace {

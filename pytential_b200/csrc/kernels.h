@@ -199,6 +199,12 @@ cudaError_t launch_tr_p2qbxl(const qbxfmm_geometry& g, const qbxfmm_transpose_in
                              int nrhs, double cq, const double* tvals, double* vals, int32_t* err,
                              cudaStream_t st);
 
+// gradient of the 3D Laplace single layer at the non-QBX targets (kernels_fmmgrad.cu)
+cudaError_t launch_grad_targets(const qbxfmm_geometry& g, double cq, double scale, int p,
+                                int nrhs, const double* strengths, const double2* mpoles,
+                                const double2* locals, double* grad, int32_t* err,
+                                cudaStream_t st);
+
 // per-level FMM orders: zero the coefficients of boxes [b0, b1) above their level's order
 cudaError_t launch_level_mask(const qbxfmm_geometry& g, int b0, int b1, const int32_t* orders,
                               int family, int ncf, int nrhs, double2* exps, cudaStream_t st);

@@ -593,6 +593,29 @@ class QBXApply:
         density = density.reshape(self.nrhs, self.ndofs).contiguous()
         return self.apply_into(density, self.new_output())
 
+    def nonqbx_target_gradients(self) -> torch.Tensor:
+        """Gradient of the last apply's potential at its non-QBX targets from the
+        apply's own strengths, multipoles and locals (``qbxfmm_eval_target_gradients``;
+        3D Laplace single layer): ``(nrhs, 3, nuser_targets)`` in user order, zero at
+        targets evaluated through QBX."""
+        nf = self.dgeo.nfiltered_targets
+        g = torch.zeros(self.nrhs, 3, max(nf, 1), dtype=torch.float64, device=self.device)
+        self.plan.call("qbxfmm_eval_target_gradients", ctypes.c_void_p(_ptr(self._ws_tensors[0])),
+                       ctypes.c_void_p(_ptr(self._ws_tensors[1])),
+                       ctypes.c_void_p(_ptr(self._ws_tensors[2])), ctypes.c_void_p(_ptr(g)),
+                       ctypes.cast(ctypes.c_void_p(_ptr(self.error_word)),
+                                   ctypes.POINTER(ctypes.c_int32)), _stream_handle())
+        out = torch.zeros(self.nrhs, 3, self.nuser_targets, dtype=torch.float64,
+                          device=self.device)
+        if nf:
+            if not hasattr(self, "_filtered_user"):
+                h = self.dgeo.host_arrays
+                t = h["unfiltered_from_filtered_target_indices"][:nf].astype(np.int64)
+                u = h["sorted_target_ids"][t].astype(np.int64) - self.dgeo.ncenters
+                self._filtered_user = torch.from_numpy(u).to(self.device)
+            out[:, :, self._filtered_user] = g[:, :, :nf]
+        return out
+
     # {{{ CUDA graph
 
     def capture(self):

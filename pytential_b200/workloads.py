@@ -326,11 +326,18 @@ def _adjoint3d(argv=None):
     tf = timed(lambda: op.apply(sig0))
     ta = timed(lambda: op.adjoint(r0))
     tb = timed(fwd_bwd)
+    grads = ""
+    if not surface:
+        op.apply(sig0)
+        tg = timed(lambda: op.target_gradient(sig0))
+        td = timed(lambda: op.target_gradient(sig0, form="direct"))
+        grads = (f", target gradient from the FMM {1e3 * tg:.2f} ms (direct sum "
+                 f"{1e3 * td:.2f} ms)")
     where = f"{op.ntargets} surface targets (QBX)" if surface else f"{op.ntargets} targets"
     form = "" if surface else f" ({op.adjoint_form} adjoint)"
     print(f"3D Laplace S adjoint, icosphere-{nref} ({w.discr.ndofs} nodes), {where}, "
           f"{'mixed' if mixed else 'FP64'}{form}: forward {1e3 * tf:.2f} ms, adjoint "
-          f"{1e3 * ta:.2f} ms, forward + backward {1e3 * tb:.2f} ms")
+          f"{1e3 * ta:.2f} ms, forward + backward {1e3 * tb:.2f} ms{grads}")
 
 
 if __name__ == "__main__":

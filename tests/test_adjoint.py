@@ -198,3 +198,89 @@ def test_exchanged_tree_adjoint_agrees_with_the_transpose(small):
         from pytential_b200.fmm import PRECISION_MIXED
         FarFieldSingleLayer(w.discr, w.targets, w.qbx_order, w.fmm_order,
                             precision=PRECISION_MIXED, adjoint_form="transpose")
+
+
+# {{{ the target gradient from the FMM's own data
+
+def test_fmm_target_gradient_against_checker_differences():
+    """qbxfmm_eval_target_gradients against central differences of the checker's apply
+    with the non-QBX targets moved and the tree held fixed (the derivative of the
+    apply's own value), far targets and near-surface ones together; zero at the
+    targets evaluated through QBX."""
+    from oracle.oracle import Oracle
+    from pytential_b200 import abi
+    from pytential_b200.fmm import LaplaceKernel, QBXApply, SourceKernelSpec
+    from pytential_b200.geometry import QBXFMMGeometryData
+    from pytential_b200.workloads import laplace3d_adjoint
+    w = laplace3d_adjoint(nrefine=2, ntargets=64, seed=13)
+    d = w.discr
+    rng = np.random.default_rng(14)
+    i = rng.integers(0, d.ndofs, 40)
+    hs = d.element_stretch[i // d.nodes_per_element] * d.normals[:, i]
+    near = d.nodes[:, i] + 0.05 * hs          # through QBX
+    mid = d.nodes[:, i] + 1.5 * hs            # close to the surface, no QBX
+    geo = QBXFMMGeometryData(d, [(w.targets, 0), (near, 0), (mid, 0)])
+    spec = SourceKernelSpec(LaplaceKernel(3), charge_coeff=1.0)
+    ap = QBXApply(geo, spec, w.qbx_order, w.fmm_order, nrhs=2)
+    sig = rng.normal(size=(2, d.ndofs))
+    ap(torch.from_numpy(sig).cuda())
+    g = ap.nonqbx_target_gradients().cpu().numpy()                 # (2, 3, nuser)
+    ap.check_error_word()
+    o = Oracle(geo, dim=3, qbx_order=w.qbx_order, fmm_order=w.fmm_order, nrhs=2,
+               charge_coeff=1.0, family=abi.QBXFMM_LAPLACE)
+    s = np.ascontiguousarray((d.upsample_density(sig) * d.quad_weights)[
+        :, o.arrays["user_source_ids"][:o.scalars["nsources"]]])
+    nf = o.scalars["nfiltered_targets"]
+    X = o.arrays["nonqbx_targets"]
+    h = 1e-5
+    fd = np.zeros_like(g)
+    assert X.shape == (3, nf)
+    for k in range(3):
+        X[k] += h
+        up = o.apply(s)
+        X[k] -= 2 * h
+        dn = o.apply(s)
+        X[k] += h
+        fd[:, k, :] = (up - dn) / (2 * h)
+    # the targets through QBX do not move (their values do not change) and get zero
+    qbx = np.ones(g.shape[2], bool)
+    sid = o.arrays["sorted_target_ids"]
+    qbx[sid[o.arrays["unfiltered_from_filtered_target_indices"][:nf]] - o.scalars["ncenters"]] = False
+    assert qbx.sum() > 0 and (~qbx).sum() > 64     # the far targets and some of mid
+    assert np.all(g[:, :, qbx] == 0)
+    assert relerr(g[:, :, ~qbx], fd[:, :, ~qbx]) < 1e-7
+
+
+def test_fmm_target_gradient_against_direct_sum(small):
+    w, op = small
+    sig = torch.from_numpy(w.sigma).cuda()
+    gf = op.target_gradient(sig).cpu().numpy()
+    gd = op.target_gradient(sig, form="direct").cpu().numpy()
+    assert relerr(gf, gd) < 1e-7
+
+
+def test_fmm_target_gradient_mixed(small):
+    from pytential_b200.adjoint import FarFieldSingleLayer
+    from pytential_b200.fmm import PRECISION_MIXED
+    w, op = small
+    opm = FarFieldSingleLayer(w.discr, w.targets, w.qbx_order, w.fmm_order,
+                              precision=PRECISION_MIXED)
+    sig = torch.from_numpy(w.sigma).cuda()
+    assert 0 < relerr(opm.target_gradient(sig).cpu().numpy(),
+                      op.target_gradient(sig).cpu().numpy()) < 1e-5
+
+
+def test_fmm_target_gradient_refuses_the_double_layer():
+    from pytential_b200 import abi, native
+    from pytential_b200.fmm import LaplaceKernel, QBXApply, SourceKernelSpec
+    from pytential_b200.geometry import QBXFMMGeometryData
+    from pytential_b200.workloads import laplace3d_adjoint
+    w = laplace3d_adjoint(nrefine=1, ntargets=16, seed=15)
+    ap = QBXApply(QBXFMMGeometryData(w.discr, [(w.targets, 0)]),
+                  SourceKernelSpec(LaplaceKernel(3), dipole_coeff=1.0), 3, 8)
+    ap(torch.zeros(1, w.discr.ndofs, dtype=torch.float64, device="cuda"))
+    with pytest.raises(native.QBXFMMError) as ei:
+        ap.nonqbx_target_gradients()
+    assert ei.value.code == abi.QBXFMM_ERR_UNSUPPORTED
+
+# }}}
