@@ -144,6 +144,15 @@ int qbxfmm_eval_target_gradients(const qbxfmm_plan* plan, const void* strengths,
                                  const void* mpoles, const void* locals, void* grad,
                                  int32_t* error_word, void* stream);
 
+/* The same at the QBX targets: the gradient of each target's center's QBX local at
+ * the target (center held fixed) from the apply's qbx_exps (after
+ * translate_box_local_to_qbx_local), plus, for a plan with the target-specific near
+ * field, the target-derivative of the list-1 Legendre sums from the strengths.
+ * grad: [nrhs][3][ntargets] in tree target order (written; zero at other targets). */
+int qbxfmm_eval_qbx_target_gradients(const qbxfmm_plan* plan, const void* strengths,
+                                     const void* qbx_exps, void* grad, int32_t* error_word,
+                                     void* stream);
+
 /* {{{ transposed QBX stages (3D Laplace single layer, FP64, one FMM order)
  *
  * The transpose of the apply is the FMM with sources and targets exchanged over

@@ -13,10 +13,12 @@ Backward:
   order-q multipoles of their targets' values), so targets that need QBX -- on the
   surface or near it -- are covered, and ``A^T`` is the transpose of the apply's own
   matrix (FP64);
-* ``dJ/dx_t = r_t grad u(x_t)`` at targets away from the surface, with ``grad u`` the
-  derivative of the apply's own value (its P2P, M2P and L2P differentiated at the
-  target, ``qbxfmm_eval_target_gradients``), or summed directly over the quad nodes
-  (``qbxfmm_laplace3d_grad_direct``).
+* ``dJ/dx_t = r_t grad u(x_t)`` with ``grad u`` the derivative of the apply's own
+  value: its P2P, M2P and L2P differentiated at the non-QBX targets
+  (``qbxfmm_eval_target_gradients``), at the QBX targets the center's QBX local and
+  the target-specific near field differentiated with the center held fixed
+  (``qbxfmm_eval_qbx_target_gradients``); or, at targets away from the surface, the
+  kernel summed directly over the quad nodes (``qbxfmm_laplace3d_grad_direct``).
 
 :class:`SingleLayer` takes any targets; :class:`FarFieldSingleLayer` is the operator
 at targets away from the surface, also in the mixed form (FP32 far field), whose
@@ -83,11 +85,11 @@ class _Operator:
         return out
 
     def _grad_fmm(self, sigma):
-        """grad u at the (non-QBX) targets from the apply's own FMM data, (3, ntargets):
-        the workspace of the last apply when it was this density, else a new apply."""
+        """grad u at the targets from the apply's own FMM data, (3, ntargets): the
+        workspace of the last apply when it was this density, else a new apply."""
         if getattr(self, "_applied", None) != (sigma.data_ptr(), sigma._version, sigma.numel()):
             self.apply(sigma)
-        return self.fwd.nonqbx_target_gradients()[0]
+        return self.fwd.target_gradients()[0]
 
     def strengths(self, sigma: torch.Tensor) -> torch.Tensor:
         """Quad-node strengths W U sigma, (nquad,)."""
@@ -127,14 +129,18 @@ class SingleLayer(_Operator):
         return self.transpose(r.reshape(1, -1).contiguous())[0]
 
     def target_gradient(self, sigma: torch.Tensor, form: str = "fmm") -> torch.Tensor:
-        """grad u at the targets, (3, ntargets); targets away from the surface only.
-        ``form``: "fmm" -- the derivative of the apply's own value (P2P, M2P and L2P
-        differentiated at the target, ``qbxfmm_eval_target_gradients``); "direct" --
-        the kernel summed over all quad nodes."""
+        """grad u at the targets, (3, ntargets).  ``form``: "fmm" -- the derivative of
+        the apply's own value: P2P, M2P and L2P differentiated at the non-QBX targets,
+        at the QBX targets the center's QBX local (and the target-specific near field)
+        with the center held fixed (the target-to-center association is piecewise
+        constant); "direct" -- the kernel summed over all quad nodes, for targets away
+        from the surface only."""
+        if form == "fmm":
+            return self._grad_fmm(sigma)
         if self.targets_need_qbx:
-            raise NotImplementedError("target-position gradients at targets evaluated "
-                                      "through QBX expansions")
-        return self._grad_fmm(sigma) if form == "fmm" else self._grad_direct(sigma)
+            raise NotImplementedError("the direct sum is the gradient at targets away from "
+                                      "the surface only")
+        return self._grad_direct(sigma)
 
 
 class FarFieldSingleLayer(_Operator):

@@ -1308,6 +1308,24 @@ int qbxfmm_eval_target_gradients(const qbxfmm_plan* p, const void* strengths, co
   return QBXFMM_OK;
 }
 
+int qbxfmm_eval_qbx_target_gradients(const qbxfmm_plan* p, const void* strengths,
+                                      const void* qbx_exps, void* grad, int32_t* err,
+                                      void* stream)
+{
+  if (int rc = check_plan(p)) return rc;
+  if (p->helm || p->kern.dim != 3 || p->sc.cd != 0.0)
+    return fail(QBXFMM_ERR_UNSUPPORTED, "target gradients cover the 3D Laplace single layer");
+  if (p->kern.qbx_order > 8) return fail(QBXFMM_ERR_UNSUPPORTED, "qbx_order > 8");
+  if (!strengths || !qbx_exps || !grad) return fail(QBXFMM_ERR_ARG, "null argument");
+  size_t bytes = (size_t)p->kern.nrhs * 3 * p->geo.ntargets * sizeof(double);
+  if (bytes) QBX_TRY(cudaMemsetAsync(grad, 0, bytes, S(stream)), "eval_qbx_target_gradients: clear");
+  QBX_TRY(launch_grad_qbx_targets(p->geo, p->sc.cq, 0.25 / M_PI, p->kern.qbx_order, p->kern.nrhs,
+                                  p->kern.target_specific_qbx != 0, (const double*)strengths,
+                                  (const double2*)qbx_exps, (double*)grad, err, S(stream)),
+          "eval_qbx_target_gradients");
+  return QBXFMM_OK;
+}
+
 // {{{ transposed QBX stages
 
 namespace {

@@ -205,6 +205,11 @@ cudaError_t launch_grad_targets(const qbxfmm_geometry& g, double cq, double scal
                                 const double2* locals, double* grad, int32_t* err,
                                 cudaStream_t st);
 
+cudaError_t launch_grad_qbx_targets(const qbxfmm_geometry& g, double cq, double scale, int q,
+                                    int nrhs, bool target_specific, const double* strengths,
+                                    const double2* qbx_exps, double* grad, int32_t* err,
+                                    cudaStream_t st);
+
 // per-level FMM orders: zero the coefficients of boxes [b0, b1) above their level's order
 cudaError_t launch_level_mask(const qbxfmm_geometry& g, int b0, int b1, const int32_t* orders,
                               int family, int ncf, int nrhs, double2* exps, cudaStream_t st);

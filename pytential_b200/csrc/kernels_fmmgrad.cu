@@ -246,6 +246,176 @@ k_grad_locals(qbxfmm_geometry g, int p, int ncf, int nrhs, double scale,
 
 // }}}
 
+// {{{ QBX targets: gradient of the center's QBX local, and of the target-specific near field
+
+// one thread per global center: the streaming L2P gradient of its order-q QBX local
+// at each of its targets (grad[r][0..2][t], tree target order)
+__global__ void __launch_bounds__(NT)
+k_grad_qbxl2p(qbxfmm_geometry g, int q, int ncq, int nrhs, double scale,
+              const double2* __restrict__ qbx_exps, double* __restrict__ grad, int32_t* err)
+{
+  int ig = blockIdx.x * blockDim.x + threadIdx.x;
+  int r = blockIdx.y;
+  if (ig >= g.nglobal_qbx_centers) return;
+  int ctr = g.global_qbx_centers[ig];
+  if ((unsigned)ctr >= (unsigned)g.ncenters) {
+    report(err, QBX_DEVERR_BAD_CENTER);
+    return;
+  }
+  double cc[3];
+  load_point<3>(g.centers, g.ncenters, ctr, cc);
+  double rho = g.expansion_radii[ctr];
+  const double2* L = qbx_exps + ((size_t)ctr * nrhs + r) * ncq;
+  for (int it = g.center_to_targets_starts[ctr]; it < g.center_to_targets_starts[ctr + 1]; ++it) {
+    int t = g.center_to_targets_lists[it];
+    if ((unsigned)t >= (unsigned)g.ntargets) {
+      report(err, QBX_DEVERR_BAD_CENTER);
+      continue;
+    }
+    double x[3];
+    load_point<3>(g.targets, g.ntargets, t, x);
+    double u0 = (x[0] - cc[0]) / rho, u1 = (x[1] - cc[1]) / rho, u2 = (x[2] - cc[2]) / rho;
+    double r2 = u0 * u0 + u1 * u1 + u2 * u2;
+    double2 mm = c2(1.0);
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+    for (int j = 0; j < q; ++j) {
+      if (j > 0) mm = cscale(0.5 * rcp(j), cmul(mm, c2(u0, u1)));
+      double2 a = mm, prev = c2(0.0);
+      double w = j ? 2.0 : 1.0;
+      for (int k = j; k < q; ++k) {
+        if (k > j) {
+          double2 bb = cscale(rcp(k + j) * rcp(k - j),
+                              csub(cscale((2.0 * k - 1) * u2, a), cscale(r2, prev)));
+          prev = a;
+          a = bb;
+        }
+        int n = k + 1;
+        double2 cp = coef(L, n, j + 1, q), cm = coef(L, n, j - 1, q), c = coef(L, n, j, q);
+        double2 vp = cmulc(cp, a), vm = cmulc(cm, a), v = cmulc(c, a);
+        a0 += vp.x - (j > 0 ? vm.x : 0.0);
+        a1 += vp.y + (j > 0 ? vm.y : 0.0);
+        a2 += w * v.x;
+      }
+    }
+    double f = scale / rho;
+    size_t o = (size_t)r * 3 * g.ntargets + t;
+    grad[o] += f * a0;
+    grad[o + g.ntargets] += f * a1;
+    grad[o + 2 * (size_t)g.ntargets] += f * a2;
+  }
+}
+
+// The target-specific near field K = sum_{n<=Q} |a|^n / |b|^{n+1} P_n(cos g),
+// a = t - c, b = y - c, cos g = a^.b^, differentiated at the target:
+//   grad_a K = sum_n |a|^{n-1} / |b|^{n+1} [(n P_n - cos g P_n') a^ + P_n' b^].
+// CTA = one chunk of <= 32 (target, center) pairs (lane = pair), a cluster of GSPL CTAs
+// dealing the list-1 sources of the center's box to its warps.
+template <int Q>
+__global__ void __cluster_dims__(GSPL, 1, 1) __launch_bounds__(NT)
+k_grad_tsqbx(qbxfmm_geometry g, double cq, double scale, int nrhs,
+             const double* __restrict__ strengths, double* __restrict__ grad, int32_t* err)
+{
+  __shared__ double s_red[NW - 1][3][32];
+  __shared__ double s_part[3][32];
+  int chunk = blockIdx.x / GSPL, part = blockIdx.x - chunk * GSPL, r = blockIdx.y;
+  int itb = g.tsqbx_chunk_target_box[chunk];
+  int i0 = g.tsqbx_chunk_start[chunk];
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  bool active = lane < g.tsqbx_chunk_count[chunk];
+  int t = active ? g.tsqbx_targets[i0 + lane] : 0;
+  int ctr = active ? g.tsqbx_centers[i0 + lane] : 0;
+  if ((unsigned)ctr >= (unsigned)g.ncenters || (unsigned)t >= (unsigned)g.ntargets) {
+    report(err, QBX_DEVERR_BAD_CENTER);
+    active = false;
+    t = ctr = 0;
+  }
+  double cc[3] = {0.0, 0.0, 0.0}, x[3] = {0.0, 0.0, 0.0};
+  load_point<3>(g.centers, g.ncenters, ctr, cc);
+  load_point<3>(g.targets, g.ntargets, t, x);
+  double a[3] = {x[0] - cc[0], x[1] - cc[1], x[2] - cc[2]};
+  double alen = sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+  double ainv = alen > 0.0 ? 1.0 / alen : 0.0;
+  double ah[3] = {a[0] * ainv, a[1] * ainv, a[2] * ainv};
+  const double* st = strengths + (size_t)r * g.nsources;
+  double gr[3] = {0.0, 0.0, 0.0};
+  const int stride = GSPL * NW, lead = part * NW + warp;
+  for (int li = g.list1_starts[itb]; li < g.list1_starts[itb + 1]; ++li) {
+    int sb = g.list1_lists[li];
+    if ((unsigned)sb >= (unsigned)g.nboxes) {
+      report(err, QBX_DEVERR_BAD_BOX);
+      continue;
+    }
+    int s0 = g.box_source_starts[sb], s1 = s0 + g.box_source_counts_nonchild[sb];
+    if (!active) continue;
+    for (int j = s0 + lead; j < s1; j += stride) {
+      double y[3];
+      load_point<3>(g.sources, g.nsources, j, y);
+      double b0 = y[0] - cc[0], b1 = y[1] - cc[1], b2 = y[2] - cc[2];
+      double binv = rsqrt(b0 * b0 + b1 * b1 + b2 * b2);
+      double bh0 = b0 * binv, bh1 = b1 * binv, bh2 = b2 * binv;
+      double cg = ah[0] * bh0 + ah[1] * bh1 + ah[2] * bh2;
+      double ratio = alen * binv;
+      // rn = |a|^{n-1} / |b|^{n+1}, from n = 1
+      double rn = binv * binv;
+      double pm1 = 1.0, pm2 = 0.0, dm1 = 0.0, sa = 0.0, sb2 = 0.0;
+#pragma unroll
+      for (int n = 1; n <= Q; ++n) {
+        double pn = n == 1 ? cg : ((2.0 * n - 1) * cg * pm1 - (n - 1.0) * pm2) * (1.0 / n);
+        double dn = n * pm1 + cg * dm1;
+        sa = fma(rn, n * pn - cg * dn, sa);
+        sb2 = fma(rn, dn, sb2);
+        pm2 = pm1;
+        pm1 = pn;
+        dm1 = dn;
+        rn *= ratio;
+      }
+      double f = scale * cq * st[j];
+      gr[0] = fma(f, sa * ah[0] + sb2 * bh0, gr[0]);
+      gr[1] = fma(f, sa * ah[1] + sb2 * bh1, gr[1]);
+      gr[2] = fma(f, sa * ah[2] + sb2 * bh2, gr[2]);
+    }
+  }
+  size_t o = (size_t)r * 3 * g.ntargets + t;
+  cluster_reduce_add(gr, s_red, s_part, active, grad + o, grad + o + g.ntargets,
+                     grad + o + 2 * (size_t)g.ntargets);
+}
+
+template <int Q>
+static cudaError_t grad_tsqbx_q(const qbxfmm_geometry& g, double cq, double scale, int nrhs,
+                                const double* s, double* grad, int32_t* err, cudaStream_t st)
+{
+  k_grad_tsqbx<Q><<<dim3(g.ntsqbx_chunks * GSPL, nrhs), NT, 0, st>>>(g, cq, scale, nrhs, s, grad,
+                                                                     err);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_grad_qbx_targets(const qbxfmm_geometry& g, double cq, double scale, int q,
+                                    int nrhs, bool target_specific, const double* strengths,
+                                    const double2* qbx_exps, double* grad, int32_t* err,
+                                    cudaStream_t st)
+{
+  if (g.nglobal_qbx_centers == 0) return cudaSuccess;
+  int ncq = idx3(q + 1, 0);
+  k_grad_qbxl2p<<<dim3((g.nglobal_qbx_centers + NT - 1) / NT, nrhs), NT, 0, st>>>(
+      g, q, ncq, nrhs, scale, qbx_exps, grad, err);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess || !target_specific || g.ntsqbx_chunks == 0) return e;
+  switch (q) {
+    case 0: return grad_tsqbx_q<0>(g, cq, scale, nrhs, strengths, grad, err, st);
+    case 1: return grad_tsqbx_q<1>(g, cq, scale, nrhs, strengths, grad, err, st);
+    case 2: return grad_tsqbx_q<2>(g, cq, scale, nrhs, strengths, grad, err, st);
+    case 3: return grad_tsqbx_q<3>(g, cq, scale, nrhs, strengths, grad, err, st);
+    case 4: return grad_tsqbx_q<4>(g, cq, scale, nrhs, strengths, grad, err, st);
+    case 5: return grad_tsqbx_q<5>(g, cq, scale, nrhs, strengths, grad, err, st);
+    case 6: return grad_tsqbx_q<6>(g, cq, scale, nrhs, strengths, grad, err, st);
+    case 7: return grad_tsqbx_q<7>(g, cq, scale, nrhs, strengths, grad, err, st);
+    case 8: return grad_tsqbx_q<8>(g, cq, scale, nrhs, strengths, grad, err, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+// }}}
+
 cudaError_t launch_grad_targets(const qbxfmm_geometry& g, double cq, double scale, int p,
                                 int nrhs, const double* strengths, const double2* mpoles,
                                 const double2* locals, double* grad, int32_t* err,

@@ -593,27 +593,43 @@ class QBXApply:
         density = density.reshape(self.nrhs, self.ndofs).contiguous()
         return self.apply_into(density, self.new_output())
 
-    def nonqbx_target_gradients(self) -> torch.Tensor:
-        """Gradient of the last apply's potential at its non-QBX targets from the
-        apply's own strengths, multipoles and locals (``qbxfmm_eval_target_gradients``;
-        3D Laplace single layer): ``(nrhs, 3, nuser_targets)`` in user order, zero at
-        targets evaluated through QBX."""
-        nf = self.dgeo.nfiltered_targets
-        g = torch.zeros(self.nrhs, 3, max(nf, 1), dtype=torch.float64, device=self.device)
-        self.plan.call("qbxfmm_eval_target_gradients", ctypes.c_void_p(_ptr(self._ws_tensors[0])),
-                       ctypes.c_void_p(_ptr(self._ws_tensors[1])),
-                       ctypes.c_void_p(_ptr(self._ws_tensors[2])), ctypes.c_void_p(_ptr(g)),
-                       ctypes.cast(ctypes.c_void_p(_ptr(self.error_word)),
-                                   ctypes.POINTER(ctypes.c_int32)), _stream_handle())
+    def target_gradients(self) -> torch.Tensor:
+        """Gradient of the last apply's potential at its user targets,
+        ``(nrhs, 3, nuser_targets)`` (3D Laplace single layer): at the non-QBX targets
+        from the apply's own strengths, multipoles and locals
+        (``qbxfmm_eval_target_gradients``), at the QBX targets the gradient of the
+        center's QBX local (with the target-specific near field differentiated too)
+        with the center held fixed (``qbxfmm_eval_qbx_target_gradients``)."""
+        h = self.dgeo.host_arrays
+        nf, nt, nc = self.dgeo.nfiltered_targets, self.dgeo.ntargets, self.dgeo.ncenters
+        err = ctypes.cast(ctypes.c_void_p(_ptr(self.error_word)), ctypes.POINTER(ctypes.c_int32))
+        vp = ctypes.c_void_p
         out = torch.zeros(self.nrhs, 3, self.nuser_targets, dtype=torch.float64,
                           device=self.device)
+        if not hasattr(self, "_grad_maps"):
+            t = h["unfiltered_from_filtered_target_indices"][:nf].astype(np.int64)
+            fu = h["sorted_target_ids"][t].astype(np.int64) - nc
+            sid = h["sorted_target_ids"][:nt].astype(np.int64)
+            tt = np.nonzero(sid >= nc)[0]
+            self._grad_maps = tuple(torch.from_numpy(a).to(self.device)
+                                    for a in (fu, tt, sid[tt] - nc))
+        fu, tt, tu = self._grad_maps
         if nf:
-            if not hasattr(self, "_filtered_user"):
-                h = self.dgeo.host_arrays
-                t = h["unfiltered_from_filtered_target_indices"][:nf].astype(np.int64)
-                u = h["sorted_target_ids"][t].astype(np.int64) - self.dgeo.ncenters
-                self._filtered_user = torch.from_numpy(u).to(self.device)
-            out[:, :, self._filtered_user] = g[:, :, :nf]
+            g = torch.empty(self.nrhs, 3, nf, dtype=torch.float64, device=self.device)
+            self.plan.call("qbxfmm_eval_target_gradients", vp(_ptr(self._ws_tensors[0])),
+                           vp(_ptr(self._ws_tensors[1])), vp(_ptr(self._ws_tensors[2])),
+                           vp(_ptr(g)), err, _stream_handle())
+            out[:, :, fu] = g
+        if self.dgeo.nglobal_qbx_centers:
+            gq = torch.empty(self.nrhs, 3, nt, dtype=torch.float64, device=self.device)
+            self.plan.call("qbxfmm_eval_qbx_target_gradients", vp(_ptr(self._ws_tensors[0])),
+                           vp(_ptr(self._ws_tensors[3])), vp(_ptr(gq)), err, _stream_handle())
+            qbx = torch.ones(nt, dtype=torch.bool, device=self.device)
+            if nf:
+                qbx[torch.from_numpy(h["unfiltered_from_filtered_target_indices"][:nf]
+                                     .astype(np.int64)).to(self.device)] = False
+            sel = qbx[tt]
+            out[:, :, tu[sel]] = gq[:, :, tt[sel]]
         return out
 
     # {{{ CUDA graph

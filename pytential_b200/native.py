@@ -54,6 +54,7 @@ _STAGES = {
     "qbxfmm_transpose_form_global_qbx_locals":
         [ctypes.POINTER(abi.QBXFMMTransposeIndex), _vp, _vp, _pi, _vp],
     "qbxfmm_eval_target_gradients": [_vp, _vp, _vp, _vp, _pi, _vp],
+    "qbxfmm_eval_qbx_target_gradients": [_vp, _vp, _vp, _pi, _vp],
     "qbxfmm_apply_transpose": [_vp, ctypes.POINTER(abi.QBXFMMTransposeIndex),
                                ctypes.POINTER(abi.QBXFMMWorkspace), _vp, _vp, _vp, _vp, _vp],
     "qbxfmm_plan_set_level_orders": [_pi, _int],

@@ -179,7 +179,7 @@ def test_near_targets_adjoint_dot_products():
         lhs, rhs = float((As * r).sum()), float((sig * ATr).sum())
         assert abs(lhs - rhs) <= 1e-12 * float(torch.linalg.norm(As) * torch.linalg.norm(r))
     with pytest.raises(NotImplementedError):
-        op.target_gradient(sig)
+        op.target_gradient(sig, form="direct")
 
 # }}}
 
@@ -202,11 +202,13 @@ def test_exchanged_tree_adjoint_agrees_with_the_transpose(small):
 
 # {{{ the target gradient from the FMM's own data
 
-def test_fmm_target_gradient_against_checker_differences():
-    """qbxfmm_eval_target_gradients against central differences of the checker's apply
-    with the non-QBX targets moved and the tree held fixed (the derivative of the
-    apply's own value), far targets and near-surface ones together; zero at the
-    targets evaluated through QBX."""
+@pytest.mark.parametrize("tsqbx", [True, False])
+def test_fmm_target_gradient_against_checker_differences(tsqbx):
+    """The target gradients of the apply against central differences of the checker's
+    apply with every target moved and the tree, lists and centers held fixed (the
+    derivative of the apply's own value): far targets, targets close to the surface
+    without QBX, and QBX targets (the center's local, with or without the
+    target-specific near field)."""
     from oracle.oracle import Oracle
     from pytential_b200 import abi
     from pytential_b200.fmm import LaplaceKernel, QBXApply, SourceKernelSpec
@@ -221,34 +223,37 @@ def test_fmm_target_gradient_against_checker_differences():
     mid = d.nodes[:, i] + 1.5 * hs            # close to the surface, no QBX
     geo = QBXFMMGeometryData(d, [(w.targets, 0), (near, 0), (mid, 0)])
     spec = SourceKernelSpec(LaplaceKernel(3), charge_coeff=1.0)
-    ap = QBXApply(geo, spec, w.qbx_order, w.fmm_order, nrhs=2)
+    ap = QBXApply(geo, spec, w.qbx_order, w.fmm_order, nrhs=2, target_specific_qbx=tsqbx)
     sig = rng.normal(size=(2, d.ndofs))
     ap(torch.from_numpy(sig).cuda())
-    g = ap.nonqbx_target_gradients().cpu().numpy()                 # (2, 3, nuser)
+    g = ap.target_gradients().cpu().numpy()                        # (2, 3, nuser)
     ap.check_error_word()
     o = Oracle(geo, dim=3, qbx_order=w.qbx_order, fmm_order=w.fmm_order, nrhs=2,
                charge_coeff=1.0, family=abi.QBXFMM_LAPLACE)
     s = np.ascontiguousarray((d.upsample_density(sig) * d.quad_weights)[
         :, o.arrays["user_source_ids"][:o.scalars["nsources"]]])
     nf = o.scalars["nfiltered_targets"]
-    X = o.arrays["nonqbx_targets"]
+    X = o.arrays["nonqbx_targets"]          # the non-QBX targets' copy ...
+    T = o.arrays["targets"]                 # ... and every tree target (QBXL2P reads these)
     h = 1e-5
     fd = np.zeros_like(g)
     assert X.shape == (3, nf)
     for k in range(3):
         X[k] += h
+        T[k] += h
         up = o.apply(s)
         X[k] -= 2 * h
+        T[k] -= 2 * h
         dn = o.apply(s)
         X[k] += h
+        T[k] += h
         fd[:, k, :] = (up - dn) / (2 * h)
-    # the targets through QBX do not move (their values do not change) and get zero
     qbx = np.ones(g.shape[2], bool)
     sid = o.arrays["sorted_target_ids"]
     qbx[sid[o.arrays["unfiltered_from_filtered_target_indices"][:nf]] - o.scalars["ncenters"]] = False
     assert qbx.sum() > 0 and (~qbx).sum() > 64     # the far targets and some of mid
-    assert np.all(g[:, :, qbx] == 0)
     assert relerr(g[:, :, ~qbx], fd[:, :, ~qbx]) < 1e-7
+    assert relerr(g[:, :, qbx], fd[:, :, qbx]) < 1e-7
 
 
 def test_fmm_target_gradient_against_direct_sum(small):
@@ -280,7 +285,7 @@ def test_fmm_target_gradient_refuses_the_double_layer():
                   SourceKernelSpec(LaplaceKernel(3), dipole_coeff=1.0), 3, 8)
     ap(torch.zeros(1, w.discr.ndofs, dtype=torch.float64, device="cuda"))
     with pytest.raises(native.QBXFMMError) as ei:
-        ap.nonqbx_target_gradients()
+        ap.target_gradients()
     assert ei.value.code == abi.QBXFMM_ERR_UNSUPPORTED
 
 # }}}
