@@ -55,6 +55,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-laplace", action="store_true",
                     help="skip the 3D Laplace measurement reported beside the headline")
+    ap.add_argument("--no-side-configs", action="store_true",
+                    help="skip the batched 2D Helmholtz solve and the 3D Laplace adjoint "
+                         "reported beside the headline")
     return ap.parse_args()
 
 
@@ -407,6 +410,103 @@ def laplace_leg(torch, dev, steps, warmup, flush, fp64_peak, cpu):
     return d
 
 
+def solve2d_leg(torch, dev):
+    """The batched 2D Helmholtz Brakhage-Werner exterior Dirichlet solve (starfish,
+    2048 x 16 nodes, k 20, q 5 / p 20, 64 plane-wave right-hand sides, GMRES to 1e-8,
+    restart 50, all densities through one apply per iteration): one warm-up solve,
+    then a timed solve (CUDA events around the whole solve), one apply timed alone,
+    and the largest true relative residual."""
+    from pytential_b200.fmm import QBXApply
+    from pytential_b200.gmres import gmres
+    from pytential_b200.workloads import helmholtz2d_starfish
+    wl = helmholtz2d_starfish(nelements=2048, nrhs=64)
+    ap = QBXApply(wl.geometry(), wl.spec, wl.qbx_order, wl.fmm_order, nrhs=wl.nrhs, device=dev)
+    b = torch.from_numpy(wl.density).to(dev)
+    napply = [0]
+
+    def op(X):
+        napply[0] += 1
+        return ap(X).clone()
+    gmres(op, b, tol=1e-8, restart=50, maxiter=300)
+    napply[0] = 0
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    res = gmres(op, b, tol=1e-8, restart=50, maxiter=300)
+    e1.record()
+    torch.cuda.synchronize()
+    solve_ms = e0.elapsed_time(e1)
+    out = ap.new_output()
+    apply_ms = statistics.mean(time_calls(torch, lambda: ap.apply_into(b, out), 5,
+                                          torch.empty(64 * 1024 * 1024, dtype=torch.float32,
+                                                      device=dev)))
+    r = b - ap(res.solution)
+    rel = float((torch.linalg.norm(r, dim=1) / torch.linalg.norm(b, dim=1)).max())
+    ap.check_error_word()
+    return {"workload": "2D Helmholtz k 20 Brakhage-Werner D - ik S, starfish 2048 x 16 nodes "
+                        "(32768 unknowns), 64 plane-wave right-hand sides, qbx_order 5, "
+                        "fmm_order 20, GMRES to 1e-8 (restart 50), complex128",
+            "solve_ms": solve_ms, "iterations": int(res.iteration_count),
+            "applies": napply[0], "apply_ms": apply_ms,
+            "max_true_relative_residual": rel, "converged": bool(res.success)}
+
+
+def adjoint_leg(torch, dev):
+    """The 3D Laplace single-layer adjoint (ellipsoid icosphere-4, 76800 nodes, 5000
+    targets on the sphere of radius 3, q 4 / p 12): forward apply, the exact transpose
+    over the apply's tree, the target gradient from the FMM, and forward + backward of
+    J = |S sigma - g|^2 / 2 (density and target-position gradients), FP64 and the
+    mixed form (FP32 far field, exchanged-tree adjoint); CUDA events, 5 calls each."""
+    from pytential_b200.adjoint import FarFieldSingleLayer, single_layer
+    from pytential_b200.fmm import PRECISION_MIXED
+    from pytential_b200.workloads import laplace3d_adjoint
+    w = laplace3d_adjoint(nrefine=4, ntargets=5000)
+    sig0 = torch.from_numpy(w.sigma).to(dev)
+    X0 = torch.from_numpy(w.targets).to(dev)
+    g = torch.from_numpy(w.g(w.targets)).to(dev)
+    r0 = torch.ones(w.targets.shape[1], dtype=torch.float64, device=dev)
+
+    def timed(f):
+        for _ in range(2):
+            f()
+        ev = _events(torch, 5)
+        for a, b in ev:
+            a.record()
+            f()
+            b.record()
+        torch.cuda.synchronize()
+        return statistics.mean(a.elapsed_time(b) for a, b in ev)
+
+    out = {"workload": "3D Laplace single layer with adjoint, ellipsoid (1,1.5,2) icosphere-4 "
+                       "(5120 tri), 76800 nodes -> 230400 sources, 5000 targets on the sphere "
+                       "of radius 3, qbx_order 4, fmm_order 12"}
+    ref = None
+    for name, kw in (("fp64", {}), ("mixed", {"precision": PRECISION_MIXED})):
+        op = FarFieldSingleLayer(w.discr, w.targets, w.qbx_order, w.fmm_order, device=dev, **kw)
+
+        def fwd_bwd():
+            sigma = sig0.clone().requires_grad_(True)
+            X = X0.clone().requires_grad_(True)
+            J = 0.5 * ((single_layer(op, sigma, X) - g) ** 2).sum()
+            J.backward()
+            return sigma.grad, X.grad
+        d = {"adjoint_form": op.adjoint_form,
+             "forward_ms": timed(lambda: op.apply(sig0)),
+             "adjoint_ms": timed(lambda: op.adjoint(r0))}
+        op.apply(sig0)
+        d["target_gradient_ms"] = timed(lambda: op.target_gradient(sig0))
+        d["forward_backward_ms"] = timed(fwd_bwd)
+        gs, gx = fwd_bwd()
+        if ref is None:
+            ref = (gs, gx)
+        else:
+            d["rel_err_vs_fp64"] = {
+                "density_gradient": float((gs - ref[0]).abs().max() / ref[0].abs().max()),
+                "target_gradient": float((gx - ref[1]).abs().max() / ref[1].abs().max())}
+        out[name] = d
+    return out
+
+
 def run_b200(args):
     import torch
     import torch.distributed as dist
@@ -582,6 +682,9 @@ def run_b200(args):
         flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
         line["laplace3d"] = laplace_leg(torch, dev, 20, 5, flush, line["roofline"]["peak"],
                                         cpu=not args.no_cpu_baseline)
+    if world == 1 and not args.no_side_configs:
+        line["helmholtz2d_solve"] = solve2d_leg(torch, dev)
+        line["laplace3d_adjoint"] = adjoint_leg(torch, dev)
     del full
     print(json.dumps(line), flush=True)
 
