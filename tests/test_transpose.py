@@ -221,3 +221,32 @@ def test_gpu_transpose_rejects_other_operators():
     assert ei.value.code == abi.QBXFMM_ERR_UNSUPPORTED
 
 # }}}
+
+
+@pytest.mark.gpu
+def test_gpu_transpose_in_a_cuda_graph():
+    """qbxfmm_apply_transpose (and the index scatter around it) captured into a CUDA
+    graph and replayed on new values equals the eager transpose."""
+    import torch
+
+    from pytential_b200.fmm import LaplaceKernel, QBXApply, SourceKernelSpec
+    from pytential_b200.transpose import QBXTransposeApply
+    geo = _geometry(**CASES["near+deep"])
+    ap = QBXApply(geo, SourceKernelSpec(LaplaceKernel(3), charge_coeff=1.0), 3, 10, nrhs=2)
+    tr = QBXTransposeApply(ap)
+    r = torch.randn(2, ap.nuser_targets, dtype=torch.float64, device="cuda")
+    ref = tr(r).clone()
+    r_static = torch.zeros_like(r)
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        tr(r_static)                                   # warm-up outside the capture
+    torch.cuda.current_stream().wait_stream(s)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=s):
+        out = tr(r_static)
+    r_static.copy_(2.0 * r)
+    g.replay()
+    torch.cuda.synchronize()
+    tr.check_error_word()
+    assert relerr(out.cpu().numpy(), 2.0 * ref.cpu().numpy()) < 1e-13
