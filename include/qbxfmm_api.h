@@ -163,7 +163,8 @@ int qbxfmm_eval_qbx_target_gradients(const qbxfmm_plan* plan, const void* streng
  * `index` its reversed lists.  center_mpoles: [ncenters][nrhs][ncoeff(qbx_order)]
  * complex128.  Each output has one writer (no atomics).  QBXFMM_ERR_UNSUPPORTED for
  * other kernels, the mixed-precision form, per-level orders, qbx_order > 8 or
- * fmm_order > 21. */
+ * fmm_order > 21; these stage entries cover the single layer (the double layer runs
+ * through qbxfmm_apply_transpose). */
 
 /* transpose of eval_qbx_expansions (fmm.py:358-389): target_values [nrhs][ntargets]
  * in tree target order -> center_mpoles (written; zero for centers without targets) */
@@ -193,19 +194,23 @@ int qbxfmm_transpose_form_global_qbx_locals(const qbxfmm_plan* plan,
                                             const void* target_values, void* source_values,
                                             int32_t* error_word, void* stream);
 
-/* The whole transpose K^T r in one call: `plan` the apply's plan, `transposed` the
- * plan of its exchanged-role geometry (same boxes, transposed lists, no centers; its
- * translation matrices built into ws by qbxfmm_precompute_translations), ws a
- * workspace of `transposed` (its qbx_exps unused).  target_values: [nrhs][ntargets]
- * of the apply's tree targets; strengths: the same values at its non-QBX targets,
+/* The whole transpose K^T r in one call, for the 3D Laplace layer potential
+ * cq S + cd D (single layer, double layer or both): `plan` the apply's plan,
+ * `transposed` the plan of its exchanged-role geometry (same boxes, transposed
+ * lists, no centers, a unit single layer: charge coefficient 1; its translation
+ * matrices built into ws by qbxfmm_precompute_translations), ws a workspace of
+ * `transposed` (its qbx_exps unused).  target_values: [nrhs][ntargets] of the apply's
+ * tree targets; strengths: the same values at its non-QBX targets,
  * [nrhs][nfiltered_targets]; center_mpoles: scratch [ncenters][nrhs][ncoeff(qbx_order)]
- * complex128; out: [nrhs][nsources] at the apply's sources in tree order, with the
- * kernel scaling (written).  Runs on the transposed plan's streams like
- * qbxfmm_apply; graph-capturable. */
+ * complex128; grad_scratch: [nrhs][3][nsources] doubles, needed when cd != 0 (the
+ * transpose of a dipole layer is the normal derivative of the exchanged-role
+ * potential at the sources), else may be NULL; out: [nrhs][nsources] at the apply's
+ * sources in tree order, with the kernel scaling (written).  Runs on the transposed
+ * plan's streams like qbxfmm_apply; graph-capturable. */
 int qbxfmm_apply_transpose(const qbxfmm_plan* plan, const qbxfmm_plan* transposed,
                            const qbxfmm_transpose_index* index, const qbxfmm_workspace* ws,
                            const void* target_values, const void* strengths,
-                           void* center_mpoles, void* out, void* stream);
+                           void* center_mpoles, void* grad_scratch, void* out, void* stream);
 
 /* }}} */
 

@@ -1330,11 +1330,15 @@ int qbxfmm_eval_qbx_target_gradients(const qbxfmm_plan* p, const void* strengths
 
 namespace {
 
-int transpose_ok(const qbxfmm_plan* p)
+int transpose_ok(const qbxfmm_plan* p, bool allow_dipole = false)
 {
   if (int rc = check_plan(p)) return rc;
-  if (p->helm || p->kern.dim != 3 || p->sc.cd != 0.0)
-    return fail(QBXFMM_ERR_UNSUPPORTED, "the transposed apply covers the 3D Laplace single layer");
+  if (p->helm || p->kern.dim != 3)
+    return fail(QBXFMM_ERR_UNSUPPORTED, "the transposed apply covers 3D Laplace");
+  if (p->sc.cd != 0.0 && !allow_dipole)
+    return fail(QBXFMM_ERR_UNSUPPORTED,
+                "the transposed stage entries cover the single layer; the double layer "
+                "runs through qbxfmm_apply_transpose");
   if (p->mixed || level_orders_on(p))
     return fail(QBXFMM_ERR_UNSUPPORTED,
                 "the transposed apply runs in FP64 with one FMM order");
@@ -1392,7 +1396,8 @@ int qbxfmm_transpose_form_global_qbx_locals(const qbxfmm_plan* p, const qbxfmm_t
   if (int rc = transpose_ok(p)) return rc;
   if (!ix || !target_values || !source_values) return fail(QBXFMM_ERR_ARG, "null argument");
   QBX_TRY(launch_tr_p2qbxl(p->geo, *ix, p->kern.qbx_order, p->kern.nrhs, p->sc.cq,
-                           (const double*)target_values, (double*)source_values, err, S(stream)),
+                           (const double*)target_values, (double*)source_values, nullptr, err,
+                           S(stream)),
           "transpose_form_global_qbx_locals");
   return QBXFMM_OK;
 }
@@ -1400,16 +1405,18 @@ int qbxfmm_transpose_form_global_qbx_locals(const qbxfmm_plan* p, const qbxfmm_t
 int qbxfmm_apply_transpose(const qbxfmm_plan* p, const qbxfmm_plan* d,
                            const qbxfmm_transpose_index* ix, const qbxfmm_workspace* ws,
                            const void* target_values, const void* strengths,
-                           void* center_mpoles, void* out, void* stream)
+                           void* center_mpoles, void* grad_scratch, void* out, void* stream)
 {
-  if (int rc = transpose_ok(p)) return rc;
+  if (int rc = transpose_ok(p, true)) return rc;
   if (int rc = check_plan(d)) return rc;
   if (d->helm || d->kern.dim != 3 || d->mixed || level_orders_on(d) || d->geo.ncenters != 0 ||
       d->kern.fmm_order != p->kern.fmm_order || d->kern.nrhs != p->kern.nrhs ||
       d->geo.nboxes != p->geo.nboxes || d->geo.nsources != p->geo.nfiltered_targets ||
-      d->geo.ntargets != p->geo.nsources)
+      d->geo.ntargets != p->geo.nsources || d->sc.cq != 1.0 || d->sc.cd != 0.0)
     return fail(QBXFMM_ERR_ARG, "the second plan is not the exchanged-role plan of the first");
-  if (!ix || !ws || !target_values || !strengths || !center_mpoles || !out)
+  const bool dip = p->sc.cd != 0.0;
+  if (!ix || !ws || !target_values || !strengths || !center_mpoles || !out ||
+      (dip && !grad_scratch))
     return fail(QBXFMM_ERR_ARG, "null argument");
   if (!ws->mpoles || !ws->locals || !ws->pot_nonqbx || !ws->pot_tree)
     return fail(QBXFMM_ERR_ARG, "incomplete workspace");
@@ -1417,19 +1424,26 @@ int qbxfmm_apply_transpose(const qbxfmm_plan* p, const qbxfmm_plan* d,
   if (int rc = qbxfmm_workspace_sizes(d, sz)) return rc;
   const bool gemm = d->trans_ok && ws->translations && ws->pair_scratch;
   cudaStream_t st = S(stream);
+  const int nrhs = p->kern.nrhs, q = p->kern.qbx_order;
   QBX_TRY(cudaMemsetAsync(ws->mpoles, 0, sz[1], st), "apply_transpose: clear");
   QBX_TRY(cudaMemsetAsync(ws->locals, 0, sz[2], st), "apply_transpose: clear");
   QBX_TRY(cudaMemsetAsync(ws->pot_nonqbx, 0, sz[4], st), "apply_transpose: clear");
-  QBX_TRY(cudaMemsetAsync(ws->pot_tree, 0, sz[5], st), "apply_transpose: clear");
+  if (dip)
+    QBX_TRY(cudaMemsetAsync(grad_scratch, 0, (size_t)nrhs * 3 * p->geo.nsources * sizeof(double),
+                            st),
+            "apply_transpose: clear");
   if (ws->error_word)
     QBX_TRY(cudaMemsetAsync(ws->error_word, 0, sizeof(int32_t), st), "apply_transpose: clear");
-  int rc;
-  if ((rc = qbxfmm_transpose_eval_qbx_expansions(p, target_values, center_mpoles, ws->error_word,
-                                                 stream)))
-    return rc;
+  // every value below is of the unit-charge exchanged-role potential; the layer's
+  // coefficients enter once, at the sources (k_tr_combine)
+  size_t cbytes = (size_t)p->geo.ncenters * nrhs * p->ncq * 2 * sizeof(double);
+  if (cbytes) QBX_TRY(cudaMemsetAsync(center_mpoles, 0, cbytes, st), "apply_transpose: clear");
+  QBX_TRY(launch_tr_qbxl2p(p->geo, q, nrhs, 1.0, (const double*)target_values,
+                           (double2*)center_mpoles, ws->error_word, st),
+          "apply_transpose: center multipoles");
   // The exchanged-role stage graph on the second plan's four streams, as in
   // qbxfmm_apply, with the transposed QBX stages where their outputs are consumed:
-  //   caller's stream: P2M, L2QBXL^T, M2M | M2L, L2L | L2P, assembly
+  //   caller's stream: P2M, L2QBXL^T, M2M | M2L, L2L | L2P, gradients, combination
   //   side[0]:         P2P, P2QBXL^T | M2P
   //   side[1]:         P2L, M2QBXL^T
   // (every stage adds into its outputs; the writers of one buffer never overlap)
@@ -1437,6 +1451,7 @@ int qbxfmm_apply_transpose(const qbxfmm_plan* p, const qbxfmm_plan* d,
   void* s1 = d->side[0];
   void* s2 = d->side[1];
   bool forked = false;
+  int rc;
   auto join = [&](int code) -> int {
     if (forked) {
       cudaEventRecord(d->ev_near, side1);
@@ -1457,19 +1472,25 @@ int qbxfmm_apply_transpose(const qbxfmm_plan* p, const qbxfmm_plan* d,
     if ((rc = cuda_check((call), what))) return join(rc);   \
   } while (0)
   QBX_CUDA_STEP(cudaEventRecord(d->ev_fork, st), "apply_transpose: fork");
-  for (cudaStream_t s : {side1, side2, side3})
-    QBX_CUDA_STEP(cudaStreamWaitEvent(s, d->ev_fork, 0), "apply_transpose: fork");
+  for (cudaStream_t sx : {side1, side2, side3})
+    QBX_CUDA_STEP(cudaStreamWaitEvent(sx, d->ev_fork, 0), "apply_transpose: fork");
   forked = true;
   QBX_STEP(qbxfmm_form_locals(d, strengths, ws->locals, ws->error_word, s2));
-  QBX_STEP(qbxfmm_transpose_translate_box_multipoles_to_qbx_local(p, ix, center_mpoles, ws->locals,
-                                                                  ws->error_word, s2));
+  QBX_CUDA_STEP(launch_tr_m2qbxl(p->geo, *ix, p->kern.fmm_order, q, nrhs,
+                                 (const double2*)center_mpoles, (double2*)ws->locals,
+                                 ws->error_word, side2),
+                "apply_transpose: M2QBXL^T");
   QBX_CUDA_STEP(cudaEventRecord(d->ev_p2l, side2), "apply_transpose: P2L event");
   QBX_STEP(qbxfmm_eval_direct(d, strengths, ws->pot_nonqbx, ws->error_word, s1));
-  QBX_STEP(qbxfmm_transpose_form_global_qbx_locals(p, ix, target_values, ws->pot_nonqbx,
-                                                   ws->error_word, s1));
+  QBX_CUDA_STEP(launch_tr_p2qbxl(p->geo, *ix, q, nrhs, 1.0, (const double*)target_values,
+                                 (double*)ws->pot_nonqbx, dip ? (double*)grad_scratch : nullptr,
+                                 ws->error_word, side1),
+                "apply_transpose: P2QBXL^T");
   QBX_STEP(qbxfmm_form_multipoles(d, strengths, ws->mpoles, stream));
-  QBX_STEP(qbxfmm_transpose_translate_box_local_to_qbx_local(p, ix, center_mpoles, ws->mpoles,
-                                                             ws->error_word, stream));
+  QBX_CUDA_STEP(launch_tr_l2qbxl(p->geo, *ix, p->kern.fmm_order, q, nrhs,
+                                 (const double2*)center_mpoles, (double2*)ws->mpoles,
+                                 ws->error_word, st),
+                "apply_transpose: L2QBXL^T");
   QBX_STEP(run_m2m(d, ws, nullptr, gemm, stream));
   QBX_CUDA_STEP(cudaEventRecord(d->ev_mpoles, st), "apply_transpose: multipole event");
   QBX_CUDA_STEP(cudaStreamWaitEvent(side1, d->ev_mpoles, 0), "apply_transpose: multipole event");
@@ -1485,7 +1506,19 @@ int qbxfmm_apply_transpose(const qbxfmm_plan* p, const qbxfmm_plan* d,
   forked = false;
 #undef QBX_STEP
 #undef QBX_CUDA_STEP
-  return qbxfmm_assemble(d, ws->pot_nonqbx, ws->pot_tree, out, stream);
+  // the dipole part: the gradient of the exchanged-role potential at the sources
+  // (P2P, M2P, L2P differentiated there), the near-field part already added
+  if (dip)
+    QBX_TRY(launch_grad_targets(d->geo, 1.0, 1.0, d->kern.fmm_order, nrhs,
+                                (const double*)strengths, (const double2*)ws->mpoles,
+                                (const double2*)ws->locals, (double*)grad_scratch, ws->error_word,
+                                st),
+            "apply_transpose: gradients");
+  QBX_TRY(launch_tr_combine(p->geo, nrhs, 0.25 / M_PI, p->sc.cq, p->sc.cd,
+                            (const double*)ws->pot_nonqbx, dip ? (const double*)grad_scratch : nullptr,
+                            (double*)out, st),
+          "apply_transpose: combination");
+  return QBXFMM_OK;
 }
 
 // }}}

@@ -196,8 +196,11 @@ cudaError_t launch_tr_m2qbxl(const qbxfmm_geometry& g, const qbxfmm_transpose_in
                              int q, int nrhs, const double2* cmp, double2* locals, int32_t* err,
                              cudaStream_t st);
 cudaError_t launch_tr_p2qbxl(const qbxfmm_geometry& g, const qbxfmm_transpose_index& ix, int q,
-                             int nrhs, double cq, const double* tvals, double* vals, int32_t* err,
-                             cudaStream_t st);
+                             int nrhs, double cq, const double* tvals, double* vals, double* grads,
+                             int32_t* err, cudaStream_t st);
+cudaError_t launch_tr_combine(const qbxfmm_geometry& g, int nrhs, double scale, double cq,
+                              double cd, const double* vals, const double* grads, double* out,
+                              cudaStream_t st);
 
 // gradient of the 3D Laplace single layer at the non-QBX targets (kernels_fmmgrad.cu)
 cudaError_t launch_grad_targets(const qbxfmm_geometry& g, double cq, double scale, int p,

@@ -16,7 +16,9 @@
 //   k_tr_tsqbx    transpose of P2QBXL (fmm.py:231-265): per source box s, the
 //                 (target, center) pairs of every center box whose list 1 holds s,
 //                 evaluated at the sources of s in the target-specific form (the
-//                 Legendre sum of the truncated expansion, symmetric in the roles)
+//                 Legendre sum of the truncated expansion, symmetric in the roles),
+//                 and for a dipole layer its gradient in the source position
+//   k_tr_combine  cq value + cd normal . gradient at the sources (charge + dipole)
 //
 // Each output (a box expansion, a source value) has one writer: the kernels gather
 // over the reversed lists of qbxfmm_transpose_index, so results do not depend on
@@ -331,10 +333,11 @@ k_tr_m2qbxl(qbxfmm_geometry g, qbxfmm_transpose_index ix, int p, int q, int ncf,
 constexpr int TR_KS = 4;
 constexpr int TR_PB = NT;
 
-template <int Q>
+template <int Q, bool DIP>
 __global__ void __launch_bounds__(NT)
 k_tr_tsqbx(qbxfmm_geometry g, qbxfmm_transpose_index ix, int nrhs, double cq,
-           const double* __restrict__ tvals, double* __restrict__ vals, int32_t* err)
+           const double* __restrict__ tvals, double* __restrict__ vals,
+           double* __restrict__ grads, int32_t* err)
 {
   __shared__ double s_c[3][TR_PB], s_ah[3][TR_PB], s_al[TR_PB], s_w[TR_PB];
   int s = ix.list1_rows[blockIdx.x];
@@ -347,11 +350,12 @@ k_tr_tsqbx(qbxfmm_geometry g, qbxfmm_transpose_index ix, int nrhs, double cq,
   }
   const double* tv = tvals + (size_t)r * g.ntargets;
   for (int g0 = 0; g0 < ns; g0 += NT * TR_KS) {
-    double y[TR_KS][3], acc[TR_KS];
+    double y[TR_KS][3], acc[TR_KS], gacc[DIP ? TR_KS : 1][3];
 #pragma unroll
     for (int k = 0; k < TR_KS; ++k) {
       int jj = g0 + threadIdx.x + k * NT;
       acc[k] = 0.0;
+      if (DIP) gacc[DIP ? k : 0][0] = gacc[DIP ? k : 0][1] = gacc[DIP ? k : 0][2] = 0.0;
       if (jj < ns) load_point<3>(g.sources, g.nsources, s0 + jj, y[k]);
       else y[k][0] = y[k][1] = y[k][2] = 0.0;
     }
@@ -396,18 +400,31 @@ k_tr_tsqbx(qbxfmm_geometry g, qbxfmm_transpose_index ix, int nrhs, double cq,
             double binv = rsqrt(b0 * b0 + b1 * b1 + b2 * b2);
             double cg = (hx * b0 + hy * b1 + hz * b2) * binv;
             double ratio = al * binv;
-            double pm1 = 1.0, pm2 = 0.0, rn = binv, sum = 0.0;
+            double pm1 = 1.0, pm2 = 0.0, dm1 = 0.0, rn = binv, sum = 0.0, sa = 0.0, sb = 0.0;
 #pragma unroll
             for (int n = 0; n <= Q; ++n) {
               double pn = n == 0 ? 1.0
                         : n == 1 ? cg
                                  : ((2.0 * n - 1) * cg * pm1 - (n - 1.0) * pm2) * (1.0 / n);
               sum = fma(rn, pn, sum);
+              if (DIP) {
+                double dn = n == 0 ? 0.0 : n * pm1 + cg * dm1;
+                sa = fma(-(n + 1.0) * rn, pn, sa);
+                sb = fma(rn, dn, sb);
+                dm1 = dn;
+              }
               pm2 = pm1;
               pm1 = pn;
               rn *= ratio;
             }
             acc[k] = fma(w, sum, acc[k]);
+            if (DIP) {
+              // grad_b K = (sa b^ + sb (a^ - cos g b^)) / |b|
+              double fb = w * binv * (sa - sb * cg), fa = w * binv * sb;
+              gacc[DIP ? k : 0][0] += fb * b0 * binv + fa * hx;
+              gacc[DIP ? k : 0][1] += fb * b1 * binv + fa * hy;
+              gacc[DIP ? k : 0][2] += fb * b2 * binv + fa * hz;
+            }
           }
         }
       }
@@ -415,7 +432,15 @@ k_tr_tsqbx(qbxfmm_geometry g, qbxfmm_transpose_index ix, int nrhs, double cq,
 #pragma unroll
     for (int k = 0; k < TR_KS; ++k) {
       int jj = g0 + threadIdx.x + k * NT;
-      if (jj < ns) vals[(size_t)r * g.nsources + s0 + jj] += acc[k];
+      if (jj < ns) {
+        vals[(size_t)r * g.nsources + s0 + jj] += acc[k];
+        if (DIP) {
+          double* gr = grads + (size_t)r * 3 * g.nsources + s0 + jj;
+          gr[0] += gacc[DIP ? k : 0][0];
+          gr[g.nsources] += gacc[DIP ? k : 0][1];
+          gr[2 * (size_t)g.nsources] += gacc[DIP ? k : 0][2];
+        }
+      }
     }
   }
 }
@@ -470,30 +495,65 @@ cudaError_t launch_tr_m2qbxl(const qbxfmm_geometry& g, const qbxfmm_transpose_in
 
 template <int Q>
 static cudaError_t tr_tsqbx_q(const qbxfmm_geometry& g, const qbxfmm_transpose_index& ix,
-                              int nrhs, double cq, const double* tvals, double* vals, int32_t* err,
-                              cudaStream_t st)
+                              int nrhs, double cq, const double* tvals, double* vals,
+                              double* grads, int32_t* err, cudaStream_t st)
 {
-  k_tr_tsqbx<Q><<<dim3(ix.nlist1_rows, nrhs), NT, 0, st>>>(g, ix, nrhs, cq, tvals, vals, err);
+  if (grads)
+    k_tr_tsqbx<Q, true><<<dim3(ix.nlist1_rows, nrhs), NT, 0, st>>>(g, ix, nrhs, cq, tvals, vals,
+                                                                   grads, err);
+  else
+    k_tr_tsqbx<Q, false><<<dim3(ix.nlist1_rows, nrhs), NT, 0, st>>>(g, ix, nrhs, cq, tvals, vals,
+                                                                    nullptr, err);
   return cudaGetLastError();
 }
 
 cudaError_t launch_tr_p2qbxl(const qbxfmm_geometry& g, const qbxfmm_transpose_index& ix, int q,
-                             int nrhs, double cq, const double* tvals, double* vals, int32_t* err,
-                             cudaStream_t st)
+                             int nrhs, double cq, const double* tvals, double* vals, double* grads,
+                             int32_t* err, cudaStream_t st)
 {
   if (ix.nlist1_rows == 0) return cudaSuccess;
   switch (q) {
-    case 0: return tr_tsqbx_q<0>(g, ix, nrhs, cq, tvals, vals, err, st);
-    case 1: return tr_tsqbx_q<1>(g, ix, nrhs, cq, tvals, vals, err, st);
-    case 2: return tr_tsqbx_q<2>(g, ix, nrhs, cq, tvals, vals, err, st);
-    case 3: return tr_tsqbx_q<3>(g, ix, nrhs, cq, tvals, vals, err, st);
-    case 4: return tr_tsqbx_q<4>(g, ix, nrhs, cq, tvals, vals, err, st);
-    case 5: return tr_tsqbx_q<5>(g, ix, nrhs, cq, tvals, vals, err, st);
-    case 6: return tr_tsqbx_q<6>(g, ix, nrhs, cq, tvals, vals, err, st);
-    case 7: return tr_tsqbx_q<7>(g, ix, nrhs, cq, tvals, vals, err, st);
-    case 8: return tr_tsqbx_q<8>(g, ix, nrhs, cq, tvals, vals, err, st);
+    case 0: return tr_tsqbx_q<0>(g, ix, nrhs, cq, tvals, vals, grads, err, st);
+    case 1: return tr_tsqbx_q<1>(g, ix, nrhs, cq, tvals, vals, grads, err, st);
+    case 2: return tr_tsqbx_q<2>(g, ix, nrhs, cq, tvals, vals, grads, err, st);
+    case 3: return tr_tsqbx_q<3>(g, ix, nrhs, cq, tvals, vals, grads, err, st);
+    case 4: return tr_tsqbx_q<4>(g, ix, nrhs, cq, tvals, vals, grads, err, st);
+    case 5: return tr_tsqbx_q<5>(g, ix, nrhs, cq, tvals, vals, grads, err, st);
+    case 6: return tr_tsqbx_q<6>(g, ix, nrhs, cq, tvals, vals, grads, err, st);
+    case 7: return tr_tsqbx_q<7>(g, ix, nrhs, cq, tvals, vals, grads, err, st);
+    case 8: return tr_tsqbx_q<8>(g, ix, nrhs, cq, tvals, vals, grads, err, st);
     default: return cudaErrorInvalidValue;
   }
+}
+
+// out[r][j] = scale (cq vals[r][j] + cd n_j . grads[r][.][j]) at the apply's sources
+// (tree order): the transpose of a charge + dipole layer from the exchanged-role
+// potential and its gradient there
+__global__ void k_tr_combine(qbxfmm_geometry g, int nrhs, double scale, double cq, double cd,
+                             const double* __restrict__ vals, const double* __restrict__ grads,
+                             double* __restrict__ out)
+{
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  int r = blockIdx.y;
+  if (j >= g.nsources) return;
+  double v = cq * vals[(size_t)r * g.nsources + j];
+  if (grads) {
+    const double* gr = grads + (size_t)r * 3 * g.nsources + j;
+    double n[3];
+    load_point<3>(g.source_normals, g.nsources, j, n);
+    v += cd * (n[0] * gr[0] + n[1] * gr[g.nsources] + n[2] * gr[2 * (size_t)g.nsources]);
+  }
+  out[(size_t)r * g.nsources + j] = scale * v;
+}
+
+cudaError_t launch_tr_combine(const qbxfmm_geometry& g, int nrhs, double scale, double cq,
+                              double cd, const double* vals, const double* grads, double* out,
+                              cudaStream_t st)
+{
+  if (g.nsources == 0) return cudaSuccess;
+  k_tr_combine<<<dim3((g.nsources + 255) / 256, nrhs), 256, 0, st>>>(g, nrhs, scale, cq, cd,
+                                                                     vals, grads, out);
+  return cudaGetLastError();
 }
 
 // }}}

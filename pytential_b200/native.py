@@ -56,7 +56,8 @@ _STAGES = {
     "qbxfmm_eval_target_gradients": [_vp, _vp, _vp, _vp, _pi, _vp],
     "qbxfmm_eval_qbx_target_gradients": [_vp, _vp, _vp, _pi, _vp],
     "qbxfmm_apply_transpose": [_vp, ctypes.POINTER(abi.QBXFMMTransposeIndex),
-                               ctypes.POINTER(abi.QBXFMMWorkspace), _vp, _vp, _vp, _vp, _vp],
+                               ctypes.POINTER(abi.QBXFMMWorkspace), _vp, _vp, _vp, _vp, _vp,
+                               _vp],
     "qbxfmm_plan_set_level_orders": [_pi, _int],
     "qbxfmm_plan_get_level_orders": [_pi, _int],
 }

@@ -268,13 +268,15 @@ def transpose_index(geo) -> TransposeIndex:
 
 
 class QBXTransposeApply:
-    """The transpose of a 3D Laplace single-layer :class:`~pytential_b200.fmm.QBXApply`
-    (FP64, one FMM order) on its device: ``A^T r`` for values ``r`` at the apply's
-    user targets, ``(nrhs, nuser_targets) -> (nrhs, ndofs)``, with ``A = K W U``
-    (upsampling ``U``, weights ``W``, the QBX-FMM kernel matrix ``K``) and
-    ``A^T = U^T W K^T``.  ``K^T`` runs over the apply's own tree in one C-ABI call
-    (``qbxfmm_apply_transpose``): the exchanged-role geometry's plan with its
-    translation matrices, and the four transposed QBX stages on the apply's plan."""
+    """The transpose of a 3D Laplace :class:`~pytential_b200.fmm.QBXApply` (single
+    layer, double layer or both; FP64, one FMM order) on its device: ``A^T r`` for
+    values ``r`` at the apply's user targets, ``(nrhs, nuser_targets) -> (nrhs,
+    ndofs)``, with ``A = K W U`` (upsampling ``U``, weights ``W``, the QBX-FMM kernel
+    matrix ``K``) and ``A^T = U^T W K^T``.  ``K^T`` runs over the apply's own tree in
+    one C-ABI call (``qbxfmm_apply_transpose``): the exchanged-role geometry's plan (a
+    unit single layer) with its translation matrices, the transposed QBX stages on the
+    apply's plan, and for a dipole part the gradient of the exchanged-role potential at
+    the sources along their normals."""
 
     def __init__(self, apply):
         import torch
@@ -282,11 +284,12 @@ class QBXTransposeApply:
         from .fmm import (PRECISION_FP64, B200QBXExpansionWrangler,
                           B200TreeIndependentDataForWrangler, DeviceGeometry, Plan, _ptr,
                           _stream_handle)
+        from .fmm import LaplaceKernel, SourceKernelSpec
         plan = apply.plan
         spec = plan.spec
-        if spec.kernel.family != abi.QBXFMM_LAPLACE or spec.kernel.dim != 3 \
-                or spec.dipole_coeff != 0:
-            raise NotImplementedError("the transposed apply covers the 3D Laplace single layer")
+        if spec.kernel.family != abi.QBXFMM_LAPLACE or spec.kernel.dim != 3:
+            raise NotImplementedError("the transposed apply covers 3D Laplace")
+        self.has_dipole = spec.dipole_coeff != 0
         if plan.precision != PRECISION_FP64 or len(set(plan.get_level_orders())) > 1:
             raise NotImplementedError("the transposed apply runs in FP64 with one FMM order")
         self.fwd = apply
@@ -294,7 +297,8 @@ class QBXTransposeApply:
         self.device = dev = apply.device
         self.dual_geo = TransposedGeometryData(apply.geo)
         self.dual_dgeo = DeviceGeometry(self.dual_geo, dev)
-        self.dual_plan = Plan(self.dual_dgeo, spec, plan.qbx_order, plan.fmm_order, nrhs)
+        self.dual_spec = SourceKernelSpec(LaplaceKernel(3), charge_coeff=1.0)
+        self.dual_plan = Plan(self.dual_dgeo, self.dual_spec, plan.qbx_order, plan.fmm_order, nrhs)
         self._wrangler_args = (B200QBXExpansionWrangler, B200TreeIndependentDataForWrangler)
         self._dual_wrangler = None
 
@@ -347,6 +351,8 @@ class QBXTransposeApply:
         self.nuser_targets = sc["nuser_targets"]
         self.ncq = plan.ncq
         self._cm = torch.zeros(max(nc, 1), nrhs, self.ncq, dtype=torch.complex128, device=dev)
+        self._grad = (torch.zeros(nrhs, 3, self.nsources, dtype=torch.float64, device=dev)
+                      if self.has_dipole else None)
 
     def _inputs(self, r):
         """Tree-target values and the non-QBX ones (the exchanged-role strengths)."""
@@ -375,9 +381,11 @@ class QBXTransposeApply:
         r_tree, s_dual = self._inputs(r)
         out = torch.empty(self.nrhs, self.nsources, dtype=torch.float64, device=self.device)
         vp = ctypes.c_void_p
+        grad = vp(_ptr(self._grad)) if self._grad is not None else vp(0)
         self.fwd.plan.call("qbxfmm_apply_transpose", self.dual_plan.handle,
                            ctypes.byref(self.index), ctypes.byref(self.ws), vp(_ptr(r_tree)),
-                           vp(_ptr(s_dual)), vp(_ptr(self._cm)), vp(_ptr(out)), _stream_handle())
+                           vp(_ptr(s_dual)), vp(_ptr(self._cm)), grad, vp(_ptr(out)),
+                           _stream_handle())
         return self._to_user(out)
 
     def kernel_transpose_by_stages(self, r):
@@ -387,6 +395,8 @@ class QBXTransposeApply:
         import torch
 
         from .fmm import _stream_handle
+        if self.has_dipole:
+            raise NotImplementedError("the transposed stage entries cover the single layer")
         if self._dual_wrangler is None:
             Wcls, Tcls = self._wrangler_args
             p = self.fwd.plan

@@ -195,19 +195,18 @@ def test_gpu_transpose_dot_products(case, tsqbx):
 
 
 @pytest.mark.gpu
-def test_gpu_transpose_rejects_other_operators():
+def test_gpu_transpose_refusals():
     from pytential_b200 import native
     from pytential_b200.fmm import PRECISION_MIXED, LaplaceKernel, QBXApply, SourceKernelSpec
     from pytential_b200.transpose import QBXTransposeApply
     geo = _geometry(0, shell=10)
     dl = QBXApply(geo, SourceKernelSpec(LaplaceKernel(3), dipole_coeff=1.0), 3, 8)
-    with pytest.raises(NotImplementedError):
-        QBXTransposeApply(dl)
     mixed = QBXApply(geo, SourceKernelSpec(LaplaceKernel(3), charge_coeff=1.0), 3, 8,
                      precision=PRECISION_MIXED)
     with pytest.raises(NotImplementedError):
         QBXTransposeApply(mixed)
-    # the C ABI refuses a double-layer plan as well, before any launch
+    # the stage entries refuse a double-layer plan (it runs through the one-call
+    # transpose), before any launch
     import ctypes
 
     import torch
@@ -250,3 +249,54 @@ def test_gpu_transpose_in_a_cuda_graph():
     torch.cuda.synchronize()
     tr.check_error_word()
     assert relerr(out.cpu().numpy(), 2.0 * ref.cpu().numpy()) < 1e-13
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("cq,cd", [(0.0, 1.0), (1.0, 0.5)])
+def test_gpu_double_layer_transpose_is_the_checker_matrix_transpose(cq, cd):
+    """The double layer and S + D/2: the GPU transpose (the normal derivative of the
+    exchanged-role potential at the sources, plus the value) applied to every unit
+    vector equals the transpose of the checker's apply matrix (20 triangles, near and
+    far targets)."""
+    import torch
+
+    from oracle.oracle import Oracle
+    from pytential_b200.fmm import LaplaceKernel, QBXApply, SourceKernelSpec
+    from pytential_b200.transpose import QBXTransposeApply
+    geo = _geometry(0, near=30, shell=20)
+    o1 = _oracle(geo, nrhs=1)
+    ns, nu = o1.scalars["nsources"], o1.scalars["nuser_targets"]
+    A = Oracle(geo, dim=3, qbx_order=3, fmm_order=10, nrhs=ns, charge_coeff=cq,
+               dipole_coeff=cd, family=abi.QBXFMM_LAPLACE).apply(np.eye(ns)).T   # (nu, ns) tree
+    spec = SourceKernelSpec(LaplaceKernel(3), charge_coeff=cq, dipole_coeff=cd)
+    ap = QBXApply(geo, spec, 3, 10, nrhs=nu)
+    tr = QBXTransposeApply(ap)
+    assert tr.has_dipole
+    got = tr.kernel_transpose(torch.eye(nu, dtype=torch.float64, device="cuda")).cpu().numpy()
+    tr.check_error_word()
+    usid = o1.arrays["user_source_ids"][:ns]
+    assert relerr(got[:, usid], A) < 1e-12          # user source order -> tree order
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("cq,cd", [(0.0, 1.0), (1.0, 0.5)])
+def test_gpu_double_layer_transpose_dot_products(case, cq, cd):
+    import torch
+
+    from pytential_b200.fmm import LaplaceKernel, QBXApply, SourceKernelSpec
+    from pytential_b200.transpose import QBXTransposeApply
+    _, geo = case
+    spec = SourceKernelSpec(LaplaceKernel(3), charge_coeff=cq, dipole_coeff=cd)
+    ap = QBXApply(geo, spec, 3, 10, nrhs=2)
+    tr = QBXTransposeApply(ap)
+    rng = np.random.default_rng(21)
+    sig = torch.from_numpy(rng.normal(size=(2, ap.ndofs))).cuda()
+    r = torch.from_numpy(rng.normal(size=(2, ap.nuser_targets))).cuda()
+    As, ATr = ap(sig), tr(r)
+    ap.check_error_word()
+    tr.check_error_word()
+    lhs, rhs = (As * r).sum(1), (sig * ATr).sum(1)
+    scale = torch.linalg.norm(As, dim=1) * torch.linalg.norm(r, dim=1)
+    assert bool(((lhs - rhs).abs() <= 1e-12 * scale).all())
+    with pytest.raises(NotImplementedError):
+        tr.kernel_transpose_by_stages(r)
