@@ -4,9 +4,11 @@
 # for the 3D QBX near field.  Sources are read in place and never copied into the
 # repository; outputs go only to oracle/_ref/ (git-ignored).
 set -euo pipefail
-REF=${PYTENTIAL_REFERENCE:-/root/reference}
-SRC="$REF/pytential/qbx/target_specific"
 HERE="$(cd "$(dirname "$0")" && pwd)"
+# the reference checkout: $PYTENTIAL_REFERENCE, else a "reference" directory beside
+# this repository
+REF=${PYTENTIAL_REFERENCE:-"$(cd "$HERE/../.." && pwd)/reference"}
+SRC="$REF/pytential/qbx/target_specific"
 OUT="$HERE/_ref"
 if [ ! -f "$SRC/impl.pyx" ]; then
   echo "reference sources not found at $SRC: oracle/_ref not built (set PYTENTIAL_REFERENCE)" >&2
