@@ -323,6 +323,52 @@ def cpu_checker_sample(threads, reps=1):
     return wl, out, times
 
 
+def reference_near_field_sample(wl, threads):
+    """The reference's own compiled target-specific QBX module
+    (pytential/qbx/target_specific, built from its sources into oracle/_ref) on the
+    near field of the CPU sample: every (QBX target, list-1 source) pair of the
+    icosphere-2 surface for D - ik S at the headline's k and qbx_order, one density, all
+    host threads (its OpenMP loop).  That module truncates the 3D Helmholtz series in
+    spherical waves (the reference's fmmlib form); the pair work is the same as the
+    near field of the headline's sumpy truncation.  None when the module is not
+    built."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle", "_ref"))
+    try:
+        import impl
+    except ImportError:
+        return None
+    from pytential_b200 import abi, costs
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    geo = wl.geometry(builders="host")
+    scal, A = abi.geometry_arrays(geo)
+    s = wl.tree_strengths()[0].astype(complex)
+    sp = wl.spec
+    charges = complex(sp.charge_coeff) * s
+    dipoles = complex(sp.dipole_coeff) * s
+    pot = np.zeros(scal["ntargets"], complex)
+    grad = np.zeros((3, scal["ntargets"]), complex)
+
+    def run():
+        pot[:] = 0
+        impl.eval_target_specific_qbx_locals(
+            1, 0, 1, 1, wl.qbx_order, A["sources"], A["targets"], A["centers"],
+            A["global_qbx_centers"], A["qbx_center_to_target_box"],
+            A["center_to_targets_starts"], A["center_to_targets_lists"], A["list1_starts"],
+            A["list1_lists"], A["box_source_starts"], A["box_source_counts_nonchild"],
+            complex(sp.wave_number), charges, dipoles, A["source_normals"], pot, grad)
+    run()
+    t0 = time.perf_counter()
+    run()
+    dt = time.perf_counter() - t0
+    pairs = costs.tsqbx_pairs(A, scal)
+    return {"kind": "reference", "cores": threads, "ms": 1e3 * dt, "pairs": int(pairs),
+            "pairs_per_s": pairs / dt,
+            "sample": "the 3D Helmholtz near field (D - ik S, k 10, qbx_order 5) of every "
+                      "QBX target over its center's list-1 sources, icosphere-2 ellipsoid "
+                      "(14400 sources), one density, by the reference's compiled "
+                      "target-specific module (spherical-wave truncation)"}
+
+
 SAMPLE_TEXT = ("the full apply of the same operator (D - ik S, k 10, qbx_order 5, fmm_order "
                "15) on the icosphere-2 ellipsoid (320 tri, 4800 nodes -> 14400 sources) with "
                "one of the 16 densities, scaled to node-applies/s")
@@ -645,7 +691,13 @@ def run_b200(args):
                 "traffic": traffic, "traffic_source": tcase,
                 "stages_ms": {k: round(v, 3) for k, v in kt.items()},
                 "stages_tflops_algorithmic": {
-                    k: round(alg[k] / (kt[k] * 1e-3) / 1e12, 3) for k in kt}},
+                    k: round(alg[k] / (kt[k] * 1e-3) / 1e12, 3) for k in kt},
+                # sum over the stages of their algorithmic bound over the step time; the
+                # algorithmic M2L count is the dense C_f^2 product, more than the
+                # rotation-based translation performs, so that stage can exceed 1
+                "apply": costs.apply_roofline(
+                    kt, alg, costs.stage_hbm_bytes(scal, 3, True, wl.fmm_order, count),
+                    fp64_peak, peaks.get("hbm_gbs"), 1e3 * t_max / K)},
             "e2e": {"value": e2e_value, "unit": UNIT,
                     "h2d_bytes_per_step": ap.h2d_bytes * world,
                     "d2h_bytes_per_step": ap.d2h_bytes * world},
@@ -666,6 +718,16 @@ def run_b200(args):
         cpu_t = statistics.mean(times)
         line["cpu_baseline"] = {"value": swl.nuser_targets * swl.nrhs / cpu_t, "unit": UNIT,
                                 "cores": threads, "kind": "port", "sample": SAMPLE_TEXT}
+        nf = reference_near_field_sample(swl, threads)
+        if nf is not None:
+            # the GPU's near field at the headline size, per (target, source) pair and
+            # density, beside it
+            arr, scal = ap.dgeo.host_arrays, ap.dgeo.scalars
+            gpu_pairs = costs.tsqbx_pairs(arr, scal) * count
+            ms = line["roofline"]["stages_ms"].get("eval_target_specific_qbx_locals")
+            if ms:
+                nf["gpu_pairs_per_s"] = gpu_pairs / (ms * 1e-3)
+            line["cpu_baseline"]["reference_near_field"] = nf
         # parity spot check on the sample: the GPU forms against the checker
         sap = QBXApply(swl.geometry(), swl.spec, swl.qbx_order, swl.fmm_order, nrhs=swl.nrhs,
                        device=dev, target_specific_qbx=True)

@@ -226,3 +226,37 @@ def algorithmic_flops(arrays: dict, scalars: dict, dim: int, complex_: bool, pf:
     return {k: int(v) * nrhs for k, v in out.items()}
 
 # }}}
+
+
+# {{{ apply-level roofline
+
+#: stages bounded by HBM bandwidth (the rest by the FP64 pipe), as classified for the
+#: apply roofline: the box-to-box shifts and the local evaluation move coefficients
+#: with a few flops per byte
+HBM_STAGES = ("coarsen_multipoles", "refine_locals", "eval_locals")
+
+
+def stage_hbm_bytes(scalars: dict, dim: int, complex_: bool, pf: int, nrhs: int = 1) -> dict:
+    """Algorithmic DRAM bytes of the HBM-bound stages: read + write of the box
+    coefficient arrays (nboxes x ncoeff x nrhs values) once each."""
+    val = (16 if complex_ else 8) * nrhs
+    box = scalars["nboxes"] * coeff_count(dim, pf) * val
+    return {"coarsen_multipoles": 2 * box, "refine_locals": 2 * box,
+            "eval_locals": box + scalars["nfiltered_targets"] * (8 if not complex_ else 16) * nrhs}
+
+
+def apply_roofline(stage_ms: dict, flops: dict, hbm_bytes: dict, fp64_tflops: float,
+                   hbm_gbs: float, step_ms: float) -> dict:
+    """sum_stage (W_stage / peak_stage) / t_step over the timed stages: the FP64 pipe for
+    the arithmetic stages (algorithmic flops), HBM for ``HBM_STAGES`` (algorithmic
+    bytes); with the per-stage lower bounds in ms."""
+    lb = {}
+    for k in stage_ms:
+        if k in HBM_STAGES and hbm_gbs:
+            lb[k] = hbm_bytes.get(k, 0) / (hbm_gbs * 1e9) * 1e3
+        else:
+            lb[k] = flops.get(k, 0) / (fp64_tflops * 1e12) * 1e3
+    return {"frac": sum(lb.values()) / step_ms,
+            "lower_bound_ms": {k: round(v, 3) for k, v in lb.items()}}
+
+# }}}
