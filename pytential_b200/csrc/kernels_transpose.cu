@@ -21,19 +21,27 @@
 //   k_tr_combine  cq value + cd normal . gradient at the sources (charge + dipole)
 //
 // Each output (a box expansion, a source value) has one writer: the kernels gather
-// over the reversed lists of qbxfmm_transpose_index, so results do not depend on
-// scheduling.  The box stages of the transpose are the library's own P2M / M2M /
+// over the reversed lists of qbxfmm_transpose_index (M2QBXL^T and P2QBXL^T, when the
+// rows are too few to fill the GPU, with a cluster of TR_CL CTAs per row whose partial
+// sums rank 0 adds in rank order through distributed shared memory), so results do not
+// depend on scheduling.  The box stages of the transpose are the library's own P2M / M2M /
 // M2L / M2P / P2L / L2L / L2P / P2P on the exchanged-role geometry.
 #include "laplace.cuh"
 #include "kernels.h"
 
 #include <algorithm>
 
+#include <cooperative_groups.h>
+namespace cg = cooperative_groups;
+
 namespace qbx {
 
 namespace {
 
 constexpr int NT = 128;
+constexpr int TR_CL = 8;      // CTAs per row (a cluster) in M2QBXL^T and P2QBXL^T when
+                              // the rows alone would not fill the GPU
+constexpr int TR_SPLIT_BELOW = 4 * 148;   // rows below which a row is split
 
 QBX_D bool box_ok(const qbxfmm_geometry& g, int b, int32_t* err)
 {
@@ -214,11 +222,14 @@ k_tr_l2qbxl(qbxfmm_geometry g, qbxfmm_transpose_index ix, int p, int q, int ncf,
 // (rows 0..p+q, columns -q..p+q), multipoles (rows 0..q, columns -q..q) and
 // (-1)^j ratio^j / rho_c factors in zero-padded dense shared arrays, so the inner
 // sums are branch-free.
-__global__ void __launch_bounds__(NT)
+template <int CL>
+__global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(NT)
 k_tr_m2qbxl(qbxfmm_geometry g, qbxfmm_transpose_index ix, int p, int q, int ncf, int ncq,
             int nrhs, int mb, const double2* __restrict__ cmp, double2* __restrict__ locals,
             int32_t* err)
 {
+  __shared__ double2 s_out[2 * NT];
+  const int row = blockIdx.x / CL, part = blockIdx.x - row * CL;
   extern __shared__ double2 smem2[];
   const int SW = p + 2 * q + 1, SS = (p + q + 1) * SW;   // S: rows 0..p+q, columns -q..p+q
   const int MW = 2 * q + 1, MS = (q + 1) * MW;
@@ -227,19 +238,21 @@ k_tr_m2qbxl(qbxfmm_geometry g, qbxfmm_transpose_index ix, int p, int q, int ncf,
   double* fac = reinterpret_cast<double*>(Mp + (size_t)mb * MS);   // [mb][p + 1]
   double* sd = fac + (size_t)mb * (p + 1);                          // [mb][3]
   int* sctr = reinterpret_cast<int*>(sd + (size_t)mb * 3);          // [mb]
-  int s = ix.list3_rows[blockIdx.x];
+  int s = ix.list3_rows[row];
   int r = blockIdx.y;
-  if (!box_ok(g, s, err)) return;
+  if (!box_ok(g, s, err)) return;          // the whole cluster (one row) leaves
   double rho_s = level_width(g, g.box_levels[s]);
   double cs[3];
   load_point<3>(g.box_centers, g.nboxes, s, cs);
   for (int i = threadIdx.x; i < mb * (SS + MS); i += NT) S[i] = c2(0.0);
   double2 acc[2] = {c2(0.0), c2(0.0)};
-  for (int e = ix.list3_rev_starts[blockIdx.x]; e < ix.list3_rev_starts[blockIdx.x + 1]; ++e) {
+  int item = 0;                            // center batches dealt round-robin to the cluster
+  for (int e = ix.list3_rev_starts[row]; e < ix.list3_rev_starts[row + 1]; ++e) {
     int b = ix.list3_rev_lists[e];
     if (!box_ok(g, b, err)) continue;
     int k0 = ix.box_center_starts[b], k1 = ix.box_center_starts[b + 1];
     for (int kb = k0; kb < k1; kb += mb) {
+      if (item++ % CL != part) continue;
       int nb = min(mb, k1 - kb);
       __syncthreads();
       if (threadIdx.x < nb) {
@@ -310,12 +323,23 @@ k_tr_m2qbxl(qbxfmm_geometry g, qbxfmm_transpose_index ix, int p, int q, int ncf,
       }
     }
   }
-  double2* L = locals + ((size_t)s * nrhs + r) * ncf;
+  // the cluster's partial locals summed by rank 0 in rank order (distributed shared memory)
+  cg::cluster_group cl = cg::this_cluster();
 #pragma unroll
-  for (int h = 0; h < 2; ++h) {
-    int o = threadIdx.x + h * NT;
-    if (o < ncf) L[o] = cadd(L[o], acc[h]);
+  for (int h = 0; h < 2; ++h) s_out[threadIdx.x + h * NT] = acc[h];
+  cl.sync();
+  if (part == 0) {
+    double2* L = locals + ((size_t)s * nrhs + r) * ncf;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      int o = threadIdx.x + h * NT;
+      if (o >= ncf) break;
+      double2 v = acc[h];
+      for (int qq = 1; qq < CL; ++qq) v = cadd(v, cl.map_shared_rank(s_out, qq)[o]);
+      L[o] = cadd(L[o], v);
+    }
   }
+  cl.sync();
 }
 
 // }}}
@@ -333,14 +357,17 @@ k_tr_m2qbxl(qbxfmm_geometry g, qbxfmm_transpose_index ix, int p, int q, int ncf,
 constexpr int TR_KS = 4;
 constexpr int TR_PB = NT;
 
-template <int Q, bool DIP>
-__global__ void __launch_bounds__(NT)
+template <int Q, bool DIP, int CL>
+__global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(NT)
 k_tr_tsqbx(qbxfmm_geometry g, qbxfmm_transpose_index ix, int nrhs, double cq,
            const double* __restrict__ tvals, double* __restrict__ vals,
            double* __restrict__ grads, int32_t* err)
 {
   __shared__ double s_c[3][TR_PB], s_ah[3][TR_PB], s_al[TR_PB], s_w[TR_PB];
-  int s = ix.list1_rows[blockIdx.x];
+  __shared__ double s_part[TR_KS][DIP ? 4 : 1][NT];
+  const int row = blockIdx.x / CL, part = blockIdx.x - row * CL;
+  cg::cluster_group cl = cg::this_cluster();
+  int s = ix.list1_rows[row];
   int r = blockIdx.y;
   if (!box_ok(g, s, err)) return;
   int s0 = g.box_source_starts[s], ns = g.box_source_counts_nonchild[s];
@@ -359,11 +386,13 @@ k_tr_tsqbx(qbxfmm_geometry g, qbxfmm_transpose_index ix, int nrhs, double cq,
       if (jj < ns) load_point<3>(g.sources, g.nsources, s0 + jj, y[k]);
       else y[k][0] = y[k][1] = y[k][2] = 0.0;
     }
-    for (int e = ix.list1_rev_starts[blockIdx.x]; e < ix.list1_rev_starts[blockIdx.x + 1]; ++e) {
+    int item = 0;                          // pair batches dealt round-robin to the cluster
+    for (int e = ix.list1_rev_starts[row]; e < ix.list1_rev_starts[row + 1]; ++e) {
       int b = ix.list1_rev_lists[e];
       if (!box_ok(g, b, err)) continue;
       int p0 = ix.box_pair_starts[b], p1 = ix.box_pair_starts[b + 1];
       for (int pb = p0; pb < p1; pb += TR_PB) {
+        if (item++ % CL != part) continue;
         int np = min(TR_PB, p1 - pb);
         __syncthreads();
         if (threadIdx.x < np) {
@@ -429,19 +458,38 @@ k_tr_tsqbx(qbxfmm_geometry g, qbxfmm_transpose_index ix, int nrhs, double cq,
         }
       }
     }
+    // the cluster's partial sums for these sources, added by rank 0 in rank order
 #pragma unroll
     for (int k = 0; k < TR_KS; ++k) {
-      int jj = g0 + threadIdx.x + k * NT;
-      if (jj < ns) {
-        vals[(size_t)r * g.nsources + s0 + jj] += acc[k];
+      s_part[k][0][threadIdx.x] = acc[k];
+      if (DIP)
+        for (int d = 0; d < 3; ++d) s_part[k][DIP ? d + 1 : 0][threadIdx.x] = gacc[DIP ? k : 0][d];
+    }
+    cl.sync();
+    if (part == 0) {
+#pragma unroll
+      for (int k = 0; k < TR_KS; ++k) {
+        int jj = g0 + threadIdx.x + k * NT;
+        if (jj >= ns) continue;
+        double v = acc[k], gv[3] = {0.0, 0.0, 0.0};
+        if (DIP)
+          for (int d = 0; d < 3; ++d) gv[d] = gacc[DIP ? k : 0][d];
+        for (int qq = 1; qq < CL; ++qq) {
+          const double* rp = &cl.map_shared_rank(&s_part[0][0][0], qq)[0];
+          v += rp[(k * (DIP ? 4 : 1)) * NT + threadIdx.x];
+          if (DIP)
+            for (int d = 0; d < 3; ++d) gv[d] += rp[(k * 4 + d + 1) * NT + threadIdx.x];
+        }
+        vals[(size_t)r * g.nsources + s0 + jj] += v;
         if (DIP) {
           double* gr = grads + (size_t)r * 3 * g.nsources + s0 + jj;
-          gr[0] += gacc[DIP ? k : 0][0];
-          gr[g.nsources] += gacc[DIP ? k : 0][1];
-          gr[2 * (size_t)g.nsources] += gacc[DIP ? k : 0][2];
+          gr[0] += gv[0];
+          gr[g.nsources] += gv[1];
+          gr[2 * (size_t)g.nsources] += gv[2];
         }
       }
     }
+    cl.sync();
   }
 }
 
@@ -485,11 +533,19 @@ cudaError_t launch_tr_m2qbxl(const qbxfmm_geometry& g, const qbxfmm_transpose_in
   int mb = std::max(1, std::min(8, NT / (p + q + 1)));
   size_t sh = (size_t)mb * ((p + q + 1) * (p + 2 * q + 1) + (q + 1) * (2 * q + 1)) * sizeof(double2) +
               (size_t)mb * (p + 4) * sizeof(double) + (size_t)mb * sizeof(int);
-  cudaError_t e = cudaFuncSetAttribute(k_tr_m2qbxl, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)sh);
-  if (e != cudaSuccess) return e;
-  k_tr_m2qbxl<<<dim3(ix.nlist3_rows, nrhs), NT, sh, st>>>(g, ix, p, q, ncf, ncq, nrhs, mb, cmp,
-                                                          locals, err);
+  if (ix.nlist3_rows < TR_SPLIT_BELOW) {
+    cudaError_t e = cudaFuncSetAttribute(k_tr_m2qbxl<TR_CL>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+    if (e != cudaSuccess) return e;
+    k_tr_m2qbxl<TR_CL><<<dim3(ix.nlist3_rows * TR_CL, nrhs), NT, sh, st>>>(
+        g, ix, p, q, ncf, ncq, nrhs, mb, cmp, locals, err);
+  } else {
+    cudaError_t e = cudaFuncSetAttribute(k_tr_m2qbxl<1>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+    if (e != cudaSuccess) return e;
+    k_tr_m2qbxl<1><<<dim3(ix.nlist3_rows, nrhs), NT, sh, st>>>(g, ix, p, q, ncf, ncq, nrhs, mb,
+                                                              cmp, locals, err);
+  }
   return cudaGetLastError();
 }
 
@@ -498,12 +554,16 @@ static cudaError_t tr_tsqbx_q(const qbxfmm_geometry& g, const qbxfmm_transpose_i
                               int nrhs, double cq, const double* tvals, double* vals,
                               double* grads, int32_t* err, cudaStream_t st)
 {
-  if (grads)
-    k_tr_tsqbx<Q, true><<<dim3(ix.nlist1_rows, nrhs), NT, 0, st>>>(g, ix, nrhs, cq, tvals, vals,
-                                                                   grads, err);
+  const bool split = ix.nlist1_rows < TR_SPLIT_BELOW;
+  const dim3 grid(ix.nlist1_rows * (split ? TR_CL : 1), nrhs);
+  if (grads && split)
+    k_tr_tsqbx<Q, true, TR_CL><<<grid, NT, 0, st>>>(g, ix, nrhs, cq, tvals, vals, grads, err);
+  else if (grads)
+    k_tr_tsqbx<Q, true, 1><<<grid, NT, 0, st>>>(g, ix, nrhs, cq, tvals, vals, grads, err);
+  else if (split)
+    k_tr_tsqbx<Q, false, TR_CL><<<grid, NT, 0, st>>>(g, ix, nrhs, cq, tvals, vals, nullptr, err);
   else
-    k_tr_tsqbx<Q, false><<<dim3(ix.nlist1_rows, nrhs), NT, 0, st>>>(g, ix, nrhs, cq, tvals, vals,
-                                                                    nullptr, err);
+    k_tr_tsqbx<Q, false, 1><<<grid, NT, 0, st>>>(g, ix, nrhs, cq, tvals, vals, nullptr, err);
   return cudaGetLastError();
 }
 

@@ -8,6 +8,8 @@ through what it allows:
 * 3D Laplace single-layer adjoint, icosphere-4 (76 800 nodes), 5000 targets on the
   sphere of radius 3, q 4 / p 12: central differences (h = 1e-6) along 32 seeded
   directions for the density and for the target positions (1e-6).
+* The 3D Laplace single-layer transpose on the icosphere-4 surface (76 800 QBX
+  targets): dot products with the apply (1e-12).
 * 3D Helmholtz combined field, icosphere-5 (921 600 sources), 16 densities, q 5 /
   p 15: every launch shape of the stage kernels gives the same apply (1e-13: the
   decompositions differ, the arithmetic does not), and the mixed-precision apply stays
@@ -108,3 +110,22 @@ def test_helmholtz3d_full_size_launch_shapes_and_mixed_form():
                    device_geometry=ap.dgeo, precision=PRECISION_MIXED)
     err = relerr(apm(dens).cpu().numpy(), base)
     assert 0.0 < err < 1e-6, err
+
+
+def test_adjoint_on_surface_full_size_dot_products():
+    """The transpose of the single layer on the config-4 surface itself (icosphere-4,
+    76 800 QBX targets; the transposed QBX kernels' one-CTA-per-row launches): the
+    identity <A sigma, r> = <sigma, A^T r> with the GPU apply (1e-12)."""
+    from pytential_b200.adjoint import SingleLayer
+    from pytential_b200.workloads import laplace3d_adjoint
+    w = laplace3d_adjoint(nrefine=4, ntargets=8)
+    op = SingleLayer(w.discr, w.discr.nodes, w.qbx_order, w.fmm_order, qbx_side=+1)
+    assert op.targets_need_qbx and op.transpose.index.nlist3_rows >= 4 * 148
+    rng = np.random.default_rng(31)
+    for _ in range(3):
+        sig = torch.from_numpy(rng.normal(size=op.ndofs)).cuda()
+        r = torch.from_numpy(rng.normal(size=op.ntargets)).cuda()
+        As, ATr = op.apply(sig), op.adjoint(r)
+        lhs, rhs = float((As * r).sum()), float((sig * ATr).sum())
+        assert abs(lhs - rhs) <= 1e-12 * float(torch.linalg.norm(As) * torch.linalg.norm(r))
+    op.transpose.check_error_word()
