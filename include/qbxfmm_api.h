@@ -153,7 +153,7 @@ int qbxfmm_eval_qbx_target_gradients(const qbxfmm_plan* plan, const void* streng
                                      const void* qbx_exps, void* grad, int32_t* error_word,
                                      void* stream);
 
-/* {{{ transposed QBX stages (3D Laplace single layer, FP64, one FMM order)
+/* {{{ transposed QBX stages (2D and 3D Laplace single layer, FP64, one FMM order)
  *
  * The transpose of the apply is the FMM with sources and targets exchanged over
  * the same boxes with transposed lists (the stage entries above on that geometry),
@@ -163,8 +163,8 @@ int qbxfmm_eval_qbx_target_gradients(const qbxfmm_plan* plan, const void* streng
  * `index` its reversed lists.  center_mpoles: [ncenters][nrhs][ncoeff(qbx_order)]
  * complex128.  Each output has one writer (no atomics).  QBXFMM_ERR_UNSUPPORTED for
  * other kernels, the mixed-precision form, per-level orders, qbx_order > 8 or
- * fmm_order > 21; these stage entries cover the single layer (the double layer runs
- * through qbxfmm_apply_transpose). */
+ * fmm_order > 21 (> 20 in 2D); these stage entries cover the single layer (the 3D
+ * double layer runs through qbxfmm_apply_transpose). */
 
 /* transpose of eval_qbx_expansions (fmm.py:358-389): target_values [nrhs][ntargets]
  * in tree target order -> center_mpoles (written; zero for centers without targets) */
@@ -194,8 +194,8 @@ int qbxfmm_transpose_form_global_qbx_locals(const qbxfmm_plan* plan,
                                             const void* target_values, void* source_values,
                                             int32_t* error_word, void* stream);
 
-/* The whole transpose K^T r in one call, for the 3D Laplace layer potential
- * cq S + cd D (single layer, double layer or both): `plan` the apply's plan,
+/* The whole transpose K^T r in one call, for the Laplace layer potential cq S + cd D
+ * (3D: single layer, double layer or both; 2D: cd = 0): `plan` the apply's plan,
  * `transposed` the plan of its exchanged-role geometry (same boxes, transposed
  * lists, no centers, a unit single layer: charge coefficient 1; its translation
  * matrices built into ws by qbxfmm_precompute_translations), ws a workspace of

@@ -129,7 +129,7 @@ class Oracle:
         return out
 
     def apply_transpose(self, user_target_values):
-        """The transpose of :meth:`apply` for the 3D Laplace single layer: values at
+        """The transpose of :meth:`apply` for the Laplace single layer (2D and 3D): values at
         the user targets ``(nrhs, nuser_targets)`` -> values at the sources in tree
         order ``(nrhs, nsources)``, so that ``sum(apply(s) * r) == sum(s *
         apply_transpose(r))``.
@@ -140,8 +140,8 @@ class Oracle:
         ``qbxfmm_oracle.c`` (which scatter per center)."""
         from pytential_b200.transpose import TransposedGeometryData
         k = self.kern
-        if k.family != abi.QBXFMM_LAPLACE or k.dim != 3 or k.dipole_coeff_re != 0:
-            raise NotImplementedError("the transposed apply covers the 3D Laplace single layer")
+        if k.family != abi.QBXFMM_LAPLACE or k.dipole_coeff_re != 0:
+            raise NotImplementedError("the transposed apply covers the Laplace single layer")
         if self.level_orders is not None:
             raise NotImplementedError("the transposed apply takes one FMM order")
         r = np.atleast_2d(np.asarray(user_target_values, np.float64))
@@ -154,7 +154,7 @@ class Oracle:
         nf = sc["nfiltered_targets"]
         s_dual = np.ascontiguousarray(
             r_tree[:, a["unfiltered_from_filtered_target_indices"][:nf].astype(np.int64)])
-        d = Oracle(TransposedGeometryData(self.geo), dim=3, qbx_order=k.qbx_order,
+        d = Oracle(TransposedGeometryData(self.geo), dim=k.dim, qbx_order=k.qbx_order,
                    fmm_order=k.fmm_order, nrhs=self.nrhs, charge_coeff=k.charge_coeff_re,
                    family=abi.QBXFMM_LAPLACE)
         mp, lo = d.zeros_box_exps(), d.zeros_box_exps()

@@ -1005,7 +1005,7 @@ int orc_apply_direct(const qbxfmm_kernel* kern, const qbxfmm_geometry* g,
 
 /* }}} */
 
-/* {{{ transposed QBX stages (3D Laplace single layer)
+/* {{{ transposed QBX stages (Laplace single layer, 2D and 3D)
  *
  * The transposes of QBXL2P, L2QBXL, M2QBXL and P2QBXL (fmm.py:231-389) in the
  * exchanged-role form: each global center carries the order-q multipole of its
@@ -1022,7 +1022,7 @@ static int transpose_ctx(const qbxfmm_kernel* kern, ctx_t* c)
 {
   int rc = make_ctx(kern, c);
   if (rc) return rc;
-  if (c->dim != 3 || c->cd != 0) return QBXFMM_ERR_UNSUPPORTED;
+  if (c->cd != 0) return QBXFMM_ERR_UNSUPPORTED;
   return 0;
 }
 
@@ -1038,15 +1038,18 @@ int orc_transpose_eval_qbx_expansions(const qbxfmm_kernel* kern, const qbxfmm_ge
   for (int ig = 0; ig < g->nglobal_qbx_centers; ++ig) {
     int ctr = g->global_qbx_centers[ig];
     double cc[3], x[3];
-    load(g->centers, g->ncenters, ctr, 3, cc);
+    load(g->centers, g->ncenters, ctr, c.dim, cc);
     double rho = g->expansion_radii[ctr];
     for (int it = g->center_to_targets_starts[ctr]; it < g->center_to_targets_starts[ctr + 1];
          ++it) {
       int t = g->center_to_targets_lists[it];
-      load(g->targets, g->ntargets, t, 3, x);
-      for (int r = 0; r < c.nrhs; ++r)
-        lap3_p2m(c.pq, rho, cc, x, c.cq * tree_vals[(size_t)r * g->ntargets + t], 0, zero,
-                 center_mpoles + ((size_t)ctr * c.nrhs + r) * c.ncq, work);
+      load(g->targets, g->ntargets, t, c.dim, x);
+      for (int r = 0; r < c.nrhs; ++r) {
+        double q = c.cq * tree_vals[(size_t)r * g->ntargets + t];
+        cplx* M = center_mpoles + ((size_t)ctr * c.nrhs + r) * c.ncq;
+        if (c.dim == 3) lap3_p2m(c.pq, rho, cc, x, q, 0, zero, M, work);
+        else lap2_p2m(c.pq, rho, cc, x, q, 0, NULL, M);
+      }
     }
   }
   free(work);
@@ -1066,16 +1069,18 @@ int orc_transpose_translate_box_local_to_qbx_local(const qbxfmm_kernel* kern,
     int ctr = g->global_qbx_centers[ig];
     int tb = g->target_boxes[g->qbx_center_to_target_box[ctr]];
     double cc[3], cb[3], d[3];
-    load(g->centers, g->ncenters, ctr, 3, cc);
-    load(g->box_centers, g->nboxes, tb, 3, cb);
+    load(g->centers, g->ncenters, ctr, c.dim, cc);
+    load(g->box_centers, g->nboxes, tb, c.dim, cb);
     double rho_b = level_width(g, g->box_levels[tb]);
     double rho_c = g->expansion_radii[ctr];
-    for (int dd = 0; dd < 3; ++dd) d[dd] = (cc[dd] - cb[dd]) / rho_b;
+    for (int dd = 0; dd < c.dim; ++dd) d[dd] = (cc[dd] - cb[dd]) / rho_b;
     for (int r = 0; r < c.nrhs; ++r) {
       /* the center multipole zero-padded to the box order */
       for (int i = 0; i < c.ncf; ++i) pad[i] = 0;
       memcpy(pad, center_mpoles + ((size_t)ctr * c.nrhs + r) * c.ncq, sizeof(cplx) * c.ncq);
-      lap3_m2m(c.pf, rho_c, rho_b, d, pad, mpoles + ((size_t)tb * c.nrhs + r) * c.ncf, work);
+      cplx* M = mpoles + ((size_t)tb * c.nrhs + r) * c.ncf;
+      if (c.dim == 3) lap3_m2m(c.pf, rho_c, rho_b, d, pad, M, work);
+      else lap2_m2m(c.pf, rho_c, rho_b, d, pad, M);
     }
   }
   free(pad);
@@ -1094,18 +1099,20 @@ int orc_transpose_translate_box_multipoles_to_qbx_local(const qbxfmm_kernel* ker
   for (int ig = 0; ig < g->nglobal_qbx_centers; ++ig) {
     int ctr = g->global_qbx_centers[ig];
     double cc[3], cs[3], d[3];
-    load(g->centers, g->ncenters, ctr, 3, cc);
+    load(g->centers, g->ncenters, ctr, c.dim, cc);
     double rho_c = g->expansion_radii[ctr];
     int itb = g->qbx_center_to_target_box[ctr];
     for (int li = g->list3_starts[itb]; li < g->list3_starts[itb + 1]; ++li) {
       int sb = g->list3_lists[li];
       double rho_s = level_width(g, g->box_levels[sb]);
-      load(g->box_centers, g->nboxes, sb, 3, cs);
-      for (int dd = 0; dd < 3; ++dd) d[dd] = (cs[dd] - cc[dd]) / rho_c;
-      for (int r = 0; r < c.nrhs; ++r)
-        lap3_m2l(c.pq, lp(&c, g->box_levels[sb]), rho_c, rho_s, d,
-                 center_mpoles + ((size_t)ctr * c.nrhs + r) * c.ncq,
-                 locals + ((size_t)sb * c.nrhs + r) * c.ncf, work);
+      load(g->box_centers, g->nboxes, sb, c.dim, cs);
+      for (int dd = 0; dd < c.dim; ++dd) d[dd] = (cs[dd] - cc[dd]) / rho_c;
+      for (int r = 0; r < c.nrhs; ++r) {
+        const cplx* M = center_mpoles + ((size_t)ctr * c.nrhs + r) * c.ncq;
+        cplx* L = locals + ((size_t)sb * c.nrhs + r) * c.ncf;
+        if (c.dim == 3) lap3_m2l(c.pq, lp(&c, g->box_levels[sb]), rho_c, rho_s, d, M, L, work);
+        else lap2_m2l(c.pq, lp(&c, g->box_levels[sb]), rho_c, rho_s, d, M, L);
+      }
     }
   }
   free(work);
@@ -1123,18 +1130,19 @@ int orc_transpose_form_global_qbx_locals(const qbxfmm_kernel* kern, const qbxfmm
   for (int ig = 0; ig < g->nglobal_qbx_centers; ++ig) {
     int ctr = g->global_qbx_centers[ig];
     double cc[3], y[3];
-    load(g->centers, g->ncenters, ctr, 3, cc);
+    load(g->centers, g->ncenters, ctr, c.dim, cc);
     double rho = g->expansion_radii[ctr];
     int itb = g->qbx_center_to_target_box[ctr];
     for (int li = g->list1_starts[itb]; li < g->list1_starts[itb + 1]; ++li) {
       int sb = g->list1_lists[li];
       int s0 = g->box_source_starts[sb], s1 = s0 + g->box_source_counts_nonchild[sb];
       for (int s = s0; s < s1; ++s) {
-        load(g->sources, g->nsources, s, 3, y);
-        for (int r = 0; r < c.nrhs; ++r)
+        load(g->sources, g->nsources, s, c.dim, y);
+        for (int r = 0; r < c.nrhs; ++r) {
+          const cplx* M = center_mpoles + ((size_t)ctr * c.nrhs + r) * c.ncq;
           source_vals[(size_t)r * g->nsources + s] +=
-              lap3_m2p(c.pq, rho, cc, y, center_mpoles + ((size_t)ctr * c.nrhs + r) * c.ncq,
-                       work);
+              (c.dim == 3) ? lap3_m2p(c.pq, rho, cc, y, M, work) : lap2_m2p(c.pq, rho, cc, y, M);
+        }
       }
     }
   }

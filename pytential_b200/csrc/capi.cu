@@ -1333,8 +1333,12 @@ namespace {
 int transpose_ok(const qbxfmm_plan* p, bool allow_dipole = false)
 {
   if (int rc = check_plan(p)) return rc;
-  if (p->helm || p->kern.dim != 3)
-    return fail(QBXFMM_ERR_UNSUPPORTED, "the transposed apply covers 3D Laplace");
+  if (p->helm)
+    return fail(QBXFMM_ERR_UNSUPPORTED, "the transposed apply covers Laplace");
+  if (p->kern.dim == 2 && p->sc.cd != 0.0)
+    return fail(QBXFMM_ERR_UNSUPPORTED, "the 2D transposed apply covers the single layer");
+  if (p->kern.dim == 2 && p->kern.fmm_order > 20)
+    return fail(QBXFMM_ERR_UNSUPPORTED, "the 2D transposed apply takes fmm_order <= 20");
   if (p->sc.cd != 0.0 && !allow_dipole)
     return fail(QBXFMM_ERR_UNSUPPORTED,
                 "the transposed stage entries cover the single layer; the double layer "
@@ -1356,9 +1360,16 @@ int qbxfmm_transpose_eval_qbx_expansions(const qbxfmm_plan* p, const void* targe
   if (!target_values || !center_mpoles) return fail(QBXFMM_ERR_ARG, "null argument");
   size_t bytes = (size_t)p->geo.ncenters * p->kern.nrhs * p->ncq * 2 * sizeof(double);
   if (bytes) QBX_TRY(cudaMemsetAsync(center_mpoles, 0, bytes, S(stream)), "transpose: clear");
-  QBX_TRY(launch_tr_qbxl2p(p->geo, p->kern.qbx_order, p->kern.nrhs, p->sc.cq,
-                           (const double*)target_values, (double2*)center_mpoles, err, S(stream)),
-          "transpose_eval_qbx_expansions");
+  if (p->kern.dim == 2)
+    QBX_TRY(launch_tr2_stages(0, p->geo, nullptr, p->kern.fmm_order, p->kern.qbx_order,
+                              p->kern.nrhs, p->sc.cq, (const double*)target_values,
+                              (double2*)center_mpoles, nullptr, nullptr, err, S(stream)),
+            "transpose_eval_qbx_expansions");
+  else
+    QBX_TRY(launch_tr_qbxl2p(p->geo, p->kern.qbx_order, p->kern.nrhs, p->sc.cq,
+                             (const double*)target_values, (double2*)center_mpoles, err,
+                             S(stream)),
+            "transpose_eval_qbx_expansions");
   return QBXFMM_OK;
 }
 
@@ -1369,9 +1380,15 @@ int qbxfmm_transpose_translate_box_local_to_qbx_local(const qbxfmm_plan* p,
 {
   if (int rc = transpose_ok(p)) return rc;
   if (!ix || !center_mpoles || !mpoles) return fail(QBXFMM_ERR_ARG, "null argument");
-  QBX_TRY(launch_tr_l2qbxl(p->geo, *ix, p->kern.fmm_order, p->kern.qbx_order, p->kern.nrhs,
-                           (const double2*)center_mpoles, (double2*)mpoles, err, S(stream)),
-          "transpose_translate_box_local_to_qbx_local");
+  if (p->kern.dim == 2)
+    QBX_TRY(launch_tr2_stages(1, p->geo, ix, p->kern.fmm_order, p->kern.qbx_order, p->kern.nrhs,
+                              1.0, nullptr, (double2*)center_mpoles, (double2*)mpoles, nullptr,
+                              err, S(stream)),
+            "transpose_translate_box_local_to_qbx_local");
+  else
+    QBX_TRY(launch_tr_l2qbxl(p->geo, *ix, p->kern.fmm_order, p->kern.qbx_order, p->kern.nrhs,
+                             (const double2*)center_mpoles, (double2*)mpoles, err, S(stream)),
+            "transpose_translate_box_local_to_qbx_local");
   return QBXFMM_OK;
 }
 
@@ -1383,9 +1400,15 @@ int qbxfmm_transpose_translate_box_multipoles_to_qbx_local(const qbxfmm_plan* p,
 {
   if (int rc = transpose_ok(p)) return rc;
   if (!ix || !center_mpoles || !locals) return fail(QBXFMM_ERR_ARG, "null argument");
-  QBX_TRY(launch_tr_m2qbxl(p->geo, *ix, p->kern.fmm_order, p->kern.qbx_order, p->kern.nrhs,
-                           (const double2*)center_mpoles, (double2*)locals, err, S(stream)),
-          "transpose_translate_box_multipoles_to_qbx_local");
+  if (p->kern.dim == 2)
+    QBX_TRY(launch_tr2_stages(2, p->geo, ix, p->kern.fmm_order, p->kern.qbx_order, p->kern.nrhs,
+                              1.0, nullptr, (double2*)center_mpoles, (double2*)locals, nullptr,
+                              err, S(stream)),
+            "transpose_translate_box_multipoles_to_qbx_local");
+  else
+    QBX_TRY(launch_tr_m2qbxl(p->geo, *ix, p->kern.fmm_order, p->kern.qbx_order, p->kern.nrhs,
+                             (const double2*)center_mpoles, (double2*)locals, err, S(stream)),
+            "transpose_translate_box_multipoles_to_qbx_local");
   return QBXFMM_OK;
 }
 
@@ -1395,10 +1418,16 @@ int qbxfmm_transpose_form_global_qbx_locals(const qbxfmm_plan* p, const qbxfmm_t
 {
   if (int rc = transpose_ok(p)) return rc;
   if (!ix || !target_values || !source_values) return fail(QBXFMM_ERR_ARG, "null argument");
-  QBX_TRY(launch_tr_p2qbxl(p->geo, *ix, p->kern.qbx_order, p->kern.nrhs, p->sc.cq,
-                           (const double*)target_values, (double*)source_values, nullptr, err,
-                           S(stream)),
-          "transpose_form_global_qbx_locals");
+  if (p->kern.dim == 2)
+    QBX_TRY(launch_tr2_stages(3, p->geo, ix, p->kern.fmm_order, p->kern.qbx_order, p->kern.nrhs,
+                              p->sc.cq, (const double*)target_values, nullptr, nullptr,
+                              (double*)source_values, err, S(stream)),
+            "transpose_form_global_qbx_locals");
+  else
+    QBX_TRY(launch_tr_p2qbxl(p->geo, *ix, p->kern.qbx_order, p->kern.nrhs, p->sc.cq,
+                             (const double*)target_values, (double*)source_values, nullptr, err,
+                             S(stream)),
+            "transpose_form_global_qbx_locals");
   return QBXFMM_OK;
 }
 
@@ -1409,12 +1438,12 @@ int qbxfmm_apply_transpose(const qbxfmm_plan* p, const qbxfmm_plan* d,
 {
   if (int rc = transpose_ok(p, true)) return rc;
   if (int rc = check_plan(d)) return rc;
-  if (d->helm || d->kern.dim != 3 || d->mixed || level_orders_on(d) || d->geo.ncenters != 0 ||
+  if (d->helm || d->kern.dim != p->kern.dim || d->mixed || level_orders_on(d) || d->geo.ncenters != 0 ||
       d->kern.fmm_order != p->kern.fmm_order || d->kern.nrhs != p->kern.nrhs ||
       d->geo.nboxes != p->geo.nboxes || d->geo.nsources != p->geo.nfiltered_targets ||
       d->geo.ntargets != p->geo.nsources || d->sc.cq != 1.0 || d->sc.cd != 0.0)
     return fail(QBXFMM_ERR_ARG, "the second plan is not the exchanged-role plan of the first");
-  const bool dip = p->sc.cd != 0.0;
+  const bool dip = p->sc.cd != 0.0, d2 = p->kern.dim == 2;
   if (!ix || !ws || !target_values || !strengths || !center_mpoles || !out ||
       (dip && !grad_scratch))
     return fail(QBXFMM_ERR_ARG, "null argument");
@@ -1438,9 +1467,15 @@ int qbxfmm_apply_transpose(const qbxfmm_plan* p, const qbxfmm_plan* d,
   // coefficients enter once, at the sources (k_tr_combine)
   size_t cbytes = (size_t)p->geo.ncenters * nrhs * p->ncq * 2 * sizeof(double);
   if (cbytes) QBX_TRY(cudaMemsetAsync(center_mpoles, 0, cbytes, st), "apply_transpose: clear");
-  QBX_TRY(launch_tr_qbxl2p(p->geo, q, nrhs, 1.0, (const double*)target_values,
-                           (double2*)center_mpoles, ws->error_word, st),
-          "apply_transpose: center multipoles");
+  if (d2)
+    QBX_TRY(launch_tr2_stages(0, p->geo, nullptr, p->kern.fmm_order, q, nrhs, 1.0,
+                              (const double*)target_values, (double2*)center_mpoles, nullptr,
+                              nullptr, ws->error_word, st),
+            "apply_transpose: center multipoles");
+  else
+    QBX_TRY(launch_tr_qbxl2p(p->geo, q, nrhs, 1.0, (const double*)target_values,
+                             (double2*)center_mpoles, ws->error_word, st),
+            "apply_transpose: center multipoles");
   // The exchanged-role stage graph on the second plan's four streams, as in
   // qbxfmm_apply, with the transposed QBX stages where their outputs are consumed:
   //   caller's stream: P2M, L2QBXL^T, M2M | M2L, L2L | L2P, gradients, combination
@@ -1476,20 +1511,30 @@ int qbxfmm_apply_transpose(const qbxfmm_plan* p, const qbxfmm_plan* d,
     QBX_CUDA_STEP(cudaStreamWaitEvent(sx, d->ev_fork, 0), "apply_transpose: fork");
   forked = true;
   QBX_STEP(qbxfmm_form_locals(d, strengths, ws->locals, ws->error_word, s2));
-  QBX_CUDA_STEP(launch_tr_m2qbxl(p->geo, *ix, p->kern.fmm_order, q, nrhs,
-                                 (const double2*)center_mpoles, (double2*)ws->locals,
-                                 ws->error_word, side2),
+  QBX_CUDA_STEP(d2 ? launch_tr2_stages(2, p->geo, ix, p->kern.fmm_order, q, nrhs, 1.0, nullptr,
+                                      (double2*)center_mpoles, (double2*)ws->locals, nullptr,
+                                      ws->error_word, side2)
+                   : launch_tr_m2qbxl(p->geo, *ix, p->kern.fmm_order, q, nrhs,
+                                      (const double2*)center_mpoles, (double2*)ws->locals,
+                                      ws->error_word, side2),
                 "apply_transpose: M2QBXL^T");
   QBX_CUDA_STEP(cudaEventRecord(d->ev_p2l, side2), "apply_transpose: P2L event");
   QBX_STEP(qbxfmm_eval_direct(d, strengths, ws->pot_nonqbx, ws->error_word, s1));
-  QBX_CUDA_STEP(launch_tr_p2qbxl(p->geo, *ix, q, nrhs, 1.0, (const double*)target_values,
-                                 (double*)ws->pot_nonqbx, dip ? (double*)grad_scratch : nullptr,
-                                 ws->error_word, side1),
+  QBX_CUDA_STEP(d2 ? launch_tr2_stages(3, p->geo, ix, p->kern.fmm_order, q, nrhs, 1.0,
+                                      (const double*)target_values, nullptr, nullptr,
+                                      (double*)ws->pot_nonqbx, ws->error_word, side1)
+                   : launch_tr_p2qbxl(p->geo, *ix, q, nrhs, 1.0, (const double*)target_values,
+                                      (double*)ws->pot_nonqbx,
+                                      dip ? (double*)grad_scratch : nullptr, ws->error_word,
+                                      side1),
                 "apply_transpose: P2QBXL^T");
   QBX_STEP(qbxfmm_form_multipoles(d, strengths, ws->mpoles, stream));
-  QBX_CUDA_STEP(launch_tr_l2qbxl(p->geo, *ix, p->kern.fmm_order, q, nrhs,
-                                 (const double2*)center_mpoles, (double2*)ws->mpoles,
-                                 ws->error_word, st),
+  QBX_CUDA_STEP(d2 ? launch_tr2_stages(1, p->geo, ix, p->kern.fmm_order, q, nrhs, 1.0, nullptr,
+                                      (double2*)center_mpoles, (double2*)ws->mpoles, nullptr,
+                                      ws->error_word, st)
+                   : launch_tr_l2qbxl(p->geo, *ix, p->kern.fmm_order, q, nrhs,
+                                      (const double2*)center_mpoles, (double2*)ws->mpoles,
+                                      ws->error_word, st),
                 "apply_transpose: L2QBXL^T");
   QBX_STEP(run_m2m(d, ws, nullptr, gemm, stream));
   QBX_CUDA_STEP(cudaEventRecord(d->ev_mpoles, st), "apply_transpose: multipole event");
@@ -1514,7 +1559,7 @@ int qbxfmm_apply_transpose(const qbxfmm_plan* p, const qbxfmm_plan* d,
                                 (const double2*)ws->locals, (double*)grad_scratch, ws->error_word,
                                 st),
             "apply_transpose: gradients");
-  QBX_TRY(launch_tr_combine(p->geo, nrhs, 0.25 / M_PI, p->sc.cq, p->sc.cd,
+  QBX_TRY(launch_tr_combine(p->geo, nrhs, d2 ? -0.5 / M_PI : 0.25 / M_PI, p->sc.cq, p->sc.cd,
                             (const double*)ws->pot_nonqbx, dip ? (const double*)grad_scratch : nullptr,
                             (double*)out, st),
           "apply_transpose: combination");

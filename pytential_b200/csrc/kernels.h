@@ -198,6 +198,12 @@ cudaError_t launch_tr_m2qbxl(const qbxfmm_geometry& g, const qbxfmm_transpose_in
 cudaError_t launch_tr_p2qbxl(const qbxfmm_geometry& g, const qbxfmm_transpose_index& ix, int q,
                              int nrhs, double cq, const double* tvals, double* vals, double* grads,
                              int32_t* err, cudaStream_t st);
+// 2D Laplace transposed QBX stages: which = 0 QBXL2P^T (tvals -> cmp), 1 L2QBXL^T
+// (cmp -> box multipoles), 2 M2QBXL^T (cmp -> box locals), 3 P2QBXL^T (tvals -> vals)
+cudaError_t launch_tr2_stages(int which, const qbxfmm_geometry& g, const qbxfmm_transpose_index* ix,
+                              int p, int q, int nrhs, double cq, const double* tvals,
+                              double2* cmp, double2* box_exps, double* vals, int32_t* err,
+                              cudaStream_t st);
 cudaError_t launch_tr_combine(const qbxfmm_geometry& g, int nrhs, double scale, double cq,
                               double cd, const double* vals, const double* grads, double* out,
                               cudaStream_t st);

@@ -1,4 +1,5 @@
-// Transposed QBX stages of the 3D Laplace single-layer apply, sm_100a.
+// Transposed QBX stages of the Laplace apply (3D single and double layer, 2D single
+// layer), sm_100a.
 //
 // The transpose of the apply is the FMM with sources and targets exchanged over the
 // same boxes and transposed lists; the QBX centers act there as sources carrying
@@ -490,6 +491,267 @@ k_tr_tsqbx(qbxfmm_geometry g, qbxfmm_transpose_index ix, int nrhs, double cq,
       }
     }
     cl.sync();
+  }
+}
+
+// }}}
+
+// {{{ 2D Laplace: the same four stages in the complex-analytic expansions
+//   multipole  Re[M_0 log(z - c) + sum_k M_k ((z - c) / rho)^-k],
+//   local      Re sum_k L_k ((z - c) / rho)^k
+
+QBX_D double2 cdiv(double2 a, double2 b)
+{
+  double d = 1.0 / (b.x * b.x + b.y * b.y);
+  return c2((a.x * b.x + a.y * b.y) * d, (a.y * b.x - a.x * b.y) * d);
+}
+
+// QBXL2P^T: per (global center, density) one thread, M_0 = cq sum r_t,
+// M_k = -cq sum r_t u_t^k / k, u_t = (x_t - c) / rho
+__global__ void __launch_bounds__(NT)
+k_tr2_qbxl2p(qbxfmm_geometry g, int q, int nrhs, double cq, const double* __restrict__ vals,
+             double2* __restrict__ cmp, int32_t* err)
+{
+  int ig = blockIdx.x * blockDim.x + threadIdx.x;
+  int r = blockIdx.y;
+  if (ig >= g.nglobal_qbx_centers) return;
+  int ctr = g.global_qbx_centers[ig];
+  if (!center_ok(g, ctr, err)) return;
+  double cc[2];
+  load_point<2>(g.centers, g.ncenters, ctr, cc);
+  double rinv = 1.0 / g.expansion_radii[ctr];
+  double2* M = cmp + ((size_t)ctr * nrhs + r) * (q + 1);
+  for (int k = 0; k <= q; ++k) M[k] = c2(0.0);
+  for (int it = g.center_to_targets_starts[ctr]; it < g.center_to_targets_starts[ctr + 1]; ++it) {
+    int t = g.center_to_targets_lists[it];
+    if ((unsigned)t >= (unsigned)g.ntargets) {
+      report(err, QBX_DEVERR_BAD_CENTER);
+      continue;
+    }
+    double x[2];
+    load_point<2>(g.targets, g.ntargets, t, x);
+    double v = cq * vals[(size_t)r * g.ntargets + t];
+    double2 u = c2((x[0] - cc[0]) * rinv, (x[1] - cc[1]) * rinv), uk = u;
+    M[0] = cadd(M[0], c2(v));
+    for (int k = 1; k <= q; ++k) {
+      M[k] = caxpy(-v * rcp(k), uk, M[k]);
+      uk = cmul(uk, u);
+    }
+  }
+}
+
+// L2QBXL^T: per (center box, density), thread = output coefficient l <= p: the M2M of
+// each center multipole (order q) to the box center
+__global__ void __launch_bounds__(32)
+k_tr2_l2qbxl(qbxfmm_geometry g, qbxfmm_transpose_index ix, int p, int q, int nrhs,
+             const double2* __restrict__ cmp, double2* __restrict__ mpoles, int32_t* err)
+{
+  int b = ix.center_boxes[blockIdx.x];
+  int r = blockIdx.y, l = threadIdx.x;
+  if (!box_ok(g, b, err) || l > p) return;
+  double rho_b = level_width(g, g.box_levels[b]);
+  double cb[2];
+  load_point<2>(g.box_centers, g.nboxes, b, cb);
+  double2 acc = c2(0.0);
+  for (int kk = ix.box_center_starts[b]; kk < ix.box_center_starts[b + 1]; ++kk) {
+    int ctr = ix.box_centers[kk];
+    if (!center_ok(g, ctr, err)) continue;
+    double cc[2];
+    load_point<2>(g.centers, g.ncenters, ctr, cc);
+    double ratio = g.expansion_radii[ctr] / rho_b;
+    double2 t = c2((cc[0] - cb[0]) / rho_b, (cc[1] - cb[1]) / rho_b);
+    const double2* Min = cmp + ((size_t)ctr * nrhs + r) * (q + 1);
+    if (l == 0) {
+      acc = cadd(acc, Min[0]);
+      continue;
+    }
+    double2 tp[24];                        // t^i, i <= l <= p <= 20
+    tp[0] = c2(1.0);
+    for (int i = 1; i <= l; ++i) tp[i] = cmul(tp[i - 1], t);
+    acc = cfma(cscale(-rcp(l), Min[0]), tp[l], acc);
+    double rk = ratio, bin = 1.0;          // C(l - 1, k - 1)
+    for (int k = 1; k <= l && k <= q; ++k) {
+      acc = cfma(cscale(rk * bin, Min[k]), tp[l - k], acc);
+      rk *= ratio;
+      bin = bin * (l - k) * rcp(k);
+    }
+  }
+  double2* M = mpoles + ((size_t)b * nrhs + r) * (p + 1);
+  M[l] = cadd(M[l], acc);
+}
+
+// M2QBXL^T: per (list-3 row s, density), thread = output coefficient l <= p: the M2L of
+// each center multipole (order q, rscale rho_c) into the local of s (rscale rho_s)
+__global__ void __launch_bounds__(32)
+k_tr2_m2qbxl(qbxfmm_geometry g, qbxfmm_transpose_index ix, int p, int q, int nrhs,
+             const double2* __restrict__ cmp, double2* __restrict__ locals, int32_t* err)
+{
+  int s = ix.list3_rows[blockIdx.x];
+  int r = blockIdx.y, l = threadIdx.x;
+  if (!box_ok(g, s, err) || l > p) return;
+  double rho_s = level_width(g, g.box_levels[s]);
+  double cs[2];
+  load_point<2>(g.box_centers, g.nboxes, s, cs);
+  double2 acc = c2(0.0);
+  for (int e = ix.list3_rev_starts[blockIdx.x]; e < ix.list3_rev_starts[blockIdx.x + 1]; ++e) {
+    int b = ix.list3_rev_lists[e];
+    if (!box_ok(g, b, err)) continue;
+    for (int kk = ix.box_center_starts[b]; kk < ix.box_center_starts[b + 1]; ++kk) {
+      int ctr = ix.box_centers[kk];
+      if (!center_ok(g, ctr, err)) continue;
+      double cc[2];
+      load_point<2>(g.centers, g.ncenters, ctr, cc);
+      double rho_c = g.expansion_radii[ctr];
+      double2 t = c2(cs[0] - cc[0], cs[1] - cc[1]);
+      double2 tinv = cdiv(c2(1.0), cscale(1.0 / rho_c, t));
+      const double2* Min = cmp + ((size_t)ctr * nrhs + r) * (q + 1);
+      if (l == 0) {
+        double2 v = cmul(Min[0], c2(0.5 * log(t.x * t.x + t.y * t.y), atan2(t.y, t.x)));
+        double2 pw = tinv;
+        for (int k = 1; k <= q; ++k) {
+          v = cfma(Min[k], pw, v);
+          pw = cmul(pw, tinv);
+        }
+        acc = cadd(acc, v);
+        continue;
+      }
+      double2 tl = c2(1.0);
+      for (int i = 0; i < l; ++i) tl = cmul(tl, tinv);
+      double2 v = cscale(((l & 1) ? 1.0 : -1.0) * rcp(l), cmul(Min[0], tl));
+      double2 sm = c2(0.0), pw = tinv;
+      double bin = 1.0;                     // C(k + l - 1, l), 1 at k = 1
+      for (int k = 1; k <= q; ++k) {
+        sm = cfma(cscale(bin, Min[k]), pw, sm);
+        pw = cmul(pw, tinv);
+        bin = bin * (k + l) * rcp(k);       // C(k + l, l) = C(k + l - 1, l) (k + l) / k
+      }
+      v = cfma(cscale((l & 1) ? -1.0 : 1.0, tl), sm, v);
+      double rl = 1.0, ratio = rho_s / rho_c;
+      for (int i = 0; i < l; ++i) rl *= ratio;
+      acc = caxpy(rl, v, acc);
+    }
+  }
+  double2* L = locals + ((size_t)s * nrhs + r) * (p + 1);
+  L[l] = cadd(L[l], acc);
+}
+
+// P2QBXL^T with QBXL2P^T, target-specific form: for a QBX target t with center c and a
+// list-1 source y, a = t - c, b = y - c: log|t - y| ~ log|b| - Re sum_{n=1..Q} (a/b)^n / n
+// (symmetric in the roles); per (source box row, density), thread = source
+template <int Q>
+__global__ void __launch_bounds__(NT)
+k_tr2_tsqbx(qbxfmm_geometry g, qbxfmm_transpose_index ix, int nrhs, double cq,
+            const double* __restrict__ tvals, double* __restrict__ vals, int32_t* err)
+{
+  __shared__ double s_c[2][NT], s_a[2][NT], s_w[NT];
+  int s = ix.list1_rows[blockIdx.x];
+  int r = blockIdx.y;
+  if (!box_ok(g, s, err)) return;
+  int s0 = g.box_source_starts[s], ns = g.box_source_counts_nonchild[s];
+  if (s0 < 0 || ns < 0 || s0 + ns > g.nsources) {
+    report(err, QBX_DEVERR_BAD_BOX);
+    return;
+  }
+  const double* tv = tvals + (size_t)r * g.ntargets;
+  for (int j0 = 0; j0 < ns; j0 += NT) {
+    int j = s0 + j0 + threadIdx.x;
+    bool active = j0 + threadIdx.x < ns;
+    double y[2] = {0.0, 0.0};
+    if (active) load_point<2>(g.sources, g.nsources, j, y);
+    double acc = 0.0;
+    for (int e = ix.list1_rev_starts[blockIdx.x]; e < ix.list1_rev_starts[blockIdx.x + 1]; ++e) {
+      int b = ix.list1_rev_lists[e];
+      if (!box_ok(g, b, err)) continue;
+      int p0 = ix.box_pair_starts[b], p1 = ix.box_pair_starts[b + 1];
+      for (int pb = p0; pb < p1; pb += NT) {
+        int np = min(NT, p1 - pb);
+        __syncthreads();
+        if (threadIdx.x < np) {
+          int t = ix.pair_targets[pb + threadIdx.x], ctr = ix.pair_centers[pb + threadIdx.x];
+          double w = 0.0, cc[2] = {0.0, 0.0}, a[2] = {0.0, 0.0};
+          if ((unsigned)t < (unsigned)g.ntargets && center_ok(g, ctr, err)) {
+            double x[2];
+            load_point<2>(g.centers, g.ncenters, ctr, cc);
+            load_point<2>(g.targets, g.ntargets, t, x);
+            a[0] = x[0] - cc[0];
+            a[1] = x[1] - cc[1];
+            w = cq * tv[t];
+          } else if ((unsigned)t >= (unsigned)g.ntargets) {
+            report(err, QBX_DEVERR_BAD_CENTER);
+          }
+          s_c[0][threadIdx.x] = cc[0];
+          s_c[1][threadIdx.x] = cc[1];
+          s_a[0][threadIdx.x] = a[0];
+          s_a[1][threadIdx.x] = a[1];
+          s_w[threadIdx.x] = w;
+        }
+        __syncthreads();
+        if (!active) continue;
+        for (int pi = 0; pi < np; ++pi) {
+          double w = s_w[pi];
+          if (w == 0.0) continue;
+          double2 bb = c2(y[0] - s_c[0][pi], y[1] - s_c[1][pi]);
+          double2 wv = cdiv(c2(s_a[0][pi], s_a[1][pi]), bb), pw = wv;
+          double sl = 0.0;
+#pragma unroll
+          for (int n = 1; n <= Q; ++n) {
+            sl += pw.x * (1.0 / n);
+            pw = cmul(pw, wv);
+          }
+          acc = fma(w, 0.5 * log(bb.x * bb.x + bb.y * bb.y) - sl, acc);
+        }
+      }
+    }
+    if (active) vals[(size_t)r * g.nsources + j] += acc;
+  }
+}
+
+template <int Q>
+static cudaError_t tr2_tsqbx_q(const qbxfmm_geometry& g, const qbxfmm_transpose_index& ix,
+                               int nrhs, double cq, const double* tvals, double* vals,
+                               int32_t* err, cudaStream_t st)
+{
+  k_tr2_tsqbx<Q><<<dim3(ix.nlist1_rows, nrhs), NT, 0, st>>>(g, ix, nrhs, cq, tvals, vals, err);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_tr2_stages(int which, const qbxfmm_geometry& g, const qbxfmm_transpose_index* ix,
+                              int p, int q, int nrhs, double cq, const double* tvals,
+                              double2* cmp, double2* box_exps, double* vals, int32_t* err,
+                              cudaStream_t st)
+{
+  if (p > 20 || q > 8) return cudaErrorInvalidValue;
+  switch (which) {
+    case 0:   // QBXL2P^T
+      if (g.nglobal_qbx_centers == 0) return cudaSuccess;
+      k_tr2_qbxl2p<<<dim3((g.nglobal_qbx_centers + NT - 1) / NT, nrhs), NT, 0, st>>>(
+          g, q, nrhs, cq, tvals, cmp, err);
+      return cudaGetLastError();
+    case 1:   // L2QBXL^T
+      if (ix->ncenter_boxes == 0) return cudaSuccess;
+      k_tr2_l2qbxl<<<dim3(ix->ncenter_boxes, nrhs), 32, 0, st>>>(g, *ix, p, q, nrhs, cmp,
+                                                                  box_exps, err);
+      return cudaGetLastError();
+    case 2:   // M2QBXL^T
+      if (ix->nlist3_rows == 0) return cudaSuccess;
+      k_tr2_m2qbxl<<<dim3(ix->nlist3_rows, nrhs), 32, 0, st>>>(g, *ix, p, q, nrhs, cmp, box_exps,
+                                                                err);
+      return cudaGetLastError();
+    case 3:   // P2QBXL^T with QBXL2P^T
+      if (ix->nlist1_rows == 0) return cudaSuccess;
+      switch (q) {
+        case 0: return tr2_tsqbx_q<0>(g, *ix, nrhs, cq, tvals, vals, err, st);
+        case 1: return tr2_tsqbx_q<1>(g, *ix, nrhs, cq, tvals, vals, err, st);
+        case 2: return tr2_tsqbx_q<2>(g, *ix, nrhs, cq, tvals, vals, err, st);
+        case 3: return tr2_tsqbx_q<3>(g, *ix, nrhs, cq, tvals, vals, err, st);
+        case 4: return tr2_tsqbx_q<4>(g, *ix, nrhs, cq, tvals, vals, err, st);
+        case 5: return tr2_tsqbx_q<5>(g, *ix, nrhs, cq, tvals, vals, err, st);
+        case 6: return tr2_tsqbx_q<6>(g, *ix, nrhs, cq, tvals, vals, err, st);
+        case 7: return tr2_tsqbx_q<7>(g, *ix, nrhs, cq, tvals, vals, err, st);
+        case 8: return tr2_tsqbx_q<8>(g, *ix, nrhs, cq, tvals, vals, err, st);
+        default: return cudaErrorInvalidValue;
+      }
+    default: return cudaErrorInvalidValue;
   }
 }
 

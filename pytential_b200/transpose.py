@@ -1,4 +1,5 @@
-"""The transpose of the QBX-FMM apply (3D Laplace), over the same tree and traversal.
+"""The transpose of the QBX-FMM apply (Laplace: 3D single and double layer, 2D single
+layer), over the same tree and traversal.
 
 The apply is a chain of real-linear stages ``u = QBXL2P(L2QBXL(...) + M2QBXL(...) +
 P2QBXL(q)) + ...`` (pytential/qbx/fmm.py:414-594).  With the bilinear pairing
@@ -268,8 +269,8 @@ def transpose_index(geo) -> TransposeIndex:
 
 
 class QBXTransposeApply:
-    """The transpose of a 3D Laplace :class:`~pytential_b200.fmm.QBXApply` (single
-    layer, double layer or both; FP64, one FMM order) on its device: ``A^T r`` for
+    """The transpose of a Laplace :class:`~pytential_b200.fmm.QBXApply` (3D: single
+    layer, double layer or both; 2D: single layer; FP64, one FMM order) on its device: ``A^T r`` for
     values ``r`` at the apply's user targets, ``(nrhs, nuser_targets) -> (nrhs,
     ndofs)``, with ``A = K W U`` (upsampling ``U``, weights ``W``, the QBX-FMM kernel
     matrix ``K``) and ``A^T = U^T W K^T``.  ``K^T`` runs over the apply's own tree in
@@ -287,9 +288,11 @@ class QBXTransposeApply:
         from .fmm import LaplaceKernel, SourceKernelSpec
         plan = apply.plan
         spec = plan.spec
-        if spec.kernel.family != abi.QBXFMM_LAPLACE or spec.kernel.dim != 3:
-            raise NotImplementedError("the transposed apply covers 3D Laplace")
+        if spec.kernel.family != abi.QBXFMM_LAPLACE:
+            raise NotImplementedError("the transposed apply covers Laplace")
         self.has_dipole = spec.dipole_coeff != 0
+        if spec.kernel.dim == 2 and self.has_dipole:
+            raise NotImplementedError("the 2D transposed apply covers the single layer")
         if plan.precision != PRECISION_FP64 or len(set(plan.get_level_orders())) > 1:
             raise NotImplementedError("the transposed apply runs in FP64 with one FMM order")
         self.fwd = apply
@@ -297,7 +300,7 @@ class QBXTransposeApply:
         self.device = dev = apply.device
         self.dual_geo = TransposedGeometryData(apply.geo)
         self.dual_dgeo = DeviceGeometry(self.dual_geo, dev)
-        self.dual_spec = SourceKernelSpec(LaplaceKernel(3), charge_coeff=1.0)
+        self.dual_spec = SourceKernelSpec(LaplaceKernel(spec.kernel.dim), charge_coeff=1.0)
         self.dual_plan = Plan(self.dual_dgeo, self.dual_spec, plan.qbx_order, plan.fmm_order, nrhs)
         self._wrangler_args = (B200QBXExpansionWrangler, B200TreeIndependentDataForWrangler)
         self._dual_wrangler = None

@@ -143,6 +143,68 @@ def test_transposed_apply_needs_the_single_layer():
         o.apply_transpose(np.zeros((1, o.scalars["nuser_targets"])))
 
 
+# {{{ 2D
+
+def _geometry2d(nelements, near=0, shell=0, leaf=None, seed=0, order_nodes=16, quad_nodes=64):
+    """Starfish with on-curve QBX targets, ``near`` exterior points at a tenth of the
+    element size from the curve and ``shell`` far points."""
+    from pytential_b200.discretization import make_starfish
+    rng = np.random.default_rng(seed)
+    d = make_starfish(nelements, order_nodes=order_nodes, quad_nodes=quad_nodes)
+    tg = [(d.nodes, +1)]
+    if near:
+        i = rng.integers(0, d.ndofs, near)
+        h = 0.1 * d.element_stretch[i // d.nodes_per_element]
+        tg.append((d.nodes[:, i] + h * d.normals[:, i], +1))
+    if shell:
+        ang = rng.uniform(0, 2 * np.pi, shell)
+        rad = rng.uniform(2.5, 3.5, shell)
+        tg.append((np.array([rad * np.cos(ang), rad * np.sin(ang)]), 0))
+    kw = {} if leaf is None else {"max_leaf_refine_weight": leaf}
+    return QBXFMMGeometryData(d, tg, **kw)
+
+
+def _oracle2d(geo, nrhs, qbx_order=4, fmm_order=10):
+    from oracle.oracle import Oracle
+    return Oracle(geo, dim=2, qbx_order=qbx_order, fmm_order=fmm_order, nrhs=nrhs,
+                  charge_coeff=1.0, family=abi.QBXFMM_LAPLACE)
+
+
+CASES2D = {
+    "starfish-24": dict(nelements=24, near=100, shell=60, leaf=64),
+    "starfish-64": dict(nelements=64, near=200, shell=40),
+}
+
+
+@pytest.fixture(scope="module", params=list(CASES2D))
+def case2d(request):
+    return request.param, _geometry2d(**CASES2D[request.param])
+
+
+def test_checker_transpose_2d_dot_products(case2d):
+    _, geo = case2d
+    o = _oracle2d(geo, nrhs=2)
+    rng = np.random.default_rng(5)
+    s = rng.normal(size=(2, o.scalars["nsources"]))
+    r = rng.normal(size=(2, o.scalars["nuser_targets"]))
+    As = o.apply(s)
+    ATr = o.apply_transpose(r)
+    lhs, rhs = (As * r).sum(1), (s * ATr).sum(1)
+    scale = np.linalg.norm(As, axis=1) * np.linalg.norm(r, axis=1)
+    assert (np.abs(lhs - rhs) <= 1e-13 * scale).all()
+
+
+def test_checker_transpose_2d_is_the_matrix_transpose():
+    geo = _geometry2d(8, near=20, shell=20, leaf=16, order_nodes=8, quad_nodes=16)
+    o1 = _oracle2d(geo, nrhs=1)
+    ns, nu = o1.scalars["nsources"], o1.scalars["nuser_targets"]
+    A = _oracle2d(geo, nrhs=ns).apply(np.eye(ns)).T
+    AT = _oracle2d(geo, nrhs=nu).apply_transpose(np.eye(nu))
+    assert relerr(AT, A) < 1e-13
+
+# }}}
+
+
 # {{{ GPU
 
 @pytest.mark.gpu
@@ -205,6 +267,10 @@ def test_gpu_transpose_refusals():
                      precision=PRECISION_MIXED)
     with pytest.raises(NotImplementedError):
         QBXTransposeApply(mixed)
+    dl2 = QBXApply(_geometry2d(8, shell=10), SourceKernelSpec(LaplaceKernel(2), dipole_coeff=1.0),
+                   3, 8)
+    with pytest.raises(NotImplementedError):
+        QBXTransposeApply(dl2)
     # the stage entries refuse a double-layer plan (it runs through the one-call
     # transpose), before any launch
     import ctypes
@@ -300,3 +366,33 @@ def test_gpu_double_layer_transpose_dot_products(case, cq, cd):
     assert bool(((lhs - rhs).abs() <= 1e-12 * scale).all())
     with pytest.raises(NotImplementedError):
         tr.kernel_transpose_by_stages(r)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("tsqbx", [False, True])
+def test_gpu_transpose_2d(case2d, tsqbx):
+    """The 2D Laplace single-layer transpose against the checker's (both the one-call
+    form and the stage entries), and the dot-product identity with the GPU apply."""
+    import torch
+
+    from pytential_b200.fmm import LaplaceKernel, QBXApply, SourceKernelSpec
+    from pytential_b200.transpose import QBXTransposeApply
+    _, geo = case2d
+    spec = SourceKernelSpec(LaplaceKernel(2), charge_coeff=1.0)
+    ap = QBXApply(geo, spec, 4, 10, nrhs=2, target_specific_qbx=tsqbx)
+    tr = QBXTransposeApply(ap)
+    rng = np.random.default_rng(6)
+    r = rng.normal(size=(2, ap.nuser_targets))
+    o = _oracle2d(geo, nrhs=2)
+    ref = o.apply_transpose(r)[:, np.argsort(o.arrays["user_source_ids"][:o.scalars["nsources"]])]
+    for f in (tr.kernel_transpose, tr.kernel_transpose_by_stages):
+        got = f(torch.from_numpy(r).cuda()).cpu().numpy()
+        tr.check_error_word()
+        assert relerr(got, ref) < 1e-12, f.__name__
+    sig = torch.from_numpy(rng.normal(size=(2, ap.ndofs))).cuda()
+    rr = torch.from_numpy(r).cuda()
+    As, ATr = ap(sig), tr(rr)
+    ap.check_error_word()
+    lhs, rhs = (As * rr).sum(1), (sig * ATr).sum(1)
+    scale = torch.linalg.norm(As, dim=1) * torch.linalg.norm(rr, dim=1)
+    assert bool(((lhs - rhs).abs() <= 1e-12 * scale).all())
