@@ -56,6 +56,12 @@ struct qbxfmm_plan {
   // qbxfmm_precompute_translations, used by the translation stage entries
   mutable const double* trans_dev = nullptr;
   mutable double* scratch_dev = nullptr;
+  // 3D Laplace: M2L classes merged by offset symmetry; their index arrays (canonical
+  // offsets, then at m2l_aux_cls the class codes) are uploaded into the translations
+  // buffer at m2l_aux_off
+  M2LSymClasses m2l_sym;
+  std::vector<uint8_t> m2l_aux;
+  size_t m2l_aux_off = 0, m2l_aux_cls = 0;
   // qbxfmm_apply runs the independent branches of the stage graph on three side
   // streams joined back into the caller's stream by events (fork/join, also
   // under stream capture): near field + M2P; P2L; P2QBXL + M2QBXL (the longest
@@ -95,6 +101,17 @@ int check_plan(const qbxfmm_plan* p)
 {
   if (!p) return fail(QBXFMM_ERR_ARG, "null plan");
   return QBXFMM_OK;
+}
+
+// the M2L class maps of a 3D Laplace plan in its translations buffer (empty otherwise)
+TransAux trans_aux(const qbxfmm_plan* p, const void* translations)
+{
+  TransAux a;
+  if (!translations || p->m2l_aux.empty()) return a;
+  const char* b = static_cast<const char*>(translations) + p->m2l_aux_off;
+  a.canon_off = reinterpret_cast<const int32_t*>(b);
+  a.cls_code = reinterpret_cast<const int32_t*>(b + p->m2l_aux_cls);
+  return a;
 }
 
 size_t h3_rot_offset(const qbxfmm_plan* p);
@@ -457,11 +474,28 @@ int qbxfmm_plan_create(const qbxfmm_kernel* kernel, const qbxfmm_geometry* geome
   if (e == cudaSuccess) e = cudaGetDevice(&p->device);
   p->h3 = p->helm && k.dim == 3;
   p->mixed = k.precision == 1;
+  if (k.dim == 3 && !p->h3 && g.m2l_nclasses > 0 && e == cudaSuccess) {
+    std::vector<int32_t> off(3 * (size_t)g.m2l_nclasses);
+    e = cudaMemcpy(off.data(), g.m2l_class_offsets, sizeof(int32_t) * off.size(),
+                   cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) p->m2l_sym = m2l_symmetry_classes(g.m2l_nclasses, off);
+  }
   if (k.dim == 3)
     p->tc = p->h3 ? trans_cfg_helm3(k.fmm_order, 0, g.nlevels)   // M2L by rotation, no class matrices
-                  : trans_cfg_laplace3(k.fmm_order, g.m2l_nclasses);
+                  : trans_cfg_laplace3(k.fmm_order, p->m2l_sym.ncanon);
   p->trans_ok = k.dim == 3 && trans_supported(p->tc) && g.nlevels <= 64;
   p->tf32_ok = p->mixed && p->trans_ok && tf32_supported(p->tc);
+  if (k.dim == 3 && !p->h3) {
+    // the index arrays after the matrices (and their TF32 planes), 16-byte aligned
+    auto al = [](size_t b) { return (b + 15) / 16 * 16; };
+    const M2LSymClasses& ms = p->m2l_sym;
+    p->m2l_aux_off = al(trans_matrix_bytes(p->tc) + (p->tf32_ok ? tf32_matrix_bytes(p->tc) : 0));
+    p->m2l_aux_cls = al(ms.canon_off.size() * sizeof(int32_t));
+    p->m2l_aux.assign(al(p->m2l_aux_cls + ms.cls_code.size() * sizeof(int32_t)), 0);
+    std::memcpy(p->m2l_aux.data(), ms.canon_off.data(), ms.canon_off.size() * sizeof(int32_t));
+    std::memcpy(p->m2l_aux.data() + p->m2l_aux_cls, ms.cls_code.data(),
+                ms.cls_code.size() * sizeof(int32_t));
+  }
   if (p->h3 && !p->trans_ok) {
     delete p;
     return fail(QBXFMM_ERR_UNSUPPORTED, "3D Helmholtz: translation matrices unsupported for this order");
@@ -1034,8 +1068,7 @@ int qbxfmm_workspace_sizes(const qbxfmm_plan* p, size_t* sizes6 /* 8 entries */)
     int npairs = std::max(p->th.m2l_npairs, g.m2m_npairs);
     size_t o[8];
     h3_layout(p, o);
-    sizes6[6] = p->h3 ? o[7] * sizeof(double)
-                      : trans_matrix_bytes(p->tc) + (p->tf32_ok ? tf32_matrix_bytes(p->tc) : 0);
+    sizes6[6] = p->h3 ? o[7] * sizeof(double) : p->m2l_aux_off + p->m2l_aux.size();
     sizes6[7] = p->h3 ? 0 : trans_scratch_bytes(p->tc, npairs, p->kern.nrhs);
   } else {
     sizes6[6] = sizes6[7] = 0;
@@ -1097,7 +1130,13 @@ int qbxfmm_precompute_translations(const qbxfmm_plan* p, const qbxfmm_workspace*
     return QBXFMM_OK;
   }
   if (!p->trans_ok || !ws->translations) return QBXFMM_OK;
-  QBX_TRY(launch_trans_build(p->geo, p->tc, (double*)ws->translations, S(stream)),
+  const TransAux aux = trans_aux(p, ws->translations);
+  if (!p->m2l_aux.empty())
+    QBX_TRY(cudaMemcpyAsync((char*)ws->translations + p->m2l_aux_off, p->m2l_aux.data(),
+                            p->m2l_aux.size(), cudaMemcpyHostToDevice, S(stream)),
+            "precompute_translations: M2L class maps");
+  QBX_TRY(launch_trans_build(p->tc, p->m2l_sym.ncanon, aux.canon_off, (double*)ws->translations,
+                             S(stream)),
           "precompute_translations");
   if (p->tf32_ok)
     QBX_TRY(launch_trans_split_tf32(p->tc, (const double*)ws->translations,
@@ -1143,12 +1182,12 @@ int run_m2l(const qbxfmm_plan* p, const qbxfmm_workspace* ws, const uint32_t* T3
   cudaStream_t st = S(stream);
   if (T32)
     QBX_TRY(launch_m2l_gemm_mixed(p->geo, p->th, p->tc, p->kern.nrhs, T32,
-                                  (const double2*)ws->mpoles, (double2*)ws->locals,
+                                  trans_aux(p, ws->translations), (const double2*)ws->mpoles, (double2*)ws->locals,
                                   (double*)ws->pair_scratch, ws->error_word, st),
             "multipole_to_local (split TF32)");
   else if (gemm)
     QBX_TRY(launch_m2l_gemm(p->geo, p->th, p->tc, p->kern.nrhs, (const double*)ws->translations,
-                            (const double2*)ws->mpoles, (double2*)ws->locals,
+                            trans_aux(p, ws->translations), (const double2*)ws->mpoles, (double2*)ws->locals,
                             (double*)ws->pair_scratch, ws->error_word, st),
             "multipole_to_local (matrix form)");
   else

@@ -3,6 +3,8 @@
 
 #include <cuda_runtime.h>
 
+#include <vector>
+
 #include "common.cuh"
 
 namespace qbx {
@@ -27,15 +29,30 @@ struct TransCfg {
   size_t nmatrices = 0;
 };
 
-TransCfg trans_cfg_laplace3(int p, int nclasses);
+// M2L classes merged by the lattice symmetries of their offsets (laplace.cuh):
+// canon_off [3][ncanon] the canonical offsets, cls_code[class] = canonical index << 4 |
+// symmetry code
+struct M2LSymClasses {
+  int ncanon = 0;
+  std::vector<int32_t> canon_off, cls_code;
+};
+M2LSymClasses m2l_symmetry_classes(int nclasses, const std::vector<int32_t>& offs);
+// the same on the device (in the translations buffer)
+struct TransAux {
+  const int32_t* canon_off = nullptr;
+  const int32_t* cls_code = nullptr;
+};
+
+TransCfg trans_cfg_laplace3(int p, int nm2l);
 TransCfg trans_cfg_helm3(int p, int nclasses, int nlevels);
 bool trans_supported(const TransCfg& c);
 size_t trans_matrix_bytes(const TransCfg& c);
 size_t trans_scratch_bytes(const TransCfg& c, int npairs, int nrhs);
-cudaError_t launch_trans_build(const qbxfmm_geometry& g, const TransCfg& c, double* T, cudaStream_t st);
+cudaError_t launch_trans_build(const TransCfg& c, int nm2l, const int32_t* offs, double* T,
+                               cudaStream_t st);
 cudaError_t launch_m2l_gemm(const qbxfmm_geometry& g, const TransHost& th, const TransCfg& c,
-                            int nrhs, const double* T, const double2* mp, double2* lo,
-                            double* cpair, int32_t* err, cudaStream_t st);
+                            int nrhs, const double* T, const TransAux& aux, const double2* mp,
+                            double2* lo, double* cpair, int32_t* err, cudaStream_t st);
 cudaError_t launch_m2m_gemm(const qbxfmm_geometry& g, const TransHost& th, const TransCfg& c,
                             int nrhs, const double* T, double2* mp, double* cpair, int32_t* err,
                             cudaStream_t st);
@@ -64,8 +81,9 @@ size_t tf32_matrix_bytes(const TransCfg& c);
 cudaError_t launch_trans_split_tf32(const TransCfg& c, const double* T, uint32_t* T32,
                                     cudaStream_t st);
 cudaError_t launch_m2l_gemm_mixed(const qbxfmm_geometry& g, const TransHost& th, const TransCfg& c,
-                                  int nrhs, const uint32_t* T32, const double2* mp, double2* lo,
-                                  double* cpair, int32_t* err, cudaStream_t st);
+                                  int nrhs, const uint32_t* T32, const TransAux& aux,
+                                  const double2* mp, double2* lo, double* cpair, int32_t* err,
+                                  cudaStream_t st);
 cudaError_t launch_m2m_gemm_mixed(const qbxfmm_geometry& g, const TransHost& th, const TransCfg& c,
                                   int nrhs, const uint32_t* T32, double2* mp, double* cpair,
                                   int32_t* err, cudaStream_t st);

@@ -501,7 +501,8 @@ constexpr int X3_MT = 16;      // max m16 tiles (rows <= 256)
 // pair_dst's expansion, or stored per pair into cpair (FP64, row stride rp).
 __global__ void __launch_bounds__(NT)
 k_trans_gemm_x3(int ncf, int rp, int rp16, int kp8, int nrhs, const uint32_t* __restrict__ Thi,
-                const uint32_t* __restrict__ Tlo, int mat_mod, const int32_t* __restrict__ group_starts,
+                const uint32_t* __restrict__ Tlo, int mat_mod, const int32_t* __restrict__ cls_code,
+                const int32_t* __restrict__ group_starts,
                 int g0, const int32_t* __restrict__ pair_src, const int32_t* __restrict__ pair_dst,
                 const double2* __restrict__ ein, double2* __restrict__ eout, double scale,
                 double* __restrict__ cpair, int32_t* err, int nboxes)
@@ -518,7 +519,14 @@ k_trans_gemm_x3(int ncf, int rp, int rp16, int kp8, int nrhs, const uint32_t* __
   int ncol = (p1 - p0) * nrhs;
   int c0 = blockIdx.x * X3_N;
   if (c0 >= ncol) return;
-  int mat = mat_mod > 0 ? (grp % mat_mod) : grp;
+  int mat = mat_mod > 0 ? (grp % mat_mod) : grp, sym = 0;
+  if (cls_code) {
+    const int code = cls_code[grp];
+    mat = code >> 4;
+    sym = code & 15;
+  }
+  __shared__ uint8_t s_opi[M2L_SYM_MAXR], s_opo[M2L_SYM_MAXR];
+  if (sym) m2l_sym_tables(sym, 2 * ncf, s_opi, s_opo, threadIdx.x, NT);
   const uint32_t* Th = Thi + (size_t)mat * rp16 * kp8;
   const uint32_t* Tl = Tlo + (size_t)mat * rp16 * kp8;
   const int R = 2 * ncf;
@@ -555,7 +563,10 @@ k_trans_gemm_x3(int ncf, int rp, int rp16, int kp8, int nrhs, const uint32_t* __
       float v = 0.0f;
       if (src >= 0 && k < kw && kc + k < R) {
         int r = (c0 + j) % nrhs;
-        v = (float)__ldg(reinterpret_cast<const double*>(ein + ((size_t)src * nrhs + r) * ncf) + kc + k);
+        const double2* x2 = ein + ((size_t)src * nrhs + r) * ncf;
+        const int kg = kc + k;
+        const double* x = reinterpret_cast<const double*>(x2);
+        v = (float)(sym ? m2l_sym_apply(x, kg, s_opi[kg]) : __ldg(x + kg));
       }
       uint32_t hi = to_tf32(v);
       Bh[k * BS + j] = hi;
@@ -588,7 +599,22 @@ k_trans_gemm_x3(int ncf, int rp, int rp16, int kp8, int nrhs, const uint32_t* __
       }
     }
   }
-  // epilogue: acc[i][v] = C[row = i*16 + g + 8 (v >> 1)][col = warp*8 + 2 tq + (v & 1)]
+  // epilogue: acc[i][v] = C[row = i*16 + g + 8 (v >> 1)][col = warp*8 + 2 tq + (v & 1)];
+  // with a class symmetry, its output map first (row ^ 1 is in lane ^ 4)
+  if (sym) {
+#pragma unroll
+    for (int i = 0; i < X3_MT; ++i)
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const float other = __shfl_xor_sync(0xffffffffu, acc[i][v], 4);
+        const int row = i * 16 + g + 8 * (v >> 1);
+        if (i < mt && row < R) {
+          const int op = s_opo[row];
+          const float w = (op & 1) ? other : acc[i][v];
+          acc[i][v] = (op & 2) ? -w : w;
+        }
+      }
+  }
 #pragma unroll
   for (int v = 0; v < 4; ++v) {
     int c = c0 + warp * 8 + 2 * tq + (v & 1);
@@ -705,7 +731,8 @@ __global__ void k_trans_umma_planes(int nmat, int rp, int kp, int rp16, int nkc,
 
 __global__ void __launch_bounds__(UM_NT)
 k_trans_gemm_umma(int ncf, int rp, int rp16, int nkc, int nrhs, const uint32_t* __restrict__ Uhi,
-                  const uint32_t* __restrict__ Ulo, const int32_t* __restrict__ group_starts,
+                  const uint32_t* __restrict__ Ulo, const int32_t* __restrict__ cls_code,
+                  const int32_t* __restrict__ group_starts,
                   const int32_t* __restrict__ pair_src, const double2* __restrict__ ein,
                   double* __restrict__ cpair, int32_t* err, int nboxes)
 {
@@ -725,8 +752,12 @@ k_trans_gemm_umma(int ncf, int rp, int rp16, int nkc, int nrhs, const uint32_t* 
   const int c0 = blockIdx.x * UM_M;
   if (c0 >= ncol) return;                               // uniform, before any allocation
   const size_t mper = (size_t)nkc * bw;
-  const uint32_t* Th = Uhi + (size_t)grp * mper;
-  const uint32_t* Tl = Ulo + (size_t)grp * mper;
+  const int code = cls_code ? cls_code[grp] : grp << 4;
+  const int mat = code >> 4, sym = code & 15;
+  __shared__ uint8_t s_opi[M2L_SYM_MAXR], s_opo[M2L_SYM_MAXR];
+  if (sym) m2l_sym_tables(sym, 2 * ncf, s_opi, s_opo, threadIdx.x, UM_NT);
+  const uint32_t* Th = Uhi + (size_t)mat * mper;
+  const uint32_t* Tl = Ulo + (size_t)mat * mper;
   const int R = 2 * ncf;
   const int warp = threadIdx.x >> 5;
   if (threadIdx.x < UM_M) {
@@ -790,7 +821,7 @@ k_trans_gemm_umma(int ncf, int rp, int rp16, int nkc, int nrhs, const uint32_t* 
     for (int j = 0; j < UM_KC / 2; ++j) {
       const int k = khalf * (UM_KC / 2) + j, kg = kc * UM_KC + k;
       float v = 0.0f;
-      if (xin && kg < R) v = (float)__ldg(xin + kg);
+      if (xin && kg < R) v = (float)(sym ? m2l_sym_apply(xin, kg, s_opi[kg]) : __ldg(xin + kg));
       const uint32_t hi = to_tf32(v);
       ah[um_off(row, k)] = hi;
       al[um_off(row, k)] = to_tf32(v - __uint_as_float(hi));
@@ -864,9 +895,20 @@ k_trans_gemm_umma(int ncf, int rp, int rp16, int nkc, int nrhs, const uint32_t* 
                    : "r"(ta));
       asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
       if (y) {
+        if (sym) {
+          // the class symmetry's output map (rows nb + 2u, nb + 2u + 1 are one coefficient)
 #pragma unroll
-        for (int j = 0; j < 16; ++j)
-          if (nb + j < R) y[nb + j] = (double)__uint_as_float(v[j]);
+          for (int j = 0; j < 16; ++j)
+            if (nb + j < R) {
+              const int op = s_opo[nb + j];
+              const float w = __uint_as_float((op & 1) ? v[j ^ 1] : v[j]);
+              y[nb + j] = (double)((op & 2) ? -w : w);
+            }
+        } else {
+#pragma unroll
+          for (int j = 0; j < 16; ++j)
+            if (nb + j < R) y[nb + j] = (double)__uint_as_float(v[j]);
+        }
       }
     }
   }
@@ -986,7 +1028,8 @@ cudaError_t launch_trans_split_tf32(const TransCfg& c, const double* T, uint32_t
 }
 
 static cudaError_t x3_launch(const qbxfmm_geometry& g, const TransCfg& c, int nrhs, const uint32_t* T32,
-                             size_t mat_base, int mat_mod, const int32_t* group_starts, int g0,
+                             size_t mat_base, int mat_mod, const int32_t* cls_code,
+                             const int32_t* group_starts, int g0,
                              int ngroups, int maxcols, const int32_t* pair_src,
                              const int32_t* pair_dst, const double2* ein, double2* eout,
                              double scale, double* cpair, int32_t* err, cudaStream_t st)
@@ -1000,7 +1043,8 @@ static cudaError_t x3_launch(const qbxfmm_geometry& g, const TransCfg& c, int nr
   cudaFuncSetAttribute(k_trans_gemm_x3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
   dim3 grid((maxcols + X3_N - 1) / X3_N, ngroups);
   k_trans_gemm_x3<<<grid, NT, sh, st>>>(c.ncf, c.rp, rp16, kp8, nrhs, T32 + mat_base * plane,
-                                        T32 + n + mat_base * plane, mat_mod, group_starts, g0,
+                                        T32 + n + mat_base * plane, mat_mod, cls_code,
+                                        group_starts, g0,
                                         pair_src, pair_dst, ein, eout, scale, cpair, err, g.nboxes);
   return cudaGetLastError();
 }
@@ -1028,7 +1072,7 @@ static size_t umma_plane_words(const TransCfg& c)
 }
 
 static cudaError_t umma_launch(const qbxfmm_geometry& g, const TransCfg& c, int nrhs,
-                               const uint32_t* U, int ngroups, int maxcols,
+                               const uint32_t* U, const int32_t* cls_code, int ngroups, int maxcols,
                                const int32_t* group_starts, const int32_t* pair_src,
                                const double2* ein, double* cpair, int32_t* err, cudaStream_t st)
 {
@@ -1041,14 +1085,16 @@ static cudaError_t umma_launch(const qbxfmm_geometry& g, const TransCfg& c, int 
   if (e != cudaSuccess) return e;
   dim3 grid((maxcols + UM_M - 1) / UM_M, ngroups);
   k_trans_gemm_umma<<<grid, UM_NT, sh, st>>>(c.ncf, c.rp, rp16, nkc, nrhs, U,
-                                             U + umma_plane_words(c), group_starts, pair_src, ein,
+                                             U + umma_plane_words(c), cls_code, group_starts,
+                                             pair_src, ein,
                                              cpair, err, g.nboxes);
   return cudaGetLastError();
 }
 
 cudaError_t launch_m2l_gemm_mixed(const qbxfmm_geometry& g, const TransHost& th, const TransCfg& c,
-                                  int nrhs, const uint32_t* T32, const double2* mp, double2* lo,
-                                  double* cpair, int32_t* err, cudaStream_t st)
+                                  int nrhs, const uint32_t* T32, const TransAux& aux,
+                                  const double2* mp, double2* lo, double* cpair, int32_t* err,
+                                  cudaStream_t st)
 {
   if (g.m2l_nclasses == 0) return cudaSuccess;
   int rp16, kp8;
@@ -1057,9 +1103,9 @@ cudaError_t launch_m2l_gemm_mixed(const qbxfmm_geometry& g, const TransHost& th,
   // (bulk copies need 16-byte aligned planes)
   const bool umma = umma_shape_ok(c) && (reinterpret_cast<uintptr_t>(U) & 15) == 0;
   cudaError_t e = umma
-      ? umma_launch(g, c, nrhs, U, g.m2l_nclasses, th.m2l_max_pairs * nrhs, g.m2l_class_starts,
-                    g.m2l_pair_src, mp, cpair, err, st)
-      : x3_launch(g, c, nrhs, T32, 0, 0, g.m2l_class_starts, 0, g.m2l_nclasses,
+      ? umma_launch(g, c, nrhs, U, aux.cls_code, g.m2l_nclasses, th.m2l_max_pairs * nrhs,
+                    g.m2l_class_starts, g.m2l_pair_src, mp, cpair, err, st)
+      : x3_launch(g, c, nrhs, T32, 0, 0, aux.cls_code, g.m2l_class_starts, 0, g.m2l_nclasses,
                   th.m2l_max_pairs * nrhs, g.m2l_pair_src, nullptr, mp, nullptr, 1.0, cpair, err,
                   st);
   if (e != cudaSuccess) return e;
@@ -1074,7 +1120,7 @@ cudaError_t launch_m2m_gemm_mixed(const qbxfmm_geometry& g, const TransHost& th,
   for (int lev = g.nlevels - 2; lev >= 0; --lev) {
     int maxp = th.m2m_level_max_group[lev];
     if (maxp == 0) continue;
-    cudaError_t e = x3_launch(g, c, nrhs, T32, c.m2m_base, c.m2m_mat_mod, g.m2m_group_starts,
+    cudaError_t e = x3_launch(g, c, nrhs, T32, c.m2m_base, c.m2m_mat_mod, nullptr, g.m2m_group_starts,
                               lev * nch, nch, maxp * nrhs, g.m2m_pair_src, nullptr, mp, nullptr,
                               1.0, cpair, err, st);
     if (e != cudaSuccess) return e;
@@ -1092,7 +1138,7 @@ cudaError_t launch_l2l_gemm_mixed(const qbxfmm_geometry& g, const TransHost& th,
   for (int lev = 1; lev < g.nlevels; ++lev) {
     int maxp = th.l2l_level_max_group[lev];
     if (maxp == 0) continue;
-    cudaError_t e = x3_launch(g, c, nrhs, T32, c.l2l_base, c.m2m_mat_mod, g.l2l_group_starts,
+    cudaError_t e = x3_launch(g, c, nrhs, T32, c.l2l_base, c.m2m_mat_mod, nullptr, g.l2l_group_starts,
                               lev * nch, nch, maxp * nrhs, g.l2l_pair_src, g.l2l_pair_dst, lo, lo,
                               1.0, nullptr, err, st);
     if (e != cudaSuccess) return e;

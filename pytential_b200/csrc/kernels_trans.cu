@@ -13,8 +13,19 @@
 //   k_trans_gemm   : one CTA per (class, 32 pairs x rhs): C = T X with X the gathered
 //                    source expansions; T and X staged in shared memory
 //   k_trans_reduce : deterministic sum of each output box's pair results (list order)
+//
+// M2L classes related by a lattice symmetry (quarter turns about z, y and z
+// reflections) share the matrix of their canonical offset: the GEMM applies the
+// class's input map to the gathered columns and its output map to the products
+// (m2l_symmetry_classes, laplace.cuh).
 #include "laplace.cuh"
 #include "kernels.h"
+
+#include <algorithm>
+#include <array>
+#include <cstdlib>
+#include <map>
+#include <vector>
 
 #include <cooperative_groups.h>
 namespace cg = cooperative_groups;
@@ -112,7 +123,8 @@ constexpr int TSTR = KC + 4;         // padded T-chunk row stride (== 4 mod 16 d
 template <int MTW>
 __global__ void __launch_bounds__(NT)
 k_trans_gemm(int ncf, int rp, int kp, int nrhs, int nwm, const double* __restrict__ T,
-             int mat_base, int mat_mod, const int32_t* __restrict__ group_starts, int g0,
+             int mat_base, int mat_mod, const int32_t* __restrict__ cls_code,
+             const int32_t* __restrict__ group_starts, int g0,
              const int32_t* __restrict__ pair_src, const int32_t* __restrict__ pair_dst,
              const double2* __restrict__ ein, double2* __restrict__ eout, double scale,
              double* __restrict__ cpair, int32_t* err, int nboxes)
@@ -128,9 +140,16 @@ k_trans_gemm(int ncf, int rp, int kp, int nrhs, int nwm, const double* __restric
   int ncol = (p1 - p0) * nrhs;
   int c0 = blockIdx.x * ntile;
   if (c0 >= ncol) return;
-  int mat = mat_base + (mat_mod > 0 ? (grp % mat_mod) : grp);
+  int mat = mat_base + (mat_mod > 0 ? (grp % mat_mod) : grp), sym = 0;
+  if (cls_code) {
+    const int code = cls_code[grp];
+    mat = mat_base + (code >> 4);
+    sym = code & 15;
+  }
   const double* Tg = T + (size_t)mat * rp * kp;
   const int R = 2 * ncf;
+  __shared__ uint8_t s_opi[M2L_SYM_MAXR], s_opo[M2L_SYM_MAXR];
+  if (sym) m2l_sym_tables(sym, R, s_opi, s_opo, threadIdx.x, NT);
   for (int j = threadIdx.x; j < ntile; j += NT) {
     int c = c0 + j;
     int src = -1;
@@ -165,8 +184,10 @@ k_trans_gemm(int ncf, int rp, int kp, int nrhs, int nwm, const double* __restric
       double v = 0.0;
       if (src >= 0 && k < kw && kc + k < R) {
         int r = (c0 + j) % nrhs;
-        const double* x = reinterpret_cast<const double*>(ein + ((size_t)src * nrhs + r) * ncf);
-        v = __ldg(x + kc + k);
+        const double2* x2 = ein + ((size_t)src * nrhs + r) * ncf;
+        const int kg = kc + k;
+        const double* x = reinterpret_cast<const double*>(x2);
+        v = sym ? m2l_sym_apply(x, kg, s_opi[kg]) : __ldg(x + kg);
       }
       Xs[k * XS + j] = v;
     }
@@ -183,7 +204,23 @@ k_trans_gemm(int ncf, int rp, int kp, int nrhs, int nwm, const double* __restric
       }
     }
   }
-  // epilogue: acc[i][v] = C[row = (mbeg + i) * 8 + g][col = wn * 8 + 2 tq + v]
+  // epilogue: acc[i][v] = C[row = (mbeg + i) * 8 + g][col = wn * 8 + 2 tq + v]; with a
+  // class symmetry, its output map first (the other half of row's coefficient, row ^ 1,
+  // is in lane ^ 4)
+  if (sym) {
+#pragma unroll
+    for (int v = 0; v < 2; ++v)
+#pragma unroll
+      for (int i = 0; i < MTW; ++i) {
+        const double other = __shfl_xor_sync(0xffffffffu, acc[i][v], 4);
+        const int row = (mbeg + i) * 8 + g;
+        if (mbeg + i < mt && row < R) {
+          const int op = s_opo[row];
+          const double w = (op & 1) ? other : acc[i][v];
+          acc[i][v] = (op & 2) ? -w : w;
+        }
+      }
+  }
 #pragma unroll
   for (int v = 0; v < 2; ++v) {
     int j = wn * 8 + 2 * tq + v;
@@ -336,11 +373,26 @@ k_trans_reduce(int ncf, int rp, int nrhs, const int32_t* __restrict__ boxes, int
   double sc = div_by_width ? ldexp(1.0, box_levels[o]) / root_extent : 1.0;
   int R = 2 * ncf;
   double* y = reinterpret_cast<double*>(eout + ((size_t)o * nrhs + r) * ncf);
-  for (int row = threadIdx.x; row < R; row += NT) {
+  const int q0 = starts[i], q1 = starts[i + 1];
+  // the box's pair rows, staged once per chunk so that the loads of successive pairs
+  // are independent
+  constexpr int QC = 256;
+  __shared__ const double* s_row[QC];
+  for (int row0 = 0; row0 < R; row0 += NT) {
+    const int row = row0 + threadIdx.x;
     double acc = 0.0;
-    for (int q = starts[i]; q < starts[i + 1]; ++q)
-      acc += cpair[((size_t)pairs[q] * nrhs + r) * rp + row];
-    y[row] += sc * acc;
+    for (int qc = q0; qc < q1; qc += QC) {
+      const int nq = min(QC, q1 - qc);
+      __syncthreads();
+      for (int t = threadIdx.x; t < nq; t += NT)
+        s_row[t] = cpair + ((size_t)pairs[qc + t] * nrhs + r) * rp;
+      __syncthreads();
+      if (row < R) {
+#pragma unroll 4
+        for (int t = 0; t < nq; ++t) acc += s_row[t][row];
+      }
+    }
+    if (row < R) y[row] += sc * acc;
   }
 }
 
@@ -534,22 +586,64 @@ static int gemm_nwm(int rp)
 
 bool trans_supported(const TransCfg& c) { return c.rp / 8 <= 96 && gemm_smem(c.rp) <= 200 * 1024; }
 
-// T layout: [0, nclasses) M2L classes, then M2M and L2L matrices (TransCfg bases)
-cudaError_t launch_trans_build(const qbxfmm_geometry& g, const TransCfg& c, double* T, cudaStream_t st)
+M2LSymClasses m2l_symmetry_classes(int nclasses, const std::vector<int32_t>& offs)
+{
+  M2LSymClasses r;
+  r.cls_code.resize(nclasses);
+  std::vector<std::array<int, 3>> canon;
+  std::map<std::array<int, 3>, int> index;
+  for (int c = 0; c < nclasses; ++c) {
+    const int dx = offs[c], dy = offs[(size_t)nclasses + c], dz = offs[2 * (size_t)nclasses + c];
+    const int a = std::max(std::abs(dx), std::abs(dy)), b = std::min(std::abs(dx), std::abs(dy));
+    const std::array<int, 3> key = {a, b, std::abs(dz)};
+    // (dx, dy) = R^q C^s (a, b)
+    int code = -1;
+    for (int q = 0; q < 4 && code < 0; ++q)
+      for (int s = 0; s < 2 && code < 0; ++s) {
+        int x = a, y = s ? -b : b;
+        for (int i = 0; i < q; ++i) {
+          const int t = x;
+          x = -y;
+          y = t;
+        }
+        if (x == dx && y == dy) code = q | s << 2 | (dz < 0 ? 8 : 0);
+      }
+    auto it = index.find(key);
+    int ci;
+    if (it == index.end()) {
+      ci = (int)canon.size();
+      index.emplace(key, ci);
+      canon.push_back(key);
+    } else {
+      ci = it->second;
+    }
+    r.cls_code[c] = ci << 4 | code;
+  }
+  r.ncanon = (int)canon.size();
+  r.canon_off.resize(3 * (size_t)r.ncanon);
+  for (int i = 0; i < r.ncanon; ++i)
+    for (int k = 0; k < 3; ++k) r.canon_off[(size_t)k * r.ncanon + i] = canon[i][k];
+  return r;
+}
+
+// T layout: [0, nm2l) M2L matrices (one per canonical offset), then M2M and L2L
+// matrices (TransCfg bases); offs: [3][nm2l] on the device
+cudaError_t launch_trans_build(const TransCfg& c, int nm2l, const int32_t* offs, double* T,
+                               cudaStream_t st)
 {
   int p = c.p;
   size_t sh = (size_t)(2 * p + 1) * (2 * p + 2) / 2 * sizeof(double2);
   size_t stride = (size_t)c.rp * c.kp;
-  if (g.m2l_nclasses > 0)
-    k_trans_build<<<g.m2l_nclasses, NT, sh, st>>>(0, p, c.ncf, c.rp, c.kp, g.m2l_nclasses,
-                                                   g.m2l_class_offsets, T);
+  if (nm2l > 0)
+    k_trans_build<<<nm2l, NT, sh, st>>>(0, p, c.ncf, c.rp, c.kp, nm2l, offs, T);
   k_trans_build<<<8, NT, sh, st>>>(1, p, c.ncf, c.rp, c.kp, 8, nullptr, T + c.m2m_base * stride);
   k_trans_build<<<8, NT, sh, st>>>(2, p, c.ncf, c.rp, c.kp, 8, nullptr, T + c.l2l_base * stride);
   return cudaGetLastError();
 }
 
 static cudaError_t gemm_launch(const qbxfmm_geometry& g, const TransCfg& c, int nrhs, const double* T,
-                               size_t mat_base, int mat_mod, const int32_t* group_starts_dev,
+                               size_t mat_base, int mat_mod, const int32_t* cls_code,
+                               const int32_t* group_starts_dev,
                                int g0, int ngroups, int maxcols, const int32_t* pair_src,
                                const int32_t* pair_dst, const double2* ein, double2* eout,
                                double scale, double* cpair, int32_t* err, cudaStream_t st)
@@ -565,7 +659,7 @@ static cudaError_t gemm_launch(const qbxfmm_geometry& g, const TransCfg& c, int 
 #define QBX_GEMM_CASE(W)                                                                        \
   if (mtw <= W) {                                                                               \
     cudaFuncSetAttribute(k_trans_gemm<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh); \
-    k_trans_gemm<W><<<grid, NT, sh, st>>>(ncf, rp, kp, nrhs, nwm, Tb, 0, mat_mod,               \
+    k_trans_gemm<W><<<grid, NT, sh, st>>>(ncf, rp, kp, nrhs, nwm, Tb, 0, mat_mod, cls_code,     \
                                           group_starts_dev, g0, pair_src, pair_dst, ein, eout,  \
                                           scale, cpair, err, g.nboxes);                         \
     return cudaGetLastError();                                                                  \
@@ -580,18 +674,15 @@ static cudaError_t gemm_launch(const qbxfmm_geometry& g, const TransCfg& c, int 
 }
 
 cudaError_t launch_m2l_gemm(const qbxfmm_geometry& g, const TransHost& th, const TransCfg& c,
-                            int nrhs, const double* T, const double2* mp, double2* lo,
-                            double* cpair, int32_t* err, cudaStream_t st)
+                            int nrhs, const double* T, const TransAux& aux, const double2* mp,
+                            double2* lo, double* cpair, int32_t* err, cudaStream_t st)
 {
   if (g.m2l_nclasses == 0) return cudaSuccess;
-  cudaError_t e = gemm_launch(g, c, nrhs, T, 0, 0, g.m2l_class_starts, 0, g.m2l_nclasses,
-                              th.m2l_max_pairs * nrhs, g.m2l_pair_src, nullptr, mp, nullptr, 1.0,
-                              cpair, err, st);
+  cudaError_t e = gemm_launch(g, c, nrhs, T, 0, 0, aux.cls_code, g.m2l_class_starts, 0,
+                              g.m2l_nclasses, th.m2l_max_pairs * nrhs, g.m2l_pair_src, nullptr, mp,
+                              nullptr, 1.0, cpair, err, st);
   if (e != cudaSuccess) return e;
-  k_trans_reduce<<<dim3(g.nttp_boxes, nrhs), NT, 0, st>>>(
-      c.ncf, c.rp, nrhs, g.target_or_target_parent_boxes, 0, g.m2l_tgt_pair_starts,
-      g.m2l_tgt_pairs, cpair, lo, c.m2l_div_by_width, g.box_levels, g.root_extent);
-  return cudaGetLastError();
+  return launch_trans_reduce_m2l(g, c, nrhs, cpair, lo, st);
 }
 
 cudaError_t launch_m2m_gemm(const qbxfmm_geometry& g, const TransHost& th, const TransCfg& c,
@@ -603,7 +694,7 @@ cudaError_t launch_m2m_gemm(const qbxfmm_geometry& g, const TransHost& th, const
     int g0 = lev * nch;
     int maxp = th.m2m_level_max_group[lev];
     if (maxp == 0) continue;
-    cudaError_t e = gemm_launch(g, c, nrhs, T, c.m2m_base, c.m2m_mat_mod, g.m2m_group_starts, g0,
+    cudaError_t e = gemm_launch(g, c, nrhs, T, c.m2m_base, c.m2m_mat_mod, nullptr, g.m2m_group_starts, g0,
                                 nch, maxp * nrhs, g.m2m_pair_src, nullptr, mp, nullptr, 1.0, cpair,
                                 err, st);
     if (e != cudaSuccess) return e;
@@ -626,7 +717,7 @@ cudaError_t launch_l2l_gemm(const qbxfmm_geometry& g, const TransHost& th, const
     int g0 = lev * nch;
     int maxp = th.l2l_level_max_group[lev];
     if (maxp == 0) continue;
-    cudaError_t e = gemm_launch(g, c, nrhs, T, c.l2l_base, c.m2m_mat_mod, g.l2l_group_starts, g0,
+    cudaError_t e = gemm_launch(g, c, nrhs, T, c.l2l_base, c.m2m_mat_mod, nullptr, g.l2l_group_starts, g0,
                                 nch, maxp * nrhs, g.l2l_pair_src, g.l2l_pair_dst, lo, lo, 1.0,
                                 nullptr, err, st);
     if (e != cudaSuccess) return e;

@@ -23,6 +23,75 @@ QBX_HD void decode3(int c, int& n, int& m)
   m = c - n * (n + 1) / 2;
 }
 
+// {{{ 3D M2L offset symmetries
+//
+// The 16 isometries that map the box lattice to itself and the z axis to itself,
+// sigma = R^q C^s Z^t (R: quarter turn about z, (x, y) -> (-y, x); C: y -> -y;
+// Z: z -> -z; code q | s << 2 | t << 3), act on the stored coefficients (m >= 0) by
+// one phase and an optional conjugation each: from S_n^m(R v) = i^m S_n^m(v),
+// S_n^m(C v) = conj S_n^m(v), S_n^m(Z v) = (-1)^(n+m) S_n^m(v), the M2L matrix of the
+// offset sigma d is
+//   T(sigma d) M = Phi_out( T(d) Phi_in(M) ),
+//   Phi_in(M)_k^l  = i^(2t(k+l) + (s ? -lq : lq)) conj^s(M_k^l),
+//   Phi_out(L)_j^i = i^(2t(j+i) + iq) conj^s(L_j^i),
+// so every list-2 offset uses the matrix of one canonical offset (dx >= dy >= 0,
+// dz >= 0).
+
+// largest real entry count (2 x coefficients) the class kernels' op tables hold
+constexpr int M2L_SYM_MAXR = 1024;
+
+// triangular index -> (n, m), single precision start (exact for c < 2^20)
+QBX_D void coef_nm3(int c, int& n, int& m)
+{
+  int nn = (int)((sqrtf(8.0f * c + 1.0f) - 1.0f) * 0.5f);
+  while ((nn + 1) * (nn + 2) / 2 <= c) ++nn;
+  while (nn * (nn + 1) / 2 > c) --nn;
+  n = nn;
+  m = c - nn * (nn + 1) / 2;
+}
+
+// key of the stored coefficient c: (n + m) mod 2 | (m mod 4) << 1 (all the maps need)
+QBX_D int m2l_sym_key(int c)
+{
+  int n, m;
+  coef_nm3(c, n, m);
+  return ((n + m) & 1) | ((m & 3) << 1);
+}
+
+// Each map sends a coefficient (a, b) to i^e conj^s(a + ib): entry `part` of the result
+// is +-a or +-b.  Returned: bit 0 = take the other entry of the coefficient (k ^ 1),
+// bit 1 = negate.  Phi_in (out = false) or Phi_out (out = true) of the coefficient
+// with key `key`.
+QBX_D int m2l_sym_op(int key, int sym, bool out, int part)
+{
+  const int q = sym & 3, s = (sym >> 2) & 1, t = (sym >> 3) & 1;
+  const int m4 = key >> 1;
+  const int e = (2 * t * (key & 1) + ((s && !out) ? -m4 * q : m4 * q)) & 3;
+  int neg;
+  if (part == 0) neg = e == 2 || (e == 1 && !s) || (e == 3 && s);
+  else neg = e == 3 || (e == 0 && s) || (e == 2 && !s);
+  return (e & 1) | neg << 1;
+}
+
+// the per-CTA op tables of a class symmetry: op_in[k], op_out[k] for real entries k < R
+QBX_D void m2l_sym_tables(int sym, int R, uint8_t* op_in, uint8_t* op_out, int tid, int nt)
+{
+  for (int k = tid; k < R; k += nt) {
+    const int key = m2l_sym_key(k >> 1);
+    op_in[k] = (uint8_t)m2l_sym_op(key, sym, false, k & 1);
+    op_out[k] = (uint8_t)m2l_sym_op(key, sym, true, k & 1);
+  }
+}
+
+// entry k of a mapped vector x (interleaved re, im) by its op
+QBX_D double m2l_sym_apply(const double* x, int k, int op)
+{
+  const double v = __ldg(x + (k ^ (op & 1)));
+  return (op & 2) ? -v : v;
+}
+
+// }}}
+
 // {{{ 3D single entries by recurrence along n (used where a thread owns one coefficient)
 
 QBX_D double2 sh3_R_nm(int n, int m, double x, double y, double z)
