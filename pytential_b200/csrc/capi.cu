@@ -479,6 +479,10 @@ int qbxfmm_plan_create(const qbxfmm_kernel* kernel, const qbxfmm_geometry* geome
     e = cudaMemcpy(off.data(), g.m2l_class_offsets, sizeof(int32_t) * off.size(),
                    cudaMemcpyDeviceToHost);
     if (e == cudaSuccess) p->m2l_sym = m2l_symmetry_classes(g.m2l_nclasses, off);
+    if (p->m2l_sym.ncanon < 0) {
+      delete p;
+      return fail(QBXFMM_ERR_ARG, "M2L class offsets are not integer lattice offsets");
+    }
   }
   if (k.dim == 3)
     p->tc = p->h3 ? trans_cfg_helm3(k.fmm_order, 0, g.nlevels)   // M2L by rotation, no class matrices

@@ -817,14 +817,22 @@ k_trans_gemm_umma(int ncf, int rp, int rp16, int nkc, int nrhs, const uint32_t* 
     ++f_iss[st];
     uint32_t* ah = Ah(st);
     uint32_t* al = Al(st);
+    // one coefficient (two entries, kg even; R is even) per load
 #pragma unroll 4
-    for (int j = 0; j < UM_KC / 2; ++j) {
+    for (int j = 0; j < UM_KC / 2; j += 2) {
       const int k = khalf * (UM_KC / 2) + j, kg = kc * UM_KC + k;
-      float v = 0.0f;
-      if (xin && kg < R) v = (float)(sym ? m2l_sym_apply(xin, kg, s_opi[kg]) : __ldg(xin + kg));
-      const uint32_t hi = to_tf32(v);
-      ah[um_off(row, k)] = hi;
-      al[um_off(row, k)] = to_tf32(v - __uint_as_float(hi));
+      double2 z = c2(0.0);
+      if (xin && kg < R) z = __ldg(reinterpret_cast<const double2*>(xin) + (kg >> 1));
+      float v[2];
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const int op = sym ? s_opi[kg + u] : 0;
+        const double w = ((u ^ op) & 1) ? z.y : z.x;
+        v[u] = (float)((op & 2) ? -w : w);
+        const uint32_t hi = to_tf32(v[u]);
+        ah[um_off(row, k + u)] = hi;
+        al[um_off(row, k + u)] = to_tf32(v[u] - __uint_as_float(hi));
+      }
     }
   };
   bool fail = false;

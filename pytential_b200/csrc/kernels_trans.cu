@@ -617,6 +617,10 @@ M2LSymClasses m2l_symmetry_classes(int nclasses, const std::vector<int32_t>& off
     } else {
       ci = it->second;
     }
+    if (code < 0) {                      // not a lattice offset: no shared matrices
+      r.ncanon = -1;
+      return r;
+    }
     r.cls_code[c] = ci << 4 | code;
   }
   r.ncanon = (int)canon.size();
