@@ -174,22 +174,34 @@ k_trans_gemm(int ncf, int rp, int kp, int nrhs, int nwm, const double* __restric
   for (int kc = 0; kc < kp; kc += KC) {
     int kw = min(KC, kp - kc);
     __syncthreads();
-    for (int e = threadIdx.x; e < rp * KC; e += NT) {
-      int row = e / KC, col = e - row * KC;
-      Ts[row * TSTR + col] = col < kw ? __ldg(Tg + (size_t)row * kp + kc + col) : 0.0;
+    // 16-byte loads and stores: kp, kc, kw, TSTR, R and every matrix offset are even
+    constexpr int KH = KC / 2;
+    for (int e = threadIdx.x; e < rp * KH; e += NT) {
+      const int row = e / KH, col = 2 * (e - row * KH);
+      const double2 v = col < kw
+          ? __ldg(reinterpret_cast<const double2*>(Tg + (size_t)row * kp + kc + col)) : c2(0.0);
+      *reinterpret_cast<double2*>(Ts + row * TSTR + col) = v;
     }
-    for (int e = threadIdx.x; e < ntile * KC; e += NT) {
-      int j = e / KC, k = e - j * KC;
-      int src = s_src[j];
-      double v = 0.0;
+    for (int e = threadIdx.x; e < ntile * KH; e += NT) {
+      const int j = e / KH, k = 2 * (e - j * KH);
+      const int src = s_src[j];
+      double v0 = 0.0, v1 = 0.0;
       if (src >= 0 && k < kw && kc + k < R) {
-        int r = (c0 + j) % nrhs;
-        const double2* x2 = ein + ((size_t)src * nrhs + r) * ncf;
-        const int kg = kc + k;
-        const double* x = reinterpret_cast<const double*>(x2);
-        v = sym ? m2l_sym_apply(x, kg, s_opi[kg]) : __ldg(x + kg);
+        const int r = (c0 + j) % nrhs, kg = kc + k;
+        const double2 z = __ldg(ein + ((size_t)src * nrhs + r) * ncf + (kg >> 1));
+        if (sym) {
+          const int o0 = s_opi[kg], o1 = s_opi[kg + 1];
+          v0 = (o0 & 1) ? z.y : z.x;
+          v1 = (o1 & 1) ? z.x : z.y;
+          if (o0 & 2) v0 = -v0;
+          if (o1 & 2) v1 = -v1;
+        } else {
+          v0 = z.x;
+          v1 = z.y;
+        }
       }
-      Xs[k * XS + j] = v;
+      Xs[k * XS + j] = v0;
+      Xs[(k + 1) * XS + j] = v1;
     }
     __syncthreads();
     for (int k0 = 0; k0 < kw; k0 += 4) {
