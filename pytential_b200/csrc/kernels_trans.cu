@@ -278,8 +278,8 @@ k_trans_gemm_tiled(int ncf, int rp, int kp, int nrhs, const double* __restrict__
                    const double2* __restrict__ ein, double2* __restrict__ eout, double scale,
                    double* __restrict__ cpair, int32_t* err, int nboxes)
 {
-  __shared__ double As[GT_M][GT_AS];
-  __shared__ double Bs[GT_K][GT_BS];
+  __shared__ __align__(16) double As[GT_M][GT_AS];
+  __shared__ __align__(16) double Bs[GT_K][GT_BS];
   __shared__ int s_src[GT_N];
   int grp = g0 + blockIdx.z;
   int p0 = group_starts[grp], p1 = group_starts[grp + 1];
@@ -312,19 +312,22 @@ k_trans_gemm_tiled(int ncf, int rp, int kp, int nrhs, const double* __restrict__
     for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
   for (int kc = 0; kc < kp; kc += GT_K) {
     __syncthreads();
-    for (int e = threadIdx.x; e < GT_M * GT_K; e += NT) {
-      int row = e / GT_K, k = e - row * GT_K;
-      As[row][k] = (m0 + row < rp && kc + k < kp) ? __ldg(Tg + (size_t)(m0 + row) * kp + kc + k) : 0.0;
+    // 16-byte loads and stores (kp, kc, GT_AS, R and the matrix offsets are even)
+    constexpr int KH = GT_K / 2;
+    for (int e = threadIdx.x; e < GT_M * KH; e += NT) {
+      const int row = e / KH, k = 2 * (e - row * KH);
+      const double2 v = (m0 + row < rp && kc + k < kp)
+          ? __ldg(reinterpret_cast<const double2*>(Tg + (size_t)(m0 + row) * kp + kc + k)) : c2(0.0);
+      *reinterpret_cast<double2*>(&As[row][k]) = v;
     }
-    for (int e = threadIdx.x; e < GT_N * GT_K; e += NT) {
-      int j = e / GT_K, k = e - j * GT_K;
-      int src = s_src[j];
-      double v = 0.0;
-      if (src >= 0 && kc + k < R) {
-        int r = (c0 + j) % nrhs;
-        v = __ldg(reinterpret_cast<const double*>(ein + ((size_t)src * nrhs + r) * ncf) + kc + k);
-      }
-      Bs[k][j] = v;
+    for (int e = threadIdx.x; e < GT_N * KH; e += NT) {
+      const int j = e / KH, k = 2 * (e - j * KH);
+      const int src = s_src[j];
+      double2 v = c2(0.0);
+      if (src >= 0 && kc + k < R)
+        v = __ldg(ein + ((size_t)src * nrhs + (c0 + j) % nrhs) * ncf + ((kc + k) >> 1));
+      Bs[k][j] = v.x;
+      Bs[k + 1][j] = v.y;
     }
     __syncthreads();
 #pragma unroll
