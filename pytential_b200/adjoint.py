@@ -1,4 +1,5 @@
-"""Adjoint of the 3D Laplace single-layer apply, behind ``torch.autograd.Function``.
+"""Adjoint of the Laplace single-layer apply (3D; in 2D the density gradient), behind
+``torch.autograd.Function``.
 
 Forward: ``u = A sigma`` with ``A = K W U`` (``U``: stage-1 -> quad-stage-2
 upsampling, ``W``: area element x quadrature weight, ``K``: the QBX-FMM kernel
@@ -19,6 +20,7 @@ Backward:
   the target-specific near field differentiated with the center held fixed
   (``qbxfmm_eval_qbx_target_gradients``); or, at targets away from the surface, the
   kernel summed directly over the quad nodes (``qbxfmm_laplace3d_grad_direct``).
+  Target gradients are built for 3D; a 2D operator gives the density gradient only.
 
 :class:`SingleLayer` takes any targets; :class:`FarFieldSingleLayer` is the operator
 at targets away from the surface, also in the mixed form (FP32 far field), whose
@@ -67,12 +69,15 @@ class _Operator:
         return self.targets.shape[1]
 
     def _setup_common(self, discr, targets, device):
-        if discr.ambient_dim != 3:
-            raise NotImplementedError("the adjoint is built for 3D Laplace")
+        if discr.ambient_dim not in (2, 3):
+            raise NotImplementedError("the adjoint is built for 2D and 3D Laplace")
+        self.dim = discr.ambient_dim
         self.discr = discr
         self.targets = np.ascontiguousarray(targets, dtype=np.float64)
+        if self.targets.shape[0] != self.dim:
+            raise ValueError(f"targets must have shape ({self.dim}, ntargets)")
         self.device = torch.device(device)
-        self.spec = SourceKernelSpec(LaplaceKernel(3), charge_coeff=1.0)
+        self.spec = SourceKernelSpec(LaplaceKernel(self.dim), charge_coeff=1.0)
         self.U = torch.from_numpy(np.ascontiguousarray(discr.upsample)).to(self.device)
         self.w = torch.from_numpy(discr.quad_weights).to(self.device)
         self.quad_nodes = torch.from_numpy(np.ascontiguousarray(discr.quad_nodes)).to(self.device)
@@ -84,9 +89,14 @@ class _Operator:
         self._applied = (sigma.data_ptr(), sigma._version, sigma.numel())
         return out
 
+    def _need_3d(self):
+        if self.dim != 3:
+            raise NotImplementedError("target gradients are built for 3D Laplace")
+
     def _grad_fmm(self, sigma):
         """grad u at the targets from the apply's own FMM data, (3, ntargets): the
         workspace of the last apply when it was this density, else a new apply."""
+        self._need_3d()
         if getattr(self, "_applied", None) != (sigma.data_ptr(), sigma._version, sigma.numel()):
             self.apply(sigma)
         return self.fwd.target_gradients()[0]
@@ -98,6 +108,7 @@ class _Operator:
         return s.reshape(-1) * self.w
 
     def _grad_direct(self, sigma, fp64=True):
+        self._need_3d()
         q = self.strengths(sigma).contiguous()
         grad = torch.empty(3, self.ntargets, dtype=torch.float64, device=self.device)
         st = ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
@@ -218,9 +229,9 @@ def single_layer(op: SingleLayer | FarFieldSingleLayer, sigma: torch.Tensor,
                  targets: torch.Tensor | None = None) -> torch.Tensor:
     """Differentiable ``S sigma`` at ``op``'s targets.  Pass ``targets`` (a (3, nt)
     tensor holding ``op.targets``) to get gradients with respect to the target
-    positions."""
+    positions (3D)."""
     if targets is None:
         targets = torch.zeros(0, dtype=torch.float64, device=sigma.device)
-    elif targets.shape != (3, op.ntargets):
-        raise ValueError("targets must have shape (3, ntargets)")
+    elif targets.shape != (op.dim, op.ntargets):
+        raise ValueError(f"targets must have shape ({op.dim}, ntargets)")
     return _SingleLayer.apply(sigma, targets, op)

@@ -1,7 +1,8 @@
-"""Adjoint of the 3D Laplace single layer at far targets (torch.autograd.Function):
-the exchanged-roles FMM against the transpose of a dense kernel matrix (the analogue
-of build_matrix at 320 triangles), and central finite differences for the gradients
-with respect to the density and the target positions (tolerance 1e-6)."""
+"""Adjoint of the Laplace single layer (torch.autograd.Function).  3D: the adjoint
+against the transpose of a dense kernel matrix (the analogue of build_matrix at 320
+triangles), and central finite differences for the gradients with respect to the
+density and the target positions (tolerance 1e-6), at far, near and on-surface
+targets.  2D: the density gradient on and away from the curve."""
 
 import numpy as np
 import pytest
@@ -273,6 +274,51 @@ def test_fmm_target_gradient_mixed(small):
     sig = torch.from_numpy(w.sigma).cuda()
     assert 0 < relerr(opm.target_gradient(sig).cpu().numpy(),
                       op.target_gradient(sig).cpu().numpy()) < 1e-5
+
+
+def test_adjoint_2d_single_layer():
+    """The 2D single layer on the starfish (q 4 / p 10, the 2D Laplace benchmark's
+    operator) on the curve (QBX targets) and at far points: autograd's density
+    gradient is the transpose, which satisfies the dot-product identity with the
+    apply (1e-12) and matches central differences (8 directions, h = 1e-6); target
+    gradients are refused in 2D."""
+    from pytential_b200.adjoint import FarFieldSingleLayer, SingleLayer, single_layer
+    from pytential_b200.discretization import make_starfish
+    d = make_starfish(32)
+    rng = np.random.default_rng(21)
+    ang = rng.uniform(0, 2 * np.pi, 50)
+    far = np.array([3 * np.cos(ang), 3 * np.sin(ang)])
+    for op in (SingleLayer(d, d.nodes, 4, 10, qbx_side=+1), FarFieldSingleLayer(d, far, 4, 10)):
+        sig_np = rng.normal(size=op.ndofs)
+        g_np = rng.normal(size=op.ntargets)
+        g = torch.from_numpy(g_np).cuda()
+        sigma = torch.from_numpy(sig_np).cuda().requires_grad_(True)
+        u = single_layer(op, sigma)
+        J = 0.5 * ((u - g) ** 2).sum()
+        J.backward()
+        r = (u - g).detach()
+        ATr = op.adjoint(r)
+        assert relerr(sigma.grad.cpu().numpy(), ATr.cpu().numpy()) < 1e-14
+        s2 = torch.from_numpy(rng.normal(size=op.ndofs)).cuda()
+        As = op.apply(s2)
+        lhs, rhs = float((As * r).sum()), float((s2 * ATr).sum())
+        assert abs(lhs - rhs) <= 1e-12 * float(torch.linalg.norm(As) * torch.linalg.norm(r))
+        gs = sigma.grad.cpu().numpy()
+
+        def J_sigma(s):
+            uu = op.apply(torch.from_numpy(s).cuda()).cpu().numpy()
+            return 0.5 * ((uu - g_np) ** 2).sum()
+
+        h = 1e-6
+        for _ in range(8):
+            v = rng.normal(size=op.ndofs)
+            fd = (J_sigma(sig_np + h * v) - J_sigma(sig_np - h * v)) / (2 * h)
+            assert abs(fd - gs @ v) <= 1e-6 * abs(gs @ v) + 1e-10
+        with pytest.raises(NotImplementedError):
+            op.target_gradient(sigma.detach())
+        with pytest.raises(ValueError):
+            single_layer(op, sigma, torch.zeros(3, op.ntargets, dtype=torch.float64,
+                                                device="cuda"))
 
 
 def test_fmm_target_gradient_refuses_the_double_layer():
