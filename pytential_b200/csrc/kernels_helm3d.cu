@@ -2177,16 +2177,20 @@ QBX_D bool mbar_wait(uint64_t* mb, unsigned parity)
 // and again before the back rotation, because it shares one buffer with the coaxial
 // table) and the coaxial table of pair q + 1 while pair q's back rotation runs.  One
 // thread issues the copies; waits are bounded: a copy that does not arrive sets the
-// error word, the CTA waits (bounded) for the copies it issued and stops.
-template <int RB, int NTHR = H3M2L_NT>
+// error word, the CTA waits (bounded) for the copies it issued and stops.  With ND = 2
+// the rotation table has two buffers: pair q + 1's is requested as soon as pair q's
+// has arrived (into the buffer pair q - 1 used), so its copy runs under all of pair
+// q's work instead of between the pairs.
+template <int RB, int NTHR = H3M2L_NT, int ND = 1>
 __global__ void __launch_bounds__(NTHR, NTHR == H3M2L_NT ? 2 : 1)
 k_h3_m2l_bulk(qbxfmm_geometry g, int pf, int nrhs, const double2* __restrict__ mp,
               double2* __restrict__ lo, const double* __restrict__ Dtab,
               const double2* __restrict__ Ctab, const double* __restrict__ clsmap,
               int32_t* err)
 {
+  static_assert(ND == 1 || ND == 2, "one or two rotation-table buffers");
   extern __shared__ double2 smem2[];
-  __shared__ uint64_t mbD, mbC;
+  __shared__ uint64_t mbD[ND], mbC;
   __shared__ int s_gn[H3M2L_NG], s_gm0[H3M2L_NG];
   __shared__ int s_cmu[H3M2L_NCG], s_cnu0[H3M2L_NCG];
   __shared__ int s_ng, s_ncg;
@@ -2196,8 +2200,8 @@ k_h3_m2l_bulk(qbxfmm_geometry g, int pf, int nrhs, const double2* __restrict__ m
   const size_t dsz = h3_m2l_dsize(pf), csz = h3_m2l_csize(pf);
   double2* X = smem2;                                              // [RB][ncf + 1]
   double2* A = X + (size_t)RB * XS;                                // [RB][ncf + 1]
-  double* Db = reinterpret_cast<double*>(A + (size_t)RB * XS);     // [dsz]
-  double2* Cb = reinterpret_cast<double2*>(Db + dsz);              // [csz]
+  double* Db0 = reinterpret_cast<double*>(A + (size_t)RB * XS);    // [ND][dsz]
+  double2* Cb = reinterpret_cast<double2*>(Db0 + ND * dsz);         // [csz]
   if (threadIdx.x == 0) {
     int ng = 0;
     for (int n = 0; n <= pf; ++n)
@@ -2215,7 +2219,7 @@ k_h3_m2l_bulk(qbxfmm_geometry g, int pf, int nrhs, const double2* __restrict__ m
         ++ncg;
       }
     s_ncg = ncg;
-    mbar_init(&mbD);
+    for (int b = 0; b < ND; ++b) mbar_init(&mbD[b]);
     mbar_init(&mbC);
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
@@ -2240,14 +2244,16 @@ k_h3_m2l_bulk(qbxfmm_geometry g, int pf, int nrhs, const double2* __restrict__ m
   };
   // copies issued / completed-and-waited per barrier (the phase parity of the next
   // wait is the completed count's)
-  int nd_issued = 0, nd_done = 0, nc_issued = 0, nc_done = 0;
-  auto issue_D = [&](int q) {
+  int nd_issued[ND], nd_done[ND], nc_issued = 0, nc_done = 0;
+#pragma unroll
+  for (int b = 0; b < ND; ++b) nd_issued[b] = nd_done[b] = 0;
+  auto issue_D = [&](int q, int b) {
     if (threadIdx.x == 0) {
       const int c = cls_of(q);
-      mbar_expect(&mbD, dbytes);
-      bulk_copy(Db, Dtab + (size_t)clsmap[2 * c] * dsz, dbytes, &mbD);
+      mbar_expect(&mbD[b], dbytes);
+      bulk_copy(Db0 + b * dsz, Dtab + (size_t)clsmap[2 * c] * dsz, dbytes, &mbD[b]);
     }
-    ++nd_issued;
+    ++nd_issued[b];
   };
   auto issue_C = [&](int q) {
     if (threadIdx.x == 0) {
@@ -2257,9 +2263,9 @@ k_h3_m2l_bulk(qbxfmm_geometry g, int pf, int nrhs, const double2* __restrict__ m
     }
     ++nc_issued;
   };
-  auto wait_D = [&]() {
-    if (!mbar_wait(&mbD, nd_done & 1)) return 1;
-    ++nd_done;
+  auto wait_D = [&](int b) {
+    if (!mbar_wait(&mbD[b], nd_done[b] & 1)) return 1;
+    ++nd_done[b];
     return 0;
   };
   auto wait_C = [&]() {
@@ -2271,7 +2277,9 @@ k_h3_m2l_bulk(qbxfmm_geometry g, int pf, int nrhs, const double2* __restrict__ m
   // still in flight so that none outlives the CTA
   auto drain = [&]() {
     if (threadIdx.x == 0) report(err, QBX_DEVERR_COPY_TIMEOUT);
-    for (; nd_done < nd_issued; ++nd_done) mbar_wait(&mbD, nd_done & 1);
+#pragma unroll
+    for (int b = 0; b < ND; ++b)
+      for (; nd_done[b] < nd_issued[b]; ++nd_done[b]) mbar_wait(&mbD[b], nd_done[b] & 1);
     for (; nc_done < nc_issued; ++nc_done) mbar_wait(&mbC, nc_done & 1);
   };
 
@@ -2281,13 +2289,17 @@ k_h3_m2l_bulk(qbxfmm_geometry g, int pf, int nrhs, const double2* __restrict__ m
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc[k][j] = c2(0.0);
 
-  issue_D(q0);
+  issue_D(q0, 0);
   issue_C(q0);
   for (int q = q0; q < q1; ++q) {
+    const int buf = ND == 2 ? ((q - q0) & 1) : 0;
+    const double* Db = Db0 + buf * dsz;
     const int src = g.m2l_pair_src[g.m2l_tgt_pairs[q]];
     const bool bad = (unsigned)src >= (unsigned)g.nboxes;
     if (bad && threadIdx.x == 0) report(err, QBX_DEVERR_BAD_BOX);
-    int fail = wait_D();
+    int fail = wait_D(buf);
+    // the other buffer was last read by pair q - 1, before the barrier that ended it
+    if (ND == 2 && q + 1 < q1) issue_D(q + 1, buf ^ 1);
     const double2* ph = reinterpret_cast<const double2*>(Db);
     const double* blocks = Db + 2 * nm;
     // X = e^{i m alpha} M
@@ -2384,7 +2396,7 @@ k_h3_m2l_bulk(qbxfmm_geometry g, int pf, int nrhs, const double2* __restrict__ m
     }
     __syncthreads();
     // the rotation buffer is free
-    if (q + 1 < q1) issue_D(q + 1);
+    if (ND == 1 && q + 1 < q1) issue_D(q + 1, 0);
   }
   const int tb = g.target_or_target_parent_boxes[i];
   if ((unsigned)tb >= (unsigned)g.nboxes) {
@@ -2408,7 +2420,19 @@ k_h3_m2l_bulk(qbxfmm_geometry g, int pf, int nrhs, const double2* __restrict__ m
 
 // }}}
 
-template <int RB, int NTHR = H3M2L_NT>
+// dynamic shared memory of k_h3_m2l_bulk: the X and A blocks, nd rotation tables,
+// the coaxial table
+static size_t h3_m2l_bulk_smem(int rb, int pf, int nd)
+{
+  return 2 * (size_t)rb * ((pf + 1) * (pf + 1) + 1) * sizeof(double2) +
+         nd * h3_m2l_dsize(pf) * sizeof(double) + h3_m2l_csize(pf) * sizeof(double2);
+}
+
+// dynamic shared memory a CTA may use beside the kernels' static arrays (227 KB less
+// a margin for them)
+constexpr size_t H3M2L_SMEM_MAX = 227 * 1024 - 4 * 1024;
+
+template <int RB, int NTHR = H3M2L_NT, int ND = 1>
 static cudaError_t h3_m2l_bulk_launch(const qbxfmm_geometry& g, int pf, int nrhs, const double2* mp,
                                       double2* lo, const double* Dtab, const double2* Ctab,
                                       const double* clsmap, int32_t* err, cudaStream_t st)
@@ -2416,12 +2440,27 @@ static cudaError_t h3_m2l_bulk_launch(const qbxfmm_geometry& g, int pf, int nrhs
   // bulk copies need 16-byte aligned tables
   if ((reinterpret_cast<uintptr_t>(Dtab) | reinterpret_cast<uintptr_t>(Ctab)) & 15)
     return cudaErrorInvalidValue;
-  size_t sh = 2 * (size_t)RB * ((pf + 1) * (pf + 1) + 1) * sizeof(double2) +
-              h3_m2l_dsize(pf) * sizeof(double) + h3_m2l_csize(pf) * sizeof(double2);
-  cudaFuncSetAttribute(k_h3_m2l_bulk<RB, NTHR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+  const size_t sh = h3_m2l_bulk_smem(RB, pf, ND);
+  if (sh > H3M2L_SMEM_MAX) return cudaErrorInvalidValue;
+  cudaError_t e = cudaFuncSetAttribute(k_h3_m2l_bulk<RB, NTHR, ND>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+  if (e != cudaSuccess) return e;
   dim3 grid(g.nttp_boxes, (nrhs + RB - 1) / RB);
-  k_h3_m2l_bulk<RB, NTHR><<<grid, NTHR, sh, st>>>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err);
+  k_h3_m2l_bulk<RB, NTHR, ND><<<grid, NTHR, sh, st>>>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err);
   return cudaGetLastError();
+}
+
+// 16 densities per CTA (512 threads, one CTA per SM): two rotation-table buffers where
+// they fit, else one, else 8 densities per CTA
+static cudaError_t h3_m2l_bulk16(const qbxfmm_geometry& g, int pf, int nrhs, const double2* mp,
+                                 double2* lo, const double* Dtab, const double2* Ctab,
+                                 const double* clsmap, int32_t* err, cudaStream_t st)
+{
+  if (h3_m2l_bulk_smem(16, pf, 2) <= H3M2L_SMEM_MAX)
+    return h3_m2l_bulk_launch<16, 2 * H3M2L_NT, 2>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err, st);
+  if (h3_m2l_bulk_smem(16, pf, 1) <= H3M2L_SMEM_MAX)
+    return h3_m2l_bulk_launch<16, 2 * H3M2L_NT, 1>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err, st);
+  return h3_m2l_bulk_launch<8>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err, st);
 }
 
 template <typename R, int RB>
@@ -2457,7 +2496,7 @@ cudaError_t h3_launch_m2l_rot(const qbxfmm_geometry& g, int pf, int nrhs, const 
                   : h3_m2l_bulk_launch<8>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err, st);
     case 16:
       if (fp32) return h3_m2l_rot_launch<float, 16>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err, st);
-      return h3_m2l_bulk_launch<16, 2 * H3M2L_NT>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err, st);
+      return h3_m2l_bulk16(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err, st);
     default: break;
   }
   if (fp32) {   // mixed form: FP32 arithmetic, all 16 densities of a pair's tables at once
@@ -2467,8 +2506,7 @@ cudaError_t h3_launch_m2l_rot(const qbxfmm_geometry& g, int pf, int nrhs, const 
   }
   // 16 densities per CTA (512 threads) when there are as many: at the 3D Helmholtz
   // benchmark size the autotuner measured 158 ms against 162 ms for 8
-  if (nrhs >= 16)
-    return h3_m2l_bulk_launch<16, 2 * H3M2L_NT>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err, st);
+  if (nrhs >= 16) return h3_m2l_bulk16(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err, st);
   if (nrhs >= 8) return h3_m2l_bulk_launch<8>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err, st);
   if (nrhs >= 2) return h3_m2l_rot_launch<double, 4>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err, st);
   return h3_m2l_rot_launch<double, 1>(g, pf, nrhs, mp, lo, Dtab, Ctab, clsmap, err, st);

@@ -51,6 +51,10 @@ def workload(name: str):
         # (q = 5, p = 15, k = 10, 16 densities) on a small surface
         return helmholtz3d_ellipsoid(nrefine=1, k=10.0, nrhs=16, op="CF", qbx_order=5,
                                      fmm_order=15, nshell=100)
+    if name == "h3d-CF-p17":
+        # the largest 3D Helmholtz FMM order with 16 densities per M2L CTA
+        return helmholtz3d_ellipsoid(nrefine=1, k=10.0, nrhs=16, op="CF", qbx_order=5,
+                                     fmm_order=17, nshell=100)
     if name == "h3d-D-small":
         return helmholtz3d_ellipsoid(nrefine=1, k=4.0, nrhs=3, op="D", qbx_order=2,
                                      fmm_order=8, nshell=100)

@@ -153,6 +153,20 @@ def test_drive_fmm_and_apply_match_checker(name):
     ap.check_error_word()
 
 
+def test_helmholtz3d_largest_fmm_order_with_16_densities():
+    """fmm_order 17 (the largest) with 16 densities: the 16-density M2L's shared
+    memory at this order decides its form (two, one or no spare rotation buffers, else
+    8 densities per CTA); the apply matches the checker."""
+    name = "h3d-CF-p17"
+    wl, w, o = wrangler_for(name)
+    ref = o.apply(wl.tree_strengths())
+    ap = QBXApply(wl.geometry(), wl.spec, wl.qbx_order, wl.fmm_order, nrhs=wl.nrhs,
+                  device_geometry=w.dgeo, target_specific_qbx=False)
+    got = host(ap(dev(wl.density)))
+    ap.check_error_word()
+    assert relerr(got, ref) < tol_for(wl)
+
+
 @pytest.mark.parametrize("name", ALL)
 def test_target_specific_mode_matches_checker(name):
     """With target-specific QBX the list-1 near field is evaluated per target; the
