@@ -132,13 +132,13 @@ int qbxfmm_eval_qbx_expansions(const qbxfmm_plan* plan, const void* qbx_exps, vo
 int qbxfmm_eval_target_specific_qbx_locals(const qbxfmm_plan* plan, const void* strengths,
                                            void* pot_tree, int32_t* error_word, void* stream);
 
-/* Gradient of the 3D Laplace single-layer potential at the non-QBX targets from the
+/* Gradient of the Laplace single-layer potential (2D or 3D) at the non-QBX targets from the
  * FMM's own data of an apply (strengths in tree order, multipoles after
  * coarsen_multipoles, locals after refine_locals -- the workspace of qbxfmm_apply
  * holds them after the call): P2P over list 1, M2P over list 3, L2P of the target
  * box's local, each differentiated at the target (the derivative of the apply's
  * value with the tree held fixed), kernel scaling included.  The reference obtains
- * it from derivative target kernels in its FMM.  grad: [nrhs][3][nfiltered_targets]
+ * it from derivative target kernels in its FMM.  grad: [nrhs][dim][nfiltered_targets]
  * (written).  QBXFMM_ERR_UNSUPPORTED for other kernels and per-level orders. */
 int qbxfmm_eval_target_gradients(const qbxfmm_plan* plan, const void* strengths,
                                  const void* mpoles, const void* locals, void* grad,
@@ -147,8 +147,9 @@ int qbxfmm_eval_target_gradients(const qbxfmm_plan* plan, const void* strengths,
 /* The same at the QBX targets: the gradient of each target's center's QBX local at
  * the target (center held fixed) from the apply's qbx_exps (after
  * translate_box_local_to_qbx_local), plus, for a plan with the target-specific near
- * field, the target-derivative of the list-1 Legendre sums from the strengths.
- * grad: [nrhs][3][ntargets] in tree target order (written; zero at other targets). */
+ * field, the target-derivative of the list-1 sums (Legendre in 3D, powers of a/b in 2D)
+ * from the strengths.  grad: [nrhs][dim][ntargets] in tree target order (written; zero
+ * at other targets). */
 int qbxfmm_eval_qbx_target_gradients(const qbxfmm_plan* plan, const void* strengths,
                                      const void* qbx_exps, void* grad, int32_t* error_word,
                                      void* stream);

@@ -1,4 +1,4 @@
-"""Adjoint of the Laplace single-layer apply (3D; in 2D the density gradient), behind
+"""Adjoint of the Laplace single-layer apply (2D and 3D), behind
 ``torch.autograd.Function``.
 
 Forward: ``u = A sigma`` with ``A = K W U`` (``U``: stage-1 -> quad-stage-2
@@ -19,8 +19,7 @@ Backward:
   (``qbxfmm_eval_target_gradients``), at the QBX targets the center's QBX local and
   the target-specific near field differentiated with the center held fixed
   (``qbxfmm_eval_qbx_target_gradients``); or, at targets away from the surface, the
-  kernel summed directly over the quad nodes (``qbxfmm_laplace3d_grad_direct``).
-  Target gradients are built for 3D; a 2D operator gives the density gradient only.
+  kernel summed directly over the quad nodes (``qbxfmm_laplace3d_grad_direct``, 3D).
 
 :class:`SingleLayer` takes any targets; :class:`FarFieldSingleLayer` is the operator
 at targets away from the surface, also in the mixed form (FP32 far field), whose
@@ -89,14 +88,9 @@ class _Operator:
         self._applied = (sigma.data_ptr(), sigma._version, sigma.numel())
         return out
 
-    def _need_3d(self):
-        if self.dim != 3:
-            raise NotImplementedError("target gradients are built for 3D Laplace")
-
     def _grad_fmm(self, sigma):
-        """grad u at the targets from the apply's own FMM data, (3, ntargets): the
+        """grad u at the targets from the apply's own FMM data, (dim, ntargets): the
         workspace of the last apply when it was this density, else a new apply."""
-        self._need_3d()
         if getattr(self, "_applied", None) != (sigma.data_ptr(), sigma._version, sigma.numel()):
             self.apply(sigma)
         return self.fwd.target_gradients()[0]
@@ -108,7 +102,8 @@ class _Operator:
         return s.reshape(-1) * self.w
 
     def _grad_direct(self, sigma, fp64=True):
-        self._need_3d()
+        if self.dim != 3:
+            raise NotImplementedError("the direct-sum target gradient is built for 3D")
         q = self.strengths(sigma).contiguous()
         grad = torch.empty(3, self.ntargets, dtype=torch.float64, device=self.device)
         st = ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
@@ -140,12 +135,12 @@ class SingleLayer(_Operator):
         return self.transpose(r.reshape(1, -1).contiguous())[0]
 
     def target_gradient(self, sigma: torch.Tensor, form: str = "fmm") -> torch.Tensor:
-        """grad u at the targets, (3, ntargets).  ``form``: "fmm" -- the derivative of
+        """grad u at the targets, (dim, ntargets).  ``form``: "fmm" -- the derivative of
         the apply's own value: P2P, M2P and L2P differentiated at the non-QBX targets,
         at the QBX targets the center's QBX local (and the target-specific near field)
         with the center held fixed (the target-to-center association is piecewise
         constant); "direct" -- the kernel summed over all quad nodes, for targets away
-        from the surface only."""
+        from the surface only (3D)."""
         if form == "fmm":
             return self._grad_fmm(sigma)
         if self.targets_need_qbx:
@@ -200,10 +195,10 @@ class FarFieldSingleLayer(_Operator):
         return (v @ self.U).reshape(-1)
 
     def target_gradient(self, sigma: torch.Tensor, form: str = "fmm") -> torch.Tensor:
-        """grad u at the targets, (3, ntargets).  ``form``: "fmm" -- the derivative of
+        """grad u at the targets, (dim, ntargets).  ``form``: "fmm" -- the derivative of
         the apply's own value (P2P, M2P and L2P differentiated at the target,
         ``qbxfmm_eval_target_gradients``, from the apply's expansions); "direct" -- the
-        kernel summed over all quad nodes (FP32 arithmetic for the mixed operator)."""
+        kernel summed over all quad nodes (3D; FP32 arithmetic for the mixed operator)."""
         if form == "fmm":
             return self._grad_fmm(sigma)
         return self._grad_direct(sigma, fp64=self.precision == PRECISION_FP64)
@@ -227,9 +222,9 @@ class _SingleLayer(torch.autograd.Function):
 
 def single_layer(op: SingleLayer | FarFieldSingleLayer, sigma: torch.Tensor,
                  targets: torch.Tensor | None = None) -> torch.Tensor:
-    """Differentiable ``S sigma`` at ``op``'s targets.  Pass ``targets`` (a (3, nt)
+    """Differentiable ``S sigma`` at ``op``'s targets.  Pass ``targets`` (a (dim, nt)
     tensor holding ``op.targets``) to get gradients with respect to the target
-    positions (3D)."""
+    positions."""
     if targets is None:
         targets = torch.zeros(0, dtype=torch.float64, device=sigma.device)
     elif targets.shape != (op.dim, op.ntargets):

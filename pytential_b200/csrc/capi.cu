@@ -1337,17 +1337,24 @@ int qbxfmm_eval_target_gradients(const qbxfmm_plan* p, const void* strengths, co
                                   const void* locals, void* grad, int32_t* err, void* stream)
 {
   if (int rc = check_plan(p)) return rc;
-  if (p->helm || p->kern.dim != 3 || p->sc.cd != 0.0)
-    return fail(QBXFMM_ERR_UNSUPPORTED, "target gradients cover the 3D Laplace single layer");
+  if (p->helm || p->sc.cd != 0.0)
+    return fail(QBXFMM_ERR_UNSUPPORTED, "target gradients cover the Laplace single layer");
   if (level_orders_on(p))
     return fail(QBXFMM_ERR_UNSUPPORTED, "target gradients take one FMM order");
   if (!strengths || !mpoles || !locals || !grad) return fail(QBXFMM_ERR_ARG, "null argument");
-  size_t bytes = (size_t)p->kern.nrhs * 3 * p->geo.nfiltered_targets * sizeof(double);
+  const int dim = p->kern.dim;
+  size_t bytes = (size_t)p->kern.nrhs * dim * p->geo.nfiltered_targets * sizeof(double);
   if (bytes) QBX_TRY(cudaMemsetAsync(grad, 0, bytes, S(stream)), "eval_target_gradients: clear");
-  QBX_TRY(launch_grad_targets(p->geo, p->sc.cq, 0.25 / M_PI, p->kern.fmm_order, p->kern.nrhs,
-                              (const double*)strengths, (const double2*)mpoles,
-                              (const double2*)locals, (double*)grad, err, S(stream)),
-          "eval_target_gradients");
+  if (dim == 2)
+    QBX_TRY(launch_grad2_targets(p->geo, p->sc.cq, -0.5 / M_PI, p->kern.fmm_order, p->kern.nrhs,
+                                 (const double*)strengths, (const double2*)mpoles,
+                                 (const double2*)locals, (double*)grad, err, S(stream)),
+            "eval_target_gradients");
+  else
+    QBX_TRY(launch_grad_targets(p->geo, p->sc.cq, 0.25 / M_PI, p->kern.fmm_order, p->kern.nrhs,
+                                (const double*)strengths, (const double2*)mpoles,
+                                (const double2*)locals, (double*)grad, err, S(stream)),
+            "eval_target_gradients");
   return QBXFMM_OK;
 }
 
@@ -1356,16 +1363,25 @@ int qbxfmm_eval_qbx_target_gradients(const qbxfmm_plan* p, const void* strengths
                                       void* stream)
 {
   if (int rc = check_plan(p)) return rc;
-  if (p->helm || p->kern.dim != 3 || p->sc.cd != 0.0)
-    return fail(QBXFMM_ERR_UNSUPPORTED, "target gradients cover the 3D Laplace single layer");
+  if (p->helm || p->sc.cd != 0.0)
+    return fail(QBXFMM_ERR_UNSUPPORTED, "target gradients cover the Laplace single layer");
   if (p->kern.qbx_order > 8) return fail(QBXFMM_ERR_UNSUPPORTED, "qbx_order > 8");
   if (!strengths || !qbx_exps || !grad) return fail(QBXFMM_ERR_ARG, "null argument");
-  size_t bytes = (size_t)p->kern.nrhs * 3 * p->geo.ntargets * sizeof(double);
+  const int dim = p->kern.dim;
+  size_t bytes = (size_t)p->kern.nrhs * dim * p->geo.ntargets * sizeof(double);
   if (bytes) QBX_TRY(cudaMemsetAsync(grad, 0, bytes, S(stream)), "eval_qbx_target_gradients: clear");
-  QBX_TRY(launch_grad_qbx_targets(p->geo, p->sc.cq, 0.25 / M_PI, p->kern.qbx_order, p->kern.nrhs,
-                                  p->kern.target_specific_qbx != 0, (const double*)strengths,
-                                  (const double2*)qbx_exps, (double*)grad, err, S(stream)),
-          "eval_qbx_target_gradients");
+  if (dim == 2)
+    QBX_TRY(launch_grad2_qbx_targets(p->geo, p->sc.cq, -0.5 / M_PI, p->kern.qbx_order,
+                                     p->kern.nrhs, p->kern.target_specific_qbx != 0,
+                                     (const double*)strengths, (const double2*)qbx_exps,
+                                     (double*)grad, err, S(stream)),
+            "eval_qbx_target_gradients");
+  else
+    QBX_TRY(launch_grad_qbx_targets(p->geo, p->sc.cq, 0.25 / M_PI, p->kern.qbx_order,
+                                    p->kern.nrhs, p->kern.target_specific_qbx != 0,
+                                    (const double*)strengths, (const double2*)qbx_exps,
+                                    (double*)grad, err, S(stream)),
+            "eval_qbx_target_gradients");
   return QBXFMM_OK;
 }
 

@@ -227,6 +227,15 @@ cudaError_t launch_tr_combine(const qbxfmm_geometry& g, int nrhs, double scale, 
                               cudaStream_t st);
 
 // gradient of the 3D Laplace single layer at the non-QBX targets (kernels_fmmgrad.cu)
+// 2D Laplace single layer: grad[r][2][n]
+cudaError_t launch_grad2_targets(const qbxfmm_geometry& g, double cq, double scale, int p,
+                                 int nrhs, const double* strengths, const double2* mpoles,
+                                 const double2* locals, double* grad, int32_t* err,
+                                 cudaStream_t st);
+cudaError_t launch_grad2_qbx_targets(const qbxfmm_geometry& g, double cq, double scale, int q,
+                                     int nrhs, bool target_specific, const double* strengths,
+                                     const double2* qbx_exps, double* grad, int32_t* err,
+                                     cudaStream_t st);
 cudaError_t launch_grad_targets(const qbxfmm_geometry& g, double cq, double scale, int p,
                                 int nrhs, const double* strengths, const double2* mpoles,
                                 const double2* locals, double* grad, int32_t* err,

@@ -1,7 +1,8 @@
-// Gradient of the 3D Laplace single-layer potential at the non-QBX targets from the
-// FMM's own data: the list-1 sources (P2P), the list-3 multipoles (M2P) and the target
-// box's local (L2P) -- the derivative of the apply's value at each target with the
-// tree held fixed, for the target-position gradient of the adjoint.
+// Gradient of the Laplace single-layer potential (3D; 2D at the end of the file) at the
+// non-QBX targets from the FMM's own data: the list-1 sources (P2P), the list-3
+// multipoles (M2P) and the target box's local (L2P) -- the derivative of the apply's
+// value at each target with the tree held fixed, for the target-position gradient of
+// the adjoint.
 //
 // With u = (x - c) / rho and the solid harmonics of laplace.cuh,
 //   d/du_z R_n^m = R_{n-1}^m,          d/du_x R_n^m = (R_{n-1}^{m-1} - R_{n-1}^{m+1}) / 2,
@@ -439,5 +440,195 @@ cudaError_t launch_grad_targets(const qbxfmm_geometry& g, double cq, double scal
         g, p, ncf, nrhs, scale, locals, grad);
   return cudaGetLastError();
 }
+
+// {{{ 2D Laplace: grad Re f = (Re f', -Im f') for the complex-analytic f of each term
+//   P2P    log|z - y|:                              f' = 1 / (z - y)
+//   M2P    M_0 log(z - c) + sum_k M_k u^-k:          f' = (M_0 / u - sum_k k M_k u^(-k-1)) / rho
+//   L2P    sum_k L_k u^k:                            f' = sum_k k L_k u^(k-1) / rho
+//   TSQBX  log|b| - Re sum_{n<=Q} (a / b)^n / n:    d/da = -sum_n a^(n-1) / b^n
+// (u = (z - c) / rho, a = t - c, b = y - c).  One thread per target; grad[r][2][n].
+
+// non-QBX targets: CTA per target box, thread per target (P2P over list 1, M2P over
+// list 3, L2P of the box's local)
+__global__ void __launch_bounds__(NT)
+k_grad2_targets(qbxfmm_geometry g, double cq, double scale, int p, int nrhs,
+                const double* __restrict__ strengths, const double2* __restrict__ mpoles,
+                const double2* __restrict__ locals, double* __restrict__ grad, int32_t* err)
+{
+  const int itb = blockIdx.x, r = blockIdx.y, ncf = p + 1;
+  const int tb = g.target_boxes[itb];
+  const int t0 = g.nonqbx_box_target_starts[tb];
+  const int nt = g.nonqbx_box_target_counts_nonchild[tb];
+  if (nt == 0) return;
+  const double* st = strengths + (size_t)r * g.nsources;
+  const double2* L = locals + ((size_t)tb * nrhs + r) * ncf;
+  const double rho_b = level_width(g, g.box_levels[tb]);
+  double cb[2];
+  load_point<2>(g.box_centers, g.nboxes, tb, cb);
+  for (int tt = threadIdx.x; tt < nt; tt += NT) {
+    double x[2];
+    load_point<2>(g.nonqbx_targets, g.nfiltered_targets, t0 + tt, x);
+    double gx = 0.0, gy = 0.0;
+    for (int li = g.list1_starts[itb]; li < g.list1_starts[itb + 1]; ++li) {
+      const int sb = g.list1_lists[li];
+      if ((unsigned)sb >= (unsigned)g.nboxes) {
+        report(err, QBX_DEVERR_BAD_BOX);
+        continue;
+      }
+      const int s0 = g.box_source_starts[sb], s1 = s0 + g.box_source_counts_nonchild[sb];
+      for (int j = s0; j < s1; ++j) {
+        double y[2];
+        load_point<2>(g.sources, g.nsources, j, y);
+        const double dx = x[0] - y[0], dy = x[1] - y[1], r2 = dx * dx + dy * dy;
+        if (r2 == 0.0) continue;
+        const double f = cq * st[j] / r2;
+        gx = fma(f, dx, gx);
+        gy = fma(f, dy, gy);
+      }
+    }
+    double2 d = c2(0.0);                   // sum of f'
+    for (int li = g.list3_starts[itb]; li < g.list3_starts[itb + 1]; ++li) {
+      const int sb = g.list3_lists[li];
+      if ((unsigned)sb >= (unsigned)g.nboxes) {
+        report(err, QBX_DEVERR_BAD_BOX);
+        continue;
+      }
+      const double2* M = mpoles + ((size_t)sb * nrhs + r) * ncf;
+      const double rho = level_width(g, g.box_levels[sb]);
+      double cs[2];
+      load_point<2>(g.box_centers, g.nboxes, sb, cs);
+      const double2 uinv = cinv(c2((x[0] - cs[0]) / rho, (x[1] - cs[1]) / rho));
+      double2 e = cmul(M[0], uinv), pw = cmul(uinv, uinv);
+      for (int k = 1; k <= p; ++k) {
+        e = csub(e, cscale((double)k, cmul(M[k], pw)));
+        pw = cmul(pw, uinv);
+      }
+      d = cadd(d, cscale(1.0 / rho, e));
+    }
+    {
+      const double2 u = c2((x[0] - cb[0]) / rho_b, (x[1] - cb[1]) / rho_b);
+      double2 e = c2(0.0), pw = c2(1.0);
+      for (int k = 1; k <= p; ++k) {
+        e = cadd(e, cscale((double)k, cmul(L[k], pw)));
+        pw = cmul(pw, u);
+      }
+      d = cadd(d, cscale(1.0 / rho_b, e));
+    }
+    const size_t o = (size_t)r * 2 * g.nfiltered_targets + t0 + tt;
+    grad[o] += scale * (gx + d.x);
+    grad[o + g.nfiltered_targets] += scale * (gy - d.y);
+  }
+}
+
+// QBX targets: thread per global center, the derivative of its QBX local at each of
+// its targets (center held fixed)
+__global__ void __launch_bounds__(NT)
+k_grad2_qbxl2p(qbxfmm_geometry g, int q, int nrhs, double scale,
+               const double2* __restrict__ qbx_exps, double* __restrict__ grad, int32_t* err)
+{
+  const int ig = blockIdx.x * blockDim.x + threadIdx.x, r = blockIdx.y;
+  if (ig >= g.nglobal_qbx_centers) return;
+  const int ctr = g.global_qbx_centers[ig];
+  if ((unsigned)ctr >= (unsigned)g.ncenters) {
+    report(err, QBX_DEVERR_BAD_CENTER);
+    return;
+  }
+  double cc[2];
+  load_point<2>(g.centers, g.ncenters, ctr, cc);
+  const double rho = g.expansion_radii[ctr];
+  const double2* L = qbx_exps + ((size_t)ctr * nrhs + r) * (q + 1);
+  for (int it = g.center_to_targets_starts[ctr]; it < g.center_to_targets_starts[ctr + 1]; ++it) {
+    const int t = g.center_to_targets_lists[it];
+    if ((unsigned)t >= (unsigned)g.ntargets) {
+      report(err, QBX_DEVERR_BAD_CENTER);
+      continue;
+    }
+    double x[2];
+    load_point<2>(g.targets, g.ntargets, t, x);
+    const double2 u = c2((x[0] - cc[0]) / rho, (x[1] - cc[1]) / rho);
+    double2 e = c2(0.0), pw = c2(1.0);
+    for (int k = 1; k <= q; ++k) {
+      e = cadd(e, cscale((double)k, cmul(L[k], pw)));
+      pw = cmul(pw, u);
+    }
+    const size_t o = (size_t)r * 2 * g.ntargets + t;
+    grad[o] += scale * e.x / rho;
+    grad[o + g.ntargets] -= scale * e.y / rho;
+  }
+}
+
+// the target-specific near field: thread per (target, center) pair of a chunk, over
+// the list-1 sources of the chunk's target box
+__global__ void __launch_bounds__(32)
+k_grad2_tsqbx(qbxfmm_geometry g, double cq, double scale, int q, int nrhs,
+              const double* __restrict__ strengths, double* __restrict__ grad, int32_t* err)
+{
+  const int chunk = blockIdx.x, r = blockIdx.y, lane = threadIdx.x;
+  const int itb = g.tsqbx_chunk_target_box[chunk];
+  if (lane >= g.tsqbx_chunk_count[chunk]) return;
+  const int t = g.tsqbx_targets[g.tsqbx_chunk_start[chunk] + lane];
+  const int ctr = g.tsqbx_centers[g.tsqbx_chunk_start[chunk] + lane];
+  if ((unsigned)ctr >= (unsigned)g.ncenters || (unsigned)t >= (unsigned)g.ntargets) {
+    report(err, QBX_DEVERR_BAD_CENTER);
+    return;
+  }
+  double cc[2], x[2];
+  load_point<2>(g.centers, g.ncenters, ctr, cc);
+  load_point<2>(g.targets, g.ntargets, t, x);
+  const double2 a = c2(x[0] - cc[0], x[1] - cc[1]);
+  const double* st = strengths + (size_t)r * g.nsources;
+  double2 h = c2(0.0);                     // sum_j q_j sum_n a^(n-1) / b_j^n
+  for (int li = g.list1_starts[itb]; li < g.list1_starts[itb + 1]; ++li) {
+    const int sb = g.list1_lists[li];
+    if ((unsigned)sb >= (unsigned)g.nboxes) {
+      report(err, QBX_DEVERR_BAD_BOX);
+      continue;
+    }
+    const int s0 = g.box_source_starts[sb], s1 = s0 + g.box_source_counts_nonchild[sb];
+    for (int j = s0; j < s1; ++j) {
+      double y[2];
+      load_point<2>(g.sources, g.nsources, j, y);
+      const double2 binv = cinv(c2(y[0] - cc[0], y[1] - cc[1]));
+      const double2 w = cmul(a, binv);
+      double2 term = binv, sum = c2(0.0);   // a^(n-1) / b^n from n = 1
+      for (int n = 1; n <= q; ++n) {
+        sum = cadd(sum, term);
+        term = cmul(term, w);
+      }
+      h = cadd(h, cscale(st[j], sum));
+    }
+  }
+  const size_t o = (size_t)r * 2 * g.ntargets + t;
+  grad[o] -= scale * cq * h.x;
+  grad[o + g.ntargets] += scale * cq * h.y;
+}
+
+cudaError_t launch_grad2_targets(const qbxfmm_geometry& g, double cq, double scale, int p,
+                                 int nrhs, const double* strengths, const double2* mpoles,
+                                 const double2* locals, double* grad, int32_t* err,
+                                 cudaStream_t st)
+{
+  if (g.nfiltered_targets == 0 || g.ntarget_boxes == 0) return cudaSuccess;
+  k_grad2_targets<<<dim3(g.ntarget_boxes, nrhs), NT, 0, st>>>(g, cq, scale, p, nrhs, strengths,
+                                                              mpoles, locals, grad, err);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_grad2_qbx_targets(const qbxfmm_geometry& g, double cq, double scale, int q,
+                                     int nrhs, bool target_specific, const double* strengths,
+                                     const double2* qbx_exps, double* grad, int32_t* err,
+                                     cudaStream_t st)
+{
+  if (g.nglobal_qbx_centers == 0) return cudaSuccess;
+  k_grad2_qbxl2p<<<dim3((g.nglobal_qbx_centers + NT - 1) / NT, nrhs), NT, 0, st>>>(
+      g, q, nrhs, scale, qbx_exps, grad, err);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess || !target_specific || g.ntsqbx_chunks == 0) return e;
+  k_grad2_tsqbx<<<dim3(g.ntsqbx_chunks, nrhs), 32, 0, st>>>(g, cq, scale, q, nrhs, strengths,
+                                                            grad, err);
+  return cudaGetLastError();
+}
+
+// }}}
 
 }  // namespace qbx

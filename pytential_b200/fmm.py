@@ -595,7 +595,7 @@ class QBXApply:
 
     def target_gradients(self) -> torch.Tensor:
         """Gradient of the last apply's potential at its user targets,
-        ``(nrhs, 3, nuser_targets)`` (3D Laplace single layer): at the non-QBX targets
+        ``(nrhs, dim, nuser_targets)`` (Laplace single layer): at the non-QBX targets
         from the apply's own strengths, multipoles and locals
         (``qbxfmm_eval_target_gradients``), at the QBX targets the gradient of the
         center's QBX local (with the target-specific near field differentiated too)
@@ -604,7 +604,8 @@ class QBXApply:
         nf, nt, nc = self.dgeo.nfiltered_targets, self.dgeo.ntargets, self.dgeo.ncenters
         err = ctypes.cast(ctypes.c_void_p(_ptr(self.error_word)), ctypes.POINTER(ctypes.c_int32))
         vp = ctypes.c_void_p
-        out = torch.zeros(self.nrhs, 3, self.nuser_targets, dtype=torch.float64,
+        dim = self.plan.spec.kernel.dim
+        out = torch.zeros(self.nrhs, dim, self.nuser_targets, dtype=torch.float64,
                           device=self.device)
         if not hasattr(self, "_grad_maps"):
             t = h["unfiltered_from_filtered_target_indices"][:nf].astype(np.int64)
@@ -615,13 +616,13 @@ class QBXApply:
                                     for a in (fu, tt, sid[tt] - nc))
         fu, tt, tu = self._grad_maps
         if nf:
-            g = torch.empty(self.nrhs, 3, nf, dtype=torch.float64, device=self.device)
+            g = torch.empty(self.nrhs, dim, nf, dtype=torch.float64, device=self.device)
             self.plan.call("qbxfmm_eval_target_gradients", vp(_ptr(self._ws_tensors[0])),
                            vp(_ptr(self._ws_tensors[1])), vp(_ptr(self._ws_tensors[2])),
                            vp(_ptr(g)), err, _stream_handle())
             out[:, :, fu] = g
         if self.dgeo.nglobal_qbx_centers:
-            gq = torch.empty(self.nrhs, 3, nt, dtype=torch.float64, device=self.device)
+            gq = torch.empty(self.nrhs, dim, nt, dtype=torch.float64, device=self.device)
             self.plan.call("qbxfmm_eval_qbx_target_gradients", vp(_ptr(self._ws_tensors[0])),
                            vp(_ptr(self._ws_tensors[3])), vp(_ptr(gq)), err, _stream_handle())
             qbx = torch.ones(nt, dtype=torch.bool, device=self.device)

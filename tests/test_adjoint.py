@@ -280,8 +280,8 @@ def test_adjoint_2d_single_layer():
     """The 2D single layer on the starfish (q 4 / p 10, the 2D Laplace benchmark's
     operator) on the curve (QBX targets) and at far points: autograd's density
     gradient is the transpose, which satisfies the dot-product identity with the
-    apply (1e-12) and matches central differences (8 directions, h = 1e-6); target
-    gradients are refused in 2D."""
+    apply (1e-12) and matches central differences (8 directions, h = 1e-6); the
+    direct-sum target gradient is 3D only."""
     from pytential_b200.adjoint import FarFieldSingleLayer, SingleLayer, single_layer
     from pytential_b200.discretization import make_starfish
     d = make_starfish(32)
@@ -314,11 +314,65 @@ def test_adjoint_2d_single_layer():
             v = rng.normal(size=op.ndofs)
             fd = (J_sigma(sig_np + h * v) - J_sigma(sig_np - h * v)) / (2 * h)
             assert abs(fd - gs @ v) <= 1e-6 * abs(gs @ v) + 1e-10
+        assert tuple(op.target_gradient(sigma.detach()).shape) == (2, op.ntargets)
         with pytest.raises(NotImplementedError):
-            op.target_gradient(sigma.detach())
+            op.target_gradient(sigma.detach(), form="direct")
         with pytest.raises(ValueError):
             single_layer(op, sigma, torch.zeros(3, op.ntargets, dtype=torch.float64,
                                                 device="cuda"))
+
+
+@pytest.mark.parametrize("tsqbx", [False, True])
+def test_fmm_target_gradient_2d_against_checker_differences(tsqbx):
+    """The 2D target gradients (starfish, q 4 / p 10) against central differences of
+    the checker's apply with every target moved and the tree, lists and centers held
+    fixed: far targets, targets near the curve without QBX, and QBX targets."""
+    from oracle.oracle import Oracle
+    from pytential_b200 import abi
+    from pytential_b200.discretization import make_starfish
+    from pytential_b200.fmm import LaplaceKernel, QBXApply, SourceKernelSpec
+    from pytential_b200.geometry import QBXFMMGeometryData
+    d = make_starfish(48)
+    rng = np.random.default_rng(24)
+    ang = rng.uniform(0, 2 * np.pi, 60)
+    far = np.array([3 * np.cos(ang), 3 * np.sin(ang)])
+    i = rng.integers(0, d.ndofs, 40)
+    hs = d.element_stretch[i // d.nodes_per_element] * d.normals[:, i]
+    near = d.nodes[:, i] + 0.05 * hs          # through QBX
+    mid = d.nodes[:, i] + 1.5 * hs            # close to the curve, no QBX
+    geo = QBXFMMGeometryData(d, [(far, 0), (near, 0), (mid, 0)])
+    spec = SourceKernelSpec(LaplaceKernel(2), charge_coeff=1.0)
+    ap = QBXApply(geo, spec, 4, 10, nrhs=2, target_specific_qbx=tsqbx)
+    sig = rng.normal(size=(2, d.ndofs))
+    ap(torch.from_numpy(sig).cuda())
+    g = ap.target_gradients().cpu().numpy()                        # (2, 2, nuser)
+    ap.check_error_word()
+    o = Oracle(geo, dim=2, qbx_order=4, fmm_order=10, nrhs=2, charge_coeff=1.0,
+               family=abi.QBXFMM_LAPLACE)
+    s = np.ascontiguousarray((d.upsample_density(sig) * d.quad_weights)[
+        :, o.arrays["user_source_ids"][:o.scalars["nsources"]]])
+    nf = o.scalars["nfiltered_targets"]
+    X = o.arrays["nonqbx_targets"]
+    T = o.arrays["targets"]
+    h = 1e-5
+    fd = np.zeros_like(g)
+    assert X.shape == (2, nf)
+    for k in range(2):
+        X[k] += h
+        T[k] += h
+        up = o.apply(s)
+        X[k] -= 2 * h
+        T[k] -= 2 * h
+        dn = o.apply(s)
+        X[k] += h
+        T[k] += h
+        fd[:, k, :] = (up - dn) / (2 * h)
+    qbx = np.ones(g.shape[2], bool)
+    sid = o.arrays["sorted_target_ids"]
+    qbx[sid[o.arrays["unfiltered_from_filtered_target_indices"][:nf]] - o.scalars["ncenters"]] = False
+    assert qbx.sum() > 0 and (~qbx).sum() > 60
+    assert relerr(g[:, :, ~qbx], fd[:, :, ~qbx]) < 1e-7
+    assert relerr(g[:, :, qbx], fd[:, :, qbx]) < 1e-7
 
 
 def test_fmm_target_gradient_refuses_the_double_layer():
