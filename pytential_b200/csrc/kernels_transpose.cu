@@ -43,6 +43,11 @@ constexpr int NT = 128;
 constexpr int TR_CL = 8;      // CTAs per row (a cluster) in M2QBXL^T and P2QBXL^T when
                               // the rows alone would not fill the GPU
 constexpr int TR_SPLIT_BELOW = 4 * 148;   // rows below which a row is split
+// M2QBXL^T: threads per CTA and accumulation tasks per thread (2 ncf <= TRM_H TRM_NT:
+// each output coefficient is split over the even and odd centers of a batch; fmm_order
+// <= 21)
+constexpr int TRM_NT = 192;
+constexpr int TRM_H = 3;
 
 QBX_D bool box_ok(const qbxfmm_geometry& g, int b, int32_t* err)
 {
@@ -224,12 +229,11 @@ k_tr_l2qbxl(qbxfmm_geometry g, qbxfmm_transpose_index ix, int p, int q, int ncf,
 // (-1)^j ratio^j / rho_c factors in zero-padded dense shared arrays, so the inner
 // sums are branch-free.
 template <int CL>
-__global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(NT)
+__global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(TRM_NT, 3)
 k_tr_m2qbxl(qbxfmm_geometry g, qbxfmm_transpose_index ix, int p, int q, int ncf, int ncq,
             int nrhs, int mb, const double2* __restrict__ cmp, double2* __restrict__ locals,
             int32_t* err)
 {
-  __shared__ double2 s_out[2 * NT];
   const int row = blockIdx.x / CL, part = blockIdx.x - row * CL;
   extern __shared__ double2 smem2[];
   const int SW = p + 2 * q + 1, SS = (p + q + 1) * SW;   // S: rows 0..p+q, columns -q..p+q
@@ -245,8 +249,10 @@ k_tr_m2qbxl(qbxfmm_geometry g, qbxfmm_transpose_index ix, int p, int q, int ncf,
   double rho_s = level_width(g, g.box_levels[s]);
   double cs[3];
   load_point<3>(g.box_centers, g.nboxes, s, cs);
-  for (int i = threadIdx.x; i < mb * (SS + MS); i += NT) S[i] = c2(0.0);
-  double2 acc[2] = {c2(0.0), c2(0.0)};
+  for (int i = threadIdx.x; i < mb * (SS + MS); i += TRM_NT) S[i] = c2(0.0);
+  double2 acc[TRM_H];
+#pragma unroll
+  for (int h = 0; h < TRM_H; ++h) acc[h] = c2(0.0);
   int item = 0;                            // center batches dealt round-robin to the cluster
   for (int e = ix.list3_rev_starts[row]; e < ix.list3_rev_starts[row + 1]; ++e) {
     int b = ix.list3_rev_lists[e];
@@ -272,7 +278,7 @@ k_tr_m2qbxl(qbxfmm_geometry g, qbxfmm_transpose_index ix, int p, int q, int ncf,
         for (int j = 0; j <= p; ++j, f *= -ratio) fac[threadIdx.x * (p + 1) + j] = f;
       }
       __syncthreads();
-      for (int w = threadIdx.x; w < nb * (p + q + 1); w += NT) {
+      for (int w = threadIdx.x; w < nb * (p + q + 1); w += TRM_NT) {
         int ci = w / (p + q + 1), m = w - ci * (p + q + 1);
         double x = sd[ci * 3], y = sd[ci * 3 + 1], z = sd[ci * 3 + 2];
         double rinv2 = 1.0 / (x * x + y * y + z * z);
@@ -291,7 +297,7 @@ k_tr_m2qbxl(qbxfmm_geometry g, qbxfmm_transpose_index ix, int p, int q, int ncf,
           if (m >= 1 && m <= q) T[n * SW - m] = (m & 1) ? c2(-a.x, a.y) : c2(a.x, -a.y);
         }
       }
-      for (int w = threadIdx.x; w < nb * ncq; w += NT) {
+      for (int w = threadIdx.x; w < nb * ncq; w += TRM_NT) {
         int ci = w / ncq, i = w - ci * ncq;
         int ctr = sctr[ci];
         int kk, l;
@@ -302,14 +308,16 @@ k_tr_m2qbxl(qbxfmm_geometry g, qbxfmm_transpose_index ix, int p, int q, int ncf,
         if (l > 0) M[kk * MW - l] = (l & 1) ? c2(-v.x, v.y) : c2(v.x, -v.y);
       }
       __syncthreads();
+      // task t = (half, o): output coefficient o over the batch's centers of one parity
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        int o = threadIdx.x + h * NT;
-        if (o >= ncf) break;
+      for (int h = 0; h < TRM_H; ++h) {
+        const int t = threadIdx.x + h * TRM_NT;
+        if (t >= 2 * ncf) break;
+        const int half = t >= ncf ? 1 : 0, o = t - half * ncf;
         int j, ii;
         decode3(o, j, ii);
         double2 a = acc[h];
-        for (int ci = 0; ci < nb; ++ci) {
+        for (int ci = half; ci < nb; ci += 2) {
           const double2* M = Mp + (size_t)ci * MS + q;
           const double2* T = S + (size_t)ci * SS + q;
           double2 v = c2(0.0);
@@ -324,19 +332,26 @@ k_tr_m2qbxl(qbxfmm_geometry g, qbxfmm_transpose_index ix, int p, int q, int ncf,
       }
     }
   }
-  // the cluster's partial locals summed by rank 0 in rank order (distributed shared memory)
+  // the two halves of each coefficient, then the cluster's CTAs, summed by rank 0 in a
+  // fixed order (distributed shared memory); the partials [2][ncf] reuse the tables'
+  // space (mb (SS + MS) >= 2 ncf for mb >= 2)
   cg::cluster_group cl = cg::this_cluster();
+  double2* s_part = smem2;
+  __syncthreads();
 #pragma unroll
-  for (int h = 0; h < 2; ++h) s_out[threadIdx.x + h * NT] = acc[h];
+  for (int h = 0; h < TRM_H; ++h) {
+    const int t = threadIdx.x + h * TRM_NT;
+    if (t < 2 * ncf) s_part[t] = acc[h];
+  }
   cl.sync();
   if (part == 0) {
     double2* L = locals + ((size_t)s * nrhs + r) * ncf;
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      int o = threadIdx.x + h * NT;
-      if (o >= ncf) break;
-      double2 v = acc[h];
-      for (int qq = 1; qq < CL; ++qq) v = cadd(v, cl.map_shared_rank(s_out, qq)[o]);
+    for (int o = threadIdx.x; o < ncf; o += TRM_NT) {
+      double2 v = cadd(s_part[o], s_part[o + ncf]);
+      for (int qq = 1; qq < CL; ++qq) {
+        const double2* rp = cl.map_shared_rank(s_part, qq);
+        v = cadd(v, cadd(rp[o], rp[o + ncf]));
+      }
       L[o] = cadd(L[o], v);
     }
   }
@@ -792,20 +807,21 @@ cudaError_t launch_tr_m2qbxl(const qbxfmm_geometry& g, const qbxfmm_transpose_in
 {
   if (ix.nlist3_rows == 0) return cudaSuccess;
   int ncf = idx3(p + 1, 0), ncq = idx3(q + 1, 0);
-  int mb = std::max(1, std::min(8, NT / (p + q + 1)));
+  int mb = std::max(1, std::min(8, TRM_NT / (p + q + 1)));
+  if (2 * ncf > TRM_H * TRM_NT || mb < 2) return cudaErrorInvalidValue;
   size_t sh = (size_t)mb * ((p + q + 1) * (p + 2 * q + 1) + (q + 1) * (2 * q + 1)) * sizeof(double2) +
               (size_t)mb * (p + 4) * sizeof(double) + (size_t)mb * sizeof(int);
   if (ix.nlist3_rows < TR_SPLIT_BELOW) {
     cudaError_t e = cudaFuncSetAttribute(k_tr_m2qbxl<TR_CL>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
     if (e != cudaSuccess) return e;
-    k_tr_m2qbxl<TR_CL><<<dim3(ix.nlist3_rows * TR_CL, nrhs), NT, sh, st>>>(
+    k_tr_m2qbxl<TR_CL><<<dim3(ix.nlist3_rows * TR_CL, nrhs), TRM_NT, sh, st>>>(
         g, ix, p, q, ncf, ncq, nrhs, mb, cmp, locals, err);
   } else {
     cudaError_t e = cudaFuncSetAttribute(k_tr_m2qbxl<1>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
     if (e != cudaSuccess) return e;
-    k_tr_m2qbxl<1><<<dim3(ix.nlist3_rows, nrhs), NT, sh, st>>>(g, ix, p, q, ncf, ncq, nrhs, mb,
+    k_tr_m2qbxl<1><<<dim3(ix.nlist3_rows, nrhs), TRM_NT, sh, st>>>(g, ix, p, q, ncf, ncq, nrhs, mb,
                                                               cmp, locals, err);
   }
   return cudaGetLastError();
